@@ -1,0 +1,185 @@
+"""ctypes mirror of ``elmm_config`` / ``elmm_stats`` (include/elmm_gpu.h).
+
+The fields are the module globals of the reference that the hot path reads
+(src/parameters.f90, src/subgrid.f90:18, src/filters.f90:14), so a host that
+already parsed an ELMM configuration can fill the struct one to one.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+ABI_VERSION = 1
+
+# Boundary-condition codes of src/parameters.f90:249-250.
+BC_NOSLIP, BC_FREESLIP, BC_PERIODIC, BC_NEUMANN = 1, 2, 3, 5
+# Sides We, Ea, So, No, Bo, To (src/parameters.f90:193, zero-based here).
+WE, EA, SO, NO, BO, TO = range(6)
+
+PREC_FP64, PREC_MIXED = 0, 1
+
+FIELD_U, FIELD_V, FIELD_W, FIELD_PR, FIELD_VISCOSITY = 0, 1, 2, 3, 4
+FIELD_U2, FIELD_V2, FIELD_W2 = 5, 6, 7
+FIELD_USTAR, FIELD_VSTAR, FIELD_WSTAR, FIELD_PHI = 8, 9, 10, 11
+
+STATUS_NAMES = {
+    0: "ELMM_OK", 1: "ELMM_ERR_INVALID_CONFIG", 2: "ELMM_ERR_OOM", 3: "ELMM_ERR_NAN",
+    4: "ELMM_ERR_CUDA", 5: "ELMM_ERR_TIMEOUT", 6: "ELMM_ERR_INVALID_ARG", 7: "ELMM_ERR_ADMISSION",
+}
+
+
+class ElmmConfig(C.Structure):
+    _fields_ = [
+        ("abi_version", C.c_int32),
+        ("Prnx", C.c_int32), ("Prny", C.c_int32), ("Prnz", C.c_int32),
+        ("Btype", C.c_int32 * 6),
+        ("xmin", C.c_double), ("ymin", C.c_double), ("zmin", C.c_double),
+        ("dxmin", C.c_double), ("dymin", C.c_double), ("dzmin", C.c_double),
+        ("zW", C.POINTER(C.c_double)),
+        ("dt", C.c_double),
+        ("molecular_viscosity", C.c_double),
+        ("C_Smagorinsky", C.c_double),
+        ("filter_ratio", C.c_double),
+        ("sgstype", C.c_int32),
+        ("wallmodeltype", C.c_int32),
+        ("z0", C.c_double * 6),
+        ("enable_pr_gradient_x_uniform", C.c_int32),
+        ("enable_pr_gradient_y_uniform", C.c_int32),
+        ("pr_gradient_x", C.c_double), ("pr_gradient_y", C.c_double),
+        ("precision", C.c_int32),
+        ("max_refine_sweeps", C.c_int32),
+        ("refine_tol", C.c_double),
+        ("enable_CFL_check", C.c_int32),
+        ("device", C.c_int32),
+    ]
+
+
+class ElmmStats(C.Structure):
+    _fields_ = [
+        ("steps_done", C.c_int32),
+        ("nan_detected", C.c_int32),
+        ("time", C.c_double),
+        ("dt", C.c_double),
+        ("cfl", C.c_double),
+        ("max_div", C.c_double),
+        ("refine_sweeps", C.c_int32),
+        ("reserved", C.c_int32),
+        ("elapsed_ms", C.c_double),
+    ]
+
+
+@dataclass
+class Grid:
+    """Sizes of the staggered grid, src/initial.f90:871-896."""
+
+    Prnx: int
+    Prny: int
+    Prnz: int
+    btype: tuple
+
+    @property
+    def Unx(self):
+        return self.Prnx if self.btype[EA] == BC_PERIODIC else self.Prnx - 1
+
+    @property
+    def Uny(self):
+        return self.Prny
+
+    @property
+    def Unz(self):
+        return self.Prnz
+
+    @property
+    def Vnx(self):
+        return self.Prnx
+
+    @property
+    def Vny(self):
+        return self.Prny if self.btype[NO] == BC_PERIODIC else self.Prny - 1
+
+    @property
+    def Vnz(self):
+        return self.Prnz
+
+    @property
+    def Wnx(self):
+        return self.Prnx
+
+    @property
+    def Wny(self):
+        return self.Prny
+
+    @property
+    def Wnz(self):
+        return self.Prnz if self.btype[TO] == BC_PERIODIC else self.Prnz - 1
+
+    # host (Fortran-layout) shapes as numpy (k, j, i) arrays
+    def shape_u(self):
+        return (self.Unz + 6, self.Uny + 6, self.Unx + 6)
+
+    def shape_v(self):
+        return (self.Vnz + 6, self.Vny + 6, self.Vnx + 6)
+
+    def shape_w(self):
+        return (self.Wnz + 6, self.Wny + 6, self.Wnx + 6)
+
+    def shape_p(self):
+        return (self.Prnz + 4, self.Prny + 4, self.Prnx + 4)
+
+    def shape_rhs(self):
+        return (self.Prnz + 2, self.Prny + 2, self.Prnx + 2)
+
+    def cells(self):
+        return self.Prnx * self.Prny * self.Prnz
+
+
+def make_config(Prnx, Prny, Prnz, *, btype=(BC_PERIODIC, BC_PERIODIC, BC_PERIODIC, BC_PERIODIC,
+                                           BC_NOSLIP, BC_FREESLIP),
+                dx=1.0, dy=1.0, dz=1.0, dt=0.02, nu=1.0 / 70000, cs=0.1, sgstype=1,
+                wallmodeltype=None, z0=0.01, precision=PREC_FP64, zW=None,
+                pr_gradient_x=None, pr_gradient_y=None, max_refine_sweeps=0,
+                refine_tol=1e-6, cfl_check=0, device=0, origin=(0.0, 0.0, 0.0)):
+    """Builds an ElmmConfig.  The wall model defaults to on when an SGS model
+    is on (src/initial.f90:2782-2787).  ``zW`` (Prnz+1 values) selects the
+    stretched-z grid; the array is kept alive on the returned struct."""
+    c = ElmmConfig()
+    c.abi_version = ABI_VERSION
+    c.Prnx, c.Prny, c.Prnz = Prnx, Prny, Prnz
+    for s in range(6):
+        c.Btype[s] = btype[s]
+    c.xmin, c.ymin, c.zmin = origin
+    c.dxmin, c.dymin, c.dzmin = dx, dy, dz
+    if zW is not None:
+        zw = np.ascontiguousarray(zW, dtype=np.float64)
+        assert zw.shape == (Prnz + 1,)
+        c._zw_keepalive = zw
+        c.zW = zw.ctypes.data_as(C.POINTER(C.c_double))
+        c.zmin = float(zw[0])
+    c.dt = dt
+    c.molecular_viscosity = nu
+    c.C_Smagorinsky = cs
+    c.filter_ratio = 1.0
+    c.sgstype = sgstype
+    if wallmodeltype is None:
+        wallmodeltype = 1 if sgstype > 0 else 0
+    c.wallmodeltype = wallmodeltype
+    for s in range(6):
+        c.z0[s] = z0
+    if pr_gradient_x is not None:
+        c.enable_pr_gradient_x_uniform = 1
+        c.pr_gradient_x = pr_gradient_x
+    if pr_gradient_y is not None:
+        c.enable_pr_gradient_y_uniform = 1
+        c.pr_gradient_y = pr_gradient_y
+    c.precision = precision
+    c.max_refine_sweeps = max_refine_sweeps
+    c.refine_tol = refine_tol
+    c.enable_CFL_check = cfl_check
+    c.device = device
+    return c
+
+
+def grid_of(cfg: ElmmConfig) -> Grid:
+    return Grid(cfg.Prnx, cfg.Prny, cfg.Prnz, tuple(cfg.Btype[s] for s in range(6)))

@@ -1,0 +1,964 @@
+// elmm_api.cu -- host side of libelmm_gpu.so: the C-ABI of include/elmm_gpu.h.
+//
+// A single-domain handle is a batch of one; every stage kernel runs once per
+// batch over the domain table (see elmm_kernels.cuh).  One RK3 step of a
+// batch is captured once into a CUDA graph and replayed.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/elmm_gpu.h"
+#include "elmm_kernels2.cuh"
+
+using namespace elmm;
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string g_err;
+
+static int fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CU(call)                                                                              \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess) {                                                                  \
+      return fail(e_ == cudaErrorMemoryAllocation ? ELMM_ERR_OOM : ELMM_ERR_CUDA,             \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                        \
+    }                                                                                         \
+  } while (0)
+
+// RK3 coefficients, src/parameters.f90:317-320
+static const double kAlpha[3] = {4.0 / 15.0, 1.0 / 15.0, 1.0 / 6.0};
+static const double kBeta[3] = {8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};
+static const double kRho[3] = {0.0, -17.0 / 60.0, -5.0 / 12.0};
+
+static bool factorize(int n, FFTFactors &f) {
+  f.n = n;
+  f.nfac = 0;
+  int r = n;
+  for (int p : {4, 2, 3, 5}) {
+    while (r % p == 0) {
+      if (f.nfac >= kMaxFac) return false;
+      f.fac[f.nfac++] = p;
+      r /= p;
+    }
+  }
+  return r == 1;
+}
+
+static int round_up(int a, int b) { return (a + b - 1) / b * b; }
+
+// ------------------------------------------------------- host grid tables
+// The same formulas as src/initial.f90:4395-4480 (and the oracle).
+struct HostGrid {
+  int nx, ny, nz;
+  std::vector<double> zW, zPr, dzPr, dzW;  // index k + 2, k in [-2, nz+3] (dzW to nz+2)
+  std::vector<double> dxPr, dyPr;          // index i (1..n)
+  bool uniform_xy;
+  std::vector<double> width;               // index k (1..nz)
+  double dzmin;
+};
+
+static void make_grid(const elmm_config &c, HostGrid &g) {
+  int nx = c.Prnx, ny = c.Prny, nz = c.Prnz;
+  g.nx = nx; g.ny = ny; g.nz = nz;
+  std::vector<double> zW2(nz + 7);  // k in [-3, nz+3] -> k + 3
+  auto Z = [&](int k) -> double & { return zW2[k + 3]; };
+  if (c.zW) {
+    for (int k = 0; k <= nz; k++) Z(k) = c.zW[k];
+    if (c.Btype[ELMM_BO] == ELMM_BC_PERIODIC)
+      for (int j = -1; j >= -3; j--) Z(j) = Z(0) - (Z(nz - 1) - Z(nz - 1 + j));
+    else
+      for (int j = -1; j >= -3; j--) Z(j) = Z(0) - (Z(-j) - Z(0));
+    if (c.Btype[ELMM_TO] == ELMM_BC_PERIODIC)
+      for (int j = nz + 1; j <= nz + 3; j++) Z(j) = Z(nz - 1) + (Z(j - nz + 1) - Z(0));
+    else
+      for (int j = nz + 1; j <= nz + 3; j++) Z(j) = Z(nz - 1) + (Z(nz - 1) - Z(nz - 1 - (j - nz + 1)));
+  } else {
+    for (int k = -3; k <= nz + 3; k++) Z(k) = k * c.dzmin + c.zmin;
+  }
+  g.zW.assign(nz + 6, 0.0); g.zPr.assign(nz + 6, 0.0); g.dzPr.assign(nz + 6, 0.0); g.dzW.assign(nz + 6, 0.0);
+  for (int k = -2; k <= nz + 3; k++) {
+    g.zW[k + 2] = Z(k);
+    g.zPr[k + 2] = (Z(k - 1) + Z(k)) / 2.0;
+    g.dzPr[k + 2] = Z(k) - Z(k - 1);
+  }
+  for (int k = -2; k <= nz + 2; k++) g.dzW[k + 2] = g.zPr[k + 1 + 2] - g.zPr[k + 2];
+  g.dzmin = c.dzmin;
+  if (c.zW) {
+    double m = g.dzPr[0];
+    for (int k = -2; k <= nz + 3; k++) m = std::min(m, g.dzPr[k + 2]);
+    g.dzmin = m;
+  }
+  g.dxPr.assign(nx + 1, 0.0); g.dyPr.assign(ny + 1, 0.0);
+  for (int i = 1; i <= nx; i++) g.dxPr[i] = (i * c.dxmin + c.xmin) - ((i - 1) * c.dxmin + c.xmin);
+  for (int j = 1; j <= ny; j++) g.dyPr[j] = (j * c.dymin + c.ymin) - ((j - 1) * c.dymin + c.ymin);
+  g.uniform_xy = true;
+  for (int i = 2; i <= nx; i++) g.uniform_xy &= g.dxPr[i] == g.dxPr[1];
+  for (int j = 2; j <= ny; j++) g.uniform_xy &= g.dyPr[j] == g.dyPr[1];
+  g.width.assign(nz + 1, 0.0);
+  for (int k = 1; k <= nz; k++)
+    g.width[k] = c.filter_ratio * std::pow(g.dxPr[1] * g.dyPr[1] * g.dzPr[k + 2], 1.0 / 3.0);
+}
+
+static int check_config(const elmm_config &c) {
+  if (c.abi_version != ELMM_ABI_VERSION) return fail(ELMM_ERR_INVALID_CONFIG, "abi_version mismatch");
+  if (c.Prnx < 4 || c.Prny < 4 || c.Prnz < 4) return fail(ELMM_ERR_INVALID_CONFIG, "grid must be at least 4 cells per axis");
+  if ((long long)c.Prnx * c.Prny * c.Prnz > (1LL << 31)) return fail(ELMM_ERR_INVALID_CONFIG, "grid too large");
+  for (int s = 0; s < 6; s++) {
+    int b = c.Btype[s];
+    if (b != ELMM_BC_NOSLIP && b != ELMM_BC_FREESLIP && b != ELMM_BC_PERIODIC && b != ELMM_BC_NEUMANN)
+      return fail(ELMM_ERR_INVALID_CONFIG, "unsupported boundary condition code " + std::to_string(b));
+  }
+  for (int a = 0; a < 3; a++)
+    if ((c.Btype[2 * a] == ELMM_BC_PERIODIC) != (c.Btype[2 * a + 1] == ELMM_BC_PERIODIC))
+      return fail(ELMM_ERR_INVALID_CONFIG, "periodic boundary conditions must be set on both sides of an axis");
+  if (c.Btype[ELMM_WE] != ELMM_BC_PERIODIC || c.Btype[ELMM_SO] != ELMM_BC_PERIODIC)
+    return fail(ELMM_ERR_INVALID_CONFIG, "the FFT Poisson solver needs periodic x and y");
+  if (c.zW && c.Btype[ELMM_BO] == ELMM_BC_PERIODIC)
+    return fail(ELMM_ERR_INVALID_CONFIG, "periodic z needs a uniform z grid");
+  FFTFactors f;
+  if (!factorize(c.Prnx, f) || !factorize(c.Prny, f))
+    return fail(ELMM_ERR_INVALID_CONFIG, "Prnx and Prny must factor into 2, 3 and 5");
+  if (c.Prnx > 4096 || c.Prny > 4096 || c.Prnz > 2048) return fail(ELMM_ERR_INVALID_CONFIG, "axis too long");
+  if (!(c.dxmin > 0 && c.dymin > 0 && c.dzmin > 0 && c.dt > 0))
+    return fail(ELMM_ERR_INVALID_CONFIG, "spacings and dt must be positive");
+  if (c.precision != ELMM_PREC_FP64 && c.precision != ELMM_PREC_MIXED)
+    return fail(ELMM_ERR_INVALID_CONFIG, "unknown precision");
+  if (c.max_refine_sweeps < 0 || c.max_refine_sweeps > 3) return fail(ELMM_ERR_INVALID_CONFIG, "max_refine_sweeps in 0..3");
+  if (c.wallmodeltype > 0 && c.molecular_viscosity <= 0) {
+    for (int s = 0; s < 6; s++)
+      if (c.Btype[s] == ELMM_BC_NOSLIP && !(c.z0[s] > 0))
+        return fail(ELMM_ERR_INVALID_CONFIG, "The wall model requires positive viscosity or roughness length.");
+  }
+  if (c.wallmodeltype > 0)
+    for (int s = 0; s < 6; s++)
+      if (c.Btype[s] == ELMM_BC_NOSLIP && !(c.z0[s] > 0))
+        return fail(ELMM_ERR_INVALID_CONFIG, "only the rough-wall (z0 > 0) wall model is implemented");
+  return ELMM_OK;
+}
+
+// ---------------------------------------------------------------- launches
+struct LaunchSet {
+  int *starts = nullptr;  // device
+  int total = 0;
+  int nd = 0;
+  Launch l() const { return Launch{starts, nd, total}; }
+};
+
+enum { LK_CELLS = 0, LK_BOX, LK_ROWS, LK_YCOLS, LK_TRI, LK_N };
+
+// -------------------------------------------------------------------- batch
+template <typename T>
+struct BatchT {
+  typedef typename Vec2<T>::type T2;
+  int nd = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr, side = nullptr;
+  std::vector<elmm_config> cfg;
+  std::vector<HostGrid> grid;
+  std::vector<Dom<T>> hdom;     // host copies of the descriptors
+  std::vector<PoisPlan> hplan;
+  Dom<T> *ddom = nullptr;       // device descriptors
+  PoisPlan *dplan = nullptr;
+  std::vector<void *> allocs;
+  LaunchSet ls[LK_N];
+  size_t smem_x = 0, smem_y = 0, smem_tri = 0;
+  int grid_cap[16];
+  // host-layout staging (double), max over domains of the largest host array
+  double *dstage = nullptr;
+  size_t stage_elems = 0;
+  std::vector<double *> pr_image;  // per domain: last host Pr image (device)
+  int *dbad = nullptr;
+  cudaGraphExec_t step_exec = nullptr;
+  bool step_has_cfl = false;
+  double time = 0;
+  // frames
+  double *frame_host = nullptr;    // pinned
+  double *frame_dev = nullptr;
+  size_t frame_elems = 0;
+  cudaEvent_t ev_ready = nullptr, ev_packed = nullptr, ev_done = nullptr;
+  bool frame_pending = false;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  long long cells = 0;
+
+  ~BatchT() { release(); }
+
+  void release() {
+    if (step_exec) cudaGraphExecDestroy(step_exec);
+    step_exec = nullptr;
+    for (void *p : allocs) cudaFree(p);
+    allocs.clear();
+    if (frame_host) cudaFreeHost(frame_host);
+    frame_host = nullptr;
+    for (cudaEvent_t *e : {&ev_ready, &ev_packed, &ev_done, &t0, &t1})
+      if (*e) { cudaEventDestroy(*e); *e = nullptr; }
+    if (stream) cudaStreamDestroy(stream);
+    if (side) cudaStreamDestroy(side);
+    stream = side = nullptr;
+  }
+
+  int dalloc(void **p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, std::max<size_t>(bytes, 256));
+    if (e != cudaSuccess) return fail(e == cudaErrorMemoryAllocation ? ELMM_ERR_OOM : ELMM_ERR_CUDA,
+                                      std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    allocs.push_back(*p);
+    return cudaMemset(*p, 0, std::max<size_t>(bytes, 256)) == cudaSuccess ? ELMM_OK : fail(ELMM_ERR_CUDA, "cudaMemset");
+  }
+
+  template <typename X>
+  int upload_table(const X **dst, const std::vector<X> &v) {
+    void *p;
+    int r = dalloc(&p, v.size() * sizeof(X));
+    if (r) return r;
+    CU(cudaMemcpy(p, v.data(), v.size() * sizeof(X), cudaMemcpyHostToDevice));
+    *dst = (const X *)p;
+    return ELMM_OK;
+  }
+
+  int init(const elmm_config *cfgs, int n) {
+    nd = n;
+    device = cfgs[0].device;
+    for (int d = 0; d < n; d++) {
+      int r = check_config(cfgs[d]);
+      if (r) return r;
+      if (cfgs[d].device != device) return fail(ELMM_ERR_INVALID_CONFIG, "all domains of a batch share one device");
+      if (cfgs[d].precision != cfgs[0].precision) return fail(ELMM_ERR_INVALID_CONFIG, "all domains of a batch share one precision");
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device) return fail(ELMM_ERR_CUDA, "no CUDA device");
+    CU(cudaSetDevice(device));
+    CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    CU(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    CU(cudaEventCreateWithFlags(&ev_ready, cudaEventDisableTiming));
+    CU(cudaEventCreateWithFlags(&ev_packed, cudaEventDisableTiming));
+    CU(cudaEventCreateWithFlags(&ev_done, cudaEventDisableTiming));
+    CU(cudaEventCreate(&t0));
+    CU(cudaEventCreate(&t1));
+    cfg.assign(cfgs, cfgs + n);
+    grid.resize(n);
+    hdom.resize(n);
+    hplan.resize(n);
+    pr_image.assign(n, nullptr);
+    for (int d = 0; d < n; d++) {
+      int r = init_domain(d);
+      if (r) return r;
+    }
+    void *p;
+    int r = dalloc(&p, sizeof(Dom<T>) * n);
+    if (r) return r;
+    ddom = (Dom<T> *)p;
+    CU(cudaMemcpy(ddom, hdom.data(), sizeof(Dom<T>) * n, cudaMemcpyHostToDevice));
+    r = dalloc(&p, sizeof(PoisPlan) * n);
+    if (r) return r;
+    dplan = (PoisPlan *)p;
+    CU(cudaMemcpy(dplan, hplan.data(), sizeof(PoisPlan) * n, cudaMemcpyHostToDevice));
+    r = dalloc((void **)&dbad, sizeof(int));
+    if (r) return r;
+    // launch maps
+    for (int k = 0; k < LK_N; k++) {
+      std::vector<int> st(n + 1, 0);
+      for (int d = 0; d < n; d++) st[d + 1] = st[d] + tiles(k, hdom[d]);
+      ls[k].nd = n;
+      ls[k].total = st[n];
+      r = dalloc((void **)&ls[k].starts, sizeof(int) * (n + 1));
+      if (r) return r;
+      CU(cudaMemcpy(ls[k].starts, st.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+    }
+    int maxnx = 0, maxny = 0, maxnz = 0, anyzper = 0;
+    for (auto &h : hdom) { maxnx = std::max(maxnx, h.nx); maxny = std::max(maxny, h.ny); maxnz = std::max(maxnz, h.nz); anyzper |= h.zper; }
+    smem_x = sizeof(T2) * 2 * (kRowsX / 2) * maxnx;
+    smem_y = sizeof(T2) * 2 * TyOf<T>::v * maxny;
+    smem_tri = sizeof(double) * kTriThreads * maxnz * (anyzper ? 2 : 1);
+    CU(cudaFuncSetAttribute(k_fftx_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_x));
+    CU(cudaFuncSetAttribute(k_fftx_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_x));
+    CU(cudaFuncSetAttribute(k_ffty<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_y));
+    CU(cudaFuncSetAttribute(k_tri<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tri));
+    int nsm = 0;
+    CU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+    auto cap = [&](const void *f, int threads, size_t sm) {
+      int b = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, threads, sm) != cudaSuccess || b < 1) b = 1;
+      return b * nsm;
+    };
+    grid_cap[0] = cap((const void *)k_sgs<T>, TX * TY, 0);
+    grid_cap[1] = cap((const void *)k_momentum<T>, TX * TY, 0);
+    grid_cap[2] = cap((const void *)k_fftx_fwd<T>, 128, smem_x);
+    grid_cap[3] = cap((const void *)k_ffty<T>, 128, smem_y);
+    grid_cap[4] = cap((const void *)k_tri<T>, kTriThreads, smem_tri);
+    grid_cap[5] = cap((const void *)k_fftx_inv<T>, 128, smem_x);
+    grid_cap[6] = cap((const void *)k_project<T>, TX * TY, 0);
+    grid_cap[7] = cap((const void *)k_divmax<T>, TX * TY, 0);
+    grid_cap[8] = cap((const void *)k_cfl<T>, TX * TY, 0);
+    // staging for host-layout copies
+    stage_elems = 0;
+    for (int d = 0; d < n; d++) {
+      const Dom<T> &h = hdom[d];
+      size_t e = (size_t)(h.nx + 6) * (h.ny + 6) * (h.nz + 6);
+      stage_elems = std::max(stage_elems, e);
+    }
+    r = dalloc((void **)&dstage, stage_elems * sizeof(double));
+    if (r) return r;
+    for (int d = 0; d < n; d++) cells += (long long)hdom[d].nx * hdom[d].ny * hdom[d].nz;
+    return ELMM_OK;
+  }
+
+  static int tiles(int kind, const Dom<T> &h) {
+    int ntx = (h.nx + TX - 1) / TX, nty = (h.ny + TY - 1) / TY;
+    switch (kind) {
+      case LK_CELLS: return ntx * nty * h.nz;
+      case LK_BOX: return ((h.nx + 2 + TX - 1) / TX) * ((h.ny + 2 + TY - 1) / TY) * (h.nz + 2);
+      case LK_ROWS: return (h.ny * h.nz + kRowsX - 1) / kRowsX;
+      case LK_YCOLS: return ((h.nxh + TyOf<T>::v - 1) / TyOf<T>::v) * h.nz;
+      default: return (h.ny * h.spitch + kTriThreads - 1) / kTriThreads;
+    }
+  }
+
+  int init_domain(int di) {
+    const elmm_config &c = cfg[di];
+    HostGrid &g = grid[di];
+    make_grid(c, g);
+    Dom<T> h;
+    memset(&h, 0, sizeof(h));
+    h.nx = c.Prnx; h.ny = c.Prny; h.nz = c.Prnz;
+    const int *b = c.Btype;
+    int Unx = b[ELMM_EA] == ELMM_BC_PERIODIC ? h.nx : h.nx - 1;
+    int Vny = b[ELMM_NO] == ELMM_BC_PERIODIC ? h.ny : h.ny - 1;
+    int Wnz = b[ELMM_TO] == ELMM_BC_PERIODIC ? h.nz : h.nz - 1;
+    int ext[3][3] = {{Unx, h.ny, h.nz}, {h.nx, Vny, h.nz}, {h.nx, h.ny, Wnz}};
+    memcpy(h.ext, ext, sizeof(ext));
+    h.aln = 128 / (int)sizeof(T);
+    h.pitch = round_up(h.aln + h.nx + 1, h.aln);
+    h.plane = (long long)h.pitch * (h.ny + 2);
+    for (int s = 0; s < 6; s++) h.bt[s] = b[s];
+    h.vz = c.zW ? 1 : 0;
+    for (int s = 0; s < 6; s++) h.wall[s] = (c.wallmodeltype > 0 && b[s] == ELMM_BC_NOSLIP) ? 1 : 0;
+    h.sgs = c.sgstype == 1;
+    h.prgx_on = c.enable_pr_gradient_x_uniform; h.prgy_on = c.enable_pr_gradient_y_uniform;
+    h.prgx = c.pr_gradient_x; h.prgy = c.pr_gradient_y;
+    h.dx = c.dxmin; h.dy = c.dymin; h.dz = g.dzmin;
+    h.xmin = c.xmin; h.ymin = c.ymin;
+    h.dt = c.dt;
+    h.nu_mol = c.molecular_viscosity;
+    h.cs = c.C_Smagorinsky;
+    if (!g.uniform_xy) return fail(ELMM_ERR_INVALID_CONFIG, "dxPr/dyPr must be uniform");
+    size_t box = (size_t)h.plane * (h.nz + 2);
+    T **fields[12] = {&h.U, &h.V, &h.W, &h.U2, &h.V2, &h.W2, &h.Us, &h.Vs, &h.Ws, &h.P, &h.nu, &h.Phi};
+    for (T **f : fields) {
+      int r = dalloc((void **)f, box * sizeof(T));
+      if (r) return r;
+    }
+    h.nxh = h.nx / 2 + 1;
+    h.spitch = round_up(h.nxh, TyOf<T>::v);
+    int r = dalloc((void **)&h.S, (size_t)h.nz * h.ny * h.spitch * sizeof(T2));
+    if (r) return r;
+    // FFT
+    PoisPlan pl;
+    factorize(h.nx, pl.fx);
+    factorize(h.ny, pl.fy);
+    hplan[di] = pl;
+    auto twiddles = [](int n) {
+      std::vector<T2> w(n);
+      for (int m = 0; m < n; m++) {
+        double a = -2.0 * M_PI * (double)m / (double)n;
+        w[m].x = (T)std::cos(a);
+        w[m].y = (T)std::sin(a);
+      }
+      return w;
+    };
+    if ((r = upload_table(&h.twx, twiddles(h.nx)))) return r;
+    if ((r = upload_table(&h.twy, twiddles(h.ny)))) return r;
+    std::vector<double> lx(h.nx), ly(h.ny);
+    double rx = 1 / (c.dxmin * c.dxmin), ry = 1 / (c.dymin * c.dymin);
+    for (int m = 0; m < h.nx; m++) { double s = std::sin(M_PI * m / h.nx); lx[m] = -4.0 * s * s * rx; }
+    for (int m = 0; m < h.ny; m++) { double s = std::sin(M_PI * m / h.ny); ly[m] = -4.0 * s * s * ry; }
+    if ((r = upload_table(&h.lamx, lx))) return r;
+    if ((r = upload_table(&h.lamy, ly))) return r;
+    h.zper = b[ELMM_BO] == ELMM_BC_PERIODIC;
+    std::vector<double> Ab(h.nz + 2, 0.0), At(h.nz + 2, 0.0), dzc(h.nz + 2, 0.0), dzf(h.nz + 2, 0.0);
+    auto zP = [&](int k) { return g.zPr[k + 2]; };
+    auto zWf = [&](int k) { return g.zW[k + 2]; };
+    for (int k = 1; k <= h.nz; k++) {
+      Ab[k] = 1 / ((zP(k) - zP(k - 1)) * (zWf(k) - zWf(k - 1)));
+      At[k] = 1 / ((zP(k + 1) - zP(k)) * (zWf(k) - zWf(k - 1)));
+      dzc[k] = zWf(k) - zWf(k - 1);
+      dzf[k] = zP(k + 1) - zP(k);
+    }
+    if (!h.zper) { Ab[1] = 0; At[h.nz] = 0; }
+    if ((r = upload_table(&h.Ab, Ab))) return r;
+    if ((r = upload_table(&h.At, At))) return r;
+    if ((r = upload_table(&h.dzc, dzc))) return r;
+    if ((r = upload_table(&h.dzf, dzf))) return r;
+    if ((r = upload_table(&h.zPr, g.zPr))) return r;
+    if ((r = upload_table(&h.dzPr, g.dzPr))) return r;
+    if ((r = upload_table(&h.zW, g.zW))) return r;
+    if ((r = upload_table(&h.dzW, g.dzW))) return r;
+    if ((r = upload_table(&h.width, g.width))) return r;
+    // wall-model planes
+    for (int s = 0; s < 6; s++) h.z0[s] = c.z0[s];
+    for (int comp = 0; comp < 3; comp++)
+      for (int s = 0; s < 6; s++) {
+        if (!h.wall[s]) continue;
+        int axis = s >> 1;
+        int a0 = axis == 0 ? 1 : 0, a1 = axis == 2 ? 1 : 2;
+        size_t np = (size_t)ext[comp][a0] * ext[comp][a1];
+        int f = comp * 6 + s;
+        if ((r = dalloc((void **)&h.wm_fluxp[f], np * sizeof(T)))) return r;
+        if ((r = dalloc((void **)&h.wm_fluxm[f], np * sizeof(T)))) return r;
+        if ((r = dalloc((void **)&h.wm_ustar[f], np * sizeof(double)))) return r;
+        std::vector<double> ones(np, 1.0);  // WMPointUVW%ustar = 1 initially (wallmodels.f90:80)
+        CU(cudaMemcpy(h.wm_ustar[f], ones.data(), np * sizeof(double), cudaMemcpyHostToDevice));
+      }
+    if ((r = dalloc((void **)&h.prm, sizeof(double)))) return r;
+    h.nprpart = ((h.nx + TX - 1) / TX) * ((h.ny + TY - 1) / TY);
+    if ((r = dalloc((void **)&h.prpart, sizeof(double) * h.nprpart))) return r;
+    if ((r = dalloc((void **)&h.maxdiv_bits, sizeof(unsigned long long)))) return r;
+    if ((r = dalloc((void **)&h.cfl_bits, sizeof(unsigned long long)))) return r;
+    if ((r = dalloc((void **)&h.flags, 4 * sizeof(int)))) return r;
+    size_t pe = (size_t)(h.nx + 4) * (h.ny + 4) * (h.nz + 4);
+    if ((r = dalloc((void **)&pr_image[di], pe * sizeof(double)))) return r;
+    // viscosity starts at the molecular value (src/initial.f90:4275)
+    std::vector<T> nuv(box, (T)c.molecular_viscosity);
+    CU(cudaMemcpy(h.nu, nuv.data(), box * sizeof(T), cudaMemcpyHostToDevice));
+    hdom[di] = h;
+    return ELMM_OK;
+  }
+
+  int gsz(int which, int total) const { return std::max(1, std::min(total, grid_cap[which])); }
+
+  // ------------------------------------------------------------ stages
+  int launch_sgs() {
+    k_sgs<T><<<gsz(0, ls[LK_BOX].total), TX * TY, 0, stream>>>(ddom, ls[LK_BOX].l());
+    return ELMM_OK;
+  }
+  int launch_momentum(int stage) {
+    StageCoef sc{kRho[stage - 1], kBeta[stage - 1], 2 * kAlpha[stage - 1], stage};
+    k_momentum<T><<<gsz(1, ls[LK_CELLS].total), TX * TY, 0, stream>>>(ddom, ls[LK_CELLS].l(), sc);
+    return ELMM_OK;
+  }
+  // PressureCorrection on U2 (in_place = 0) or on U itself (initial projection)
+  int launch_projection(double coef_alpha2, int use_dt, int in_place) {
+    k_fftx_fwd<T><<<gsz(2, ls[LK_ROWS].total), 128, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan, coef_alpha2,
+                                                                        use_dt, nullptr);
+    k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), 128, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, 0);
+    k_tri<T><<<gsz(4, ls[LK_TRI].total), kTriThreads, smem_tri, stream>>>(ddom, ls[LK_TRI].l());
+    k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), 128, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, 1);
+    k_fftx_inv<T><<<gsz(5, ls[LK_ROWS].total), 128, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan);
+    k_project<T><<<gsz(6, ls[LK_CELLS].total), TX * TY, 0, stream>>>(ddom, ls[LK_CELLS].l(), coef_alpha2, use_dt,
+                                                                     in_place);
+    k_prref<T><<<std::min(nd, 1024), 256, 0, stream>>>(ddom, nd);
+    return ELMM_OK;
+  }
+  int launch_divmax() {
+    for (int d = 0; d < nd; d++) cudaMemsetAsync(hdom[d].maxdiv_bits, 0, sizeof(unsigned long long), stream);
+    k_divmax<T><<<gsz(7, ls[LK_CELLS].total), TX * TY, 0, stream>>>(ddom, ls[LK_CELLS].l());
+    return ELMM_OK;
+  }
+  int launch_cfl() {
+    for (int d = 0; d < nd; d++) cudaMemsetAsync(hdom[d].cfl_bits, 0, sizeof(unsigned long long), stream);
+    k_cfl<T><<<gsz(8, ls[LK_CELLS].total), TX * TY, 0, stream>>>(ddom, ls[LK_CELLS].l());
+    return ELMM_OK;
+  }
+  void swap_state() {
+    // U <-> U2 after the projection wrote U directly: nothing to swap; the
+    // projection writes the new velocity into U (exchange_alloc in tsteps.f90:211-213)
+  }
+  int run_stage(int stage, int stop) {
+    launch_sgs();
+    if (stop == 1) return ELMM_OK;
+    launch_momentum(stage);
+    if (stop == 2) return ELMM_OK;
+    launch_projection(2 * kAlpha[stage - 1], 1, 0);
+    return ELMM_OK;
+  }
+  int enqueue_step(bool cfl, bool div) {
+    if (cfl) launch_cfl();
+    for (int s = 1; s <= 3; s++) run_stage(s, 3);
+    if (div) launch_divmax();
+    return ELMM_OK;
+  }
+
+  int step(int nsteps, elmm_stats *st) {
+    CU(cudaSetDevice(device));
+    if (frame_pending) CU(cudaStreamWaitEvent(stream, ev_packed, 0));
+    bool cfl = false;
+    for (auto &c : cfg) cfl |= c.enable_CFL_check != 0;
+    if (!step_exec || step_has_cfl != cfl) {
+      if (step_exec) { cudaGraphExecDestroy(step_exec); step_exec = nullptr; }
+      cudaGraph_t g;
+      CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      enqueue_step(cfl, true);
+      CU(cudaStreamEndCapture(stream, &g));
+      cudaError_t e = cudaGraphInstantiate(&step_exec, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return fail(ELMM_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+      step_has_cfl = cfl;
+    }
+    CU(cudaEventRecord(t0, stream));
+    for (int s = 0; s < nsteps; s++) CU(cudaGraphLaunch(step_exec, stream));
+    CU(cudaEventRecord(t1, stream));
+    CU(cudaStreamSynchronize(stream));
+    CU(cudaGetLastError());
+    time += nsteps * cfg[0].dt;
+    return fill_stats(st, nsteps);
+  }
+
+  int fill_stats(elmm_stats *st, int nsteps) {
+    double md = 0, cf = 0;
+    for (int d = 0; d < nd; d++) {
+      unsigned long long b1 = 0, b2 = 0;
+      CU(cudaMemcpy(&b1, hdom[d].maxdiv_bits, sizeof(b1), cudaMemcpyDeviceToHost));
+      CU(cudaMemcpy(&b2, hdom[d].cfl_bits, sizeof(b2), cudaMemcpyDeviceToHost));
+      double a, c2;
+      memcpy(&a, &b1, 8);
+      memcpy(&c2, &b2, 8);
+      if (!(a <= md)) md = a;
+      c2 = c2 * cfg[d].dt;
+      if (!(c2 <= cf)) cf = c2;
+    }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, t0, t1);
+    if (st) {
+      memset(st, 0, sizeof(*st));
+      st->steps_done = nsteps;
+      st->time = time;
+      st->dt = cfg[0].dt;
+      st->cfl = cf;
+      st->max_div = md;
+      st->nan_detected = !(md == md) || !(cf == cf);
+      st->elapsed_ms = ms;
+    }
+    if (!(md == md)) return fail(ELMM_ERR_NAN, "NaN in the velocity field");
+    return ELMM_OK;
+  }
+
+  int project(double coef, elmm_stats *st) {
+    CU(cudaSetDevice(device));
+    if (frame_pending) CU(cudaStreamWaitEvent(stream, ev_packed, 0));
+    CU(cudaEventRecord(t0, stream));
+    // the fused divergence of k_fftx_fwd reads U2: make U2 the current field
+    for (int d = 0; d < nd; d++) {
+      size_t box = (size_t)hdom[d].plane * (hdom[d].nz + 2) * sizeof(T);
+      CU(cudaMemcpyAsync(hdom[d].U2, hdom[d].U, box, cudaMemcpyDeviceToDevice, stream));
+      CU(cudaMemcpyAsync(hdom[d].V2, hdom[d].V, box, cudaMemcpyDeviceToDevice, stream));
+      CU(cudaMemcpyAsync(hdom[d].W2, hdom[d].W, box, cudaMemcpyDeviceToDevice, stream));
+    }
+    launch_projection(coef, 0, 0);
+    launch_divmax();
+    CU(cudaEventRecord(t1, stream));
+    CU(cudaStreamSynchronize(stream));
+    CU(cudaGetLastError());
+    return fill_stats(st, 0);
+  }
+
+  // --------------------------------------------------------- host copies
+  HostBox hbox_vel(int d, int comp) const {
+    const Dom<T> &h = hdom[d];
+    return HostBox{-2, h.ext[comp][0] + 6, h.ext[comp][1] + 6, h.ext[comp][2] + 6};
+  }
+  HostBox hbox_p(int d) const {
+    const Dom<T> &h = hdom[d];
+    return HostBox{-1, h.nx + 4, h.ny + 4, h.nz + 4};
+  }
+
+  int upload(int d, const double *U, const double *V, const double *W, const double *Pr) {
+    if (d < 0 || d >= nd) return fail(ELMM_ERR_INVALID_ARG, "domain index");
+    if (!U || !V || !W) return fail(ELMM_ERR_INVALID_ARG, "NULL velocity array");
+    CU(cudaSetDevice(device));
+    if (frame_pending) CU(cudaStreamWaitEvent(stream, ev_packed, 0));
+    const Dom<T> &h = hdom[d];
+    CU(cudaMemsetAsync(dbad, 0, sizeof(int), stream));
+    const double *src[3] = {U, V, W};
+    T *dst[3] = {h.U, h.V, h.W};
+    for (int c = 0; c < 3; c++) {
+      HostBox hb = hbox_vel(d, c);
+      size_t n = (size_t)hb.n0 * hb.n1 * hb.n2;
+      CU(cudaMemcpyAsync(dstage, src[c], n * sizeof(double), cudaMemcpyHostToDevice, stream));
+      k_unpack<T><<<256, 256, 0, stream>>>(ddom + d, dst[c], dstage, hb, h.ext[c][0], h.ext[c][1], h.ext[c][2], dbad);
+      k_halo_vel<T><<<256, 256, 0, stream>>>(ddom + d, c);
+    }
+    HostBox hp = hbox_p(d);
+    size_t np = (size_t)hp.n0 * hp.n1 * hp.n2;
+    if (Pr) {
+      CU(cudaMemcpyAsync(pr_image[d], Pr, np * sizeof(double), cudaMemcpyHostToDevice, stream));
+      k_unpack<T><<<256, 256, 0, stream>>>(ddom + d, h.P, pr_image[d], hp, h.nx, h.ny, h.nz, dbad);
+    } else {
+      CU(cudaMemsetAsync(pr_image[d], 0, np * sizeof(double), stream));
+      CU(cudaMemsetAsync(h.P, 0, (size_t)h.plane * (h.nz + 2) * sizeof(T), stream));
+    }
+    k_halo_p<T><<<256, 256, 0, stream>>>(ddom + d);
+    CU(cudaMemsetAsync(h.prm, 0, sizeof(double), stream));
+    int bad = 0;
+    CU(cudaMemcpyAsync(&bad, dbad, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    CU(cudaStreamSynchronize(stream));
+    CU(cudaGetLastError());
+    if (bad) return fail(ELMM_ERR_NAN, "non-finite value in the uploaded state");
+    return ELMM_OK;
+  }
+
+  // pack one field into dst (device, host layout); returns elements
+  size_t pack(int d, int field, double *dst, cudaStream_t s) {
+    const Dom<T> &h = hdom[d];
+    const T *F;
+    switch (field) {
+      case ELMM_FIELD_U: case ELMM_FIELD_V: case ELMM_FIELD_W:
+      case ELMM_FIELD_U2: case ELMM_FIELD_V2: case ELMM_FIELD_W2: {
+        int comp = (field == ELMM_FIELD_U || field == ELMM_FIELD_U2) ? 0 : (field == ELMM_FIELD_V || field == ELMM_FIELD_V2) ? 1 : 2;
+        F = field <= ELMM_FIELD_W ? (comp == 0 ? h.U : comp == 1 ? h.V : h.W) : (comp == 0 ? h.U2 : comp == 1 ? h.V2 : h.W2);
+        HostBox hb = hbox_vel(d, comp);
+        k_pack_vel<T><<<256, 256, 0, s>>>(ddom + d, F, comp, dst, hb);
+        return (size_t)hb.n0 * hb.n1 * hb.n2;
+      }
+      case ELMM_FIELD_USTAR: case ELMM_FIELD_VSTAR: case ELMM_FIELD_WSTAR: {
+        int comp = field - ELMM_FIELD_USTAR;
+        F = comp == 0 ? h.Us : comp == 1 ? h.Vs : h.Ws;
+        HostBox hb = hbox_vel(d, comp);
+        size_t n = (size_t)hb.n0 * hb.n1 * hb.n2;
+        cudaMemsetAsync(dst, 0, n * sizeof(double), s);
+        k_pack_scalar<T><<<256, 256, 0, s>>>(ddom + d, F, dst, hb, 0, 0, h.ext[comp][0], h.ext[comp][1], h.ext[comp][2]);
+        return n;
+      }
+      case ELMM_FIELD_PR: {
+        HostBox hb = hbox_p(d);
+        size_t n = (size_t)hb.n0 * hb.n1 * hb.n2;
+        cudaMemcpyAsync(dst, pr_image[d], n * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        k_pack_scalar<T><<<256, 256, 0, s>>>(ddom + d, h.P, dst, hb, 1, 1, h.nx, h.ny, h.nz);
+        return n;
+      }
+      case ELMM_FIELD_VISCOSITY: case ELMM_FIELD_PHI: {
+        HostBox hb = hbox_p(d);
+        size_t n = (size_t)hb.n0 * hb.n1 * hb.n2;
+        cudaMemsetAsync(dst, 0, n * sizeof(double), s);
+        k_pack_scalar<T><<<256, 256, 0, s>>>(ddom + d, field == ELMM_FIELD_PHI ? h.Phi : h.nu, dst, hb,
+                                              field == ELMM_FIELD_PHI ? 2 : 3, 0, h.nx, h.ny, h.nz);
+        return n;
+      }
+    }
+    return 0;
+  }
+
+  int download_field(int d, int field, double *host) {
+    if (d < 0 || d >= nd) return fail(ELMM_ERR_INVALID_ARG, "domain index");
+    if (field < 0 || field > ELMM_FIELD_PHI) return fail(ELMM_ERR_INVALID_ARG, "field id");
+    if (!host) return fail(ELMM_ERR_INVALID_ARG, "NULL host array");
+    CU(cudaSetDevice(device));
+    size_t n = pack(d, field, dstage, stream);
+    CU(cudaMemcpyAsync(host, dstage, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    CU(cudaStreamSynchronize(stream));
+    CU(cudaGetLastError());
+    return ELMM_OK;
+  }
+
+  int download(int d, double *U, double *V, double *W, double *Pr) {
+    double *dst[4] = {U, V, W, Pr};
+    for (int f = 0; f < 4; f++)
+      if (dst[f]) {
+        int r = download_field(d, f, dst[f]);
+        if (r) return r;
+      }
+    return ELMM_OK;
+  }
+
+  // ----------------------------------------------------- async frames
+  size_t frame_offsets(int d, size_t off[5]) {
+    off[0] = 0;
+    for (int c = 0; c < 3; c++) {
+      HostBox hb = hbox_vel(d, c);
+      off[c + 1] = off[c] + (size_t)hb.n0 * hb.n1 * hb.n2;
+    }
+    HostBox hp = hbox_p(d);
+    off[4] = off[3] + (size_t)hp.n0 * hp.n1 * hp.n2;
+    return off[4];
+  }
+
+  int frame_begin() {
+    if (nd != 1) return fail(ELMM_ERR_INVALID_ARG, "frames are per single-domain handle");
+    CU(cudaSetDevice(device));
+    if (frame_pending) {
+      CU(cudaEventSynchronize(ev_done));
+      frame_pending = false;
+    }
+    size_t off[5];
+    size_t need = frame_offsets(0, off);
+    if (need > frame_elems) {
+      if (frame_host) cudaFreeHost(frame_host);
+      frame_host = nullptr;
+      CU(cudaMallocHost((void **)&frame_host, need * sizeof(double)));
+      int r = dalloc((void **)&frame_dev, need * sizeof(double));
+      if (r) return r;
+      frame_elems = need;
+    }
+    CU(cudaEventRecord(ev_ready, stream));
+    CU(cudaStreamWaitEvent(side, ev_ready, 0));
+    for (int f = 0; f < 4; f++) pack(0, f, frame_dev + off[f], side);
+    CU(cudaEventRecord(ev_packed, side));
+    CU(cudaMemcpyAsync(frame_host, frame_dev, need * sizeof(double), cudaMemcpyDeviceToHost, side));
+    CU(cudaEventRecord(ev_done, side));
+    frame_pending = true;
+    return ELMM_OK;
+  }
+
+  int frame_wait(double *U, double *V, double *W, double *Pr) {
+    if (!frame_pending) return fail(ELMM_ERR_INVALID_ARG, "no frame in flight");
+    CU(cudaEventSynchronize(ev_done));
+    frame_pending = false;
+    size_t off[5];
+    frame_offsets(0, off);
+    double *dst[4] = {U, V, W, Pr};
+    for (int f = 0; f < 4; f++)
+      if (dst[f]) memcpy(dst[f], frame_host + off[f], (off[f + 1] - off[f]) * sizeof(double));
+    return ELMM_OK;
+  }
+};
+
+// ------------------------------------------------------------ handle types
+struct elmm_batch {
+  int precision = 0;
+  std::unique_ptr<BatchT<double>> b64;
+  std::unique_ptr<BatchT<float>> b32;
+};
+
+struct elmm_handle {
+  elmm_batch b;
+};
+
+struct elmm_poisson {
+  elmm_batch b;
+  int nx, ny, nz;
+};
+
+#define DISPATCH(B, EXPR) ((B).precision == ELMM_PREC_MIXED ? (B).b32->EXPR : (B).b64->EXPR)
+
+static int batch_init(elmm_batch &B, const elmm_config *cfgs, int n) {
+  if (!cfgs || n < 1) return fail(ELMM_ERR_INVALID_ARG, "no configuration");
+  B.precision = cfgs[0].precision;
+  int r;
+  if (B.precision == ELMM_PREC_MIXED) {
+    B.b32.reset(new BatchT<float>());
+    r = B.b32->init(cfgs, n);
+  } else {
+    B.b64.reset(new BatchT<double>());
+    r = B.b64->init(cfgs, n);
+  }
+  return r;
+}
+
+template <typename T>
+static int poisson_exec(BatchT<T> &B, double *Phi, const double *RHS) {
+  CU(cudaSetDevice(B.device));
+  const Dom<T> &h = B.hdom[0];
+  // RHS(0:n+1)^3 -> box field (Phi is free until the inverse transform) -> transforms
+  HostBox hb{0, h.nx + 2, h.ny + 2, h.nz + 2};
+  size_t n = (size_t)hb.n0 * hb.n1 * hb.n2;
+  CU(cudaMemcpyAsync(B.dstage, RHS, n * sizeof(double), cudaMemcpyHostToDevice, B.stream));
+  CU(cudaMemsetAsync(B.dbad, 0, sizeof(int), B.stream));
+  k_unpack<T><<<256, 256, 0, B.stream>>>(B.ddom, h.Phi, B.dstage, hb, h.nx, h.ny, h.nz, B.dbad);
+  k_fftx_fwd<T><<<B.gsz(2, B.ls[LK_ROWS].total), 128, B.smem_x, B.stream>>>(
+      B.ddom, B.ls[LK_ROWS].l(), B.dplan, 1.0, 0, h.Phi);
+  k_ffty<T><<<B.gsz(3, B.ls[LK_YCOLS].total), 128, B.smem_y, B.stream>>>(B.ddom, B.ls[LK_YCOLS].l(), B.dplan, 0);
+  k_tri<T><<<B.gsz(4, B.ls[LK_TRI].total), kTriThreads, B.smem_tri, B.stream>>>(B.ddom, B.ls[LK_TRI].l());
+  k_ffty<T><<<B.gsz(3, B.ls[LK_YCOLS].total), 128, B.smem_y, B.stream>>>(B.ddom, B.ls[LK_YCOLS].l(), B.dplan, 1);
+  k_fftx_inv<T><<<B.gsz(5, B.ls[LK_ROWS].total), 128, B.smem_x, B.stream>>>(B.ddom, B.ls[LK_ROWS].l(), B.dplan);
+  HostBox hp = B.hbox_p(0);
+  size_t np = (size_t)hp.n0 * hp.n1 * hp.n2;
+  CU(cudaMemcpyAsync(B.dstage, Phi, np * sizeof(double), cudaMemcpyHostToDevice, B.stream));
+  k_pack_scalar<T><<<256, 256, 0, B.stream>>>(B.ddom, h.Phi, B.dstage, hp, 0, 0, h.nx, h.ny, h.nz);
+  CU(cudaMemcpyAsync(Phi, B.dstage, np * sizeof(double), cudaMemcpyDeviceToHost, B.stream));
+  CU(cudaStreamSynchronize(B.stream));
+  CU(cudaGetLastError());
+  return ELMM_OK;
+}
+
+
+extern "C" {
+
+const char *elmm_version(void) { return "elmm-b200 1.0 (sm_100a)"; }
+
+const char *elmm_last_error(void) { return g_err.c_str(); }
+
+int elmm_config_defaults(elmm_config *c, int32_t Prnx, int32_t Prny, int32_t Prnz) {
+  if (!c) return fail(ELMM_ERR_INVALID_ARG, "NULL config");
+  memset(c, 0, sizeof(*c));
+  c->abi_version = ELMM_ABI_VERSION;
+  c->Prnx = Prnx; c->Prny = Prny; c->Prnz = Prnz;
+  int bt[6] = {ELMM_BC_PERIODIC, ELMM_BC_PERIODIC, ELMM_BC_PERIODIC, ELMM_BC_PERIODIC, ELMM_BC_NOSLIP, ELMM_BC_FREESLIP};
+  memcpy(c->Btype, bt, sizeof(bt));
+  c->dxmin = c->dymin = c->dzmin = 1.0;
+  c->dt = 0.02;
+  c->molecular_viscosity = 1.0 / 70000;
+  c->C_Smagorinsky = 0.122;
+  c->filter_ratio = 1.0;
+  c->sgstype = 1;
+  c->wallmodeltype = 1;
+  for (int s = 0; s < 6; s++) c->z0[s] = 0.01;
+  c->precision = ELMM_PREC_FP64;
+  c->refine_tol = 1e-6;
+  return ELMM_OK;
+}
+
+int elmm_create(const elmm_config *cfg, elmm_handle **out) {
+  if (!cfg || !out) return fail(ELMM_ERR_INVALID_ARG, "NULL argument");
+  *out = nullptr;
+  elmm_handle *h = new elmm_handle();
+  int r = batch_init(h->b, cfg, 1);
+  if (r) { delete h; return r; }
+  *out = h;
+  return ELMM_OK;
+}
+
+int elmm_destroy(elmm_handle *h) {
+  delete h;
+  return ELMM_OK;
+}
+
+int elmm_upload_state(elmm_handle *h, const double *U, const double *V, const double *W, const double *Pr) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  return DISPATCH(h->b, upload(0, U, V, W, Pr));
+}
+
+int elmm_download_state(elmm_handle *h, double *U, double *V, double *W, double *Pr) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  return DISPATCH(h->b, download(0, U, V, W, Pr));
+}
+
+int elmm_download_field(elmm_handle *h, int32_t field, double *host) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  return DISPATCH(h->b, download_field(0, field, host));
+}
+
+int elmm_frame_begin(elmm_handle *h) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  return DISPATCH(h->b, frame_begin());
+}
+
+int elmm_frame_wait(elmm_handle *h, double *U, double *V, double *W, double *Pr) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  return DISPATCH(h->b, frame_wait(U, V, W, Pr));
+}
+
+int elmm_project(elmm_handle *h, double coef, elmm_stats *st) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  if (!(coef > 0)) return fail(ELMM_ERR_INVALID_ARG, "coef must be positive");
+  return DISPATCH(h->b, project(coef, st));
+}
+
+int elmm_step(elmm_handle *h, int32_t nsteps, elmm_stats *st) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  if (nsteps < 0) return fail(ELMM_ERR_INVALID_ARG, "nsteps < 0");
+  return DISPATCH(h->b, step(nsteps, st));
+}
+
+int elmm_run_stage(elmm_handle *h, int32_t stage, int32_t stop) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  if (stage < 1 || stage > 3 || stop < 1 || stop > 3) return fail(ELMM_ERR_INVALID_ARG, "stage 1..3, stop 1..3");
+  int r = DISPATCH(h->b, run_stage(stage, stop));
+  if (r) return r;
+  cudaStream_t s = h->b.precision == ELMM_PREC_MIXED ? h->b.b32->stream : h->b.b64->stream;
+  CU(cudaStreamSynchronize(s));
+  CU(cudaGetLastError());
+  return ELMM_OK;
+}
+
+// ------------------------------------------------------------- batches
+int elmm_batch_create(const elmm_config *cfgs, int32_t n, elmm_batch **out) {
+  if (!cfgs || !out || n < 1) return fail(ELMM_ERR_INVALID_ARG, "bad arguments");
+  *out = nullptr;
+  elmm_batch *b = new elmm_batch();
+  int r = batch_init(*b, cfgs, n);
+  if (r) { delete b; return r; }
+  *out = b;
+  return ELMM_OK;
+}
+
+int elmm_batch_destroy(elmm_batch *b) {
+  delete b;
+  return ELMM_OK;
+}
+
+int elmm_batch_upload_state(elmm_batch *b, int32_t d, const double *U, const double *V, const double *W,
+                            const double *Pr) {
+  if (!b) return fail(ELMM_ERR_INVALID_ARG, "NULL batch");
+  return DISPATCH(*b, upload(d, U, V, W, Pr));
+}
+
+int elmm_batch_download_state(elmm_batch *b, int32_t d, double *U, double *V, double *W, double *Pr) {
+  if (!b) return fail(ELMM_ERR_INVALID_ARG, "NULL batch");
+  return DISPATCH(*b, download(d, U, V, W, Pr));
+}
+
+int elmm_batch_project(elmm_batch *b, double coef) {
+  if (!b) return fail(ELMM_ERR_INVALID_ARG, "NULL batch");
+  return DISPATCH(*b, project(coef, nullptr));
+}
+
+int elmm_batch_step(elmm_batch *b, int32_t nsteps, elmm_stats *st) {
+  if (!b) return fail(ELMM_ERR_INVALID_ARG, "NULL batch");
+  return DISPATCH(*b, step(nsteps, st));
+}
+
+int64_t elmm_batch_cells(const elmm_batch *b) {
+  if (!b) return 0;
+  return b->precision == ELMM_PREC_MIXED ? b->b32->cells : b->b64->cells;
+}
+
+// ---------------------------------------------------- PoisSolver interface
+static int poisson_new(elmm_poisson **out, const int32_t n[3], double Lx, double Ly, const double *zW, double Lz,
+                       const int32_t bcs[6], int32_t precision, int32_t device) {
+  if (!out || !n || !bcs) return fail(ELMM_ERR_INVALID_ARG, "NULL argument");
+  *out = nullptr;
+  elmm_config c;
+  elmm_config_defaults(&c, n[0], n[1], n[2]);
+  for (int s = 0; s < 6; s++) {
+    if (bcs[s] != ELMM_BC_PERIODIC && bcs[s] != ELMM_BC_NEUMANN)
+      return fail(ELMM_ERR_INVALID_CONFIG, "Poisson BCs must be periodic or staggered Neumann");
+    c.Btype[s] = bcs[s] == ELMM_BC_PERIODIC ? ELMM_BC_PERIODIC : ELMM_BC_NEUMANN;
+  }
+  c.dxmin = Lx / n[0];
+  c.dymin = Ly / n[1];
+  c.dzmin = zW ? (zW[n[2]] - zW[0]) / n[2] : Lz / n[2];
+  c.zW = zW;
+  c.sgstype = 0;
+  c.wallmodeltype = 0;
+  c.precision = precision;
+  c.device = device;
+  elmm_poisson *p = new elmm_poisson();
+  p->nx = n[0]; p->ny = n[1]; p->nz = n[2];
+  int r = batch_init(p->b, &c, 1);
+  if (r) { delete p; return r; }
+  *out = p;
+  return ELMM_OK;
+}
+
+int elmm_poisson_solver_new(elmm_poisson **out, const int32_t n[3], const double L[3], const int32_t bcs[6],
+                            int32_t precision, int32_t device) {
+  if (!L) return fail(ELMM_ERR_INVALID_ARG, "NULL L");
+  return poisson_new(out, n, L[0], L[1], nullptr, L[2], bcs, precision, device);
+}
+
+int elmm_poisson_solver_nonuniform_z_new(elmm_poisson **out, const int32_t n[3], const double Lxy[2],
+                                         const double *zPr, const double *zW, const int32_t bcs[6],
+                                         int32_t precision, int32_t device) {
+  (void)zPr;  // zPr(k) = (zW(k-1) + zW(k)) / 2 is recomputed from zW
+  if (!Lxy || !zW) return fail(ELMM_ERR_INVALID_ARG, "NULL grid");
+  return poisson_new(out, n, Lxy[0], Lxy[1], zW, 0.0, bcs, precision, device);
+}
+
+int elmm_poisson_solver_execute(elmm_poisson *s, double *Phi, const double *RHS) {
+  if (!s || !Phi || !RHS) return fail(ELMM_ERR_INVALID_ARG, "NULL argument");
+  return s->b.precision == ELMM_PREC_MIXED ? poisson_exec(*s->b.b32, Phi, RHS) : poisson_exec(*s->b.b64, Phi, RHS);
+}
+
+int elmm_poisson_solver_finalize(elmm_poisson *s) {
+  delete s;
+  return ELMM_OK;
+}
+
+}  // extern "C"

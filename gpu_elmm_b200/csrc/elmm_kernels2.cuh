@@ -1,0 +1,365 @@
+// elmm_kernels2.cuh -- inverse transform, projection, reductions and the
+// host-layout pack / unpack kernels.
+#pragma once
+
+#include "elmm_kernels.cuh"
+
+namespace elmm {
+
+// inverse real FFT along x of kRowsX rows -> Phi(1:nx) with its ghosts
+// (Bound_Phi, src/boundaries.f90:1817-1948, one cell deep).
+template <typename T>
+__global__ void __launch_bounds__(128) k_fftx_inv(const Dom<T> *__restrict__ doms, Launch L,
+                                                  const PoisPlan *__restrict__ plans) {
+  typedef typename Vec2<T>::type T2;
+  extern __shared__ unsigned char smem_raw[];
+  T2 *buf0 = reinterpret_cast<T2 *>(smem_raw);
+  for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
+    const int di = find_dom(L.starts, L.nd, t);
+    const Dom<T> &d = doms[di];
+    const PoisPlan &pl = plans[di];
+    const int N = d.nx, nxh = d.nxh;
+    const int ntr = kRowsX / 2;
+    T2 *buf1 = buf0 + ntr * N;
+    const int lt = t - __ldg(L.starts + di);
+    const int row0 = lt * kRowsX;
+    const int nrows = d.ny * d.nz;
+    // Z_m = A_m + i B_m with the Hermitian completion A_{N-m} = conj(A_m);
+    // A_0 and A_{N/2} are real for a real row.
+    for (int w = threadIdx.x; w < ntr * N; w += blockDim.x) {
+      const int p = w / N, m = w - p * N;
+      const int ra = row0 + 2 * p, rb = ra + 1;
+      const int mm = m < nxh ? m : N - m;
+      const bool cj = m >= nxh;
+      T2 A, B;
+      A.x = 0; A.y = 0; B.x = 0; B.y = 0;
+      if (ra < nrows) A = d.S[((long long)(ra / d.ny) * d.ny + ra % d.ny) * d.spitch + mm];
+      if (rb < nrows) B = d.S[((long long)(rb / d.ny) * d.ny + rb % d.ny) * d.spitch + mm];
+      if (mm == 0 || 2 * mm == N) { A.y = 0; B.y = 0; }
+      if (cj) { A.y = -A.y; B.y = -B.y; }
+      T2 z;
+      z.x = A.x - B.y;
+      z.y = A.y + B.x;
+      buf0[p * N + m] = z;
+    }
+    __syncthreads();
+    T2 *res = fft_block<T, T2>(buf0, buf1, ntr, pl.fx, d.twx, true);
+    const bool px = d.bt[SIDE_WE] == BC_PERIODIC, py = d.bt[SIDE_SO] == BC_PERIODIC, pz = d.bt[SIDE_BO] == BC_PERIODIC;
+    for (int w = threadIdx.x; w < kRowsX * N; w += blockDim.x) {
+      const int r = w / N, i = w - r * N + 1;
+      const int row = row0 + r;
+      if (row >= nrows) continue;
+      const int j = row % d.ny + 1, k = row / d.ny + 1;
+      const T2 z = res[(r >> 1) * N + i - 1];
+      const T v = (r & 1) ? z.y : z.x;
+      d.Phi[bidx(d, i, j, k)] = v;
+      Images ix = images_rep(i, d.nx, px), iy = images_rep(j, d.ny, py), iz = images_rep(k, d.nz, pz);
+      push_ghosts(d, d.Phi, ix, iy, iz, v);
+    }
+    __syncthreads();
+  }
+}
+
+// PostPoisson (src/pressure.f90:728-870): velocity correction, Pr += Phi and
+// the partial sums of the top layer for FixPressureToReference.  src may be
+// the same array as dst (initial projection in place).
+template <typename T>
+__global__ void __launch_bounds__(TX *TY) k_project(const Dom<T> *__restrict__ doms, Launch L, double coef_alpha2,
+                                                    int use_dt, int in_place) {
+  __shared__ double red[TX * TY / 32];
+  for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
+    const int di = find_dom(L.starts, L.nd, t);
+    const Dom<T> &d = doms[di];
+    int lt = t - __ldg(L.starts + di);
+    const int ntx = (d.nx + TX - 1) / TX, nty = (d.ny + TY - 1) / TY;
+    const int tx = lt % ntx; lt /= ntx;
+    const int ty = lt % nty;
+    const int k = lt / nty + 1;
+    const int i = tx * TX + (threadIdx.x % TX) + 1;
+    const int j = ty * TY + (threadIdx.x / TX) + 1;
+    const bool inside = i <= d.nx && j <= d.ny;
+    const double coef = use_dt ? coef_alpha2 * d.dt : coef_alpha2;
+    const T dt2 = (T)coef;
+    const T Au = (T)(coef / d.dx), Av = (T)(coef / d.dy), Aw = (T)(coef / d.dz);
+    const T *Us = in_place ? d.U : d.U2;
+    const T *Vs = in_place ? d.V : d.V2;
+    const T *Ws = in_place ? d.W : d.W2;
+    double top = 0;
+    if (inside) {
+      const long long c = bidx(d, i, j, k);
+      const T phi = ld(d.Phi, c);
+      if (i <= d.ext[0][0] && j <= d.ext[0][1] && k <= d.ext[0][2]) {
+        T u = Us[c] - Au * (ld(d.Phi, c + 1) - phi);
+        d.U[c] = u;
+        push_vel(d, d.U, 0, i, j, k, u);
+      }
+      if (i <= d.ext[1][0] && j <= d.ext[1][1] && k <= d.ext[1][2]) {
+        T v = Vs[c] - Av * (ld(d.Phi, c + d.pitch) - phi);
+        d.V[c] = v;
+        push_vel(d, d.V, 1, i, j, k, v);
+      }
+      if (i <= d.ext[2][0] && j <= d.ext[2][1] && k <= d.ext[2][2]) {
+        T w;
+        if (d.vz) w = Ws[c] - dt2 * (ld(d.Phi, c + d.plane) - phi) / (T)d.dzW[k + 2];
+        else w = Ws[c] - Aw * (ld(d.Phi, c + d.plane) - phi);
+        d.W[c] = w;
+        push_vel(d, d.W, 2, i, j, k, w);
+      }
+      const T m = (T)(*d.prm);
+      T p = (d.P[c] - m) + phi;
+      d.P[c] = p;
+      Images ix = images_per(i, d.nx, d.bt[SIDE_WE] == BC_PERIODIC);
+      Images iy = images_per(j, d.ny, d.bt[SIDE_SO] == BC_PERIODIC);
+      Images iz = images_per(k, d.nz, d.bt[SIDE_BO] == BC_PERIODIC);
+      push_ghosts(d, d.P, ix, iy, iz, p);
+      if (k == d.nz) top = (double)p;
+    }
+    if (k == d.nz) {  // block-uniform branch
+      for (int o = 16; o > 0; o >>= 1) top += __shfl_down_sync(0xffffffffu, top, o);
+      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = top;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double s = 0;
+        for (int w = 0; w < TX * TY / 32; w++) s += red[w];
+        d.prpart[ty * ntx + tx] = s;
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// FixPressureToReference, reference at side To (src/pressure.f90:1160-1229):
+// the new reference is the mean of the top layer; it is applied lazily,
+// every reader of P subtracts it.
+template <typename T>
+__global__ void k_prref(const Dom<T> *__restrict__ doms, int nd) {
+  __shared__ double red[32];
+  for (int di = blockIdx.x; di < nd; di += gridDim.x) {
+    const Dom<T> &d = doms[di];
+    double s = 0;
+    for (int p = threadIdx.x; p < d.nprpart; p += blockDim.x) s += d.prpart[p];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double tot = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) tot += red[w];
+      *d.prm = tot / ((double)d.nx * (double)d.ny);
+    }
+    __syncthreads();
+  }
+}
+
+// max |div u| in FP64 (the check of src/pressure.f90:884-989)
+template <typename T>
+__global__ void __launch_bounds__(TX *TY) k_divmax(const Dom<T> *__restrict__ doms, Launch L) {
+  __shared__ double red[TX * TY / 32];
+  for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
+    const int di = find_dom(L.starts, L.nd, t);
+    const Dom<T> &d = doms[di];
+    int lt = t - __ldg(L.starts + di);
+    const int ntx = (d.nx + TX - 1) / TX, nty = (d.ny + TY - 1) / TY;
+    const int tx = lt % ntx; lt /= ntx;
+    const int ty = lt % nty;
+    const int k = lt / nty + 1;
+    const int i = tx * TX + (threadIdx.x % TX) + 1;
+    const int j = ty * TY + (threadIdx.x / TX) + 1;
+    double a = 0;
+    if (i <= d.nx && j <= d.ny) {
+      const long long c = bidx(d, i, j, k);
+      const double dzk = d.vz ? d.dzPr[k + 2] : d.dz;
+      double p = ((double)ld(d.U, c) - (double)ld(d.U, c - 1)) / d.dx +
+                 ((double)ld(d.V, c) - (double)ld(d.V, c - d.pitch)) / d.dy +
+                 ((double)ld(d.W, c) - (double)ld(d.W, c - d.plane)) / dzk;
+      a = fabs(p);
+      if (!(a == a)) a = __longlong_as_double(0x7ff8000000000000ULL);
+    }
+    for (int o = 16; o > 0; o >>= 1) a = fmax(a, __shfl_down_sync(0xffffffffu, a, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double m = 0;
+      for (int w = 0; w < TX * TY / 32; w++) m = fmax(m, red[w]);
+      atomic_max_pos(d.maxdiv_bits, m);
+    }
+    __syncthreads();
+  }
+}
+
+// CFL of TimeStepLength (src/dynamics.f90:553-595)
+template <typename T>
+__global__ void __launch_bounds__(TX *TY) k_cfl(const Dom<T> *__restrict__ doms, Launch L) {
+  __shared__ double red[TX * TY / 32];
+  for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
+    const int di = find_dom(L.starts, L.nd, t);
+    const Dom<T> &d = doms[di];
+    int lt = t - __ldg(L.starts + di);
+    const int ntx = (d.nx + TX - 1) / TX, nty = (d.ny + TY - 1) / TY;
+    const int tx = lt % ntx; lt /= ntx;
+    const int ty = lt % nty;
+    const int k = lt / nty + 1;
+    const int i = tx * TX + (threadIdx.x % TX) + 1;
+    const int j = ty * TY + (threadIdx.x / TX) + 1;
+    double a = 0;
+    if (i <= d.nx && j <= d.ny) {
+      const long long c = bidx(d, i, j, k);
+      const double dzk = d.vz ? d.dzPr[k + 2] : d.dz;
+      double p = fmax(fabs((double)ld(d.U, c)), fabs((double)ld(d.U, c - 1))) / d.dx;
+      p = p + fmax(fabs((double)ld(d.V, c)), fabs((double)ld(d.V, c - d.pitch))) / d.dy;
+      p = p + fmax(fabs((double)ld(d.W, c)), fabs((double)ld(d.W, c - d.plane))) / dzk;
+      a = p;
+      if (!(p == p)) a = __longlong_as_double(0x7ff8000000000000ULL);
+    }
+    for (int o = 16; o > 0; o >>= 1) a = fmax(a, __shfl_down_sync(0xffffffffu, a, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double m = 0;
+      for (int w = 0; w < TX * TY / 32; w++) m = fmax(m, red[w]);
+      atomic_max_pos(d.cfl_bits, m);
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------ host layout copies
+// Host arrays: Fortran layout, lower bound lo, extents n + 2*(1-lo) per dim.
+struct HostBox {
+  int lo;
+  int n0, n1, n2;  // full extents of the host array
+};
+
+__device__ __forceinline__ long long hidx(const HostBox &h, int i, int j, int k) {
+  return (long long)(i - h.lo) + (long long)h.n0 * ((long long)(j - h.lo) + (long long)h.n1 * (k - h.lo));
+}
+
+// interior of a host array (double) -> device box (T); counts non-finite values
+template <typename T>
+__global__ void k_unpack(const Dom<T> *__restrict__ dom, T *dst, const double *__restrict__ src, HostBox h, int nx,
+                         int ny, int nz, int *bad) {
+  const Dom<T> &d = *dom;
+  long long total = (long long)nx * ny * nz;
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < total; w += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(w % nx) + 1;
+    long long r = w / nx;
+    int j = (int)(r % ny) + 1, k = (int)(r / ny) + 1;
+    double v = src[hidx(h, i, j, k)];
+    if (!isfinite(v)) atomicAdd(bad, 1);
+    dst[bidx(d, i, j, k)] = (T)v;
+  }
+}
+
+// ghost shell of a velocity component from its interior (BoundUVW rules)
+template <typename T>
+__global__ void k_halo_vel(const Dom<T> *__restrict__ dom, int comp) {
+  const Dom<T> &d = *dom;
+  T *F = comp == 0 ? d.U : comp == 1 ? d.V : d.W;
+  const int *e = d.ext[comp];
+  const int bx = d.nx + 2, by = d.ny + 2, bz = d.nz + 2;
+  long long total = (long long)bx * by * bz;
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < total; w += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(w % bx);
+    long long r = w / bx;
+    int j = (int)(r % by), k = (int)(r / by);
+    if (i > e[0] + 1 || j > e[1] + 1 || k > e[2] + 1) continue;
+    bool gi = i < 1 || i > e[0], gj = j < 1 || j > e[1], gk = k < 1 || k > e[2];
+    if (!(gi || gj || gk)) continue;
+    Fold fx = fold_vel(i, e[0], d.bt[0], d.bt[1], comp == 0);
+    Fold fy = fold_vel(j, e[1], d.bt[2], d.bt[3], comp == 1);
+    Fold fz = fold_vel(k, e[2], d.bt[4], d.bt[5], comp == 2);
+    T v = 0;
+    if (!(fx.zero | fy.zero | fz.zero)) {
+      v = F[bidx(d, fx.src, fy.src, fz.src)];
+      if (fx.sign * fy.sign * fz.sign < 0) v = -v;
+    }
+    F[bidx(d, i, j, k)] = v;
+  }
+}
+
+// periodic ghosts of P from its interior
+template <typename T>
+__global__ void k_halo_p(const Dom<T> *__restrict__ dom) {
+  const Dom<T> &d = *dom;
+  const int bx = d.nx + 2, by = d.ny + 2, bz = d.nz + 2;
+  const bool px = d.bt[SIDE_WE] == BC_PERIODIC, py = d.bt[SIDE_SO] == BC_PERIODIC, pz = d.bt[SIDE_BO] == BC_PERIODIC;
+  long long total = (long long)bx * by * bz;
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < total; w += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(w % bx);
+    long long r = w / bx;
+    int j = (int)(r % by), k = (int)(r / by);
+    bool gi = i < 1 || i > d.nx, gj = j < 1 || j > d.ny, gk = k < 1 || k > d.nz;
+    if (!(gi || gj || gk)) continue;
+    if ((gi && !px) || (gj && !py) || (gk && !pz)) continue;
+    d.P[bidx(d, i, j, k)] = d.P[bidx(d, fold_rep(i, d.nx, px), fold_rep(j, d.ny, py), fold_rep(k, d.nz, pz))];
+  }
+}
+
+// device box -> host layout with the reference's three-deep ghosts (BoundUVW)
+template <typename T>
+__global__ void k_pack_vel(const Dom<T> *__restrict__ dom, const T *F, int comp, double *dst, HostBox h) {
+  const Dom<T> &d = *dom;
+  const int *e = d.ext[comp];
+  long long total = (long long)h.n0 * h.n1 * h.n2;
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < total; w += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(w % h.n0) + h.lo;
+    long long r = w / h.n0;
+    int j = (int)(r % h.n1) + h.lo, k = (int)(r / h.n1) + h.lo;
+    Fold fx = fold_vel(i, e[0], d.bt[0], d.bt[1], comp == 0);
+    Fold fy = fold_vel(j, e[1], d.bt[2], d.bt[3], comp == 1);
+    Fold fz = fold_vel(k, e[2], d.bt[4], d.bt[5], comp == 2);
+    double v = 0;
+    if (!(fx.zero | fy.zero | fz.zero)) {
+      v = (double)F[bidx(d, fx.src, fy.src, fz.src)];
+      if (fx.sign * fy.sign * fz.sign < 0) v = -v;
+    }
+    dst[w] = v;
+  }
+}
+
+// interior of a box field -> host (double), optional subtraction of the
+// pressure reference; mode 1: Bound_Pr faces, mode 2: Bound_Phi faces,
+// mode 3: the one-cell shell as stored (Viscosity); other cells untouched.
+// mode 0: interior only.  (nx, ny, nz): interior extents of the field.
+template <typename T>
+__global__ void k_pack_scalar(const Dom<T> *__restrict__ dom, const T *F, double *dst, HostBox h, int mode,
+                              int sub_prm, int nx, int ny, int nz) {
+  const Dom<T> &d = *dom;
+  const double m = sub_prm ? *d.prm : 0.0;
+  long long total = (long long)h.n0 * h.n1 * h.n2;
+  const bool per[3] = {d.bt[SIDE_WE] == BC_PERIODIC, d.bt[SIDE_SO] == BC_PERIODIC, d.bt[SIDE_BO] == BC_PERIODIC};
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < total; w += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(w % h.n0) + h.lo;
+    long long r = w / h.n0;
+    int j = (int)(r % h.n1) + h.lo, k = (int)(r / h.n1) + h.lo;
+    bool gi = i < 1 || i > nx, gj = j < 1 || j > ny, gk = k < 1 || k > nz;
+    int ng = (int)gi + (int)gj + (int)gk;
+    auto val = [&](int a, int b, int c) { return (double)F[bidx(d, a, b, c)] - m; };
+    if (ng == 0) { dst[w] = val(i, j, k); continue; }
+    if (mode == 0) continue;
+    if (mode == 3) {
+      if (i >= 0 && i <= nx + 1 && j >= 0 && j <= ny + 1 && k >= 0 && k <= nz + 1) dst[w] = (double)F[bidx(d, i, j, k)];
+      continue;
+    }
+    if (ng != 1) continue;  // edges and corners are not written by Bound_Pr / Bound_Phi
+    int dim = gi ? 0 : gj ? 1 : 2;
+    int g = dim == 0 ? i : dim == 1 ? j : k;
+    int n = dim == 0 ? nx : dim == 1 ? ny : nz;
+    auto at = [&](int q) {
+      return dim == 0 ? val(q, j, k) : dim == 1 ? val(i, q, k) : val(i, j, q);
+    };
+    double v;
+    if (per[dim]) {
+      v = at(g < 1 ? n + g : g - n);
+    } else if (mode == 1) {  // Neumann extrapolation of Bound_Pr (boundaries.f90:1976-1981)
+      if (g == 0) v = at(3) - 3 * (at(2) - at(1));
+      else if (g == -1) v = at(2);
+      else if (g == n + 1) v = at(n - 2) - 3 * (at(n - 1) - at(n));
+      else v = at(n - 1);
+    } else {  // even reflection of Bound_Phi
+      v = g < 1 ? at(1 - g) : at(2 * n + 1 - g);
+    }
+    dst[w] = v;
+  }
+}
+
+}  // namespace elmm

@@ -1,0 +1,208 @@
+"""ctypes front end of libelmm_gpu.so (include/elmm_gpu.h).
+
+Host arrays use the reference's Fortran layout (see workloads.py).  Every
+call goes to the CUDA library; there is no CPU fallback: if the shared
+library is missing or no CUDA device is usable, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .config import ElmmConfig, ElmmStats, Grid, STATUS_NAMES, grid_of
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libelmm_gpu.so")
+
+_lib = None
+
+_dp = C.POINTER(C.c_double)
+
+
+class ElmmError(RuntimeError):
+    def __init__(self, code: int, what: str, msg: str):
+        super().__init__(f"{what}: {STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def lib():
+    """Loads the in-tree library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} not built: run `make -C gpu_elmm_b200` (or __graft_entry__.build())")
+        L = C.CDLL(LIB_PATH)
+        P = C.c_void_p
+        L.elmm_version.restype = C.c_char_p
+        L.elmm_last_error.restype = C.c_char_p
+        L.elmm_config_defaults.argtypes = [C.POINTER(ElmmConfig), C.c_int32, C.c_int32, C.c_int32]
+        L.elmm_create.argtypes = [C.POINTER(ElmmConfig), C.POINTER(P)]
+        L.elmm_destroy.argtypes = [P]
+        L.elmm_upload_state.argtypes = [P, _dp, _dp, _dp, _dp]
+        L.elmm_download_state.argtypes = [P, _dp, _dp, _dp, _dp]
+        L.elmm_download_field.argtypes = [P, C.c_int32, _dp]
+        L.elmm_frame_begin.argtypes = [P]
+        L.elmm_frame_wait.argtypes = [P, _dp, _dp, _dp, _dp]
+        L.elmm_project.argtypes = [P, C.c_double, C.POINTER(ElmmStats)]
+        L.elmm_step.argtypes = [P, C.c_int32, C.POINTER(ElmmStats)]
+        L.elmm_run_stage.argtypes = [P, C.c_int32, C.c_int32]
+        L.elmm_poisson_solver_new.argtypes = [C.POINTER(P), C.POINTER(C.c_int32), _dp, C.POINTER(C.c_int32),
+                                              C.c_int32, C.c_int32]
+        L.elmm_poisson_solver_nonuniform_z_new.argtypes = [C.POINTER(P), C.POINTER(C.c_int32), _dp, _dp, _dp,
+                                                           C.POINTER(C.c_int32), C.c_int32, C.c_int32]
+        L.elmm_poisson_solver_execute.argtypes = [P, _dp, _dp]
+        L.elmm_poisson_solver_finalize.argtypes = [P]
+        L.elmm_batch_create.argtypes = [C.POINTER(ElmmConfig), C.c_int32, C.POINTER(P)]
+        L.elmm_batch_destroy.argtypes = [P]
+        L.elmm_batch_upload_state.argtypes = [P, C.c_int32, _dp, _dp, _dp, _dp]
+        L.elmm_batch_download_state.argtypes = [P, C.c_int32, _dp, _dp, _dp, _dp]
+        L.elmm_batch_project.argtypes = [P, C.c_double]
+        L.elmm_batch_step.argtypes = [P, C.c_int32, C.POINTER(ElmmStats)]
+        L.elmm_batch_cells.argtypes = [P]
+        L.elmm_batch_cells.restype = C.c_int64
+        _lib = L
+    return _lib
+
+
+def check(code: int, what: str):
+    if code != 0:
+        raise ElmmError(code, what, lib().elmm_last_error().decode())
+
+
+def ptr(a):
+    if a is None:
+        return None
+    assert isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous, "host arrays: C-contiguous float64"
+    return a.ctypes.data_as(_dp)
+
+
+class Domain:
+    """One domain whose state stays resident on the GPU (an elmm_handle)."""
+
+    def __init__(self, cfg: ElmmConfig):
+        self.cfg = cfg
+        self.grid: Grid = grid_of(cfg)
+        h = C.c_void_p()
+        check(lib().elmm_create(C.byref(cfg), C.byref(h)), "elmm_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().elmm_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def upload(self, U, V, W, Pr=None):
+        check(lib().elmm_upload_state(self.h, ptr(U), ptr(V), ptr(W), ptr(Pr)), "elmm_upload_state")
+
+    def download(self):
+        g = self.grid
+        U, V, W, Pr = np.zeros(g.shape_u()), np.zeros(g.shape_v()), np.zeros(g.shape_w()), np.zeros(g.shape_p())
+        check(lib().elmm_download_state(self.h, ptr(U), ptr(V), ptr(W), ptr(Pr)), "elmm_download_state")
+        return U, V, W, Pr
+
+    def field(self, fid: int, out=None):
+        g = self.grid
+        shape = {0: g.shape_u(), 5: g.shape_u(), 8: g.shape_u(), 1: g.shape_v(), 6: g.shape_v(), 9: g.shape_v(),
+                 2: g.shape_w(), 7: g.shape_w(), 10: g.shape_w()}.get(fid, g.shape_p())
+        a = np.zeros(shape) if out is None else out
+        check(lib().elmm_download_field(self.h, fid, ptr(a)), "elmm_download_field")
+        return a
+
+    def project(self, coef=1.0) -> ElmmStats:
+        st = ElmmStats()
+        check(lib().elmm_project(self.h, coef, C.byref(st)), "elmm_project")
+        return st
+
+    def step(self, n=1) -> ElmmStats:
+        st = ElmmStats()
+        check(lib().elmm_step(self.h, n, C.byref(st)), "elmm_step")
+        return st
+
+    def run_stage(self, stage, stop):
+        check(lib().elmm_run_stage(self.h, stage, stop), "elmm_run_stage")
+
+    def frame_begin(self):
+        check(lib().elmm_frame_begin(self.h), "elmm_frame_begin")
+
+    def frame_wait(self):
+        g = self.grid
+        U, V, W, Pr = np.zeros(g.shape_u()), np.zeros(g.shape_v()), np.zeros(g.shape_w()), np.zeros(g.shape_p())
+        check(lib().elmm_frame_wait(self.h, ptr(U), ptr(V), ptr(W), ptr(Pr)), "elmm_frame_wait")
+        return U, V, W, Pr
+
+
+class Batch:
+    """n independent domains of uneven sizes stepped together (elmm_batch)."""
+
+    def __init__(self, cfgs):
+        self.cfgs = list(cfgs)
+        arr = (ElmmConfig * len(self.cfgs))(*self.cfgs)
+        self._arr = arr
+        h = C.c_void_p()
+        check(lib().elmm_batch_create(arr, len(self.cfgs), C.byref(h)), "elmm_batch_create")
+        self.h = h
+        self.grids = [grid_of(c) for c in self.cfgs]
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().elmm_batch_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def cells(self) -> int:
+        return lib().elmm_batch_cells(self.h)
+
+    def upload(self, d, U, V, W, Pr=None):
+        check(lib().elmm_batch_upload_state(self.h, d, ptr(U), ptr(V), ptr(W), ptr(Pr)), "elmm_batch_upload_state")
+
+    def download(self, d):
+        g = self.grids[d]
+        U, V, W, Pr = np.zeros(g.shape_u()), np.zeros(g.shape_v()), np.zeros(g.shape_w()), np.zeros(g.shape_p())
+        check(lib().elmm_batch_download_state(self.h, d, ptr(U), ptr(V), ptr(W), ptr(Pr)),
+              "elmm_batch_download_state")
+        return U, V, W, Pr
+
+    def project(self, coef=1.0):
+        check(lib().elmm_batch_project(self.h, coef), "elmm_batch_project")
+
+    def step(self, n=1) -> ElmmStats:
+        st = ElmmStats()
+        check(lib().elmm_batch_step(self.h, n, C.byref(st)), "elmm_batch_step")
+        return st
+
+
+class PoissonSolver:
+    """The PoisSolver-compatible solver (poisson_solver_new/_execute/_finalize)."""
+
+    def __init__(self, n, L=None, bcs=(3, 3, 3, 3, 5, 5), precision=0, device=0, zW=None):
+        self.n = tuple(int(x) for x in n)
+        nn = (C.c_int32 * 3)(*self.n)
+        bb = (C.c_int32 * 6)(*bcs)
+        h = C.c_void_p()
+        if zW is None:
+            LL = (C.c_double * 3)(*L)
+            check(lib().elmm_poisson_solver_new(C.byref(h), nn, LL, bb, precision, device), "poisson_solver_new")
+        else:
+            zW = np.ascontiguousarray(zW, dtype=np.float64)
+            zPr = (zW[:-1] + zW[1:]) / 2
+            self._keep = (zW, zPr)
+            Lxy = (C.c_double * 2)(L[0], L[1])
+            check(lib().elmm_poisson_solver_nonuniform_z_new(C.byref(h), nn, Lxy, ptr(zPr), ptr(zW), bb, precision,
+                                                             device), "poisson_solver_nonuniform_z_new")
+        self.h = h
+
+    def execute(self, Phi, RHS):
+        check(lib().elmm_poisson_solver_execute(self.h, ptr(Phi), ptr(RHS)), "poisson_solver_execute")
+        return Phi
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().elmm_poisson_solver_finalize(self.h)
+            self.h = None
+
+    __del__ = close

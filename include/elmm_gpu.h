@@ -1,0 +1,216 @@
+/*
+ * elmm_gpu.h -- C-ABI of the B200 (sm_100a) per-timestep flow solve of ELMM.
+ *
+ * This library replaces, behind plain C entry points, the RK3 stage loop of
+ * the ELMM LES model and the external Poisson solver it calls:
+ *
+ *   TMarchRK3(U,V,W,Pr,Temperature,Moisture,Scalar,delta)   src/tsteps.f90:24-243
+ *       called from the time loop in src/main.f90:112
+ *   PressureCorrection(U,V,W,Pr,Q,coef)                      src/pressure.f90:169-266
+ *       called for the initial projection in src/initial.f90:4290
+ *   poisson_solver_new / _execute / _finalize (PoisSolver)   src/poisson.f90:76-210
+ *       (module of the un-vendored PoisFFT / poisson-solver library)
+ *
+ * Conventions
+ *   - Every entry point returns an int status: ELMM_OK (0) or an ELMM_ERR_* code.
+ *     The Fortran host maps a nonzero status to error_stop (src/stop.f90).
+ *   - Host arrays are Fortran-ordered (x fastest) with the reference's bounds:
+ *       U(-2:Unx+3,-2:Uny+3,-2:Unz+3), V(-2:Vnx+3,..), W(-2:Wnx+3,..)  (src/main.f90:231-233)
+ *       Pr(-1:Prnx+2,-1:Prny+2,-1:Prnz+2), Viscosity likewise            (src/main.f90:234, :272)
+ *       Phi(-1:Prnx+2,..), RHS(0:Prnx+1,..)                               (src/pressure.f90:189-190)
+ *     where Unx = Prnx if x is periodic else Prnx-1, and likewise Vny, Wnz
+ *     (src/initial.f90:871-896).
+ *   - A handle owns all of its device memory; the state U, V, W, Pr stays
+ *     resident in HBM between calls.  Calls on one handle are serialised by the
+ *     caller; different handles may be used from different host threads.
+ *   - No entry point falls back to the CPU: without a usable CUDA device every
+ *     call that needs one returns ELMM_ERR_CUDA.
+ */
+#ifndef ELMM_GPU_H
+#define ELMM_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ELMM_ABI_VERSION 1
+
+/* Status codes. */
+enum {
+  ELMM_OK = 0,
+  ELMM_ERR_INVALID_CONFIG = 1, /* a config field is out of range or unsupported */
+  ELMM_ERR_OOM = 2,            /* device allocation failed */
+  ELMM_ERR_NAN = 3,            /* NaN/Inf in the input state or produced by a step */
+  ELMM_ERR_CUDA = 4,           /* a CUDA call failed, or no device */
+  ELMM_ERR_TIMEOUT = 5,        /* a bounded device-side wait gave up */
+  ELMM_ERR_INVALID_ARG = 6,    /* NULL pointer, bad size, bad field id */
+  ELMM_ERR_ADMISSION = 7       /* request refused by the HBM budget of a serving loop */
+};
+
+/* Boundary-condition codes: the values of BC_NOSLIP.. in src/parameters.f90:249-250. */
+enum {
+  ELMM_BC_NOSLIP = 1,
+  ELMM_BC_FREESLIP = 2,
+  ELMM_BC_PERIODIC = 3,
+  ELMM_BC_NEUMANN = 5
+};
+
+/* Side indices (src/parameters.f90:193 numbers them We=1..To=6; here 0..5). */
+enum { ELMM_WE = 0, ELMM_EA = 1, ELMM_SO = 2, ELMM_NO = 3, ELMM_BO = 4, ELMM_TO = 5 };
+
+/* Arithmetic of the state and of the stencil / FFT kernels. */
+enum {
+  ELMM_PREC_FP64 = 0,  /* plain FP64 everywhere */
+  ELMM_PREC_MIXED = 1  /* FP32 state, stencils and FFT; FP64 reductions, FP64
+                          zero-wavenumber mode and FP64 divergence residual for
+                          the defect correction of the pressure solve */
+};
+
+/* Fields that elmm_download_field can return (host layout as above). */
+enum {
+  ELMM_FIELD_U = 0, ELMM_FIELD_V = 1, ELMM_FIELD_W = 2, ELMM_FIELD_PR = 3,
+  ELMM_FIELD_VISCOSITY = 4,
+  ELMM_FIELD_U2 = 5, ELMM_FIELD_V2 = 6, ELMM_FIELD_W2 = 7,
+  ELMM_FIELD_USTAR = 8, ELMM_FIELD_VSTAR = 9, ELMM_FIELD_WSTAR = 10,
+  ELMM_FIELD_PHI = 11
+};
+
+/*
+ * Configuration of one domain.  It carries the module globals of
+ * src/parameters.f90 that the hot path reads, filled by the host from its own
+ * parsed configuration (src/initial.f90 ReadConfiguration).
+ */
+typedef struct elmm_config {
+  int32_t abi_version;          /* must be ELMM_ABI_VERSION */
+  int32_t Prnx, Prny, Prnz;     /* pressure-grid cells (src/parameters.f90:55) */
+  int32_t Btype[6];             /* velocity BC per side, ELMM_BC_* */
+  double xmin, ymin, zmin;      /* im_xmin.. : xU(0), yV(0), zW(0) */
+  double dxmin, dymin, dzmin;   /* uniform spacings */
+  const double *zW;             /* NULL: uniform z.  Else zW(0:Prnz), Prnz+1 values,
+                                   the stretched grid of zgrid.txt (src/initial.f90:254-283) */
+  double dt;                    /* dt_constant (src/parameters.f90:89) */
+  double molecular_viscosity;   /* src/parameters.f90:133 (1/70000 by default) */
+  double C_Smagorinsky;         /* src/subgrid.f90:18 (0.122 by default) */
+  double filter_ratio;          /* filter_ratios(filtertype), 1.0 (src/filters.f90:14) */
+  int32_t sgstype;              /* 0: molecular only, 1: Smagorinsky (src/subgrid.f90:15) */
+  int32_t wallmodeltype;        /* 0: off, 1: log-law wall model at no-slip sides */
+  double z0[6];                 /* roughness per side z0W..z0T (src/parameters.f90:145) */
+  int32_t enable_pr_gradient_x_uniform, enable_pr_gradient_y_uniform;
+  double pr_gradient_x, pr_gradient_y; /* mean pressure-gradient forcing (src/dynamics.f90:83-117) */
+  int32_t precision;            /* ELMM_PREC_* */
+  int32_t max_refine_sweeps;    /* mixed path: defect-correction sweeps, 0..3 */
+  double refine_tol;            /* mixed path: max|div u| that triggers a sweep */
+  int32_t enable_CFL_check;     /* compute the CFL number each step (src/dynamics.f90:541) */
+  int32_t device;               /* CUDA device ordinal */
+} elmm_config;
+
+/* Diagnostics of elmm_step / elmm_project. */
+typedef struct elmm_stats {
+  int32_t steps_done;           /* steps completed by this call */
+  int32_t nan_detected;         /* 1 if a NaN was seen in the CFL / divergence check */
+  double time;                  /* simulated time after the call */
+  double dt;                    /* time step used */
+  double cfl;                   /* CFL number of the last step (enable_CFL_check) */
+  double max_div;               /* max |div u| after the last projection, FP64 */
+  int32_t refine_sweeps;        /* defect-correction sweeps run in the last stage */
+  int32_t reserved;
+  double elapsed_ms;            /* device time of the call (CUDA events) */
+} elmm_stats;
+
+typedef struct elmm_handle elmm_handle;
+
+/* Library identification: returns a static string. */
+const char *elmm_version(void);
+
+/* Fills *cfg with the reference defaults for a Prnx x Prny x Prnz box
+ * (periodic x,y, no-slip bottom, free-slip top, Smagorinsky + wall model). */
+int elmm_config_defaults(elmm_config *cfg, int32_t Prnx, int32_t Prny, int32_t Prnz);
+
+/* Allocates the device state of one domain (the module arrays of src/dynamics.f90:13-17,
+ * src/main.f90:229-285) and prepares the wall-model points
+ * (src/wallmodels.f90:690-909) and the Poisson solver. */
+int elmm_create(const elmm_config *cfg, elmm_handle **out);
+int elmm_destroy(elmm_handle *h);
+
+/* Host -> device copy of the state.  U, V, W, Pr are host arrays in the
+ * Fortran layout above; Pr may be NULL (zero).  Returns ELMM_ERR_NAN if an
+ * interior value is not finite. */
+int elmm_upload_state(elmm_handle *h, const double *U, const double *V,
+                      const double *W, const double *Pr);
+
+/* Device -> host copy of the state, ghost cells filled as BoundUVW / Bound_Pr
+ * leave them (src/boundaries.f90:398-1812, :1951-2091).  NULL pointers are skipped. */
+int elmm_download_state(elmm_handle *h, double *U, double *V, double *W, double *Pr);
+
+/* Device -> host copy of one field (ELMM_FIELD_*). */
+int elmm_download_field(elmm_handle *h, int32_t field, double *host);
+
+/* Asynchronous frame: copies U, V, W, Pr on a side stream into pinned staging
+ * buffers owned by the handle and returns at once.  elmm_frame_wait blocks
+ * until the copy has finished and copies the frame into the host arrays.
+ * Replaces the pthread frame writer of src/frames_common.f90:120-164. */
+int elmm_frame_begin(elmm_handle *h);
+int elmm_frame_wait(elmm_handle *h, double *U, double *V, double *W, double *Pr);
+
+/* PressureCorrection(U,V,W,Pr,Q,coef) on the resident state
+ * (src/pressure.f90:169-266, Q = 0): the initial projection uses coef = 1
+ * (src/initial.f90:4290). */
+int elmm_project(elmm_handle *h, double coef, elmm_stats *stats);
+
+/* nsteps calls of TMarchRK3 (src/tsteps.f90:24-243) on the resident state. */
+int elmm_step(elmm_handle *h, int32_t nsteps, elmm_stats *stats);
+
+/* One RK3 stage up to a stop point, for operator-level checks:
+ *   stop = 1: after SubgridStresses (Viscosity, wall-model fluxes)
+ *   stop = 2: after Convection + OtherTerms + BoundUVW (U2, Ustar)
+ *   stop = 3: the full stage (projection and swap)
+ * stage is 1..3.  Fields are read back with elmm_download_field. */
+int elmm_run_stage(elmm_handle *h, int32_t stage, int32_t stop);
+
+/*
+ * PoisSolver-compatible solver (the interface of src/poisson.f90:108-121,
+ * :132, :178-189, :201).  Solves the discrete problem of Residue_variable_z
+ * (src/poisson.f90:23-60): periodic x and y, periodic or staggered Neumann z,
+ * by FFT in x and y and a tridiagonal solve in z.  bcs[6] are
+ * ELMM_BC_PERIODIC or ELMM_BC_NEUMANN per side.
+ */
+typedef struct elmm_poisson elmm_poisson;
+int elmm_poisson_solver_new(elmm_poisson **out, const int32_t n[3], const double L[3],
+                            const int32_t bcs[6], int32_t precision, int32_t device);
+int elmm_poisson_solver_nonuniform_z_new(elmm_poisson **out, const int32_t n[3],
+                                         const double Lxy[2], const double *zPr,
+                                         const double *zW, const int32_t bcs[6],
+                                         int32_t precision, int32_t device);
+/* Phi(-1:nx+2,-1:ny+2,-1:nz+2) out (interior written, ghosts untouched),
+ * RHS(0:nx+1,0:ny+1,0:nz+1) in; host arrays. */
+int elmm_poisson_solver_execute(elmm_poisson *s, double *Phi, const double *RHS);
+int elmm_poisson_solver_finalize(elmm_poisson *s);
+
+/*
+ * Batched ensemble: n independent domains of uneven sizes stepped together.
+ * Every kernel of a stage runs once for the whole batch over a device table of
+ * domains; each RK3 step is one captured CUDA graph.
+ */
+typedef struct elmm_batch elmm_batch;
+int elmm_batch_create(const elmm_config *cfgs, int32_t n, elmm_batch **out);
+int elmm_batch_destroy(elmm_batch *b);
+int elmm_batch_upload_state(elmm_batch *b, int32_t d, const double *U, const double *V,
+                            const double *W, const double *Pr);
+int elmm_batch_download_state(elmm_batch *b, int32_t d, double *U, double *V, double *W,
+                              double *Pr);
+int elmm_batch_project(elmm_batch *b, double coef);
+int elmm_batch_step(elmm_batch *b, int32_t nsteps, elmm_stats *stats);
+/* total interior cells of the batch (for cell-steps/s) */
+int64_t elmm_batch_cells(const elmm_batch *b);
+
+/* Last error message of this thread (static storage). */
+const char *elmm_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ELMM_GPU_H */

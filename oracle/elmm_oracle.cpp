@@ -1,0 +1,1501 @@
+// elmm_oracle.cpp -- TEST INFRASTRUCTURE ONLY (the checker; never the product).
+//
+// A CPU, FP64 restatement of the ELMM per-timestep flow solve, written from the
+// reference Fortran so that the CUDA library can be checked against it, and
+// timed as the CPU baseline.  Only tests/, __graft_entry__.smoke() and the
+// cpu_baseline / reference legs of bench.py load it.
+//
+// Parity status: the reference (Fortran 2008 + an un-vendored PoisFFT module)
+// cannot be compiled in this environment, so this restatement is not pinned
+// to outputs of the reference itself ("parity unpinned" w.r.t. reference
+// binaries).  It is pinned to known answers derived from the mathematics:
+// the analytic Taylor-Green decay, the discrete divergence after a projection,
+// the residual of the Poisson operator of src/poisson.f90:23-60, and a dense
+// scipy solve of the same operator (tests/test_oracle_*.py).
+//
+// Every routine cites the reference lines it follows.  Arrays keep the
+// reference's Fortran layout and lower bounds (x fastest):
+//   U,V,W(-2:n+3)^3, Pr,Viscosity,Phi(-1:n+2)^3, RHS(0:n+1)^3.
+// Loops keep the reference's order of floating-point operations so that the
+// CUDA kernels, which follow the same formulas, agree to rounding.
+//
+// Supported subset (the hot path of the configurations in scope):
+//   BCs NOSLIP / FREESLIP / PERIODIC / NEUMANN on any side; uniform grid or
+//   stretched z (GRID_VARIABLE_Z); CDS2 skew-symmetric advection; Smagorinsky;
+//   explicit 2nd-order diffusion with the rough-wall log-law wall model at
+//   no-slip sides; incremental projection with FFT(x,y) + tridiagonal(z)
+//   Poisson solve; PRESSURE_REFERENCE_BOUNDARY at To; RK3.
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "../include/elmm_gpu.h"
+
+namespace orc {
+
+typedef std::complex<double> cd;
+
+// ---------------------------------------------------------------- arrays
+struct A1 {
+  int lo = 0;
+  std::vector<double> v;
+  void init(int l, int h) { lo = l; v.assign((size_t)(h - l + 1), 0.0); }
+  double &operator()(int i) { return v[(size_t)(i - lo)]; }
+  double operator()(int i) const { return v[(size_t)(i - lo)]; }
+};
+
+struct A3 {
+  int l0 = 0, l1 = 0, l2 = 0, n0 = 0, n1 = 0, n2 = 0;
+  std::vector<double> v;
+  void init(int a0, int b0, int a1, int b1, int a2, int b2) {
+    l0 = a0; l1 = a1; l2 = a2;
+    n0 = b0 - a0 + 1; n1 = b1 - a1 + 1; n2 = b2 - a2 + 1;
+    v.assign((size_t)n0 * n1 * n2, 0.0);
+  }
+  double &operator()(int i, int j, int k) {
+    return v[(size_t)(i - l0) + (size_t)n0 * ((size_t)(j - l1) + (size_t)n1 * (size_t)(k - l2))];
+  }
+  double operator()(int i, int j, int k) const {
+    return v[(size_t)(i - l0) + (size_t)n0 * ((size_t)(j - l1) + (size_t)n1 * (size_t)(k - l2))];
+  }
+  void fill(double x) { std::fill(v.begin(), v.end(), x); }
+};
+
+// Side indices as src/parameters.f90:193 (We=1 .. To=6).
+enum { We = 1, Ea = 2, So = 3, No = 4, Bo = 5, To = 6 };
+enum { BC_NOSLIP = 1, BC_FREESLIP = 2, BC_PERIODIC = 3, BC_NEUMANN = 5 };
+// Directions of src/wallmodels.f90:151.
+enum { MINUSX = 1, PLUSX = 2, MINUSY = 3, PLUSY = 4, MINUSZ = 5, PLUSZ = 6 };
+
+// RK3 coefficients, src/parameters.f90:317-320.
+static const double RK_alpha[3] = {4.0 / 15.0, 1.0 / 15.0, 1.0 / 6.0};
+static const double RK_beta[3] = {8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};
+static const double RK_rho[3] = {0.0, -17.0 / 60.0, -5.0 / 12.0};
+
+// WMPointUVW, src/wallmodels.f90:68-98 (fields used on the hot path).
+struct WMPointUVW {
+  double fluxp = 0, fluxm = 0;
+  int xi = 0, yj = 0, zk = 0;
+  double distx = 0, disty = 0, distz = 0;
+  double z0 = 0;
+  double ustar = 1;
+  double wallu = 0, wallv = 0, wallw = 0;
+};
+
+// ------------------------------------------------------------------- FFT
+// Mixed-radix decimation-in-time DFT, X[m] = sum_j x[j] exp(-2 pi i j m / n).
+struct FFTPlan {
+  int n = 0;
+  std::vector<int> fac;
+  std::vector<cd> w;  // w[m] = exp(-2 pi i m / n)
+  bool init(int n_) {
+    n = n_;
+    fac.clear();
+    int r = n;
+    for (int p : {4, 2, 3, 5}) {
+      while (r % p == 0) { fac.push_back(p); r /= p; }
+    }
+    if (r != 1) return false;
+    w.resize(n);
+    for (int m = 0; m < n; m++) {
+      double a = -2.0 * M_PI * (double)m / (double)n;
+      w[m] = cd(std::cos(a), std::sin(a));
+    }
+    return true;
+  }
+  void rec(const cd *x, int xs, cd *y, int len, int fi, int wstep) const {
+    if (len == 1) { y[0] = x[0]; return; }
+    int p = fac[fi], m = len / p;
+    for (int r = 0; r < p; r++) rec(x + (size_t)r * xs, xs * p, y + (size_t)r * m, m, fi + 1, wstep * p);
+    cd t[5];
+    for (int k = 0; k < m; k++) {
+      for (int r = 0; r < p; r++) t[r] = y[r * m + k] * w[((size_t)r * k * wstep) % n];
+      for (int q = 0; q < p; q++) {
+        cd s = 0;
+        for (int r = 0; r < p; r++) s += t[r] * w[((size_t)r * q * m * wstep) % n];
+        y[k + q * m] = s;
+      }
+    }
+  }
+  // forward DFT of x into y (distinct buffers)
+  void forward(const cd *x, cd *y) const { rec(x, 1, y, n, 0, 1); }
+  // unnormalised inverse, X -> sum_m X[m] exp(+2 pi i j m / n)
+  void inverse(const cd *x, cd *y, std::vector<cd> &tmp) const {
+    tmp.resize(n);
+    for (int i = 0; i < n; i++) tmp[i] = std::conj(x[i]);
+    rec(tmp.data(), 1, y, n, 0, 1);
+    for (int i = 0; i < n; i++) y[i] = std::conj(y[i]);
+  }
+};
+
+// -------------------------------------------------------------- domain
+struct Domain {
+  int Prnx, Prny, Prnz, Unx, Uny, Unz, Vnx, Vny, Vnz, Wnx, Wny, Wnz;
+  int Btype[7], PrBtype[7];
+  int gridtype;  // 0 uniform, 1 variable z
+  double dxmin, dymin, dzmin;
+  A1 xU, yV, zW, xPr, dxPr, yPr, dyPr, zPr, dzPr, dxU, dyV, dzW;
+  double molecular_viscosity, C_Smagorinsky, filter_ratio;
+  int sgstype, wallmodeltype;
+  double z0s[7];
+  int en_prgx, en_prgy;
+  double prgx, prgy;
+  double dt, time;
+  int enable_CFL_check;
+  double CFL;
+  A3 U, V, W, U2, V2, W2, Ustar, Vstar, Wstar, Pr, Viscosity, Phi, RHS;
+  std::vector<WMPointUVW> wm[7][4];  // [direction][component]
+  // Poisson
+  FFTPlan px, py;
+  int nxh;
+  std::vector<double> lamx, lamy, Ab, At, dzc, dzf;  // tridiagonal data
+  int zper;
+  double max_div;
+};
+
+// ------------------------------------------------- grid, initial.f90:4395-4480
+static void init_grid(Domain &d, const elmm_config &c) {
+  int nx = d.Prnx, ny = d.Prny, nz = d.Prnz;
+  A1 xU2, yV2, zW2;
+  xU2.init(-3, nx + 3);
+  yV2.init(-3, ny + 3);
+  zW2.init(-3, nz + 3);
+  for (int i = -3; i <= nx + 3; i++) xU2(i) = i * d.dxmin + c.xmin;
+  for (int j = -3; j <= ny + 3; j++) yV2(j) = j * d.dymin + c.ymin;
+  if (c.zW) {
+    for (int k = 0; k <= nz; k++) zW2(k) = c.zW[k];
+    if (d.Btype[Bo] == BC_PERIODIC) {
+      for (int j = -1; j >= -3; j--) zW2(j) = zW2(0) - (zW2(nz - 1) - zW2(nz - 1 + j));
+    } else {
+      for (int j = -1; j >= -3; j--) zW2(j) = zW2(0) - (zW2(-j) - zW2(0));
+    }
+    if (d.Btype[To] == BC_PERIODIC) {
+      for (int j = nz + 1; j <= nz + 3; j++) zW2(j) = zW2(nz - 1) + (zW2(j - nz + 1) - zW2(0));
+    } else {
+      // initial.f90:4427-4430, kept as written (mirror about zW(nz-1))
+      for (int j = nz + 1; j <= nz + 3; j++)
+        zW2(j) = zW2(nz - 1) + (zW2(nz - 1) - zW2(nz - 1 - (j - nz + 1)));
+    }
+  } else {
+    for (int k = -3; k <= nz + 3; k++) zW2(k) = k * d.dzmin + c.zmin;
+  }
+  d.xU = xU2; d.yV = yV2; d.zW = zW2;
+  d.xPr.init(-2, nx + 3); d.dxPr.init(-2, nx + 3);
+  d.yPr.init(-2, ny + 3); d.dyPr.init(-2, ny + 3);
+  d.zPr.init(-2, nz + 3); d.dzPr.init(-2, nz + 3);
+  d.dxU.init(-2, nx + 2); d.dyV.init(-2, ny + 2); d.dzW.init(-2, nz + 2);
+  for (int i = -2; i <= nx + 3; i++) { d.xPr(i) = (d.xU(i - 1) + d.xU(i)) / 2.0; d.dxPr(i) = d.xU(i) - d.xU(i - 1); }
+  for (int j = -2; j <= ny + 3; j++) { d.yPr(j) = (d.yV(j - 1) + d.yV(j)) / 2.0; d.dyPr(j) = d.yV(j) - d.yV(j - 1); }
+  for (int k = -2; k <= nz + 3; k++) { d.zPr(k) = (d.zW(k - 1) + d.zW(k)) / 2.0; d.dzPr(k) = d.zW(k) - d.zW(k - 1); }
+  for (int i = -2; i <= nx + 2; i++) d.dxU(i) = d.xPr(i + 1) - d.xPr(i);
+  for (int j = -2; j <= ny + 2; j++) d.dyV(j) = d.yPr(j + 1) - d.yPr(j);
+  for (int k = -2; k <= nz + 2; k++) d.dzW(k) = d.zPr(k + 1) - d.zPr(k);
+  if (c.zW) {
+    double m = d.dzPr(-2);
+    for (int k = -2; k <= nz + 3; k++) m = std::min(m, d.dzPr(k));
+    d.dzmin = m;
+  }
+}
+
+// ------------------------------------ wall-model points, wallmodels.f90:690-909
+static void add_wm_points(Domain &d) {
+  for (int comp = 1; comp <= 3; comp++) {
+    int nx = comp == 1 ? d.Unx : comp == 2 ? d.Vnx : d.Wnx;
+    int ny = comp == 1 ? d.Uny : comp == 2 ? d.Vny : d.Wny;
+    int nz = comp == 1 ? d.Unz : comp == 2 ? d.Vnz : d.Wnz;
+    const A1 &x = comp == 1 ? d.xU : d.xPr;
+    const A1 &y = comp == 2 ? d.yV : d.yPr;
+    const A1 &z = comp == 3 ? d.zW : d.zPr;
+    WMPointUVW p;
+    if (d.Btype[We] == BC_NOSLIP)
+      for (int k = 1; k <= nz; k++)
+        for (int j = 1; j <= ny; j++) {
+          p = WMPointUVW(); p.xi = 1; p.yj = j; p.zk = k;
+          p.distx = d.xU(0) - x(1); p.z0 = d.z0s[We];
+          d.wm[MINUSX][comp].push_back(p);
+        }
+    if (d.Btype[Ea] == BC_NOSLIP)
+      for (int k = 1; k <= nz; k++)
+        for (int j = 1; j <= ny; j++) {
+          p = WMPointUVW(); p.xi = nx; p.yj = j; p.zk = k;
+          p.distx = d.xU(d.Unx + 1) - x(nx); p.z0 = d.z0s[Ea];
+          d.wm[PLUSX][comp].push_back(p);
+        }
+    if (d.Btype[So] == BC_NOSLIP)
+      for (int k = 1; k <= nz; k++)
+        for (int i = 1; i <= nx; i++) {
+          p = WMPointUVW(); p.xi = i; p.yj = 1; p.zk = k;
+          p.disty = d.yV(0) - y(1); p.z0 = d.z0s[So];
+          d.wm[MINUSY][comp].push_back(p);
+        }
+    if (d.Btype[No] == BC_NOSLIP)
+      for (int k = 1; k <= nz; k++)
+        for (int i = 1; i <= nx; i++) {
+          p = WMPointUVW(); p.xi = i; p.yj = ny; p.zk = k;
+          p.disty = d.yV(d.Vny + 1) - y(ny); p.z0 = d.z0s[No];
+          d.wm[PLUSY][comp].push_back(p);
+        }
+    if (d.Btype[Bo] == BC_NOSLIP)
+      for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++) {
+          p = WMPointUVW(); p.xi = i; p.yj = j; p.zk = 1;
+          p.distz = d.zW(0) - z(1); p.z0 = d.z0s[Bo];
+          d.wm[MINUSZ][comp].push_back(p);
+        }
+    if (d.Btype[To] == BC_NOSLIP)
+      for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++) {
+          p = WMPointUVW(); p.xi = i; p.yj = j; p.zk = nz;
+          p.distz = d.zW(d.Wnz + 1) - z(nz); p.z0 = d.z0s[To];
+          d.wm[PLUSZ][comp].push_back(p);
+        }
+  }
+}
+
+// ------------------------------------------ BoundUVW_do_BC, boundaries.f90:398-1791
+// The x pass fills i-ghosts for interior j,k; the y pass all i; the z pass all
+// i,j.  periodic_corners_edges (boundaries.f90:189-394) only writes cells that
+// these three passes overwrite afterwards, so it does not change the result.
+static void bound_x(Domain &d, A3 &X, int comp, int n, int ny, int nz) {
+  bool normal = comp == 1;
+  for (int k = 1; k <= nz; k++)
+    for (int j = 1; j <= ny; j++) {
+      switch (d.Btype[We]) {
+        case BC_NOSLIP:
+          if (normal) { X(0, j, k) = 0; X(-1, j, k) = -X(1, j, k); X(-2, j, k) = -X(2, j, k); }
+          else { X(0, j, k) = -X(1, j, k); X(-1, j, k) = -X(2, j, k); X(-2, j, k) = -X(3, j, k); }
+          break;
+        case BC_NEUMANN:
+          X(0, j, k) = X(1, j, k); X(-1, j, k) = X(1, j, k); X(-2, j, k) = X(1, j, k);
+          break;
+        case BC_FREESLIP:
+          if (normal) { X(0, j, k) = 0; X(-1, j, k) = -X(1, j, k); X(-2, j, k) = -X(2, j, k); }
+          else { X(0, j, k) = X(1, j, k); X(-1, j, k) = X(1, j, k); X(-2, j, k) = X(1, j, k); }
+          break;
+        case BC_PERIODIC:
+          X(0, j, k) = X(n, j, k); X(-1, j, k) = X(n - 1, j, k); X(-2, j, k) = X(n - 2, j, k);
+          break;
+      }
+    }
+  for (int k = 1; k <= nz; k++)
+    for (int j = 1; j <= ny; j++) {
+      switch (d.Btype[Ea]) {
+        case BC_NOSLIP:
+          if (normal) { X(n + 1, j, k) = 0; X(n + 2, j, k) = -X(n, j, k); X(n + 3, j, k) = -X(n - 1, j, k); }
+          else { X(n + 1, j, k) = -X(n, j, k); X(n + 2, j, k) = -X(n - 1, j, k); X(n + 3, j, k) = -X(n - 2, j, k); }
+          break;
+        case BC_NEUMANN:
+          X(n + 1, j, k) = X(n, j, k); X(n + 2, j, k) = X(n, j, k); X(n + 3, j, k) = X(n, j, k);
+          break;
+        case BC_FREESLIP:
+          if (normal) { X(n + 1, j, k) = 0; X(n + 2, j, k) = -X(n, j, k); X(n + 3, j, k) = -X(n - 1, j, k); }
+          else { X(n + 1, j, k) = X(n, j, k); X(n + 2, j, k) = X(n, j, k); X(n + 3, j, k) = X(n, j, k); }
+          break;
+        case BC_PERIODIC:
+          X(n + 1, j, k) = X(1, j, k); X(n + 2, j, k) = X(2, j, k); X(n + 3, j, k) = X(3, j, k);
+          break;
+      }
+    }
+}
+
+static void bound_y(Domain &d, A3 &X, int comp, int nx, int n, int nz) {
+  bool normal = comp == 2;
+  for (int k = 1; k <= nz; k++)
+    for (int i = -2; i <= nx + 3; i++) {
+      switch (d.Btype[So]) {
+        case BC_NOSLIP:
+          if (normal) { X(i, 0, k) = 0; X(i, -1, k) = -X(i, 1, k); X(i, -2, k) = -X(i, 2, k); }
+          else { X(i, 0, k) = -X(i, 1, k); X(i, -1, k) = -X(i, 2, k); X(i, -2, k) = -X(i, 3, k); }
+          break;
+        case BC_NEUMANN:
+          X(i, 0, k) = X(i, 1, k); X(i, -1, k) = X(i, 1, k); X(i, -2, k) = X(i, 1, k);
+          break;
+        case BC_FREESLIP:
+          if (normal) { X(i, 0, k) = 0; X(i, -1, k) = -X(i, 1, k); X(i, -2, k) = -X(i, 2, k); }
+          else { X(i, 0, k) = X(i, 1, k); X(i, -1, k) = X(i, 1, k); X(i, -2, k) = X(i, 1, k); }
+          break;
+        case BC_PERIODIC:
+          X(i, 0, k) = X(i, n, k); X(i, -1, k) = X(i, n - 1, k); X(i, -2, k) = X(i, n - 2, k);
+          break;
+      }
+    }
+  for (int k = 1; k <= nz; k++)
+    for (int i = -2; i <= nx + 3; i++) {
+      switch (d.Btype[No]) {
+        case BC_NOSLIP:
+          if (normal) { X(i, n + 1, k) = 0; X(i, n + 2, k) = -X(i, n, k); X(i, n + 3, k) = -X(i, n - 1, k); }
+          else { X(i, n + 1, k) = -X(i, n, k); X(i, n + 2, k) = -X(i, n - 1, k); X(i, n + 3, k) = -X(i, n - 2, k); }
+          break;
+        case BC_NEUMANN:
+          X(i, n + 1, k) = X(i, n, k); X(i, n + 2, k) = X(i, n, k); X(i, n + 3, k) = X(i, n, k);
+          break;
+        case BC_FREESLIP:
+          if (normal) { X(i, n + 1, k) = 0; X(i, n + 2, k) = -X(i, n, k); X(i, n + 3, k) = -X(i, n - 1, k); }
+          else { X(i, n + 1, k) = X(i, n, k); X(i, n + 2, k) = X(i, n, k); X(i, n + 3, k) = X(i, n, k); }
+          break;
+        case BC_PERIODIC:
+          X(i, n + 1, k) = X(i, 1, k); X(i, n + 2, k) = X(i, 2, k); X(i, n + 3, k) = X(i, 3, k);
+          break;
+      }
+    }
+}
+
+static void bound_z(Domain &d, A3 &X, int comp, int nx, int ny, int n) {
+  bool normal = comp == 3;
+  for (int j = -2; j <= ny + 3; j++)
+    for (int i = -2; i <= nx + 3; i++) {
+      switch (d.Btype[Bo]) {
+        case BC_NOSLIP:
+          if (normal) { X(i, j, 0) = 0; X(i, j, -1) = -X(i, j, 1); X(i, j, -2) = -X(i, j, 2); }
+          else { X(i, j, 0) = -X(i, j, 1); X(i, j, -1) = -X(i, j, 2); X(i, j, -2) = -X(i, j, 3); }
+          break;
+        case BC_NEUMANN:
+          X(i, j, 0) = X(i, j, 1); X(i, j, -1) = X(i, j, 1); X(i, j, -2) = X(i, j, 1);
+          break;
+        case BC_FREESLIP:
+          if (normal) { X(i, j, 0) = 0; X(i, j, -1) = -X(i, j, 1); X(i, j, -2) = -X(i, j, 2); }
+          else { X(i, j, 0) = X(i, j, 1); X(i, j, -1) = X(i, j, 1); X(i, j, -2) = X(i, j, 1); }
+          break;
+        case BC_PERIODIC:
+          X(i, j, 0) = X(i, j, n); X(i, j, -1) = X(i, j, n - 1); X(i, j, -2) = X(i, j, n - 2);
+          break;
+      }
+    }
+  for (int j = -2; j <= ny + 3; j++)
+    for (int i = -2; i <= nx + 3; i++) {
+      switch (d.Btype[To]) {
+        case BC_NOSLIP:
+          if (normal) { X(i, j, n + 1) = 0; X(i, j, n + 2) = -X(i, j, n); X(i, j, n + 3) = -X(i, j, n - 1); }
+          else { X(i, j, n + 1) = -X(i, j, n); X(i, j, n + 2) = -X(i, j, n - 1); X(i, j, n + 3) = -X(i, j, n - 2); }
+          break;
+        case BC_NEUMANN:
+          X(i, j, n + 1) = X(i, j, n); X(i, j, n + 2) = X(i, j, n); X(i, j, n + 3) = X(i, j, n);
+          break;
+        case BC_FREESLIP:
+          if (normal) { X(i, j, n + 1) = 0; X(i, j, n + 2) = -X(i, j, n); X(i, j, n + 3) = -X(i, j, n - 1); }
+          else { X(i, j, n + 1) = X(i, j, n); X(i, j, n + 2) = X(i, j, n); X(i, j, n + 3) = X(i, j, n); }
+          break;
+        case BC_PERIODIC:
+          X(i, j, n + 1) = X(i, j, 1); X(i, j, n + 2) = X(i, j, 2); X(i, j, n + 3) = X(i, j, 3);
+          break;
+      }
+    }
+}
+
+static void BoundUVW(Domain &d, A3 &U, A3 &V, A3 &W) {
+  bound_x(d, U, 1, d.Unx, d.Uny, d.Unz);
+  bound_x(d, V, 2, d.Vnx, d.Vny, d.Vnz);
+  bound_x(d, W, 3, d.Wnx, d.Wny, d.Wnz);
+  bound_y(d, V, 2, d.Vnx, d.Vny, d.Vnz);
+  bound_y(d, U, 1, d.Unx, d.Uny, d.Unz);
+  bound_y(d, W, 3, d.Wnx, d.Wny, d.Wnz);
+  bound_z(d, W, 3, d.Wnx, d.Wny, d.Wnz);
+  bound_z(d, U, 1, d.Unx, d.Uny, d.Unz);
+  bound_z(d, V, 2, d.Vnx, d.Vny, d.Vnz);
+}
+
+// --------------------------------- BoundViscosity, scalarboundaries.f90:326-431
+static void BoundViscosity(Domain &d, A3 &Nu) {
+  int nx = d.Prnx, ny = d.Prny, nz = d.Prnz;
+  for (int k = 1; k <= nz; k++)
+    for (int j = 1; j <= ny; j++) Nu(0, j, k) = d.Btype[We] == BC_PERIODIC ? Nu(nx, j, k) : Nu(1, j, k);
+  for (int k = 1; k <= nz; k++)
+    for (int j = 1; j <= ny; j++) Nu(nx + 1, j, k) = d.Btype[Ea] == BC_PERIODIC ? Nu(1, j, k) : Nu(nx, j, k);
+  for (int k = 1; k <= nz; k++)
+    for (int i = 0; i <= nx + 1; i++) Nu(i, 0, k) = d.Btype[So] == BC_PERIODIC ? Nu(i, ny, k) : Nu(i, 1, k);
+  for (int k = 1; k <= nz; k++)
+    for (int i = 0; i <= nx + 1; i++) Nu(i, ny + 1, k) = d.Btype[No] == BC_PERIODIC ? Nu(i, 1, k) : Nu(i, ny, k);
+  for (int j = 0; j <= ny + 1; j++)
+    for (int i = 0; i <= nx + 1; i++) Nu(i, j, 0) = d.Btype[Bo] == BC_PERIODIC ? Nu(i, j, nz) : Nu(i, j, 1);
+  for (int j = 0; j <= ny + 1; j++)
+    for (int i = 0; i <= nx + 1; i++) Nu(i, j, nz + 1) = d.Btype[To] == BC_PERIODIC ? Nu(i, j, 1) : Nu(i, j, nz);
+}
+
+// --------------------------------------------- Bound_Phi, boundaries.f90:1817-1948
+static void Bound_Phi(Domain &d, A3 &Phi) {
+  int nx = d.Prnx, ny = d.Prny, nz = d.Prnz;
+  for (int k = 1; k <= nz; k++)
+    for (int j = 1; j <= ny; j++) {
+      if (d.PrBtype[We] == BC_PERIODIC) { Phi(-1, j, k) = Phi(nx - 1, j, k); Phi(0, j, k) = Phi(nx, j, k); }
+      else { Phi(-1, j, k) = Phi(2, j, k); Phi(0, j, k) = Phi(1, j, k); }
+      if (d.PrBtype[Ea] == BC_PERIODIC) { Phi(nx + 1, j, k) = Phi(1, j, k); Phi(nx + 2, j, k) = Phi(2, j, k); }
+      else { Phi(nx + 1, j, k) = Phi(nx, j, k); Phi(nx + 2, j, k) = Phi(nx - 1, j, k); }
+    }
+  for (int k = 1; k <= nz; k++)
+    for (int i = 1; i <= nx; i++) {
+      if (d.PrBtype[So] == BC_PERIODIC) { Phi(i, -1, k) = Phi(i, ny - 1, k); Phi(i, 0, k) = Phi(i, ny, k); }
+      else { Phi(i, -1, k) = Phi(i, 2, k); Phi(i, 0, k) = Phi(i, 1, k); }
+      if (d.PrBtype[No] == BC_PERIODIC) { Phi(i, ny + 1, k) = Phi(i, 1, k); Phi(i, ny + 2, k) = Phi(i, 2, k); }
+      else { Phi(i, ny + 1, k) = Phi(i, ny, k); Phi(i, ny + 2, k) = Phi(i, ny - 1, k); }
+    }
+  for (int j = 1; j <= ny; j++)
+    for (int i = 1; i <= nx; i++) {
+      if (d.PrBtype[Bo] == BC_PERIODIC) { Phi(i, j, -1) = Phi(i, j, nz - 1); Phi(i, j, 0) = Phi(i, j, nz); }
+      else { Phi(i, j, -1) = Phi(i, j, 2); Phi(i, j, 0) = Phi(i, j, 1); }
+      if (d.PrBtype[To] == BC_PERIODIC) { Phi(i, j, nz + 1) = Phi(i, j, 1); Phi(i, j, nz + 2) = Phi(i, j, 2); }
+      else { Phi(i, j, nz + 1) = Phi(i, j, nz); Phi(i, j, nz + 2) = Phi(i, j, nz - 1); }
+    }
+}
+
+// ---------------------------------------------- Bound_Pr, boundaries.f90:1951-2091
+static void Bound_Pr(Domain &d, A3 &Pr) {
+  int nx = d.Prnx, ny = d.Prny, nz = d.Prnz;
+  for (int k = 1; k <= nz; k++)
+    for (int j = 1; j <= ny; j++) {
+      if (d.PrBtype[We] == BC_PERIODIC) { Pr(-1, j, k) = Pr(nx - 1, j, k); Pr(0, j, k) = Pr(nx, j, k); }
+      else { Pr(0, j, k) = Pr(3, j, k) - 3 * (Pr(2, j, k) - Pr(1, j, k)); Pr(-1, j, k) = Pr(2, j, k); }
+      if (d.PrBtype[Ea] == BC_PERIODIC) { Pr(nx + 1, j, k) = Pr(1, j, k); Pr(nx + 2, j, k) = Pr(2, j, k); }
+      else { Pr(nx + 1, j, k) = Pr(nx - 2, j, k) - 3 * (Pr(nx - 1, j, k) - Pr(nx, j, k)); Pr(nx + 2, j, k) = Pr(nx - 1, j, k); }
+    }
+  for (int k = 1; k <= nz; k++)
+    for (int i = 1; i <= nx; i++) {
+      if (d.PrBtype[So] == BC_PERIODIC) { Pr(i, -1, k) = Pr(i, ny - 1, k); Pr(i, 0, k) = Pr(i, ny, k); }
+      else { Pr(i, 0, k) = Pr(i, 3, k) - 3 * (Pr(i, 2, k) - Pr(i, 1, k)); Pr(i, -1, k) = Pr(i, 2, k); }
+      if (d.PrBtype[No] == BC_PERIODIC) { Pr(i, ny + 1, k) = Pr(i, 1, k); Pr(i, ny + 2, k) = Pr(i, 2, k); }
+      else { Pr(i, ny + 1, k) = Pr(i, ny - 2, k) - 3 * (Pr(i, ny - 1, k) - Pr(i, ny, k)); Pr(i, ny + 2, k) = Pr(i, ny - 1, k); }
+    }
+  for (int j = 1; j <= ny; j++)
+    for (int i = 1; i <= nx; i++) {
+      if (d.PrBtype[Bo] == BC_PERIODIC) { Pr(i, j, -1) = Pr(i, j, nz - 1); Pr(i, j, 0) = Pr(i, j, nz); }
+      else { Pr(i, j, 0) = Pr(i, j, 3) - 3 * (Pr(i, j, 2) - Pr(i, j, 1)); Pr(i, j, -1) = Pr(i, j, 2); }
+      if (d.PrBtype[To] == BC_PERIODIC) { Pr(i, j, nz + 1) = Pr(i, j, 1); Pr(i, j, nz + 2) = Pr(i, j, 2); }
+      else { Pr(i, j, nz + 1) = Pr(i, j, nz - 2) - 3 * (Pr(i, j, nz - 1) - Pr(i, j, nz)); Pr(i, j, nz + 2) = Pr(i, j, nz - 1); }
+    }
+}
+
+// --------------------------------------- SGS_Smag / NuSmag, subgrid.f90:30-67, :170-209
+static inline double nusmag(const Domain &d, int i, int j, int k) {
+  const A3 &U = d.U, &V = d.V, &W = d.W;
+  double width = d.filter_ratio * std::pow(d.dxPr(i) * d.dyPr(j) * d.dzPr(k), 1.0 / 3.0);
+  double D[3][3];
+  D[0][0] = (U(i, j, k) - U(i - 1, j, k)) / d.dxmin;
+  D[1][1] = (V(i, j, k) - V(i, j - 1, k)) / d.dymin;
+  D[2][2] = (W(i, j, k) - W(i, j, k - 1)) / d.dzPr(k);
+  D[0][1] = (U(i, j + 1, k) + U(i - 1, j + 1, k) - U(i, j - 1, k) - U(i - 1, j - 1, k)) / (4 * d.dymin);
+  D[0][2] = (U(i, j, k + 1) + U(i - 1, j, k + 1) - U(i, j, k - 1) - U(i - 1, j, k - 1)) / (2 * (d.zPr(k + 1) - d.zPr(k - 1)));
+  D[1][0] = (V(i + 1, j, k) + V(i + 1, j - 1, k) - V(i - 1, j, k) - V(i - 1, j - 1, k)) / (4 * d.dxmin);
+  D[1][2] = (V(i, j, k + 1) + V(i, j - 1, k + 1) - V(i, j, k - 1) - V(i, j - 1, k - 1)) / (2 * (d.zPr(k + 1) - d.zPr(k - 1)));
+  D[2][0] = (W(i + 1, j, k) + W(i + 1, j, k - 1) - W(i - 1, j, k) - W(i - 1, j, k - 1)) / (4 * d.dxmin);
+  D[2][1] = (W(i, j + 1, k) + W(i, j + 1, k - 1) - W(i, j - 1, k) - W(i, j - 1, k - 1)) / (4 * d.dymin);
+  double S = 0;
+  for (int jj = 0; jj < 3; jj++)
+    for (int ii = 0; ii < 3; ii++) {
+      double s = (D[ii][jj] + D[jj][ii]) / 2;
+      S = S + s * s;
+    }
+  double Sbar = std::sqrt(2.0 * S);
+  double wc = width * d.C_Smagorinsky;
+  return Sbar * (wc * wc);
+}
+
+static void SubgridModel(Domain &d) {
+  if (d.sgstype == 1) {
+#pragma omp parallel for collapse(2)
+    for (int k = 1; k <= d.Prnz; k++)
+      for (int j = 1; j <= d.Prny; j++)
+        for (int i = 1; i <= d.Prnx; i++) d.Viscosity(i, j, k) = nusmag(d, i, j, k);
+    if (d.molecular_viscosity > 0)
+      for (auto &x : d.Viscosity.v) x = x + d.molecular_viscosity;
+  } else {
+    d.Viscosity.fill(d.molecular_viscosity);
+  }
+}
+
+// ----------------------------------------------- wall model, wallmodels.f90:1190-1400
+// NORM2 evaluated with the scaled sum of squares used by gfortran.
+static inline double norm2_3(const double *x) {
+  double scale = 0, ssq = 1;
+  for (int m = 0; m < 3; m++) {
+    if (x[m] != 0) {
+      double ax = std::fabs(x[m]);
+      if (scale < ax) { double r = scale / ax; ssq = 1 + ssq * (r * r); scale = ax; }
+      else { double r = ax / scale; ssq = ssq + r * r; }
+    }
+  }
+  return scale * std::sqrt(ssq);
+}
+
+static void WMFlatUstar(const Domain &d, double &ustar, double vel, double dist) {
+  const double nu = d.molecular_viscosity;
+  const double eps = 1e-4, zpl_lam = 5.0, zpl_turb = 30.0;
+  if (nu <= 0) { ustar = 0; return; }
+  double ustar_lam = std::sqrt(nu * vel / dist);
+  if ((dist * ustar_lam / nu) < zpl_lam) {
+    ustar = ustar_lam;
+  } else {
+    int i = 0;
+    for (;;) {
+      i = i + 1;
+      double ustar2 = ustar;
+      double z_pl = dist * ustar2 / nu;
+      if (z_pl <= zpl_lam) ustar = std::sqrt(nu * vel / dist);
+      else if (z_pl < zpl_turb) ustar = vel / (5 * std::log(z_pl) - (double)3.05f);  // 3.05 is a default-real literal
+      else ustar = vel / (std::log(z_pl) / 0.4 + 5.5);
+      if (std::fabs(ustar - ustar2) / std::fabs(ustar) < eps) break;
+      if (i >= 50) { ustar = 0; break; }
+    }
+  }
+}
+
+static void WMRoughUstar(const Domain &d, double &ustar, double vel, double dist, double z0) {
+  const double nu = d.molecular_viscosity;
+  const double yplcrit = 11.225;
+  if (nu > 0) {
+    ustar = std::sqrt(nu * vel / dist);
+    if (dist * ustar / nu < yplcrit * 1.1) return;
+  }
+  if (dist <= z0 * 2) {
+    if (nu > 0) WMFlatUstar(d, ustar, vel, dist);
+    else ustar = 0;
+  } else {
+    ustar = vel * 0.41 / std::log(dist / z0);
+  }
+}
+
+// local_velocity, wallmodels.f90:2354-2396
+static void local_velocity(const Domain &d, int comp, int xi, int yj, int zk, double *vel) {
+  const A3 &U = d.U, &V = d.V, &W = d.W;
+  if (comp == 1) {
+    vel[0] = U(xi, yj, zk);
+    vel[1] = (V(xi + 1, yj, zk) + V(xi, yj, zk) + V(xi + 1, yj - 1, zk) + V(xi, yj - 1, zk)) / 4.0;
+    vel[2] = (W(xi + 1, yj, zk) + W(xi, yj, zk) + W(xi + 1, yj, zk - 1) + W(xi, yj, zk - 1)) / 4.0;
+  } else if (comp == 2) {
+    vel[0] = (U(xi, yj + 1, zk) + U(xi, yj, zk) + U(xi - 1, yj + 1, zk) + U(xi - 1, yj, zk)) / 4.0;
+    vel[1] = V(xi, yj, zk);
+    vel[2] = (W(xi, yj + 1, zk) + W(xi, yj, zk) + W(xi, yj + 1, zk - 1) + W(xi, yj, zk - 1)) / 4.0;
+  } else {
+    vel[0] = (U(xi, yj, zk + 1) + U(xi, yj, zk) + U(xi - 1, yj, zk + 1) + U(xi - 1, yj, zk)) / 4.0;
+    vel[1] = (V(xi, yj, zk + 1) + V(xi, yj, zk) + V(xi, yj - 1, zk + 1) + V(xi, yj - 1, zk)) / 4.0;
+    vel[2] = W(xi, yj, zk);
+  }
+}
+
+// ComputeUVWFluxesWM / fluxes, wallmodels.f90:2159-2338 (rough wall, neutral)
+static void ComputeUVWFluxesWM(Domain &d) {
+  const double eps = std::sqrt(2.220446049250313e-16);
+  double drec[7] = {0, 1 / d.dxmin, 1 / d.dxmin, 1 / d.dymin, 1 / d.dymin, 1 / d.dzmin, 1 / d.dzmin};
+  for (int comp = 1; comp <= 3; comp++)
+    for (int dir = 1; dir <= 6; dir++) {
+      auto &pts = d.wm[dir][comp];
+      for (size_t n = 0; n < pts.size(); n++) {
+        WMPointUVW &p = pts[n];
+        double dist[3] = {p.distx, p.disty, p.distz};
+        double vel[3];
+        local_velocity(d, comp, p.xi, p.yj, p.zk, vel);
+        double wallvel[3] = {p.wallu, p.wallv, p.wallw};
+        // WMRoughStress -> vel_and_dist (wallmodels.f90:1383-1389)
+        double dd = norm2_3(dist);
+        double t[3];
+        for (int m = 0; m < 3; m++) t[m] = vel[m] - wallvel[m];
+        double dot = t[0] * dist[0] + t[1] * dist[1] + t[2] * dist[2];
+        for (int m = 0; m < 3; m++) t[m] = t[m] - dot * dist[m] / (dd * dd);
+        double tv = norm2_3(t);
+        if (tv != 0) WMRoughUstar(d, p.ustar, tv, dd, p.z0);
+        if (p.ustar < 0) p.ustar = 0;
+        double mag = norm2_3(t);
+        if (mag > eps) {
+          if (d.gridtype == 1 && dir == MINUSZ) {
+            p.fluxp = (t[comp - 1] / mag) * (p.ustar * p.ustar);
+            p.fluxm = p.fluxp;
+            if (comp == 1 || comp == 2) { p.fluxp = p.fluxp / d.dzPr(p.zk); p.fluxm = p.fluxm / d.dzPr(p.zk - 1); }
+            else { p.fluxp = p.fluxp / d.dzW(p.zk); p.fluxm = p.fluxm / d.dzW(p.zk - 1); }
+          } else if (d.gridtype == 1 && dir == PLUSZ) {
+            p.fluxp = (t[comp - 1] / mag) * (p.ustar * p.ustar);
+            p.fluxm = p.fluxp;
+            if (comp == 1 || comp == 2) { p.fluxp = p.fluxp / d.dzPr(p.zk + 1); p.fluxm = p.fluxm / d.dzPr(p.zk); }
+            else { p.fluxp = p.fluxp / d.dzW(p.zk + 1); p.fluxm = p.fluxm / d.dzW(p.zk); }
+          } else {
+            p.fluxp = (t[comp - 1] / mag) * (p.ustar * p.ustar) * drec[dir];
+            p.fluxm = p.fluxp;
+          }
+          if (dir % 2 == 1) { p.fluxp = -p.fluxp; p.fluxm = -p.fluxm; }
+        } else {
+          p.fluxp = 0;
+          p.fluxm = p.fluxp;
+        }
+      }
+    }
+}
+
+// SubgridStresses, dynamics.f90:869-908 (ComputeViscsWM only sets Viscosity at
+// wall cells, which SubgridModel then overwrites everywhere; it is omitted).
+static void SubgridStresses(Domain &d) {
+  SubgridModel(d);
+  if (d.wallmodeltype > 0) ComputeUVWFluxesWM(d);
+  BoundViscosity(d, d.Viscosity);
+}
+
+// ---------------------------------------------- CDS2 advection, advection.f90:15-327
+static void CDU(Domain &d, A3 &U2) {
+  const A3 &U = d.U, &V = d.V, &W = d.W;
+  U2.fill(0);
+  if (d.gridtype == 0) {
+    double Ax = 0.25 / d.dxmin, Ay = 0.25 / d.dymin, Az = 0.25 / d.dzmin;
+#pragma omp parallel for collapse(2)
+    for (int k = 1; k <= d.Unz; k++)
+      for (int j = 1; j <= d.Uny; j++)
+        for (int i = 1; i <= d.Unx; i++) {
+          U2(i, j, k) = -((Ax * (U(i + 1, j, k) + U(i, j, k)) * (U(i + 1, j, k) + U(i, j, k))
+                           - Ax * (U(i, j, k) + U(i - 1, j, k)) * (U(i, j, k) + U(i - 1, j, k)))
+                          + (Ay * (U(i, j + 1, k) + U(i, j, k)) * (V(i + 1, j, k) + V(i, j, k))
+                             - Ay * (U(i, j, k) + U(i, j - 1, k)) * (V(i + 1, j - 1, k) + V(i, j - 1, k)))
+                          + (Az * (U(i, j, k + 1) + U(i, j, k)) * (W(i + 1, j, k) + W(i, j, k))
+                             - Az * (U(i, j, k) + U(i, j, k - 1)) * (W(i + 1, j, k - 1) + W(i, j, k - 1))));
+        }
+    Ax = 0.5 / d.dxmin; Ay = 0.125 / d.dymin; Az = 0.125 / d.dzmin;
+#pragma omp parallel for collapse(2)
+    for (int k = 1; k <= d.Unz; k++)
+      for (int j = 1; j <= d.Uny; j++)
+        for (int i = 1; i <= d.Unx; i++) {
+          double Vadv = (V(i, j, k) + V(i + 1, j, k) + V(i, j - 1, k) + V(i + 1, j - 1, k));
+          double Wadv = (W(i, j, k) + W(i + 1, j, k) + W(i, j, k - 1) + W(i + 1, j, k - 1));
+          U2(i, j, k) = U2(i, j, k) - (Ax * (U(i + 1, j, k) - U(i - 1, j, k)) * U(i, j, k)
+                                       + Ay * (U(i, j + 1, k) - U(i, j - 1, k)) * Vadv
+                                       + Az * (U(i, j, k + 1) - U(i, j, k - 1)) * Wadv);
+        }
+  } else {  // advection_variable_z.f90:15-46, :151-181
+    double Ax = 0.25 / d.dxmin, Ay = 0.25 / d.dymin;
+#pragma omp parallel for collapse(2)
+    for (int k = 1; k <= d.Unz; k++)
+      for (int j = 1; j <= d.Uny; j++)
+        for (int i = 1; i <= d.Unx; i++) {
+          U2(i, j, k) = -((Ax * (U(i + 1, j, k) + U(i, j, k)) * (U(i + 1, j, k) + U(i, j, k))
+                           - Ax * (U(i, j, k) + U(i - 1, j, k)) * (U(i, j, k) + U(i - 1, j, k)))
+                          + (Ay * (U(i, j + 1, k) + U(i, j, k)) * (V(i + 1, j, k) + V(i, j, k))
+                             - Ay * (U(i, j, k) + U(i, j - 1, k)) * (V(i + 1, j - 1, k) + V(i, j - 1, k)))
+                          + ((U(i, j, k + 1) + U(i, j, k)) * (W(i + 1, j, k) + W(i, j, k))
+                             - (U(i, j, k) + U(i, j, k - 1)) * (W(i + 1, j, k - 1) + W(i, j, k - 1))) / d.dzPr(k) / 4);
+        }
+    Ax = 0.5 / d.dxmin; Ay = 0.125 / d.dymin;
+#pragma omp parallel for collapse(2)
+    for (int k = 1; k <= d.Unz; k++)
+      for (int j = 1; j <= d.Uny; j++)
+        for (int i = 1; i <= d.Unx; i++) {
+          double Vadv = (V(i, j, k) + V(i + 1, j, k) + V(i, j - 1, k) + V(i + 1, j - 1, k));
+          double Wadv = (W(i, j, k) + W(i + 1, j, k) + W(i, j, k - 1) + W(i + 1, j, k - 1)) / 4;
+          U2(i, j, k) = U2(i, j, k) - (Ax * (U(i + 1, j, k) - U(i - 1, j, k)) * U(i, j, k)
+                                       + Ay * (U(i, j + 1, k) - U(i, j - 1, k)) * Vadv
+                                       + (U(i, j, k + 1) - U(i, j, k - 1)) / (d.zPr(k + 1) - d.zPr(k - 1)) * Wadv);
+        }
+  }
+  for (auto &x : U2.v) x = x * 0.5;
+}
+
+static void CDV(Domain &d, A3 &V2) {
+  const A3 &U = d.U, &V = d.V, &W = d.W;
+  V2.fill(0);
+  if (d.gridtype == 0) {
+    double Ax = 0.25 / d.dxmin, Ay = 0.25 / d.dymin, Az = 0.25 / d.dzmin;
+#pragma omp parallel for collapse(2)
+    for (int k = 1; k <= d.Vnz; k++)
+      for (int j = 1; j <= d.Vny; j++)
+        for (int i = 1; i <= d.Vnx; i++) {
+          V2(i, j, k) = -((Ay * (V(i, j + 1, k) + V(i, j, k)) * (V(i, j + 1, k) + V(i, j, k))
+                           - Ay * (V(i, j, k) + V(i, j - 1, k)) * (V(i, j, k) + V(i, j - 1, k)))
+                          + (Ax * (V(i + 1, j, k) + V(i, j, k)) * (U(i, j + 1, k) + U(i, j, k))
+                             - Ax * (V(i, j, k) + V(i - 1, j, k)) * (U(i - 1, j + 1, k) + U(i - 1, j, k)))
+                          + (Az * (V(i, j, k + 1) + V(i, j, k)) * (W(i, j + 1, k) + W(i, j, k))
+                             - Az * (V(i, j, k) + V(i, j, k - 1)) * (W(i, j + 1, k - 1) + W(i, j, k - 1))));
+        }
+    Ax = 0.125 / d.dxmin; Ay = 0.5 / d.dymin; Az = 0.125 / d.dzmin;
+#pragma omp parallel for collapse(2)
+    for (int k = 1; k <= d.Vnz; k++)
+      for (int j = 1; j <= d.Vny; j++)
+        for (int i = 1; i <= d.Vnx; i++) {
+          double Uadv = (U(i, j, k) + U(i, j + 1, k) + U(i - 1, j, k) + U(i - 1, j + 1, k));
+          double Wadv = (W(i, j, k) + W(i, j + 1, k) + W(i, j, k - 1) + W(i, j + 1, k - 1));
+          V2(i, j, k) = V2(i, j, k) - (Ax * (V(i + 1, j, k) - V(i - 1, j, k)) * Uadv
+                                       + Ay * (V(i, j + 1, k) - V(i, j - 1, k)) * V(i, j, k)
+                                       + Az * (V(i, j, k + 1) - V(i, j, k - 1)) * Wadv);
+        }
+  } else {  // advection_variable_z.f90:54-84, :184-214
+    double Ax = 0.25 / d.dxmin, Ay = 0.25 / d.dymin;
+#pragma omp parallel for collapse(2)
+    for (int k = 1; k <= d.Vnz; k++)
+      for (int j = 1; j <= d.Vny; j++)
+        for (int i = 1; i <= d.Vnx; i++) {
+          V2(i, j, k) = -((Ay * (V(i, j + 1, k) + V(i, j, k)) * (V(i, j + 1, k) + V(i, j, k))
+                           - Ay * (V(i, j, k) + V(i, j - 1, k)) * (V(i, j, k) + V(i, j - 1, k)))
+                          + (Ax * (V(i + 1, j, k) + V(i, j, k)) * (U(i, j + 1, k) + U(i, j, k))
+                             - Ax * (V(i, j, k) + V(i - 1, j, k)) * (U(i - 1, j + 1, k) + U(i - 1, j, k)))
+                          + ((V(i, j, k + 1) + V(i, j, k)) * (W(i, j + 1, k) + W(i, j, k))
+                             - (V(i, j, k) + V(i, j, k - 1)) * (W(i, j + 1, k - 1) + W(i, j, k - 1))) / d.dzPr(k) / 4);
+        }
+    Ax = 0.125 / d.dxmin; Ay = 0.5 / d.dymin;
+#pragma omp parallel for collapse(2)
+    for (int k = 1; k <= d.Vnz; k++)
+      for (int j = 1; j <= d.Vny; j++)
+        for (int i = 1; i <= d.Vnx; i++) {
+          double Uadv = (U(i, j, k) + U(i, j + 1, k) + U(i - 1, j, k) + U(i - 1, j + 1, k));
+          double Wadv = (W(i, j, k) + W(i, j + 1, k) + W(i, j, k - 1) + W(i, j + 1, k - 1)) / 4;
+          V2(i, j, k) = V2(i, j, k) - (Ax * (V(i + 1, j, k) - V(i - 1, j, k)) * Uadv
+                                       + Ay * (V(i, j + 1, k) - V(i, j - 1, k)) * V(i, j, k)
+                                       + (V(i, j, k + 1) - V(i, j, k - 1)) / (d.zPr(k + 1) - d.zPr(k - 1)) * Wadv);
+        }
+  }
+  for (auto &x : V2.v) x = x * 0.5;
+}
+
+static void CDW(Domain &d, A3 &W2) {
+  const A3 &U = d.U, &V = d.V, &W = d.W;
+  W2.fill(0);
+  if (d.gridtype == 0) {
+    double Ax = 0.25 / d.dxmin, Ay = 0.25 / d.dymin, Az = 0.25 / d.dzmin;
+#pragma omp parallel for collapse(2)
+    for (int k = 1; k <= d.Wnz; k++)
+      for (int j = 1; j <= d.Wny; j++)
+        for (int i = 1; i <= d.Wnx; i++) {
+          W2(i, j, k) = -((Az * (W(i, j, k + 1) + W(i, j, k)) * (W(i, j, k + 1) + W(i, j, k))
+                           - Az * (W(i, j, k) + W(i, j, k - 1)) * (W(i, j, k) + W(i, j, k - 1)))
+                          + (Ay * (W(i, j + 1, k) + W(i, j, k)) * (V(i, j, k + 1) + V(i, j, k))
+                             - Ay * (W(i, j, k) + W(i, j - 1, k)) * (V(i, j - 1, k) + V(i, j - 1, k + 1)))
+                          + (Ax * (W(i + 1, j, k) + W(i, j, k)) * (U(i, j, k + 1) + U(i, j, k))
+                             - Ax * (W(i, j, k) + W(i - 1, j, k)) * (U(i - 1, j, k + 1) + U(i - 1, j, k))));
+        }
+    Ax = 0.125 / d.dxmin; Ay = 0.125 / d.dymin; Az = 0.5 / d.dzmin;
+#pragma omp parallel for collapse(2)
+    for (int k = 1; k <= d.Wnz; k++)
+      for (int j = 1; j <= d.Wny; j++)
+        for (int i = 1; i <= d.Wnx; i++) {
+          double Uadv = (U(i, j, k) + U(i, j, k + 1) + U(i - 1, j, k) + U(i - 1, j, k + 1));
+          double Vadv = (V(i, j, k) + V(i, j, k + 1) + V(i, j - 1, k) + V(i, j - 1, k + 1));
+          W2(i, j, k) = W2(i, j, k) - (Ax * (W(i + 1, j, k) - W(i - 1, j, k)) * Uadv
+                                       + Ay * (W(i, j + 1, k) - W(i, j - 1, k)) * Vadv
+                                       + Az * (W(i, j, k + 1) - W(i, j, k - 1)) * W(i, j, k));
+        }
+  } else {  // advection_variable_z.f90:92-122, :217-247
+    double Ax = 0.25 / d.dxmin, Ay = 0.25 / d.dymin;
+#pragma omp parallel for collapse(2)
+    for (int k = 1; k <= d.Wnz; k++)
+      for (int j = 1; j <= d.Wny; j++)
+        for (int i = 1; i <= d.Wnx; i++) {
+          W2(i, j, k) = -(((W(i, j, k + 1) + W(i, j, k)) * (W(i, j, k + 1) + W(i, j, k))
+                           - (W(i, j, k) + W(i, j, k - 1)) * (W(i, j, k) + W(i, j, k - 1))) / d.dzW(k) / 4
+                          + (Ay * (W(i, j + 1, k) + W(i, j, k)) * (V(i, j, k + 1) + V(i, j, k))
+                             - Ay * (W(i, j, k) + W(i, j - 1, k)) * (V(i, j - 1, k + 1) + V(i, j - 1, k)))
+                          + (Ax * (W(i + 1, j, k) + W(i, j, k)) * (U(i, j, k + 1) + U(i, j, k))
+                             - Ax * (W(i, j, k) + W(i - 1, j, k)) * (U(i - 1, j, k + 1) + U(i - 1, j, k))));
+        }
+    Ax = 0.125 / d.dxmin; Ay = 0.125 / d.dymin;
+#pragma omp parallel for collapse(2)
+    for (int k = 1; k <= d.Wnz; k++)
+      for (int j = 1; j <= d.Wny; j++)
+        for (int i = 1; i <= d.Wnx; i++) {
+          double Uadv = (U(i, j, k) + U(i, j, k + 1) + U(i - 1, j, k) + U(i - 1, j, k + 1));
+          double Vadv = (V(i, j, k) + V(i, j, k + 1) + V(i, j - 1, k) + V(i, j - 1, k + 1));
+          W2(i, j, k) = W2(i, j, k) - (Ax * (W(i + 1, j, k) - W(i - 1, j, k)) * Uadv
+                                       + Ay * (W(i, j + 1, k) - W(i, j - 1, k)) * Vadv
+                                       + (W(i, j, k + 1) - W(i, j, k - 1)) / (d.zW(k + 1) - d.zW(k - 1)) * W(i, j, k));
+        }
+  }
+  for (auto &x : W2.v) x = x * 0.5;
+}
+
+// ------------------------ MomentumDiffusion_nobranch_2ord, momentum_diffusion.f90:169-420
+// followed by the wall-flux includes wmfluxes-[variable_z-]nobranch-{U,V,W}-inc.f90.
+static void MomentumDiffusion(Domain &d, A3 &U2, A3 &V2, A3 &W2) {
+  const A3 &U = d.U, &V = d.V, &W = d.W, &nu = d.Viscosity;
+  const double rx = 1.0 / (d.dxmin * d.dxmin), ry = 1.0 / (d.dymin * d.dymin), rz = 1.0 / (d.dzmin * d.dzmin);
+  const bool vz = d.gridtype == 1;
+  const A1 &dzW = d.dzW, &dzPr = d.dzPr;
+  // U
+#pragma omp parallel for collapse(2)
+  for (int k = 1; k <= d.Unz; k++)
+    for (int j = 1; j <= d.Uny; j++)
+      for (int i = 1; i <= d.Unx; i++) {
+        double a = U2(i, j, k);
+        a = a + nu(i + 1, j, k) * (U(i + 1, j, k) - U(i, j, k)) * rx;
+        a = a - nu(i, j, k) * (U(i, j, k) - U(i - 1, j, k)) * rx;
+        a = a + 0.25 * (nu(i + 1, j + 1, k) + nu(i + 1, j, k) + nu(i, j + 1, k) + nu(i, j, k)) * (U(i, j + 1, k) - U(i, j, k)) * ry;
+        a = a - 0.25 * (nu(i + 1, j, k) + nu(i + 1, j - 1, k) + nu(i, j, k) + nu(i, j - 1, k)) * (U(i, j, k) - U(i, j - 1, k)) * ry;
+        if (!vz) {
+          a = a + 0.25 * (nu(i + 1, j, k + 1) + nu(i + 1, j, k) + nu(i, j, k + 1) + nu(i, j, k)) * (U(i, j, k + 1) - U(i, j, k)) * rz;
+          a = a - 0.25 * (nu(i + 1, j, k) + nu(i + 1, j, k - 1) + nu(i, j, k) + nu(i, j, k - 1)) * (U(i, j, k) - U(i, j, k - 1)) * rz;
+        } else {
+          double t = 0.25 * (nu(i + 1, j, k + 1) + nu(i + 1, j, k) + nu(i, j, k + 1) + nu(i, j, k)) * (U(i, j, k + 1) - U(i, j, k)) / dzW(k);
+          t = t - 0.25 * (nu(i + 1, j, k) + nu(i + 1, j, k - 1) + nu(i, j, k) + nu(i, j, k - 1)) * (U(i, j, k) - U(i, j, k - 1)) / dzW(k - 1);
+          t = t / dzPr(k);
+          a = a + t;
+        }
+        U2(i, j, k) = a;
+      }
+  // wmfluxes-nobranch-U-inc.f90 / wmfluxes-variable_z-nobranch-U-inc.f90
+  for (auto &p : d.wm[MINUSX][1]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = nu((x - 1) + 1, y, z) * (U((x - 1) + 1, y, z) - U(x - 1, y, z)) * rx;
+    U2(x, y, z) = U2(x, y, z) + f; U2(x, y, z) = U2(x, y, z) + p.fluxp;
+  }
+  for (auto &p : d.wm[MINUSX][1]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = nu((x - 1) + 1, y, z) * (U((x - 1) + 1, y, z) - U(x - 1, y, z)) * rx;
+    if (vz) f = f / dzPr(z - 1);
+    U2(x - 1, y, z) = U2(x - 1, y, z) - f; U2(x - 1, y, z) = U2(x - 1, y, z) - (vz ? p.fluxm : p.fluxp);
+  }
+  for (auto &p : d.wm[PLUSX][1]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = nu(x + 1, y, z) * (U(x + 1, y, z) - U(x, y, z)) * rx;
+    U2(x + 1, y, z) = U2(x + 1, y, z) + f; U2(x + 1, y, z) = U2(x + 1, y, z) + p.fluxp;
+  }
+  for (auto &p : d.wm[PLUSX][1]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = nu(x + 1, y, z) * (U(x + 1, y, z) - U(x, y, z)) * rx;
+    U2(x, y, z) = U2(x, y, z) - f; U2(x, y, z) = U2(x, y, z) - (vz ? p.fluxm : p.fluxp);
+  }
+  for (auto &p : d.wm[MINUSY][1]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = (nu(x + 1, y, z) + nu(x + 1, y - 1, z) + nu(x, y, z) + nu(x, y - 1, z)) * (U(x, y, z) - U(x, y - 1, z)) * ry / 4;
+    U2(x, y, z) = U2(x, y, z) + f; U2(x, y, z) = U2(x, y, z) + p.fluxp;
+  }
+  for (auto &p : d.wm[MINUSY][1]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = (nu(x + 1, y, z) + nu(x + 1, y - 1, z) + nu(x, y, z) + nu(x, y - 1, z)) * (U(x, y, z) - U(x, y - 1, z)) * ry / 4;
+    U2(x, y - 1, z) = U2(x, y - 1, z) - f; U2(x, y - 1, z) = U2(x, y - 1, z) - (vz ? p.fluxm : p.fluxp);
+  }
+  for (auto &p : d.wm[PLUSY][1]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = (nu(x + 1, y + 1, z) + nu(x + 1, y, z) + nu(x, y + 1, z) + nu(x, y, z)) * (U(x, y + 1, z) - U(x, y, z)) * ry / 4;
+    U2(x, y + 1, z) = U2(x, y + 1, z) + f; U2(x, y + 1, z) = U2(x, y + 1, z) + p.fluxp;
+  }
+  for (auto &p : d.wm[PLUSY][1]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = (nu(x + 1, y + 1, z) + nu(x + 1, y, z) + nu(x, y + 1, z) + nu(x, y, z)) * (U(x, y + 1, z) - U(x, y, z)) * ry / 4;
+    U2(x, y, z) = U2(x, y, z) - f; U2(x, y, z) = U2(x, y, z) - (vz ? p.fluxm : p.fluxp);
+  }
+  for (auto &p : d.wm[MINUSZ][1]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double s = nu(x + 1, y, z) + nu(x + 1, y, z - 1) + nu(x, y, z) + nu(x, y, z - 1);
+    double f = vz ? s * (U(x, y, z) - U(x, y, z - 1)) / dzW(z - 1) / 4 / dzPr(z) : s * (U(x, y, z) - U(x, y, z - 1)) * rz / 4;
+    U2(x, y, z) = U2(x, y, z) + f; U2(x, y, z) = U2(x, y, z) + p.fluxp;
+  }
+  for (auto &p : d.wm[MINUSZ][1]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double s = nu(x + 1, y, z) + nu(x + 1, y, z - 1) + nu(x, y, z) + nu(x, y, z - 1);
+    double f = vz ? s * (U(x, y, z) - U(x, y, z - 1)) / dzW(z - 1) / 4 / dzPr(z - 1) : s * (U(x, y, z) - U(x, y, z - 1)) * rz / 4;
+    U2(x, y, z - 1) = U2(x, y, z - 1) - f; U2(x, y, z - 1) = U2(x, y, z - 1) - (vz ? p.fluxm : p.fluxp);
+  }
+  for (auto &p : d.wm[PLUSZ][1]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double s = nu(x + 1, y, z + 1) + nu(x + 1, y, z) + nu(x, y, z + 1) + nu(x, y, z);
+    double f = vz ? s * (U(x, y, z + 1) - U(x, y, z)) / dzW(z) / 4 / dzPr(z + 1) : s * (U(x, y, z + 1) - U(x, y, z)) * rz / 4;
+    U2(x, y, z + 1) = U2(x, y, z + 1) + f; U2(x, y, z + 1) = U2(x, y, z + 1) + p.fluxp;
+  }
+  for (auto &p : d.wm[PLUSZ][1]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double s = nu(x + 1, y, z + 1) + nu(x + 1, y, z) + nu(x, y, z + 1) + nu(x, y, z);
+    double f = vz ? s * (U(x, y, z + 1) - U(x, y, z)) / dzW(z) / 4 / dzPr(z) : s * (U(x, y, z + 1) - U(x, y, z)) * rz / 4;
+    U2(x, y, z) = U2(x, y, z) - f; U2(x, y, z) = U2(x, y, z) - (vz ? p.fluxm : p.fluxp);
+  }
+
+  // V
+#pragma omp parallel for collapse(2)
+  for (int k = 1; k <= d.Vnz; k++)
+    for (int j = 1; j <= d.Vny; j++)
+      for (int i = 1; i <= d.Vnx; i++) {
+        double a = V2(i, j, k);
+        a = a + 0.25 * (nu(i + 1, j + 1, k) + nu(i + 1, j, k) + nu(i, j + 1, k) + nu(i, j, k)) * (V(i + 1, j, k) - V(i, j, k)) * rx;
+        a = a - 0.25 * (nu(i, j + 1, k) + nu(i, j, k) + nu(i - 1, j + 1, k) + nu(i - 1, j, k)) * (V(i, j, k) - V(i - 1, j, k)) * rx;
+        a = a + nu(i, j + 1, k) * (V(i, j + 1, k) - V(i, j, k)) * ry;
+        a = a - nu(i, j, k) * (V(i, j, k) - V(i, j - 1, k)) * ry;
+        if (!vz) {
+          a = a + 0.25 * (nu(i, j + 1, k + 1) + nu(i, j + 1, k) + nu(i, j, k + 1) + nu(i, j, k)) * (V(i, j, k + 1) - V(i, j, k)) * rz;
+          a = a - 0.25 * (nu(i, j + 1, k) + nu(i, j + 1, k - 1) + nu(i, j, k) + nu(i, j, k - 1)) * (V(i, j, k) - V(i, j, k - 1)) * rz;
+        } else {
+          double t = 0.25 * (nu(i, j + 1, k + 1) + nu(i, j + 1, k) + nu(i, j, k + 1) + nu(i, j, k)) * (V(i, j, k + 1) - V(i, j, k)) / dzW(k);
+          t = t - 0.25 * (nu(i, j + 1, k) + nu(i, j + 1, k - 1) + nu(i, j, k) + nu(i, j, k - 1)) * (V(i, j, k) - V(i, j, k - 1)) / dzW(k - 1);
+          t = t / dzPr(k);
+          a = a + t;
+        }
+        V2(i, j, k) = a;
+      }
+  for (auto &p : d.wm[MINUSX][2]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = (nu(x, y + 1, z) + nu(x, y, z) + nu(x - 1, y + 1, z) + nu(x - 1, y, z)) * (V(x, y, z) - V(x - 1, y, z)) * rx / 4;
+    V2(x, y, z) = V2(x, y, z) + f; V2(x, y, z) = V2(x, y, z) + p.fluxp;
+  }
+  for (auto &p : d.wm[MINUSX][2]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = (nu(x, y + 1, z) + nu(x, y, z) + nu(x - 1, y + 1, z) + nu(x - 1, y, z)) * (V(x, y, z) - V(x - 1, y, z)) * rx / 4;
+    if (vz) f = f / dzPr(z - 1);
+    V2(x - 1, y, z) = V2(x - 1, y, z) - f; V2(x - 1, y, z) = V2(x - 1, y, z) - (vz ? p.fluxm : p.fluxp);
+  }
+  for (auto &p : d.wm[PLUSX][2]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = (nu(x + 1, y + 1, z) + nu(x + 1, y, z) + nu(x, y + 1, z) + nu(x, y, z)) * (V(x + 1, y, z) - V(x, y, z)) * rx / 4;
+    V2(x + 1, y, z) = V2(x + 1, y, z) + f; V2(x + 1, y, z) = V2(x + 1, y, z) + p.fluxp;
+  }
+  for (auto &p : d.wm[PLUSX][2]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = (nu(x + 1, y + 1, z) + nu(x + 1, y, z) + nu(x, y + 1, z) + nu(x, y, z)) * (V(x + 1, y, z) - V(x, y, z)) * rx / 4;
+    V2(x, y, z) = V2(x, y, z) - f; V2(x, y, z) = V2(x, y, z) - (vz ? p.fluxm : p.fluxp);
+  }
+  for (auto &p : d.wm[MINUSY][2]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = nu(x, y, z) * (V(x, y, z) - V(x, y - 1, z)) * ry;
+    V2(x, y, z) = V2(x, y, z) + f; V2(x, y, z) = V2(x, y, z) + p.fluxp;
+  }
+  for (auto &p : d.wm[MINUSY][2]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = nu(x, y, z) * (V(x, y, z) - V(x, y - 1, z)) * ry;
+    V2(x, y - 1, z) = V2(x, y - 1, z) - f; V2(x, y - 1, z) = V2(x, y - 1, z) - (vz ? p.fluxm : p.fluxp);
+  }
+  for (auto &p : d.wm[PLUSY][2]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = nu(x, y + 1, z) * (V(x, y + 1, z) - V(x, y, z)) * ry;
+    V2(x, y + 1, z) = V2(x, y + 1, z) + f; V2(x, y + 1, z) = V2(x, y + 1, z) + p.fluxp;
+  }
+  for (auto &p : d.wm[PLUSY][2]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = nu(x, y + 1, z) * (V(x, y + 1, z) - V(x, y, z)) * ry;
+    V2(x, y, z) = V2(x, y, z) - f; V2(x, y, z) = V2(x, y, z) - (vz ? p.fluxm : p.fluxp);
+  }
+  for (auto &p : d.wm[MINUSZ][2]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double s = nu(x, y + 1, z) + nu(x, y + 1, z - 1) + nu(x, y, z) + nu(x, y, z - 1);
+    double f = vz ? s * (V(x, y, z) - V(x, y, z - 1)) / dzW(z - 1) / 4 / dzPr(z) : s * (V(x, y, z) - V(x, y, z - 1)) * rz / 4;
+    V2(x, y, z) = V2(x, y, z) + f; V2(x, y, z) = V2(x, y, z) + p.fluxp;
+  }
+  for (auto &p : d.wm[MINUSZ][2]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double s = nu(x, y + 1, z) + nu(x, y + 1, z - 1) + nu(x, y, z) + nu(x, y, z - 1);
+    double f = vz ? s * (V(x, y, z) - V(x, y, z - 1)) / dzW(z - 1) / 4 / dzPr(z - 1) : s * (V(x, y, z) - V(x, y, z - 1)) * rz / 4;
+    V2(x, y, z - 1) = V2(x, y, z - 1) - f; V2(x, y, z - 1) = V2(x, y, z - 1) - (vz ? p.fluxm : p.fluxp);
+  }
+  for (auto &p : d.wm[PLUSZ][2]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double s = nu(x, y + 1, z + 1) + nu(x, y + 1, z) + nu(x, y, z + 1) + nu(x, y, z);
+    double f = vz ? s * (V(x, y, z + 1) - V(x, y, z)) / dzW(z) / 4 / dzPr(z + 1) : s * (V(x, y, z + 1) - V(x, y, z)) * rz / 4;
+    V2(x, y, z + 1) = V2(x, y, z + 1) + f; V2(x, y, z + 1) = V2(x, y, z + 1) + p.fluxp;
+  }
+  for (auto &p : d.wm[PLUSZ][2]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double s = nu(x, y + 1, z + 1) + nu(x, y + 1, z) + nu(x, y, z + 1) + nu(x, y, z);
+    double f = vz ? s * (V(x, y, z + 1) - V(x, y, z)) / dzW(z) / 4 / dzPr(z) : s * (V(x, y, z + 1) - V(x, y, z)) * rz / 4;
+    V2(x, y, z) = V2(x, y, z) - f; V2(x, y, z) = V2(x, y, z) - (vz ? p.fluxm : p.fluxp);
+  }
+
+  // W
+#pragma omp parallel for collapse(2)
+  for (int k = 1; k <= d.Wnz; k++)
+    for (int j = 1; j <= d.Wny; j++)
+      for (int i = 1; i <= d.Wnx; i++) {
+        double a = W2(i, j, k);
+        a = a + 0.25 * (nu(i + 1, j, k + 1) + nu(i + 1, j, k) + nu(i, j, k + 1) + nu(i, j, k)) * (W(i + 1, j, k) - W(i, j, k)) * rx;
+        a = a - 0.25 * (nu(i, j, k + 1) + nu(i, j, k) + nu(i - 1, j, k + 1) + nu(i - 1, j, k)) * (W(i, j, k) - W(i - 1, j, k)) * rx;
+        a = a + 0.25 * (nu(i, j + 1, k + 1) + nu(i, j, k + 1) + nu(i, j + 1, k) + nu(i, j, k)) * (W(i, j + 1, k) - W(i, j, k)) * ry;
+        a = a - 0.25 * (nu(i, j, k + 1) + nu(i, j - 1, k + 1) + nu(i, j, k) + nu(i, j - 1, k)) * (W(i, j, k) - W(i, j - 1, k)) * ry;
+        if (!vz) {
+          a = a + nu(i, j, k + 1) * (W(i, j, k + 1) - W(i, j, k)) * rz;
+          a = a - nu(i, j, k) * (W(i, j, k) - W(i, j, k - 1)) * rz;
+        } else {
+          double t = nu(i, j, k + 1) * (W(i, j, k + 1) - W(i, j, k)) / dzPr(k + 1);
+          t = t - nu(i, j, k) * (W(i, j, k) - W(i, j, k - 1)) / dzPr(k);
+          t = t / dzW(k);
+          a = a + t;
+        }
+        W2(i, j, k) = a;
+      }
+  for (auto &p : d.wm[MINUSX][3]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = (nu(x, y, z + 1) + nu(x, y, z) + nu(x - 1, y, z + 1) + nu(x - 1, y, z)) * (W(x, y, z) - W(x - 1, y, z)) * rx / 4;
+    W2(x, y, z) = W2(x, y, z) + f; W2(x, y, z) = W2(x, y, z) + p.fluxp;
+  }
+  for (auto &p : d.wm[MINUSX][3]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = (nu(x, y, z + 1) + nu(x, y, z) + nu(x - 1, y, z + 1) + nu(x - 1, y, z)) * (W(x, y, z) - W(x - 1, y, z)) * rx / 4;
+    if (vz) f = f / dzW(z - 1);
+    W2(x - 1, y, z) = W2(x - 1, y, z) - f; W2(x - 1, y, z) = W2(x - 1, y, z) - (vz ? p.fluxm : p.fluxp);
+  }
+  for (auto &p : d.wm[PLUSX][3]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = (nu(x + 1, y, z + 1) + nu(x + 1, y, z) + nu(x, y, z + 1) + nu(x, y, z)) * (W(x + 1, y, z) - W(x, y, z)) * rx / 4;
+    W2(x + 1, y, z) = W2(x + 1, y, z) + f; W2(x + 1, y, z) = W2(x + 1, y, z) + p.fluxp;
+  }
+  for (auto &p : d.wm[PLUSX][3]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = (nu(x + 1, y, z + 1) + nu(x + 1, y, z) + nu(x, y, z + 1) + nu(x, y, z)) * (W(x + 1, y, z) - W(x, y, z)) * rx / 4;
+    W2(x, y, z) = W2(x, y, z) - f; W2(x, y, z) = W2(x, y, z) - (vz ? p.fluxm : p.fluxp);
+  }
+  for (auto &p : d.wm[MINUSY][3]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = (nu(x, y, z + 1) + nu(x, y - 1, z + 1) + nu(x, y, z) + nu(x, y - 1, z)) * (W(x, y, z) - W(x, y - 1, z)) * ry / 4;
+    W2(x, y, z) = W2(x, y, z) + f; W2(x, y, z) = W2(x, y, z) + p.fluxp;
+  }
+  for (auto &p : d.wm[MINUSY][3]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = (nu(x, y, z + 1) + nu(x, y - 1, z + 1) + nu(x, y, z) + nu(x, y - 1, z)) * (W(x, y, z) - W(x, y - 1, z)) * ry / 4;
+    W2(x, y - 1, z) = W2(x, y - 1, z) - f; W2(x, y - 1, z) = W2(x, y - 1, z) - (vz ? p.fluxm : p.fluxp);
+  }
+  for (auto &p : d.wm[PLUSY][3]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = (nu(x, y + 1, z + 1) + nu(x, y, z + 1) + nu(x, y + 1, z) + nu(x, y, z)) * (W(x, y + 1, z) - W(x, y, z)) * ry / 4;
+    W2(x, y + 1, z) = W2(x, y + 1, z) + f; W2(x, y + 1, z) = W2(x, y + 1, z) + p.fluxp;
+  }
+  for (auto &p : d.wm[PLUSY][3]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = (nu(x, y + 1, z + 1) + nu(x, y, z + 1) + nu(x, y + 1, z) + nu(x, y, z)) * (W(x, y + 1, z) - W(x, y, z)) * ry / 4;
+    W2(x, y, z) = W2(x, y, z) - f; W2(x, y, z) = W2(x, y, z) - (vz ? p.fluxm : p.fluxp);
+  }
+  for (auto &p : d.wm[MINUSZ][3]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = vz ? nu(x, y, z) * (W(x, y, z) - W(x, y, z - 1)) / dzPr(z) / dzW(z) : nu(x, y, z) * (W(x, y, z) - W(x, y, z - 1)) * rz;
+    W2(x, y, z) = W2(x, y, z) + f; W2(x, y, z) = W2(x, y, z) + p.fluxp;
+  }
+  for (auto &p : d.wm[MINUSZ][3]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = vz ? nu(x, y, z) * (W(x, y, z) - W(x, y, z - 1)) / dzPr(z) / dzW(z - 1) : nu(x, y, z) * (W(x, y, z) - W(x, y, z - 1)) * rz;
+    W2(x, y, z - 1) = W2(x, y, z - 1) - f; W2(x, y, z - 1) = W2(x, y, z - 1) - (vz ? p.fluxm : p.fluxp);
+  }
+  for (auto &p : d.wm[PLUSZ][3]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = vz ? nu(x, y, z + 1) * (W(x, y, z + 1) - W(x, y, z)) / dzPr(z + 1) / dzW(z + 1) : nu(x, y, z + 1) * (W(x, y, z + 1) - W(x, y, z)) * rz;
+    W2(x, y, z + 1) = W2(x, y, z + 1) + f; W2(x, y, z + 1) = W2(x, y, z + 1) + p.fluxp;
+  }
+  for (auto &p : d.wm[PLUSZ][3]) {
+    int x = p.xi, y = p.yj, z = p.zk;
+    double f = vz ? nu(x, y, z + 1) * (W(x, y, z + 1) - W(x, y, z)) / dzPr(z + 1) / dzW(z) : nu(x, y, z + 1) * (W(x, y, z + 1) - W(x, y, z)) * rz;
+    W2(x, y, z) = W2(x, y, z) - f; W2(x, y, z) = W2(x, y, z) - (vz ? p.fluxm : p.fluxp);
+  }
+}
+
+// ------------------------------------------------- Convection, dynamics.f90:230-499
+static void Convection(Domain &d, int stage, double dt) {
+  const double rho = RK_rho[stage - 1], beta = RK_beta[stage - 1];
+  if (stage > 1) {
+    for (int k = 1; k <= d.Unz; k++) for (int j = 1; j <= d.Uny; j++) for (int i = 1; i <= d.Unx; i++) d.U2(i, j, k) = d.Ustar(i, j, k) * rho * dt;
+    for (int k = 1; k <= d.Vnz; k++) for (int j = 1; j <= d.Vny; j++) for (int i = 1; i <= d.Vnx; i++) d.V2(i, j, k) = d.Vstar(i, j, k) * rho * dt;
+    for (int k = 1; k <= d.Wnz; k++) for (int j = 1; j <= d.Wny; j++) for (int i = 1; i <= d.Wnx; i++) d.W2(i, j, k) = d.Wstar(i, j, k) * rho * dt;
+  } else {
+    for (int k = 1; k <= d.Unz; k++) for (int j = 1; j <= d.Uny; j++) for (int i = 1; i <= d.Unx; i++) { d.Ustar(i, j, k) = 0; d.U2(i, j, k) = 0; }
+    for (int k = 1; k <= d.Vnz; k++) for (int j = 1; j <= d.Vny; j++) for (int i = 1; i <= d.Vnx; i++) { d.Vstar(i, j, k) = 0; d.V2(i, j, k) = 0; }
+    for (int k = 1; k <= d.Wnz; k++) for (int j = 1; j <= d.Wny; j++) for (int i = 1; i <= d.Wnx; i++) { d.Wstar(i, j, k) = 0; d.W2(i, j, k) = 0; }
+  }
+  // advection_method == 2: CDU/CDV/CDW (dynamics.f90:359-368)
+  CDU(d, d.Ustar);
+  CDV(d, d.Vstar);
+  CDW(d, d.Wstar);
+  MomentumDiffusion(d, d.Ustar, d.Vstar, d.Wstar);
+  for (int k = 1; k <= d.Unz; k++) for (int j = 1; j <= d.Uny; j++) for (int i = 1; i <= d.Unx; i++) d.U2(i, j, k) = d.U2(i, j, k) + d.Ustar(i, j, k) * beta * dt;
+  for (int k = 1; k <= d.Vnz; k++) for (int j = 1; j <= d.Vny; j++) for (int i = 1; i <= d.Vnx; i++) d.V2(i, j, k) = d.V2(i, j, k) + d.Vstar(i, j, k) * beta * dt;
+  for (int k = 1; k <= d.Wnz; k++) for (int j = 1; j <= d.Wny; j++) for (int i = 1; i <= d.Wnx; i++) d.W2(i, j, k) = d.W2(i, j, k) + d.Wstar(i, j, k) * beta * dt;
+}
+
+// ------------------------ OtherTerms, tsteps.f90:263-358; PressureGrad, dynamics.f90:58-199
+static void OtherTerms(Domain &d, double coef) {
+  const double A = -coef, Ax = -coef / d.dxmin, Ay = -coef / d.dymin, Az = -coef / d.dzmin;
+  A3 &Pr = d.Pr;
+  if (d.en_prgx)
+    for (int k = 1; k <= d.Unz; k++) for (int j = 1; j <= d.Uny; j++) for (int i = 1; i <= d.Unx; i++) d.U2(i, j, k) = d.U2(i, j, k) + A * d.prgx;
+  if (d.en_prgy)
+    for (int k = 1; k <= d.Vnz; k++) for (int j = 1; j <= d.Vny; j++) for (int i = 1; i <= d.Vnx; i++) d.V2(i, j, k) = d.V2(i, j, k) + A * d.prgy;
+  for (int k = 1; k <= d.Unz; k++) for (int j = 1; j <= d.Uny; j++) for (int i = 1; i <= d.Unx; i++) d.U2(i, j, k) = d.U2(i, j, k) + Ax * (Pr(i + 1, j, k) - Pr(i, j, k));
+  for (int k = 1; k <= d.Vnz; k++) for (int j = 1; j <= d.Vny; j++) for (int i = 1; i <= d.Vnx; i++) d.V2(i, j, k) = d.V2(i, j, k) + Ay * (Pr(i, j + 1, k) - Pr(i, j, k));
+  if (d.gridtype == 1) {
+    for (int k = 1; k <= d.Wnz; k++) for (int j = 1; j <= d.Wny; j++) for (int i = 1; i <= d.Wnx; i++) d.W2(i, j, k) = d.W2(i, j, k) - coef * (Pr(i, j, k + 1) - Pr(i, j, k)) / d.dzW(k);
+  } else {
+    for (int k = 1; k <= d.Wnz; k++) for (int j = 1; j <= d.Wny; j++) for (int i = 1; i <= d.Wnx; i++) d.W2(i, j, k) = d.W2(i, j, k) + Az * (Pr(i, j, k + 1) - Pr(i, j, k));
+  }
+  // explicit_diffusion: add(U2, U) over the whole arrays (tsteps.f90:352-354)
+  for (size_t n = 0; n < d.U2.v.size(); n++) d.U2.v[n] = d.U2.v[n] + d.U.v[n];
+  for (size_t n = 0; n < d.V2.v.size(); n++) d.V2.v[n] = d.V2.v[n] + d.V.v[n];
+  for (size_t n = 0; n < d.W2.v.size(); n++) d.W2.v[n] = d.W2.v[n] + d.W.v[n];
+}
+
+// ---------------------------------------------------------------- Poisson
+// Exact FP64 solve of the operator of Residue_variable_z (poisson.f90:23-60):
+// FFT in x and y, then for each (kx,ky) a tridiagonal system in z.
+static bool init_poisson(Domain &d) {
+  int nx = d.Prnx, ny = d.Prny, nz = d.Prnz;
+  if (d.PrBtype[We] != BC_PERIODIC || d.PrBtype[So] != BC_PERIODIC) return false;
+  if (!d.px.init(nx) || !d.py.init(ny)) return false;
+  d.nxh = nx / 2 + 1;
+  double rx = 1 / (d.dxmin * d.dxmin), ry = 1 / (d.dymin * d.dymin);
+  d.lamx.resize(nx); d.lamy.resize(ny);
+  for (int m = 0; m < nx; m++) { double s = std::sin(M_PI * m / nx); d.lamx[m] = -4.0 * s * s * rx; }
+  for (int m = 0; m < ny; m++) { double s = std::sin(M_PI * m / ny); d.lamy[m] = -4.0 * s * s * ry; }
+  d.zper = d.PrBtype[Bo] == BC_PERIODIC;
+  d.Ab.assign(nz + 2, 0.0); d.At.assign(nz + 2, 0.0); d.dzc.assign(nz + 2, 0.0); d.dzf.assign(nz + 2, 0.0);
+  for (int k = 1; k <= nz; k++) {
+    d.Ab[k] = 1 / ((d.zPr(k) - d.zPr(k - 1)) * (d.zW(k) - d.zW(k - 1)));
+    d.At[k] = 1 / ((d.zPr(k + 1) - d.zPr(k)) * (d.zW(k) - d.zW(k - 1)));
+    d.dzc[k] = d.zW(k) - d.zW(k - 1);      // cell height
+    d.dzf[k] = d.zPr(k + 1) - d.zPr(k);    // distance of centres k, k+1
+  }
+  if (!d.zper) { d.Ab[1] = 0; d.At[nz] = 0; }
+  return true;
+}
+
+// Solves (Lz + lam) x = r for one column; lam == 0 with Neumann z is the
+// singular mode, solved by two prefix sums and pinned to zero mean.
+static void tridiag(const Domain &d, double lam, bool zero_mode, const cd *r, cd *x, std::vector<cd> &cp_) {
+  int nz = d.Prnz;
+  const std::vector<double> &Ab = d.Ab, &At = d.At;
+  if (zero_mode && !d.zper) {
+    cd F = 0;
+    x[0] = 0;
+    for (int k = 1; k <= nz - 1; k++) {
+      F = F + r[k - 1] * d.dzc[k];
+      x[k] = x[k - 1] + F * d.dzf[k];
+    }
+    cd s = 0;
+    for (int k = 0; k < nz; k++) s += x[k];
+    s = s / (double)nz;
+    for (int k = 0; k < nz; k++) x[k] -= s;
+    return;
+  }
+  if (zero_mode && d.zper) {
+    // periodic singular mode: fluxes F(k) = F(0) + sum dzc r, with F(0) chosen
+    // so that sum_k dzf(k) F(k) = 0 (periodicity of x).
+    std::vector<cd> F(nz + 1);
+    F[0] = 0;
+    for (int k = 1; k <= nz; k++) F[k] = F[k - 1] + r[k - 1] * d.dzc[k];
+    cd sw = 0; double sd = 0;
+    for (int k = 1; k <= nz; k++) { sw += F[k] * d.dzf[k]; sd += d.dzf[k]; }
+    cd F0 = -sw / sd;
+    x[0] = 0;
+    for (int k = 1; k <= nz - 1; k++) x[k] = x[k - 1] + (F[k] + F0) * d.dzf[k];
+    cd s = 0;
+    for (int k = 0; k < nz; k++) s += x[k];
+    s = s / (double)nz;
+    for (int k = 0; k < nz; k++) x[k] -= s;
+    return;
+  }
+  std::vector<double> cp(nz);
+  if (!d.zper) {
+    // Thomas algorithm, rows k=1..nz: Ab(k) x(k-1) + (-(Ab+At)+lam) x(k) + At(k) x(k+1)
+    double b = -(Ab[1] + At[1]) + lam;
+    cp[0] = At[1] / b;
+    x[0] = r[0] / b;
+    for (int k = 2; k <= nz; k++) {
+      double den = (-(Ab[k] + At[k]) + lam) - Ab[k] * cp[k - 2];
+      cp[k - 1] = At[k] / den;
+      x[k - 1] = (r[k - 1] - Ab[k] * x[k - 2]) / den;
+    }
+    for (int k = nz - 1; k >= 1; k--) x[k - 1] = x[k - 1] - cp[k - 1] * x[k];
+  } else {
+    // cyclic system by Sherman-Morrison
+    std::vector<double> a(nz), b(nz), c(nz);
+    for (int k = 1; k <= nz; k++) { a[k - 1] = Ab[k]; c[k - 1] = At[k]; b[k - 1] = -(Ab[k] + At[k]) + lam; }
+    double alpha = c[nz - 1], beta = a[0];
+    double gamma = -b[0];
+    std::vector<double> bb(b);
+    bb[0] = b[0] - gamma;
+    bb[nz - 1] = b[nz - 1] - alpha * beta / gamma;
+    std::vector<cd> y(nz);
+    std::vector<double> u(nz, 0.0), z(nz);
+    u[0] = gamma; u[nz - 1] = alpha;
+    // solve bb-system for r -> y and for u -> z
+    std::vector<double> c2(nz);
+    double den = bb[0];
+    c2[0] = c[0] / den; y[0] = r[0] / den; z[0] = u[0] / den;
+    for (int k = 1; k < nz; k++) {
+      den = bb[k] - a[k] * c2[k - 1];
+      c2[k] = c[k] / den;
+      y[k] = (r[k] - a[k] * y[k - 1]) / den;
+      z[k] = (u[k] - a[k] * z[k - 1]) / den;
+    }
+    for (int k = nz - 2; k >= 0; k--) { y[k] = y[k] - c2[k] * y[k + 1]; z[k] = z[k] - c2[k] * z[k + 1]; }
+    cd fac = (y[0] + beta * y[nz - 1] / gamma) / (1.0 + z[0] + beta * z[nz - 1] / gamma);
+    for (int k = 0; k < nz; k++) x[k] = y[k] - fac * z[k];
+  }
+  (void)cp_;
+}
+
+static void poisson_solve(Domain &d) {
+  int nx = d.Prnx, ny = d.Prny, nz = d.Prnz, nxh = d.nxh;
+  // S[k][ky][kx]
+  std::vector<cd> S((size_t)nz * ny * nxh);
+  const double norm = 1.0 / ((double)nx * ny);
+#pragma omp parallel
+  {
+    std::vector<cd> a(nx), b(nx), t(std::max(nx, std::max(ny, nz))), c(ny), e(ny), rz(nz), xz(nz);
+    std::vector<cd> cp;
+#pragma omp for collapse(2)
+    for (int k = 1; k <= nz; k++)
+      for (int j = 1; j <= ny; j++) {
+        for (int i = 1; i <= nx; i++) a[i - 1] = d.RHS(i, j, k);
+        d.px.forward(a.data(), b.data());
+        for (int m = 0; m < nxh; m++) S[((size_t)(k - 1) * ny + (j - 1)) * nxh + m] = b[m];
+      }
+#pragma omp for collapse(2)
+    for (int k = 0; k < nz; k++)
+      for (int m = 0; m < nxh; m++) {
+        for (int j = 0; j < ny; j++) c[j] = S[((size_t)k * ny + j) * nxh + m];
+        d.py.forward(c.data(), e.data());
+        for (int j = 0; j < ny; j++) S[((size_t)k * ny + j) * nxh + m] = e[j];
+      }
+#pragma omp for collapse(2)
+    for (int j = 0; j < ny; j++)
+      for (int m = 0; m < nxh; m++) {
+        for (int k = 0; k < nz; k++) rz[k] = S[((size_t)k * ny + j) * nxh + m] * norm;
+        double lam = d.lamx[m] + d.lamy[j];
+        tridiag(d, lam, m == 0 && j == 0, rz.data(), xz.data(), cp);
+        for (int k = 0; k < nz; k++) S[((size_t)k * ny + j) * nxh + m] = xz[k];
+      }
+#pragma omp for collapse(2)
+    for (int k = 0; k < nz; k++)
+      for (int m = 0; m < nxh; m++) {
+        for (int j = 0; j < ny; j++) c[j] = S[((size_t)k * ny + j) * nxh + m];
+        d.py.inverse(c.data(), e.data(), t);
+        for (int j = 0; j < ny; j++) S[((size_t)k * ny + j) * nxh + m] = e[j];
+      }
+#pragma omp for collapse(2)
+    for (int k = 1; k <= nz; k++)
+      for (int j = 1; j <= ny; j++) {
+        const cd *row = &S[((size_t)(k - 1) * ny + (j - 1)) * nxh];
+        for (int m = 0; m < nxh; m++) a[m] = row[m];
+        for (int m = nxh; m < nx; m++) a[m] = std::conj(row[nx - m]);
+        d.px.inverse(a.data(), b.data(), t);
+        for (int i = 1; i <= nx; i++) d.Phi(i, j, k) = b[i - 1].real();
+      }
+  }
+}
+
+// ------------------------------------------ PressureCorrection, pressure.f90:169-266
+static void PressureCorrection(Domain &d, double coef, bool check_div) {
+  A3 &U = d.U2, &V = d.V2, &W = d.W2;
+  const double dt2 = coef;
+  // PrePoisson (pressure.f90:272-723): ghosts, then RHS = (div U - Q) / dt2 with Q = 0
+  BoundUVW(d, U, V, W);
+  const double dt2_rec = 1.0 / dt2;
+#pragma omp parallel for collapse(2)
+  for (int k = 1; k <= d.Prnz; k++)
+    for (int j = 1; j <= d.Prny; j++)
+      for (int i = 1; i <= d.Prnx; i++) {
+        double r;
+        if (d.gridtype == 1)
+          r = (U(i, j, k) - U(i - 1, j, k)) / d.dxmin + (V(i, j, k) - V(i, j - 1, k)) / d.dymin + (W(i, j, k) - W(i, j, k - 1)) / d.dzPr(k) - 0.0;
+        else
+          r = (U(i, j, k) - U(i - 1, j, k)) / d.dxmin + (V(i, j, k) - V(i, j - 1, k)) / d.dymin + (W(i, j, k) - W(i, j, k - 1)) / d.dzmin - 0.0;
+        d.RHS(i, j, k) = r * dt2_rec;
+      }
+  poisson_solve(d);
+  Bound_Phi(d, d.Phi);
+  // PostPoisson (pressure.f90:728-991)
+  const double Au = dt2 / d.dxmin, Av = dt2 / d.dymin, Aw = dt2 / d.dzmin;
+  A3 &Phi = d.Phi;
+  for (int k = 1; k <= d.Unz; k++) for (int j = 1; j <= d.Uny; j++) for (int i = 1; i <= d.Unx; i++) U(i, j, k) = U(i, j, k) - Au * (Phi(i + 1, j, k) - Phi(i, j, k));
+  for (int k = 1; k <= d.Vnz; k++) for (int j = 1; j <= d.Vny; j++) for (int i = 1; i <= d.Vnx; i++) V(i, j, k) = V(i, j, k) - Av * (Phi(i, j + 1, k) - Phi(i, j, k));
+  if (d.gridtype == 1) {
+    for (int k = 1; k <= d.Wnz; k++) for (int j = 1; j <= d.Wny; j++) for (int i = 1; i <= d.Wnx; i++) W(i, j, k) = W(i, j, k) - dt2 * (Phi(i, j, k + 1) - Phi(i, j, k)) / d.dzW(k);
+  } else {
+    for (int k = 1; k <= d.Wnz; k++) for (int j = 1; j <= d.Wny; j++) for (int i = 1; i <= d.Wnx; i++) W(i, j, k) = W(i, j, k) - Aw * (Phi(i, j, k + 1) - Phi(i, j, k));
+  }
+  A3 &Pr = d.Pr;
+  for (int k = 1; k <= d.Prnz; k++) for (int j = 1; j <= d.Prny; j++) for (int i = 1; i <= d.Prnx; i++) Pr(i, j, k) = Pr(i, j, k) + Phi(i, j, k);
+  // FixPressureToReference, PRESSURE_REFERENCE_BOUNDARY at To (pressure.f90:1160-1220)
+  double Phi_ref = 0;
+  for (int j = 1; j <= d.Prny; j++) for (int i = 1; i <= d.Prnx; i++) Phi_ref = Phi_ref + Pr(i, j, d.Prnz);
+  Phi_ref = Phi_ref / (d.Prnx * d.Prny);
+  if (Phi_ref != 0)
+    for (int k = 1; k <= d.Prnz; k++) for (int j = 1; j <= d.Prny; j++) for (int i = 1; i <= d.Prnx; i++) Pr(i, j, k) = Pr(i, j, k) - Phi_ref;
+  Bound_Pr(d, Pr);
+  if (check_div) {  // pressure.f90:884-989, after BoundUVW
+    BoundUVW(d, U, V, W);
+    double S = 0;
+    for (int k = 1; k <= d.Prnz; k++)
+      for (int j = 1; j <= d.Prny; j++)
+        for (int i = 1; i <= d.Prnx; i++) {
+          double dzk = d.gridtype == 1 ? d.dzPr(k) : d.dzmin;
+          double p = (U(i, j, k) - U(i - 1, j, k)) / d.dxmin + (V(i, j, k) - V(i, j - 1, k)) / d.dymin + (W(i, j, k) - W(i, j, k - 1)) / dzk - 0.0;
+          S = std::max(S, std::fabs(p));
+        }
+    d.max_div = S;
+  }
+}
+
+// ---------------------------------------------- TimeStepLength, dynamics.f90:511-600
+static void TimeStepLength(Domain &d) {
+  if (!d.enable_CFL_check) { d.CFL = 0; return; }
+  double U_dx_max = 0;
+  for (int k = 1; k <= d.Prnz; k++)
+    for (int j = 1; j <= d.Prny; j++)
+      for (int i = 1; i <= d.Prnx; i++) {
+        double dx = d.gridtype == 1 ? d.dxPr(i) : d.dxmin;
+        double dy = d.gridtype == 1 ? d.dyPr(j) : d.dymin;
+        double dz = d.gridtype == 1 ? d.dzPr(k) : d.dzmin;
+        double p = std::max(std::fabs(d.U(i, j, k)), std::fabs(d.U(i - 1, j, k))) / dx;
+        p = p + std::max(std::fabs(d.V(i, j, k)), std::fabs(d.V(i, j - 1, k))) / dy;
+        p = p + std::max(std::fabs(d.W(i, j, k)), std::fabs(d.W(i, j, k - 1))) / dz;
+        U_dx_max = std::max(U_dx_max, p);
+      }
+  d.CFL = U_dx_max * d.dt;
+}
+
+// one RK3 stage of TMarchRK3 (tsteps.f90:111-241) up to a stop point
+static void run_stage(Domain &d, int stage, int stop) {
+  const double dt = d.dt;
+  SubgridStresses(d);
+  if (stop == 1) return;
+  Convection(d, stage, dt);
+  OtherTerms(d, 2 * RK_alpha[stage - 1] * dt);
+  BoundUVW(d, d.U2, d.V2, d.W2);
+  if (stop == 2) return;
+  PressureCorrection(d, 2 * RK_alpha[stage - 1] * dt, true);
+  std::swap(d.U.v, d.U2.v);
+  std::swap(d.V.v, d.V2.v);
+  std::swap(d.W.v, d.W2.v);
+  BoundUVW(d, d.U, d.V, d.W);
+}
+
+static void TMarchRK3(Domain &d) {
+  BoundUVW(d, d.U, d.V, d.W);
+  TimeStepLength(d);
+  for (int s = 1; s <= 3; s++) run_stage(d, s, 3);
+  d.time += d.dt;
+}
+
+}  // namespace orc
+
+// ================================================================ C API
+using namespace orc;
+
+extern "C" {
+
+struct orc_domain;
+
+static int sides_ok(const int *b) {
+  for (int s = 0; s < 6; s++)
+    if (b[s] != BC_NOSLIP && b[s] != BC_FREESLIP && b[s] != BC_PERIODIC && b[s] != BC_NEUMANN) return 0;
+  for (int a = 0; a < 3; a++)
+    if ((b[2 * a] == BC_PERIODIC) != (b[2 * a + 1] == BC_PERIODIC)) return 0;
+  return 1;
+}
+
+void *orc_create(const elmm_config *c) {
+  if (!c || c->Prnx < 4 || c->Prny < 4 || c->Prnz < 4 || !sides_ok(c->Btype)) return nullptr;
+  Domain *d = new Domain();
+  d->Prnx = c->Prnx; d->Prny = c->Prny; d->Prnz = c->Prnz;
+  for (int s = 0; s < 6; s++) d->Btype[s + 1] = c->Btype[s];
+  // PrBtype from Btype, initial.f90:817-826
+  for (int s = 1; s <= 6; s++) d->PrBtype[s] = d->Btype[s] == BC_PERIODIC ? BC_PERIODIC : BC_NEUMANN;
+  d->Unx = d->Btype[Ea] == BC_PERIODIC ? d->Prnx : d->Prnx - 1; d->Uny = d->Prny; d->Unz = d->Prnz;
+  d->Vnx = d->Prnx; d->Vny = d->Btype[No] == BC_PERIODIC ? d->Prny : d->Prny - 1; d->Vnz = d->Prnz;
+  d->Wnx = d->Prnx; d->Wny = d->Prny; d->Wnz = d->Btype[To] == BC_PERIODIC ? d->Prnz : d->Prnz - 1;
+  d->gridtype = c->zW ? 1 : 0;
+  d->dxmin = c->dxmin; d->dymin = c->dymin; d->dzmin = c->dzmin;
+  d->molecular_viscosity = c->molecular_viscosity;
+  d->C_Smagorinsky = c->C_Smagorinsky;
+  d->filter_ratio = c->filter_ratio;
+  d->sgstype = c->sgstype;
+  d->wallmodeltype = c->wallmodeltype;
+  for (int s = 0; s < 6; s++) d->z0s[s + 1] = c->z0[s];
+  d->en_prgx = c->enable_pr_gradient_x_uniform; d->en_prgy = c->enable_pr_gradient_y_uniform;
+  d->prgx = c->pr_gradient_x; d->prgy = c->pr_gradient_y;
+  d->dt = c->dt; d->time = 0;
+  d->enable_CFL_check = c->enable_CFL_check; d->CFL = 0; d->max_div = 0;
+  init_grid(*d, *c);
+  int nx = d->Prnx, ny = d->Prny, nz = d->Prnz;
+  for (A3 *a : {&d->U, &d->U2, &d->Ustar}) a->init(-2, d->Unx + 3, -2, d->Uny + 3, -2, d->Unz + 3);
+  for (A3 *a : {&d->V, &d->V2, &d->Vstar}) a->init(-2, d->Vnx + 3, -2, d->Vny + 3, -2, d->Vnz + 3);
+  for (A3 *a : {&d->W, &d->W2, &d->Wstar}) a->init(-2, d->Wnx + 3, -2, d->Wny + 3, -2, d->Wnz + 3);
+  for (A3 *a : {&d->Pr, &d->Viscosity, &d->Phi}) a->init(-1, nx + 2, -1, ny + 2, -1, nz + 2);
+  d->RHS.init(0, nx + 1, 0, ny + 1, 0, nz + 1);
+  d->Viscosity.fill(d->molecular_viscosity);
+  if (d->wallmodeltype > 0) add_wm_points(*d);
+  if (!init_poisson(*d)) { delete d; return nullptr; }
+  return d;
+}
+
+void orc_destroy(void *h) { delete (Domain *)h; }
+
+int orc_sizes(void *h, int32_t *out12) {
+  Domain *d = (Domain *)h;
+  int v[12] = {d->Prnx, d->Prny, d->Prnz, d->Unx, d->Uny, d->Unz, d->Vnx, d->Vny, d->Vnz, d->Wnx, d->Wny, d->Wnz};
+  for (int i = 0; i < 12; i++) out12[i] = v[i];
+  return 0;
+}
+
+static A3 *field_of(Domain *d, int f) {
+  switch (f) {
+    case ELMM_FIELD_U: return &d->U;
+    case ELMM_FIELD_V: return &d->V;
+    case ELMM_FIELD_W: return &d->W;
+    case ELMM_FIELD_PR: return &d->Pr;
+    case ELMM_FIELD_VISCOSITY: return &d->Viscosity;
+    case ELMM_FIELD_U2: return &d->U2;
+    case ELMM_FIELD_V2: return &d->V2;
+    case ELMM_FIELD_W2: return &d->W2;
+    case ELMM_FIELD_USTAR: return &d->Ustar;
+    case ELMM_FIELD_VSTAR: return &d->Vstar;
+    case ELMM_FIELD_WSTAR: return &d->Wstar;
+    case ELMM_FIELD_PHI: return &d->Phi;
+  }
+  return nullptr;
+}
+
+int orc_set_field(void *h, int f, const double *src) {
+  A3 *a = field_of((Domain *)h, f);
+  if (!a) return ELMM_ERR_INVALID_ARG;
+  std::memcpy(a->v.data(), src, a->v.size() * sizeof(double));
+  return 0;
+}
+
+int orc_get_field(void *h, int f, double *dst) {
+  A3 *a = field_of((Domain *)h, f);
+  if (!a) return ELMM_ERR_INVALID_ARG;
+  std::memcpy(dst, a->v.data(), a->v.size() * sizeof(double));
+  return 0;
+}
+
+int orc_project(void *h, double coef, double *max_div) {
+  Domain *d = (Domain *)h;
+  std::swap(d->U.v, d->U2.v); std::swap(d->V.v, d->V2.v); std::swap(d->W.v, d->W2.v);
+  PressureCorrection(*d, coef, true);
+  std::swap(d->U.v, d->U2.v); std::swap(d->V.v, d->V2.v); std::swap(d->W.v, d->W2.v);
+  if (max_div) *max_div = d->max_div;
+  return 0;
+}
+
+int orc_step(void *h, int nsteps, double *max_div, double *cfl) {
+  Domain *d = (Domain *)h;
+  for (int s = 0; s < nsteps; s++) TMarchRK3(*d);
+  if (max_div) *max_div = d->max_div;
+  if (cfl) *cfl = d->CFL;
+  return 0;
+}
+
+int orc_run_stage(void *h, int stage, int stop) {
+  Domain *d = (Domain *)h;
+  if (stage < 1 || stage > 3 || stop < 1 || stop > 3) return ELMM_ERR_INVALID_ARG;
+  if (stage == 1) BoundUVW(*d, d->U, d->V, d->W);
+  run_stage(*d, stage, stop);
+  return 0;
+}
+
+// Poisson operator alone: RHS(0:n+1)^3 in, Phi(-1:n+2)^3 out (interior).
+int orc_poisson(void *h, const double *RHS, double *Phi) {
+  Domain *d = (Domain *)h;
+  std::memcpy(d->RHS.v.data(), RHS, d->RHS.v.size() * sizeof(double));
+  poisson_solve(*d);
+  std::memcpy(Phi, d->Phi.v.data(), d->Phi.v.size() * sizeof(double));
+  return 0;
+}
+
+// BoundUVW on the resident U, V, W (for ghost-cell parity checks)
+int orc_bound_uvw(void *h) {
+  Domain *d = (Domain *)h;
+  BoundUVW(*d, d->U, d->V, d->W);
+  Bound_Pr(*d, d->Pr);
+  return 0;
+}
+
+int orc_num_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+  return omp_get_max_threads();
+#else
+  (void)n;
+  return 1;
+#endif
+}
+
+}  // extern "C"

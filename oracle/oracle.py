@@ -1,0 +1,134 @@
+"""ctypes front end of the FP64 CPU oracle (oracle/elmm_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and the
+cpu_baseline / reference legs of bench.py, always as the checker or the timed
+CPU baseline, never as a code path of the library.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libelmm_oracle.so")
+
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    if force or not os.path.exists(LIB_PATH) or (
+            os.path.getmtime(LIB_PATH) < os.path.getmtime(os.path.join(HERE, "elmm_oracle.cpp"))):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        P = C.c_void_p
+        dp = C.POINTER(C.c_double)
+        L.orc_create.restype = P
+        L.orc_create.argtypes = [P]
+        L.orc_destroy.argtypes = [P]
+        L.orc_sizes.argtypes = [P, C.POINTER(C.c_int32)]
+        L.orc_set_field.argtypes = [P, C.c_int, dp]
+        L.orc_get_field.argtypes = [P, C.c_int, dp]
+        L.orc_project.argtypes = [P, C.c_double, dp]
+        L.orc_step.argtypes = [P, C.c_int, dp, dp]
+        L.orc_run_stage.argtypes = [P, C.c_int, C.c_int]
+        L.orc_poisson.argtypes = [P, dp, dp]
+        L.orc_bound_uvw.argtypes = [P]
+        L.orc_num_threads.argtypes = [C.c_int]
+        L.orc_num_threads.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def set_threads(n: int) -> int:
+    return lib().orc_num_threads(n)
+
+
+class Oracle:
+    """One domain of the CPU restatement; field arrays use the host layout of
+    gpu_elmm_b200.workloads (Fortran bounds, x contiguous)."""
+
+    def __init__(self, cfg):
+        self.cfg = cfg
+        self.h = lib().orc_create(C.byref(cfg))
+        if not self.h:
+            raise ValueError("oracle rejected the configuration")
+        s = (C.c_int32 * 12)()
+        lib().orc_sizes(self.h, s)
+        self.sizes = tuple(s)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_destroy(self.h)
+            self.h = None
+
+    def _shape(self, field):
+        Prnx, Prny, Prnz, Unx, Uny, Unz, Vnx, Vny, Vnz, Wnx, Wny, Wnz = self.sizes
+        if field in (0, 5, 8):
+            return (Unz + 6, Uny + 6, Unx + 6)
+        if field in (1, 6, 9):
+            return (Vnz + 6, Vny + 6, Vnx + 6)
+        if field in (2, 7, 10):
+            return (Wnz + 6, Wny + 6, Wnx + 6)
+        return (Prnz + 4, Prny + 4, Prnx + 4)
+
+    def set_field(self, field, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        assert a.shape == self._shape(field), (a.shape, self._shape(field))
+        lib().orc_set_field(self.h, field, _ptr(a))
+
+    def get_field(self, field):
+        a = np.empty(self._shape(field))
+        lib().orc_get_field(self.h, field, _ptr(a))
+        return a
+
+    def set_state(self, U, V, W, Pr=None):
+        self.set_field(0, U)
+        self.set_field(1, V)
+        self.set_field(2, W)
+        if Pr is not None:
+            self.set_field(3, Pr)
+
+    def state(self):
+        return tuple(self.get_field(f) for f in (0, 1, 2, 3))
+
+    def project(self, coef=1.0) -> float:
+        md = C.c_double(0)
+        lib().orc_project(self.h, coef, C.byref(md))
+        return md.value
+
+    def step(self, n=1):
+        md = C.c_double(0)
+        cfl = C.c_double(0)
+        lib().orc_step(self.h, n, C.byref(md), C.byref(cfl))
+        return md.value, cfl.value
+
+    def run_stage(self, stage, stop):
+        r = lib().orc_run_stage(self.h, stage, stop)
+        assert r == 0
+
+    def poisson(self, RHS):
+        Prnx, Prny, Prnz = self.sizes[:3]
+        RHS = np.ascontiguousarray(RHS, dtype=np.float64)
+        assert RHS.shape == (Prnz + 2, Prny + 2, Prnx + 2)
+        Phi = np.zeros((Prnz + 4, Prny + 4, Prnx + 4))
+        lib().orc_poisson(self.h, _ptr(RHS), _ptr(Phi))
+        return Phi
+
+    def bound(self):
+        lib().orc_bound_uvw(self.h)
