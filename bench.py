@@ -1,0 +1,357 @@
+"""Benchmark of the per-timestep flow solve on B200.
+
+Workload: one 256 x 256 x 128 channel domain per GPU (periodic x and y,
+no-slip bottom with the log-law wall model, free-slip top, Smagorinsky
+Cs = 0.1, RK3, dt = 0.02): the single large domain on which the FP64 and the
+mixed path are compared.  A "step" is one RK3 time step (three stages, each
+with a full pressure projection) of that domain, inputs resident in HBM.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun every rank steps its own independent domain (weak scaling,
+no collective on the data path); the value is the total over ranks divided
+by the slowest rank's time.  `--impl reference` times the CPU restatement of
+the reference (the oracle, C++ FP64 with OpenMP on all host threads), since
+the Fortran reference itself cannot be built here.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from gpu_elmm_b200.config import grid_of, make_config  # noqa: E402
+from gpu_elmm_b200.workloads import interiors, log_profile_state  # noqa: E402
+
+METRIC = "cell-steps/s mixed vs FP64 plain, 1 B200, at ≤1e-5 rel err; p50/p99 latency"
+N = (256, 256, 128)
+WORKLOAD = ("256x256x128 channel: periodic x,y; no-slip bottom with log-law wall model (z0=0.01); "
+            "free-slip top; Smagorinsky Cs=0.1; CDS2; RK3 dt=0.02; FFT(x,y)+tridiagonal(z) projection")
+DATA = "synthetic: seeded log profile u*=0.3 + U(-0.1,0.1) perturbations on u,v,w, FP32-rounded, projected"
+# words moved per cell by the momentum kernel in stages 2 and 3: reads U,V,W,nu,Pr,Ustar x3;
+# writes Ustar x3, U2 x3 (the per-cell figure of the momentum phase)
+MOMENTUM_WORDS = 14
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend=backend, timeout=timedelta(seconds=120))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allreduce_max(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allreduce_sum(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx = float(f[2])
+                except ValueError:
+                    continue
+                for n, v in zip(names, f[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+            os.unlink(self.path)
+        except OSError:
+            pass
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        busy = [x for x in sm if x > 0.5 * (mx or max(sm))] or sm
+        return {"sm_mhz": statistics.median(busy), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def rel(a, b):
+    s = float(np.abs(b).max())
+    return float(np.abs(a - b).max()) / (s if s > 0 else 1.0)
+
+
+def cpu_baseline(steps=1):
+    """The FP64 oracle on all host threads, a bounded sample of the workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    orc.build()
+    threads = os.cpu_count() or 1
+    orc.set_threads(threads)
+    cfg = make_config(*N)
+    g = grid_of(cfg)
+    o = orc.Oracle(cfg)
+    o.set_state(*log_profile_state(g, seed=0))
+    o.project(1.0)
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    return {"value": g.cells() * steps / dt, "unit": "cell-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{steps} RK3 step(s) of the 256x256x128 workload in FP64 (oracle/elmm_oracle.cpp, "
+                      f"OpenMP, {threads} threads)", "seconds": dt}
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    orc.build()
+    threads = os.cpu_count() or 1
+    orc.set_threads(threads)
+    cfg = make_config(*N)
+    g = grid_of(cfg)
+    o = orc.Oracle(cfg)
+    o.set_state(*log_profile_state(g, seed=0))
+    o.project(1.0)
+    o.step(args.warmup)
+    t0 = time.perf_counter()
+    o.step(args.steps)
+    dt = time.perf_counter() - t0
+    v = g.cells() * args.steps / dt
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "cell-steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": DATA, "config": {"workload": WORKLOAD, "cells": g.cells(), "precision": "fp64"},
+            "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} RK3 steps of the workload (the Fortran reference cannot be "
+                                       f"built here; its C++ FP64 restatement in oracle/ is timed)"},
+            "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    from gpu_elmm_b200 import lib as L
+    torch.cuda.set_device(local)
+    g = grid_of(make_config(*N))
+    st = log_profile_state(g, seed=rank)
+    cells = g.cells()
+
+    # FP64 plain path on the same state
+    d64 = L.Domain(make_config(*N, precision=0, device=local))
+    d64.upload(*st)
+    d64.project(1.0)
+    d64.step(args.warmup)
+    barrier(ws)
+    torch.cuda.synchronize()
+    s64 = d64.step(args.steps)
+    torch.cuda.synchronize()
+    barrier(ws)
+    ms64 = allreduce_max(s64.elapsed_ms, ws)
+
+    # accuracy of the mixed path against FP64 after one step from the same state
+    a64 = L.Domain(make_config(*N, precision=0, device=local))
+    a64.upload(*st)
+    a64.project(1.0)
+    ref0 = a64.download()
+    a64.step(1)
+    ref1 = a64.download()
+    a64.close()
+    d64.close()
+    am = L.Domain(make_config(*N, precision=1, device=local))
+    am.upload(*ref0)
+    am.step(1)
+    mix1 = am.download()
+    am.close()
+    errs = [rel(a, b) for a, b in zip(interiors(g, *mix1), interiors(g, *ref1))]
+
+    # the mixed path: headline
+    dm = L.Domain(make_config(*N, precision=1, device=local))
+    dm.upload(*st)
+    dm.project(1.0)
+    dm.step(args.warmup)
+    with Clocks(local) as clk:
+        barrier(ws)
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        sm = dm.step(args.steps)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - w0
+        barrier(ws)
+    msm = allreduce_max(sm.elapsed_ms, ws)
+    total_cells = allreduce_sum(float(cells), ws)
+    value = total_cells * args.steps / (msm / 1e3)
+    v64 = total_cells * args.steps / (ms64 / 1e3)
+    max_div = allreduce_max(sm.max_div, ws)
+
+    # per-step latency distribution (device time of single-step calls)
+    lat = []
+    for _ in range(args.steps):
+        lat.append(dm.step(1).elapsed_ms)
+    lat.sort()
+    p50 = lat[len(lat) // 2]
+    p99 = lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))]
+
+    # roofline of the dominant kernel, timed live with CUDA events on the library's stream
+    kt = dm.profile_stage(stage=2, reps=5)
+    mom_ms = kt["momentum"]
+    alg_bytes = MOMENTUM_WORDS * 4 * cells
+    peak, peak_kind = peaks()
+    achieved = alg_bytes / (mom_ms / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "k_momentum_256x256x128_mixed.md")
+    if os.path.exists(tp):
+        for line in open(tp):
+            if line.startswith("dram_bytes_per_launch:"):
+                traffic = float(line.split(":")[1])
+
+    # end to end through the C-ABI with pinned host buffers: H2D of the state,
+    # one step, D2H of the state, every step
+    pinned = [torch.empty(a.shape, dtype=torch.float64, pin_memory=True).numpy() for a in st]
+    for p, a in zip(pinned, dm.download()):
+        p[...] = a
+    h2d = sum(a.nbytes for a in pinned)
+    e2e_t = []
+    for _ in range(max(3, args.steps // 2)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dm.upload(*pinned)
+        dm.step(1)
+        L.check(L.lib().elmm_download_state(dm.h, *[L.ptr(p) for p in pinned]), "elmm_download_state")
+        torch.cuda.synchronize()
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_s = allreduce_max(statistics.median(e2e_t), ws)
+    e2e = total_cells / e2e_s
+
+    cpu = cpu_baseline(1) if (rank == 0 and ws == 1) else None
+    barrier(ws)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": msm / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (FP64 reductions, zero mode, tridiagonal)", "data": DATA,
+            "config": {"workload": WORKLOAD, "cells_per_gpu": cells, "precision": "mixed",
+                       "l2": "inputs larger than L2 (mixed state ~0.5 GB per GPU)",
+                       "parallelism": "one independent domain per GPU" if ws > 1 else "single domain"},
+            "fp64_plain": {"value": v64, "unit": "cell-steps/s", "ms_per_step": ms64 / args.steps},
+            "mixed_over_fp64": value / v64,
+            "accuracy_vs_fp64_1step": {"u": errs[0], "v": errs[1], "w": errs[2], "p": errs[3],
+                                       "max_div_mixed": max_div},
+            "latency_ms": {"p50": p50, "p99": p99, "what": "device time of one RK3 step"},
+            "roofline": {"bound": "hbm", "kernel": "k_momentum (stage 2)", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": traffic, "algorithmic_bytes": alg_bytes, "ms": mom_ms},
+            "kernel_ms_stage2": kt,
+            "e2e": {"value": e2e, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
+            "gpu_launches": sm.kernels,
+            "clocks": clk.summary(),
+            "wall_s_timed": wall,
+        }
+        if cpu:
+            line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        print(json.dumps(line), flush=True)
+    dm.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    ws, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            rc = run_reference(args, ws, rank)
+        else:
+            rc = run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+    return rc
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -65,7 +65,7 @@ class ElmmStats(C.Structure):
         ("cfl", C.c_double),
         ("max_div", C.c_double),
         ("refine_sweeps", C.c_int32),
-        ("reserved", C.c_int32),
+        ("kernels", C.c_int32),
         ("elapsed_ms", C.c_double),
     ]
 

@@ -154,7 +154,7 @@ struct LaunchSet {
   Launch l() const { return Launch{starts, nd, total}; }
 };
 
-enum { LK_CELLS = 0, LK_BOX, LK_ROWS, LK_YCOLS, LK_TRI, LK_N };
+enum { LK_CELLS = 0, LK_BOX, LK_ROWS, LK_YCOLS, LK_TRI, LK_MOM, LK_N };
 
 // -------------------------------------------------------------------- batch
 template <typename T>
@@ -189,6 +189,8 @@ struct BatchT {
   bool frame_pending = false;
   cudaEvent_t t0 = nullptr, t1 = nullptr;
   long long cells = 0;
+  int step_kernels = 0;  // kernel launches of one captured step
+  int nlaunch = 0;       // running count while enqueuing
 
   ~BatchT() { release(); }
 
@@ -289,13 +291,13 @@ struct BatchT {
       if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, threads, sm) != cudaSuccess || b < 1) b = 1;
       return b * nsm;
     };
-    grid_cap[0] = cap((const void *)k_sgs<T>, TX * TY, 0);
-    grid_cap[1] = cap((const void *)k_momentum<T>, TX * TY, 0);
-    grid_cap[2] = cap((const void *)k_fftx_fwd<T>, 128, smem_x);
-    grid_cap[3] = cap((const void *)k_ffty<T>, 128, smem_y);
+    grid_cap[0] = cap((const void *)k_sgs<T>, MX * MY, 0);
+    grid_cap[1] = cap((const void *)k_momentum<T>, MX * MY, 0);
+    grid_cap[2] = cap((const void *)k_fftx_fwd<T>, kFFTThreads, smem_x);
+    grid_cap[3] = cap((const void *)k_ffty<T>, kFFTThreads, smem_y);
     grid_cap[4] = cap((const void *)k_tri<T>, kTriThreads, smem_tri);
-    grid_cap[5] = cap((const void *)k_fftx_inv<T>, 128, smem_x);
-    grid_cap[6] = cap((const void *)k_project<T>, TX * TY, 0);
+    grid_cap[5] = cap((const void *)k_fftx_inv<T>, kFFTThreads, smem_x);
+    grid_cap[6] = cap((const void *)k_project<T>, MX * MY, 0);
     grid_cap[7] = cap((const void *)k_divmax<T>, TX * TY, 0);
     grid_cap[8] = cap((const void *)k_cfl<T>, TX * TY, 0);
     // staging for host-layout copies
@@ -318,6 +320,7 @@ struct BatchT {
       case LK_BOX: return ((h.nx + 2 + TX - 1) / TX) * ((h.ny + 2 + TY - 1) / TY) * (h.nz + 2);
       case LK_ROWS: return (h.ny * h.nz + kRowsX - 1) / kRowsX;
       case LK_YCOLS: return ((h.nxh + TyOf<T>::v - 1) / TyOf<T>::v) * h.nz;
+      case LK_MOM: return ((h.nx + MX - 1) / MX) * ((h.ny + MY - 1) / MY) * ((h.nz + MKC - 1) / MKC);
       default: return (h.ny * h.spitch + kTriThreads - 1) / kTriThreads;
     }
   }
@@ -348,6 +351,14 @@ struct BatchT {
     h.xmin = c.xmin; h.ymin = c.ymin;
     h.dt = c.dt;
     h.nu_mol = c.molecular_viscosity;
+    {
+      const double dd[3] = {c.dxmin, c.dymin, g.dzmin};
+      for (int a = 0; a < 3; a++) {
+        h.cA[a] = 0.25 / dd[a];
+        h.rec2[a] = 1.0 / (dd[a] * dd[a]);
+        for (int comp = 0; comp < 3; comp++) h.cB[comp][a] = (comp == a ? 0.5 : 0.125) / dd[a];
+      }
+    }
     h.cs = c.C_Smagorinsky;
     if (!g.uniform_xy) return fail(ELMM_ERR_INVALID_CONFIG, "dxPr/dyPr must be uniform");
     size_t box = (size_t)h.plane * (h.nz + 2);
@@ -418,7 +429,7 @@ struct BatchT {
         CU(cudaMemcpy(h.wm_ustar[f], ones.data(), np * sizeof(double), cudaMemcpyHostToDevice));
       }
     if ((r = dalloc((void **)&h.prm, sizeof(double)))) return r;
-    h.nprpart = ((h.nx + TX - 1) / TX) * ((h.ny + TY - 1) / TY);
+    h.nprpart = ((h.nx + MX - 1) / MX) * ((h.ny + MY - 1) / MY);
     if ((r = dalloc((void **)&h.prpart, sizeof(double) * h.nprpart))) return r;
     if ((r = dalloc((void **)&h.maxdiv_bits, sizeof(unsigned long long)))) return r;
     if ((r = dalloc((void **)&h.cfl_bits, sizeof(unsigned long long)))) return r;
@@ -436,33 +447,38 @@ struct BatchT {
 
   // ------------------------------------------------------------ stages
   int launch_sgs() {
-    k_sgs<T><<<gsz(0, ls[LK_BOX].total), TX * TY, 0, stream>>>(ddom, ls[LK_BOX].l());
+    nlaunch++;
+    k_sgs<T><<<gsz(0, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l());
     return ELMM_OK;
   }
   int launch_momentum(int stage) {
     StageCoef sc{kRho[stage - 1], kBeta[stage - 1], 2 * kAlpha[stage - 1], stage};
-    k_momentum<T><<<gsz(1, ls[LK_CELLS].total), TX * TY, 0, stream>>>(ddom, ls[LK_CELLS].l(), sc);
+    nlaunch++;
+    k_momentum<T><<<gsz(1, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l(), sc);
     return ELMM_OK;
   }
   // PressureCorrection on U2 (in_place = 0) or on U itself (initial projection)
   int launch_projection(double coef_alpha2, int use_dt, int in_place) {
-    k_fftx_fwd<T><<<gsz(2, ls[LK_ROWS].total), 128, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan, coef_alpha2,
+    nlaunch += 7;
+    k_fftx_fwd<T><<<gsz(2, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan, coef_alpha2,
                                                                         use_dt, nullptr);
-    k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), 128, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, 0);
+    k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), kFFTThreads, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, 0);
     k_tri<T><<<gsz(4, ls[LK_TRI].total), kTriThreads, smem_tri, stream>>>(ddom, ls[LK_TRI].l());
-    k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), 128, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, 1);
-    k_fftx_inv<T><<<gsz(5, ls[LK_ROWS].total), 128, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan);
-    k_project<T><<<gsz(6, ls[LK_CELLS].total), TX * TY, 0, stream>>>(ddom, ls[LK_CELLS].l(), coef_alpha2, use_dt,
+    k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), kFFTThreads, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, 1);
+    k_fftx_inv<T><<<gsz(5, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan);
+    k_project<T><<<gsz(6, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l(), coef_alpha2, use_dt,
                                                                      in_place);
     k_prref<T><<<std::min(nd, 1024), 256, 0, stream>>>(ddom, nd);
     return ELMM_OK;
   }
   int launch_divmax() {
+    nlaunch++;
     for (int d = 0; d < nd; d++) cudaMemsetAsync(hdom[d].maxdiv_bits, 0, sizeof(unsigned long long), stream);
     k_divmax<T><<<gsz(7, ls[LK_CELLS].total), TX * TY, 0, stream>>>(ddom, ls[LK_CELLS].l());
     return ELMM_OK;
   }
   int launch_cfl() {
+    nlaunch++;
     for (int d = 0; d < nd; d++) cudaMemsetAsync(hdom[d].cfl_bits, 0, sizeof(unsigned long long), stream);
     k_cfl<T><<<gsz(8, ls[LK_CELLS].total), TX * TY, 0, stream>>>(ddom, ls[LK_CELLS].l());
     return ELMM_OK;
@@ -495,7 +511,9 @@ struct BatchT {
       if (step_exec) { cudaGraphExecDestroy(step_exec); step_exec = nullptr; }
       cudaGraph_t g;
       CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      nlaunch = 0;
       enqueue_step(cfl, true);
+      step_kernels = nlaunch;
       CU(cudaStreamEndCapture(stream, &g));
       cudaError_t e = cudaGraphInstantiate(&step_exec, g, 0);
       cudaGraphDestroy(g);
@@ -508,7 +526,9 @@ struct BatchT {
     CU(cudaStreamSynchronize(stream));
     CU(cudaGetLastError());
     time += nsteps * cfg[0].dt;
-    return fill_stats(st, nsteps);
+    int r = fill_stats(st, nsteps);
+    if (st) st->kernels = nsteps * step_kernels;
+    return r;
   }
 
   int fill_stats(elmm_stats *st, int nsteps) {
@@ -557,6 +577,49 @@ struct BatchT {
     CU(cudaStreamSynchronize(stream));
     CU(cudaGetLastError());
     return fill_stats(st, 0);
+  }
+
+  // per-kernel timing of one stage (CUDA events on the launching stream)
+  int profile_stage(int stage, int reps, double *ms) {
+    CU(cudaSetDevice(device));
+    const int nk = ELMM_NKERNELS;
+    std::vector<cudaEvent_t> ev(nk + 1);
+    for (auto &e : ev) CU(cudaEventCreate(&e));
+    std::vector<double> acc(nk, 0.0);
+    const double a2 = 2 * kAlpha[stage - 1];
+    StageCoef sc{kRho[stage - 1], kBeta[stage - 1], a2, stage};
+    for (int r = 0; r < reps; r++) {
+      int q = 0;
+      CU(cudaEventRecord(ev[q++], stream));
+      k_sgs<T><<<gsz(0, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l());
+      CU(cudaEventRecord(ev[q++], stream));
+      k_momentum<T><<<gsz(1, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l(), sc);
+      CU(cudaEventRecord(ev[q++], stream));
+      k_fftx_fwd<T><<<gsz(2, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan, a2, 1, nullptr);
+      CU(cudaEventRecord(ev[q++], stream));
+      k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), kFFTThreads, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, 0);
+      CU(cudaEventRecord(ev[q++], stream));
+      k_tri<T><<<gsz(4, ls[LK_TRI].total), kTriThreads, smem_tri, stream>>>(ddom, ls[LK_TRI].l());
+      CU(cudaEventRecord(ev[q++], stream));
+      k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), kFFTThreads, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, 1);
+      CU(cudaEventRecord(ev[q++], stream));
+      k_fftx_inv<T><<<gsz(5, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan);
+      CU(cudaEventRecord(ev[q++], stream));
+      k_project<T><<<gsz(6, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l(), a2, 1, 0);
+      CU(cudaEventRecord(ev[q++], stream));
+      k_prref<T><<<std::min(nd, 1024), 256, 0, stream>>>(ddom, nd);
+      CU(cudaEventRecord(ev[q++], stream));
+      CU(cudaStreamSynchronize(stream));
+      CU(cudaGetLastError());
+      for (int k = 0; k < nk; k++) {
+        float t = 0;
+        CU(cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
+        acc[k] += t;
+      }
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    for (int k = 0; k < nk; k++) ms[k] = acc[k] / reps;
+    return ELMM_OK;
   }
 
   // --------------------------------------------------------- host copies
@@ -761,12 +824,12 @@ static int poisson_exec(BatchT<T> &B, double *Phi, const double *RHS) {
   CU(cudaMemcpyAsync(B.dstage, RHS, n * sizeof(double), cudaMemcpyHostToDevice, B.stream));
   CU(cudaMemsetAsync(B.dbad, 0, sizeof(int), B.stream));
   k_unpack<T><<<256, 256, 0, B.stream>>>(B.ddom, h.Phi, B.dstage, hb, h.nx, h.ny, h.nz, B.dbad);
-  k_fftx_fwd<T><<<B.gsz(2, B.ls[LK_ROWS].total), 128, B.smem_x, B.stream>>>(
+  k_fftx_fwd<T><<<B.gsz(2, B.ls[LK_ROWS].total), kFFTThreads, B.smem_x, B.stream>>>(
       B.ddom, B.ls[LK_ROWS].l(), B.dplan, 1.0, 0, h.Phi);
-  k_ffty<T><<<B.gsz(3, B.ls[LK_YCOLS].total), 128, B.smem_y, B.stream>>>(B.ddom, B.ls[LK_YCOLS].l(), B.dplan, 0);
+  k_ffty<T><<<B.gsz(3, B.ls[LK_YCOLS].total), kFFTThreads, B.smem_y, B.stream>>>(B.ddom, B.ls[LK_YCOLS].l(), B.dplan, 0);
   k_tri<T><<<B.gsz(4, B.ls[LK_TRI].total), kTriThreads, B.smem_tri, B.stream>>>(B.ddom, B.ls[LK_TRI].l());
-  k_ffty<T><<<B.gsz(3, B.ls[LK_YCOLS].total), 128, B.smem_y, B.stream>>>(B.ddom, B.ls[LK_YCOLS].l(), B.dplan, 1);
-  k_fftx_inv<T><<<B.gsz(5, B.ls[LK_ROWS].total), 128, B.smem_x, B.stream>>>(B.ddom, B.ls[LK_ROWS].l(), B.dplan);
+  k_ffty<T><<<B.gsz(3, B.ls[LK_YCOLS].total), kFFTThreads, B.smem_y, B.stream>>>(B.ddom, B.ls[LK_YCOLS].l(), B.dplan, 1);
+  k_fftx_inv<T><<<B.gsz(5, B.ls[LK_ROWS].total), kFFTThreads, B.smem_x, B.stream>>>(B.ddom, B.ls[LK_ROWS].l(), B.dplan);
   HostBox hp = B.hbox_p(0);
   size_t np = (size_t)hp.n0 * hp.n1 * hp.n2;
   CU(cudaMemcpyAsync(B.dstage, Phi, np * sizeof(double), cudaMemcpyHostToDevice, B.stream));
@@ -865,6 +928,12 @@ int elmm_run_stage(elmm_handle *h, int32_t stage, int32_t stop) {
   CU(cudaStreamSynchronize(s));
   CU(cudaGetLastError());
   return ELMM_OK;
+}
+
+int elmm_profile_stage(elmm_handle *h, int32_t stage, int32_t reps, double *ms) {
+  if (!h || !ms) return fail(ELMM_ERR_INVALID_ARG, "NULL argument");
+  if (stage < 1 || stage > 3 || reps < 1) return fail(ELMM_ERR_INVALID_ARG, "stage 1..3, reps >= 1");
+  return DISPATCH(h->b, profile_stage(stage, reps, ms));
 }
 
 // ------------------------------------------------------------- batches

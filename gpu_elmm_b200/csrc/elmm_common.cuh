@@ -51,6 +51,12 @@ struct Dom {
   double xmin, ymin;     // xU(0), yV(0)
   double dt;
   double nu_mol, cs;
+  // coefficients computed once on the host as the reference computes them
+  // once per call (advection.f90: Ax = 0.25/dxmin etc.; momentum_diffusion.f90:
+  // recdxmin2 = 1/dxmin**2)
+  double cA[3];          // 0.25 / dxmin, dymin, dzmin
+  double cB[3][3];       // advective-form factors of component c: 0.5 along c, 0.125 across
+  double rec2[3];        // 1 / dxmin**2, ...
   // fields (box layout)
   T *U, *V, *W, *U2, *V2, *W2, *Us, *Vs, *Ws, *P, *nu, *Phi;
   // spectral data S[k][ky][kx], row pitch spitch (complex elements)
@@ -138,44 +144,39 @@ ELMM_HD int fold_rep(int g, int n, bool periodic) {
 
 // The ghost images of interior index t along one dimension for a one-deep
 // shell: the producer of cell t also writes the ghosts that fold onto it.
+// Only t == 1 and t == n can have images; fixed slots keep everything in
+// registers.
 struct Images {
-  int n;
-  int idx[3];
-  int sign[3];
-  int zero[3];
+  int t, n1;            // the index itself and the hi ghost index n + 1
+  int lo_ok, hi_ok;     // ghost 0 / ghost n+1 fold onto t
+  int lo_sign, hi_sign;
+  int lo_zero, hi_zero; // the ghost is a constant 0 written by this cell
 };
 
+ELMM_HD Images images_none(int t, int n) { return Images{t, n + 1, 0, 0, 1, 1, 0, 0}; }
+
 ELMM_HD Images images_vel(int t, int n, int blo, int bhi, bool normal) {
-  Images im;
-  im.n = 1; im.idx[0] = t; im.sign[0] = 1; im.zero[0] = 0;
+  Images im = images_none(t, n);
+  if (t != 1 && t != n) return im;
   Fold lo = fold_vel(0, n, blo, bhi, normal);
-  if (lo.zero ? (t == 1) : (lo.src == t)) {
-    im.idx[im.n] = 0; im.sign[im.n] = lo.zero ? 1 : lo.sign; im.zero[im.n] = lo.zero; im.n++;
-  }
+  if (lo.zero ? (t == 1) : (lo.src == t)) { im.lo_ok = 1; im.lo_sign = lo.zero ? 1 : lo.sign; im.lo_zero = lo.zero; }
   Fold hi = fold_vel(n + 1, n, blo, bhi, normal);
-  if (hi.zero ? (t == n) : (hi.src == t)) {
-    im.idx[im.n] = n + 1; im.sign[im.n] = hi.zero ? 1 : hi.sign; im.zero[im.n] = hi.zero; im.n++;
-  }
+  if (hi.zero ? (t == n) : (hi.src == t)) { im.hi_ok = 1; im.hi_sign = hi.zero ? 1 : hi.sign; im.hi_zero = hi.zero; }
   return im;
 }
 
 ELMM_HD Images images_rep(int t, int n, bool periodic) {
-  Images im;
-  im.n = 1; im.idx[0] = t; im.sign[0] = 1; im.zero[0] = 0;
-  if (fold_rep(0, n, periodic) == t) { im.idx[im.n] = 0; im.sign[im.n] = 1; im.zero[im.n] = 0; im.n++; }
-  if (fold_rep(n + 1, n, periodic) == t) { im.idx[im.n] = n + 1; im.sign[im.n] = 1; im.zero[im.n] = 0; im.n++; }
+  Images im = images_none(t, n);
+  if (fold_rep(0, n, periodic) == t) im.lo_ok = 1;
+  if (fold_rep(n + 1, n, periodic) == t) im.hi_ok = 1;
   return im;
 }
 
 // Only periodic copies (pressure: its non-periodic ghosts are never read by
 // the second-order kernels).
 ELMM_HD Images images_per(int t, int n, bool periodic) {
-  Images im;
-  im.n = 1; im.idx[0] = t; im.sign[0] = 1; im.zero[0] = 0;
-  if (periodic) {
-    if (t == n) { im.idx[im.n] = 0; im.sign[im.n] = 1; im.zero[im.n] = 0; im.n++; }
-    if (t == 1) { im.idx[im.n] = n + 1; im.sign[im.n] = 1; im.zero[im.n] = 0; im.n++; }
-  }
+  Images im = images_none(t, n);
+  if (periodic) { im.lo_ok = (t == n); im.hi_ok = (t == 1); }
   return im;
 }
 
@@ -183,21 +184,30 @@ ELMM_HD Images images_per(int t, int n, bool periodic) {
 template <typename T>
 __device__ __forceinline__ void push_ghosts(const Dom<T> &d, T *F, const Images &ix, const Images &iy,
                                             const Images &iz, T v) {
-  if (ix.n == 1 && iy.n == 1 && iz.n == 1) return;
-  for (int c = 0; c < iz.n; c++)
-    for (int b = 0; b < iy.n; b++)
-      for (int a = 0; a < ix.n; a++) {
+  if (!(ix.lo_ok | ix.hi_ok | iy.lo_ok | iy.hi_ok | iz.lo_ok | iz.hi_ok)) return;
+  const int xi[3] = {ix.t, 0, ix.n1}, yi[3] = {iy.t, 0, iy.n1}, zi[3] = {iz.t, 0, iz.n1};
+  const int xo[3] = {1, ix.lo_ok, ix.hi_ok}, yo[3] = {1, iy.lo_ok, iy.hi_ok}, zo[3] = {1, iz.lo_ok, iz.hi_ok};
+  const int xs[3] = {1, ix.lo_sign, ix.hi_sign}, ys[3] = {1, iy.lo_sign, iy.hi_sign}, zs[3] = {1, iz.lo_sign, iz.hi_sign};
+  const int xz[3] = {0, ix.lo_zero, ix.hi_zero}, yz[3] = {0, iy.lo_zero, iy.hi_zero}, zz[3] = {0, iz.lo_zero, iz.hi_zero};
+#pragma unroll
+  for (int c = 0; c < 3; c++)
+#pragma unroll
+    for (int b = 0; b < 3; b++)
+#pragma unroll
+      for (int a = 0; a < 3; a++) {
         if (a == 0 && b == 0 && c == 0) continue;
-        int s = ix.sign[a] * iy.sign[b] * iz.sign[c];
-        bool z = ix.zero[a] | iy.zero[b] | iz.zero[c];
-        T w = z ? T(0) : (s > 0 ? v : -v);
-        F[bidx(d, ix.idx[a], iy.idx[b], iz.idx[c])] = w;
+        if (!(xo[a] && yo[b] && zo[c])) continue;
+        const int s = xs[a] * ys[b] * zs[c];
+        const bool z = xz[a] | yz[b] | zz[c];
+        const T w = z ? T(0) : (s > 0 ? v : -v);
+        F[bidx(d, xi[a], yi[b], zi[c])] = w;
       }
 }
 
 template <typename T>
 __device__ __forceinline__ void push_vel(const Dom<T> &d, T *F, int comp, int i, int j, int k, T v) {
   const int *e = d.ext[comp];
+  if (i != 1 && i != e[0] && j != 1 && j != e[1] && k != 1 && k != e[2]) return;
   Images ix = images_vel(i, e[0], d.bt[0], d.bt[1], comp == 0);
   Images iy = images_vel(j, e[1], d.bt[2], d.bt[3], comp == 1);
   Images iz = images_vel(k, e[2], d.bt[4], d.bt[5], comp == 2);

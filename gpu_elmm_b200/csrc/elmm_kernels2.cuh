@@ -9,7 +9,7 @@ namespace elmm {
 // inverse real FFT along x of kRowsX rows -> Phi(1:nx) with its ghosts
 // (Bound_Phi, src/boundaries.f90:1817-1948, one cell deep).
 template <typename T>
-__global__ void __launch_bounds__(128) k_fftx_inv(const Dom<T> *__restrict__ doms, Launch L,
+__global__ void __launch_bounds__(kFFTThreads) k_fftx_inv(const Dom<T> *__restrict__ doms, Launch L,
                                                   const PoisPlan *__restrict__ plans) {
   typedef typename Vec2<T>::type T2;
   extern __shared__ unsigned char smem_raw[];
@@ -26,6 +26,7 @@ __global__ void __launch_bounds__(128) k_fftx_inv(const Dom<T> *__restrict__ dom
     const int nrows = d.ny * d.nz;
     // Z_m = A_m + i B_m with the Hermitian completion A_{N-m} = conj(A_m);
     // A_0 and A_{N/2} are real for a real row.
+#pragma unroll 4
     for (int w = threadIdx.x; w < ntr * N; w += blockDim.x) {
       const int p = w / N, m = w - p * N;
       const int ra = row0 + 2 * p, rb = ra + 1;
@@ -45,6 +46,7 @@ __global__ void __launch_bounds__(128) k_fftx_inv(const Dom<T> *__restrict__ dom
     __syncthreads();
     T2 *res = fft_block<T, T2>(buf0, buf1, ntr, pl.fx, d.twx, true);
     const bool px = d.bt[SIDE_WE] == BC_PERIODIC, py = d.bt[SIDE_SO] == BC_PERIODIC, pz = d.bt[SIDE_BO] == BC_PERIODIC;
+#pragma unroll 4
     for (int w = threadIdx.x; w < kRowsX * N; w += blockDim.x) {
       const int r = w / N, i = w - r * N + 1;
       const int row = row0 + r;
@@ -53,77 +55,110 @@ __global__ void __launch_bounds__(128) k_fftx_inv(const Dom<T> *__restrict__ dom
       const T2 z = res[(r >> 1) * N + i - 1];
       const T v = (r & 1) ? z.y : z.x;
       d.Phi[bidx(d, i, j, k)] = v;
-      Images ix = images_rep(i, d.nx, px), iy = images_rep(j, d.ny, py), iz = images_rep(k, d.nz, pz);
-      push_ghosts(d, d.Phi, ix, iy, iz, v);
+      if (i == 1 || i == d.nx || j == 1 || j == d.ny || k == 1 || k == d.nz) {
+        Images ix = images_rep(i, d.nx, px), iy = images_rep(j, d.ny, py), iz = images_rep(k, d.nz, pz);
+        push_ghosts(d, d.Phi, ix, iy, iz, v);
+      }
     }
     __syncthreads();
   }
 }
 
 // PostPoisson (src/pressure.f90:728-870): velocity correction, Pr += Phi and
-// the partial sums of the top layer for FixPressureToReference.  src may be
-// the same array as dst (initial projection in place).
+// the partial sums of the top layer for FixPressureToReference.  A block
+// marches up an MX x MY column of MKC planes; the inputs of plane k+1 are in
+// flight while plane k is written, and Phi(k+1) of plane k is Phi of k+1.
 template <typename T>
-__global__ void __launch_bounds__(TX *TY) k_project(const Dom<T> *__restrict__ doms, Launch L, double coef_alpha2,
+__global__ void __launch_bounds__(MX *MY) k_project(const Dom<T> *__restrict__ doms, Launch L, double coef_alpha2,
                                                     int use_dt, int in_place) {
-  __shared__ double red[TX * TY / 32];
+  __shared__ double red[MX * MY / 32];
   for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
     const int di = find_dom(L.starts, L.nd, t);
     const Dom<T> &d = doms[di];
     int lt = t - __ldg(L.starts + di);
-    const int ntx = (d.nx + TX - 1) / TX, nty = (d.ny + TY - 1) / TY;
-    const int tx = lt % ntx; lt /= ntx;
-    const int ty = lt % nty;
-    const int k = lt / nty + 1;
-    const int i = tx * TX + (threadIdx.x % TX) + 1;
-    const int j = ty * TY + (threadIdx.x / TX) + 1;
-    const bool inside = i <= d.nx && j <= d.ny;
+    const int ntx = (d.nx + MX - 1) / MX, nty = (d.ny + MY - 1) / MY;
+    const int bx = lt % ntx; lt /= ntx;
+    const int by = lt % nty;
+    const int bk = lt / nty;
+    const int k0 = bk * MKC + 1, k1 = min(k0 + MKC - 1, d.nz);
+    const int i = bx * MX + (threadIdx.x % MX) + 1;
+    const int j = by * MY + (threadIdx.x / MX) + 1;
+    const int nx = d.nx, ny = d.ny, nz = d.nz;
+    const bool inside = i <= nx && j <= ny;
     const double coef = use_dt ? coef_alpha2 * d.dt : coef_alpha2;
     const T dt2 = (T)coef;
     const T Au = (T)(coef / d.dx), Av = (T)(coef / d.dy), Aw = (T)(coef / d.dz);
-    const T *Us = in_place ? d.U : d.U2;
-    const T *Vs = in_place ? d.V : d.V2;
-    const T *Ws = in_place ? d.W : d.W2;
-    double top = 0;
+    const T *__restrict__ Usrc = in_place ? d.U : d.U2;
+    const T *__restrict__ Vsrc = in_place ? d.V : d.V2;
+    const T *__restrict__ Wsrc = in_place ? d.W : d.W2;
+    const T *__restrict__ Phi = d.Phi;
+    T *__restrict__ P = d.P;
+    const long long pitch = d.pitch, plane = d.plane;
+    const bool hu = inside && i <= d.ext[0][0] && j <= d.ext[0][1];
+    const bool hv = inside && i <= d.ext[1][0] && j <= d.ext[1][1];
+    const bool hw = inside && i <= d.ext[2][0] && j <= d.ext[2][1];
+    const T m = (T)(*d.prm);
+    const bool px = d.bt[SIDE_WE] == BC_PERIODIC, py = d.bt[SIDE_SO] == BC_PERIODIC, pz = d.bt[SIDE_BO] == BC_PERIODIC;
+    long long c = bidx(d, inside ? i : 1, inside ? j : 1, k0);
+    T phi = 0, pe = 0, pn = 0, pt = 0, u0 = 0, v0 = 0, w0 = 0, p0 = 0;
     if (inside) {
-      const long long c = bidx(d, i, j, k);
-      const T phi = ld(d.Phi, c);
-      if (i <= d.ext[0][0] && j <= d.ext[0][1] && k <= d.ext[0][2]) {
-        T u = Us[c] - Au * (ld(d.Phi, c + 1) - phi);
-        d.U[c] = u;
-        push_vel(d, d.U, 0, i, j, k, u);
-      }
-      if (i <= d.ext[1][0] && j <= d.ext[1][1] && k <= d.ext[1][2]) {
-        T v = Vs[c] - Av * (ld(d.Phi, c + d.pitch) - phi);
-        d.V[c] = v;
-        push_vel(d, d.V, 1, i, j, k, v);
-      }
-      if (i <= d.ext[2][0] && j <= d.ext[2][1] && k <= d.ext[2][2]) {
-        T w;
-        if (d.vz) w = Ws[c] - dt2 * (ld(d.Phi, c + d.plane) - phi) / (T)d.dzW[k + 2];
-        else w = Ws[c] - Aw * (ld(d.Phi, c + d.plane) - phi);
-        d.W[c] = w;
-        push_vel(d, d.W, 2, i, j, k, w);
-      }
-      const T m = (T)(*d.prm);
-      T p = (d.P[c] - m) + phi;
-      d.P[c] = p;
-      Images ix = images_per(i, d.nx, d.bt[SIDE_WE] == BC_PERIODIC);
-      Images iy = images_per(j, d.ny, d.bt[SIDE_SO] == BC_PERIODIC);
-      Images iz = images_per(k, d.nz, d.bt[SIDE_BO] == BC_PERIODIC);
-      push_ghosts(d, d.P, ix, iy, iz, p);
-      if (k == d.nz) top = (double)p;
+      phi = __ldg(Phi + c); pe = __ldg(Phi + c + 1); pn = __ldg(Phi + c + pitch); pt = __ldg(Phi + c + plane);
+      if (hu) u0 = __ldg(Usrc + c);
+      if (hv) v0 = __ldg(Vsrc + c);
+      if (hw) w0 = __ldg(Wsrc + c);
+      p0 = P[c];
     }
-    if (k == d.nz) {  // block-uniform branch
-      for (int o = 16; o > 0; o >>= 1) top += __shfl_down_sync(0xffffffffu, top, o);
-      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = top;
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        double s = 0;
-        for (int w = 0; w < TX * TY / 32; w++) s += red[w];
-        d.prpart[ty * ntx + tx] = s;
+    for (int k = k0; k <= k1; k++) {
+      const bool more = k + 1 <= k1;
+      T npe = 0, npn = 0, npt = 0, nu0 = 0, nv0 = 0, nw0 = 0, np0 = 0;
+      if (more && inside) {
+        const long long cn = c + plane;
+        npe = __ldg(Phi + cn + 1); npn = __ldg(Phi + cn + pitch); npt = __ldg(Phi + cn + plane);
+        if (hu) nu0 = __ldg(Usrc + cn);
+        if (hv) nv0 = __ldg(Vsrc + cn);
+        if (hw) nw0 = __ldg(Wsrc + cn);
+        np0 = P[cn];
       }
-      __syncthreads();
+      double top = 0;
+      if (inside) {
+        if (hu && k <= d.ext[0][2]) {
+          T u = u0 - Au * (pe - phi);
+          d.U[c] = u;
+          push_vel(d, d.U, 0, i, j, k, u);
+        }
+        if (hv && k <= d.ext[1][2]) {
+          T v = v0 - Av * (pn - phi);
+          d.V[c] = v;
+          push_vel(d, d.V, 1, i, j, k, v);
+        }
+        if (hw && k <= d.ext[2][2]) {
+          T w;
+          if (d.vz) w = w0 - dt2 * (pt - phi) / (T)d.dzW[k + 2];
+          else w = w0 - Aw * (pt - phi);
+          d.W[c] = w;
+          push_vel(d, d.W, 2, i, j, k, w);
+        }
+        T p = (p0 - m) + phi;
+        P[c] = p;
+        if (i == 1 || i == nx || j == 1 || j == ny || k == 1 || k == nz) {
+          Images ix = images_per(i, nx, px), iy = images_per(j, ny, py), iz = images_per(k, nz, pz);
+          push_ghosts(d, P, ix, iy, iz, p);
+        }
+        top = (double)p;
+      }
+      if (k == nz) {  // block-uniform: the top layer's partial sum of this column
+        for (int o = 16; o > 0; o >>= 1) top += __shfl_down_sync(0xffffffffu, top, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = top;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          double sum = 0;
+          for (int w = 0; w < MX * MY / 32; w++) sum += red[w];
+          d.prpart[by * ntx + bx] = sum;
+        }
+        __syncthreads();
+      }
+      phi = pt; pe = npe; pn = npn; pt = npt; u0 = nu0; v0 = nv0; w0 = nw0; p0 = np0;
+      c += plane;
     }
   }
 }

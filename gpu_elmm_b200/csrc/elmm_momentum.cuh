@@ -1,0 +1,571 @@
+// elmm_momentum.cuh -- Convection + OtherTerms of one RK3 stage in one pass:
+// CDS2 skew-symmetric advection (advection.f90:15-327,
+// advection_variable_z.f90:15-324), explicit diffusion with the wall-flux
+// corrections (momentum_diffusion.f90:169-420 and the wmfluxes-*-inc.f90
+// includes), the RK combine (dynamics.f90:266-354, :450-478), the
+// old-pressure gradient (dynamics.f90:58-199) and U2 += U (tsteps.f90:352-354).
+//
+// A block owns an MX x MY column of cells and marches up a chunk of MKC
+// planes.  U, V, W and Viscosity of planes k-1, k, k+1 (with a one-cell
+// halo in x and y) sit in a three-slot ring in shared memory; while plane k
+// is computed, plane k+2 is already on its way into registers.  Every input
+// cell is thus read from HBM once per chunk instead of once per stencil use.
+#pragma once
+
+#include "elmm_common.cuh"
+
+namespace elmm {
+
+struct StageCoef {
+  double rho, beta, alpha2;  // RK_rho, RK_beta, 2*RK_alpha of the stage
+  int stage;
+};
+
+constexpr int MX = 32, MY = 8, MKC = 16;
+constexpr int MPW = MX + 2, MPH = MY + 2, MPS = MPW * MPH;
+
+// stencil accessor over the plane ring: field f (0 U, 1 V, 2 W, 3 nu)
+template <typename T>
+struct Ring {
+  const T *p[3];  // planes k-1, k, k+1 (field-major, MPS elements per field)
+  int o;          // offset of the thread's own cell in a plane
+  __device__ __forceinline__ T g(int f, int dx, int dy, int dz) const { return p[dz + 1][f * MPS + o + dy * MPW + dx]; }
+};
+
+template <typename T>
+struct MomTabs {
+  T cA[3], cB[3][3], rec2[3];
+};
+
+// one velocity component's tendency at (i,j,k): advection + diffusion +
+// wall corrections, in the reference's order of operations
+template <typename T, int C>
+__device__ __forceinline__ T tendency(const Dom<T> &d, const MomTabs<T> &m, const Ring<T> &R, int i, int j, int k) {
+  // X(dx,dy,dz) with the component's own axis first: along = C, a1, a2 the others
+#define FU(dx, dy, dz) R.g(0, dx, dy, dz)
+#define FV(dx, dy, dz) R.g(1, dx, dy, dz)
+#define FW(dx, dy, dz) R.g(2, dx, dy, dz)
+#define FN(dx, dy, dz) R.g(3, dx, dy, dz)
+  T a;
+  const T rx = m.rec2[0], ry = m.rec2[1], rz = m.rec2[2];
+  if (C == 0) {
+    const T u = FU(0, 0, 0), ue = FU(1, 0, 0), uw = FU(-1, 0, 0), un = FU(0, 1, 0), us = FU(0, -1, 0);
+    const T ut = FU(0, 0, 1), ub = FU(0, 0, -1);
+    const T v = FV(0, 0, 0), ve = FV(1, 0, 0), vs = FV(0, -1, 0), vse = FV(1, -1, 0);
+    const T w = FW(0, 0, 0), we = FW(1, 0, 0), wb = FW(0, 0, -1), wbe = FW(1, 0, -1);
+    const T Ax = m.cA[0], Ay = m.cA[1];
+    const T Bx = m.cB[0][0], By = m.cB[0][1];
+    if (!d.vz) {
+      const T Az = m.cA[2], Bz = m.cB[0][2];
+      a = -((Ax * (ue + u) * (ue + u) - Ax * (u + uw) * (u + uw)) + (Ay * (un + u) * (ve + v) - Ay * (u + us) * (vse + vs)) +
+            (Az * (ut + u) * (we + w) - Az * (u + ub) * (wbe + wb)));
+      T Vadv = (v + ve + vs + vse);
+      T Wadv = (w + we + wb + wbe);
+      a = a - (Bx * (ue - uw) * u + By * (un - us) * Vadv + Bz * (ut - ub) * Wadv);
+    } else {
+      const T dzp = (T)d.dzPr[k + 2];
+      a = -((Ax * (ue + u) * (ue + u) - Ax * (u + uw) * (u + uw)) + (Ay * (un + u) * (ve + v) - Ay * (u + us) * (vse + vs)) +
+            ((ut + u) * (we + w) - (u + ub) * (wbe + wb)) / dzp / 4);
+      T Vadv = (v + ve + vs + vse);
+      T Wadv = (w + we + wb + wbe) / 4;
+      a = a - (Bx * (ue - uw) * u + By * (un - us) * Vadv + (ut - ub) / (T)(d.zPr[k + 1 + 2] - d.zPr[k - 1 + 2]) * Wadv);
+    }
+    a = a * (T)0.5;
+    const T n0 = FN(0, 0, 0), ne = FN(1, 0, 0), nn = FN(0, 1, 0), nne = FN(1, 1, 0), ns = FN(0, -1, 0), nse = FN(1, -1, 0);
+    const T nt = FN(0, 0, 1), nte = FN(1, 0, 1), nb = FN(0, 0, -1), nbe = FN(1, 0, -1);
+    a = a + ne * (ue - u) * rx;
+    a = a - n0 * (u - uw) * rx;
+    a = a + (T)0.25 * (nne + ne + nn + n0) * (un - u) * ry;
+    a = a - (T)0.25 * (ne + nse + n0 + ns) * (u - us) * ry;
+    if (!d.vz) {
+      a = a + (T)0.25 * (nte + ne + nt + n0) * (ut - u) * rz;
+      a = a - (T)0.25 * (ne + nbe + n0 + nb) * (u - ub) * rz;
+    } else {
+      T tz = (T)0.25 * (nte + ne + nt + n0) * (ut - u) / (T)d.dzW[k + 2];
+      tz = tz - (T)0.25 * (ne + nbe + n0 + nb) * (u - ub) / (T)d.dzW[k - 1 + 2];
+      tz = tz / (T)d.dzPr[k + 2];
+      a = a + tz;
+    }
+    const int *e = d.ext[0];
+    if (d.wall[SIDE_WE] && i == 1) {
+      long long p = (long long)(j - 1) + (long long)e[1] * (k - 1);
+      a = a + n0 * (u - uw) * rx;
+      a = a + d.wm_fluxp[0 * 6 + SIDE_WE][p];
+    }
+    if (d.wall[SIDE_EA] && i == e[0]) {
+      long long p = (long long)(j - 1) + (long long)e[1] * (k - 1);
+      a = a - ne * (ue - u) * rx;
+      a = a - d.wm_fluxm[0 * 6 + SIDE_EA][p];
+    }
+    if (d.wall[SIDE_SO] && j == 1) {
+      long long p = (long long)(i - 1) + (long long)e[0] * (k - 1);
+      a = a + (ne + nse + n0 + ns) * (u - us) * ry / 4;
+      a = a + d.wm_fluxp[0 * 6 + SIDE_SO][p];
+    }
+    if (d.wall[SIDE_NO] && j == e[1]) {
+      long long p = (long long)(i - 1) + (long long)e[0] * (k - 1);
+      a = a - (nne + ne + nn + n0) * (un - u) * ry / 4;
+      a = a - d.wm_fluxm[0 * 6 + SIDE_NO][p];
+    }
+    if (d.wall[SIDE_BO] && k == 1) {
+      long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
+      T s = ne + nbe + n0 + nb;
+      if (d.vz) a = a + s * (u - ub) / (T)d.dzW[k - 1 + 2] / 4 / (T)d.dzPr[k + 2];
+      else a = a + s * (u - ub) * rz / 4;
+      a = a + d.wm_fluxp[0 * 6 + SIDE_BO][p];
+    }
+    if (d.wall[SIDE_TO] && k == e[2]) {
+      long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
+      T s = nte + ne + nt + n0;
+      if (d.vz) a = a - s * (ut - u) / (T)d.dzW[k + 2] / 4 / (T)d.dzPr[k + 2];
+      else a = a - s * (ut - u) * rz / 4;
+      a = a - d.wm_fluxm[0 * 6 + SIDE_TO][p];
+    }
+  } else if (C == 1) {
+    const T v = FV(0, 0, 0), ve = FV(1, 0, 0), vw = FV(-1, 0, 0), vn = FV(0, 1, 0), vs = FV(0, -1, 0);
+    const T vt = FV(0, 0, 1), vb = FV(0, 0, -1);
+    const T u = FU(0, 0, 0), un = FU(0, 1, 0), uw = FU(-1, 0, 0), unw = FU(-1, 1, 0);
+    const T w = FW(0, 0, 0), wn = FW(0, 1, 0), wb = FW(0, 0, -1), wbn = FW(0, 1, -1);
+    const T Ax = m.cA[0], Ay = m.cA[1];
+    const T Bx = m.cB[1][0], By = m.cB[1][1];
+    if (!d.vz) {
+      const T Az = m.cA[2], Bz = m.cB[1][2];
+      a = -((Ay * (vn + v) * (vn + v) - Ay * (v + vs) * (v + vs)) + (Ax * (ve + v) * (un + u) - Ax * (v + vw) * (unw + uw)) +
+            (Az * (vt + v) * (wn + w) - Az * (v + vb) * (wbn + wb)));
+      T Uadv = (u + un + uw + unw);
+      T Wadv = (w + wn + wb + wbn);
+      a = a - (Bx * (ve - vw) * Uadv + By * (vn - vs) * v + Bz * (vt - vb) * Wadv);
+    } else {
+      const T dzp = (T)d.dzPr[k + 2];
+      a = -((Ay * (vn + v) * (vn + v) - Ay * (v + vs) * (v + vs)) + (Ax * (ve + v) * (un + u) - Ax * (v + vw) * (unw + uw)) +
+            ((vt + v) * (wn + w) - (v + vb) * (wbn + wb)) / dzp / 4);
+      T Uadv = (u + un + uw + unw);
+      T Wadv = (w + wn + wb + wbn) / 4;
+      a = a - (Bx * (ve - vw) * Uadv + By * (vn - vs) * v + (vt - vb) / (T)(d.zPr[k + 1 + 2] - d.zPr[k - 1 + 2]) * Wadv);
+    }
+    a = a * (T)0.5;
+    const T n0 = FN(0, 0, 0), ne = FN(1, 0, 0), nn = FN(0, 1, 0), nne = FN(1, 1, 0), nw = FN(-1, 0, 0), nnw = FN(-1, 1, 0);
+    const T nt = FN(0, 0, 1), nnt = FN(0, 1, 1), nb = FN(0, 0, -1), nnb = FN(0, 1, -1);
+    a = a + (T)0.25 * (nne + ne + nn + n0) * (ve - v) * rx;
+    a = a - (T)0.25 * (nn + n0 + nnw + nw) * (v - vw) * rx;
+    a = a + nn * (vn - v) * ry;
+    a = a - n0 * (v - vs) * ry;
+    if (!d.vz) {
+      a = a + (T)0.25 * (nnt + nn + nt + n0) * (vt - v) * rz;
+      a = a - (T)0.25 * (nn + nnb + n0 + nb) * (v - vb) * rz;
+    } else {
+      T tz = (T)0.25 * (nnt + nn + nt + n0) * (vt - v) / (T)d.dzW[k + 2];
+      tz = tz - (T)0.25 * (nn + nnb + n0 + nb) * (v - vb) / (T)d.dzW[k - 1 + 2];
+      tz = tz / (T)d.dzPr[k + 2];
+      a = a + tz;
+    }
+    const int *e = d.ext[1];
+    if (d.wall[SIDE_WE] && i == 1) {
+      long long p = (long long)(j - 1) + (long long)e[1] * (k - 1);
+      a = a + (nn + n0 + nnw + nw) * (v - vw) * rx / 4;
+      a = a + d.wm_fluxp[1 * 6 + SIDE_WE][p];
+    }
+    if (d.wall[SIDE_EA] && i == e[0]) {
+      long long p = (long long)(j - 1) + (long long)e[1] * (k - 1);
+      a = a - (nne + ne + nn + n0) * (ve - v) * rx / 4;
+      a = a - d.wm_fluxm[1 * 6 + SIDE_EA][p];
+    }
+    if (d.wall[SIDE_SO] && j == 1) {
+      long long p = (long long)(i - 1) + (long long)e[0] * (k - 1);
+      a = a + n0 * (v - vs) * ry;
+      a = a + d.wm_fluxp[1 * 6 + SIDE_SO][p];
+    }
+    if (d.wall[SIDE_NO] && j == e[1]) {
+      long long p = (long long)(i - 1) + (long long)e[0] * (k - 1);
+      a = a - nn * (vn - v) * ry;
+      a = a - d.wm_fluxm[1 * 6 + SIDE_NO][p];
+    }
+    if (d.wall[SIDE_BO] && k == 1) {
+      long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
+      T s = nn + nnb + n0 + nb;
+      if (d.vz) a = a + s * (v - vb) / (T)d.dzW[k - 1 + 2] / 4 / (T)d.dzPr[k + 2];
+      else a = a + s * (v - vb) * rz / 4;
+      a = a + d.wm_fluxp[1 * 6 + SIDE_BO][p];
+    }
+    if (d.wall[SIDE_TO] && k == e[2]) {
+      long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
+      T s = nnt + nn + nt + n0;
+      if (d.vz) a = a - s * (vt - v) / (T)d.dzW[k + 2] / 4 / (T)d.dzPr[k + 2];
+      else a = a - s * (vt - v) * rz / 4;
+      a = a - d.wm_fluxm[1 * 6 + SIDE_TO][p];
+    }
+  } else {
+    const T w = FW(0, 0, 0), we = FW(1, 0, 0), ww = FW(-1, 0, 0), wn = FW(0, 1, 0), ws = FW(0, -1, 0);
+    const T wt = FW(0, 0, 1), wb = FW(0, 0, -1);
+    const T u = FU(0, 0, 0), ut = FU(0, 0, 1), uw = FU(-1, 0, 0), utw = FU(-1, 0, 1);
+    const T v = FV(0, 0, 0), vt = FV(0, 0, 1), vs = FV(0, -1, 0), vts = FV(0, -1, 1);
+    const T Ax = m.cA[0], Ay = m.cA[1];
+    const T Bx = m.cB[2][0], By = m.cB[2][1];
+    if (!d.vz) {
+      const T Az = m.cA[2], Bz = m.cB[2][2];
+      a = -((Az * (wt + w) * (wt + w) - Az * (w + wb) * (w + wb)) + (Ay * (wn + w) * (vt + v) - Ay * (w + ws) * (vs + vts)) +
+            (Ax * (we + w) * (ut + u) - Ax * (w + ww) * (utw + uw)));
+      T Uadv = (u + ut + uw + utw);
+      T Vadv = (v + vt + vs + vts);
+      a = a - (Bx * (we - ww) * Uadv + By * (wn - ws) * Vadv + Bz * (wt - wb) * w);
+    } else {
+      const T dzw = (T)d.dzW[k + 2];
+      a = -(((wt + w) * (wt + w) - (w + wb) * (w + wb)) / dzw / 4 + (Ay * (wn + w) * (vt + v) - Ay * (w + ws) * (vts + vs)) +
+            (Ax * (we + w) * (ut + u) - Ax * (w + ww) * (utw + uw)));
+      T Uadv = (u + ut + uw + utw);
+      T Vadv = (v + vt + vs + vts);
+      a = a - (Bx * (we - ww) * Uadv + By * (wn - ws) * Vadv + (wt - wb) / (T)(d.zW[k + 1 + 2] - d.zW[k - 1 + 2]) * w);
+    }
+    a = a * (T)0.5;
+    const T n0 = FN(0, 0, 0), ne = FN(1, 0, 0), nt = FN(0, 0, 1), nte = FN(1, 0, 1), nw = FN(-1, 0, 0), ntw = FN(-1, 0, 1);
+    const T nn = FN(0, 1, 0), ntn = FN(0, 1, 1), ns = FN(0, -1, 0), nts = FN(0, -1, 1);
+    a = a + (T)0.25 * (nte + ne + nt + n0) * (we - w) * rx;
+    a = a - (T)0.25 * (nt + n0 + ntw + nw) * (w - ww) * rx;
+    a = a + (T)0.25 * (ntn + nt + nn + n0) * (wn - w) * ry;
+    a = a - (T)0.25 * (nt + nts + n0 + ns) * (w - ws) * ry;
+    if (!d.vz) {
+      a = a + nt * (wt - w) * rz;
+      a = a - n0 * (w - wb) * rz;
+    } else {
+      T tz = nt * (wt - w) / (T)d.dzPr[k + 1 + 2];
+      tz = tz - n0 * (w - wb) / (T)d.dzPr[k + 2];
+      tz = tz / (T)d.dzW[k + 2];
+      a = a + tz;
+    }
+    const int *e = d.ext[2];
+    if (d.wall[SIDE_WE] && i == 1) {
+      long long p = (long long)(j - 1) + (long long)e[1] * (k - 1);
+      a = a + (nt + n0 + ntw + nw) * (w - ww) * rx / 4;
+      a = a + d.wm_fluxp[2 * 6 + SIDE_WE][p];
+    }
+    if (d.wall[SIDE_EA] && i == e[0]) {
+      long long p = (long long)(j - 1) + (long long)e[1] * (k - 1);
+      a = a - (nte + ne + nt + n0) * (we - w) * rx / 4;
+      a = a - d.wm_fluxm[2 * 6 + SIDE_EA][p];
+    }
+    if (d.wall[SIDE_SO] && j == 1) {
+      long long p = (long long)(i - 1) + (long long)e[0] * (k - 1);
+      a = a + (nt + nts + n0 + ns) * (w - ws) * ry / 4;
+      a = a + d.wm_fluxp[2 * 6 + SIDE_SO][p];
+    }
+    if (d.wall[SIDE_NO] && j == e[1]) {
+      long long p = (long long)(i - 1) + (long long)e[0] * (k - 1);
+      a = a - (ntn + nt + nn + n0) * (wn - w) * ry / 4;
+      a = a - d.wm_fluxm[2 * 6 + SIDE_NO][p];
+    }
+    if (d.wall[SIDE_BO] && k == 1) {
+      long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
+      if (d.vz) a = a + n0 * (w - wb) / (T)d.dzPr[k + 2] / (T)d.dzW[k + 2];
+      else a = a + n0 * (w - wb) * rz;
+      a = a + d.wm_fluxp[2 * 6 + SIDE_BO][p];
+    }
+    if (d.wall[SIDE_TO] && k == e[2]) {
+      long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
+      if (d.vz) a = a - nt * (wt - w) / (T)d.dzPr[k + 1 + 2] / (T)d.dzW[k + 2];
+      else a = a - nt * (wt - w) * rz;
+      a = a - d.wm_fluxm[2 * 6 + SIDE_TO][p];
+    }
+  }
+#undef FU
+#undef FV
+#undef FW
+#undef FN
+  return a;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(MX *MY, 2) k_momentum(const Dom<T> *__restrict__ doms, Launch L, StageCoef sc) {
+  __shared__ T ring[3][4 * MPS];
+  __shared__ MomTabs<T> tab;
+  constexpr int NPF = (MPS + MX * MY - 1) / (MX * MY);  // plane elements per thread and field
+  const int tx = threadIdx.x % MX, ty = threadIdx.x / MX;
+  for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
+    const int di = find_dom(L.starts, L.nd, t);
+    const Dom<T> &d = doms[di];
+    int lt = t - __ldg(L.starts + di);
+    const int ntx = (d.nx + MX - 1) / MX, nty = (d.ny + MY - 1) / MY;
+    const int bx = lt % ntx; lt /= ntx;
+    const int by = lt % nty;
+    const int bk = lt / nty;
+    const int i0 = bx * MX + 1, j0 = by * MY + 1, k0 = bk * MKC + 1;
+    const int k1 = min(k0 + MKC - 1, d.nz);
+    const int i = i0 + tx, j = j0 + ty;
+    const int nx = d.nx, ny = d.ny;
+    const long long pitch = d.pitch, plane = d.plane;
+    const T *__restrict__ F[4] = {d.U, d.V, d.W, d.nu};
+    T *__restrict__ Us = d.Us;
+    T *__restrict__ Vs = d.Vs;
+    T *__restrict__ Ws = d.Ws;
+    const T *__restrict__ P = d.P;
+    __syncthreads();  // the ring and table of the previous tile are no longer read
+    if (threadIdx.x < 3) {
+      const int a = threadIdx.x;
+      tab.cA[a] = (T)d.cA[a];
+      tab.rec2[a] = (T)d.rec2[a];
+      for (int c = 0; c < 3; c++) tab.cB[c][a] = (T)d.cB[c][a];
+    }
+    // plane element e of this thread: (li, lj) in the haloed tile
+    int goff[NPF];
+    bool gok[NPF];
+#pragma unroll
+    for (int q = 0; q < NPF; q++) {
+      int e = threadIdx.x + q * MX * MY;
+      int li = e % MPW, lj = e / MPW;
+      int gi = i0 - 1 + li, gj = j0 - 1 + lj;
+      gok[q] = e < MPS && gi <= nx + 1 && gj <= ny + 1;
+      goff[q] = gok[q] ? (d.aln - 1 + gi) + (int)pitch * gj : 0;
+    }
+    for (int kk = k0 - 1; kk <= k0 + 1; kk++) {
+      T *dst = ring[kk % 3];
+#pragma unroll
+      for (int f = 0; f < 4; f++)
+#pragma unroll
+        for (int q = 0; q < NPF; q++) {
+          int e = threadIdx.x + q * MX * MY;
+          if (e < MPS) dst[f * MPS + e] = gok[q] ? __ldg(F[f] + goff[q] + plane * kk) : (T)0;
+        }
+    }
+    const T dt = (T)d.dt, rdt = (T)sc.rho, bdt = (T)sc.beta;
+    const double coefd = sc.alpha2 * d.dt;
+    const T coef = (T)coefd;
+    const T gx = (T)(-coefd / d.dx), gy = (T)(-coefd / d.dy), gz = (T)(-coefd / d.dz);
+    const T m = (T)(*d.prm);
+    const bool inside = i <= nx && j <= ny;
+    const bool hasU = i <= d.ext[0][0] && j <= d.ext[0][1];
+    const bool hasV = i <= d.ext[1][0] && j <= d.ext[1][1];
+    const bool hasW = i <= d.ext[2][0] && j <= d.ext[2][1];
+    const bool stage1 = sc.stage == 1;
+    // per-cell inputs of the current plane, fetched one plane ahead
+    long long c = bidx(d, inside ? i : 1, inside ? j : 1, k0);
+    T cUs = 0, cVs = 0, cWs = 0, cP = 0, cPx = 0, cPy = 0, cPz = 0;
+    if (inside) {
+      if (!stage1) { cUs = Us[c]; cVs = Vs[c]; cWs = Ws[c]; }
+      cP = __ldg(P + c); cPx = __ldg(P + c + 1); cPy = __ldg(P + c + pitch); cPz = __ldg(P + c + plane);
+    }
+    __syncthreads();
+    for (int k = k0; k <= k1; k++) {
+      const bool more = k + 1 <= k1;
+      // prefetch plane k+2 of the ring and the per-cell inputs of plane k+1
+      T pre[4][NPF];
+      T nUs = 0, nVs = 0, nWs = 0, nP = 0, nPx = 0, nPy = 0, nPz = 0;
+      if (more) {
+#pragma unroll
+        for (int f = 0; f < 4; f++)
+#pragma unroll
+          for (int q = 0; q < NPF; q++) pre[f][q] = gok[q] ? __ldg(F[f] + goff[q] + plane * (k + 2)) : (T)0;
+        if (inside) {
+          const long long cn = c + plane;
+          if (!stage1) { nUs = Us[cn]; nVs = Vs[cn]; nWs = Ws[cn]; }
+          nP = __ldg(P + cn); nPx = __ldg(P + cn + 1); nPy = __ldg(P + cn + pitch); nPz = __ldg(P + cn + plane);
+        }
+      }
+      if (inside) {
+        Ring<T> R;
+        R.p[0] = ring[(k - 1) % 3];
+        R.p[1] = ring[k % 3];
+        R.p[2] = ring[(k + 1) % 3];
+        R.o = (ty + 1) * MPW + (tx + 1);
+        const T p0 = cP - m;
+        if (hasU && k <= d.ext[0][2]) {
+          T ts = tendency<T, 0>(d, tab, R, i, j, k);
+          T u2 = stage1 ? (T)0 : cUs * rdt * dt;
+          Us[c] = ts;
+          u2 = u2 + ts * bdt * dt;
+          if (d.prgx_on) u2 = u2 + (-coef) * (T)d.prgx;
+          u2 = u2 + gx * ((cPx - m) - p0);
+          u2 = u2 + R.g(0, 0, 0, 0);
+          d.U2[c] = u2;
+          push_vel(d, d.U2, 0, i, j, k, u2);
+        }
+        if (hasV && k <= d.ext[1][2]) {
+          T ts = tendency<T, 1>(d, tab, R, i, j, k);
+          T v2 = stage1 ? (T)0 : cVs * rdt * dt;
+          Vs[c] = ts;
+          v2 = v2 + ts * bdt * dt;
+          if (d.prgy_on) v2 = v2 + (-coef) * (T)d.prgy;
+          v2 = v2 + gy * ((cPy - m) - p0);
+          v2 = v2 + R.g(1, 0, 0, 0);
+          d.V2[c] = v2;
+          push_vel(d, d.V2, 1, i, j, k, v2);
+        }
+        if (hasW && k <= d.ext[2][2]) {
+          T ts = tendency<T, 2>(d, tab, R, i, j, k);
+          T w2 = stage1 ? (T)0 : cWs * rdt * dt;
+          Ws[c] = ts;
+          w2 = w2 + ts * bdt * dt;
+          if (d.vz) w2 = w2 - coef * ((cPz - m) - p0) / (T)d.dzW[k + 2];
+          else w2 = w2 + gz * ((cPz - m) - p0);
+          w2 = w2 + R.g(2, 0, 0, 0);
+          d.W2[c] = w2;
+          push_vel(d, d.W2, 2, i, j, k, w2);
+        }
+      }
+      __syncthreads();  // plane k-1 is no longer read
+      if (more) {
+        T *dst = ring[(k + 2) % 3];
+#pragma unroll
+        for (int f = 0; f < 4; f++)
+#pragma unroll
+          for (int q = 0; q < NPF; q++) {
+            int e = threadIdx.x + q * MX * MY;
+            if (e < MPS) dst[f * MPS + e] = pre[f][q];
+          }
+        cUs = nUs; cVs = nVs; cWs = nWs; cP = nP; cPx = nPx; cPy = nPy; cPz = nPz;
+        c += plane;
+      }
+      __syncthreads();
+    }
+  }
+}
+
+
+// ---------------------------------------------------------------- k_sgs
+// SubgridStresses (src/dynamics.f90:869-908): Smagorinsky viscosity
+// (SGS_Smag / NuSmag / StrainIJ, src/subgrid.f90:30-67, :170-209) from a
+// ring of U, V, W planes; each cell also writes the ghost cells that fold
+// onto it (BoundViscosity, src/scalarboundaries.f90:326-431).  Cells next to
+// a wall-model side compute the wall fluxes of the velocity points there.
+template <typename T>
+__device__ __forceinline__ T nusmag_ring(const Dom<T> &d, const Ring<T> &R, int k) {
+#define GU(dx, dy, dz) R.g(0, dx, dy, dz)
+#define GV(dx, dy, dz) R.g(1, dx, dy, dz)
+#define GW(dx, dy, dz) R.g(2, dx, dy, dz)
+  const T dx = (T)d.dx, dy = (T)d.dy;
+  const T dzk = (T)d.dzPr[k + 2];
+  const T zz = (T)(d.zPr[k + 1 + 2] - d.zPr[k - 1 + 2]);
+  T D00 = (GU(0, 0, 0) - GU(-1, 0, 0)) / dx;
+  T D11 = (GV(0, 0, 0) - GV(0, -1, 0)) / dy;
+  T D22 = (GW(0, 0, 0) - GW(0, 0, -1)) / dzk;
+  T D01 = (GU(0, 1, 0) + GU(-1, 1, 0) - GU(0, -1, 0) - GU(-1, -1, 0)) / (4 * dy);
+  T D02 = (GU(0, 0, 1) + GU(-1, 0, 1) - GU(0, 0, -1) - GU(-1, 0, -1)) / (2 * zz);
+  T D10 = (GV(1, 0, 0) + GV(1, -1, 0) - GV(-1, 0, 0) - GV(-1, -1, 0)) / (4 * dx);
+  T D12 = (GV(0, 0, 1) + GV(0, -1, 1) - GV(0, 0, -1) - GV(0, -1, -1)) / (2 * zz);
+  T D20 = (GW(1, 0, 0) + GW(1, 0, -1) - GW(-1, 0, 0) - GW(-1, 0, -1)) / (4 * dx);
+  T D21 = (GW(0, 1, 0) + GW(0, 1, -1) - GW(0, -1, 0) - GW(0, -1, -1)) / (4 * dy);
+#undef GU
+#undef GV
+#undef GW
+  T s, S = 0;
+  s = (D00 + D00) / 2; S = S + s * s;
+  s = (D10 + D01) / 2; S = S + s * s;
+  s = (D20 + D02) / 2; S = S + s * s;
+  s = (D01 + D10) / 2; S = S + s * s;
+  s = (D11 + D11) / 2; S = S + s * s;
+  s = (D21 + D12) / 2; S = S + s * s;
+  s = (D02 + D20) / 2; S = S + s * s;
+  s = (D12 + D21) / 2; S = S + s * s;
+  s = (D22 + D22) / 2; S = S + s * s;
+  T Sbar = sqrt((T)2 * S);
+  T wc = (T)d.width[k] * (T)d.cs;
+  return Sbar * (wc * wc);
+}
+
+template <typename T>
+__device__ void wm_point(const Dom<T> &d, int comp, int f, int i, int j, int k, long long pidx);
+template <typename T>
+__device__ long long wm_plane_index(const Dom<T> &d, int comp, int f, int i, int j, int k);
+
+template <typename T>
+__global__ void __launch_bounds__(MX *MY, 3) k_sgs(const Dom<T> *__restrict__ doms, Launch L) {
+  __shared__ T ring[3][3 * MPS];
+  constexpr int NPF = (MPS + MX * MY - 1) / (MX * MY);
+  const int tx = threadIdx.x % MX, ty = threadIdx.x / MX;
+  for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
+    const int di = find_dom(L.starts, L.nd, t);
+    const Dom<T> &d = doms[di];
+    int lt = t - __ldg(L.starts + di);
+    const int ntx = (d.nx + MX - 1) / MX, nty = (d.ny + MY - 1) / MY;
+    const int bx = lt % ntx; lt /= ntx;
+    const int by = lt % nty;
+    const int bk = lt / nty;
+    const int i0 = bx * MX + 1, j0 = by * MY + 1, k0 = bk * MKC + 1;
+    const int k1 = min(k0 + MKC - 1, d.nz);
+    const int i = i0 + tx, j = j0 + ty;
+    const int nx = d.nx, ny = d.ny, nz = d.nz;
+    const long long pitch = d.pitch, plane = d.plane;
+    const T *__restrict__ F[3] = {d.U, d.V, d.W};
+    T *__restrict__ nu = d.nu;
+    int goff[NPF];
+    bool gok[NPF];
+#pragma unroll
+    for (int q = 0; q < NPF; q++) {
+      int e = threadIdx.x + q * MX * MY;
+      int li = e % MPW, lj = e / MPW;
+      int gi = i0 - 1 + li, gj = j0 - 1 + lj;
+      gok[q] = e < MPS && gi <= nx + 1 && gj <= ny + 1;
+      goff[q] = gok[q] ? (d.aln - 1 + gi) + (int)pitch * gj : 0;
+    }
+    __syncthreads();
+    for (int kk = k0 - 1; kk <= k0 + 1; kk++) {
+      T *dst = ring[kk % 3];
+#pragma unroll
+      for (int f = 0; f < 3; f++)
+#pragma unroll
+        for (int q = 0; q < NPF; q++) {
+          int e = threadIdx.x + q * MX * MY;
+          if (e < MPS) dst[f * MPS + e] = gok[q] ? __ldg(F[f] + goff[q] + plane * kk) : (T)0;
+        }
+    }
+    __syncthreads();
+    const bool inside = i <= nx && j <= ny;
+    const bool px = d.bt[SIDE_WE] == BC_PERIODIC, py = d.bt[SIDE_SO] == BC_PERIODIC, pz = d.bt[SIDE_BO] == BC_PERIODIC;
+    const bool anywall = d.wall[0] | d.wall[1] | d.wall[2] | d.wall[3] | d.wall[4] | d.wall[5];
+    const T num = (T)d.nu_mol;
+    for (int k = k0; k <= k1; k++) {
+      const bool more = k + 1 <= k1;
+      T pre[3][NPF];
+      if (more) {
+#pragma unroll
+        for (int f = 0; f < 3; f++)
+#pragma unroll
+          for (int q = 0; q < NPF; q++) pre[f][q] = gok[q] ? __ldg(F[f] + goff[q] + plane * (k + 2)) : (T)0;
+      }
+      if (inside) {
+        Ring<T> R;
+        R.p[0] = ring[(k - 1) % 3];
+        R.p[1] = ring[k % 3];
+        R.p[2] = ring[(k + 1) % 3];
+        R.o = (ty + 1) * MPW + (tx + 1);
+        T v;
+        if (d.sgs) {
+          v = nusmag_ring(d, R, k);
+          if (d.nu_mol > 0) v = v + num;
+        } else {
+          v = num;
+        }
+        const long long c = bidx(d, i, j, k);
+        nu[c] = v;
+        const bool edge = i == 1 || i == nx || j == 1 || j == ny || k == 1 || k == nz;
+        if (edge) {
+          Images ix = images_rep(i, nx, px), iy = images_rep(j, ny, py), iz = images_rep(k, nz, pz);
+          push_ghosts(d, nu, ix, iy, iz, v);
+        }
+        if (anywall && (edge || k == nz - 1 || i == nx - 1 || j == ny - 1)) {
+#pragma unroll 1
+          for (int f = 0; f < 6; f++) {
+            if (!d.wall[f]) continue;
+#pragma unroll 1
+            for (int comp = 0; comp < 3; comp++) {
+              long long p = wm_plane_index(d, comp, f, i, j, k);
+              if (p >= 0) wm_point(d, comp, f, i, j, k, p);
+            }
+          }
+        }
+      }
+      __syncthreads();
+      if (more) {
+        T *dst = ring[(k + 2) % 3];
+#pragma unroll
+        for (int f = 0; f < 3; f++)
+#pragma unroll
+          for (int q = 0; q < NPF; q++) {
+            int e = threadIdx.x + q * MX * MY;
+            if (e < MPS) dst[f * MPS + e] = pre[f][q];
+          }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+}  // namespace elmm

@@ -20,6 +20,9 @@ _lib = None
 
 _dp = C.POINTER(C.c_double)
 
+KERNEL_NAMES = ("sgs", "momentum", "fftx_fwd", "ffty_fwd", "tri", "ffty_inv", "fftx_inv", "project", "prref")
+KERNEL_COUNT = len(KERNEL_NAMES)
+
 
 class ElmmError(RuntimeError):
     def __init__(self, code: int, what: str, msg: str):
@@ -48,6 +51,7 @@ def lib():
         L.elmm_project.argtypes = [P, C.c_double, C.POINTER(ElmmStats)]
         L.elmm_step.argtypes = [P, C.c_int32, C.POINTER(ElmmStats)]
         L.elmm_run_stage.argtypes = [P, C.c_int32, C.c_int32]
+        L.elmm_profile_stage.argtypes = [P, C.c_int32, C.c_int32, _dp]
         L.elmm_poisson_solver_new.argtypes = [C.POINTER(P), C.POINTER(C.c_int32), _dp, C.POINTER(C.c_int32),
                                               C.c_int32, C.c_int32]
         L.elmm_poisson_solver_nonuniform_z_new.argtypes = [C.POINTER(P), C.POINTER(C.c_int32), _dp, _dp, _dp,
@@ -124,6 +128,12 @@ class Domain:
 
     def run_stage(self, stage, stop):
         check(lib().elmm_run_stage(self.h, stage, stop), "elmm_run_stage")
+
+    def profile_stage(self, stage=2, reps=5):
+        """Mean device time (ms) of each kernel of one RK3 stage, CUDA events on the library's stream."""
+        ms = (C.c_double * KERNEL_COUNT)()
+        check(lib().elmm_profile_stage(self.h, stage, reps, ms), "elmm_profile_stage")
+        return dict(zip(KERNEL_NAMES, list(ms)))
 
     def frame_begin(self):
         check(lib().elmm_frame_begin(self.h), "elmm_frame_begin")

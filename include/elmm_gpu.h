@@ -116,7 +116,7 @@ typedef struct elmm_stats {
   double cfl;                   /* CFL number of the last step (enable_CFL_check) */
   double max_div;               /* max |div u| after the last projection, FP64 */
   int32_t refine_sweeps;        /* defect-correction sweeps run in the last stage */
-  int32_t reserved;
+  int32_t kernels;              /* kernel launches of the library in this call */
   double elapsed_ms;            /* device time of the call (CUDA events) */
 } elmm_stats;
 
@@ -169,6 +169,16 @@ int elmm_step(elmm_handle *h, int32_t nsteps, elmm_stats *stats);
  *   stop = 3: the full stage (projection and swap)
  * stage is 1..3.  Fields are read back with elmm_download_field. */
 int elmm_run_stage(elmm_handle *h, int32_t stage, int32_t stop);
+
+/* Kernel timing of one stage (no counterpart in the reference; the
+ * reference's per-part timers are src/tsteps.f90:113, :234-238): runs the
+ * kernels of RK3 stage `stage` `reps` times on the handle's stream, each
+ * bracketed by CUDA events, and writes the mean duration in ms of each
+ * kernel kind to ms[ELMM_NKERNELS] in the order of ELMM_KERNEL_NAMES.  The
+ * state advances as by `reps` stages. */
+#define ELMM_NKERNELS 9
+#define ELMM_KERNEL_NAMES "sgs,momentum,fftx_fwd,ffty_fwd,tri,ffty_inv,fftx_inv,project,prref"
+int elmm_profile_stage(elmm_handle *h, int32_t stage, int32_t reps, double *ms);
 
 /*
  * PoisSolver-compatible solver (the interface of src/poisson.f90:108-121,

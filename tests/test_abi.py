@@ -1,0 +1,103 @@
+"""C-ABI surface of libelmm_gpu.so: every entry point declared in
+include/elmm_gpu.h is exported, the ctypes mirrors have the C layout, and
+argument / configuration errors come back as status codes without a GPU."""
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+from conftest import ROOT
+from gpu_elmm_b200 import config as cfgmod
+from gpu_elmm_b200 import lib as L
+
+HEADER = os.path.join(ROOT, "include", "elmm_gpu.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?[a-z_0-9]+\s*\**\s*(elmm_\w+)\s*\(", src, flags=re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    names = declared_functions()
+    assert len(names) >= 24 and "elmm_step" in names and "elmm_poisson_solver_execute" in names
+    lib = L.lib()
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    out = subprocess.run(["nm", "-D", "--defined-only", L.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (elmm_\w+)", out))
+    assert set(names) <= exported
+
+
+def _c_layout():
+    prog = r'''
+#include <stdio.h>
+#include <stddef.h>
+#include "elmm_gpu.h"
+#define O(s, f) printf(#s "." #f " %zu\n", offsetof(s, f));
+int main(void) {
+  printf("elmm_config.size %zu\n", sizeof(elmm_config));
+  printf("elmm_stats.size %zu\n", sizeof(elmm_stats));
+  O(elmm_config, Btype) O(elmm_config, xmin) O(elmm_config, zW) O(elmm_config, dt)
+  O(elmm_config, sgstype) O(elmm_config, z0) O(elmm_config, pr_gradient_x) O(elmm_config, precision)
+  O(elmm_config, refine_tol) O(elmm_config, device)
+  O(elmm_stats, time) O(elmm_stats, max_div) O(elmm_stats, refine_sweeps) O(elmm_stats, elapsed_ms)
+  return 0;
+}
+'''
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "l.c")
+        open(c, "w").write(prog)
+        exe = os.path.join(d, "l")
+        subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe], check=True)
+        out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout
+    return dict((l.split()[0], int(l.split()[1])) for l in out.splitlines())
+
+
+def test_ctypes_layout_matches_c():
+    lay = _c_layout()
+    assert lay["elmm_config.size"] == C.sizeof(cfgmod.ElmmConfig)
+    assert lay["elmm_stats.size"] == C.sizeof(cfgmod.ElmmStats)
+    for key, off in lay.items():
+        s, f = key.split(".")
+        if f == "size":
+            continue
+        cls = cfgmod.ElmmConfig if s == "elmm_config" else cfgmod.ElmmStats
+        assert getattr(cls, f).offset == off, key
+
+
+def test_config_defaults_and_errors_without_gpu():
+    lib = L.lib()
+    c = cfgmod.ElmmConfig()
+    assert lib.elmm_config_defaults(C.byref(c), 64, 64, 32) == 0
+    assert c.Btype[4] == cfgmod.BC_NOSLIP and c.Btype[5] == cfgmod.BC_FREESLIP
+    assert abs(c.molecular_viscosity - 1 / 70000) < 1e-20 and c.wallmodeltype == 1
+    h = C.c_void_p()
+    bad = cfgmod.make_config(64, 64, 32)
+    bad.Btype[0] = 1  # no-slip x needs the FFT in x: refused
+    assert lib.elmm_create(C.byref(bad), C.byref(h)) == 1
+    assert b"periodic" in lib.elmm_last_error()
+    bad = cfgmod.make_config(64, 64, 32)
+    bad.Prnx = 7 * 11
+    assert lib.elmm_create(C.byref(bad), C.byref(h)) == 1
+    bad = cfgmod.make_config(64, 64, 32)
+    bad.abi_version = 99
+    assert lib.elmm_create(C.byref(bad), C.byref(h)) == 1
+    assert lib.elmm_create(None, C.byref(h)) == 6
+    assert lib.elmm_step(None, 1, None) == 6
+
+
+def test_no_cpu_fallback_without_device():
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    with pytest.raises(L.ElmmError) as e:
+        L.Domain(cfgmod.make_config(32, 24, 16))
+    assert e.value.code == 4  # ELMM_ERR_CUDA

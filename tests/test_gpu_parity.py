@@ -1,0 +1,281 @@
+"""Parity of the CUDA library (through its C-ABI) with the FP64 oracle.
+
+Tolerances (relative = max|gpu - oracle| / max|oracle|):
+  * FP64 path, velocities U, V, W: 1e-12 after 1 and 10 steps;
+  * FP64 path, pressure: 1e-11.  The pressure is ill-conditioned with
+    respect to its inputs: a perturbation of the input velocities by one
+    unit in the last place moves the oracle's own pressure by ~2e-12 after
+    one step (test_pressure_conditioning_floor measures it), so two correct
+    FP64 implementations cannot agree on it to 1e-12;
+  * max |div u| after every projection: 1e-10 (FP64), 1e-6 (mixed);
+  * mixed FP32 path: velocities 1e-5 after 1 step; the pressure error is
+    reported (FP32 rounding of the state times the same conditioning).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, rel
+from gpu_elmm_b200 import lib as L
+from gpu_elmm_b200.config import (BC_FREESLIP, BC_NOSLIP, BC_PERIODIC, FIELD_PHI, FIELD_U2, FIELD_USTAR,
+                                  FIELD_V2, FIELD_VISCOSITY, FIELD_VSTAR, FIELD_W2, FIELD_WSTAR, grid_of,
+                                  make_config)
+from gpu_elmm_b200.workloads import interior, interiors, log_profile_state
+from oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+CHANNEL = (BC_PERIODIC, BC_PERIODIC, BC_PERIODIC, BC_PERIODIC, BC_NOSLIP, BC_FREESLIP)
+
+
+def stretched(nz, first=0.5, ratio=1.04):
+    return np.concatenate([[0.0], np.cumsum(first * ratio ** np.arange(nz))])
+
+
+def pair(cfg, seed=0, project=True):
+    g = grid_of(cfg)
+    zW = None
+    if cfg.zW:
+        zW = np.ctypeslib.as_array(cfg.zW, shape=(cfg.Prnz + 1,)).copy()
+    st = log_profile_state(g, seed=seed, zW=zW)
+    o = Oracle(cfg)
+    o.set_state(*st)
+    d = L.Domain(cfg)
+    d.upload(*st)
+    if project:
+        o.project(1.0)
+        d.project(1.0)
+    return g, o, d, st
+
+
+def errs(g, gpu_state, orc_state):
+    return [rel(a, b) for a, b in zip(interiors(g, *gpu_state), interiors(g, *orc_state))]
+
+
+@pytest.mark.parametrize("n", [(32, 24, 16), (64, 64, 32)])
+def test_initial_projection(n):
+    cfg = make_config(*n)
+    g, o, d, _ = pair(cfg, project=False)
+    md_o = o.project(1.0)
+    st = d.project(1.0)
+    e = errs(g, d.download(), o.state())
+    assert max(e[:3]) < 1e-13, e
+    assert e[3] < 1e-12, e
+    assert st.max_div < 1e-10 and md_o < 1e-10
+
+
+def test_uploaded_ghosts_follow_bounduvw():
+    for bt in (CHANNEL, (3, 3, 3, 3, 1, 1), (3, 3, 3, 3, 3, 3)):
+        cfg = make_config(16, 12, 8, btype=bt)
+        g, o, d, _ = pair(cfg, project=False)
+        o.bound()
+        for a, b in zip(d.download()[:3], o.state()[:3]):
+            assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("zstretch", [False, True])
+def test_poisson_solver_interface(zstretch):
+    n = (48, 32, 20)
+    zW = stretched(n[2]) if zstretch else None
+    cfg = make_config(*n, zW=zW, sgstype=0)
+    g = grid_of(cfg)
+    rng = np.random.default_rng(0)
+    r = rng.standard_normal((n[2], n[1], n[0]))
+    w = np.diff(zW) if zstretch else np.ones(n[2])
+    r -= (r * w[:, None, None]).sum() / (w.sum() * n[0] * n[1])
+    RHS = np.zeros(g.shape_rhs())
+    RHS[1:-1, 1:-1, 1:-1] = r
+    po = Oracle(cfg).poisson(RHS)
+    ps = L.PoissonSolver(n, L=(float(n[0]), float(n[1]), float(n[2])), zW=zW)
+    Phi = np.full(g.shape_p(), 7.0)
+    ps.execute(Phi, RHS)
+    assert rel(Phi[2:-2, 2:-2, 2:-2], po[2:-2, 2:-2, 2:-2]) < 1e-12
+    assert (Phi[0] == 7.0).all() and (Phi[:, :, 1] == 7.0).all()  # ghosts untouched
+
+
+def test_stage_operators():
+    cfg = make_config(32, 24, 16)
+    g, o, d, _ = pair(cfg)
+    o.run_stage(1, 1)
+    d.run_stage(1, 1)
+    nu_o, nu_g = o.get_field(FIELD_VISCOSITY), d.field(FIELD_VISCOSITY)
+    assert rel(nu_g[1:-1, 1:-1, 1:-1], nu_o[1:-1, 1:-1, 1:-1]) < 1e-13
+    g2, o2, d2, _ = pair(cfg)
+    o2.run_stage(1, 2)
+    d2.run_stage(1, 2)
+    for f in (FIELD_U2, FIELD_V2, FIELD_W2):
+        assert rel(d2.field(f), o2.get_field(f)) < 1e-13
+    ext = {FIELD_USTAR: (g.Unx, g.Uny, g.Unz), FIELD_VSTAR: (g.Vnx, g.Vny, g.Vnz), FIELD_WSTAR: (g.Wnx, g.Wny, g.Wnz)}
+    for f, e in ext.items():
+        assert rel(interior(d2.field(f), -2, e), interior(o2.get_field(f), -2, e)) < 1e-13
+
+
+def test_fp64_steps_1_and_10():
+    cfg = make_config(64, 64, 32)
+    g, o, d, _ = pair(cfg)
+    o.step(1)
+    s = d.step(1)
+    e1 = errs(g, d.download(), o.state())
+    assert max(e1[:3]) < 1e-12 and e1[3] < 1e-11, e1
+    assert s.max_div < 1e-10
+    o.step(9)
+    s = d.step(9)
+    e10 = errs(g, d.download(), o.state())
+    assert max(e10[:3]) < 1e-12 and e10[3] < 1e-11, e10
+    assert s.max_div < 1e-10
+    print("FP64 errors after 1 / 10 steps (U, V, W, P):", e1, e10, "max div", s.max_div)
+
+
+def test_pressure_conditioning_floor():
+    """The oracle against itself with inputs perturbed by ~1 ulp: the pressure
+    moves by the same order as the GPU-oracle difference."""
+    cfg = make_config(32, 24, 16)
+    g = grid_of(cfg)
+    st = log_profile_state(g, seed=0)
+    o = Oracle(cfg)
+    o.set_state(*st)
+    o.project(1.0)
+    s0 = o.state()
+    rng = np.random.default_rng(3)
+    pert = [x * (1 + 1e-16 * rng.standard_normal(x.shape)) for x in s0[:3]] + [s0[3]]
+    a, b = Oracle(cfg), Oracle(cfg)
+    a.set_state(*s0)
+    b.set_state(*pert)
+    a.step(1)
+    b.step(1)
+    floor = rel(interiors(g, *b.state())[3], interiors(g, *a.state())[3])
+    d = L.Domain(cfg)
+    d.upload(*s0)
+    d.step(1)
+    gpu = rel(interiors(g, *d.download())[3], interiors(g, *a.state())[3])
+    print("pressure: 1-ulp floor", floor, "gpu-oracle", gpu)
+    assert floor > 1e-14
+    assert gpu < 10 * max(floor, 1e-13)
+
+
+@pytest.mark.parametrize("case", ["noslip_top", "periodic_z", "stretched_z", "pr_gradient"])
+def test_boundary_and_grid_variants(case):
+    kw = {}
+    if case == "noslip_top":
+        kw = dict(btype=(3, 3, 3, 3, 1, 1))
+    elif case == "periodic_z":
+        kw = dict(btype=(3, 3, 3, 3, 3, 3))
+    elif case == "stretched_z":
+        kw = dict(zW=stretched(24))
+    else:
+        kw = dict(pr_gradient_x=-0.002, pr_gradient_y=0.001)
+    cfg = make_config(32, 24, 24, **kw)
+    g, o, d, _ = pair(cfg)
+    o.step(3)
+    s = d.step(3)
+    e = errs(g, d.download(), o.state())
+    assert max(e[:3]) < 1e-12 and e[3] < 1e-11, (case, e)
+    assert s.max_div < 1e-10
+
+
+def test_golden_fixture_on_gpu():
+    gold = np.load(os.path.join(ROOT, "tests", "golden", "channel_16x12x8.npz"))
+    cfg = make_config(16, 12, 8)
+    g = grid_of(cfg)
+    st = log_profile_state(g, seed=0)
+    assert np.array_equal(st[0], gold["U0"])
+    d = L.Domain(cfg)
+    d.upload(*st)
+    d.project(1.0)
+    d.step(int(gold["steps"]))
+    for a, key in zip(interiors(g, *d.download()), ("U", "V", "W", "P")):
+        assert rel(a, gold[key]) < (1e-11 if key == "P" else 1e-12), key
+
+
+def test_mixed_path_one_step():
+    cfg64 = make_config(64, 64, 32)
+    cfg32 = make_config(64, 64, 32, precision=1)
+    g, o, _, st = pair(cfg64)
+    d = L.Domain(cfg32)
+    d.upload(*st)
+    d.project(1.0)
+    o.step(1)
+    s = d.step(1)
+    e = errs(g, d.download(), o.state())
+    print("mixed errors after 1 step (U, V, W, P):", e, "max div", s.max_div)
+    assert max(e[:3]) < 1e-5, e
+    assert s.max_div < 1e-6
+
+
+def test_batch_equals_single_domains():
+    sizes = [(32, 24, 16), (48, 32, 24), (32, 32, 8)]
+    cfgs = [make_config(*n) for n in sizes]
+    b = L.Batch(cfgs)
+    singles = []
+    for i, c in enumerate(cfgs):
+        g = grid_of(c)
+        st = log_profile_state(g, seed=i)
+        b.upload(i, *st)
+        d = L.Domain(c)
+        d.upload(*st)
+        singles.append(d)
+    b.project(1.0)
+    b.step(2)
+    for i, d in enumerate(singles):
+        d.project(1.0)
+        d.step(2)
+        for x, y in zip(b.download(i), d.download()):
+            assert np.array_equal(x, y)
+    assert b.cells() == sum(a * bb * c for a, bb, c in sizes)
+
+
+def test_async_frame_equals_download():
+    cfg = make_config(32, 24, 16)
+    g, o, d, _ = pair(cfg)
+    d.step(1)
+    d.frame_begin()
+    f = d.frame_wait()
+    for x, y in zip(f, d.download()):
+        assert np.array_equal(x, y)
+    d.frame_begin()
+    d.step(2)  # overlaps the copy; the frame holds the state before these steps
+    o.step(1)
+    f = d.frame_wait()
+    for x, y in zip(interiors(g, *f)[:3], interiors(g, *o.state())[:3]):
+        assert rel(x, y) < 1e-12
+
+
+def test_non_finite_upload_is_refused():
+    cfg = make_config(16, 12, 8)
+    g = grid_of(cfg)
+    U, V, W, P = log_profile_state(g, seed=0)
+    U[5, 5, 5] = np.nan
+    d = L.Domain(cfg)
+    with pytest.raises(L.ElmmError) as e:
+        d.upload(U, V, W, P)
+    assert e.value.code == 3
+
+
+@pytest.mark.parametrize("prec,tol", [(0, 1e-10), (1, 1e-6)])
+def test_full_size_divergence(prec, tol):
+    """256 x 256 x 128: the projected field stays divergence-free in FP64."""
+    cfg = make_config(256, 256, 128, precision=prec)
+    g = grid_of(cfg)
+    d = L.Domain(cfg)
+    d.upload(*log_profile_state(g, seed=0))
+    assert d.project(1.0).max_div < tol
+    s = d.step(3)
+    assert s.max_div < tol and s.nan_detected == 0
+
+
+def test_full_size_mixed_vs_fp64():
+    """256 x 256 x 128, one step: the mixed path against the FP64 path."""
+    g = grid_of(make_config(256, 256, 128))
+    st = log_profile_state(g, seed=0)
+    out = []
+    for prec in (0, 1):
+        d = L.Domain(make_config(256, 256, 128, precision=prec))
+        d.upload(*st)
+        d.project(1.0)
+        d.step(1)
+        out.append(d.download())
+        d.close()
+    e = errs(g, out[1], out[0])
+    print("256x256x128 mixed vs FP64 after 1 step (U, V, W, P):", e)
+    assert max(e[:3]) < 1e-5, e
