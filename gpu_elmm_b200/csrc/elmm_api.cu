@@ -280,10 +280,16 @@ struct BatchT {
     smem_x = sizeof(T2) * 2 * (kRowsX / 2) * maxnx;
     smem_y = sizeof(T2) * 2 * TyOf<T>::v * maxny;
     smem_tri = sizeof(double) * kTriThreads * maxnz * (anyzper ? 2 : 1);
-    CU(cudaFuncSetAttribute(k_fftx_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_x));
-    CU(cudaFuncSetAttribute(k_fftx_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_x));
-    CU(cudaFuncSetAttribute(k_ffty<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_y));
-    CU(cudaFuncSetAttribute(k_tri<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_tri));
+    // the opt-in maximum, so that handles of different sizes never lower the
+    // limit under each other's launches
+    int optin = 0;
+    CU(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    if (smem_x > (size_t)optin || smem_y > (size_t)optin || smem_tri > (size_t)optin)
+      return fail(ELMM_ERR_INVALID_CONFIG, "grid too large for the shared-memory transforms");
+    CU(cudaFuncSetAttribute(k_fftx_fwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    CU(cudaFuncSetAttribute(k_fftx_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    CU(cudaFuncSetAttribute(k_ffty<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    CU(cudaFuncSetAttribute(k_tri<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     int nsm = 0;
     CU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
     auto cap = [&](const void *f, int threads, size_t sm) {
@@ -298,7 +304,7 @@ struct BatchT {
     grid_cap[4] = cap((const void *)k_tri<T>, kTriThreads, smem_tri);
     grid_cap[5] = cap((const void *)k_fftx_inv<T>, kFFTThreads, smem_x);
     grid_cap[6] = cap((const void *)k_project<T>, MX * MY, 0);
-    grid_cap[7] = cap((const void *)k_divmax<T>, TX * TY, 0);
+    grid_cap[7] = cap((const void *)k_divres<T>, TX * TY, 0);
     grid_cap[8] = cap((const void *)k_cfl<T>, TX * TY, 0);
     // staging for host-layout copies
     stage_elems = 0;
@@ -413,6 +419,18 @@ struct BatchT {
     if ((r = upload_table(&h.zW, g.zW))) return r;
     if ((r = upload_table(&h.dzW, g.dzW))) return r;
     if ((r = upload_table(&h.width, g.width))) return r;
+    {
+      std::vector<double> rdz(h.nz + 1, 0.0), r2zz(h.nz + 1, 0.0), wc2(h.nz + 1, 0.0);
+      for (int k = 1; k <= h.nz; k++) {
+        rdz[k] = 1.0 / g.dzPr[k + 2];
+        r2zz[k] = 1.0 / (2 * (g.zPr[k + 1 + 2] - g.zPr[k - 1 + 2]));
+        double wc = g.width[k] * c.C_Smagorinsky;
+        wc2[k] = wc * wc;
+      }
+      if ((r = upload_table(&h.sgs_rdz, rdz))) return r;
+      if ((r = upload_table(&h.sgs_r2zz, r2zz))) return r;
+      if ((r = upload_table(&h.sgs_wc2, wc2))) return r;
+    }
     // wall-model planes
     for (int s = 0; s < 6; s++) h.z0[s] = c.z0[s];
     for (int comp = 0; comp < 3; comp++)
@@ -434,6 +452,10 @@ struct BatchT {
     if ((r = dalloc((void **)&h.maxdiv_bits, sizeof(unsigned long long)))) return r;
     if ((r = dalloc((void **)&h.cfl_bits, sizeof(unsigned long long)))) return r;
     if ((r = dalloc((void **)&h.flags, 4 * sizeof(int)))) return r;
+    if ((r = dalloc((void **)&h.refine_flag, sizeof(int)))) return r;
+    if ((r = dalloc((void **)&h.refine_count, 2 * sizeof(int)))) return r;
+    h.refine_tol = c.refine_tol;
+    h.max_refine = c.max_refine_sweeps;
     size_t pe = (size_t)(h.nx + 4) * (h.ny + 4) * (h.nz + 4);
     if ((r = dalloc((void **)&pr_image[di], pe * sizeof(double)))) return r;
     // viscosity starts at the molecular value (src/initial.f90:4275)
@@ -460,16 +482,44 @@ struct BatchT {
   // PressureCorrection on U2 (in_place = 0) or on U itself (initial projection)
   int launch_projection(double coef_alpha2, int use_dt, int in_place) {
     nlaunch += 7;
-    k_fftx_fwd<T><<<gsz(2, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan, coef_alpha2,
-                                                                        use_dt, nullptr);
-    k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), kFFTThreads, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, 0);
-    k_tri<T><<<gsz(4, ls[LK_TRI].total), kTriThreads, smem_tri, stream>>>(ddom, ls[LK_TRI].l());
-    k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), kFFTThreads, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, 1);
-    k_fftx_inv<T><<<gsz(5, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan);
+    launch_poisson(coef_alpha2, use_dt, 0, 0);
     k_project<T><<<gsz(6, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l(), coef_alpha2, use_dt,
-                                                                     in_place);
-    k_prref<T><<<std::min(nd, 1024), 256, 0, stream>>>(ddom, nd);
+                                                                   in_place, 0);
+    k_prref<T><<<std::min(nd, 1024), 256, 0, stream>>>(ddom, nd, 0);
     return ELMM_OK;
+  }
+  // the five transform kernels; rhs_from_phi: the right-hand side is in Phi
+  void launch_poisson(double coef_alpha2, int use_dt, int rhs_from_phi, int gate) {
+    k_fftx_fwd<T><<<gsz(2, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan, coef_alpha2,
+                                                                                use_dt, rhs_from_phi, gate);
+    k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), kFFTThreads, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, 0, gate);
+    k_tri<T><<<gsz(4, ls[LK_TRI].total), kTriThreads, smem_tri, stream>>>(ddom, ls[LK_TRI].l(), gate);
+    k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), kFFTThreads, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, 1, gate);
+    k_fftx_inv<T><<<gsz(5, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan, gate);
+  }
+  int max_refine() const {
+    int m = 0;
+    for (auto &c : cfg) m = std::max(m, c.max_refine_sweeps);
+    return m;
+  }
+  // Defect correction after a projection (mixed path): FP64 divergence
+  // residual -> correction solve -> velocity / pressure update, at most
+  // max_refine_sweeps times; the kernels of a sweep return at once for a
+  // domain that does not need it, so the sweep stays inside the step graph.
+  void launch_refine(double coef_alpha2, int use_dt) {
+    const int R = max_refine();
+    if (R == 0) return;
+    for (int d = 0; d < nd; d++) cudaMemsetAsync(hdom[d].maxdiv_bits, 0, sizeof(unsigned long long), stream);
+    k_divres<T><<<gsz(7, ls[LK_CELLS].total), TX * TY, 0, stream>>>(ddom, ls[LK_CELLS].l(), 0);
+    nlaunch++;
+    for (int sw = 0; sw < R; sw++) {
+      k_refine_decide<T><<<(nd + 127) / 128, 128, 0, stream>>>(ddom, nd, sw == 0);
+      launch_poisson(coef_alpha2, use_dt, 1, 1);
+      k_project<T><<<gsz(6, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l(), coef_alpha2, use_dt, 1, 1);
+      k_prref<T><<<std::min(nd, 1024), 256, 0, stream>>>(ddom, nd, 1);
+      k_divres<T><<<gsz(7, ls[LK_CELLS].total), TX * TY, 0, stream>>>(ddom, ls[LK_CELLS].l(), 1);
+      nlaunch += 10;
+    }
   }
   int launch_divmax() {
     nlaunch++;
@@ -493,6 +543,7 @@ struct BatchT {
     launch_momentum(stage);
     if (stop == 2) return ELMM_OK;
     launch_projection(2 * kAlpha[stage - 1], 1, 0);
+    launch_refine(2 * kAlpha[stage - 1], 1);
     return ELMM_OK;
   }
   int enqueue_step(bool cfl, bool div) {
@@ -520,6 +571,7 @@ struct BatchT {
       if (e != cudaSuccess) return fail(ELMM_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
       step_has_cfl = cfl;
     }
+    for (int d = 0; d < nd; d++) CU(cudaMemsetAsync(hdom[d].refine_count, 0, sizeof(int), stream));
     CU(cudaEventRecord(t0, stream));
     for (int s = 0; s < nsteps; s++) CU(cudaGraphLaunch(step_exec, stream));
     CU(cudaEventRecord(t1, stream));
@@ -527,7 +579,16 @@ struct BatchT {
     CU(cudaGetLastError());
     time += nsteps * cfg[0].dt;
     int r = fill_stats(st, nsteps);
-    if (st) st->kernels = nsteps * step_kernels;
+    if (st) {
+      st->kernels = nsteps * step_kernels;
+      int tot = 0;
+      for (int d = 0; d < nd; d++) {
+        int c0 = 0;
+        CU(cudaMemcpy(&c0, hdom[d].refine_count, sizeof(int), cudaMemcpyDeviceToHost));
+        tot = std::max(tot, c0);
+      }
+      st->refine_sweeps = tot;
+    }
     return r;
   }
 
@@ -572,6 +633,7 @@ struct BatchT {
       CU(cudaMemcpyAsync(hdom[d].W2, hdom[d].W, box, cudaMemcpyDeviceToDevice, stream));
     }
     launch_projection(coef, 0, 0);
+    launch_refine(coef, 0);
     launch_divmax();
     CU(cudaEventRecord(t1, stream));
     CU(cudaStreamSynchronize(stream));
@@ -595,19 +657,19 @@ struct BatchT {
       CU(cudaEventRecord(ev[q++], stream));
       k_momentum<T><<<gsz(1, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l(), sc);
       CU(cudaEventRecord(ev[q++], stream));
-      k_fftx_fwd<T><<<gsz(2, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan, a2, 1, nullptr);
+      k_fftx_fwd<T><<<gsz(2, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan, a2, 1, 0, 0);
       CU(cudaEventRecord(ev[q++], stream));
-      k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), kFFTThreads, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, 0);
+      k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), kFFTThreads, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, 0, 0);
       CU(cudaEventRecord(ev[q++], stream));
-      k_tri<T><<<gsz(4, ls[LK_TRI].total), kTriThreads, smem_tri, stream>>>(ddom, ls[LK_TRI].l());
+      k_tri<T><<<gsz(4, ls[LK_TRI].total), kTriThreads, smem_tri, stream>>>(ddom, ls[LK_TRI].l(), 0);
       CU(cudaEventRecord(ev[q++], stream));
-      k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), kFFTThreads, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, 1);
+      k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), kFFTThreads, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, 1, 0);
       CU(cudaEventRecord(ev[q++], stream));
-      k_fftx_inv<T><<<gsz(5, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan);
+      k_fftx_inv<T><<<gsz(5, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan, 0);
       CU(cudaEventRecord(ev[q++], stream));
-      k_project<T><<<gsz(6, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l(), a2, 1, 0);
+      k_project<T><<<gsz(6, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l(), a2, 1, 0, 0);
       CU(cudaEventRecord(ev[q++], stream));
-      k_prref<T><<<std::min(nd, 1024), 256, 0, stream>>>(ddom, nd);
+      k_prref<T><<<std::min(nd, 1024), 256, 0, stream>>>(ddom, nd, 0);
       CU(cudaEventRecord(ev[q++], stream));
       CU(cudaStreamSynchronize(stream));
       CU(cudaGetLastError());
@@ -824,12 +886,7 @@ static int poisson_exec(BatchT<T> &B, double *Phi, const double *RHS) {
   CU(cudaMemcpyAsync(B.dstage, RHS, n * sizeof(double), cudaMemcpyHostToDevice, B.stream));
   CU(cudaMemsetAsync(B.dbad, 0, sizeof(int), B.stream));
   k_unpack<T><<<256, 256, 0, B.stream>>>(B.ddom, h.Phi, B.dstage, hb, h.nx, h.ny, h.nz, B.dbad);
-  k_fftx_fwd<T><<<B.gsz(2, B.ls[LK_ROWS].total), kFFTThreads, B.smem_x, B.stream>>>(
-      B.ddom, B.ls[LK_ROWS].l(), B.dplan, 1.0, 0, h.Phi);
-  k_ffty<T><<<B.gsz(3, B.ls[LK_YCOLS].total), kFFTThreads, B.smem_y, B.stream>>>(B.ddom, B.ls[LK_YCOLS].l(), B.dplan, 0);
-  k_tri<T><<<B.gsz(4, B.ls[LK_TRI].total), kTriThreads, B.smem_tri, B.stream>>>(B.ddom, B.ls[LK_TRI].l());
-  k_ffty<T><<<B.gsz(3, B.ls[LK_YCOLS].total), kFFTThreads, B.smem_y, B.stream>>>(B.ddom, B.ls[LK_YCOLS].l(), B.dplan, 1);
-  k_fftx_inv<T><<<B.gsz(5, B.ls[LK_ROWS].total), kFFTThreads, B.smem_x, B.stream>>>(B.ddom, B.ls[LK_ROWS].l(), B.dplan);
+  B.launch_poisson(1.0, 0, 1, 0);
   HostBox hp = B.hbox_p(0);
   size_t np = (size_t)hp.n0 * hp.n1 * hp.n2;
   CU(cudaMemcpyAsync(B.dstage, Phi, np * sizeof(double), cudaMemcpyHostToDevice, B.stream));

@@ -70,6 +70,8 @@ struct Dom {
   // grid tables (FP64), index k + 2 for k in [-2, nz + 3]
   const double *zPr, *dzPr, *zW, *dzW;
   const double *width;   // Smagorinsky filter width per k, index k (1..nz)
+  // per-k factors of NuSmag (index k, 1..nz): 1/dzPr(k), 1/(2 (zPr(k+1)-zPr(k-1))), (width Cs)^2
+  const double *sgs_rdz, *sgs_r2zz, *sgs_wc2;
   // wall model: per face plane fluxp/fluxm/ustar, plane dims from ext[]
   T *wm_fluxp[kFaces], *wm_fluxm[kFaces];
   double *wm_ustar[kFaces];
@@ -82,6 +84,11 @@ struct Dom {
   unsigned long long *maxdiv_bits;  // max |div u| as the bits of a positive double
   unsigned long long *cfl_bits;
   int *flags;            // [0]: NaN seen
+  // defect correction of the mixed path
+  int *refine_flag;      // 1: the next correction sweep runs for this domain
+  int *refine_count;     // sweeps run since the counter was reset
+  double refine_tol;
+  int max_refine;
 };
 
 template <typename T>
@@ -206,6 +213,9 @@ __device__ __forceinline__ void push_ghosts(const Dom<T> &d, T *F, const Images 
 
 template <typename T>
 __device__ __forceinline__ void push_vel(const Dom<T> &d, T *F, int comp, int i, int j, int k, T v) {
+  // cells off every face of the box have no ghost images (the extents of a
+  // component are nx-1..nx etc., so i in [2, nx-2] is interior for all)
+  if (i > 1 && i < d.nx - 1 && j > 1 && j < d.ny - 1 && k > 1 && k < d.nz - 1) return;
   const int *e = d.ext[comp];
   if (i != 1 && i != e[0] && j != 1 && j != e[1] && k != 1 && k != e[2]) return;
   Images ix = images_vel(i, e[0], d.bt[0], d.bt[1], comp == 0);

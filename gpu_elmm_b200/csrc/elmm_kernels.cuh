@@ -190,13 +190,14 @@ constexpr int kFFTThreads = 256;
 template <typename T>
 __global__ void __launch_bounds__(kFFTThreads) k_fftx_fwd(const Dom<T> *__restrict__ doms, Launch L,
                                                   const PoisPlan *__restrict__ plans, double coef_alpha2,
-                                                  int use_dt, const T *rhs_direct) {
+                                                  int use_dt, int rhs_from_phi, int gate) {
   typedef typename Vec2<T>::type T2;
   extern __shared__ unsigned char smem_raw[];
   T2 *buf0 = reinterpret_cast<T2 *>(smem_raw);
   for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
     const int di = find_dom(L.starts, L.nd, t);
     const Dom<T> &d = doms[di];
+    if (gate && !*d.refine_flag) continue;  // defect-correction sweep not needed
     const PoisPlan &pl = plans[di];
     const int N = d.nx;
     const int ntr = kRowsX / 2;
@@ -207,7 +208,7 @@ __global__ void __launch_bounds__(kFFTThreads) k_fftx_fwd(const Dom<T> *__restri
     const double coef = use_dt ? coef_alpha2 * d.dt : coef_alpha2;
     const T rdt2 = (T)(1.0 / coef);
     const T *U2 = d.U2, *V2 = d.V2, *W2 = d.W2;
-    const T dx = (T)d.dx, dy = (T)d.dy, dz = (T)d.dz;
+    const T rdx = (T)(1.0 / d.dx), rdy = (T)(1.0 / d.dy), rdz = (T)(1.0 / d.dz);
 #pragma unroll 4
     for (int w = threadIdx.x; w < kRowsX * N; w += blockDim.x) {
       const int r = w / N, i = w - r * N + 1;
@@ -216,12 +217,12 @@ __global__ void __launch_bounds__(kFFTThreads) k_fftx_fwd(const Dom<T> *__restri
       if (row < nrows) {
         const int j = row % d.ny + 1, k = row / d.ny + 1;
         const long long c = bidx(d, i, j, k);
-        if (rhs_direct) {  // PoisSolver interface: the RHS is given
-          rhs = ld(rhs_direct, c);
+        if (rhs_from_phi) {  // the RHS was put in Phi (PoisSolver interface, defect correction)
+          rhs = ld((const T *)d.Phi, c) * rdt2;
         } else {
-          const T dzk = d.vz ? (T)d.dzPr[k + 2] : dz;
-          T div = (ld(U2, c) - ld(U2, c - 1)) / dx + (ld(V2, c) - ld(V2, c - d.pitch)) / dy +
-                  (ld(W2, c) - ld(W2, c - d.plane)) / dzk - (T)0;
+          const T rdzk = d.vz ? (T)d.sgs_rdz[k] : rdz;
+          T div = (ld(U2, c) - ld(U2, c - 1)) * rdx + (ld(V2, c) - ld(V2, c - d.pitch)) * rdy +
+                  (ld(W2, c) - ld(W2, c - d.plane)) * rdzk - (T)0;
           rhs = div * rdt2;
         }
       }
@@ -257,7 +258,7 @@ template <> struct TyOf<float> { static constexpr int v = 16; };
 
 template <typename T>
 __global__ void __launch_bounds__(kFFTThreads) k_ffty(const Dom<T> *__restrict__ doms, Launch L,
-                                              const PoisPlan *__restrict__ plans, int inverse) {
+                                              const PoisPlan *__restrict__ plans, int inverse, int gate) {
   typedef typename Vec2<T>::type T2;
   constexpr int C = TyOf<T>::v;
   extern __shared__ unsigned char smem_raw[];
@@ -265,6 +266,7 @@ __global__ void __launch_bounds__(kFFTThreads) k_ffty(const Dom<T> *__restrict__
   for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
     const int di = find_dom(L.starts, L.nd, t);
     const Dom<T> &d = doms[di];
+    if (gate && !*d.refine_flag) continue;  // defect-correction sweep not needed
     const PoisPlan &pl = plans[di];
     const int N = d.ny;
     T2 *buf1 = buf0 + C * N;
@@ -299,12 +301,13 @@ __global__ void __launch_bounds__(kFFTThreads) k_ffty(const Dom<T> *__restrict__
 constexpr int kTriThreads = 64;
 
 template <typename T>
-__global__ void __launch_bounds__(kTriThreads) k_tri(const Dom<T> *__restrict__ doms, Launch L) {
+__global__ void __launch_bounds__(kTriThreads) k_tri(const Dom<T> *__restrict__ doms, Launch L, int gate) {
   typedef typename Vec2<T>::type T2;
   extern __shared__ double cps[];  // [nz][kTriThreads]
   for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
     const int di = find_dom(L.starts, L.nd, t);
     const Dom<T> &d = doms[di];
+    if (gate && !*d.refine_flag) continue;  // defect-correction sweep not needed
     const int lt = t - __ldg(L.starts + di);
     const int col = lt * kTriThreads + threadIdx.x;
     const int ky = col / d.spitch, kx = col - ky * d.spitch;

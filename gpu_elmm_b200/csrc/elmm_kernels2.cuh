@@ -10,13 +10,14 @@ namespace elmm {
 // (Bound_Phi, src/boundaries.f90:1817-1948, one cell deep).
 template <typename T>
 __global__ void __launch_bounds__(kFFTThreads) k_fftx_inv(const Dom<T> *__restrict__ doms, Launch L,
-                                                  const PoisPlan *__restrict__ plans) {
+                                                  const PoisPlan *__restrict__ plans, int gate) {
   typedef typename Vec2<T>::type T2;
   extern __shared__ unsigned char smem_raw[];
   T2 *buf0 = reinterpret_cast<T2 *>(smem_raw);
   for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
     const int di = find_dom(L.starts, L.nd, t);
     const Dom<T> &d = doms[di];
+    if (gate && !*d.refine_flag) continue;
     const PoisPlan &pl = plans[di];
     const int N = d.nx, nxh = d.nxh;
     const int ntr = kRowsX / 2;
@@ -70,11 +71,12 @@ __global__ void __launch_bounds__(kFFTThreads) k_fftx_inv(const Dom<T> *__restri
 // flight while plane k is written, and Phi(k+1) of plane k is Phi of k+1.
 template <typename T>
 __global__ void __launch_bounds__(MX *MY) k_project(const Dom<T> *__restrict__ doms, Launch L, double coef_alpha2,
-                                                    int use_dt, int in_place) {
+                                                    int use_dt, int in_place, int gate) {
   __shared__ double red[MX * MY / 32];
   for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
     const int di = find_dom(L.starts, L.nd, t);
     const Dom<T> &d = doms[di];
+    if (gate && !*d.refine_flag) continue;
     int lt = t - __ldg(L.starts + di);
     const int ntx = (d.nx + MX - 1) / MX, nty = (d.ny + MY - 1) / MY;
     const int bx = lt % ntx; lt /= ntx;
@@ -167,10 +169,11 @@ __global__ void __launch_bounds__(MX *MY) k_project(const Dom<T> *__restrict__ d
 // the new reference is the mean of the top layer; it is applied lazily,
 // every reader of P subtracts it.
 template <typename T>
-__global__ void k_prref(const Dom<T> *__restrict__ doms, int nd) {
+__global__ void k_prref(const Dom<T> *__restrict__ doms, int nd, int gate) {
   __shared__ double red[32];
   for (int di = blockIdx.x; di < nd; di += gridDim.x) {
     const Dom<T> &d = doms[di];
+    if (gate && !*d.refine_flag) continue;
     double s = 0;
     for (int p = threadIdx.x; p < d.nprpart; p += blockDim.x) s += d.prpart[p];
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
@@ -218,6 +221,71 @@ __global__ void __launch_bounds__(TX *TY) k_divmax(const Dom<T> *__restrict__ do
       atomic_max_pos(d.maxdiv_bits, m);
     }
     __syncthreads();
+  }
+}
+
+
+// Defect correction of the mixed path: the divergence residual of the
+// FP32 velocity field evaluated in FP64 (the discrete divergence of
+// src/pressure.f90:688-717), stored as the right-hand side of a correction
+// solve, and its maximum.  gate: run only for domains whose flag is set.
+template <typename T>
+__global__ void __launch_bounds__(TX *TY) k_divres(const Dom<T> *__restrict__ doms, Launch L, int gate) {
+  __shared__ double red[TX * TY / 32];
+  for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
+    const int di = find_dom(L.starts, L.nd, t);
+    const Dom<T> &d = doms[di];
+    if (gate && !*d.refine_flag) continue;
+    int lt = t - __ldg(L.starts + di);
+    const int ntx = (d.nx + TX - 1) / TX, nty = (d.ny + TY - 1) / TY;
+    const int tx = lt % ntx; lt /= ntx;
+    const int ty = lt % nty;
+    const int k = lt / nty + 1;
+    const int i = tx * TX + (threadIdx.x % TX) + 1;
+    const int j = ty * TY + (threadIdx.x / TX) + 1;
+    double a = 0;
+    if (i <= d.nx && j <= d.ny) {
+      const long long c = bidx(d, i, j, k);
+      const double dzk = d.vz ? d.dzPr[k + 2] : d.dz;
+      double p = ((double)ld(d.U, c) - (double)ld(d.U, c - 1)) / d.dx +
+                 ((double)ld(d.V, c) - (double)ld(d.V, c - d.pitch)) / d.dy +
+                 ((double)ld(d.W, c) - (double)ld(d.W, c - d.plane)) / dzk;
+      d.Phi[c] = (T)p;
+      a = fabs(p);
+      if (!(a == a)) a = __longlong_as_double(0x7ff8000000000000ULL);
+    }
+    for (int o = 16; o > 0; o >>= 1) a = fmax(a, __shfl_down_sync(0xffffffffu, a, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double m = 0;
+      for (int w = 0; w < TX * TY / 32; w++) m = fmax(m, red[w]);
+      atomic_max_pos(d.maxdiv_bits, m);
+    }
+    __syncthreads();
+  }
+}
+
+// Whether another correction sweep runs: max |div u| above the tolerance
+// and fewer than max_refine sweeps in this stage.  first: a new stage.
+template <typename T>
+__global__ void k_refine_decide(const Dom<T> *__restrict__ doms, int nd, int first) {
+  for (int di = blockIdx.x * blockDim.x + threadIdx.x; di < nd; di += gridDim.x * blockDim.x) {
+    const Dom<T> &d = doms[di];
+    if (first) *d.refine_flag = 1;  // the residual of the first decision is always current
+    if (!*d.refine_flag) continue;
+    unsigned long long b = *d.maxdiv_bits;
+    double md = __longlong_as_double((long long)b);
+    int sweeps = first ? 0 : d.refine_count[1];
+    int go = (md > d.refine_tol) && sweeps < d.max_refine;
+    *d.refine_flag = go;
+    if (go) {
+      d.refine_count[0] += 1;      // total sweeps since the host reset the counter
+      d.refine_count[1] = sweeps + 1;
+      *d.maxdiv_bits = 0ULL;       // the sweep ends with a new residual
+    } else if (first) {
+      d.refine_count[1] = 0;
+    }
   }
 }
 

@@ -32,15 +32,38 @@ struct Ring {
   __device__ __forceinline__ T g(int f, int dx, int dy, int dz) const { return p[dz + 1][f * MPS + o + dy * MPW + dx]; }
 };
 
+// per-tile context in shared memory: everything the stencil code reads
+// besides the fields, so that no descriptor load sits on its critical path
 template <typename T>
-struct MomTabs {
+struct MomCtx {
   T cA[3], cB[3][3], rec2[3];
+  int wallmask;  // bit s: wall-model fluxes on side s
+  int vz;
+  int ext[3][3];
+  const double *dzPr, *dzW, *zPr, *zW;
+  const T *fluxp[kFaces], *fluxm[kFaces];
 };
+
+template <typename T>
+__device__ __forceinline__ void fill_ctx(MomCtx<T> &m, const Dom<T> &d) {
+  // called by one thread
+  for (int a = 0; a < 3; a++) {
+    m.cA[a] = (T)d.cA[a];
+    m.rec2[a] = (T)d.rec2[a];
+    for (int c = 0; c < 3; c++) { m.cB[c][a] = (T)d.cB[c][a]; m.ext[c][a] = d.ext[c][a]; }
+  }
+  int wm = 0;
+  for (int f = 0; f < 6; f++) wm |= d.wall[f] ? (1 << f) : 0;
+  m.wallmask = wm;
+  m.vz = d.vz;
+  m.dzPr = d.dzPr; m.dzW = d.dzW; m.zPr = d.zPr; m.zW = d.zW;
+  for (int f = 0; f < kFaces; f++) { m.fluxp[f] = d.wm_fluxp[f]; m.fluxm[f] = d.wm_fluxm[f]; }
+}
 
 // one velocity component's tendency at (i,j,k): advection + diffusion +
 // wall corrections, in the reference's order of operations
 template <typename T, int C>
-__device__ __forceinline__ T tendency(const Dom<T> &d, const MomTabs<T> &m, const Ring<T> &R, int i, int j, int k) {
+__device__ __forceinline__ T tendency(const MomCtx<T> &m, const Ring<T> &R, int i, int j, int k) {
   // X(dx,dy,dz) with the component's own axis first: along = C, a1, a2 the others
 #define FU(dx, dy, dz) R.g(0, dx, dy, dz)
 #define FV(dx, dy, dz) R.g(1, dx, dy, dz)
@@ -55,7 +78,7 @@ __device__ __forceinline__ T tendency(const Dom<T> &d, const MomTabs<T> &m, cons
     const T w = FW(0, 0, 0), we = FW(1, 0, 0), wb = FW(0, 0, -1), wbe = FW(1, 0, -1);
     const T Ax = m.cA[0], Ay = m.cA[1];
     const T Bx = m.cB[0][0], By = m.cB[0][1];
-    if (!d.vz) {
+    if (!m.vz) {
       const T Az = m.cA[2], Bz = m.cB[0][2];
       a = -((Ax * (ue + u) * (ue + u) - Ax * (u + uw) * (u + uw)) + (Ay * (un + u) * (ve + v) - Ay * (u + us) * (vse + vs)) +
             (Az * (ut + u) * (we + w) - Az * (u + ub) * (wbe + wb)));
@@ -63,12 +86,12 @@ __device__ __forceinline__ T tendency(const Dom<T> &d, const MomTabs<T> &m, cons
       T Wadv = (w + we + wb + wbe);
       a = a - (Bx * (ue - uw) * u + By * (un - us) * Vadv + Bz * (ut - ub) * Wadv);
     } else {
-      const T dzp = (T)d.dzPr[k + 2];
+      const T dzp = (T)m.dzPr[k + 2];
       a = -((Ax * (ue + u) * (ue + u) - Ax * (u + uw) * (u + uw)) + (Ay * (un + u) * (ve + v) - Ay * (u + us) * (vse + vs)) +
             ((ut + u) * (we + w) - (u + ub) * (wbe + wb)) / dzp / 4);
       T Vadv = (v + ve + vs + vse);
       T Wadv = (w + we + wb + wbe) / 4;
-      a = a - (Bx * (ue - uw) * u + By * (un - us) * Vadv + (ut - ub) / (T)(d.zPr[k + 1 + 2] - d.zPr[k - 1 + 2]) * Wadv);
+      a = a - (Bx * (ue - uw) * u + By * (un - us) * Vadv + (ut - ub) / (T)(m.zPr[k + 1 + 2] - m.zPr[k - 1 + 2]) * Wadv);
     }
     a = a * (T)0.5;
     const T n0 = FN(0, 0, 0), ne = FN(1, 0, 0), nn = FN(0, 1, 0), nne = FN(1, 1, 0), ns = FN(0, -1, 0), nse = FN(1, -1, 0);
@@ -77,49 +100,49 @@ __device__ __forceinline__ T tendency(const Dom<T> &d, const MomTabs<T> &m, cons
     a = a - n0 * (u - uw) * rx;
     a = a + (T)0.25 * (nne + ne + nn + n0) * (un - u) * ry;
     a = a - (T)0.25 * (ne + nse + n0 + ns) * (u - us) * ry;
-    if (!d.vz) {
+    if (!m.vz) {
       a = a + (T)0.25 * (nte + ne + nt + n0) * (ut - u) * rz;
       a = a - (T)0.25 * (ne + nbe + n0 + nb) * (u - ub) * rz;
     } else {
-      T tz = (T)0.25 * (nte + ne + nt + n0) * (ut - u) / (T)d.dzW[k + 2];
-      tz = tz - (T)0.25 * (ne + nbe + n0 + nb) * (u - ub) / (T)d.dzW[k - 1 + 2];
-      tz = tz / (T)d.dzPr[k + 2];
+      T tz = (T)0.25 * (nte + ne + nt + n0) * (ut - u) / (T)m.dzW[k + 2];
+      tz = tz - (T)0.25 * (ne + nbe + n0 + nb) * (u - ub) / (T)m.dzW[k - 1 + 2];
+      tz = tz / (T)m.dzPr[k + 2];
       a = a + tz;
     }
-    const int *e = d.ext[0];
-    if (d.wall[SIDE_WE] && i == 1) {
+    const int *e = m.ext[0];
+    if ((m.wallmask & (1 << SIDE_WE)) && i == 1) {
       long long p = (long long)(j - 1) + (long long)e[1] * (k - 1);
       a = a + n0 * (u - uw) * rx;
-      a = a + d.wm_fluxp[0 * 6 + SIDE_WE][p];
+      a = a + m.fluxp[0 * 6 + SIDE_WE][p];
     }
-    if (d.wall[SIDE_EA] && i == e[0]) {
+    if ((m.wallmask & (1 << SIDE_EA)) && i == e[0]) {
       long long p = (long long)(j - 1) + (long long)e[1] * (k - 1);
       a = a - ne * (ue - u) * rx;
-      a = a - d.wm_fluxm[0 * 6 + SIDE_EA][p];
+      a = a - m.fluxm[0 * 6 + SIDE_EA][p];
     }
-    if (d.wall[SIDE_SO] && j == 1) {
+    if ((m.wallmask & (1 << SIDE_SO)) && j == 1) {
       long long p = (long long)(i - 1) + (long long)e[0] * (k - 1);
       a = a + (ne + nse + n0 + ns) * (u - us) * ry / 4;
-      a = a + d.wm_fluxp[0 * 6 + SIDE_SO][p];
+      a = a + m.fluxp[0 * 6 + SIDE_SO][p];
     }
-    if (d.wall[SIDE_NO] && j == e[1]) {
+    if ((m.wallmask & (1 << SIDE_NO)) && j == e[1]) {
       long long p = (long long)(i - 1) + (long long)e[0] * (k - 1);
       a = a - (nne + ne + nn + n0) * (un - u) * ry / 4;
-      a = a - d.wm_fluxm[0 * 6 + SIDE_NO][p];
+      a = a - m.fluxm[0 * 6 + SIDE_NO][p];
     }
-    if (d.wall[SIDE_BO] && k == 1) {
+    if ((m.wallmask & (1 << SIDE_BO)) && k == 1) {
       long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
       T s = ne + nbe + n0 + nb;
-      if (d.vz) a = a + s * (u - ub) / (T)d.dzW[k - 1 + 2] / 4 / (T)d.dzPr[k + 2];
+      if (m.vz) a = a + s * (u - ub) / (T)m.dzW[k - 1 + 2] / 4 / (T)m.dzPr[k + 2];
       else a = a + s * (u - ub) * rz / 4;
-      a = a + d.wm_fluxp[0 * 6 + SIDE_BO][p];
+      a = a + m.fluxp[0 * 6 + SIDE_BO][p];
     }
-    if (d.wall[SIDE_TO] && k == e[2]) {
+    if ((m.wallmask & (1 << SIDE_TO)) && k == e[2]) {
       long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
       T s = nte + ne + nt + n0;
-      if (d.vz) a = a - s * (ut - u) / (T)d.dzW[k + 2] / 4 / (T)d.dzPr[k + 2];
+      if (m.vz) a = a - s * (ut - u) / (T)m.dzW[k + 2] / 4 / (T)m.dzPr[k + 2];
       else a = a - s * (ut - u) * rz / 4;
-      a = a - d.wm_fluxm[0 * 6 + SIDE_TO][p];
+      a = a - m.fluxm[0 * 6 + SIDE_TO][p];
     }
   } else if (C == 1) {
     const T v = FV(0, 0, 0), ve = FV(1, 0, 0), vw = FV(-1, 0, 0), vn = FV(0, 1, 0), vs = FV(0, -1, 0);
@@ -128,7 +151,7 @@ __device__ __forceinline__ T tendency(const Dom<T> &d, const MomTabs<T> &m, cons
     const T w = FW(0, 0, 0), wn = FW(0, 1, 0), wb = FW(0, 0, -1), wbn = FW(0, 1, -1);
     const T Ax = m.cA[0], Ay = m.cA[1];
     const T Bx = m.cB[1][0], By = m.cB[1][1];
-    if (!d.vz) {
+    if (!m.vz) {
       const T Az = m.cA[2], Bz = m.cB[1][2];
       a = -((Ay * (vn + v) * (vn + v) - Ay * (v + vs) * (v + vs)) + (Ax * (ve + v) * (un + u) - Ax * (v + vw) * (unw + uw)) +
             (Az * (vt + v) * (wn + w) - Az * (v + vb) * (wbn + wb)));
@@ -136,12 +159,12 @@ __device__ __forceinline__ T tendency(const Dom<T> &d, const MomTabs<T> &m, cons
       T Wadv = (w + wn + wb + wbn);
       a = a - (Bx * (ve - vw) * Uadv + By * (vn - vs) * v + Bz * (vt - vb) * Wadv);
     } else {
-      const T dzp = (T)d.dzPr[k + 2];
+      const T dzp = (T)m.dzPr[k + 2];
       a = -((Ay * (vn + v) * (vn + v) - Ay * (v + vs) * (v + vs)) + (Ax * (ve + v) * (un + u) - Ax * (v + vw) * (unw + uw)) +
             ((vt + v) * (wn + w) - (v + vb) * (wbn + wb)) / dzp / 4);
       T Uadv = (u + un + uw + unw);
       T Wadv = (w + wn + wb + wbn) / 4;
-      a = a - (Bx * (ve - vw) * Uadv + By * (vn - vs) * v + (vt - vb) / (T)(d.zPr[k + 1 + 2] - d.zPr[k - 1 + 2]) * Wadv);
+      a = a - (Bx * (ve - vw) * Uadv + By * (vn - vs) * v + (vt - vb) / (T)(m.zPr[k + 1 + 2] - m.zPr[k - 1 + 2]) * Wadv);
     }
     a = a * (T)0.5;
     const T n0 = FN(0, 0, 0), ne = FN(1, 0, 0), nn = FN(0, 1, 0), nne = FN(1, 1, 0), nw = FN(-1, 0, 0), nnw = FN(-1, 1, 0);
@@ -150,49 +173,49 @@ __device__ __forceinline__ T tendency(const Dom<T> &d, const MomTabs<T> &m, cons
     a = a - (T)0.25 * (nn + n0 + nnw + nw) * (v - vw) * rx;
     a = a + nn * (vn - v) * ry;
     a = a - n0 * (v - vs) * ry;
-    if (!d.vz) {
+    if (!m.vz) {
       a = a + (T)0.25 * (nnt + nn + nt + n0) * (vt - v) * rz;
       a = a - (T)0.25 * (nn + nnb + n0 + nb) * (v - vb) * rz;
     } else {
-      T tz = (T)0.25 * (nnt + nn + nt + n0) * (vt - v) / (T)d.dzW[k + 2];
-      tz = tz - (T)0.25 * (nn + nnb + n0 + nb) * (v - vb) / (T)d.dzW[k - 1 + 2];
-      tz = tz / (T)d.dzPr[k + 2];
+      T tz = (T)0.25 * (nnt + nn + nt + n0) * (vt - v) / (T)m.dzW[k + 2];
+      tz = tz - (T)0.25 * (nn + nnb + n0 + nb) * (v - vb) / (T)m.dzW[k - 1 + 2];
+      tz = tz / (T)m.dzPr[k + 2];
       a = a + tz;
     }
-    const int *e = d.ext[1];
-    if (d.wall[SIDE_WE] && i == 1) {
+    const int *e = m.ext[1];
+    if ((m.wallmask & (1 << SIDE_WE)) && i == 1) {
       long long p = (long long)(j - 1) + (long long)e[1] * (k - 1);
       a = a + (nn + n0 + nnw + nw) * (v - vw) * rx / 4;
-      a = a + d.wm_fluxp[1 * 6 + SIDE_WE][p];
+      a = a + m.fluxp[1 * 6 + SIDE_WE][p];
     }
-    if (d.wall[SIDE_EA] && i == e[0]) {
+    if ((m.wallmask & (1 << SIDE_EA)) && i == e[0]) {
       long long p = (long long)(j - 1) + (long long)e[1] * (k - 1);
       a = a - (nne + ne + nn + n0) * (ve - v) * rx / 4;
-      a = a - d.wm_fluxm[1 * 6 + SIDE_EA][p];
+      a = a - m.fluxm[1 * 6 + SIDE_EA][p];
     }
-    if (d.wall[SIDE_SO] && j == 1) {
+    if ((m.wallmask & (1 << SIDE_SO)) && j == 1) {
       long long p = (long long)(i - 1) + (long long)e[0] * (k - 1);
       a = a + n0 * (v - vs) * ry;
-      a = a + d.wm_fluxp[1 * 6 + SIDE_SO][p];
+      a = a + m.fluxp[1 * 6 + SIDE_SO][p];
     }
-    if (d.wall[SIDE_NO] && j == e[1]) {
+    if ((m.wallmask & (1 << SIDE_NO)) && j == e[1]) {
       long long p = (long long)(i - 1) + (long long)e[0] * (k - 1);
       a = a - nn * (vn - v) * ry;
-      a = a - d.wm_fluxm[1 * 6 + SIDE_NO][p];
+      a = a - m.fluxm[1 * 6 + SIDE_NO][p];
     }
-    if (d.wall[SIDE_BO] && k == 1) {
+    if ((m.wallmask & (1 << SIDE_BO)) && k == 1) {
       long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
       T s = nn + nnb + n0 + nb;
-      if (d.vz) a = a + s * (v - vb) / (T)d.dzW[k - 1 + 2] / 4 / (T)d.dzPr[k + 2];
+      if (m.vz) a = a + s * (v - vb) / (T)m.dzW[k - 1 + 2] / 4 / (T)m.dzPr[k + 2];
       else a = a + s * (v - vb) * rz / 4;
-      a = a + d.wm_fluxp[1 * 6 + SIDE_BO][p];
+      a = a + m.fluxp[1 * 6 + SIDE_BO][p];
     }
-    if (d.wall[SIDE_TO] && k == e[2]) {
+    if ((m.wallmask & (1 << SIDE_TO)) && k == e[2]) {
       long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
       T s = nnt + nn + nt + n0;
-      if (d.vz) a = a - s * (vt - v) / (T)d.dzW[k + 2] / 4 / (T)d.dzPr[k + 2];
+      if (m.vz) a = a - s * (vt - v) / (T)m.dzW[k + 2] / 4 / (T)m.dzPr[k + 2];
       else a = a - s * (vt - v) * rz / 4;
-      a = a - d.wm_fluxm[1 * 6 + SIDE_TO][p];
+      a = a - m.fluxm[1 * 6 + SIDE_TO][p];
     }
   } else {
     const T w = FW(0, 0, 0), we = FW(1, 0, 0), ww = FW(-1, 0, 0), wn = FW(0, 1, 0), ws = FW(0, -1, 0);
@@ -201,7 +224,7 @@ __device__ __forceinline__ T tendency(const Dom<T> &d, const MomTabs<T> &m, cons
     const T v = FV(0, 0, 0), vt = FV(0, 0, 1), vs = FV(0, -1, 0), vts = FV(0, -1, 1);
     const T Ax = m.cA[0], Ay = m.cA[1];
     const T Bx = m.cB[2][0], By = m.cB[2][1];
-    if (!d.vz) {
+    if (!m.vz) {
       const T Az = m.cA[2], Bz = m.cB[2][2];
       a = -((Az * (wt + w) * (wt + w) - Az * (w + wb) * (w + wb)) + (Ay * (wn + w) * (vt + v) - Ay * (w + ws) * (vs + vts)) +
             (Ax * (we + w) * (ut + u) - Ax * (w + ww) * (utw + uw)));
@@ -209,12 +232,12 @@ __device__ __forceinline__ T tendency(const Dom<T> &d, const MomTabs<T> &m, cons
       T Vadv = (v + vt + vs + vts);
       a = a - (Bx * (we - ww) * Uadv + By * (wn - ws) * Vadv + Bz * (wt - wb) * w);
     } else {
-      const T dzw = (T)d.dzW[k + 2];
+      const T dzw = (T)m.dzW[k + 2];
       a = -(((wt + w) * (wt + w) - (w + wb) * (w + wb)) / dzw / 4 + (Ay * (wn + w) * (vt + v) - Ay * (w + ws) * (vts + vs)) +
             (Ax * (we + w) * (ut + u) - Ax * (w + ww) * (utw + uw)));
       T Uadv = (u + ut + uw + utw);
       T Vadv = (v + vt + vs + vts);
-      a = a - (Bx * (we - ww) * Uadv + By * (wn - ws) * Vadv + (wt - wb) / (T)(d.zW[k + 1 + 2] - d.zW[k - 1 + 2]) * w);
+      a = a - (Bx * (we - ww) * Uadv + By * (wn - ws) * Vadv + (wt - wb) / (T)(m.zW[k + 1 + 2] - m.zW[k - 1 + 2]) * w);
     }
     a = a * (T)0.5;
     const T n0 = FN(0, 0, 0), ne = FN(1, 0, 0), nt = FN(0, 0, 1), nte = FN(1, 0, 1), nw = FN(-1, 0, 0), ntw = FN(-1, 0, 1);
@@ -223,47 +246,47 @@ __device__ __forceinline__ T tendency(const Dom<T> &d, const MomTabs<T> &m, cons
     a = a - (T)0.25 * (nt + n0 + ntw + nw) * (w - ww) * rx;
     a = a + (T)0.25 * (ntn + nt + nn + n0) * (wn - w) * ry;
     a = a - (T)0.25 * (nt + nts + n0 + ns) * (w - ws) * ry;
-    if (!d.vz) {
+    if (!m.vz) {
       a = a + nt * (wt - w) * rz;
       a = a - n0 * (w - wb) * rz;
     } else {
-      T tz = nt * (wt - w) / (T)d.dzPr[k + 1 + 2];
-      tz = tz - n0 * (w - wb) / (T)d.dzPr[k + 2];
-      tz = tz / (T)d.dzW[k + 2];
+      T tz = nt * (wt - w) / (T)m.dzPr[k + 1 + 2];
+      tz = tz - n0 * (w - wb) / (T)m.dzPr[k + 2];
+      tz = tz / (T)m.dzW[k + 2];
       a = a + tz;
     }
-    const int *e = d.ext[2];
-    if (d.wall[SIDE_WE] && i == 1) {
+    const int *e = m.ext[2];
+    if ((m.wallmask & (1 << SIDE_WE)) && i == 1) {
       long long p = (long long)(j - 1) + (long long)e[1] * (k - 1);
       a = a + (nt + n0 + ntw + nw) * (w - ww) * rx / 4;
-      a = a + d.wm_fluxp[2 * 6 + SIDE_WE][p];
+      a = a + m.fluxp[2 * 6 + SIDE_WE][p];
     }
-    if (d.wall[SIDE_EA] && i == e[0]) {
+    if ((m.wallmask & (1 << SIDE_EA)) && i == e[0]) {
       long long p = (long long)(j - 1) + (long long)e[1] * (k - 1);
       a = a - (nte + ne + nt + n0) * (we - w) * rx / 4;
-      a = a - d.wm_fluxm[2 * 6 + SIDE_EA][p];
+      a = a - m.fluxm[2 * 6 + SIDE_EA][p];
     }
-    if (d.wall[SIDE_SO] && j == 1) {
+    if ((m.wallmask & (1 << SIDE_SO)) && j == 1) {
       long long p = (long long)(i - 1) + (long long)e[0] * (k - 1);
       a = a + (nt + nts + n0 + ns) * (w - ws) * ry / 4;
-      a = a + d.wm_fluxp[2 * 6 + SIDE_SO][p];
+      a = a + m.fluxp[2 * 6 + SIDE_SO][p];
     }
-    if (d.wall[SIDE_NO] && j == e[1]) {
+    if ((m.wallmask & (1 << SIDE_NO)) && j == e[1]) {
       long long p = (long long)(i - 1) + (long long)e[0] * (k - 1);
       a = a - (ntn + nt + nn + n0) * (wn - w) * ry / 4;
-      a = a - d.wm_fluxm[2 * 6 + SIDE_NO][p];
+      a = a - m.fluxm[2 * 6 + SIDE_NO][p];
     }
-    if (d.wall[SIDE_BO] && k == 1) {
+    if ((m.wallmask & (1 << SIDE_BO)) && k == 1) {
       long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
-      if (d.vz) a = a + n0 * (w - wb) / (T)d.dzPr[k + 2] / (T)d.dzW[k + 2];
+      if (m.vz) a = a + n0 * (w - wb) / (T)m.dzPr[k + 2] / (T)m.dzW[k + 2];
       else a = a + n0 * (w - wb) * rz;
-      a = a + d.wm_fluxp[2 * 6 + SIDE_BO][p];
+      a = a + m.fluxp[2 * 6 + SIDE_BO][p];
     }
-    if (d.wall[SIDE_TO] && k == e[2]) {
+    if ((m.wallmask & (1 << SIDE_TO)) && k == e[2]) {
       long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
-      if (d.vz) a = a - nt * (wt - w) / (T)d.dzPr[k + 1 + 2] / (T)d.dzW[k + 2];
+      if (m.vz) a = a - nt * (wt - w) / (T)m.dzPr[k + 1 + 2] / (T)m.dzW[k + 2];
       else a = a - nt * (wt - w) * rz;
-      a = a - d.wm_fluxm[2 * 6 + SIDE_TO][p];
+      a = a - m.fluxm[2 * 6 + SIDE_TO][p];
     }
   }
 #undef FU
@@ -276,7 +299,7 @@ __device__ __forceinline__ T tendency(const Dom<T> &d, const MomTabs<T> &m, cons
 template <typename T>
 __global__ void __launch_bounds__(MX *MY, 2) k_momentum(const Dom<T> *__restrict__ doms, Launch L, StageCoef sc) {
   __shared__ T ring[3][4 * MPS];
-  __shared__ MomTabs<T> tab;
+  __shared__ MomCtx<T> ctx;
   constexpr int NPF = (MPS + MX * MY - 1) / (MX * MY);  // plane elements per thread and field
   const int tx = threadIdx.x % MX, ty = threadIdx.x / MX;
   for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
@@ -298,12 +321,7 @@ __global__ void __launch_bounds__(MX *MY, 2) k_momentum(const Dom<T> *__restrict
     T *__restrict__ Ws = d.Ws;
     const T *__restrict__ P = d.P;
     __syncthreads();  // the ring and table of the previous tile are no longer read
-    if (threadIdx.x < 3) {
-      const int a = threadIdx.x;
-      tab.cA[a] = (T)d.cA[a];
-      tab.rec2[a] = (T)d.rec2[a];
-      for (int c = 0; c < 3; c++) tab.cB[c][a] = (T)d.cB[c][a];
-    }
+    if (threadIdx.x == 0) fill_ctx(ctx, d);
     // plane element e of this thread: (li, lj) in the haloed tile
     int goff[NPF];
     bool gok[NPF];
@@ -334,7 +352,15 @@ __global__ void __launch_bounds__(MX *MY, 2) k_momentum(const Dom<T> *__restrict
     const bool hasU = i <= d.ext[0][0] && j <= d.ext[0][1];
     const bool hasV = i <= d.ext[1][0] && j <= d.ext[1][1];
     const bool hasW = i <= d.ext[2][0] && j <= d.ext[2][1];
+    const int kU = d.ext[0][2], kV = d.ext[1][2], kW = d.ext[2][2];
     const bool stage1 = sc.stage == 1;
+    const bool vz = d.vz != 0;
+    const T fx = d.prgx_on ? (-coef) * (T)d.prgx : (T)0, fy = d.prgy_on ? (-coef) * (T)d.prgy : (T)0;
+    const bool prgx_on = d.prgx_on != 0, prgy_on = d.prgy_on != 0;
+    const double *dzW = d.dzW;
+    T *__restrict__ U2o = d.U2;
+    T *__restrict__ V2o = d.V2;
+    T *__restrict__ W2o = d.W2;
     // per-cell inputs of the current plane, fetched one plane ahead
     long long c = bidx(d, inside ? i : 1, inside ? j : 1, k0);
     T cUs = 0, cVs = 0, cWs = 0, cP = 0, cPx = 0, cPy = 0, cPz = 0;
@@ -366,38 +392,38 @@ __global__ void __launch_bounds__(MX *MY, 2) k_momentum(const Dom<T> *__restrict
         R.p[2] = ring[(k + 1) % 3];
         R.o = (ty + 1) * MPW + (tx + 1);
         const T p0 = cP - m;
-        if (hasU && k <= d.ext[0][2]) {
-          T ts = tendency<T, 0>(d, tab, R, i, j, k);
+        if (hasU && k <= kU) {
+          T ts = tendency<T, 0>(ctx, R, i, j, k);
           T u2 = stage1 ? (T)0 : cUs * rdt * dt;
           Us[c] = ts;
           u2 = u2 + ts * bdt * dt;
-          if (d.prgx_on) u2 = u2 + (-coef) * (T)d.prgx;
+          if (prgx_on) u2 = u2 + fx;
           u2 = u2 + gx * ((cPx - m) - p0);
           u2 = u2 + R.g(0, 0, 0, 0);
-          d.U2[c] = u2;
-          push_vel(d, d.U2, 0, i, j, k, u2);
+          U2o[c] = u2;
+          push_vel(d, U2o, 0, i, j, k, u2);
         }
-        if (hasV && k <= d.ext[1][2]) {
-          T ts = tendency<T, 1>(d, tab, R, i, j, k);
+        if (hasV && k <= kV) {
+          T ts = tendency<T, 1>(ctx, R, i, j, k);
           T v2 = stage1 ? (T)0 : cVs * rdt * dt;
           Vs[c] = ts;
           v2 = v2 + ts * bdt * dt;
-          if (d.prgy_on) v2 = v2 + (-coef) * (T)d.prgy;
+          if (prgy_on) v2 = v2 + fy;
           v2 = v2 + gy * ((cPy - m) - p0);
           v2 = v2 + R.g(1, 0, 0, 0);
-          d.V2[c] = v2;
-          push_vel(d, d.V2, 1, i, j, k, v2);
+          V2o[c] = v2;
+          push_vel(d, V2o, 1, i, j, k, v2);
         }
-        if (hasW && k <= d.ext[2][2]) {
-          T ts = tendency<T, 2>(d, tab, R, i, j, k);
+        if (hasW && k <= kW) {
+          T ts = tendency<T, 2>(ctx, R, i, j, k);
           T w2 = stage1 ? (T)0 : cWs * rdt * dt;
           Ws[c] = ts;
           w2 = w2 + ts * bdt * dt;
-          if (d.vz) w2 = w2 - coef * ((cPz - m) - p0) / (T)d.dzW[k + 2];
+          if (vz) w2 = w2 - coef * ((cPz - m) - p0) / (T)dzW[k + 2];
           else w2 = w2 + gz * ((cPz - m) - p0);
           w2 = w2 + R.g(2, 0, 0, 0);
-          d.W2[c] = w2;
-          push_vel(d, d.W2, 2, i, j, k, w2);
+          W2o[c] = w2;
+          push_vel(d, W2o, 2, i, j, k, w2);
         }
       }
       __syncthreads();  // plane k-1 is no longer read
@@ -426,22 +452,27 @@ __global__ void __launch_bounds__(MX *MY, 2) k_momentum(const Dom<T> *__restrict
 // onto it (BoundViscosity, src/scalarboundaries.f90:326-431).  Cells next to
 // a wall-model side compute the wall fluxes of the velocity points there.
 template <typename T>
-__device__ __forceinline__ T nusmag_ring(const Dom<T> &d, const Ring<T> &R, int k) {
+struct SgsK {  // factors of NuSmag at one level k
+  T rdx, rdy, r4dx, r4dy, rdz, r2zz, wc2;
+};
+
+// The divisions by the (uniform) spacings of StrainIJ are multiplications by
+// reciprocals computed once, which changes the result by at most one
+// rounding; the sum of squares keeps the order of Strainu.
+template <typename T>
+__device__ __forceinline__ T nusmag_ring(const SgsK<T> &q, const Ring<T> &R) {
 #define GU(dx, dy, dz) R.g(0, dx, dy, dz)
 #define GV(dx, dy, dz) R.g(1, dx, dy, dz)
 #define GW(dx, dy, dz) R.g(2, dx, dy, dz)
-  const T dx = (T)d.dx, dy = (T)d.dy;
-  const T dzk = (T)d.dzPr[k + 2];
-  const T zz = (T)(d.zPr[k + 1 + 2] - d.zPr[k - 1 + 2]);
-  T D00 = (GU(0, 0, 0) - GU(-1, 0, 0)) / dx;
-  T D11 = (GV(0, 0, 0) - GV(0, -1, 0)) / dy;
-  T D22 = (GW(0, 0, 0) - GW(0, 0, -1)) / dzk;
-  T D01 = (GU(0, 1, 0) + GU(-1, 1, 0) - GU(0, -1, 0) - GU(-1, -1, 0)) / (4 * dy);
-  T D02 = (GU(0, 0, 1) + GU(-1, 0, 1) - GU(0, 0, -1) - GU(-1, 0, -1)) / (2 * zz);
-  T D10 = (GV(1, 0, 0) + GV(1, -1, 0) - GV(-1, 0, 0) - GV(-1, -1, 0)) / (4 * dx);
-  T D12 = (GV(0, 0, 1) + GV(0, -1, 1) - GV(0, 0, -1) - GV(0, -1, -1)) / (2 * zz);
-  T D20 = (GW(1, 0, 0) + GW(1, 0, -1) - GW(-1, 0, 0) - GW(-1, 0, -1)) / (4 * dx);
-  T D21 = (GW(0, 1, 0) + GW(0, 1, -1) - GW(0, -1, 0) - GW(0, -1, -1)) / (4 * dy);
+  T D00 = (GU(0, 0, 0) - GU(-1, 0, 0)) * q.rdx;
+  T D11 = (GV(0, 0, 0) - GV(0, -1, 0)) * q.rdy;
+  T D22 = (GW(0, 0, 0) - GW(0, 0, -1)) * q.rdz;
+  T D01 = (GU(0, 1, 0) + GU(-1, 1, 0) - GU(0, -1, 0) - GU(-1, -1, 0)) * q.r4dy;
+  T D02 = (GU(0, 0, 1) + GU(-1, 0, 1) - GU(0, 0, -1) - GU(-1, 0, -1)) * q.r2zz;
+  T D10 = (GV(1, 0, 0) + GV(1, -1, 0) - GV(-1, 0, 0) - GV(-1, -1, 0)) * q.r4dx;
+  T D12 = (GV(0, 0, 1) + GV(0, -1, 1) - GV(0, 0, -1) - GV(0, -1, -1)) * q.r2zz;
+  T D20 = (GW(1, 0, 0) + GW(1, 0, -1) - GW(-1, 0, 0) - GW(-1, 0, -1)) * q.r4dx;
+  T D21 = (GW(0, 1, 0) + GW(0, 1, -1) - GW(0, -1, 0) - GW(0, -1, -1)) * q.r4dy;
 #undef GU
 #undef GV
 #undef GW
@@ -456,8 +487,7 @@ __device__ __forceinline__ T nusmag_ring(const Dom<T> &d, const Ring<T> &R, int 
   s = (D12 + D21) / 2; S = S + s * s;
   s = (D22 + D22) / 2; S = S + s * s;
   T Sbar = sqrt((T)2 * S);
-  T wc = (T)d.width[k] * (T)d.cs;
-  return Sbar * (wc * wc);
+  return Sbar * q.wc2;
 }
 
 template <typename T>
@@ -511,7 +541,13 @@ __global__ void __launch_bounds__(MX *MY, 3) k_sgs(const Dom<T> *__restrict__ do
     const bool px = d.bt[SIDE_WE] == BC_PERIODIC, py = d.bt[SIDE_SO] == BC_PERIODIC, pz = d.bt[SIDE_BO] == BC_PERIODIC;
     const bool anywall = d.wall[0] | d.wall[1] | d.wall[2] | d.wall[3] | d.wall[4] | d.wall[5];
     const T num = (T)d.nu_mol;
+    const bool sgs = d.sgs != 0, addmol = d.nu_mol > 0;
+    SgsK<T> q;
+    q.rdx = (T)(1.0 / d.dx); q.rdy = (T)(1.0 / d.dy);
+    q.r4dx = (T)(1.0 / (4 * d.dx)); q.r4dy = (T)(1.0 / (4 * d.dy));
+    const double *tr = d.sgs_rdz, *t2 = d.sgs_r2zz, *tw = d.sgs_wc2;
     for (int k = k0; k <= k1; k++) {
+      q.rdz = (T)tr[k]; q.r2zz = (T)t2[k]; q.wc2 = (T)tw[k];
       const bool more = k + 1 <= k1;
       T pre[3][NPF];
       if (more) {
@@ -527,9 +563,9 @@ __global__ void __launch_bounds__(MX *MY, 3) k_sgs(const Dom<T> *__restrict__ do
         R.p[2] = ring[(k + 1) % 3];
         R.o = (ty + 1) * MPW + (tx + 1);
         T v;
-        if (d.sgs) {
-          v = nusmag_ring(d, R, k);
-          if (d.nu_mol > 0) v = v + num;
+        if (sgs) {
+          v = nusmag_ring(q, R);
+          if (addmol) v = v + num;
         } else {
           v = num;
         }

@@ -279,3 +279,20 @@ def test_full_size_mixed_vs_fp64():
     e = errs(g, out[1], out[0])
     print("256x256x128 mixed vs FP64 after 1 step (U, V, W, P):", e)
     assert max(e[:3]) < 1e-5, e
+
+
+def test_mixed_defect_correction_sweeps():
+    """Defect correction of the mixed path: with an unreachable tolerance each
+    of the three stages runs all its sweeps; with a loose one none run.  The
+    sweeps must not spoil the result."""
+    g, o, _, st = pair(make_config(64, 64, 32))
+    o.step(2)
+    for tol, expect in ((1e-12, 2 * 3 * 3), (1e-3, 0)):
+        d = L.Domain(make_config(64, 64, 32, precision=1, max_refine_sweeps=3, refine_tol=tol))
+        d.upload(*st)
+        d.project(1.0)
+        s = d.step(2)
+        assert s.refine_sweeps == expect, (tol, s.refine_sweeps)
+        e = errs(g, d.download(), o.state())
+        assert max(e[:3]) < 1e-5, e
+        assert s.max_div < 1e-6
