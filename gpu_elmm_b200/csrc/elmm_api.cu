@@ -3,7 +3,9 @@
 // A single-domain handle is a batch of one; every stage kernel runs once per
 // batch over the domain table (see elmm_kernels.cuh).  One RK3 step of a
 // batch is captured once into a CUDA graph and replayed.
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <cmath>
@@ -55,6 +57,38 @@ static bool factorize(int n, FFTFactors &f) {
 }
 
 static int round_up(int a, int b) { return (a + b - 1) / b * b; }
+
+// cuTensorMapEncodeTiled from the driver the runtime already loaded, so the
+// library does not link against libcuda itself.
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }
+  return fn;
+}
+
+// A 3-D tile map over one box field: x the padded row (pitch elements), y
+// the ny+2 rows, z the nz+2 planes.  Boxes are one plane deep; out-of-range
+// elements read as zero.
+template <typename T>
+static int encode_box_map(CUtensorMap *m, T *base, long long pitch, int ny, int nz, unsigned bx, unsigned by) {
+  auto enc = tensor_map_encoder();
+  if (!enc) return fail(ELMM_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  cuuint64_t dims[3] = {(cuuint64_t)pitch, (cuuint64_t)(ny + 2), (cuuint64_t)(nz + 2)};
+  cuuint64_t strides[2] = {(cuuint64_t)pitch * sizeof(T), (cuuint64_t)pitch * (ny + 2) * sizeof(T)};
+  cuuint32_t box[3] = {bx, by, 1};
+  cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = enc(m, sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)base,
+                   dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(ELMM_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  return ELMM_OK;
+}
 
 // ------------------------------------------------------- host grid tables
 // The same formulas as src/initial.f90:4395-4480 (and the oracle).
@@ -172,6 +206,7 @@ struct BatchT {
   std::vector<void *> allocs;
   LaunchSet ls[LK_N];
   size_t smem_x = 0, smem_y = 0, smem_tri = 0;
+  size_t smem_mom = (size_t)kRingSlots * SlotLayout<T, 5, 3>::BYTES;
   int grid_cap[16];
   // host-layout staging (double), max over domains of the largest host array
   double *dstage = nullptr;
@@ -290,6 +325,7 @@ struct BatchT {
     CU(cudaFuncSetAttribute(k_fftx_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     CU(cudaFuncSetAttribute(k_ffty<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     CU(cudaFuncSetAttribute(k_tri<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    CU(cudaFuncSetAttribute(k_momentum<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 1024));
     int nsm = 0;
     CU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
     auto cap = [&](const void *f, int threads, size_t sm) {
@@ -298,7 +334,7 @@ struct BatchT {
       return b * nsm;
     };
     grid_cap[0] = cap((const void *)k_sgs<T>, MX * MY, 0);
-    grid_cap[1] = cap((const void *)k_momentum<T>, MX * MY, 0);
+    grid_cap[1] = cap((const void *)k_momentum<T>, MX * MY, smem_mom);
     grid_cap[2] = cap((const void *)k_fftx_fwd<T>, kFFTThreads, smem_x);
     grid_cap[3] = cap((const void *)k_ffty<T>, kFFTThreads, smem_y);
     grid_cap[4] = cap((const void *)k_tri<T>, kTriThreads, smem_tri);
@@ -368,10 +404,28 @@ struct BatchT {
     h.cs = c.C_Smagorinsky;
     if (!g.uniform_xy) return fail(ELMM_ERR_INVALID_CONFIG, "dxPr/dyPr must be uniform");
     size_t box = (size_t)h.plane * (h.nz + 2);
+    // a margin of two rows past the box
+    const size_t alloc_elems = box + 2 * (size_t)h.pitch + 64;
     T **fields[12] = {&h.U, &h.V, &h.W, &h.U2, &h.V2, &h.W2, &h.Us, &h.Vs, &h.Ws, &h.P, &h.nu, &h.Phi};
     for (T **f : fields) {
-      int r = dalloc((void **)f, box * sizeof(T));
+      int r = dalloc((void **)f, alloc_elems * sizeof(T));
       if (r) return r;
+    }
+    {
+      // tensor maps of the box fields for the plane rings (wide: tile plus
+      // halo, narrow: tile alone), in field order F_U..F_PHI
+      typedef SlotLayout<T, 5, 3> Lay;
+      std::vector<CUtensorMap> maps(2 * F_COUNT);
+      for (int f = 0; f < F_COUNT; f++) {
+        int r = encode_box_map(&maps[BOX_WIDE * F_COUNT + f], *fields[f], h.pitch, h.ny, h.nz, Lay::SPW, Lay::WROWS);
+        if (!r) r = encode_box_map(&maps[BOX_NARROW * F_COUNT + f], *fields[f], h.pitch, h.ny, h.nz, MX, MY);
+        if (r) return r;
+      }
+      void *p;
+      int r = dalloc(&p, maps.size() * sizeof(CUtensorMap));
+      if (r) return r;
+      CU(cudaMemcpy(p, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
+      h.tmaps = p;
     }
     h.nxh = h.nx / 2 + 1;
     h.spitch = round_up(h.nxh, TyOf<T>::v);
@@ -476,7 +530,7 @@ struct BatchT {
   int launch_momentum(int stage) {
     StageCoef sc{kRho[stage - 1], kBeta[stage - 1], 2 * kAlpha[stage - 1], stage};
     nlaunch++;
-    k_momentum<T><<<gsz(1, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l(), sc);
+    k_momentum<T><<<gsz(1, ls[LK_MOM].total), MX * MY, smem_mom, stream>>>(ddom, ls[LK_MOM].l(), sc);
     return ELMM_OK;
   }
   // PressureCorrection on U2 (in_place = 0) or on U itself (initial projection)
@@ -655,7 +709,7 @@ struct BatchT {
       CU(cudaEventRecord(ev[q++], stream));
       k_sgs<T><<<gsz(0, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l());
       CU(cudaEventRecord(ev[q++], stream));
-      k_momentum<T><<<gsz(1, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l(), sc);
+      k_momentum<T><<<gsz(1, ls[LK_MOM].total), MX * MY, smem_mom, stream>>>(ddom, ls[LK_MOM].l(), sc);
       CU(cudaEventRecord(ev[q++], stream));
       k_fftx_fwd<T><<<gsz(2, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan, a2, 1, 0, 0);
       CU(cudaEventRecord(ev[q++], stream));

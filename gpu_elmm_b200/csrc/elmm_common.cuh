@@ -24,6 +24,11 @@ namespace elmm {
 enum { BC_NOSLIP = 1, BC_FREESLIP = 2, BC_PERIODIC = 3, BC_NEUMANN = 5 };
 enum { SIDE_WE = 0, SIDE_EA = 1, SIDE_SO = 2, SIDE_NO = 3, SIDE_BO = 4, SIDE_TO = 5 };
 
+// box fields of a domain, the order of the tensor maps
+enum { F_U = 0, F_V, F_W, F_U2, F_V2, F_W2, F_US, F_VS, F_WS, F_P, F_NU, F_PHI, F_COUNT };
+// tensor-map box shapes: the tile with its one-cell halo, and the tile alone
+enum { BOX_WIDE = 0, BOX_NARROW = 1 };
+
 // wall-model face planes: index = comp*6 + side
 constexpr int kFaces = 18;
 
@@ -83,7 +88,8 @@ struct Dom {
   // diagnostics
   unsigned long long *maxdiv_bits;  // max |div u| as the bits of a positive double
   unsigned long long *cfl_bits;
-  int *flags;            // [0]: NaN seen
+  int *flags;            // [0]: NaN seen, [1]: a bounded wait gave up
+  const void *tmaps;     // CUtensorMap[2][F_COUNT] (device memory, 64-byte aligned)
   // defect correction of the mixed path
   int *refine_flag;      // 1: the next correction sweep runs for this domain
   int *refine_count;     // sweeps run since the counter was reset

@@ -13,6 +13,7 @@
 #pragma once
 
 #include "elmm_common.cuh"
+#include "elmm_stream.cuh"
 
 namespace elmm {
 
@@ -62,8 +63,8 @@ __device__ __forceinline__ void fill_ctx(MomCtx<T> &m, const Dom<T> &d) {
 
 // one velocity component's tendency at (i,j,k): advection + diffusion +
 // wall corrections, in the reference's order of operations
-template <typename T, int C>
-__device__ __forceinline__ T tendency(const MomCtx<T> &m, const Ring<T> &R, int i, int j, int k) {
+template <typename T, int C, typename RT>
+__device__ __forceinline__ T tendency(const MomCtx<T> &m, const RT &R, int i, int j, int k, int wallhere) {
   // X(dx,dy,dz) with the component's own axis first: along = C, a1, a2 the others
 #define FU(dx, dy, dz) R.g(0, dx, dy, dz)
 #define FV(dx, dy, dz) R.g(1, dx, dy, dz)
@@ -109,40 +110,42 @@ __device__ __forceinline__ T tendency(const MomCtx<T> &m, const Ring<T> &R, int 
       tz = tz / (T)m.dzPr[k + 2];
       a = a + tz;
     }
-    const int *e = m.ext[0];
-    if ((m.wallmask & (1 << SIDE_WE)) && i == 1) {
-      long long p = (long long)(j - 1) + (long long)e[1] * (k - 1);
-      a = a + n0 * (u - uw) * rx;
-      a = a + m.fluxp[0 * 6 + SIDE_WE][p];
-    }
-    if ((m.wallmask & (1 << SIDE_EA)) && i == e[0]) {
-      long long p = (long long)(j - 1) + (long long)e[1] * (k - 1);
-      a = a - ne * (ue - u) * rx;
-      a = a - m.fluxm[0 * 6 + SIDE_EA][p];
-    }
-    if ((m.wallmask & (1 << SIDE_SO)) && j == 1) {
-      long long p = (long long)(i - 1) + (long long)e[0] * (k - 1);
-      a = a + (ne + nse + n0 + ns) * (u - us) * ry / 4;
-      a = a + m.fluxp[0 * 6 + SIDE_SO][p];
-    }
-    if ((m.wallmask & (1 << SIDE_NO)) && j == e[1]) {
-      long long p = (long long)(i - 1) + (long long)e[0] * (k - 1);
-      a = a - (nne + ne + nn + n0) * (un - u) * ry / 4;
-      a = a - m.fluxm[0 * 6 + SIDE_NO][p];
-    }
-    if ((m.wallmask & (1 << SIDE_BO)) && k == 1) {
-      long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
-      T s = ne + nbe + n0 + nb;
-      if (m.vz) a = a + s * (u - ub) / (T)m.dzW[k - 1 + 2] / 4 / (T)m.dzPr[k + 2];
-      else a = a + s * (u - ub) * rz / 4;
-      a = a + m.fluxp[0 * 6 + SIDE_BO][p];
-    }
-    if ((m.wallmask & (1 << SIDE_TO)) && k == e[2]) {
-      long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
-      T s = nte + ne + nt + n0;
-      if (m.vz) a = a - s * (ut - u) / (T)m.dzW[k + 2] / 4 / (T)m.dzPr[k + 2];
-      else a = a - s * (ut - u) * rz / 4;
-      a = a - m.fluxm[0 * 6 + SIDE_TO][p];
+    if (wallhere) {
+      const int *e = m.ext[0];
+      if ((m.wallmask & (1 << SIDE_WE)) && i == 1) {
+        long long p = (long long)(j - 1) + (long long)e[1] * (k - 1);
+        a = a + n0 * (u - uw) * rx;
+        a = a + m.fluxp[0 * 6 + SIDE_WE][p];
+      }
+      if ((m.wallmask & (1 << SIDE_EA)) && i == e[0]) {
+        long long p = (long long)(j - 1) + (long long)e[1] * (k - 1);
+        a = a - ne * (ue - u) * rx;
+        a = a - m.fluxm[0 * 6 + SIDE_EA][p];
+      }
+      if ((m.wallmask & (1 << SIDE_SO)) && j == 1) {
+        long long p = (long long)(i - 1) + (long long)e[0] * (k - 1);
+        a = a + (ne + nse + n0 + ns) * (u - us) * ry / 4;
+        a = a + m.fluxp[0 * 6 + SIDE_SO][p];
+      }
+      if ((m.wallmask & (1 << SIDE_NO)) && j == e[1]) {
+        long long p = (long long)(i - 1) + (long long)e[0] * (k - 1);
+        a = a - (nne + ne + nn + n0) * (un - u) * ry / 4;
+        a = a - m.fluxm[0 * 6 + SIDE_NO][p];
+      }
+      if ((m.wallmask & (1 << SIDE_BO)) && k == 1) {
+        long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
+        T s = ne + nbe + n0 + nb;
+        if (m.vz) a = a + s * (u - ub) / (T)m.dzW[k - 1 + 2] / 4 / (T)m.dzPr[k + 2];
+        else a = a + s * (u - ub) * rz / 4;
+        a = a + m.fluxp[0 * 6 + SIDE_BO][p];
+      }
+      if ((m.wallmask & (1 << SIDE_TO)) && k == e[2]) {
+        long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
+        T s = nte + ne + nt + n0;
+        if (m.vz) a = a - s * (ut - u) / (T)m.dzW[k + 2] / 4 / (T)m.dzPr[k + 2];
+        else a = a - s * (ut - u) * rz / 4;
+        a = a - m.fluxm[0 * 6 + SIDE_TO][p];
+      }
     }
   } else if (C == 1) {
     const T v = FV(0, 0, 0), ve = FV(1, 0, 0), vw = FV(-1, 0, 0), vn = FV(0, 1, 0), vs = FV(0, -1, 0);
@@ -182,40 +185,42 @@ __device__ __forceinline__ T tendency(const MomCtx<T> &m, const Ring<T> &R, int 
       tz = tz / (T)m.dzPr[k + 2];
       a = a + tz;
     }
-    const int *e = m.ext[1];
-    if ((m.wallmask & (1 << SIDE_WE)) && i == 1) {
-      long long p = (long long)(j - 1) + (long long)e[1] * (k - 1);
-      a = a + (nn + n0 + nnw + nw) * (v - vw) * rx / 4;
-      a = a + m.fluxp[1 * 6 + SIDE_WE][p];
-    }
-    if ((m.wallmask & (1 << SIDE_EA)) && i == e[0]) {
-      long long p = (long long)(j - 1) + (long long)e[1] * (k - 1);
-      a = a - (nne + ne + nn + n0) * (ve - v) * rx / 4;
-      a = a - m.fluxm[1 * 6 + SIDE_EA][p];
-    }
-    if ((m.wallmask & (1 << SIDE_SO)) && j == 1) {
-      long long p = (long long)(i - 1) + (long long)e[0] * (k - 1);
-      a = a + n0 * (v - vs) * ry;
-      a = a + m.fluxp[1 * 6 + SIDE_SO][p];
-    }
-    if ((m.wallmask & (1 << SIDE_NO)) && j == e[1]) {
-      long long p = (long long)(i - 1) + (long long)e[0] * (k - 1);
-      a = a - nn * (vn - v) * ry;
-      a = a - m.fluxm[1 * 6 + SIDE_NO][p];
-    }
-    if ((m.wallmask & (1 << SIDE_BO)) && k == 1) {
-      long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
-      T s = nn + nnb + n0 + nb;
-      if (m.vz) a = a + s * (v - vb) / (T)m.dzW[k - 1 + 2] / 4 / (T)m.dzPr[k + 2];
-      else a = a + s * (v - vb) * rz / 4;
-      a = a + m.fluxp[1 * 6 + SIDE_BO][p];
-    }
-    if ((m.wallmask & (1 << SIDE_TO)) && k == e[2]) {
-      long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
-      T s = nnt + nn + nt + n0;
-      if (m.vz) a = a - s * (vt - v) / (T)m.dzW[k + 2] / 4 / (T)m.dzPr[k + 2];
-      else a = a - s * (vt - v) * rz / 4;
-      a = a - m.fluxm[1 * 6 + SIDE_TO][p];
+    if (wallhere) {
+      const int *e = m.ext[1];
+      if ((m.wallmask & (1 << SIDE_WE)) && i == 1) {
+        long long p = (long long)(j - 1) + (long long)e[1] * (k - 1);
+        a = a + (nn + n0 + nnw + nw) * (v - vw) * rx / 4;
+        a = a + m.fluxp[1 * 6 + SIDE_WE][p];
+      }
+      if ((m.wallmask & (1 << SIDE_EA)) && i == e[0]) {
+        long long p = (long long)(j - 1) + (long long)e[1] * (k - 1);
+        a = a - (nne + ne + nn + n0) * (ve - v) * rx / 4;
+        a = a - m.fluxm[1 * 6 + SIDE_EA][p];
+      }
+      if ((m.wallmask & (1 << SIDE_SO)) && j == 1) {
+        long long p = (long long)(i - 1) + (long long)e[0] * (k - 1);
+        a = a + n0 * (v - vs) * ry;
+        a = a + m.fluxp[1 * 6 + SIDE_SO][p];
+      }
+      if ((m.wallmask & (1 << SIDE_NO)) && j == e[1]) {
+        long long p = (long long)(i - 1) + (long long)e[0] * (k - 1);
+        a = a - nn * (vn - v) * ry;
+        a = a - m.fluxm[1 * 6 + SIDE_NO][p];
+      }
+      if ((m.wallmask & (1 << SIDE_BO)) && k == 1) {
+        long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
+        T s = nn + nnb + n0 + nb;
+        if (m.vz) a = a + s * (v - vb) / (T)m.dzW[k - 1 + 2] / 4 / (T)m.dzPr[k + 2];
+        else a = a + s * (v - vb) * rz / 4;
+        a = a + m.fluxp[1 * 6 + SIDE_BO][p];
+      }
+      if ((m.wallmask & (1 << SIDE_TO)) && k == e[2]) {
+        long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
+        T s = nnt + nn + nt + n0;
+        if (m.vz) a = a - s * (vt - v) / (T)m.dzW[k + 2] / 4 / (T)m.dzPr[k + 2];
+        else a = a - s * (vt - v) * rz / 4;
+        a = a - m.fluxm[1 * 6 + SIDE_TO][p];
+      }
     }
   } else {
     const T w = FW(0, 0, 0), we = FW(1, 0, 0), ww = FW(-1, 0, 0), wn = FW(0, 1, 0), ws = FW(0, -1, 0);
@@ -255,38 +260,40 @@ __device__ __forceinline__ T tendency(const MomCtx<T> &m, const Ring<T> &R, int 
       tz = tz / (T)m.dzW[k + 2];
       a = a + tz;
     }
-    const int *e = m.ext[2];
-    if ((m.wallmask & (1 << SIDE_WE)) && i == 1) {
-      long long p = (long long)(j - 1) + (long long)e[1] * (k - 1);
-      a = a + (nt + n0 + ntw + nw) * (w - ww) * rx / 4;
-      a = a + m.fluxp[2 * 6 + SIDE_WE][p];
-    }
-    if ((m.wallmask & (1 << SIDE_EA)) && i == e[0]) {
-      long long p = (long long)(j - 1) + (long long)e[1] * (k - 1);
-      a = a - (nte + ne + nt + n0) * (we - w) * rx / 4;
-      a = a - m.fluxm[2 * 6 + SIDE_EA][p];
-    }
-    if ((m.wallmask & (1 << SIDE_SO)) && j == 1) {
-      long long p = (long long)(i - 1) + (long long)e[0] * (k - 1);
-      a = a + (nt + nts + n0 + ns) * (w - ws) * ry / 4;
-      a = a + m.fluxp[2 * 6 + SIDE_SO][p];
-    }
-    if ((m.wallmask & (1 << SIDE_NO)) && j == e[1]) {
-      long long p = (long long)(i - 1) + (long long)e[0] * (k - 1);
-      a = a - (ntn + nt + nn + n0) * (wn - w) * ry / 4;
-      a = a - m.fluxm[2 * 6 + SIDE_NO][p];
-    }
-    if ((m.wallmask & (1 << SIDE_BO)) && k == 1) {
-      long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
-      if (m.vz) a = a + n0 * (w - wb) / (T)m.dzPr[k + 2] / (T)m.dzW[k + 2];
-      else a = a + n0 * (w - wb) * rz;
-      a = a + m.fluxp[2 * 6 + SIDE_BO][p];
-    }
-    if ((m.wallmask & (1 << SIDE_TO)) && k == e[2]) {
-      long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
-      if (m.vz) a = a - nt * (wt - w) / (T)m.dzPr[k + 1 + 2] / (T)m.dzW[k + 2];
-      else a = a - nt * (wt - w) * rz;
-      a = a - m.fluxm[2 * 6 + SIDE_TO][p];
+    if (wallhere) {
+      const int *e = m.ext[2];
+      if ((m.wallmask & (1 << SIDE_WE)) && i == 1) {
+        long long p = (long long)(j - 1) + (long long)e[1] * (k - 1);
+        a = a + (nt + n0 + ntw + nw) * (w - ww) * rx / 4;
+        a = a + m.fluxp[2 * 6 + SIDE_WE][p];
+      }
+      if ((m.wallmask & (1 << SIDE_EA)) && i == e[0]) {
+        long long p = (long long)(j - 1) + (long long)e[1] * (k - 1);
+        a = a - (nte + ne + nt + n0) * (we - w) * rx / 4;
+        a = a - m.fluxm[2 * 6 + SIDE_EA][p];
+      }
+      if ((m.wallmask & (1 << SIDE_SO)) && j == 1) {
+        long long p = (long long)(i - 1) + (long long)e[0] * (k - 1);
+        a = a + (nt + nts + n0 + ns) * (w - ws) * ry / 4;
+        a = a + m.fluxp[2 * 6 + SIDE_SO][p];
+      }
+      if ((m.wallmask & (1 << SIDE_NO)) && j == e[1]) {
+        long long p = (long long)(i - 1) + (long long)e[0] * (k - 1);
+        a = a - (ntn + nt + nn + n0) * (wn - w) * ry / 4;
+        a = a - m.fluxm[2 * 6 + SIDE_NO][p];
+      }
+      if ((m.wallmask & (1 << SIDE_BO)) && k == 1) {
+        long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
+        if (m.vz) a = a + n0 * (w - wb) / (T)m.dzPr[k + 2] / (T)m.dzW[k + 2];
+        else a = a + n0 * (w - wb) * rz;
+        a = a + m.fluxp[2 * 6 + SIDE_BO][p];
+      }
+      if ((m.wallmask & (1 << SIDE_TO)) && k == e[2]) {
+        long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
+        if (m.vz) a = a - nt * (wt - w) / (T)m.dzPr[k + 1 + 2] / (T)m.dzW[k + 2];
+        else a = a - nt * (wt - w) * rz;
+        a = a - m.fluxm[2 * 6 + SIDE_TO][p];
+      }
     }
   }
 #undef FU
@@ -296,12 +303,78 @@ __device__ __forceinline__ T tendency(const MomCtx<T> &m, const Ring<T> &R, int 
   return a;
 }
 
+// Layout of one ring slot (one plane k of the tile): NWF "wide" fields with
+// the x/y halo (rows j0-1..j0+MY, columns i0-XO..i0+MX+XO-1) and NNF
+// "narrow" fields of the tile's own cells (rows j0..j0+MY-1, columns
+// i0..i0+MX-1).  XO = 16 bytes of halo on each side keeps every copied row
+// segment 16-byte aligned in global and shared memory.
+template <typename T, int NWF, int NNF>
+struct SlotLayout {
+  static constexpr int XO = 16 / (int)sizeof(T);
+  static constexpr int SPW = MX + 2 * XO;  // wide row
+  static constexpr int WROWS = MY + 2;
+  static constexpr int WB = ((WROWS * SPW * (int)sizeof(T) + 127) / 128) * 128 / (int)sizeof(T);  // wide block
+  static constexpr int NB = ((MY * MX * (int)sizeof(T) + 127) / 128) * 128 / (int)sizeof(T);      // narrow block
+  static constexpr int WIDE = NWF * WB;
+  static constexpr int SIZE = WIDE + NNF * NB;  // elements per slot (a multiple of 128 bytes)
+  static constexpr int BYTES = SIZE * (int)sizeof(T);
+  static constexpr uint32_t WBOX = WROWS * SPW * sizeof(T);  // bytes one wide box delivers
+  static constexpr uint32_t NBOX = MY * MX * sizeof(T);
+};
+
+// ring accessor: field f (wide), offsets (dx,dy) of the thread's cell and
+// plane k+dz
+template <typename T, int NWF, int NNF>
+struct WideRing {
+  typedef SlotLayout<T, NWF, NNF> Lay;
+  const T *p[3];
+  int o;
+  __device__ __forceinline__ T g(int f, int dx, int dy, int dz) const {
+    return p[dz + 1][f * Lay::WB + o + dy * Lay::SPW + dx];
+  }
+};
+
+// Issues the tensor-map loads of plane kk of the tile into one slot: one
+// box per field (thread 0 only).
+template <typename T, int NWF, int NNF>
+__device__ __forceinline__ void issue_plane(T *slot, uint64_t *bar, const CUtensorMap *maps, const int *wide,
+                                            const int *narrow, bool with_narrow, int aln, int i0, int j0, int kk) {
+  typedef SlotLayout<T, NWF, NNF> Lay;
+  const uint32_t bytes = NWF * Lay::WBOX + (with_narrow ? NNF * Lay::NBOX : 0u);
+  mbar_expect_tx(bar, bytes);
+  const int xw = aln - 1 + i0 - Lay::XO, xn = aln - 1 + i0;
+#pragma unroll
+  for (int f = 0; f < NWF; f++) tma_load_3d(slot + f * Lay::WB, maps + BOX_WIDE * F_COUNT + wide[f], xw, j0 - 1, kk, bar);
+  if (with_narrow) {
+#pragma unroll
+    for (int f = 0; f < NNF; f++)
+      tma_load_3d(slot + Lay::WIDE + f * Lay::NB, maps + BOX_NARROW * F_COUNT + narrow[f], xn, j0, kk, bar);
+  }
+}
+
+constexpr int kRingSlots = 5;
+
 template <typename T>
 __global__ void __launch_bounds__(MX *MY, 2) k_momentum(const Dom<T> *__restrict__ doms, Launch L, StageCoef sc) {
-  __shared__ T ring[3][4 * MPS];
+  typedef SlotLayout<T, 5, 3> Lay;
+  extern __shared__ __align__(128) unsigned char dyn_smem[];
+  T *ring = reinterpret_cast<T *>(dyn_smem);
+  __shared__ __align__(8) uint64_t bars[kRingSlots];
   __shared__ MomCtx<T> ctx;
-  constexpr int NPF = (MPS + MX * MY - 1) / (MX * MY);  // plane elements per thread and field
+  __shared__ int abort_flag;
   const int tx = threadIdx.x % MX, ty = threadIdx.x / MX;
+  // tensor copies need 128-byte aligned destinations
+  if (smem_addr(ring) & 127u) {
+    if (threadIdx.x == 0) doms[0].flags[1] = 1;
+    return;
+  }
+  if (threadIdx.x == 0) {
+    for (int s2 = 0; s2 < kRingSlots; s2++) mbar_init(&bars[s2], 1);
+    abort_flag = 0;
+    fence_async_shared();
+  }
+  __syncthreads();
+  uint32_t phase = 0;  // bit s: parity of the next wait on slot s
   for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
     const int di = find_dom(L.starts, L.nd, t);
     const Dom<T> &d = doms[di];
@@ -315,34 +388,19 @@ __global__ void __launch_bounds__(MX *MY, 2) k_momentum(const Dom<T> *__restrict
     const int i = i0 + tx, j = j0 + ty;
     const int nx = d.nx, ny = d.ny;
     const long long pitch = d.pitch, plane = d.plane;
-    const T *__restrict__ F[4] = {d.U, d.V, d.W, d.nu};
-    T *__restrict__ Us = d.Us;
-    T *__restrict__ Vs = d.Vs;
-    T *__restrict__ Ws = d.Ws;
-    const T *__restrict__ P = d.P;
-    __syncthreads();  // the ring and table of the previous tile are no longer read
+    const bool stage1 = sc.stage == 1;
+    const int wide[5] = {F_U, F_V, F_W, F_NU, F_P};
+    const int narrow[3] = {F_US, F_VS, F_WS};
+    const CUtensorMap *maps = reinterpret_cast<const CUtensorMap *>(d.tmaps);
+    __syncthreads();  // every slot and the context of the previous tile are free
     if (threadIdx.x == 0) fill_ctx(ctx, d);
-    // plane element e of this thread: (li, lj) in the haloed tile
-    int goff[NPF];
-    bool gok[NPF];
-#pragma unroll
-    for (int q = 0; q < NPF; q++) {
-      int e = threadIdx.x + q * MX * MY;
-      int li = e % MPW, lj = e / MPW;
-      int gi = i0 - 1 + li, gj = j0 - 1 + lj;
-      gok[q] = e < MPS && gi <= nx + 1 && gj <= ny + 1;
-      goff[q] = gok[q] ? (d.aln - 1 + gi) + (int)pitch * gj : 0;
+    if (threadIdx.x == 0) {
+      fence_async_shared();
+      for (int kk = k0 - 1; kk <= min(k0 - 1 + kRingSlots - 1, k1 + 1); kk++)
+        issue_plane<T, 5, 3>(ring + (kk % kRingSlots) * Lay::SIZE, &bars[kk % kRingSlots], maps, wide, narrow, !stage1,
+                             d.aln, i0, j0, kk);
     }
-    for (int kk = k0 - 1; kk <= k0 + 1; kk++) {
-      T *dst = ring[kk % 3];
-#pragma unroll
-      for (int f = 0; f < 4; f++)
-#pragma unroll
-        for (int q = 0; q < NPF; q++) {
-          int e = threadIdx.x + q * MX * MY;
-          if (e < MPS) dst[f * MPS + e] = gok[q] ? __ldg(F[f] + goff[q] + plane * kk) : (T)0;
-        }
-    }
+    __syncthreads();  // the context is written
     const T dt = (T)d.dt, rdt = (T)sc.rho, bdt = (T)sc.beta;
     const double coefd = sc.alpha2 * d.dt;
     const T coef = (T)coefd;
@@ -353,97 +411,103 @@ __global__ void __launch_bounds__(MX *MY, 2) k_momentum(const Dom<T> *__restrict
     const bool hasV = i <= d.ext[1][0] && j <= d.ext[1][1];
     const bool hasW = i <= d.ext[2][0] && j <= d.ext[2][1];
     const int kU = d.ext[0][2], kV = d.ext[1][2], kW = d.ext[2][2];
-    const bool stage1 = sc.stage == 1;
     const bool vz = d.vz != 0;
-    const T fx = d.prgx_on ? (-coef) * (T)d.prgx : (T)0, fy = d.prgy_on ? (-coef) * (T)d.prgy : (T)0;
     const bool prgx_on = d.prgx_on != 0, prgy_on = d.prgy_on != 0;
+    const T fx = prgx_on ? (-coef) * (T)d.prgx : (T)0, fy = prgy_on ? (-coef) * (T)d.prgy : (T)0;
     const double *dzW = d.dzW;
     T *__restrict__ U2o = d.U2;
     T *__restrict__ V2o = d.V2;
     T *__restrict__ W2o = d.W2;
-    // per-cell inputs of the current plane, fetched one plane ahead
+    T *__restrict__ Us = d.Us;
+    T *__restrict__ Vs = d.Vs;
+    T *__restrict__ Ws = d.Ws;
+    const int o = (ty + 1) * Lay::SPW + (tx + Lay::XO);
     long long c = bidx(d, inside ? i : 1, inside ? j : 1, k0);
-    T cUs = 0, cVs = 0, cWs = 0, cP = 0, cPx = 0, cPy = 0, cPz = 0;
-    if (inside) {
-      if (!stage1) { cUs = Us[c]; cVs = Vs[c]; cWs = Ws[c]; }
-      cP = __ldg(P + c); cPx = __ldg(P + c + 1); cPy = __ldg(P + c + pitch); cPz = __ldg(P + c + plane);
-    }
-    __syncthreads();
+    // block-uniform: only tiles on a side of the box and the planes next to
+    // the bottom and top have ghost images or wall-model corrections
+    const int nz = d.nz;
+    // a component's last index is n or n-1 (src/initial.f90:871-896)
+    const bool xlo = i0 == 1, xhi = i0 + MX - 1 >= nx - 1, ylo = j0 == 1, yhi = j0 + MY - 1 >= ny - 1;
+    const bool edge_tile = xlo || xhi || ylo || yhi;
+    int wmask = 0;
+    for (int f = 0; f < 6; f++) wmask |= d.wall[f] ? (1 << f) : 0;
+    const int wtile = wmask & ((xlo ? 1 : 0) | (xhi ? 2 : 0) | (ylo ? 4 : 0) | (yhi ? 8 : 0));
     for (int k = k0; k <= k1; k++) {
-      const bool more = k + 1 <= k1;
-      // prefetch plane k+2 of the ring and the per-cell inputs of plane k+1
-      T pre[4][NPF];
-      T nUs = 0, nVs = 0, nWs = 0, nP = 0, nPx = 0, nPy = 0, nPz = 0;
-      if (more) {
-#pragma unroll
-        for (int f = 0; f < 4; f++)
-#pragma unroll
-          for (int q = 0; q < NPF; q++) pre[f][q] = gok[q] ? __ldg(F[f] + goff[q] + plane * (k + 2)) : (T)0;
-        if (inside) {
-          const long long cn = c + plane;
-          if (!stage1) { nUs = Us[cn]; nVs = Vs[cn]; nWs = Ws[cn]; }
-          nP = __ldg(P + cn); nPx = __ldg(P + cn + 1); nPy = __ldg(P + cn + pitch); nPz = __ldg(P + cn + plane);
-        }
+      // planes k-1, k, k+1 must have landed
+      bool ok = true;
+      for (int kk = (k == k0 ? k0 - 1 : k + 1); kk <= k + 1; kk++) {
+        const int s2 = kk % kRingSlots;
+        ok &= mbar_wait(&bars[s2], (phase >> s2) & 1u);
+        phase ^= 1u << s2;
       }
-      if (inside) {
-        Ring<T> R;
-        R.p[0] = ring[(k - 1) % 3];
-        R.p[1] = ring[k % 3];
-        R.p[2] = ring[(k + 1) % 3];
-        R.o = (ty + 1) * MPW + (tx + 1);
-        const T p0 = cP - m;
+      if (!ok) { abort_flag = 1; d.flags[1] = 1; }
+      const bool edge = edge_tile || k <= 1 || k >= nz - 1;
+      const int wallhere = wtile | (wmask & ((k == 1 ? 16 : 0) | (k >= nz - 1 ? 32 : 0)));
+      if (inside && ok) {
+        WideRing<T, 5, 3> R;
+        R.p[0] = ring + ((k - 1) % kRingSlots) * Lay::SIZE;
+        R.p[1] = ring + (k % kRingSlots) * Lay::SIZE;
+        R.p[2] = ring + ((k + 1) % kRingSlots) * Lay::SIZE;
+        R.o = o;
+        const T *nar = R.p[1] + Lay::WIDE + ty * MX + tx;  // narrow blocks are NB apart
+        const T p0 = R.g(4, 0, 0, 0) - m;
         if (hasU && k <= kU) {
-          T ts = tendency<T, 0>(ctx, R, i, j, k);
-          T u2 = stage1 ? (T)0 : cUs * rdt * dt;
+          T ts = tendency<T, 0>(ctx, R, i, j, k, wallhere);
+          T u2 = stage1 ? (T)0 : nar[0] * rdt * dt;
           Us[c] = ts;
           u2 = u2 + ts * bdt * dt;
           if (prgx_on) u2 = u2 + fx;
-          u2 = u2 + gx * ((cPx - m) - p0);
+          u2 = u2 + gx * ((R.g(4, 1, 0, 0) - m) - p0);
           u2 = u2 + R.g(0, 0, 0, 0);
           U2o[c] = u2;
-          push_vel(d, U2o, 0, i, j, k, u2);
+          if (edge) push_vel(d, U2o, 0, i, j, k, u2);
         }
         if (hasV && k <= kV) {
-          T ts = tendency<T, 1>(ctx, R, i, j, k);
-          T v2 = stage1 ? (T)0 : cVs * rdt * dt;
+          T ts = tendency<T, 1>(ctx, R, i, j, k, wallhere);
+          T v2 = stage1 ? (T)0 : nar[Lay::NB] * rdt * dt;
           Vs[c] = ts;
           v2 = v2 + ts * bdt * dt;
           if (prgy_on) v2 = v2 + fy;
-          v2 = v2 + gy * ((cPy - m) - p0);
+          v2 = v2 + gy * ((R.g(4, 0, 1, 0) - m) - p0);
           v2 = v2 + R.g(1, 0, 0, 0);
           V2o[c] = v2;
-          push_vel(d, V2o, 1, i, j, k, v2);
+          if (edge) push_vel(d, V2o, 1, i, j, k, v2);
         }
         if (hasW && k <= kW) {
-          T ts = tendency<T, 2>(ctx, R, i, j, k);
-          T w2 = stage1 ? (T)0 : cWs * rdt * dt;
+          T ts = tendency<T, 2>(ctx, R, i, j, k, wallhere);
+          T w2 = stage1 ? (T)0 : nar[2 * Lay::NB] * rdt * dt;
           Ws[c] = ts;
           w2 = w2 + ts * bdt * dt;
-          if (vz) w2 = w2 - coef * ((cPz - m) - p0) / (T)dzW[k + 2];
-          else w2 = w2 + gz * ((cPz - m) - p0);
+          const T dpz = (R.g(4, 0, 0, 1) - m) - p0;
+          if (vz) w2 = w2 - coef * dpz / (T)dzW[k + 2];
+          else w2 = w2 + gz * dpz;
           w2 = w2 + R.g(2, 0, 0, 0);
           W2o[c] = w2;
-          push_vel(d, W2o, 2, i, j, k, w2);
+          if (edge) push_vel(d, W2o, 2, i, j, k, w2);
         }
       }
       __syncthreads();  // plane k-1 is no longer read
-      if (more) {
-        T *dst = ring[(k + 2) % 3];
-#pragma unroll
-        for (int f = 0; f < 4; f++)
-#pragma unroll
-          for (int q = 0; q < NPF; q++) {
-            int e = threadIdx.x + q * MX * MY;
-            if (e < MPS) dst[f * MPS + e] = pre[f][q];
+      if (abort_flag) {
+        // a plane did not arrive: wait (bounded) for the copies still in
+        // flight into this block's shared memory, then give up
+        if (threadIdx.x == 0)
+          for (int kk = k + 2; kk <= min(k - 1 + kRingSlots - 1, k1 + 1); kk++) {
+            const int s2 = kk % kRingSlots;
+            mbar_wait(&bars[s2], (phase >> s2) & 1u);
+            phase ^= 1u << s2;
           }
-        cUs = nUs; cVs = nVs; cWs = nWs; cP = nP; cPx = nPx; cPy = nPy; cPz = nPz;
-        c += plane;
+        return;
       }
-      __syncthreads();
+      const int kn = k - 1 + kRingSlots;
+      if (threadIdx.x == 0 && kn <= k1 + 1) {
+        fence_async_shared();
+        issue_plane<T, 5, 3>(ring + (kn % kRingSlots) * Lay::SIZE, &bars[kn % kRingSlots], maps, wide, narrow, !stage1,
+                             d.aln, i0, j0, kn);
+      }
+      c += plane;
     }
   }
 }
-
 
 // ---------------------------------------------------------------- k_sgs
 // SubgridStresses (src/dynamics.f90:869-908): Smagorinsky viscosity
@@ -459,8 +523,8 @@ struct SgsK {  // factors of NuSmag at one level k
 // The divisions by the (uniform) spacings of StrainIJ are multiplications by
 // reciprocals computed once, which changes the result by at most one
 // rounding; the sum of squares keeps the order of Strainu.
-template <typename T>
-__device__ __forceinline__ T nusmag_ring(const SgsK<T> &q, const Ring<T> &R) {
+template <typename T, typename RT>
+__device__ __forceinline__ T nusmag_ring(const SgsK<T> &q, const RT &R) {
 #define GU(dx, dy, dz) R.g(0, dx, dy, dz)
 #define GV(dx, dy, dz) R.g(1, dx, dy, dz)
 #define GW(dx, dy, dz) R.g(2, dx, dy, dz)
