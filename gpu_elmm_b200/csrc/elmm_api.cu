@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1142,3 +1143,220 @@ int elmm_poisson_solver_finalize(elmm_poisson *s) {
 }
 
 }  // extern "C"
+
+// ============================================================================
+// elmm_poisson_solve_noalloc: the solve of elmm_poisson_solver_execute on
+// device arrays, for callers that cannot allocate device memory (a host
+// whose pool already owns the GPU, or a path where cudaMalloc/cudaFree would
+// synchronise the device).  All working memory sits in noalloc_scratch, a
+// fixed array in this library's device image; nothing here calls cudaMalloc,
+// cudaFree or any other allocating routine.  The kernels are the ones of the
+// handle-based solver; only their descriptors and buffers live elsewhere.
+
+// Every GPU that loads the library holds this array until the process exits.
+static __device__ __align__(256) unsigned char noalloc_scratch[ELMM_NOALLOC_SCRATCH_BYTES];
+
+// byte offsets of the pieces carved out of noalloc_scratch (256-aligned)
+struct NoAllocLayout {
+  size_t dom, plan, starts, bad, twx, twy, lamx, lamy, Ab, At, dzc, dzf, box, S, total;
+};
+
+static NoAllocLayout noalloc_layout(int nx, int ny, int nz, size_t box_elems, size_t s_elems) {
+  NoAllocLayout l;
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    size_t at = o;
+    o += (bytes + 255) / 256 * 256;
+    return at;
+  };
+  l.dom = take(sizeof(Dom<double>));
+  l.plan = take(sizeof(PoisPlan));
+  l.starts = take(2 * sizeof(int));
+  l.bad = take(sizeof(int));
+  l.twx = take(sizeof(double2) * nx);
+  l.twy = take(sizeof(double2) * ny);
+  l.lamx = take(sizeof(double) * nx);
+  l.lamy = take(sizeof(double) * ny);
+  l.Ab = take(sizeof(double) * (nz + 2));
+  l.At = take(sizeof(double) * (nz + 2));
+  l.dzc = take(sizeof(double) * (nz + 2));
+  l.dzf = take(sizeof(double) * (nz + 2));
+  l.box = take(sizeof(double) * box_elems);
+  l.S = take(sizeof(double2) * s_elems);
+  l.total = o;
+  return l;
+}
+
+// Writes the descriptors and the FFT / tridiagonal tables of one solve into
+// the scratch array and zeroes its one accumulator (the count of non-finite
+// right-hand-side values).  Nothing else in the array needs to start at zero:
+// every other element a solve reads is written earlier in the same solve.
+// The tables follow the handle-based set-up: twiddles exp(-2 pi i m / n), the
+// eigenvalues -4 sin^2(pi m / n) / d^2, and the z coefficients of a uniform
+// grid with zW(k) = k dz (src/poisson.f90:23-60 for the discrete problem).
+static __global__ void k_noalloc_setup(Dom<double> h, PoisPlan pl, NoAllocLayout lay, unsigned char *base) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  if (tid == 0) {
+    *reinterpret_cast<Dom<double> *>(base + lay.dom) = h;
+    *reinterpret_cast<PoisPlan *>(base + lay.plan) = pl;
+    int *st = reinterpret_cast<int *>(base + lay.starts);
+    st[0] = 0;
+    st[1] = 0;
+    *reinterpret_cast<int *>(base + lay.bad) = 0;
+  }
+  double2 *twx = reinterpret_cast<double2 *>(base + lay.twx), *twy = reinterpret_cast<double2 *>(base + lay.twy);
+  double *lamx = reinterpret_cast<double *>(base + lay.lamx), *lamy = reinterpret_cast<double *>(base + lay.lamy);
+  const double rx = 1.0 / (h.dx * h.dx), ry = 1.0 / (h.dy * h.dy);
+  for (int m = tid; m < h.nx; m += nth) {
+    const double a = __ddiv_rn(__dmul_rn(-2.0 * M_PI, (double)m), (double)h.nx);
+    twx[m] = make_double2(cos(a), sin(a));
+    const double sn = sin(__ddiv_rn(__dmul_rn(M_PI, (double)m), (double)h.nx));
+    lamx[m] = -4.0 * sn * sn * rx;
+  }
+  for (int m = tid; m < h.ny; m += nth) {
+    const double a = __ddiv_rn(__dmul_rn(-2.0 * M_PI, (double)m), (double)h.ny);
+    twy[m] = make_double2(cos(a), sin(a));
+    const double sn = sin(__ddiv_rn(__dmul_rn(M_PI, (double)m), (double)h.ny));
+    lamy[m] = -4.0 * sn * sn * ry;
+  }
+  double *Ab = reinterpret_cast<double *>(base + lay.Ab), *At = reinterpret_cast<double *>(base + lay.At);
+  double *dzc = reinterpret_cast<double *>(base + lay.dzc), *dzf = reinterpret_cast<double *>(base + lay.dzf);
+  auto zW = [&](int k) { return __dmul_rn((double)k, h.dz); };
+  auto zP = [&](int k) { return __dmul_rn(__dadd_rn(zW(k - 1), zW(k)), 0.5); };
+  for (int k = tid; k <= h.nz + 1; k += nth) {
+    double ab = 0, at = 0, c = 0, f = 0;
+    if (k >= 1 && k <= h.nz) {
+      const double w = __dsub_rn(zW(k), zW(k - 1));
+      ab = 1.0 / __dmul_rn(__dsub_rn(zP(k), zP(k - 1)), w);
+      at = 1.0 / __dmul_rn(__dsub_rn(zP(k + 1), zP(k)), w);
+      c = w;
+      f = __dsub_rn(zP(k + 1), zP(k));
+      if (!h.zper && k == 1) ab = 0;
+      if (!h.zper && k == h.nz) at = 0;
+    }
+    Ab[k] = ab; At[k] = at; dzc[k] = c; dzf[k] = f;
+  }
+}
+
+static std::mutex noalloc_mu;
+static unsigned char *noalloc_base[64];  // device address of noalloc_scratch, per device
+static int noalloc_optin[64], noalloc_nsm[64];
+
+// Once per device, with that device current: the device address of the
+// scratch array (host code only holds a stand-in for it) and the kernels'
+// shared-memory limit.  Later calls only read what this stored.
+static int noalloc_setup(int device) {
+  std::lock_guard<std::mutex> lock(noalloc_mu);
+  if (noalloc_base[device]) return ELMM_OK;
+  unsigned char *ptr = nullptr;
+  CU(cudaGetSymbolAddress((void **)&ptr, noalloc_scratch));
+  int optin = 0, nsm = 0;
+  CU(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+  CU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+  CU(cudaFuncSetAttribute(k_fftx_fwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  CU(cudaFuncSetAttribute(k_fftx_inv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  CU(cudaFuncSetAttribute(k_ffty<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  CU(cudaFuncSetAttribute(k_tri<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  noalloc_optin[device] = optin;
+  noalloc_nsm[device] = nsm;
+  noalloc_base[device] = ptr;
+  return ELMM_OK;
+}
+
+extern "C" int elmm_poisson_solve_noalloc(const int32_t n[3], const double L[3], const int32_t bcs[6], int32_t device,
+                                          double *Phi, const double *RHS, void *stream) {
+  if (!n || !L || !bcs || !Phi || !RHS) return fail(ELMM_ERR_INVALID_ARG, "NULL argument");
+  // the same problem as elmm_poisson_solver_new (uniform z)
+  elmm_config c;
+  elmm_config_defaults(&c, n[0], n[1], n[2]);
+  for (int s = 0; s < 6; s++) {
+    if (bcs[s] != ELMM_BC_PERIODIC && bcs[s] != ELMM_BC_NEUMANN)
+      return fail(ELMM_ERR_INVALID_CONFIG, "Poisson BCs must be periodic or staggered Neumann");
+    c.Btype[s] = bcs[s];
+  }
+  c.dxmin = L[0] / n[0];
+  c.dymin = L[1] / n[1];
+  c.dzmin = L[2] / n[2];
+  c.sgstype = 0;
+  c.wallmodeltype = 0;
+  c.precision = ELMM_PREC_FP64;
+  c.device = device;
+  int r = check_config(c);
+  if (r) return r;
+  const int nx = n[0], ny = n[1], nz = n[2];
+  const int aln = 128 / (int)sizeof(double);
+  const int pitch = round_up(aln + nx + 1, aln);
+  const long long plane = (long long)pitch * (ny + 2);
+  const int nxh = nx / 2 + 1, spitch = round_up(nxh, TyOf<double>::v);
+  const size_t box_elems = (size_t)plane * (nz + 2) + 2 * (size_t)pitch + 64;
+  const NoAllocLayout lay = noalloc_layout(nx, ny, nz, box_elems, (size_t)nz * ny * spitch);
+  if (lay.total > ELMM_NOALLOC_SCRATCH_BYTES)
+    return fail(ELMM_ERR_INVALID_ARG, "elmm_poisson_solve_noalloc: a " + std::to_string(nx) + "x" + std::to_string(ny) +
+                                          "x" + std::to_string(nz) + " grid needs " + std::to_string(lay.total) +
+                                          " bytes of scratch, more than the fixed " +
+                                          std::to_string((size_t)ELMM_NOALLOC_SCRATCH_BYTES) + " bytes");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev || device >= 64)
+    return fail(ELMM_ERR_INVALID_ARG, "no CUDA device " + std::to_string(device));
+  CU(cudaSetDevice(device));
+  if ((r = noalloc_setup(device))) return r;
+  unsigned char *base = noalloc_base[device];
+  const size_t smem_x = sizeof(double2) * 2 * (kRowsX / 2) * nx, smem_y = sizeof(double2) * 2 * TyOf<double>::v * ny;
+  const int zper = bcs[ELMM_BO] == ELMM_BC_PERIODIC;
+  const size_t smem_tri = sizeof(double) * kTriThreads * nz * (zper ? 2 : 1);
+  const size_t optin = (size_t)noalloc_optin[device];
+  if (smem_x > optin || smem_y > optin || smem_tri > optin)
+    return fail(ELMM_ERR_INVALID_CONFIG, "grid too large for the shared-memory transforms");
+
+  Dom<double> h;
+  memset(&h, 0, sizeof(h));
+  h.nx = nx; h.ny = ny; h.nz = nz;
+  h.aln = aln; h.pitch = pitch; h.plane = plane;
+  for (int s = 0; s < 6; s++) h.bt[s] = bcs[s];
+  h.dx = c.dxmin; h.dy = c.dymin; h.dz = c.dzmin;
+  h.dt = 1.0;
+  h.zper = zper;
+  h.nxh = nxh; h.spitch = spitch;
+  h.Phi = reinterpret_cast<double *>(base + lay.box);
+  h.S = reinterpret_cast<double2 *>(base + lay.S);
+  h.twx = reinterpret_cast<const double2 *>(base + lay.twx);
+  h.twy = reinterpret_cast<const double2 *>(base + lay.twy);
+  h.lamx = reinterpret_cast<const double *>(base + lay.lamx);
+  h.lamy = reinterpret_cast<const double *>(base + lay.lamy);
+  h.Ab = reinterpret_cast<const double *>(base + lay.Ab);
+  h.At = reinterpret_cast<const double *>(base + lay.At);
+  h.dzc = reinterpret_cast<const double *>(base + lay.dzc);
+  h.dzf = reinterpret_cast<const double *>(base + lay.dzf);
+  PoisPlan pl;
+  factorize(nx, pl.fx);
+  factorize(ny, pl.fy);
+  const Dom<double> *ddom = reinterpret_cast<const Dom<double> *>(base + lay.dom);
+  const PoisPlan *dplan = reinterpret_cast<const PoisPlan *>(base + lay.plan);
+  const int *starts = reinterpret_cast<const int *>(base + lay.starts);
+  int *bad = reinterpret_cast<int *>(base + lay.bad);
+  const int nsm = noalloc_nsm[device];
+  auto blocks = [&](const void *f, int threads, size_t smem, int total) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, threads, smem) != cudaSuccess || b < 1) b = 1;
+    return std::max(1, std::min(total, b * nsm));
+  };
+  const Launch rows{starts, 1, (ny * nz + kRowsX - 1) / kRowsX};
+  const Launch ycols{starts, 1, ((nxh + TyOf<double>::v - 1) / TyOf<double>::v) * nz};
+  const Launch tri{starts, 1, (ny * spitch + kTriThreads - 1) / kTriThreads};
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int gset = std::max(1, std::min(64, (std::max(std::max(nx, ny), nz + 2) + 255) / 256));
+  k_noalloc_setup<<<gset, 256, 0, st>>>(h, pl, lay, base);
+  k_unpack<double><<<256, 256, 0, st>>>(ddom, h.Phi, RHS, HostBox{0, nx + 2, ny + 2, nz + 2}, nx, ny, nz, bad);
+  k_fftx_fwd<double><<<blocks((const void *)k_fftx_fwd<double>, kFFTThreads, smem_x, rows.total), kFFTThreads, smem_x,
+                       st>>>(ddom, rows, dplan, 1.0, 0, 1, 0);
+  const int gy = blocks((const void *)k_ffty<double>, kFFTThreads, smem_y, ycols.total);
+  k_ffty<double><<<gy, kFFTThreads, smem_y, st>>>(ddom, ycols, dplan, 0, 0);
+  k_tri<double><<<blocks((const void *)k_tri<double>, kTriThreads, smem_tri, tri.total), kTriThreads, smem_tri, st>>>(
+      ddom, tri, 0);
+  k_ffty<double><<<gy, kFFTThreads, smem_y, st>>>(ddom, ycols, dplan, 1, 0);
+  k_fftx_inv<double><<<blocks((const void *)k_fftx_inv<double>, kFFTThreads, smem_x, rows.total), kFFTThreads, smem_x,
+                       st>>>(ddom, rows, dplan, 0);
+  k_pack_scalar<double><<<256, 256, 0, st>>>(ddom, h.Phi, Phi, HostBox{-1, nx + 4, ny + 4, nz + 4}, 0, 0, nx, ny, nz);
+  CU(cudaGetLastError());
+  return ELMM_OK;
+}

@@ -200,6 +200,41 @@ int elmm_poisson_solver_execute(elmm_poisson *s, double *Phi, const double *RHS)
 int elmm_poisson_solver_finalize(elmm_poisson *s);
 
 /*
+ * No counterpart in the reference.  The solve of elmm_poisson_solver_execute
+ * (FP64, uniform z grid) on arrays that are already in device memory,
+ * without allocating anything.  It is meant for callers that cannot call
+ * cudaMalloc: a host whose memory pool already owns the GPU's memory (a
+ * CUDA Fortran or OpenACC program, or a framework's caching allocator, that
+ * reserved it up front), and a caller on a path where cudaMalloc/cudaFree
+ * would synchronise the whole device.
+ *
+ * Its working memory (spectral buffer, box copy of Phi, FFT tables and
+ * descriptors) is one fixed array of ELMM_NOALLOC_SCRATCH_BYTES in the
+ * library's device image: every GPU that loads the library holds those
+ * 16 MiB until the process exits.  That covers grids up to about 64x64x64
+ * or 128x128x48; a grid needing more is rejected with ELMM_ERR_INVALID_ARG
+ * and a message giving the bytes it needs.  The caller still owns the input
+ * and the output:
+ *   RHS  device pointer, RHS(0:nx+1,0:ny+1,0:nz+1), interior read
+ *   Phi  device pointer, Phi(-1:nx+2,-1:ny+2,-1:nz+2), interior written,
+ *        ghosts untouched
+ * n, L and bcs mean what they mean for elmm_poisson_solver_new.  The call
+ * makes `device` current and enqueues its work on `stream` (a cudaStream_t;
+ * NULL is the legacy default stream), then returns: Phi is ready once the
+ * stream gets there.  Non-finite RHS values are not reported.
+ *
+ * The first call on a device does a one-time set-up (it looks up the
+ * array's device address and raises the kernels' shared-memory limit), so
+ * make that first call before any stream capture.  Every call shares the
+ * one array: calls whose work overlaps on the GPU (two streams, or two host
+ * threads on one device) race and give wrong results, so order them on one
+ * stream or with events.
+ */
+#define ELMM_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
+int elmm_poisson_solve_noalloc(const int32_t n[3], const double L[3], const int32_t bcs[6],
+                               int32_t device, double *Phi, const double *RHS, void *stream);
+
+/*
  * Batched ensemble: n independent domains of uneven sizes stepped together.
  * Every kernel of a stage runs once for the whole batch over a device table of
  * domains; each RK3 step is one captured CUDA graph.
