@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <initializer_list>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -189,7 +190,7 @@ struct LaunchSet {
   Launch l() const { return Launch{starts, nd, total}; }
 };
 
-enum { LK_CELLS = 0, LK_BOX, LK_ROWS, LK_YCOLS, LK_TRI, LK_MOM, LK_N };
+enum { LK_CELLS = 0, LK_BOX, LK_ROWS, LK_YCOLS, LK_TRI, LK_MOM, LK_SHELL, LK_N };
 
 // -------------------------------------------------------------------- batch
 template <typename T>
@@ -343,6 +344,7 @@ struct BatchT {
     grid_cap[6] = cap((const void *)k_project<T>, MX * MY, 0);
     grid_cap[7] = cap((const void *)k_divres<T>, TX * TY, 0);
     grid_cap[8] = cap((const void *)k_cfl<T>, TX * TY, 0);
+    grid_cap[9] = cap((const void *)k_ghosts<T>, kShellThreads, 0);
     // staging for host-layout copies
     stage_elems = 0;
     for (int d = 0; d < n; d++) {
@@ -364,6 +366,7 @@ struct BatchT {
       case LK_ROWS: return (h.ny * h.nz + kRowsX - 1) / kRowsX;
       case LK_YCOLS: return ((h.nxh + TyOf<T>::v - 1) / TyOf<T>::v) * h.nz;
       case LK_MOM: return ((h.nx + MX - 1) / MX) * ((h.ny + MY - 1) / MY) * ((h.nz + MKC - 1) / MKC);
+      case LK_SHELL: return (int)((shell_cells(h.nx, h.ny, h.nz) + kShellThreads - 1) / kShellThreads);
       default: return (h.ny * h.spitch + kTriThreads - 1) / kTriThreads;
     }
   }
@@ -523,27 +526,39 @@ struct BatchT {
   int gsz(int which, int total) const { return std::max(1, std::min(total, grid_cap[which])); }
 
   // ------------------------------------------------------------ stages
+  // ghost shells of the listed fields after the kernel that wrote them
+  void launch_ghosts(std::initializer_list<int> fields, int gate) {
+    unsigned packed = 0;
+    int nf = 0;
+    for (int f : fields) packed |= (unsigned)f << (8 * nf++);
+    k_ghosts<T><<<gsz(9, ls[LK_SHELL].total * nf), kShellThreads, 0, stream>>>(ddom, ls[LK_SHELL].l(), packed, nf,
+                                                                                 gate);
+  }
   int launch_sgs() {
-    nlaunch++;
+    nlaunch += 2;
     k_sgs<T><<<gsz(0, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l());
+    launch_ghosts({F_NU}, 0);
     return ELMM_OK;
   }
   int launch_momentum(int stage) {
     StageCoef sc{kRho[stage - 1], kBeta[stage - 1], 2 * kAlpha[stage - 1], stage};
-    nlaunch++;
+    nlaunch += 2;
     k_momentum<T><<<gsz(1, ls[LK_MOM].total), MX * MY, smem_mom, stream>>>(ddom, ls[LK_MOM].l(), sc);
+    launch_ghosts({F_U2, F_V2, F_W2}, 0);
     return ELMM_OK;
   }
   // PressureCorrection on U2 (in_place = 0) or on U itself (initial projection)
   int launch_projection(double coef_alpha2, int use_dt, int in_place) {
-    nlaunch += 7;
+    nlaunch += 9;
     launch_poisson(coef_alpha2, use_dt, 0, 0);
     k_project<T><<<gsz(6, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l(), coef_alpha2, use_dt,
                                                                    in_place, 0);
+    launch_ghosts({F_U, F_V, F_W, F_P}, 0);
     k_prref<T><<<std::min(nd, 1024), 256, 0, stream>>>(ddom, nd, 0);
     return ELMM_OK;
   }
-  // the five transform kernels; rhs_from_phi: the right-hand side is in Phi
+  // the five transform kernels and the ghosts of Phi; rhs_from_phi: the
+  // right-hand side is in Phi
   void launch_poisson(double coef_alpha2, int use_dt, int rhs_from_phi, int gate) {
     k_fftx_fwd<T><<<gsz(2, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan, coef_alpha2,
                                                                                 use_dt, rhs_from_phi, gate);
@@ -551,6 +566,7 @@ struct BatchT {
     k_tri<T><<<gsz(4, ls[LK_TRI].total), kTriThreads, smem_tri, stream>>>(ddom, ls[LK_TRI].l(), gate);
     k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), kFFTThreads, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, 1, gate);
     k_fftx_inv<T><<<gsz(5, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan, gate);
+    launch_ghosts({F_PHI}, gate);
   }
   int max_refine() const {
     int m = 0;
@@ -571,9 +587,10 @@ struct BatchT {
       k_refine_decide<T><<<(nd + 127) / 128, 128, 0, stream>>>(ddom, nd, sw == 0);
       launch_poisson(coef_alpha2, use_dt, 1, 1);
       k_project<T><<<gsz(6, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l(), coef_alpha2, use_dt, 1, 1);
+      launch_ghosts({F_U, F_V, F_W, F_P}, 1);
       k_prref<T><<<std::min(nd, 1024), 256, 0, stream>>>(ddom, nd, 1);
       k_divres<T><<<gsz(7, ls[LK_CELLS].total), TX * TY, 0, stream>>>(ddom, ls[LK_CELLS].l(), 1);
-      nlaunch += 10;
+      nlaunch += 12;
     }
   }
   int launch_divmax() {
@@ -696,42 +713,47 @@ struct BatchT {
     return fill_stats(st, 0);
   }
 
-  // per-kernel timing of one stage (CUDA events on the launching stream)
+  // per-kernel timing of one stage (CUDA events on the launching stream);
+  // the ghost-shell launches of the stage are summed into the last slot
   int profile_stage(int stage, int reps, double *ms) {
     CU(cudaSetDevice(device));
     const int nk = ELMM_NKERNELS;
-    std::vector<cudaEvent_t> ev(nk + 1);
+    const int kGhost = nk - 1, nev = 2 * (nk + 3);
+    std::vector<cudaEvent_t> ev(nev);
     for (auto &e : ev) CU(cudaEventCreate(&e));
     std::vector<double> acc(nk, 0.0);
+    std::vector<int> slot;
     const double a2 = 2 * kAlpha[stage - 1];
     StageCoef sc{kRho[stage - 1], kBeta[stage - 1], a2, stage};
     for (int r = 0; r < reps; r++) {
-      int q = 0;
-      CU(cudaEventRecord(ev[q++], stream));
-      k_sgs<T><<<gsz(0, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l());
-      CU(cudaEventRecord(ev[q++], stream));
-      k_momentum<T><<<gsz(1, ls[LK_MOM].total), MX * MY, smem_mom, stream>>>(ddom, ls[LK_MOM].l(), sc);
-      CU(cudaEventRecord(ev[q++], stream));
-      k_fftx_fwd<T><<<gsz(2, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan, a2, 1, 0, 0);
-      CU(cudaEventRecord(ev[q++], stream));
-      k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), kFFTThreads, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, 0, 0);
-      CU(cudaEventRecord(ev[q++], stream));
-      k_tri<T><<<gsz(4, ls[LK_TRI].total), kTriThreads, smem_tri, stream>>>(ddom, ls[LK_TRI].l(), 0);
-      CU(cudaEventRecord(ev[q++], stream));
-      k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), kFFTThreads, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, 1, 0);
-      CU(cudaEventRecord(ev[q++], stream));
-      k_fftx_inv<T><<<gsz(5, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan, 0);
-      CU(cudaEventRecord(ev[q++], stream));
-      k_project<T><<<gsz(6, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l(), a2, 1, 0, 0);
-      CU(cudaEventRecord(ev[q++], stream));
-      k_prref<T><<<std::min(nd, 1024), 256, 0, stream>>>(ddom, nd, 0);
-      CU(cudaEventRecord(ev[q++], stream));
+      slot.clear();
+      auto timed = [&](int k, auto launch) {
+        cudaEventRecord(ev[2 * slot.size()], stream);
+        launch();
+        cudaEventRecord(ev[2 * slot.size() + 1], stream);
+        slot.push_back(k);
+      };
+      timed(0, [&] { k_sgs<T><<<gsz(0, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l()); });
+      timed(kGhost, [&] { launch_ghosts({F_NU}, 0); });
+      timed(1, [&] { k_momentum<T><<<gsz(1, ls[LK_MOM].total), MX * MY, smem_mom, stream>>>(ddom, ls[LK_MOM].l(), sc); });
+      timed(kGhost, [&] { launch_ghosts({F_U2, F_V2, F_W2}, 0); });
+      timed(2, [&] {
+        k_fftx_fwd<T><<<gsz(2, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan, a2, 1, 0, 0);
+      });
+      timed(3, [&] { k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), kFFTThreads, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, 0, 0); });
+      timed(4, [&] { k_tri<T><<<gsz(4, ls[LK_TRI].total), kTriThreads, smem_tri, stream>>>(ddom, ls[LK_TRI].l(), 0); });
+      timed(5, [&] { k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), kFFTThreads, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, 1, 0); });
+      timed(6, [&] { k_fftx_inv<T><<<gsz(5, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan, 0); });
+      timed(kGhost, [&] { launch_ghosts({F_PHI}, 0); });
+      timed(7, [&] { k_project<T><<<gsz(6, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l(), a2, 1, 0, 0); });
+      timed(kGhost, [&] { launch_ghosts({F_U, F_V, F_W, F_P}, 0); });
+      timed(8, [&] { k_prref<T><<<std::min(nd, 1024), 256, 0, stream>>>(ddom, nd, 0); });
       CU(cudaStreamSynchronize(stream));
       CU(cudaGetLastError());
-      for (int k = 0; k < nk; k++) {
+      for (size_t q = 0; q < slot.size(); q++) {
         float t = 0;
-        CU(cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
-        acc[k] += t;
+        CU(cudaEventElapsedTime(&t, ev[2 * q], ev[2 * q + 1]));
+        acc[slot[q]] += t;
       }
     }
     for (auto &e : ev) cudaEventDestroy(e);

@@ -6,8 +6,8 @@
 
 namespace elmm {
 
-// inverse real FFT along x of kRowsX rows -> Phi(1:nx) with its ghosts
-// (Bound_Phi, src/boundaries.f90:1817-1948, one cell deep).
+// inverse real FFT along x of kRowsX rows -> interior of Phi (its ghosts are
+// filled afterwards by k_ghosts)
 template <typename T>
 __global__ void __launch_bounds__(kFFTThreads) k_fftx_inv(const Dom<T> *__restrict__ doms, Launch L,
                                                   const PoisPlan *__restrict__ plans, int gate) {
@@ -46,7 +46,6 @@ __global__ void __launch_bounds__(kFFTThreads) k_fftx_inv(const Dom<T> *__restri
     }
     __syncthreads();
     T2 *res = fft_block<T, T2>(buf0, buf1, ntr, pl.fx, d.twx, true);
-    const bool px = d.bt[SIDE_WE] == BC_PERIODIC, py = d.bt[SIDE_SO] == BC_PERIODIC, pz = d.bt[SIDE_BO] == BC_PERIODIC;
 #pragma unroll 4
     for (int w = threadIdx.x; w < kRowsX * N; w += blockDim.x) {
       const int r = w / N, i = w - r * N + 1;
@@ -54,12 +53,7 @@ __global__ void __launch_bounds__(kFFTThreads) k_fftx_inv(const Dom<T> *__restri
       if (row >= nrows) continue;
       const int j = row % d.ny + 1, k = row / d.ny + 1;
       const T2 z = res[(r >> 1) * N + i - 1];
-      const T v = (r & 1) ? z.y : z.x;
-      d.Phi[bidx(d, i, j, k)] = v;
-      if (i == 1 || i == d.nx || j == 1 || j == d.ny || k == 1 || k == d.nz) {
-        Images ix = images_rep(i, d.nx, px), iy = images_rep(j, d.ny, py), iz = images_rep(k, d.nz, pz);
-        push_ghosts(d, d.Phi, ix, iy, iz, v);
-      }
+      d.Phi[bidx(d, i, j, k)] = (r & 1) ? z.y : z.x;
     }
     __syncthreads();
   }
@@ -100,7 +94,6 @@ __global__ void __launch_bounds__(MX *MY) k_project(const Dom<T> *__restrict__ d
     const bool hv = inside && i <= d.ext[1][0] && j <= d.ext[1][1];
     const bool hw = inside && i <= d.ext[2][0] && j <= d.ext[2][1];
     const T m = (T)(*d.prm);
-    const bool px = d.bt[SIDE_WE] == BC_PERIODIC, py = d.bt[SIDE_SO] == BC_PERIODIC, pz = d.bt[SIDE_BO] == BC_PERIODIC;
     long long c = bidx(d, inside ? i : 1, inside ? j : 1, k0);
     T phi = 0, pe = 0, pn = 0, pt = 0, u0 = 0, v0 = 0, w0 = 0, p0 = 0;
     if (inside) {
@@ -126,26 +119,19 @@ __global__ void __launch_bounds__(MX *MY) k_project(const Dom<T> *__restrict__ d
         if (hu && k <= d.ext[0][2]) {
           T u = u0 - Au * (pe - phi);
           d.U[c] = u;
-          push_vel(d, d.U, 0, i, j, k, u);
         }
         if (hv && k <= d.ext[1][2]) {
           T v = v0 - Av * (pn - phi);
           d.V[c] = v;
-          push_vel(d, d.V, 1, i, j, k, v);
         }
         if (hw && k <= d.ext[2][2]) {
           T w;
           if (d.vz) w = w0 - dt2 * (pt - phi) / (T)d.dzW[k + 2];
           else w = w0 - Aw * (pt - phi);
           d.W[c] = w;
-          push_vel(d, d.W, 2, i, j, k, w);
         }
         T p = (p0 - m) + phi;
         P[c] = p;
-        if (i == 1 || i == nx || j == 1 || j == ny || k == 1 || k == nz) {
-          Images ix = images_per(i, nx, px), iy = images_per(j, ny, py), iz = images_per(k, nz, pz);
-          push_ghosts(d, P, ix, iy, iz, p);
-        }
         top = (double)p;
       }
       if (k == nz) {  // block-uniform: the top layer's partial sum of this column
@@ -185,6 +171,94 @@ __global__ void k_prref(const Dom<T> *__restrict__ doms, int nd, int gate) {
       *d.prm = tot / ((double)d.nx * (double)d.ny);
     }
     __syncthreads();
+  }
+}
+
+// Ghost shell of up to four box fields, pulled from the interior after the
+// kernel that wrote it: every one-deep ghost cell takes the value of the
+// interior cell it folds onto.  Velocities follow BoundUVW
+// (src/boundaries.f90:398-1791; the sequential x, y, z passes there make the
+// fold a product of per-dimension folds), viscosity and Phi a periodic or
+// adjacent-cell copy (src/scalarboundaries.f90:326-431,
+// src/boundaries.f90:1817-1948), and the pressure only its periodic copies
+// (its other ghosts are never read before the next Bound_Pr).
+// fields: up to four field ids (F_*), one per byte; the grid covers
+// L.total shell tiles of kShellThreads cells per field.
+constexpr int kShellThreads = 256;
+
+template <typename T>
+__device__ __forceinline__ T *box_field(const Dom<T> &d, int f) {
+  switch (f) {
+    case F_U: return d.U;
+    case F_V: return d.V;
+    case F_W: return d.W;
+    case F_U2: return d.U2;
+    case F_V2: return d.V2;
+    case F_W2: return d.W2;
+    case F_P: return d.P;
+    case F_NU: return d.nu;
+    default: return d.Phi;
+  }
+}
+
+// cells of the one-deep shell around an ex x ey x ez interior
+__host__ __device__ __forceinline__ long long shell_cells(int ex, int ey, int ez) {
+  return 2LL * (ex + 2) * (ey + 2) + 2LL * (ex + 2) * ez + 2LL * ey * ez;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kShellThreads) k_ghosts(const Dom<T> *__restrict__ doms, Launch L, unsigned fields,
+                                                          int nf, int gate) {
+  const long long nblk = (long long)L.total * nf;
+  for (long long b = blockIdx.x; b < nblk; b += gridDim.x) {
+    const int f = (int)(b / L.total), t = (int)(b - (long long)f * L.total);
+    const int di = find_dom(L.starts, L.nd, t);
+    const Dom<T> &d = doms[di];
+    if (gate && !*d.refine_flag) continue;
+    const int fid = (fields >> (8 * f)) & 0xff;
+    const bool vel = fid <= F_W2;
+    const int comp = fid % 3;
+    const int ex = vel ? d.ext[comp][0] : d.nx, ey = vel ? d.ext[comp][1] : d.ny, ez = vel ? d.ext[comp][2] : d.nz;
+    long long w = (long long)(t - __ldg(L.starts + di)) * kShellThreads + threadIdx.x;
+    if (w >= shell_cells(ex, ey, ez)) continue;
+    // z faces (full planes), then y faces (k in 1..ez), then x faces
+    int i, j, k;
+    const long long zf = (long long)(ex + 2) * (ey + 2), yf = (long long)(ex + 2) * ez, xf = (long long)ey * ez;
+    if (w < 2 * zf) {
+      const int side = w >= zf;
+      w -= side * zf;
+      i = (int)(w % (ex + 2)); j = (int)(w / (ex + 2)); k = side ? ez + 1 : 0;
+    } else if ((w -= 2 * zf) < 2 * yf) {
+      const int side = w >= yf;
+      w -= side * yf;
+      i = (int)(w % (ex + 2)); k = (int)(w / (ex + 2)) + 1; j = side ? ey + 1 : 0;
+    } else {
+      w -= 2 * yf;
+      const int side = w >= xf;
+      w -= side * xf;
+      j = (int)(w % ey) + 1; k = (int)(w / ey) + 1; i = side ? ex + 1 : 0;
+    }
+    T *F = box_field(d, fid);
+    const bool per[3] = {d.bt[SIDE_WE] == BC_PERIODIC, d.bt[SIDE_SO] == BC_PERIODIC, d.bt[SIDE_BO] == BC_PERIODIC};
+    T v;
+    if (vel) {
+      const Fold fx = fold_vel(i, ex, d.bt[0], d.bt[1], comp == 0);
+      const Fold fy = fold_vel(j, ey, d.bt[2], d.bt[3], comp == 1);
+      const Fold fz = fold_vel(k, ez, d.bt[4], d.bt[5], comp == 2);
+      if (fx.zero | fy.zero | fz.zero) {
+        v = (T)0;
+      } else {
+        v = F[bidx(d, fx.src, fy.src, fz.src)];
+        if (fx.sign * fy.sign * fz.sign < 0) v = -v;
+      }
+    } else if (fid == F_P) {
+      const bool gx = i < 1 || i > ex, gy = j < 1 || j > ey, gz = k < 1 || k > ez;
+      if ((gx && !per[0]) || (gy && !per[1]) || (gz && !per[2])) continue;
+      v = F[bidx(d, fold_rep(i, ex, true), fold_rep(j, ey, true), fold_rep(k, ez, true))];
+    } else {
+      v = F[bidx(d, fold_rep(i, ex, per[0]), fold_rep(j, ey, per[1]), fold_rep(k, ez, per[2]))];
+    }
+    F[bidx(d, i, j, k)] = v;
   }
 }
 

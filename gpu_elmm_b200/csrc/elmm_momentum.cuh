@@ -424,11 +424,10 @@ __global__ void __launch_bounds__(MX *MY, 2) k_momentum(const Dom<T> *__restrict
     const int o = (ty + 1) * Lay::SPW + (tx + Lay::XO);
     long long c = bidx(d, inside ? i : 1, inside ? j : 1, k0);
     // block-uniform: only tiles on a side of the box and the planes next to
-    // the bottom and top have ghost images or wall-model corrections
+    // the bottom and top have wall-model corrections
     const int nz = d.nz;
     // a component's last index is n or n-1 (src/initial.f90:871-896)
     const bool xlo = i0 == 1, xhi = i0 + MX - 1 >= nx - 1, ylo = j0 == 1, yhi = j0 + MY - 1 >= ny - 1;
-    const bool edge_tile = xlo || xhi || ylo || yhi;
     int wmask = 0;
     for (int f = 0; f < 6; f++) wmask |= d.wall[f] ? (1 << f) : 0;
     const int wtile = wmask & ((xlo ? 1 : 0) | (xhi ? 2 : 0) | (ylo ? 4 : 0) | (yhi ? 8 : 0));
@@ -441,7 +440,6 @@ __global__ void __launch_bounds__(MX *MY, 2) k_momentum(const Dom<T> *__restrict
         phase ^= 1u << s2;
       }
       if (!ok) { abort_flag = 1; d.flags[1] = 1; }
-      const bool edge = edge_tile || k <= 1 || k >= nz - 1;
       const int wallhere = wtile | (wmask & ((k == 1 ? 16 : 0) | (k >= nz - 1 ? 32 : 0)));
       if (inside && ok) {
         WideRing<T, 5, 3> R;
@@ -460,7 +458,6 @@ __global__ void __launch_bounds__(MX *MY, 2) k_momentum(const Dom<T> *__restrict
           u2 = u2 + gx * ((R.g(4, 1, 0, 0) - m) - p0);
           u2 = u2 + R.g(0, 0, 0, 0);
           U2o[c] = u2;
-          if (edge) push_vel(d, U2o, 0, i, j, k, u2);
         }
         if (hasV && k <= kV) {
           T ts = tendency<T, 1>(ctx, R, i, j, k, wallhere);
@@ -471,7 +468,6 @@ __global__ void __launch_bounds__(MX *MY, 2) k_momentum(const Dom<T> *__restrict
           v2 = v2 + gy * ((R.g(4, 0, 1, 0) - m) - p0);
           v2 = v2 + R.g(1, 0, 0, 0);
           V2o[c] = v2;
-          if (edge) push_vel(d, V2o, 1, i, j, k, v2);
         }
         if (hasW && k <= kW) {
           T ts = tendency<T, 2>(ctx, R, i, j, k, wallhere);
@@ -483,7 +479,6 @@ __global__ void __launch_bounds__(MX *MY, 2) k_momentum(const Dom<T> *__restrict
           else w2 = w2 + gz * dpz;
           w2 = w2 + R.g(2, 0, 0, 0);
           W2o[c] = w2;
-          if (edge) push_vel(d, W2o, 2, i, j, k, w2);
         }
       }
       __syncthreads();  // plane k-1 is no longer read
@@ -512,9 +507,10 @@ __global__ void __launch_bounds__(MX *MY, 2) k_momentum(const Dom<T> *__restrict
 // ---------------------------------------------------------------- k_sgs
 // SubgridStresses (src/dynamics.f90:869-908): Smagorinsky viscosity
 // (SGS_Smag / NuSmag / StrainIJ, src/subgrid.f90:30-67, :170-209) from a
-// ring of U, V, W planes; each cell also writes the ghost cells that fold
-// onto it (BoundViscosity, src/scalarboundaries.f90:326-431).  Cells next to
-// a wall-model side compute the wall fluxes of the velocity points there.
+// ring of U, V, W planes (the ghosts of BoundViscosity,
+// src/scalarboundaries.f90:326-431, are filled afterwards by k_ghosts).
+// Cells next to a wall-model side compute the wall fluxes of the velocity
+// points there.
 template <typename T>
 struct SgsK {  // factors of NuSmag at one level k
   T rdx, rdy, r4dx, r4dy, rdz, r2zz, wc2;
@@ -602,7 +598,6 @@ __global__ void __launch_bounds__(MX *MY, 3) k_sgs(const Dom<T> *__restrict__ do
     }
     __syncthreads();
     const bool inside = i <= nx && j <= ny;
-    const bool px = d.bt[SIDE_WE] == BC_PERIODIC, py = d.bt[SIDE_SO] == BC_PERIODIC, pz = d.bt[SIDE_BO] == BC_PERIODIC;
     const bool anywall = d.wall[0] | d.wall[1] | d.wall[2] | d.wall[3] | d.wall[4] | d.wall[5];
     const T num = (T)d.nu_mol;
     const bool sgs = d.sgs != 0, addmol = d.nu_mol > 0;
@@ -636,10 +631,6 @@ __global__ void __launch_bounds__(MX *MY, 3) k_sgs(const Dom<T> *__restrict__ do
         const long long c = bidx(d, i, j, k);
         nu[c] = v;
         const bool edge = i == 1 || i == nx || j == 1 || j == ny || k == 1 || k == nz;
-        if (edge) {
-          Images ix = images_rep(i, nx, px), iy = images_rep(j, ny, py), iz = images_rep(k, nz, pz);
-          push_ghosts(d, nu, ix, iy, iz, v);
-        }
         if (anywall && (edge || k == nz - 1 || i == nx - 1 || j == ny - 1)) {
 #pragma unroll 1
           for (int f = 0; f < 6; f++) {

@@ -20,7 +20,7 @@ _lib = None
 
 _dp = C.POINTER(C.c_double)
 
-KERNEL_NAMES = ("sgs", "momentum", "fftx_fwd", "ffty_fwd", "tri", "ffty_inv", "fftx_inv", "project", "prref")
+KERNEL_NAMES = ("sgs", "momentum", "fftx_fwd", "ffty_fwd", "tri", "ffty_inv", "fftx_inv", "project", "prref", "ghosts")
 KERNEL_COUNT = len(KERNEL_NAMES)
 
 

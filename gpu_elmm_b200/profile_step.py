@@ -1,0 +1,46 @@
+"""Runs the benchmark workload for a profiler: one channel domain (by default
+256 x 256 x 128, the same configuration and seeded state as bench.py), the
+initial projection, W warm-up steps and S profiled steps, then prints the
+device time of the steps and the per-kernel times of one stage.
+
+    python -m gpu_elmm_b200.profile_step [--precision mixed|fp64] [--n 256,256,128]
+                                         [--warmup 1] [--steps 1]
+
+Under `ncu -k regex:<kernel> -s <skip> -c <count>` the launches of the
+profiled steps follow those of the projection and the warm-up steps.
+"""
+import argparse
+import json
+
+from .config import grid_of, make_config
+from .workloads import log_profile_state
+from . import lib as L
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--n", default="256,256,128")
+    ap.add_argument("--warmup", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1)
+    ap.add_argument("--stage-times", action="store_true", help="also time each kernel of stage 2 (5 repetitions)")
+    a = ap.parse_args()
+    n = tuple(int(x) for x in a.n.split(","))
+    cfg = make_config(*n, precision=1 if a.precision == "mixed" else 0)
+    g = grid_of(cfg)
+    d = L.Domain(cfg)
+    d.upload(*log_profile_state(g, seed=0))
+    d.project(1.0)
+    if a.warmup:
+        d.step(a.warmup)
+    s = d.step(a.steps)
+    out = {"n": n, "precision": a.precision, "steps": a.steps, "ms_per_step": s.elapsed_ms / max(1, a.steps),
+           "max_div": s.max_div, "kernels_per_step": s.kernels / max(1, a.steps)}
+    if a.stage_times:
+        out["stage2_kernel_ms"] = d.profile_stage(2, 5)
+    print(json.dumps(out))
+    d.close()
+
+
+if __name__ == "__main__":
+    main()

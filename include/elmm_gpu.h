@@ -174,10 +174,11 @@ int elmm_run_stage(elmm_handle *h, int32_t stage, int32_t stop);
  * reference's per-part timers are src/tsteps.f90:113, :234-238): runs the
  * kernels of RK3 stage `stage` `reps` times on the handle's stream, each
  * bracketed by CUDA events, and writes the mean duration in ms of each
- * kernel kind to ms[ELMM_NKERNELS] in the order of ELMM_KERNEL_NAMES.  The
- * state advances as by `reps` stages. */
-#define ELMM_NKERNELS 9
-#define ELMM_KERNEL_NAMES "sgs,momentum,fftx_fwd,ffty_fwd,tri,ffty_inv,fftx_inv,project,prref"
+ * kernel kind to ms[ELMM_NKERNELS] in the order of ELMM_KERNEL_NAMES; "ghosts"
+ * is the sum of the stage's ghost-shell launches.  The state advances as by
+ * `reps` stages. */
+#define ELMM_NKERNELS 10
+#define ELMM_KERNEL_NAMES "sgs,momentum,fftx_fwd,ffty_fwd,tri,ffty_inv,fftx_inv,project,prref,ghosts"
 int elmm_profile_stage(elmm_handle *h, int32_t stage, int32_t reps, double *ms);
 
 /*
