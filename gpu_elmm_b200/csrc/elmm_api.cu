@@ -19,6 +19,7 @@
 
 #include "../../include/elmm_gpu.h"
 #include "elmm_kernels2.cuh"
+#include "elmm_poisson_reg.cuh"
 
 using namespace elmm;
 
@@ -190,7 +191,7 @@ struct LaunchSet {
   Launch l() const { return Launch{starts, nd, total}; }
 };
 
-enum { LK_CELLS = 0, LK_BOX, LK_ROWS, LK_YCOLS, LK_TRI, LK_MOM, LK_SHELL, LK_N };
+enum { LK_CELLS = 0, LK_BOX, LK_ROWS, LK_YCOLS, LK_TRI, LK_MOM, LK_SHELL, LK_XREG, LK_YREG, LK_TRIT, LK_N };
 
 // -------------------------------------------------------------------- batch
 template <typename T>
@@ -208,6 +209,16 @@ struct BatchT {
   std::vector<void *> allocs;
   LaunchSet ls[LK_N];
   size_t smem_x = 0, smem_y = 0, smem_tri = 0;
+  // register FFTs / tiled z solve when every domain of the batch allows them
+  bool reg_x = false, reg_y = false, tri_tile = false;
+  size_t smem_xr = 0, smem_yr = 0, smem_trit = 0;
+  struct RegSet {
+    const FFTRegKernels<T> *k = nullptr;
+    LaunchSet ls;
+    size_t smem = 0;
+    int cap_fwd = 1, cap_inv = 1;
+  };
+  std::vector<RegSet> xreg, yreg;
   size_t smem_mom = (size_t)kRingSlots * SlotLayout<T, 5, 3>::BYTES;
   int grid_cap[16];
   // host-layout staging (double), max over domains of the largest host array
@@ -328,6 +339,19 @@ struct BatchT {
     CU(cudaFuncSetAttribute(k_ffty<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     CU(cudaFuncSetAttribute(k_tri<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     CU(cudaFuncSetAttribute(k_momentum<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 1024));
+    for (auto &h : hdom) {
+      reg_x |= fft_reg_supported(h.nx);
+      reg_y |= fft_reg_supported(h.ny);
+      tri_tile |= tri_tiled(h);
+      if (fft_reg_supported(h.nx))
+        smem_xr = std::max(smem_xr, sizeof(T2) * fft_reg_batch(h.nx) * fft_reg_seq(h.nx));
+      if (fft_reg_supported(h.ny))
+        smem_yr = std::max(smem_yr, sizeof(T2) * fft_reg_batch(h.ny) * fft_reg_seq(h.ny));
+      if (tri_tiled(h)) smem_trit = std::max(smem_trit, tri_tile_smem<T>(h.nz));
+    }
+    if (smem_xr > (size_t)optin || smem_yr > (size_t)optin || smem_trit > (size_t)optin)
+      return fail(ELMM_ERR_INVALID_CONFIG, "shared memory of the register transforms exceeds the device limit");
+    CU(cudaFuncSetAttribute(k_tri_tile<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     int nsm = 0;
     CU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
     auto cap = [&](const void *f, int threads, size_t sm) {
@@ -345,6 +369,39 @@ struct BatchT {
     grid_cap[7] = cap((const void *)k_divres<T>, TX * TY, 0);
     grid_cap[8] = cap((const void *)k_cfl<T>, TX * TY, 0);
     grid_cap[9] = cap((const void *)k_ghosts<T>, kShellThreads, 0);
+    grid_cap[13] = cap((const void *)k_tri_tile<T>, kTriTileThreads, smem_trit);
+    // one launch set per distinct x (y) length, holding only its domains
+    auto reg_sets = [&](bool use, bool ydir, std::vector<RegSet> &out) -> int {
+      if (!use) return ELMM_OK;
+      std::vector<int> lens;
+      for (auto &h : hdom) {
+        const int n = ydir ? h.ny : h.nx;
+        if (fft_reg_supported(n) && std::find(lens.begin(), lens.end(), n) == lens.end()) lens.push_back(n);
+      }
+      for (int n : lens) {
+        RegSet r;
+        r.k = fft_reg_kernels<T>(n);
+        r.smem = sizeof(T2) * fft_reg_batch(n) * fft_reg_seq(n);
+        std::vector<int> st(nd + 1, 0);
+        for (int d = 0; d < nd; d++)
+          st[d + 1] = st[d] + ((ydir ? hdom[d].ny : hdom[d].nx) == n ? tiles(ydir ? LK_YREG : LK_XREG, hdom[d]) : 0);
+        r.ls.nd = nd;
+        r.ls.total = st[nd];
+        int rr = dalloc((void **)&r.ls.starts, sizeof(int) * (nd + 1));
+        if (rr) return rr;
+        CU(cudaMemcpy(r.ls.starts, st.data(), sizeof(int) * (nd + 1), cudaMemcpyHostToDevice));
+        const void *f1 = ydir ? (const void *)r.k->yf : (const void *)r.k->fwd;
+        const void *f2 = ydir ? (const void *)r.k->yi : (const void *)r.k->inv;
+        CU(cudaFuncSetAttribute(f1, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+        CU(cudaFuncSetAttribute(f2, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+        r.cap_fwd = cap(f1, kRegThreads, r.smem);
+        r.cap_inv = cap(f2, kRegThreads, r.smem);
+        out.push_back(r);
+      }
+      return ELMM_OK;
+    };
+    if ((r = reg_sets(reg_x, false, xreg))) return r;
+    if ((r = reg_sets(reg_y, true, yreg))) return r;
     // staging for host-layout copies
     stage_elems = 0;
     for (int d = 0; d < n; d++) {
@@ -358,16 +415,32 @@ struct BatchT {
     return ELMM_OK;
   }
 
+  // whether a domain's transforms / z solve use the register FFTs and the
+  // tiled Thomas kernel (decided per domain, so that a domain gives the same
+  // result alone and in any batch)
+  static bool tri_tiled(const Dom<T> &h) { return !h.zper && h.nz <= kTriTileMaxNz; }
+
   static int tiles(int kind, const Dom<T> &h) {
     int ntx = (h.nx + TX - 1) / TX, nty = (h.ny + TY - 1) / TY;
     switch (kind) {
       case LK_CELLS: return ntx * nty * h.nz;
       case LK_BOX: return ((h.nx + 2 + TX - 1) / TX) * ((h.ny + 2 + TY - 1) / TY) * (h.nz + 2);
-      case LK_ROWS: return (h.ny * h.nz + kRowsX - 1) / kRowsX;
-      case LK_YCOLS: return ((h.nxh + TyOf<T>::v - 1) / TyOf<T>::v) * h.nz;
+      case LK_ROWS: return fft_reg_supported(h.nx) ? 0 : (h.ny * h.nz + kRowsX - 1) / kRowsX;
+      case LK_YCOLS: return fft_reg_supported(h.ny) ? 0 : ((h.nxh + TyOf<T>::v - 1) / TyOf<T>::v) * h.nz;
       case LK_MOM: return ((h.nx + MX - 1) / MX) * ((h.ny + MY - 1) / MY) * ((h.nz + MKC - 1) / MKC);
       case LK_SHELL: return (int)((shell_cells(h.nx, h.ny, h.nz) + kShellThreads - 1) / kShellThreads);
-      default: return (h.ny * h.spitch + kTriThreads - 1) / kTriThreads;
+      case LK_XREG: {
+        if (!fft_reg_supported(h.nx)) return 0;
+        const int rows = 2 * fft_reg_batch(h.nx);
+        return (h.ny * h.nz + rows - 1) / rows;
+      }
+      case LK_YREG: {
+        if (!fft_reg_supported(h.ny)) return 0;
+        const int C = fft_reg_batch(h.ny);
+        return ((h.nxh + C - 1) / C) * h.nz;
+      }
+      case LK_TRIT: return tri_tiled(h) ? (h.ny * h.spitch + kTriCols - 1) / kTriCols : 0;
+      default: return tri_tiled(h) ? 0 : (h.ny * h.spitch + kTriThreads - 1) / kTriThreads;
     }
   }
 
@@ -472,6 +545,15 @@ struct BatchT {
     if ((r = upload_table(&h.At, At))) return r;
     if ((r = upload_table(&h.dzc, dzc))) return r;
     if ((r = upload_table(&h.dzf, dzf))) return r;
+    if (tri_tiled(h)) {  // reciprocal pivots of the tiled z solve, once per domain
+      const int ncol = h.ny * h.spitch;
+      double *iv;
+      if ((r = dalloc((void **)&iv, (size_t)h.nz * ncol * sizeof(double)))) return r;
+      k_tri_factors<<<(ncol + 255) / 256, 256, 0, stream>>>(iv, h.lamx, h.lamy, h.Ab, h.At, h.nxh, h.spitch, h.ny, h.nz);
+      CU(cudaStreamSynchronize(stream));
+      CU(cudaGetLastError());
+      h.tri_iv = iv;
+    }
     if ((r = upload_table(&h.zPr, g.zPr))) return r;
     if ((r = upload_table(&h.dzPr, g.dzPr))) return r;
     if ((r = upload_table(&h.zW, g.zW))) return r;
@@ -531,41 +613,91 @@ struct BatchT {
     unsigned packed = 0;
     int nf = 0;
     for (int f : fields) packed |= (unsigned)f << (8 * nf++);
+    nlaunch++;
     k_ghosts<T><<<gsz(9, ls[LK_SHELL].total * nf), kShellThreads, 0, stream>>>(ddom, ls[LK_SHELL].l(), packed, nf,
                                                                                  gate);
   }
   int launch_sgs() {
-    nlaunch += 2;
+    nlaunch++;
     k_sgs<T><<<gsz(0, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l());
     launch_ghosts({F_NU}, 0);
     return ELMM_OK;
   }
   int launch_momentum(int stage) {
     StageCoef sc{kRho[stage - 1], kBeta[stage - 1], 2 * kAlpha[stage - 1], stage};
-    nlaunch += 2;
+    nlaunch++;
     k_momentum<T><<<gsz(1, ls[LK_MOM].total), MX * MY, smem_mom, stream>>>(ddom, ls[LK_MOM].l(), sc);
     launch_ghosts({F_U2, F_V2, F_W2}, 0);
     return ELMM_OK;
   }
+  void launch_project(double coef_alpha2, int use_dt, int in_place, int gate) {
+    nlaunch += 2;
+    k_project<T><<<gsz(6, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l(), coef_alpha2, use_dt,
+                                                                   in_place, gate);
+    launch_ghosts({F_U, F_V, F_W, F_P}, gate);
+    k_prref<T><<<std::min(nd, 1024), 256, 0, stream>>>(ddom, nd, gate);
+  }
   // PressureCorrection on U2 (in_place = 0) or on U itself (initial projection)
   int launch_projection(double coef_alpha2, int use_dt, int in_place) {
-    nlaunch += 9;
     launch_poisson(coef_alpha2, use_dt, 0, 0);
-    k_project<T><<<gsz(6, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l(), coef_alpha2, use_dt,
-                                                                   in_place, 0);
-    launch_ghosts({F_U, F_V, F_W, F_P}, 0);
-    k_prref<T><<<std::min(nd, 1024), 256, 0, stream>>>(ddom, nd, 0);
+    launch_project(coef_alpha2, use_dt, in_place, 0);
     return ELMM_OK;
+  }
+  // the pieces of the Poisson solve: register FFTs (one launch per distinct
+  // length) and the tiled z solve where the whole batch allows them, the
+  // generic kernels otherwise
+  void launch_fftx_fwd(double coef_alpha2, int use_dt, int rhs_from_phi, int gate) {
+    for (auto &r : xreg) {
+      nlaunch++;
+      r.k->fwd<<<std::max(1, std::min(r.ls.total, r.cap_fwd)), kRegThreads, r.smem, stream>>>(
+          ddom, r.ls.l(), coef_alpha2, use_dt, rhs_from_phi, gate);
+    }
+    if (ls[LK_ROWS].total > 0) {
+      nlaunch++;
+      k_fftx_fwd<T><<<gsz(2, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan,
+                                                                                  coef_alpha2, use_dt, rhs_from_phi, gate);
+    }
+  }
+  void launch_ffty(int inverse, int gate) {
+    for (auto &r : yreg) {
+      nlaunch++;
+      (inverse ? r.k->yi : r.k->yf)<<<std::max(1, std::min(r.ls.total, inverse ? r.cap_inv : r.cap_fwd)), kRegThreads,
+                                       r.smem, stream>>>(ddom, r.ls.l(), gate);
+    }
+    if (ls[LK_YCOLS].total > 0) {
+      nlaunch++;
+      k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), kFFTThreads, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, inverse,
+                                                                              gate);
+    }
+  }
+  void launch_tri(int gate) {
+    if (ls[LK_TRIT].total > 0) {
+      nlaunch++;
+      k_tri_tile<T><<<gsz(13, ls[LK_TRIT].total), kTriTileThreads, smem_trit, stream>>>(ddom, ls[LK_TRIT].l(), gate);
+    }
+    if (ls[LK_TRI].total > 0) {
+      nlaunch++;
+      k_tri<T><<<gsz(4, ls[LK_TRI].total), kTriThreads, smem_tri, stream>>>(ddom, ls[LK_TRI].l(), gate);
+    }
+  }
+  void launch_fftx_inv(int gate) {
+    for (auto &r : xreg) {
+      nlaunch++;
+      r.k->inv<<<std::max(1, std::min(r.ls.total, r.cap_inv)), kRegThreads, r.smem, stream>>>(ddom, r.ls.l(), gate);
+    }
+    if (ls[LK_ROWS].total > 0) {
+      nlaunch++;
+      k_fftx_inv<T><<<gsz(5, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan, gate);
+    }
   }
   // the five transform kernels and the ghosts of Phi; rhs_from_phi: the
   // right-hand side is in Phi
   void launch_poisson(double coef_alpha2, int use_dt, int rhs_from_phi, int gate) {
-    k_fftx_fwd<T><<<gsz(2, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan, coef_alpha2,
-                                                                                use_dt, rhs_from_phi, gate);
-    k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), kFFTThreads, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, 0, gate);
-    k_tri<T><<<gsz(4, ls[LK_TRI].total), kTriThreads, smem_tri, stream>>>(ddom, ls[LK_TRI].l(), gate);
-    k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), kFFTThreads, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, 1, gate);
-    k_fftx_inv<T><<<gsz(5, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan, gate);
+    launch_fftx_fwd(coef_alpha2, use_dt, rhs_from_phi, gate);
+    launch_ffty(0, gate);
+    launch_tri(gate);
+    launch_ffty(1, gate);
+    launch_fftx_inv(gate);
     launch_ghosts({F_PHI}, gate);
   }
   int max_refine() const {
@@ -586,11 +718,9 @@ struct BatchT {
     for (int sw = 0; sw < R; sw++) {
       k_refine_decide<T><<<(nd + 127) / 128, 128, 0, stream>>>(ddom, nd, sw == 0);
       launch_poisson(coef_alpha2, use_dt, 1, 1);
-      k_project<T><<<gsz(6, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l(), coef_alpha2, use_dt, 1, 1);
-      launch_ghosts({F_U, F_V, F_W, F_P}, 1);
-      k_prref<T><<<std::min(nd, 1024), 256, 0, stream>>>(ddom, nd, 1);
+      launch_project(coef_alpha2, use_dt, 1, 1);
       k_divres<T><<<gsz(7, ls[LK_CELLS].total), TX * TY, 0, stream>>>(ddom, ls[LK_CELLS].l(), 1);
-      nlaunch += 12;
+      nlaunch += 2;
     }
   }
   int launch_divmax() {
@@ -737,13 +867,11 @@ struct BatchT {
       timed(kGhost, [&] { launch_ghosts({F_NU}, 0); });
       timed(1, [&] { k_momentum<T><<<gsz(1, ls[LK_MOM].total), MX * MY, smem_mom, stream>>>(ddom, ls[LK_MOM].l(), sc); });
       timed(kGhost, [&] { launch_ghosts({F_U2, F_V2, F_W2}, 0); });
-      timed(2, [&] {
-        k_fftx_fwd<T><<<gsz(2, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan, a2, 1, 0, 0);
-      });
-      timed(3, [&] { k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), kFFTThreads, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, 0, 0); });
-      timed(4, [&] { k_tri<T><<<gsz(4, ls[LK_TRI].total), kTriThreads, smem_tri, stream>>>(ddom, ls[LK_TRI].l(), 0); });
-      timed(5, [&] { k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), kFFTThreads, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, 1, 0); });
-      timed(6, [&] { k_fftx_inv<T><<<gsz(5, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan, 0); });
+      timed(2, [&] { launch_fftx_fwd(a2, 1, 0, 0); });
+      timed(3, [&] { launch_ffty(0, 0); });
+      timed(4, [&] { launch_tri(0); });
+      timed(5, [&] { launch_ffty(1, 0); });
+      timed(6, [&] { launch_fftx_inv(0); });
       timed(kGhost, [&] { launch_ghosts({F_PHI}, 0); });
       timed(7, [&] { k_project<T><<<gsz(6, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l(), a2, 1, 0, 0); });
       timed(kGhost, [&] { launch_ghosts({F_U, F_V, F_W, F_P}, 0); });
@@ -1172,8 +1300,9 @@ int elmm_poisson_solver_finalize(elmm_poisson *s) {
 // whose pool already owns the GPU, or a path where cudaMalloc/cudaFree would
 // synchronise the device).  All working memory sits in noalloc_scratch, a
 // fixed array in this library's device image; nothing here calls cudaMalloc,
-// cudaFree or any other allocating routine.  The kernels are the ones of the
-// handle-based solver; only their descriptors and buffers live elsewhere.
+// cudaFree or any other allocating routine.  The kernels are the generic-length
+// kernels of the handle-based solver; only their descriptors and buffers live
+// elsewhere.
 
 // Every GPU that loads the library holds this array until the process exits.
 static __device__ __align__(256) unsigned char noalloc_scratch[ELMM_NOALLOC_SCRATCH_BYTES];

@@ -1,0 +1,325 @@
+// elmm_poisson_reg.cuh -- the transforms and the z solve of the Poisson
+// problem (src/poisson.f90:23-60, the PoisFFT replacement) for the common
+// case: x and y lengths with a register FFT (ELMM_FFT_SIZES) and a
+// non-periodic z axis of at most kTriTileMaxNz cells.  Other grids use the
+// generic kernels of elmm_kernels.cuh / elmm_kernels2.cuh; both compute the
+// same discrete solution.
+#pragma once
+
+#include "elmm_fftreg.cuh"
+#include "elmm_stream.cuh"
+
+namespace elmm {
+
+constexpr int kRegThreads = 256;
+
+// right-hand side at box index c: the divergence of (U2, V2, W2) / coef, or
+// the value already stored in Phi (PoisSolver interface, defect correction)
+template <typename T>
+__device__ __forceinline__ T poisson_rhs(const Dom<T> &d, long long c, T rdx, T rdy, T rdzk, T rdt2, int rhs_from_phi) {
+  if (rhs_from_phi) return ld((const T *)d.Phi, c) * rdt2;
+  const T div = (ld((const T *)d.U2, c) - ld((const T *)d.U2, c - 1)) * rdx +
+                (ld((const T *)d.V2, c) - ld((const T *)d.V2, c - d.pitch)) * rdy +
+                (ld((const T *)d.W2, c) - ld((const T *)d.W2, c - d.plane)) * rdzk;
+  return div * rdt2;
+}
+
+// ------------------------------------------------------------ x forward
+// Divergence + real FFT along x of 2 * NS rows (two real rows per complex
+// sequence), split into the half spectra of the two rows: S[row][0..nx/2].
+template <typename T, int N>
+__device__ __forceinline__ void fftx_fwd_tile(const Dom<T> &d, int lt, typename Vec2<T>::type *smem, double coef,
+                                              int rhs_from_phi) {
+  typedef typename Vec2<T>::type T2;
+  typedef FPlan<N> Pl;
+  constexpr int P = Pl::P, E = Pl::E, NS = kRegThreads / P;
+  const int s = threadIdx.x / P, t = threadIdx.x - s * P;
+  const int ny = d.ny, nrows = ny * d.nz;
+  const int ra = 2 * (lt * NS + s), rb = ra + 1;
+  const bool va = ra < nrows, vb = rb < nrows;
+  const int qa = va ? ra : 0, qb = vb ? rb : 0;  // rows past the end are not read
+  const int ka = qa / ny + 1, kb = qb / ny + 1;
+  const long long ca = bidx(d, 1, qa - (ka - 1) * ny + 1, ka), cb = bidx(d, 1, qb - (kb - 1) * ny + 1, kb);
+  const T rdt2 = (T)(1.0 / coef);
+  const T rdx = (T)(1.0 / d.dx), rdy = (T)(1.0 / d.dy), rdz = (T)(1.0 / d.dz);
+  const T rdza = (d.vz && va) ? (T)d.sgs_rdz[ka] : rdz, rdzb = (d.vz && vb) ? (T)d.sgs_rdz[kb] : rdz;
+  T2 v[E];
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    const int i0 = t + P * e;
+    v[e].x = va ? poisson_rhs(d, ca + i0, rdx, rdy, rdza, rdt2, rhs_from_phi) : (T)0;
+    v[e].y = vb ? poisson_rhs(d, cb + i0, rdx, rdy, rdzb, rdt2, rhs_from_phi) : (T)0;
+  }
+  T2 *sh = smem + s * Pl::SEQ;
+  fft_reg<T, T2, N, false>(v, sh, t, d.twx);
+  // Z = FFT(a + i b): A_m = (Z_m + conj Z_{N-m}) / 2, B_m = (Z_m - conj Z_{N-m}) / 2i
+  constexpr int nxh = N / 2 + 1;
+  T2 *Sa = d.S + (long long)qa * d.spitch, *Sb = d.S + (long long)qb * d.spitch;
+#pragma unroll
+  for (int m = t; m < nxh; m += P) {
+    const T2 zk = sh[m], zc = sh[m == 0 ? 0 : N - m];
+    T2 A, B;
+    A.x = (zk.x + zc.x) * (T)0.5;
+    A.y = (zk.y - zc.y) * (T)0.5;
+    B.x = (zk.y + zc.y) * (T)0.5;
+    B.y = (zc.x - zk.x) * (T)0.5;
+    if (va) Sa[m] = A;
+    if (vb) Sb[m] = B;
+  }
+  __syncthreads();  // the next tile reuses sh
+}
+
+// One launch per x length N: the launch set holds only the domains with
+// nx == N.
+template <typename T, int N>
+__global__ void __launch_bounds__(kRegThreads) k_fftx_fwd_reg(const Dom<T> *__restrict__ doms, Launch L,
+                                                              double coef_alpha2, int use_dt, int rhs_from_phi,
+                                                              int gate) {
+  typedef typename Vec2<T>::type T2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T2 *sm = reinterpret_cast<T2 *>(smem_raw);
+  for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
+    const int di = find_dom(L.starts, L.nd, t);
+    const Dom<T> &d = doms[di];
+    if (gate && !*d.refine_flag) continue;
+    const double coef = use_dt ? coef_alpha2 * d.dt : coef_alpha2;
+    fftx_fwd_tile<T, N>(d, t - __ldg(L.starts + di), sm, coef, rhs_from_phi);
+  }
+}
+
+// --------------------------------------------------------------- y (both)
+// Complex FFT along y of C = kRegThreads / P consecutive kx columns of one
+// k plane of S, in place.
+template <typename T, int N, bool INV>
+__device__ __forceinline__ void ffty_tile(const Dom<T> &d, int lt, typename Vec2<T>::type *smem) {
+  typedef typename Vec2<T>::type T2;
+  typedef FPlan<N> Pl;
+  constexpr int P = Pl::P, E = Pl::E, C = kRegThreads / P;
+  const int c = threadIdx.x % C, t = threadIdx.x / C;
+  const int nxh = d.nxh, ncx = (nxh + C - 1) / C;
+  const int k = lt / ncx, kx = (lt - k * ncx) * C + c;
+  const bool ok = kx < nxh;
+  const long long sp = d.spitch;
+  T2 *S = d.S + (long long)k * N * sp + kx;
+  T2 v[E];
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    if (ok) v[e] = S[(long long)(t + P * e) * sp];
+    else { v[e].x = 0; v[e].y = 0; }
+  }
+  T2 *sh = smem + c * Pl::SEQ;
+  fft_reg<T, T2, N, INV>(v, sh, t, d.twy);
+#pragma unroll
+  for (int e = 0; e < E; e++)
+    if (ok) S[(long long)(t + P * e) * sp] = sh[t + P * e];
+  __syncthreads();
+}
+
+template <typename T, int N, bool INV>
+__global__ void __launch_bounds__(kRegThreads) k_ffty_reg(const Dom<T> *__restrict__ doms, Launch L, int gate) {
+  typedef typename Vec2<T>::type T2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T2 *sm = reinterpret_cast<T2 *>(smem_raw);
+  for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
+    const int di = find_dom(L.starts, L.nd, t);
+    const Dom<T> &d = doms[di];
+    if (gate && !*d.refine_flag) continue;
+    ffty_tile<T, N, INV>(d, t - __ldg(L.starts + di), sm);
+  }
+}
+
+// ------------------------------------------------------------ x inverse
+// Two rows per complex sequence: Z_m = A_m + i B_m with the Hermitian
+// completion A_{N-m} = conj(A_m); the real and imaginary parts of the
+// inverse transform are the two rows of Phi (interior only).
+template <typename T, int N>
+__device__ __forceinline__ void fftx_inv_tile(const Dom<T> &d, int lt, typename Vec2<T>::type *smem) {
+  typedef typename Vec2<T>::type T2;
+  typedef FPlan<N> Pl;
+  constexpr int P = Pl::P, E = Pl::E, NS = kRegThreads / P;
+  constexpr int nxh = N / 2 + 1;
+  const int s = threadIdx.x / P, t = threadIdx.x - s * P;
+  const int ny = d.ny, nrows = ny * d.nz;
+  const int ra = 2 * (lt * NS + s), rb = ra + 1;
+  const bool va = ra < nrows, vb = rb < nrows;
+  const int qa = va ? ra : 0, qb = vb ? rb : 0;  // rows past the end are not read
+  const T2 *Sa = d.S + (long long)qa * d.spitch, *Sb = d.S + (long long)qb * d.spitch;
+  T2 v[E];
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    const int m = t + P * e;
+    const int mm = m < nxh ? m : N - m;
+    T2 A, B;
+    A.x = 0; A.y = 0; B.x = 0; B.y = 0;
+    if (va) A = Sa[mm];
+    if (vb) B = Sb[mm];
+    if (mm == 0 || 2 * mm == N) { A.y = 0; B.y = 0; }
+    if (m >= nxh) { A.y = -A.y; B.y = -B.y; }
+    v[e].x = A.x - B.y;
+    v[e].y = A.y + B.x;
+  }
+  T2 *sh = smem + s * Pl::SEQ;
+  fft_reg<T, T2, N, true>(v, sh, t, d.twx);
+  const int ka = qa / ny + 1, kb = qb / ny + 1;
+  T *Pa = d.Phi + bidx(d, 1, qa - (ka - 1) * ny + 1, ka), *Pb = d.Phi + bidx(d, 1, qb - (kb - 1) * ny + 1, kb);
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    const int i0 = t + P * e;
+    const T2 z = sh[i0];
+    if (va) Pa[i0] = z.x;
+    if (vb) Pb[i0] = z.y;
+  }
+  __syncthreads();
+}
+
+template <typename T, int N>
+__global__ void __launch_bounds__(kRegThreads) k_fftx_inv_reg(const Dom<T> *__restrict__ doms, Launch L, int gate) {
+  typedef typename Vec2<T>::type T2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T2 *sm = reinterpret_cast<T2 *>(smem_raw);
+  for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
+    const int di = find_dom(L.starts, L.nd, t);
+    const Dom<T> &d = doms[di];
+    if (gate && !*d.refine_flag) continue;
+    fftx_inv_tile<T, N>(d, t - __ldg(L.starts + di), sm);
+  }
+}
+
+// The kernels of one length, for the host's dispatch table.
+template <typename T>
+struct FFTRegKernels {
+  int n;
+  void (*fwd)(const Dom<T> *, Launch, double, int, int, int);
+  void (*inv)(const Dom<T> *, Launch, int);
+  void (*yf)(const Dom<T> *, Launch, int);
+  void (*yi)(const Dom<T> *, Launch, int);
+};
+
+template <typename T>
+inline const FFTRegKernels<T> *fft_reg_kernels(int n) {
+#define ELMM_REG_ENTRY(n_) {n_, k_fftx_fwd_reg<T, n_>, k_fftx_inv_reg<T, n_>, k_ffty_reg<T, n_, false>, k_ffty_reg<T, n_, true>},
+  static const FFTRegKernels<T> table[] = {ELMM_FFT_SIZES(ELMM_REG_ENTRY)};
+#undef ELMM_REG_ENTRY
+  for (const auto &e : table)
+    if (e.n == n) return &e;
+  return nullptr;
+}
+
+// sequences (x) or columns (y) one block of the register kernels handles
+__host__ __device__ constexpr int fft_reg_batch(int n) { return kRegThreads / fplan_P(n); }
+
+// ------------------------------------------------- tiled tridiagonal solve
+// The z solve of every (kx, ky) mode (Thomas algorithm, non-periodic z) for
+// kTriCols consecutive spectral columns.  The pivots of the forward sweep
+// depend on the grid only, so their reciprocals are computed once per domain
+// (k_tri_factors); a solve copies the nz x kTriCols tile of S and of those
+// reciprocals into shared memory with cp.async, solves the real and
+// imaginary part of each column with a pair of threads, and writes the tile
+// back.  The arithmetic is that of the generic kernel, k_tri: the same pivots,
+// c(k) = At(k) / pivot(k), and the zero-mean prefix-sum solution of the
+// (0,0) mode.
+constexpr int kTriCols = 32;
+constexpr int kTriTileThreads = 2 * kTriCols;
+constexpr int kTriTileMaxNz = 256;
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+template <typename T>
+__host__ __device__ constexpr size_t tri_tile_smem(int nz) {
+  return (size_t)nz * kTriCols * (2 * sizeof(T) + sizeof(double));
+}
+
+// iv[(k-1) * ncol + col] = 1 / pivot(k) of mode col = ky * spitch + kx
+__global__ void k_tri_factors(double *iv, const double *__restrict__ lamx, const double *__restrict__ lamy,
+                              const double *__restrict__ Ab, const double *__restrict__ At, int nxh, int spitch, int ny,
+                              int nz) {
+  const int ncol = ny * spitch;
+  for (int col = blockIdx.x * blockDim.x + threadIdx.x; col < ncol; col += gridDim.x * blockDim.x) {
+    const int ky = col / spitch, kx = col - ky * spitch;
+    const bool mode = kx < nxh && !(kx == 0 && ky == 0);
+    const double lam = mode ? lamx[kx] + lamy[ky] : 0.0;
+    double cprev = 0;
+    for (int k = 1; k <= nz; k++) {
+      double v = 0;
+      if (mode) {
+        const double den = (-(Ab[k] + At[k]) + lam) - (k > 1 ? Ab[k] * cprev : 0.0);
+        v = 1.0 / den;
+        cprev = At[k] * v;
+      }
+      iv[(long long)(k - 1) * ncol + col] = v;
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kTriTileThreads) k_tri_tile(const Dom<T> *__restrict__ doms, Launch L, int gate) {
+  typedef typename Vec2<T>::type T2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int kChunk = 16 / (int)sizeof(T2), kPerRow = kTriCols / kChunk, XS = 2 * kTriCols;
+  constexpr int kIvPerRow = kTriCols / 2;  // 16-byte copies of the reciprocals per k
+  for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
+    const int di = find_dom(L.starts, L.nd, t);
+    const Dom<T> &d = doms[di];
+    if (gate && !*d.refine_flag) continue;
+    const int lt = t - __ldg(L.starts + di);
+    const int nz = d.nz, ncol = d.ny * d.spitch;
+    const long long ps = ncol;
+    const int col0 = lt * kTriCols;
+    T2 *tile = reinterpret_cast<T2 *>(smem_raw);                                            // [nz][kTriCols]
+    double *ivs = reinterpret_cast<double *>(smem_raw + (size_t)nz * kTriCols * sizeof(T2));  // [nz][kTriCols]
+    for (int q = threadIdx.x; q < nz * kPerRow; q += kTriTileThreads) {
+      const int k = q / kPerRow, c = (q - k * kPerRow) * kChunk;
+      if (col0 + c < ncol) cp_async16(tile + k * kTriCols + c, d.S + k * ps + col0 + c);
+    }
+    for (int q = threadIdx.x; q < nz * kIvPerRow; q += kTriTileThreads) {
+      const int k = q / kIvPerRow, c = (q - k * kIvPerRow) * 2;
+      if (col0 + c < ncol) cp_async16(ivs + k * kTriCols + c, d.tri_iv + k * ps + col0 + c);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    const int c = threadIdx.x >> 1, part = threadIdx.x & 1;
+    const int col = col0 + c, ky = col / d.spitch, kx = col - ky * d.spitch;
+    const bool active = col < ncol && kx < d.nxh;
+    T *x = reinterpret_cast<T *>(tile) + 2 * c + part;  // element k - 1 at x[(k - 1) * XS]
+    const double *iv = ivs + c;                          // element k - 1 at iv[(k - 1) * kTriCols]
+    const double norm = 1.0 / ((double)d.nx * (double)d.ny);
+    const double *Ab = d.Ab, *At = d.At;
+    if (active && kx == 0 && ky == 0) {
+      // F(k) = F(k-1) + dzc(k) r(k) is the flux (x(k+1) - x(k)) / dzf(k)
+      double F = 0, xx = 0, sx = 0;
+      for (int k = 1; k <= nz - 1; k++) {
+        F = F + ((double)x[(k - 1) * XS] * norm) * d.dzc[k];
+        x[(k - 1) * XS] = (T)xx;
+        sx += xx;
+        xx = xx + F * d.dzf[k];
+      }
+      sx += xx;
+      sx = sx / nz;
+      for (int k = 0; k < nz - 1; k++) x[k * XS] = (T)((double)x[k * XS] - sx);
+      x[(nz - 1) * XS] = (T)(xx - sx);
+    } else if (active) {
+      double px = (double)x[0] * norm * iv[0];
+      x[0] = (T)px;
+      for (int k = 2; k <= nz; k++) {
+        px = ((double)x[(k - 1) * XS] * norm - Ab[k] * px) * iv[(k - 1) * kTriCols];
+        x[(k - 1) * XS] = (T)px;
+      }
+      for (int k = nz - 1; k >= 1; k--) {
+        px = (double)x[(k - 1) * XS] - (At[k] * iv[(k - 1) * kTriCols]) * px;
+        x[(k - 1) * XS] = (T)px;
+      }
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < nz * kPerRow; q += kTriTileThreads) {
+      const int k = q / kPerRow, c2 = (q - k * kPerRow) * kChunk;
+      if (col0 + c2 < ncol)
+        *reinterpret_cast<int4 *>(d.S + k * ps + col0 + c2) = *reinterpret_cast<const int4 *>(tile + k * kTriCols + c2);
+    }
+    __syncthreads();  // the tile is free for the next one
+  }
+}
+
+}  // namespace elmm
