@@ -209,9 +209,9 @@ __host__ __device__ __forceinline__ long long shell_cells(int ex, int ey, int ez
 template <typename T>
 __global__ void __launch_bounds__(kShellThreads) k_ghosts(const Dom<T> *__restrict__ doms, Launch L, unsigned fields,
                                                           int nf, int gate) {
-  const long long nblk = (long long)L.total * nf;
-  for (long long b = blockIdx.x; b < nblk; b += gridDim.x) {
-    const int f = (int)(b / L.total), t = (int)(b - (long long)f * L.total);
+  const int nblk = L.total * nf;  // shell tiles times fields (a few million at most)
+  for (int b = blockIdx.x; b < nblk; b += gridDim.x) {
+    const int f = b / L.total, t = b - f * L.total;
     const int di = find_dom(L.starts, L.nd, t);
     const Dom<T> &d = doms[di];
     if (gate && !*d.refine_flag) continue;
@@ -219,24 +219,24 @@ __global__ void __launch_bounds__(kShellThreads) k_ghosts(const Dom<T> *__restri
     const bool vel = fid <= F_W2;
     const int comp = fid % 3;
     const int ex = vel ? d.ext[comp][0] : d.nx, ey = vel ? d.ext[comp][1] : d.ny, ez = vel ? d.ext[comp][2] : d.nz;
-    long long w = (long long)(t - __ldg(L.starts + di)) * kShellThreads + threadIdx.x;
-    if (w >= shell_cells(ex, ey, ez)) continue;
+    int w = (t - __ldg(L.starts + di)) * kShellThreads + threadIdx.x;
+    if (w >= (int)shell_cells(ex, ey, ez)) continue;
     // z faces (full planes), then y faces (k in 1..ez), then x faces
     int i, j, k;
-    const long long zf = (long long)(ex + 2) * (ey + 2), yf = (long long)(ex + 2) * ez, xf = (long long)ey * ez;
+    const int rx = ex + 2, zf = rx * (ey + 2), yf = rx * ez, xf = ey * ez;
     if (w < 2 * zf) {
       const int side = w >= zf;
       w -= side * zf;
-      i = (int)(w % (ex + 2)); j = (int)(w / (ex + 2)); k = side ? ez + 1 : 0;
+      j = w / rx; i = w - j * rx; k = side ? ez + 1 : 0;
     } else if ((w -= 2 * zf) < 2 * yf) {
       const int side = w >= yf;
       w -= side * yf;
-      i = (int)(w % (ex + 2)); k = (int)(w / (ex + 2)) + 1; j = side ? ey + 1 : 0;
+      k = w / rx; i = w - k * rx; k += 1; j = side ? ey + 1 : 0;
     } else {
       w -= 2 * yf;
       const int side = w >= xf;
       w -= side * xf;
-      j = (int)(w % ey) + 1; k = (int)(w / ey) + 1; i = side ? ex + 1 : 0;
+      k = w / ey; j = w - k * ey + 1; k += 1; i = side ? ex + 1 : 0;
     }
     T *F = box_field(d, fid);
     const bool per[3] = {d.bt[SIDE_WE] == BC_PERIODIC, d.bt[SIDE_SO] == BC_PERIODIC, d.bt[SIDE_BO] == BC_PERIODIC};

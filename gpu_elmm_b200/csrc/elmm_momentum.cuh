@@ -327,7 +327,7 @@ struct SlotLayout {
 template <typename T, int NWF, int NNF>
 struct WideRing {
   typedef SlotLayout<T, NWF, NNF> Lay;
-  const T *p[3];
+  const T *__restrict__ p[3];
   int o;
   __device__ __forceinline__ T g(int f, int dx, int dy, int dz) const {
     return p[dz + 1][f * Lay::WB + o + dy * Lay::SPW + dx];
@@ -449,37 +449,32 @@ __global__ void __launch_bounds__(MX *MY, 2) k_momentum(const Dom<T> *__restrict
         R.o = o;
         const T *nar = R.p[1] + Lay::WIDE + ty * MX + tx;  // narrow blocks are NB apart
         const T p0 = R.g(4, 0, 0, 0) - m;
-        if (hasU && k <= kU) {
-          T ts = tendency<T, 0>(ctx, R, i, j, k, wallhere);
-          T u2 = stage1 ? (T)0 : nar[0] * rdt * dt;
-          Us[c] = ts;
-          u2 = u2 + ts * bdt * dt;
-          if (prgx_on) u2 = u2 + fx;
-          u2 = u2 + gx * ((R.g(4, 1, 0, 0) - m) - p0);
-          u2 = u2 + R.g(0, 0, 0, 0);
-          U2o[c] = u2;
-        }
-        if (hasV && k <= kV) {
-          T ts = tendency<T, 1>(ctx, R, i, j, k, wallhere);
-          T v2 = stage1 ? (T)0 : nar[Lay::NB] * rdt * dt;
-          Vs[c] = ts;
-          v2 = v2 + ts * bdt * dt;
-          if (prgy_on) v2 = v2 + fy;
-          v2 = v2 + gy * ((R.g(4, 0, 1, 0) - m) - p0);
-          v2 = v2 + R.g(1, 0, 0, 0);
-          V2o[c] = v2;
-        }
-        if (hasW && k <= kW) {
-          T ts = tendency<T, 2>(ctx, R, i, j, k, wallhere);
-          T w2 = stage1 ? (T)0 : nar[2 * Lay::NB] * rdt * dt;
-          Ws[c] = ts;
-          w2 = w2 + ts * bdt * dt;
-          const T dpz = (R.g(4, 0, 0, 1) - m) - p0;
-          if (vz) w2 = w2 - coef * dpz / (T)dzW[k + 2];
-          else w2 = w2 + gz * dpz;
-          w2 = w2 + R.g(2, 0, 0, 0);
-          W2o[c] = w2;
-        }
+        // all shared-memory reads first, then the stores: a global store in
+        // between would make the compiler reload every shared value it may
+        // alias
+        const bool doU = hasU && k <= kU, doV = hasV && k <= kV, doW = hasW && k <= kW;
+        const T tu = doU ? tendency<T, 0>(ctx, R, i, j, k, wallhere) : (T)0;
+        const T tv = doV ? tendency<T, 1>(ctx, R, i, j, k, wallhere) : (T)0;
+        const T tw = doW ? tendency<T, 2>(ctx, R, i, j, k, wallhere) : (T)0;
+        T u2 = stage1 ? (T)0 : nar[0] * rdt * dt;
+        T v2 = stage1 ? (T)0 : nar[Lay::NB] * rdt * dt;
+        T w2 = stage1 ? (T)0 : nar[2 * Lay::NB] * rdt * dt;
+        u2 = u2 + tu * bdt * dt;
+        if (prgx_on) u2 = u2 + fx;
+        u2 = u2 + gx * ((R.g(4, 1, 0, 0) - m) - p0);
+        u2 = u2 + R.g(0, 0, 0, 0);
+        v2 = v2 + tv * bdt * dt;
+        if (prgy_on) v2 = v2 + fy;
+        v2 = v2 + gy * ((R.g(4, 0, 1, 0) - m) - p0);
+        v2 = v2 + R.g(1, 0, 0, 0);
+        w2 = w2 + tw * bdt * dt;
+        const T dpz = (R.g(4, 0, 0, 1) - m) - p0;
+        if (vz) w2 = w2 - coef * dpz / (T)dzW[k + 2];
+        else w2 = w2 + gz * dpz;
+        w2 = w2 + R.g(2, 0, 0, 0);
+        if (doU) { Us[c] = tu; U2o[c] = u2; }
+        if (doV) { Vs[c] = tv; V2o[c] = v2; }
+        if (doW) { Ws[c] = tw; W2o[c] = w2; }
       }
       __syncthreads();  // plane k-1 is no longer read
       if (abort_flag) {
@@ -598,7 +593,12 @@ __global__ void __launch_bounds__(MX *MY, 3) k_sgs(const Dom<T> *__restrict__ do
     }
     __syncthreads();
     const bool inside = i <= nx && j <= ny;
-    const bool anywall = d.wall[0] | d.wall[1] | d.wall[2] | d.wall[3] | d.wall[4] | d.wall[5];
+    // block-uniform: the wall sides whose wall-model points this tile can
+    // hold (a point sits next to its side: i in {1, nx-1, nx} and so on)
+    int wmask = 0;
+    for (int f = 0; f < 6; f++) wmask |= d.wall[f] ? (1 << f) : 0;
+    const int wtile = wmask & ((i0 == 1 ? 1 : 0) | (i0 + MX - 1 >= nx - 1 ? 2 : 0) | (j0 == 1 ? 4 : 0) |
+                               (j0 + MY - 1 >= ny - 1 ? 8 : 0));
     const T num = (T)d.nu_mol;
     const bool sgs = d.sgs != 0, addmol = d.nu_mol > 0;
     SgsK<T> q;
@@ -628,13 +628,12 @@ __global__ void __launch_bounds__(MX *MY, 3) k_sgs(const Dom<T> *__restrict__ do
         } else {
           v = num;
         }
-        const long long c = bidx(d, i, j, k);
-        nu[c] = v;
-        const bool edge = i == 1 || i == nx || j == 1 || j == ny || k == 1 || k == nz;
-        if (anywall && (edge || k == nz - 1 || i == nx - 1 || j == ny - 1)) {
+        nu[bidx(d, i, j, k)] = v;
+        const int wk = wtile | (wmask & ((k == 1 ? 16 : 0) | (k >= nz - 1 ? 32 : 0)));
+        if (wk) {
 #pragma unroll 1
           for (int f = 0; f < 6; f++) {
-            if (!d.wall[f]) continue;
+            if (!((wk >> f) & 1)) continue;
 #pragma unroll 1
             for (int comp = 0; comp < 3; comp++) {
               long long p = wm_plane_index(d, comp, f, i, j, k);

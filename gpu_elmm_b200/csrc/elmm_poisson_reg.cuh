@@ -12,6 +12,11 @@
 namespace elmm {
 
 constexpr int kRegThreads = 256;
+// resident blocks per SM the x-transform kernels are compiled for: for up to
+// 16 elements per thread three (FP32, 80 registers) or two (FP64, 128
+// registers) fit without spills; longer sequences get the compiler's choice
+template <typename T, int N>
+constexpr int fft_reg_min_blocks() { return N / fplan_P(N) <= 16 ? (sizeof(T) == 4 ? 3 : 2) : 1; }
 
 // right-hand side at box index c: the divergence of (U2, V2, W2) / coef, or
 // the value already stored in Phi (PoisSolver interface, defect correction)
@@ -72,7 +77,7 @@ __device__ __forceinline__ void fftx_fwd_tile(const Dom<T> &d, int lt, typename 
 // One launch per x length N: the launch set holds only the domains with
 // nx == N.
 template <typename T, int N>
-__global__ void __launch_bounds__(kRegThreads) k_fftx_fwd_reg(const Dom<T> *__restrict__ doms, Launch L,
+__global__ void __launch_bounds__(kRegThreads, fft_reg_min_blocks<T, N>()) k_fftx_fwd_reg(const Dom<T> *__restrict__ doms, Launch L,
                                                               double coef_alpha2, int use_dt, int rhs_from_phi,
                                                               int gate) {
   typedef typename Vec2<T>::type T2;
@@ -173,7 +178,7 @@ __device__ __forceinline__ void fftx_inv_tile(const Dom<T> &d, int lt, typename 
 }
 
 template <typename T, int N>
-__global__ void __launch_bounds__(kRegThreads) k_fftx_inv_reg(const Dom<T> *__restrict__ doms, Launch L, int gate) {
+__global__ void __launch_bounds__(kRegThreads, fft_reg_min_blocks<T, N>()) k_fftx_inv_reg(const Dom<T> *__restrict__ doms, Launch L, int gate) {
   typedef typename Vec2<T>::type T2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T2 *sm = reinterpret_cast<T2 *>(smem_raw);
@@ -211,15 +216,21 @@ __host__ __device__ constexpr int fft_reg_batch(int n) { return kRegThreads / fp
 // ------------------------------------------------- tiled tridiagonal solve
 // The z solve of every (kx, ky) mode (Thomas algorithm, non-periodic z) for
 // kTriCols consecutive spectral columns.  The pivots of the forward sweep
-// depend on the grid only, so their reciprocals are computed once per domain
-// (k_tri_factors); a solve copies the nz x kTriCols tile of S and of those
-// reciprocals into shared memory with cp.async, solves the real and
-// imaginary part of each column with a pair of threads, and writes the tile
-// back.  The arithmetic is that of the generic kernel, k_tri: the same pivots,
-// c(k) = At(k) / pivot(k), and the zero-mean prefix-sum solution of the
-// (0,0) mode.
+// depend on the grid only, so their reciprocals iv(k) are computed once per
+// domain (k_tri_factors).  With them both sweeps are first-order linear
+// recurrences,
+//   forward   y(k) = r(k) iv(k) - Ab(k) iv(k) y(k-1),
+//   backward  x(k) = y(k) - At(k) iv(k) x(k+1),
+// which a block solves for the real and imaginary part of each column with
+// kTriSegs threads per part: each thread composes the affine map of its
+// segment of k, the segment maps are chained through shared memory, and each
+// thread then replays its segment from the exact entry value.  The tile of S
+// and of iv is copied into shared memory with cp.async first and written
+// back at the end.  The (0,0) mode is the zero-mean prefix-sum solution of
+// the generic kernel, k_tri.
 constexpr int kTriCols = 32;
-constexpr int kTriTileThreads = 2 * kTriCols;
+constexpr int kTriSegs = 4;
+constexpr int kTriTileThreads = 2 * kTriCols * kTriSegs;
 constexpr int kTriTileMaxNz = 256;
 
 __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
@@ -227,9 +238,10 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
+// tile of S, reciprocal pivots, and the (A, B) maps of the segments
 template <typename T>
 __host__ __device__ constexpr size_t tri_tile_smem(int nz) {
-  return (size_t)nz * kTriCols * (2 * sizeof(T) + sizeof(double));
+  return (size_t)nz * kTriCols * (2 * sizeof(T) + sizeof(double)) + 2 * sizeof(double) * kTriSegs * 2 * kTriCols;
 }
 
 // iv[(k-1) * ncol + col] = 1 / pivot(k) of mode col = ky * spitch + kx
@@ -260,6 +272,7 @@ __global__ void __launch_bounds__(kTriTileThreads) k_tri_tile(const Dom<T> *__re
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int kChunk = 16 / (int)sizeof(T2), kPerRow = kTriCols / kChunk, XS = 2 * kTriCols;
   constexpr int kIvPerRow = kTriCols / 2;  // 16-byte copies of the reciprocals per k
+  constexpr int NP = 2 * kTriCols;         // systems (column parts) per tile
   for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
     const int di = find_dom(L.starts, L.nd, t);
     const Dom<T> &d = doms[di];
@@ -270,6 +283,8 @@ __global__ void __launch_bounds__(kTriTileThreads) k_tri_tile(const Dom<T> *__re
     const int col0 = lt * kTriCols;
     T2 *tile = reinterpret_cast<T2 *>(smem_raw);                                            // [nz][kTriCols]
     double *ivs = reinterpret_cast<double *>(smem_raw + (size_t)nz * kTriCols * sizeof(T2));  // [nz][kTriCols]
+    double *mapA = ivs + (size_t)nz * kTriCols;                                              // [kTriSegs][NP]
+    double *mapB = mapA + kTriSegs * NP;
     for (int q = threadIdx.x; q < nz * kPerRow; q += kTriTileThreads) {
       const int k = q / kPerRow, c = (q - k * kPerRow) * kChunk;
       if (col0 + c < ncol) cp_async16(tile + k * kTriCols + c, d.S + k * ps + col0 + c);
@@ -280,14 +295,63 @@ __global__ void __launch_bounds__(kTriTileThreads) k_tri_tile(const Dom<T> *__re
     }
     cp_async_wait_all();
     __syncthreads();
-    const int c = threadIdx.x >> 1, part = threadIdx.x & 1;
+    const int sys = threadIdx.x % NP, seg = threadIdx.x / NP;
+    const int c = sys >> 1;  // column; sys & 1 selects the real or imaginary part
     const int col = col0 + c, ky = col / d.spitch, kx = col - ky * d.spitch;
     const bool active = col < ncol && kx < d.nxh;
-    T *x = reinterpret_cast<T *>(tile) + 2 * c + part;  // element k - 1 at x[(k - 1) * XS]
-    const double *iv = ivs + c;                          // element k - 1 at iv[(k - 1) * kTriCols]
+    const bool zero_mode = kx == 0 && ky == 0;
+    const bool solve = active && !zero_mode;
+    T *x = reinterpret_cast<T *>(tile) + sys;  // element k - 1 at x[(k - 1) * XS]
+    const double *iv = ivs + c;                // element k - 1 at iv[(k - 1) * kTriCols]
     const double norm = 1.0 / ((double)d.nx * (double)d.ny);
     const double *Ab = d.Ab, *At = d.At;
-    if (active && kx == 0 && ky == 0) {
+    const int len = (nz + kTriSegs - 1) / kTriSegs;
+    const int kb = 1 + seg * len, ke = min(nz, kb + len - 1);  // this thread's segment, kb > ke if empty
+    // forward: y(k) = a(k) + b(k) y(k-1), a = r norm iv, b = -Ab iv (b(1) = 0)
+    double A = 0, B = 1;
+    if (solve)
+      for (int k = kb; k <= ke; k++) {
+        const double ivk = iv[(k - 1) * kTriCols];
+        const double a = (double)x[(k - 1) * XS] * norm * ivk, b = -Ab[k] * ivk;
+        A = a + b * A;
+        B = b * B;
+      }
+    mapA[seg * NP + sys] = A;
+    mapB[seg * NP + sys] = B;
+    __syncthreads();
+    if (solve) {
+      double y = 0;  // y(kb - 1), y(0) = 0
+      for (int s2 = 0; s2 < seg; s2++) y = mapA[s2 * NP + sys] + mapB[s2 * NP + sys] * y;
+      for (int k = kb; k <= ke; k++) {
+        const double ivk = iv[(k - 1) * kTriCols];
+        y = (double)x[(k - 1) * XS] * norm * ivk - Ab[k] * ivk * y;
+        x[(k - 1) * XS] = (T)y;
+      }
+    }
+    __syncthreads();
+    // backward: x(k) = y(k) + g(k) x(k+1), g = -At iv (g(nz) = 0); segments
+    // run from their top end down
+    A = 0;
+    B = 1;
+    if (solve)
+      for (int k = ke; k >= kb; k--) {
+        const double g = -At[k] * iv[(k - 1) * kTriCols];
+        A = (double)x[(k - 1) * XS] + g * A;
+        B = g * B;
+      }
+    __syncthreads();  // every thread has read the forward maps
+    mapA[seg * NP + sys] = A;
+    mapB[seg * NP + sys] = B;
+    __syncthreads();
+    if (solve) {
+      double xv = 0;  // x(ke + 1), x(nz + 1) = 0
+      for (int s2 = kTriSegs - 1; s2 > seg; s2--) xv = mapA[s2 * NP + sys] + mapB[s2 * NP + sys] * xv;
+      for (int k = ke; k >= kb; k--) {
+        xv = (double)x[(k - 1) * XS] - At[k] * iv[(k - 1) * kTriCols] * xv;
+        x[(k - 1) * XS] = (T)xv;
+      }
+    }
+    if (active && zero_mode && seg == 0) {
       // F(k) = F(k-1) + dzc(k) r(k) is the flux (x(k+1) - x(k)) / dzf(k)
       double F = 0, xx = 0, sx = 0;
       for (int k = 1; k <= nz - 1; k++) {
@@ -300,17 +364,6 @@ __global__ void __launch_bounds__(kTriTileThreads) k_tri_tile(const Dom<T> *__re
       sx = sx / nz;
       for (int k = 0; k < nz - 1; k++) x[k * XS] = (T)((double)x[k * XS] - sx);
       x[(nz - 1) * XS] = (T)(xx - sx);
-    } else if (active) {
-      double px = (double)x[0] * norm * iv[0];
-      x[0] = (T)px;
-      for (int k = 2; k <= nz; k++) {
-        px = ((double)x[(k - 1) * XS] * norm - Ab[k] * px) * iv[(k - 1) * kTriCols];
-        x[(k - 1) * XS] = (T)px;
-      }
-      for (int k = nz - 1; k >= 1; k--) {
-        px = (double)x[(k - 1) * XS] - (At[k] * iv[(k - 1) * kTriCols]) * px;
-        x[(k - 1) * XS] = (T)px;
-      }
     }
     __syncthreads();
     for (int q = threadIdx.x; q < nz * kPerRow; q += kTriTileThreads) {
