@@ -112,7 +112,7 @@ class Clocks:
         os.close(fd)
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
@@ -266,7 +266,7 @@ def run_ours(args, ws, rank, local):
 
     # per-step latency distribution (device time of single-step calls)
     lat = []
-    for _ in range(args.steps):
+    for _ in range(min(args.steps, 50)):
         lat.append(dm.step(1).elapsed_ms)
     lat.sort()
     p50 = lat[len(lat) // 2]
@@ -337,7 +337,7 @@ def run_ours(args, ws, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     args = ap.parse_args()

@@ -796,7 +796,14 @@ struct BatchT {
 
   int fill_stats(elmm_stats *st, int nsteps) {
     double md = 0, cf = 0;
+    int gave_up = 0;
     for (int d = 0; d < nd; d++) {
+      int fl[2] = {0, 0};
+      CU(cudaMemcpy(fl, hdom[d].flags, sizeof(fl), cudaMemcpyDeviceToHost));
+      if (fl[1]) {  // a bounded device-side wait gave up: report it once
+        gave_up = 1;
+        CU(cudaMemset(hdom[d].flags + 1, 0, sizeof(int)));
+      }
       unsigned long long b1 = 0, b2 = 0;
       CU(cudaMemcpy(&b1, hdom[d].maxdiv_bits, sizeof(b1), cudaMemcpyDeviceToHost));
       CU(cudaMemcpy(&b2, hdom[d].cfl_bits, sizeof(b2), cudaMemcpyDeviceToHost));
@@ -820,6 +827,7 @@ struct BatchT {
       st->elapsed_ms = ms;
     }
     if (!(md == md)) return fail(ELMM_ERR_NAN, "NaN in the velocity field");
+    if (gave_up) return fail(ELMM_ERR_TIMEOUT, "a device-side wait for a plane copy gave up; the step is incomplete");
     return ELMM_OK;
   }
 
