@@ -823,10 +823,10 @@ struct BatchT {
       st->dt = cfg[0].dt;
       st->cfl = cf;
       st->max_div = md;
-      st->nan_detected = !(md == md) || !(cf == cf);
+      st->nan_detected = !std::isfinite(md) || !std::isfinite(cf);
       st->elapsed_ms = ms;
     }
-    if (!(md == md)) return fail(ELMM_ERR_NAN, "NaN in the velocity field");
+    if (!std::isfinite(md) || !std::isfinite(cf)) return fail(ELMM_ERR_NAN, "NaN or Inf in the velocity field");
     if (gave_up) return fail(ELMM_ERR_TIMEOUT, "a device-side wait for a plane copy gave up; the step is incomplete");
     return ELMM_OK;
   }

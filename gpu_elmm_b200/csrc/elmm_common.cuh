@@ -241,10 +241,4 @@ __device__ __forceinline__ int find_dom(const int *starts, int nd, int t) {
   return lo;
 }
 
-// Order-preserving bits of a non-negative double for atomicMax.
-__device__ __forceinline__ void atomic_max_pos(unsigned long long *a, double v) {
-  if (!(v >= 0)) v = __longlong_as_double(0x7ff8000000000000ULL);  // NaN wins
-  atomicMax(a, (unsigned long long)__double_as_longlong(v));
-}
-
 }  // namespace elmm

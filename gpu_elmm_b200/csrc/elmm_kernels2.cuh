@@ -262,12 +262,46 @@ __global__ void __launch_bounds__(kShellThreads) k_ghosts(const Dom<T> *__restri
   }
 }
 
+// Order-preserving bits of a non-negative double; NaN maps above every
+// finite value, so an integer maximum propagates it.
+__device__ __forceinline__ unsigned long long max_bits(double v) {
+  return v >= 0 ? (unsigned long long)__double_as_longlong(v) : 0x7ff8000000000000ULL;
+}
+
+// Block-wide maximum of per-thread bits b, merged into *dst with one atomic.
+// Every thread of the block calls it.
+template <int NT>
+__device__ __forceinline__ void block_max_flush(unsigned long long *dst, unsigned long long b,
+                                                unsigned long long *red) {
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long x = __shfl_down_sync(0xffffffffu, b, o);
+    b = x > b ? x : b;
+  }
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = b;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long m = 0;
+    for (int w = 0; w < NT / 32; w++) m = red[w] > m ? red[w] : m;
+    if (m) atomicMax(dst, m);
+  }
+  __syncthreads();
+}
+
 // max |div u| in FP64 (the check of src/pressure.f90:884-989)
 template <typename T>
 __global__ void __launch_bounds__(TX *TY) k_divmax(const Dom<T> *__restrict__ doms, Launch L) {
-  __shared__ double red[TX * TY / 32];
+  // a running maximum per thread over the block's tiles; one block
+  // reduction and one atomic per domain the block visits
+  __shared__ unsigned long long red[TX * TY / 32];
+  unsigned long long run = 0;
+  int cur = -1;
   for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
     const int di = find_dom(L.starts, L.nd, t);
+    if (di != cur) {  // block-uniform
+      if (cur >= 0) block_max_flush<TX * TY>(doms[cur].maxdiv_bits, run, red);
+      run = 0;
+      cur = di;
+    }
     const Dom<T> &d = doms[di];
     int lt = t - __ldg(L.starts + di);
     const int ntx = (d.nx + TX - 1) / TX, nty = (d.ny + TY - 1) / TY;
@@ -276,26 +310,17 @@ __global__ void __launch_bounds__(TX *TY) k_divmax(const Dom<T> *__restrict__ do
     const int k = lt / nty + 1;
     const int i = tx * TX + (threadIdx.x % TX) + 1;
     const int j = ty * TY + (threadIdx.x / TX) + 1;
-    double a = 0;
     if (i <= d.nx && j <= d.ny) {
       const long long c = bidx(d, i, j, k);
       const double dzk = d.vz ? d.dzPr[k + 2] : d.dz;
-      double p = ((double)ld(d.U, c) - (double)ld(d.U, c - 1)) / d.dx +
-                 ((double)ld(d.V, c) - (double)ld(d.V, c - d.pitch)) / d.dy +
-                 ((double)ld(d.W, c) - (double)ld(d.W, c - d.plane)) / dzk;
-      a = fabs(p);
-      if (!(a == a)) a = __longlong_as_double(0x7ff8000000000000ULL);
+      const double a = fabs(((double)ld(d.U, c) - (double)ld(d.U, c - 1)) / d.dx +
+                            ((double)ld(d.V, c) - (double)ld(d.V, c - d.pitch)) / d.dy +
+                            ((double)ld(d.W, c) - (double)ld(d.W, c - d.plane)) / dzk);
+      const unsigned long long b = max_bits(a);
+      run = b > run ? b : run;
     }
-    for (int o = 16; o > 0; o >>= 1) a = fmax(a, __shfl_down_sync(0xffffffffu, a, o));
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double m = 0;
-      for (int w = 0; w < TX * TY / 32; w++) m = fmax(m, red[w]);
-      atomic_max_pos(d.maxdiv_bits, m);
-    }
-    __syncthreads();
   }
+  if (cur >= 0) block_max_flush<TX * TY>(doms[cur].maxdiv_bits, run, red);
 }
 
 
@@ -305,9 +330,18 @@ __global__ void __launch_bounds__(TX *TY) k_divmax(const Dom<T> *__restrict__ do
 // solve, and its maximum.  gate: run only for domains whose flag is set.
 template <typename T>
 __global__ void __launch_bounds__(TX *TY) k_divres(const Dom<T> *__restrict__ doms, Launch L, int gate) {
-  __shared__ double red[TX * TY / 32];
+  // a running maximum per thread over the block's tiles; one block
+  // reduction and one atomic per domain the block visits
+  __shared__ unsigned long long red[TX * TY / 32];
+  unsigned long long run = 0;
+  int cur = -1;
   for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
     const int di = find_dom(L.starts, L.nd, t);
+    if (di != cur) {  // block-uniform
+      if (cur >= 0) block_max_flush<TX * TY>(doms[cur].maxdiv_bits, run, red);
+      run = 0;
+      cur = di;
+    }
     const Dom<T> &d = doms[di];
     if (gate && !*d.refine_flag) continue;
     int lt = t - __ldg(L.starts + di);
@@ -317,27 +351,19 @@ __global__ void __launch_bounds__(TX *TY) k_divres(const Dom<T> *__restrict__ do
     const int k = lt / nty + 1;
     const int i = tx * TX + (threadIdx.x % TX) + 1;
     const int j = ty * TY + (threadIdx.x / TX) + 1;
-    double a = 0;
     if (i <= d.nx && j <= d.ny) {
       const long long c = bidx(d, i, j, k);
       const double dzk = d.vz ? d.dzPr[k + 2] : d.dz;
-      double p = ((double)ld(d.U, c) - (double)ld(d.U, c - 1)) / d.dx +
-                 ((double)ld(d.V, c) - (double)ld(d.V, c - d.pitch)) / d.dy +
-                 ((double)ld(d.W, c) - (double)ld(d.W, c - d.plane)) / dzk;
+      const double p = ((double)ld(d.U, c) - (double)ld(d.U, c - 1)) / d.dx +
+                       ((double)ld(d.V, c) - (double)ld(d.V, c - d.pitch)) / d.dy +
+                       ((double)ld(d.W, c) - (double)ld(d.W, c - d.plane)) / dzk;
       d.Phi[c] = (T)p;
-      a = fabs(p);
-      if (!(a == a)) a = __longlong_as_double(0x7ff8000000000000ULL);
+      const double a = fabs(p);
+      const unsigned long long b = max_bits(a);
+      run = b > run ? b : run;
     }
-    for (int o = 16; o > 0; o >>= 1) a = fmax(a, __shfl_down_sync(0xffffffffu, a, o));
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double m = 0;
-      for (int w = 0; w < TX * TY / 32; w++) m = fmax(m, red[w]);
-      atomic_max_pos(d.maxdiv_bits, m);
-    }
-    __syncthreads();
   }
+  if (cur >= 0) block_max_flush<TX * TY>(doms[cur].maxdiv_bits, run, red);
 }
 
 // Whether another correction sweep runs: max |div u| above the tolerance
@@ -366,9 +392,18 @@ __global__ void k_refine_decide(const Dom<T> *__restrict__ doms, int nd, int fir
 // CFL of TimeStepLength (src/dynamics.f90:553-595)
 template <typename T>
 __global__ void __launch_bounds__(TX *TY) k_cfl(const Dom<T> *__restrict__ doms, Launch L) {
-  __shared__ double red[TX * TY / 32];
+  // a running maximum per thread over the block's tiles; one block
+  // reduction and one atomic per domain the block visits
+  __shared__ unsigned long long red[TX * TY / 32];
+  unsigned long long run = 0;
+  int cur = -1;
   for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
     const int di = find_dom(L.starts, L.nd, t);
+    if (di != cur) {  // block-uniform
+      if (cur >= 0) block_max_flush<TX * TY>(doms[cur].cfl_bits, run, red);
+      run = 0;
+      cur = di;
+    }
     const Dom<T> &d = doms[di];
     int lt = t - __ldg(L.starts + di);
     const int ntx = (d.nx + TX - 1) / TX, nty = (d.ny + TY - 1) / TY;
@@ -377,26 +412,19 @@ __global__ void __launch_bounds__(TX *TY) k_cfl(const Dom<T> *__restrict__ doms,
     const int k = lt / nty + 1;
     const int i = tx * TX + (threadIdx.x % TX) + 1;
     const int j = ty * TY + (threadIdx.x / TX) + 1;
-    double a = 0;
     if (i <= d.nx && j <= d.ny) {
       const long long c = bidx(d, i, j, k);
       const double dzk = d.vz ? d.dzPr[k + 2] : d.dz;
-      double p = fmax(fabs((double)ld(d.U, c)), fabs((double)ld(d.U, c - 1))) / d.dx;
-      p = p + fmax(fabs((double)ld(d.V, c)), fabs((double)ld(d.V, c - d.pitch))) / d.dy;
-      p = p + fmax(fabs((double)ld(d.W, c)), fabs((double)ld(d.W, c - d.plane))) / dzk;
-      a = p;
-      if (!(p == p)) a = __longlong_as_double(0x7ff8000000000000ULL);
+      // NaN-propagating maximum of |u| over the two faces (fmax would drop a NaN)
+      auto fm = [](double x, double y) { return (x != x || x > y) ? x : y; };
+      double a = fm(fabs((double)ld(d.U, c)), fabs((double)ld(d.U, c - 1))) / d.dx;
+      a = a + fm(fabs((double)ld(d.V, c)), fabs((double)ld(d.V, c - d.pitch))) / d.dy;
+      a = a + fm(fabs((double)ld(d.W, c)), fabs((double)ld(d.W, c - d.plane))) / dzk;
+      const unsigned long long b = max_bits(a);
+      run = b > run ? b : run;
     }
-    for (int o = 16; o > 0; o >>= 1) a = fmax(a, __shfl_down_sync(0xffffffffu, a, o));
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double m = 0;
-      for (int w = 0; w < TX * TY / 32; w++) m = fmax(m, red[w]);
-      atomic_max_pos(d.cfl_bits, m);
-    }
-    __syncthreads();
   }
+  if (cur >= 0) block_max_flush<TX * TY>(doms[cur].cfl_bits, run, red);
 }
 
 // ------------------------------------------------------ host layout copies

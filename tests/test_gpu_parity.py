@@ -252,6 +252,23 @@ def test_non_finite_upload_is_refused():
     assert e.value.code == 3
 
 
+@pytest.mark.parametrize("prec", [0, 1])
+def test_blow_up_is_reported(prec):
+    """A time step far above the CFL limit makes the run diverge; the step
+    that produces a non-finite velocity returns ELMM_ERR_NAN (code 3) and
+    flags nan_detected, however few cells are affected."""
+    cfg = make_config(32, 24, 16, precision=prec, dt=1000.0)
+    g = grid_of(cfg)
+    d = L.Domain(cfg)
+    d.upload(*log_profile_state(g, seed=0))
+    d.project(1.0)
+    with pytest.raises(L.ElmmError) as e:
+        for _ in range(40):
+            d.step(1)
+    assert e.value.code == 3
+    d.close()
+
+
 @pytest.mark.parametrize("prec,tol", [(0, 1e-10), (1, 1e-6)])
 def test_full_size_divergence(prec, tol):
     """256 x 256 x 128: the projected field stays divergence-free in FP64."""
