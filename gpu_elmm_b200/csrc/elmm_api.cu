@@ -219,7 +219,8 @@ struct BatchT {
     int cap_fwd = 1, cap_inv = 1;
   };
   std::vector<RegSet> xreg, yreg;
-  size_t smem_mom = (size_t)kRingSlots * SlotLayout<T, 5, 3>::BYTES;
+  size_t smem_mom = (size_t)MomShape<T>::slots * SlotLayout<T, 5, 3>::BYTES;
+  size_t smem_sgs = (size_t)kRingSlots * SlotLayout<T, 3, 0>::BYTES;
   int grid_cap[16];
   // host-layout staging (double), max over domains of the largest host array
   double *dstage = nullptr;
@@ -339,6 +340,7 @@ struct BatchT {
     CU(cudaFuncSetAttribute(k_ffty<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     CU(cudaFuncSetAttribute(k_tri<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     CU(cudaFuncSetAttribute(k_momentum<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 1024));
+    CU(cudaFuncSetAttribute(k_sgs<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 1024));
     for (auto &h : hdom) {
       reg_x |= fft_reg_supported(h.nx);
       reg_y |= fft_reg_supported(h.ny);
@@ -359,8 +361,8 @@ struct BatchT {
       if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, threads, sm) != cudaSuccess || b < 1) b = 1;
       return b * nsm;
     };
-    grid_cap[0] = cap((const void *)k_sgs<T>, MX * MY, 0);
-    grid_cap[1] = cap((const void *)k_momentum<T>, MX * MY, smem_mom);
+    grid_cap[0] = cap((const void *)k_sgs<T>, MX * MY, smem_sgs);
+    grid_cap[1] = cap((const void *)k_momentum<T>, MomShape<T>::threads, smem_mom);
     grid_cap[2] = cap((const void *)k_fftx_fwd<T>, kFFTThreads, smem_x);
     grid_cap[3] = cap((const void *)k_ffty<T>, kFFTThreads, smem_y);
     grid_cap[4] = cap((const void *)k_tri<T>, kTriThreads, smem_tri);
@@ -619,14 +621,14 @@ struct BatchT {
   }
   int launch_sgs() {
     nlaunch++;
-    k_sgs<T><<<gsz(0, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l());
+    k_sgs<T><<<gsz(0, ls[LK_MOM].total), MX * MY, smem_sgs, stream>>>(ddom, ls[LK_MOM].l());
     launch_ghosts({F_NU}, 0);
     return ELMM_OK;
   }
   int launch_momentum(int stage) {
     StageCoef sc{kRho[stage - 1], kBeta[stage - 1], 2 * kAlpha[stage - 1], stage};
     nlaunch++;
-    k_momentum<T><<<gsz(1, ls[LK_MOM].total), MX * MY, smem_mom, stream>>>(ddom, ls[LK_MOM].l(), sc);
+    k_momentum<T><<<gsz(1, ls[LK_MOM].total), MomShape<T>::threads, smem_mom, stream>>>(ddom, ls[LK_MOM].l(), sc);
     launch_ghosts({F_U2, F_V2, F_W2}, 0);
     return ELMM_OK;
   }
@@ -871,9 +873,11 @@ struct BatchT {
         cudaEventRecord(ev[2 * slot.size() + 1], stream);
         slot.push_back(k);
       };
-      timed(0, [&] { k_sgs<T><<<gsz(0, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l()); });
+      timed(0, [&] { k_sgs<T><<<gsz(0, ls[LK_MOM].total), MX * MY, smem_sgs, stream>>>(ddom, ls[LK_MOM].l()); });
       timed(kGhost, [&] { launch_ghosts({F_NU}, 0); });
-      timed(1, [&] { k_momentum<T><<<gsz(1, ls[LK_MOM].total), MX * MY, smem_mom, stream>>>(ddom, ls[LK_MOM].l(), sc); });
+      timed(1, [&] {
+        k_momentum<T><<<gsz(1, ls[LK_MOM].total), MomShape<T>::threads, smem_mom, stream>>>(ddom, ls[LK_MOM].l(), sc);
+      });
       timed(kGhost, [&] { launch_ghosts({F_U2, F_V2, F_W2}, 0); });
       timed(2, [&] { launch_fftx_fwd(a2, 1, 0, 0); });
       timed(3, [&] { launch_ffty(0, 0); });

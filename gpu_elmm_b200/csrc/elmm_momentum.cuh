@@ -6,13 +6,16 @@
 // old-pressure gradient (dynamics.f90:58-199) and U2 += U (tsteps.f90:352-354).
 //
 // A block owns an MX x MY column of cells and marches up a chunk of MKC
-// planes.  U, V, W and Viscosity of planes k-1, k, k+1 (with a one-cell
-// halo in x and y) sit in a three-slot ring in shared memory; while plane k
-// is computed, plane k+2 is already on its way into registers.  Every input
-// cell is thus read from HBM once per chunk instead of once per stencil use.
+// planes.  U, V, W, Viscosity and Pr of each plane (with a one-cell halo in
+// x and y) and the old Ustar (tile only) arrive by tensor-map TMA in a ring
+// of kRingSlots plane slots in shared memory, requested several planes ahead
+// of their use.  Every input cell is thus read from HBM once per chunk
+// instead of once per stencil use.  The SGS kernel, k_sgs, streams U, V, W
+// the same way.
 #pragma once
 
 #include "elmm_common.cuh"
+#include "elmm_packed.cuh"
 #include "elmm_stream.cuh"
 
 namespace elmm {
@@ -23,16 +26,6 @@ struct StageCoef {
 };
 
 constexpr int MX = 32, MY = 8, MKC = 16;
-constexpr int MPW = MX + 2, MPH = MY + 2, MPS = MPW * MPH;
-
-// stencil accessor over the plane ring: field f (0 U, 1 V, 2 W, 3 nu)
-template <typename T>
-struct Ring {
-  const T *p[3];  // planes k-1, k, k+1 (field-major, MPS elements per field)
-  int o;          // offset of the thread's own cell in a plane
-  __device__ __forceinline__ T g(int f, int dx, int dy, int dz) const { return p[dz + 1][f * MPS + o + dy * MPW + dx]; }
-};
-
 // per-tile context in shared memory: everything the stencil code reads
 // besides the fields, so that no descriptor load sits on its critical path
 template <typename T>
@@ -354,22 +347,37 @@ __device__ __forceinline__ void issue_plane(T *slot, uint64_t *bar, const CUtens
 
 constexpr int kRingSlots = 5;
 
+// Cells per thread along x and ring slots of the momentum kernel: FP32
+// threads compute two x-adjacent cells with packed FP32x2 arithmetic
+// (elmm_packed.cuh); a four-slot ring leaves room for four 128-thread blocks
+// per SM.  FP64 keeps one cell per thread and five slots.
 template <typename T>
-__global__ void __launch_bounds__(MX *MY, 2) k_momentum(const Dom<T> *__restrict__ doms, Launch L, StageCoef sc) {
+struct MomShape {
+  static constexpr int cpt = 1, slots = 5, threads = MX * MY, min_blocks = 2;
+};
+template <>
+struct MomShape<float> {
+  static constexpr int cpt = 2, slots = 4, threads = MX * MY / 2, min_blocks = 4;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
+    k_momentum(const Dom<T> *__restrict__ doms, Launch L, StageCoef sc) {
   typedef SlotLayout<T, 5, 3> Lay;
+  constexpr int CPT = MomShape<T>::cpt, NSL = MomShape<T>::slots, TXN = MX / CPT;
   extern __shared__ __align__(128) unsigned char dyn_smem[];
   T *ring = reinterpret_cast<T *>(dyn_smem);
-  __shared__ __align__(8) uint64_t bars[kRingSlots];
+  __shared__ __align__(8) uint64_t bars[NSL];
   __shared__ MomCtx<T> ctx;
   __shared__ int abort_flag;
-  const int tx = threadIdx.x % MX, ty = threadIdx.x / MX;
+  const int tx = threadIdx.x % TXN, ty = threadIdx.x / TXN;
   // tensor copies need 128-byte aligned destinations
   if (smem_addr(ring) & 127u) {
     if (threadIdx.x == 0) doms[0].flags[1] = 1;
     return;
   }
   if (threadIdx.x == 0) {
-    for (int s2 = 0; s2 < kRingSlots; s2++) mbar_init(&bars[s2], 1);
+    for (int s2 = 0; s2 < NSL; s2++) mbar_init(&bars[s2], 1);
     abort_flag = 0;
     fence_async_shared();
   }
@@ -385,9 +393,9 @@ __global__ void __launch_bounds__(MX *MY, 2) k_momentum(const Dom<T> *__restrict
     const int bk = lt / nty;
     const int i0 = bx * MX + 1, j0 = by * MY + 1, k0 = bk * MKC + 1;
     const int k1 = min(k0 + MKC - 1, d.nz);
-    const int i = i0 + tx, j = j0 + ty;
+    const int i = i0 + CPT * tx, j = j0 + ty;  // the thread's first cell
     const int nx = d.nx, ny = d.ny;
-    const long long pitch = d.pitch, plane = d.plane;
+    const long long plane = d.plane;
     const bool stage1 = sc.stage == 1;
     const int wide[5] = {F_U, F_V, F_W, F_NU, F_P};
     const int narrow[3] = {F_US, F_VS, F_WS};
@@ -396,9 +404,9 @@ __global__ void __launch_bounds__(MX *MY, 2) k_momentum(const Dom<T> *__restrict
     if (threadIdx.x == 0) fill_ctx(ctx, d);
     if (threadIdx.x == 0) {
       fence_async_shared();
-      for (int kk = k0 - 1; kk <= min(k0 - 1 + kRingSlots - 1, k1 + 1); kk++)
-        issue_plane<T, 5, 3>(ring + (kk % kRingSlots) * Lay::SIZE, &bars[kk % kRingSlots], maps, wide, narrow, !stage1,
-                             d.aln, i0, j0, kk);
+      for (int kk = k0 - 1; kk <= min(k0 - 1 + NSL - 1, k1 + 1); kk++)
+        issue_plane<T, 5, 3>(ring + (kk % NSL) * Lay::SIZE, &bars[kk % NSL], maps, wide, narrow, !stage1, d.aln, i0,
+                             j0, kk);
     }
     __syncthreads();  // the context is written
     const T dt = (T)d.dt, rdt = (T)sc.rho, bdt = (T)sc.beta;
@@ -406,10 +414,6 @@ __global__ void __launch_bounds__(MX *MY, 2) k_momentum(const Dom<T> *__restrict
     const T coef = (T)coefd;
     const T gx = (T)(-coefd / d.dx), gy = (T)(-coefd / d.dy), gz = (T)(-coefd / d.dz);
     const T m = (T)(*d.prm);
-    const bool inside = i <= nx && j <= ny;
-    const bool hasU = i <= d.ext[0][0] && j <= d.ext[0][1];
-    const bool hasV = i <= d.ext[1][0] && j <= d.ext[1][1];
-    const bool hasW = i <= d.ext[2][0] && j <= d.ext[2][1];
     const int kU = d.ext[0][2], kV = d.ext[1][2], kW = d.ext[2][2];
     const bool vz = d.vz != 0;
     const bool prgx_on = d.prgx_on != 0, prgy_on = d.prgy_on != 0;
@@ -421,78 +425,134 @@ __global__ void __launch_bounds__(MX *MY, 2) k_momentum(const Dom<T> *__restrict
     T *__restrict__ Us = d.Us;
     T *__restrict__ Vs = d.Vs;
     T *__restrict__ Ws = d.Ws;
-    const int o = (ty + 1) * Lay::SPW + (tx + Lay::XO);
-    long long c = bidx(d, inside ? i : 1, inside ? j : 1, k0);
-    // block-uniform: only tiles on a side of the box and the planes next to
-    // the bottom and top have wall-model corrections
+    const int o = (ty + 1) * Lay::SPW + (CPT * tx + Lay::XO);
+    const bool inside0 = i <= nx && j <= ny;
+    long long c = bidx(d, inside0 ? i : 1, inside0 ? j : 1, k0);
     const int nz = d.nz;
-    // a component's last index is n or n-1 (src/initial.f90:871-896)
+    // block-uniform: only tiles on a side of the box and the planes next to
+    // the bottom and top have wall-model corrections; a component's last
+    // index is n or n-1 (src/initial.f90:871-896)
     const bool xlo = i0 == 1, xhi = i0 + MX - 1 >= nx - 1, ylo = j0 == 1, yhi = j0 + MY - 1 >= ny - 1;
     int wmask = 0;
     for (int f = 0; f < 6; f++) wmask |= d.wall[f] ? (1 << f) : 0;
     const int wtile = wmask & ((xlo ? 1 : 0) | (xhi ? 2 : 0) | (ylo ? 4 : 0) | (yhi ? 8 : 0));
+    // block-uniform: every cell of the tile has all three components
+    const bool full_tile = i0 + MX - 1 <= min(d.ext[0][0], min(d.ext[1][0], d.ext[2][0])) &&
+                           j0 + MY - 1 <= min(d.ext[0][1], min(d.ext[1][1], d.ext[2][1]));
+    MomK2 K2;
+    if constexpr (CPT == 2) {
+      K2.Ax = bc2((float)ctx.cA[0]); K2.Ay = bc2((float)ctx.cA[1]); K2.Az = bc2((float)ctx.cA[2]);
+      K2.rx = bc2((float)ctx.rec2[0]); K2.ry = bc2((float)ctx.rec2[1]); K2.rz = bc2((float)ctx.rec2[2]);
+      K2.q = bc2(0.25f);
+      for (int cc = 0; cc < 3; cc++)
+        for (int a2 = 0; a2 < 3; a2++) K2.B[cc][a2] = bc2((float)ctx.cB[cc][a2]);
+    }
     for (int k = k0; k <= k1; k++) {
       // planes k-1, k, k+1 must have landed
       bool ok = true;
       for (int kk = (k == k0 ? k0 - 1 : k + 1); kk <= k + 1; kk++) {
-        const int s2 = kk % kRingSlots;
+        const int s2 = kk % NSL;
         ok &= mbar_wait(&bars[s2], (phase >> s2) & 1u);
         phase ^= 1u << s2;
       }
       if (!ok) { abort_flag = 1; d.flags[1] = 1; }
       const int wallhere = wtile | (wmask & ((k == 1 ? 16 : 0) | (k >= nz - 1 ? 32 : 0)));
-      if (inside && ok) {
-        WideRing<T, 5, 3> R;
-        R.p[0] = ring + ((k - 1) % kRingSlots) * Lay::SIZE;
-        R.p[1] = ring + (k % kRingSlots) * Lay::SIZE;
-        R.p[2] = ring + ((k + 1) % kRingSlots) * Lay::SIZE;
-        R.o = o;
-        const T *nar = R.p[1] + Lay::WIDE + ty * MX + tx;  // narrow blocks are NB apart
-        const T p0 = R.g(4, 0, 0, 0) - m;
-        // all shared-memory reads first, then the stores: a global store in
-        // between would make the compiler reload every shared value it may
-        // alias
-        const bool doU = hasU && k <= kU, doV = hasV && k <= kV, doW = hasW && k <= kW;
-        const T tu = doU ? tendency<T, 0>(ctx, R, i, j, k, wallhere) : (T)0;
-        const T tv = doV ? tendency<T, 1>(ctx, R, i, j, k, wallhere) : (T)0;
-        const T tw = doW ? tendency<T, 2>(ctx, R, i, j, k, wallhere) : (T)0;
-        T u2 = stage1 ? (T)0 : nar[0] * rdt * dt;
-        T v2 = stage1 ? (T)0 : nar[Lay::NB] * rdt * dt;
-        T w2 = stage1 ? (T)0 : nar[2 * Lay::NB] * rdt * dt;
-        u2 = u2 + tu * bdt * dt;
-        if (prgx_on) u2 = u2 + fx;
-        u2 = u2 + gx * ((R.g(4, 1, 0, 0) - m) - p0);
-        u2 = u2 + R.g(0, 0, 0, 0);
-        v2 = v2 + tv * bdt * dt;
-        if (prgy_on) v2 = v2 + fy;
-        v2 = v2 + gy * ((R.g(4, 0, 1, 0) - m) - p0);
-        v2 = v2 + R.g(1, 0, 0, 0);
-        w2 = w2 + tw * bdt * dt;
-        const T dpz = (R.g(4, 0, 0, 1) - m) - p0;
-        if (vz) w2 = w2 - coef * dpz / (T)dzW[k + 2];
-        else w2 = w2 + gz * dpz;
-        w2 = w2 + R.g(2, 0, 0, 0);
-        if (doU) { Us[c] = tu; U2o[c] = u2; }
-        if (doV) { Vs[c] = tv; V2o[c] = v2; }
-        if (doW) { Ws[c] = tw; W2o[c] = w2; }
+      const T *p0s = ring + ((k - 1) % NSL) * Lay::SIZE, *p1s = ring + (k % NSL) * Lay::SIZE,
+              *p2s = ring + ((k + 1) % NSL) * Lay::SIZE;
+      bool packed = false;
+      if constexpr (CPT == 2)
+        packed = !vz && !wallhere && full_tile && k <= min(kU, min(kV, kW)) && j <= ny;
+      if (packed && ok) {
+        if constexpr (CPT == 2) {
+          // two cells per thread, every operation on a pair
+          Ring2<Lay::WB, Lay::SPW> R2;
+          R2.p[0] = p0s; R2.p[1] = p1s; R2.p[2] = p2s;
+          R2.o = o;
+          const float *nar = p1s + Lay::WIDE + ty * MX + CPT * tx;
+          const F2 mm = bc2(m);
+          const F2 p0 = R2.g(4, 0, 0, 0) - mm;
+          const F2 tu = tendency2<0>(K2, R2), tv = tendency2<1>(K2, R2), tw = tendency2<2>(K2, R2);
+          const F2 rd = bc2(rdt), dd = bc2(dt), bd = bc2(bdt);
+          const F2 zero = bc2(0.f);
+          F2 u2 = stage1 ? zero : F2{*reinterpret_cast<const float2 *>(nar)} * rd * dd;
+          F2 v2 = stage1 ? zero : F2{*reinterpret_cast<const float2 *>(nar + Lay::NB)} * rd * dd;
+          F2 w2 = stage1 ? zero : F2{*reinterpret_cast<const float2 *>(nar + 2 * Lay::NB)} * rd * dd;
+          u2 = u2 + tu * bd * dd;
+          if (prgx_on) u2 = u2 + bc2(fx);
+          u2 = u2 + bc2(gx) * ((R2.g(4, 1, 0, 0) - mm) - p0);
+          u2 = u2 + R2.g(0, 0, 0, 0);
+          v2 = v2 + tv * bd * dd;
+          if (prgy_on) v2 = v2 + bc2(fy);
+          v2 = v2 + bc2(gy) * ((R2.g(4, 0, 1, 0) - mm) - p0);
+          v2 = v2 + R2.g(1, 0, 0, 0);
+          w2 = w2 + tw * bd * dd;
+          w2 = w2 + bc2(gz) * ((R2.g(4, 0, 0, 1) - mm) - p0);
+          w2 = w2 + R2.g(2, 0, 0, 0);
+          *reinterpret_cast<float2 *>(Us + c) = tu.v;
+          *reinterpret_cast<float2 *>(U2o + c) = u2.v;
+          *reinterpret_cast<float2 *>(Vs + c) = tv.v;
+          *reinterpret_cast<float2 *>(V2o + c) = v2.v;
+          *reinterpret_cast<float2 *>(Ws + c) = tw.v;
+          *reinterpret_cast<float2 *>(W2o + c) = w2.v;
+        }
+      } else if (ok) {
+#pragma unroll
+        for (int q = 0; q < CPT; q++) {
+          const int iq = i + q;
+          if (!(iq <= nx && j <= ny)) continue;
+          WideRing<T, 5, 3> R;
+          R.p[0] = p0s; R.p[1] = p1s; R.p[2] = p2s;
+          R.o = o + q;
+          const T *nar = p1s + Lay::WIDE + ty * MX + CPT * tx + q;  // narrow blocks are NB apart
+          const long long cq = c + q;
+          const T p0 = R.g(4, 0, 0, 0) - m;
+          // all shared-memory reads first, then the stores: a global store in
+          // between would make the compiler reload every shared value it may
+          // alias
+          const bool doU = iq <= d.ext[0][0] && j <= d.ext[0][1] && k <= kU;
+          const bool doV = iq <= d.ext[1][0] && j <= d.ext[1][1] && k <= kV;
+          const bool doW = iq <= d.ext[2][0] && j <= d.ext[2][1] && k <= kW;
+          const T tu = doU ? tendency<T, 0>(ctx, R, iq, j, k, wallhere) : (T)0;
+          const T tv = doV ? tendency<T, 1>(ctx, R, iq, j, k, wallhere) : (T)0;
+          const T tw = doW ? tendency<T, 2>(ctx, R, iq, j, k, wallhere) : (T)0;
+          T u2 = stage1 ? (T)0 : nar[0] * rdt * dt;
+          T v2 = stage1 ? (T)0 : nar[Lay::NB] * rdt * dt;
+          T w2 = stage1 ? (T)0 : nar[2 * Lay::NB] * rdt * dt;
+          u2 = u2 + tu * bdt * dt;
+          if (prgx_on) u2 = u2 + fx;
+          u2 = u2 + gx * ((R.g(4, 1, 0, 0) - m) - p0);
+          u2 = u2 + R.g(0, 0, 0, 0);
+          v2 = v2 + tv * bdt * dt;
+          if (prgy_on) v2 = v2 + fy;
+          v2 = v2 + gy * ((R.g(4, 0, 1, 0) - m) - p0);
+          v2 = v2 + R.g(1, 0, 0, 0);
+          w2 = w2 + tw * bdt * dt;
+          const T dpz = (R.g(4, 0, 0, 1) - m) - p0;
+          if (vz) w2 = w2 - coef * dpz / (T)dzW[k + 2];
+          else w2 = w2 + gz * dpz;
+          w2 = w2 + R.g(2, 0, 0, 0);
+          if (doU) { Us[cq] = tu; U2o[cq] = u2; }
+          if (doV) { Vs[cq] = tv; V2o[cq] = v2; }
+          if (doW) { Ws[cq] = tw; W2o[cq] = w2; }
+        }
       }
       __syncthreads();  // plane k-1 is no longer read
       if (abort_flag) {
         // a plane did not arrive: wait (bounded) for the copies still in
         // flight into this block's shared memory, then give up
         if (threadIdx.x == 0)
-          for (int kk = k + 2; kk <= min(k - 1 + kRingSlots - 1, k1 + 1); kk++) {
-            const int s2 = kk % kRingSlots;
+          for (int kk = k + 2; kk <= min(k - 1 + NSL - 1, k1 + 1); kk++) {
+            const int s2 = kk % NSL;
             mbar_wait(&bars[s2], (phase >> s2) & 1u);
             phase ^= 1u << s2;
           }
         return;
       }
-      const int kn = k - 1 + kRingSlots;
+      const int kn = k - 1 + NSL;
       if (threadIdx.x == 0 && kn <= k1 + 1) {
         fence_async_shared();
-        issue_plane<T, 5, 3>(ring + (kn % kRingSlots) * Lay::SIZE, &bars[kn % kRingSlots], maps, wide, narrow, !stage1,
-                             d.aln, i0, j0, kn);
+        issue_plane<T, 5, 3>(ring + (kn % NSL) * Lay::SIZE, &bars[kn % NSL], maps, wide, narrow, !stage1, d.aln, i0,
+                             j0, kn);
       }
       c += plane;
     }
@@ -552,9 +612,25 @@ __device__ long long wm_plane_index(const Dom<T> &d, int comp, int f, int i, int
 
 template <typename T>
 __global__ void __launch_bounds__(MX *MY, 3) k_sgs(const Dom<T> *__restrict__ doms, Launch L) {
-  __shared__ T ring[3][3 * MPS];
-  constexpr int NPF = (MPS + MX * MY - 1) / (MX * MY);
+  // planes of U, V, W (tile plus one-cell halo) arrive by tensor-map TMA in
+  // a ring of kRingSlots slots, as in k_momentum
+  typedef SlotLayout<T, 3, 0> Lay;
+  extern __shared__ __align__(128) unsigned char dyn_smem[];
+  T *ring = reinterpret_cast<T *>(dyn_smem);
+  __shared__ __align__(8) uint64_t bars[kRingSlots];
+  __shared__ int abort_flag;
   const int tx = threadIdx.x % MX, ty = threadIdx.x / MX;
+  if (smem_addr(ring) & 127u) {  // tensor copies need 128-byte aligned destinations
+    if (threadIdx.x == 0) doms[0].flags[1] = 1;
+    return;
+  }
+  if (threadIdx.x == 0) {
+    for (int s2 = 0; s2 < kRingSlots; s2++) mbar_init(&bars[s2], 1);
+    abort_flag = 0;
+    fence_async_shared();
+  }
+  __syncthreads();
+  uint32_t phase = 0;  // bit s: parity of the next wait on slot s
   for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
     const int di = find_dom(L.starts, L.nd, t);
     const Dom<T> &d = doms[di];
@@ -567,31 +643,16 @@ __global__ void __launch_bounds__(MX *MY, 3) k_sgs(const Dom<T> *__restrict__ do
     const int k1 = min(k0 + MKC - 1, d.nz);
     const int i = i0 + tx, j = j0 + ty;
     const int nx = d.nx, ny = d.ny, nz = d.nz;
-    const long long pitch = d.pitch, plane = d.plane;
-    const T *__restrict__ F[3] = {d.U, d.V, d.W};
-    T *__restrict__ nu = d.nu;
-    int goff[NPF];
-    bool gok[NPF];
-#pragma unroll
-    for (int q = 0; q < NPF; q++) {
-      int e = threadIdx.x + q * MX * MY;
-      int li = e % MPW, lj = e / MPW;
-      int gi = i0 - 1 + li, gj = j0 - 1 + lj;
-      gok[q] = e < MPS && gi <= nx + 1 && gj <= ny + 1;
-      goff[q] = gok[q] ? (d.aln - 1 + gi) + (int)pitch * gj : 0;
+    const int wide[3] = {F_U, F_V, F_W};
+    const int none[1] = {0};
+    const CUtensorMap *maps = reinterpret_cast<const CUtensorMap *>(d.tmaps);
+    __syncthreads();  // every slot of the previous tile is free
+    if (threadIdx.x == 0) {
+      fence_async_shared();
+      for (int kk = k0 - 1; kk <= min(k0 - 1 + kRingSlots - 1, k1 + 1); kk++)
+        issue_plane<T, 3, 0>(ring + (kk % kRingSlots) * Lay::SIZE, &bars[kk % kRingSlots], maps, wide, none, false,
+                             d.aln, i0, j0, kk);
     }
-    __syncthreads();
-    for (int kk = k0 - 1; kk <= k0 + 1; kk++) {
-      T *dst = ring[kk % 3];
-#pragma unroll
-      for (int f = 0; f < 3; f++)
-#pragma unroll
-        for (int q = 0; q < NPF; q++) {
-          int e = threadIdx.x + q * MX * MY;
-          if (e < MPS) dst[f * MPS + e] = gok[q] ? __ldg(F[f] + goff[q] + plane * kk) : (T)0;
-        }
-    }
-    __syncthreads();
     const bool inside = i <= nx && j <= ny;
     // block-uniform: the wall sides whose wall-model points this tile can
     // hold (a point sits next to its side: i in {1, nx-1, nx} and so on)
@@ -605,30 +666,32 @@ __global__ void __launch_bounds__(MX *MY, 3) k_sgs(const Dom<T> *__restrict__ do
     q.rdx = (T)(1.0 / d.dx); q.rdy = (T)(1.0 / d.dy);
     q.r4dx = (T)(1.0 / (4 * d.dx)); q.r4dy = (T)(1.0 / (4 * d.dy));
     const double *tr = d.sgs_rdz, *t2 = d.sgs_r2zz, *tw = d.sgs_wc2;
+    T *__restrict__ nu = d.nu;
+    const int o = (ty + 1) * Lay::SPW + (tx + Lay::XO);
+    long long c = bidx(d, inside ? i : 1, inside ? j : 1, k0);
+    const long long plane = d.plane;
     for (int k = k0; k <= k1; k++) {
       q.rdz = (T)tr[k]; q.r2zz = (T)t2[k]; q.wc2 = (T)tw[k];
-      const bool more = k + 1 <= k1;
-      T pre[3][NPF];
-      if (more) {
-#pragma unroll
-        for (int f = 0; f < 3; f++)
-#pragma unroll
-          for (int q = 0; q < NPF; q++) pre[f][q] = gok[q] ? __ldg(F[f] + goff[q] + plane * (k + 2)) : (T)0;
+      // planes k-1, k, k+1 must have landed
+      bool ok = true;
+      for (int kk = (k == k0 ? k0 - 1 : k + 1); kk <= k + 1; kk++) {
+        const int s2 = kk % kRingSlots;
+        ok &= mbar_wait(&bars[s2], (phase >> s2) & 1u);
+        phase ^= 1u << s2;
       }
-      if (inside) {
-        Ring<T> R;
-        R.p[0] = ring[(k - 1) % 3];
-        R.p[1] = ring[k % 3];
-        R.p[2] = ring[(k + 1) % 3];
-        R.o = (ty + 1) * MPW + (tx + 1);
-        T v;
+      if (!ok) { abort_flag = 1; d.flags[1] = 1; }
+      if (inside && ok) {
+        WideRing<T, 3, 0> R;
+        R.p[0] = ring + ((k - 1) % kRingSlots) * Lay::SIZE;
+        R.p[1] = ring + (k % kRingSlots) * Lay::SIZE;
+        R.p[2] = ring + ((k + 1) % kRingSlots) * Lay::SIZE;
+        R.o = o;
+        T v = num;
         if (sgs) {
           v = nusmag_ring(q, R);
           if (addmol) v = v + num;
-        } else {
-          v = num;
         }
-        nu[bidx(d, i, j, k)] = v;
+        nu[c] = v;
         const int wk = wtile | (wmask & ((k == 1 ? 16 : 0) | (k >= nz - 1 ? 32 : 0)));
         if (wk) {
 #pragma unroll 1
@@ -642,18 +705,25 @@ __global__ void __launch_bounds__(MX *MY, 3) k_sgs(const Dom<T> *__restrict__ do
           }
         }
       }
-      __syncthreads();
-      if (more) {
-        T *dst = ring[(k + 2) % 3];
-#pragma unroll
-        for (int f = 0; f < 3; f++)
-#pragma unroll
-          for (int q = 0; q < NPF; q++) {
-            int e = threadIdx.x + q * MX * MY;
-            if (e < MPS) dst[f * MPS + e] = pre[f][q];
+      __syncthreads();  // plane k-1 is no longer read
+      if (abort_flag) {
+        // a plane did not arrive: wait (bounded) for the copies still in
+        // flight into this block's shared memory, then give up
+        if (threadIdx.x == 0)
+          for (int kk = k + 2; kk <= min(k - 1 + kRingSlots - 1, k1 + 1); kk++) {
+            const int s2 = kk % kRingSlots;
+            mbar_wait(&bars[s2], (phase >> s2) & 1u);
+            phase ^= 1u << s2;
           }
+        return;
       }
-      __syncthreads();
+      const int kn = k - 1 + kRingSlots;
+      if (threadIdx.x == 0 && kn <= k1 + 1) {
+        fence_async_shared();
+        issue_plane<T, 3, 0>(ring + (kn % kRingSlots) * Lay::SIZE, &bars[kn % kRingSlots], maps, wide, none, false,
+                             d.aln, i0, j0, kn);
+      }
+      c += plane;
     }
   }
 }
