@@ -361,7 +361,7 @@ struct BatchT {
       if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, threads, sm) != cudaSuccess || b < 1) b = 1;
       return b * nsm;
     };
-    grid_cap[0] = cap((const void *)k_sgs<T>, MX * MY, smem_sgs);
+    grid_cap[0] = cap((const void *)k_sgs<T>, SgsShape<T>::threads, smem_sgs);
     grid_cap[1] = cap((const void *)k_momentum<T>, MomShape<T>::threads, smem_mom);
     grid_cap[2] = cap((const void *)k_fftx_fwd<T>, kFFTThreads, smem_x);
     grid_cap[3] = cap((const void *)k_ffty<T>, kFFTThreads, smem_y);
@@ -621,7 +621,7 @@ struct BatchT {
   }
   int launch_sgs() {
     nlaunch++;
-    k_sgs<T><<<gsz(0, ls[LK_MOM].total), MX * MY, smem_sgs, stream>>>(ddom, ls[LK_MOM].l());
+    k_sgs<T><<<gsz(0, ls[LK_MOM].total), SgsShape<T>::threads, smem_sgs, stream>>>(ddom, ls[LK_MOM].l());
     launch_ghosts({F_NU}, 0);
     return ELMM_OK;
   }
@@ -873,7 +873,7 @@ struct BatchT {
         cudaEventRecord(ev[2 * slot.size() + 1], stream);
         slot.push_back(k);
       };
-      timed(0, [&] { k_sgs<T><<<gsz(0, ls[LK_MOM].total), MX * MY, smem_sgs, stream>>>(ddom, ls[LK_MOM].l()); });
+      timed(0, [&] { k_sgs<T><<<gsz(0, ls[LK_MOM].total), SgsShape<T>::threads, smem_sgs, stream>>>(ddom, ls[LK_MOM].l()); });
       timed(kGhost, [&] { launch_ghosts({F_NU}, 0); });
       timed(1, [&] {
         k_momentum<T><<<gsz(1, ls[LK_MOM].total), MomShape<T>::threads, smem_mom, stream>>>(ddom, ls[LK_MOM].l(), sc);

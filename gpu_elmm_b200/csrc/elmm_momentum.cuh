@@ -605,21 +605,68 @@ __device__ __forceinline__ T nusmag_ring(const SgsK<T> &q, const RT &R) {
   return Sbar * q.wc2;
 }
 
+// nusmag_ring for a pair of x-adjacent cells with packed FP32x2 arithmetic;
+// the square root is taken per cell
+template <typename RT>
+__device__ __forceinline__ F2 nusmag2(const SgsK<float> &q, const RT &R) {
+#define GU(dx, dy, dz) R.g(0, dx, dy, dz)
+#define GV(dx, dy, dz) R.g(1, dx, dy, dz)
+#define GW(dx, dy, dz) R.g(2, dx, dy, dz)
+  const F2 rdx = bc2(q.rdx), rdy = bc2(q.rdy), rdz = bc2(q.rdz), r4dx = bc2(q.r4dx), r4dy = bc2(q.r4dy),
+           r2zz = bc2(q.r2zz), half = bc2(0.5f);
+  const F2 D00 = (GU(0, 0, 0) - GU(-1, 0, 0)) * rdx;
+  const F2 D11 = (GV(0, 0, 0) - GV(0, -1, 0)) * rdy;
+  const F2 D22 = (GW(0, 0, 0) - GW(0, 0, -1)) * rdz;
+  const F2 D01 = (((GU(0, 1, 0) + GU(-1, 1, 0)) - GU(0, -1, 0)) - GU(-1, -1, 0)) * r4dy;
+  const F2 D02 = (((GU(0, 0, 1) + GU(-1, 0, 1)) - GU(0, 0, -1)) - GU(-1, 0, -1)) * r2zz;
+  const F2 D10 = (((GV(1, 0, 0) + GV(1, -1, 0)) - GV(-1, 0, 0)) - GV(-1, -1, 0)) * r4dx;
+  const F2 D12 = (((GV(0, 0, 1) + GV(0, -1, 1)) - GV(0, 0, -1)) - GV(0, -1, -1)) * r2zz;
+  const F2 D20 = (((GW(1, 0, 0) + GW(1, 0, -1)) - GW(-1, 0, 0)) - GW(-1, 0, -1)) * r4dx;
+  const F2 D21 = (((GW(0, 1, 0) + GW(0, 1, -1)) - GW(0, -1, 0)) - GW(0, -1, -1)) * r4dy;
+#undef GU
+#undef GV
+#undef GW
+  F2 s, S = bc2(0.f);
+  s = (D00 + D00) * half; S = S + s * s;
+  s = (D10 + D01) * half; S = S + s * s;
+  s = (D20 + D02) * half; S = S + s * s;
+  s = (D01 + D10) * half; S = S + s * s;
+  s = (D11 + D11) * half; S = S + s * s;
+  s = (D21 + D12) * half; S = S + s * s;
+  s = (D02 + D20) * half; S = S + s * s;
+  s = (D12 + D21) * half; S = S + s * s;
+  s = (D22 + D22) * half; S = S + s * s;
+  const F2 Sbar{make_float2(sqrtf(2.f * S.v.x), sqrtf(2.f * S.v.y))};
+  return Sbar * bc2(q.wc2);
+}
+
 template <typename T>
 __device__ void wm_point(const Dom<T> &d, int comp, int f, int i, int j, int k, long long pidx);
 template <typename T>
 __device__ long long wm_plane_index(const Dom<T> &d, int comp, int f, int i, int j, int k);
 
+// Cells per thread of k_sgs: two for FP32 (packed arithmetic), one for FP64.
 template <typename T>
-__global__ void __launch_bounds__(MX *MY, 3) k_sgs(const Dom<T> *__restrict__ doms, Launch L) {
+struct SgsShape {
+  static constexpr int cpt = 1, threads = MX * MY, min_blocks = 3;
+};
+template <>
+struct SgsShape<float> {
+  static constexpr int cpt = 2, threads = MX * MY / 2, min_blocks = 6;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
+    k_sgs(const Dom<T> *__restrict__ doms, Launch L) {
   // planes of U, V, W (tile plus one-cell halo) arrive by tensor-map TMA in
   // a ring of kRingSlots slots, as in k_momentum
   typedef SlotLayout<T, 3, 0> Lay;
+  constexpr int CPT = SgsShape<T>::cpt, TXN = MX / CPT;
   extern __shared__ __align__(128) unsigned char dyn_smem[];
   T *ring = reinterpret_cast<T *>(dyn_smem);
   __shared__ __align__(8) uint64_t bars[kRingSlots];
   __shared__ int abort_flag;
-  const int tx = threadIdx.x % MX, ty = threadIdx.x / MX;
+  const int tx = threadIdx.x % TXN, ty = threadIdx.x / TXN;
   if (smem_addr(ring) & 127u) {  // tensor copies need 128-byte aligned destinations
     if (threadIdx.x == 0) doms[0].flags[1] = 1;
     return;
@@ -641,7 +688,7 @@ __global__ void __launch_bounds__(MX *MY, 3) k_sgs(const Dom<T> *__restrict__ do
     const int bk = lt / nty;
     const int i0 = bx * MX + 1, j0 = by * MY + 1, k0 = bk * MKC + 1;
     const int k1 = min(k0 + MKC - 1, d.nz);
-    const int i = i0 + tx, j = j0 + ty;
+    const int i = i0 + CPT * tx, j = j0 + ty;  // the thread's first cell
     const int nx = d.nx, ny = d.ny, nz = d.nz;
     const int wide[3] = {F_U, F_V, F_W};
     const int none[1] = {0};
@@ -653,7 +700,6 @@ __global__ void __launch_bounds__(MX *MY, 3) k_sgs(const Dom<T> *__restrict__ do
         issue_plane<T, 3, 0>(ring + (kk % kRingSlots) * Lay::SIZE, &bars[kk % kRingSlots], maps, wide, none, false,
                              d.aln, i0, j0, kk);
     }
-    const bool inside = i <= nx && j <= ny;
     // block-uniform: the wall sides whose wall-model points this tile can
     // hold (a point sits next to its side: i in {1, nx-1, nx} and so on)
     int wmask = 0;
@@ -667,8 +713,10 @@ __global__ void __launch_bounds__(MX *MY, 3) k_sgs(const Dom<T> *__restrict__ do
     q.r4dx = (T)(1.0 / (4 * d.dx)); q.r4dy = (T)(1.0 / (4 * d.dy));
     const double *tr = d.sgs_rdz, *t2 = d.sgs_r2zz, *tw = d.sgs_wc2;
     T *__restrict__ nu = d.nu;
-    const int o = (ty + 1) * Lay::SPW + (tx + Lay::XO);
-    long long c = bidx(d, inside ? i : 1, inside ? j : 1, k0);
+    const int o = (ty + 1) * Lay::SPW + (CPT * tx + Lay::XO);
+    const bool inside0 = i <= nx && j <= ny;
+    const bool pair_inside = i + CPT - 1 <= nx && j <= ny;
+    long long c = bidx(d, inside0 ? i : 1, inside0 ? j : 1, k0);
     const long long plane = d.plane;
     for (int k = k0; k <= k1; k++) {
       q.rdz = (T)tr[k]; q.r2zz = (T)t2[k]; q.wc2 = (T)tw[k];
@@ -680,27 +728,45 @@ __global__ void __launch_bounds__(MX *MY, 3) k_sgs(const Dom<T> *__restrict__ do
         phase ^= 1u << s2;
       }
       if (!ok) { abort_flag = 1; d.flags[1] = 1; }
-      if (inside && ok) {
-        WideRing<T, 3, 0> R;
-        R.p[0] = ring + ((k - 1) % kRingSlots) * Lay::SIZE;
-        R.p[1] = ring + (k % kRingSlots) * Lay::SIZE;
-        R.p[2] = ring + ((k + 1) % kRingSlots) * Lay::SIZE;
-        R.o = o;
-        T v = num;
-        if (sgs) {
-          v = nusmag_ring(q, R);
-          if (addmol) v = v + num;
+      const T *p0s = ring + ((k - 1) % kRingSlots) * Lay::SIZE, *p1s = ring + (k % kRingSlots) * Lay::SIZE,
+              *p2s = ring + ((k + 1) % kRingSlots) * Lay::SIZE;
+      if (ok && CPT == 2 && sgs && pair_inside) {
+        if constexpr (CPT == 2) {
+          Ring2<Lay::WB, Lay::SPW> R2;
+          R2.p[0] = p0s; R2.p[1] = p1s; R2.p[2] = p2s;
+          R2.o = o;
+          F2 v = nusmag2(q, R2);
+          if (addmol) v = v + bc2(num);
+          *reinterpret_cast<float2 *>(nu + c) = v.v;
         }
-        nu[c] = v;
-        const int wk = wtile | (wmask & ((k == 1 ? 16 : 0) | (k >= nz - 1 ? 32 : 0)));
-        if (wk) {
+      } else if (ok) {
+#pragma unroll
+        for (int qc = 0; qc < CPT; qc++) {
+          if (!(i + qc <= nx && j <= ny)) continue;
+          WideRing<T, 3, 0> R;
+          R.p[0] = p0s; R.p[1] = p1s; R.p[2] = p2s;
+          R.o = o + qc;
+          T v = num;
+          if (sgs) {
+            v = nusmag_ring(q, R);
+            if (addmol) v = v + num;
+          }
+          nu[c + qc] = v;
+        }
+      }
+      const int wk = wtile | (wmask & ((k == 1 ? 16 : 0) | (k >= nz - 1 ? 32 : 0)));
+      if (ok && wk) {
+#pragma unroll 1
+        for (int qc = 0; qc < CPT; qc++) {
+          const int iq = i + qc;
+          if (!(iq <= nx && j <= ny)) continue;
 #pragma unroll 1
           for (int f = 0; f < 6; f++) {
             if (!((wk >> f) & 1)) continue;
 #pragma unroll 1
             for (int comp = 0; comp < 3; comp++) {
-              long long p = wm_plane_index(d, comp, f, i, j, k);
-              if (p >= 0) wm_point(d, comp, f, i, j, k, p);
+              long long p = wm_plane_index(d, comp, f, iq, j, k);
+              if (p >= 0) wm_point(d, comp, f, iq, j, k, p);
             }
           }
         }
