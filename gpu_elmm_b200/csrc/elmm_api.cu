@@ -628,8 +628,9 @@ struct BatchT {
   int launch_momentum(int stage) {
     StageCoef sc{kRho[stage - 1], kBeta[stage - 1], 2 * kAlpha[stage - 1], stage};
     nlaunch++;
+    // no ghost pass for U2, V2, W2: their only reader, the divergence of the
+    // forward x transform, folds its neighbours on the box faces itself
     k_momentum<T><<<gsz(1, ls[LK_MOM].total), MomShape<T>::threads, smem_mom, stream>>>(ddom, ls[LK_MOM].l(), sc);
-    launch_ghosts({F_U2, F_V2, F_W2}, 0);
     return ELMM_OK;
   }
   void launch_project(double coef_alpha2, int use_dt, int in_place, int gate) {
@@ -692,15 +693,15 @@ struct BatchT {
       k_fftx_inv<T><<<gsz(5, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan, gate);
     }
   }
-  // the five transform kernels and the ghosts of Phi; rhs_from_phi: the
-  // right-hand side is in Phi
+  // the five transform kernels; rhs_from_phi: the right-hand side is in Phi.
+  // Phi gets no ghost pass: its only reader, k_project, folds the i+1, j+1,
+  // k+1 neighbours on the box faces itself.
   void launch_poisson(double coef_alpha2, int use_dt, int rhs_from_phi, int gate) {
     launch_fftx_fwd(coef_alpha2, use_dt, rhs_from_phi, gate);
     launch_ffty(0, gate);
     launch_tri(gate);
     launch_ffty(1, gate);
     launch_fftx_inv(gate);
-    launch_ghosts({F_PHI}, gate);
   }
   int max_refine() const {
     int m = 0;
@@ -878,13 +879,11 @@ struct BatchT {
       timed(1, [&] {
         k_momentum<T><<<gsz(1, ls[LK_MOM].total), MomShape<T>::threads, smem_mom, stream>>>(ddom, ls[LK_MOM].l(), sc);
       });
-      timed(kGhost, [&] { launch_ghosts({F_U2, F_V2, F_W2}, 0); });
       timed(2, [&] { launch_fftx_fwd(a2, 1, 0, 0); });
       timed(3, [&] { launch_ffty(0, 0); });
       timed(4, [&] { launch_tri(0); });
       timed(5, [&] { launch_ffty(1, 0); });
       timed(6, [&] { launch_fftx_inv(0); });
-      timed(kGhost, [&] { launch_ghosts({F_PHI}, 0); });
       timed(7, [&] { k_project<T><<<gsz(6, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l(), a2, 1, 0, 0); });
       timed(kGhost, [&] { launch_ghosts({F_U, F_V, F_W, F_P}, 0); });
       timed(8, [&] { k_prref<T><<<std::min(nd, 1024), 256, 0, stream>>>(ddom, nd, 0); });

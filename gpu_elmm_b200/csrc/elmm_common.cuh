@@ -231,6 +231,21 @@ __device__ __forceinline__ void push_vel(const Dom<T> &d, T *F, int comp, int i,
   push_ghosts(d, F, ix, iy, iz, v);
 }
 
+// Velocity component comp at any index of its one-deep shell, read from the
+// interior: a ghost index folds onto its source by the BoundUVW rules.
+// Kernels use it for the few neighbours on a box face instead of relying on
+// the device ghost cells.
+template <typename T>
+__device__ __forceinline__ T vel_folded(const Dom<T> &d, const T *F, int comp, int i, int j, int k) {
+  const int *e = d.ext[comp];
+  const Fold fx = fold_vel(i, e[0], d.bt[0], d.bt[1], comp == 0);
+  const Fold fy = fold_vel(j, e[1], d.bt[2], d.bt[3], comp == 1);
+  const Fold fz = fold_vel(k, e[2], d.bt[4], d.bt[5], comp == 2);
+  if (fx.zero | fy.zero | fz.zero) return (T)0;
+  const T v = __ldg(F + bidx(d, fx.src, fy.src, fz.src));
+  return fx.sign * fy.sign * fz.sign < 0 ? -v : v;
+}
+
 // Domain lookup of a flattened tile index (batched launches).
 __device__ __forceinline__ int find_dom(const int *starts, int nd, int t) {
   int lo = 0, hi = nd - 1;

@@ -221,8 +221,20 @@ __global__ void __launch_bounds__(kFFTThreads) k_fftx_fwd(const Dom<T> *__restri
           rhs = ld((const T *)d.Phi, c) * rdt2;
         } else {
           const T rdzk = d.vz ? (T)d.sgs_rdz[k] : rdz;
-          T div = (ld(U2, c) - ld(U2, c - 1)) * rdx + (ld(V2, c) - ld(V2, c - d.pitch)) * rdy +
-                  (ld(W2, c) - ld(W2, c - d.plane)) * rdzk - (T)0;
+          // on a box face the neighbours fold onto the interior (BoundUVW)
+          const bool face = i == 1 || i > d.ext[0][0] || j == 1 || j > d.ext[1][1] || k == 1 || k > d.ext[2][2] ||
+                            j > d.ext[0][1] || j > d.ext[2][1] || k > d.ext[0][2] || k > d.ext[1][2];
+          T uc, uw, vc, vs, wc, wb;
+          if (!face) {
+            uc = ld(U2, c); uw = ld(U2, c - 1);
+            vc = ld(V2, c); vs = ld(V2, c - d.pitch);
+            wc = ld(W2, c); wb = ld(W2, c - d.plane);
+          } else {
+            uc = vel_folded(d, U2, 0, i, j, k); uw = vel_folded(d, U2, 0, i - 1, j, k);
+            vc = vel_folded(d, V2, 1, i, j, k); vs = vel_folded(d, V2, 1, i, j - 1, k);
+            wc = vel_folded(d, W2, 2, i, j, k); wb = vel_folded(d, W2, 2, i, j, k - 1);
+          }
+          T div = (uc - uw) * rdx + (vc - vs) * rdy + (wc - wb) * rdzk;
           rhs = div * rdt2;
         }
       }

@@ -95,9 +95,15 @@ __global__ void __launch_bounds__(MX *MY) k_project(const Dom<T> *__restrict__ d
     const bool hw = inside && i <= d.ext[2][0] && j <= d.ext[2][1];
     const T m = (T)(*d.prm);
     long long c = bidx(d, inside ? i : 1, inside ? j : 1, k0);
+    // Phi at i+1, j+1, k+1: past the last cell the neighbour folds onto the
+    // interior as Bound_Phi fills it (periodic copy, else the cell itself)
+    const bool px = d.bt[SIDE_WE] == BC_PERIODIC, py = d.bt[SIDE_SO] == BC_PERIODIC, pz = d.bt[SIDE_BO] == BC_PERIODIC;
+    const long long oe = i < nx ? 1 : (px ? 1 - nx : 0);
+    const long long on = j < ny ? pitch : (py ? pitch - (long long)ny * pitch : 0);
+    auto ot = [&](int kk) -> long long { return kk < nz ? plane : (pz ? plane - (long long)nz * plane : 0); };
     T phi = 0, pe = 0, pn = 0, pt = 0, u0 = 0, v0 = 0, w0 = 0, p0 = 0;
     if (inside) {
-      phi = __ldg(Phi + c); pe = __ldg(Phi + c + 1); pn = __ldg(Phi + c + pitch); pt = __ldg(Phi + c + plane);
+      phi = __ldg(Phi + c); pe = __ldg(Phi + c + oe); pn = __ldg(Phi + c + on); pt = __ldg(Phi + c + ot(k0));
       if (hu) u0 = __ldg(Usrc + c);
       if (hv) v0 = __ldg(Vsrc + c);
       if (hw) w0 = __ldg(Wsrc + c);
@@ -108,7 +114,7 @@ __global__ void __launch_bounds__(MX *MY) k_project(const Dom<T> *__restrict__ d
       T npe = 0, npn = 0, npt = 0, nu0 = 0, nv0 = 0, nw0 = 0, np0 = 0;
       if (more && inside) {
         const long long cn = c + plane;
-        npe = __ldg(Phi + cn + 1); npn = __ldg(Phi + cn + pitch); npt = __ldg(Phi + cn + plane);
+        npe = __ldg(Phi + cn + oe); npn = __ldg(Phi + cn + on); npt = __ldg(Phi + cn + ot(k + 1));
         if (hu) nu0 = __ldg(Usrc + cn);
         if (hv) nv0 = __ldg(Vsrc + cn);
         if (hw) nw0 = __ldg(Wsrc + cn);

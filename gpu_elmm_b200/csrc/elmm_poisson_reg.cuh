@@ -18,14 +18,50 @@ constexpr int kRegThreads = 256;
 template <typename T, int N>
 constexpr int fft_reg_min_blocks() { return N / fplan_P(N) <= 16 ? (sizeof(T) == 4 ? 3 : 2) : 1; }
 
-// right-hand side at box index c: the divergence of (U2, V2, W2) / coef, or
-// the value already stored in Phi (PoisSolver interface, defect correction)
+// The reads of the divergence stencil of one x row (j, k) of the x
+// transforms.  Away from the box faces the neighbours are the adjacent box
+// cells; on a face a neighbour folds onto an interior cell as BoundUVW fills
+// the ghost, so each read is scale * F[c + offset] with scale in {1, -1, 0}
+// (exact).  x and y are periodic (the FFT solve requires it), so only the
+// i = 0 column folds in x.
 template <typename T>
-__device__ __forceinline__ T poisson_rhs(const Dom<T> &d, long long c, T rdx, T rdy, T rdzk, T rdt2, int rhs_from_phi) {
+struct RhsRow {
+  long long o_uw1, o_vs, o_wc, o_wb;  // offsets: U2 at i - 1 for i = 1, V2 at j - 1, W2 at k, W2 at k - 1
+  T s_uw1, s_vs, s_wc, s_wb;
+};
+
+template <typename T>
+__device__ __forceinline__ RhsRow<T> rhs_row(const Dom<T> &d, int j, int k) {
+  RhsRow<T> r;
+  const long long pitch = d.pitch, plane = d.plane;
+  auto fold = [&](int comp, int axis, int g, long long stride, long long &off, T &scale) {
+    const int *e = d.ext[comp];
+    const Fold f = fold_vel(g, e[axis], d.bt[2 * axis], d.bt[2 * axis + 1], comp == axis);
+    const int own = axis == 0 ? 1 : axis == 1 ? j : k;  // the interior index the row itself sits at
+    off = f.zero ? 0 : (long long)(f.src - own) * stride;
+    scale = f.zero ? (T)0 : (T)f.sign;
+  };
+  fold(0, 0, 0, 1, r.o_uw1, r.s_uw1);
+  fold(1, 1, j - 1, pitch, r.o_vs, r.s_vs);
+  fold(2, 2, k, plane, r.o_wc, r.s_wc);
+  fold(2, 2, k - 1, plane, r.o_wb, r.s_wb);
+  return r;
+}
+
+// right-hand side at interior cell i of a row, box index c: the divergence
+// of (U2, V2, W2) / coef, or the value already stored in Phi (PoisSolver
+// interface, defect correction)
+template <typename T>
+__device__ __forceinline__ T poisson_rhs(const Dom<T> &d, const RhsRow<T> &r, long long c, int i, T rdx, T rdy,
+                                         T rdzk, T rdt2, int rhs_from_phi) {
   if (rhs_from_phi) return ld((const T *)d.Phi, c) * rdt2;
-  const T div = (ld((const T *)d.U2, c) - ld((const T *)d.U2, c - 1)) * rdx +
-                (ld((const T *)d.V2, c) - ld((const T *)d.V2, c - d.pitch)) * rdy +
-                (ld((const T *)d.W2, c) - ld((const T *)d.W2, c - d.plane)) * rdzk;
+  const T *U2 = d.U2, *V2 = d.V2, *W2 = d.W2;
+  const long long ouw = i == 1 ? r.o_uw1 : -1;
+  const T suw = i == 1 ? r.s_uw1 : (T)1;
+  const T uc = ld(U2, c), uw = suw * ld(U2, c + ouw);
+  const T vc = ld(V2, c), vs = r.s_vs * ld(V2, c + r.o_vs);
+  const T wc = r.s_wc * ld(W2, c + r.o_wc), wb = r.s_wb * ld(W2, c + r.o_wb);
+  const T div = (uc - uw) * rdx + (vc - vs) * rdy + (wc - wb) * rdzk;
   return div * rdt2;
 }
 
@@ -48,12 +84,13 @@ __device__ __forceinline__ void fftx_fwd_tile(const Dom<T> &d, int lt, typename 
   const T rdt2 = (T)(1.0 / coef);
   const T rdx = (T)(1.0 / d.dx), rdy = (T)(1.0 / d.dy), rdz = (T)(1.0 / d.dz);
   const T rdza = (d.vz && va) ? (T)d.sgs_rdz[ka] : rdz, rdzb = (d.vz && vb) ? (T)d.sgs_rdz[kb] : rdz;
+  const RhsRow<T> rwa = rhs_row(d, qa - (ka - 1) * ny + 1, ka), rwb = rhs_row(d, qb - (kb - 1) * ny + 1, kb);
   T2 v[E];
 #pragma unroll
   for (int e = 0; e < E; e++) {
-    const int i0 = t + P * e;
-    v[e].x = va ? poisson_rhs(d, ca + i0, rdx, rdy, rdza, rdt2, rhs_from_phi) : (T)0;
-    v[e].y = vb ? poisson_rhs(d, cb + i0, rdx, rdy, rdzb, rdt2, rhs_from_phi) : (T)0;
+    const int i = t + P * e + 1;
+    v[e].x = va ? poisson_rhs(d, rwa, ca + i - 1, i, rdx, rdy, rdza, rdt2, rhs_from_phi) : (T)0;
+    v[e].y = vb ? poisson_rhs(d, rwb, cb + i - 1, i, rdx, rdy, rdzb, rdt2, rhs_from_phi) : (T)0;
   }
   T2 *sh = smem + s * Pl::SEQ;
   fft_reg<T, T2, N, false>(v, sh, t, d.twx);
