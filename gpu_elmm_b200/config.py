@@ -11,10 +11,10 @@ from dataclasses import dataclass
 
 import numpy as np
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 # Boundary-condition codes of src/parameters.f90:249-250.
-BC_NOSLIP, BC_FREESLIP, BC_PERIODIC, BC_NEUMANN = 1, 2, 3, 5
+BC_NOSLIP, BC_FREESLIP, BC_PERIODIC, BC_DIRICHLET, BC_NEUMANN, BC_CONSTFLUX = 1, 2, 3, 4, 5, 6
 # Sides We, Ea, So, No, Bo, To (src/parameters.f90:193, zero-based here).
 WE, EA, SO, NO, BO, TO = range(6)
 
@@ -23,6 +23,7 @@ PREC_FP64, PREC_MIXED = 0, 1
 FIELD_U, FIELD_V, FIELD_W, FIELD_PR, FIELD_VISCOSITY = 0, 1, 2, 3, 4
 FIELD_U2, FIELD_V2, FIELD_W2 = 5, 6, 7
 FIELD_USTAR, FIELD_VSTAR, FIELD_WSTAR, FIELD_PHI = 8, 9, 10, 11
+FIELD_TEMPERATURE, FIELD_TDIFF, FIELD_TEMPERATURE_ADV = 12, 13, 14
 
 STATUS_NAMES = {
     0: "ELMM_OK", 1: "ELMM_ERR_INVALID_CONFIG", 2: "ELMM_ERR_OOM", 3: "ELMM_ERR_NAN",
@@ -53,6 +54,12 @@ class ElmmConfig(C.Structure):
         ("refine_tol", C.c_double),
         ("enable_CFL_check", C.c_int32),
         ("device", C.c_int32),
+        ("enable_buoyancy", C.c_int32),
+        ("TempBtype", C.c_int32 * 6),
+        ("sideTemp", C.c_double * 6),
+        ("temperature_ref", C.c_double),
+        ("grav_acc", C.c_double),
+        ("molecular_diffusivity", C.c_double),
     ]
 
 
@@ -131,6 +138,10 @@ class Grid:
     def shape_rhs(self):
         return (self.Prnz + 2, self.Prny + 2, self.Prnx + 2)
 
+    def shape_t(self):
+        """Temperature(-2:Prnx+3,-2:Prny+3,-2:Prnz+3)."""
+        return (self.Prnz + 6, self.Prny + 6, self.Prnx + 6)
+
     def cells(self):
         return self.Prnx * self.Prny * self.Prnz
 
@@ -140,10 +151,13 @@ def make_config(Prnx, Prny, Prnz, *, btype=(BC_PERIODIC, BC_PERIODIC, BC_PERIODI
                 dx=1.0, dy=1.0, dz=1.0, dt=0.02, nu=1.0 / 70000, cs=0.1, sgstype=1,
                 wallmodeltype=None, z0=0.01, precision=PREC_FP64, zW=None,
                 pr_gradient_x=None, pr_gradient_y=None, max_refine_sweeps=0,
-                refine_tol=1e-6, cfl_check=0, device=0, origin=(0.0, 0.0, 0.0)):
+                refine_tol=1e-6, cfl_check=0, device=0, origin=(0.0, 0.0, 0.0), buoyancy=False,
+                temperature_ref=295.0, grav_acc=9.81, prandtl=0.7):
     """Builds an ElmmConfig.  The wall model defaults to on when an SGS model
     is on (src/initial.f90:2782-2787).  ``zW`` (Prnz+1 values) selects the
-    stretched-z grid; the array is kept alive on the returned struct."""
+    stretched-z grid; the array is kept alive on the returned struct.
+    ``buoyancy`` adds the potential-temperature field with adiabatic
+    (zero-flux) bottom and top and periodic x and y."""
     c = ElmmConfig()
     c.abi_version = ABI_VERSION
     c.Prnx, c.Prny, c.Prnz = Prnx, Prny, Prnz
@@ -178,6 +192,13 @@ def make_config(Prnx, Prny, Prnz, *, btype=(BC_PERIODIC, BC_PERIODIC, BC_PERIODI
     c.refine_tol = refine_tol
     c.enable_CFL_check = cfl_check
     c.device = device
+    c.enable_buoyancy = 1 if buoyancy else 0
+    for s in range(6):
+        c.TempBtype[s] = BC_PERIODIC if btype[s] == BC_PERIODIC else BC_CONSTFLUX
+        c.sideTemp[s] = 0.0
+    c.temperature_ref = temperature_ref
+    c.grav_acc = grav_acc
+    c.molecular_diffusivity = nu / prandtl
     return c
 
 

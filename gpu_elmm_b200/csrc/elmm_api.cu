@@ -20,6 +20,7 @@
 #include "../../include/elmm_gpu.h"
 #include "elmm_kernels2.cuh"
 #include "elmm_poisson_reg.cuh"
+#include "elmm_temperature.cuh"
 
 using namespace elmm;
 
@@ -180,6 +181,19 @@ static int check_config(const elmm_config &c) {
     for (int s = 0; s < 6; s++)
       if (c.Btype[s] == ELMM_BC_NOSLIP && !(c.z0[s] > 0))
         return fail(ELMM_ERR_INVALID_CONFIG, "only the rough-wall (z0 > 0) wall model is implemented");
+  if (c.enable_buoyancy) {
+    for (int s = 0; s < 6; s++) {
+      const bool per = c.Btype[s] == ELMM_BC_PERIODIC;
+      if (per && c.TempBtype[s] != ELMM_BC_PERIODIC)
+        return fail(ELMM_ERR_INVALID_CONFIG, "the temperature must be periodic where the flow is");
+      if (!per && !(c.TempBtype[s] == ELMM_BC_CONSTFLUX && c.sideTemp[s] == 0))
+        return fail(ELMM_ERR_INVALID_CONFIG,
+                    "temperature walls must be adiabatic (ELMM_BC_CONSTFLUX with sideTemp = 0)");
+    }
+    if (c.zW) return fail(ELMM_ERR_INVALID_CONFIG, "the temperature field needs a uniform z grid");
+    if (!(c.temperature_ref > 0) || !(c.molecular_diffusivity >= 0))
+      return fail(ELMM_ERR_INVALID_CONFIG, "temperature_ref must be positive and molecular_diffusivity non-negative");
+  }
   return ELMM_OK;
 }
 
@@ -588,6 +602,16 @@ struct BatchT {
         std::vector<double> ones(np, 1.0);  // WMPointUVW%ustar = 1 initially (wallmodels.f90:80)
         CU(cudaMemcpy(h.wm_ustar[f], ones.data(), np * sizeof(double), cudaMemcpyHostToDevice));
       }
+    if (c.enable_buoyancy) {
+      h.buoy = 1;
+      for (int s2 = 0; s2 < 6; s2++) h.tbt[s2] = c.TempBtype[s2];
+      h.tref = c.temperature_ref;
+      h.grav = c.grav_acc;
+      h.kappa_mol = c.molecular_diffusivity;
+      h.toff = sizeof(T) == 4 ? c.temperature_ref : 0.0;  // FP32 stores theta - T_ref
+      for (T **f : {&h.Tm, &h.Tn, &h.Tadv, &h.TDiff})
+        if ((r = dalloc((void **)f, alloc_elems * sizeof(T)))) return r;
+    }
     if ((r = dalloc((void **)&h.prm, sizeof(double)))) return r;
     h.nprpart = ((h.nx + MX - 1) / MX) * ((h.ny + MY - 1) / MY);
     if ((r = dalloc((void **)&h.prpart, sizeof(double) * h.nprpart))) return r;
@@ -639,6 +663,21 @@ struct BatchT {
                                                                    in_place, gate);
     launch_ghosts({F_U, F_V, F_W, F_P}, gate);
     k_prref<T><<<std::min(nd, 1024), 256, 0, stream>>>(ddom, nd, gate);
+  }
+  bool any_buoy() const {
+    for (auto &h : hdom)
+      if (h.buoy) return true;
+    return false;
+  }
+  // one ScalarRK3 stage of the temperature; the new value then becomes the
+  // current one (the stage reads the old value at neighbours while writing)
+  void launch_temperature(int stage) {
+    if (!any_buoy()) return;
+    nlaunch++;
+    k_temperature<T><<<gsz(7, ls[LK_CELLS].total), TX * TY, 0, stream>>>(ddom, ls[LK_CELLS].l(), kRho[stage - 1],
+                                                                          kBeta[stage - 1], stage == 1);
+    for (auto &h : hdom)
+      if (h.buoy) cudaMemcpyAsync(h.Tm, h.Tn, (size_t)h.plane * (h.nz + 2) * sizeof(T), cudaMemcpyDeviceToDevice, stream);
   }
   // PressureCorrection on U2 (in_place = 0) or on U itself (initial projection)
   int launch_projection(double coef_alpha2, int use_dt, int in_place) {
@@ -746,6 +785,7 @@ struct BatchT {
     launch_sgs();
     if (stop == 1) return ELMM_OK;
     launch_momentum(stage);
+    launch_temperature(stage);  // ScalarRK3 between Convection and the projection (tsteps.f90:132-135)
     if (stop == 2) return ELMM_OK;
     launch_projection(2 * kAlpha[stage - 1], 1, 0);
     launch_refine(2 * kAlpha[stage - 1], 1);
@@ -859,7 +899,7 @@ struct BatchT {
   int profile_stage(int stage, int reps, double *ms) {
     CU(cudaSetDevice(device));
     const int nk = ELMM_NKERNELS;
-    const int kGhost = nk - 1, nev = 2 * (nk + 3);
+    const int kGhost = 9, nev = 2 * (nk + 3);
     std::vector<cudaEvent_t> ev(nev);
     for (auto &e : ev) CU(cudaEventCreate(&e));
     std::vector<double> acc(nk, 0.0);
@@ -887,6 +927,7 @@ struct BatchT {
       timed(7, [&] { k_project<T><<<gsz(6, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l(), a2, 1, 0, 0); });
       timed(kGhost, [&] { launch_ghosts({F_U, F_V, F_W, F_P}, 0); });
       timed(8, [&] { k_prref<T><<<std::min(nd, 1024), 256, 0, stream>>>(ddom, nd, 0); });
+      timed(10, [&] { launch_temperature(stage); });
       CU(cudaStreamSynchronize(stream));
       CU(cudaGetLastError());
       for (size_t q = 0; q < slot.size(); q++) {
@@ -945,6 +986,25 @@ struct BatchT {
     return ELMM_OK;
   }
 
+  int upload_temperature(int d, const double *Th) {
+    if (d < 0 || d >= nd) return fail(ELMM_ERR_INVALID_ARG, "domain index");
+    if (!Th) return fail(ELMM_ERR_INVALID_ARG, "NULL temperature array");
+    if (!hdom[d].buoy) return fail(ELMM_ERR_INVALID_ARG, "no temperature field (enable_buoyancy is 0)");
+    CU(cudaSetDevice(device));
+    if (frame_pending) CU(cudaStreamWaitEvent(stream, ev_packed, 0));
+    const Dom<T> &h = hdom[d];
+    const size_t n = (size_t)(h.nx + 6) * (h.ny + 6) * (h.nz + 6);
+    CU(cudaMemsetAsync(dbad, 0, sizeof(int), stream));
+    CU(cudaMemcpyAsync(dstage, Th, n * sizeof(double), cudaMemcpyHostToDevice, stream));
+    k_unpack_temperature<T><<<256, 256, 0, stream>>>(ddom + d, dstage, dbad);
+    int bad = 0;
+    CU(cudaMemcpyAsync(&bad, dbad, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    CU(cudaStreamSynchronize(stream));
+    CU(cudaGetLastError());
+    if (bad) return fail(ELMM_ERR_NAN, "non-finite value in the uploaded temperature");
+    return ELMM_OK;
+  }
+
   // pack one field into dst (device, host layout); returns elements
   size_t pack(int d, int field, double *dst, cudaStream_t s) {
     const Dom<T> &h = hdom[d];
@@ -974,6 +1034,14 @@ struct BatchT {
         k_pack_scalar<T><<<256, 256, 0, s>>>(ddom + d, h.P, dst, hb, 1, 1, h.nx, h.ny, h.nz);
         return n;
       }
+      case ELMM_FIELD_TEMPERATURE: case ELMM_FIELD_TDIFF: case ELMM_FIELD_TEMPERATURE_ADV: {
+        const int lo = field == ELMM_FIELD_TDIFF ? -1 : -2;
+        const size_t n = (size_t)(h.nx + 2 * (1 - lo)) * (h.ny + 2 * (1 - lo)) * (h.nz + 2 * (1 - lo));
+        const T *Fs = field == ELMM_FIELD_TEMPERATURE ? h.Tm : field == ELMM_FIELD_TDIFF ? h.TDiff : h.Tadv;
+        k_pack_temperature<T><<<256, 256, 0, s>>>(ddom + d, Fs, dst, lo, field == ELMM_FIELD_TEMPERATURE ? h.toff : 0.0,
+                                                  field == ELMM_FIELD_TEMPERATURE_ADV);
+        return n;
+      }
       case ELMM_FIELD_VISCOSITY: case ELMM_FIELD_PHI: {
         HostBox hb = hbox_p(d);
         size_t n = (size_t)hb.n0 * hb.n1 * hb.n2;
@@ -988,7 +1056,9 @@ struct BatchT {
 
   int download_field(int d, int field, double *host) {
     if (d < 0 || d >= nd) return fail(ELMM_ERR_INVALID_ARG, "domain index");
-    if (field < 0 || field > ELMM_FIELD_PHI) return fail(ELMM_ERR_INVALID_ARG, "field id");
+    if (field < 0 || field > ELMM_FIELD_TEMPERATURE_ADV) return fail(ELMM_ERR_INVALID_ARG, "field id");
+    if (field >= ELMM_FIELD_TEMPERATURE && !hdom[d].buoy)
+      return fail(ELMM_ERR_INVALID_ARG, "no temperature field (enable_buoyancy is 0)");
     if (!host) return fail(ELMM_ERR_INVALID_ARG, "NULL host array");
     CU(cudaSetDevice(device));
     size_t n = pack(d, field, dstage, stream);
@@ -1137,6 +1207,10 @@ int elmm_config_defaults(elmm_config *c, int32_t Prnx, int32_t Prny, int32_t Prn
   for (int s = 0; s < 6; s++) c->z0[s] = 0.01;
   c->precision = ELMM_PREC_FP64;
   c->refine_tol = 1e-6;
+  for (int s = 0; s < 6; s++) c->TempBtype[s] = bt[s] == ELMM_BC_PERIODIC ? ELMM_BC_PERIODIC : ELMM_BC_CONSTFLUX;
+  c->temperature_ref = 295;                             // src/parameters.f90:220
+  c->grav_acc = 9.81;                                   // src/parameters.f90:146
+  c->molecular_diffusivity = c->molecular_viscosity / 0.7;  // src/parameters.f90:129
   return ELMM_OK;
 }
 
@@ -1168,6 +1242,11 @@ int elmm_download_state(elmm_handle *h, double *U, double *V, double *W, double 
 int elmm_download_field(elmm_handle *h, int32_t field, double *host) {
   if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
   return DISPATCH(h->b, download_field(0, field, host));
+}
+
+int elmm_upload_temperature(elmm_handle *h, const double *T) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  return DISPATCH(h->b, upload_temperature(0, T));
 }
 
 int elmm_frame_begin(elmm_handle *h) {

@@ -96,6 +96,14 @@ struct Dom {
   int *refine_count;     // sweeps run since the counter was reset
   double refine_tol;
   int max_refine;
+  // potential temperature (enable_buoyancy): box fields of the current and
+  // the next value, the stage tendency and the diffusivity.  Stored as
+  // theta - toff: toff = temperature_ref on the mixed path (FP32 keeps the
+  // perturbations' digits), 0 on the FP64 path.
+  int buoy;
+  int tbt[6];            // temperature BC per side
+  T *Tm, *Tn, *Tadv, *TDiff;
+  double toff, tref, grav, kappa_mol;
 };
 
 template <typename T>

@@ -56,8 +56,11 @@ __device__ __forceinline__ void fill_ctx(MomCtx<T> &m, const Dom<T> &d) {
 
 // one velocity component's tendency at (i,j,k): advection + diffusion +
 // wall corrections, in the reference's order of operations
+// bt, bsub: the buoyancy of W, (a + bt) - bsub after the advection
+// (BuoyancyForce, src/dynamics.f90:679-688; zero without a temperature field)
 template <typename T, int C, typename RT>
-__device__ __forceinline__ T tendency(const MomCtx<T> &m, const RT &R, int i, int j, int k, int wallhere) {
+__device__ __forceinline__ T tendency(const MomCtx<T> &m, const RT &R, int i, int j, int k, int wallhere,
+                                      T bt = (T)0, T bsub = (T)0) {
   // X(dx,dy,dz) with the component's own axis first: along = C, a1, a2 the others
 #define FU(dx, dy, dz) R.g(0, dx, dy, dz)
 #define FV(dx, dy, dz) R.g(1, dx, dy, dz)
@@ -238,6 +241,7 @@ __device__ __forceinline__ T tendency(const MomCtx<T> &m, const RT &R, int i, in
       a = a - (Bx * (we - ww) * Uadv + By * (wn - ws) * Vadv + (wt - wb) / (T)(m.zW[k + 1 + 2] - m.zW[k - 1 + 2]) * w);
     }
     a = a * (T)0.5;
+    a = (a + bt) - bsub;
     const T n0 = FN(0, 0, 0), ne = FN(1, 0, 0), nt = FN(0, 0, 1), nte = FN(1, 0, 1), nw = FN(-1, 0, 0), ntw = FN(-1, 0, 1);
     const T nn = FN(0, 1, 0), ntn = FN(0, 1, 1), ns = FN(0, -1, 0), nts = FN(0, -1, 1);
     a = a + (T)0.25 * (nte + ne + nt + n0) * (we - w) * rx;
@@ -439,6 +443,12 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
     // block-uniform: every cell of the tile has all three components
     const bool full_tile = i0 + MX - 1 <= min(d.ext[0][0], min(d.ext[1][0], d.ext[2][0])) &&
                            j0 + MY - 1 <= min(d.ext[0][1], min(d.ext[1][1], d.ext[2][1]));
+    // buoyancy of W (BuoyancyForce, src/dynamics.f90:679-688): A = g / T_ref;
+    // with theta stored as theta - T_ref the constant term cancels exactly
+    const bool buoy = d.buoy != 0;
+    const T bA2 = (T)(d.grav / d.tref / 2.0);
+    const T bsub = buoy && d.toff == 0 ? (T)(d.grav / d.tref * d.tref) : (T)0;
+    const T *__restrict__ Tm = d.Tm;
     MomK2 K2;
     if constexpr (CPT == 2) {
       K2.Ax = bc2((float)ctx.cA[0]); K2.Ay = bc2((float)ctx.cA[1]); K2.Az = bc2((float)ctx.cA[2]);
@@ -471,7 +481,11 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
           const float *nar = p1s + Lay::WIDE + ty * MX + CPT * tx;
           const F2 mm = bc2(m);
           const F2 p0 = R2.g(4, 0, 0, 0) - mm;
-          const F2 tu = tendency2<0>(K2, R2), tv = tendency2<1>(K2, R2), tw = tendency2<2>(K2, R2);
+          F2 btp = bc2(0.f);
+          if (buoy)
+            btp = bc2(bA2) * (F2{*reinterpret_cast<const float2 *>(Tm + c + plane)} +
+                              F2{*reinterpret_cast<const float2 *>(Tm + c)});
+          const F2 tu = tendency2<0>(K2, R2), tv = tendency2<1>(K2, R2), tw = tendency2<2>(K2, R2, btp);
           const F2 rd = bc2(rdt), dd = bc2(dt), bd = bc2(bdt);
           const F2 zero = bc2(0.f);
           F2 u2 = stage1 ? zero : F2{*reinterpret_cast<const float2 *>(nar)} * rd * dd;
@@ -514,7 +528,9 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
           const bool doW = iq <= d.ext[2][0] && j <= d.ext[2][1] && k <= kW;
           const T tu = doU ? tendency<T, 0>(ctx, R, iq, j, k, wallhere) : (T)0;
           const T tv = doV ? tendency<T, 1>(ctx, R, iq, j, k, wallhere) : (T)0;
-          const T tw = doW ? tendency<T, 2>(ctx, R, iq, j, k, wallhere) : (T)0;
+          T bt = (T)0;
+          if (buoy && doW) bt = bA2 * (ld(Tm, cq + plane) + ld(Tm, cq));
+          const T tw = doW ? tendency<T, 2>(ctx, R, iq, j, k, wallhere, bt, bsub) : (T)0;
           T u2 = stage1 ? (T)0 : nar[0] * rdt * dt;
           T v2 = stage1 ? (T)0 : nar[Lay::NB] * rdt * dt;
           T w2 = stage1 ? (T)0 : nar[2 * Lay::NB] * rdt * dt;
@@ -645,6 +661,14 @@ __device__ void wm_point(const Dom<T> &d, int comp, int f, int i, int j, int k, 
 template <typename T>
 __device__ long long wm_plane_index(const Dom<T> &d, int comp, int f, int i, int j, int k);
 
+// ComputeTDiff (src/scalar_diffusion.f90:983-1009): the temperature
+// diffusivity from the viscosity, constant Pr_sgs = 0.6
+// (src/scalar_diffusion.f90:22)
+template <typename T>
+__device__ __forceinline__ T tdiff_of(T nu, T nu_mol, T kappa_mol) {
+  return nu_mol > 0 ? (nu - nu_mol) / (T)0.6 + kappa_mol : nu / (T)0.6;
+}
+
 // Cells per thread of k_sgs: two for FP32 (packed arithmetic), one for FP64.
 template <typename T>
 struct SgsShape {
@@ -708,6 +732,8 @@ __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
                                (j0 + MY - 1 >= ny - 1 ? 8 : 0));
     const T num = (T)d.nu_mol;
     const bool sgs = d.sgs != 0, addmol = d.nu_mol > 0;
+    const bool buoy = d.buoy != 0;  // temperature diffusivity too (ComputeTDiff)
+    const T kap = (T)d.kappa_mol;
     SgsK<T> q;
     q.rdx = (T)(1.0 / d.dx); q.rdy = (T)(1.0 / d.dy);
     q.r4dx = (T)(1.0 / (4 * d.dx)); q.r4dy = (T)(1.0 / (4 * d.dy));
@@ -738,6 +764,10 @@ __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
           F2 v = nusmag2(q, R2);
           if (addmol) v = v + bc2(num);
           *reinterpret_cast<float2 *>(nu + c) = v.v;
+          if (buoy) {
+            const float2 td = make_float2(tdiff_of(v.v.x, num, kap), tdiff_of(v.v.y, num, kap));
+            *reinterpret_cast<float2 *>(d.TDiff + c) = td;
+          }
         }
       } else if (ok) {
 #pragma unroll
@@ -752,6 +782,7 @@ __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
             if (addmol) v = v + num;
           }
           nu[c + qc] = v;
+          if (buoy) d.TDiff[c + qc] = tdiff_of(v, num, kap);
         }
       }
       const int wk = wtile | (wmask & ((k == 1 ? 16 : 0) | (k >= nz - 1 ? 32 : 0)));

@@ -47,7 +47,7 @@ struct MomK2 {
 };
 
 template <int C, typename RT>
-__device__ __forceinline__ F2 tendency2(const MomK2 &K, const RT &R) {
+__device__ __forceinline__ F2 tendency2(const MomK2 &K, const RT &R, F2 bt = F2{make_float2(0.f, 0.f)}) {
 #define FU(dx, dy, dz) R.g(0, dx, dy, dz)
 #define FV(dx, dy, dz) R.g(1, dx, dy, dz)
 #define FW(dx, dy, dz) R.g(2, dx, dy, dz)
@@ -108,6 +108,7 @@ __device__ __forceinline__ F2 tendency2(const MomK2 &K, const RT &R) {
     const F2 Vadv = ((v + vt) + vs) + vts;
     a = a - ((Bx * (we - ww) * Uadv + By * (wn - ws) * Vadv) + Bz * (wt - wb) * w);
     a = a * bc2(0.5f);
+    a = a + bt;  // buoyancy (the mixed path stores theta - temperature_ref)
     const F2 n0 = FN(0, 0, 0), ne = FN(1, 0, 0), nt = FN(0, 0, 1), nte = FN(1, 0, 1), nw = FN(-1, 0, 0);
     const F2 ntw = FN(-1, 0, 1), nn = FN(0, 1, 0), ntn = FN(0, 1, 1), ns = FN(0, -1, 0), nts = FN(0, -1, 1);
     a = a + K.q * (((nte + ne) + nt) + n0) * (we - w) * K.rx;

@@ -20,7 +20,8 @@ _lib = None
 
 _dp = C.POINTER(C.c_double)
 
-KERNEL_NAMES = ("sgs", "momentum", "fftx_fwd", "ffty_fwd", "tri", "ffty_inv", "fftx_inv", "project", "prref", "ghosts")
+KERNEL_NAMES = ("sgs", "momentum", "fftx_fwd", "ffty_fwd", "tri", "ffty_inv", "fftx_inv", "project", "prref", "ghosts",
+                "temperature")
 KERNEL_COUNT = len(KERNEL_NAMES)
 
 
@@ -45,6 +46,7 @@ def lib():
         L.elmm_destroy.argtypes = [P]
         L.elmm_upload_state.argtypes = [P, _dp, _dp, _dp, _dp]
         L.elmm_download_state.argtypes = [P, _dp, _dp, _dp, _dp]
+        L.elmm_upload_temperature.argtypes = [P, _dp]
         L.elmm_download_field.argtypes = [P, C.c_int32, _dp]
         L.elmm_frame_begin.argtypes = [P]
         L.elmm_frame_wait.argtypes = [P, _dp, _dp, _dp, _dp]
@@ -111,10 +113,17 @@ class Domain:
     def field(self, fid: int, out=None):
         g = self.grid
         shape = {0: g.shape_u(), 5: g.shape_u(), 8: g.shape_u(), 1: g.shape_v(), 6: g.shape_v(), 9: g.shape_v(),
-                 2: g.shape_w(), 7: g.shape_w(), 10: g.shape_w()}.get(fid, g.shape_p())
+                 2: g.shape_w(), 7: g.shape_w(), 10: g.shape_w(), 12: g.shape_t(), 14: g.shape_t()}.get(fid, g.shape_p())
         a = np.zeros(shape) if out is None else out
         check(lib().elmm_download_field(self.h, fid, ptr(a)), "elmm_download_field")
         return a
+
+    def upload_temperature(self, T):
+        """Temperature(-2:nx+3,-2:ny+3,-2:nz+3), host array (enable_buoyancy)."""
+        check(lib().elmm_upload_temperature(self.h, ptr(T)), "elmm_upload_temperature")
+
+    def temperature(self):
+        return self.field(12)
 
     def project(self, coef=1.0) -> ElmmStats:
         st = ElmmStats()

@@ -79,6 +79,20 @@ def log_profile_state(grid: Grid, *, seed=0, ustar=0.3, z0=0.01, amp=0.1, dz=1.0
     return U, V, W, Pr
 
 
+def temperature_state(grid: Grid, *, seed=0, t0=295.0, gradient=0.01, amp=0.05, dz=1.0, zmin=0.0, zW=None):
+    """Potential temperature theta = t0 + gradient * zPr + U(-amp, amp), rounded
+    to FP32; returns the host array Temperature(-2:nx+3,-2:ny+3,-2:nz+3) with
+    zero ghosts (the library fills them)."""
+    g = grid
+    T = np.zeros(g.shape_t())
+    zpr = zpr_of(g, dz, zmin, zW)
+    r = uniform(seed, "theta", g.cells()).reshape(g.Prnz, g.Prny, g.Prnx)
+    interior(T, -2, (g.Prnx, g.Prny, g.Prnz))[...] = (t0 + gradient * zpr[: g.Prnz])[:, None, None] + \
+        amp * (2.0 * r - 1.0)
+    T[...] = T.astype(np.float32).astype(np.float64)
+    return T
+
+
 def interior(a: np.ndarray, lo: int, n: tuple) -> np.ndarray:
     """Interior view a(1:nx,1:ny,1:nz) of a Fortran-layout array with lower bound lo."""
     nx, ny, nz = n

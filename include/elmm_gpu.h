@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define ELMM_ABI_VERSION 1
+#define ELMM_ABI_VERSION 2
 
 /* Status codes. */
 enum {
@@ -55,7 +55,9 @@ enum {
   ELMM_BC_NOSLIP = 1,
   ELMM_BC_FREESLIP = 2,
   ELMM_BC_PERIODIC = 3,
-  ELMM_BC_NEUMANN = 5
+  ELMM_BC_DIRICHLET = 4,
+  ELMM_BC_NEUMANN = 5,
+  ELMM_BC_CONSTFLUX = 6
 };
 
 /* Side indices (src/parameters.f90:193 numbers them We=1..To=6; here 0..5). */
@@ -75,7 +77,10 @@ enum {
   ELMM_FIELD_VISCOSITY = 4,
   ELMM_FIELD_U2 = 5, ELMM_FIELD_V2 = 6, ELMM_FIELD_W2 = 7,
   ELMM_FIELD_USTAR = 8, ELMM_FIELD_VSTAR = 9, ELMM_FIELD_WSTAR = 10,
-  ELMM_FIELD_PHI = 11
+  ELMM_FIELD_PHI = 11,
+  ELMM_FIELD_TEMPERATURE = 12,   /* Temperature(-2:Prnx+3,-2:Prny+3,-2:Prnz+3) */
+  ELMM_FIELD_TDIFF = 13,         /* TDiff(-1:Prnx+2,...), turbulent + molecular diffusivity */
+  ELMM_FIELD_TEMPERATURE_ADV = 14 /* Temperature_adv(-2:...), the stage tendency */
 };
 
 /*
@@ -105,6 +110,16 @@ typedef struct elmm_config {
   double refine_tol;            /* mixed path: max|div u| that triggers a sweep */
   int32_t enable_CFL_check;     /* compute the CFL number each step (src/dynamics.f90:541) */
   int32_t device;               /* CUDA device ordinal */
+  /* Potential temperature: transport by ScalarRK3 (src/scalars.f90:88-381) and
+   * buoyancy in the W tendency (BuoyancyForce, src/dynamics.f90:608-690).
+   * Supported: TempBtype periodic on the periodic x and y sides and
+   * ELMM_BC_CONSTFLUX with sideTemp = 0 (adiabatic) at the bottom and top. */
+  int32_t enable_buoyancy;      /* 0: no temperature field */
+  int32_t TempBtype[6];         /* temperature BC per side (src/initial.f90:347-352) */
+  double sideTemp[6];           /* BC values: the flux for ELMM_BC_CONSTFLUX */
+  double temperature_ref;       /* src/parameters.f90:220 (295 K) */
+  double grav_acc;              /* src/parameters.f90:146 (9.81) */
+  double molecular_diffusivity; /* molecular_viscosity / Prandtl (src/initial.f90:791; Prandtl 0.7) */
 } elmm_config;
 
 /* Diagnostics of elmm_step / elmm_project. */
@@ -148,6 +163,12 @@ int elmm_download_state(elmm_handle *h, double *U, double *V, double *W, double 
 /* Device -> host copy of one field (ELMM_FIELD_*). */
 int elmm_download_field(elmm_handle *h, int32_t field, double *host);
 
+/* Host -> device copy of Temperature(-2:Prnx+3,-2:Prny+3,-2:Prnz+3) (interior
+ * read; enable_buoyancy must be set).  Returns ELMM_ERR_NAN for non-finite
+ * interior values.  The state is read back with elmm_download_field
+ * (ELMM_FIELD_TEMPERATURE). */
+int elmm_upload_temperature(elmm_handle *h, const double *T);
+
 /* Asynchronous frame: copies U, V, W, Pr on a side stream into pinned staging
  * buffers owned by the handle and returns at once.  elmm_frame_wait blocks
  * until the copy has finished and copies the frame into the host arrays.
@@ -175,10 +196,11 @@ int elmm_run_stage(elmm_handle *h, int32_t stage, int32_t stop);
  * kernels of RK3 stage `stage` `reps` times on the handle's stream, each
  * bracketed by CUDA events, and writes the mean duration in ms of each
  * kernel kind to ms[ELMM_NKERNELS] in the order of ELMM_KERNEL_NAMES; "ghosts"
- * is the sum of the stage's ghost-shell launches.  The state advances as by
+ * is the sum of the stage's ghost-shell launches, "temperature" the
+ * temperature stage (0 without a temperature field).  The state advances as by
  * `reps` stages. */
-#define ELMM_NKERNELS 10
-#define ELMM_KERNEL_NAMES "sgs,momentum,fftx_fwd,ffty_fwd,tri,ffty_inv,fftx_inv,project,prref,ghosts"
+#define ELMM_NKERNELS 11
+#define ELMM_KERNEL_NAMES "sgs,momentum,fftx_fwd,ffty_fwd,tri,ffty_inv,fftx_inv,project,prref,ghosts,temperature"
 int elmm_profile_stage(elmm_handle *h, int32_t stage, int32_t reps, double *ms);
 
 /*

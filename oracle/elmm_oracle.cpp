@@ -160,6 +160,12 @@ struct Domain {
   std::vector<double> lamx, lamy, Ab, At, dzc, dzf;  // tridiagonal data
   int zper;
   double max_div;
+  // potential temperature (ScalarRK3, scalars.f90:88-381)
+  int enable_buoyancy;
+  int TempBtype[7];
+  double sideTemp[7];
+  double temperature_ref, grav_acc, molecular_diffusivity;
+  A3 T, Tadv, T2, TDiff;
 };
 
 // ------------------------------------------------- grid, initial.f90:4395-4480
@@ -626,12 +632,215 @@ static void ComputeUVWFluxesWM(Domain &d) {
     }
 }
 
+// ComputeTDiff, scalar_diffusion.f90:983-1009 (constant Pr_sgs = 0.6,
+// scalar_diffusion.f90:22)
+static void ComputeTDiff(Domain &d) {
+  const double Pr_sgs = 0.6;
+  for (int k = 1; k <= d.Prnz; k++)
+    for (int j = 1; j <= d.Prny; j++)
+      for (int i = 1; i <= d.Prnx; i++) {
+        if (d.molecular_viscosity > 0)
+          d.TDiff(i, j, k) = (d.Viscosity(i, j, k) - d.molecular_viscosity) / Pr_sgs + d.molecular_diffusivity;
+        else
+          d.TDiff(i, j, k) = d.Viscosity(i, j, k) / Pr_sgs;
+      }
+}
+
 // SubgridStresses, dynamics.f90:869-908 (ComputeViscsWM only sets Viscosity at
 // wall cells, which SubgridModel then overwrites everywhere; it is omitted).
 static void SubgridStresses(Domain &d) {
   SubgridModel(d);
   if (d.wallmodeltype > 0) ComputeUVWFluxesWM(d);
   BoundViscosity(d, d.Viscosity);
+  if (d.enable_buoyancy) {  // dynamics.f90:904-906
+    ComputeTDiff(d);
+    BoundViscosity(d, d.TDiff);
+  }
+}
+
+// BuoyancyForce, FD2 branch of dynamics.f90:679-688
+static void BuoyancyForce(Domain &d, A3 &Wst) {
+  const double A = d.grav_acc / d.temperature_ref, A2 = A / 2.0;
+  for (int k = 1; k <= d.Wnz; k++)
+    for (int j = 1; j <= d.Wny; j++)
+      for (int i = 1; i <= d.Wnx; i++)
+        Wst(i, j, k) = Wst(i, j, k) + A2 * (d.T(i, j, k + 1) + d.T(i, j, k)) - A * d.temperature_ref;
+}
+
+// BoundTemperature -> CommonBase, scalarboundaries.f90:12-300, for periodic
+// and constant-flux sides (the x, y loops run over the ranges of the
+// reference, corners included where it includes them)
+static void BoundTemperature(Domain &d, A3 &a) {
+  const int nx = d.Prnx, ny = d.Prny, nz = d.Prnz;
+  const int *bt = d.TempBtype;
+  const double *side = d.sideTemp;
+  for (int k = 1; k <= nz; k++)
+    for (int j = 1; j <= ny; j++) {
+      if (bt[We] == BC_PERIODIC) {
+        for (int g = -2; g <= 0; g++) a(g, j, k) = a(nx + g, j, k);
+      } else {
+        a(0, j, k) = a(1, j, k) + side[We] * d.dxU(0) / ((d.TDiff(1, j, k) + d.TDiff(0, j, k)) / 2.0);
+        a(-1, j, k) = a(0, j, k) - (a(1, j, k) - a(0, j, k));
+        a(-2, j, k) = a(0, j, k) - 2 * (a(1, j, k) - a(0, j, k));
+      }
+      if (bt[Ea] == BC_PERIODIC) {
+        for (int g = 1; g <= 3; g++) a(nx + g, j, k) = a(g, j, k);
+      } else {
+        a(nx + 1, j, k) = a(nx, j, k) - side[Ea] * d.dxU(nx) / ((d.TDiff(nx, j, k) + d.TDiff(nx + 1, j, k)) / 2.0);
+        a(nx + 2, j, k) = a(nx + 1, j, k) - (a(nx, j, k) - a(nx + 1, j, k));
+        a(nx + 3, j, k) = a(nx + 1, j, k) - 2 * (a(nx, j, k) - a(nx + 1, j, k));
+      }
+    }
+  for (int k = 1; k <= nz; k++)
+    for (int i = -1; i <= nx + 2; i++) {
+      if (bt[So] == BC_PERIODIC) {
+        for (int g = -2; g <= 0; g++) a(i, g, k) = a(i, ny + g, k);
+      } else {
+        a(i, 0, k) = a(i, 1, k) + side[So] * d.dyV(0) / ((d.TDiff(i, 1, k) + d.TDiff(i, 0, k)) / 2.0);
+        a(i, -1, k) = a(i, 0, k) - (a(i, 1, k) - a(i, 0, k));
+        a(i, -2, k) = a(i, 0, k) - 2 * (a(i, 1, k) - a(i, 0, k));
+      }
+      if (bt[No] == BC_PERIODIC) {
+        for (int g = 1; g <= 3; g++) a(i, ny + g, k) = a(i, g, k);
+      } else {
+        a(i, ny + 1, k) = a(i, ny + 1, k) - side[No] * d.dyV(ny) / ((d.TDiff(i, ny, k) + d.TDiff(i, ny + 1, k)) / 2.0);
+        a(i, ny + 2, k) = a(i, ny + 1, k) - (a(i, ny, k) - a(i, ny + 1, k));
+        a(i, ny + 3, k) = a(i, ny + 1, k) - 2 * (a(i, ny, k) - a(i, ny + 1, k));
+      }
+    }
+  for (int j = -1; j <= ny + 2; j++)
+    for (int i = -1; i <= nx + 2; i++) {
+      if (bt[Bo] == BC_PERIODIC) {
+        for (int g = -2; g <= 0; g++) a(i, j, g) = a(i, j, nz + g);
+      } else {
+        a(i, j, 0) = a(i, j, 1) + side[Bo] * d.dzW(0) / ((d.TDiff(i, j, 1) + d.TDiff(i, j, 0)) / 2.0);
+        a(i, j, -1) = a(i, j, 0) - (a(i, j, 1) - a(i, j, 0));
+        a(i, j, -2) = a(i, j, 0) - 2 * (a(i, j, 1) - a(i, j, 0));
+      }
+      if (bt[To] == BC_PERIODIC) {
+        for (int g = 1; g <= 3; g++) a(i, j, nz + g) = a(i, j, g);
+      } else {
+        a(i, j, nz + 1) = a(i, j, nz) - side[To] * d.dzW(nz) / ((d.TDiff(i, j, nz) + d.TDiff(i, j, nz + 1)) / 2.0);
+        a(i, j, nz + 2) = a(i, j, nz + 1) - (a(i, j, nz) - a(i, j, nz + 1));
+        a(i, j, nz + 3) = a(i, j, nz + 1) - 2 * (a(i, j, nz) - a(i, j, nz + 1));
+      }
+    }
+}
+
+// FluxLimiter of KappaScalar, scalar_advection.f90:262-270
+static inline double kappa_limiter(double r) { return std::max(0.0, std::min(2 * r, std::min(2.0, (1 + 2 * r) / 3))); }
+static inline double fsign(double a, double b) { return std::signbit(b) ? -std::fabs(a) : std::fabs(a); }
+
+// KappaScalar, scalar_advection.f90:102-272 (no masked faces without solid
+// bodies, wallmodels.f90:910-950): slopes and fluxes per face, accumulated in
+// the reference's loop order (the z faces even before odd)
+static void KappaScalar(Domain &d, A3 &S2, const A3 &S) {
+  const int nx = d.Prnx, ny = d.Prny, nz = d.Prnz;
+  const A3 &U = d.U, &V = d.V, &W = d.W;
+  const double eps = 1e-8;
+  const double Ax = 1 / d.dxmin, Ay = 1 / d.dymin, Az = 1 / d.dzmin;
+  S2.fill(0);
+  auto slope = [&](double sr, double sl) { return kappa_limiter((sr + eps * fsign(1.0, sl)) / (sl + eps * fsign(1.0, sl))); };
+  for (int k = 1; k <= nz; k++)
+    for (int j = 1; j <= ny; j++)
+      for (int i = 0; i <= nx; i++) {
+        double sr, sl, flux;
+        if (U(i, j, k) > 0) { sr = S(i + 1, j, k) - S(i, j, k); sl = S(i, j, k) - S(i - 1, j, k); }
+        else { sr = S(i, j, k) - S(i + 1, j, k); sl = S(i + 1, j, k) - S(i + 2, j, k); }
+        const double sp = slope(sr, sl);
+        if (U(i, j, k) > 0) flux = U(i, j, k) * (S(i, j, k) + (S(i, j, k) - S(i - 1, j, k)) * sp / 2.0);
+        else flux = U(i, j, k) * (S(i + 1, j, k) + (S(i + 1, j, k) - S(i + 2, j, k)) * sp / 2.0);
+        S2(i, j, k) = S2(i, j, k) - Ax * flux;
+        S2(i + 1, j, k) = S2(i + 1, j, k) + Ax * flux;
+      }
+  for (int k = 1; k <= nz; k++)
+    for (int j = 0; j <= ny; j++)
+      for (int i = 1; i <= nx; i++) {
+        double sr, sl, flux;
+        if (V(i, j, k) > 0) { sr = S(i, j + 1, k) - S(i, j, k); sl = S(i, j, k) - S(i, j - 1, k); }
+        else { sr = S(i, j, k) - S(i, j + 1, k); sl = S(i, j + 1, k) - S(i, j + 2, k); }
+        const double sp = slope(sr, sl);
+        if (V(i, j, k) > 0) flux = V(i, j, k) * (S(i, j, k) + (S(i, j, k) - S(i, j - 1, k)) * sp / 2.0);
+        else flux = V(i, j, k) * (S(i, j + 1, k) + (S(i, j + 1, k) - S(i, j + 2, k)) * sp / 2.0);
+        S2(i, j, k) = S2(i, j, k) - Ay * flux;
+        S2(i, j + 1, k) = S2(i, j + 1, k) + Ay * flux;
+      }
+  for (int l = 0; l <= 1; l++)
+    for (int k = l; k <= nz; k += 2)
+      for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++) {
+          double sr, sl, flux;
+          const double vel = W(i, j, k);
+          if (vel > 0) { sr = S(i, j, k + 1) - S(i, j, k); sl = S(i, j, k) - S(i, j, k - 1); }
+          else { sr = S(i, j, k) - S(i, j, k + 1); sl = S(i, j, k + 1) - S(i, j, k + 2); }
+          const double sp = slope(sr, sl);
+          if (vel > 0) flux = vel * (S(i, j, k) + (S(i, j, k) - S(i, j, k - 1)) * sp / 2.0);
+          else flux = vel * (S(i, j, k + 1) + (S(i, j, k + 1) - S(i, j, k + 2)) * sp / 2.0);
+          S2(i, j, k) = S2(i, j, k) - Az * flux;
+          S2(i, j, k + 1) = S2(i, j, k + 1) + Az * flux;
+        }
+}
+
+// ScalarDiffusion_nobranch, scalar_diffusion.f90:404-507 (no flux points
+// without solid bodies)
+static void ScalarDiffusion(Domain &d, A3 &S2, const A3 &S) {
+  const A3 &K = d.TDiff;
+  const double Ax = 1 / (2 * d.dxmin * d.dxmin), Ay = 1 / (2 * d.dymin * d.dymin), Az = 1 / (2 * d.dzmin * d.dzmin);
+  for (int k = 1; k <= d.Prnz; k++)
+    for (int j = 1; j <= d.Prny; j++)
+      for (int i = 1; i <= d.Prnx; i++) {
+        double a = S2(i, j, k);
+        a = a + (K(i + 1, j, k) + K(i, j, k)) * (S(i + 1, j, k) - S(i, j, k)) * Ax;
+        a = a - (K(i, j, k) + K(i - 1, j, k)) * (S(i, j, k) - S(i - 1, j, k)) * Ax;
+        a = a + (K(i, j + 1, k) + K(i, j, k)) * (S(i, j + 1, k) - S(i, j, k)) * Ay;
+        a = a - (K(i, j, k) + K(i, j - 1, k)) * (S(i, j, k) - S(i, j - 1, k)) * Ay;
+        a = a + (K(i, j, k + 1) + K(i, j, k)) * (S(i, j, k + 1) - S(i, j, k)) * Az;
+        a = a - (K(i, j, k) + K(i, j, k - 1)) * (S(i, j, k) - S(i, j, k - 1)) * Az;
+        S2(i, j, k) = a;
+      }
+}
+
+// one stage of ScalarRK3 for the temperature (scalars.f90:88-299): the
+// scalar wall-model points are the cells next to a wall-model side
+// (DivergenceWM, wallmodels.f90:1150-1166; TemperatureExtra with a zero
+// surface flux, scalars.f90:301-334)
+static void TemperatureStage(Domain &d, int stage, double dt) {
+  const int nx = d.Prnx, ny = d.Prny, nz = d.Prnz;
+  // DivergenceWM with the velocity at the start of the stage
+  std::vector<double> divb((size_t)nx * ny, 0.0), divt((size_t)nx * ny, 0.0);
+  const bool wb = d.wallmodeltype > 0 && d.Btype[Bo] == BC_NOSLIP, wt = d.wallmodeltype > 0 && d.Btype[To] == BC_NOSLIP;
+  auto wmdiv = [&](int i, int j, int k) {
+    double div = 0;
+    div = div + d.U(i, j, k) / d.dxmin;
+    div = div - d.U(i - 1, j, k) / d.dxmin;
+    div = div + d.V(i, j, k) / d.dymin;
+    div = div - d.V(i, j - 1, k) / d.dymin;
+    div = div + d.W(i, j, k) / d.dzPr(k);
+    div = div - d.W(i, j, k - 1) / d.dzPr(k);
+    return div;
+  };
+  for (int j = 1; j <= ny; j++)
+    for (int i = 1; i <= nx; i++) {
+      if (wb) divb[(size_t)(j - 1) * nx + i - 1] = wmdiv(i, j, 1);
+      if (wt) divt[(size_t)(j - 1) * nx + i - 1] = wmdiv(i, j, nz);
+    }
+  BoundTemperature(d, d.T);
+  const double rdt = RK_rho[stage - 1] * dt, bdt = RK_beta[stage - 1] * dt;
+  if (stage > 1) {
+    for (size_t q = 0; q < d.T2.v.size(); q++) d.T2.v[q] = d.Tadv.v[q] * rdt;
+  } else {
+    d.T2.fill(0);
+  }
+  KappaScalar(d, d.Tadv, d.T);
+  ScalarDiffusion(d, d.Tadv, d.T);
+  for (int j = 1; j <= ny; j++)
+    for (int i = 1; i <= nx; i++) {
+      if (wb) d.Tadv(i, j, 1) = d.Tadv(i, j, 1) + divb[(size_t)(j - 1) * nx + i - 1] * d.T(i, j, 1);
+      if (wt) d.Tadv(i, j, nz) = d.Tadv(i, j, nz) + divt[(size_t)(j - 1) * nx + i - 1] * d.T(i, j, nz);
+    }
+  for (size_t q = 0; q < d.T2.v.size(); q++) d.T2.v[q] = d.T2.v[q] + d.Tadv.v[q] * bdt;
+  for (size_t q = 0; q < d.T.v.size(); q++) d.T.v[q] = d.T.v[q] + d.T2.v[q];
+  BoundTemperature(d, d.T);
 }
 
 // ---------------------------------------------- CDS2 advection, advection.f90:15-327
@@ -1082,6 +1291,7 @@ static void Convection(Domain &d, int stage, double dt) {
   CDU(d, d.Ustar);
   CDV(d, d.Vstar);
   CDW(d, d.Wstar);
+  if (d.enable_buoyancy) BuoyancyForce(d, d.Wstar);  // dynamics.f90:423
   MomentumDiffusion(d, d.Ustar, d.Vstar, d.Wstar);
   for (int k = 1; k <= d.Unz; k++) for (int j = 1; j <= d.Uny; j++) for (int i = 1; i <= d.Unx; i++) d.U2(i, j, k) = d.U2(i, j, k) + d.Ustar(i, j, k) * beta * dt;
   for (int k = 1; k <= d.Vnz; k++) for (int j = 1; j <= d.Vny; j++) for (int i = 1; i <= d.Vnx; i++) d.V2(i, j, k) = d.V2(i, j, k) + d.Vstar(i, j, k) * beta * dt;
@@ -1336,6 +1546,7 @@ static void run_stage(Domain &d, int stage, int stop) {
   SubgridStresses(d);
   if (stop == 1) return;
   Convection(d, stage, dt);
+  if (d.enable_buoyancy) TemperatureStage(d, stage, dt);  // ScalarRK3, tsteps.f90:132-135
   OtherTerms(d, 2 * RK_alpha[stage - 1] * dt);
   BoundUVW(d, d.U2, d.V2, d.W2);
   if (stop == 2) return;
@@ -1400,6 +1611,16 @@ void *orc_create(const elmm_config *c) {
   for (A3 *a : {&d->Pr, &d->Viscosity, &d->Phi}) a->init(-1, nx + 2, -1, ny + 2, -1, nz + 2);
   d->RHS.init(0, nx + 1, 0, ny + 1, 0, nz + 1);
   d->Viscosity.fill(d->molecular_viscosity);
+  d->enable_buoyancy = c->enable_buoyancy;
+  for (int s = 0; s < 6; s++) { d->TempBtype[s + 1] = c->TempBtype[s]; d->sideTemp[s + 1] = c->sideTemp[s]; }
+  d->temperature_ref = c->temperature_ref;
+  d->grav_acc = c->grav_acc;
+  d->molecular_diffusivity = c->molecular_diffusivity;
+  if (d->enable_buoyancy) {
+    for (A3 *a : {&d->T, &d->Tadv, &d->T2}) a->init(-2, nx + 3, -2, ny + 3, -2, nz + 3);
+    d->TDiff.init(-1, nx + 2, -1, ny + 2, -1, nz + 2);
+    d->TDiff.fill(d->molecular_diffusivity);  // initial.f90:4266
+  }
   if (d->wallmodeltype > 0) add_wm_points(*d);
   if (!init_poisson(*d)) { delete d; return nullptr; }
   return d;
@@ -1428,6 +1649,9 @@ static A3 *field_of(Domain *d, int f) {
     case ELMM_FIELD_VSTAR: return &d->Vstar;
     case ELMM_FIELD_WSTAR: return &d->Wstar;
     case ELMM_FIELD_PHI: return &d->Phi;
+    case ELMM_FIELD_TEMPERATURE: return d->enable_buoyancy ? &d->T : nullptr;
+    case ELMM_FIELD_TDIFF: return d->enable_buoyancy ? &d->TDiff : nullptr;
+    case ELMM_FIELD_TEMPERATURE_ADV: return d->enable_buoyancy ? &d->Tadv : nullptr;
   }
   return nullptr;
 }

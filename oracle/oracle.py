@@ -85,6 +85,8 @@ class Oracle:
             return (Vnz + 6, Vny + 6, Vnx + 6)
         if field in (2, 7, 10):
             return (Wnz + 6, Wny + 6, Wnx + 6)
+        if field in (12, 14):  # Temperature, Temperature_adv: (-2:n+3)
+            return (Prnz + 6, Prny + 6, Prnx + 6)
         return (Prnz + 4, Prny + 4, Prnx + 4)
 
     def set_field(self, field, a):

@@ -313,3 +313,80 @@ def test_mixed_defect_correction_sweeps():
         e = errs(g, d.download(), o.state())
         assert max(e[:3]) < 1e-5, e
         assert s.max_div < 1e-6
+
+
+def _buoyant_pair(n=(32, 24, 16), precision=0, seed=0):
+    from gpu_elmm_b200.config import FIELD_TEMPERATURE
+    from gpu_elmm_b200.workloads import temperature_state
+    cfg = make_config(*n, buoyancy=True, precision=precision)
+    g = grid_of(cfg)
+    st = log_profile_state(g, seed=seed)
+    T0 = temperature_state(g, seed=seed)
+    o = Oracle(make_config(*n, buoyancy=True))
+    o.set_state(*st)
+    o.set_field(FIELD_TEMPERATURE, T0)
+    d = L.Domain(cfg)
+    d.upload(*st)
+    d.upload_temperature(T0)
+    return g, o, d
+
+
+@pytest.mark.parametrize("nsteps", [1, 10])
+def test_fp64_buoyant_channel(nsteps):
+    """Config-1 physics with the potential temperature: FP64 GPU vs oracle.
+    The temperature is compared as its deviation from T_ref (the field is
+    ~295 K, the dynamics live in the ~1 K deviation)."""
+    from gpu_elmm_b200.config import FIELD_TEMPERATURE
+    g, o, d = _buoyant_pair()
+    o.project(1.0)
+    d.project(1.0)
+    o.step(nsteps)
+    d.step(nsteps)
+    for a, b, name in zip(interiors(g, *d.download()), interiors(g, *o.state()), "UVWP"):
+        assert rel(a, b) < (1e-11 if name == "P" else 1e-12), (name, rel(a, b))
+    n = (g.Prnx, g.Prny, g.Prnz)
+    Tg = interior(d.field(FIELD_TEMPERATURE), -2, n) - 295.0
+    To = interior(o.get_field(FIELD_TEMPERATURE), -2, n) - 295.0
+    assert rel(Tg, To) < 1e-11, rel(Tg, To)
+    d.close()
+
+
+def test_temperature_diffusivity_after_sgs():
+    from gpu_elmm_b200.config import FIELD_TDIFF
+    g, o, d = _buoyant_pair()
+    o.run_stage(1, 1)
+    d.run_stage(1, 1)
+    n = (g.Prnx, g.Prny, g.Prnz)
+    a = interior(d.field(FIELD_TDIFF), -1, n)
+    b = interior(o.get_field(FIELD_TDIFF), -1, n)
+    assert rel(a, b) < 1e-13
+    d.close()
+
+
+def test_mixed_buoyant_channel_one_step():
+    """Mixed path (theta stored as theta - T_ref in FP32) against FP64 after
+    one step from the same projected state."""
+    from gpu_elmm_b200.config import FIELD_TEMPERATURE
+    from gpu_elmm_b200.workloads import temperature_state
+    n = (32, 24, 16)
+    g = grid_of(make_config(*n))
+    st = log_profile_state(g, seed=1)
+    T0 = temperature_state(g, seed=1)
+    d64 = L.Domain(make_config(*n, buoyancy=True))
+    d64.upload(*st)
+    d64.upload_temperature(T0)
+    d64.project(1.0)
+    ref0 = d64.download()
+    d64.step(1)
+    dm = L.Domain(make_config(*n, buoyancy=True, precision=1))
+    dm.upload(*ref0)
+    dm.upload_temperature(T0)
+    dm.step(1)
+    for a, b in zip(interiors(g, *dm.download())[:3], interiors(g, *d64.download())[:3]):
+        assert rel(a, b) < 1e-5
+    m = (g.Prnx, g.Prny, g.Prnz)
+    Tm = interior(dm.field(FIELD_TEMPERATURE), -2, m) - 295.0
+    T64 = interior(d64.field(FIELD_TEMPERATURE), -2, m) - 295.0
+    assert rel(Tm, T64) < 1e-5, rel(Tm, T64)
+    d64.close()
+    dm.close()

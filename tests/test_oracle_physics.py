@@ -86,3 +86,56 @@ def test_taylor_green_decay():
     decay = np.exp(-nu * lam * dt * steps)
     assert rel(Ui, U0 * decay) < 1e-6
     assert rel(Vi, V0 * decay) < 1e-6
+
+
+def _buoyant_channel(seed=0, n=(16, 12, 10)):
+    from gpu_elmm_b200.config import FIELD_TEMPERATURE, grid_of, make_config
+    from gpu_elmm_b200.workloads import log_profile_state, temperature_state
+    cfg = make_config(*n, buoyancy=True)
+    g = grid_of(cfg)
+    o = Oracle(cfg)
+    o.set_state(*log_profile_state(g, seed=seed))
+    o.set_field(FIELD_TEMPERATURE, temperature_state(g, seed=seed))
+    o.project(1.0)
+    return g, o
+
+
+def test_temperature_heat_is_conserved():
+    """Adiabatic (zero-flux) walls and periodic x, y: KappaScalar and the
+    diffusion are in flux form, so the heat content only changes by the
+    wall-model divergence term, which is of the size of the discrete
+    divergence (~1e-15) times theta."""
+    from gpu_elmm_b200.config import FIELD_TEMPERATURE
+    from gpu_elmm_b200.workloads import interior
+    g, o = _buoyant_channel()
+    n = (g.Prnx, g.Prny, g.Prnz)
+    h0 = interior(o.get_field(FIELD_TEMPERATURE), -2, n).sum()
+    o.step(5)
+    T = interior(o.get_field(FIELD_TEMPERATURE), -2, n)
+    assert np.isfinite(T).all()
+    assert abs(T.sum() - h0) / abs(h0) < 1e-12
+    # the run did transport heat: the field changed
+    assert np.abs(T - T.mean()).max() > 0
+
+
+def test_buoyancy_vanishes_for_the_reference_temperature():
+    """theta = temperature_ref everywhere: the FD2 buoyancy term
+    A/2 (T(k+1) + T(k)) - A T_ref vanishes, so the flow equals the run without
+    the temperature field up to the rounding of (W + g) - g in the reference's
+    order of operations."""
+    from gpu_elmm_b200.config import FIELD_TEMPERATURE, grid_of, make_config
+    from gpu_elmm_b200.workloads import log_profile_state
+    cfg0 = make_config(16, 12, 10)
+    cfg1 = make_config(16, 12, 10, buoyancy=True)
+    g = grid_of(cfg0)
+    st = log_profile_state(g, seed=3)
+    a, b = Oracle(cfg0), Oracle(cfg1)
+    a.set_state(*st)
+    b.set_state(*st)
+    b.set_field(FIELD_TEMPERATURE, np.full(g.shape_t(), 295.0))
+    a.project(1.0)
+    b.project(1.0)
+    a.step(2)
+    b.step(2)
+    for x, y, tol in zip(a.state(), b.state(), (1e-12, 1e-12, 1e-12, 1e-11)):  # P: conditioning floor
+        assert rel(x, y) < tol
