@@ -2,8 +2,9 @@
 
 Workload: one 256 x 256 x 128 channel domain per GPU (periodic x and y,
 no-slip bottom with the log-law wall model, free-slip top, Smagorinsky
-Cs = 0.1, RK3, dt = 0.02): the single large domain on which the FP64 and the
-mixed path are compared.  A "step" is one RK3 time step (three stages, each
+Cs = 0.1, RK3, dt = 0.02) with the potential temperature (0.01 K/m gradient
+and +-0.05 K perturbations, adiabatic walls, buoyancy): the single large
+domain on which the FP64 and the mixed path are compared.  A "step" is one RK3 time step (three stages, each
 with a full pressure projection) of that domain, inputs resident in HBM.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
@@ -32,16 +33,19 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 from gpu_elmm_b200.config import grid_of, make_config  # noqa: E402
-from gpu_elmm_b200.workloads import interiors, log_profile_state  # noqa: E402
+from gpu_elmm_b200.config import FIELD_TEMPERATURE  # noqa: E402
+from gpu_elmm_b200.workloads import interior, interiors, log_profile_state, temperature_state  # noqa: E402
 
 METRIC = "cell-steps/s mixed vs FP64 plain, 1 B200, at ≤1e-5 rel err; p50/p99 latency"
 N = (256, 256, 128)
 WORKLOAD = ("256x256x128 channel: periodic x,y; no-slip bottom with log-law wall model (z0=0.01); "
-            "free-slip top; Smagorinsky Cs=0.1; CDS2; RK3 dt=0.02; FFT(x,y)+tridiagonal(z) projection")
-DATA = "synthetic: seeded log profile u*=0.3 + U(-0.1,0.1) perturbations on u,v,w, FP32-rounded, projected"
-# words moved per cell by the momentum kernel in stages 2 and 3: reads U,V,W,nu,Pr,Ustar x3;
+            "free-slip top; Smagorinsky Cs=0.1; CDS2; RK3 dt=0.02; FFT(x,y)+tridiagonal(z) projection; "
+            "potential temperature (KappaScalar advection, SGS diffusion Pr_sgs=0.6, adiabatic walls) with buoyancy")
+DATA = ("synthetic: seeded log profile u*=0.3 + U(-0.1,0.1) perturbations on u,v,w; theta = 295 K + 0.01 K/m z "
+        "+ U(-0.05,0.05) K; FP32-rounded, projected")
+# words moved per cell by the momentum kernel in stages 2 and 3: reads U,V,W,nu,Pr,theta,Ustar x3;
 # writes Ustar x3, U2 x3 (the per-cell figure of the momentum phase)
-MOMENTUM_WORDS = 14
+MOMENTUM_WORDS = 15
 # oracle steps timed by the reference arm (a bounded sample of the workload)
 REF_STEPS = 10
 
@@ -166,10 +170,11 @@ def cpu_baseline(steps=1):
     orc.build()
     threads = os.cpu_count() or 1
     orc.set_threads(threads)
-    cfg = make_config(*N)
+    cfg = make_config(*N, buoyancy=True)
     g = grid_of(cfg)
     o = orc.Oracle(cfg)
     o.set_state(*log_profile_state(g, seed=0))
+    o.set_field(FIELD_TEMPERATURE, temperature_state(g, seed=0))
     o.project(1.0)
     t0 = time.perf_counter()
     o.step(steps)
@@ -187,10 +192,11 @@ def run_reference(args, ws, rank):
     orc.build()
     threads = os.cpu_count() or 1
     orc.set_threads(threads)
-    cfg = make_config(*N)
+    cfg = make_config(*N, buoyancy=True)
     g = grid_of(cfg)
     o = orc.Oracle(cfg)
     o.set_state(*log_profile_state(g, seed=0))
+    o.set_field(FIELD_TEMPERATURE, temperature_state(g, seed=0))
     o.project(1.0)
     # a bounded sample: one RK3 step of the full domain takes ~1.5 s on 16
     # cores, so at most REF_STEPS steps are timed after one warm-up step
@@ -219,11 +225,17 @@ def run_ours(args, ws, rank, local):
     torch.cuda.set_device(local)
     g = grid_of(make_config(*N))
     st = log_profile_state(g, seed=rank)
+    T0 = temperature_state(g, seed=rank)
     cells = g.cells()
 
+    def domain(precision, state, temp):
+        dd = L.Domain(make_config(*N, precision=precision, device=local, buoyancy=True))
+        dd.upload(*state)
+        dd.upload_temperature(temp)
+        return dd
+
     # FP64 plain path on the same state
-    d64 = L.Domain(make_config(*N, precision=0, device=local))
-    d64.upload(*st)
+    d64 = domain(0, st, T0)
     d64.project(1.0)
     d64.step(args.warmup)
     barrier(ws)
@@ -234,24 +246,25 @@ def run_ours(args, ws, rank, local):
     ms64 = allreduce_max(s64.elapsed_ms, ws)
 
     # accuracy of the mixed path against FP64 after one step from the same state
-    a64 = L.Domain(make_config(*N, precision=0, device=local))
-    a64.upload(*st)
+    a64 = domain(0, st, T0)
     a64.project(1.0)
     ref0 = a64.download()
     a64.step(1)
     ref1 = a64.download()
+    refT = a64.field(FIELD_TEMPERATURE)
     a64.close()
     d64.close()
-    am = L.Domain(make_config(*N, precision=1, device=local))
-    am.upload(*ref0)
+    am = domain(1, ref0, T0)
     am.step(1)
     mix1 = am.download()
+    mixT = am.field(FIELD_TEMPERATURE)
     am.close()
     errs = [rel(a, b) for a, b in zip(interiors(g, *mix1), interiors(g, *ref1))]
+    nT = (g.Prnx, g.Prny, g.Prnz)
+    errs.append(rel(interior(mixT, -2, nT) - 295.0, interior(refT, -2, nT) - 295.0))
 
     # the mixed path: headline
-    dm = L.Domain(make_config(*N, precision=1, device=local))
-    dm.upload(*st)
+    dm = domain(1, st, T0)
     dm.project(1.0)
     dm.step(args.warmup)
     with Clocks(local) as clk:
@@ -296,14 +309,18 @@ def run_ours(args, ws, rank, local):
     pinned = [torch.empty(a.shape, dtype=torch.float64, pin_memory=True).numpy() for a in st]
     for p, a in zip(pinned, dm.download()):
         p[...] = a
-    h2d = sum(a.nbytes for a in pinned)
+    pinT = torch.empty(T0.shape, dtype=torch.float64, pin_memory=True).numpy()
+    pinT[...] = dm.field(FIELD_TEMPERATURE)
+    h2d = sum(a.nbytes for a in pinned) + pinT.nbytes
     e2e_t = []
     for _ in range(max(3, args.steps // 2)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         dm.upload(*pinned)
+        dm.upload_temperature(pinT)
         dm.step(1)
         L.check(L.lib().elmm_download_state(dm.h, *[L.ptr(p) for p in pinned]), "elmm_download_state")
+        dm.field(FIELD_TEMPERATURE, out=pinT)
         torch.cuda.synchronize()
         e2e_t.append(time.perf_counter() - t0)
     e2e_s = allreduce_max(statistics.median(e2e_t), ws)
@@ -322,7 +339,7 @@ def run_ours(args, ws, rank, local):
             "fp64_plain": {"value": v64, "unit": "cell-steps/s", "ms_per_step": ms64 / args.steps},
             "mixed_over_fp64": value / v64,
             "accuracy_vs_fp64_1step": {"u": errs[0], "v": errs[1], "w": errs[2], "p": errs[3],
-                                       "max_div_mixed": max_div},
+                                       "theta_minus_ref": errs[4], "max_div_mixed": max_div},
             "latency_ms": {"p50": p50, "p99": p99, "what": "device time of one RK3 step"},
             "roofline": {"bound": "hbm", "kernel": "k_momentum (stage 2)", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,

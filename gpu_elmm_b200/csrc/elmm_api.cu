@@ -205,7 +205,7 @@ struct LaunchSet {
   Launch l() const { return Launch{starts, nd, total}; }
 };
 
-enum { LK_CELLS = 0, LK_BOX, LK_ROWS, LK_YCOLS, LK_TRI, LK_MOM, LK_SHELL, LK_XREG, LK_YREG, LK_TRIT, LK_N };
+enum { LK_CELLS = 0, LK_BOX, LK_ROWS, LK_YCOLS, LK_TRI, LK_MOM, LK_SHELL, LK_XREG, LK_YREG, LK_TRIT, LK_TCOL, LK_N };
 
 // -------------------------------------------------------------------- batch
 template <typename T>
@@ -456,6 +456,7 @@ struct BatchT {
         return ((h.nxh + C - 1) / C) * h.nz;
       }
       case LK_TRIT: return tri_tiled(h) ? (h.ny * h.spitch + kTriCols - 1) / kTriCols : 0;
+      case LK_TCOL: return h.buoy ? ntx * nty * ((h.nz + TMKC - 1) / TMKC) : 0;
       default: return tri_tiled(h) ? 0 : (h.ny * h.spitch + kTriThreads - 1) / kTriThreads;
     }
   }
@@ -674,8 +675,8 @@ struct BatchT {
   void launch_temperature(int stage) {
     if (!any_buoy()) return;
     nlaunch++;
-    k_temperature<T><<<gsz(7, ls[LK_CELLS].total), TX * TY, 0, stream>>>(ddom, ls[LK_CELLS].l(), kRho[stage - 1],
-                                                                          kBeta[stage - 1], stage == 1);
+    k_temperature<T><<<gsz(7, ls[LK_TCOL].total), TX * TY, 0, stream>>>(ddom, ls[LK_TCOL].l(), kRho[stage - 1],
+                                                                         kBeta[stage - 1], stage == 1);
     for (auto &h : hdom)
       if (h.buoy) cudaMemcpyAsync(h.Tm, h.Tn, (size_t)h.plane * (h.nz + 2) * sizeof(T), cudaMemcpyDeviceToDevice, stream);
   }

@@ -26,11 +26,22 @@ __device__ __forceinline__ int scal_fold(int g, int n, bool periodic) {
   return g < 1 ? 1 : n;
 }
 
-// FluxLimiter of KappaScalar (src/scalar_advection.f90:262-270)
+// FluxLimiter of KappaScalar (src/scalar_advection.f90:262-270).  The FP32
+// path of the mixed precision mode divides by 3 as a multiplication by 1/3
+// and forms the slope ratio with the fast division (both within a few ulp);
+// the FP64 path keeps the reference's divisions.
 template <typename T>
 __device__ __forceinline__ T kappa_limiter(T r) {
   return fmax((T)0, fmin((T)2 * r, fmin((T)2, ((T)1 + (T)2 * r) / (T)3)));
 }
+template <>
+__device__ __forceinline__ float kappa_limiter<float>(float r) {
+  return fmaxf(0.f, fminf(2.f * r, fminf(2.f, (1.f + 2.f * r) * (1.f / 3.f))));
+}
+template <typename T>
+__device__ __forceinline__ T kappa_ratio(T num, T den) { return num / den; }
+template <>
+__device__ __forceinline__ float kappa_ratio<float>(float num, float den) { return __fdividef(num, den); }
 
 // the flux through the face between cells b and c, with a the cell before b
 // and e the cell after c along the face normal, velocity vel on the face
@@ -41,13 +52,18 @@ __device__ __forceinline__ T kappa_flux(T vel, T a, T b, T c, T e) {
   if (vel > 0) { sr = c - b; sl = b - a; }
   else { sr = b - c; sl = c - e; }
   const T sg = signbit(sl) ? (T)-1 : (T)1;
-  const T slope = kappa_limiter<T>((sr + eps * sg) / (sl + eps * sg));
+  const T slope = kappa_limiter<T>(kappa_ratio<T>(sr + eps * sg, sl + eps * sg));
   return vel > 0 ? vel * (b + (b - a) * slope / (T)2) : vel * (c + (c - e) * slope / (T)2);
 }
 
+// A block owns a TX x TY column of cells and marches up a chunk of TMKC
+// planes; theta(k-2..k+2), the diffusivity (k-1..k+1) and W(k-1) ride along
+// in registers, x and y neighbours come from offsets folded once per thread.
+constexpr int TMKC = 16;
+
 template <typename T>
-__global__ void __launch_bounds__(TX *TY) k_temperature(const Dom<T> *__restrict__ doms, Launch L, double rho,
-                                                        double beta, int stage1) {
+__global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
+    k_temperature(const Dom<T> *__restrict__ doms, Launch L, double rho, double beta, int stage1) {
   for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
     const int di = find_dom(L.starts, L.nd, t);
     const Dom<T> &d = doms[di];
@@ -57,74 +73,106 @@ __global__ void __launch_bounds__(TX *TY) k_temperature(const Dom<T> *__restrict
     const int ntx = (nx + TX - 1) / TX, nty = (ny + TY - 1) / TY;
     const int tx = lt % ntx; lt /= ntx;
     const int ty = lt % nty;
-    const int k = lt / nty + 1;
+    const int k0 = (lt / nty) * TMKC + 1, k1 = min(k0 + TMKC - 1, nz);
     const int i = tx * TX + (threadIdx.x % TX) + 1;
     const int j = ty * TY + (threadIdx.x / TX) + 1;
     if (i > nx || j > ny) continue;
     const bool px = d.tbt[SIDE_WE] == BC_PERIODIC, py = d.tbt[SIDE_SO] == BC_PERIODIC,
                pz = d.tbt[SIDE_BO] == BC_PERIODIC;
-    const T *__restrict__ S = d.Tm;
-    const T *__restrict__ K = d.TDiff;
-    // folded coordinates of the neighbours i-2..i+2 (index 0..4)
-    int xs[5], ys[5], zs[5];
+    const long long pitch = d.pitch, plane = d.plane;
+    // folded offsets of the x and y neighbours -2..+2 (index 0..4); a plane
+    // holds fewer than 2^31 elements
+    int ox[5], oy[5];
 #pragma unroll
     for (int q = 0; q < 5; q++) {
-      xs[q] = scal_fold(i - 2 + q, nx, px);
-      ys[q] = scal_fold(j - 2 + q, ny, py);
-      zs[q] = scal_fold(k - 2 + q, nz, pz);
+      ox[q] = scal_fold(i - 2 + q, nx, px) - i;
+      oy[q] = (scal_fold(j - 2 + q, ny, py) - j) * (int)pitch;
     }
-    auto s_at = [&](int a, int b, int c) { return ld(S, bidx(d, xs[a], ys[b], zs[c])); };
-    auto k_at = [&](int a, int b, int c) { return ld(K, bidx(d, xs[a], ys[b], zs[c])); };
-    const long long cc = bidx(d, i, j, k);
-    // velocities on the six faces (their ghosts are filled)
-    const T ue = ld(d.U, cc), uw = ld(d.U, cc - 1);
-    const T vn = ld(d.V, cc), vs = ld(d.V, cc - d.pitch);
-    const T wt = ld(d.W, cc), wb = ld(d.W, cc - d.plane);
-    const T s0 = s_at(2, 2, 2);
+    auto zoff = [&](int kk) { return (long long)(scal_fold(kk, nz, pz) - kk) * plane; };  // fold of plane kk
+    const T *__restrict__ S = d.Tm;
+    const T *__restrict__ K = d.TDiff;
+    const T *__restrict__ U = d.U;
+    const T *__restrict__ V = d.V;
+    const T *__restrict__ W = d.W;
     const T Ax = (T)(1.0 / d.dx), Ay = (T)(1.0 / d.dy), Az = (T)(1.0 / d.dz);
-    // advection: the loop order of KappaScalar gives each cell +A f(low face)
-    // then -A f(high face) in x and y; in z the even faces come first
-    T a = (T)0;
-    a = a + Ax * kappa_flux<T>(uw, s_at(0, 2, 2), s_at(1, 2, 2), s0, s_at(3, 2, 2));
-    a = a - Ax * kappa_flux<T>(ue, s_at(1, 2, 2), s0, s_at(3, 2, 2), s_at(4, 2, 2));
-    a = a + Ay * kappa_flux<T>(vs, s_at(2, 0, 2), s_at(2, 1, 2), s0, s_at(2, 3, 2));
-    a = a - Ay * kappa_flux<T>(vn, s_at(2, 1, 2), s0, s_at(2, 3, 2), s_at(2, 4, 2));
-    const T fzb = kappa_flux<T>(wb, s_at(2, 2, 0), s_at(2, 2, 1), s0, s_at(2, 2, 3));
-    const T fzt = kappa_flux<T>(wt, s_at(2, 2, 1), s0, s_at(2, 2, 3), s_at(2, 2, 4));
-    if (((k - 1) & 1) == 0) {  // face k-1 is even
-      a = a + Az * fzb;
-      a = a - Az * fzt;
-    } else {
-      a = a - Az * fzt;
-      a = a + Az * fzb;
-    }
-    // diffusion, in the order of ScalarDiffusion_nobranch
     const T Dx = (T)(1.0 / (2 * d.dx * d.dx)), Dy = (T)(1.0 / (2 * d.dy * d.dy)), Dz = (T)(1.0 / (2 * d.dz * d.dz));
-    const T k0 = k_at(2, 2, 2);
-    a = a + (k_at(3, 2, 2) + k0) * (s_at(3, 2, 2) - s0) * Dx;
-    a = a - (k0 + k_at(1, 2, 2)) * (s0 - s_at(1, 2, 2)) * Dx;
-    a = a + (k_at(2, 3, 2) + k0) * (s_at(2, 3, 2) - s0) * Dy;
-    a = a - (k0 + k_at(2, 1, 2)) * (s0 - s_at(2, 1, 2)) * Dy;
-    a = a + (k_at(2, 2, 3) + k0) * (s_at(2, 2, 3) - s0) * Dz;
-    a = a - (k0 + k_at(2, 2, 1)) * (s0 - s_at(2, 2, 1)) * Dz;
-    // wall-model point next to a wall-model side: + div * theta (the surface
-    // flux is zero); div as DivergenceWM with dzPr(k)
-    if ((k == 1 && d.wall[SIDE_BO]) || (k == nz && d.wall[SIDE_TO])) {
-      const T dzk = (T)d.dzPr[k + 2];
-      T div = (T)0;
-      div = div + ue / (T)d.dx;
-      div = div - uw / (T)d.dx;
-      div = div + vn / (T)d.dy;
-      div = div - vs / (T)d.dy;
-      div = div + wt / dzk;
-      div = div - wb / dzk;
-      a = a + div * s0;
+    const T rdx = (T)d.dx, rdy = (T)d.dy;
+    const T rdt = (T)(rho * d.dt), bdt = (T)(beta * d.dt);
+    const bool wm_lo = d.wall[SIDE_BO] != 0, wm_hi = d.wall[SIDE_TO] != 0;
+    long long cc = bidx(d, i, j, k0);
+    // column windows: theta at k-2..k+2, diffusivity at k-1..k+1, W at k-1
+    T sz[5], kz[3];
+#pragma unroll
+    for (int q = 0; q < 5; q++) sz[q] = ld(S, cc + (long long)(q - 2) * plane + zoff(k0 - 2 + q));
+#pragma unroll
+    for (int q = 0; q < 3; q++) kz[q] = ld(K, cc + (long long)(q - 1) * plane + zoff(k0 - 1 + q));
+    T wb = ld(W, cc - plane);
+    // the bottom-face flux of plane k is the top-face flux of plane k-1
+    T fzb = kappa_flux<T>(wb, sz[0], sz[1], sz[2], sz[3]);
+    for (int k = k0; k <= k1; k++) {
+      const T s0 = sz[2];
+      const T ue = ld(U, cc), uw = ld(U, cc - 1);
+      const T vn = ld(V, cc), vs = ld(V, cc - pitch);
+      const T wt = ld(W, cc);
+      const T sxm2 = ld(S, cc + ox[0]), sxm1 = ld(S, cc + ox[1]), sxp1 = ld(S, cc + ox[3]), sxp2 = ld(S, cc + ox[4]);
+      const T sym2 = ld(S, cc + oy[0]), sym1 = ld(S, cc + oy[1]), syp1 = ld(S, cc + oy[3]), syp2 = ld(S, cc + oy[4]);
+      const T k0v = kz[1];
+      const T kxm = ld(K, cc + ox[1]), kxp = ld(K, cc + ox[3]), kym = ld(K, cc + oy[1]), kyp = ld(K, cc + oy[3]);
+      const T told = stage1 ? (T)0 : ld((const T *)d.Tadv, cc);
+      // advection: the loop order of KappaScalar gives each cell +A f(low
+      // face) then -A f(high face) in x and y; in z the even faces come first
+      T a = (T)0;
+      a = a + Ax * kappa_flux<T>(uw, sxm2, sxm1, s0, sxp1);
+      a = a - Ax * kappa_flux<T>(ue, sxm1, s0, sxp1, sxp2);
+      a = a + Ay * kappa_flux<T>(vs, sym2, sym1, s0, syp1);
+      a = a - Ay * kappa_flux<T>(vn, sym1, s0, syp1, syp2);
+      const T fzt = kappa_flux<T>(wt, sz[1], s0, sz[3], sz[4]);
+      if (((k - 1) & 1) == 0) {  // face k-1 is even
+        a = a + Az * fzb;
+        a = a - Az * fzt;
+      } else {
+        a = a - Az * fzt;
+        a = a + Az * fzb;
+      }
+      // diffusion, in the order of ScalarDiffusion_nobranch
+      a = a + (kxp + k0v) * (sxp1 - s0) * Dx;
+      a = a - (k0v + kxm) * (s0 - sxm1) * Dx;
+      a = a + (kyp + k0v) * (syp1 - s0) * Dy;
+      a = a - (k0v + kym) * (s0 - sym1) * Dy;
+      a = a + (kz[2] + k0v) * (sz[3] - s0) * Dz;
+      a = a - (k0v + kz[0]) * (s0 - sz[1]) * Dz;
+      // wall-model point next to a wall-model side: + div * theta (the
+      // surface flux is zero); div as DivergenceWM with dzPr(k)
+      if ((k == 1 && wm_lo) || (k == nz && wm_hi)) {
+        const T dzk = (T)d.dzPr[k + 2];
+        T div = (T)0;
+        div = div + ue / rdx;
+        div = div - uw / rdx;
+        div = div + vn / rdy;
+        div = div - vs / rdy;
+        div = div + wt / dzk;
+        div = div - wb / dzk;
+        a = a + div * s0;
+      }
+      // RK combine of the stage: T2 = Tadv_old * (rho dt) + Tadv * (beta dt)
+      T t2 = stage1 ? (T)0 : told * rdt;
+      t2 = t2 + a * bdt;
+      d.Tadv[cc] = a;
+      d.Tn[cc] = s0 + t2;
+      // shift the windows up one plane
+      if (k < k1) {
+        const long long cn = cc + plane;
+#pragma unroll
+        for (int q = 0; q < 4; q++) sz[q] = sz[q + 1];
+        sz[4] = ld(S, cn + 2 * plane + zoff(k + 3));
+        kz[0] = kz[1];
+        kz[1] = kz[2];
+        kz[2] = ld(K, cn + plane + zoff(k + 2));
+        wb = wt;
+        fzb = fzt;
+        cc = cn;
+      }
     }
-    // RK combine of the stage: T2 = Tadv_old * (rho dt) + Tadv * (beta dt)
-    T t2 = stage1 ? (T)0 : ld((const T *)d.Tadv, cc) * (T)(rho * d.dt);
-    t2 = t2 + a * (T)(beta * d.dt);
-    d.Tadv[cc] = a;
-    d.Tn[cc] = s0 + t2;
   }
 }
 

@@ -1,10 +1,11 @@
 """Runs the benchmark workload for a profiler: one channel domain (by default
-256 x 256 x 128, the same configuration and seeded state as bench.py), the
-initial projection, W warm-up steps and S profiled steps, then prints the
-device time of the steps and the per-kernel times of one stage.
+256 x 256 x 128 with the potential temperature, the same configuration and
+seeded state as bench.py), the initial projection, W warm-up steps and S
+profiled steps, then prints the device time of the steps and the per-kernel
+times of one stage.
 
     python -m gpu_elmm_b200.profile_step [--precision mixed|fp64] [--n 256,256,128]
-                                         [--warmup 1] [--steps 1]
+                                         [--warmup 1] [--steps 1] [--no-temperature]
 
 Under `ncu -k regex:<kernel> -s <skip> -c <count>` the launches of the
 profiled steps follow those of the projection and the warm-up steps.
@@ -13,7 +14,7 @@ import argparse
 import json
 
 from .config import grid_of, make_config
-from .workloads import log_profile_state
+from .workloads import log_profile_state, temperature_state
 from . import lib as L
 
 
@@ -24,12 +25,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--stage-times", action="store_true", help="also time each kernel of stage 2 (5 repetitions)")
+    ap.add_argument("--no-temperature", action="store_true", help="the channel without the temperature field")
     a = ap.parse_args()
     n = tuple(int(x) for x in a.n.split(","))
-    cfg = make_config(*n, precision=1 if a.precision == "mixed" else 0)
+    buoy = not a.no_temperature
+    cfg = make_config(*n, precision=1 if a.precision == "mixed" else 0, buoyancy=buoy)
     g = grid_of(cfg)
     d = L.Domain(cfg)
     d.upload(*log_profile_state(g, seed=0))
+    if buoy:
+        d.upload_temperature(temperature_state(g, seed=0))
     d.project(1.0)
     if a.warmup:
         d.step(a.warmup)
