@@ -205,7 +205,7 @@ struct LaunchSet {
   Launch l() const { return Launch{starts, nd, total}; }
 };
 
-enum { LK_CELLS = 0, LK_BOX, LK_ROWS, LK_YCOLS, LK_TRI, LK_MOM, LK_SHELL, LK_XREG, LK_YREG, LK_TRIT, LK_TCOL, LK_N };
+enum { LK_CELLS = 0, LK_BOX, LK_ROWS, LK_YCOLS, LK_TRI, LK_MOM, LK_SHELL, LK_XREG, LK_YREG, LK_TRIT, LK_TCOL, LK_DCOL, LK_N };
 
 // -------------------------------------------------------------------- batch
 template <typename T>
@@ -457,6 +457,7 @@ struct BatchT {
       }
       case LK_TRIT: return tri_tiled(h) ? (h.ny * h.spitch + kTriCols - 1) / kTriCols : 0;
       case LK_TCOL: return h.buoy ? ntx * nty * ((h.nz + TMKC - 1) / TMKC) : 0;
+      case LK_DCOL: return ntx * nty * ((h.nz + kDivChunk - 1) / kDivChunk);
       default: return tri_tiled(h) ? 0 : (h.ny * h.spitch + kTriThreads - 1) / kTriThreads;
     }
   }
@@ -769,7 +770,7 @@ struct BatchT {
   int launch_divmax() {
     nlaunch++;
     for (int d = 0; d < nd; d++) cudaMemsetAsync(hdom[d].maxdiv_bits, 0, sizeof(unsigned long long), stream);
-    k_divmax<T><<<gsz(7, ls[LK_CELLS].total), TX * TY, 0, stream>>>(ddom, ls[LK_CELLS].l());
+    k_divmax<T><<<gsz(7, ls[LK_DCOL].total), TX * TY, 0, stream>>>(ddom, ls[LK_DCOL].l());
     return ELMM_OK;
   }
   int launch_cfl() {

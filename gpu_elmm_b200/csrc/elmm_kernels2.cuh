@@ -268,6 +268,9 @@ __global__ void __launch_bounds__(kShellThreads) k_ghosts(const Dom<T> *__restri
   }
 }
 
+// planes per column chunk of k_divmax
+constexpr int kDivChunk = 16;
+
 // Order-preserving bits of a non-negative double; NaN maps above every
 // finite value, so an integer maximum propagates it.
 __device__ __forceinline__ unsigned long long max_bits(double v) {
@@ -296,8 +299,9 @@ __device__ __forceinline__ void block_max_flush(unsigned long long *dst, unsigne
 // max |div u| in FP64 (the check of src/pressure.f90:884-989)
 template <typename T>
 __global__ void __launch_bounds__(TX *TY) k_divmax(const Dom<T> *__restrict__ doms, Launch L) {
-  // a running maximum per thread over the block's tiles; one block
-  // reduction and one atomic per domain the block visits
+  // a TX x TY column of cells marches up a chunk of kDivChunk planes; W at
+  // k-1 rides along in a register.  One block reduction and one atomic per
+  // domain the block visits.
   __shared__ unsigned long long red[TX * TY / 32];
   unsigned long long run = 0;
   int cur = -1;
@@ -310,20 +314,32 @@ __global__ void __launch_bounds__(TX *TY) k_divmax(const Dom<T> *__restrict__ do
     }
     const Dom<T> &d = doms[di];
     int lt = t - __ldg(L.starts + di);
-    const int ntx = (d.nx + TX - 1) / TX, nty = (d.ny + TY - 1) / TY;
+    const int nx = d.nx, ny = d.ny, nz = d.nz;
+    const int ntx = (nx + TX - 1) / TX, nty = (ny + TY - 1) / TY;
     const int tx = lt % ntx; lt /= ntx;
     const int ty = lt % nty;
-    const int k = lt / nty + 1;
+    const int k0 = (lt / nty) * kDivChunk + 1, k1 = min(k0 + kDivChunk - 1, nz);
     const int i = tx * TX + (threadIdx.x % TX) + 1;
     const int j = ty * TY + (threadIdx.x / TX) + 1;
-    if (i <= d.nx && j <= d.ny) {
-      const long long c = bidx(d, i, j, k);
-      const double dzk = d.vz ? d.dzPr[k + 2] : d.dz;
-      const double a = fabs(((double)ld(d.U, c) - (double)ld(d.U, c - 1)) / d.dx +
-                            ((double)ld(d.V, c) - (double)ld(d.V, c - d.pitch)) / d.dy +
-                            ((double)ld(d.W, c) - (double)ld(d.W, c - d.plane)) / dzk);
-      const unsigned long long b = max_bits(a);
-      run = b > run ? b : run;
+    if (i > nx || j > ny) continue;
+    const T *__restrict__ U = d.U;
+    const T *__restrict__ V = d.V;
+    const T *__restrict__ W = d.W;
+    const long long pitch = d.pitch, plane = d.plane;
+    const double dx = d.dx, dy = d.dy, dz = d.dz;
+    const bool vz = d.vz != 0;
+    const double *dzPr = d.dzPr;
+    long long c = bidx(d, i, j, k0);
+    double wb = (double)ld(W, c - plane);
+    for (int k = k0; k <= k1; k++) {
+      const double dzk = vz ? dzPr[k + 2] : dz;
+      const double wt = (double)ld(W, c);
+      const double a = fabs(((double)ld(U, c) - (double)ld(U, c - 1)) / dx +
+                            ((double)ld(V, c) - (double)ld(V, c - pitch)) / dy + (wt - wb) / dzk);
+      const unsigned long long bits = max_bits(a);
+      run = bits > run ? bits : run;
+      wb = wt;
+      c += plane;
     }
   }
   if (cur >= 0) block_max_flush<TX * TY>(doms[cur].maxdiv_bits, run, red);
