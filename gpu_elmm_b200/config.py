@@ -11,7 +11,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 # Boundary-condition codes of src/parameters.f90:249-250.
 BC_NOSLIP, BC_FREESLIP, BC_PERIODIC, BC_DIRICHLET, BC_NEUMANN, BC_CONSTFLUX = 1, 2, 3, 4, 5, 6
@@ -24,11 +24,24 @@ FIELD_U, FIELD_V, FIELD_W, FIELD_PR, FIELD_VISCOSITY = 0, 1, 2, 3, 4
 FIELD_U2, FIELD_V2, FIELD_W2 = 5, 6, 7
 FIELD_USTAR, FIELD_VSTAR, FIELD_WSTAR, FIELD_PHI = 8, 9, 10, 11
 FIELD_TEMPERATURE, FIELD_TDIFF, FIELD_TEMPERATURE_ADV = 12, 13, 14
+FIELD_SCALAR, FIELD_SCALAR_ADV = 16, 20  # + (sc - 1)
+
+MAX_SCALARS, MAX_POINT_SOURCES = 4, 8
 
 STATUS_NAMES = {
     0: "ELMM_OK", 1: "ELMM_ERR_INVALID_CONFIG", 2: "ELMM_ERR_OOM", 3: "ELMM_ERR_NAN",
     4: "ELMM_ERR_CUDA", 5: "ELMM_ERR_TIMEOUT", 6: "ELMM_ERR_INVALID_ARG", 7: "ELMM_ERR_ADMISSION",
 }
+
+
+class ElmmPointSource(C.Structure):
+    """ScalarPointSource (src/pointsources.f90:8-13)."""
+    _fields_ = [
+        ("scalar_number", C.c_int32),
+        ("reserved", C.c_int32),
+        ("position", C.c_double * 3),
+        ("flux", C.c_double),
+    ]
 
 
 class ElmmConfig(C.Structure):
@@ -60,6 +73,15 @@ class ElmmConfig(C.Structure):
         ("temperature_ref", C.c_double),
         ("grav_acc", C.c_double),
         ("molecular_diffusivity", C.c_double),
+        ("num_scalars", C.c_int32),
+        ("ScalBtype", C.c_int32 * 6),
+        ("sideScal", C.c_double * 6),
+        ("num_point_sources", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("point_sources", ElmmPointSource * MAX_POINT_SOURCES),
+        ("avg_slice_k", C.c_int32),
+        ("avg_slice_j", C.c_int32),
+        ("avg_weight", C.c_double),
     ]
 
 
@@ -152,12 +174,16 @@ def make_config(Prnx, Prny, Prnz, *, btype=(BC_PERIODIC, BC_PERIODIC, BC_PERIODI
                 wallmodeltype=None, z0=0.01, precision=PREC_FP64, zW=None,
                 pr_gradient_x=None, pr_gradient_y=None, max_refine_sweeps=0,
                 refine_tol=1e-6, cfl_check=0, device=0, origin=(0.0, 0.0, 0.0), buoyancy=False,
-                temperature_ref=295.0, grav_acc=9.81, prandtl=0.7):
+                temperature_ref=295.0, grav_acc=9.81, prandtl=0.7, num_scalars=0, point_sources=(),
+                avg_slice_k=0, avg_slice_j=0, avg_weight=0.0):
     """Builds an ElmmConfig.  The wall model defaults to on when an SGS model
     is on (src/initial.f90:2782-2787).  ``zW`` (Prnz+1 values) selects the
     stretched-z grid; the array is kept alive on the returned struct.
     ``buoyancy`` adds the potential-temperature field with adiabatic
-    (zero-flux) bottom and top and periodic x and y."""
+    (zero-flux) bottom and top and periodic x and y; ``num_scalars`` passive
+    scalars get the same boundary kinds.  ``point_sources``: (scalar_number,
+    (x, y, z), flux) triples.  ``avg_slice_k`` / ``avg_slice_j`` select the
+    time-averaged slices, ``avg_weight`` the weight of one step."""
     c = ElmmConfig()
     c.abi_version = ABI_VERSION
     c.Prnx, c.Prny, c.Prnz = Prnx, Prny, Prnz
@@ -199,6 +225,18 @@ def make_config(Prnx, Prny, Prnz, *, btype=(BC_PERIODIC, BC_PERIODIC, BC_PERIODI
     c.temperature_ref = temperature_ref
     c.grav_acc = grav_acc
     c.molecular_diffusivity = nu / prandtl
+    c.num_scalars = num_scalars
+    for s in range(6):
+        c.ScalBtype[s] = BC_PERIODIC if btype[s] == BC_PERIODIC else BC_CONSTFLUX
+        c.sideScal[s] = 0.0
+    assert len(point_sources) <= MAX_POINT_SOURCES
+    c.num_point_sources = len(point_sources)
+    for q, (sc, pos, flux) in enumerate(point_sources):
+        c.point_sources[q].scalar_number = sc
+        for a in range(3):
+            c.point_sources[q].position[a] = pos[a]
+        c.point_sources[q].flux = flux
+    c.avg_slice_k, c.avg_slice_j, c.avg_weight = avg_slice_k, avg_slice_j, avg_weight
     return c
 
 

@@ -194,7 +194,46 @@ static int check_config(const elmm_config &c) {
     if (!(c.temperature_ref > 0) || !(c.molecular_diffusivity >= 0))
       return fail(ELMM_ERR_INVALID_CONFIG, "temperature_ref must be positive and molecular_diffusivity non-negative");
   }
+  if (c.num_scalars < 0 || c.num_scalars > ELMM_MAX_SCALARS)
+    return fail(ELMM_ERR_INVALID_CONFIG, "num_scalars in 0.." + std::to_string(ELMM_MAX_SCALARS));
+  if (c.num_scalars > 0) {
+    for (int s = 0; s < 6; s++) {
+      const bool per = c.Btype[s] == ELMM_BC_PERIODIC;
+      if (per && c.ScalBtype[s] != ELMM_BC_PERIODIC)
+        return fail(ELMM_ERR_INVALID_CONFIG, "the scalars must be periodic where the flow is");
+      if (!per && !(c.ScalBtype[s] == ELMM_BC_CONSTFLUX && c.sideScal[s] == 0))
+        return fail(ELMM_ERR_INVALID_CONFIG, "scalar walls must be zero-flux (ELMM_BC_CONSTFLUX with sideScal = 0)");
+    }
+    if (c.zW) return fail(ELMM_ERR_INVALID_CONFIG, "the scalar fields need a uniform z grid");
+    if (!(c.molecular_diffusivity >= 0)) return fail(ELMM_ERR_INVALID_CONFIG, "molecular_diffusivity must be non-negative");
+  }
+  if (c.num_point_sources < 0 || c.num_point_sources > ELMM_MAX_POINT_SOURCES)
+    return fail(ELMM_ERR_INVALID_CONFIG, "num_point_sources in 0.." + std::to_string(ELMM_MAX_POINT_SOURCES));
+  for (int q = 0; q < c.num_point_sources; q++) {
+    const elmm_point_source &p = c.point_sources[q];
+    if (p.scalar_number < 1 || p.scalar_number > c.num_scalars)
+      return fail(ELMM_ERR_INVALID_CONFIG, "point source " + std::to_string(q) + ": scalar_number outside 1..num_scalars");
+    if (!std::isfinite(p.flux) || !std::isfinite(p.position[0]) || !std::isfinite(p.position[1]) ||
+        !std::isfinite(p.position[2]))
+      return fail(ELMM_ERR_INVALID_CONFIG, "point source " + std::to_string(q) + ": non-finite position or flux");
+  }
+  if (c.avg_slice_k < 0 || c.avg_slice_k > c.Prnz || c.avg_slice_j < 0 || c.avg_slice_j > c.Prny)
+    return fail(ELMM_ERR_INVALID_CONFIG, "avg_slice_k in 0..Prnz and avg_slice_j in 0..Prny");
+  if (!std::isfinite(c.avg_weight)) return fail(ELMM_ERR_INVALID_CONFIG, "avg_weight must be finite");
   return ELMM_OK;
+}
+
+// InDomain (src/boundaries.f90:163-168) and GridCoords_scalar
+// (src/boundaries.f90:54-97) on a uniform grid: the cell that holds a point
+// source, or false when the point lies outside the domain.  nint rounds half
+// away from zero.
+static bool point_cell(const elmm_config &c, const double *r, int *ip) {
+  const double lo[3] = {c.xmin, c.ymin, c.zmin}, h[3] = {c.dxmin, c.dymin, c.dzmin};
+  const int n[3] = {c.Prnx, c.Prny, c.Prnz};
+  for (int a = 0; a < 3; a++)
+    if (!(r[a] >= lo[a] && r[a] <= n[a] * h[a] + lo[a])) return false;
+  for (int a = 0; a < 3; a++) ip[a] = std::min(std::max((int)std::lround((r[a] - lo[a]) / h[a] + 0.5), 1), n[a]);
+  return true;
 }
 
 // ---------------------------------------------------------------- launches
@@ -205,7 +244,8 @@ struct LaunchSet {
   Launch l() const { return Launch{starts, nd, total}; }
 };
 
-enum { LK_CELLS = 0, LK_BOX, LK_ROWS, LK_YCOLS, LK_TRI, LK_MOM, LK_SHELL, LK_XREG, LK_YREG, LK_TRIT, LK_TCOL, LK_DCOL, LK_N };
+enum { LK_CELLS = 0, LK_BOX, LK_ROWS, LK_YCOLS, LK_TRI, LK_MOM, LK_SHELL, LK_XREG, LK_YREG, LK_TRIT, LK_TCOL, LK_DCOL,
+       LK_AVG, LK_N };
 
 // -------------------------------------------------------------------- batch
 template <typename T>
@@ -456,8 +496,9 @@ struct BatchT {
         return ((h.nxh + C - 1) / C) * h.nz;
       }
       case LK_TRIT: return tri_tiled(h) ? (h.ny * h.spitch + kTriCols - 1) / kTriCols : 0;
-      case LK_TCOL: return h.buoy ? ntx * nty * ((h.nz + TMKC - 1) / TMKC) : 0;
+      case LK_TCOL: return ntx * nty * ((h.nz + TMKC - 1) / TMKC) * h.nslot;
       case LK_DCOL: return ntx * nty * ((h.nz + kDivChunk - 1) / kDivChunk);
+      case LK_AVG: return (h.nslot - (h.buoy ? 1 : 0)) * ((h.avg_k > 0 ? h.ny : 0) + (h.avg_j > 0 ? h.nz : 0));
       default: return tri_tiled(h) ? 0 : (h.ny * h.spitch + kTriThreads - 1) / kTriThreads;
     }
   }
@@ -611,8 +652,45 @@ struct BatchT {
       h.grav = c.grav_acc;
       h.kappa_mol = c.molecular_diffusivity;
       h.toff = sizeof(T) == 4 ? c.temperature_ref : 0.0;  // FP32 stores theta - T_ref
-      for (T **f : {&h.Tm, &h.Tn, &h.Tadv, &h.TDiff})
+      for (T **f : {&h.Tm, &h.Tn, &h.Tadv})
         if ((r = dalloc((void **)f, alloc_elems * sizeof(T)))) return r;
+      ScalSlot<T> &sl = h.slot[h.nslot++];
+      sl.m = h.Tm; sl.n = h.Tn; sl.adv = h.Tadv;
+      for (int s2 = 0; s2 < 6; s2++) sl.bt[s2] = c.TempBtype[s2];
+      sl.off = h.toff;
+      h.tdiff_live = 1;
+    }
+    h.kappa_mol = c.molecular_diffusivity;
+    for (int sc = 0; sc < c.num_scalars; sc++) {
+      ScalSlot<T> &sl = h.slot[h.nslot++];
+      for (T **f : {&sl.m, &sl.n, &sl.adv})
+        if ((r = dalloc((void **)f, alloc_elems * sizeof(T)))) return r;
+      for (int s2 = 0; s2 < 6; s2++) sl.bt[s2] = c.ScalBtype[s2];
+      sl.off = 0;
+      if (c.avg_slice_k > 0 && (r = dalloc((void **)&sl.acc_xy, sizeof(double) * h.nx * h.ny))) return r;
+      if (c.avg_slice_j > 0 && (r = dalloc((void **)&sl.acc_xz, sizeof(double) * h.nx * h.nz))) return r;
+    }
+    h.avg_k = c.avg_slice_k;
+    h.avg_j = c.avg_slice_j;
+    h.avg_w = c.avg_weight;
+    // point sources -> volume sources of one cell each (ScalarPointSource's
+    // point_source, src/pointsources.f90:24-39): flux / volumePr
+    for (int q = 0; q < c.num_point_sources; q++) {
+      const elmm_point_source &p = c.point_sources[q];
+      int ip[3];
+      if (!point_cell(c, p.position, ip)) continue;  // outside the domain: no volume
+      const int e = h.nsrc++;
+      h.src_slot[e] = (h.buoy ? 1 : 0) + p.scalar_number - 1;
+      h.src_i[e] = ip[0]; h.src_j[e] = ip[1]; h.src_k[e] = ip[2];
+      h.src_q[e] = p.flux / (g.dxPr[ip[0]] * g.dyPr[ip[1]] * g.dzPr[ip[2] + 2]);
+    }
+    if (c.enable_buoyancy || c.num_scalars > 0) {
+      if ((r = dalloc((void **)&h.TDiff, alloc_elems * sizeof(T)))) return r;
+      // TDiff starts at the molecular diffusivity (src/initial.f90:4262-4268)
+      if (c.molecular_viscosity > 0) {
+        std::vector<T> kv(alloc_elems, (T)c.molecular_diffusivity);
+        CU(cudaMemcpy(h.TDiff, kv.data(), alloc_elems * sizeof(T), cudaMemcpyHostToDevice));
+      }
     }
     if ((r = dalloc((void **)&h.prm, sizeof(double)))) return r;
     h.nprpart = ((h.nx + MX - 1) / MX) * ((h.ny + MY - 1) / MY);
@@ -647,7 +725,7 @@ struct BatchT {
   }
   int launch_sgs() {
     nlaunch++;
-    k_sgs<T><<<gsz(0, ls[LK_MOM].total), SgsShape<T>::threads, smem_sgs, stream>>>(ddom, ls[LK_MOM].l());
+    k_sgs<T><<<gsz(0, ls[LK_MOM].total), SgsShape<T>::threads, smem_sgs, stream>>>(ddom, ls[LK_MOM].l(), 0);
     launch_ghosts({F_NU}, 0);
     return ELMM_OK;
   }
@@ -666,20 +744,23 @@ struct BatchT {
     launch_ghosts({F_U, F_V, F_W, F_P}, gate);
     k_prref<T><<<std::min(nd, 1024), 256, 0, stream>>>(ddom, nd, gate);
   }
-  bool any_buoy() const {
-    for (auto &h : hdom)
-      if (h.buoy) return true;
-    return false;
-  }
-  // one ScalarRK3 stage of the temperature; the new value then becomes the
-  // current one (the stage reads the old value at neighbours while writing)
-  void launch_temperature(int stage) {
-    if (!any_buoy()) return;
+  // one ScalarRK3 stage of every transported scalar; the new values then
+  // become the current ones (the stage reads the old value at neighbours
+  // while writing).  accumulate: the last stage of a step, which also feeds
+  // the time-averaged slices.
+  void launch_scalars(int stage, int accumulate) {
+    if (ls[LK_TCOL].total == 0) return;
     nlaunch++;
-    k_temperature<T><<<gsz(7, ls[LK_TCOL].total), TX * TY, 0, stream>>>(ddom, ls[LK_TCOL].l(), kRho[stage - 1],
-                                                                         kBeta[stage - 1], stage == 1);
+    k_scalar<T><<<gsz(7, ls[LK_TCOL].total), TX * TY, 0, stream>>>(ddom, ls[LK_TCOL].l(), kRho[stage - 1],
+                                                                    kBeta[stage - 1], stage == 1);
     for (auto &h : hdom)
-      if (h.buoy) cudaMemcpyAsync(h.Tm, h.Tn, (size_t)h.plane * (h.nz + 2) * sizeof(T), cudaMemcpyDeviceToDevice, stream);
+      for (int q = 0; q < h.nslot; q++)
+        cudaMemcpyAsync(h.slot[q].m, h.slot[q].n, (size_t)h.plane * (h.nz + 2) * sizeof(T), cudaMemcpyDeviceToDevice,
+                        stream);
+    if (accumulate && ls[LK_AVG].total > 0) {
+      nlaunch++;
+      k_scalar_avg<T><<<std::min(ls[LK_AVG].total, 8 * 148), 128, 0, stream>>>(ddom, ls[LK_AVG].l());
+    }
   }
   // PressureCorrection on U2 (in_place = 0) or on U itself (initial projection)
   int launch_projection(double coef_alpha2, int use_dt, int in_place) {
@@ -783,11 +864,11 @@ struct BatchT {
     // U <-> U2 after the projection wrote U directly: nothing to swap; the
     // projection writes the new velocity into U (exchange_alloc in tsteps.f90:211-213)
   }
-  int run_stage(int stage, int stop) {
+  int run_stage(int stage, int stop, int accumulate = 0) {
     launch_sgs();
     if (stop == 1) return ELMM_OK;
     launch_momentum(stage);
-    launch_temperature(stage);  // ScalarRK3 between Convection and the projection (tsteps.f90:132-135)
+    launch_scalars(stage, accumulate);  // ScalarRK3 between Convection and the projection (tsteps.f90:132-135)
     if (stop == 2) return ELMM_OK;
     launch_projection(2 * kAlpha[stage - 1], 1, 0);
     launch_refine(2 * kAlpha[stage - 1], 1);
@@ -795,7 +876,7 @@ struct BatchT {
   }
   int enqueue_step(bool cfl, bool div) {
     if (cfl) launch_cfl();
-    for (int s = 1; s <= 3; s++) run_stage(s, 3);
+    for (int s = 1; s <= 3; s++) run_stage(s, 3, s == 3);
     if (div) launch_divmax();
     return ELMM_OK;
   }
@@ -890,6 +971,10 @@ struct BatchT {
     launch_projection(coef, 0, 0);
     launch_refine(coef, 0);
     launch_divmax();
+    // the end of InitialConditions (src/initial.f90:4291-4313): eddy
+    // viscosity of the projected field and, with scalars, their diffusivity
+    k_sgs<T><<<gsz(0, ls[LK_MOM].total), SgsShape<T>::threads, smem_sgs, stream>>>(ddom, ls[LK_MOM].l(), 1);
+    launch_ghosts({F_NU}, 0);
     CU(cudaEventRecord(t1, stream));
     CU(cudaStreamSynchronize(stream));
     CU(cudaGetLastError());
@@ -916,7 +1001,7 @@ struct BatchT {
         cudaEventRecord(ev[2 * slot.size() + 1], stream);
         slot.push_back(k);
       };
-      timed(0, [&] { k_sgs<T><<<gsz(0, ls[LK_MOM].total), SgsShape<T>::threads, smem_sgs, stream>>>(ddom, ls[LK_MOM].l()); });
+      timed(0, [&] { k_sgs<T><<<gsz(0, ls[LK_MOM].total), SgsShape<T>::threads, smem_sgs, stream>>>(ddom, ls[LK_MOM].l(), 0); });
       timed(kGhost, [&] { launch_ghosts({F_NU}, 0); });
       timed(1, [&] {
         k_momentum<T><<<gsz(1, ls[LK_MOM].total), MomShape<T>::threads, smem_mom, stream>>>(ddom, ls[LK_MOM].l(), sc);
@@ -929,7 +1014,7 @@ struct BatchT {
       timed(7, [&] { k_project<T><<<gsz(6, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l(), a2, 1, 0, 0); });
       timed(kGhost, [&] { launch_ghosts({F_U, F_V, F_W, F_P}, 0); });
       timed(8, [&] { k_prref<T><<<std::min(nd, 1024), 256, 0, stream>>>(ddom, nd, 0); });
-      timed(10, [&] { launch_temperature(stage); });
+      timed(10, [&] { launch_scalars(stage, 0); });
       CU(cudaStreamSynchronize(stream));
       CU(cudaGetLastError());
       for (size_t q = 0; q < slot.size(); q++) {
@@ -998,12 +1083,57 @@ struct BatchT {
     const size_t n = (size_t)(h.nx + 6) * (h.ny + 6) * (h.nz + 6);
     CU(cudaMemsetAsync(dbad, 0, sizeof(int), stream));
     CU(cudaMemcpyAsync(dstage, Th, n * sizeof(double), cudaMemcpyHostToDevice, stream));
-    k_unpack_temperature<T><<<256, 256, 0, stream>>>(ddom + d, dstage, dbad);
+    k_unpack_scalar<T><<<256, 256, 0, stream>>>(ddom + d, 0, dstage, dbad);
     int bad = 0;
     CU(cudaMemcpyAsync(&bad, dbad, sizeof(int), cudaMemcpyDeviceToHost, stream));
     CU(cudaStreamSynchronize(stream));
     CU(cudaGetLastError());
     if (bad) return fail(ELMM_ERR_NAN, "non-finite value in the uploaded temperature");
+    return ELMM_OK;
+  }
+
+  int upload_scalar(int d, int sc, const double *S) {
+    if (d < 0 || d >= nd) return fail(ELMM_ERR_INVALID_ARG, "domain index");
+    if (!S) return fail(ELMM_ERR_INVALID_ARG, "NULL scalar array");
+    if (sc < 1 || sc > cfg[d].num_scalars) return fail(ELMM_ERR_INVALID_ARG, "scalar number outside 1..num_scalars");
+    CU(cudaSetDevice(device));
+    if (frame_pending) CU(cudaStreamWaitEvent(stream, ev_packed, 0));
+    const Dom<T> &h = hdom[d];
+    const size_t n = (size_t)(h.nx + 6) * (h.ny + 6) * (h.nz + 6);
+    CU(cudaMemsetAsync(dbad, 0, sizeof(int), stream));
+    CU(cudaMemcpyAsync(dstage, S, n * sizeof(double), cudaMemcpyHostToDevice, stream));
+    k_unpack_scalar<T><<<256, 256, 0, stream>>>(ddom + d, (h.buoy ? 1 : 0) + sc - 1, dstage, dbad);
+    int bad = 0;
+    CU(cudaMemcpyAsync(&bad, dbad, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    CU(cudaStreamSynchronize(stream));
+    CU(cudaGetLastError());
+    if (bad) return fail(ELMM_ERR_NAN, "non-finite value in the uploaded scalar");
+    return ELMM_OK;
+  }
+
+  int download_scalar_slices(int d, int sc, double *xy, double *xz) {
+    if (d < 0 || d >= nd) return fail(ELMM_ERR_INVALID_ARG, "domain index");
+    if (sc < 1 || sc > cfg[d].num_scalars) return fail(ELMM_ERR_INVALID_ARG, "scalar number outside 1..num_scalars");
+    const Dom<T> &h = hdom[d];
+    const ScalSlot<T> &sl = h.slot[(h.buoy ? 1 : 0) + sc - 1];
+    if ((xy && !sl.acc_xy) || (xz && !sl.acc_xz))
+      return fail(ELMM_ERR_INVALID_ARG, "no such slice (avg_slice_k / avg_slice_j is 0)");
+    CU(cudaSetDevice(device));
+    if (xy) CU(cudaMemcpyAsync(xy, sl.acc_xy, sizeof(double) * h.nx * h.ny, cudaMemcpyDeviceToHost, stream));
+    if (xz) CU(cudaMemcpyAsync(xz, sl.acc_xz, sizeof(double) * h.nx * h.nz, cudaMemcpyDeviceToHost, stream));
+    CU(cudaStreamSynchronize(stream));
+    CU(cudaGetLastError());
+    return ELMM_OK;
+  }
+
+  int reset_scalar_averages() {
+    CU(cudaSetDevice(device));
+    for (auto &h : hdom)
+      for (int q = 0; q < h.nslot; q++) {
+        if (h.slot[q].acc_xy) CU(cudaMemsetAsync(h.slot[q].acc_xy, 0, sizeof(double) * h.nx * h.ny, stream));
+        if (h.slot[q].acc_xz) CU(cudaMemsetAsync(h.slot[q].acc_xz, 0, sizeof(double) * h.nx * h.nz, stream));
+      }
+    CU(cudaStreamSynchronize(stream));
     return ELMM_OK;
   }
 
@@ -1040,8 +1170,11 @@ struct BatchT {
         const int lo = field == ELMM_FIELD_TDIFF ? -1 : -2;
         const size_t n = (size_t)(h.nx + 2 * (1 - lo)) * (h.ny + 2 * (1 - lo)) * (h.nz + 2 * (1 - lo));
         const T *Fs = field == ELMM_FIELD_TEMPERATURE ? h.Tm : field == ELMM_FIELD_TDIFF ? h.TDiff : h.Tadv;
-        k_pack_temperature<T><<<256, 256, 0, s>>>(ddom + d, Fs, dst, lo, field == ELMM_FIELD_TEMPERATURE ? h.toff : 0.0,
-                                                  field == ELMM_FIELD_TEMPERATURE_ADV);
+        // TDiff folds like the viscosity: periodic where the flow is
+        const int *bt = field == ELMM_FIELD_TDIFF ? h.bt : h.tbt;
+        k_pack_scalar_box<T><<<256, 256, 0, s>>>(ddom + d, Fs, dst, lo, field == ELMM_FIELD_TEMPERATURE ? h.toff : 0.0,
+                                                 field == ELMM_FIELD_TEMPERATURE_ADV, bt[0] == BC_PERIODIC,
+                                                 bt[2] == BC_PERIODIC, bt[4] == BC_PERIODIC);
         return n;
       }
       case ELMM_FIELD_VISCOSITY: case ELMM_FIELD_PHI: {
@@ -1053,13 +1186,26 @@ struct BatchT {
         return n;
       }
     }
+    if (field >= ELMM_FIELD_SCALAR && field < ELMM_FIELD_SCALAR_ADV + ELMM_MAX_SCALARS) {
+      const bool adv = field >= ELMM_FIELD_SCALAR_ADV;
+      const ScalSlot<T> &sl = h.slot[(h.buoy ? 1 : 0) + field - (adv ? ELMM_FIELD_SCALAR_ADV : ELMM_FIELD_SCALAR)];
+      const size_t n = (size_t)(h.nx + 6) * (h.ny + 6) * (h.nz + 6);
+      k_pack_scalar_box<T><<<256, 256, 0, s>>>(ddom + d, adv ? sl.adv : sl.m, dst, -2, sl.off, adv,
+                                               sl.bt[0] == BC_PERIODIC, sl.bt[2] == BC_PERIODIC, sl.bt[4] == BC_PERIODIC);
+      return n;
+    }
     return 0;
   }
 
   int download_field(int d, int field, double *host) {
     if (d < 0 || d >= nd) return fail(ELMM_ERR_INVALID_ARG, "domain index");
-    if (field < 0 || field > ELMM_FIELD_TEMPERATURE_ADV) return fail(ELMM_ERR_INVALID_ARG, "field id");
-    if (field >= ELMM_FIELD_TEMPERATURE && !hdom[d].buoy)
+    const int nsc = cfg[d].num_scalars;
+    const bool scal = (field >= ELMM_FIELD_SCALAR && field < ELMM_FIELD_SCALAR + nsc) ||
+                      (field >= ELMM_FIELD_SCALAR_ADV && field < ELMM_FIELD_SCALAR_ADV + nsc);
+    if (!scal && (field < 0 || field > ELMM_FIELD_TEMPERATURE_ADV)) return fail(ELMM_ERR_INVALID_ARG, "field id");
+    if (field == ELMM_FIELD_TDIFF && !hdom[d].TDiff)
+      return fail(ELMM_ERR_INVALID_ARG, "no diffusivity field (no temperature and no scalars)");
+    if ((field == ELMM_FIELD_TEMPERATURE || field == ELMM_FIELD_TEMPERATURE_ADV) && !hdom[d].buoy)
       return fail(ELMM_ERR_INVALID_ARG, "no temperature field (enable_buoyancy is 0)");
     if (!host) return fail(ELMM_ERR_INVALID_ARG, "NULL host array");
     CU(cudaSetDevice(device));
@@ -1251,6 +1397,21 @@ int elmm_upload_temperature(elmm_handle *h, const double *T) {
   return DISPATCH(h->b, upload_temperature(0, T));
 }
 
+int elmm_upload_scalar(elmm_handle *h, int32_t sc, const double *S) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  return DISPATCH(h->b, upload_scalar(0, sc, S));
+}
+
+int elmm_download_scalar_slices(elmm_handle *h, int32_t sc, double *xy, double *xz) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  return DISPATCH(h->b, download_scalar_slices(0, sc, xy, xz));
+}
+
+int elmm_reset_scalar_averages(elmm_handle *h) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  return DISPATCH(h->b, reset_scalar_averages());
+}
+
 int elmm_frame_begin(elmm_handle *h) {
   if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
   return DISPATCH(h->b, frame_begin());
@@ -1315,6 +1476,21 @@ int elmm_batch_upload_state(elmm_batch *b, int32_t d, const double *U, const dou
 int elmm_batch_download_state(elmm_batch *b, int32_t d, double *U, double *V, double *W, double *Pr) {
   if (!b) return fail(ELMM_ERR_INVALID_ARG, "NULL batch");
   return DISPATCH(*b, download(d, U, V, W, Pr));
+}
+
+int elmm_batch_upload_scalar(elmm_batch *b, int32_t d, int32_t sc, const double *S) {
+  if (!b) return fail(ELMM_ERR_INVALID_ARG, "NULL batch");
+  return DISPATCH(*b, upload_scalar(d, sc, S));
+}
+
+int elmm_batch_download_field(elmm_batch *b, int32_t d, int32_t field, double *host) {
+  if (!b) return fail(ELMM_ERR_INVALID_ARG, "NULL batch");
+  return DISPATCH(*b, download_field(d, field, host));
+}
+
+int elmm_batch_download_scalar_slices(elmm_batch *b, int32_t d, int32_t sc, double *xy, double *xz) {
+  if (!b) return fail(ELMM_ERR_INVALID_ARG, "NULL batch");
+  return DISPATCH(*b, download_scalar_slices(d, sc, xy, xz));
 }
 
 int elmm_batch_project(elmm_batch *b, double coef) {

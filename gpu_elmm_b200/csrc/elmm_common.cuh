@@ -36,6 +36,19 @@ template <typename T> struct Vec2;
 template <> struct Vec2<double> { typedef double2 type; };
 template <> struct Vec2<float> { typedef float2 type; };
 
+// One transported scalar of ScalarRK3 (src/scalars.f90:233-299): the
+// potential temperature or a passive scalar.  Box fields in the layout of
+// the velocity boxes.
+constexpr int kMaxSlots = 5;    // temperature + ELMM_MAX_SCALARS passive scalars
+constexpr int kMaxSources = 8;  // ELMM_MAX_POINT_SOURCES
+template <typename T>
+struct ScalSlot {
+  T *m, *n, *adv;        // value at the stage start, the stage's new value, the stage tendency
+  int bt[6];             // BC per side (TempBtype / ScalBtype)
+  double off;            // the box stores value - off
+  double *acc_xy, *acc_xz;  // time-averaged slices (FP64, [j][i] and [k][i]) or null
+};
+
 // Domain descriptor, copied to device memory once at creation.  Coefficients
 // are kept in FP64 and converted to the kernel's arithmetic type on use.
 template <typename T>
@@ -104,6 +117,19 @@ struct Dom {
   int tbt[6];            // temperature BC per side
   T *Tm, *Tn, *Tadv, *TDiff;
   double toff, tref, grav, kappa_mol;
+  // scalar slots of the ScalarRK3 kernel: slot 0 is the temperature when
+  // buoy is set (its fields alias Tm, Tn, Tadv), then the passive scalars
+  int nslot;
+  ScalSlot<T> slot[kMaxSlots];
+  int tdiff_live;        // 1: TDiff follows the viscosity every stage (buoyancy)
+  // volume sources of the point sources, in the order of the configuration:
+  // slot, cell, flux / volume of the cell
+  int nsrc;
+  int src_slot[kMaxSources], src_i[kMaxSources], src_j[kMaxSources], src_k[kMaxSources];
+  double src_q[kMaxSources];
+  // time-averaged slices: plane k, plane j (0: none), weight of one step
+  int avg_k, avg_j;
+  double avg_w;
 };
 
 template <typename T>

@@ -681,7 +681,7 @@ struct SgsShape<float> {
 
 template <typename T>
 __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
-    k_sgs(const Dom<T> *__restrict__ doms, Launch L) {
+    k_sgs(const Dom<T> *__restrict__ doms, Launch L, int init) {
   // planes of U, V, W (tile plus one-cell halo) arrive by tensor-map TMA in
   // a ring of kRingSlots slots, as in k_momentum
   typedef SlotLayout<T, 3, 0> Lay;
@@ -732,7 +732,11 @@ __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
                                (j0 + MY - 1 >= ny - 1 ? 8 : 0));
     const T num = (T)d.nu_mol;
     const bool sgs = d.sgs != 0, addmol = d.nu_mol > 0;
-    const bool buoy = d.buoy != 0;  // temperature diffusivity too (ComputeTDiff)
+    // the scalar diffusivity too: every stage with buoyancy (ComputeTDiff,
+    // src/dynamics.f90:904), and once after the initial projection whenever
+    // a scalar is transported (src/initial.f90:4296-4313, which uses the
+    // first formula of ComputeTDiff for any molecular viscosity)
+    const bool buoy = d.tdiff_live != 0 || (init && d.nslot > 0);
     const T kap = (T)d.kappa_mol;
     SgsK<T> q;
     q.rdx = (T)(1.0 / d.dx); q.rdy = (T)(1.0 / d.dy);
@@ -765,7 +769,8 @@ __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
           if (addmol) v = v + bc2(num);
           *reinterpret_cast<float2 *>(nu + c) = v.v;
           if (buoy) {
-            const float2 td = make_float2(tdiff_of(v.v.x, num, kap), tdiff_of(v.v.y, num, kap));
+            const float2 td = init ? make_float2((v.v.x - num) / 0.6f + kap, (v.v.y - num) / 0.6f + kap)
+                                   : make_float2(tdiff_of(v.v.x, num, kap), tdiff_of(v.v.y, num, kap));
             *reinterpret_cast<float2 *>(d.TDiff + c) = td;
           }
         }
@@ -782,11 +787,11 @@ __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
             if (addmol) v = v + num;
           }
           nu[c + qc] = v;
-          if (buoy) d.TDiff[c + qc] = tdiff_of(v, num, kap);
+          if (buoy) d.TDiff[c + qc] = init ? (v - num) / (T)0.6 + kap : tdiff_of(v, num, kap);
         }
       }
       const int wk = wtile | (wmask & ((k == 1 ? 16 : 0) | (k >= nz - 1 ? 32 : 0)));
-      if (ok && wk) {
+      if (ok && wk && !init) {  // the initial eddy viscosity leaves the wall model alone
 #pragma unroll 1
         for (int qc = 0; qc < CPT; qc++) {
           const int iq = i + qc;

@@ -1,17 +1,22 @@
-// elmm_temperature.cuh -- one stage of ScalarRK3 for the potential
-// temperature (src/scalars.f90:88-299): KappaScalar advection
-// (src/scalar_advection.f90:102-272), ScalarDiffusion_nobranch
-// (src/scalar_diffusion.f90:404-507), the wall-model point term of
-// TemperatureExtra (src/scalars.f90:301-334, DivergenceWM
-// src/wallmodels.f90:1150-1166) and the RK combine, one cell per thread.
+// elmm_temperature.cuh -- one stage of ScalarRK3 (src/scalars.f90:88-299)
+// for every transported scalar of a domain, the potential temperature and the
+// passive scalars: KappaScalar advection (src/scalar_advection.f90:102-272),
+// ScalarDiffusion_nobranch (src/scalar_diffusion.f90:404-507), the volume
+// sources of the point sources (ScalarExtra -> ScalarVolumeSources,
+// src/scalars.f90:364-379, src/volumesources.f90:741-771), the wall-model
+// point term (TemperatureExtra / ScalarExtra, DivergenceWM
+// src/wallmodels.f90:1150-1166) and the RK combine, one cell per thread; in
+// the last stage of a step the new value also enters the time-averaged
+// slices (Scalar_avg, src/outputs.f90:1043-1045).
 //
 // The stencil reaches two cells in each direction.  Instead of a two-deep
 // ghost shell the kernel folds every neighbour index onto the interior as
-// BoundTemperature (src/scalarboundaries.f90:12-300) fills it for the
-// supported conditions: periodic copies, and the first interior cell for a
-// zero-flux (constant-flux 0) side at every ghost depth.  The diffusivity
-// folds by BoundViscosity (periodic copy or adjacent cell), the same map.
-// Without solid bodies every face carries flux (src/wallmodels.f90:910-950).
+// BoundTemperature / BoundScalar (src/scalarboundaries.f90:12-308) fill it
+// for the supported conditions: periodic copies, and the first interior cell
+// for a zero-flux (constant-flux 0) side at every ghost depth.  The
+// diffusivity folds by BoundViscosity (periodic copy or adjacent cell), the
+// same map.  Without solid bodies every face carries flux
+// (src/wallmodels.f90:910-950).
 #pragma once
 
 #include "elmm_common.cuh"
@@ -56,29 +61,32 @@ __device__ __forceinline__ T kappa_flux(T vel, T a, T b, T c, T e) {
   return vel > 0 ? vel * (b + (b - a) * slope / (T)2) : vel * (c + (c - e) * slope / (T)2);
 }
 
-// A block owns a TX x TY column of cells and marches up a chunk of TMKC
-// planes; theta(k-2..k+2), the diffusivity (k-1..k+1) and W(k-1) ride along
-// in registers, x and y neighbours come from offsets folded once per thread.
+// A block owns a TX x TY column of cells of one scalar slot and marches up a
+// chunk of TMKC planes; the scalar (k-2..k+2), the diffusivity (k-1..k+1)
+// and W(k-1) ride along in registers, x and y neighbours come from offsets
+// folded once per thread.  Tiles: (slot, column, chunk) per domain.
 constexpr int TMKC = 16;
 
 template <typename T>
 __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
-    k_temperature(const Dom<T> *__restrict__ doms, Launch L, double rho, double beta, int stage1) {
+    k_scalar(const Dom<T> *__restrict__ doms, Launch L, double rho, double beta, int stage1) {
   for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
     const int di = find_dom(L.starts, L.nd, t);
     const Dom<T> &d = doms[di];
-    if (!d.buoy) continue;
     int lt = t - __ldg(L.starts + di);
     const int nx = d.nx, ny = d.ny, nz = d.nz;
-    const int ntx = (nx + TX - 1) / TX, nty = (ny + TY - 1) / TY;
+    const int ntx = (nx + TX - 1) / TX, nty = (ny + TY - 1) / TY, nkc = (nz + TMKC - 1) / TMKC;
     const int tx = lt % ntx; lt /= ntx;
-    const int ty = lt % nty;
-    const int k0 = (lt / nty) * TMKC + 1, k1 = min(k0 + TMKC - 1, nz);
+    const int ty = lt % nty; lt /= nty;
+    const int kc = lt % nkc;
+    const int s = lt / nkc;
+    const ScalSlot<T> &sl = d.slot[s];
+    const int k0 = kc * TMKC + 1, k1 = min(k0 + TMKC - 1, nz);
     const int i = tx * TX + (threadIdx.x % TX) + 1;
     const int j = ty * TY + (threadIdx.x / TX) + 1;
     if (i > nx || j > ny) continue;
-    const bool px = d.tbt[SIDE_WE] == BC_PERIODIC, py = d.tbt[SIDE_SO] == BC_PERIODIC,
-               pz = d.tbt[SIDE_BO] == BC_PERIODIC;
+    const bool px = sl.bt[SIDE_WE] == BC_PERIODIC, py = sl.bt[SIDE_SO] == BC_PERIODIC,
+               pz = sl.bt[SIDE_BO] == BC_PERIODIC;
     const long long pitch = d.pitch, plane = d.plane;
     // folded offsets of the x and y neighbours -2..+2 (index 0..4); a plane
     // holds fewer than 2^31 elements
@@ -89,18 +97,24 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
       oy[q] = (scal_fold(j - 2 + q, ny, py) - j) * (int)pitch;
     }
     auto zoff = [&](int kk) { return (long long)(scal_fold(kk, nz, pz) - kk) * plane; };  // fold of plane kk
-    const T *__restrict__ S = d.Tm;
+    // volume sources of this slot in this column, in configuration order
+    unsigned srcm = 0;
+    for (int q = 0; q < d.nsrc; q++)
+      if (d.src_slot[q] == s && d.src_i[q] == i && d.src_j[q] == j) srcm |= 1u << q;
+    const T *__restrict__ S = sl.m;
     const T *__restrict__ K = d.TDiff;
     const T *__restrict__ U = d.U;
     const T *__restrict__ V = d.V;
     const T *__restrict__ W = d.W;
+    T *__restrict__ Sadv = sl.adv;
+    T *__restrict__ Snew = sl.n;
     const T Ax = (T)(1.0 / d.dx), Ay = (T)(1.0 / d.dy), Az = (T)(1.0 / d.dz);
     const T Dx = (T)(1.0 / (2 * d.dx * d.dx)), Dy = (T)(1.0 / (2 * d.dy * d.dy)), Dz = (T)(1.0 / (2 * d.dz * d.dz));
     const T rdx = (T)d.dx, rdy = (T)d.dy;
     const T rdt = (T)(rho * d.dt), bdt = (T)(beta * d.dt);
     const bool wm_lo = d.wall[SIDE_BO] != 0, wm_hi = d.wall[SIDE_TO] != 0;
     long long cc = bidx(d, i, j, k0);
-    // column windows: theta at k-2..k+2, diffusivity at k-1..k+1, W at k-1
+    // column windows: the scalar at k-2..k+2, diffusivity at k-1..k+1, W at k-1
     T sz[5], kz[3];
 #pragma unroll
     for (int q = 0; q < 5; q++) sz[q] = ld(S, cc + (long long)(q - 2) * plane + zoff(k0 - 2 + q));
@@ -118,7 +132,7 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
       const T sym2 = ld(S, cc + oy[0]), sym1 = ld(S, cc + oy[1]), syp1 = ld(S, cc + oy[3]), syp2 = ld(S, cc + oy[4]);
       const T k0v = kz[1];
       const T kxm = ld(K, cc + ox[1]), kxp = ld(K, cc + ox[3]), kym = ld(K, cc + oy[1]), kyp = ld(K, cc + oy[3]);
-      const T told = stage1 ? (T)0 : ld((const T *)d.Tadv, cc);
+      const T told = stage1 ? (T)0 : ld((const T *)Sadv, cc);
       // advection: the loop order of KappaScalar gives each cell +A f(low
       // face) then -A f(high face) in x and y; in z the even faces come first
       T a = (T)0;
@@ -141,7 +155,12 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
       a = a - (k0v + kym) * (s0 - sym1) * Dy;
       a = a + (kz[2] + k0v) * (sz[3] - s0) * Dz;
       a = a - (k0v + kz[0]) * (s0 - sz[1]) * Dz;
-      // wall-model point next to a wall-model side: + div * theta (the
+      // volume sources (FluxKernel: + flux / volume of the cell)
+      if (srcm) {
+        for (int q = 0; q < d.nsrc; q++)
+          if (((srcm >> q) & 1u) && d.src_k[q] == k) a = a + (T)d.src_q[q];
+      }
+      // wall-model point next to a wall-model side: + div * value (the
       // surface flux is zero); div as DivergenceWM with dzPr(k)
       if ((k == 1 && wm_lo) || (k == nz && wm_hi)) {
         const T dzk = (T)d.dzPr[k + 2];
@@ -154,11 +173,11 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
         div = div - wb / dzk;
         a = a + div * s0;
       }
-      // RK combine of the stage: T2 = Tadv_old * (rho dt) + Tadv * (beta dt)
+      // RK combine of the stage: S2 = Sadv_old * (rho dt) + Sadv * (beta dt)
       T t2 = stage1 ? (T)0 : told * rdt;
       t2 = t2 + a * bdt;
-      d.Tadv[cc] = a;
-      d.Tn[cc] = s0 + t2;
+      Sadv[cc] = a;
+      Snew[cc] = s0 + t2;
       // shift the windows up one plane
       if (k < k1) {
         const long long cn = cc + plane;
@@ -176,9 +195,33 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
   }
 }
 
-// interior of Temperature(-2:n+3) (host, double) -> device box, minus toff
+// Scalar_avg = Scalar_avg + Scalar * time_weight (src/outputs.f90:1043-1045)
+// on the two slice planes of every passive scalar, after the last stage of a
+// step.  Tiles: (slot, row of the slice planes) per domain, rows of the xy
+// plane first; one thread per cell of the row.
 template <typename T>
-__global__ void k_unpack_temperature(const Dom<T> *__restrict__ dom, const double *__restrict__ src, int *bad) {
+__global__ void k_scalar_avg(const Dom<T> *__restrict__ doms, Launch L) {
+  for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
+    const int di = find_dom(L.starts, L.nd, t);
+    const Dom<T> &d = doms[di];
+    int lt = t - __ldg(L.starts + di);
+    const int nx = d.nx, ny = d.ny, nz = d.nz;
+    const int rows = (d.avg_k > 0 ? ny : 0) + (d.avg_j > 0 ? nz : 0);
+    const int s = (d.buoy ? 1 : 0) + lt / rows;  // the passive slots follow the temperature
+    const int r = lt % rows;
+    const ScalSlot<T> &sl = d.slot[s];
+    const bool xy = d.avg_k > 0 && r < ny;
+    const int j = xy ? r + 1 : d.avg_j, k = xy ? d.avg_k : r - (d.avg_k > 0 ? ny : 0) + 1;
+    double *acc = xy ? sl.acc_xy + (size_t)(j - 1) * nx : sl.acc_xz + (size_t)(k - 1) * nx;
+    const T *S = sl.m + bidx(d, 1, j, k);
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) acc[i] = acc[i] + ((double)S[i] + sl.off) * d.avg_w;
+  }
+}
+
+// interior of Temperature(-2:n+3) or Scalar(-2:n+3,sc) (host, double) ->
+// the box of scalar slot s, minus its offset
+template <typename T>
+__global__ void k_unpack_scalar(const Dom<T> *__restrict__ dom, int s, const double *__restrict__ src, int *bad) {
   const Dom<T> &d = *dom;
   const int nx = d.nx, ny = d.ny, nz = d.nz;
   const long long total = (long long)nx * ny * nz;
@@ -189,21 +232,20 @@ __global__ void k_unpack_temperature(const Dom<T> *__restrict__ dom, const doubl
     const int j = (int)(r % ny) + 1, k = (int)(r / ny) + 1;
     const double v = src[(i + 2) + n0 * ((j + 2) + n1 * (k + 2))];
     if (!isfinite(v)) atomicAdd(bad, 1);
-    d.Tm[bidx(d, i, j, k)] = (T)(v - d.toff);
+    d.slot[s].m[bidx(d, i, j, k)] = (T)(v - d.slot[s].off);
   }
 }
 
-// box field F with lower bound lo (-2: Temperature, Temperature_adv; -1:
-// TDiff) -> host array, every ghost folded onto the interior (periodic copy,
-// else the nearest interior cell), plus add.  interior_only: ghosts are 0.
+// box field F with lower bound lo (-2: Temperature, Scalar and their _adv;
+// -1: TDiff) -> host array, every ghost folded onto the interior (periodic
+// copy where per[axis], else the nearest interior cell), plus add.
+// interior_only: ghosts are 0.
 template <typename T>
-__global__ void k_pack_temperature(const Dom<T> *__restrict__ dom, const T *F, double *dst, int lo, double add,
-                                   int interior_only) {
+__global__ void k_pack_scalar_box(const Dom<T> *__restrict__ dom, const T *F, double *dst, int lo, double add,
+                                  int interior_only, int px, int py, int pz) {
   const Dom<T> &d = *dom;
   const int nx = d.nx, ny = d.ny, nz = d.nz;
   const int n0 = nx + 2 * (1 - lo), n1 = ny + 2 * (1 - lo), n2 = nz + 2 * (1 - lo);
-  const bool px = d.tbt[SIDE_WE] == BC_PERIODIC, py = d.tbt[SIDE_SO] == BC_PERIODIC,
-             pz = d.tbt[SIDE_BO] == BC_PERIODIC;
   const long long total = (long long)n0 * n1 * n2;
   for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < total; w += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(w % n0) + lo;

@@ -11,7 +11,8 @@ import os
 
 import numpy as np
 
-from .config import ElmmConfig, ElmmStats, Grid, STATUS_NAMES, grid_of
+from .config import (FIELD_SCALAR, FIELD_SCALAR_ADV, MAX_SCALARS, ElmmConfig, ElmmStats, Grid, STATUS_NAMES,
+                     grid_of)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libelmm_gpu.so")
@@ -47,6 +48,9 @@ def lib():
         L.elmm_upload_state.argtypes = [P, _dp, _dp, _dp, _dp]
         L.elmm_download_state.argtypes = [P, _dp, _dp, _dp, _dp]
         L.elmm_upload_temperature.argtypes = [P, _dp]
+        L.elmm_upload_scalar.argtypes = [P, C.c_int32, _dp]
+        L.elmm_download_scalar_slices.argtypes = [P, C.c_int32, _dp, _dp]
+        L.elmm_reset_scalar_averages.argtypes = [P]
         L.elmm_download_field.argtypes = [P, C.c_int32, _dp]
         L.elmm_frame_begin.argtypes = [P]
         L.elmm_frame_wait.argtypes = [P, _dp, _dp, _dp, _dp]
@@ -64,6 +68,9 @@ def lib():
         L.elmm_batch_destroy.argtypes = [P]
         L.elmm_batch_upload_state.argtypes = [P, C.c_int32, _dp, _dp, _dp, _dp]
         L.elmm_batch_download_state.argtypes = [P, C.c_int32, _dp, _dp, _dp, _dp]
+        L.elmm_batch_upload_scalar.argtypes = [P, C.c_int32, C.c_int32, _dp]
+        L.elmm_batch_download_field.argtypes = [P, C.c_int32, C.c_int32, _dp]
+        L.elmm_batch_download_scalar_slices.argtypes = [P, C.c_int32, C.c_int32, _dp, _dp]
         L.elmm_batch_project.argtypes = [P, C.c_double]
         L.elmm_batch_step.argtypes = [P, C.c_int32, C.POINTER(ElmmStats)]
         L.elmm_batch_cells.argtypes = [P]
@@ -114,6 +121,8 @@ class Domain:
         g = self.grid
         shape = {0: g.shape_u(), 5: g.shape_u(), 8: g.shape_u(), 1: g.shape_v(), 6: g.shape_v(), 9: g.shape_v(),
                  2: g.shape_w(), 7: g.shape_w(), 10: g.shape_w(), 12: g.shape_t(), 14: g.shape_t()}.get(fid, g.shape_p())
+        if FIELD_SCALAR <= fid < FIELD_SCALAR_ADV + MAX_SCALARS:
+            shape = g.shape_t()
         a = np.zeros(shape) if out is None else out
         check(lib().elmm_download_field(self.h, fid, ptr(a)), "elmm_download_field")
         return a
@@ -124,6 +133,25 @@ class Domain:
 
     def temperature(self):
         return self.field(12)
+
+    def upload_scalar(self, sc, S):
+        """Scalar(-2:nx+3,-2:ny+3,-2:nz+3,sc), host array, sc in 1..num_scalars."""
+        check(lib().elmm_upload_scalar(self.h, sc, ptr(S)), "elmm_upload_scalar")
+
+    def scalar(self, sc):
+        return self.field(FIELD_SCALAR + sc - 1)
+
+    def scalar_slices(self, sc):
+        """Time-averaged slices of scalar sc: xy (Prny, Prnx) at avg_slice_k and
+        xz (Prnz, Prnx) at avg_slice_j (None where the slice is off)."""
+        g = self.grid
+        xy = np.zeros((g.Prny, g.Prnx)) if self.cfg.avg_slice_k > 0 else None
+        xz = np.zeros((g.Prnz, g.Prnx)) if self.cfg.avg_slice_j > 0 else None
+        check(lib().elmm_download_scalar_slices(self.h, sc, ptr(xy), ptr(xz)), "elmm_download_scalar_slices")
+        return xy, xz
+
+    def reset_scalar_averages(self):
+        check(lib().elmm_reset_scalar_averages(self.h), "elmm_reset_scalar_averages")
 
     def project(self, coef=1.0) -> ElmmStats:
         st = ElmmStats()
@@ -185,6 +213,22 @@ class Batch:
         check(lib().elmm_batch_download_state(self.h, d, ptr(U), ptr(V), ptr(W), ptr(Pr)),
               "elmm_batch_download_state")
         return U, V, W, Pr
+
+    def upload_scalar(self, d, sc, S):
+        check(lib().elmm_batch_upload_scalar(self.h, d, sc, ptr(S)), "elmm_batch_upload_scalar")
+
+    def scalar(self, d, sc):
+        a = np.zeros(self.grids[d].shape_t())
+        check(lib().elmm_batch_download_field(self.h, d, FIELD_SCALAR + sc - 1, ptr(a)), "elmm_batch_download_field")
+        return a
+
+    def scalar_slices(self, d, sc):
+        g, c = self.grids[d], self.cfgs[d]
+        xy = np.zeros((g.Prny, g.Prnx)) if c.avg_slice_k > 0 else None
+        xz = np.zeros((g.Prnz, g.Prnx)) if c.avg_slice_j > 0 else None
+        check(lib().elmm_batch_download_scalar_slices(self.h, d, sc, ptr(xy), ptr(xz)),
+              "elmm_batch_download_scalar_slices")
+        return xy, xz
 
     def project(self, coef=1.0):
         check(lib().elmm_batch_project(self.h, coef), "elmm_batch_project")

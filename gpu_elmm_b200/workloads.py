@@ -34,7 +34,7 @@ def splitmix64(x: np.ndarray) -> np.ndarray:
     return z
 
 
-FIELD_KEYS = {"u": 1, "v": 2, "w": 3, "theta": 4, "ustar": 5, "sizes": 6}
+FIELD_KEYS = {"u": 1, "v": 2, "w": 3, "theta": 4, "ustar": 5, "sizes": 6, "requests": 7, "arrivals": 8}
 
 
 def uniform(seed: int, field: str, n: int) -> np.ndarray:
@@ -91,6 +91,56 @@ def temperature_state(grid: Grid, *, seed=0, t0=295.0, gradient=0.01, amp=0.05, 
         amp * (2.0 * r - 1.0)
     T[...] = T.astype(np.float32).astype(np.float64)
     return T
+
+
+def puff_state(grid: Grid, center, *, sigma=2.0, amp=1.0):
+    """A Gaussian puff of passive scalar, amp exp(-r^2 / (2 sigma^2)) with r
+    the distance in cells from the centre cell (i, j, k), the shortest
+    periodic distance along x and y; rounded to FP32.  Returns the host array
+    Scalar(-2:nx+3,-2:ny+3,-2:nz+3) with zero ghosts."""
+    g = grid
+    S = np.zeros(g.shape_t())
+    ci, cj, ck = center
+
+    def dist(idx, c, n, periodic):
+        d = np.abs(idx - c).astype(np.float64)
+        return np.minimum(d, n - d) if periodic else d
+
+    di = dist(np.arange(1, g.Prnx + 1), ci, g.Prnx, True)
+    dj = dist(np.arange(1, g.Prny + 1), cj, g.Prny, True)
+    dk = dist(np.arange(1, g.Prnz + 1), ck, g.Prnz, False)
+    r2 = dk[:, None, None] ** 2 + dj[None, :, None] ** 2 + di[None, None, :] ** 2
+    interior(S, -2, (g.Prnx, g.Prny, g.Prnz))[...] = amp * np.exp(-r2 / (2.0 * sigma * sigma))
+    S[...] = S.astype(np.float32).astype(np.float64)
+    return S
+
+
+# dispersion requests of the serving workload: horizontal sides and depths
+REQUEST_SIDES = (64, 96, 128, 192)
+REQUEST_DEPTHS = (64, 96)
+
+
+def dispersion_request(seed: int, index: int, *, min_steps=200, max_steps=2000):
+    """Request `index` of stream `seed`: a channel of s x s x nz cells
+    (s from REQUEST_SIDES, nz from REQUEST_DEPTHS, so 64^3 .. 192x192x96),
+    min_steps..max_steps steps, and the interior cell (i, j, k) of its
+    continuous point source, which is also the centre of the initial puff
+    (k in 2..nz-1, away from the walls).  Returns a dict."""
+    r = uniform(seed, "requests", 8 * (index + 1))[8 * index:8 * index + 8]
+    s = REQUEST_SIDES[int(r[0] * len(REQUEST_SIDES))]
+    nz = REQUEST_DEPTHS[int(r[1] * len(REQUEST_DEPTHS))]
+    steps = min_steps + int(r[2] * (max_steps - min_steps + 1))
+    i = 1 + int(r[3] * s)
+    j = 1 + int(r[4] * s)
+    k = 2 + int(r[5] * (nz - 2))
+    return {"n": (s, s, nz), "steps": steps, "source": (i, j, k), "seed": seed * 1000003 + index}
+
+
+def poisson_arrivals(seed: int, rate: float, count: int) -> np.ndarray:
+    """Arrival times (s) of a Poisson process of the given rate: cumulative
+    exponential gaps -ln(1 - U) / rate."""
+    u = uniform(seed, "arrivals", count)
+    return np.cumsum(-np.log1p(-u) / rate)
 
 
 def interior(a: np.ndarray, lo: int, n: tuple) -> np.ndarray:

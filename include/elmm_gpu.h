@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define ELMM_ABI_VERSION 2
+#define ELMM_ABI_VERSION 3
 
 /* Status codes. */
 enum {
@@ -80,8 +80,26 @@ enum {
   ELMM_FIELD_PHI = 11,
   ELMM_FIELD_TEMPERATURE = 12,   /* Temperature(-2:Prnx+3,-2:Prny+3,-2:Prnz+3) */
   ELMM_FIELD_TDIFF = 13,         /* TDiff(-1:Prnx+2,...), turbulent + molecular diffusivity */
-  ELMM_FIELD_TEMPERATURE_ADV = 14 /* Temperature_adv(-2:...), the stage tendency */
+  ELMM_FIELD_TEMPERATURE_ADV = 14, /* Temperature_adv(-2:...), the stage tendency */
+  ELMM_FIELD_SCALAR = 16,        /* + (sc - 1): Scalar(-2:Prnx+3,-2:Prny+3,-2:Prnz+3,sc) */
+  ELMM_FIELD_SCALAR_ADV = 20     /* + (sc - 1): Scalar_adv(-2:...,sc), the stage tendency */
 };
+
+/* Passive scalars and their point sources (src/scalars.f90:88-381,
+ * src/pointsources.f90:1-68). */
+#define ELMM_MAX_SCALARS 4
+#define ELMM_MAX_POINT_SOURCES 8
+
+/* ScalarPointSource (src/pointsources.f90:8-13): a continuous source of
+ * `flux` units per time unit at `position`, released into the single grid
+ * cell that contains it (GridCoords, src/boundaries.f90:54-97) as a volume
+ * source flux / volumePr of that cell. */
+typedef struct elmm_point_source {
+  int32_t scalar_number;        /* 1..num_scalars */
+  int32_t reserved;             /* 0 */
+  double position[3];           /* x, y, z */
+  double flux;                  /* total flux, units per time unit */
+} elmm_point_source;
 
 /*
  * Configuration of one domain.  It carries the module globals of
@@ -120,6 +138,25 @@ typedef struct elmm_config {
   double temperature_ref;       /* src/parameters.f90:220 (295 K) */
   double grav_acc;              /* src/parameters.f90:146 (9.81) */
   double molecular_diffusivity; /* molecular_viscosity / Prandtl (src/initial.f90:791; Prandtl 0.7) */
+  /* Passive scalars (ScalarRK3's loop over num_of_scalars, src/scalars.f90:217-223):
+   * the same KappaScalar advection, scalar diffusion with TDiff and wall-model
+   * term as the temperature, plus point sources.  Without buoyancy TDiff is
+   * set once by the initial projection and then kept, as in the reference
+   * (src/initial.f90:4296-4313; src/dynamics.f90:904 updates it only with
+   * buoyancy).  Supported ScalBtype: as TempBtype. */
+  int32_t num_scalars;          /* 0..ELMM_MAX_SCALARS */
+  int32_t ScalBtype[6];         /* scalar BC per side (src/initial.f90:508-519) */
+  double sideScal[6];           /* BC values: the flux for ELMM_BC_CONSTFLUX */
+  int32_t num_point_sources;    /* 0..ELMM_MAX_POINT_SOURCES */
+  int32_t reserved0;            /* 0 */
+  elmm_point_source point_sources[ELMM_MAX_POINT_SOURCES];
+  /* Time-averaged scalar slices (Scalar_avg of src/outputs.f90:1043-1045,
+   * restricted to two planes): after every step avg += Scalar * avg_weight,
+   * with avg_weight = dt / (timeavg2 - timeavg1) for an averaging window
+   * that spans the run.  In FP64 on both precision paths. */
+  int32_t avg_slice_k;          /* horizontal plane k = 1..Prnz, 0: none */
+  int32_t avg_slice_j;          /* vertical x-z plane j = 1..Prny, 0: none */
+  double avg_weight;
 } elmm_config;
 
 /* Diagnostics of elmm_step / elmm_project. */
@@ -168,6 +205,17 @@ int elmm_download_field(elmm_handle *h, int32_t field, double *host);
  * interior values.  The state is read back with elmm_download_field
  * (ELMM_FIELD_TEMPERATURE). */
 int elmm_upload_temperature(elmm_handle *h, const double *T);
+
+/* Host -> device copy of passive scalar sc (1..num_scalars) from
+ * Scalar(-2:Prnx+3,-2:Prny+3,-2:Prnz+3,sc) (only the interior is read).
+ * Returns ELMM_ERR_NAN for non-finite values. */
+int elmm_upload_scalar(elmm_handle *h, int32_t sc, const double *S);
+
+/* The time-averaged slices of scalar sc: xy(1:Prnx,1:Prny) at avg_slice_k and
+ * xz(1:Prnx,1:Prnz) at avg_slice_j, column-major; either pointer may be NULL.
+ * elmm_reset_scalar_averages zeroes both accumulators of every scalar. */
+int elmm_download_scalar_slices(elmm_handle *h, int32_t sc, double *xy, double *xz);
+int elmm_reset_scalar_averages(elmm_handle *h);
 
 /* Asynchronous frame: copies U, V, W, Pr on a side stream into pinned staging
  * buffers owned by the handle and returns at once.  elmm_frame_wait blocks
@@ -269,6 +317,9 @@ int elmm_batch_upload_state(elmm_batch *b, int32_t d, const double *U, const dou
                             const double *W, const double *Pr);
 int elmm_batch_download_state(elmm_batch *b, int32_t d, double *U, double *V, double *W,
                               double *Pr);
+int elmm_batch_upload_scalar(elmm_batch *b, int32_t d, int32_t sc, const double *S);
+int elmm_batch_download_field(elmm_batch *b, int32_t d, int32_t field, double *host);
+int elmm_batch_download_scalar_slices(elmm_batch *b, int32_t d, int32_t sc, double *xy, double *xz);
 int elmm_batch_project(elmm_batch *b, double coef);
 int elmm_batch_step(elmm_batch *b, int32_t nsteps, elmm_stats *stats);
 /* total interior cells of the batch (for cell-steps/s) */

@@ -166,6 +166,19 @@ struct Domain {
   double sideTemp[7];
   double temperature_ref, grav_acc, molecular_diffusivity;
   A3 T, Tadv, T2, TDiff;
+  // passive scalars (ScalarRK3's loop over num_of_scalars, scalars.f90:217-223)
+  int num_scalars;
+  int ScalBtype[7];
+  double sideScal[7];
+  A3 S[ELMM_MAX_SCALARS], Sadv[ELMM_MAX_SCALARS], S2[ELMM_MAX_SCALARS];
+  // ScalFlVolumes from the point sources (pointsources.f90:24-39), in the
+  // order they were added: scalar, cell, flux / volumePr
+  struct FlVolume { int sc, i, j, k; double flux; };
+  std::vector<FlVolume> flvolumes;
+  // time-averaged slices of Scalar_avg (outputs.f90:1043-1045)
+  int avg_k, avg_j;
+  double avg_w;
+  std::vector<double> acc_xy[ELMM_MAX_SCALARS], acc_xz[ELMM_MAX_SCALARS];
 };
 
 // ------------------------------------------------- grid, initial.f90:4395-4480
@@ -652,10 +665,8 @@ static void SubgridStresses(Domain &d) {
   SubgridModel(d);
   if (d.wallmodeltype > 0) ComputeUVWFluxesWM(d);
   BoundViscosity(d, d.Viscosity);
-  if (d.enable_buoyancy) {  // dynamics.f90:904-906
-    ComputeTDiff(d);
-    BoundViscosity(d, d.TDiff);
-  }
+  if (d.enable_buoyancy) ComputeTDiff(d);  // dynamics.f90:904
+  if (d.enable_buoyancy || d.num_scalars > 0) BoundViscosity(d, d.TDiff);  // dynamics.f90:906
 }
 
 // BuoyancyForce, FD2 branch of dynamics.f90:679-688
@@ -670,10 +681,8 @@ static void BuoyancyForce(Domain &d, A3 &Wst) {
 // BoundTemperature -> CommonBase, scalarboundaries.f90:12-300, for periodic
 // and constant-flux sides (the x, y loops run over the ranges of the
 // reference, corners included where it includes them)
-static void BoundTemperature(Domain &d, A3 &a) {
+static void CommonBase(Domain &d, A3 &a, const int *bt, const double *side) {
   const int nx = d.Prnx, ny = d.Prny, nz = d.Prnz;
-  const int *bt = d.TempBtype;
-  const double *side = d.sideTemp;
   for (int k = 1; k <= nz; k++)
     for (int j = 1; j <= ny; j++) {
       if (bt[We] == BC_PERIODIC) {
@@ -726,6 +735,10 @@ static void BoundTemperature(Domain &d, A3 &a) {
       }
     }
 }
+
+static void BoundTemperature(Domain &d, A3 &a) { CommonBase(d, a, d.TempBtype, d.sideTemp); }
+// BoundScalar, scalarboundaries.f90:284-289
+static void BoundScalar(Domain &d, A3 &a) { CommonBase(d, a, d.ScalBtype, d.sideScal); }
 
 // FluxLimiter of KappaScalar, scalar_advection.f90:262-270
 static inline double kappa_limiter(double r) { return std::max(0.0, std::min(2 * r, std::min(2.0, (1 + 2 * r) / 3))); }
@@ -800,13 +813,16 @@ static void ScalarDiffusion(Domain &d, A3 &S2, const A3 &S) {
       }
 }
 
-// one stage of ScalarRK3 for the temperature (scalars.f90:88-299): the
-// scalar wall-model points are the cells next to a wall-model side
-// (DivergenceWM, wallmodels.f90:1150-1166; TemperatureExtra with a zero
-// surface flux, scalars.f90:301-334)
-static void TemperatureStage(Domain &d, int stage, double dt) {
+// stage() of ScalarRK3 (scalars.f90:233-299) for one field: the temperature
+// (sc = 0) or passive scalar sc.  The scalar wall-model points are the cells
+// next to a wall-model side (DivergenceWM, wallmodels.f90:1150-1166, with the
+// velocity at the start of the stage); TemperatureExtra adds a zero surface
+// flux and div * T there (scalars.f90:301-334), ScalarExtra first the volume
+// sources of the scalar (ScalarVolumeSources -> FluxKernel,
+// volumesources.f90:741-771) and then div * S (scalars.f90:364-379).
+static void ScalarStage(Domain &d, int stage, double dt, A3 &Arr, A3 &Arr2, A3 &Adv, int sc) {
   const int nx = d.Prnx, ny = d.Prny, nz = d.Prnz;
-  // DivergenceWM with the velocity at the start of the stage
+  auto bound = [&](A3 &a) { if (sc == 0) BoundTemperature(d, a); else BoundScalar(d, a); };
   std::vector<double> divb((size_t)nx * ny, 0.0), divt((size_t)nx * ny, 0.0);
   const bool wb = d.wallmodeltype > 0 && d.Btype[Bo] == BC_NOSLIP, wt = d.wallmodeltype > 0 && d.Btype[To] == BC_NOSLIP;
   auto wmdiv = [&](int i, int j, int k) {
@@ -824,23 +840,54 @@ static void TemperatureStage(Domain &d, int stage, double dt) {
       if (wb) divb[(size_t)(j - 1) * nx + i - 1] = wmdiv(i, j, 1);
       if (wt) divt[(size_t)(j - 1) * nx + i - 1] = wmdiv(i, j, nz);
     }
-  BoundTemperature(d, d.T);
+  bound(Arr);
   const double rdt = RK_rho[stage - 1] * dt, bdt = RK_beta[stage - 1] * dt;
   if (stage > 1) {
-    for (size_t q = 0; q < d.T2.v.size(); q++) d.T2.v[q] = d.Tadv.v[q] * rdt;
+    for (size_t q = 0; q < Arr2.v.size(); q++) Arr2.v[q] = Adv.v[q] * rdt;
   } else {
-    d.T2.fill(0);
+    Arr2.fill(0);
   }
-  KappaScalar(d, d.Tadv, d.T);
-  ScalarDiffusion(d, d.Tadv, d.T);
+  KappaScalar(d, Adv, Arr);
+  ScalarDiffusion(d, Adv, Arr);
+  if (sc > 0)
+    for (const auto &v : d.flvolumes)
+      if (v.sc == sc) Adv(v.i, v.j, v.k) = Adv(v.i, v.j, v.k) + v.flux;
   for (int j = 1; j <= ny; j++)
     for (int i = 1; i <= nx; i++) {
-      if (wb) d.Tadv(i, j, 1) = d.Tadv(i, j, 1) + divb[(size_t)(j - 1) * nx + i - 1] * d.T(i, j, 1);
-      if (wt) d.Tadv(i, j, nz) = d.Tadv(i, j, nz) + divt[(size_t)(j - 1) * nx + i - 1] * d.T(i, j, nz);
+      if (wb) Adv(i, j, 1) = Adv(i, j, 1) + divb[(size_t)(j - 1) * nx + i - 1] * Arr(i, j, 1);
+      if (wt) Adv(i, j, nz) = Adv(i, j, nz) + divt[(size_t)(j - 1) * nx + i - 1] * Arr(i, j, nz);
     }
-  for (size_t q = 0; q < d.T2.v.size(); q++) d.T2.v[q] = d.T2.v[q] + d.Tadv.v[q] * bdt;
-  for (size_t q = 0; q < d.T.v.size(); q++) d.T.v[q] = d.T.v[q] + d.T2.v[q];
-  BoundTemperature(d, d.T);
+  for (size_t q = 0; q < Arr2.v.size(); q++) Arr2.v[q] = Arr2.v[q] + Adv.v[q] * bdt;
+  for (size_t q = 0; q < Arr.v.size(); q++) Arr.v[q] = Arr.v[q] + Arr2.v[q];
+  bound(Arr);
+}
+
+// ScalarRK3 (scalars.f90:88-381): the temperature, then each passive scalar
+static void ScalarRK3(Domain &d, int stage, double dt) {
+  if (d.enable_buoyancy) ScalarStage(d, stage, dt, d.T, d.T2, d.Tadv, 0);
+  for (int sc = 1; sc <= d.num_scalars; sc++)
+    ScalarStage(d, stage, dt, d.S[sc - 1], d.S2[sc - 1], d.Sadv[sc - 1], sc);
+}
+
+// Scalar_avg = Scalar_avg + Scalar * time_weight (outputs.f90:1043-1045) on
+// the two slice planes
+static void AccumulateScalarAverages(Domain &d) {
+  const int nx = d.Prnx, ny = d.Prny, nz = d.Prnz;
+  for (int sc = 0; sc < d.num_scalars; sc++) {
+    const A3 &S = d.S[sc];
+    if (d.avg_k > 0)
+      for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++) {
+          double &a = d.acc_xy[sc][(size_t)(j - 1) * nx + i - 1];
+          a = a + S(i, j, d.avg_k) * d.avg_w;
+        }
+    if (d.avg_j > 0)
+      for (int k = 1; k <= nz; k++)
+        for (int i = 1; i <= nx; i++) {
+          double &a = d.acc_xz[sc][(size_t)(k - 1) * nx + i - 1];
+          a = a + S(i, d.avg_j, k) * d.avg_w;
+        }
+  }
 }
 
 // ---------------------------------------------- CDS2 advection, advection.f90:15-327
@@ -1546,7 +1593,7 @@ static void run_stage(Domain &d, int stage, int stop) {
   SubgridStresses(d);
   if (stop == 1) return;
   Convection(d, stage, dt);
-  if (d.enable_buoyancy) TemperatureStage(d, stage, dt);  // ScalarRK3, tsteps.f90:132-135
+  if (d.enable_buoyancy || d.num_scalars > 0) ScalarRK3(d, stage, dt);  // tsteps.f90:132-135
   OtherTerms(d, 2 * RK_alpha[stage - 1] * dt);
   BoundUVW(d, d.U2, d.V2, d.W2);
   if (stop == 2) return;
@@ -1562,6 +1609,43 @@ static void TMarchRK3(Domain &d) {
   TimeStepLength(d);
   for (int s = 1; s <= 3; s++) run_stage(d, s, 3);
   d.time += d.dt;
+  AccumulateScalarAverages(d);
+}
+
+// InDomain (boundaries.f90:163-168) and GridCoords_scalar
+// (boundaries.f90:54-97): the cell of a point; nint rounds half away from 0
+static bool GridCoords(const Domain &d, const double *r, int *ip) {
+  const int nx = d.Prnx, ny = d.Prny, nz = d.Prnz;
+  if (!((r[0] >= d.xU(0) && r[0] <= d.xU(nx)) && (r[1] >= d.yV(0) && r[1] <= d.yV(ny)) &&
+        (r[2] >= d.zW(0) && r[2] <= d.zW(nz))))
+    return false;
+  if (d.gridtype == 0) {
+    ip[0] = std::min(std::max((int)std::lround((r[0] - d.xU(0)) / d.dxmin + 0.5), 1), nx);
+    ip[1] = std::min(std::max((int)std::lround((r[1] - d.yV(0)) / d.dymin + 0.5), 1), ny);
+    ip[2] = std::min(std::max((int)std::lround((r[2] - d.zW(0)) / d.dzmin + 0.5), 1), nz);
+  } else {
+    ip[0] = nx; ip[1] = ny; ip[2] = nz;
+    for (int i = 1; i <= nx; i++) if (d.xU(i) >= r[0]) { ip[0] = i; break; }
+    for (int j = 1; j <= ny; j++) if (d.yV(j) >= r[1]) { ip[1] = j; break; }
+    for (int k = 1; k <= nz; k++) if (d.zW(k) >= r[2]) { ip[2] = k; break; }
+  }
+  return true;
+}
+
+// the end of InitialConditions after the projection (initial.f90:4290-4320):
+// eddy viscosity, its ghosts and, with any scalar, the diffusivity
+static void InitialDiffusivity(Domain &d) {
+  SubgridModel(d);
+  BoundViscosity(d, d.Viscosity);
+  if (d.enable_buoyancy || d.num_scalars > 0) {
+    const double Pr_sgs = 0.6;  // constPr_sgs, scalar_diffusion.f90:22
+    for (int k = 1; k <= d.Prnz; k++)
+      for (int j = 1; j <= d.Prny; j++)
+        for (int i = 1; i <= d.Prnx; i++)
+          d.TDiff(i, j, k) = (d.Viscosity(i, j, k) - d.molecular_viscosity) / Pr_sgs + d.molecular_diffusivity;
+    BoundViscosity(d, d.TDiff);
+  }
+  if (d.enable_buoyancy) BoundTemperature(d, d.T);
 }
 
 }  // namespace orc
@@ -1616,10 +1700,36 @@ void *orc_create(const elmm_config *c) {
   d->temperature_ref = c->temperature_ref;
   d->grav_acc = c->grav_acc;
   d->molecular_diffusivity = c->molecular_diffusivity;
+  if (c->num_scalars < 0 || c->num_scalars > ELMM_MAX_SCALARS) { delete d; return nullptr; }
+  d->num_scalars = c->num_scalars;
+  for (int s = 0; s < 6; s++) { d->ScalBtype[s + 1] = c->ScalBtype[s]; d->sideScal[s + 1] = c->sideScal[s]; }
   if (d->enable_buoyancy) {
     for (A3 *a : {&d->T, &d->Tadv, &d->T2}) a->init(-2, nx + 3, -2, ny + 3, -2, nz + 3);
+  }
+  for (int sc = 0; sc < d->num_scalars; sc++)
+    for (A3 *a : {&d->S[sc], &d->Sadv[sc], &d->S2[sc]}) a->init(-2, nx + 3, -2, ny + 3, -2, nz + 3);
+  if (d->enable_buoyancy || d->num_scalars > 0) {
     d->TDiff.init(-1, nx + 2, -1, ny + 2, -1, nz + 2);
-    d->TDiff.fill(d->molecular_diffusivity);  // initial.f90:4266
+    if (d->molecular_viscosity > 0) d->TDiff.fill(d->molecular_diffusivity);  // initial.f90:4262-4268
+  }
+  // point sources -> single-cell volume sources (pointsources.f90:24-39,
+  // InitPointSources :41-60)
+  if (c->num_point_sources < 0 || c->num_point_sources > ELMM_MAX_POINT_SOURCES) { delete d; return nullptr; }
+  for (int q = 0; q < c->num_point_sources; q++) {
+    const elmm_point_source &ps = c->point_sources[q];
+    if (ps.scalar_number < 1 || ps.scalar_number > d->num_scalars) { delete d; return nullptr; }
+    int ip[3];
+    if (!GridCoords(*d, ps.position, ip)) continue;
+    const double vol = d->dxPr(ip[0]) * d->dyPr(ip[1]) * d->dzPr(ip[2]);
+    d->flvolumes.push_back({ps.scalar_number, ip[0], ip[1], ip[2], ps.flux / vol});
+  }
+  d->avg_k = c->avg_slice_k;
+  d->avg_j = c->avg_slice_j;
+  d->avg_w = c->avg_weight;
+  if (d->avg_k < 0 || d->avg_k > nz || d->avg_j < 0 || d->avg_j > ny) { delete d; return nullptr; }
+  for (int sc = 0; sc < d->num_scalars; sc++) {
+    d->acc_xy[sc].assign((size_t)nx * ny, 0.0);
+    d->acc_xz[sc].assign((size_t)nx * nz, 0.0);
   }
   if (d->wallmodeltype > 0) add_wm_points(*d);
   if (!init_poisson(*d)) { delete d; return nullptr; }
@@ -1650,10 +1760,21 @@ static A3 *field_of(Domain *d, int f) {
     case ELMM_FIELD_WSTAR: return &d->Wstar;
     case ELMM_FIELD_PHI: return &d->Phi;
     case ELMM_FIELD_TEMPERATURE: return d->enable_buoyancy ? &d->T : nullptr;
-    case ELMM_FIELD_TDIFF: return d->enable_buoyancy ? &d->TDiff : nullptr;
+    case ELMM_FIELD_TDIFF: return d->enable_buoyancy || d->num_scalars > 0 ? &d->TDiff : nullptr;
     case ELMM_FIELD_TEMPERATURE_ADV: return d->enable_buoyancy ? &d->Tadv : nullptr;
   }
+  if (f >= ELMM_FIELD_SCALAR && f < ELMM_FIELD_SCALAR + d->num_scalars) return &d->S[f - ELMM_FIELD_SCALAR];
+  if (f >= ELMM_FIELD_SCALAR_ADV && f < ELMM_FIELD_SCALAR_ADV + d->num_scalars) return &d->Sadv[f - ELMM_FIELD_SCALAR_ADV];
   return nullptr;
+}
+
+// the time-averaged slices of scalar sc (1-based): xy (ny, nx), xz (nz, nx)
+int orc_scalar_slices(void *h, int sc, double *xy, double *xz) {
+  Domain *d = (Domain *)h;
+  if (sc < 1 || sc > d->num_scalars) return ELMM_ERR_INVALID_ARG;
+  if (xy) std::memcpy(xy, d->acc_xy[sc - 1].data(), d->acc_xy[sc - 1].size() * sizeof(double));
+  if (xz) std::memcpy(xz, d->acc_xz[sc - 1].data(), d->acc_xz[sc - 1].size() * sizeof(double));
+  return 0;
 }
 
 int orc_set_field(void *h, int f, const double *src) {
@@ -1675,6 +1796,8 @@ int orc_project(void *h, double coef, double *max_div) {
   std::swap(d->U.v, d->U2.v); std::swap(d->V.v, d->V2.v); std::swap(d->W.v, d->W2.v);
   PressureCorrection(*d, coef, true);
   std::swap(d->U.v, d->U2.v); std::swap(d->V.v, d->V2.v); std::swap(d->W.v, d->W2.v);
+  BoundUVW(*d, d->U, d->V, d->W);
+  InitialDiffusivity(*d);
   if (max_div) *max_div = d->max_div;
   return 0;
 }

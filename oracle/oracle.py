@@ -46,6 +46,7 @@ def lib():
         L.orc_bound_uvw.argtypes = [P]
         L.orc_num_threads.argtypes = [C.c_int]
         L.orc_num_threads.restype = C.c_int
+        L.orc_scalar_slices.argtypes = [P, C.c_int, dp, dp]
         _lib = L
     return _lib
 
@@ -85,7 +86,7 @@ class Oracle:
             return (Vnz + 6, Vny + 6, Vnx + 6)
         if field in (2, 7, 10):
             return (Wnz + 6, Wny + 6, Wnx + 6)
-        if field in (12, 14):  # Temperature, Temperature_adv: (-2:n+3)
+        if field in (12, 14) or 16 <= field < 24:  # Temperature, Scalar, their _adv: (-2:n+3)
             return (Prnz + 6, Prny + 6, Prnx + 6)
         return (Prnz + 4, Prny + 4, Prnx + 4)
 
@@ -131,6 +132,13 @@ class Oracle:
         Phi = np.zeros((Prnz + 4, Prny + 4, Prnx + 4))
         lib().orc_poisson(self.h, _ptr(RHS), _ptr(Phi))
         return Phi
+
+    def scalar_slices(self, sc):
+        """Time-averaged slices of scalar sc: xy (Prny, Prnx), xz (Prnz, Prnx)."""
+        Prnx, Prny, Prnz = self.sizes[:3]
+        xy, xz = np.zeros((Prny, Prnx)), np.zeros((Prnz, Prnx))
+        assert lib().orc_scalar_slices(self.h, sc, _ptr(xy), _ptr(xz)) == 0
+        return xy, xz
 
     def bound(self):
         lib().orc_bound_uvw(self.h)

@@ -44,7 +44,11 @@ int main(void) {
   printf("elmm_stats.size %zu\n", sizeof(elmm_stats));
   O(elmm_config, Btype) O(elmm_config, xmin) O(elmm_config, zW) O(elmm_config, dt)
   O(elmm_config, sgstype) O(elmm_config, z0) O(elmm_config, pr_gradient_x) O(elmm_config, precision)
-  O(elmm_config, refine_tol) O(elmm_config, device)
+  O(elmm_config, refine_tol) O(elmm_config, device) O(elmm_config, TempBtype) O(elmm_config, molecular_diffusivity)
+  O(elmm_config, num_scalars) O(elmm_config, ScalBtype) O(elmm_config, sideScal) O(elmm_config, num_point_sources)
+  O(elmm_config, point_sources) O(elmm_config, avg_slice_k) O(elmm_config, avg_slice_j) O(elmm_config, avg_weight)
+  O(elmm_point_source, position) O(elmm_point_source, flux)
+  printf("elmm_point_source.size %zu\n", sizeof(elmm_point_source));
   O(elmm_stats, time) O(elmm_stats, max_div) O(elmm_stats, refine_sweeps) O(elmm_stats, elapsed_ms)
   return 0;
 }
@@ -62,11 +66,13 @@ def test_ctypes_layout_matches_c():
     lay = _c_layout()
     assert lay["elmm_config.size"] == C.sizeof(cfgmod.ElmmConfig)
     assert lay["elmm_stats.size"] == C.sizeof(cfgmod.ElmmStats)
+    assert lay["elmm_point_source.size"] == C.sizeof(cfgmod.ElmmPointSource)
     for key, off in lay.items():
         s, f = key.split(".")
         if f == "size":
             continue
-        cls = cfgmod.ElmmConfig if s == "elmm_config" else cfgmod.ElmmStats
+        cls = {"elmm_config": cfgmod.ElmmConfig, "elmm_stats": cfgmod.ElmmStats,
+               "elmm_point_source": cfgmod.ElmmPointSource}[s]
         assert getattr(cls, f).offset == off, key
 
 
@@ -86,6 +92,16 @@ def test_config_defaults_and_errors_without_gpu():
     assert lib.elmm_create(C.byref(bad), C.byref(h)) == 1
     bad = cfgmod.make_config(64, 64, 32)
     bad.abi_version = 99
+    assert lib.elmm_create(C.byref(bad), C.byref(h)) == 1
+    bad = cfgmod.make_config(64, 64, 32, num_scalars=1, point_sources=[(2, (1.0, 1.0, 1.0), 1.0)])
+    assert lib.elmm_create(C.byref(bad), C.byref(h)) == 1
+    assert b"scalar_number" in lib.elmm_last_error()
+    bad = cfgmod.make_config(64, 64, 32, num_scalars=5)
+    assert lib.elmm_create(C.byref(bad), C.byref(h)) == 1
+    bad = cfgmod.make_config(64, 64, 32, num_scalars=1, avg_slice_k=33)
+    assert lib.elmm_create(C.byref(bad), C.byref(h)) == 1
+    bad = cfgmod.make_config(64, 64, 32, num_scalars=1)
+    bad.sideScal[4] = 1.0  # a non-zero wall flux is not supported
     assert lib.elmm_create(C.byref(bad), C.byref(h)) == 1
     assert lib.elmm_create(None, C.byref(h)) == 6
     assert lib.elmm_step(None, 1, None) == 6

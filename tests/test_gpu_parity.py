@@ -390,3 +390,135 @@ def test_mixed_buoyant_channel_one_step():
     assert rel(Tm, T64) < 1e-5, rel(Tm, T64)
     d64.close()
     dm.close()
+
+
+def _dispersion_cfg(n, src, *, precision=0, steps=1, buoyancy=False, extra_sources=(), num_scalars=1, flux=2.5):
+    i, j, k = src
+    sources = [(1, (i - 0.5, j - 0.5, k - 0.5), flux)] + list(extra_sources)
+    return make_config(*n, precision=precision, buoyancy=buoyancy, num_scalars=num_scalars, point_sources=sources,
+                       avg_slice_k=k, avg_slice_j=j, avg_weight=1.0 / steps)
+
+
+def _dispersion_pair(cfg, src, seed=0):
+    from gpu_elmm_b200.config import FIELD_SCALAR, FIELD_TEMPERATURE
+    from gpu_elmm_b200.workloads import puff_state, temperature_state
+    g = grid_of(cfg)
+    st = log_profile_state(g, seed=seed)
+    S0 = puff_state(g, src)
+    o = Oracle(cfg)
+    o.set_state(*st)
+    d = L.Domain(cfg)
+    d.upload(*st)
+    for sc in range(1, cfg.num_scalars + 1):
+        o.set_field(FIELD_SCALAR + sc - 1, S0 * sc)
+        d.upload_scalar(sc, S0 * sc)
+    if cfg.enable_buoyancy:
+        T0 = temperature_state(g, seed=seed)
+        o.set_field(FIELD_TEMPERATURE, T0)
+        d.upload_temperature(T0)
+    o.project(1.0)
+    d.project(1.0)
+    return g, o, d
+
+
+@pytest.mark.parametrize("nsteps", [1, 10])
+def test_fp64_dispersion_channel(nsteps):
+    """Config-0 physics with a passive scalar, a Gaussian puff and a
+    continuous point source (the serving workload): FP64 GPU vs oracle for
+    the flow, the scalar, its initial diffusivity and the time-averaged
+    slices."""
+    from gpu_elmm_b200.config import FIELD_TDIFF
+    n, src = (32, 24, 16), (9, 17, 6)
+    g, o, d = _dispersion_pair(_dispersion_cfg(n, src, steps=nsteps), src)
+    m = (g.Prnx, g.Prny, g.Prnz)
+    assert rel(interior(d.field(FIELD_TDIFF), -1, m), interior(o.get_field(FIELD_TDIFF), -1, m)) < 1e-13
+    o.step(nsteps)
+    d.step(nsteps)
+    for a, b, name in zip(interiors(g, *d.download()), interiors(g, *o.state()), "UVWP"):
+        assert rel(a, b) < (1e-11 if name == "P" else 1e-12), (name, rel(a, b))
+    Sg, So = interior(d.scalar(1), -2, m), interior(o.get_field(16), -2, m)
+    assert rel(Sg, So) < 1e-11, rel(Sg, So)
+    for a, b in zip(d.scalar_slices(1), o.scalar_slices(1)):
+        assert rel(a, b) < 1e-11, rel(a, b)
+    d.close()
+
+
+def test_fp64_scalars_with_temperature_and_sources():
+    """Temperature plus two passive scalars (slots 0, 1, 2) and several point
+    sources: two in one cell (added in configuration order), one next to the
+    bottom wall (before the wall-model term), one outside the domain."""
+    n, src = (32, 24, 16), (5, 4, 3)
+    extra = [(2, (20.5, 10.5, 0.5), 1.0), (1, (4.6, 3.2, 2.9), -0.75), (2, (40.0, 1.0, 1.0), 3.0)]
+    cfg = _dispersion_cfg(n, src, steps=3, buoyancy=True, extra_sources=extra, num_scalars=2)
+    g, o, d = _dispersion_pair(cfg, src, seed=2)
+    o.step(3)
+    d.step(3)
+    m = (g.Prnx, g.Prny, g.Prnz)
+    for a, b, name in zip(interiors(g, *d.download()), interiors(g, *o.state()), "UVWP"):
+        assert rel(a, b) < (1e-11 if name == "P" else 1e-12), (name, rel(a, b))
+    for sc in (1, 2):
+        Sg, So = interior(d.scalar(sc), -2, m), interior(o.get_field(15 + sc), -2, m)
+        assert rel(Sg, So) < 1e-11, (sc, rel(Sg, So))
+        for a, b in zip(d.scalar_slices(sc), o.scalar_slices(sc)):
+            assert rel(a, b) < 1e-11, (sc, rel(a, b))
+    Tg = interior(d.temperature(), -2, m) - 295.0
+    To = interior(o.get_field(12), -2, m) - 295.0
+    assert rel(Tg, To) < 1e-11
+    d.close()
+
+
+def test_mixed_dispersion_one_step():
+    """Mixed path against the FP64 GPU path after one step from the same
+    projected state: velocities and the scalar within 1e-5."""
+    n, src = (32, 24, 16), (9, 17, 6)
+    from gpu_elmm_b200.workloads import puff_state
+    g = grid_of(make_config(*n))
+    st = log_profile_state(g, seed=1)
+    S0 = puff_state(g, src)
+    out = []
+    for prec in (0, 1):
+        d = L.Domain(_dispersion_cfg(n, src, precision=prec))
+        d.upload(*st)
+        d.upload_scalar(1, S0)
+        d.project(1.0)
+        d.step(1)
+        m = (g.Prnx, g.Prny, g.Prnz)
+        out.append((interiors(g, *d.download())[:3], interior(d.scalar(1), -2, m), d.scalar_slices(1)))
+        d.close()
+    (v64, s64, sl64), (vm, sm, slm) = out
+    for a, b in zip(vm, v64):
+        assert rel(a, b) < 1e-5
+    assert rel(sm, s64) < 1e-5, rel(sm, s64)
+    for a, b in zip(slm, sl64):
+        assert rel(a, b) < 1e-5
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_dispersion_alone_and_in_batch(precision):
+    """A dispersion domain gives bit-identical results alone and inside a
+    batch of domains of other sizes (every choice of kernel path is made per
+    domain)."""
+    from gpu_elmm_b200.workloads import puff_state
+    cases = [((32, 24, 16), (9, 17, 6), 0), ((48, 32, 16), (30, 3, 12), 1), ((64, 64, 32), (1, 64, 2), 2)]
+    cfgs = [_dispersion_cfg(n, s, precision=precision, steps=4) for n, s, _ in cases]
+    b = L.Batch(cfgs)
+    for q, (n, s, seed) in enumerate(cases):
+        g = grid_of(cfgs[q])
+        b.upload(q, *log_profile_state(g, seed=seed))
+        b.upload_scalar(q, 1, puff_state(g, s))
+    b.project(1.0)
+    b.step(4)
+    for q, (n, s, seed) in enumerate(cases):
+        g = grid_of(cfgs[q])
+        d = L.Domain(cfgs[q])
+        d.upload(*log_profile_state(g, seed=seed))
+        d.upload_scalar(1, puff_state(g, s))
+        d.project(1.0)
+        d.step(4)
+        for a, c in zip(d.download(), b.download(q)):
+            assert np.array_equal(a, c)
+        assert np.array_equal(d.scalar(1), b.scalar(q, 1))
+        for a, c in zip(d.scalar_slices(1), b.scalar_slices(q, 1)):
+            assert np.array_equal(a, c)
+        d.close()
+    b.close()

@@ -139,3 +139,95 @@ def test_buoyancy_vanishes_for_the_reference_temperature():
     b.step(2)
     for x, y, tol in zip(a.state(), b.state(), (1e-12, 1e-12, 1e-12, 1e-11)):  # P: conditioning floor
         assert rel(x, y) < tol
+
+
+def _dispersion_channel(n=(16, 12, 10), source=(5, 7, 4), flux=2.5, steps=0, seed=0, avg=True):
+    """A channel with one passive scalar: a Gaussian puff around the source
+    cell and a continuous point source at its centre."""
+    from gpu_elmm_b200.config import FIELD_SCALAR, grid_of, make_config
+    from gpu_elmm_b200.workloads import log_profile_state, puff_state
+    i, j, k = source
+    pos = (i - 0.5, j - 0.5, k - 0.5)  # the cell centre (dx = dy = dz = 1, origin 0)
+    cfg = make_config(*n, num_scalars=1, point_sources=[(1, pos, flux)],
+                      avg_slice_k=k if avg else 0, avg_slice_j=j if avg else 0,
+                      avg_weight=1.0 / steps if steps else 0.0)
+    g = grid_of(cfg)
+    o = Oracle(cfg)
+    o.set_state(*log_profile_state(g, seed=seed))
+    o.set_field(FIELD_SCALAR, puff_state(g, source))
+    o.project(1.0)
+    return cfg, g, o
+
+
+def test_point_source_adds_its_flux():
+    """Zero-flux walls and periodic x, y: the scalar content changes only by
+    the point source, flux * dt per step (the RK3 weights of a stage sum to
+    one over a step), and by the wall-model divergence term (~1e-15)."""
+    from gpu_elmm_b200.config import FIELD_SCALAR
+    from gpu_elmm_b200.workloads import interior
+    flux, nsteps = 2.5, 4
+    cfg, g, o = _dispersion_channel(flux=flux)
+    n = (g.Prnx, g.Prny, g.Prnz)
+    m0 = interior(o.get_field(FIELD_SCALAR), -2, n).sum()  # cell volume 1
+    o.step(nsteps)
+    S = interior(o.get_field(FIELD_SCALAR), -2, n)
+    assert np.isfinite(S).all()
+    assert abs((S.sum() - m0) - flux * cfg.dt * nsteps) < 1e-11 * max(1.0, abs(m0))
+
+
+def test_scalar_averages_are_the_mean_of_the_steps():
+    """The time-averaged slices equal the mean, over the steps, of the
+    scalar's slice planes after each step (avg_weight = 1 / steps)."""
+    from gpu_elmm_b200.config import FIELD_SCALAR
+    from gpu_elmm_b200.workloads import interior
+    nsteps, src = 3, (5, 7, 4)
+    cfg, g, o = _dispersion_channel(steps=nsteps, source=src)
+    n = (g.Prnx, g.Prny, g.Prnz)
+    xy, xz = np.zeros((g.Prny, g.Prnx)), np.zeros((g.Prnz, g.Prnx))
+    for _ in range(nsteps):
+        o.step(1)
+        S = interior(o.get_field(FIELD_SCALAR), -2, n)
+        xy += S[src[2] - 1] / nsteps
+        xz += S[:, src[1] - 1, :] / nsteps
+    axy, axz = o.scalar_slices(1)
+    assert rel(axy, xy) < 1e-14 and rel(axz, xz) < 1e-14
+    assert np.abs(axy).max() > 0
+
+
+def test_scalar_diffusivity_is_set_once_without_buoyancy():
+    """Without buoyancy TDiff is computed once, after the initial projection
+    (src/initial.f90:4296-4313), and then kept: ComputeTDiff runs per stage
+    only with buoyancy (src/dynamics.f90:904)."""
+    from gpu_elmm_b200.config import FIELD_TDIFF, FIELD_VISCOSITY
+    from gpu_elmm_b200.workloads import interior
+    cfg, g, o = _dispersion_channel()
+    n = (g.Prnx, g.Prny, g.Prnz)
+    nu = interior(o.get_field(FIELD_VISCOSITY), -1, n)
+    td0 = interior(o.get_field(FIELD_TDIFF), -1, n).copy()
+    want = (nu - cfg.molecular_viscosity) / 0.6 + cfg.molecular_diffusivity
+    assert rel(td0, want) < 1e-15
+    o.step(2)
+    assert np.array_equal(interior(o.get_field(FIELD_TDIFF), -1, n), td0)
+    assert not np.array_equal(interior(o.get_field(FIELD_VISCOSITY), -1, n), nu)
+
+
+def test_point_source_cell_follows_gridcoords():
+    """GridCoords on a uniform grid: nint((x - xU(0)) / dx + 0.5), clamped; a
+    point outside the domain adds no source."""
+    from gpu_elmm_b200.config import FIELD_SCALAR, grid_of, make_config
+    from gpu_elmm_b200.workloads import interior
+    n = (8, 8, 6)
+    for pos, cell in (((2.2, 3.9, 1.0), (3, 4, 1)), ((7.99, 0.0, 5.5), (8, 1, 6))):
+        cfg = make_config(*n, num_scalars=1, point_sources=[(1, pos, 1.0)], sgstype=0, wallmodeltype=0)
+        g = grid_of(cfg)
+        o = Oracle(cfg)
+        o.set_state(np.zeros(g.shape_u()), np.zeros(g.shape_v()), np.zeros(g.shape_w()))
+        o.step(1)
+        S = interior(o.get_field(FIELD_SCALAR), -2, n)
+        i, j, k = cell
+        assert S[k - 1, j - 1, i - 1] > 0 and np.count_nonzero(S) > 0
+    cfg = make_config(*n, num_scalars=1, point_sources=[(1, (9.5, 1.0, 1.0), 1.0)], sgstype=0, wallmodeltype=0)
+    o = Oracle(cfg)
+    o.set_state(np.zeros(g.shape_u()), np.zeros(g.shape_v()), np.zeros(g.shape_w()))
+    o.step(1)
+    assert np.count_nonzero(o.get_field(FIELD_SCALAR)) == 0
