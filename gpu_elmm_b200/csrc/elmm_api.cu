@@ -15,12 +15,14 @@
 #include <initializer_list>
 #include <mutex>
 #include <string>
+#include <deque>
 #include <vector>
 
 #include "../../include/elmm_gpu.h"
 #include "elmm_kernels2.cuh"
 #include "elmm_poisson_reg.cuh"
 #include "elmm_temperature.cuh"
+#include "elmm_arena.h"
 
 using namespace elmm;
 
@@ -294,29 +296,61 @@ struct BatchT {
   long long cells = 0;
   int step_kernels = 0;  // kernel launches of one captured step
   int nlaunch = 0;       // running count while enqueuing
+  // device memory from a serving loop's budget instead of cudaMalloc
+  Arena *arena = nullptr;
+  size_t arena_bytes = 0;
+  // a view steps domains whose fields other batches own, on a borrowed stream
+  bool is_view = false;
 
   ~BatchT() { release(); }
 
   void release() {
     if (step_exec) cudaGraphExecDestroy(step_exec);
     step_exec = nullptr;
-    for (void *p : allocs) cudaFree(p);
+    for (void *p : allocs) {
+      if (arena) arena->release(p);
+      else cudaFree(p);
+    }
     allocs.clear();
+    arena_bytes = 0;
     if (frame_host) cudaFreeHost(frame_host);
     frame_host = nullptr;
     for (cudaEvent_t *e : {&ev_ready, &ev_packed, &ev_done, &t0, &t1})
       if (*e) { cudaEventDestroy(*e); *e = nullptr; }
-    if (stream) cudaStreamDestroy(stream);
-    if (side) cudaStreamDestroy(side);
+    if (!is_view) {
+      if (stream) cudaStreamDestroy(stream);
+      if (side) cudaStreamDestroy(side);
+    }
     stream = side = nullptr;
   }
 
   int dalloc(void **p, size_t bytes) {
-    cudaError_t e = cudaMalloc(p, std::max<size_t>(bytes, 256));
-    if (e != cudaSuccess) return fail(e == cudaErrorMemoryAllocation ? ELMM_ERR_OOM : ELMM_ERR_CUDA,
-                                      std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    bytes = std::max<size_t>(bytes, 256);
+    if (arena) {
+      *p = arena->alloc(bytes);
+      if (!*p) return fail(ELMM_ERR_ADMISSION, "the serving loop's HBM budget has no room for the request now");
+      arena_bytes += Arena::round(bytes);
+    } else {
+      cudaError_t e = cudaMalloc(p, bytes);
+      if (e != cudaSuccess) return fail(e == cudaErrorMemoryAllocation ? ELMM_ERR_OOM : ELMM_ERR_CUDA,
+                                        std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
     allocs.push_back(*p);
-    return cudaMemset(*p, 0, std::max<size_t>(bytes, 256)) == cudaSuccess ? ELMM_OK : fail(ELMM_ERR_CUDA, "cudaMemset");
+    return cudaMemset(*p, 0, bytes) == cudaSuccess ? ELMM_OK : fail(ELMM_ERR_CUDA, "cudaMemset");
+  }
+  // returns one allocation early (the host-layout staging of a serving
+  // request after its upload)
+  void dfree(void *p) {
+    auto it = std::find(allocs.begin(), allocs.end(), p);
+    if (it == allocs.end()) return;
+    allocs.erase(it);
+    if (arena) {
+      const size_t before = arena->in_use();
+      arena->release(p);
+      arena_bytes -= before - arena->in_use();
+    } else {
+      cudaFree(p);
+    }
   }
 
   template <typename X>
@@ -357,6 +391,33 @@ struct BatchT {
       int r = init_domain(d);
       if (r) return r;
     }
+    return init_tables();
+  }
+
+  // A batch over domains that other single-domain batches own (the active
+  // requests of a serving loop), launched on `on_stream`; its own memory is
+  // only the tables, from the same budget.
+  int init_view(const std::vector<BatchT<T> *> &members, cudaStream_t on_stream, Arena *budget) {
+    is_view = true;
+    arena = budget;
+    nd = (int)members.size();
+    device = members[0]->device;
+    stream = on_stream;
+    CU(cudaEventCreate(&t0));
+    CU(cudaEventCreate(&t1));
+    for (BatchT<T> *m : members) {
+      cfg.push_back(m->cfg[0]);
+      grid.push_back(m->grid[0]);
+      hdom.push_back(m->hdom[0]);
+      hplan.push_back(m->hplan[0]);
+      pr_image.push_back(nullptr);
+    }
+    return init_tables();
+  }
+
+  // device tables of the domains, launch maps and kernel attributes
+  int init_tables() {
+    const int n = nd;
     void *p;
     int r = dalloc(&p, sizeof(Dom<T>) * n);
     if (r) return r;
@@ -458,17 +519,25 @@ struct BatchT {
     };
     if ((r = reg_sets(reg_x, false, xreg))) return r;
     if ((r = reg_sets(reg_y, true, yreg))) return r;
-    // staging for host-layout copies
+    // staging for host-layout copies (a view copies nothing to the host)
     stage_elems = 0;
-    for (int d = 0; d < n; d++) {
+    for (int d = 0; d < n && !is_view; d++) {
       const Dom<T> &h = hdom[d];
       size_t e = (size_t)(h.nx + 6) * (h.ny + 6) * (h.nz + 6);
       stage_elems = std::max(stage_elems, e);
     }
-    r = dalloc((void **)&dstage, stage_elems * sizeof(double));
-    if (r) return r;
+    if (!is_view && (r = dalloc((void **)&dstage, stage_elems * sizeof(double)))) return r;
     for (int d = 0; d < n; d++) cells += (long long)hdom[d].nx * hdom[d].ny * hdom[d].nz;
     return ELMM_OK;
+  }
+
+  // after the upload of a serving request: the host-layout staging and the
+  // Pr image serve only copies to and from the host
+  void drop_host_staging() {
+    dfree(dstage);
+    dstage = nullptr;
+    stage_elems = 0;
+    for (auto &pi : pr_image) { dfree(pi); pi = nullptr; }
   }
 
   // whether a domain's transforms / z solve use the register FFTs and the
@@ -882,6 +951,14 @@ struct BatchT {
   }
 
   int step(int nsteps, elmm_stats *st) {
+    int r = step_launch(nsteps);
+    if (r) return r;
+    return step_finish(nsteps, st);
+  }
+
+  // enqueues nsteps replays of the step graph (captured on first use) without
+  // waiting for them
+  int step_launch(int nsteps) {
     CU(cudaSetDevice(device));
     if (frame_pending) CU(cudaStreamWaitEvent(stream, ev_packed, 0));
     bool cfl = false;
@@ -903,6 +980,11 @@ struct BatchT {
     CU(cudaEventRecord(t0, stream));
     for (int s = 0; s < nsteps; s++) CU(cudaGraphLaunch(step_exec, stream));
     CU(cudaEventRecord(t1, stream));
+    return ELMM_OK;
+  }
+
+  // waits for the steps of step_launch and reports them
+  int step_finish(int nsteps, elmm_stats *st) {
     CU(cudaStreamSynchronize(stream));
     CU(cudaGetLastError());
     time += nsteps * cfg[0].dt;
@@ -1332,6 +1414,8 @@ static int poisson_exec(BatchT<T> &B, double *Phi, const double *RHS) {
 }
 
 
+#include "elmm_server.inl"
+
 extern "C" {
 
 const char *elmm_version(void) { return "elmm-b200 1.0 (sm_100a)"; }
@@ -1476,6 +1560,65 @@ int elmm_batch_upload_state(elmm_batch *b, int32_t d, const double *U, const dou
 int elmm_batch_download_state(elmm_batch *b, int32_t d, double *U, double *V, double *W, double *Pr) {
   if (!b) return fail(ELMM_ERR_INVALID_ARG, "NULL batch");
   return DISPATCH(*b, download(d, U, V, W, Pr));
+}
+
+// ------------------------------------------------------------- serving
+int elmm_server_create(const elmm_server_config *cfg, elmm_server **out) {
+  if (!cfg || !out) return fail(ELMM_ERR_INVALID_ARG, "NULL argument");
+  *out = nullptr;
+  if (cfg->precision != ELMM_PREC_FP64 && cfg->precision != ELMM_PREC_MIXED)
+    return fail(ELMM_ERR_INVALID_CONFIG, "unknown precision");
+  if (cfg->max_active < 1 || cfg->max_active > ELMM_SERVER_MAX_ACTIVE)
+    return fail(ELMM_ERR_INVALID_CONFIG, "max_active in 1.." + std::to_string(ELMM_SERVER_MAX_ACTIVE));
+  if (cfg->chunk_steps < 1) return fail(ELMM_ERR_INVALID_CONFIG, "chunk_steps must be positive");
+  if (cfg->hbm_budget_bytes < (1 << 20)) return fail(ELMM_ERR_INVALID_CONFIG, "hbm_budget_bytes below 1 MiB");
+  elmm_server *s = new elmm_server();
+  s->precision = cfg->precision;
+  int r;
+  if (s->precision == ELMM_PREC_MIXED) {
+    s->s32.reset(new ServerT<float>());
+    r = s->s32->init(*cfg);
+  } else {
+    s->s64.reset(new ServerT<double>());
+    r = s->s64->init(*cfg);
+  }
+  if (r) { delete s; return r; }
+  *out = s;
+  return ELMM_OK;
+}
+
+int elmm_server_destroy(elmm_server *s) {
+  delete s;
+  return ELMM_OK;
+}
+
+#define SDISPATCH(S, EXPR) ((S)->precision == ELMM_PREC_MIXED ? (S)->s32->EXPR : (S)->s64->EXPR)
+
+int elmm_server_submit(elmm_server *s, const elmm_config *cfg, const double *U, const double *V, const double *W,
+                       const double *Pr, const double *S0, int32_t nsteps, int64_t *id) {
+  if (!s || !cfg || !id) return fail(ELMM_ERR_INVALID_ARG, "NULL argument");
+  return SDISPATCH(s, submit(*cfg, U, V, W, Pr, S0, nsteps, id));
+}
+
+int elmm_server_wait_any(elmm_server *s, int32_t timeout_ms, elmm_request_info *info) {
+  if (!s || !info) return fail(ELMM_ERR_INVALID_ARG, "NULL argument");
+  return SDISPATCH(s, wait_any(std::max(0, (int)timeout_ms), info));
+}
+
+int elmm_server_collect(elmm_server *s, int64_t id, double *xy, double *xz) {
+  if (!s) return fail(ELMM_ERR_INVALID_ARG, "NULL server");
+  return SDISPATCH(s, collect(id, xy, xz));
+}
+
+int elmm_server_stats_get(elmm_server *s, elmm_server_stats *st) {
+  if (!s || !st) return fail(ELMM_ERR_INVALID_ARG, "NULL argument");
+  SDISPATCH(s, stats(st));
+  return ELMM_OK;
+}
+
+double elmm_server_now(const elmm_server *s) {
+  if (!s) return 0;
+  return s->precision == ELMM_PREC_MIXED ? s->s32->now() : s->s64->now();
 }
 
 int elmm_batch_upload_scalar(elmm_batch *b, int32_t d, int32_t sc, const double *S) {

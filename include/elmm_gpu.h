@@ -325,6 +325,74 @@ int elmm_batch_step(elmm_batch *b, int32_t nsteps, elmm_stats *stats);
 /* total interior cells of the batch (for cell-steps/s) */
 int64_t elmm_batch_cells(const elmm_batch *b);
 
+/*
+ * Serving loop with continuous batching (dispersion runs of different grid
+ * sizes).  A worker thread owns the device: every admitted request is a
+ * domain whose state stays in HBM, and all admitted requests advance together
+ * through one batched launch set per RK3 step (one CUDA graph, rebuilt when
+ * the set changes).  Between chunks of at most chunk_steps steps, and while a
+ * chunk runs, queued requests are admitted in arrival order as long as their
+ * memory fits the server's HBM budget (one device allocation made at
+ * creation; a request's fields are carved from it) and fewer than max_active
+ * requests are on the device.  A request that has run its steps leaves the
+ * set; the time-averaged slices of its scalar 1 are copied to the host and
+ * its memory returns to the budget.  Each request computes exactly what it
+ * computes alone (every kernel choice is made per domain).
+ */
+typedef struct elmm_server elmm_server;
+
+#define ELMM_SERVER_MAX_ACTIVE 256
+
+typedef struct elmm_server_config {
+  int32_t device;
+  int32_t precision;            /* ELMM_PREC_*, shared by every request */
+  int64_t hbm_budget_bytes;     /* device memory the server holds for requests */
+  int32_t max_active;           /* requests on the device at once, 1..ELMM_SERVER_MAX_ACTIVE */
+  int32_t chunk_steps;          /* steps between admission points, >= 1 */
+} elmm_server_config;
+
+typedef struct elmm_request_info {
+  int64_t id;
+  int32_t status;               /* ELMM_OK, or the ELMM_ERR_* that ended the request */
+  int32_t steps;                /* steps run */
+  double t_submit, t_admit, t_done; /* seconds on the server clock (elmm_server_now) */
+  int64_t bytes;                /* device memory the request held */
+  double max_div;               /* max |div u| after its last step */
+  int64_t cells;                /* Prnx * Prny * Prnz */
+} elmm_request_info;
+
+typedef struct elmm_server_stats {
+  int64_t submitted, admitted, finished, failed;
+  int64_t cell_steps;           /* interior cells x steps of all finished chunks */
+  int64_t chunks, graph_builds;
+  int32_t active, queued, peak_active;
+  int32_t reserved;
+  int64_t bytes_in_use, bytes_peak, budget_bytes;
+  double busy_s;                /* device time of the chunks (CUDA events) */
+} elmm_server_stats;
+
+int elmm_server_create(const elmm_server_config *cfg, elmm_server **out);
+/* Stops the worker after its current chunk; unfinished requests are dropped. */
+int elmm_server_destroy(elmm_server *s);
+/* Queues a request of nsteps steps.  cfg->precision and cfg->device must be
+ * the server's.  U, V, W, Pr (may be NULL) and S0 (scalar 1, may be NULL for
+ * zero) are host arrays in the layouts of elmm_upload_state and
+ * elmm_upload_scalar; they must stay valid until the request is reported by
+ * elmm_server_wait_any.  A request that does not fit the whole budget, even
+ * with no other request on the device, ends with status ELMM_ERR_ADMISSION. */
+int elmm_server_submit(elmm_server *s, const elmm_config *cfg, const double *U, const double *V,
+                       const double *W, const double *Pr, const double *S0, int32_t nsteps,
+                       int64_t *id);
+/* Waits up to timeout_ms for a finished request that has not been reported
+ * yet and fills *info; ELMM_ERR_TIMEOUT when none finished in time. */
+int elmm_server_wait_any(elmm_server *s, int32_t timeout_ms, elmm_request_info *info);
+/* Copies the time-averaged slices of scalar 1 of a reported request (layouts
+ * of elmm_download_scalar_slices; NULL skips one) and forgets the request. */
+int elmm_server_collect(elmm_server *s, int64_t id, double *xy, double *xz);
+int elmm_server_stats_get(elmm_server *s, elmm_server_stats *st);
+/* Seconds since the server was created, on the clock of elmm_request_info. */
+double elmm_server_now(const elmm_server *s);
+
 /* Last error message of this thread (static storage). */
 const char *elmm_last_error(void);
 
