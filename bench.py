@@ -48,6 +48,13 @@ DATA = ("synthetic: seeded log profile u*=0.3 + U(-0.1,0.1) perturbations on u,v
 MOMENTUM_WORDS = 15
 # oracle steps timed by the reference arm (a bounded sample of the workload)
 REF_STEPS = 10
+# batched ensemble: domains per GPU and the axis lengths they draw from
+BATCH_DOMAINS = 64
+BATCH_AXES = (32, 48, 64, 96, 128)
+# serving loop: requests per GPU at each arrival rate (per GPU), HBM budget
+SERVE_REQUESTS = 16
+SERVE_RATES = (5.0, 200.0)
+SERVE_BUDGET = 40 << 30
 
 
 def peaks():
@@ -326,6 +333,10 @@ def run_ours(args, ws, rank, local):
     e2e_s = allreduce_max(statistics.median(e2e_t), ws)
     e2e = total_cells / e2e_s
 
+    dm.close()
+    batched = batched_leg(args, ws, rank, local)
+    serving = serving_leg(args, ws, rank, local)
+
     cpu = cpu_baseline(1) if (rank == 0 and ws == 1) else None
     barrier(ws)
     if rank == 0:
@@ -349,12 +360,90 @@ def run_ours(args, ws, rank, local):
             "gpu_launches": sm.kernels,
             "clocks": clk.summary(),
             "wall_s_timed": wall,
+            "batched": batched,
+            "serving": serving,
         }
         if cpu:
             line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
         print(json.dumps(line), flush=True)
-    dm.close()
     return 0
+
+
+def gather(x, ws):
+    """Every rank's x, on every rank."""
+    if ws == 1:
+        return [x]
+    import torch.distributed as dist
+    out = [None] * ws
+    dist.all_gather_object(out, x)
+    return out
+
+
+def batched_leg(args, ws, rank, local):
+    """The batched ensemble: BATCH_DOMAINS channel domains per GPU, each axis
+    drawn from BATCH_AXES (seed 0), config-0 physics with each domain's own
+    seed and log-profile u* in [0.2, 0.5], all stepped by one launch set and
+    one CUDA graph per step; mixed and FP64, device time, max over ranks."""
+    from gpu_elmm_b200 import lib as L
+    from gpu_elmm_b200.workloads import uniform
+    r = uniform(0, "sizes", 3 * BATCH_DOMAINS)
+    sizes = [tuple(BATCH_AXES[int(r[3 * q + a] * len(BATCH_AXES))] for a in range(3)) for q in range(BATCH_DOMAINS)]
+    ustar = 0.2 + 0.3 * uniform(0, "ustar", BATCH_DOMAINS)
+    out = {}
+    steps = max(3, min(args.steps, 20))
+    for prec, name in ((1, "mixed"), (0, "fp64")):
+        cfgs = [make_config(*n, precision=prec, device=local) for n in sizes]
+        b = L.Batch(cfgs)
+        for q, n in enumerate(sizes):
+            b.upload(q, *log_profile_state(grid_of(cfgs[q]), seed=1000 * rank + q + 1, ustar=float(ustar[q])))
+        b.project(1.0)
+        b.step(args.warmup)
+        barrier(ws)
+        st = b.step(steps)
+        ms = allreduce_max(st.elapsed_ms, ws)
+        cells = allreduce_sum(float(b.cells()), ws)
+        out[name] = {"value": cells * steps / (ms / 1e3), "unit": "cell-steps/s", "ms_per_step": ms / steps,
+                     "max_div": allreduce_max(st.max_div, ws), "kernels_per_step": st.kernels / steps}
+        b.close()
+    out["mixed_over_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    out["config"] = {"domains_per_gpu": BATCH_DOMAINS, "axes_from": BATCH_AXES,
+                     "cells_per_gpu": int(sum(a * b * c for a, b, c in sizes)), "steps": steps,
+                     "physics": "config-0 channel, u* ~ U[0.2, 0.5] per domain, seed per domain"}
+    return out
+
+
+def serving_leg(args, ws, rank, local):
+    """The serving loop under Poisson arrivals of dispersion requests (64^3 ..
+    192x192x96 cells, 200..2000 steps, a passive scalar with a point source and
+    a Gaussian puff).  Each rank serves every ws-th request on its own GPU;
+    latency is arrival to slices on the host, p50 / p99 over all requests."""
+    from gpu_elmm_b200.serve import Server, percentile, request_inputs, run_arrivals
+    from gpu_elmm_b200.workloads import dispersion_request, poisson_arrivals
+    reqs_all = [dispersion_request(0, q) for q in range(SERVE_REQUESTS * ws)]
+    out = []
+    for rate in SERVE_RATES:
+        arr_all = poisson_arrivals(0, rate * ws, len(reqs_all))
+        mine = list(range(rank, len(reqs_all), ws))
+        reqs = [reqs_all[q] for q in mine]
+        inputs = [request_inputs(q) for q in reqs]
+        srv = Server(precision=1, budget_bytes=SERVE_BUDGET, max_active=64, chunk_steps=50, device=local)
+        barrier(ws)
+        done, span = run_arrivals(srv, reqs, arr_all[mine], inputs)
+        st = srv.stats()
+        srv.close()
+        lat = [i.t_done - i.t_submit for _, i, _ in done]
+        cs = float(sum(i.cells * i.steps for _, i, _ in done))
+        lats = [x for part in gather(lat, ws) for x in part]
+        out.append({"rate_per_s": rate * ws, "requests": len(reqs_all),
+                    "p50_latency_s": percentile(lats, 50), "p99_latency_s": percentile(lats, 99),
+                    "cell_steps_per_s": allreduce_sum(cs, ws) / allreduce_max(span, ws),
+                    "peak_active": int(allreduce_max(float(st.peak_active), ws)),
+                    "graph_builds": int(allreduce_sum(float(st.graph_builds), ws)),
+                    "busy_frac": allreduce_sum(st.busy_s, ws) / (ws * allreduce_max(span, ws))})
+    return {"points": out, "precision": "mixed", "budget_gb_per_gpu": SERVE_BUDGET / 2 ** 30,
+            "latency": "Poisson arrival to time-averaged slices on the host (wall clock of the serving loop)",
+            "workload": "dispersion requests: s x s x nz, s in {64,96,128,192}, nz in {64,96}, 200..2000 steps, "
+                        "passive scalar with a continuous point source and a sigma=2 Gaussian puff"}
 
 
 def main():

@@ -193,6 +193,8 @@ static int check_config(const elmm_config &c) {
                     "temperature walls must be adiabatic (ELMM_BC_CONSTFLUX with sideTemp = 0)");
     }
     if (c.zW) return fail(ELMM_ERR_INVALID_CONFIG, "the temperature field needs a uniform z grid");
+    if (c.Btype[ELMM_BO] == ELMM_BC_PERIODIC)
+      return fail(ELMM_ERR_INVALID_CONFIG, "the temperature field needs walls at the bottom and top");
     if (!(c.temperature_ref > 0) || !(c.molecular_diffusivity >= 0))
       return fail(ELMM_ERR_INVALID_CONFIG, "temperature_ref must be positive and molecular_diffusivity non-negative");
   }
@@ -247,7 +249,7 @@ struct LaunchSet {
 };
 
 enum { LK_CELLS = 0, LK_BOX, LK_ROWS, LK_YCOLS, LK_TRI, LK_MOM, LK_SHELL, LK_XREG, LK_YREG, LK_TRIT, LK_TCOL, LK_DCOL,
-       LK_AVG, LK_N };
+       LK_AVG, LK_COMMIT, LK_N };
 
 // -------------------------------------------------------------------- batch
 template <typename T>
@@ -568,6 +570,10 @@ struct BatchT {
       case LK_TCOL: return ntx * nty * ((h.nz + TMKC - 1) / TMKC) * h.nslot;
       case LK_DCOL: return ntx * nty * ((h.nz + kDivChunk - 1) / kDivChunk);
       case LK_AVG: return (h.nslot - (h.buoy ? 1 : 0)) * ((h.avg_k > 0 ? h.ny : 0) + (h.avg_j > 0 ? h.nz : 0));
+      case LK_COMMIT: {
+        const long long nvec = h.plane * h.nz * (long long)sizeof(T) / 16;
+        return h.nslot * (int)((nvec + kCommitVecs - 1) / kCommitVecs);
+      }
       default: return tri_tiled(h) ? 0 : (h.ny * h.spitch + kTriThreads - 1) / kTriThreads;
     }
   }
@@ -822,10 +828,8 @@ struct BatchT {
     nlaunch++;
     k_scalar<T><<<gsz(7, ls[LK_TCOL].total), TX * TY, 0, stream>>>(ddom, ls[LK_TCOL].l(), kRho[stage - 1],
                                                                     kBeta[stage - 1], stage == 1);
-    for (auto &h : hdom)
-      for (int q = 0; q < h.nslot; q++)
-        cudaMemcpyAsync(h.slot[q].m, h.slot[q].n, (size_t)h.plane * (h.nz + 2) * sizeof(T), cudaMemcpyDeviceToDevice,
-                        stream);
+    nlaunch++;
+    k_scalar_commit<T><<<std::min(ls[LK_COMMIT].total, 4 * 148), 256, 0, stream>>>(ddom, ls[LK_COMMIT].l());
     if (accumulate && ls[LK_AVG].total > 0) {
       nlaunch++;
       k_scalar_avg<T><<<std::min(ls[LK_AVG].total, 8 * 148), 128, 0, stream>>>(ddom, ls[LK_AVG].l());

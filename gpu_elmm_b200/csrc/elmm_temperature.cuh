@@ -195,6 +195,31 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
   }
 }
 
+// After a stage the new values become the current ones: planes 1..nz of
+// every slot of every domain, n -> m, in 16-byte vectors (a box starts on a
+// 256-byte boundary and a plane is a whole number of 128-byte rows).  One
+// launch for the whole batch.  Tiles: (slot, chunk of kCommitVecs vectors).
+constexpr int kCommitVecs = 4096;
+
+template <typename T>
+__global__ void k_scalar_commit(const Dom<T> *__restrict__ doms, Launch L) {
+  typedef typename Vec2<T>::type V2;
+  typedef float4 V;  // 16 bytes: 4 floats or 2 doubles
+  static_assert(sizeof(V2) * 2 == sizeof(V) || sizeof(V2) == sizeof(V), "16-byte vectors");
+  for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
+    const int di = find_dom(L.starts, L.nd, t);
+    const Dom<T> &d = doms[di];
+    const int lt = t - __ldg(L.starts + di);
+    const long long nvec = d.plane * d.nz * (long long)sizeof(T) / 16;
+    const int per = (int)((nvec + kCommitVecs - 1) / kCommitVecs);
+    const int s = lt / per, c = lt % per;
+    const V *src = reinterpret_cast<const V *>(d.slot[s].n + d.plane);
+    V *dst = reinterpret_cast<V *>(d.slot[s].m + d.plane);
+    const long long v0 = (long long)c * kCommitVecs, v1 = min(nvec, v0 + kCommitVecs);
+    for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x) dst[v] = __ldg(src + v);
+  }
+}
+
 // Scalar_avg = Scalar_avg + Scalar * time_weight (src/outputs.f90:1043-1045)
 // on the two slice planes of every passive scalar, after the last stage of a
 // step.  Tiles: (slot, row of the slice planes) per domain, rows of the xy
