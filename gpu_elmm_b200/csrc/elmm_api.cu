@@ -17,6 +17,7 @@
 #include <string>
 #include <deque>
 #include <vector>
+#include <type_traits>
 
 #include "../../include/elmm_gpu.h"
 #include "elmm_kernels2.cuh"
@@ -249,7 +250,7 @@ struct LaunchSet {
 };
 
 enum { LK_CELLS = 0, LK_BOX, LK_ROWS, LK_YCOLS, LK_TRI, LK_MOM, LK_SHELL, LK_XREG, LK_YREG, LK_TRIT, LK_TCOL, LK_DCOL,
-       LK_AVG, LK_COMMIT, LK_N };
+       LK_AVG, LK_COMMIT, LK_TPAIR, LK_N };
 
 // -------------------------------------------------------------------- batch
 template <typename T>
@@ -489,6 +490,8 @@ struct BatchT {
     grid_cap[8] = cap((const void *)k_cfl<T>, TX * TY, 0);
     grid_cap[9] = cap((const void *)k_ghosts<T>, kShellThreads, 0);
     grid_cap[13] = cap((const void *)k_tri_tile<T>, kTriTileThreads, smem_trit);
+    grid_cap[11] = cap((const void *)k_scalar<T>, TX * TY, 0);
+    grid_cap[12] = std::is_same<T, float>::value ? cap((const void *)k_scalar_pair, SPX * SPY, 0) : 1;
     // one launch set per distinct x (y) length, holding only its domains
     auto reg_sets = [&](bool use, bool ydir, std::vector<RegSet> &out) -> int {
       if (!use) return ELMM_OK;
@@ -546,6 +549,9 @@ struct BatchT {
   // tiled Thomas kernel (decided per domain, so that a domain gives the same
   // result alone and in any batch)
   static bool tri_tiled(const Dom<T> &h) { return !h.zper && h.nz <= kTriTileMaxNz; }
+  // the FP32 scalar stage runs two cells per thread when the pairs tile the
+  // periodic x axis
+  static bool scalar_pairs(const Dom<T> &h) { return sizeof(T) == 4 && h.nx % 2 == 0; }
 
   static int tiles(int kind, const Dom<T> &h) {
     int ntx = (h.nx + TX - 1) / TX, nty = (h.ny + TY - 1) / TY;
@@ -567,7 +573,11 @@ struct BatchT {
         return ((h.nxh + C - 1) / C) * h.nz;
       }
       case LK_TRIT: return tri_tiled(h) ? (h.ny * h.spitch + kTriCols - 1) / kTriCols : 0;
-      case LK_TCOL: return ntx * nty * ((h.nz + TMKC - 1) / TMKC) * h.nslot;
+      case LK_TCOL: return scalar_pairs(h) ? 0 : ntx * nty * ((h.nz + TMKC - 1) / TMKC) * h.nslot;
+      case LK_TPAIR:
+        return scalar_pairs(h) ? ((h.nx + 2 * SPX - 1) / (2 * SPX)) * ((h.ny + SPY - 1) / SPY) *
+                                     ((h.nz + TMKC - 1) / TMKC) * h.nslot
+                               : 0;
       case LK_DCOL: return ntx * nty * ((h.nz + kDivChunk - 1) / kDivChunk);
       case LK_AVG: return (h.nslot - (h.buoy ? 1 : 0)) * ((h.avg_k > 0 ? h.ny : 0) + (h.avg_j > 0 ? h.nz : 0));
       case LK_COMMIT: {
@@ -824,12 +834,22 @@ struct BatchT {
   // while writing).  accumulate: the last stage of a step, which also feeds
   // the time-averaged slices.
   void launch_scalars(int stage, int accumulate) {
-    if (ls[LK_TCOL].total == 0) return;
+    if (ls[LK_TCOL].total == 0 && ls[LK_TPAIR].total == 0) return;
+    if (ls[LK_TCOL].total > 0) {
+      nlaunch++;
+      k_scalar<T><<<gsz(11, ls[LK_TCOL].total), TX * TY, 0, stream>>>(ddom, ls[LK_TCOL].l(), kRho[stage - 1],
+                                                                       kBeta[stage - 1], stage == 1);
+    }
+    if constexpr (std::is_same<T, float>::value) {
+      if (ls[LK_TPAIR].total > 0) {
+        nlaunch++;
+        k_scalar_pair<<<gsz(12, ls[LK_TPAIR].total), SPX * SPY, 0, stream>>>(ddom, ls[LK_TPAIR].l(), kRho[stage - 1],
+                                                                            kBeta[stage - 1], stage == 1);
+      }
+    }
     nlaunch++;
-    k_scalar<T><<<gsz(7, ls[LK_TCOL].total), TX * TY, 0, stream>>>(ddom, ls[LK_TCOL].l(), kRho[stage - 1],
-                                                                    kBeta[stage - 1], stage == 1);
-    nlaunch++;
-    k_scalar_commit<T><<<std::min(ls[LK_COMMIT].total, 4 * 148), 256, 0, stream>>>(ddom, ls[LK_COMMIT].l());
+    k_scalar_commit<T><<<std::min(ls[LK_COMMIT].total, 16 * 148), kCommitThreads, 0, stream>>>(ddom,
+                                                                                                ls[LK_COMMIT].l());
     if (accumulate && ls[LK_AVG].total > 0) {
       nlaunch++;
       k_scalar_avg<T><<<std::min(ls[LK_AVG].total, 8 * 148), 128, 0, stream>>>(ddom, ls[LK_AVG].l());
@@ -1623,6 +1643,12 @@ int elmm_server_stats_get(elmm_server *s, elmm_server_stats *st) {
 double elmm_server_now(const elmm_server *s) {
   if (!s) return 0;
   return s->precision == ELMM_PREC_MIXED ? s->s32->now() : s->s64->now();
+}
+
+int elmm_batch_profile_stage(elmm_batch *b, int32_t stage, int32_t reps, double *ms) {
+  if (!b || !ms) return fail(ELMM_ERR_INVALID_ARG, "NULL argument");
+  if (stage < 1 || stage > 3 || reps < 1) return fail(ELMM_ERR_INVALID_ARG, "stage 1..3, reps >= 1");
+  return DISPATCH(*b, profile_stage(stage, reps, ms));
 }
 
 int elmm_batch_upload_scalar(elmm_batch *b, int32_t d, int32_t sc, const double *S) {

@@ -195,11 +195,167 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
   }
 }
 
+// The FP32 stage with two x-adjacent cells per thread (domains with an even
+// Prnx; x is periodic for every scalar): the pair's x faces are three fluxes
+// for two cells, every load and store is a float2, and the per-plane
+// bookkeeping of the column march is shared by the pair.  Same operations in
+// the same order as k_scalar.  A block is 16 x 8 threads, a tile 32 x 8 cells.
+constexpr int SPX = 16, SPY = 8;
+#ifndef ELMM_SCALAR_PAIR_MIN_BLOCKS
+#define ELMM_SCALAR_PAIR_MIN_BLOCKS 5
+#endif
+
+__device__ __forceinline__ float2 ld2(const float *p, long long o) {
+  return __ldg(reinterpret_cast<const float2 *>(p + o));
+}
+
+__global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS)
+    k_scalar_pair(const Dom<float> *__restrict__ doms, Launch L, double rho, double beta, int stage1) {
+  typedef float T;
+  for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
+    const int di = find_dom(L.starts, L.nd, t);
+    const Dom<T> &d = doms[di];
+    int lt = t - __ldg(L.starts + di);
+    const int nx = d.nx, ny = d.ny, nz = d.nz;
+    const int ntx = (nx + 2 * SPX - 1) / (2 * SPX), nty = (ny + SPY - 1) / SPY, nkc = (nz + TMKC - 1) / TMKC;
+    const int tx = lt % ntx; lt /= ntx;
+    const int ty = lt % nty; lt /= nty;
+    const int kc = lt % nkc;
+    const int s = lt / nkc;
+    const ScalSlot<T> &sl = d.slot[s];
+    const int k0 = kc * TMKC + 1, k1 = min(k0 + TMKC - 1, nz);
+    const int i = tx * 2 * SPX + 2 * (threadIdx.x % SPX) + 1;  // odd: the pair is 8-byte aligned
+    const int j = ty * SPY + (threadIdx.x / SPX) + 1;
+    if (i > nx || j > ny) continue;
+    const bool py = sl.bt[SIDE_SO] == BC_PERIODIC, pz = sl.bt[SIDE_BO] == BC_PERIODIC;
+    const long long pitch = d.pitch, plane = d.plane;
+    // the aligned pairs (i-2, i-1) and (i+2, i+3), periodic in x (nx even
+    // keeps them aligned); rows j-2..j+2 folded
+    const int oxm = (i - 2 >= 1 ? i - 2 : i - 2 + nx) - i, oxp = (i + 2 <= nx ? i + 2 : i + 2 - nx) - i;
+    int oy[5];
+#pragma unroll
+    for (int q = 0; q < 5; q++) oy[q] = (scal_fold(j - 2 + q, ny, py) - j) * (int)pitch;
+    auto zoff = [&](int kk) { return (long long)(scal_fold(kk, nz, pz) - kk) * plane; };
+    unsigned srcm = 0;  // volume sources of this slot in this pair's columns
+    for (int q = 0; q < d.nsrc; q++)
+      if (d.src_slot[q] == s && (d.src_i[q] == i || d.src_i[q] == i + 1) && d.src_j[q] == j) srcm |= 1u << q;
+    const T *__restrict__ S = sl.m;
+    const T *__restrict__ K = d.TDiff;
+    const T *__restrict__ U = d.U;
+    const T *__restrict__ V = d.V;
+    const T *__restrict__ W = d.W;
+    T *__restrict__ Sadv = sl.adv;
+    T *__restrict__ Snew = sl.n;
+    const T Ax = (T)(1.0 / d.dx), Ay = (T)(1.0 / d.dy), Az = (T)(1.0 / d.dz);
+    const T Dx = (T)(1.0 / (2 * d.dx * d.dx)), Dy = (T)(1.0 / (2 * d.dy * d.dy)), Dz = (T)(1.0 / (2 * d.dz * d.dz));
+    const T rdx = (T)d.dx, rdy = (T)d.dy;
+    const T rdt = (T)(rho * d.dt), bdt = (T)(beta * d.dt);
+    const bool wm_lo = d.wall[SIDE_BO] != 0, wm_hi = d.wall[SIDE_TO] != 0;
+    long long cc = bidx(d, i, j, k0);
+    float2 sz[5], kz[3];
+#pragma unroll
+    for (int q = 0; q < 5; q++) sz[q] = ld2(S, cc + (long long)(q - 2) * plane + zoff(k0 - 2 + q));
+#pragma unroll
+    for (int q = 0; q < 3; q++) kz[q] = ld2(K, cc + (long long)(q - 1) * plane + zoff(k0 - 1 + q));
+    float2 wb = ld2(W, cc - plane);
+    float2 fzb = make_float2(kappa_flux<T>(wb.x, sz[0].x, sz[1].x, sz[2].x, sz[3].x),
+                             kappa_flux<T>(wb.y, sz[0].y, sz[1].y, sz[2].y, sz[3].y));
+    for (int k = k0; k <= k1; k++) {
+      const float2 s0 = sz[2];
+      const float2 sm = ld2(S, cc + oxm), sp = ld2(S, cc + oxp);  // S(i-2, i-1), S(i+2, i+3)
+      const float2 km = ld2(K, cc + oxm), kp = ld2(K, cc + oxp);  // .y = K(i-1), .x = K(i+2)
+      const float2 um = ld2(U, cc - 2), u0 = ld2(U, cc);          // .y = U(i-1); U(i), U(i+1)
+      const float2 vs = ld2(V, cc - pitch), vn = ld2(V, cc);
+      const float2 wt = ld2(W, cc);
+      const float2 sym2 = ld2(S, cc + oy[0]), sym1 = ld2(S, cc + oy[1]), syp1 = ld2(S, cc + oy[3]),
+                   syp2 = ld2(S, cc + oy[4]);
+      const float2 kym = ld2(K, cc + oy[1]), kyp = ld2(K, cc + oy[3]);
+      const float2 told = stage1 ? make_float2(0.f, 0.f) : ld2(Sadv, cc);
+      // x faces: low face of cell i, the face between the pair, high face of i+1
+      const T f0 = kappa_flux<T>(um.y, sm.x, sm.y, s0.x, s0.y);
+      const T f1 = kappa_flux<T>(u0.x, sm.y, s0.x, s0.y, sp.x);
+      const T f2 = kappa_flux<T>(u0.y, s0.x, s0.y, sp.x, sp.y);
+      const float2 fzt = make_float2(kappa_flux<T>(wt.x, sz[1].x, s0.x, sz[3].x, sz[4].x),
+                                     kappa_flux<T>(wt.y, sz[1].y, s0.y, sz[3].y, sz[4].y));
+      const bool even = ((k - 1) & 1) == 0;  // face k-1 is even
+      const bool wmk = (k == 1 && wm_lo) || (k == nz && wm_hi);
+      float2 out_a, out_n;
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        // the pair's lanes: x neighbours, y and z neighbours of cell i + c
+        const T sc = c ? s0.y : s0.x;
+        const T sxm1 = c ? s0.x : sm.y, sxp1 = c ? sp.x : s0.y;
+        const T kxm = c ? kz[1].x : km.y, kxp = c ? kp.x : kz[1].y, k0v = c ? kz[1].y : kz[1].x;
+        const T fl = c ? f1 : f0, fh = c ? f2 : f1;
+        const T vsc = c ? vs.y : vs.x, vnc = c ? vn.y : vn.x;
+        const T a2 = c ? sym2.y : sym2.x, a1 = c ? sym1.y : sym1.x, b1 = c ? syp1.y : syp1.x, b2 = c ? syp2.y : syp2.x;
+        T a = (T)0;
+        a = a + Ax * fl;
+        a = a - Ax * fh;
+        a = a + Ay * kappa_flux<T>(vsc, a2, a1, sc, b1);
+        a = a - Ay * kappa_flux<T>(vnc, a1, sc, b1, b2);
+        const T fb = c ? fzb.y : fzb.x, ft = c ? fzt.y : fzt.x;
+        if (even) {
+          a = a + Az * fb;
+          a = a - Az * ft;
+        } else {
+          a = a - Az * ft;
+          a = a + Az * fb;
+        }
+        const T kym_c = c ? kym.y : kym.x, kyp_c = c ? kyp.y : kyp.x;
+        const T zp = c ? sz[3].y : sz[3].x, zm = c ? sz[1].y : sz[1].x;
+        const T kzp = c ? kz[2].y : kz[2].x, kzm = c ? kz[0].y : kz[0].x;
+        a = a + (kxp + k0v) * (sxp1 - sc) * Dx;
+        a = a - (k0v + kxm) * (sc - sxm1) * Dx;
+        a = a + (kyp_c + k0v) * (b1 - sc) * Dy;
+        a = a - (k0v + kym_c) * (sc - a1) * Dy;
+        a = a + (kzp + k0v) * (zp - sc) * Dz;
+        a = a - (k0v + kzm) * (sc - zm) * Dz;
+        if (srcm) {
+          for (int q = 0; q < d.nsrc; q++)
+            if (((srcm >> q) & 1u) && d.src_i[q] == i + c && d.src_k[q] == k) a = a + (T)d.src_q[q];
+        }
+        if (wmk) {
+          const T dzk = (T)d.dzPr[k + 2];
+          const T ue = c ? u0.y : u0.x, uw = c ? u0.x : um.y;
+          const T wtc = c ? wt.y : wt.x, wbc = c ? wb.y : wb.x;
+          T div = (T)0;
+          div = div + ue / rdx;
+          div = div - uw / rdx;
+          div = div + vnc / rdy;
+          div = div - vsc / rdy;
+          div = div + wtc / dzk;
+          div = div - wbc / dzk;
+          a = a + div * sc;
+        }
+        T t2 = stage1 ? (T)0 : (c ? told.y : told.x) * rdt;
+        t2 = t2 + a * bdt;
+        if (c) { out_a.y = a; out_n.y = sc + t2; } else { out_a.x = a; out_n.x = sc + t2; }
+      }
+      *reinterpret_cast<float2 *>(Sadv + cc) = out_a;
+      *reinterpret_cast<float2 *>(Snew + cc) = out_n;
+      if (k < k1) {
+        const long long cn = cc + plane;
+#pragma unroll
+        for (int q = 0; q < 4; q++) sz[q] = sz[q + 1];
+        sz[4] = ld2(S, cn + 2 * plane + zoff(k + 3));
+        kz[0] = kz[1];
+        kz[1] = kz[2];
+        kz[2] = ld2(K, cn + plane + zoff(k + 2));
+        wb = wt;
+        fzb = fzt;
+        cc = cn;
+      }
+    }
+  }
+}
+
 // After a stage the new values become the current ones: planes 1..nz of
 // every slot of every domain, n -> m, in 16-byte vectors (a box starts on a
 // 256-byte boundary and a plane is a whole number of 128-byte rows).  One
-// launch for the whole batch.  Tiles: (slot, chunk of kCommitVecs vectors).
-constexpr int kCommitVecs = 4096;
+// launch for the whole batch.  Tiles: (slot, chunk of kCommitVecs vectors);
+// a thread moves kCommitPer vectors with all its loads issued first.
+constexpr int kCommitThreads = 256, kCommitPer = 4, kCommitVecs = kCommitThreads * kCommitPer;
 
 template <typename T>
 __global__ void k_scalar_commit(const Dom<T> *__restrict__ doms, Launch L) {
@@ -215,8 +371,14 @@ __global__ void k_scalar_commit(const Dom<T> *__restrict__ doms, Launch L) {
     const int s = lt / per, c = lt % per;
     const V *src = reinterpret_cast<const V *>(d.slot[s].n + d.plane);
     V *dst = reinterpret_cast<V *>(d.slot[s].m + d.plane);
-    const long long v0 = (long long)c * kCommitVecs, v1 = min(nvec, v0 + kCommitVecs);
-    for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x) dst[v] = __ldg(src + v);
+    const long long v0 = (long long)c * kCommitVecs + threadIdx.x;
+    V x[kCommitPer];
+#pragma unroll
+    for (int q = 0; q < kCommitPer; q++)
+      if (v0 + q * kCommitThreads < nvec) x[q] = __ldg(src + v0 + q * kCommitThreads);
+#pragma unroll
+    for (int q = 0; q < kCommitPer; q++)
+      if (v0 + q * kCommitThreads < nvec) dst[v0 + q * kCommitThreads] = x[q];
   }
 }
 

@@ -72,6 +72,7 @@ def lib():
         L.elmm_batch_download_field.argtypes = [P, C.c_int32, C.c_int32, _dp]
         L.elmm_batch_download_scalar_slices.argtypes = [P, C.c_int32, C.c_int32, _dp, _dp]
         L.elmm_batch_project.argtypes = [P, C.c_double]
+        L.elmm_batch_profile_stage.argtypes = [P, C.c_int32, C.c_int32, _dp]
         L.elmm_batch_step.argtypes = [P, C.c_int32, C.POINTER(ElmmStats)]
         L.elmm_batch_cells.argtypes = [P]
         L.elmm_batch_cells.restype = C.c_int64
@@ -237,6 +238,12 @@ class Batch:
         st = ElmmStats()
         check(lib().elmm_batch_step(self.h, n, C.byref(st)), "elmm_batch_step")
         return st
+
+    def profile_stage(self, stage=2, reps=5):
+        """Mean device time (ms) of each kernel kind of one RK3 stage over the whole batch."""
+        ms = (C.c_double * KERNEL_COUNT)()
+        check(lib().elmm_batch_profile_stage(self.h, stage, reps, ms), "elmm_batch_profile_stage")
+        return dict(zip(KERNEL_NAMES, list(ms)))
 
 
 class PoissonSolver:

@@ -6,6 +6,10 @@ times of one stage.
 
     python -m gpu_elmm_b200.profile_step [--precision mixed|fp64] [--n 256,256,128]
                                          [--warmup 1] [--steps 1] [--no-temperature]
+                                         [--batched 64]
+
+--batched D runs the batched ensemble instead: D channel domains, each axis
+drawn from 32, 48, 64, 96, 128 (seed 0), one launch set for all of them.
 
 Under `ncu -k regex:<kernel> -s <skip> -c <count>` the launches of the
 profiled steps follow those of the projection and the warm-up steps.
@@ -26,7 +30,10 @@ def main():
     ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--stage-times", action="store_true", help="also time each kernel of stage 2 (5 repetitions)")
     ap.add_argument("--no-temperature", action="store_true", help="the channel without the temperature field")
+    ap.add_argument("--batched", type=int, default=0, help="run the batched ensemble of this many domains")
     a = ap.parse_args()
+    if a.batched:
+        return batched(a)
     n = tuple(int(x) for x in a.n.split(","))
     buoy = not a.no_temperature
     cfg = make_config(*n, precision=1 if a.precision == "mixed" else 0, buoyancy=buoy)
@@ -45,6 +52,28 @@ def main():
         out["stage2_kernel_ms"] = d.profile_stage(2, 5)
     print(json.dumps(out))
     d.close()
+
+
+def batched(a):
+    from .workloads import uniform
+    axes = (32, 48, 64, 96, 128)
+    r = uniform(0, "sizes", 3 * a.batched)
+    sizes = [tuple(axes[int(r[3 * q + k] * len(axes))] for k in range(3)) for q in range(a.batched)]
+    ustar = 0.2 + 0.3 * uniform(0, "ustar", a.batched)
+    cfgs = [make_config(*n, precision=1 if a.precision == "mixed" else 0) for n in sizes]
+    b = L.Batch(cfgs)
+    for q in range(a.batched):
+        b.upload(q, *log_profile_state(grid_of(cfgs[q]), seed=q + 1, ustar=float(ustar[q])))
+    b.project(1.0)
+    if a.warmup:
+        b.step(a.warmup)
+    s = b.step(a.steps)
+    out = {"domains": a.batched, "cells": b.cells(), "precision": a.precision, "steps": a.steps,
+           "ms_per_step": s.elapsed_ms / max(1, a.steps), "kernels_per_step": s.kernels / max(1, a.steps)}
+    if a.stage_times:
+        out["stage2_kernel_ms"] = b.profile_stage(2, 5)
+    print(json.dumps(out))
+    b.close()
 
 
 if __name__ == "__main__":

@@ -321,6 +321,8 @@ int elmm_batch_upload_scalar(elmm_batch *b, int32_t d, int32_t sc, const double 
 int elmm_batch_download_field(elmm_batch *b, int32_t d, int32_t field, double *host);
 int elmm_batch_download_scalar_slices(elmm_batch *b, int32_t d, int32_t sc, double *xy, double *xz);
 int elmm_batch_project(elmm_batch *b, double coef);
+/* elmm_profile_stage for a whole batch */
+int elmm_batch_profile_stage(elmm_batch *b, int32_t stage, int32_t reps, double *ms);
 int elmm_batch_step(elmm_batch *b, int32_t nsteps, elmm_stats *stats);
 /* total interior cells of the batch (for cell-steps/s) */
 int64_t elmm_batch_cells(const elmm_batch *b);
