@@ -412,6 +412,11 @@ def batched_leg(args, ws, rank, local):
     return out
 
 
+def serving_shard(n, ws, rank):
+    """The requests a rank serves: every ws-th of the stream, from its rank."""
+    return list(range(rank, n, ws))
+
+
 def serving_leg(args, ws, rank, local):
     """The serving loop under Poisson arrivals of dispersion requests (64^3 ..
     192x192x96 cells, 200..2000 steps, a passive scalar with a point source and
@@ -423,7 +428,7 @@ def serving_leg(args, ws, rank, local):
     out = []
     for rate in SERVE_RATES:
         arr_all = poisson_arrivals(0, rate * ws, len(reqs_all))
-        mine = list(range(rank, len(reqs_all), ws))
+        mine = serving_shard(len(reqs_all), ws, rank)
         reqs = [reqs_all[q] for q in mine]
         inputs = [request_inputs(q) for q in reqs]
         srv = Server(precision=1, budget_bytes=SERVE_BUDGET, max_active=64, chunk_steps=50, device=local)
