@@ -48,6 +48,8 @@ DATA = ("synthetic: seeded log profile u*=0.3 + U(-0.1,0.1) perturbations on u,v
 MOMENTUM_WORDS = 15
 # oracle steps timed by the reference arm (a bounded sample of the workload)
 REF_STEPS = 10
+# long run of the single domain on both paths (errors after 1, 10 and this many steps)
+LONG_STEPS = 1000
 # batched ensemble: domains per GPU and the axis lengths they draw from
 BATCH_DOMAINS = 64
 BATCH_AXES = (32, 48, 64, 96, 128)
@@ -334,6 +336,7 @@ def run_ours(args, ws, rank, local):
     e2e = total_cells / e2e_s
 
     dm.close()
+    long_run = long_run_leg(st, T0, local) if rank == 0 else None
     batched = batched_leg(args, ws, rank, local)
     serving = serving_leg(args, ws, rank, local)
 
@@ -360,6 +363,7 @@ def run_ours(args, ws, rank, local):
             "gpu_launches": sm.kernels,
             "clocks": clk.summary(),
             "wall_s_timed": wall,
+            "long_run": long_run,
             "batched": batched,
             "serving": serving,
         }
@@ -367,6 +371,47 @@ def run_ours(args, ws, rank, local):
             line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
         print(json.dumps(line), flush=True)
     return 0
+
+
+def long_run_leg(st, T0, local):
+    """Config 1 on both paths from one projected state for LONG_STEPS steps:
+    the relative error of the mixed path after 1, 10 and LONG_STEPS steps,
+    and the vertical profiles of mean velocity, resolved TKE and theta
+    averaged over the second half of the run (src/vertical_profiles.f90)."""
+    from gpu_elmm_b200 import lib as L
+    from gpu_elmm_b200.stats import Profiles, compare
+    g = grid_of(make_config(*N))
+    doms = {}
+    for prec in (0, 1):
+        doms[prec] = L.Domain(make_config(*N, precision=prec, device=local, buoyancy=True))
+    doms[0].upload(*st)
+    doms[0].upload_temperature(T0)
+    doms[0].project(1.0)
+    doms[1].upload(*doms[0].download())
+    doms[1].upload_temperature(T0)
+    prof = {0: Profiles(g), 1: Profiles(g)}
+    errs = {}
+    nT = (g.Prnx, g.Prny, g.Prnz)
+    done = 0
+    marks = sorted({1, 10, LONG_STEPS} | set(range(LONG_STEPS // 2, LONG_STEPS + 1, LONG_STEPS // 20)))
+    for target in marks:
+        for p in (0, 1):
+            doms[p].step(target - done)
+        done = target
+        s = {p: doms[p].download() for p in (0, 1)}
+        T = {p: doms[p].field(FIELD_TEMPERATURE) for p in (0, 1)}
+        if target in (1, 10, LONG_STEPS):
+            e = [rel(a, b) for a, b in zip(interiors(g, *s[1]), interiors(g, *s[0]))]
+            e.append(rel(interior(T[1], -2, nT) - 295.0, interior(T[0], -2, nT) - 295.0))
+            errs[str(target)] = dict(zip(("u", "v", "w", "p", "theta_minus_ref"), e))
+        if target >= LONG_STEPS // 2:
+            for p in (0, 1):
+                prof[p].add(*s[p][:3], T[p])
+    for p in (0, 1):
+        doms[p].close()
+    return {"steps": LONG_STEPS, "rel_err_mixed_vs_fp64": errs,
+            "profiles_rel_diff": compare(prof[1].result(), prof[0].result(), keys=("u", "tke", "theta")),
+            "profiles_window": f"steps {LONG_STEPS // 2}..{LONG_STEPS}, every {LONG_STEPS // 20}"}
 
 
 def gather(x, ws):

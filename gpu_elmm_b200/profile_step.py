@@ -12,7 +12,8 @@ times of one stage.
 drawn from 32, 48, 64, 96, 128 (seed 0), one launch set for all of them.
 
 Under `ncu -k regex:<kernel> -s <skip> -c <count>` the launches of the
-profiled steps follow those of the projection and the warm-up steps.
+profiled steps follow those of the projection and the warm-up steps; the
+NVTX range "timed_steps" brackets the profiled steps.
 """
 import argparse
 import json
@@ -20,6 +21,22 @@ import json
 from .config import grid_of, make_config
 from .workloads import log_profile_state, temperature_state
 from . import lib as L
+
+
+def nvtx_push(name):
+    try:
+        import torch
+        torch.cuda.nvtx.range_push(name)
+    except Exception:
+        pass
+
+
+def nvtx_pop():
+    try:
+        import torch
+        torch.cuda.nvtx.range_pop()
+    except Exception:
+        pass
 
 
 def main():
@@ -45,7 +62,9 @@ def main():
     d.project(1.0)
     if a.warmup:
         d.step(a.warmup)
+    nvtx_push("timed_steps")  # `ncu --nvtx --nvtx-include "timed_steps/"` selects these launches
     s = d.step(a.steps)
+    nvtx_pop()
     out = {"n": n, "precision": a.precision, "steps": a.steps, "ms_per_step": s.elapsed_ms / max(1, a.steps),
            "max_div": s.max_div, "kernels_per_step": s.kernels / max(1, a.steps)}
     if a.stage_times:

@@ -522,3 +522,33 @@ def test_dispersion_alone_and_in_batch(precision):
             assert np.array_equal(a, c)
         d.close()
     b.close()
+
+
+def test_long_run_mixed_matches_fp64():
+    """Config 0 for 1000 steps from one projected state on both paths: the
+    velocity of the mixed path stays within 1e-3 of the FP64 path, and the
+    vertical profiles of the mean velocity and of the resolved TKE, averaged
+    over steps 500..1000, agree within 1%."""
+    from gpu_elmm_b200.stats import Profiles, compare
+    n = (64, 64, 32)
+    g = grid_of(make_config(*n))
+    st = log_profile_state(g, seed=0)
+    d64 = L.Domain(make_config(*n))
+    d64.upload(*st)
+    d64.project(1.0)
+    dm = L.Domain(make_config(*n, precision=1))
+    dm.upload(*d64.download())
+    prof = {0: Profiles(g), 1: Profiles(g)}
+    done = 0
+    for target in range(500, 1001, 50):
+        for d in (d64, dm):
+            d.step(target - done)
+        done = target
+        for p, d in ((0, d64), (1, dm)):
+            prof[p].add(*d.download()[:3])
+    for a, b in zip(interiors(g, *dm.download())[:3], interiors(g, *d64.download())[:3]):
+        assert rel(a, b) < 1e-3
+    c = compare(prof[1].result(), prof[0].result())
+    assert c["u"] < 1e-2 and c["tke"] < 1e-2, c
+    d64.close()
+    dm.close()

@@ -31,3 +31,27 @@ def test_log_profile_state():
     assert (P == 0).all()
     # ghosts are left zero for the library / oracle to fill
     assert (U[:2] == 0).all() and (U[:, :, -3:] == 0).all()
+
+
+def test_profiles_of_a_known_field():
+    """Vertical profiles (src/vertical_profiles.f90): mean, resolved variance
+    and resolved TKE of a field with a known answer."""
+    import numpy as np
+    from gpu_elmm_b200.config import grid_of, make_config
+    from gpu_elmm_b200.stats import Profiles
+    from gpu_elmm_b200.workloads import interior
+    g = grid_of(make_config(8, 6, 5))
+    U, V, W = np.zeros(g.shape_u()), np.zeros(g.shape_v()), np.zeros(g.shape_w())
+    k = np.arange(1, g.Unz + 1)[:, None, None]
+    i = np.arange(1, g.Unx + 1)[None, None, :]
+    j = np.arange(1, g.Wny + 1)[None, :, None]
+    interior(U, -2, (g.Unx, g.Uny, g.Unz))[...] = k + 0.5 * (-1.0) ** i
+    interior(W, -2, (g.Wnx, g.Wny, g.Wnz))[...] = 0.3 * (-1.0) ** j
+    p = Profiles(g)
+    p.add(U, V, W)
+    p.add(U, V, W)
+    r = p.result()
+    assert np.allclose(r["u"], np.arange(1, g.Unz + 1)) and np.allclose(r["uu"], 0.25)
+    assert np.allclose(r["ww"][1:g.Wnz + 1], 0.09) and r["ww"][0] == 0 and r["ww"][g.Prnz] == 0
+    want = (0.25 + 0.0 + (r["ww"][:-1] + r["ww"][1:]) / 2) / 2
+    assert np.allclose(r["tke"], want)
