@@ -514,8 +514,14 @@ struct BatchT {
         CU(cudaMemcpy(r.ls.starts, st.data(), sizeof(int) * (nd + 1), cudaMemcpyHostToDevice));
         const void *f1 = ydir ? (const void *)r.k->yf : (const void *)r.k->fwd;
         const void *f2 = ydir ? (const void *)r.k->yi : (const void *)r.k->inv;
-        CU(cudaFuncSetAttribute(f1, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-        CU(cudaFuncSetAttribute(f2, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+        // the dynamic maximum leaves room for the kernel's static shared memory
+        for (const void *f : {f1, f2}) {
+          cudaFuncAttributes fa;
+          CU(cudaFuncGetAttributes(&fa, f));
+          if (r.smem + fa.sharedSizeBytes > (size_t)optin)
+            return fail(ELMM_ERR_INVALID_CONFIG, "shared memory of the register transforms exceeds the device limit");
+          CU(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes));
+        }
         r.cap_fwd = cap(f1, kRegThreads, r.smem);
         r.cap_inv = cap(f2, kRegThreads, r.smem);
         out.push_back(r);
@@ -689,14 +695,14 @@ struct BatchT {
     if ((r = upload_table(&h.At, At))) return r;
     if ((r = upload_table(&h.dzc, dzc))) return r;
     if ((r = upload_table(&h.dzf, dzf))) return r;
-    if (tri_tiled(h)) {  // reciprocal pivots of the tiled z solve, once per domain
+    if (tri_tiled(h)) {  // pivot carries of the tiled z solve at its segment starts, once per domain
       const int ncol = h.ny * h.spitch;
-      double *iv;
-      if ((r = dalloc((void **)&iv, (size_t)h.nz * ncol * sizeof(double)))) return r;
-      k_tri_factors<<<(ncol + 255) / 256, 256, 0, stream>>>(iv, h.lamx, h.lamy, h.Ab, h.At, h.nxh, h.spitch, h.ny, h.nz);
+      double *c0;
+      if ((r = dalloc((void **)&c0, (size_t)kTriPivSegs * ncol * sizeof(double)))) return r;
+      k_tri_factors<<<(ncol + 255) / 256, 256, 0, stream>>>(c0, h.lamx, h.lamy, h.Ab, h.At, h.nxh, h.spitch, h.ny, h.nz);
       CU(cudaStreamSynchronize(stream));
       CU(cudaGetLastError());
-      h.tri_iv = iv;
+      h.tri_c0 = c0;
     }
     if ((r = upload_table(&h.zPr, g.zPr))) return r;
     if ((r = upload_table(&h.dzPr, g.dzPr))) return r;

@@ -84,7 +84,7 @@ struct Dom {
   const T2 *twx, *twy;
   // Poisson tables (FP64): eigenvalues and z-operator rows, index 1..nz
   const double *lamx, *lamy, *Ab, *At, *dzc, *dzf;
-  const double *tri_iv;  // [nz][ny * spitch]: 1 / pivot of the Thomas sweep per mode (tiled z solve)
+  const double *tri_c0;  // [piece][ny * spitch]: carry of the pivot recurrence at each piece start (tiled z solve)
   int zper;
   // grid tables (FP64), index k + 2 for k in [-2, nz + 3]
   const double *zPr, *dzPr, *zW, *dzW;

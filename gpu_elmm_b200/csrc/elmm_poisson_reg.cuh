@@ -66,37 +66,103 @@ __device__ __forceinline__ T poisson_rhs(const Dom<T> &d, const RhsRow<T> &r, lo
 }
 
 // ------------------------------------------------------------ x forward
+// 16-byte vectors of a row: four floats or two doubles (rows start on a
+// 128-byte boundary and every register-FFT length is a multiple of 16)
+template <typename T> struct Row16;
+template <> struct Row16<float> {
+  static constexpr int n = 4;
+  static __device__ __forceinline__ void ld(const float *p, float (&v)[4]) {
+    const float4 q = __ldg(reinterpret_cast<const float4 *>(p));
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+  }
+};
+template <> struct Row16<double> {
+  static constexpr int n = 2;
+  static __device__ __forceinline__ void ld(const double *p, double (&v)[2]) {
+    const double2 q = __ldg(reinterpret_cast<const double2 *>(p));
+    v[0] = q.x; v[1] = q.y;
+  }
+};
+
 // Divergence + real FFT along x of 2 * NS rows (two real rows per complex
 // sequence), split into the half spectra of the two rows: S[row][0..nx/2].
+// The divergence is formed from 16-byte row vectors (a thread takes one
+// chunk of both rows of a sequence) into shared memory, from where each FFT
+// thread picks its strided elements; the arithmetic per cell is that of
+// poisson_rhs.
 template <typename T, int N>
 __device__ __forceinline__ void fftx_fwd_tile(const Dom<T> &d, int lt, typename Vec2<T>::type *smem, double coef,
                                               int rhs_from_phi) {
   typedef typename Vec2<T>::type T2;
   typedef FPlan<N> Pl;
+  typedef Row16<T> RV;
   constexpr int P = Pl::P, E = Pl::E, NS = kRegThreads / P;
+  constexpr int VE = RV::n, NCH = N / VE;
+  __shared__ RhsRow<T> rinfo[2 * NS];
   const int s = threadIdx.x / P, t = threadIdx.x - s * P;
   const int ny = d.ny, nrows = ny * d.nz;
-  const int ra = 2 * (lt * NS + s), rb = ra + 1;
-  const bool va = ra < nrows, vb = rb < nrows;
-  const int qa = va ? ra : 0, qb = vb ? rb : 0;  // rows past the end are not read
-  const int ka = qa / ny + 1, kb = qb / ny + 1;
-  const long long ca = bidx(d, 1, qa - (ka - 1) * ny + 1, ka), cb = bidx(d, 1, qb - (kb - 1) * ny + 1, kb);
+  const int r0 = 2 * lt * NS;  // first row of the tile; sequence q holds rows r0 + 2q, r0 + 2q + 1
   const T rdt2 = (T)(1.0 / coef);
   const T rdx = (T)(1.0 / d.dx), rdy = (T)(1.0 / d.dy), rdz = (T)(1.0 / d.dz);
-  const T rdza = (d.vz && va) ? (T)d.sgs_rdz[ka] : rdz, rdzb = (d.vz && vb) ? (T)d.sgs_rdz[kb] : rdz;
-  const RhsRow<T> rwa = rhs_row(d, qa - (ka - 1) * ny + 1, ka), rwb = rhs_row(d, qb - (kb - 1) * ny + 1, kb);
+  if (threadIdx.x < 2 * NS) {
+    const int q = min(r0 + (int)threadIdx.x, nrows - 1);
+    const int k = q / ny + 1;
+    rinfo[threadIdx.x] = rhs_row(d, q - (k - 1) * ny + 1, k);
+  }
+  __syncthreads();
+  for (int task = threadIdx.x; task < NS * NCH; task += kRegThreads) {
+    const int sq = task / NCH, c = task - sq * NCH;
+    T va[VE], vb[VE];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      T *out = h ? vb : va;
+      const int q = r0 + 2 * sq + h;
+#pragma unroll
+      for (int e = 0; e < VE; e++) out[e] = (T)0;
+      if (q >= nrows) continue;  // rows past the end are not read
+      const int k = q / ny + 1, j = q - (k - 1) * ny + 1;
+      const long long c0 = bidx(d, 1, j, k) + (long long)c * VE;
+      if (rhs_from_phi) {
+        T p[VE];
+        RV::ld(d.Phi + c0, p);
+#pragma unroll
+        for (int e = 0; e < VE; e++) out[e] = p[e] * rdt2;
+        continue;
+      }
+      const RhsRow<T> &r = rinfo[2 * sq + h];
+      const T rdzk = d.vz ? (T)d.sgs_rdz[k] : rdz;
+      T uc[VE], vc[VE], vs[VE], wc[VE], wb[VE];
+      RV::ld(d.U2 + c0, uc);
+      RV::ld(d.V2 + c0, vc);
+      RV::ld(d.V2 + c0 + r.o_vs, vs);
+      RV::ld(d.W2 + c0 + r.o_wc, wc);
+      RV::ld(d.W2 + c0 + r.o_wb, wb);
+      const T uw0 = c == 0 ? r.s_uw1 * ld((const T *)d.U2, c0 + r.o_uw1) : ld((const T *)d.U2, c0 - 1);
+#pragma unroll
+      for (int e = 0; e < VE; e++) {
+        const T uw = e == 0 ? uw0 : uc[e - 1];
+        const T vse = r.s_vs * vs[e];
+        const T wce = r.s_wc * wc[e], wbe = r.s_wb * wb[e];
+        const T div = (uc[e] - uw) * rdx + (vc[e] - vse) * rdy + (wce - wbe) * rdzk;
+        out[e] = div * rdt2;
+      }
+    }
+    T2 *dst = smem + sq * Pl::SEQ + c * VE;
+#pragma unroll
+    for (int e = 0; e < VE; e++) dst[e] = T2{va[e], vb[e]};
+  }
+  __syncthreads();
+  T2 *sh = smem + s * Pl::SEQ;
   T2 v[E];
 #pragma unroll
-  for (int e = 0; e < E; e++) {
-    const int i = t + P * e + 1;
-    v[e].x = va ? poisson_rhs(d, rwa, ca + i - 1, i, rdx, rdy, rdza, rdt2, rhs_from_phi) : (T)0;
-    v[e].y = vb ? poisson_rhs(d, rwb, cb + i - 1, i, rdx, rdy, rdzb, rdt2, rhs_from_phi) : (T)0;
-  }
-  T2 *sh = smem + s * Pl::SEQ;
+  for (int e = 0; e < E; e++) v[e] = sh[t + P * e];
+  __syncthreads();  // fft_reg writes sh
   fft_reg<T, T2, N, false>(v, sh, t, d.twx);
   // Z = FFT(a + i b): A_m = (Z_m + conj Z_{N-m}) / 2, B_m = (Z_m - conj Z_{N-m}) / 2i
+  const int ra = r0 + 2 * s, rb = ra + 1;
+  const bool va_ok = ra < nrows, vb_ok = rb < nrows;
   constexpr int nxh = N / 2 + 1;
-  T2 *Sa = d.S + (long long)qa * d.spitch, *Sb = d.S + (long long)qb * d.spitch;
+  T2 *Sa = d.S + (long long)(va_ok ? ra : 0) * d.spitch, *Sb = d.S + (long long)(vb_ok ? rb : 0) * d.spitch;
 #pragma unroll
   for (int m = t; m < nxh; m += P) {
     const T2 zk = sh[m], zc = sh[m == 0 ? 0 : N - m];
@@ -105,10 +171,10 @@ __device__ __forceinline__ void fftx_fwd_tile(const Dom<T> &d, int lt, typename 
     A.y = (zk.y - zc.y) * (T)0.5;
     B.x = (zk.y + zc.y) * (T)0.5;
     B.y = (zc.x - zk.x) * (T)0.5;
-    if (va) Sa[m] = A;
-    if (vb) Sb[m] = B;
+    if (va_ok) Sa[m] = A;
+    if (vb_ok) Sb[m] = B;
   }
-  __syncthreads();  // the next tile reuses sh
+  __syncthreads();  // the next tile reuses sh and rinfo
 }
 
 // One launch per x length N: the launch set holds only the domains with
@@ -253,8 +319,10 @@ __host__ __device__ constexpr int fft_reg_batch(int n) { return kRegThreads / fp
 // ------------------------------------------------- tiled tridiagonal solve
 // The z solve of every (kx, ky) mode (Thomas algorithm, non-periodic z) for
 // kTriCols consecutive spectral columns.  The pivots of the forward sweep
-// depend on the grid only, so their reciprocals iv(k) are computed once per
-// domain (k_tri_factors).  With them both sweeps are first-order linear
+// depend on the grid only: k_tri_factors stores, once per domain, the pivot
+// recurrence's carry at the first level of each segment, from which the
+// tile rebuilds the reciprocals iv(k) of its segment in shared memory (the
+// same operations, so the same values).  With them both sweeps are first-order linear
 // recurrences,
 //   forward   y(k) = r(k) iv(k) - Ab(k) iv(k) y(k-1),
 //   backward  x(k) = y(k) - At(k) iv(k) x(k+1),
@@ -262,11 +330,17 @@ __host__ __device__ constexpr int fft_reg_batch(int n) { return kRegThreads / fp
 // kTriSegs threads per part: each thread composes the affine map of its
 // segment of k, the segment maps are chained through shared memory, and each
 // thread then replays its segment from the exact entry value.  The tile of S
-// and of iv is copied into shared memory with cp.async first and written
-// back at the end.  The (0,0) mode is the zero-mean prefix-sum solution of
+// is copied into shared memory with cp.async (while the pivots are rebuilt)
+// and written back at the end.  The (0,0) mode is the zero-mean prefix-sum solution of
 // the generic kernel, k_tri.
-constexpr int kTriCols = 32;
-constexpr int kTriSegs = 4;
+#ifndef ELMM_TRI_COLS
+#define ELMM_TRI_COLS 16
+#endif
+#ifndef ELMM_TRI_SEGS
+#define ELMM_TRI_SEGS 8
+#endif
+constexpr int kTriCols = ELMM_TRI_COLS;
+constexpr int kTriSegs = ELMM_TRI_SEGS;
 constexpr int kTriTileThreads = 2 * kTriCols * kTriSegs;
 constexpr int kTriTileMaxNz = 256;
 
@@ -281,8 +355,33 @@ __host__ __device__ constexpr size_t tri_tile_smem(int nz) {
   return (size_t)nz * kTriCols * (2 * sizeof(T) + sizeof(double)) + 2 * sizeof(double) * kTriSegs * 2 * kTriCols;
 }
 
-// iv[(k-1) * ncol + col] = 1 / pivot(k) of mode col = ky * spitch + kx
-__global__ void k_tri_factors(double *iv, const double *__restrict__ lamx, const double *__restrict__ lamy,
+// One step of the pivot recurrence of the forward sweep: the reciprocal
+// pivot iv(k) of a mode with eigenvalue lam, and c(k) = At(k) iv(k) carried
+// to k + 1.
+__device__ __forceinline__ double tri_pivot(const double *__restrict__ Ab, const double *__restrict__ At, int k,
+                                            double lam, double &cprev) {
+  const double den = (-(Ab[k] + At[k]) + lam) - (k > 1 ? Ab[k] * cprev : 0.0);
+  const double v = 1.0 / den;
+  cprev = At[k] * v;
+  return v;
+}
+
+// the first level of segment seg of the tiled z solve (segments of
+// ceil(nz / kTriSegs) levels)
+__host__ __device__ __forceinline__ int tri_seg_begin(int nz, int seg) {
+  return 1 + seg * ((nz + kTriSegs - 1) / kTriSegs);
+}
+// the pivots are rebuilt in twice as many pieces: both threads of a column
+// and segment take one half
+constexpr int kTriPivSegs = 2 * kTriSegs;
+__host__ __device__ __forceinline__ int tri_piv_begin(int nz, int p) {
+  return 1 + p * ((nz + kTriPivSegs - 1) / kTriPivSegs);
+}
+
+// c0[p * ncol + col]: c(kb - 1) of mode col = ky * spitch + kx at the first
+// level kb of each pivot piece p (0 for the first); the tiled solve rebuilds
+// the reciprocal pivots of its pieces from it
+__global__ void k_tri_factors(double *c0, const double *__restrict__ lamx, const double *__restrict__ lamy,
                               const double *__restrict__ Ab, const double *__restrict__ At, int nxh, int spitch, int ny,
                               int nz) {
   const int ncol = ny * spitch;
@@ -291,15 +390,12 @@ __global__ void k_tri_factors(double *iv, const double *__restrict__ lamx, const
     const bool mode = kx < nxh && !(kx == 0 && ky == 0);
     const double lam = mode ? lamx[kx] + lamy[ky] : 0.0;
     double cprev = 0;
+    int p = 0;
     for (int k = 1; k <= nz; k++) {
-      double v = 0;
-      if (mode) {
-        const double den = (-(Ab[k] + At[k]) + lam) - (k > 1 ? Ab[k] * cprev : 0.0);
-        v = 1.0 / den;
-        cprev = At[k] * v;
-      }
-      iv[(long long)(k - 1) * ncol + col] = v;
+      while (p < kTriPivSegs && tri_piv_begin(nz, p) == k) c0[(long long)(p++) * ncol + col] = mode ? cprev : 0.0;
+      if (mode) tri_pivot(Ab, At, k, lam, cprev);
     }
+    for (; p < kTriPivSegs; p++) c0[(long long)p * ncol + col] = 0.0;  // empty pieces
   }
 }
 
@@ -308,7 +404,6 @@ __global__ void __launch_bounds__(kTriTileThreads) k_tri_tile(const Dom<T> *__re
   typedef typename Vec2<T>::type T2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int kChunk = 16 / (int)sizeof(T2), kPerRow = kTriCols / kChunk, XS = 2 * kTriCols;
-  constexpr int kIvPerRow = kTriCols / 2;  // 16-byte copies of the reciprocals per k
   constexpr int NP = 2 * kTriCols;         // systems (column parts) per tile
   for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
     const int di = find_dom(L.starts, L.nd, t);
@@ -322,28 +417,35 @@ __global__ void __launch_bounds__(kTriTileThreads) k_tri_tile(const Dom<T> *__re
     double *ivs = reinterpret_cast<double *>(smem_raw + (size_t)nz * kTriCols * sizeof(T2));  // [nz][kTriCols]
     double *mapA = ivs + (size_t)nz * kTriCols;                                              // [kTriSegs][NP]
     double *mapB = mapA + kTriSegs * NP;
+    const double *Ab = d.Ab, *At = d.At;
     for (int q = threadIdx.x; q < nz * kPerRow; q += kTriTileThreads) {
       const int k = q / kPerRow, c = (q - k * kPerRow) * kChunk;
       if (col0 + c < ncol) cp_async16(tile + k * kTriCols + c, d.S + k * ps + col0 + c);
     }
-    for (int q = threadIdx.x; q < nz * kIvPerRow; q += kTriTileThreads) {
-      const int k = q / kIvPerRow, c = (q - k * kIvPerRow) * 2;
-      if (col0 + c < ncol) cp_async16(ivs + k * kTriCols + c, d.tri_iv + k * ps + col0 + c);
-    }
-    cp_async_wait_all();
-    __syncthreads();
     const int sys = threadIdx.x % NP, seg = threadIdx.x / NP;
     const int c = sys >> 1;  // column; sys & 1 selects the real or imaginary part
     const int col = col0 + c, ky = col / d.spitch, kx = col - ky * d.spitch;
     const bool active = col < ncol && kx < d.nxh;
     const bool zero_mode = kx == 0 && ky == 0;
     const bool solve = active && !zero_mode;
+    const int len = (nz + kTriSegs - 1) / kTriSegs;
+    const int kb = tri_seg_begin(nz, seg), ke = min(nz, kb + len - 1);  // this thread's segment, kb > ke if empty
+    // the reciprocal pivots of the column, rebuilt piece by piece from the
+    // stored carries (each thread of the column takes one piece) while the
+    // tile of S lands
+    if (col < ncol) {
+      const int p = 2 * seg + (sys & 1);
+      const int pl = (nz + kTriPivSegs - 1) / kTriPivSegs;
+      const int pb = tri_piv_begin(nz, p), pe = min(nz, pb + pl - 1);
+      double cprev = d.tri_c0[(long long)p * ncol + col];
+      const double lam = solve ? d.lamx[kx] + d.lamy[ky] : 0.0;
+      for (int k = pb; k <= pe; k++) ivs[(k - 1) * kTriCols + c] = solve ? tri_pivot(Ab, At, k, lam, cprev) : 0.0;
+    }
+    cp_async_wait_all();
+    __syncthreads();
     T *x = reinterpret_cast<T *>(tile) + sys;  // element k - 1 at x[(k - 1) * XS]
     const double *iv = ivs + c;                // element k - 1 at iv[(k - 1) * kTriCols]
     const double norm = 1.0 / ((double)d.nx * (double)d.ny);
-    const double *Ab = d.Ab, *At = d.At;
-    const int len = (nz + kTriSegs - 1) / kTriSegs;
-    const int kb = 1 + seg * len, ke = min(nz, kb + len - 1);  // this thread's segment, kb > ke if empty
     // forward: y(k) = a(k) + b(k) y(k-1), a = r norm iv, b = -Ab iv (b(1) = 0)
     double A = 0, B = 1;
     if (solve)
