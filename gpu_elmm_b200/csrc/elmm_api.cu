@@ -250,7 +250,7 @@ struct LaunchSet {
 };
 
 enum { LK_CELLS = 0, LK_BOX, LK_ROWS, LK_YCOLS, LK_TRI, LK_MOM, LK_SHELL, LK_XREG, LK_YREG, LK_TRIT, LK_TCOL, LK_DCOL,
-       LK_AVG, LK_COMMIT, LK_TPAIR, LK_N };
+       LK_AVG, LK_COMMIT, LK_TPAIR, LK_PROJ, LK_PROJ2, LK_N };
 
 // -------------------------------------------------------------------- batch
 template <typename T>
@@ -486,6 +486,7 @@ struct BatchT {
     grid_cap[4] = cap((const void *)k_tri<T>, kTriThreads, smem_tri);
     grid_cap[5] = cap((const void *)k_fftx_inv<T>, kFFTThreads, smem_x);
     grid_cap[6] = cap((const void *)k_project<T>, MX * MY, 0);
+    grid_cap[10] = std::is_same<T, float>::value ? cap((const void *)k_project_pair, MX * MY / 2, 0) : 1;
     grid_cap[7] = cap((const void *)k_divres<T>, TX * TY, 0);
     grid_cap[8] = cap((const void *)k_cfl<T>, TX * TY, 0);
     grid_cap[9] = cap((const void *)k_ghosts<T>, kShellThreads, 0);
@@ -558,6 +559,8 @@ struct BatchT {
   // the FP32 scalar stage runs two cells per thread when the pairs tile the
   // periodic x axis
   static bool scalar_pairs(const Dom<T> &h) { return sizeof(T) == 4 && h.nx % 2 == 0; }
+  // the same for the projection (the velocity is periodic in x for every domain)
+  static bool fp32_pairs(const Dom<T> &h) { return sizeof(T) == 4 && h.nx % 2 == 0 && h.bt[SIDE_WE] == BC_PERIODIC; }
 
   static int tiles(int kind, const Dom<T> &h) {
     int ntx = (h.nx + TX - 1) / TX, nty = (h.ny + TY - 1) / TY;
@@ -567,6 +570,8 @@ struct BatchT {
       case LK_ROWS: return fft_reg_supported(h.nx) ? 0 : (h.ny * h.nz + kRowsX - 1) / kRowsX;
       case LK_YCOLS: return fft_reg_supported(h.ny) ? 0 : ((h.nxh + TyOf<T>::v - 1) / TyOf<T>::v) * h.nz;
       case LK_MOM: return ((h.nx + MX - 1) / MX) * ((h.ny + MY - 1) / MY) * ((h.nz + MKC - 1) / MKC);
+      case LK_PROJ: return fp32_pairs(h) ? 0 : tiles(LK_MOM, h);
+      case LK_PROJ2: return fp32_pairs(h) ? tiles(LK_MOM, h) : 0;
       case LK_SHELL: return (int)((shell_cells(h.nx, h.ny, h.nz) + kShellThreads - 1) / kShellThreads);
       case LK_XREG: {
         if (!fft_reg_supported(h.nx)) return 0;
@@ -829,11 +834,25 @@ struct BatchT {
     return ELMM_OK;
   }
   void launch_project(double coef_alpha2, int use_dt, int in_place, int gate) {
-    nlaunch += 2;
-    k_project<T><<<gsz(6, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l(), coef_alpha2, use_dt,
-                                                                   in_place, gate);
+    nlaunch++;  // k_prref; the projection kernels count themselves
+    k_project_any(coef_alpha2, use_dt, in_place, gate);
     launch_ghosts({F_U, F_V, F_W, F_P}, gate);
     k_prref<T><<<std::min(nd, 1024), 256, 0, stream>>>(ddom, nd, gate);
+  }
+  // k_project for the domains that take it, k_project_pair (FP32, even Prnx) for the others
+  void k_project_any(double coef_alpha2, int use_dt, int in_place, int gate) {
+    if (ls[LK_PROJ].total > 0) {
+      nlaunch++;
+      k_project<T><<<gsz(6, ls[LK_PROJ].total), MX * MY, 0, stream>>>(ddom, ls[LK_PROJ].l(), coef_alpha2, use_dt,
+                                                                       in_place, gate);
+    }
+    if constexpr (std::is_same<T, float>::value) {
+      if (ls[LK_PROJ2].total > 0) {
+        nlaunch++;
+        k_project_pair<<<gsz(10, ls[LK_PROJ2].total), MX * MY / 2, 0, stream>>>(ddom, ls[LK_PROJ2].l(), coef_alpha2,
+                                                                               use_dt, in_place, gate);
+      }
+    }
   }
   // one ScalarRK3 stage of every transported scalar; the new values then
   // become the current ones (the stage reads the old value at neighbours
@@ -1123,7 +1142,7 @@ struct BatchT {
       timed(4, [&] { launch_tri(0); });
       timed(5, [&] { launch_ffty(1, 0); });
       timed(6, [&] { launch_fftx_inv(0); });
-      timed(7, [&] { k_project<T><<<gsz(6, ls[LK_MOM].total), MX * MY, 0, stream>>>(ddom, ls[LK_MOM].l(), a2, 1, 0, 0); });
+      timed(7, [&] { k_project_any(a2, 1, 0, 0); });
       timed(kGhost, [&] { launch_ghosts({F_U, F_V, F_W, F_P}, 0); });
       timed(8, [&] { k_prref<T><<<std::min(nd, 1024), 256, 0, stream>>>(ddom, nd, 0); });
       timed(10, [&] { launch_scalars(stage, 0); });

@@ -157,6 +157,111 @@ __global__ void __launch_bounds__(MX *MY) k_project(const Dom<T> *__restrict__ d
   }
 }
 
+// k_project for FP32 domains with an even Prnx (x is periodic for every
+// domain): two x-adjacent cells per thread, float2 loads and stores, the
+// same tiles (MX x MY x MKC) and partial sums per tile column.
+__global__ void __launch_bounds__(MX *MY / 2) k_project_pair(const Dom<float> *__restrict__ doms, Launch L,
+                                                          double coef_alpha2, int use_dt, int in_place, int gate) {
+  typedef float T;
+  __shared__ double red[MX * MY / 64];
+  for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
+    const int di = find_dom(L.starts, L.nd, t);
+    const Dom<T> &d = doms[di];
+    if (gate && !*d.refine_flag) continue;
+    int lt = t - __ldg(L.starts + di);
+    const int ntx = (d.nx + MX - 1) / MX, nty = (d.ny + MY - 1) / MY;
+    const int bx = lt % ntx; lt /= ntx;
+    const int by = lt % nty;
+    const int bk = lt / nty;
+    const int k0 = bk * MKC + 1, k1 = min(k0 + MKC - 1, d.nz);
+    const int i = bx * MX + 2 * (threadIdx.x % (MX / 2)) + 1;  // odd: the pair is 8-byte aligned
+    const int j = by * MY + (threadIdx.x / (MX / 2)) + 1;
+    const int nx = d.nx, ny = d.ny, nz = d.nz;
+    const bool inside = i <= nx && j <= ny;  // nx even: i + 1 <= nx too
+    const double coef = use_dt ? coef_alpha2 * d.dt : coef_alpha2;
+    const T dt2 = (T)coef;
+    const T Au = (T)(coef / d.dx), Av = (T)(coef / d.dy), Aw = (T)(coef / d.dz);
+    const T *__restrict__ Usrc = in_place ? d.U : d.U2;
+    const T *__restrict__ Vsrc = in_place ? d.V : d.V2;
+    const T *__restrict__ Wsrc = in_place ? d.W : d.W2;
+    const T *__restrict__ Phi = d.Phi;
+    T *__restrict__ P = d.P;
+    const long long pitch = d.pitch, plane = d.plane;
+    const bool hu = inside && j <= d.ext[0][1], hv = inside && j <= d.ext[1][1], hw = inside && j <= d.ext[2][1];
+    const T m = (T)(*d.prm);
+    long long c = bidx(d, inside ? i : 1, inside ? j : 1, k0);
+    // Phi at i+2 (the second cell's x neighbour), j+1, k+1, folded as Bound_Phi fills the ghosts
+    const bool px = d.bt[SIDE_WE] == BC_PERIODIC, py = d.bt[SIDE_SO] == BC_PERIODIC, pz = d.bt[SIDE_BO] == BC_PERIODIC;
+    const bool last = i + 1 >= nx;
+    const long long oe = !last ? 2 : (px ? 1 - i : 0);  // the neighbour pair; for a wall, the cell itself
+    const long long on = j < ny ? pitch : (py ? pitch - (long long)ny * pitch : 0);
+    auto ot = [&](int kk) -> long long { return kk < nz ? plane : (pz ? plane - (long long)nz * plane : 0); };
+    auto ld2 = [](const T *p, long long o) { return __ldg(reinterpret_cast<const float2 *>(p + o)); };
+    float2 phi = {0, 0}, pe = {0, 0}, pn = {0, 0}, pt = {0, 0}, u0 = {0, 0}, v0 = {0, 0}, w0 = {0, 0}, p0 = {0, 0};
+    auto east = [&](const float2 &own, long long cc) {
+      const float2 nb = ld2(Phi, cc + oe);
+      return make_float2(own.y, (last && !px) ? own.y : nb.x);
+    };
+    if (inside) {
+      phi = ld2(Phi, c);
+      pe = east(phi, c);
+      pn = ld2(Phi, c + on);
+      pt = ld2(Phi, c + ot(k0));
+      if (hu) u0 = ld2(Usrc, c);
+      if (hv) v0 = ld2(Vsrc, c);
+      if (hw) w0 = ld2(Wsrc, c);
+      p0 = *reinterpret_cast<const float2 *>(P + c);
+    }
+    for (int k = k0; k <= k1; k++) {
+      const bool more = k + 1 <= k1;
+      float2 npe = {0, 0}, npn = {0, 0}, npt = {0, 0}, nu0 = {0, 0}, nv0 = {0, 0}, nw0 = {0, 0}, np0 = {0, 0};
+      if (more && inside) {
+        const long long cn = c + plane;
+        npe = east(pt, cn);
+        npn = ld2(Phi, cn + on);
+        npt = ld2(Phi, cn + ot(k + 1));
+        if (hu) nu0 = ld2(Usrc, cn);
+        if (hv) nv0 = ld2(Vsrc, cn);
+        if (hw) nw0 = ld2(Wsrc, cn);
+        np0 = *reinterpret_cast<const float2 *>(P + cn);
+      }
+      double top = 0;
+      if (inside) {
+        if (hu && k <= d.ext[0][2])
+          *reinterpret_cast<float2 *>(d.U + c) = make_float2(u0.x - Au * (pe.x - phi.x), u0.y - Au * (pe.y - phi.y));
+        if (hv && k <= d.ext[1][2])
+          *reinterpret_cast<float2 *>(d.V + c) = make_float2(v0.x - Av * (pn.x - phi.x), v0.y - Av * (pn.y - phi.y));
+        if (hw && k <= d.ext[2][2]) {
+          float2 w;
+          if (d.vz) {
+            const T dzw = (T)d.dzW[k + 2];
+            w = make_float2(w0.x - dt2 * (pt.x - phi.x) / dzw, w0.y - dt2 * (pt.y - phi.y) / dzw);
+          } else {
+            w = make_float2(w0.x - Aw * (pt.x - phi.x), w0.y - Aw * (pt.y - phi.y));
+          }
+          *reinterpret_cast<float2 *>(d.W + c) = w;
+        }
+        const float2 p = make_float2((p0.x - m) + phi.x, (p0.y - m) + phi.y);
+        *reinterpret_cast<float2 *>(P + c) = p;
+        top = (double)p.x + (double)p.y;
+      }
+      if (k == nz) {  // block-uniform: the top layer's partial sum of this column
+        for (int o = 16; o > 0; o >>= 1) top += __shfl_down_sync(0xffffffffu, top, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = top;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          double sum = 0;
+          for (int w = 0; w < MX * MY / 64; w++) sum += red[w];
+          d.prpart[by * ntx + bx] = sum;
+        }
+        __syncthreads();
+      }
+      phi = pt; pe = npe; pn = npn; pt = npt; u0 = nu0; v0 = nv0; w0 = nw0; p0 = np0;
+      c += plane;
+    }
+  }
+}
+
 // FixPressureToReference, reference at side To (src/pressure.f90:1160-1229):
 // the new reference is the mean of the top layer; it is applied lazily,
 // every reader of P subtracts it.
