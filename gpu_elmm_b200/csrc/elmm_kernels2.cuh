@@ -122,22 +122,33 @@ __global__ void __launch_bounds__(MX *MY) k_project(const Dom<T> *__restrict__ d
       }
       double top = 0;
       if (inside) {
+        // x is periodic: the end cells of a row also write their ghost
+        // images (the ghost pass covers y and z)
+        const bool g1 = i == 1, gn = i == nx;
+        auto ghost = [&](T *F, T v) {
+          if (g1) F[c + nx] = v;
+          if (gn) F[c - nx] = v;
+        };
         if (hu && k <= d.ext[0][2]) {
           T u = u0 - Au * (pe - phi);
           d.U[c] = u;
+          ghost(d.U, u);
         }
         if (hv && k <= d.ext[1][2]) {
           T v = v0 - Av * (pn - phi);
           d.V[c] = v;
+          ghost(d.V, v);
         }
         if (hw && k <= d.ext[2][2]) {
           T w;
           if (d.vz) w = w0 - dt2 * (pt - phi) / (T)d.dzW[k + 2];
           else w = w0 - Aw * (pt - phi);
           d.W[c] = w;
+          ghost(d.W, w);
         }
         T p = (p0 - m) + phi;
         P[c] = p;
+        ghost(P, p);
         top = (double)p;
       }
       if (k == nz) {  // block-uniform: the top layer's partial sum of this column
@@ -227,10 +238,23 @@ __global__ void __launch_bounds__(MX *MY / 2) k_project_pair(const Dom<float> *_
       }
       double top = 0;
       if (inside) {
-        if (hu && k <= d.ext[0][2])
-          *reinterpret_cast<float2 *>(d.U + c) = make_float2(u0.x - Au * (pe.x - phi.x), u0.y - Au * (pe.y - phi.y));
-        if (hv && k <= d.ext[1][2])
-          *reinterpret_cast<float2 *>(d.V + c) = make_float2(v0.x - Av * (pn.x - phi.x), v0.y - Av * (pn.y - phi.y));
+        // periodic x ghost images of the row's end cells (the ghost pass
+        // covers y and z): cell 1 -> column nx + 1, cell nx -> column 0
+        const bool g1 = i == 1, gn = i + 1 == nx;
+        auto ghost = [&](T *F, const float2 &v) {
+          if (g1) F[c + nx] = v.x;
+          if (gn) F[c + 1 - nx] = v.y;
+        };
+        if (hu && k <= d.ext[0][2]) {
+          const float2 u = make_float2(u0.x - Au * (pe.x - phi.x), u0.y - Au * (pe.y - phi.y));
+          *reinterpret_cast<float2 *>(d.U + c) = u;
+          ghost(d.U, u);
+        }
+        if (hv && k <= d.ext[1][2]) {
+          const float2 v = make_float2(v0.x - Av * (pn.x - phi.x), v0.y - Av * (pn.y - phi.y));
+          *reinterpret_cast<float2 *>(d.V + c) = v;
+          ghost(d.V, v);
+        }
         if (hw && k <= d.ext[2][2]) {
           float2 w;
           if (d.vz) {
@@ -240,9 +264,11 @@ __global__ void __launch_bounds__(MX *MY / 2) k_project_pair(const Dom<float> *_
             w = make_float2(w0.x - Aw * (pt.x - phi.x), w0.y - Aw * (pt.y - phi.y));
           }
           *reinterpret_cast<float2 *>(d.W + c) = w;
+          ghost(d.W, w);
         }
         const float2 p = make_float2((p0.x - m) + phi.x, (p0.y - m) + phi.y);
         *reinterpret_cast<float2 *>(P + c) = p;
+        ghost(P, p);
         top = (double)p.x + (double)p.y;
       }
       if (k == nz) {  // block-uniform: the top layer's partial sum of this column
@@ -286,8 +312,9 @@ __global__ void k_prref(const Dom<T> *__restrict__ doms, int nd, int gate) {
 }
 
 // Ghost shell of up to four box fields, pulled from the interior after the
-// kernel that wrote it: every one-deep ghost cell takes the value of the
-// interior cell it folds onto.  Velocities follow BoundUVW
+// kernel that wrote it: every one-deep ghost cell of the y and z faces takes
+// the value of the interior cell it folds onto (the periodic x images are
+// written by the producers: k_sgs, k_project, k_project_pair).  Velocities follow BoundUVW
 // (src/boundaries.f90:398-1791; the sequential x, y, z passes there make the
 // fold a product of per-dimension folds), viscosity and Phi a periodic or
 // adjacent-cell copy (src/scalarboundaries.f90:326-431,
@@ -312,9 +339,11 @@ __device__ __forceinline__ T *box_field(const Dom<T> &d, int f) {
   }
 }
 
-// cells of the one-deep shell around an ex x ey x ez interior
+// cells of the one-deep shell around an ex x ey x ez interior, without the
+// x faces (j in 1..ey, k in 1..ez): x is periodic for every domain and the
+// producers of the fields with a ghost pass write those images themselves
 __host__ __device__ __forceinline__ long long shell_cells(int ex, int ey, int ez) {
-  return 2LL * (ex + 2) * (ey + 2) + 2LL * (ex + 2) * ez + 2LL * ey * ez;
+  return 2LL * (ex + 2) * (ey + 2) + 2LL * (ex + 2) * ez;
 }
 
 template <typename T>
@@ -332,22 +361,18 @@ __global__ void __launch_bounds__(kShellThreads) k_ghosts(const Dom<T> *__restri
     const int ex = vel ? d.ext[comp][0] : d.nx, ey = vel ? d.ext[comp][1] : d.ny, ez = vel ? d.ext[comp][2] : d.nz;
     int w = (t - __ldg(L.starts + di)) * kShellThreads + threadIdx.x;
     if (w >= (int)shell_cells(ex, ey, ez)) continue;
-    // z faces (full planes), then y faces (k in 1..ez), then x faces
+    // z faces (full planes), then y faces (k in 1..ez)
     int i, j, k;
-    const int rx = ex + 2, zf = rx * (ey + 2), yf = rx * ez, xf = ey * ez;
+    const int rx = ex + 2, zf = rx * (ey + 2), yf = rx * ez;
     if (w < 2 * zf) {
       const int side = w >= zf;
       w -= side * zf;
       j = w / rx; i = w - j * rx; k = side ? ez + 1 : 0;
-    } else if ((w -= 2 * zf) < 2 * yf) {
+    } else {
+      w -= 2 * zf;
       const int side = w >= yf;
       w -= side * yf;
       k = w / rx; i = w - k * rx; k += 1; j = side ? ey + 1 : 0;
-    } else {
-      w -= 2 * yf;
-      const int side = w >= xf;
-      w -= side * xf;
-      k = w / ey; j = w - k * ey + 1; k += 1; i = side ? ex + 1 : 0;
     }
     T *F = box_field(d, fid);
     const bool per[3] = {d.bt[SIDE_WE] == BC_PERIODIC, d.bt[SIDE_SO] == BC_PERIODIC, d.bt[SIDE_BO] == BC_PERIODIC};

@@ -768,6 +768,9 @@ __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
           F2 v = nusmag2(q, R2);
           if (addmol) v = v + bc2(num);
           *reinterpret_cast<float2 *>(nu + c) = v.v;
+          // the periodic x ghosts of the row's end cells (the ghost pass covers y and z)
+          if (i == 1) nu[c + nx] = v.v.x;
+          if (i + 1 == nx) nu[c + 1 - nx] = v.v.y;
           if (buoy) {
             const float2 td = init ? make_float2((v.v.x - num) / 0.6f + kap, (v.v.y - num) / 0.6f + kap)
                                    : make_float2(tdiff_of(v.v.x, num, kap), tdiff_of(v.v.y, num, kap));
@@ -787,6 +790,8 @@ __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
             if (addmol) v = v + num;
           }
           nu[c + qc] = v;
+          if (i + qc == 1) nu[c + qc + nx] = v;  // periodic x ghosts (the ghost pass covers y and z)
+          if (i + qc == nx) nu[c + qc - nx] = v;
           if (buoy) d.TDiff[c + qc] = init ? (v - num) / (T)0.6 + kap : tdiff_of(v, num, kap);
         }
       }
