@@ -55,3 +55,30 @@ def test_profiles_of_a_known_field():
     assert np.allclose(r["ww"][1:g.Wnz + 1], 0.09) and r["ww"][0] == 0 and r["ww"][g.Prnz] == 0
     want = (0.25 + 0.0 + (r["ww"][:-1] + r["ww"][1:]) / 2) / 2
     assert np.allclose(r["tke"], want)
+
+
+def test_vtk_frames_round_trip(tmp_path):
+    """Frames and slices in the reference's legacy-VTK layout (float32
+    big-endian rectilinear grids, src/outputs.f90:2260-2300) read back to the
+    FP32-rounded fields on the right staggered coordinates."""
+    import numpy as np
+    from gpu_elmm_b200.config import grid_of, make_config
+    from gpu_elmm_b200.vtk import read_rectilinear, write_scalar_slices, write_uvw
+    from gpu_elmm_b200.workloads import interior, log_profile_state
+    g = grid_of(make_config(8, 6, 5))
+    U, V, W, Pr = log_profile_state(g, seed=4)
+    write_uvw(g, U, V, W, str(tmp_path / "frame_"))
+    (x, y, z), f = read_rectilinear(str(tmp_path / "frame_W.vtk"))
+    assert np.allclose(z, np.arange(1, g.Wnz + 1)) and np.allclose(x, np.arange(1, 9) - 0.5)
+    assert np.array_equal(f["W"], interior(W, -2, (g.Wnx, g.Wny, g.Wnz)).astype(np.float32))
+    raw = open(tmp_path / "frame_U.vtk", "rb").read()
+    assert raw.startswith(b"# vtk DataFile Version 2.0\n") and b"DATASET RECTILINEAR_GRID\n" in raw
+    first = interior(U, -2, (g.Unx, g.Uny, g.Unz))[0, 0, 0]
+    assert np.array([first], dtype=">f4").tobytes() in raw  # big-endian float32
+    xy = np.arange(48.0).reshape(6, 8)
+    xz = np.arange(40.0).reshape(5, 8)
+    write_scalar_slices(g, xy, xz, 3, 2, str(tmp_path / "c"))
+    (_, _, zz), f = read_rectilinear(str(tmp_path / "c_xy.vtk"))
+    assert np.allclose(zz, [2.5]) and np.array_equal(f["scalar01_avg"][0], xy.astype(np.float32))
+    (_, yy, _), f = read_rectilinear(str(tmp_path / "c_xz.vtk"))
+    assert np.allclose(yy, [1.5]) and np.array_equal(f["scalar01_avg"][:, 0, :], xz.astype(np.float32))
