@@ -448,7 +448,8 @@ def batched_leg(args, ws, rank, local):
         ms = allreduce_max(st.elapsed_ms, ws)
         cells = allreduce_sum(float(b.cells()), ws)
         out[name] = {"value": cells * steps / (ms / 1e3), "unit": "cell-steps/s", "ms_per_step": ms / steps,
-                     "max_div": allreduce_max(st.max_div, ws), "kernels_per_step": st.kernels / steps}
+                     "max_div": allreduce_max(st.max_div, ws), "kernels_per_step": st.kernels / steps,
+                     "autotuned_tiles": b.tuning()}
         b.close()
     out["mixed_over_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
     out["config"] = {"domains_per_gpu": BATCH_DOMAINS, "axes_from": BATCH_AXES,

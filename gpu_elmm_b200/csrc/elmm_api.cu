@@ -270,7 +270,7 @@ struct BatchT {
   size_t smem_x = 0, smem_y = 0, smem_tri = 0;
   // register FFTs / tiled z solve when every domain of the batch allows them
   bool reg_x = false, reg_y = false, tri_tile = false;
-  size_t smem_xr = 0, smem_yr = 0, smem_trit = 0;
+  size_t smem_xr = 0, smem_yr = 0, smem_trit = 0, smem_trit32 = 0;
   struct RegSet {
     const FFTRegKernels<T> *k = nullptr;
     LaunchSet ls;
@@ -280,7 +280,7 @@ struct BatchT {
   std::vector<RegSet> xreg, yreg;
   size_t smem_mom = (size_t)MomShape<T>::slots * SlotLayout<T, 5, 3>::BYTES;
   size_t smem_sgs = (size_t)kRingSlots * SlotLayout<T, 3, 0>::BYTES;
-  int grid_cap[16];
+  int grid_cap[16] = {};
   // host-layout staging (double), max over domains of the largest host array
   double *dstage = nullptr;
   size_t stage_elems = 0;
@@ -304,6 +304,11 @@ struct BatchT {
   size_t arena_bytes = 0;
   // a view steps domains whose fields other batches own, on a borrowed stream
   bool is_view = false;
+  // tile shapes chosen by the autotuner at the first step: rows of a tile of
+  // the FP32 scalar stage, spectral columns of a tile of the z solve
+  int tune_rows = 8, tune_cols = 16;
+  bool tuned = false;
+  float tune_ms[4] = {0, 0, 0, 0};  // rows 8, rows 4, cols 16, cols 32
 
   ~BatchT() { release(); }
 
@@ -467,11 +472,15 @@ struct BatchT {
         smem_xr = std::max(smem_xr, sizeof(T2) * fft_reg_batch(h.nx) * fft_reg_seq(h.nx));
       if (fft_reg_supported(h.ny))
         smem_yr = std::max(smem_yr, sizeof(T2) * fft_reg_batch(h.ny) * fft_reg_seq(h.ny));
-      if (tri_tiled(h)) smem_trit = std::max(smem_trit, tri_tile_smem<T>(h.nz));
+      if (tri_tiled(h)) {
+        smem_trit = std::max(smem_trit, tri_tile_smem<T, 16>(h.nz));
+        smem_trit32 = std::max(smem_trit32, tri_tile_smem<T, 32>(h.nz));
+      }
     }
-    if (smem_xr > (size_t)optin || smem_yr > (size_t)optin || smem_trit > (size_t)optin)
+    if (smem_xr > (size_t)optin || smem_yr > (size_t)optin || smem_trit32 > (size_t)optin)
       return fail(ELMM_ERR_INVALID_CONFIG, "shared memory of the register transforms exceeds the device limit");
-    CU(cudaFuncSetAttribute(k_tri_tile<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    CU(cudaFuncSetAttribute(k_tri_tile<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    CU(cudaFuncSetAttribute(k_tri_tile<T, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     int nsm = 0;
     CU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
     auto cap = [&](const void *f, int threads, size_t sm) {
@@ -490,9 +499,11 @@ struct BatchT {
     grid_cap[7] = cap((const void *)k_divres<T>, TX * TY, 0);
     grid_cap[8] = cap((const void *)k_cfl<T>, TX * TY, 0);
     grid_cap[9] = cap((const void *)k_ghosts<T>, kShellThreads, 0);
-    grid_cap[13] = cap((const void *)k_tri_tile<T>, kTriTileThreads, smem_trit);
+    grid_cap[13] = cap((const void *)k_tri_tile<T, 16>, tri_tile_threads<16>(), smem_trit);
+    grid_cap[15] = cap((const void *)k_tri_tile<T, 32>, tri_tile_threads<32>(), smem_trit32);
     grid_cap[11] = cap((const void *)k_scalar<T>, TX * TY, 0);
-    grid_cap[12] = std::is_same<T, float>::value ? cap((const void *)k_scalar_pair, SPX * SPY, 0) : 1;
+    grid_cap[12] = std::is_same<T, float>::value ? cap((const void *)k_scalar_pair<8>, SPX * 8, 0) : 1;
+    grid_cap[14] = std::is_same<T, float>::value ? cap((const void *)k_scalar_pair<4>, SPX * 4, 0) : 1;
     // one launch set per distinct x (y) length, holding only its domains
     auto reg_sets = [&](bool use, bool ydir, std::vector<RegSet> &out) -> int {
       if (!use) return ELMM_OK;
@@ -562,7 +573,7 @@ struct BatchT {
   // the same for the projection (the velocity is periodic in x for every domain)
   static bool fp32_pairs(const Dom<T> &h) { return sizeof(T) == 4 && h.nx % 2 == 0 && h.bt[SIDE_WE] == BC_PERIODIC; }
 
-  static int tiles(int kind, const Dom<T> &h) {
+  int tiles(int kind, const Dom<T> &h) const {
     int ntx = (h.nx + TX - 1) / TX, nty = (h.ny + TY - 1) / TY;
     switch (kind) {
       case LK_CELLS: return ntx * nty * h.nz;
@@ -583,10 +594,10 @@ struct BatchT {
         const int C = fft_reg_batch(h.ny);
         return ((h.nxh + C - 1) / C) * h.nz;
       }
-      case LK_TRIT: return tri_tiled(h) ? (h.ny * h.spitch + kTriCols - 1) / kTriCols : 0;
+      case LK_TRIT: return tri_tiled(h) ? (h.ny * h.spitch + tune_cols - 1) / tune_cols : 0;
       case LK_TCOL: return scalar_pairs(h) ? 0 : ntx * nty * ((h.nz + TMKC - 1) / TMKC) * h.nslot;
       case LK_TPAIR:
-        return scalar_pairs(h) ? ((h.nx + 2 * SPX - 1) / (2 * SPX)) * ((h.ny + SPY - 1) / SPY) *
+        return scalar_pairs(h) ? ((h.nx + 2 * SPX - 1) / (2 * SPX)) * ((h.ny + tune_rows - 1) / tune_rows) *
                                      ((h.nz + TMKC - 1) / TMKC) * h.nslot
                                : 0;
       case LK_DCOL: return ntx * nty * ((h.nz + kDivChunk - 1) / kDivChunk);
@@ -868,8 +879,7 @@ struct BatchT {
     if constexpr (std::is_same<T, float>::value) {
       if (ls[LK_TPAIR].total > 0) {
         nlaunch++;
-        k_scalar_pair<<<gsz(12, ls[LK_TPAIR].total), SPX * SPY, 0, stream>>>(ddom, ls[LK_TPAIR].l(), kRho[stage - 1],
-                                                                            kBeta[stage - 1], stage == 1);
+        launch_scalar_pair(stage);
       }
     }
     nlaunch++;
@@ -913,10 +923,25 @@ struct BatchT {
                                                                               gate);
     }
   }
+  void launch_scalar_pair(int stage) {
+    if constexpr (std::is_same<T, float>::value) {
+      if (tune_rows == 8)
+        k_scalar_pair<8><<<gsz(12, ls[LK_TPAIR].total), SPX * 8, 0, stream>>>(ddom, ls[LK_TPAIR].l(), kRho[stage - 1],
+                                                                             kBeta[stage - 1], stage == 1);
+      else
+        k_scalar_pair<4><<<gsz(14, ls[LK_TPAIR].total), SPX * 4, 0, stream>>>(ddom, ls[LK_TPAIR].l(), kRho[stage - 1],
+                                                                             kBeta[stage - 1], stage == 1);
+    }
+  }
   void launch_tri(int gate) {
     if (ls[LK_TRIT].total > 0) {
       nlaunch++;
-      k_tri_tile<T><<<gsz(13, ls[LK_TRIT].total), kTriTileThreads, smem_trit, stream>>>(ddom, ls[LK_TRIT].l(), gate);
+      if (tune_cols == 16)
+        k_tri_tile<T, 16><<<gsz(13, ls[LK_TRIT].total), tri_tile_threads<16>(), smem_trit, stream>>>(
+            ddom, ls[LK_TRIT].l(), gate);
+      else
+        k_tri_tile<T, 32><<<gsz(15, ls[LK_TRIT].total), tri_tile_threads<32>(), smem_trit32, stream>>>(
+            ddom, ls[LK_TRIT].l(), gate);
     }
     if (ls[LK_TRI].total > 0) {
       nlaunch++;
@@ -1005,10 +1030,70 @@ struct BatchT {
     return step_finish(nsteps, st);
   }
 
+  // the launch map of one kind after a change of tile shape
+  int rebuild_ls(int kind) {
+    std::vector<int> st(nd + 1, 0);
+    for (int d = 0; d < nd; d++) st[d + 1] = st[d] + tiles(kind, hdom[d]);
+    CU(cudaMemcpy(ls[kind].starts, st.data(), sizeof(int) * (nd + 1), cudaMemcpyHostToDevice));
+    ls[kind].total = st[nd];
+    return ELMM_OK;
+  }
+
+  // The autotuner: before the first step of a batch (or view), times each
+  // candidate tile shape of the z solve and of the FP32 scalar stage on the
+  // batch's own domains (three launches each, CUDA events) and keeps the
+  // fastest.  The launches it times only write scratch (the spectral buffer,
+  // the new scalar value and the tendency that a first stage overwrites), and
+  // no shape changes any result.
+  int autotune() {
+    tuned = true;
+    cudaEvent_t a, b;
+    CU(cudaEventCreate(&a));
+    CU(cudaEventCreate(&b));
+    auto time3 = [&](auto launch) -> float {
+      launch();  // warm
+      cudaEventRecord(a, stream);
+      for (int r = 0; r < 3; r++) launch();
+      cudaEventRecord(b, stream);
+      cudaEventSynchronize(b);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, a, b);
+      return ms;
+    };
+    int r = ELMM_OK;
+    if (ls[LK_TRIT].total > 0) {
+      for (int v = 0; v < 2 && !r; v++) {
+        tune_cols = v ? 32 : 16;
+        if ((r = rebuild_ls(LK_TRIT))) break;
+        tune_ms[2 + v] = time3([&] { launch_tri(0); });
+      }
+      tune_cols = tune_ms[3] < tune_ms[2] ? 32 : 16;
+      if (!r) r = rebuild_ls(LK_TRIT);
+    }
+    if (!r && ls[LK_TPAIR].total > 0) {
+      for (int v = 0; v < 2 && !r; v++) {
+        tune_rows = v ? 4 : 8;
+        if ((r = rebuild_ls(LK_TPAIR))) break;
+        tune_ms[v] = time3([&] { launch_scalar_pair(1); });
+      }
+      tune_rows = tune_ms[1] < tune_ms[0] ? 4 : 8;
+      if (!r) r = rebuild_ls(LK_TPAIR);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (r) return r;
+    CU(cudaGetLastError());
+    return ELMM_OK;
+  }
+
   // enqueues nsteps replays of the step graph (captured on first use) without
   // waiting for them
   int step_launch(int nsteps) {
     CU(cudaSetDevice(device));
+    if (!tuned) {
+      int r = autotune();
+      if (r) return r;
+    }
     if (frame_pending) CU(cudaStreamWaitEvent(stream, ev_packed, 0));
     bool cfl = false;
     for (auto &c : cfg) cfl |= c.enable_CFL_check != 0;
@@ -1674,6 +1759,13 @@ int elmm_batch_profile_stage(elmm_batch *b, int32_t stage, int32_t reps, double 
   if (!b || !ms) return fail(ELMM_ERR_INVALID_ARG, "NULL argument");
   if (stage < 1 || stage > 3 || reps < 1) return fail(ELMM_ERR_INVALID_ARG, "stage 1..3, reps >= 1");
   return DISPATCH(*b, profile_stage(stage, reps, ms));
+}
+
+int elmm_batch_tuning(const elmm_batch *b, int32_t out[2]) {
+  if (!b || !out) return fail(ELMM_ERR_INVALID_ARG, "NULL argument");
+  out[0] = b->precision == ELMM_PREC_MIXED ? b->b32->tune_rows : b->b64->tune_rows;
+  out[1] = b->precision == ELMM_PREC_MIXED ? b->b32->tune_cols : b->b64->tune_cols;
+  return ELMM_OK;
 }
 
 int elmm_batch_upload_scalar(elmm_batch *b, int32_t d, int32_t sc, const double *S) {

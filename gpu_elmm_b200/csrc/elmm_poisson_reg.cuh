@@ -349,11 +349,15 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// tile of S, reciprocal pivots, and the (A, B) maps of the segments
-template <typename T>
+// tile of S, reciprocal pivots, and the (A, B) maps of the segments, for a
+// tile of COLS spectral columns
+template <typename T, int COLS = kTriCols>
 __host__ __device__ constexpr size_t tri_tile_smem(int nz) {
-  return (size_t)nz * kTriCols * (2 * sizeof(T) + sizeof(double)) + 2 * sizeof(double) * kTriSegs * 2 * kTriCols;
+  return (size_t)nz * COLS * (2 * sizeof(T) + sizeof(double)) + 2 * sizeof(double) * kTriSegs * 2 * COLS;
 }
+// threads of a tile of COLS columns: kTriSegs per real or imaginary part
+template <int COLS>
+constexpr int tri_tile_threads() { return 2 * COLS * kTriSegs; }
 
 // One step of the pivot recurrence of the forward sweep: the reciprocal
 // pivot iv(k) of a mode with eigenvalue lam, and c(k) = At(k) iv(k) carried
@@ -399,8 +403,12 @@ __global__ void k_tri_factors(double *c0, const double *__restrict__ lamx, const
   }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kTriTileThreads) k_tri_tile(const Dom<T> *__restrict__ doms, Launch L, int gate) {
+// COLS: the tile width, a tuning choice (every column is solved alone, so
+// the result does not depend on it)
+template <typename T, int COLS = kTriCols>
+__global__ void __launch_bounds__(tri_tile_threads<COLS>()) k_tri_tile(const Dom<T> *__restrict__ doms, Launch L,
+                                                                      int gate) {
+  constexpr int kTriCols = COLS, kTriTileThreads = tri_tile_threads<COLS>();
   typedef typename Vec2<T>::type T2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int kChunk = 16 / (int)sizeof(T2), kPerRow = kTriCols / kChunk, XS = 2 * kTriCols;

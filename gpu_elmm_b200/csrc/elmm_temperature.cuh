@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
 // for two cells, every load and store is a float2, and the per-plane
 // bookkeeping of the column march is shared by the pair.  Same operations in
 // the same order as k_scalar.  A block is 16 x 8 threads, a tile 32 x 8 cells.
-constexpr int SPX = 16, SPY = 8;
+constexpr int SPX = 16;
 #ifndef ELMM_SCALAR_PAIR_MIN_BLOCKS
 #define ELMM_SCALAR_PAIR_MIN_BLOCKS 5
 #endif
@@ -209,7 +209,10 @@ __device__ __forceinline__ float2 ld2(const float *p, long long o) {
   return __ldg(reinterpret_cast<const float2 *>(p + o));
 }
 
-__global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS)
+// SPY: the rows of a tile, a tuning choice (8 or 4; the arithmetic of a
+// cell does not depend on it)
+template <int SPY>
+__global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SPY)
     k_scalar_pair(const Dom<float> *__restrict__ doms, Launch L, double rho, double beta, int stage1) {
   typedef float T;
   for (int t = blockIdx.x; t < L.total; t += gridDim.x) {

@@ -73,6 +73,7 @@ def lib():
         L.elmm_batch_download_scalar_slices.argtypes = [P, C.c_int32, C.c_int32, _dp, _dp]
         L.elmm_batch_project.argtypes = [P, C.c_double]
         L.elmm_batch_profile_stage.argtypes = [P, C.c_int32, C.c_int32, _dp]
+        L.elmm_batch_tuning.argtypes = [P, C.POINTER(C.c_int32)]
         L.elmm_batch_step.argtypes = [P, C.c_int32, C.POINTER(ElmmStats)]
         L.elmm_batch_cells.argtypes = [P]
         L.elmm_batch_cells.restype = C.c_int64
@@ -238,6 +239,12 @@ class Batch:
         st = ElmmStats()
         check(lib().elmm_batch_step(self.h, n, C.byref(st)), "elmm_batch_step")
         return st
+
+    def tuning(self):
+        """Tile shapes chosen by the autotuner at the first step."""
+        out = (C.c_int32 * 2)()
+        check(lib().elmm_batch_tuning(self.h, out), "elmm_batch_tuning")
+        return {"scalar_tile_rows": out[0], "tri_tile_cols": out[1]}
 
     def profile_stage(self, stage=2, reps=5):
         """Mean device time (ms) of each kernel kind of one RK3 stage over the whole batch."""

@@ -88,7 +88,8 @@ def batched(a):
         b.step(a.warmup)
     s = b.step(a.steps)
     out = {"domains": a.batched, "cells": b.cells(), "precision": a.precision, "steps": a.steps,
-           "ms_per_step": s.elapsed_ms / max(1, a.steps), "kernels_per_step": s.kernels / max(1, a.steps)}
+           "ms_per_step": s.elapsed_ms / max(1, a.steps), "kernels_per_step": s.kernels / max(1, a.steps),
+           "tuning": b.tuning()}
     if a.stage_times:
         out["stage2_kernel_ms"] = b.profile_stage(2, 5)
     print(json.dumps(out))

@@ -321,6 +321,10 @@ int elmm_batch_upload_scalar(elmm_batch *b, int32_t d, int32_t sc, const double 
 int elmm_batch_download_field(elmm_batch *b, int32_t d, int32_t field, double *host);
 int elmm_batch_download_scalar_slices(elmm_batch *b, int32_t d, int32_t sc, double *xy, double *xz);
 int elmm_batch_project(elmm_batch *b, double coef);
+/* The tile shapes the autotuner chose at the first step (out[0]: rows of a
+ * tile of the FP32 scalar stage, out[1]: spectral columns of a tile of the z
+ * solve); the defaults before it. */
+int elmm_batch_tuning(const elmm_batch *b, int32_t out[2]);
 /* elmm_profile_stage for a whole batch */
 int elmm_batch_profile_stage(elmm_batch *b, int32_t stage, int32_t reps, double *ms);
 int elmm_batch_step(elmm_batch *b, int32_t nsteps, elmm_stats *stats);

@@ -508,6 +508,8 @@ def test_dispersion_alone_and_in_batch(precision):
         b.upload_scalar(q, 1, puff_state(g, s))
     b.project(1.0)
     b.step(4)
+    tun = b.tuning()  # whatever shapes the autotuner chose, the results equal the runs alone
+    assert tun["scalar_tile_rows"] in (4, 8) and tun["tri_tile_cols"] in (16, 32)
     for q, (n, s, seed) in enumerate(cases):
         g = grid_of(cfgs[q])
         d = L.Domain(cfgs[q])
