@@ -456,16 +456,18 @@ __global__ void __launch_bounds__(TX *TY) k_divmax(const Dom<T> *__restrict__ do
     const T *__restrict__ V = d.V;
     const T *__restrict__ W = d.W;
     const long long pitch = d.pitch, plane = d.plane;
-    const double dx = d.dx, dy = d.dy, dz = d.dz;
+    // reciprocal spacings: a multiplication instead of an FP64 division per
+    // term (the check is a diagnostic; it moves by at most an ulp)
+    const double rdx = 1.0 / d.dx, rdy = 1.0 / d.dy, rdz = 1.0 / d.dz;
     const bool vz = d.vz != 0;
-    const double *dzPr = d.dzPr;
+    const double *rdzk_tab = d.sgs_rdz;  // 1 / dzPr(k), index k
     long long c = bidx(d, i, j, k0);
     double wb = (double)ld(W, c - plane);
     for (int k = k0; k <= k1; k++) {
-      const double dzk = vz ? dzPr[k + 2] : dz;
+      const double rdzk = vz ? rdzk_tab[k] : rdz;
       const double wt = (double)ld(W, c);
-      const double a = fabs(((double)ld(U, c) - (double)ld(U, c - 1)) / dx +
-                            ((double)ld(V, c) - (double)ld(V, c - pitch)) / dy + (wt - wb) / dzk);
+      const double a = fabs(((double)ld(U, c) - (double)ld(U, c - 1)) * rdx +
+                            ((double)ld(V, c) - (double)ld(V, c - pitch)) * rdy + (wt - wb) * rdzk);
       const unsigned long long bits = max_bits(a);
       run = bits > run ? bits : run;
       wb = wt;
