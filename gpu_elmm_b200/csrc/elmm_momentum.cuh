@@ -25,7 +25,10 @@ struct StageCoef {
   int stage;
 };
 
-constexpr int MX = 32, MY = 8, MKC = 16;
+#ifndef ELMM_MOM_CHUNK
+#define ELMM_MOM_CHUNK 16
+#endif
+constexpr int MX = 32, MY = 8, MKC = ELMM_MOM_CHUNK;
 // per-tile context in shared memory: everything the stencil code reads
 // besides the fields, so that no descriptor load sits on its critical path
 template <typename T>

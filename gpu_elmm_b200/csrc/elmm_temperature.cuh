@@ -65,7 +65,10 @@ __device__ __forceinline__ T kappa_flux(T vel, T a, T b, T c, T e) {
 // chunk of TMKC planes; the scalar (k-2..k+2), the diffusivity (k-1..k+1)
 // and W(k-1) ride along in registers, x and y neighbours come from offsets
 // folded once per thread.  Tiles: (slot, column, chunk) per domain.
-constexpr int TMKC = 16;
+#ifndef ELMM_SCALAR_CHUNK
+#define ELMM_SCALAR_CHUNK 16
+#endif
+constexpr int TMKC = ELMM_SCALAR_CHUNK;
 
 template <typename T>
 __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
