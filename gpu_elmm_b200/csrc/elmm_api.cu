@@ -308,6 +308,12 @@ struct BatchT {
   // the FP32 scalar stage, spectral columns of a tile of the z solve
   int tune_rows = 8, tune_cols = 16;
   bool tuned = false;
+  // parallel branches for the independent per-length launches of one
+  // transform phase (a batch with several x or y lengths); joined back into
+  // the stream before the next phase, captured as graph branches
+  static constexpr int kBranches = 4;
+  cudaStream_t branch[kBranches] = {};
+  cudaEvent_t ev_fork = nullptr, ev_join[kBranches] = {};
   float tune_ms[4] = {0, 0, 0, 0};  // rows 8, rows 4, cols 16, cols 32
 
   ~BatchT() { release(); }
@@ -330,6 +336,14 @@ struct BatchT {
       if (side) cudaStreamDestroy(side);
     }
     stream = side = nullptr;
+    for (int b = 0; b < kBranches; b++) {
+      if (branch[b]) cudaStreamDestroy(branch[b]);
+      if (ev_join[b]) cudaEventDestroy(ev_join[b]);
+      branch[b] = nullptr;
+      ev_join[b] = nullptr;
+    }
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    ev_fork = nullptr;
   }
 
   int dalloc(void **p, size_t bytes) {
@@ -426,6 +440,11 @@ struct BatchT {
   // device tables of the domains, launch maps and kernel attributes
   int init_tables() {
     const int n = nd;
+    CU(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    for (int b = 1; b < kBranches; b++) {
+      CU(cudaStreamCreateWithFlags(&branch[b], cudaStreamNonBlocking));
+      CU(cudaEventCreateWithFlags(&ev_join[b], cudaEventDisableTiming));
+    }
     void *p;
     int r = dalloc(&p, sizeof(Dom<T>) * n);
     if (r) return r;
@@ -899,29 +918,50 @@ struct BatchT {
   // the pieces of the Poisson solve: register FFTs (one launch per distinct
   // length) and the tiled z solve where the whole batch allows them, the
   // generic kernels otherwise
-  void launch_fftx_fwd(double coef_alpha2, int use_dt, int rhs_from_phi, int gate) {
-    for (auto &r : xreg) {
-      nlaunch++;
-      r.k->fwd<<<std::max(1, std::min(r.ls.total, r.cap_fwd)), kRegThreads, r.smem, stream>>>(
-          ddom, r.ls.l(), coef_alpha2, use_dt, rhs_from_phi, gate);
+  // n independent launches, launch(q, s) for q < n, spread over the branches
+  // and joined back into the stream
+  template <typename F>
+  void fan_out(int n, F launch) {
+    if (n <= 1 || !ev_fork) {
+      for (int q = 0; q < n; q++) launch(q, stream);
+      return;
     }
-    if (ls[LK_ROWS].total > 0) {
-      nlaunch++;
-      k_fftx_fwd<T><<<gsz(2, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan,
-                                                                                  coef_alpha2, use_dt, rhs_from_phi, gate);
+    const int nb = std::min(n, kBranches);
+    cudaEventRecord(ev_fork, stream);
+    for (int b = 1; b < nb; b++) cudaStreamWaitEvent(branch[b], ev_fork, 0);
+    for (int q = 0; q < n; q++) launch(q, q % nb ? branch[q % nb] : stream);
+    for (int b = 1; b < nb; b++) {
+      cudaEventRecord(ev_join[b], branch[b]);
+      cudaStreamWaitEvent(stream, ev_join[b], 0);
     }
   }
+  void launch_fftx_fwd(double coef_alpha2, int use_dt, int rhs_from_phi, int gate) {
+    const int nr = (int)xreg.size(), ng = ls[LK_ROWS].total > 0 ? 1 : 0;
+    nlaunch += nr + ng;
+    fan_out(nr + ng, [&](int q, cudaStream_t s) {
+      if (q < nr) {
+        const RegSet &r = xreg[q];
+        r.k->fwd<<<std::max(1, std::min(r.ls.total, r.cap_fwd)), kRegThreads, r.smem, s>>>(ddom, r.ls.l(), coef_alpha2,
+                                                                                           use_dt, rhs_from_phi, gate);
+      } else {
+        k_fftx_fwd<T><<<gsz(2, ls[LK_ROWS].total), kFFTThreads, smem_x, s>>>(ddom, ls[LK_ROWS].l(), dplan, coef_alpha2,
+                                                                             use_dt, rhs_from_phi, gate);
+      }
+    });
+  }
   void launch_ffty(int inverse, int gate) {
-    for (auto &r : yreg) {
-      nlaunch++;
-      (inverse ? r.k->yi : r.k->yf)<<<std::max(1, std::min(r.ls.total, inverse ? r.cap_inv : r.cap_fwd)), kRegThreads,
-                                       r.smem, stream>>>(ddom, r.ls.l(), gate);
-    }
-    if (ls[LK_YCOLS].total > 0) {
-      nlaunch++;
-      k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), kFFTThreads, smem_y, stream>>>(ddom, ls[LK_YCOLS].l(), dplan, inverse,
-                                                                              gate);
-    }
+    const int nr = (int)yreg.size(), ng = ls[LK_YCOLS].total > 0 ? 1 : 0;
+    nlaunch += nr + ng;
+    fan_out(nr + ng, [&](int q, cudaStream_t s) {
+      if (q < nr) {
+        const RegSet &r = yreg[q];
+        (inverse ? r.k->yi : r.k->yf)<<<std::max(1, std::min(r.ls.total, inverse ? r.cap_inv : r.cap_fwd)),
+                                         kRegThreads, r.smem, s>>>(ddom, r.ls.l(), gate);
+      } else {
+        k_ffty<T><<<gsz(3, ls[LK_YCOLS].total), kFFTThreads, smem_y, s>>>(ddom, ls[LK_YCOLS].l(), dplan, inverse,
+                                                                         gate);
+      }
+    });
   }
   void launch_scalar_pair(int stage) {
     if constexpr (std::is_same<T, float>::value) {
@@ -949,14 +989,16 @@ struct BatchT {
     }
   }
   void launch_fftx_inv(int gate) {
-    for (auto &r : xreg) {
-      nlaunch++;
-      r.k->inv<<<std::max(1, std::min(r.ls.total, r.cap_inv)), kRegThreads, r.smem, stream>>>(ddom, r.ls.l(), gate);
-    }
-    if (ls[LK_ROWS].total > 0) {
-      nlaunch++;
-      k_fftx_inv<T><<<gsz(5, ls[LK_ROWS].total), kFFTThreads, smem_x, stream>>>(ddom, ls[LK_ROWS].l(), dplan, gate);
-    }
+    const int nr = (int)xreg.size(), ng = ls[LK_ROWS].total > 0 ? 1 : 0;
+    nlaunch += nr + ng;
+    fan_out(nr + ng, [&](int q, cudaStream_t s) {
+      if (q < nr) {
+        const RegSet &r = xreg[q];
+        r.k->inv<<<std::max(1, std::min(r.ls.total, r.cap_inv)), kRegThreads, r.smem, s>>>(ddom, r.ls.l(), gate);
+      } else {
+        k_fftx_inv<T><<<gsz(5, ls[LK_ROWS].total), kFFTThreads, smem_x, s>>>(ddom, ls[LK_ROWS].l(), dplan, gate);
+      }
+    });
   }
   // the five transform kernels; rhs_from_phi: the right-hand side is in Phi.
   // Phi gets no ghost pass: its only reader, k_project, folds the i+1, j+1,
