@@ -443,9 +443,10 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
     int wmask = 0;
     for (int f = 0; f < 6; f++) wmask |= d.wall[f] ? (1 << f) : 0;
     const int wtile = wmask & ((xlo ? 1 : 0) | (xhi ? 2 : 0) | (ylo ? 4 : 0) | (yhi ? 8 : 0));
-    // block-uniform: every cell of the tile has all three components
-    const bool full_tile = i0 + MX - 1 <= min(d.ext[0][0], min(d.ext[1][0], d.ext[2][0])) &&
-                           j0 + MY - 1 <= min(d.ext[0][1], min(d.ext[1][1], d.ext[2][1]));
+    // both cells of the thread's pair have all three components (the pairs of
+    // a partial tile past the last cell take the per-cell path)
+    const bool pair_full = i + CPT - 1 <= min(d.ext[0][0], min(d.ext[1][0], d.ext[2][0])) &&
+                           j <= min(d.ext[0][1], min(d.ext[1][1], d.ext[2][1]));
     // buoyancy of W (BuoyancyForce, src/dynamics.f90:679-688): A = g / T_ref;
     // with theta stored as theta - T_ref the constant term cancels exactly
     const bool buoy = d.buoy != 0;
@@ -474,7 +475,7 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
               *p2s = ring + ((k + 1) % NSL) * Lay::SIZE;
       bool packed = false;
       if constexpr (CPT == 2)
-        packed = !vz && !wallhere && full_tile && k <= min(kU, min(kV, kW)) && j <= ny;
+        packed = !vz && !wallhere && pair_full && k <= min(kU, min(kV, kW));
       if (packed && ok) {
         if constexpr (CPT == 2) {
           // two cells per thread, every operation on a pair
