@@ -181,3 +181,29 @@ def test_server_admits_while_others_run():
     assert info[1].t_admit < info[0].t_done and info[1].t_done < info[0].t_done
     assert srv.stats().graph_builds >= 3  # long alone, long + short, long alone again
     srv.close()
+
+
+@pytest.mark.gpu
+def test_server_isolates_a_failing_request():
+    """A request whose flow blows up (a velocity far past the CFL limit)
+    ends with ELMM_ERR_NAN; the request beside it finishes with the result it
+    has alone."""
+    from gpu_elmm_b200.serve import Server, request_config, request_inputs
+    good = {"n": (32, 32, 16), "steps": 30, "source": (5, 9, 4), "seed": 31}
+    bad = {"n": (32, 32, 16), "steps": 30, "source": (6, 6, 6), "seed": 32}
+    U, V, W, Pr, S0 = request_inputs(bad)
+    U = U * 1e6  # the explicit RK3 step diverges to Inf / NaN within a few steps
+    srv = Server(precision=1, budget_bytes=2 << 30, max_active=8, chunk_steps=5)
+    ids = {srv.submit(request_config(good), *request_inputs(good), nsteps=good["steps"]): "good",
+           srv.submit(request_config(bad), U, V, W, Pr, S0, nsteps=bad["steps"]): "bad"}
+    infos = {}
+    while len(infos) < 2:
+        info = srv.wait_any(120000)
+        assert info is not None
+        infos[ids[info.id]] = info
+    assert infos["bad"].status == 3  # ELMM_ERR_NAN
+    assert infos["good"].status == 0 and infos["good"].steps == good["steps"]
+    xy, xz = srv.collect(infos["good"].id)
+    axy, axz = _alone(good, 1)
+    assert np.array_equal(xy, axy) and np.array_equal(xz, axz)
+    srv.close()
