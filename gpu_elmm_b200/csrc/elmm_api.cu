@@ -778,10 +778,11 @@ struct BatchT {
       h.grav = c.grav_acc;
       h.kappa_mol = c.molecular_diffusivity;
       h.toff = sizeof(T) == 4 ? c.temperature_ref : 0.0;  // FP32 stores theta - T_ref
-      for (T **f : {&h.Tm, &h.Tn, &h.Tadv})
-        if ((r = dalloc((void **)f, alloc_elems * sizeof(T)))) return r;
       ScalSlot<T> &sl = h.slot[h.nslot++];
-      sl.m = h.Tm; sl.n = h.Tn; sl.adv = h.Tadv;
+      for (T **f : {&sl.buf[0], &sl.buf[1], &sl.buf[2], &sl.adv})
+        if ((r = dalloc((void **)f, alloc_elems * sizeof(T)))) return r;
+      h.Tm = sl.buf[0];
+      h.Tadv = sl.adv;
       for (int s2 = 0; s2 < 6; s2++) sl.bt[s2] = c.TempBtype[s2];
       sl.off = h.toff;
       h.tdiff_live = 1;
@@ -789,7 +790,7 @@ struct BatchT {
     h.kappa_mol = c.molecular_diffusivity;
     for (int sc = 0; sc < c.num_scalars; sc++) {
       ScalSlot<T> &sl = h.slot[h.nslot++];
-      for (T **f : {&sl.m, &sl.n, &sl.adv})
+      for (T **f : {&sl.buf[0], &sl.buf[1], &sl.buf[2], &sl.adv})
         if ((r = dalloc((void **)f, alloc_elems * sizeof(T)))) return r;
       for (int s2 = 0; s2 < 6; s2++) sl.bt[s2] = c.ScalBtype[s2];
       sl.off = 0;
@@ -888,12 +889,14 @@ struct BatchT {
   // become the current ones (the stage reads the old value at neighbours
   // while writing).  accumulate: the last stage of a step, which also feeds
   // the time-averaged slices.
-  void launch_scalars(int stage, int accumulate) {
+  // standalone: a stage run on its own (elmm_run_stage), whose new value is
+  // copied to buf[0] where the host reads it
+  void launch_scalars(int stage, int accumulate, bool standalone = false) {
     if (ls[LK_TCOL].total == 0 && ls[LK_TPAIR].total == 0) return;
     if (ls[LK_TCOL].total > 0) {
       nlaunch++;
       k_scalar<T><<<gsz(11, ls[LK_TCOL].total), TX * TY, 0, stream>>>(ddom, ls[LK_TCOL].l(), kRho[stage - 1],
-                                                                       kBeta[stage - 1], stage == 1);
+                                                                       kBeta[stage - 1], stage);
     }
     if constexpr (std::is_same<T, float>::value) {
       if (ls[LK_TPAIR].total > 0) {
@@ -901,9 +904,9 @@ struct BatchT {
         launch_scalar_pair(stage);
       }
     }
-    nlaunch++;
-    k_scalar_commit<T><<<std::min(ls[LK_COMMIT].total, 16 * 148), kCommitThreads, 0, stream>>>(ddom,
-                                                                                                ls[LK_COMMIT].l());
+    if (standalone && stage % 3 != 0)
+      k_scalar_commit<T><<<std::min(ls[LK_COMMIT].total, 16 * 148), kCommitThreads, 0, stream>>>(
+          ddom, ls[LK_COMMIT].l(), stage % 3);
     if (accumulate && ls[LK_AVG].total > 0) {
       nlaunch++;
       k_scalar_avg<T><<<std::min(ls[LK_AVG].total, 8 * 148), 128, 0, stream>>>(ddom, ls[LK_AVG].l());
@@ -967,10 +970,10 @@ struct BatchT {
     if constexpr (std::is_same<T, float>::value) {
       if (tune_rows == 8)
         k_scalar_pair<8><<<gsz(12, ls[LK_TPAIR].total), SPX * 8, 0, stream>>>(ddom, ls[LK_TPAIR].l(), kRho[stage - 1],
-                                                                             kBeta[stage - 1], stage == 1);
+                                                                             kBeta[stage - 1], stage);
       else
         k_scalar_pair<4><<<gsz(14, ls[LK_TPAIR].total), SPX * 4, 0, stream>>>(ddom, ls[LK_TPAIR].l(), kRho[stage - 1],
-                                                                             kBeta[stage - 1], stage == 1);
+                                                                             kBeta[stage - 1], stage);
     }
   }
   void launch_tri(int gate) {
@@ -1049,11 +1052,11 @@ struct BatchT {
     // U <-> U2 after the projection wrote U directly: nothing to swap; the
     // projection writes the new velocity into U (exchange_alloc in tsteps.f90:211-213)
   }
-  int run_stage(int stage, int stop, int accumulate = 0) {
+  int run_stage(int stage, int stop, int accumulate = 0, bool standalone = false) {
     launch_sgs();
     if (stop == 1) return ELMM_OK;
     launch_momentum(stage);
-    launch_scalars(stage, accumulate);  // ScalarRK3 between Convection and the projection (tsteps.f90:132-135)
+    launch_scalars(stage, accumulate, standalone);  // ScalarRK3 between Convection and the projection (tsteps.f90:132-135)
     if (stop == 2) return ELMM_OK;
     launch_projection(2 * kAlpha[stage - 1], 1, 0);
     launch_refine(2 * kAlpha[stage - 1], 1);
@@ -1448,7 +1451,7 @@ struct BatchT {
       const bool adv = field >= ELMM_FIELD_SCALAR_ADV;
       const ScalSlot<T> &sl = h.slot[(h.buoy ? 1 : 0) + field - (adv ? ELMM_FIELD_SCALAR_ADV : ELMM_FIELD_SCALAR)];
       const size_t n = (size_t)(h.nx + 6) * (h.ny + 6) * (h.nz + 6);
-      k_pack_scalar_box<T><<<256, 256, 0, s>>>(ddom + d, adv ? sl.adv : sl.m, dst, -2, sl.off, adv,
+      k_pack_scalar_box<T><<<256, 256, 0, s>>>(ddom + d, adv ? sl.adv : sl.buf[0], dst, -2, sl.off, adv,
                                                sl.bt[0] == BC_PERIODIC, sl.bt[2] == BC_PERIODIC, sl.bt[4] == BC_PERIODIC);
       return n;
     }
@@ -1697,7 +1700,7 @@ int elmm_step(elmm_handle *h, int32_t nsteps, elmm_stats *st) {
 int elmm_run_stage(elmm_handle *h, int32_t stage, int32_t stop) {
   if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
   if (stage < 1 || stage > 3 || stop < 1 || stop > 3) return fail(ELMM_ERR_INVALID_ARG, "stage 1..3, stop 1..3");
-  int r = DISPATCH(h->b, run_stage(stage, stop));
+  int r = DISPATCH(h->b, run_stage(stage, stop, 0, true));
   if (r) return r;
   cudaStream_t s = h->b.precision == ELMM_PREC_MIXED ? h->b.b32->stream : h->b.b64->stream;
   CU(cudaStreamSynchronize(s));

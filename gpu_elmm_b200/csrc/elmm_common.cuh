@@ -43,7 +43,11 @@ constexpr int kMaxSlots = 5;    // temperature + ELMM_MAX_SCALARS passive scalar
 constexpr int kMaxSources = 8;  // ELMM_MAX_POINT_SOURCES
 template <typename T>
 struct ScalSlot {
-  T *m, *n, *adv;        // value at the stage start, the stage's new value, the stage tendency
+  // three value buffers in rotation: stage s of a step reads buf[(s-1) % 3]
+  // and writes buf[s % 3], so the value is in buf[0] again after the third
+  // stage and between steps (no copy-back), and one graph serves every step
+  T *buf[3];
+  T *adv;                // the stage tendency
   int bt[6];             // BC per side (TempBtype / ScalBtype)
   double off;            // the box stores value - off
   double *acc_xy, *acc_xz;  // time-averaged slices (FP64, [j][i] and [k][i]) or null
@@ -115,10 +119,11 @@ struct Dom {
   // perturbations' digits), 0 on the FP64 path.
   int buoy;
   int tbt[6];            // temperature BC per side
-  T *Tm, *Tn, *Tadv, *TDiff;
+  T *Tm, *Tadv, *TDiff;
   double toff, tref, grav, kappa_mol;
   // scalar slots of the ScalarRK3 kernel: slot 0 is the temperature when
-  // buoy is set (its fields alias Tm, Tn, Tadv), then the passive scalars
+  // buoy is set (Tm aliases its buf[0], Tadv its tendency), then the passive
+  // scalars
   int nslot;
   ScalSlot<T> slot[kMaxSlots];
   int tdiff_live;        // 1: TDiff follows the viscosity every stage (buoyancy)

@@ -452,7 +452,7 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
     const bool buoy = d.buoy != 0;
     const T bA2 = (T)(d.grav / d.tref / 2.0);
     const T bsub = buoy && d.toff == 0 ? (T)(d.grav / d.tref * d.tref) : (T)0;
-    const T *__restrict__ Tm = d.Tm;
+    const T *__restrict__ Tm = buoy ? d.slot[0].buf[(sc.stage - 1) % 3] : nullptr;  // theta at the stage start
     MomK2 K2;
     if constexpr (CPT == 2) {
       K2.Ax = bc2((float)ctx.cA[0]); K2.Ay = bc2((float)ctx.cA[1]); K2.Az = bc2((float)ctx.cA[2]);

@@ -72,7 +72,8 @@ constexpr int TMKC = ELMM_SCALAR_CHUNK;
 
 template <typename T>
 __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
-    k_scalar(const Dom<T> *__restrict__ doms, Launch L, double rho, double beta, int stage1) {
+    k_scalar(const Dom<T> *__restrict__ doms, Launch L, double rho, double beta, int stage) {
+  const int stage1 = stage == 1;
   for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
     const int di = find_dom(L.starts, L.nd, t);
     const Dom<T> &d = doms[di];
@@ -104,13 +105,13 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
     unsigned srcm = 0;
     for (int q = 0; q < d.nsrc; q++)
       if (d.src_slot[q] == s && d.src_i[q] == i && d.src_j[q] == j) srcm |= 1u << q;
-    const T *__restrict__ S = sl.m;
+    const T *__restrict__ S = sl.buf[(stage - 1) % 3];
     const T *__restrict__ K = d.TDiff;
     const T *__restrict__ U = d.U;
     const T *__restrict__ V = d.V;
     const T *__restrict__ W = d.W;
     T *__restrict__ Sadv = sl.adv;
-    T *__restrict__ Snew = sl.n;
+    T *__restrict__ Snew = sl.buf[stage % 3];
     const T Ax = (T)(1.0 / d.dx), Ay = (T)(1.0 / d.dy), Az = (T)(1.0 / d.dz);
     const T Dx = (T)(1.0 / (2 * d.dx * d.dx)), Dy = (T)(1.0 / (2 * d.dy * d.dy)), Dz = (T)(1.0 / (2 * d.dz * d.dz));
     const T rdx = (T)d.dx, rdy = (T)d.dy;
@@ -216,8 +217,9 @@ __device__ __forceinline__ float2 ld2(const float *p, long long o) {
 // cell does not depend on it)
 template <int SPY>
 __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SPY)
-    k_scalar_pair(const Dom<float> *__restrict__ doms, Launch L, double rho, double beta, int stage1) {
+    k_scalar_pair(const Dom<float> *__restrict__ doms, Launch L, double rho, double beta, int stage) {
   typedef float T;
+  const int stage1 = stage == 1;
   for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
     const int di = find_dom(L.starts, L.nd, t);
     const Dom<T> &d = doms[di];
@@ -245,13 +247,13 @@ __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SP
     unsigned srcm = 0;  // volume sources of this slot in this pair's columns
     for (int q = 0; q < d.nsrc; q++)
       if (d.src_slot[q] == s && (d.src_i[q] == i || d.src_i[q] == i + 1) && d.src_j[q] == j) srcm |= 1u << q;
-    const T *__restrict__ S = sl.m;
+    const T *__restrict__ S = sl.buf[(stage - 1) % 3];
     const T *__restrict__ K = d.TDiff;
     const T *__restrict__ U = d.U;
     const T *__restrict__ V = d.V;
     const T *__restrict__ W = d.W;
     T *__restrict__ Sadv = sl.adv;
-    T *__restrict__ Snew = sl.n;
+    T *__restrict__ Snew = sl.buf[stage % 3];
     const T Ax = (T)(1.0 / d.dx), Ay = (T)(1.0 / d.dy), Az = (T)(1.0 / d.dz);
     const T Dx = (T)(1.0 / (2 * d.dx * d.dx)), Dy = (T)(1.0 / (2 * d.dy * d.dy)), Dz = (T)(1.0 / (2 * d.dz * d.dz));
     const T rdx = (T)d.dx, rdy = (T)d.dy;
@@ -356,15 +358,17 @@ __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SP
   }
 }
 
-// After a stage the new values become the current ones: planes 1..nz of
-// every slot of every domain, n -> m, in 16-byte vectors (a box starts on a
-// 256-byte boundary and a plane is a whole number of 128-byte rows).  One
-// launch for the whole batch.  Tiles: (slot, chunk of kCommitVecs vectors);
-// a thread moves kCommitPer vectors with all its loads issued first.
+// A stage run on its own (elmm_run_stage) leaves the new value in buf[from];
+// this copies planes 1..nz of every slot of every domain into buf[0], where
+// the host reads it, in 16-byte vectors (a box starts on a 256-byte boundary
+// and a plane is a whole number of 128-byte rows).  Tiles: (slot, chunk of
+// kCommitVecs vectors); a thread moves kCommitPer vectors with all its loads
+// issued first.  Steps never need it: the rotation of the buffers brings the
+// value back to buf[0] after the third stage.
 constexpr int kCommitThreads = 256, kCommitPer = 4, kCommitVecs = kCommitThreads * kCommitPer;
 
 template <typename T>
-__global__ void k_scalar_commit(const Dom<T> *__restrict__ doms, Launch L) {
+__global__ void k_scalar_commit(const Dom<T> *__restrict__ doms, Launch L, int from) {
   typedef typename Vec2<T>::type V2;
   typedef float4 V;  // 16 bytes: 4 floats or 2 doubles
   static_assert(sizeof(V2) * 2 == sizeof(V) || sizeof(V2) == sizeof(V), "16-byte vectors");
@@ -375,8 +379,8 @@ __global__ void k_scalar_commit(const Dom<T> *__restrict__ doms, Launch L) {
     const long long nvec = d.plane * d.nz * (long long)sizeof(T) / 16;
     const int per = (int)((nvec + kCommitVecs - 1) / kCommitVecs);
     const int s = lt / per, c = lt % per;
-    const V *src = reinterpret_cast<const V *>(d.slot[s].n + d.plane);
-    V *dst = reinterpret_cast<V *>(d.slot[s].m + d.plane);
+    const V *src = reinterpret_cast<const V *>(d.slot[s].buf[from] + d.plane);
+    V *dst = reinterpret_cast<V *>(d.slot[s].buf[0] + d.plane);
     const long long v0 = (long long)c * kCommitVecs + threadIdx.x;
     V x[kCommitPer];
 #pragma unroll
@@ -406,7 +410,7 @@ __global__ void k_scalar_avg(const Dom<T> *__restrict__ doms, Launch L) {
     const bool xy = d.avg_k > 0 && r < ny;
     const int j = xy ? r + 1 : d.avg_j, k = xy ? d.avg_k : r - (d.avg_k > 0 ? ny : 0) + 1;
     double *acc = xy ? sl.acc_xy + (size_t)(j - 1) * nx : sl.acc_xz + (size_t)(k - 1) * nx;
-    const T *S = sl.m + bidx(d, 1, j, k);
+    const T *S = sl.buf[0] + bidx(d, 1, j, k);
     for (int i = threadIdx.x; i < nx; i += blockDim.x) acc[i] = acc[i] + ((double)S[i] + sl.off) * d.avg_w;
   }
 }
@@ -425,7 +429,7 @@ __global__ void k_unpack_scalar(const Dom<T> *__restrict__ dom, int s, const dou
     const int j = (int)(r % ny) + 1, k = (int)(r / ny) + 1;
     const double v = src[(i + 2) + n0 * ((j + 2) + n1 * (k + 2))];
     if (!isfinite(v)) atomicAdd(bad, 1);
-    d.slot[s].m[bidx(d, i, j, k)] = (T)(v - d.slot[s].off);
+    d.slot[s].buf[0][bidx(d, i, j, k)] = (T)(v - d.slot[s].off);
   }
 }
 
