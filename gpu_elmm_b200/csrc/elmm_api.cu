@@ -1750,6 +1750,8 @@ int elmm_server_create(const elmm_server_config *cfg, elmm_server **out) {
   if (cfg->max_active < 1 || cfg->max_active > ELMM_SERVER_MAX_ACTIVE)
     return fail(ELMM_ERR_INVALID_CONFIG, "max_active in 1.." + std::to_string(ELMM_SERVER_MAX_ACTIVE));
   if (cfg->chunk_steps < 1) return fail(ELMM_ERR_INVALID_CONFIG, "chunk_steps must be positive");
+  if (cfg->policy != ELMM_SERVE_FIFO && cfg->policy != ELMM_SERVE_SHORTEST_FIRST)
+    return fail(ELMM_ERR_INVALID_CONFIG, "unknown admission policy");
   if (cfg->hbm_budget_bytes < (1 << 20)) return fail(ELMM_ERR_INVALID_CONFIG, "hbm_budget_bytes below 1 MiB");
   elmm_server *s = new elmm_server();
   s->precision = cfg->precision;

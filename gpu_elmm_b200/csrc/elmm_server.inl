@@ -204,10 +204,14 @@ struct ServerT {
   void admit() {
     for (;;) {
       Req *r;
+      size_t qi = 0;
       {
         std::lock_guard<std::mutex> lk(mu);
         if (queue.empty() || (int)(active.size() + joining.size()) >= sc.max_active) return;
-        r = queue.front();
+        if (sc.policy == ELMM_SERVE_SHORTEST_FIRST)
+          for (size_t q = 1; q < queue.size(); q++)
+            if (queue[q]->cells * queue[q]->nsteps < queue[qi]->cells * queue[qi]->nsteps) qi = q;
+        r = queue[qi];
       }
       auto b = std::make_unique<BatchT<T>>();
       b->arena = &arena;
@@ -221,7 +225,7 @@ struct ServerT {
       }
       {
         std::lock_guard<std::mutex> lk(mu);
-        queue.pop_front();
+        queue.erase(queue.begin() + qi);
         st.queued = (int32_t)queue.size();
       }
       if (rc) {

@@ -37,7 +37,12 @@ class ServerConfig(C.Structure):
         ("hbm_budget_bytes", C.c_int64),
         ("max_active", C.c_int32),
         ("chunk_steps", C.c_int32),
+        ("policy", C.c_int32),
+        ("reserved", C.c_int32),
     ]
+
+
+SERVE_FIFO, SERVE_SHORTEST_FIRST = 0, 1
 
 
 class RequestInfo(C.Structure):
@@ -94,9 +99,10 @@ class Server:
     """One serving loop on one device.  The input arrays of a request are
     kept referenced here until the request has been reported."""
 
-    def __init__(self, *, precision=1, budget_bytes=8 << 30, max_active=64, chunk_steps=50, device=0):
+    def __init__(self, *, precision=1, budget_bytes=8 << 30, max_active=64, chunk_steps=50, device=0,
+                 policy=SERVE_FIFO):
         lib = _bind()
-        c = ServerConfig(device, precision, int(budget_bytes), max_active, chunk_steps)
+        c = ServerConfig(device, precision, int(budget_bytes), max_active, chunk_steps, policy, 0)
         h = C.c_void_p()
         L.check(lib.elmm_server_create(C.byref(c), C.byref(h)), "elmm_server_create")
         self.h = h
@@ -252,17 +258,20 @@ def main():
     ap.add_argument("--max-active", type=int, default=64)
     ap.add_argument("--chunk-steps", type=int, default=50)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--policy", default="fifo", choices=["fifo", "shortest"])
     a = ap.parse_args()
     prec = 1 if a.precision == "mixed" else 0
     reqs = [dispersion_request(a.seed, q) for q in range(a.requests)]
     inputs = [request_inputs(r) for r in reqs]
     for rate in (float(x) for x in a.rates.split(",")):
         srv = Server(precision=prec, budget_bytes=int(a.budget_gb * (1 << 30)), max_active=a.max_active,
-                     chunk_steps=a.chunk_steps)
+                     chunk_steps=a.chunk_steps, policy=SERVE_SHORTEST_FIRST if a.policy == "shortest" else SERVE_FIFO)
         arrivals = poisson_arrivals(a.seed, rate, len(reqs))
         done, span = run_arrivals(srv, reqs, arrivals, inputs, precision=prec)
         out = summarize(reqs, done, span, rate, srv)
         out["precision"] = a.precision
+        out["policy"] = a.policy
+        out["max_active"] = a.max_active
         print(json.dumps(out), flush=True)
         srv.close()
 

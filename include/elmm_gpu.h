@@ -355,7 +355,13 @@ typedef struct elmm_server_config {
   int64_t hbm_budget_bytes;     /* device memory the server holds for requests */
   int32_t max_active;           /* requests on the device at once, 1..ELMM_SERVER_MAX_ACTIVE */
   int32_t chunk_steps;          /* steps between admission points, >= 1 */
+  int32_t policy;               /* ELMM_SERVE_FIFO or ELMM_SERVE_SHORTEST_FIRST */
+  int32_t reserved;             /* 0 */
 } elmm_server_config;
+
+/* Admission order of queued requests: arrival order, or the least work
+ * (cells x steps) first, which lowers the median latency under load. */
+enum { ELMM_SERVE_FIFO = 0, ELMM_SERVE_SHORTEST_FIRST = 1 };
 
 typedef struct elmm_request_info {
   int64_t id;

@@ -207,3 +207,27 @@ def test_server_isolates_a_failing_request():
     axy, axz = _alone(good, 1)
     assert np.array_equal(xy, axy) and np.array_equal(xz, axz)
     srv.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("policy", [0, 1])
+def test_server_admission_order(policy):
+    """One request at a time: while a first request runs, a large and then a
+    small request queue up; arrival order admits the large one next, the
+    shortest-work-first policy the small one."""
+    from gpu_elmm_b200.serve import Server, request_config, request_inputs
+    first = {"n": (64, 64, 32), "steps": 300, "source": (3, 3, 3), "seed": 41}
+    large = {"n": (64, 64, 32), "steps": 60, "source": (4, 4, 4), "seed": 42}
+    small = {"n": (32, 32, 16), "steps": 10, "source": (5, 5, 5), "seed": 43}
+    srv = Server(precision=1, budget_bytes=2 << 30, max_active=1, chunk_steps=10, policy=policy)
+    names = {}
+    for r, name in ((first, "first"), (large, "large"), (small, "small")):
+        names[srv.submit(request_config(r), *request_inputs(r), nsteps=r["steps"])] = name
+    order = []
+    while len(order) < 3:
+        info = srv.wait_any(120000)
+        assert info is not None and info.status == 0
+        order.append(names[info.id])
+    assert order[0] == "first"
+    assert order[1:] == (["large", "small"] if policy == 0 else ["small", "large"])
+    srv.close()
