@@ -1048,16 +1048,14 @@ struct BatchT {
     k_cfl<T><<<gsz(8, ls[LK_CELLS].total), TX * TY, 0, stream>>>(ddom, ls[LK_CELLS].l());
     return ELMM_OK;
   }
-  void swap_state() {
-    // U <-> U2 after the projection wrote U directly: nothing to swap; the
-    // projection writes the new velocity into U (exchange_alloc in tsteps.f90:211-213)
-  }
   int run_stage(int stage, int stop, int accumulate = 0, bool standalone = false) {
     launch_sgs();
     if (stop == 1) return ELMM_OK;
     launch_momentum(stage);
     launch_scalars(stage, accumulate, standalone);  // ScalarRK3 between Convection and the projection (tsteps.f90:132-135)
     if (stop == 2) return ELMM_OK;
+    // the projection writes the new velocity into U itself, which takes the
+    // place of the U <-> U2 pointer exchange (exchange_alloc, tsteps.f90:211-213)
     launch_projection(2 * kAlpha[stage - 1], 1, 0);
     launch_refine(2 * kAlpha[stage - 1], 1);
     return ELMM_OK;

@@ -341,7 +341,6 @@ __host__ __device__ constexpr int fft_reg_batch(int n) { return kRegThreads / fp
 #endif
 constexpr int kTriCols = ELMM_TRI_COLS;
 constexpr int kTriSegs = ELMM_TRI_SEGS;
-constexpr int kTriTileThreads = 2 * kTriCols * kTriSegs;
 constexpr int kTriTileMaxNz = 256;
 
 __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
@@ -408,7 +407,7 @@ __global__ void k_tri_factors(double *c0, const double *__restrict__ lamx, const
 template <typename T, int COLS = kTriCols>
 __global__ void __launch_bounds__(tri_tile_threads<COLS>()) k_tri_tile(const Dom<T> *__restrict__ doms, Launch L,
                                                                       int gate) {
-  constexpr int kTriCols = COLS, kTriTileThreads = tri_tile_threads<COLS>();
+  constexpr int kTriCols = COLS, kTriTileThreads = tri_tile_threads<COLS>();  // this tile's shape
   typedef typename Vec2<T>::type T2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int kChunk = 16 / (int)sizeof(T2), kPerRow = kTriCols / kChunk, XS = 2 * kTriCols;
