@@ -250,7 +250,7 @@ struct LaunchSet {
 };
 
 enum { LK_CELLS = 0, LK_BOX, LK_ROWS, LK_YCOLS, LK_TRI, LK_MOM, LK_SHELL, LK_XREG, LK_YREG, LK_TRIT, LK_TCOL, LK_DCOL,
-       LK_AVG, LK_COMMIT, LK_TPAIR, LK_PROJ, LK_PROJ2, LK_N };
+       LK_AVG, LK_COMMIT, LK_TPAIR, LK_PROJ, LK_PROJ2, LK_DCOL2, LK_N };
 
 // -------------------------------------------------------------------- batch
 template <typename T>
@@ -619,7 +619,9 @@ struct BatchT {
         return scalar_pairs(h) ? ((h.nx + 2 * SPX - 1) / (2 * SPX)) * ((h.ny + tune_rows - 1) / tune_rows) *
                                      ((h.nz + TMKC - 1) / TMKC) * h.nslot
                                : 0;
-      case LK_DCOL: return ntx * nty * ((h.nz + kDivChunk - 1) / kDivChunk);
+      case LK_DCOL: return scalar_pairs(h) ? 0 : ntx * nty * ((h.nz + kDivChunk - 1) / kDivChunk);
+      case LK_DCOL2:
+        return scalar_pairs(h) ? ((h.nx + 2 * TX - 1) / (2 * TX)) * nty * ((h.nz + kDivChunk - 1) / kDivChunk) : 0;
       case LK_AVG: return (h.nslot - (h.buoy ? 1 : 0)) * ((h.avg_k > 0 ? h.ny : 0) + (h.avg_j > 0 ? h.nz : 0));
       case LK_COMMIT: {
         const long long nvec = h.plane * h.nz * (long long)sizeof(T) / 16;
@@ -1039,7 +1041,14 @@ struct BatchT {
   int launch_divmax() {
     nlaunch++;
     for (int d = 0; d < nd; d++) cudaMemsetAsync(hdom[d].maxdiv_bits, 0, sizeof(unsigned long long), stream);
-    k_divmax<T><<<gsz(7, ls[LK_DCOL].total), TX * TY, 0, stream>>>(ddom, ls[LK_DCOL].l());
+    if (ls[LK_DCOL].total > 0)
+      k_divmax<T><<<gsz(7, ls[LK_DCOL].total), TX * TY, 0, stream>>>(ddom, ls[LK_DCOL].l());
+    if constexpr (std::is_same<T, float>::value) {
+      if (ls[LK_DCOL2].total > 0) {
+        nlaunch += ls[LK_DCOL].total > 0 ? 1 : 0;
+        k_divmax_pair<<<gsz(7, ls[LK_DCOL2].total), TX * TY, 0, stream>>>(ddom, ls[LK_DCOL2].l());
+      }
+    }
     return ELMM_OK;
   }
   int launch_cfl() {

@@ -478,6 +478,57 @@ __global__ void __launch_bounds__(TX *TY) k_divmax(const Dom<T> *__restrict__ do
 }
 
 
+// k_divmax for FP32 domains with an even Prnx: two x-adjacent cells per
+// thread with float2 loads, a tile of 2 * TX x TY cells; the same FP64
+// arithmetic per cell.
+__global__ void __launch_bounds__(TX *TY) k_divmax_pair(const Dom<float> *__restrict__ doms, Launch L) {
+  __shared__ unsigned long long red[TX * TY / 32];
+  unsigned long long run = 0;
+  int cur = -1;
+  auto ld2 = [](const float *p, long long o) { return __ldg(reinterpret_cast<const float2 *>(p + o)); };
+  for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
+    const int di = find_dom(L.starts, L.nd, t);
+    if (di != cur) {  // block-uniform
+      if (cur >= 0) block_max_flush<TX * TY>(doms[cur].maxdiv_bits, run, red);
+      run = 0;
+      cur = di;
+    }
+    const Dom<float> &d = doms[di];
+    int lt = t - __ldg(L.starts + di);
+    const int nx = d.nx, ny = d.ny, nz = d.nz;
+    const int ntx = (nx + 2 * TX - 1) / (2 * TX), nty = (ny + TY - 1) / TY;
+    const int tx = lt % ntx; lt /= ntx;
+    const int ty = lt % nty;
+    const int k0 = (lt / nty) * kDivChunk + 1, k1 = min(k0 + kDivChunk - 1, nz);
+    const int i = tx * 2 * TX + 2 * (threadIdx.x % TX) + 1;  // odd: the pair is 8-byte aligned
+    const int j = ty * TY + (threadIdx.x / TX) + 1;
+    if (i > nx || j > ny) continue;
+    const float *__restrict__ U = d.U;
+    const float *__restrict__ V = d.V;
+    const float *__restrict__ W = d.W;
+    const long long pitch = d.pitch, plane = d.plane;
+    const double rdx = 1.0 / d.dx, rdy = 1.0 / d.dy, rdz = 1.0 / d.dz;
+    const bool vz = d.vz != 0;
+    const double *rdzk_tab = d.sgs_rdz;
+    long long c = bidx(d, i, j, k0);
+    float2 wb = ld2(W, c - plane);
+    for (int k = k0; k <= k1; k++) {
+      const double rdzk = vz ? rdzk_tab[k] : rdz;
+      const float2 wt = ld2(W, c), u = ld2(U, c), um = ld2(U, c - 2), v = ld2(V, c), vs = ld2(V, c - pitch);
+      const double a0 = fabs(((double)u.x - (double)um.y) * rdx + ((double)v.x - (double)vs.x) * rdy +
+                             ((double)wt.x - (double)wb.x) * rdzk);
+      const double a1 = fabs(((double)u.y - (double)u.x) * rdx + ((double)v.y - (double)vs.y) * rdy +
+                             ((double)wt.y - (double)wb.y) * rdzk);
+      const unsigned long long b0 = max_bits(a0), b1 = max_bits(a1);
+      run = b0 > run ? b0 : run;
+      run = b1 > run ? b1 : run;
+      wb = wt;
+      c += plane;
+    }
+  }
+  if (cur >= 0) block_max_flush<TX * TY>(doms[cur].maxdiv_bits, run, red);
+}
+
 // Defect correction of the mixed path: the divergence residual of the
 // FP32 velocity field evaluated in FP64 (the discrete divergence of
 // src/pressure.f90:688-717), stored as the right-hand side of a correction

@@ -554,3 +554,61 @@ def test_long_run_mixed_matches_fp64():
     assert c["u"] < 1e-2 and c["tke"] < 1e-2, c
     d64.close()
     dm.close()
+
+
+def test_odd_lengths_with_temperature_and_scalar():
+    """Odd Prnx and Prny (45 = 3^2 * 5, 27 = 3^3): the radix-3 and radix-5
+    FFT passes, and on the mixed path the one-cell-per-thread stencil, scalar
+    and projection kernels that an odd Prnx selects.  FP64 GPU against the
+    oracle after 3 steps (flow, temperature, scalar, slices); mixed against
+    FP64 GPU within 1e-5."""
+    n, src = (45, 27, 16), (7, 20, 5)
+    g, o, d = _dispersion_pair(_dispersion_cfg(n, src, steps=3, buoyancy=True), src, seed=4)
+    o.step(3)
+    d.step(3)
+    m = (g.Prnx, g.Prny, g.Prnz)
+    for a, b, name in zip(interiors(g, *d.download()), interiors(g, *o.state()), "UVWP"):
+        assert rel(a, b) < (1e-11 if name == "P" else 1e-12), (name, rel(a, b))
+    assert rel(interior(d.scalar(1), -2, m), interior(o.get_field(16), -2, m)) < 1e-11
+    assert rel(interior(d.temperature(), -2, m) - 295.0, interior(o.get_field(12), -2, m) - 295.0) < 1e-11
+    for a, b in zip(d.scalar_slices(1), o.scalar_slices(1)):
+        assert rel(a, b) < 1e-11
+    _, _, dm = _dispersion_pair(_dispersion_cfg(n, src, precision=1, steps=3, buoyancy=True), src, seed=4)
+    dm.step(3)
+    for a, b in zip(interiors(g, *dm.download())[:3], interiors(g, *d.download())[:3]):
+        assert rel(a, b) < 1e-5, rel(a, b)
+    assert rel(interior(dm.scalar(1), -2, m), interior(d.scalar(1), -2, m)) < 1e-5
+    d.close()
+    dm.close()
+
+
+@pytest.mark.parametrize("case", ["even", "odd", "stretched"])
+def test_mixed_divergence_maximum_is_exact(case):
+    """The max |div u| a mixed step reports equals the FP64 divergence of the
+    FP32 velocities it leaves behind (downloaded and recomputed here): the
+    two-cells-per-thread kernel for an even Prnx, one cell per thread for an
+    odd one, the 1 / dzPr(k) table of a stretched grid.  The device multiplies
+    by reciprocal spacings and contracts to FMAs: within a few units in the
+    last place of the terms."""
+    n, kw = {"even": ((64, 48, 24), {}), "odd": ((45, 27, 16), {}),
+             "stretched": ((64, 48, 20), {"zW": stretched(20)})}[case]
+    cfg = make_config(*n, precision=1, dx=1.25, dy=0.75, dz=1.125, **kw)  # uniform: i * dx exact
+    g = grid_of(cfg)
+    d = L.Domain(cfg)
+    d.upload(*log_profile_state(g, seed=5, zW=kw.get("zW")))
+    d.project(1.0)
+    s = d.step(2)
+    U, V, W, _ = d.download()
+    nx, ny, nz = g.Prnx, g.Prny, g.Prnz
+    o = 2  # array position of index 0 (lower bound -2)
+    zW = kw["zW"] if "zW" in kw else cfg.dzmin * np.arange(nz + 1)
+    dzpr = np.diff(zW)[:, None, None]
+    div = (np.diff(U[o + 1:o + nz + 1, o + 1:o + ny + 1, o:o + nx + 1], axis=2) / cfg.dxmin +
+           np.diff(V[o + 1:o + nz + 1, o:o + ny + 1, o + 1:o + nx + 1], axis=1) / cfg.dymin +
+           np.diff(W[o:o + nz + 1, o + 1:o + ny + 1, o + 1:o + nx + 1], axis=0) / dzpr)
+    ref = float(np.abs(div).max())
+    # the divergence is a cancellation of terms of size |U| / dx: rounding
+    # differences are bounded by a few ulps of those terms, not of the result
+    scale = np.abs(U).max() / cfg.dxmin + np.abs(V).max() / cfg.dymin + np.abs(W).max() / dzpr.min()
+    assert 0 < ref and abs(s.max_div - ref) <= 8 * np.finfo(np.float64).eps * scale, (s.max_div, ref)
+    d.close()
