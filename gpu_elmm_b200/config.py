@@ -11,7 +11,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 # Boundary-condition codes of src/parameters.f90:249-250.
 BC_NOSLIP, BC_FREESLIP, BC_PERIODIC, BC_DIRICHLET, BC_NEUMANN, BC_CONSTFLUX = 1, 2, 3, 4, 5, 6
@@ -82,6 +82,37 @@ class ElmmConfig(C.Structure):
         ("avg_slice_k", C.c_int32),
         ("avg_slice_j", C.c_int32),
         ("avg_weight", C.c_double),
+    ]
+
+
+IB_MAX_INTERP = 6
+
+
+class ElmmIBPoint(C.Structure):
+    """TIBPoint (src/immersedboundary.f90:552-564)."""
+    _fields_ = [
+        ("xi", C.c_int32), ("yj", C.c_int32), ("zk", C.c_int32), ("interp", C.c_int32),
+        ("ii", C.c_int32 * IB_MAX_INTERP), ("jj", C.c_int32 * IB_MAX_INTERP), ("kk", C.c_int32 * IB_MAX_INTERP),
+        ("coef", C.c_double * IB_MAX_INTERP),
+    ]
+
+
+class ElmmWMPoint(C.Structure):
+    """WMPointUVW at a solid face (src/wallmodels.f90:68-98)."""
+    _fields_ = [
+        ("component", C.c_int32), ("direction", C.c_int32),
+        ("xi", C.c_int32), ("yj", C.c_int32), ("zk", C.c_int32), ("reserved", C.c_int32),
+        ("dist", C.c_double * 3), ("z0", C.c_double),
+    ]
+
+
+class ElmmSolids(C.Structure):
+    _fields_ = [
+        ("n_ib", C.c_int64 * 3), ("ib", C.POINTER(ElmmIBPoint) * 3),
+        ("n_null", C.c_int64 * 3), ("null_ijk", C.POINTER(C.c_int32) * 3),
+        ("n_scalfl", C.c_int64), ("scalfl", C.POINTER(ElmmIBPoint)),
+        ("n_wm", C.c_int64), ("wm", C.POINTER(ElmmWMPoint)),
+        ("n_bottom_skip", C.c_int64 * 3), ("bottom_skip_ij", C.POINTER(C.c_int32) * 3),
     ]
 
 

@@ -23,6 +23,7 @@
 #include "elmm_kernels2.cuh"
 #include "elmm_poisson_reg.cuh"
 #include "elmm_temperature.cuh"
+#include "elmm_solids.cuh"
 #include "elmm_arena.h"
 
 using namespace elmm;
@@ -315,6 +316,23 @@ struct BatchT {
   cudaStream_t branch[kBranches] = {};
   cudaEvent_t ev_fork = nullptr, ev_join[kBranches] = {};
   float tune_ms[4] = {0, 0, 0, 0};  // rows 8, rows 4, cols 16, cols 32
+  // immersed solid bodies per domain (elmm_set_solids): the gathers of the
+  // velocity IB points followed by the nullified points, the gathers of the
+  // ScalFl viscosity, the solid-face wall-model points and their u* state
+  struct SolidSet {
+    IBGather *vel = nullptr, *visc = nullptr;
+    int nvel = 0, nib = 0, nvisc = 0;
+    WMSolid *wm = nullptr;
+    double *wm_ustar = nullptr;
+    int nwm = 0;
+    unsigned char *bskip[3] = {nullptr, nullptr, nullptr};
+    bool on = false, primed = false;
+  };
+  std::vector<SolidSet> sol;
+  bool any_solids() const {
+    for (auto &x : sol) if (x.on) return true;
+    return false;
+  }
 
   ~BatchT() { release(); }
 
@@ -1057,23 +1075,72 @@ struct BatchT {
     k_cfl<T><<<gsz(8, ls[LK_CELLS].total), TX * TY, 0, stream>>>(ddom, ls[LK_CELLS].l());
     return ELMM_OK;
   }
-  int run_stage(int stage, int stop, int accumulate = 0, bool standalone = false) {
+  // the solid-body launches of one stage phase (no-ops without bodies)
+  // which: 0 viscosity of the ScalFl points, 1 wall-model corrections and the
+  // IB points of U2 zeroed, 2 NullInterior + IBMomentum on the new velocity
+  void launch_ib(int which, int stage) {
+    for (int d = 0; d < nd && d < (int)sol.size(); d++) {
+      const SolidSet &x = sol[d];
+      if (!x.on) continue;
+      if (which == 0 && x.nvisc > 0) {
+        nlaunch++;
+        k_ib_gather<T><<<std::min((x.nvisc + 255) / 256, 148 * 8), 256, 0, stream>>>(ddom, d, x.visc, x.nvisc, 0);
+      }
+      if (which == 1) {
+        if (x.nwm > 0) {
+          nlaunch++;
+          k_ib_wm<T><<<std::min((x.nwm + 127) / 128, 148 * 8), 128, 0, stream>>>(ddom, d, x.wm, x.wm_ustar, x.nwm,
+                                                                               kBeta[stage - 1] * cfg[d].dt);
+        }
+        if (x.nib > 0) {
+          nlaunch++;
+          k_ib_gather<T><<<std::min((x.nib + 255) / 256, 148 * 8), 256, 0, stream>>>(ddom, d, x.vel, x.nib, 1);
+        }
+      }
+      if (which == 2 && x.nvel > 0) {
+        nlaunch++;
+        k_ib_gather<T><<<std::min((x.nvel + 255) / 256, 148 * 8), 256, 0, stream>>>(ddom, d, x.vel, x.nvel, 0);
+      }
+    }
+  }
+  // div: the divergence check of the step, taken on the projected field before
+  // IBMomentum replaces the IB points (the check of PostPoisson,
+  // src/pressure.f90:884-989, is div U - Q on that field)
+  int run_stage(int stage, int stop, int accumulate = 0, bool standalone = false, bool div = false) {
     launch_sgs();
+    if (any_solids()) launch_ib(0, stage);  // after BoundViscosity (src/dynamics.f90:896-902)
     if (stop == 1) return ELMM_OK;
     launch_momentum(stage);
     launch_scalars(stage, accumulate, standalone);  // ScalarRK3 between Convection and the projection (tsteps.f90:132-135)
+    if (any_solids()) launch_ib(1, stage);
     if (stop == 2) return ELMM_OK;
     // the projection writes the new velocity into U itself, which takes the
     // place of the U <-> U2 pointer exchange (exchange_alloc, tsteps.f90:211-213)
     launch_projection(2 * kAlpha[stage - 1], 1, 0);
     launch_refine(2 * kAlpha[stage - 1], 1);
+    if (any_solids()) {
+      if (div) launch_divmax();
+      launch_ib(2, stage);  // NullInterior, BoundUVW, IBMomentum, BoundUVW (tsteps.f90:201-206)
+      launch_ghosts({F_U, F_V, F_W}, 0);
+    }
     return ELMM_OK;
   }
   int enqueue_step(bool cfl, bool div) {
     if (cfl) launch_cfl();
-    for (int s = 1; s <= 3; s++) run_stage(s, 3, s == 3);
-    if (div) launch_divmax();
+    for (int s = 1; s <= 3; s++) run_stage(s, 3, s == 3, false, div && s == 3);
+    if (div && !any_solids()) launch_divmax();
     return ELMM_OK;
+  }
+  // the first TMarchRK3 call after the bodies were set: IBMomentum on the
+  // state, the ghosts left as they are (src/tsteps.f90:44-48)
+  void prime_solids() {
+    for (int d = 0; d < nd && d < (int)sol.size(); d++) {
+      SolidSet &x = sol[d];
+      if (!x.on || x.primed) continue;
+      if (x.nib > 0)
+        k_ib_gather<T><<<std::min((x.nib + 255) / 256, 148 * 8), 256, 0, stream>>>(ddom, d, x.vel, x.nib, 0);
+      x.primed = true;
+    }
   }
 
   int step(int nsteps, elmm_stats *st) {
@@ -1138,6 +1205,175 @@ struct BatchT {
     return ELMM_OK;
   }
 
+  // ------------------------------------------------------------ solids
+  void drop_solids(int d) {
+    if (d >= (int)sol.size()) return;
+    SolidSet &x = sol[d];
+    for (void *p : {(void *)x.vel, (void *)x.visc, (void *)x.wm, (void *)x.wm_ustar, (void *)x.bskip[0],
+                    (void *)x.bskip[1], (void *)x.bskip[2]})
+      if (p) dfree(p);
+    x = SolidSet();
+    for (int c = 0; c < 3; c++) hdom[d].bskip[c] = nullptr;
+  }
+  // elmm_set_solids: checks the lists, turns (i, j, k) into box indices with
+  // the ghost folds applied, uploads them and marks the step graph stale
+  int set_solids(int d, const elmm_solids *s) {
+    CU(cudaSetDevice(device));
+    CU(cudaStreamSynchronize(stream));
+    if ((int)sol.size() < nd) sol.resize(nd);
+    drop_solids(d);
+    if (step_exec) { cudaGraphExecDestroy(step_exec); step_exec = nullptr; }
+    if (!s) return push_dom(d);
+    Dom<T> &h = hdom[d];
+    const elmm_config &c = cfg[d];
+    if (c.enable_buoyancy || c.num_scalars > 0)
+      return fail(ELMM_ERR_INVALID_ARG, "solid bodies with a temperature or passive scalars are not supported");
+    if (!h.wall[SIDE_BO] || h.bt[SIDE_BO] != BC_NOSLIP)
+      return fail(ELMM_ERR_INVALID_ARG, "solid bodies need the wall model on a no-slip bottom");
+    const bool per[3] = {h.bt[SIDE_WE] == BC_PERIODIC, h.bt[SIDE_SO] == BC_PERIODIC, h.bt[SIDE_BO] == BC_PERIODIC};
+    // extents: 0..2 velocity components, 3 the pressure grid (viscosity)
+    auto ext = [&](int comp, int a) { return comp < 3 ? h.ext[comp][a] : (a == 0 ? h.nx : a == 1 ? h.ny : h.nz); };
+    auto in_target = [&](int comp, int i, int j, int k) {
+      const int v[3] = {i, j, k};
+      for (int a = 0; a < 3; a++) {
+        const int lo = per[a] ? 2 : 1, hi = per[a] ? ext(comp, a) - 1 : ext(comp, a);
+        if (v[a] < lo || v[a] > hi) return false;
+      }
+      return true;
+    };
+    // a source one cell into the ghosts -> the interior cell its ghost copies
+    auto fold = [&](int comp, int i, int j, int k, long long &idx, double &sign) {
+      const int v[3] = {i, j, k};
+      int o[3];
+      sign = 1;
+      for (int a = 0; a < 3; a++) {
+        const int n = ext(comp, a);
+        if (v[a] < 0 || v[a] > n + 1) return false;
+        if (comp < 3) {
+          Fold f = fold_vel(v[a], n, h.bt[2 * a], h.bt[2 * a + 1], a == comp);
+          o[a] = f.src;
+          if (f.zero) sign = 0;
+          else sign *= f.sign;
+        } else {
+          o[a] = fold_rep(v[a], n, per[a]);
+        }
+      }
+      idx = bidx(h, o[0], o[1], o[2]);
+      return true;
+    };
+    std::vector<IBGather> vel, visc;
+    std::vector<long long> targets[4];
+    auto add_points = [&](int comp, const elmm_ib_point *pts, int64_t n, std::vector<IBGather> &out) {
+      for (int64_t q = 0; q < n; q++) {
+        const elmm_ib_point &p = pts[q];
+        if (!in_target(comp, p.xi, p.yj, p.zk) || p.interp < 0 || p.interp > ELMM_IB_MAX_INTERP) return false;
+        IBGather g{};
+        g.tgt = bidx(h, p.xi, p.yj, p.zk);
+        g.comp = comp;
+        g.n = p.interp;
+        for (int m = 0; m < p.interp; m++) {
+          double sg;
+          if (!fold(comp, p.ii[m], p.jj[m], p.kk[m], g.src[m], sg) || !std::isfinite(p.coef[m])) return false;
+          g.coef[m] = p.coef[m] * sg;
+        }
+        targets[comp].push_back(g.tgt);
+        out.push_back(g);
+      }
+      return true;
+    };
+    for (int comp = 0; comp < 3; comp++)
+      if (s->n_ib[comp] < 0 || (s->n_ib[comp] > 0 && !s->ib[comp]) ||
+          !add_points(comp, s->ib[comp], s->n_ib[comp], vel))
+        return fail(ELMM_ERR_INVALID_ARG, "IB point out of range (or within one cell of a periodic boundary)");
+    const int nib = (int)vel.size();
+    for (int comp = 0; comp < 3; comp++) {
+      if (s->n_null[comp] < 0 || (s->n_null[comp] > 0 && !s->null_ijk[comp]))
+        return fail(ELMM_ERR_INVALID_ARG, "nullified points");
+      for (int64_t q = 0; q < s->n_null[comp]; q++) {
+        const int32_t *t = s->null_ijk[comp] + 3 * q;
+        if (!in_target(comp, t[0], t[1], t[2]))
+          return fail(ELMM_ERR_INVALID_ARG, "nullified point out of range (or within one cell of a periodic boundary)");
+        IBGather g{};
+        g.tgt = bidx(h, t[0], t[1], t[2]);
+        g.comp = comp;
+        g.n = -1;
+        targets[comp].push_back(g.tgt);
+        vel.push_back(g);
+      }
+    }
+    if (s->n_scalfl < 0 || (s->n_scalfl > 0 && !s->scalfl) || !add_points(3, s->scalfl, s->n_scalfl, visc))
+      return fail(ELMM_ERR_INVALID_ARG, "ScalFl point out of range (or within one cell of a periodic boundary)");
+    // one parallel pass is exact only if no point reads a value the pass writes
+    for (int comp = 0; comp < 4; comp++) std::sort(targets[comp].begin(), targets[comp].end());
+    auto is_target = [&](int comp, long long i) {
+      return std::binary_search(targets[comp].begin(), targets[comp].end(), i);
+    };
+    for (auto *list : {&vel, &visc})
+      for (auto &g : *list)
+        for (int m = 0; m < g.n; m++)
+          if (g.coef[m] != 0 && is_target(g.comp, g.src[m]))
+            return fail(ELMM_ERR_INVALID_ARG, "an interpolation point is itself a forcing or nullified point");
+    std::vector<WMSolid> wm;
+    if (s->n_wm < 0 || (s->n_wm > 0 && !s->wm)) return fail(ELMM_ERR_INVALID_ARG, "wall-model points");
+    for (int64_t q = 0; q < s->n_wm; q++) {
+      const elmm_wm_point &p = s->wm[q];
+      const int comp = p.component - 1;
+      if (comp < 0 || comp > 2 || p.direction < 1 || p.direction > 6 || !(p.z0 > 0) ||
+          p.xi < 1 || p.xi > h.ext[comp][0] || p.yj < 1 || p.yj > h.ext[comp][1] || p.zk < 1 || p.zk > h.ext[comp][2])
+        return fail(ELMM_ERR_INVALID_ARG, "solid-face wall-model point out of range (rough walls only)");
+      WMSolid w{};
+      w.c = bidx(h, p.xi, p.yj, p.zk);
+      w.comp = comp;
+      w.dir = p.direction;
+      w.k = p.zk;
+      for (int a = 0; a < 3; a++) w.dist[a] = p.dist[a];
+      w.z0 = p.z0;
+      if (!(norm_host(w.dist) > 0)) return fail(ELMM_ERR_INVALID_ARG, "wall-model point on the wall");
+      wm.push_back(w);
+    }
+    SolidSet &x = sol[d];
+    int r;
+    auto up = [&](void **dst, const void *src, size_t bytes) {
+      if (bytes == 0) return (int)ELMM_OK;
+      int rr = dalloc(dst, bytes);
+      if (rr) return rr;
+      return cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice) == cudaSuccess ? (int)ELMM_OK
+                                                                                 : fail(ELMM_ERR_CUDA, "cudaMemcpy");
+    };
+    if ((r = up((void **)&x.vel, vel.data(), vel.size() * sizeof(IBGather)))) return r;
+    if ((r = up((void **)&x.visc, visc.data(), visc.size() * sizeof(IBGather)))) return r;
+    if ((r = up((void **)&x.wm, wm.data(), wm.size() * sizeof(WMSolid)))) return r;
+    std::vector<double> us(wm.size(), 1.0);  // WMPointUVW%ustar starts at 1 (immersedboundary.f90:235)
+    if ((r = up((void **)&x.wm_ustar, us.data(), us.size() * sizeof(double)))) return r;
+    x.nvel = (int)vel.size();
+    x.nib = nib;
+    x.nvisc = (int)visc.size();
+    x.nwm = (int)wm.size();
+    for (int comp = 0; comp < 3; comp++) {
+      const int e0 = h.ext[comp][0], e1 = h.ext[comp][1];
+      std::vector<unsigned char> m((size_t)e0 * e1, 0);
+      if (s->n_bottom_skip[comp] < 0 || (s->n_bottom_skip[comp] > 0 && !s->bottom_skip_ij[comp]))
+        return fail(ELMM_ERR_INVALID_ARG, "bottom skip list");
+      for (int64_t q = 0; q < s->n_bottom_skip[comp]; q++) {
+        const int32_t *t = s->bottom_skip_ij[comp] + 2 * q;
+        if (t[0] < 1 || t[0] > e0 || t[1] < 1 || t[1] > e1) return fail(ELMM_ERR_INVALID_ARG, "bottom skip point");
+        m[(size_t)(t[0] - 1) + (size_t)e0 * (t[1] - 1)] = 1;
+      }
+      if (s->n_bottom_skip[comp] > 0) {
+        if ((r = up((void **)&x.bskip[comp], m.data(), m.size()))) return r;
+        h.bskip[comp] = x.bskip[comp];
+      }
+    }
+    x.on = true;
+    x.primed = false;
+    return push_dom(d);
+  }
+  static double norm_host(const double *v) { return std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]); }
+  int push_dom(int d) {
+    CU(cudaMemcpy(ddom + d, &hdom[d], sizeof(Dom<T>), cudaMemcpyHostToDevice));
+    return ELMM_OK;
+  }
+
   // enqueues nsteps replays of the step graph (captured on first use) without
   // waiting for them
   int step_launch(int nsteps) {
@@ -1163,6 +1399,7 @@ struct BatchT {
       step_has_cfl = cfl;
     }
     for (int d = 0; d < nd; d++) CU(cudaMemsetAsync(hdom[d].refine_count, 0, sizeof(int), stream));
+    if (nsteps > 0) prime_solids();
     CU(cudaEventRecord(t0, stream));
     for (int s = 0; s < nsteps; s++) CU(cudaGraphLaunch(step_exec, stream));
     CU(cudaEventRecord(t1, stream));
@@ -1702,6 +1939,11 @@ int elmm_step(elmm_handle *h, int32_t nsteps, elmm_stats *st) {
   if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
   if (nsteps < 0) return fail(ELMM_ERR_INVALID_ARG, "nsteps < 0");
   return DISPATCH(h->b, step(nsteps, st));
+}
+
+int elmm_set_solids(elmm_handle *h, const elmm_solids *s) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  return DISPATCH(h->b, set_solids(0, s));
 }
 
 int elmm_run_stage(elmm_handle *h, int32_t stage, int32_t stop) {

@@ -98,6 +98,9 @@ struct Dom {
   // wall model: per face plane fluxp/fluxm/ustar, plane dims from ext[]
   T *wm_fluxp[kFaces], *wm_fluxm[kFaces];
   double *wm_ustar[kFaces];
+  // per component: 1 marks a bottom-plane point without a wall-model point
+  // (next to or under a solid body), or null for none
+  const unsigned char *bskip[3];
   double z0[6];
   // pressure reference: stored P = true Pr + prm; top-layer partial sums
   double *prm;           // 1 value

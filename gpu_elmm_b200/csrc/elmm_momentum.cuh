@@ -39,6 +39,7 @@ struct MomCtx {
   int ext[3][3];
   const double *dzPr, *dzW, *zPr, *zW;
   const T *fluxp[kFaces], *fluxm[kFaces];
+  const unsigned char *bskip[3];
 };
 
 template <typename T>
@@ -55,6 +56,7 @@ __device__ __forceinline__ void fill_ctx(MomCtx<T> &m, const Dom<T> &d) {
   m.vz = d.vz;
   m.dzPr = d.dzPr; m.dzW = d.dzW; m.zPr = d.zPr; m.zW = d.zW;
   for (int f = 0; f < kFaces; f++) { m.fluxp[f] = d.wm_fluxp[f]; m.fluxm[f] = d.wm_fluxm[f]; }
+  for (int c = 0; c < 3; c++) m.bskip[c] = d.bskip[c];
 }
 
 // one velocity component's tendency at (i,j,k): advection + diffusion +
@@ -131,7 +133,8 @@ __device__ __forceinline__ T tendency(const MomCtx<T> &m, const RT &R, int i, in
         a = a - (nne + ne + nn + n0) * (un - u) * ry / 4;
         a = a - m.fluxm[0 * 6 + SIDE_NO][p];
       }
-      if ((m.wallmask & (1 << SIDE_BO)) && k == 1) {
+      if ((m.wallmask & (1 << SIDE_BO)) && k == 1 &&
+          !(m.bskip[0] && m.bskip[0][(long long)(i - 1) + (long long)e[0] * (j - 1)])) {
         long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
         T s = ne + nbe + n0 + nb;
         if (m.vz) a = a + s * (u - ub) / (T)m.dzW[k - 1 + 2] / 4 / (T)m.dzPr[k + 2];
@@ -206,7 +209,8 @@ __device__ __forceinline__ T tendency(const MomCtx<T> &m, const RT &R, int i, in
         a = a - nn * (vn - v) * ry;
         a = a - m.fluxm[1 * 6 + SIDE_NO][p];
       }
-      if ((m.wallmask & (1 << SIDE_BO)) && k == 1) {
+      if ((m.wallmask & (1 << SIDE_BO)) && k == 1 &&
+          !(m.bskip[1] && m.bskip[1][(long long)(i - 1) + (long long)e[0] * (j - 1)])) {
         long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
         T s = nn + nnb + n0 + nb;
         if (m.vz) a = a + s * (v - vb) / (T)m.dzW[k - 1 + 2] / 4 / (T)m.dzPr[k + 2];
@@ -282,7 +286,8 @@ __device__ __forceinline__ T tendency(const MomCtx<T> &m, const RT &R, int i, in
         a = a - (ntn + nt + nn + n0) * (wn - w) * ry / 4;
         a = a - m.fluxm[2 * 6 + SIDE_NO][p];
       }
-      if ((m.wallmask & (1 << SIDE_BO)) && k == 1) {
+      if ((m.wallmask & (1 << SIDE_BO)) && k == 1 &&
+          !(m.bskip[2] && m.bskip[2][(long long)(i - 1) + (long long)e[0] * (j - 1)])) {
         long long p = (long long)(i - 1) + (long long)e[0] * (j - 1);
         if (m.vz) a = a + n0 * (w - wb) / (T)m.dzPr[k + 2] / (T)m.dzW[k + 2];
         else a = a + n0 * (w - wb) * rz;

@@ -49,6 +49,7 @@ def lib():
         L.elmm_download_state.argtypes = [P, _dp, _dp, _dp, _dp]
         L.elmm_upload_temperature.argtypes = [P, _dp]
         L.elmm_upload_scalar.argtypes = [P, C.c_int32, _dp]
+        L.elmm_set_solids.argtypes = [P, P]
         L.elmm_download_scalar_slices.argtypes = [P, C.c_int32, _dp, _dp]
         L.elmm_reset_scalar_averages.argtypes = [P]
         L.elmm_download_field.argtypes = [P, C.c_int32, _dp]
@@ -135,6 +136,12 @@ class Domain:
 
     def temperature(self):
         return self.field(12)
+
+    def set_solids(self, solids):
+        """Installs solid bodies (gpu_elmm_b200.solids.Solids, or None to remove them)."""
+        st = None if solids is None else solids.struct()
+        check(lib().elmm_set_solids(self.h, None if st is None else C.cast(C.byref(st), C.c_void_p)),
+              "elmm_set_solids")
 
     def upload_scalar(self, sc, S):
         """Scalar(-2:nx+3,-2:ny+3,-2:nz+3,sc), host array, sc in 1..num_scalars."""

@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define ELMM_ABI_VERSION 3
+#define ELMM_ABI_VERSION 4
 
 /* Status codes. */
 enum {
@@ -210,6 +210,70 @@ int elmm_upload_temperature(elmm_handle *h, const double *T);
  * Scalar(-2:Prnx+3,-2:Prny+3,-2:Prnz+3,sc) (only the interior is read).
  * Returns ELMM_ERR_NAN for non-finite values. */
 int elmm_upload_scalar(elmm_handle *h, int32_t sc, const double *S);
+
+/* ---- immersed solid bodies ----------------------------------------------
+ * The host describes its solid bodies by the point lists its own geometry
+ * pass builds once at start-up: GetSolidBodiesBC (FindInsideCells,
+ * FindNeighbouringCells, InitImBoundaries, GetSolidBodiesWM_UVW;
+ * src/immersedboundary.f90:1750-1771, src/solidbodies.f90:75-206) and
+ * SetNullifiedPoints (src/initial.f90:4861-4962).  The library then applies,
+ * every RK3 stage as TMarchRK3 does (src/tsteps.f90:146-206):
+ *   - the viscosity of the ScalFl points from their interpolation points
+ *     (SubgridStresses, src/dynamics.f90:899-902);
+ *   - the wall-model fluxes at the solid faces (ComputeUVWFluxesWM and the
+ *     wmfluxes-*-inc.f90 corrections, src/wallmodels.f90:2159-2338);
+ *   - IBMomentum, IBMassSources and NullInterior (src/tsteps.f90:360-567).
+ * Indices are the reference's: 1..n of the point's own field; interpolation
+ * points may lie one cell into the ghost layer. */
+#define ELMM_IB_MAX_INTERP 6
+
+/* TIBPoint (src/immersedboundary.f90:552-564): the value at (xi,yj,zk) is
+ * replaced by sum_n coef[n] * F(ii[n],jj[n],kk[n]) (TIBPoint_Interpolate,
+ * :637-651); interp = 0 sets it to zero. */
+typedef struct elmm_ib_point {
+  int32_t xi, yj, zk;
+  int32_t interp;
+  int32_t ii[ELMM_IB_MAX_INTERP], jj[ELMM_IB_MAX_INTERP], kk[ELMM_IB_MAX_INTERP];
+  double coef[ELMM_IB_MAX_INTERP];
+} elmm_ib_point;
+
+/* WMPointUVW at a solid face (src/wallmodels.f90:68-98, built by
+ * GetSolidBodiesWM_UVW, src/immersedboundary.f90:139-306): a free velocity
+ * point of `component` (1 U, 2 V, 3 W) whose neighbour in `direction`
+ * (1..6 = -x, +x, -y, +y, -z, +z) is solid; dist is the vector to the
+ * nearest point of the body, z0 its roughness length (> 0). */
+typedef struct elmm_wm_point {
+  int32_t component, direction;
+  int32_t xi, yj, zk, reserved;
+  double dist[3];
+  double z0;
+} elmm_wm_point;
+
+typedef struct elmm_solids {
+  int64_t n_ib[3];                   /* UIBPoints, VIBPoints, WIBPoints */
+  const elmm_ib_point *ib[3];
+  int64_t n_null[3];                 /* Unull, Vnull, Wnull: (i, j, k) triples */
+  const int32_t *null_ijk[3];
+  int64_t n_scalfl;                  /* ScalFlIBPoints (viscosity interpolation) */
+  const elmm_ib_point *scalfl;
+  int64_t n_wm;                      /* wall-model points at solid faces */
+  const elmm_wm_point *wm;
+  /* (i, j) pairs of the bottom-wall plane k = 1 that carry no wall-model
+   * point, per component: GetOutsideBoundariesWM_UVW adds a bottom point only
+   * where Xtype(i,j,1) == 0 and Xtype(i,j,0) <= 0 (src/wallmodels.f90:700-820) */
+  int64_t n_bottom_skip[3];
+  const int32_t *bottom_skip_ij[3];
+} elmm_solids;
+
+/* Installs the solid bodies of a single-domain handle (copied; the host
+ * arrays may be freed afterwards).  Requirements, checked here
+ * (ELMM_ERR_INVALID_ARG otherwise): indices in range; no interpolation point
+ * of a list is a forcing point of the same list; no forcing or nullified
+ * point within one cell of a periodic boundary; a rough bottom wall with the
+ * wall model; no temperature and no passive scalars.  The next elmm_step
+ * applies IBMomentum once first, as the first call of TMarchRK3 does
+ * (src/tsteps.f90:44-48).  Passing NULL removes the bodies. */
+int elmm_set_solids(elmm_handle *h, const elmm_solids *s);
 
 /* The time-averaged slices of scalar sc: xy(1:Prnx,1:Prny) at avg_slice_k and
  * xz(1:Prnx,1:Prnz) at avg_slice_j, column-major; either pointer may be NULL.

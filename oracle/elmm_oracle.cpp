@@ -27,6 +27,7 @@
 //   Poisson solve; PRESSURE_REFERENCE_BOUNDARY at To; RK3.
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <complex>
 #include <cstdint>
@@ -179,6 +180,13 @@ struct Domain {
   int avg_k, avg_j;
   double avg_w;
   std::vector<double> acc_xy[ELMM_MAX_SCALARS], acc_xz[ELMM_MAX_SCALARS];
+  // immersed solids: UIBPoints.. (index = component), ScalFlIBPoints, Unull..
+  // (src/immersedboundary.f90:519-580, src/tsteps.f90:360-567)
+  bool solids = false;
+  std::vector<elmm_ib_point> ibp[4], scalfl;
+  std::vector<std::array<int, 3>> nullp[4];
+  A3 Q;        // IBMassSources, Q(0:Prnx+1,0:Prny+1,0:Prnz+1)
+  int called = 0;  // the "called" flag of TMarchRK3 (src/tsteps.f90:35)
 };
 
 // ------------------------------------------------- grid, initial.f90:4395-4480
@@ -661,10 +669,19 @@ static void ComputeTDiff(Domain &d) {
 
 // SubgridStresses, dynamics.f90:869-908 (ComputeViscsWM only sets Viscosity at
 // wall cells, which SubgridModel then overwrites everywhere; it is omitted).
+// TIBPoint_Interpolate, immersedboundary.f90:637-651
+static double IBInterpolate(const elmm_ib_point &p, const A3 &F) {
+  double v = 0;
+  for (int n = 0; n < p.interp; n++) v = v + p.coef[n] * F(p.ii[n], p.jj[n], p.kk[n]);
+  return v;
+}
+
 static void SubgridStresses(Domain &d) {
   SubgridModel(d);
   if (d.wallmodeltype > 0) ComputeUVWFluxesWM(d);
   BoundViscosity(d, d.Viscosity);
+  // viscosity of the ScalFl IB points, in place in list order (dynamics.f90:899-902)
+  for (auto &p : d.scalfl) d.Viscosity(p.xi, p.yj, p.zk) = IBInterpolate(p, d.Viscosity);
   if (d.enable_buoyancy) ComputeTDiff(d);  // dynamics.f90:904
   if (d.enable_buoyancy || d.num_scalars > 0) BoundViscosity(d, d.TDiff);  // dynamics.f90:906
 }
@@ -1517,10 +1534,48 @@ static void poisson_solve(Domain &d) {
 }
 
 // ------------------------------------------ PressureCorrection, pressure.f90:169-266
-static void PressureCorrection(Domain &d, double coef, bool check_div) {
+// ------------------------------------------- immersed solids, tsteps.f90:360-567
+// IBMomentum: every value interpolated first, then all assigned (:360-409)
+static void IBMomentum(Domain &d, A3 &U, A3 &V, A3 &W) {
+  A3 *F[4] = {nullptr, &U, &V, &W};
+  for (int c = 1; c <= 3; c++) {
+    std::vector<double> wm(d.ibp[c].size());
+    for (size_t i = 0; i < wm.size(); i++) wm[i] = IBInterpolate(d.ibp[c][i], *F[c]);
+    for (size_t i = 0; i < wm.size(); i++) (*F[c])(d.ibp[c][i].xi, d.ibp[c][i].yj, d.ibp[c][i].zk) = wm[i];
+  }
+}
+
+// IBMassSources, second-order branch (:415-533); Bound_Q fills ghosts that
+// the right-hand side does not read
+static void IBMassSources(Domain &d, const A3 &U, const A3 &V, const A3 &W) {
+  d.Q.fill(0);
+  for (auto &p : d.ibp[1]) {
+    d.Q(p.xi, p.yj, p.zk) = d.Q(p.xi, p.yj, p.zk) + U(p.xi, p.yj, p.zk) / d.dxPr(p.xi);
+    d.Q(p.xi + 1, p.yj, p.zk) = d.Q(p.xi + 1, p.yj, p.zk) - U(p.xi, p.yj, p.zk) / d.dxPr(p.xi + 1);
+  }
+  for (auto &p : d.ibp[2]) {
+    d.Q(p.xi, p.yj, p.zk) = d.Q(p.xi, p.yj, p.zk) + V(p.xi, p.yj, p.zk) / d.dyPr(p.yj);
+    d.Q(p.xi, p.yj + 1, p.zk) = d.Q(p.xi, p.yj + 1, p.zk) - V(p.xi, p.yj, p.zk) / d.dyPr(p.yj + 1);
+  }
+  for (auto &p : d.ibp[3]) {
+    d.Q(p.xi, p.yj, p.zk) = d.Q(p.xi, p.yj, p.zk) + W(p.xi, p.yj, p.zk) / d.dzPr(p.zk);
+    d.Q(p.xi, p.yj, p.zk + 1) = d.Q(p.xi, p.yj, p.zk + 1) - W(p.xi, p.yj, p.zk) / d.dzPr(p.zk + 1);
+  }
+}
+
+// NullInterior (:540-567)
+static void NullInterior(Domain &d, A3 &U, A3 &V, A3 &W) {
+  A3 *F[4] = {nullptr, &U, &V, &W};
+  for (int c = 1; c <= 3; c++)
+    for (auto &q : d.nullp[c]) (*F[c])(q[0], q[1], q[2]) = 0;
+}
+
+static void PressureCorrection(Domain &d, double coef, bool check_div, bool with_q = false) {
   A3 &U = d.U2, &V = d.V2, &W = d.W2;
   const double dt2 = coef;
-  // PrePoisson (pressure.f90:272-723): ghosts, then RHS = (div U - Q) / dt2 with Q = 0
+  // PrePoisson (pressure.f90:272-723): ghosts, then RHS = (div U - Q) / dt2;
+  // Q is the IB mass source inside TMarchRK3 and absent in the initial
+  // projection (a local, unallocated Q in InitialConditions, initial.f90:3829)
   BoundUVW(d, U, V, W);
   const double dt2_rec = 1.0 / dt2;
 #pragma omp parallel for collapse(2)
@@ -1529,9 +1584,9 @@ static void PressureCorrection(Domain &d, double coef, bool check_div) {
       for (int i = 1; i <= d.Prnx; i++) {
         double r;
         if (d.gridtype == 1)
-          r = (U(i, j, k) - U(i - 1, j, k)) / d.dxmin + (V(i, j, k) - V(i, j - 1, k)) / d.dymin + (W(i, j, k) - W(i, j, k - 1)) / d.dzPr(k) - 0.0;
+          r = (U(i, j, k) - U(i - 1, j, k)) / d.dxmin + (V(i, j, k) - V(i, j - 1, k)) / d.dymin + (W(i, j, k) - W(i, j, k - 1)) / d.dzPr(k) - (with_q ? d.Q(i, j, k) : 0.0);
         else
-          r = (U(i, j, k) - U(i - 1, j, k)) / d.dxmin + (V(i, j, k) - V(i, j - 1, k)) / d.dymin + (W(i, j, k) - W(i, j, k - 1)) / d.dzmin - 0.0;
+          r = (U(i, j, k) - U(i - 1, j, k)) / d.dxmin + (V(i, j, k) - V(i, j - 1, k)) / d.dymin + (W(i, j, k) - W(i, j, k - 1)) / d.dzmin - (with_q ? d.Q(i, j, k) : 0.0);
         d.RHS(i, j, k) = r * dt2_rec;
       }
   poisson_solve(d);
@@ -1562,7 +1617,7 @@ static void PressureCorrection(Domain &d, double coef, bool check_div) {
       for (int j = 1; j <= d.Prny; j++)
         for (int i = 1; i <= d.Prnx; i++) {
           double dzk = d.gridtype == 1 ? d.dzPr(k) : d.dzmin;
-          double p = (U(i, j, k) - U(i - 1, j, k)) / d.dxmin + (V(i, j, k) - V(i, j - 1, k)) / d.dymin + (W(i, j, k) - W(i, j, k - 1)) / dzk - 0.0;
+          double p = (U(i, j, k) - U(i - 1, j, k)) / d.dxmin + (V(i, j, k) - V(i, j - 1, k)) / d.dymin + (W(i, j, k) - W(i, j, k - 1)) / dzk - (with_q ? d.Q(i, j, k) : 0.0);
           S = std::max(S, std::fabs(p));
         }
     d.max_div = S;
@@ -1596,16 +1651,30 @@ static void run_stage(Domain &d, int stage, int stop) {
   if (d.enable_buoyancy || d.num_scalars > 0) ScalarRK3(d, stage, dt);  // tsteps.f90:132-135
   OtherTerms(d, 2 * RK_alpha[stage - 1] * dt);
   BoundUVW(d, d.U2, d.V2, d.W2);
+  if (d.solids) {  // tsteps.f90:146-152
+    IBMomentum(d, d.U2, d.V2, d.W2);
+    BoundUVW(d, d.U2, d.V2, d.W2);
+    IBMassSources(d, d.U2, d.V2, d.W2);
+  }
   if (stop == 2) return;
-  PressureCorrection(d, 2 * RK_alpha[stage - 1] * dt, true);
+  PressureCorrection(d, 2 * RK_alpha[stage - 1] * dt, true, d.solids);
   std::swap(d.U.v, d.U2.v);
   std::swap(d.V.v, d.V2.v);
   std::swap(d.W.v, d.W2.v);
+  if (d.solids) {  // tsteps.f90:201-206
+    NullInterior(d, d.U, d.V, d.W);
+    BoundUVW(d, d.U, d.V, d.W);
+    IBMomentum(d, d.U, d.V, d.W);
+  }
   BoundUVW(d, d.U, d.V, d.W);
 }
 
 static void TMarchRK3(Domain &d) {
   BoundUVW(d, d.U, d.V, d.W);
+  // first call: IBMomentum after the ghosts, which keep their values until
+  // the end of the first stage (tsteps.f90:31-54)
+  if (d.called == 0 && d.solids) IBMomentum(d, d.U, d.V, d.W);
+  d.called = 1;
   TimeStepLength(d);
   for (int s = 1; s <= 3; s++) run_stage(d, s, 3);
   d.time += d.dt;
@@ -1737,6 +1806,54 @@ void *orc_create(const elmm_config *c) {
 }
 
 void orc_destroy(void *h) { delete (Domain *)h; }
+
+// The solid bodies of GetSolidBodiesBC / SetNullifiedPoints as lists (the
+// layout of elmm_solids): IB points, nullified points, ScalFl points, the
+// solid-face wall-model points appended to the lists of
+// GetOutsideBoundariesWM_UVW, and the bottom-wall points that list leaves
+// out next to and under the bodies (wallmodels.f90:700-820).
+int orc_set_solids(void *h, const elmm_solids *s) {
+  Domain &d = *(Domain *)h;
+  for (int c = 1; c <= 3; c++) { d.ibp[c].clear(); d.nullp[c].clear(); }
+  d.scalfl.clear();
+  d.solids = false;
+  d.called = 0;
+  if (!s) return 0;
+  for (int c = 1; c <= 3; c++) {
+    if (s->n_ib[c - 1] > 0) d.ibp[c].assign(s->ib[c - 1], s->ib[c - 1] + s->n_ib[c - 1]);
+    for (int64_t q = 0; q < s->n_null[c - 1]; q++) {
+      const int32_t *t = s->null_ijk[c - 1] + 3 * q;
+      d.nullp[c].push_back({t[0], t[1], t[2]});
+    }
+    if (s->n_bottom_skip[c - 1] > 0) {
+      std::vector<char> skip;
+      const int nx = c == 1 ? d.Unx : c == 2 ? d.Vnx : d.Wnx, ny = c == 1 ? d.Uny : c == 2 ? d.Vny : d.Wny;
+      skip.assign((size_t)(nx + 2) * (ny + 2), 0);
+      for (int64_t q = 0; q < s->n_bottom_skip[c - 1]; q++) {
+        const int32_t *t = s->bottom_skip_ij[c - 1] + 2 * q;
+        skip[(size_t)t[0] + (size_t)(nx + 2) * t[1]] = 1;
+      }
+      auto &pts = d.wm[MINUSZ][c];
+      std::vector<WMPointUVW> keep;
+      for (auto &p : pts)
+        if (!(p.zk == 1 && skip[(size_t)p.xi + (size_t)(nx + 2) * p.yj])) keep.push_back(p);
+      pts.swap(keep);
+    }
+  }
+  if (s->n_scalfl > 0) d.scalfl.assign(s->scalfl, s->scalfl + s->n_scalfl);
+  for (int64_t q = 0; q < s->n_wm; q++) {
+    const elmm_wm_point &w = s->wm[q];
+    if (w.component < 1 || w.component > 3 || w.direction < 1 || w.direction > 6) return 1;
+    WMPointUVW p;
+    p.xi = w.xi; p.yj = w.yj; p.zk = w.zk;
+    p.distx = w.dist[0]; p.disty = w.dist[1]; p.distz = w.dist[2];
+    p.z0 = w.z0;
+    d.wm[w.direction][w.component].push_back(p);
+  }
+  d.Q.init(0, d.Prnx + 1, 0, d.Prny + 1, 0, d.Prnz + 1);
+  d.solids = true;
+  return 0;
+}
 
 int orc_sizes(void *h, int32_t *out12) {
   Domain *d = (Domain *)h;

@@ -47,6 +47,7 @@ def lib():
         L.orc_num_threads.argtypes = [C.c_int]
         L.orc_num_threads.restype = C.c_int
         L.orc_scalar_slices.argtypes = [P, C.c_int, dp, dp]
+        L.orc_set_solids.argtypes = [P, P]
         _lib = L
     return _lib
 
@@ -139,6 +140,12 @@ class Oracle:
         xy, xz = np.zeros((Prny, Prnx)), np.zeros((Prnz, Prnx))
         assert lib().orc_scalar_slices(self.h, sc, _ptr(xy), _ptr(xz)) == 0
         return xy, xz
+
+    def set_solids(self, solids):
+        """Installs solid bodies: a gpu_elmm_b200.solids.Solids (or None)."""
+        st = None if solids is None else solids.struct()
+        assert lib().orc_set_solids(self.h, None if st is None else C.cast(C.byref(st), C.c_void_p)) == 0
+        self._solids = solids
 
     def bound(self):
         lib().orc_bound_uvw(self.h)

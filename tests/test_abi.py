@@ -50,6 +50,13 @@ int main(void) {
   O(elmm_point_source, position) O(elmm_point_source, flux)
   printf("elmm_point_source.size %zu\n", sizeof(elmm_point_source));
   O(elmm_stats, time) O(elmm_stats, max_div) O(elmm_stats, refine_sweeps) O(elmm_stats, elapsed_ms)
+  printf("elmm_ib_point.size %zu\n", sizeof(elmm_ib_point));
+  printf("elmm_wm_point.size %zu\n", sizeof(elmm_wm_point));
+  printf("elmm_solids.size %zu\n", sizeof(elmm_solids));
+  O(elmm_ib_point, interp) O(elmm_ib_point, kk) O(elmm_ib_point, coef)
+  O(elmm_wm_point, dist) O(elmm_wm_point, z0)
+  O(elmm_solids, ib) O(elmm_solids, n_null) O(elmm_solids, null_ijk) O(elmm_solids, n_scalfl) O(elmm_solids, scalfl)
+  O(elmm_solids, n_wm) O(elmm_solids, wm) O(elmm_solids, n_bottom_skip) O(elmm_solids, bottom_skip_ij)
   return 0;
 }
 '''
@@ -72,8 +79,12 @@ def test_ctypes_layout_matches_c():
         if f == "size":
             continue
         cls = {"elmm_config": cfgmod.ElmmConfig, "elmm_stats": cfgmod.ElmmStats,
-               "elmm_point_source": cfgmod.ElmmPointSource}[s]
+               "elmm_point_source": cfgmod.ElmmPointSource, "elmm_ib_point": cfgmod.ElmmIBPoint,
+               "elmm_wm_point": cfgmod.ElmmWMPoint, "elmm_solids": cfgmod.ElmmSolids}[s]
         assert getattr(cls, f).offset == off, key
+    for s, cls in (("elmm_ib_point", cfgmod.ElmmIBPoint), ("elmm_wm_point", cfgmod.ElmmWMPoint),
+                   ("elmm_solids", cfgmod.ElmmSolids)):
+        assert lay[s + ".size"] == C.sizeof(cls), s
 
 
 def test_config_defaults_and_errors_without_gpu():

@@ -1,0 +1,124 @@
+"""Immersed solid bodies (an array of cubes on a stretched grid with a mean
+pressure gradient).
+
+CPU: the geometry pass of gpu_elmm_b200/solids.py (the point lists of
+GetSolidBodiesBC / SetNullifiedPoints for boxes) has the properties the
+reference's construction gives them, and the oracle keeps the solid interior
+at rest.  GPU: the library, given the same lists, follows the oracle
+(IBMomentum, IBMassSources, NullInterior, the ScalFl viscosity and the
+wall-model fluxes at the solid faces) on the FP64 path to 1e-11, and the
+mixed path follows the FP64 one."""
+import numpy as np
+import pytest
+
+from conftest import rel
+from gpu_elmm_b200.config import grid_of, make_config
+from gpu_elmm_b200.solids import build_solids, cube_array
+from gpu_elmm_b200.workloads import interiors, log_profile_state
+from oracle import Oracle
+
+NZ = 24
+ZW = np.concatenate([[0.0], np.cumsum(0.5 * 1.04 ** np.arange(NZ))])  # dz_k = 0.5 * 1.04^(k-1)
+
+
+def _cfg(precision=0, n=(48, 48, NZ)):
+    return make_config(*n, zW=ZW, pr_gradient_x=-0.001, precision=precision)
+
+
+def _boxes():
+    # 2 x 2 cubes of 8 cells at a 24-cell pitch, 8 levels tall, set 5 units into the ground
+    return cube_array(2, 8.0, 24.0, float(ZW[8]), offset=8.0, depth=5.0)
+
+
+def _state(cfg, seed=1):
+    g = grid_of(cfg)
+    return g, log_profile_state(g, seed=seed, zW=ZW)
+
+
+def test_geometry_lists():
+    cfg = _cfg()
+    s = build_solids(cfg, _boxes())
+    g = s.geometry
+    c = s.counts()
+    assert min(c["ib"]) > 0 and min(c["null"]) > 0 and c["scalfl"] > 0 and c["wm"] > 0
+    for q in range(3):
+        t = g.types[q + 1]
+        for (i, j, k), pts, cf in s.ib[q]:
+            assert t[k + 2, j + 2, i + 2] > 0  # forcing points are solid
+            assert len(pts) == len(cf) <= 6
+            for (a, b, cc) in pts:
+                assert t[cc + 2, b + 2, a + 2] <= 0  # interpolation points are free
+            if pts:  # the fit through zero at the wall extrapolates: weights of the other sign
+                assert all(w < 0 for w in cf)
+        for (i, j, k) in s.null[q]:
+            assert t[k + 2, j + 2, i + 2] > 0
+            for d in ((1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)):
+                assert t[k + d[2] + 2, j + d[1] + 2, i + d[0] + 2] > 0
+    # every solid point of the interior is either an IB point or nullified
+    for q in range(3):
+        (nx, ny, nz) = g.grids[q + 1][0]
+        solid = int((g.types[q + 1][3:nz + 3, 3:ny + 3, 3:nx + 3] > 0).sum())
+        assert solid == len(s.ib[q]) + len(s.null[q])
+    for comp, dr, i, j, k, dv, z0 in s.wm:
+        assert g.typ(comp, i, j, k) < 0 and z0 == 0.1
+        assert np.linalg.norm(dv) > 0
+    # the ground next to and under the cubes has no wall-model point
+    for q in range(3):
+        for i, j in s.bottom_skip[q]:
+            assert g.typ(q + 1, i, j, 1) != 0 or g.typ(q + 1, i, j, 0) > 0
+
+
+def test_oracle_keeps_the_interior_at_rest():
+    cfg = _cfg()
+    s = build_solids(cfg, _boxes())
+    g, st = _state(cfg)
+    o = Oracle(cfg)
+    o.set_state(*st)
+    o.project(1.0)
+    o.set_solids(s)
+    md, _ = o.step(3)
+    U, V, W, _ = o.state()
+    assert md < 1e-12  # div U - Q after the projection
+    for F, nl in zip((U, V, W), s.null):
+        assert np.abs(F[nl[:, 2] + 2, nl[:, 1] + 2, nl[:, 0] + 2]).max() == 0
+    assert np.isfinite(U).all() and np.abs(U).max() < 20
+
+
+def _pair(precision, nsteps):
+    from gpu_elmm_b200 import lib as L
+    cfg = _cfg(precision)
+    s = build_solids(cfg, _boxes())
+    g, st = _state(cfg)
+    o = Oracle(_cfg(0))
+    o.set_state(*st)
+    o.project(1.0)
+    o.set_solids(s)
+    d = L.Domain(cfg)
+    d.upload(*st)
+    d.project(1.0)
+    d.set_solids(s)
+    md_o, _ = o.step(nsteps)
+    sd = d.step(nsteps)
+    out = d.download()
+    d.close()
+    return g, out, o.state(), sd, md_o
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nsteps", [1, 5])
+def test_fp64_cubes_match_the_oracle(nsteps):
+    g, gpu, orc, sd, md_o = _pair(0, nsteps)
+    e = [rel(a, b) for a, b in zip(interiors(g, *gpu), interiors(g, *orc))]
+    print("FP64 errors with cubes after", nsteps, "steps (U, V, W, P):", e, "max div", sd.max_div, md_o)
+    assert max(e[:3]) < 1e-11 and e[3] < 1e-10, e
+    assert sd.max_div < 1e-10
+
+
+@pytest.mark.gpu
+def test_mixed_cubes_follow_fp64():
+    g, m, _, sd, _ = _pair(1, 3)
+    _, f, _, _, _ = _pair(0, 3)
+    e = [rel(a, b) for a, b in zip(interiors(g, *m)[:3], interiors(g, *f)[:3])]
+    print("mixed vs FP64 with cubes after 3 steps (U, V, W):", e, "max div", sd.max_div)
+    assert max(e) < 1e-5, e
+    assert sd.max_div < 1e-5
