@@ -50,6 +50,8 @@ MOMENTUM_WORDS = 15
 REF_STEPS = 10
 # long run of the single domain on both paths (errors after 1, 10 and this many steps)
 LONG_STEPS = 1000
+# the array of cubes: steps run on both paths (device time over steps 10..CUBES_STEPS)
+CUBES_STEPS = 100
 # batched ensemble: domains per GPU and the axis lengths they draw from
 BATCH_DOMAINS = 64
 BATCH_AXES = (32, 48, 64, 96, 128)
@@ -337,6 +339,7 @@ def run_ours(args, ws, rank, local):
 
     dm.close()
     long_run = long_run_leg(st, T0, local) if rank == 0 else None
+    cubes = cubes_leg(local) if rank == 0 else None
     batched = batched_leg(args, ws, rank, local)
     serving = serving_leg(args, ws, rank, local)
 
@@ -364,6 +367,7 @@ def run_ours(args, ws, rank, local):
             "clocks": clk.summary(),
             "wall_s_timed": wall,
             "long_run": long_run,
+            "cubes": cubes,
             "batched": batched,
             "serving": serving,
         }
@@ -412,6 +416,62 @@ def long_run_leg(st, T0, local):
     return {"steps": LONG_STEPS, "rel_err_mixed_vs_fp64": errs,
             "profiles_rel_diff": compare(prof[1].result(), prof[0].result(), keys=("u", "tke", "theta")),
             "profiles_window": f"steps {LONG_STEPS // 2}..{LONG_STEPS}, every {LONG_STEPS // 20}"}
+
+
+def cubes_leg(local):
+    """The array of cubes (384x384x96, stretched z, 8x8 cubes, mean pressure
+    gradient): device time per step of both paths over CUBES_TIMED steps,
+    the mixed path's error against FP64 after 1, 10 and CUBES_STEPS steps from
+    one projected state, the divergence check of each, and the mean profiles
+    of the second half of the run."""
+    from gpu_elmm_b200 import lib as L
+    from gpu_elmm_b200.solids import build_solids
+    from gpu_elmm_b200.stats import Profiles, compare
+    from gpu_elmm_b200.workloads import CUBES_N, cubes_boxes, cubes_config, stretched_zw
+    cfgs = {p: cubes_config(precision=p, device=local) for p in (0, 1)}
+    g = grid_of(cfgs[0])
+    t0 = time.perf_counter()
+    sol = build_solids(cfgs[0], cubes_boxes())
+    t_geo = time.perf_counter() - t0
+    st = log_profile_state(g, seed=0, zW=stretched_zw(CUBES_N[2]))
+    doms = {p: L.Domain(cfgs[p]) for p in (0, 1)}
+    doms[0].upload(*st)
+    doms[0].project(1.0)
+    doms[1].upload(*doms[0].download())
+    for p in (0, 1):
+        doms[p].set_solids(sol)
+    prof = {0: Profiles(g), 1: Profiles(g)}
+    errs, ms, div = {}, {0: [], 1: []}, {}
+    done = 0
+    marks = sorted({1, 10, CUBES_STEPS} | set(range(CUBES_STEPS // 2, CUBES_STEPS + 1, CUBES_STEPS // 10)))
+    for target in marks:
+        for p in (0, 1):
+            s = doms[p].step(target - done)
+            if done >= 10:
+                ms[p].append((s.elapsed_ms, target - done))
+            div[p] = s.max_div
+        done = target
+        sd = {p: doms[p].download() for p in (0, 1)}
+        if target in (1, 10, CUBES_STEPS):
+            e = [rel(a, b) for a, b in zip(interiors(g, *sd[1]), interiors(g, *sd[0]))]
+            errs[str(target)] = dict(zip(("u", "v", "w", "p"), e))
+        if target >= CUBES_STEPS // 2:
+            for p in (0, 1):
+                prof[p].add(*sd[p][:3])
+    for p in (0, 1):
+        doms[p].close()
+    cells = g.Prnx * g.Prny * g.Prnz
+    per = {p: sum(a for a, _ in ms[p]) / max(1, sum(b for _, b in ms[p])) for p in (0, 1)}
+    return {"workload": f"{CUBES_N[0]}x{CUBES_N[1]}x{CUBES_N[2]} stretched z (dz_k = 0.5*1.04^(k-1)), 8x8 cubes of "
+                        "16 cells at a 48-cell pitch (z0 = 0.1), mean pressure gradient in x",
+            "cells": cells, "points": sol.counts(), "geometry_pass_s": t_geo,
+            "mixed": {"cell_steps_per_s": cells / (per[1] / 1e3), "ms_per_step": per[1]},
+            "fp64": {"cell_steps_per_s": cells / (per[0] / 1e3), "ms_per_step": per[0]},
+            "mixed_over_fp64": per[0] / per[1],
+            "timed_steps": sum(b for _, b in ms[1]),
+            "rel_err_mixed_vs_fp64": errs, "max_div": {"mixed": div[1], "fp64": div[0]},
+            "profiles_rel_diff": compare(prof[1].result(), prof[0].result(), keys=("u", "tke")),
+            "profiles_window": f"steps {CUBES_STEPS // 2}..{CUBES_STEPS}, every {CUBES_STEPS // 10}"}
 
 
 def gather(x, ws):

@@ -776,6 +776,26 @@ struct BatchT {
       if ((r = upload_table(&h.sgs_r2zz, r2zz))) return r;
       if ((r = upload_table(&h.sgs_wc2, wc2))) return r;
     }
+    if (h.vz && sizeof(T) == 4) {  // per-level factors of the packed FP32 momentum path
+      const int nzp = h.nz + 2;
+      std::vector<float> kz((size_t)kZ2 * nzp, 0.f);
+      auto zP = [&](int k) { return g.zPr[k + 2]; };
+      auto zWv = [&](int k) { return g.zW[k + 2]; };
+      auto dP = [&](int k) { return g.dzPr[k + 2]; };
+      auto dW = [&](int k) { return g.dzW[k + 2]; };
+      for (int k = 1; k <= h.nz; k++) {
+        kz[KZ_AUV * nzp + k] = (float)(1.0 / (4.0 * dP(k)));
+        kz[KZ_BUV * nzp + k] = (float)(1.0 / (4.0 * (zP(k + 1) - zP(k - 1))));
+        kz[KZ_D1UV * nzp + k] = (float)(1.0 / (dW(k) * dP(k)));
+        kz[KZ_D2UV * nzp + k] = (float)(1.0 / (dW(k - 1) * dP(k)));
+        kz[KZ_AW * nzp + k] = (float)(1.0 / (4.0 * dW(k)));
+        kz[KZ_BW * nzp + k] = (float)(1.0 / (zWv(k + 1) - zWv(k - 1)));
+        kz[KZ_D1W * nzp + k] = (float)(1.0 / (dP(k + 1) * dW(k)));
+        kz[KZ_D2W * nzp + k] = (float)(1.0 / (dP(k) * dW(k)));
+        kz[KZ_RDZW * nzp + k] = (float)(1.0 / dW(k));
+      }
+      if ((r = upload_table(&h.kz2, kz))) return r;
+    }
     // wall-model planes
     for (int s = 0; s < 6; s++) h.z0[s] = c.z0[s];
     for (int comp = 0; comp < 3; comp++)

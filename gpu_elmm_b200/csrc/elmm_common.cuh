@@ -98,6 +98,9 @@ struct Dom {
   // wall model: per face plane fluxp/fluxm/ustar, plane dims from ext[]
   T *wm_fluxp[kFaces], *wm_fluxm[kFaces];
   double *wm_ustar[kFaces];
+  // stretched z, packed FP32 momentum path: per-level factors kz2[q * (nz + 2) + k]
+  // (q: kZ2 entries, see elmm_packed.cuh)
+  const float *kz2;
   // per component: 1 marks a bottom-plane point without a wall-model point
   // (next to or under a solid body), or null for none
   const unsigned char *bskip[3];

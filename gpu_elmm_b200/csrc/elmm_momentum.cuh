@@ -480,7 +480,7 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
               *p2s = ring + ((k + 1) % NSL) * Lay::SIZE;
       bool packed = false;
       if constexpr (CPT == 2)
-        packed = !vz && !wallhere && pair_full && k <= min(kU, min(kV, kW));
+        packed = (!vz || d.kz2) && !wallhere && pair_full && k <= min(kU, min(kV, kW));
       if (packed && ok) {
         if constexpr (CPT == 2) {
           // two cells per thread, every operation on a pair
@@ -494,7 +494,25 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
           if (buoy)
             btp = bc2(bA2) * (F2{*reinterpret_cast<const float2 *>(Tm + c + plane)} +
                               F2{*reinterpret_cast<const float2 *>(Tm + c)});
-          const F2 tu = tendency2<0>(K2, R2), tv = tendency2<1>(K2, R2), tw = tendency2<2>(K2, R2, btp);
+          F2 tu, tv, tw;
+          F2 gz2 = bc2(gz);
+          if (!vz) {
+            tu = tendency2<0>(K2, R2);
+            tv = tendency2<1>(K2, R2);
+            tw = tendency2<2>(K2, R2, btp);
+          } else {
+            const int nzp = nz + 2;
+            const float *kz = d.kz2 + k;
+            KZ2 Z;
+            Z.auv = bc2(__ldg(kz + KZ_AUV * nzp)); Z.buv = bc2(__ldg(kz + KZ_BUV * nzp));
+            Z.d1uv = bc2(__ldg(kz + KZ_D1UV * nzp)); Z.d2uv = bc2(__ldg(kz + KZ_D2UV * nzp));
+            Z.aw = bc2(__ldg(kz + KZ_AW * nzp)); Z.bw = bc2(__ldg(kz + KZ_BW * nzp));
+            Z.d1w = bc2(__ldg(kz + KZ_D1W * nzp)); Z.d2w = bc2(__ldg(kz + KZ_D2W * nzp));
+            gz2 = bc2((-coef) * __ldg(kz + KZ_RDZW * nzp));
+            tu = tendency2<0, true>(K2, R2, bc2(0.f), &Z);
+            tv = tendency2<1, true>(K2, R2, bc2(0.f), &Z);
+            tw = tendency2<2, true>(K2, R2, btp, &Z);
+          }
           const F2 rd = bc2(rdt), dd = bc2(dt), bd = bc2(bdt);
           const F2 zero = bc2(0.f);
           F2 u2 = stage1 ? zero : F2{*reinterpret_cast<const float2 *>(nar)} * rd * dd;
@@ -509,7 +527,7 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
           v2 = v2 + bc2(gy) * ((R2.g(4, 0, 1, 0) - mm) - p0);
           v2 = v2 + R2.g(1, 0, 0, 0);
           w2 = w2 + tw * bd * dd;
-          w2 = w2 + bc2(gz) * ((R2.g(4, 0, 0, 1) - mm) - p0);
+          w2 = w2 + gz2 * ((R2.g(4, 0, 0, 1) - mm) - p0);
           w2 = w2 + R2.g(2, 0, 0, 0);
           *reinterpret_cast<float2 *>(Us + c) = tu.v;
           *reinterpret_cast<float2 *>(U2o + c) = u2.v;

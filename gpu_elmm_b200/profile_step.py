@@ -48,9 +48,12 @@ def main():
     ap.add_argument("--stage-times", action="store_true", help="also time each kernel of stage 2 (5 repetitions)")
     ap.add_argument("--no-temperature", action="store_true", help="the channel without the temperature field")
     ap.add_argument("--batched", type=int, default=0, help="run the batched ensemble of this many domains")
+    ap.add_argument("--cubes", action="store_true", help="run the array of cubes (384x384x96, stretched z)")
     a = ap.parse_args()
     if a.batched:
         return batched(a)
+    if a.cubes:
+        return cubes(a)
     n = tuple(int(x) for x in a.n.split(","))
     buoy = not a.no_temperature
     cfg = make_config(*n, precision=1 if a.precision == "mixed" else 0, buoyancy=buoy)
@@ -67,6 +70,29 @@ def main():
     nvtx_pop()
     out = {"n": n, "precision": a.precision, "steps": a.steps, "ms_per_step": s.elapsed_ms / max(1, a.steps),
            "max_div": s.max_div, "kernels_per_step": s.kernels / max(1, a.steps)}
+    if a.stage_times:
+        out["stage2_kernel_ms"] = d.profile_stage(2, 5)
+    print(json.dumps(out))
+    d.close()
+
+
+def cubes(a):
+    from .solids import build_solids
+    from .workloads import CUBES_N, cubes_boxes, cubes_config, stretched_zw
+    cfg = cubes_config(precision=1 if a.precision == "mixed" else 0)
+    g = grid_of(cfg)
+    sol = build_solids(cfg, cubes_boxes())
+    d = L.Domain(cfg)
+    d.upload(*log_profile_state(g, seed=0, zW=stretched_zw(CUBES_N[2])))
+    d.project(1.0)
+    d.set_solids(sol)
+    if a.warmup:
+        d.step(a.warmup)
+    nvtx_push("timed_steps")
+    s = d.step(a.steps)
+    nvtx_pop()
+    out = {"n": CUBES_N, "precision": a.precision, "steps": a.steps, "ms_per_step": s.elapsed_ms / max(1, a.steps),
+           "max_div": s.max_div, "kernels_per_step": s.kernels / max(1, a.steps), "points": sol.counts()}
     if a.stage_times:
         out["stage2_kernel_ms"] = d.profile_stage(2, 5)
     print(json.dumps(out))

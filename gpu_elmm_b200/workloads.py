@@ -178,3 +178,30 @@ def taylor_green_2d(grid: Grid, *, dx: float, dy: float, amp=1.0):
     interior(V, -2, (g.Vnx, g.Vny, g.Vnz))[...] = vv[None]
     interior(Pr, -1, (g.Prnx, g.Prny, g.Prnz))[...] = pp[None]
     return U, V, W, Pr
+
+
+# ------------------------------------------------ the array of cubes
+# 384 x 384 x 96 cells, dx = dy = 1, dz_k = 0.5 * 1.04^(k-1) (z extent ~527),
+# 8 x 8 cubes of 16 cells (16 levels tall) at a 48-cell pitch, rough (z0 =
+# 0.1), driven by a uniform mean pressure gradient in x
+CUBES_N = (384, 384, 96)
+CUBES_PR_GRADIENT_X = -2e-4
+
+
+def stretched_zw(nz: int, first: float = 0.5, ratio: float = 1.04) -> np.ndarray:
+    """zW(0:nz) of the geometrically stretched grid, dz_k = first * ratio^(k-1)."""
+    return np.concatenate([[0.0], np.cumsum(first * ratio ** np.arange(nz))])
+
+
+def cubes_config(precision=0, device=0, n=CUBES_N, **kw):
+    from .config import make_config
+    return make_config(*n, zW=stretched_zw(n[2]), pr_gradient_x=CUBES_PR_GRADIENT_X, precision=precision,
+                       device=device, **kw)
+
+
+def cubes_boxes(n=CUBES_N, per_side=8, edge=16.0, pitch=48.0, levels=16):
+    """The solid bodies: cubes from x, y = 16 + 48 a to 32 + 48 a and from
+    below the ground up to zW(levels)."""
+    from .solids import cube_array
+    zw = stretched_zw(n[2])
+    return cube_array(per_side, edge, pitch, float(zw[levels]), offset=(pitch - edge) / 2, depth=5.0)

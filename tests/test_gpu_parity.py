@@ -612,3 +612,28 @@ def test_mixed_divergence_maximum_is_exact(case):
     scale = np.abs(U).max() / cfg.dxmin + np.abs(V).max() / cfg.dymin + np.abs(W).max() / dzpr.min()
     assert 0 < ref and abs(s.max_div - ref) <= 8 * np.finfo(np.float64).eps * scale, (s.max_div, ref)
     d.close()
+
+
+def test_mixed_stretched_grid_follows_fp64():
+    """The mixed path on a stretched z grid (the packed two-cell momentum
+    path with per-level factors, the per-cell path next to the walls) against
+    the FP64 path after 1 and 5 steps from one projected state: 1e-5 and
+    2e-5 (FP32 rounding of the state grows over the steps)."""
+    nz = 40
+    zW = stretched(nz)
+    g = grid_of(make_config(64, 48, nz, zW=zW))
+    st = log_profile_state(g, seed=7, zW=zW)
+    out = {}
+    for prec in (0, 1):
+        d = L.Domain(make_config(64, 48, nz, zW=zW, precision=prec, pr_gradient_x=-1e-3))
+        d.upload(*st)
+        d.project(1.0)
+        d.step(1)
+        a = interiors(g, *d.download())[:3]
+        d.step(4)
+        out[prec] = (a, interiors(g, *d.download())[:3])
+        d.close()
+    for n in (0, 1):
+        e = [rel(a, b) for a, b in zip(out[1][n], out[0][n])]
+        print("mixed vs FP64, stretched z, after", (1, 5)[n], "steps:", e)
+        assert max(e) < (1e-5, 2e-5)[n], e
