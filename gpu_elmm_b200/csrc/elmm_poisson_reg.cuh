@@ -14,9 +14,11 @@ namespace elmm {
 constexpr int kRegThreads = 256;
 // resident blocks per SM the x-transform kernels are compiled for: for up to
 // 16 elements per thread three (FP32, 80 registers) or two (FP64, 128
-// registers) fit without spills; longer sequences get the compiler's choice
+// registers) fit without spills; longer FP32 sequences (24 elements: lengths
+// 192, 384) two blocks of 128 registers, faster than one block of ~200 (the
+// y transform of those lengths spills at 128 and keeps the compiler's choice)
 template <typename T, int N>
-constexpr int fft_reg_min_blocks() { return N / fplan_P(N) <= 16 ? (sizeof(T) == 4 ? 3 : 2) : 1; }
+constexpr int fft_reg_min_blocks() { return N / fplan_P(N) <= 16 ? (sizeof(T) == 4 ? 3 : 2) : (sizeof(T) == 4 ? 2 : 1); }
 
 // The reads of the divergence stencil of one x row (j, k) of the x
 // transforms.  Away from the box faces the neighbours are the adjacent box
