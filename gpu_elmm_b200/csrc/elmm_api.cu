@@ -882,13 +882,14 @@ struct BatchT {
 
   // ------------------------------------------------------------ stages
   // ghost shells of the listed fields after the kernel that wrote them
-  void launch_ghosts(std::initializer_list<int> fields, int gate) {
+  // prref: the launch also reduces the pressure reference (after the projection)
+  void launch_ghosts(std::initializer_list<int> fields, int gate, int prref = 0) {
     unsigned packed = 0;
     int nf = 0;
     for (int f : fields) packed |= (unsigned)f << (8 * nf++);
     nlaunch++;
     k_ghosts<T><<<gsz(9, ls[LK_SHELL].total * nf), kShellThreads, 0, stream>>>(ddom, ls[LK_SHELL].l(), packed, nf,
-                                                                                 gate);
+                                                                                 gate, prref);
   }
   int launch_sgs() {
     nlaunch++;
@@ -905,10 +906,8 @@ struct BatchT {
     return ELMM_OK;
   }
   void launch_project(double coef_alpha2, int use_dt, int in_place, int gate) {
-    nlaunch++;  // k_prref; the projection kernels count themselves
     k_project_any(coef_alpha2, use_dt, in_place, gate);
-    launch_ghosts({F_U, F_V, F_W, F_P}, gate);
-    k_prref<T><<<std::min(nd, 1024), 256, 0, stream>>>(ddom, nd, gate);
+    launch_ghosts({F_U, F_V, F_W, F_P}, gate, 1);  // and the pressure reference of k_prref
   }
   // k_project for the domains that take it, k_project_pair (FP32, even Prnx) for the others
   void k_project_any(double coef_alpha2, int use_dt, int in_place, int gate) {
@@ -1236,14 +1235,24 @@ struct BatchT {
     for (int c = 0; c < 3; c++) hdom[d].bskip[c] = nullptr;
   }
   // elmm_set_solids: checks the lists, turns (i, j, k) into box indices with
-  // the ghost folds applied, uploads them and marks the step graph stale
+  // the ghost folds applied, uploads them and marks the step graph stale.
+  // On any error the domain is left without bodies.
   int set_solids(int d, const elmm_solids *s) {
     CU(cudaSetDevice(device));
     CU(cudaStreamSynchronize(stream));
     if ((int)sol.size() < nd) sol.resize(nd);
     drop_solids(d);
     if (step_exec) { cudaGraphExecDestroy(step_exec); step_exec = nullptr; }
-    if (!s) return push_dom(d);
+    int r = push_dom(d);
+    if (r || !s) return r;
+    r = install_solids(d, s);
+    if (r) {
+      drop_solids(d);
+      push_dom(d);
+    }
+    return r;
+  }
+  int install_solids(int d, const elmm_solids *s) {
     Dom<T> &h = hdom[d];
     const elmm_config &c = cfg[d];
     if (c.enable_buoyancy || c.num_scalars > 0)

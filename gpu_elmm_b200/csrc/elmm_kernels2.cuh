@@ -292,9 +292,9 @@ __global__ void __launch_bounds__(MX *MY / 2) k_project_pair(const Dom<float> *_
 // the new reference is the mean of the top layer; it is applied lazily,
 // every reader of P subtracts it.
 template <typename T>
-__global__ void k_prref(const Dom<T> *__restrict__ doms, int nd, int gate) {
-  __shared__ double red[32];
-  for (int di = blockIdx.x; di < nd; di += gridDim.x) {
+__device__ __forceinline__ void prref_reduce(const Dom<T> *__restrict__ doms, int nd, int gate, int b0, int nb,
+                                             double *red) {
+  for (int di = b0; di < nd; di += nb) {
     const Dom<T> &d = doms[di];
     if (gate && !*d.refine_flag) continue;
     double s = 0;
@@ -309,6 +309,12 @@ __global__ void k_prref(const Dom<T> *__restrict__ doms, int nd, int gate) {
     }
     __syncthreads();
   }
+}
+
+template <typename T>
+__global__ void k_prref(const Dom<T> *__restrict__ doms, int nd, int gate) {
+  __shared__ double red[32];
+  prref_reduce(doms, nd, gate, blockIdx.x, gridDim.x, red);
 }
 
 // Ghost shell of up to four box fields, pulled from the interior after the
@@ -348,7 +354,7 @@ __host__ __device__ __forceinline__ long long shell_cells(int ex, int ey, int ez
 
 template <typename T>
 __global__ void __launch_bounds__(kShellThreads) k_ghosts(const Dom<T> *__restrict__ doms, Launch L, unsigned fields,
-                                                          int nf, int gate) {
+                                                          int nf, int gate, int prref = 0) {
   const int nblk = L.total * nf;  // shell tiles times fields (a few million at most)
   for (int b = blockIdx.x; b < nblk; b += gridDim.x) {
     const int f = b / L.total, t = b - f * L.total;
@@ -395,6 +401,14 @@ __global__ void __launch_bounds__(kShellThreads) k_ghosts(const Dom<T> *__restri
       v = F[bidx(d, fold_rep(i, ex, per[0]), fold_rep(j, ey, per[1]), fold_rep(k, ez, per[2]))];
     }
     F[bidx(d, i, j, k)] = v;
+  }
+  // prref: the last blocks (one per domain, as many as there are) also reduce
+  // the top-layer partial sums of the projection into the pressure reference
+  // (k_prref without a launch of its own)
+  const int nb = min(L.nd, (int)gridDim.x), b0 = (int)gridDim.x - 1 - (int)blockIdx.x;
+  if (prref && b0 < nb) {
+    __shared__ double red[32];
+    prref_reduce(doms, L.nd, gate, b0, nb, red);
   }
 }
 

@@ -122,3 +122,42 @@ def test_mixed_cubes_follow_fp64():
     print("mixed vs FP64 with cubes after 3 steps (U, V, W):", e, "max div", sd.max_div)
     assert max(e) < 1e-5, e
     assert sd.max_div < 1e-5
+
+
+@pytest.mark.gpu
+def test_set_solids_rejects_what_it_cannot_apply():
+    """elmm_set_solids refuses (ELMM_ERR_INVALID_ARG = 6) lists it could not
+    apply exactly: a forcing point next to a periodic boundary, an
+    interpolation point that is itself a forcing point, a smooth solid wall;
+    None removes the bodies again."""
+    from gpu_elmm_b200 import lib as L
+    cfg = _cfg()
+    s = build_solids(cfg, _boxes())
+    g, st = _state(cfg)
+    d = L.Domain(cfg)
+    d.upload(*st)
+    d.project(1.0)
+
+    def code(sol):
+        try:
+            d.set_solids(sol)
+            return 0
+        except L.ElmmError as e:
+            return e.code
+
+    bad = build_solids(cfg, _boxes())
+    (i, j, k), pts, cf = bad.ib[0][0]
+    bad.ib[0][0] = ((1, j, k), pts, cf)
+    assert code(bad) == 6
+    bad = build_solids(cfg, _boxes())
+    first = next(p for p in bad.ib[0] if p[1])
+    other = bad.ib[0][1][0]
+    bad.ib[0][0] = (first[0], [other] + first[1][1:], first[2])
+    assert code(bad) == 6
+    bad = build_solids(cfg, _boxes())
+    c, dr, i, j, k, dv, z0 = bad.wm[0]
+    bad.wm[0] = (c, dr, i, j, k, dv, 0.0)
+    assert code(bad) == 6
+    assert code(s) == 0 and code(None) == 0 and code(s) == 0
+    d.step(1)
+    d.close()
