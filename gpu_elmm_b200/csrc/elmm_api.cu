@@ -253,6 +253,9 @@ struct LaunchSet {
 enum { LK_CELLS = 0, LK_BOX, LK_ROWS, LK_YCOLS, LK_TRI, LK_MOM, LK_SHELL, LK_XREG, LK_YREG, LK_TRIT, LK_TCOL, LK_DCOL,
        LK_AVG, LK_COMMIT, LK_TPAIR, LK_PROJ, LK_PROJ2, LK_DCOL2, LK_N };
 
+// blocks of the host-layout pack / unpack kernels (8 per SM)
+constexpr int kPackBlocks = 148 * 8;
+
 // -------------------------------------------------------------------- batch
 template <typename T>
 struct BatchT {
@@ -285,6 +288,11 @@ struct BatchT {
   // host-layout staging (double), max over domains of the largest host array
   double *dstage = nullptr;
   size_t stage_elems = 0;
+  // a second staging buffer (single-domain handles, allocated at the first
+  // state transfer): the host copy of one field overlaps the pack or unpack
+  // of the next on the side stream
+  double *dstage2 = nullptr;
+  cudaEvent_t ev_stage[2][2] = {};  // [buffer][0: filled on its producer, 1: drained by its consumer]
   std::vector<double *> pr_image;  // per domain: last host Pr image (device)
   int *dbad = nullptr;
   cudaGraphExec_t step_exec = nullptr;
@@ -362,6 +370,28 @@ struct BatchT {
     }
     if (ev_fork) cudaEventDestroy(ev_fork);
     ev_fork = nullptr;
+    for (auto &pair : ev_stage)
+      for (auto &e : pair)
+        if (e) { cudaEventDestroy(e); e = nullptr; }
+  }
+  // the second staging buffer and its events, or false (views, serving
+  // requests and batches keep one buffer and copy field by field)
+  int stage_state = 0;  // 0 untried, 1 two buffers, -1 one buffer
+  bool two_stages() {
+    if (is_view || arena || nd != 1 || !dstage) return false;
+    if (stage_state == 0) {
+      stage_state = -1;
+      if (dalloc((void **)&dstage2, stage_elems * sizeof(double))) { dstage2 = nullptr; return false; }
+      for (auto &pair : ev_stage)
+        for (auto &e : pair)
+          if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return false;
+      for (int b = 0; b < 2; b++) {  // both buffers start free
+        if (cudaEventRecord(ev_stage[b][1], stream) != cudaSuccess) return false;
+        if (cudaEventRecord(ev_stage[b][0], side) != cudaSuccess) return false;
+      }
+      stage_state = 1;
+    }
+    return stage_state == 1;
   }
 
   int dalloc(void **p, size_t bytes) {
@@ -596,6 +626,9 @@ struct BatchT {
   void drop_host_staging() {
     dfree(dstage);
     dstage = nullptr;
+    if (dstage2) dfree(dstage2);
+    dstage2 = nullptr;
+    stage_state = -1;
     stage_elems = 0;
     for (auto &pi : pr_image) { dfree(pi); pi = nullptr; }
   }
@@ -1581,18 +1614,30 @@ struct BatchT {
     CU(cudaMemsetAsync(dbad, 0, sizeof(int), stream));
     const double *src[3] = {U, V, W};
     T *dst[3] = {h.U, h.V, h.W};
+    const bool two = two_stages();
     for (int c = 0; c < 3; c++) {
       HostBox hb = hbox_vel(d, c);
       size_t n = (size_t)hb.n0 * hb.n1 * hb.n2;
-      CU(cudaMemcpyAsync(dstage, src[c], n * sizeof(double), cudaMemcpyHostToDevice, stream));
-      k_unpack<T><<<256, 256, 0, stream>>>(ddom + d, dst[c], dstage, hb, h.ext[c][0], h.ext[c][1], h.ext[c][2], dbad);
+      double *stg = dstage;
+      if (two) {  // copy on the side stream once the buffer's last unpack is done
+        const int b = c & 1;
+        stg = b ? dstage2 : dstage;
+        CU(cudaStreamWaitEvent(side, ev_stage[b][1], 0));
+        CU(cudaMemcpyAsync(stg, src[c], n * sizeof(double), cudaMemcpyHostToDevice, side));
+        CU(cudaEventRecord(ev_stage[b][0], side));
+        CU(cudaStreamWaitEvent(stream, ev_stage[b][0], 0));
+      } else {
+        CU(cudaMemcpyAsync(stg, src[c], n * sizeof(double), cudaMemcpyHostToDevice, stream));
+      }
+      k_unpack<T><<<kPackBlocks, 256, 0, stream>>>(ddom + d, dst[c], stg, hb, h.ext[c][0], h.ext[c][1], h.ext[c][2], dbad);
       k_halo_vel<T><<<256, 256, 0, stream>>>(ddom + d, c);
+      if (two) CU(cudaEventRecord(ev_stage[c & 1][1], stream));
     }
     HostBox hp = hbox_p(d);
     size_t np = (size_t)hp.n0 * hp.n1 * hp.n2;
     if (Pr) {
       CU(cudaMemcpyAsync(pr_image[d], Pr, np * sizeof(double), cudaMemcpyHostToDevice, stream));
-      k_unpack<T><<<256, 256, 0, stream>>>(ddom + d, h.P, pr_image[d], hp, h.nx, h.ny, h.nz, dbad);
+      k_unpack<T><<<kPackBlocks, 256, 0, stream>>>(ddom + d, h.P, pr_image[d], hp, h.nx, h.ny, h.nz, dbad);
     } else {
       CU(cudaMemsetAsync(pr_image[d], 0, np * sizeof(double), stream));
       CU(cudaMemsetAsync(h.P, 0, (size_t)h.plane * (h.nz + 2) * sizeof(T), stream));
@@ -1617,7 +1662,7 @@ struct BatchT {
     const size_t n = (size_t)(h.nx + 6) * (h.ny + 6) * (h.nz + 6);
     CU(cudaMemsetAsync(dbad, 0, sizeof(int), stream));
     CU(cudaMemcpyAsync(dstage, Th, n * sizeof(double), cudaMemcpyHostToDevice, stream));
-    k_unpack_scalar<T><<<256, 256, 0, stream>>>(ddom + d, 0, dstage, dbad);
+    k_unpack_scalar<T><<<kPackBlocks, 256, 0, stream>>>(ddom + d, 0, dstage, dbad);
     int bad = 0;
     CU(cudaMemcpyAsync(&bad, dbad, sizeof(int), cudaMemcpyDeviceToHost, stream));
     CU(cudaStreamSynchronize(stream));
@@ -1636,7 +1681,7 @@ struct BatchT {
     const size_t n = (size_t)(h.nx + 6) * (h.ny + 6) * (h.nz + 6);
     CU(cudaMemsetAsync(dbad, 0, sizeof(int), stream));
     CU(cudaMemcpyAsync(dstage, S, n * sizeof(double), cudaMemcpyHostToDevice, stream));
-    k_unpack_scalar<T><<<256, 256, 0, stream>>>(ddom + d, (h.buoy ? 1 : 0) + sc - 1, dstage, dbad);
+    k_unpack_scalar<T><<<kPackBlocks, 256, 0, stream>>>(ddom + d, (h.buoy ? 1 : 0) + sc - 1, dstage, dbad);
     int bad = 0;
     CU(cudaMemcpyAsync(&bad, dbad, sizeof(int), cudaMemcpyDeviceToHost, stream));
     CU(cudaStreamSynchronize(stream));
@@ -1681,7 +1726,7 @@ struct BatchT {
         int comp = (field == ELMM_FIELD_U || field == ELMM_FIELD_U2) ? 0 : (field == ELMM_FIELD_V || field == ELMM_FIELD_V2) ? 1 : 2;
         F = field <= ELMM_FIELD_W ? (comp == 0 ? h.U : comp == 1 ? h.V : h.W) : (comp == 0 ? h.U2 : comp == 1 ? h.V2 : h.W2);
         HostBox hb = hbox_vel(d, comp);
-        k_pack_vel<T><<<256, 256, 0, s>>>(ddom + d, F, comp, dst, hb);
+        k_pack_vel<T><<<kPackBlocks, 256, 0, s>>>(ddom + d, F, comp, dst, hb);
         return (size_t)hb.n0 * hb.n1 * hb.n2;
       }
       case ELMM_FIELD_USTAR: case ELMM_FIELD_VSTAR: case ELMM_FIELD_WSTAR: {
@@ -1690,14 +1735,14 @@ struct BatchT {
         HostBox hb = hbox_vel(d, comp);
         size_t n = (size_t)hb.n0 * hb.n1 * hb.n2;
         cudaMemsetAsync(dst, 0, n * sizeof(double), s);
-        k_pack_scalar<T><<<256, 256, 0, s>>>(ddom + d, F, dst, hb, 0, 0, h.ext[comp][0], h.ext[comp][1], h.ext[comp][2]);
+        k_pack_scalar<T><<<kPackBlocks, 256, 0, s>>>(ddom + d, F, dst, hb, 0, 0, h.ext[comp][0], h.ext[comp][1], h.ext[comp][2]);
         return n;
       }
       case ELMM_FIELD_PR: {
         HostBox hb = hbox_p(d);
         size_t n = (size_t)hb.n0 * hb.n1 * hb.n2;
         cudaMemcpyAsync(dst, pr_image[d], n * sizeof(double), cudaMemcpyDeviceToDevice, s);
-        k_pack_scalar<T><<<256, 256, 0, s>>>(ddom + d, h.P, dst, hb, 1, 1, h.nx, h.ny, h.nz);
+        k_pack_scalar<T><<<kPackBlocks, 256, 0, s>>>(ddom + d, h.P, dst, hb, 1, 1, h.nx, h.ny, h.nz);
         return n;
       }
       case ELMM_FIELD_TEMPERATURE: case ELMM_FIELD_TDIFF: case ELMM_FIELD_TEMPERATURE_ADV: {
@@ -1706,7 +1751,7 @@ struct BatchT {
         const T *Fs = field == ELMM_FIELD_TEMPERATURE ? h.Tm : field == ELMM_FIELD_TDIFF ? h.TDiff : h.Tadv;
         // TDiff folds like the viscosity: periodic where the flow is
         const int *bt = field == ELMM_FIELD_TDIFF ? h.bt : h.tbt;
-        k_pack_scalar_box<T><<<256, 256, 0, s>>>(ddom + d, Fs, dst, lo, field == ELMM_FIELD_TEMPERATURE ? h.toff : 0.0,
+        k_pack_scalar_box<T><<<kPackBlocks, 256, 0, s>>>(ddom + d, Fs, dst, lo, field == ELMM_FIELD_TEMPERATURE ? h.toff : 0.0,
                                                  field == ELMM_FIELD_TEMPERATURE_ADV, bt[0] == BC_PERIODIC,
                                                  bt[2] == BC_PERIODIC, bt[4] == BC_PERIODIC);
         return n;
@@ -1715,7 +1760,7 @@ struct BatchT {
         HostBox hb = hbox_p(d);
         size_t n = (size_t)hb.n0 * hb.n1 * hb.n2;
         cudaMemsetAsync(dst, 0, n * sizeof(double), s);
-        k_pack_scalar<T><<<256, 256, 0, s>>>(ddom + d, field == ELMM_FIELD_PHI ? h.Phi : h.nu, dst, hb,
+        k_pack_scalar<T><<<kPackBlocks, 256, 0, s>>>(ddom + d, field == ELMM_FIELD_PHI ? h.Phi : h.nu, dst, hb,
                                               field == ELMM_FIELD_PHI ? 2 : 3, 0, h.nx, h.ny, h.nz);
         return n;
       }
@@ -1724,7 +1769,7 @@ struct BatchT {
       const bool adv = field >= ELMM_FIELD_SCALAR_ADV;
       const ScalSlot<T> &sl = h.slot[(h.buoy ? 1 : 0) + field - (adv ? ELMM_FIELD_SCALAR_ADV : ELMM_FIELD_SCALAR)];
       const size_t n = (size_t)(h.nx + 6) * (h.ny + 6) * (h.nz + 6);
-      k_pack_scalar_box<T><<<256, 256, 0, s>>>(ddom + d, adv ? sl.adv : sl.buf[0], dst, -2, sl.off, adv,
+      k_pack_scalar_box<T><<<kPackBlocks, 256, 0, s>>>(ddom + d, adv ? sl.adv : sl.buf[0], dst, -2, sl.off, adv,
                                                sl.bt[0] == BC_PERIODIC, sl.bt[2] == BC_PERIODIC, sl.bt[4] == BC_PERIODIC);
       return n;
     }
@@ -1752,11 +1797,32 @@ struct BatchT {
 
   int download(int d, double *U, double *V, double *W, double *Pr) {
     double *dst[4] = {U, V, W, Pr};
-    for (int f = 0; f < 4; f++)
-      if (dst[f]) {
-        int r = download_field(d, f, dst[f]);
-        if (r) return r;
-      }
+    if (d < 0 || d >= nd) return fail(ELMM_ERR_INVALID_ARG, "domain index");
+    CU(cudaSetDevice(device));
+    if (!two_stages()) {
+      for (int f = 0; f < 4; f++)
+        if (dst[f]) {
+          int r = download_field(d, f, dst[f]);
+          if (r) return r;
+        }
+      return ELMM_OK;
+    }
+    // pack field f into one buffer while the other is copied to the host
+    int b = 0;
+    for (int f = 0; f < 4; f++) {
+      if (!dst[f]) continue;
+      double *stg = b ? dstage2 : dstage;
+      CU(cudaStreamWaitEvent(stream, ev_stage[b][1], 0));  // its last host copy is done
+      size_t n = pack(d, f, stg, stream);
+      CU(cudaEventRecord(ev_stage[b][0], stream));
+      CU(cudaStreamWaitEvent(side, ev_stage[b][0], 0));
+      CU(cudaMemcpyAsync(dst[f], stg, n * sizeof(double), cudaMemcpyDeviceToHost, side));
+      CU(cudaEventRecord(ev_stage[b][1], side));
+      b ^= 1;
+    }
+    CU(cudaStreamSynchronize(side));
+    CU(cudaStreamSynchronize(stream));
+    CU(cudaGetLastError());
     return ELMM_OK;
   }
 
@@ -1853,12 +1919,12 @@ static int poisson_exec(BatchT<T> &B, double *Phi, const double *RHS) {
   size_t n = (size_t)hb.n0 * hb.n1 * hb.n2;
   CU(cudaMemcpyAsync(B.dstage, RHS, n * sizeof(double), cudaMemcpyHostToDevice, B.stream));
   CU(cudaMemsetAsync(B.dbad, 0, sizeof(int), B.stream));
-  k_unpack<T><<<256, 256, 0, B.stream>>>(B.ddom, h.Phi, B.dstage, hb, h.nx, h.ny, h.nz, B.dbad);
+  k_unpack<T><<<kPackBlocks, 256, 0, B.stream>>>(B.ddom, h.Phi, B.dstage, hb, h.nx, h.ny, h.nz, B.dbad);
   B.launch_poisson(1.0, 0, 1, 0);
   HostBox hp = B.hbox_p(0);
   size_t np = (size_t)hp.n0 * hp.n1 * hp.n2;
   CU(cudaMemcpyAsync(B.dstage, Phi, np * sizeof(double), cudaMemcpyHostToDevice, B.stream));
-  k_pack_scalar<T><<<256, 256, 0, B.stream>>>(B.ddom, h.Phi, B.dstage, hp, 0, 0, h.nx, h.ny, h.nz);
+  k_pack_scalar<T><<<kPackBlocks, 256, 0, B.stream>>>(B.ddom, h.Phi, B.dstage, hp, 0, 0, h.nx, h.ny, h.nz);
   CU(cudaMemcpyAsync(Phi, B.dstage, np * sizeof(double), cudaMemcpyDeviceToHost, B.stream));
   CU(cudaStreamSynchronize(B.stream));
   CU(cudaGetLastError());
