@@ -330,6 +330,8 @@ struct BatchT {
   struct SolidSet {
     IBGather *vel = nullptr, *visc = nullptr;
     int nvel = 0, nib = 0, nvisc = 0;
+    long long *null = nullptr;  // box indices of the nullified points of U, then V, then W
+    NullCounts nnull{{0, 0, 0}};
     WMSolid *wm = nullptr;
     double *wm_ustar = nullptr;
     int nwm = 0;
@@ -1149,9 +1151,11 @@ struct BatchT {
           k_ib_gather<T><<<std::min((x.nib + 255) / 256, 148 * 8), 256, 0, stream>>>(ddom, d, x.vel, x.nib, 1);
         }
       }
-      if (which == 2 && x.nvel > 0) {
+      const int nnull = x.nnull.n[0] + x.nnull.n[1] + x.nnull.n[2];
+      if (which == 2 && x.nib + nnull > 0) {
         nlaunch++;
-        k_ib_gather<T><<<std::min((x.nvel + 255) / 256, 148 * 8), 256, 0, stream>>>(ddom, d, x.vel, x.nvel, 0);
+        k_ib_gather<T><<<std::min((x.nib + nnull + 255) / 256, 148 * 8), 256, 0, stream>>>(ddom, d, x.vel, x.nib, 0,
+                                                                                         x.null, x.nnull);
       }
     }
   }
@@ -1262,7 +1266,7 @@ struct BatchT {
     if (d >= (int)sol.size()) return;
     SolidSet &x = sol[d];
     for (void *p : {(void *)x.vel, (void *)x.visc, (void *)x.wm, (void *)x.wm_ustar, (void *)x.bskip[0],
-                    (void *)x.bskip[1], (void *)x.bskip[2]})
+                    (void *)x.bskip[1], (void *)x.bskip[2], (void *)x.null})
       if (p) dfree(p);
     x = SolidSet();
     for (int c = 0; c < 3; c++) hdom[d].bskip[c] = nullptr;
@@ -1348,6 +1352,8 @@ struct BatchT {
           !add_points(comp, s->ib[comp], s->n_ib[comp], vel))
         return fail(ELMM_ERR_INVALID_ARG, "IB point out of range (or within one cell of a periodic boundary)");
     const int nib = (int)vel.size();
+    std::vector<long long> nulls;
+    int ncomp_null[3] = {0, 0, 0};
     for (int comp = 0; comp < 3; comp++) {
       if (s->n_null[comp] < 0 || (s->n_null[comp] > 0 && !s->null_ijk[comp]))
         return fail(ELMM_ERR_INVALID_ARG, "nullified points");
@@ -1355,12 +1361,10 @@ struct BatchT {
         const int32_t *t = s->null_ijk[comp] + 3 * q;
         if (!in_target(comp, t[0], t[1], t[2]))
           return fail(ELMM_ERR_INVALID_ARG, "nullified point out of range (or within one cell of a periodic boundary)");
-        IBGather g{};
-        g.tgt = bidx(h, t[0], t[1], t[2]);
-        g.comp = comp;
-        g.n = -1;
-        targets[comp].push_back(g.tgt);
-        vel.push_back(g);
+        const long long idx = bidx(h, t[0], t[1], t[2]);
+        targets[comp].push_back(idx);
+        nulls.push_back(idx);
+        ncomp_null[comp]++;
       }
     }
     if (s->n_scalfl < 0 || (s->n_scalfl > 0 && !s->scalfl) || !add_points(3, s->scalfl, s->n_scalfl, visc))
@@ -1403,6 +1407,8 @@ struct BatchT {
                                                                                  : fail(ELMM_ERR_CUDA, "cudaMemcpy");
     };
     if ((r = up((void **)&x.vel, vel.data(), vel.size() * sizeof(IBGather)))) return r;
+    if ((r = up((void **)&x.null, nulls.data(), nulls.size() * sizeof(long long)))) return r;
+    for (int comp = 0; comp < 3; comp++) x.nnull.n[comp] = ncomp_null[comp];
     if ((r = up((void **)&x.visc, visc.data(), visc.size() * sizeof(IBGather)))) return r;
     if ((r = up((void **)&x.wm, wm.data(), wm.size() * sizeof(WMSolid)))) return r;
     std::vector<double> us(wm.size(), 1.0);  // WMPointUVW%ustar starts at 1 (immersedboundary.f90:235)

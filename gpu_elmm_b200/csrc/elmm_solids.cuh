@@ -12,8 +12,8 @@ namespace elmm {
 
 // One target of a gather: F[tgt] = sum_m coef[m] * F[src[m]] (TIBPoint_Interpolate,
 // src/immersedboundary.f90:637-651).  comp: 0..2 velocity component, 3 the
-// viscosity.  n = -1 marks a nullified point (NullInterior), n = 0 an IB
-// point without interpolation points (its value becomes 0).  Interpolation
+// viscosity.  n = 0: an IB point without interpolation points (its value
+// becomes 0).  Nullified points are a separate list of box indices.  Interpolation
 // points in the ghost layer are folded onto the interior cell (and sign) that
 // the ghost rule copies, so a gather reads interior cells only.
 struct IBGather {
@@ -34,21 +34,34 @@ struct WMSolid {
 };
 
 // mode 0: the gathers (after the projection, and the first IBMomentum of a
-// run; or the viscosity of the ScalFl points);
+// run; or the viscosity of the ScalFl points), and after the n gathers the
+// nullified points: box indices null[0 .. nnull[0]) of U, then of V, then of W;
 // mode 1: U2, V2, W2 at the IB points set to zero before the divergence.
 // IBMassSources adds U2(p)/dx at the cell behind an IB point p and takes it
 // off the cell in front (src/tsteps.f90:490-533), and the right-hand side
 // is div U2 - Q (src/pressure.f90:658-670): together they remove the face
 // velocity of p from both divergences, which is the divergence of U2 with
 // U2(p) = 0.  The value at p itself is replaced after the projection.
+struct NullCounts {
+  int n[3];  // nullified points of U, V, W
+};
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_ib_gather(const Dom<T> *__restrict__ doms, int di,
-                                                   const IBGather *__restrict__ pts, int n, int mode) {
+                                                   const IBGather *__restrict__ pts, int n, int mode,
+                                                   const long long *__restrict__ null = nullptr,
+                                                   NullCounts nn = NullCounts{{0, 0, 0}}) {
   const Dom<T> &d = doms[di];
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+  const int ntot = n + nn.n[0] + nn.n[1] + nn.n[2];
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < ntot; q += gridDim.x * blockDim.x) {
+    if (q >= n) {  // NullInterior (src/tsteps.f90:540-567)
+      const int r = q - n;
+      T *F = r < nn.n[0] ? d.U : r < nn.n[0] + nn.n[1] ? d.V : d.W;
+      F[null[r]] = (T)0;
+      continue;
+    }
     const IBGather &p = pts[q];
     if (mode == 1) {
-      if (p.n < 0) continue;
       T *F = p.comp == 0 ? d.U2 : p.comp == 1 ? d.V2 : d.W2;
       F[p.tgt] = (T)0;
       continue;
