@@ -85,6 +85,33 @@ class ElmmConfig(C.Structure):
     ]
 
 
+MAX_PUFFS, MAX_PUFF_VOLUMES = 4, 16
+
+
+class ElmmPuff(C.Structure):
+    """PuffSource (src/puffs.f90:15-21)."""
+    _fields_ = [("start_time", C.c_double), ("end_time", C.c_double), ("period", C.c_double),
+                ("duration", C.c_double), ("clear", C.c_int32), ("reserved", C.c_int32)]
+
+
+class ElmmPuffVolume(C.Structure):
+    """A ScalarFlVolume of a puff."""
+    _fields_ = [("puff", C.c_int32), ("scalar_number", C.c_int32), ("xi", C.c_int32), ("yj", C.c_int32),
+                ("zk", C.c_int32), ("reserved", C.c_int32), ("flux", C.c_double)]
+
+
+def make_puffs(puffs, volumes):
+    """ctypes arrays and counts for elmm_set_puffs: puffs as (start, end,
+    period, duration, clear), volumes as (puff, scalar_number, (i, j, k), flux)."""
+    P = (ElmmPuff * max(1, len(puffs)))()
+    for n, (a, b, per, dur, clr) in enumerate(puffs):
+        P[n] = ElmmPuff(a, b, per, dur, int(clr), 0)
+    V = (ElmmPuffVolume * max(1, len(volumes)))()
+    for n, (p, sc, (i, j, k), fl) in enumerate(volumes):
+        V[n] = ElmmPuffVolume(p, sc, i, j, k, 0, fl)
+    return P, len(puffs), V, len(volumes)
+
+
 IB_MAX_INTERP = 6
 
 

@@ -8,6 +8,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <limits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -1183,6 +1184,19 @@ struct BatchT {
   }
   int enqueue_step(bool cfl, bool div) {
     if (cfl) launch_cfl();
+    bool puffs = false, clear = false;
+    for (int d = 0; d < nd; d++) {
+      puffs |= hdom[d].npuff > 0;
+      clear |= hdom[d].puff_clear_any != 0;
+    }
+    if (puffs) {  // PreparePuffs before the first stage's scalars (src/scalars.f90:217)
+      nlaunch++;
+      k_puff_step<T><<<(nd + 127) / 128, 128, 0, stream>>>(ddom, nd);
+      if (clear) {
+        nlaunch++;
+        k_puff_clear<T><<<148 * 4, 256, 0, stream>>>(ddom, nd);
+      }
+    }
     for (int s = 1; s <= 3; s++) run_stage(s, 3, s == 3, false, div && s == 3);
     if (div && !any_solids()) launch_divmax();
     return ELMM_OK;
@@ -1259,6 +1273,63 @@ struct BatchT {
     if (r) return r;
     CU(cudaGetLastError());
     return ELMM_OK;
+  }
+
+  // ------------------------------------------------------------ puffs
+  // elmm_set_puffs: windows and volumes into the descriptor, the state (last
+  // release -huge, as PuffSource%last_start starts) and the clock on the device
+  int set_puffs(int d, const elmm_puff *pf, int np, const elmm_puff_volume *vol, int nv) {
+    CU(cudaSetDevice(device));
+    CU(cudaStreamSynchronize(stream));
+    Dom<T> &h = hdom[d];
+    const elmm_config &c = cfg[d];
+    if (np < 0 || np > kMaxPuffs || nv < 0 || nv > kMaxPuffVols || (np > 0 && !pf) || (nv > 0 && !vol))
+      return fail(ELMM_ERR_INVALID_ARG, "puffs: at most ELMM_MAX_PUFFS puffs and ELMM_MAX_PUFF_VOLUMES volumes");
+    for (int q = 0; q < np; q++)
+      if (!std::isfinite(pf[q].start_time) || !std::isfinite(pf[q].end_time) || !std::isfinite(pf[q].period) ||
+          !std::isfinite(pf[q].duration))
+        return fail(ELMM_ERR_INVALID_ARG, "puffs: non-finite window");
+    for (int q = 0; q < nv; q++) {
+      const elmm_puff_volume &v = vol[q];
+      if (v.puff < 0 || v.puff >= np || v.scalar_number < 1 || v.scalar_number > c.num_scalars || v.xi < 1 ||
+          v.xi > h.nx || v.yj < 1 || v.yj > h.ny || v.zk < 1 || v.zk > h.nz || !std::isfinite(v.flux))
+        return fail(ELMM_ERR_INVALID_ARG, "puff volume: puff index, scalar or cell out of range");
+    }
+    if (step_exec) { cudaGraphExecDestroy(step_exec); step_exec = nullptr; }
+    if (!h.puff_state) {
+      double *st;
+      int r = dalloc((void **)&st, (4 * kMaxPuffs + 1) * sizeof(double));
+      if (r) return r;
+      h.puff_state = st;
+    }
+    std::vector<double> st(4 * kMaxPuffs + 1, 0.0);
+    h.npuff = np;
+    h.puff_clear_any = 0;
+    for (int q = 0; q < np; q++) {
+      st[4 * q] = -std::numeric_limits<double>::max();
+      h.puff_start[q] = pf[q].start_time;
+      h.puff_end[q] = pf[q].end_time;
+      h.puff_period[q] = pf[q].period;
+      h.puff_dur[q] = pf[q].duration;
+      h.puff_clear_slots[q] = 0;
+    }
+    st[4 * kMaxPuffs] = time;
+    h.npv = nv;
+    for (int q = 0; q < nv; q++) {
+      const int slot = (h.buoy ? 1 : 0) + vol[q].scalar_number - 1;
+      h.pv_puff[q] = vol[q].puff;
+      h.pv_slot[q] = slot;
+      h.pv_i[q] = vol[q].xi;
+      h.pv_j[q] = vol[q].yj;
+      h.pv_k[q] = vol[q].zk;
+      h.pv_q[q] = vol[q].flux;
+      if (pf[vol[q].puff].clear) {
+        h.puff_clear_slots[vol[q].puff] |= 1u << slot;
+        h.puff_clear_any = 1;
+      }
+    }
+    CU(cudaMemcpy(h.puff_state, st.data(), st.size() * sizeof(double), cudaMemcpyHostToDevice));
+    return push_dom(d);
   }
 
   // ------------------------------------------------------------ solids
@@ -2040,6 +2111,12 @@ int elmm_step(elmm_handle *h, int32_t nsteps, elmm_stats *st) {
   if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
   if (nsteps < 0) return fail(ELMM_ERR_INVALID_ARG, "nsteps < 0");
   return DISPATCH(h->b, step(nsteps, st));
+}
+
+int elmm_set_puffs(elmm_handle *h, const elmm_puff *puffs, int32_t npuffs, const elmm_puff_volume *volumes,
+                   int32_t nvolumes) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  return DISPATCH(h->b, set_puffs(0, puffs, npuffs, volumes, nvolumes));
 }
 
 int elmm_set_solids(elmm_handle *h, const elmm_solids *s) {

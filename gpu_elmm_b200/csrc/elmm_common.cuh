@@ -41,6 +41,8 @@ template <> struct Vec2<float> { typedef float2 type; };
 // the velocity boxes.
 constexpr int kMaxSlots = 5;    // temperature + ELMM_MAX_SCALARS passive scalars
 constexpr int kMaxSources = 8;  // ELMM_MAX_POINT_SOURCES
+constexpr int kMaxPuffs = 4;    // ELMM_MAX_PUFFS
+constexpr int kMaxPuffVols = 16;  // ELMM_MAX_PUFF_VOLUMES
 template <typename T>
 struct ScalSlot {
   // three value buffers in rotation: stage s of a step reads buf[(s-1) % 3]
@@ -138,6 +140,16 @@ struct Dom {
   int nsrc;
   int src_slot[kMaxSources], src_i[kMaxSources], src_j[kMaxSources], src_k[kMaxSources];
   double src_q[kMaxSources];
+  // puffs (src/puffs.f90): windows and volumes; puff_state on the device holds
+  // per puff {last_start, dt_fraction, restart, -} and, after them, the time
+  // of the next step
+  int npuff, puff_clear_any;
+  double puff_start[kMaxPuffs], puff_end[kMaxPuffs], puff_period[kMaxPuffs], puff_dur[kMaxPuffs];
+  unsigned puff_clear_slots[kMaxPuffs];  // bit s: slot s is cleared at a release of the puff
+  double *puff_state;
+  int npv;
+  int pv_puff[kMaxPuffVols], pv_slot[kMaxPuffVols], pv_i[kMaxPuffVols], pv_j[kMaxPuffVols], pv_k[kMaxPuffVols];
+  double pv_q[kMaxPuffVols];
   // time-averaged slices: plane k, plane j (0: none), weight of one step
   int avg_k, avg_j;
   double avg_w;

@@ -102,9 +102,11 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
     }
     auto zoff = [&](int kk) { return (long long)(scal_fold(kk, nz, pz) - kk) * plane; };  // fold of plane kk
     // volume sources of this slot in this column, in configuration order
-    unsigned srcm = 0;
+    unsigned srcm = 0, pvm = 0;
     for (int q = 0; q < d.nsrc; q++)
       if (d.src_slot[q] == s && d.src_i[q] == i && d.src_j[q] == j) srcm |= 1u << q;
+    for (int q = 0; q < d.npv; q++)
+      if (d.pv_slot[q] == s && d.pv_i[q] == i && d.pv_j[q] == j) pvm |= 1u << q;
     const T *__restrict__ S = sl.buf[(stage - 1) % 3];
     const T *__restrict__ K = d.TDiff;
     const T *__restrict__ U = d.U;
@@ -163,6 +165,13 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
       if (srcm) {
         for (int q = 0; q < d.nsrc; q++)
           if (((srcm >> q) & 1u) && d.src_k[q] == k) a = a + (T)d.src_q[q];
+      }
+      if (pvm) {  // DoPuffs, after the point sources (src/scalars.f90:368-370)
+        for (int q = 0; q < d.npv; q++)
+          if (((pvm >> q) & 1u) && d.pv_k[q] == k) {
+            const double f = d.puff_state[4 * d.pv_puff[q] + 1];
+            if (f > 0) a = a + (T)(f * d.pv_q[q]);
+          }
       }
       // wall-model point next to a wall-model side: + div * value (the
       // surface flux is zero); div as DivergenceWM with dzPr(k)
@@ -244,9 +253,11 @@ __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SP
 #pragma unroll
     for (int q = 0; q < 5; q++) oy[q] = (scal_fold(j - 2 + q, ny, py) - j) * (int)pitch;
     auto zoff = [&](int kk) { return (long long)(scal_fold(kk, nz, pz) - kk) * plane; };
-    unsigned srcm = 0;  // volume sources of this slot in this pair's columns
+    unsigned srcm = 0, pvm = 0;  // volume sources (point sources, puffs) of this slot in this pair's columns
     for (int q = 0; q < d.nsrc; q++)
       if (d.src_slot[q] == s && (d.src_i[q] == i || d.src_i[q] == i + 1) && d.src_j[q] == j) srcm |= 1u << q;
+    for (int q = 0; q < d.npv; q++)
+      if (d.pv_slot[q] == s && (d.pv_i[q] == i || d.pv_i[q] == i + 1) && d.pv_j[q] == j) pvm |= 1u << q;
     const T *__restrict__ S = sl.buf[(stage - 1) % 3];
     const T *__restrict__ K = d.TDiff;
     const T *__restrict__ U = d.U;
@@ -323,6 +334,13 @@ __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SP
           for (int q = 0; q < d.nsrc; q++)
             if (((srcm >> q) & 1u) && d.src_i[q] == i + c && d.src_k[q] == k) a = a + (T)d.src_q[q];
         }
+        if (pvm) {  // DoPuffs, after the point sources (src/scalars.f90:368-370)
+          for (int q = 0; q < d.npv; q++)
+            if (((pvm >> q) & 1u) && d.pv_i[q] == i + c && d.pv_k[q] == k) {
+              const double f = d.puff_state[4 * d.pv_puff[q] + 1];
+              if (f > 0) a = a + (T)(f * d.pv_q[q]);
+            }
+        }
         if (wmk) {
           const T dzk = (T)d.dzPr[k + 2];
           const T ue = c ? u0.y : u0.x, uw = c ? u0.x : um.y;
@@ -354,6 +372,59 @@ __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SP
         fzb = fzt;
         cc = cn;
       }
+    }
+  }
+}
+
+// PreparePuffs (src/puffs.f90:30-84) at the start of a step, one thread per
+// domain: whether each puff restarts in this step, the fraction of the step
+// its window covers (the restart branch keeps the reference's
+// `time + dt - max(...) / dt`), the time of its last release (updated at the
+// last stage there; nothing reads it in between), and the clock.
+template <typename T>
+__global__ void k_puff_step(const Dom<T> *__restrict__ doms, int nd) {
+  const int di = blockIdx.x * blockDim.x + threadIdx.x;
+  if (di >= nd) return;
+  const Dom<T> &d = doms[di];
+  if (d.npuff == 0) return;
+  double *st = d.puff_state;
+  const double time = st[4 * kMaxPuffs], dt = d.dt;
+  for (int p = 0; p < d.npuff; p++) {
+    double last = st[4 * p];
+    const double start = d.puff_start[p], end = d.puff_end[p], period = d.puff_period[p], dur = d.puff_dur[p];
+    const bool restart = time + dt > last + period && time + dt >= start && time <= end;
+    double f;
+    if (!restart && time <= last + dur && time >= start)
+      f = fmax(fmin(fmin(last + dur, time + dt), end) - time, 0.0) / dt;
+    else if (restart)
+      f = time + dt - fmax(fmax(last + period, time), start) / dt;
+    else
+      f = 0;
+    st[4 * p + 1] = f;
+    st[4 * p + 2] = restart ? 1.0 : 0.0;
+    if (restart) last = last >= start ? last + period : start;
+    st[4 * p] = last;
+  }
+  st[4 * kMaxPuffs] = time + dt;
+}
+
+// The `clear` of a releasing puff: its scalars are set to zero, ghosts
+// included, before the first stage reads them (src/puffs.f90:66-74).
+template <typename T>
+__global__ void k_puff_clear(const Dom<T> *__restrict__ doms, int nd) {
+  for (int di = 0; di < nd; di++) {
+    const Dom<T> &d = doms[di];
+    if (!d.puff_clear_any) continue;
+    unsigned slots = 0;
+    for (int p = 0; p < d.npuff; p++)
+      if (d.puff_state[4 * p + 2] != 0) slots |= d.puff_clear_slots[p];
+    if (!slots) continue;
+    const long long n = d.plane * (long long)(d.nz + 2);
+    for (int s = 0; s < d.nslot; s++) {
+      if (!((slots >> s) & 1u)) continue;
+      T *F = d.slot[s].buf[0];
+      for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        F[q] = (T)(0.0 - d.slot[s].off);
     }
   }
 }

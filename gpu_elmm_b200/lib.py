@@ -50,6 +50,7 @@ def lib():
         L.elmm_upload_temperature.argtypes = [P, _dp]
         L.elmm_upload_scalar.argtypes = [P, C.c_int32, _dp]
         L.elmm_set_solids.argtypes = [P, P]
+        L.elmm_set_puffs.argtypes = [P, P, C.c_int32, P, C.c_int32]
         L.elmm_download_scalar_slices.argtypes = [P, C.c_int32, _dp, _dp]
         L.elmm_reset_scalar_averages.argtypes = [P]
         L.elmm_download_field.argtypes = [P, C.c_int32, _dp]
@@ -136,6 +137,14 @@ class Domain:
 
     def temperature(self):
         return self.field(12)
+
+    def set_puffs(self, puffs, volumes):
+        """Puff sources: puffs as (start, end, period, duration, clear),
+        volumes as (puff, scalar_number, (i, j, k), flux); [] removes them."""
+        from .config import make_puffs
+        P, n_p, V, n_v = make_puffs(puffs, volumes)
+        check(lib().elmm_set_puffs(self.h, C.cast(P, C.c_void_p), n_p, C.cast(V, C.c_void_p), n_v), "elmm_set_puffs")
+        self._puffs = (P, V)
 
     def set_solids(self, solids):
         """Installs solid bodies (gpu_elmm_b200.solids.Solids, or None to remove them)."""

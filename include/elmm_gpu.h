@@ -211,6 +211,39 @@ int elmm_upload_temperature(elmm_handle *h, const double *T);
  * Returns ELMM_ERR_NAN for non-finite values. */
 int elmm_upload_scalar(elmm_handle *h, int32_t sc, const double *S);
 
+/* ---- puffs ----------------------------------------------------------------
+ * PuffSource of src/puffs.f90:15-21: volume sources of passive scalars that
+ * are switched on in windows of `duration` every `period` between
+ * `start_time` and `end_time`; `clear` zeroes the puff's scalars at each
+ * release.  The reference builds them in custom code (CustomPuffSources,
+ * src/puffs.f90:129-139); here the host passes them.  Every elmm_step
+ * applies PreparePuffs at the start of the step (the fraction of the step
+ * that a window covers, :30-84) and DoPuffs in each scalar stage after the
+ * point sources (:86-126, src/scalars.f90:366-372). */
+#define ELMM_MAX_PUFFS 4
+#define ELMM_MAX_PUFF_VOLUMES 16
+typedef struct elmm_puff {
+  double start_time, end_time, period, duration;
+  int32_t clear, reserved;
+} elmm_puff;
+
+/* ScalarFlVolume of a puff: cell (xi, yj, zk) of the pressure grid, the
+ * scalar it feeds (1..num_scalars) and its flux per unit volume. */
+typedef struct elmm_puff_volume {
+  int32_t puff;           /* 0..npuffs-1 */
+  int32_t scalar_number;
+  int32_t xi, yj, zk, reserved;
+  double flux;
+} elmm_puff_volume;
+
+/* Installs the puffs of a single-domain handle (npuffs = 0 removes them);
+ * their clock starts at the handle's current time.  Up to ELMM_MAX_PUFFS
+ * puffs and ELMM_MAX_PUFF_VOLUMES volumes; ELMM_ERR_INVALID_ARG otherwise or
+ * for a cell, scalar or puff index out of range.  elmm_run_stage does not
+ * advance the puffs. */
+int elmm_set_puffs(elmm_handle *h, const elmm_puff *puffs, int32_t npuffs, const elmm_puff_volume *volumes,
+                   int32_t nvolumes);
+
 /* ---- immersed solid bodies ----------------------------------------------
  * The host describes its solid bodies by the point lists its own geometry
  * pass builds once at start-up: GetSolidBodiesBC (FindInsideCells,

@@ -28,6 +28,7 @@
 
 #include <algorithm>
 #include <array>
+#include <limits>
 #include <cmath>
 #include <complex>
 #include <cstdint>
@@ -186,6 +187,17 @@ struct Domain {
   std::vector<elmm_ib_point> ibp[4], scalfl;
   std::vector<std::array<int, 3>> nullp[4];
   A3 Q;        // IBMassSources, Q(0:Prnx+1,0:Prny+1,0:Prnz+1)
+  // PuffSources (src/puffs.f90:15-23) and their ScalarFlVolumes
+  struct Puff {
+    double start_time, end_time, period, duration;
+    bool clear;
+    double last_start;
+    bool restart;
+    double dt_fraction;
+  };
+  std::vector<Puff> puffs;
+  struct PuffVol { int puff, sc, i, j, k; double flux; };
+  std::vector<PuffVol> puffvols;
   int called = 0;  // the "called" flag of TMarchRK3 (src/tsteps.f90:35)
 };
 
@@ -869,6 +881,13 @@ static void ScalarStage(Domain &d, int stage, double dt, A3 &Arr, A3 &Arr2, A3 &
   if (sc > 0)
     for (const auto &v : d.flvolumes)
       if (v.sc == sc) Adv(v.i, v.j, v.k) = Adv(v.i, v.j, v.k) + v.flux;
+  // DoPuffs / DoPuff, puffs.f90:86-126 (ScalarExtra, scalars.f90:366-372)
+  if (sc > 0)
+    for (size_t q = 0; q < d.puffs.size(); q++)
+      if (d.puffs[q].dt_fraction > 0)
+        for (const auto &v : d.puffvols)
+          if (v.puff == (int)q && v.sc == sc)
+            Adv(v.i, v.j, v.k) = Adv(v.i, v.j, v.k) + d.puffs[q].dt_fraction * v.flux;
   for (int j = 1; j <= ny; j++)
     for (int i = 1; i <= nx; i++) {
       if (wb) Adv(i, j, 1) = Adv(i, j, 1) + divb[(size_t)(j - 1) * nx + i - 1] * Arr(i, j, 1);
@@ -879,9 +898,31 @@ static void ScalarStage(Domain &d, int stage, double dt, A3 &Arr, A3 &Arr2, A3 &
   bound(Arr);
 }
 
+// PreparePuffs, puffs.f90:30-84 (RK_stages = 3), with its
+// `time + dt - max(...) / dt` as written
+static void PreparePuffs(Domain &d, int stage, double time, double dt) {
+  for (size_t q = 0; q < d.puffs.size(); q++) {
+    Domain::Puff &p = d.puffs[q];
+    if (stage == 1) {
+      p.restart = time + dt > p.last_start + p.period && time + dt >= p.start_time && time <= p.end_time;
+      if (!p.restart && time <= p.last_start + p.duration && time >= p.start_time)
+        p.dt_fraction = std::max(std::min(std::min(p.last_start + p.duration, time + dt), p.end_time) - time, 0.0) / dt;
+      else if (p.restart)
+        p.dt_fraction = time + dt - std::max(std::max(p.last_start + p.period, time), p.start_time) / dt;
+      else
+        p.dt_fraction = 0;
+      if (p.clear && p.restart)
+        for (const auto &v : d.puffvols)
+          if (v.puff == (int)q && v.sc >= 1 && v.sc <= d.num_scalars) d.S[v.sc - 1].fill(0);
+    }
+    if (p.restart && stage == 3) p.last_start = p.last_start >= p.start_time ? p.last_start + p.period : p.start_time;
+  }
+}
+
 // ScalarRK3 (scalars.f90:88-381): the temperature, then each passive scalar
 static void ScalarRK3(Domain &d, int stage, double dt) {
   if (d.enable_buoyancy) ScalarStage(d, stage, dt, d.T, d.T2, d.Tadv, 0);
+  PreparePuffs(d, stage, d.time, dt);  // scalars.f90:217
   for (int sc = 1; sc <= d.num_scalars; sc++)
     ScalarStage(d, stage, dt, d.S[sc - 1], d.S2[sc - 1], d.Sadv[sc - 1], sc);
 }
@@ -1806,6 +1847,22 @@ void *orc_create(const elmm_config *c) {
 }
 
 void orc_destroy(void *h) { delete (Domain *)h; }
+
+// Puff sources in the layout of elmm_set_puffs; PuffSource%last_start starts
+// at -huge (puffs.f90:16)
+int orc_set_puffs(void *h, const elmm_puff *pf, int np, const elmm_puff_volume *vol, int nv) {
+  Domain &d = *(Domain *)h;
+  d.puffs.clear();
+  d.puffvols.clear();
+  for (int q = 0; q < np; q++)
+    d.puffs.push_back({pf[q].start_time, pf[q].end_time, pf[q].period, pf[q].duration, pf[q].clear != 0,
+                       -std::numeric_limits<double>::max(), false, 0.0});
+  for (int q = 0; q < nv; q++) {
+    if (vol[q].puff < 0 || vol[q].puff >= np) return 1;
+    d.puffvols.push_back({vol[q].puff, vol[q].scalar_number, vol[q].xi, vol[q].yj, vol[q].zk, vol[q].flux});
+  }
+  return 0;
+}
 
 // The solid bodies of GetSolidBodiesBC / SetNullifiedPoints as lists (the
 // layout of elmm_solids): IB points, nullified points, ScalFl points, the

@@ -48,6 +48,7 @@ def lib():
         L.orc_num_threads.restype = C.c_int
         L.orc_scalar_slices.argtypes = [P, C.c_int, dp, dp]
         L.orc_set_solids.argtypes = [P, P]
+        L.orc_set_puffs.argtypes = [P, P, C.c_int, P, C.c_int]
         _lib = L
     return _lib
 
@@ -140,6 +141,14 @@ class Oracle:
         xy, xz = np.zeros((Prny, Prnx)), np.zeros((Prnz, Prnx))
         assert lib().orc_scalar_slices(self.h, sc, _ptr(xy), _ptr(xz)) == 0
         return xy, xz
+
+    def set_puffs(self, puffs, volumes):
+        """puffs as (start, end, period, duration, clear), volumes as
+        (puff, scalar_number, (i, j, k), flux)."""
+        from gpu_elmm_b200.config import make_puffs
+        P, n_p, V, n_v = make_puffs(puffs, volumes)
+        assert lib().orc_set_puffs(self.h, C.cast(P, C.c_void_p), n_p, C.cast(V, C.c_void_p), n_v) == 0
+        self._puffs = (P, V)
 
     def set_solids(self, solids):
         """Installs solid bodies: a gpu_elmm_b200.solids.Solids (or None)."""

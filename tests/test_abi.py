@@ -53,6 +53,9 @@ int main(void) {
   printf("elmm_ib_point.size %zu\n", sizeof(elmm_ib_point));
   printf("elmm_wm_point.size %zu\n", sizeof(elmm_wm_point));
   printf("elmm_solids.size %zu\n", sizeof(elmm_solids));
+  printf("elmm_puff.size %zu\n", sizeof(elmm_puff));
+  printf("elmm_puff_volume.size %zu\n", sizeof(elmm_puff_volume));
+  O(elmm_puff, clear) O(elmm_puff_volume, zk) O(elmm_puff_volume, flux)
   O(elmm_ib_point, interp) O(elmm_ib_point, kk) O(elmm_ib_point, coef)
   O(elmm_wm_point, dist) O(elmm_wm_point, z0)
   O(elmm_solids, ib) O(elmm_solids, n_null) O(elmm_solids, null_ijk) O(elmm_solids, n_scalfl) O(elmm_solids, scalfl)
@@ -80,10 +83,12 @@ def test_ctypes_layout_matches_c():
             continue
         cls = {"elmm_config": cfgmod.ElmmConfig, "elmm_stats": cfgmod.ElmmStats,
                "elmm_point_source": cfgmod.ElmmPointSource, "elmm_ib_point": cfgmod.ElmmIBPoint,
-               "elmm_wm_point": cfgmod.ElmmWMPoint, "elmm_solids": cfgmod.ElmmSolids}[s]
+               "elmm_wm_point": cfgmod.ElmmWMPoint, "elmm_solids": cfgmod.ElmmSolids,
+               "elmm_puff": cfgmod.ElmmPuff, "elmm_puff_volume": cfgmod.ElmmPuffVolume}[s]
         assert getattr(cls, f).offset == off, key
     for s, cls in (("elmm_ib_point", cfgmod.ElmmIBPoint), ("elmm_wm_point", cfgmod.ElmmWMPoint),
-                   ("elmm_solids", cfgmod.ElmmSolids)):
+                   ("elmm_solids", cfgmod.ElmmSolids), ("elmm_puff", cfgmod.ElmmPuff),
+                   ("elmm_puff_volume", cfgmod.ElmmPuffVolume)):
         assert lay[s + ".size"] == C.sizeof(cls), s
 
 

@@ -231,3 +231,35 @@ def test_point_source_cell_follows_gridcoords():
     o.set_state(np.zeros(g.shape_u()), np.zeros(g.shape_v()), np.zeros(g.shape_w()))
     o.step(1)
     assert np.count_nonzero(o.get_field(FIELD_SCALAR)) == 0
+
+
+def test_puff_windows_follow_prepare_puffs():
+    """The oracle's PreparePuffs / DoPuffs (src/puffs.f90:30-126) on one
+    scalar: the amount a puff adds per step is dt_fraction * flux * dt (the
+    RK3 weights sum to one), with dt_fraction as the reference computes it,
+    including the restart branch's `time + dt - max(...) / dt` (negative, so
+    nothing is added, on a restart after t = 0), and `clear` empties the
+    scalar at each release."""
+    import numpy as np
+    from gpu_elmm_b200.config import grid_of, make_config
+    from gpu_elmm_b200.workloads import interior
+    from oracle import Oracle
+    cfg = make_config(16, 12, 8, num_scalars=2, sgstype=0, wallmodeltype=0)
+    g = grid_of(cfg)
+    o = Oracle(cfg)
+    z = [np.zeros(s) for s in (g.shape_u(), g.shape_v(), g.shape_w(), g.shape_p())]
+    o.set_state(*z)
+    o.set_puffs([(0.03, 0.5, 0.1, 0.05, 1), (0.0, 1.0, 10.0, 0.07, 0)],
+                [(0, 1, (5, 6, 3), 2.0), (0, 1, (6, 6, 3), 1.0), (1, 2, (10, 7, 4), 3.0)])
+    n = (g.Prnx, g.Prny, g.Prnz)
+    sums = []
+    for _ in range(9):
+        o.step(1)
+        sums.append((interior(o.get_field(16), -2, n).sum(), interior(o.get_field(17), -2, n).sum()))
+    s1 = [round(a, 10) for a, _ in sums]
+    s2 = [round(b, 10) for _, b in sums]
+    # puff 1 (once, 0.07 long from t = 0): fraction 0.02 (restart at t = 0), 1, 1, 0.5, then 0
+    assert s2 == [0.0012, 0.0612, 0.1212, 0.1512, 0.1512, 0.1512, 0.1512, 0.1512, 0.1512]
+    # puff 0: release at t = 0.02 (negative fraction), full steps at 0.04, 0.06, then closed;
+    # cleared at the next release (t = 0.12, the 7th step)
+    assert s1 == [0.0, 0.0, 0.06, 0.12, 0.12, 0.12, 0.0, 0.06, 0.12]
