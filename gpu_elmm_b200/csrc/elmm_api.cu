@@ -979,6 +979,12 @@ struct BatchT {
         launch_scalar_pair(stage);
       }
     }
+    bool puffs = false;
+    for (int d = 0; d < nd; d++) puffs |= hdom[d].npv > 0;
+    if (puffs) {
+      nlaunch++;
+      k_puff_add<T><<<1, kMaxPuffVols, 0, stream>>>(ddom, nd, stage, kBeta[stage - 1]);
+    }
     if (standalone && stage % 3 != 0)
       k_scalar_commit<T><<<std::min(ls[LK_COMMIT].total, 16 * 148), kCommitThreads, 0, stream>>>(
           ddom, ls[LK_COMMIT].l(), stage % 3);

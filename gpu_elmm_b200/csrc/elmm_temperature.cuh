@@ -102,11 +102,9 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
     }
     auto zoff = [&](int kk) { return (long long)(scal_fold(kk, nz, pz) - kk) * plane; };  // fold of plane kk
     // volume sources of this slot in this column, in configuration order
-    unsigned srcm = 0, pvm = 0;
+    unsigned srcm = 0;
     for (int q = 0; q < d.nsrc; q++)
       if (d.src_slot[q] == s && d.src_i[q] == i && d.src_j[q] == j) srcm |= 1u << q;
-    for (int q = 0; q < d.npv; q++)
-      if (d.pv_slot[q] == s && d.pv_i[q] == i && d.pv_j[q] == j) pvm |= 1u << q;
     const T *__restrict__ S = sl.buf[(stage - 1) % 3];
     const T *__restrict__ K = d.TDiff;
     const T *__restrict__ U = d.U;
@@ -165,13 +163,6 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
       if (srcm) {
         for (int q = 0; q < d.nsrc; q++)
           if (((srcm >> q) & 1u) && d.src_k[q] == k) a = a + (T)d.src_q[q];
-      }
-      if (pvm) {  // DoPuffs, after the point sources (src/scalars.f90:368-370)
-        for (int q = 0; q < d.npv; q++)
-          if (((pvm >> q) & 1u) && d.pv_k[q] == k) {
-            const double f = d.puff_state[4 * d.pv_puff[q] + 1];
-            if (f > 0) a = a + (T)(f * d.pv_q[q]);
-          }
       }
       // wall-model point next to a wall-model side: + div * value (the
       // surface flux is zero); div as DivergenceWM with dzPr(k)
@@ -253,11 +244,9 @@ __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SP
 #pragma unroll
     for (int q = 0; q < 5; q++) oy[q] = (scal_fold(j - 2 + q, ny, py) - j) * (int)pitch;
     auto zoff = [&](int kk) { return (long long)(scal_fold(kk, nz, pz) - kk) * plane; };
-    unsigned srcm = 0, pvm = 0;  // volume sources (point sources, puffs) of this slot in this pair's columns
+    unsigned srcm = 0;  // volume sources of this slot in this pair's columns
     for (int q = 0; q < d.nsrc; q++)
       if (d.src_slot[q] == s && (d.src_i[q] == i || d.src_i[q] == i + 1) && d.src_j[q] == j) srcm |= 1u << q;
-    for (int q = 0; q < d.npv; q++)
-      if (d.pv_slot[q] == s && (d.pv_i[q] == i || d.pv_i[q] == i + 1) && d.pv_j[q] == j) pvm |= 1u << q;
     const T *__restrict__ S = sl.buf[(stage - 1) % 3];
     const T *__restrict__ K = d.TDiff;
     const T *__restrict__ U = d.U;
@@ -334,13 +323,6 @@ __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SP
           for (int q = 0; q < d.nsrc; q++)
             if (((srcm >> q) & 1u) && d.src_i[q] == i + c && d.src_k[q] == k) a = a + (T)d.src_q[q];
         }
-        if (pvm) {  // DoPuffs, after the point sources (src/scalars.f90:368-370)
-          for (int q = 0; q < d.npv; q++)
-            if (((pvm >> q) & 1u) && d.pv_i[q] == i + c && d.pv_k[q] == k) {
-              const double f = d.puff_state[4 * d.pv_puff[q] + 1];
-              if (f > 0) a = a + (T)(f * d.pv_q[q]);
-            }
-        }
         if (wmk) {
           const T dzk = (T)d.dzPr[k + 2];
           const T ue = c ? u0.y : u0.x, uw = c ? u0.x : um.y;
@@ -406,6 +388,28 @@ __global__ void k_puff_step(const Dom<T> *__restrict__ doms, int nd) {
     st[4 * p] = last;
   }
   st[4 * kMaxPuffs] = time + dt;
+}
+
+// DoPuffs (src/puffs.f90:86-126) after a scalar stage, one thread per puff
+// volume: the volume's fraction x flux joins the stage tendency of its cell,
+// and beta dt of it the new value (the RK combine is linear in the
+// tendency; in the reference the term comes after the point sources,
+// src/scalars.f90:366-372).  Kept out of the stencil kernels, whose
+// registers are spoken for.
+template <typename T>
+__global__ void k_puff_add(const Dom<T> *__restrict__ doms, int nd, int stage, double beta) {
+  for (int di = 0; di < nd; di++) {
+    const Dom<T> &d = doms[di];
+    const int q = threadIdx.x;
+    if (q >= d.npv) continue;
+    const double f = d.puff_state[4 * d.pv_puff[q] + 1];
+    if (!(f > 0)) continue;
+    const ScalSlot<T> &sl = d.slot[d.pv_slot[q]];
+    const long long c = bidx(d, d.pv_i[q], d.pv_j[q], d.pv_k[q]);
+    const double add = f * d.pv_q[q];
+    atomicAdd(sl.adv + c, (T)add);
+    atomicAdd(sl.buf[stage % 3] + c, (T)(beta * d.dt * add));
+  }
 }
 
 // The `clear` of a releasing puff: its scalars are set to zero, ghosts
