@@ -294,6 +294,7 @@ struct BatchT {
   // of the next on the side stream
   double *dstage2 = nullptr;
   cudaEvent_t ev_stage[2][2] = {};  // [buffer][0: filled on its producer, 1: drained by its consumer]
+  cudaEvent_t ev_pr = nullptr;      // the host copy of Pr into its image has landed
   std::vector<double *> pr_image;  // per domain: last host Pr image (device)
   int *dbad = nullptr;
   cudaGraphExec_t step_exec = nullptr;
@@ -376,6 +377,8 @@ struct BatchT {
     for (auto &pair : ev_stage)
       for (auto &e : pair)
         if (e) { cudaEventDestroy(e); e = nullptr; }
+    if (ev_pr) cudaEventDestroy(ev_pr);
+    ev_pr = nullptr;
   }
   // the second staging buffer and its events, or false (views, serving
   // requests and batches keep one buffer and copy field by field)
@@ -388,6 +391,7 @@ struct BatchT {
       for (auto &pair : ev_stage)
         for (auto &e : pair)
           if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return false;
+      if (cudaEventCreateWithFlags(&ev_pr, cudaEventDisableTiming) != cudaSuccess) return false;
       for (int b = 0; b < 2; b++) {  // both buffers start free
         if (cudaEventRecord(ev_stage[b][1], stream) != cudaSuccess) return false;
         if (cudaEventRecord(ev_stage[b][0], side) != cudaSuccess) return false;
@@ -1688,6 +1692,108 @@ struct BatchT {
     return HostBox{-1, h.nx + 4, h.ny + 4, h.nz + 4};
   }
 
+  // The state and the temperature in one pipelined pass (elmm_march_host):
+  // every host copy runs on the side stream into a staging buffer (Pr into
+  // its own image) while the stream unpacks the field before it.  Needs the
+  // two staging buffers; otherwise the field-by-field calls.
+  int upload_all(int d, const double *U, const double *V, const double *W, const double *Pr, const double *Th) {
+    if (!two_stages() || !ev_pr) {
+      int r = upload(d, U, V, W, Pr);
+      if (r || !Th) return r;
+      return upload_temperature(d, Th);
+    }
+    if (!U || !V || !W) return fail(ELMM_ERR_INVALID_ARG, "NULL velocity array");
+    if (Th && !hdom[d].buoy) return fail(ELMM_ERR_INVALID_ARG, "no temperature field (enable_buoyancy is 0)");
+    CU(cudaSetDevice(device));
+    if (frame_pending) CU(cudaStreamWaitEvent(stream, ev_packed, 0));
+    const Dom<T> &h = hdom[d];
+    CU(cudaMemsetAsync(dbad, 0, sizeof(int), stream));
+    const double *src[4] = {U, V, W, Th};
+    int b = 0;
+    for (int f = 0; f < 5; f++) {
+      if (f == 3) {  // Pr into its own image, no staging buffer
+        HostBox hp = hbox_p(d);
+        size_t np = (size_t)hp.n0 * hp.n1 * hp.n2;
+        if (Pr) {
+          CU(cudaMemcpyAsync(pr_image[d], Pr, np * sizeof(double), cudaMemcpyHostToDevice, side));
+          CU(cudaEventRecord(ev_pr, side));
+          CU(cudaStreamWaitEvent(stream, ev_pr, 0));
+          k_unpack<T><<<kPackBlocks, 256, 0, stream>>>(ddom + d, h.P, pr_image[d], hp, h.nx, h.ny, h.nz, dbad);
+        } else {
+          CU(cudaMemsetAsync(pr_image[d], 0, np * sizeof(double), stream));
+          CU(cudaMemsetAsync(h.P, 0, (size_t)h.plane * (h.nz + 2) * sizeof(T), stream));
+        }
+        continue;
+      }
+      const int c = f < 3 ? f : 3;
+      if (c == 3 && !Th) continue;
+      const size_t n = c < 3 ? (size_t)hbox_vel(d, c).n0 * hbox_vel(d, c).n1 * hbox_vel(d, c).n2
+                             : (size_t)(h.nx + 6) * (h.ny + 6) * (h.nz + 6);
+      double *stg = b ? dstage2 : dstage;
+      CU(cudaStreamWaitEvent(side, ev_stage[b][1], 0));
+      CU(cudaMemcpyAsync(stg, src[c], n * sizeof(double), cudaMemcpyHostToDevice, side));
+      CU(cudaEventRecord(ev_stage[b][0], side));
+      CU(cudaStreamWaitEvent(stream, ev_stage[b][0], 0));
+      if (c < 3) {
+        HostBox hb = hbox_vel(d, c);
+        k_unpack<T><<<kPackBlocks, 256, 0, stream>>>(ddom + d, c == 0 ? h.U : c == 1 ? h.V : h.W, stg, hb,
+                                                     h.ext[c][0], h.ext[c][1], h.ext[c][2], dbad);
+        k_halo_vel<T><<<256, 256, 0, stream>>>(ddom + d, c);
+      } else {
+        k_unpack_scalar<T><<<kPackBlocks, 256, 0, stream>>>(ddom + d, 0, stg, dbad);
+      }
+      CU(cudaEventRecord(ev_stage[b][1], stream));
+      b ^= 1;
+    }
+    k_halo_p<T><<<256, 256, 0, stream>>>(ddom + d);
+    CU(cudaMemsetAsync(hdom[d].prm, 0, sizeof(double), stream));
+    int bad = 0;
+    CU(cudaMemcpyAsync(&bad, dbad, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    CU(cudaStreamSynchronize(stream));
+    CU(cudaStreamSynchronize(side));
+    CU(cudaGetLastError());
+    if (bad) return fail(ELMM_ERR_NAN, "non-finite value in the uploaded state");
+    return ELMM_OK;
+  }
+  // the state and the temperature back to the host, the pack of one field
+  // overlapping the host copy of the one before
+  int download_all(int d, double *U, double *V, double *W, double *Pr, double *Th) {
+    if (Th && !hdom[d].buoy) return fail(ELMM_ERR_INVALID_ARG, "no temperature field (enable_buoyancy is 0)");
+    if (!two_stages()) {
+      int r = download(d, U, V, W, Pr);
+      if (r || !Th) return r;
+      return download_field(d, ELMM_FIELD_TEMPERATURE, Th);
+    }
+    CU(cudaSetDevice(device));
+    double *dst[5] = {U, V, W, Pr, Th};
+    const int fid[5] = {ELMM_FIELD_U, ELMM_FIELD_V, ELMM_FIELD_W, ELMM_FIELD_PR, ELMM_FIELD_TEMPERATURE};
+    int b = 0;
+    for (int f = 0; f < 5; f++) {
+      if (!dst[f]) continue;
+      double *stg = b ? dstage2 : dstage;
+      CU(cudaStreamWaitEvent(stream, ev_stage[b][1], 0));
+      size_t n = pack(d, fid[f], stg, stream);
+      CU(cudaEventRecord(ev_stage[b][0], stream));
+      CU(cudaStreamWaitEvent(side, ev_stage[b][0], 0));
+      CU(cudaMemcpyAsync(dst[f], stg, n * sizeof(double), cudaMemcpyDeviceToHost, side));
+      CU(cudaEventRecord(ev_stage[b][1], side));
+      b ^= 1;
+    }
+    CU(cudaStreamSynchronize(side));
+    CU(cudaStreamSynchronize(stream));
+    CU(cudaGetLastError());
+    return ELMM_OK;
+  }
+  // TMarchRK3 on host arrays: upload, nsteps steps, download
+  int march_host(double *U, double *V, double *W, double *Pr, double *Th, int nsteps, elmm_stats *st) {
+    if (nd != 1) return fail(ELMM_ERR_INVALID_ARG, "host-array steps are per single-domain handle");
+    int r = upload_all(0, U, V, W, Pr, Th);
+    if (r) return r;
+    r = step(nsteps, st);
+    if (r) return r;
+    return download_all(0, U, V, W, Pr, Th);
+  }
+
   int upload(int d, const double *U, const double *V, const double *W, const double *Pr) {
     if (d < 0 || d >= nd) return fail(ELMM_ERR_INVALID_ARG, "domain index");
     if (!U || !V || !W) return fail(ELMM_ERR_INVALID_ARG, "NULL velocity array");
@@ -2117,6 +2223,13 @@ int elmm_step(elmm_handle *h, int32_t nsteps, elmm_stats *st) {
   if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
   if (nsteps < 0) return fail(ELMM_ERR_INVALID_ARG, "nsteps < 0");
   return DISPATCH(h->b, step(nsteps, st));
+}
+
+int elmm_march_host(elmm_handle *h, double *U, double *V, double *W, double *Pr, double *Temperature,
+                    int32_t nsteps, elmm_stats *stats) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  if (nsteps < 0) return fail(ELMM_ERR_INVALID_ARG, "nsteps < 0");
+  return DISPATCH(h->b, march_host(U, V, W, Pr, Temperature, nsteps, stats));
 }
 
 int elmm_set_puffs(elmm_handle *h, const elmm_puff *puffs, int32_t npuffs, const elmm_puff_volume *volumes,

@@ -51,6 +51,7 @@ def lib():
         L.elmm_upload_scalar.argtypes = [P, C.c_int32, _dp]
         L.elmm_set_solids.argtypes = [P, P]
         L.elmm_set_puffs.argtypes = [P, P, C.c_int32, P, C.c_int32]
+        L.elmm_march_host.argtypes = [P, _dp, _dp, _dp, _dp, _dp, C.c_int32, C.POINTER(ElmmStats)]
         L.elmm_download_scalar_slices.argtypes = [P, C.c_int32, _dp, _dp]
         L.elmm_reset_scalar_averages.argtypes = [P]
         L.elmm_download_field.argtypes = [P, C.c_int32, _dp]
@@ -137,6 +138,14 @@ class Domain:
 
     def temperature(self):
         return self.field(12)
+
+    def march_host(self, U, V, W, Pr, T=None, n=1) -> ElmmStats:
+        """TMarchRK3 on host arrays: upload, n steps, write the state back into
+        the same arrays (elmm_march_host)."""
+        st = ElmmStats()
+        check(lib().elmm_march_host(self.h, ptr(U), ptr(V), ptr(W), ptr(Pr), ptr(T), n, C.byref(st)),
+              "elmm_march_host")
+        return st
 
     def set_puffs(self, puffs, volumes):
         """Puff sources: puffs as (start, end, period, duration, clear),

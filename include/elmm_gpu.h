@@ -329,6 +329,18 @@ int elmm_project(elmm_handle *h, double coef, elmm_stats *stats);
 /* nsteps calls of TMarchRK3 (src/tsteps.f90:24-243) on the resident state. */
 int elmm_step(elmm_handle *h, int32_t nsteps, elmm_stats *stats);
 
+/* TMarchRK3(U,V,W,Pr,Temperature,...) on host arrays (src/tsteps.f90:24-243,
+ * called from src/main.f90:112), for a host that keeps the state in its own
+ * arrays between steps: uploads U, V, W, Pr (and Temperature when
+ * enable_buoyancy is set; NULL otherwise), runs nsteps steps and writes the
+ * state back, ghosts filled as BoundUVW / Bound_Pr leave them.  The host
+ * copies of the fields overlap the device-side unpacking and packing of the
+ * neighbouring fields; page-locked host arrays give the full copy bandwidth.
+ * Equivalent to elmm_upload_state + elmm_upload_temperature + elmm_step +
+ * elmm_download_state + elmm_download_field(ELMM_FIELD_TEMPERATURE). */
+int elmm_march_host(elmm_handle *h, double *U, double *V, double *W, double *Pr, double *Temperature,
+                    int32_t nsteps, elmm_stats *stats);
+
 /* One RK3 stage up to a stop point, for operator-level checks:
  *   stop = 1: after SubgridStresses (Viscosity, wall-model fluxes)
  *   stop = 2: after Convection + OtherTerms + BoundUVW (U2, Ustar)

@@ -675,3 +675,35 @@ def test_puffs_follow_the_oracle(precision):
         assert rel(a, b) < (1e-12 if precision == 0 else 1e-5)
     d.set_puffs([], [])
     d.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_march_host_equals_the_separate_calls(precision):
+    """elmm_march_host (upload, steps and download on host arrays, the copies
+    pipelined over two staging buffers) gives bit for bit what the separate
+    upload / step / download calls give, two calls in a row, with the
+    temperature."""
+    from gpu_elmm_b200.config import FIELD_TEMPERATURE
+    from gpu_elmm_b200.workloads import temperature_state
+    n = (64, 48, 32)
+    cfg = make_config(*n, buoyancy=True, precision=precision)
+    g = grid_of(cfg)
+    st = list(log_profile_state(g, seed=4))
+    T0 = temperature_state(g, seed=4)
+    a, b = L.Domain(cfg), L.Domain(cfg)
+    for d in (a, b):
+        d.upload(*st)
+        d.upload_temperature(T0)
+        d.project(1.0)
+    arrs = [x.copy() for x in a.download()] + [a.field(FIELD_TEMPERATURE)]
+    ref = [x.copy() for x in arrs]
+    for it in range(2):
+        b.upload(*ref[:4])
+        b.upload_temperature(ref[4])
+        b.step(1 + it)
+        ref = [x.copy() for x in b.download()] + [b.field(FIELD_TEMPERATURE)]
+        a.march_host(*arrs, n=1 + it)
+        for x, y, name in zip(arrs, ref, ("U", "V", "W", "Pr", "T")):
+            assert np.array_equal(x, y), (it, name)
+    a.close()
+    b.close()
