@@ -1,4 +1,5 @@
-"""The Python examples of INTEGRATION.md run as written (on a B200)."""
+"""The Python usage examples of the integration guide (section 4) run as
+written, on a B200."""
 import re
 
 import numpy as np
@@ -9,12 +10,13 @@ from conftest import ROOT
 
 @pytest.mark.gpu
 def test_integration_python_examples_run():
-    text = open(f"{ROOT}/INTEGRATION.md").read()
+    guide = f"{ROOT}/INTEGRATION.md"
+    text = open(guide).read()
     sec = text[text.index("## 4. Python"):text.index("## 5.")]
     code = re.findall(r"```python\n(.*?)```", sec, flags=re.S)
     assert code
     env = {}
-    exec(compile(code[0], "INTEGRATION.md", "exec"), env)
+    exec(compile(code[0], guide, "exec"), env)
     assert env["stats"].max_div < 1e-5 and env["stats"].nan_detected == 0
     assert np.isfinite(env["U"]).all()
     c = env["concentration"]
