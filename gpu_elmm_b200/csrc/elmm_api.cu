@@ -2361,6 +2361,24 @@ int elmm_batch_tuning(const elmm_batch *b, int32_t out[2]) {
   return ELMM_OK;
 }
 
+static int batch_domain_ok(const elmm_batch *b, int32_t d) {
+  const int nd = b->precision == ELMM_PREC_MIXED ? b->b32->nd : b->b64->nd;
+  return d >= 0 && d < nd;
+}
+
+int elmm_batch_set_solids(elmm_batch *b, int32_t d, const elmm_solids *s) {
+  if (!b) return fail(ELMM_ERR_INVALID_ARG, "NULL batch");
+  if (!batch_domain_ok(b, d)) return fail(ELMM_ERR_INVALID_ARG, "domain index");
+  return DISPATCH(*b, set_solids(d, s));
+}
+
+int elmm_batch_set_puffs(elmm_batch *b, int32_t d, const elmm_puff *puffs, int32_t npuffs,
+                         const elmm_puff_volume *volumes, int32_t nvolumes) {
+  if (!b) return fail(ELMM_ERR_INVALID_ARG, "NULL batch");
+  if (!batch_domain_ok(b, d)) return fail(ELMM_ERR_INVALID_ARG, "domain index");
+  return DISPATCH(*b, set_puffs(d, puffs, npuffs, volumes, nvolumes));
+}
+
 int elmm_batch_upload_scalar(elmm_batch *b, int32_t d, int32_t sc, const double *S) {
   if (!b) return fail(ELMM_ERR_INVALID_ARG, "NULL batch");
   return DISPATCH(*b, upload_scalar(d, sc, S));

@@ -51,6 +51,8 @@ def lib():
         L.elmm_upload_scalar.argtypes = [P, C.c_int32, _dp]
         L.elmm_set_solids.argtypes = [P, P]
         L.elmm_set_puffs.argtypes = [P, P, C.c_int32, P, C.c_int32]
+        L.elmm_batch_set_solids.argtypes = [P, C.c_int32, P]
+        L.elmm_batch_set_puffs.argtypes = [P, C.c_int32, P, C.c_int32, P, C.c_int32]
         L.elmm_march_host.argtypes = [P, _dp, _dp, _dp, _dp, _dp, C.c_int32, C.POINTER(ElmmStats)]
         L.elmm_download_scalar_slices.argtypes = [P, C.c_int32, _dp, _dp]
         L.elmm_reset_scalar_averages.argtypes = [P]
@@ -264,6 +266,20 @@ class Batch:
         st = ElmmStats()
         check(lib().elmm_batch_step(self.h, n, C.byref(st)), "elmm_batch_step")
         return st
+
+    def set_solids(self, d, solids):
+        """Solid bodies of domain d (gpu_elmm_b200.solids.Solids, or None)."""
+        st = None if solids is None else solids.struct()
+        check(lib().elmm_batch_set_solids(self.h, d, None if st is None else C.cast(C.byref(st), C.c_void_p)),
+              "elmm_batch_set_solids")
+
+    def set_puffs(self, d, puffs, volumes):
+        """Puff sources of domain d, as for Domain.set_puffs."""
+        from .config import make_puffs
+        P, n_p, V, n_v = make_puffs(puffs, volumes)
+        check(lib().elmm_batch_set_puffs(self.h, d, C.cast(P, C.c_void_p), n_p, C.cast(V, C.c_void_p), n_v),
+              "elmm_batch_set_puffs")
+        self.__dict__.setdefault("_puffs", {})[d] = (P, V)
 
     def tuning(self):
         """Tile shapes chosen by the autotuner at the first step."""

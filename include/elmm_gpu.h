@@ -434,6 +434,12 @@ int elmm_batch_project(elmm_batch *b, double coef);
  * tile of the FP32 scalar stage, out[1]: spectral columns of a tile of the z
  * solve); the defaults before it. */
 int elmm_batch_tuning(const elmm_batch *b, int32_t out[2]);
+
+/* elmm_set_solids and elmm_set_puffs for domain d of a batch: each domain
+ * keeps its own bodies and puffs, and computes the same values as alone. */
+int elmm_batch_set_solids(elmm_batch *b, int32_t d, const elmm_solids *s);
+int elmm_batch_set_puffs(elmm_batch *b, int32_t d, const elmm_puff *puffs, int32_t npuffs,
+                         const elmm_puff_volume *volumes, int32_t nvolumes);
 /* elmm_profile_stage for a whole batch */
 int elmm_batch_profile_stage(elmm_batch *b, int32_t stage, int32_t reps, double *ms);
 int elmm_batch_step(elmm_batch *b, int32_t nsteps, elmm_stats *stats);
