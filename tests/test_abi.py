@@ -133,3 +133,15 @@ def test_no_cpu_fallback_without_device():
     with pytest.raises(L.ElmmError) as e:
         L.Domain(cfgmod.make_config(32, 24, 16))
     assert e.value.code == 4  # ELMM_ERR_CUDA
+
+
+def test_new_entry_points_refuse_null_handles_without_gpu():
+    """The solid-body, puff and host-array entry points check their handle
+    before touching a device: NULL comes back as ELMM_ERR_INVALID_ARG (6)."""
+    lib = L.lib()
+    assert lib.elmm_set_solids(None, None) == 6
+    assert lib.elmm_set_puffs(None, None, 0, None, 0) == 6
+    assert lib.elmm_march_host(None, None, None, None, None, None, 1, None) == 6
+    assert lib.elmm_batch_set_solids(None, 0, None) == 6
+    assert lib.elmm_batch_set_puffs(None, 0, None, 0, None, 0) == 6
+    assert b"NULL" in lib.elmm_last_error()
