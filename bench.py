@@ -46,8 +46,8 @@ DATA = ("synthetic: seeded log profile u*=0.3 + U(-0.1,0.1) perturbations on u,v
 # words moved per cell by the momentum kernel in stages 2 and 3: reads U,V,W,nu,Pr,theta,Ustar x3;
 # writes Ustar x3, U2 x3 (the per-cell figure of the momentum phase)
 MOMENTUM_WORDS = 15
-# oracle steps timed by the reference arm (a bounded sample of the workload)
-REF_STEPS = 10
+# timed oracle steps of the main line's cpu_baseline (a bounded sample: ~10 s on 16 cores)
+CPU_STEPS = 5
 # long run of the single domain on both paths (errors after 1, 10 and this many steps)
 LONG_STEPS = 1000
 # the array of cubes: steps run on both paths (device time over steps 10..CUBES_STEPS)
@@ -174,57 +174,58 @@ def rel(a, b):
     return float(np.abs(a - b).max()) / (s if s > 0 else 1.0)
 
 
-def cpu_baseline(steps=1):
-    """The FP64 oracle on all host threads, a bounded sample of the workload."""
+def _native_oracle():
+    """The oracle built with -O3 -march=native -fopenmp on this host (the
+    timed CPU baseline; the parity build of the tests keeps FMA contraction
+    off), with every host thread."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
-    orc.build()
+    orc.build(native=True)
     threads = os.cpu_count() or 1
-    orc.set_threads(threads)
+    orc.set_threads(threads, native=True)
     cfg = make_config(*N, buoyancy=True)
     g = grid_of(cfg)
-    o = orc.Oracle(cfg)
+    o = orc.Oracle(cfg, native=True)
     o.set_state(*log_profile_state(g, seed=0))
     o.set_field(FIELD_TEMPERATURE, temperature_state(g, seed=0))
     o.project(1.0)
+    return o, g, threads
+
+
+def cpu_baseline(steps=CPU_STEPS):
+    """The FP64 oracle on all host threads, a bounded sample of the workload:
+    one untimed step, then `steps` timed RK3 steps of the full domain."""
+    o, g, threads = _native_oracle()
+    o.step(1)
     t0 = time.perf_counter()
     o.step(steps)
     dt = time.perf_counter() - t0
     return {"value": g.cells() * steps / dt, "unit": "cell-steps/s", "cores": threads, "kind": "port",
-            "sample": f"{steps} RK3 step(s) of the 256x256x128 workload in FP64 (oracle/elmm_oracle.cpp, "
-                      f"OpenMP, {threads} threads)", "seconds": dt}
+            "sample": f"{steps} RK3 steps of the 256x256x128 workload in FP64 after 1 untimed step "
+                      f"(oracle/elmm_oracle.cpp built -O3 -march=native -fopenmp, {threads} threads)",
+            "seconds": dt}
 
 
 def run_reference(args, ws, rank):
+    """The CPU restatement of the reference on this host's cores (the Fortran
+    reference cannot be built here): W untimed and exactly K timed RK3 steps
+    of the full 256x256x128 domain, on rank 0 only."""
     if rank != 0:
         return 0
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as orc
-    orc.build()
-    threads = os.cpu_count() or 1
-    orc.set_threads(threads)
-    cfg = make_config(*N, buoyancy=True)
-    g = grid_of(cfg)
-    o = orc.Oracle(cfg)
-    o.set_state(*log_profile_state(g, seed=0))
-    o.set_field(FIELD_TEMPERATURE, temperature_state(g, seed=0))
-    o.project(1.0)
-    # a bounded sample: one RK3 step of the full domain takes ~1.5 s on 16
-    # cores, so at most REF_STEPS steps are timed after one warm-up step
-    timed = min(args.steps, REF_STEPS)
-    o.step(1)
+    o, g, threads = _native_oracle()
+    o.step(args.warmup)
     t0 = time.perf_counter()
-    o.step(timed)
+    o.step(args.steps)
     dt = time.perf_counter() - t0
-    v = g.cells() * timed / dt
+    v = g.cells() * args.steps / dt
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "cell-steps/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / timed * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": DATA, "config": {"workload": WORKLOAD, "cells": g.cells(), "precision": "fp64"},
             "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": threads, "kind": "port",
-                             "sample": f"{timed} RK3 steps of the 256x256x128 workload after 1 warm-up step (the "
-                                       f"Fortran reference cannot be built here; its C++ FP64 restatement in oracle/ "
-                                       f"is timed)"},
+                             "sample": f"{args.steps} RK3 steps of the 256x256x128 workload after {args.warmup} "
+                                       f"untimed steps (the Fortran reference cannot be built here; its C++ FP64 "
+                                       f"restatement in oracle/, built -O3 -march=native -fopenmp, is timed)"},
             "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -308,12 +309,16 @@ def run_ours(args, ws, rank, local):
     alg_bytes = MOMENTUM_WORDS * 4 * cells
     peak, peak_kind = peaks()
     achieved = alg_bytes / (mom_ms / 1e3) / 1e9
-    traffic = None
+    # DRAM bytes of one launch are not measurable inside a timed run; they
+    # come from the committed ncu capture of this kernel on this workload
+    traffic, traffic_source = None, None
     tp = os.path.join(ROOT, "profiles", "k_momentum_256x256x128_mixed.md")
     if os.path.exists(tp):
         for line in open(tp):
             if line.startswith("dram_bytes_per_launch:"):
                 traffic = float(line.split(":")[1])
+                traffic_source = ("stored ncu capture (dram__bytes_read.sum + dram__bytes_write.sum of one launch), "
+                                  "profiles/k_momentum_256x256x128_mixed.md")
 
     # end to end through the C-ABI with pinned host buffers: one
     # elmm_march_host call per step (H2D of the state and temperature, one
@@ -340,7 +345,7 @@ def run_ours(args, ws, rank, local):
     batched = batched_leg(args, ws, rank, local)
     serving = serving_leg(args, ws, rank, local)
 
-    cpu = cpu_baseline(1) if (rank == 0 and ws == 1) else None
+    cpu = cpu_baseline() if (rank == 0 and ws == 1) else None
     barrier(ws)
     if rank == 0:
         line = {
@@ -357,7 +362,8 @@ def run_ours(args, ws, rank, local):
             "latency_ms": {"p50": p50, "p99": p99, "what": "device time of one RK3 step"},
             "roofline": {"bound": "hbm", "kernel": "k_momentum (stage 2)", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": traffic, "algorithmic_bytes": alg_bytes, "ms": mom_ms},
+                         "traffic": traffic, "traffic_source": traffic_source, "algorithmic_bytes": alg_bytes,
+                         "ms": mom_ms},
             "kernel_ms_stage2": kt,
             "e2e": {"value": e2e, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
             "gpu_launches": sm.kernels,
@@ -557,7 +563,7 @@ def serving_leg(args, ws, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     args = ap.parse_args()

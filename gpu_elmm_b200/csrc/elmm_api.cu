@@ -2117,6 +2117,9 @@ static int poisson_exec(BatchT<T> &B, double *Phi, const double *RHS) {
   CU(cudaMemcpyAsync(Phi, B.dstage, np * sizeof(double), cudaMemcpyDeviceToHost, B.stream));
   CU(cudaStreamSynchronize(B.stream));
   CU(cudaGetLastError());
+  int bad = 0;
+  CU(cudaMemcpy(&bad, B.dbad, sizeof(int), cudaMemcpyDeviceToHost));
+  if (bad) return fail(ELMM_ERR_NAN, std::to_string(bad) + " non-finite right-hand-side value(s)");
   return ELMM_OK;
 }
 
@@ -2559,17 +2562,68 @@ static __global__ void k_noalloc_setup(Dom<double> h, PoisPlan pl, NoAllocLayout
 }
 
 static std::mutex noalloc_mu;
-static unsigned char *noalloc_base[64];  // device address of noalloc_scratch, per device
-static int noalloc_optin[64], noalloc_nsm[64];
+// per device: the context the set-up ran in, the device address of
+// noalloc_scratch in that context, and the kernels' limits
+struct NoAllocDev {
+  unsigned long long ctx_id = 0;  // 0: no set-up yet
+  unsigned char *base = nullptr;
+  int optin = 0, nsm = 0;
+};
+static NoAllocDev noalloc_dev[64];
 
-// Once per device, with that device current: the device address of the
-// scratch array (host code only holds a stand-in for it) and the kernels'
-// shared-memory limit.  Later calls only read what this stored.
-static int noalloc_setup(int device) {
+// The unique id of the current context (cuCtxGetCurrent + cuCtxGetId from
+// the driver the runtime already loaded, as for cuTensorMapEncodeTiled), or
+// 0 if it cannot be had.  A context that was destroyed and created again
+// (cudaDeviceReset, a torn-down primary context) has a new id, and the
+// module holding noalloc_scratch may then sit at a new address.
+static unsigned long long current_ctx_id() {
+  typedef CUresult (*GetCurrent)(CUcontext *);
+  typedef CUresult (*GetId)(CUcontext, unsigned long long *);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static bool looked = false;
+  if (!looked) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = (GetCurrent)p;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = (GetId)p;
+    looked = true;
+  }
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS)
+    return 0;
+  return id;
+}
+
+// With `device` current: the device address of the scratch array (host code
+// only holds a stand-in for it) and the kernels' shared-memory limit, once
+// per context.  A call in a context other than the one of the stored set-up
+// (or when the context id is unknown) repeats the set-up, so a stale address
+// of an earlier context is never used.
+static int noalloc_setup(int device, NoAllocDev *out) {
   std::lock_guard<std::mutex> lock(noalloc_mu);
-  if (noalloc_base[device]) return ELMM_OK;
+  // the caller's cudaSetDevice made the device's primary context current
+  // (CUDA 12 creates it there), so it has an id
+  const unsigned long long id = current_ctx_id();
+  NoAllocDev &nd = noalloc_dev[device];
+  if (id != 0 && nd.ctx_id == id) {
+    *out = nd;
+    return ELMM_OK;
+  }
   unsigned char *ptr = nullptr;
-  CU(cudaGetSymbolAddress((void **)&ptr, noalloc_scratch));
+  cudaError_t e = cudaGetSymbolAddress((void **)&ptr, noalloc_scratch);
+  if (e == cudaErrorMemoryAllocation)
+    return fail(ELMM_ERR_OOM, "elmm_poisson_solve_noalloc: loading the library's device image, which holds the fixed " +
+                                  std::to_string((size_t)ELMM_NOALLOC_SCRATCH_BYTES) +
+                                  "-byte scratch array, ran out of device memory (make the first call on a device "
+                                  "before the host's memory pool reserves the GPU's memory)");
+  if (e != cudaSuccess)
+    return fail(ELMM_ERR_CUDA, std::string("cudaGetSymbolAddress(noalloc_scratch): ") + cudaGetErrorString(e));
   int optin = 0, nsm = 0;
   CU(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
   CU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
@@ -2577,9 +2631,11 @@ static int noalloc_setup(int device) {
   CU(cudaFuncSetAttribute(k_fftx_inv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
   CU(cudaFuncSetAttribute(k_ffty<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
   CU(cudaFuncSetAttribute(k_tri<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-  noalloc_optin[device] = optin;
-  noalloc_nsm[device] = nsm;
-  noalloc_base[device] = ptr;
+  nd.base = ptr;
+  nd.optin = optin;
+  nd.nsm = nsm;
+  nd.ctx_id = id;  // 0 (id unknown) keeps the next call doing the set-up again
+  *out = nd;
   return ELMM_OK;
 }
 
@@ -2619,12 +2675,13 @@ extern "C" int elmm_poisson_solve_noalloc(const int32_t n[3], const double L[3],
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev || device >= 64)
     return fail(ELMM_ERR_INVALID_ARG, "no CUDA device " + std::to_string(device));
   CU(cudaSetDevice(device));
-  if ((r = noalloc_setup(device))) return r;
-  unsigned char *base = noalloc_base[device];
+  NoAllocDev nd;
+  if ((r = noalloc_setup(device, &nd))) return r;
+  unsigned char *base = nd.base;
   const size_t smem_x = sizeof(double2) * 2 * (kRowsX / 2) * nx, smem_y = sizeof(double2) * 2 * TyOf<double>::v * ny;
   const int zper = bcs[ELMM_BO] == ELMM_BC_PERIODIC;
   const size_t smem_tri = sizeof(double) * kTriThreads * nz * (zper ? 2 : 1);
-  const size_t optin = (size_t)noalloc_optin[device];
+  const size_t optin = (size_t)nd.optin;
   if (smem_x > optin || smem_y > optin || smem_tri > optin)
     return fail(ELMM_ERR_INVALID_CONFIG, "grid too large for the shared-memory transforms");
 
@@ -2654,7 +2711,7 @@ extern "C" int elmm_poisson_solve_noalloc(const int32_t n[3], const double L[3],
   const PoisPlan *dplan = reinterpret_cast<const PoisPlan *>(base + lay.plan);
   const int *starts = reinterpret_cast<const int *>(base + lay.starts);
   int *bad = reinterpret_cast<int *>(base + lay.bad);
-  const int nsm = noalloc_nsm[device];
+  const int nsm = nd.nsm;
   auto blocks = [&](const void *f, int threads, size_t smem, int total) {
     int b = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, threads, smem) != cudaSuccess || b < 1) b = 1;
@@ -2666,6 +2723,9 @@ extern "C" int elmm_poisson_solve_noalloc(const int32_t n[3], const double L[3],
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int gset = std::max(1, std::min(64, (std::max(std::max(nx, ny), nz + 2) + 255) / 256));
   k_noalloc_setup<<<gset, 256, 0, st>>>(h, pl, lay, base);
+  // `bad` counts non-finite right-hand-side values; this asynchronous entry
+  // point never reads it back (it would have to synchronise), so non-finite
+  // input is not reported, as the header states
   k_unpack<double><<<256, 256, 0, st>>>(ddom, h.Phi, RHS, HostBox{0, nx + 2, ny + 2, nz + 2}, nx, ny, nz, bad);
   k_fftx_fwd<double><<<blocks((const void *)k_fftx_fwd<double>, kFFTThreads, smem_x, rows.total), kFFTThreads, smem_x,
                        st>>>(ddom, rows, dplan, 1.0, 0, 1, 0);

@@ -375,7 +375,8 @@ int elmm_poisson_solver_nonuniform_z_new(elmm_poisson **out, const int32_t n[3],
                                          const double *zW, const int32_t bcs[6],
                                          int32_t precision, int32_t device);
 /* Phi(-1:nx+2,-1:ny+2,-1:nz+2) out (interior written, ghosts untouched),
- * RHS(0:nx+1,0:ny+1,0:nz+1) in; host arrays. */
+ * RHS(0:nx+1,0:ny+1,0:nz+1) in; host arrays.  Returns ELMM_ERR_NAN if an
+ * interior RHS value is not finite (Phi then holds no solution). */
 int elmm_poisson_solver_execute(elmm_poisson *s, double *Phi, const double *RHS);
 int elmm_poisson_solver_finalize(elmm_poisson *s);
 
@@ -405,7 +406,13 @@ int elmm_poisson_solver_finalize(elmm_poisson *s);
  *
  * The first call on a device does a one-time set-up (it looks up the
  * array's device address and raises the kernels' shared-memory limit), so
- * make that first call before any stream capture.  Every call shares the
+ * make that first call before any stream capture.  The device image that
+ * holds the array may itself be loaded only then (lazy module loading), so
+ * also make that first call before the host's memory pool reserves the
+ * GPU's memory; if the image cannot be loaded the call returns ELMM_ERR_OOM
+ * with a message naming the fixed array.  The set-up is tied to the CUDA
+ * context: after the context is destroyed and created again (for example
+ * by cudaDeviceReset) the next call repeats it.  Every call shares the
  * one array: calls whose work overlaps on the GPU (two streams, or two host
  * threads on one device) race and give wrong results, so order them on one
  * stream or with events.

@@ -14,23 +14,32 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libelmm_oracle.so")
+# the timed CPU baseline: the same source built with -O3 -march=native for
+# the host that runs it (oracle/Makefile, target `native`)
+NATIVE_PATH = os.path.join(HERE, "_build", "libelmm_oracle_native.so")
 
-_lib = None
+_libs = {}
 
 
-def build(force: bool = False) -> str:
+def build(force: bool = False, native: bool = False) -> str:
+    """Builds the parity library, or with native=True the timed baseline
+    (make rebuilds it whenever the host CPU differs from the one it was
+    built for)."""
+    if native:
+        subprocess.run(["make", "-s", "-C", HERE, "native"], check=True)
+        return NATIVE_PATH
     if force or not os.path.exists(LIB_PATH) or (
             os.path.getmtime(LIB_PATH) < os.path.getmtime(os.path.join(HERE, "elmm_oracle.cpp"))):
         subprocess.run(["make", "-s", "-C", HERE], check=True)
     return LIB_PATH
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(LIB_PATH):
-            build()
-        L = C.CDLL(LIB_PATH)
+def lib(native: bool = False):
+    if native not in _libs:
+        path = NATIVE_PATH if native else LIB_PATH
+        if not os.path.exists(path):
+            build(native=native)
+        L = C.CDLL(path)
         P = C.c_void_p
         dp = C.POINTER(C.c_double)
         L.orc_create.restype = P
@@ -49,8 +58,8 @@ def lib():
         L.orc_scalar_slices.argtypes = [P, C.c_int, dp, dp]
         L.orc_set_solids.argtypes = [P, P]
         L.orc_set_puffs.argtypes = [P, P, C.c_int, P, C.c_int]
-        _lib = L
-    return _lib
+        _libs[native] = L
+    return _libs[native]
 
 
 def _ptr(a: np.ndarray):
@@ -58,26 +67,28 @@ def _ptr(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
-def set_threads(n: int) -> int:
-    return lib().orc_num_threads(n)
+def set_threads(n: int, native: bool = False) -> int:
+    return lib(native).orc_num_threads(n)
 
 
 class Oracle:
     """One domain of the CPU restatement; field arrays use the host layout of
     gpu_elmm_b200.workloads (Fortran bounds, x contiguous)."""
 
-    def __init__(self, cfg):
+    def __init__(self, cfg, native: bool = False):
+        """native=True: an instance of the timed -march=native build."""
         self.cfg = cfg
-        self.h = lib().orc_create(C.byref(cfg))
+        self.L = lib(native)
+        self.h = self.L.orc_create(C.byref(cfg))
         if not self.h:
             raise ValueError("oracle rejected the configuration")
         s = (C.c_int32 * 12)()
-        lib().orc_sizes(self.h, s)
+        self.L.orc_sizes(self.h, s)
         self.sizes = tuple(s)
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().orc_destroy(self.h)
+            self.L.orc_destroy(self.h)
             self.h = None
 
     def _shape(self, field):
@@ -95,11 +106,11 @@ class Oracle:
     def set_field(self, field, a):
         a = np.ascontiguousarray(a, dtype=np.float64)
         assert a.shape == self._shape(field), (a.shape, self._shape(field))
-        lib().orc_set_field(self.h, field, _ptr(a))
+        self.L.orc_set_field(self.h, field, _ptr(a))
 
     def get_field(self, field):
         a = np.empty(self._shape(field))
-        lib().orc_get_field(self.h, field, _ptr(a))
+        self.L.orc_get_field(self.h, field, _ptr(a))
         return a
 
     def set_state(self, U, V, W, Pr=None):
@@ -114,17 +125,17 @@ class Oracle:
 
     def project(self, coef=1.0) -> float:
         md = C.c_double(0)
-        lib().orc_project(self.h, coef, C.byref(md))
+        self.L.orc_project(self.h, coef, C.byref(md))
         return md.value
 
     def step(self, n=1):
         md = C.c_double(0)
         cfl = C.c_double(0)
-        lib().orc_step(self.h, n, C.byref(md), C.byref(cfl))
+        self.L.orc_step(self.h, n, C.byref(md), C.byref(cfl))
         return md.value, cfl.value
 
     def run_stage(self, stage, stop):
-        r = lib().orc_run_stage(self.h, stage, stop)
+        r = self.L.orc_run_stage(self.h, stage, stop)
         assert r == 0
 
     def poisson(self, RHS):
@@ -132,14 +143,14 @@ class Oracle:
         RHS = np.ascontiguousarray(RHS, dtype=np.float64)
         assert RHS.shape == (Prnz + 2, Prny + 2, Prnx + 2)
         Phi = np.zeros((Prnz + 4, Prny + 4, Prnx + 4))
-        lib().orc_poisson(self.h, _ptr(RHS), _ptr(Phi))
+        self.L.orc_poisson(self.h, _ptr(RHS), _ptr(Phi))
         return Phi
 
     def scalar_slices(self, sc):
         """Time-averaged slices of scalar sc: xy (Prny, Prnx), xz (Prnz, Prnx)."""
         Prnx, Prny, Prnz = self.sizes[:3]
         xy, xz = np.zeros((Prny, Prnx)), np.zeros((Prnz, Prnx))
-        assert lib().orc_scalar_slices(self.h, sc, _ptr(xy), _ptr(xz)) == 0
+        assert self.L.orc_scalar_slices(self.h, sc, _ptr(xy), _ptr(xz)) == 0
         return xy, xz
 
     def set_puffs(self, puffs, volumes):
@@ -147,14 +158,14 @@ class Oracle:
         (puff, scalar_number, (i, j, k), flux)."""
         from gpu_elmm_b200.config import make_puffs
         P, n_p, V, n_v = make_puffs(puffs, volumes)
-        assert lib().orc_set_puffs(self.h, C.cast(P, C.c_void_p), n_p, C.cast(V, C.c_void_p), n_v) == 0
+        assert self.L.orc_set_puffs(self.h, C.cast(P, C.c_void_p), n_p, C.cast(V, C.c_void_p), n_v) == 0
         self._puffs = (P, V)
 
     def set_solids(self, solids):
         """Installs solid bodies: a gpu_elmm_b200.solids.Solids (or None)."""
         st = None if solids is None else solids.struct()
-        assert lib().orc_set_solids(self.h, None if st is None else C.cast(C.byref(st), C.c_void_p)) == 0
+        assert self.L.orc_set_solids(self.h, None if st is None else C.cast(C.byref(st), C.c_void_p)) == 0
         self._solids = solids
 
     def bound(self):
-        lib().orc_bound_uvw(self.h)
+        self.L.orc_bound_uvw(self.h)
