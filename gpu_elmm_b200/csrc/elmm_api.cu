@@ -345,6 +345,24 @@ struct BatchT {
     for (auto &x : sol) if (x.on) return true;
     return false;
   }
+  bool solids_on(int d) const { return d < (int)sol.size() && sol[d].on; }
+  // Mixed path: the per-level offsets of velocity component c (0: U, 1: V)
+  // of domain d from the host-layout array staged in stg (zero for a domain
+  // with solid bodies), on the stream; returns the offsets for k_unpack, or
+  // null for the FP64 path and for W.
+  const float *stage_offsets(int d, int c, const double *stg, const HostBox &hb) {
+    const Dom<T> &h = hdom[d];
+    if (sizeof(T) != 4 || c > 1 || !h.voff) return nullptr;
+    float *off = h.voff + c * (h.nz + 2);
+    if (solids_on(d)) cudaMemsetAsync(off, 0, sizeof(float) * (h.nz + 2), stream);
+    else k_level_offsets<T><<<h.nz + 2, 256, 0, stream>>>(ddom + d, stg, hb, c, h.voff);
+    return off;
+  }
+  // the offsets the pack of velocity component comp of domain d adds back, or null
+  const float *pack_offsets(int d, int comp) const {
+    const Dom<T> &h = hdom[d];
+    return (sizeof(T) == 4 && comp < 2 && h.voff) ? h.voff + comp * (h.nz + 2) : nullptr;
+  }
 
   ~BatchT() { release(); }
 
@@ -899,6 +917,9 @@ struct BatchT {
         CU(cudaMemcpy(h.TDiff, kv.data(), alloc_elems * sizeof(T), cudaMemcpyHostToDevice));
       }
     }
+    // mixed path: the per-level offsets of U and V (zero until the first
+    // upload; see Dom::voff)
+    if (sizeof(T) == 4 && (r = dalloc((void **)&h.voff, sizeof(float) * 2 * (h.nz + 2)))) return r;
     if ((r = dalloc((void **)&h.prm, sizeof(double)))) return r;
     h.nprpart = ((h.nx + MX - 1) / MX) * ((h.ny + MY - 1) / MY);
     if ((r = dalloc((void **)&h.prpart, sizeof(double) * h.nprpart))) return r;
@@ -1367,8 +1388,17 @@ struct BatchT {
     if (r) {
       drop_solids(d);
       push_dom(d);
+      return r;
     }
-    return r;
+    // the immersed-boundary kernels work on full velocities: the mixed
+    // path's stored deviations become full values and its offsets zero
+    if (sizeof(T) == 4 && hdom[d].voff) {
+      k_drop_offsets<T><<<148 * 4, 256, 0, stream>>>(ddom + d);
+      CU(cudaMemsetAsync(hdom[d].voff, 0, sizeof(float) * 2 * (hdom[d].nz + 2), stream));
+      CU(cudaStreamSynchronize(stream));
+      CU(cudaGetLastError());
+    }
+    return ELMM_OK;
   }
   int install_solids(int d, const elmm_solids *s) {
     Dom<T> &h = hdom[d];
@@ -1736,8 +1766,9 @@ struct BatchT {
       CU(cudaStreamWaitEvent(stream, ev_stage[b][0], 0));
       if (c < 3) {
         HostBox hb = hbox_vel(d, c);
+        const float *off = stage_offsets(d, c, stg, hb);
         k_unpack<T><<<kPackBlocks, 256, 0, stream>>>(ddom + d, c == 0 ? h.U : c == 1 ? h.V : h.W, stg, hb,
-                                                     h.ext[c][0], h.ext[c][1], h.ext[c][2], dbad);
+                                                     h.ext[c][0], h.ext[c][1], h.ext[c][2], dbad, off);
         k_halo_vel<T><<<256, 256, 0, stream>>>(ddom + d, c);
       } else {
         k_unpack_scalar<T><<<kPackBlocks, 256, 0, stream>>>(ddom + d, 0, stg, dbad);
@@ -1818,7 +1849,9 @@ struct BatchT {
       } else {
         CU(cudaMemcpyAsync(stg, src[c], n * sizeof(double), cudaMemcpyHostToDevice, stream));
       }
-      k_unpack<T><<<kPackBlocks, 256, 0, stream>>>(ddom + d, dst[c], stg, hb, h.ext[c][0], h.ext[c][1], h.ext[c][2], dbad);
+      const float *off = stage_offsets(d, c, stg, hb);
+      k_unpack<T><<<kPackBlocks, 256, 0, stream>>>(ddom + d, dst[c], stg, hb, h.ext[c][0], h.ext[c][1], h.ext[c][2], dbad,
+                                                   off);
       k_halo_vel<T><<<256, 256, 0, stream>>>(ddom + d, c);
       if (two) CU(cudaEventRecord(ev_stage[c & 1][1], stream));
     }
@@ -1915,7 +1948,7 @@ struct BatchT {
         int comp = (field == ELMM_FIELD_U || field == ELMM_FIELD_U2) ? 0 : (field == ELMM_FIELD_V || field == ELMM_FIELD_V2) ? 1 : 2;
         F = field <= ELMM_FIELD_W ? (comp == 0 ? h.U : comp == 1 ? h.V : h.W) : (comp == 0 ? h.U2 : comp == 1 ? h.V2 : h.W2);
         HostBox hb = hbox_vel(d, comp);
-        k_pack_vel<T><<<kPackBlocks, 256, 0, s>>>(ddom + d, F, comp, dst, hb);
+        k_pack_vel<T><<<kPackBlocks, 256, 0, s>>>(ddom + d, F, comp, dst, hb, pack_offsets(d, comp));
         return (size_t)hb.n0 * hb.n1 * hb.n2;
       }
       case ELMM_FIELD_USTAR: case ELMM_FIELD_VSTAR: case ELMM_FIELD_WSTAR: {

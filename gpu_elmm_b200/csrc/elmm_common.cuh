@@ -111,6 +111,18 @@ struct Dom {
   double *prm;           // 1 value
   double *prpart;        // partial sums of the top layer of P
   int nprpart;
+  // Mixed path: U and V are stored as deviations from a per-level offset,
+  // value = stored + voff[c * (nz + 2) + k] for c = 0 (U), 1 (V) and k in
+  // [0, nz + 1].  With a mean velocity of several m/s, FP32 rounding of the
+  // full value leaves noise whose divergence every projection then turns
+  // into pressure; the deviations round ~10-50x finer.  The offset is
+  // constant over each level, so every x and y difference (divergence,
+  // projection, ghost images) works on the stored values unchanged; the
+  // ghost levels 0 and nz+1 follow the BoundUVW fold of their source level
+  // (odd at a no-slip wall, even at a free-slip one, periodic copies), so a
+  // fold of stored values is the fold of full values.  Null on the FP64
+  // path; zero on a domain with solid bodies.
+  float *voff;
   // diagnostics
   unsigned long long *maxdiv_bits;  // max |div u| as the bits of a positive double
   unsigned long long *cfl_bits;
@@ -301,6 +313,17 @@ __device__ __forceinline__ T vel_folded(const Dom<T> &d, const T *F, int comp, i
   if (fx.zero | fy.zero | fz.zero) return (T)0;
   const T v = __ldg(F + bidx(d, fx.src, fy.src, fz.src));
   return fx.sign * fy.sign * fz.sign < 0 ? -v : v;
+}
+
+// The offset of velocity component c (0: U, 1: V, 2: W, which has none) at
+// level k in [0, nz + 1]; zero on the FP64 path.
+template <typename T>
+__device__ __forceinline__ T vel_off(const Dom<T> &d, int c, int k) {
+  if constexpr (sizeof(T) == 4) {
+    return c < 2 ? __ldg(d.voff + c * (d.nz + 2) + k) : 0.f;
+  } else {
+    return (T)0;
+  }
 }
 
 // Domain lookup of a flattened tile index (batched launches).

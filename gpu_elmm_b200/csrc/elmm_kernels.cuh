@@ -86,18 +86,30 @@ template <typename T>
 __device__ void wm_point(const Dom<T> &d, int comp, int f, int i, int j, int k, long long pidx) {
   const T *U = d.U, *V = d.V, *W = d.W;
   const long long c = bidx(d, i, j, k), sx = 1, sy = d.pitch, sz = d.plane;
+  // full velocities: stored values plus the per-level offsets of U and V of
+  // the mixed path (the FP64 path reads the stored values alone), in FP64
+  const double ou0 = (double)vel_off(d, 0, k), ov0 = (double)vel_off(d, 1, k);
+  auto lu = [&](long long o, double off) {
+    if constexpr (sizeof(T) == 4) return (double)ld(U, c + o) + off;
+    else return (double)ld(U, c + o);
+  };
+  auto lv = [&](long long o, double off) {
+    if constexpr (sizeof(T) == 4) return (double)ld(V, c + o) + off;
+    else return (double)ld(V, c + o);
+  };
   double vel[3];
   if (comp == 0) {
-    vel[0] = (double)ld(U, c);
-    vel[1] = ((double)ld(V, c + sx) + (double)ld(V, c) + (double)ld(V, c + sx - sy) + (double)ld(V, c - sy)) / 4.0;
+    vel[0] = lu(0, ou0);
+    vel[1] = (lv(sx, ov0) + lv(0, ov0) + lv(sx - sy, ov0) + lv(-sy, ov0)) / 4.0;
     vel[2] = ((double)ld(W, c + sx) + (double)ld(W, c) + (double)ld(W, c + sx - sz) + (double)ld(W, c - sz)) / 4.0;
   } else if (comp == 1) {
-    vel[0] = ((double)ld(U, c + sy) + (double)ld(U, c) + (double)ld(U, c - sx + sy) + (double)ld(U, c - sx)) / 4.0;
-    vel[1] = (double)ld(V, c);
+    vel[0] = (lu(sy, ou0) + lu(0, ou0) + lu(-sx + sy, ou0) + lu(-sx, ou0)) / 4.0;
+    vel[1] = lv(0, ov0);
     vel[2] = ((double)ld(W, c + sy) + (double)ld(W, c) + (double)ld(W, c + sy - sz) + (double)ld(W, c - sz)) / 4.0;
   } else {
-    vel[0] = ((double)ld(U, c + sz) + (double)ld(U, c) + (double)ld(U, c - sx + sz) + (double)ld(U, c - sx)) / 4.0;
-    vel[1] = ((double)ld(V, c + sz) + (double)ld(V, c) + (double)ld(V, c - sy + sz) + (double)ld(V, c - sy)) / 4.0;
+    const double ou1 = (double)vel_off(d, 0, k + 1), ov1 = (double)vel_off(d, 1, k + 1);
+    vel[0] = (lu(sz, ou1) + lu(0, ou0) + lu(-sx + sz, ou1) + lu(-sx, ou0)) / 4.0;
+    vel[1] = (lv(sz, ov1) + lv(0, ov0) + lv(-sy + sz, ov1) + lv(-sy, ov0)) / 4.0;
     vel[2] = (double)ld(W, c);
   }
   // distance to the wall: xU(0) - x(1) etc. with the staggered coordinate of the component

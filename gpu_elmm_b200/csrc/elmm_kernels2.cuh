@@ -636,8 +636,15 @@ __global__ void __launch_bounds__(TX *TY) k_cfl(const Dom<T> *__restrict__ doms,
       const double dzk = d.vz ? d.dzPr[k + 2] : d.dz;
       // NaN-propagating maximum of |u| over the two faces (fmax would drop a NaN)
       auto fm = [](double x, double y) { return (x != x || x > y) ? x : y; };
-      double a = fm(fabs((double)ld(d.U, c)), fabs((double)ld(d.U, c - 1))) / d.dx;
-      a = a + fm(fabs((double)ld(d.V, c)), fabs((double)ld(d.V, c - d.pitch))) / d.dy;
+      // full velocities (the per-level offsets of the mixed path; none in FP64)
+      double uc = (double)ld(d.U, c), uw = (double)ld(d.U, c - 1);
+      double vc = (double)ld(d.V, c), vs = (double)ld(d.V, c - d.pitch);
+      if constexpr (sizeof(T) == 4) {
+        const double uo = vel_off(d, 0, k), vo = vel_off(d, 1, k);
+        uc += uo; uw += uo; vc += vo; vs += vo;
+      }
+      double a = fm(fabs(uc), fabs(uw)) / d.dx;
+      a = a + fm(fabs(vc), fabs(vs)) / d.dy;
       a = a + fm(fabs((double)ld(d.W, c)), fabs((double)ld(d.W, c - d.plane))) / dzk;
       const unsigned long long b = max_bits(a);
       run = b > run ? b : run;
@@ -657,10 +664,12 @@ __device__ __forceinline__ long long hidx(const HostBox &h, int i, int j, int k)
   return (long long)(i - h.lo) + (long long)h.n0 * ((long long)(j - h.lo) + (long long)h.n1 * (k - h.lo));
 }
 
-// interior of a host array (double) -> device box (T); counts non-finite values
+// interior of a host array (double) -> device box (T); counts non-finite
+// values.  off: per-level offsets subtracted before the rounding to T (the
+// U and V of the mixed path), or null.
 template <typename T>
 __global__ void k_unpack(const Dom<T> *__restrict__ dom, T *dst, const double *__restrict__ src, HostBox h, int nx,
-                         int ny, int nz, int *bad) {
+                         int ny, int nz, int *bad, const float *off = nullptr) {
   const Dom<T> &d = *dom;
   long long total = (long long)nx * ny * nz;
   for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < total; w += (long long)gridDim.x * blockDim.x) {
@@ -669,7 +678,45 @@ __global__ void k_unpack(const Dom<T> *__restrict__ dom, T *dst, const double *_
     int j = (int)(r % ny) + 1, k = (int)(r / ny) + 1;
     double v = src[hidx(h, i, j, k)];
     if (!isfinite(v)) atomicAdd(bad, 1);
+    if (off) v -= (double)off[k];
     dst[bidx(d, i, j, k)] = (T)v;
+  }
+}
+
+// The per-level offsets of velocity component c (0: U, 1: V) of the mixed
+// path from a host-layout array (double, interior read): block g handles
+// level g in [0, nz + 1] and writes the mean over the level that the
+// BoundUVW fold of g points to, with the fold's sign (so the ghost levels
+// fold as the velocity does), rounded to FP32.  Any fixed value would do;
+// the mean keeps the stored deviations small.  A non-finite mean (the
+// upload reports non-finite input anyway) is written as 0.
+template <typename T>
+__global__ void __launch_bounds__(256) k_level_offsets(const Dom<T> *__restrict__ dom, const double *__restrict__ src,
+                                                       HostBox h, int c, float *off) {
+  const Dom<T> &d = *dom;
+  const int *e = d.ext[c];
+  const int g = blockIdx.x;  // level, 0..nz+1 (the offset table's range)
+  if (g > d.nz + 1) return;
+  const Fold fz = fold_vel(g, e[2], d.bt[4], d.bt[5], false);  // U and V are tangential in z
+  __shared__ double red[8];
+  double s = 0;
+  if (!fz.zero) {
+    const long long n = (long long)e[0] * e[1];
+    for (long long w = threadIdx.x; w < n; w += blockDim.x) {
+      const int i = (int)(w % e[0]) + 1, j = (int)(w / e[0]) + 1;
+      s += src[hidx(h, i, j, fz.src)];
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); q++) t += red[q];
+    double m = fz.zero ? 0.0 : t / ((double)e[0] * (double)e[1]);
+    if (!isfinite(m)) m = 0.0;
+    const float f = (float)m;
+    off[c * (d.nz + 2) + g] = fz.sign < 0 ? -f : f;
   }
 }
 
@@ -718,9 +765,12 @@ __global__ void k_halo_p(const Dom<T> *__restrict__ dom) {
   }
 }
 
-// device box -> host layout with the reference's three-deep ghosts (BoundUVW)
+// device box -> host layout with the reference's three-deep ghosts
+// (BoundUVW).  off: per-level offsets added to the stored values (the U and
+// V of the mixed path, and their U2, V2), or null.
 template <typename T>
-__global__ void k_pack_vel(const Dom<T> *__restrict__ dom, const T *F, int comp, double *dst, HostBox h) {
+__global__ void k_pack_vel(const Dom<T> *__restrict__ dom, const T *F, int comp, double *dst, HostBox h,
+                           const float *off = nullptr) {
   const Dom<T> &d = *dom;
   const int *e = d.ext[comp];
   long long total = (long long)h.n0 * h.n1 * h.n2;
@@ -734,9 +784,27 @@ __global__ void k_pack_vel(const Dom<T> *__restrict__ dom, const T *F, int comp,
     double v = 0;
     if (!(fx.zero | fy.zero | fz.zero)) {
       v = (double)F[bidx(d, fx.src, fy.src, fz.src)];
+      if (off) v += (double)off[fz.src];
       if (fx.sign * fy.sign * fz.sign < 0) v = -v;
     }
     dst[w] = v;
+  }
+}
+
+// Mixed path, before solid bodies are installed: the stored deviations of
+// U and V (every box cell, ghosts included) become full values, since the
+// immersed-boundary kernels work on full values; the host then zeroes the
+// offsets.
+template <typename T>
+__global__ void k_drop_offsets(const Dom<T> *__restrict__ dom) {
+  const Dom<T> &d = *dom;
+  if constexpr (sizeof(T) == 4) {
+    const long long n = d.plane * (d.nz + 2);
+    for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n; w += (long long)gridDim.x * blockDim.x) {
+      const int k = (int)(w / d.plane);
+      d.U[w] = d.U[w] + d.voff[k];
+      d.V[w] = d.V[w] + d.voff[d.nz + 2 + k];
+    }
   }
 }
 

@@ -14,6 +14,8 @@
 // the same way.
 #pragma once
 
+#include <type_traits>
+
 #include "elmm_common.cuh"
 #include "elmm_packed.cuh"
 #include "elmm_stream.cuh"
@@ -308,6 +310,87 @@ __device__ __forceinline__ T tendency(const MomCtx<T> &m, const RT &R, int i, in
   return a;
 }
 
+// The wall-model corrections of one cell on the mixed path (the wall blocks
+// of tendency<T, C>: the diffusive flux through the face towards a wall-model
+// side taken back, the wall-model flux added; the wmfluxes-*-inc.f90
+// includes), on stored deviations: a difference across levels is the stored
+// difference plus the difference of the offsets (O, see tendency_dev).
+template <int C, typename RT>
+__device__ __forceinline__ float wall_dev(const MomCtx<float> &m, const RT &R, const VelOffN<float> &O, int i, int j,
+                                          int k) {
+#define FN(dx, dy, dz) R.g(3, dx, dy, dz)
+  const float rx = m.rec2[0], ry = m.rec2[1], rz = m.rec2[2];
+  const int *e = m.ext[C];
+  float a = 0.f;
+  const long long pyz = (long long)(j - 1) + (long long)e[1] * (k - 1), pxz = (long long)(i - 1) + (long long)e[0] * (k - 1);
+  const long long pxy = (long long)(i - 1) + (long long)e[0] * (j - 1);
+  const bool bo = (m.wallmask & (1 << SIDE_BO)) && k == 1 && !(m.bskip[C] && m.bskip[C][pxy]);
+  const bool to = (m.wallmask & (1 << SIDE_TO)) && k == e[2];
+  if (C < 2) {
+    // U (C = 0) or V (C = 1): the component F and its offsets
+    const float f = R.g(C, 0, 0, 0), fe = R.g(C, 1, 0, 0), fw = R.g(C, -1, 0, 0), fn = R.g(C, 0, 1, 0);
+    const float fs = R.g(C, 0, -1, 0), ft = R.g(C, 0, 0, 1), fb = R.g(C, 0, 0, -1);
+    const float *o = C == 0 ? O.o : O.p;
+    const float n0 = FN(0, 0, 0), ne = FN(1, 0, 0), nn = FN(0, 1, 0), nne = FN(1, 1, 0);
+    // the viscosities of the x- and y-faces of the point
+    const float nW = C == 0 ? n0 : 0.25f * (((nn + n0) + FN(-1, 1, 0)) + FN(-1, 0, 0));
+    const float nE = C == 0 ? ne : 0.25f * (((nne + ne) + nn) + n0);
+    const float nS = C == 0 ? 0.25f * (((ne + FN(1, -1, 0)) + n0) + FN(0, -1, 0)) : n0;
+    const float nN = C == 0 ? 0.25f * (((nne + ne) + nn) + n0) : nn;
+    if ((m.wallmask & (1 << SIDE_WE)) && i == 1) { a = a + nW * (f - fw) * rx; a = a + m.fluxp[C * 6 + SIDE_WE][pyz]; }
+    if ((m.wallmask & (1 << SIDE_EA)) && i == e[0]) { a = a - nE * (fe - f) * rx; a = a - m.fluxm[C * 6 + SIDE_EA][pyz]; }
+    if ((m.wallmask & (1 << SIDE_SO)) && j == 1) { a = a + nS * (f - fs) * ry; a = a + m.fluxp[C * 6 + SIDE_SO][pxz]; }
+    if ((m.wallmask & (1 << SIDE_NO)) && j == e[1]) { a = a - nN * (fn - f) * ry; a = a - m.fluxm[C * 6 + SIDE_NO][pxz]; }
+    if (bo) {
+      const float s = C == 0 ? ((ne + FN(1, 0, -1)) + n0) + FN(0, 0, -1) : ((nn + FN(0, 1, -1)) + n0) + FN(0, 0, -1);
+      const float db = (f - fb) + (o[1] - o[0]);
+      if (m.vz) a = a + s * db / (float)m.dzW[k - 1 + 2] / 4 / (float)m.dzPr[k + 2];
+      else a = a + s * db * rz / 4;
+      a = a + m.fluxp[C * 6 + SIDE_BO][pxy];
+    }
+    if (to) {
+      const float s = C == 0 ? ((FN(1, 0, 1) + ne) + FN(0, 0, 1)) + n0 : ((FN(0, 1, 1) + nn) + FN(0, 0, 1)) + n0;
+      const float dt = (ft - f) + (o[2] - o[1]);
+      if (m.vz) a = a - s * dt / (float)m.dzW[k + 2] / 4 / (float)m.dzPr[k + 2];
+      else a = a - s * dt * rz / 4;
+      a = a - m.fluxm[C * 6 + SIDE_TO][pxy];
+    }
+  } else {
+    const float w = R.g(2, 0, 0, 0), we = R.g(2, 1, 0, 0), ww = R.g(2, -1, 0, 0), wn = R.g(2, 0, 1, 0);
+    const float ws = R.g(2, 0, -1, 0), wt = R.g(2, 0, 0, 1), wb = R.g(2, 0, 0, -1);
+    const float n0 = FN(0, 0, 0), ne = FN(1, 0, 0), nt = FN(0, 0, 1), nte = FN(1, 0, 1), nw = FN(-1, 0, 0);
+    const float ntw = FN(-1, 0, 1), nn = FN(0, 1, 0), ntn = FN(0, 1, 1), ns = FN(0, -1, 0), nts = FN(0, -1, 1);
+    if ((m.wallmask & (1 << SIDE_WE)) && i == 1) {
+      a = a + (((nt + n0) + ntw) + nw) * (w - ww) * rx / 4;
+      a = a + m.fluxp[2 * 6 + SIDE_WE][pyz];
+    }
+    if ((m.wallmask & (1 << SIDE_EA)) && i == e[0]) {
+      a = a - (((nte + ne) + nt) + n0) * (we - w) * rx / 4;
+      a = a - m.fluxm[2 * 6 + SIDE_EA][pyz];
+    }
+    if ((m.wallmask & (1 << SIDE_SO)) && j == 1) {
+      a = a + (((nt + nts) + n0) + ns) * (w - ws) * ry / 4;
+      a = a + m.fluxp[2 * 6 + SIDE_SO][pxz];
+    }
+    if ((m.wallmask & (1 << SIDE_NO)) && j == e[1]) {
+      a = a - (((ntn + nt) + nn) + n0) * (wn - w) * ry / 4;
+      a = a - m.fluxm[2 * 6 + SIDE_NO][pxz];
+    }
+    if (bo) {
+      if (m.vz) a = a + n0 * (w - wb) / (float)m.dzPr[k + 2] / (float)m.dzW[k + 2];
+      else a = a + n0 * (w - wb) * rz;
+      a = a + m.fluxp[2 * 6 + SIDE_BO][pxy];
+    }
+    if (to) {
+      if (m.vz) a = a - nt * (wt - w) / (float)m.dzPr[k + 1 + 2] / (float)m.dzW[k + 2];
+      else a = a - nt * (wt - w) * rz;
+      a = a - m.fluxm[2 * 6 + SIDE_TO][pxy];
+    }
+  }
+#undef FN
+  return a;
+}
+
 // Layout of one ring slot (one plane k of the tile): NWF "wide" fields with
 // the x/y halo (rows j0-1..j0+MY, columns i0-XO..i0+MX+XO-1) and NNF
 // "narrow" fields of the tile's own cells (rows j0..j0+MY-1, columns
@@ -381,6 +464,8 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
   T *ring = reinterpret_cast<T *>(dyn_smem);
   __shared__ __align__(8) uint64_t bars[NSL];
   __shared__ MomCtx<T> ctx;
+  // mixed path: offsets of U and V on planes k0-1 .. k0+MKC of the tile (see Dom::voff)
+  __shared__ float soff[2][MKC + 2];
   __shared__ int abort_flag;
   const int tx = threadIdx.x % TXN, ty = threadIdx.x / TXN;
   // tensor copies need 128-byte aligned destinations
@@ -414,6 +499,12 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
     const CUtensorMap *maps = reinterpret_cast<const CUtensorMap *>(d.tmaps);
     __syncthreads();  // every slot and the context of the previous tile are free
     if (threadIdx.x == 0) fill_ctx(ctx, d);
+    if constexpr (sizeof(T) == 4) {
+      if (threadIdx.x < 2 * (MKC + 2)) {
+        const int c = threadIdx.x / (MKC + 2), kk = k0 - 1 + threadIdx.x % (MKC + 2);
+        soff[c][kk - k0 + 1] = kk <= d.nz + 1 ? __ldg(d.voff + c * (d.nz + 2) + kk) : 0.f;
+      }
+    }
     if (threadIdx.x == 0) {
       fence_async_shared();
       for (int kk = k0 - 1; kk <= min(k0 - 1 + NSL - 1, k1 + 1); kk++)
@@ -487,6 +578,12 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
           Ring2<Lay::WB, Lay::SPW> R2;
           R2.p[0] = p0s; R2.p[1] = p1s; R2.p[2] = p2s;
           R2.o = o;
+          // the stencils take the offsets of U and V separately
+          // (tendency_dev); the RK combine below works on the stored
+          // deviations (U2 is stored the same way)
+          VelOffN<F2> O;
+#pragma unroll
+          for (int q = 0; q < 3; q++) { O.o[q] = bc2(soff[0][k - k0 + q]); O.p[q] = bc2(soff[1][k - k0 + q]); }
           const float *nar = p1s + Lay::WIDE + ty * MX + CPT * tx;
           const F2 mm = bc2(m);
           const F2 p0 = R2.g(4, 0, 0, 0) - mm;
@@ -497,9 +594,9 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
           F2 tu, tv, tw;
           F2 gz2 = bc2(gz);
           if (!vz) {
-            tu = tendency2<0>(K2, R2);
-            tv = tendency2<1>(K2, R2);
-            tw = tendency2<2>(K2, R2, btp);
+            tu = tendency_dev<0, false>(K2, R2, O, bc2(0.f), (const KZ2 *)nullptr);
+            tv = tendency_dev<1, false>(K2, R2, O, bc2(0.f), (const KZ2 *)nullptr);
+            tw = tendency_dev<2, false>(K2, R2, O, btp, (const KZ2 *)nullptr);
           } else {
             const int nzp = nz + 2;
             const float *kz = d.kz2 + k;
@@ -509,9 +606,9 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
             Z.aw = bc2(__ldg(kz + KZ_AW * nzp)); Z.bw = bc2(__ldg(kz + KZ_BW * nzp));
             Z.d1w = bc2(__ldg(kz + KZ_D1W * nzp)); Z.d2w = bc2(__ldg(kz + KZ_D2W * nzp));
             gz2 = bc2((-coef) * __ldg(kz + KZ_RDZW * nzp));
-            tu = tendency2<0, true>(K2, R2, bc2(0.f), &Z);
-            tv = tendency2<1, true>(K2, R2, bc2(0.f), &Z);
-            tw = tendency2<2, true>(K2, R2, btp, &Z);
+            tu = tendency_dev<0, true>(K2, R2, O, bc2(0.f), &Z);
+            tv = tendency_dev<1, true>(K2, R2, O, bc2(0.f), &Z);
+            tw = tendency_dev<2, true>(K2, R2, O, btp, &Z);
           }
           const F2 rd = bc2(rdt), dd = bc2(dt), bd = bc2(bdt);
           const F2 zero = bc2(0.f);
@@ -553,11 +650,45 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
           const bool doU = iq <= d.ext[0][0] && j <= d.ext[0][1] && k <= kU;
           const bool doV = iq <= d.ext[1][0] && j <= d.ext[1][1] && k <= kV;
           const bool doW = iq <= d.ext[2][0] && j <= d.ext[2][1] && k <= kW;
-          const T tu = doU ? tendency<T, 0>(ctx, R, iq, j, k, wallhere) : (T)0;
-          const T tv = doV ? tendency<T, 1>(ctx, R, iq, j, k, wallhere) : (T)0;
           T bt = (T)0;
           if (buoy && doW) bt = bA2 * (ld(Tm, cq + plane) + ld(Tm, cq));
-          const T tw = doW ? tendency<T, 2>(ctx, R, iq, j, k, wallhere, bt, bsub) : (T)0;
+          T tu, tv, tw;
+          if constexpr (sizeof(T) == 4) {
+            // mixed path: the deviation forms of tendency_dev plus the wall
+            // corrections of wall_dev (U and V are stored as deviations)
+            VelOffN<float> O;
+#pragma unroll
+            for (int q3 = 0; q3 < 3; q3++) { O.o[q3] = soff[0][k - k0 + q3]; O.p[q3] = soff[1][k - k0 + q3]; }
+            MomKN<float> K1;
+            K1.Ax = ctx.cA[0]; K1.Ay = ctx.cA[1]; K1.Az = ctx.cA[2];
+            K1.rx = ctx.rec2[0]; K1.ry = ctx.rec2[1]; K1.rz = ctx.rec2[2];
+            K1.q = 0.25f;
+            for (int c3 = 0; c3 < 3; c3++)
+              for (int a3 = 0; a3 < 3; a3++) K1.B[c3][a3] = ctx.cB[c3][a3];
+            KZN<float> Z1;
+            if (vz) {
+              const int nzp = nz + 2;
+              const float *kz = d.kz2 + k;
+              Z1.auv = __ldg(kz + KZ_AUV * nzp); Z1.buv = __ldg(kz + KZ_BUV * nzp);
+              Z1.d1uv = __ldg(kz + KZ_D1UV * nzp); Z1.d2uv = __ldg(kz + KZ_D2UV * nzp);
+              Z1.aw = __ldg(kz + KZ_AW * nzp); Z1.bw = __ldg(kz + KZ_BW * nzp);
+              Z1.d1w = __ldg(kz + KZ_D1W * nzp); Z1.d2w = __ldg(kz + KZ_D2W * nzp);
+            }
+            auto td = [&](auto cc) -> float {
+              constexpr int CC = decltype(cc)::value;
+              const float b3 = CC == 2 ? bt : 0.f;
+              float a3 = vz ? tendency_dev<CC, true>(K1, R, O, b3, &Z1) : tendency_dev<CC, false>(K1, R, O, b3, &Z1);
+              if (wallhere) a3 = a3 + wall_dev<CC>(ctx, R, O, iq, j, k);
+              return a3;
+            };
+            tu = doU ? td(std::integral_constant<int, 0>{}) : 0.f;
+            tv = doV ? td(std::integral_constant<int, 1>{}) : 0.f;
+            tw = doW ? td(std::integral_constant<int, 2>{}) : 0.f;
+          } else {
+            tu = doU ? tendency<T, 0>(ctx, R, iq, j, k, wallhere) : (T)0;
+            tv = doV ? tendency<T, 1>(ctx, R, iq, j, k, wallhere) : (T)0;
+            tw = doW ? tendency<T, 2>(ctx, R, iq, j, k, wallhere, bt, bsub) : (T)0;
+          }
           T u2 = stage1 ? (T)0 : nar[0] * rdt * dt;
           T v2 = stage1 ? (T)0 : nar[Lay::NB] * rdt * dt;
           T w2 = stage1 ? (T)0 : nar[2 * Lay::NB] * rdt * dt;
@@ -612,6 +743,12 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
 template <typename T>
 struct SgsK {  // factors of NuSmag at one level k
   T rdx, rdy, r4dx, r4dy, rdz, r2zz, wc2;
+  // mixed path: the part of the z differences of U and V (D02, D12) that
+  // comes from their per-level offsets, 2 (off(k+1) - off(k-1)) r2zz, in
+  // shared memory per plane of the tile (the ring holds the stored
+  // deviations; every other difference is taken within one level, where the
+  // offset cancels)
+  const float *du, *dv;
 };
 
 // The divisions by the (uniform) spacings of StrainIJ are multiplications by
@@ -629,6 +766,10 @@ __device__ __forceinline__ T nusmag_ring(const SgsK<T> &q, const RT &R) {
   T D02 = (GU(0, 0, 1) + GU(-1, 0, 1) - GU(0, 0, -1) - GU(-1, 0, -1)) * q.r2zz;
   T D10 = (GV(1, 0, 0) + GV(1, -1, 0) - GV(-1, 0, 0) - GV(-1, -1, 0)) * q.r4dx;
   T D12 = (GV(0, 0, 1) + GV(0, -1, 1) - GV(0, 0, -1) - GV(0, -1, -1)) * q.r2zz;
+  if constexpr (sizeof(T) == 4) {
+    D02 = D02 + *q.du;
+    D12 = D12 + *q.dv;
+  }
   T D20 = (GW(1, 0, 0) + GW(1, 0, -1) - GW(-1, 0, 0) - GW(-1, 0, -1)) * q.r4dx;
   T D21 = (GW(0, 1, 0) + GW(0, 1, -1) - GW(0, -1, 0) - GW(0, -1, -1)) * q.r4dy;
 #undef GU
@@ -661,9 +802,9 @@ __device__ __forceinline__ F2 nusmag2(const SgsK<float> &q, const RT &R) {
   const F2 D11 = (GV(0, 0, 0) - GV(0, -1, 0)) * rdy;
   const F2 D22 = (GW(0, 0, 0) - GW(0, 0, -1)) * rdz;
   const F2 D01 = (((GU(0, 1, 0) + GU(-1, 1, 0)) - GU(0, -1, 0)) - GU(-1, -1, 0)) * r4dy;
-  const F2 D02 = (((GU(0, 0, 1) + GU(-1, 0, 1)) - GU(0, 0, -1)) - GU(-1, 0, -1)) * r2zz;
+  const F2 D02 = (((GU(0, 0, 1) + GU(-1, 0, 1)) - GU(0, 0, -1)) - GU(-1, 0, -1)) * r2zz + bc2(*q.du);
   const F2 D10 = (((GV(1, 0, 0) + GV(1, -1, 0)) - GV(-1, 0, 0)) - GV(-1, -1, 0)) * r4dx;
-  const F2 D12 = (((GV(0, 0, 1) + GV(0, -1, 1)) - GV(0, 0, -1)) - GV(0, -1, -1)) * r2zz;
+  const F2 D12 = (((GV(0, 0, 1) + GV(0, -1, 1)) - GV(0, 0, -1)) - GV(0, -1, -1)) * r2zz + bc2(*q.dv);
   const F2 D20 = (((GW(1, 0, 0) + GW(1, 0, -1)) - GW(-1, 0, 0)) - GW(-1, 0, -1)) * r4dx;
   const F2 D21 = (((GW(0, 1, 0) + GW(0, 1, -1)) - GW(0, -1, 0)) - GW(0, -1, -1)) * r4dy;
 #undef GU
@@ -717,6 +858,8 @@ __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
   T *ring = reinterpret_cast<T *>(dyn_smem);
   __shared__ __align__(8) uint64_t bars[kRingSlots];
   __shared__ int abort_flag;
+  // mixed path: the z-difference parts du, dv of the tile's planes (SgsK)
+  __shared__ float sdz[2][MKC];
   const int tx = threadIdx.x % TXN, ty = threadIdx.x / TXN;
   if (smem_addr(ring) & 127u) {  // tensor copies need 128-byte aligned destinations
     if (threadIdx.x == 0) doms[0].flags[1] = 1;
@@ -744,7 +887,17 @@ __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
     const int wide[3] = {F_U, F_V, F_W};
     const int none[1] = {0};
     const CUtensorMap *maps = reinterpret_cast<const CUtensorMap *>(d.tmaps);
-    __syncthreads();  // every slot of the previous tile is free
+    __syncthreads();  // every slot and the z-difference parts of the previous tile are free
+    if constexpr (sizeof(T) == 4) {
+      if (threadIdx.x < 2 * MKC) {
+        const int c = threadIdx.x / MKC, kk = k0 + threadIdx.x % MKC;
+        if (kk <= k1) {
+          const float *o = d.voff + c * (d.nz + 2);
+          sdz[c][kk - k0] = 2.f * (__ldg(o + kk + 1) - __ldg(o + kk - 1)) * (float)d.sgs_r2zz[kk];
+        }
+      }
+      __syncthreads();
+    }
     if (threadIdx.x == 0) {
       fence_async_shared();
       for (int kk = k0 - 1; kk <= min(k0 - 1 + kRingSlots - 1, k1 + 1); kk++)
@@ -777,6 +930,8 @@ __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
     const long long plane = d.plane;
     for (int k = k0; k <= k1; k++) {
       q.rdz = (T)tr[k]; q.r2zz = (T)t2[k]; q.wc2 = (T)tw[k];
+      q.du = &sdz[0][k - k0];
+      q.dv = &sdz[1][k - k0];
       // planes k-1, k, k+1 must have landed
       bool ok = true;
       for (int kk = (k == k0 ? k0 - 1 : k + 1); kk <= k + 1; kk++) {

@@ -140,10 +140,17 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
       // advection: the loop order of KappaScalar gives each cell +A f(low
       // face) then -A f(high face) in x and y; in z the even faces come first
       T a = (T)0;
-      a = a + Ax * kappa_flux<T>(uw, sxm2, sxm1, s0, sxp1);
-      a = a - Ax * kappa_flux<T>(ue, sxm1, s0, sxp1, sxp2);
-      a = a + Ay * kappa_flux<T>(vs, sym2, sym1, s0, syp1);
-      a = a - Ay * kappa_flux<T>(vn, sym1, s0, syp1, syp2);
+      // the face velocities in full (the mixed path stores U and V as
+      // deviations from a per-level offset; the FP64 path has none)
+      T uwf = uw, uef = ue, vsf = vs, vnf = vn;
+      if constexpr (sizeof(T) == 4) {
+        const T uo = vel_off(d, 0, k), vo = vel_off(d, 1, k);
+        uwf = uw + uo; uef = ue + uo; vsf = vs + vo; vnf = vn + vo;
+      }
+      a = a + Ax * kappa_flux<T>(uwf, sxm2, sxm1, s0, sxp1);
+      a = a - Ax * kappa_flux<T>(uef, sxm1, s0, sxp1, sxp2);
+      a = a + Ay * kappa_flux<T>(vsf, sym2, sym1, s0, syp1);
+      a = a - Ay * kappa_flux<T>(vnf, sym1, s0, syp1, syp2);
       const T fzt = kappa_flux<T>(wt, sz[1], s0, sz[3], sz[4]);
       if (((k - 1) & 1) == 0) {  // face k-1 is even
         a = a + Az * fzb;
@@ -279,10 +286,12 @@ __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SP
                    syp2 = ld2(S, cc + oy[4]);
       const float2 kym = ld2(K, cc + oy[1]), kyp = ld2(K, cc + oy[3]);
       const float2 told = stage1 ? make_float2(0.f, 0.f) : ld2(Sadv, cc);
-      // x faces: low face of cell i, the face between the pair, high face of i+1
-      const T f0 = kappa_flux<T>(um.y, sm.x, sm.y, s0.x, s0.y);
-      const T f1 = kappa_flux<T>(u0.x, sm.y, s0.x, s0.y, sp.x);
-      const T f2 = kappa_flux<T>(u0.y, s0.x, s0.y, sp.x, sp.y);
+      // x faces: low face of cell i, the face between the pair, high face of
+      // i+1, with the full face velocities (stored deviation + level offset)
+      const T uo = vel_off(d, 0, k), vo = vel_off(d, 1, k);
+      const T f0 = kappa_flux<T>(um.y + uo, sm.x, sm.y, s0.x, s0.y);
+      const T f1 = kappa_flux<T>(u0.x + uo, sm.y, s0.x, s0.y, sp.x);
+      const T f2 = kappa_flux<T>(u0.y + uo, s0.x, s0.y, sp.x, sp.y);
       const float2 fzt = make_float2(kappa_flux<T>(wt.x, sz[1].x, s0.x, sz[3].x, sz[4].x),
                                      kappa_flux<T>(wt.y, sz[1].y, s0.y, sz[3].y, sz[4].y));
       const bool even = ((k - 1) & 1) == 0;  // face k-1 is even
@@ -295,7 +304,7 @@ __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SP
         const T sxm1 = c ? s0.x : sm.y, sxp1 = c ? sp.x : s0.y;
         const T kxm = c ? kz[1].x : km.y, kxp = c ? kp.x : kz[1].y, k0v = c ? kz[1].y : kz[1].x;
         const T fl = c ? f1 : f0, fh = c ? f2 : f1;
-        const T vsc = c ? vs.y : vs.x, vnc = c ? vn.y : vn.x;
+        const T vsc = (c ? vs.y : vs.x) + vo, vnc = (c ? vn.y : vn.x) + vo;
         const T a2 = c ? sym2.y : sym2.x, a1 = c ? sym1.y : sym1.x, b1 = c ? syp1.y : syp1.x, b2 = c ? syp2.y : syp2.x;
         T a = (T)0;
         a = a + Ax * fl;
@@ -330,8 +339,8 @@ __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SP
           T div = (T)0;
           div = div + ue / rdx;
           div = div - uw / rdx;
-          div = div + vnc / rdy;
-          div = div - vsc / rdy;
+          div = div + (c ? vn.y : vn.x) / rdy;  // stored values: the level offset cancels
+          div = div - (c ? vs.y : vs.x) / rdy;
           div = div + wtc / dzk;
           div = div - wbc / dzk;
           a = a + div * sc;

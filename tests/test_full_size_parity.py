@@ -20,8 +20,9 @@ that size:
 Tolerances (relative = max |gpu - oracle| / max |oracle|) are those of
 test_gpu_parity.py: 1e-12 for the FP64 velocities and the temperature
 deviation, 1e-11 for the FP64 pressure (its conditioning floor), 1e-5 for
-the mixed path; max |div u| 1e-10 (FP64) and 1e-6 (mixed).  The oracle runs
-on every host core.
+the mixed path (the pressure included on the headline workload); max |div u|
+1e-10 (FP64), 1e-6 (mixed) and 1e-7 on the mixed headline step.  The oracle
+runs on every host core.
 """
 import os
 
@@ -83,7 +84,7 @@ def test_headline_channel_fp64_and_mixed():
     e, et, md = out[0]
     assert max(e[:3]) < 1e-12 and e[3] < 1e-11 and et < 1e-12 and md < 1e-10, out[0]
     e, et, md = out[1]
-    assert max(e[:3]) < 1e-5 and et < 1e-5 and md < 1e-6, out[1]
+    assert max(e) < 1e-5 and et < 1e-5 and md < 1e-7, out[1]
     doms[1].close()
     o.step(9)
     s = doms[0].step(9)
