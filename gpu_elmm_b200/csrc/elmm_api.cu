@@ -283,7 +283,7 @@ struct BatchT {
     int cap_fwd = 1, cap_inv = 1;
   };
   std::vector<RegSet> xreg, yreg;
-  size_t smem_mom = (size_t)MomShape<T>::slots * SlotLayout<T, 5, 3>::BYTES;
+  size_t smem_mom = (size_t)MomShape<T>::slots * SlotLayout<T, 5, MomShape<T>::nnf>::BYTES;
   size_t smem_sgs = (size_t)kRingSlots * SlotLayout<T, 3, 0>::BYTES;
   int grid_cap[16] = {};
   // host-layout staging (double), max over domains of the largest host array
@@ -754,7 +754,7 @@ struct BatchT {
     {
       // tensor maps of the box fields for the plane rings (wide: tile plus
       // halo, narrow: tile alone), in field order F_U..F_PHI
-      typedef SlotLayout<T, 5, 3> Lay;
+      typedef SlotLayout<T, 5, MomShape<T>::nnf> Lay;
       std::vector<CUtensorMap> maps(2 * F_COUNT);
       for (int f = 0; f < F_COUNT; f++) {
         int r = encode_box_map(&maps[BOX_WIDE * F_COUNT + f], *fields[f], h.pitch, h.ny, h.nz, Lay::SPW, Lay::WROWS);
@@ -881,6 +881,15 @@ struct BatchT {
         if ((r = dalloc((void **)f, alloc_elems * sizeof(T)))) return r;
       h.Tm = sl.buf[0];
       h.Tadv = sl.adv;
+      if (MomShape<T>::nnf == 4) {  // the temperature's planes for the momentum ring
+        std::vector<CUtensorMap> tm(3);
+        for (int b2 = 0; b2 < 3; b2++)
+          if ((r = encode_box_map(&tm[b2], sl.buf[b2], h.pitch, h.ny, h.nz, MX, MY))) return r;
+        void *p;
+        if ((r = dalloc(&p, tm.size() * sizeof(CUtensorMap)))) return r;
+        CU(cudaMemcpy(p, tm.data(), tm.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
+        h.tmapT = p;
+      }
       for (int s2 = 0; s2 < 6; s2++) sl.bt[s2] = c.TempBtype[s2];
       sl.off = h.toff;
       h.tdiff_live = 1;

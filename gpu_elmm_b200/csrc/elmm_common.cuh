@@ -128,6 +128,7 @@ struct Dom {
   unsigned long long *cfl_bits;
   int *flags;            // [0]: NaN seen, [1]: a bounded wait gave up
   const void *tmaps;     // CUtensorMap[2][F_COUNT] (device memory, 64-byte aligned)
+  const void *tmapT;     // FP32 with buoyancy: CUtensorMap[3], narrow boxes of the temperature's value buffers
   // defect correction of the mixed path
   int *refine_flag;      // 1: the next correction sweep runs for this domain
   int *refine_count;     // sweeps run since the counter was reset

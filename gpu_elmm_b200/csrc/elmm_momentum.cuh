@@ -440,25 +440,51 @@ __device__ __forceinline__ void issue_plane(T *slot, uint64_t *bar, const CUtens
   }
 }
 
+// The momentum kernel's planes: U, V, W, Viscosity, P wide; the old Ustar,
+// Vstar, Wstar narrow (stages 2 and 3), and on the FP32 path also the
+// potential temperature of the stage as a fourth narrow field (buoyancy),
+// from its own tensor maps (tmapT: one per value buffer).
+template <typename T, int NNF>
+__device__ __forceinline__ void issue_mom_plane(T *slot, uint64_t *bar, const CUtensorMap *maps,
+                                                const CUtensorMap *tmapT, bool with_star, int aln, int i0, int j0,
+                                                int kk) {
+  typedef SlotLayout<T, 5, NNF> Lay;
+  const uint32_t bytes = 5 * Lay::WBOX + (with_star ? 3 * Lay::NBOX : 0u) + (tmapT ? Lay::NBOX : 0u);
+  mbar_expect_tx(bar, bytes);
+  const int xw = aln - 1 + i0 - Lay::XO, xn = aln - 1 + i0;
+  const int wide[5] = {F_U, F_V, F_W, F_NU, F_P};
+#pragma unroll
+  for (int f = 0; f < 5; f++) tma_load_3d(slot + f * Lay::WB, maps + BOX_WIDE * F_COUNT + wide[f], xw, j0 - 1, kk, bar);
+  if (with_star) {
+#pragma unroll
+    for (int f = 0; f < 3; f++)
+      tma_load_3d(slot + Lay::WIDE + f * Lay::NB, maps + BOX_NARROW * F_COUNT + F_US + f, xn, j0, kk, bar);
+  }
+  if (NNF == 4 && tmapT) tma_load_3d(slot + Lay::WIDE + 3 * Lay::NB, tmapT, xn, j0, kk, bar);
+}
+
 constexpr int kRingSlots = 5;
 
 // Cells per thread along x and ring slots of the momentum kernel: FP32
 // threads compute two x-adjacent cells with packed FP32x2 arithmetic
 // (elmm_packed.cuh); a four-slot ring leaves room for four 128-thread blocks
 // per SM.  FP64 keeps one cell per thread and five slots.
+// nnf: narrow fields per slot (FP32 adds the temperature; the FP64 slots
+// would not leave room for two blocks per SM and read it from global memory).
 template <typename T>
 struct MomShape {
-  static constexpr int cpt = 1, slots = 5, threads = MX * MY, min_blocks = 2;
+  static constexpr int cpt = 1, slots = 5, threads = MX * MY, min_blocks = 2, nnf = 3;
 };
 template <>
 struct MomShape<float> {
-  static constexpr int cpt = 2, slots = 4, threads = MX * MY / 2, min_blocks = 4;
+  static constexpr int cpt = 2, slots = 4, threads = MX * MY / 2, min_blocks = 4, nnf = 4;
 };
 
 template <typename T>
 __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
     k_momentum(const Dom<T> *__restrict__ doms, Launch L, StageCoef sc) {
-  typedef SlotLayout<T, 5, 3> Lay;
+  constexpr int NNF = MomShape<T>::nnf;
+  typedef SlotLayout<T, 5, NNF> Lay;
   constexpr int CPT = MomShape<T>::cpt, NSL = MomShape<T>::slots, TXN = MX / CPT;
   extern __shared__ __align__(128) unsigned char dyn_smem[];
   T *ring = reinterpret_cast<T *>(dyn_smem);
@@ -494,9 +520,11 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
     const int nx = d.nx, ny = d.ny;
     const long long plane = d.plane;
     const bool stage1 = sc.stage == 1;
-    const int wide[5] = {F_U, F_V, F_W, F_NU, F_P};
-    const int narrow[3] = {F_US, F_VS, F_WS};
     const CUtensorMap *maps = reinterpret_cast<const CUtensorMap *>(d.tmaps);
+    // the temperature of the stage start through the ring (FP32 with buoyancy)
+    const CUtensorMap *tmapT = (NNF == 4 && d.buoy && d.tmapT)
+                                   ? reinterpret_cast<const CUtensorMap *>(d.tmapT) + (sc.stage - 1) % 3
+                                   : nullptr;
     __syncthreads();  // every slot and the context of the previous tile are free
     if (threadIdx.x == 0) fill_ctx(ctx, d);
     if constexpr (sizeof(T) == 4) {
@@ -508,8 +536,8 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
     if (threadIdx.x == 0) {
       fence_async_shared();
       for (int kk = k0 - 1; kk <= min(k0 - 1 + NSL - 1, k1 + 1); kk++)
-        issue_plane<T, 5, 3>(ring + (kk % NSL) * Lay::SIZE, &bars[kk % NSL], maps, wide, narrow, !stage1, d.aln, i0,
-                             j0, kk);
+        issue_mom_plane<T, NNF>(ring + (kk % NSL) * Lay::SIZE, &bars[kk % NSL], maps, tmapT, !stage1, d.aln, i0, j0,
+                                kk);
     }
     __syncthreads();  // the context is written
     const T dt = (T)d.dt, rdt = (T)sc.rho, bdt = (T)sc.beta;
@@ -588,9 +616,11 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
           const F2 mm = bc2(m);
           const F2 p0 = R2.g(4, 0, 0, 0) - mm;
           F2 btp = bc2(0.f);
-          if (buoy)
-            btp = bc2(bA2) * (F2{*reinterpret_cast<const float2 *>(Tm + c + plane)} +
-                              F2{*reinterpret_cast<const float2 *>(Tm + c)});
+          if (buoy) {
+            const int ot = Lay::WIDE + 3 * Lay::NB + ty * MX + CPT * tx;  // the temperature, narrow field 3
+            btp = bc2(bA2) * (F2{*reinterpret_cast<const float2 *>(p2s + ot)} +
+                              F2{*reinterpret_cast<const float2 *>(p1s + ot)});
+          }
           F2 tu, tv, tw;
           F2 gz2 = bc2(gz);
           if (!vz) {
@@ -651,7 +681,14 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
           const bool doV = iq <= d.ext[1][0] && j <= d.ext[1][1] && k <= kV;
           const bool doW = iq <= d.ext[2][0] && j <= d.ext[2][1] && k <= kW;
           T bt = (T)0;
-          if (buoy && doW) bt = bA2 * (ld(Tm, cq + plane) + ld(Tm, cq));
+          if (buoy && doW) {
+            if constexpr (NNF == 4) {  // the temperature of planes k+1 and k from the ring
+              const int ot = Lay::WIDE + 3 * Lay::NB + ty * MX + CPT * tx + q;
+              bt = bA2 * (p2s[ot] + p1s[ot]);
+            } else {
+              bt = bA2 * (ld(Tm, cq + plane) + ld(Tm, cq));
+            }
+          }
           T tu, tv, tw;
           if constexpr (sizeof(T) == 4) {
             // mixed path: the deviation forms of tendency_dev plus the wall
@@ -725,8 +762,8 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
       const int kn = k - 1 + NSL;
       if (threadIdx.x == 0 && kn <= k1 + 1) {
         fence_async_shared();
-        issue_plane<T, 5, 3>(ring + (kn % NSL) * Lay::SIZE, &bars[kn % NSL], maps, wide, narrow, !stage1, d.aln, i0,
-                             j0, kn);
+        issue_mom_plane<T, NNF>(ring + (kn % NSL) * Lay::SIZE, &bars[kn % NSL], maps, tmapT, !stage1, d.aln, i0, j0,
+                                kn);
       }
       c += plane;
     }
