@@ -297,6 +297,10 @@ struct BatchT {
   cudaEvent_t ev_pr = nullptr;      // the host copy of Pr into its image has landed
   std::vector<double *> pr_image;  // per domain: last host Pr image (device)
   int *dbad = nullptr;
+  // single-precision host arrays (the *_float entry points): hostf is set for
+  // the duration of such a call; fstage holds the floats on the device
+  int hostf = 0;
+  float *fstage = nullptr;
   cudaGraphExec_t step_exec = nullptr;
   bool step_has_cfl = false;
   double time = 0;
@@ -357,6 +361,41 @@ struct BatchT {
     if (solids_on(d)) cudaMemsetAsync(off, 0, sizeof(float) * (h.nz + 2), stream);
     else k_level_offsets<T><<<h.nz + 2, 256, 0, stream>>>(ddom + d, stg, hb, c, h.voff);
     return off;
+  }
+  // One host-layout array of n elements into the double staging buffer stg
+  // on stream st: a double host array is copied as it is, a float one (hostf)
+  // through fstage and widened.
+  int h2d(double *stg, const void *host, size_t n, cudaStream_t st) {
+    if (!hostf) {
+      CU(cudaMemcpyAsync(stg, host, n * sizeof(double), cudaMemcpyHostToDevice, st));
+      return ELMM_OK;
+    }
+    int r = ensure_fstage();
+    if (r) return r;
+    CU(cudaMemcpyAsync(fstage, host, n * sizeof(float), cudaMemcpyHostToDevice, st));
+    k_widen<<<kPackBlocks, 256, 0, st>>>(stg, fstage, (long long)n);
+    return ELMM_OK;
+  }
+  // the staged double array back to a host array of the call's type
+  int d2h(void *host, const double *stg, size_t n, cudaStream_t st) {
+    if (!hostf) {
+      CU(cudaMemcpyAsync(host, stg, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+      return ELMM_OK;
+    }
+    int r = ensure_fstage();
+    if (r) return r;
+    k_narrow<<<kPackBlocks, 256, 0, st>>>(fstage, stg, (long long)n);
+    CU(cudaMemcpyAsync(host, fstage, n * sizeof(float), cudaMemcpyDeviceToHost, st));
+    return ELMM_OK;
+  }
+  int ensure_fstage() {
+    if (fstage) return ELMM_OK;
+    size_t n = stage_elems;
+    for (int d = 0; d < nd; d++) {  // the Pr image and the Poisson arrays fit the velocity boxes' staging
+      const size_t pe = (size_t)(hdom[d].nx + 4) * (hdom[d].ny + 4) * (hdom[d].nz + 4);
+      n = std::max(n, pe);
+    }
+    return dalloc((void **)&fstage, n * sizeof(float));
   }
   // the offsets the pack of velocity component comp of domain d adds back, or null
   const float *pack_offsets(int d, int comp) const {
@@ -1834,16 +1873,16 @@ struct BatchT {
     return download_all(0, U, V, W, Pr, Th);
   }
 
-  int upload(int d, const double *U, const double *V, const double *W, const double *Pr) {
+  int upload(int d, const void *U, const void *V, const void *W, const void *Pr) {
     if (d < 0 || d >= nd) return fail(ELMM_ERR_INVALID_ARG, "domain index");
     if (!U || !V || !W) return fail(ELMM_ERR_INVALID_ARG, "NULL velocity array");
     CU(cudaSetDevice(device));
     if (frame_pending) CU(cudaStreamWaitEvent(stream, ev_packed, 0));
     const Dom<T> &h = hdom[d];
     CU(cudaMemsetAsync(dbad, 0, sizeof(int), stream));
-    const double *src[3] = {U, V, W};
+    const void *src[3] = {U, V, W};
     T *dst[3] = {h.U, h.V, h.W};
-    const bool two = two_stages();
+    const bool two = !hostf && two_stages();
     for (int c = 0; c < 3; c++) {
       HostBox hb = hbox_vel(d, c);
       size_t n = (size_t)hb.n0 * hb.n1 * hb.n2;
@@ -1856,7 +1895,8 @@ struct BatchT {
         CU(cudaEventRecord(ev_stage[b][0], side));
         CU(cudaStreamWaitEvent(stream, ev_stage[b][0], 0));
       } else {
-        CU(cudaMemcpyAsync(stg, src[c], n * sizeof(double), cudaMemcpyHostToDevice, stream));
+        int r = h2d(stg, src[c], n, stream);
+        if (r) return r;
       }
       const float *off = stage_offsets(d, c, stg, hb);
       k_unpack<T><<<kPackBlocks, 256, 0, stream>>>(ddom + d, dst[c], stg, hb, h.ext[c][0], h.ext[c][1], h.ext[c][2], dbad,
@@ -1867,7 +1907,8 @@ struct BatchT {
     HostBox hp = hbox_p(d);
     size_t np = (size_t)hp.n0 * hp.n1 * hp.n2;
     if (Pr) {
-      CU(cudaMemcpyAsync(pr_image[d], Pr, np * sizeof(double), cudaMemcpyHostToDevice, stream));
+      int r = h2d(pr_image[d], Pr, np, stream);
+      if (r) return r;
       k_unpack<T><<<kPackBlocks, 256, 0, stream>>>(ddom + d, h.P, pr_image[d], hp, h.nx, h.ny, h.nz, dbad);
     } else {
       CU(cudaMemsetAsync(pr_image[d], 0, np * sizeof(double), stream));
@@ -1883,7 +1924,7 @@ struct BatchT {
     return ELMM_OK;
   }
 
-  int upload_temperature(int d, const double *Th) {
+  int upload_temperature(int d, const void *Th) {
     if (d < 0 || d >= nd) return fail(ELMM_ERR_INVALID_ARG, "domain index");
     if (!Th) return fail(ELMM_ERR_INVALID_ARG, "NULL temperature array");
     if (!hdom[d].buoy) return fail(ELMM_ERR_INVALID_ARG, "no temperature field (enable_buoyancy is 0)");
@@ -1892,7 +1933,7 @@ struct BatchT {
     const Dom<T> &h = hdom[d];
     const size_t n = (size_t)(h.nx + 6) * (h.ny + 6) * (h.nz + 6);
     CU(cudaMemsetAsync(dbad, 0, sizeof(int), stream));
-    CU(cudaMemcpyAsync(dstage, Th, n * sizeof(double), cudaMemcpyHostToDevice, stream));
+    if (int r = h2d(dstage, Th, n, stream)) return r;
     k_unpack_scalar<T><<<kPackBlocks, 256, 0, stream>>>(ddom + d, 0, dstage, dbad);
     int bad = 0;
     CU(cudaMemcpyAsync(&bad, dbad, sizeof(int), cudaMemcpyDeviceToHost, stream));
@@ -1902,7 +1943,7 @@ struct BatchT {
     return ELMM_OK;
   }
 
-  int upload_scalar(int d, int sc, const double *S) {
+  int upload_scalar(int d, int sc, const void *S) {
     if (d < 0 || d >= nd) return fail(ELMM_ERR_INVALID_ARG, "domain index");
     if (!S) return fail(ELMM_ERR_INVALID_ARG, "NULL scalar array");
     if (sc < 1 || sc > cfg[d].num_scalars) return fail(ELMM_ERR_INVALID_ARG, "scalar number outside 1..num_scalars");
@@ -1911,7 +1952,7 @@ struct BatchT {
     const Dom<T> &h = hdom[d];
     const size_t n = (size_t)(h.nx + 6) * (h.ny + 6) * (h.nz + 6);
     CU(cudaMemsetAsync(dbad, 0, sizeof(int), stream));
-    CU(cudaMemcpyAsync(dstage, S, n * sizeof(double), cudaMemcpyHostToDevice, stream));
+    if (int r = h2d(dstage, S, n, stream)) return r;
     k_unpack_scalar<T><<<kPackBlocks, 256, 0, stream>>>(ddom + d, (h.buoy ? 1 : 0) + sc - 1, dstage, dbad);
     int bad = 0;
     CU(cudaMemcpyAsync(&bad, dbad, sizeof(int), cudaMemcpyDeviceToHost, stream));
@@ -2007,7 +2048,7 @@ struct BatchT {
     return 0;
   }
 
-  int download_field(int d, int field, double *host) {
+  int download_field(int d, int field, void *host) {
     if (d < 0 || d >= nd) return fail(ELMM_ERR_INVALID_ARG, "domain index");
     const int nsc = cfg[d].num_scalars;
     const bool scal = (field >= ELMM_FIELD_SCALAR && field < ELMM_FIELD_SCALAR + nsc) ||
@@ -2020,17 +2061,17 @@ struct BatchT {
     if (!host) return fail(ELMM_ERR_INVALID_ARG, "NULL host array");
     CU(cudaSetDevice(device));
     size_t n = pack(d, field, dstage, stream);
-    CU(cudaMemcpyAsync(host, dstage, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    if (int r = d2h(host, dstage, n, stream)) return r;
     CU(cudaStreamSynchronize(stream));
     CU(cudaGetLastError());
     return ELMM_OK;
   }
 
-  int download(int d, double *U, double *V, double *W, double *Pr) {
-    double *dst[4] = {U, V, W, Pr};
+  int download(int d, void *U, void *V, void *W, void *Pr) {
+    void *dst[4] = {U, V, W, Pr};
     if (d < 0 || d >= nd) return fail(ELMM_ERR_INVALID_ARG, "domain index");
     CU(cudaSetDevice(device));
-    if (!two_stages()) {
+    if (hostf || !two_stages()) {
       for (int f = 0; f < 4; f++)
         if (dst[f]) {
           int r = download_field(d, f, dst[f]);
@@ -2141,22 +2182,23 @@ static int batch_init(elmm_batch &B, const elmm_config *cfgs, int n) {
   return r;
 }
 
+// Phi and RHS are double host arrays, or float ones when B.hostf is set
 template <typename T>
-static int poisson_exec(BatchT<T> &B, double *Phi, const double *RHS) {
+static int poisson_exec(BatchT<T> &B, void *Phi, const void *RHS) {
   CU(cudaSetDevice(B.device));
   const Dom<T> &h = B.hdom[0];
   // RHS(0:n+1)^3 -> box field (Phi is free until the inverse transform) -> transforms
   HostBox hb{0, h.nx + 2, h.ny + 2, h.nz + 2};
   size_t n = (size_t)hb.n0 * hb.n1 * hb.n2;
-  CU(cudaMemcpyAsync(B.dstage, RHS, n * sizeof(double), cudaMemcpyHostToDevice, B.stream));
+  if (int r = B.h2d(B.dstage, RHS, n, B.stream)) return r;
   CU(cudaMemsetAsync(B.dbad, 0, sizeof(int), B.stream));
   k_unpack<T><<<kPackBlocks, 256, 0, B.stream>>>(B.ddom, h.Phi, B.dstage, hb, h.nx, h.ny, h.nz, B.dbad);
   B.launch_poisson(1.0, 0, 1, 0);
   HostBox hp = B.hbox_p(0);
   size_t np = (size_t)hp.n0 * hp.n1 * hp.n2;
-  CU(cudaMemcpyAsync(B.dstage, Phi, np * sizeof(double), cudaMemcpyHostToDevice, B.stream));
+  if (int r = B.h2d(B.dstage, Phi, np, B.stream)) return r;  // the host's ghosts stay as they are
   k_pack_scalar<T><<<kPackBlocks, 256, 0, B.stream>>>(B.ddom, h.Phi, B.dstage, hp, 0, 0, h.nx, h.ny, h.nz);
-  CU(cudaMemcpyAsync(Phi, B.dstage, np * sizeof(double), cudaMemcpyDeviceToHost, B.stream));
+  if (int r = B.d2h(Phi, B.dstage, np, B.stream)) return r;
   CU(cudaStreamSynchronize(B.stream));
   CU(cudaGetLastError());
   int bad = 0;
@@ -2165,6 +2207,22 @@ static int poisson_exec(BatchT<T> &B, double *Phi, const double *RHS) {
   return ELMM_OK;
 }
 
+
+// Runs f on the batch with its host arrays taken as float (the *_float entry
+// points of a single-precision host).
+template <typename F>
+static int with_float_host(elmm_batch &B, F f) {
+  if (B.precision == ELMM_PREC_MIXED) {
+    B.b32->hostf = 1;
+    const int r = f(*B.b32);
+    B.b32->hostf = 0;
+    return r;
+  }
+  B.b64->hostf = 1;
+  const int r = f(*B.b64);
+  B.b64->hostf = 0;
+  return r;
+}
 
 #include "elmm_server.inl"
 
@@ -2275,6 +2333,45 @@ int elmm_march_host(elmm_handle *h, double *U, double *V, double *W, double *Pr,
   if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
   if (nsteps < 0) return fail(ELMM_ERR_INVALID_ARG, "nsteps < 0");
   return DISPATCH(h->b, march_host(U, V, W, Pr, Temperature, nsteps, stats));
+}
+
+int elmm_upload_state_float(elmm_handle *h, const float *U, const float *V, const float *W, const float *Pr) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  return with_float_host(h->b, [&](auto &b) { return b.upload(0, U, V, W, Pr); });
+}
+
+int elmm_download_state_float(elmm_handle *h, float *U, float *V, float *W, float *Pr) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  return with_float_host(h->b, [&](auto &b) { return b.download(0, U, V, W, Pr); });
+}
+
+int elmm_download_field_float(elmm_handle *h, int32_t field, float *host) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  return with_float_host(h->b, [&](auto &b) { return b.download_field(0, field, host); });
+}
+
+int elmm_upload_temperature_float(elmm_handle *h, const float *T) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  return with_float_host(h->b, [&](auto &b) { return b.upload_temperature(0, T); });
+}
+
+int elmm_upload_scalar_float(elmm_handle *h, int32_t sc, const float *S) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  return with_float_host(h->b, [&](auto &b) { return b.upload_scalar(0, sc, S); });
+}
+
+int elmm_march_host_float(elmm_handle *h, float *U, float *V, float *W, float *Pr, float *Temperature, int32_t nsteps,
+                          elmm_stats *stats) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  if (nsteps < 0) return fail(ELMM_ERR_INVALID_ARG, "nsteps < 0");
+  return with_float_host(h->b, [&](auto &b) {
+    int r = b.upload(0, U, V, W, Pr);
+    if (!r && Temperature) r = b.upload_temperature(0, Temperature);
+    if (!r) r = b.step(nsteps, stats);
+    if (!r) r = b.download(0, U, V, W, Pr);
+    if (!r && Temperature) r = b.download_field(0, ELMM_FIELD_TEMPERATURE, Temperature);
+    return r;
+  });
 }
 
 int elmm_set_puffs(elmm_handle *h, const elmm_puff *puffs, int32_t npuffs, const elmm_puff_volume *volumes,
@@ -2505,6 +2602,30 @@ int elmm_poisson_solver_finalize(elmm_poisson *s) {
   delete s;
   return ELMM_OK;
 }
+
+// ---- single-precision host arrays (prec=sp hosts) -------------------------
+int elmm_poisson_solver_new_float(elmm_poisson **out, const int32_t n[3], const float L[3], const int32_t bcs[6],
+                                  int32_t precision, int32_t device) {
+  if (!L) return fail(ELMM_ERR_INVALID_ARG, "NULL L");
+  return poisson_new(out, n, (double)L[0], (double)L[1], nullptr, (double)L[2], bcs, precision, device);
+}
+
+int elmm_poisson_solver_nonuniform_z_new_float(elmm_poisson **out, const int32_t n[3], const float Lxy[2],
+                                               const float *zPr, const float *zW, const int32_t bcs[6],
+                                               int32_t precision, int32_t device) {
+  (void)zPr;  // zPr(k) = (zW(k-1) + zW(k)) / 2 is recomputed from zW
+  if (!Lxy || !zW || !n) return fail(ELMM_ERR_INVALID_ARG, "NULL grid");
+  if (n[2] < 1) return fail(ELMM_ERR_INVALID_CONFIG, "nz < 1");
+  std::vector<double> zw(zW, zW + n[2] + 1);
+  return poisson_new(out, n, (double)Lxy[0], (double)Lxy[1], zw.data(), 0.0, bcs, precision, device);
+}
+
+int elmm_poisson_solver_execute_float(elmm_poisson *s, float *Phi, const float *RHS) {
+  if (!s || !Phi || !RHS) return fail(ELMM_ERR_INVALID_ARG, "NULL argument");
+  return with_float_host(s->b, [&](auto &b) { return poisson_exec(b, Phi, RHS); });
+}
+
+int elmm_poisson_solver_finalize_float(elmm_poisson *s) { return elmm_poisson_solver_finalize(s); }
 
 }  // extern "C"
 

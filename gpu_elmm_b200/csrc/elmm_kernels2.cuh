@@ -720,6 +720,19 @@ __global__ void __launch_bounds__(256) k_level_offsets(const Dom<T> *__restrict_
   }
 }
 
+// Host arrays of a single-precision host (the reference's default prec=sp
+// build): widened to double in a staging buffer on the way in, narrowed
+// (round to nearest) on the way out, so every pack and unpack kernel keeps
+// its double host layout.
+__global__ void k_widen(double *dst, const float *__restrict__ src, long long n) {
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n; w += (long long)gridDim.x * blockDim.x)
+    dst[w] = (double)src[w];
+}
+__global__ void k_narrow(float *dst, const double *__restrict__ src, long long n) {
+  for (long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x; w < n; w += (long long)gridDim.x * blockDim.x)
+    dst[w] = (float)src[w];
+}
+
 // ghost shell of a velocity component from its interior (BoundUVW rules)
 template <typename T>
 __global__ void k_halo_vel(const Dom<T> *__restrict__ dom, int comp) {

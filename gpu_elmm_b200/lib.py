@@ -82,6 +82,19 @@ def lib():
         L.elmm_batch_step.argtypes = [P, C.c_int32, C.POINTER(ElmmStats)]
         L.elmm_batch_cells.argtypes = [P]
         L.elmm_batch_cells.restype = C.c_int64
+        fp = C.POINTER(C.c_float)
+        L.elmm_upload_state_float.argtypes = [P, fp, fp, fp, fp]
+        L.elmm_download_state_float.argtypes = [P, fp, fp, fp, fp]
+        L.elmm_download_field_float.argtypes = [P, C.c_int32, fp]
+        L.elmm_upload_temperature_float.argtypes = [P, fp]
+        L.elmm_upload_scalar_float.argtypes = [P, C.c_int32, fp]
+        L.elmm_march_host_float.argtypes = [P, fp, fp, fp, fp, fp, C.c_int32, C.POINTER(ElmmStats)]
+        L.elmm_poisson_solver_new_float.argtypes = [C.POINTER(P), C.POINTER(C.c_int32), fp, C.POINTER(C.c_int32),
+                                                    C.c_int32, C.c_int32]
+        L.elmm_poisson_solver_nonuniform_z_new_float.argtypes = [C.POINTER(P), C.POINTER(C.c_int32), fp, fp, fp,
+                                                                 C.POINTER(C.c_int32), C.c_int32, C.c_int32]
+        L.elmm_poisson_solver_execute_float.argtypes = [P, fp, fp]
+        L.elmm_poisson_solver_finalize_float.argtypes = [P]
         _lib = L
     return _lib
 
@@ -96,6 +109,14 @@ def ptr(a):
         return None
     assert isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous, "host arrays: C-contiguous float64"
     return a.ctypes.data_as(_dp)
+
+
+def fptr(a):
+    """A float32 host array (the *_float entry points of a single-precision host)."""
+    if a is None:
+        return None
+    assert isinstance(a, np.ndarray) and a.dtype == np.float32 and a.flags.c_contiguous, "host arrays: C-contiguous float32"
+    return a.ctypes.data_as(C.POINTER(C.c_float))
 
 
 class Domain:
@@ -124,13 +145,17 @@ class Domain:
         check(lib().elmm_download_state(self.h, ptr(U), ptr(V), ptr(W), ptr(Pr)), "elmm_download_state")
         return U, V, W, Pr
 
-    def field(self, fid: int, out=None):
+    def field_shape(self, fid: int):
+        """Host shape of field fid (ELMM_FIELD_*)."""
         g = self.grid
         shape = {0: g.shape_u(), 5: g.shape_u(), 8: g.shape_u(), 1: g.shape_v(), 6: g.shape_v(), 9: g.shape_v(),
                  2: g.shape_w(), 7: g.shape_w(), 10: g.shape_w(), 12: g.shape_t(), 14: g.shape_t()}.get(fid, g.shape_p())
         if FIELD_SCALAR <= fid < FIELD_SCALAR_ADV + MAX_SCALARS:
             shape = g.shape_t()
-        a = np.zeros(shape) if out is None else out
+        return shape
+
+    def field(self, fid: int, out=None):
+        a = np.zeros(self.field_shape(fid)) if out is None else out
         check(lib().elmm_download_field(self.h, fid, ptr(a)), "elmm_download_field")
         return a
 
@@ -147,6 +172,31 @@ class Domain:
         st = ElmmStats()
         check(lib().elmm_march_host(self.h, ptr(U), ptr(V), ptr(W), ptr(Pr), ptr(T), n, C.byref(st)),
               "elmm_march_host")
+        return st
+
+    # single-precision host arrays (a host built with prec=sp): float32 arrays
+    # in the same layouts
+    def upload_f32(self, U, V, W, Pr=None):
+        check(lib().elmm_upload_state_float(self.h, fptr(U), fptr(V), fptr(W), fptr(Pr)), "elmm_upload_state_float")
+
+    def download_f32(self):
+        g = self.grid
+        out = [np.zeros(s, dtype=np.float32) for s in (g.shape_u(), g.shape_v(), g.shape_w(), g.shape_p())]
+        check(lib().elmm_download_state_float(self.h, *[fptr(a) for a in out]), "elmm_download_state_float")
+        return tuple(out)
+
+    def field_f32(self, fid):
+        a = np.zeros(self.field_shape(fid), dtype=np.float32)
+        check(lib().elmm_download_field_float(self.h, fid, fptr(a)), "elmm_download_field_float")
+        return a
+
+    def upload_temperature_f32(self, T):
+        check(lib().elmm_upload_temperature_float(self.h, fptr(T)), "elmm_upload_temperature_float")
+
+    def march_host_f32(self, U, V, W, Pr, T=None, n=1) -> ElmmStats:
+        st = ElmmStats()
+        check(lib().elmm_march_host_float(self.h, fptr(U), fptr(V), fptr(W), fptr(Pr), fptr(T), n, C.byref(st)),
+              "elmm_march_host_float")
         return st
 
     def set_puffs(self, puffs, volumes):
@@ -295,14 +345,30 @@ class Batch:
 
 
 class PoissonSolver:
-    """The PoisSolver-compatible solver (poisson_solver_new/_execute/_finalize)."""
+    """The PoisSolver-compatible solver (poisson_solver_new/_execute/_finalize);
+    host_f32=True: the *_float variants of a single-precision host (float32
+    lengths, grid and arrays)."""
 
-    def __init__(self, n, L=None, bcs=(3, 3, 3, 3, 5, 5), precision=0, device=0, zW=None):
+    def __init__(self, n, L=None, bcs=(3, 3, 3, 3, 5, 5), precision=0, device=0, zW=None, host_f32=False):
         self.n = tuple(int(x) for x in n)
+        self.f32 = host_f32
         nn = (C.c_int32 * 3)(*self.n)
         bb = (C.c_int32 * 6)(*bcs)
         h = C.c_void_p()
-        if zW is None:
+        if host_f32:
+            if zW is None:
+                LL = (C.c_float * 3)(*L)
+                check(lib().elmm_poisson_solver_new_float(C.byref(h), nn, LL, bb, precision, device),
+                      "poisson_solver_new_float")
+            else:
+                zW = np.ascontiguousarray(zW, dtype=np.float32)
+                zPr = ((zW[:-1] + zW[1:]) / 2).astype(np.float32)
+                self._keep = (zW, zPr)
+                Lxy = (C.c_float * 2)(L[0], L[1])
+                check(lib().elmm_poisson_solver_nonuniform_z_new_float(C.byref(h), nn, Lxy, fptr(zPr), fptr(zW), bb,
+                                                                       precision, device),
+                      "poisson_solver_nonuniform_z_new_float")
+        elif zW is None:
             LL = (C.c_double * 3)(*L)
             check(lib().elmm_poisson_solver_new(C.byref(h), nn, LL, bb, precision, device), "poisson_solver_new")
         else:
@@ -315,7 +381,10 @@ class PoissonSolver:
         self.h = h
 
     def execute(self, Phi, RHS):
-        check(lib().elmm_poisson_solver_execute(self.h, ptr(Phi), ptr(RHS)), "poisson_solver_execute")
+        if self.f32:
+            check(lib().elmm_poisson_solver_execute_float(self.h, fptr(Phi), fptr(RHS)), "poisson_solver_execute_float")
+        else:
+            check(lib().elmm_poisson_solver_execute(self.h, ptr(Phi), ptr(RHS)), "poisson_solver_execute")
         return Phi
 
     def close(self):

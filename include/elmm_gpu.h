@@ -341,6 +341,24 @@ int elmm_step(elmm_handle *h, int32_t nsteps, elmm_stats *stats);
 int elmm_march_host(elmm_handle *h, double *U, double *V, double *W, double *Pr, double *Temperature,
                     int32_t nsteps, elmm_stats *stats);
 
+/* ---- single-precision host arrays ------------------------------------------
+ * The reference's default release build is single precision: make_release
+ * passes prec=sp (src/make_release:2), so knd = real32 (src/parameters.f90:
+ * 17-21) and the host's U, V, W, Pr, Temperature, Scalar, Phi and RHS are
+ * real32.  These entry points take float host arrays in the same layouts as
+ * their double counterparts above; the library widens them on the way in
+ * and rounds to nearest on the way out.  The device keeps the handle's own
+ * precision (ELMM_PREC_*).  Same checks and status codes as the double
+ * versions; elmm_march_host_float copies field by field (no overlap of the
+ * copies). */
+int elmm_upload_state_float(elmm_handle *h, const float *U, const float *V, const float *W, const float *Pr);
+int elmm_download_state_float(elmm_handle *h, float *U, float *V, float *W, float *Pr);
+int elmm_download_field_float(elmm_handle *h, int32_t field, float *host);
+int elmm_upload_temperature_float(elmm_handle *h, const float *T);
+int elmm_upload_scalar_float(elmm_handle *h, int32_t sc, const float *S);
+int elmm_march_host_float(elmm_handle *h, float *U, float *V, float *W, float *Pr, float *Temperature,
+                          int32_t nsteps, elmm_stats *stats);
+
 /* One RK3 stage up to a stop point, for operator-level checks:
  *   stop = 1: after SubgridStresses (Viscosity, wall-model fluxes)
  *   stop = 2: after Convection + OtherTerms + BoundUVW (U2, Ustar)
@@ -379,6 +397,19 @@ int elmm_poisson_solver_nonuniform_z_new(elmm_poisson **out, const int32_t n[3],
  * interior RHS value is not finite (Phi then holds no solution). */
 int elmm_poisson_solver_execute(elmm_poisson *s, double *Phi, const double *RHS);
 int elmm_poisson_solver_finalize(elmm_poisson *s);
+/* The float variants that a prec=sp host binds (poisson_solver_new_float,
+ * poisson_solver_nonuniform_z_new_float, ..._execute_float,
+ * ..._finalize_float: src/poisson.f90:82-84, :152-154): lengths, zPr(1:nz),
+ * zW(0:nz), Phi and RHS are float host arrays with the bounds above.  The
+ * arithmetic is the solver's `precision`.  One solver handle serves both the
+ * uniform and the nonuniform-z execute and finalize calls. */
+int elmm_poisson_solver_new_float(elmm_poisson **out, const int32_t n[3], const float L[3], const int32_t bcs[6],
+                                  int32_t precision, int32_t device);
+int elmm_poisson_solver_nonuniform_z_new_float(elmm_poisson **out, const int32_t n[3], const float Lxy[2],
+                                               const float *zPr, const float *zW, const int32_t bcs[6],
+                                               int32_t precision, int32_t device);
+int elmm_poisson_solver_execute_float(elmm_poisson *s, float *Phi, const float *RHS);
+int elmm_poisson_solver_finalize_float(elmm_poisson *s);
 
 /*
  * No counterpart in the reference.  The solve of elmm_poisson_solver_execute
