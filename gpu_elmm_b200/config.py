@@ -11,7 +11,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-ABI_VERSION = 4
+ABI_VERSION = 5
 
 # Boundary-condition codes of src/parameters.f90:249-250.
 BC_NOSLIP, BC_FREESLIP, BC_PERIODIC, BC_DIRICHLET, BC_NEUMANN, BC_CONSTFLUX = 1, 2, 3, 4, 5, 6
@@ -82,6 +82,11 @@ class ElmmConfig(C.Structure):
         ("avg_slice_k", C.c_int32),
         ("avg_slice_j", C.c_int32),
         ("avg_weight", C.c_double),
+        ("variable_time_steps", C.c_int32),
+        ("reserved1", C.c_int32),
+        ("CFL", C.c_double),
+        ("dt_max", C.c_double),
+        ("end_time", C.c_double),
     ]
 
 
@@ -233,7 +238,8 @@ def make_config(Prnx, Prny, Prnz, *, btype=(BC_PERIODIC, BC_PERIODIC, BC_PERIODI
                 pr_gradient_x=None, pr_gradient_y=None, max_refine_sweeps=0,
                 refine_tol=1e-6, cfl_check=0, device=0, origin=(0.0, 0.0, 0.0), buoyancy=False,
                 temperature_ref=295.0, grav_acc=9.81, prandtl=0.7, num_scalars=0, point_sources=(),
-                avg_slice_k=0, avg_slice_j=0, avg_weight=0.0):
+                avg_slice_k=0, avg_slice_j=0, avg_weight=0.0, variable_dt=False, cfl=0.5, dt_max=None,
+                end_time=0.0):
     """Builds an ElmmConfig.  The wall model defaults to on when an SGS model
     is on (src/initial.f90:2782-2787).  ``zW`` (Prnz+1 values) selects the
     stretched-z grid; the array is kept alive on the returned struct.
@@ -241,7 +247,10 @@ def make_config(Prnx, Prny, Prnz, *, btype=(BC_PERIODIC, BC_PERIODIC, BC_PERIODI
     (zero-flux) bottom and top and periodic x and y; ``num_scalars`` passive
     scalars get the same boundary kinds.  ``point_sources``: (scalar_number,
     (x, y, z), flux) triples.  ``avg_slice_k`` / ``avg_slice_j`` select the
-    time-averaged slices, ``avg_weight`` the weight of one step."""
+    time-averaged slices, ``avg_weight`` the weight of one step.
+    ``variable_dt`` switches on the variable time steps of TimeStepLength
+    with target ``cfl``, longest step ``dt_max`` (default ``dt``) and, if
+    positive, ``end_time``."""
     c = ElmmConfig()
     c.abi_version = ABI_VERSION
     c.Prnx, c.Prny, c.Prnz = Prnx, Prny, Prnz
@@ -295,6 +304,10 @@ def make_config(Prnx, Prny, Prnz, *, btype=(BC_PERIODIC, BC_PERIODIC, BC_PERIODI
             c.point_sources[q].position[a] = pos[a]
         c.point_sources[q].flux = flux
     c.avg_slice_k, c.avg_slice_j, c.avg_weight = avg_slice_k, avg_slice_j, avg_weight
+    c.variable_time_steps = 1 if variable_dt else 0
+    c.CFL = cfl
+    c.dt_max = dt if dt_max is None else dt_max
+    c.end_time = end_time
     return c
 
 

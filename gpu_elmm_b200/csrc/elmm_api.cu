@@ -176,6 +176,9 @@ static int check_config(const elmm_config &c) {
     return fail(ELMM_ERR_INVALID_CONFIG, "spacings and dt must be positive");
   if (c.precision != ELMM_PREC_FP64 && c.precision != ELMM_PREC_MIXED)
     return fail(ELMM_ERR_INVALID_CONFIG, "unknown precision");
+  if (c.variable_time_steps &&
+      !(c.CFL > 0 && std::isfinite(c.CFL) && c.dt_max > 0 && std::isfinite(c.dt_max) && c.end_time >= 0))
+    return fail(ELMM_ERR_INVALID_CONFIG, "variable time steps need CFL > 0, dt_max > 0 and end_time >= 0");
   if (c.max_refine_sweeps < 0 || c.max_refine_sweeps > 3) return fail(ELMM_ERR_INVALID_CONFIG, "max_refine_sweeps in 0..3");
   if (c.wallmodeltype > 0 && c.molecular_viscosity <= 0) {
     for (int s = 0; s < 6; s++)
@@ -771,6 +774,11 @@ struct BatchT {
     h.dx = c.dxmin; h.dy = c.dymin; h.dz = g.dzmin;
     h.xmin = c.xmin; h.ymin = c.ymin;
     h.dt = c.dt;
+    h.dt0 = c.dt;
+    h.vdt = c.variable_time_steps ? 1 : 0;
+    h.cfl_target = c.CFL;
+    h.dt_max = c.dt_max;
+    h.end_time = c.end_time;
     h.nu_mol = c.molecular_viscosity;
     {
       const double dd[3] = {c.dxmin, c.dymin, g.dzmin};
@@ -973,7 +981,14 @@ struct BatchT {
     if ((r = dalloc((void **)&h.prpart, sizeof(double) * h.nprpart))) return r;
     if ((r = dalloc((void **)&h.maxdiv_bits, sizeof(unsigned long long)))) return r;
     if ((r = dalloc((void **)&h.cfl_bits, sizeof(unsigned long long)))) return r;
+    {
+      const double ts[2] = {0.0, c.dt};  // time 0, no step yet
+      if ((r = dalloc((void **)&h.tstate, sizeof(ts)))) return r;
+      CU(cudaMemcpy(h.tstate, ts, sizeof(ts), cudaMemcpyHostToDevice));
+    }
     if ((r = dalloc((void **)&h.flags, 4 * sizeof(int)))) return r;
+    h.wait_limit = kWaitLimit;
+    h.skip_plane = -1;
     if ((r = dalloc((void **)&h.refine_flag, sizeof(int)))) return r;
     if ((r = dalloc((void **)&h.refine_count, 2 * sizeof(int)))) return r;
     h.refine_tol = c.refine_tol;
@@ -1224,7 +1239,7 @@ struct BatchT {
         if (x.nwm > 0) {
           nlaunch++;
           k_ib_wm<T><<<std::min((x.nwm + 127) / 128, 148 * 8), 128, 0, stream>>>(ddom, d, x.wm, x.wm_ustar, x.nwm,
-                                                                               kBeta[stage - 1] * cfg[d].dt);
+                                                                               kBeta[stage - 1]);
         }
         if (x.nib > 0) {
           nlaunch++;
@@ -1263,6 +1278,12 @@ struct BatchT {
   }
   int enqueue_step(bool cfl, bool div) {
     if (cfl) launch_cfl();
+    bool vdt = false;
+    for (int d = 0; d < nd; d++) vdt |= hdom[d].vdt != 0;
+    if (vdt) {  // the variable steps' length, before any kernel reads dt
+      nlaunch++;
+      k_dt<T><<<(nd + 127) / 128, 128, 0, stream>>>(ddom, nd);
+    }
     bool puffs = false, clear = false;
     for (int d = 0; d < nd; d++) {
       puffs |= hdom[d].npuff > 0;
@@ -1596,6 +1617,20 @@ struct BatchT {
     return push_dom(d);
   }
   static double norm_host(const double *v) { return std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]); }
+  // elmm_set_fault_injection: the wait limit and the skipped plane of every
+  // domain (read by the kernels from the device descriptors, so the captured
+  // step graph stays valid)
+  int set_fault_injection(int wait_limit, int skip_plane) {
+    CU(cudaSetDevice(device));
+    CU(cudaStreamSynchronize(stream));
+    for (int d = 0; d < nd; d++) {
+      hdom[d].wait_limit = wait_limit;
+      hdom[d].skip_plane = skip_plane;
+      int r = push_dom(d);
+      if (r) return r;
+    }
+    return ELMM_OK;
+  }
   int push_dom(int d) {
     CU(cudaMemcpy(ddom + d, &hdom[d], sizeof(Dom<T>), cudaMemcpyHostToDevice));
     return ELMM_OK;
@@ -1611,7 +1646,7 @@ struct BatchT {
     }
     if (frame_pending) CU(cudaStreamWaitEvent(stream, ev_packed, 0));
     bool cfl = false;
-    for (auto &c : cfg) cfl |= c.enable_CFL_check != 0;
+    for (auto &c : cfg) cfl |= c.enable_CFL_check != 0 || c.variable_time_steps != 0;
     if (!step_exec || step_has_cfl != cfl) {
       if (step_exec) { cudaGraphExecDestroy(step_exec); step_exec = nullptr; }
       cudaGraph_t g;
@@ -1637,7 +1672,13 @@ struct BatchT {
   int step_finish(int nsteps, elmm_stats *st) {
     CU(cudaStreamSynchronize(stream));
     CU(cudaGetLastError());
-    time += nsteps * cfg[0].dt;
+    if (hdom[0].vdt) {  // the device clock of variable steps
+      double ts[2];
+      CU(cudaMemcpy(ts, hdom[0].tstate, sizeof(ts), cudaMemcpyDeviceToHost));
+      time = ts[0];
+    } else {
+      time += nsteps * cfg[0].dt;
+    }
     int r = fill_stats(st, nsteps);
     if (st) {
       st->kernels = nsteps * step_kernels;
@@ -1653,14 +1694,18 @@ struct BatchT {
   }
 
   int fill_stats(elmm_stats *st, int nsteps) {
-    double md = 0, cf = 0;
-    int gave_up = 0;
+    double md = 0, cf = 0, dt0 = cfg[0].dt;
+    int gave_up = 0, past_end = 0;
     for (int d = 0; d < nd; d++) {
-      int fl[2] = {0, 0};
+      int fl[3] = {0, 0, 0};
       CU(cudaMemcpy(fl, hdom[d].flags, sizeof(fl), cudaMemcpyDeviceToHost));
       if (fl[1]) {  // a bounded device-side wait gave up: report it once
         gave_up = 1;
         CU(cudaMemset(hdom[d].flags + 1, 0, sizeof(int)));
+      }
+      if (fl[2]) {  // a variable step started at end_time
+        past_end = 1;
+        CU(cudaMemset(hdom[d].flags + 2, 0, sizeof(int)));
       }
       unsigned long long b1 = 0, b2 = 0;
       CU(cudaMemcpy(&b1, hdom[d].maxdiv_bits, sizeof(b1), cudaMemcpyDeviceToHost));
@@ -1669,7 +1714,14 @@ struct BatchT {
       memcpy(&a, &b1, 8);
       memcpy(&c2, &b2, 8);
       if (!(a <= md)) md = a;
-      c2 = c2 * cfg[d].dt;
+      double dtd = cfg[d].dt;
+      if (hdom[d].vdt) {  // the length of the last variable step
+        double ts[2];
+        CU(cudaMemcpy(ts, hdom[d].tstate, sizeof(ts), cudaMemcpyDeviceToHost));
+        dtd = ts[1];
+        if (d == 0) dt0 = dtd;
+      }
+      c2 = c2 * dtd;
       if (!(c2 <= cf)) cf = c2;
     }
     float ms = 0;
@@ -1678,14 +1730,17 @@ struct BatchT {
       memset(st, 0, sizeof(*st));
       st->steps_done = nsteps;
       st->time = time;
-      st->dt = cfg[0].dt;
+      st->dt = dt0;
       st->cfl = cf;
       st->max_div = md;
       st->nan_detected = !std::isfinite(md) || !std::isfinite(cf);
       st->elapsed_ms = ms;
     }
-    if (!std::isfinite(md) || !std::isfinite(cf)) return fail(ELMM_ERR_NAN, "NaN or Inf in the velocity field");
     if (gave_up) return fail(ELMM_ERR_TIMEOUT, "a device-side wait for a plane copy gave up; the step is incomplete");
+    if (past_end)
+      return fail(ELMM_ERR_INVALID_ARG, "a variable time step started at end_time (the run was over; it took the "
+                                        "step length of its CFL limit)");
+    if (!std::isfinite(md) || !std::isfinite(cf)) return fail(ELMM_ERR_NAN, "NaN or Inf in the velocity field");
     return ELMM_OK;
   }
 
@@ -2241,6 +2296,8 @@ int elmm_config_defaults(elmm_config *c, int32_t Prnx, int32_t Prny, int32_t Prn
   memcpy(c->Btype, bt, sizeof(bt));
   c->dxmin = c->dymin = c->dzmin = 1.0;
   c->dt = 0.02;
+  c->CFL = 0.3;     // time_step_control%CFL (src/parameters.f90:110); used with variable steps
+  c->dt_max = 0.02;
   c->molecular_viscosity = 1.0 / 70000;
   c->C_Smagorinsky = 0.122;
   c->filter_ratio = 1.0;
@@ -2333,6 +2390,12 @@ int elmm_march_host(elmm_handle *h, double *U, double *V, double *W, double *Pr,
   if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
   if (nsteps < 0) return fail(ELMM_ERR_INVALID_ARG, "nsteps < 0");
   return DISPATCH(h->b, march_host(U, V, W, Pr, Temperature, nsteps, stats));
+}
+
+int elmm_set_fault_injection(elmm_handle *h, int32_t wait_limit, int32_t skip_plane) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  if (wait_limit < 1) return fail(ELMM_ERR_INVALID_ARG, "wait_limit < 1");
+  return DISPATCH(h->b, set_fault_injection(wait_limit, skip_plane));
 }
 
 int elmm_upload_state_float(elmm_handle *h, const float *U, const float *V, const float *W, const float *Pr) {

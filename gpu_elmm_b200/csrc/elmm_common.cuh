@@ -73,8 +73,14 @@ struct Dom {
   double prgx, prgy;
   double dx, dy, dz;     // dxmin, dymin, dzmin
   double xmin, ymin;     // xU(0), yV(0)
-  double dt;
+  double dt;             // the current step's length (rewritten on the device by k_dt with variable steps)
   double nu_mol, cs;
+  // variable time steps (TimeStepLength, src/dynamics.f90:517-548): target
+  // CFL, longest step, end time (0: none), the configured dt; tstate on the
+  // device holds the time after the last step and that step's length
+  int vdt;
+  double cfl_target, dt_max, end_time, dt0;
+  double *tstate;
   // coefficients computed once on the host as the reference computes them
   // once per call (advection.f90: Ax = 0.25/dxmin etc.; momentum_diffusion.f90:
   // recdxmin2 = 1/dxmin**2)
@@ -127,6 +133,10 @@ struct Dom {
   unsigned long long *maxdiv_bits;  // max |div u| as the bits of a positive double
   unsigned long long *cfl_bits;
   int *flags;            // [0]: NaN seen, [1]: a bounded wait gave up
+  // the bounded plane waits of k_momentum / k_sgs: tries before giving up,
+  // and the plane whose copies are not issued (-1: none; fault injection by
+  // elmm_set_fault_injection for tests of the timeout path)
+  int wait_limit, skip_plane;
   const void *tmaps;     // CUtensorMap[2][F_COUNT] (device memory, 64-byte aligned)
   const void *tmapT;     // FP32 with buoyancy: CUtensorMap[3], narrow boxes of the temperature's value buffers
   // defect correction of the mixed path

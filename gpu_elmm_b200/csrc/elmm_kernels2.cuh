@@ -2,6 +2,8 @@
 // host-layout pack / unpack kernels.
 #pragma once
 
+#include <cfloat>
+
 #include "elmm_kernels.cuh"
 
 namespace elmm {
@@ -651,6 +653,31 @@ __global__ void __launch_bounds__(TX *TY) k_cfl(const Dom<T> *__restrict__ doms,
     }
   }
   if (cur >= 0) block_max_flush<TX * TY>(doms[cur].cfl_bits, run, red);
+}
+
+// TimeStepLength with variable time steps (src/dynamics.f90:517-529,
+// :547-548), one thread per domain after k_cfl: the step's length from the
+// largest U_dx_max of the state at its start, written into the descriptor
+// that every kernel of the step reads, and the domain's clock.
+template <typename T>
+__global__ void k_dt(Dom<T> *doms, int nd) {
+  const int di = blockIdx.x * blockDim.x + threadIdx.x;
+  if (di >= nd) return;
+  Dom<T> &d = doms[di];
+  if (!d.vdt) return;
+  const double u = __longlong_as_double((long long)*d.cfl_bits);  // a NaN in the field reads as NaN here
+  double dt;
+  if (u != u) dt = DBL_MIN;                                      // tiny(dt)
+  else if (u > 0) dt = fmin(d.cfl_target / u, d.dt_max);
+  else dt = d.dt_max;
+  const double time = d.tstate[0];
+  if (d.end_time > 0) {
+    if (d.end_time - time <= 1e-12 * d.end_time) d.flags[2] = 1;  // the run is over: the host should not step
+    else if (dt + time > d.end_time) dt = d.end_time - time;
+  }
+  d.dt = dt;
+  d.tstate[0] = time + dt;
+  d.tstate[1] = dt;
 }
 
 // ------------------------------------------------------ host layout copies

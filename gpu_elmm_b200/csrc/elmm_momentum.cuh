@@ -536,8 +536,9 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
     if (threadIdx.x == 0) {
       fence_async_shared();
       for (int kk = k0 - 1; kk <= min(k0 - 1 + NSL - 1, k1 + 1); kk++)
-        issue_mom_plane<T, NNF>(ring + (kk % NSL) * Lay::SIZE, &bars[kk % NSL], maps, tmapT, !stage1, d.aln, i0, j0,
-                                kk);
+        if (kk != d.skip_plane)
+          issue_mom_plane<T, NNF>(ring + (kk % NSL) * Lay::SIZE, &bars[kk % NSL], maps, tmapT, !stage1, d.aln, i0, j0,
+                                  kk);
     }
     __syncthreads();  // the context is written
     const T dt = (T)d.dt, rdt = (T)sc.rho, bdt = (T)sc.beta;
@@ -590,7 +591,12 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
       bool ok = true;
       for (int kk = (k == k0 ? k0 - 1 : k + 1); kk <= k + 1; kk++) {
         const int s2 = kk % NSL;
-        ok &= mbar_wait(&bars[s2], (phase >> s2) & 1u);
+        bool w = mbar_wait(&bars[s2], (phase >> s2) & 1u, d.wait_limit);
+        // a plane whose copies were issued always lands before the block
+        // moves on or gives up (so no copy into this block's shared memory
+        // outlives it): a lowered limit only cuts the wait on a skipped one
+        if (!w && kk != d.skip_plane) w = mbar_wait(&bars[s2], (phase >> s2) & 1u);
+        ok &= w;
         phase ^= 1u << s2;
       }
       if (!ok) { abort_flag = 1; d.flags[1] = 1; }
@@ -754,13 +760,13 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
         if (threadIdx.x == 0)
           for (int kk = k + 2; kk <= min(k - 1 + NSL - 1, k1 + 1); kk++) {
             const int s2 = kk % NSL;
-            mbar_wait(&bars[s2], (phase >> s2) & 1u);
+            if (kk != d.skip_plane) mbar_wait(&bars[s2], (phase >> s2) & 1u);  // issued copies land: the full limit
             phase ^= 1u << s2;
           }
         return;
       }
       const int kn = k - 1 + NSL;
-      if (threadIdx.x == 0 && kn <= k1 + 1) {
+      if (threadIdx.x == 0 && kn <= k1 + 1 && kn != d.skip_plane) {
         fence_async_shared();
         issue_mom_plane<T, NNF>(ring + (kn % NSL) * Lay::SIZE, &bars[kn % NSL], maps, tmapT, !stage1, d.aln, i0, j0,
                                 kn);
@@ -938,8 +944,9 @@ __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
     if (threadIdx.x == 0) {
       fence_async_shared();
       for (int kk = k0 - 1; kk <= min(k0 - 1 + kRingSlots - 1, k1 + 1); kk++)
-        issue_plane<T, 3, 0>(ring + (kk % kRingSlots) * Lay::SIZE, &bars[kk % kRingSlots], maps, wide, none, false,
-                             d.aln, i0, j0, kk);
+        if (kk != d.skip_plane)
+          issue_plane<T, 3, 0>(ring + (kk % kRingSlots) * Lay::SIZE, &bars[kk % kRingSlots], maps, wide, none, false,
+                               d.aln, i0, j0, kk);
     }
     // block-uniform: the wall sides whose wall-model points this tile can
     // hold (a point sits next to its side: i in {1, nx-1, nx} and so on)
@@ -973,7 +980,12 @@ __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
       bool ok = true;
       for (int kk = (k == k0 ? k0 - 1 : k + 1); kk <= k + 1; kk++) {
         const int s2 = kk % kRingSlots;
-        ok &= mbar_wait(&bars[s2], (phase >> s2) & 1u);
+        bool w = mbar_wait(&bars[s2], (phase >> s2) & 1u, d.wait_limit);
+        // a plane whose copies were issued always lands before the block
+        // moves on or gives up (so no copy into this block's shared memory
+        // outlives it): a lowered limit only cuts the wait on a skipped one
+        if (!w && kk != d.skip_plane) w = mbar_wait(&bars[s2], (phase >> s2) & 1u);
+        ok &= w;
         phase ^= 1u << s2;
       }
       if (!ok) { abort_flag = 1; d.flags[1] = 1; }
@@ -1038,13 +1050,13 @@ __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
         if (threadIdx.x == 0)
           for (int kk = k + 2; kk <= min(k - 1 + kRingSlots - 1, k1 + 1); kk++) {
             const int s2 = kk % kRingSlots;
-            mbar_wait(&bars[s2], (phase >> s2) & 1u);
+            if (kk != d.skip_plane) mbar_wait(&bars[s2], (phase >> s2) & 1u);  // issued copies land: the full limit
             phase ^= 1u << s2;
           }
         return;
       }
       const int kn = k - 1 + kRingSlots;
-      if (threadIdx.x == 0 && kn <= k1 + 1) {
+      if (threadIdx.x == 0 && kn <= k1 + 1 && kn != d.skip_plane) {
         fence_async_shared();
         issue_plane<T, 3, 0>(ring + (kn % kRingSlots) * Lay::SIZE, &bars[kn % kRingSlots], maps, wide, none, false,
                              d.aln, i0, j0, kn);

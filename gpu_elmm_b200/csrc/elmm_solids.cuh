@@ -83,8 +83,9 @@ __global__ void __launch_bounds__(256) k_ib_gather(const Dom<T> *__restrict__ do
 template <typename T>
 __global__ void __launch_bounds__(128) k_ib_wm(const Dom<T> *__restrict__ doms, int di,
                                                const WMSolid *__restrict__ pts, double *__restrict__ ustar_state,
-                                               int n, double beta_dt) {
+                                               int n, double beta) {
   const Dom<T> &d = doms[di];
+  const double beta_dt = beta * d.dt;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
     const WMSolid &p = pts[q];
     const T *U = d.U, *V = d.V, *W = d.W, *nu = d.nu;

@@ -57,12 +57,13 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, i
 }
 
 // Bounded wait: every try_wait already suspends for a while in hardware; a
-// phase that has not completed after kWaitLimit tries is reported as a
-// timeout instead of spinning for ever.
+// phase that has not completed after `limit` tries (kWaitLimit unless a test
+// of the failure path lowered it) is reported as a timeout instead of
+// spinning for ever.
 constexpr int kWaitLimit = 1 << 20;
 
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-  for (int n = 0; n < kWaitLimit; n++)
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int limit = kWaitLimit) {
+  for (int n = 0; n < limit; n++)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }

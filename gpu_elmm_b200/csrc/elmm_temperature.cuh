@@ -495,7 +495,9 @@ __global__ void k_scalar_avg(const Dom<T> *__restrict__ doms, Launch L) {
     const int j = xy ? r + 1 : d.avg_j, k = xy ? d.avg_k : r - (d.avg_k > 0 ? ny : 0) + 1;
     double *acc = xy ? sl.acc_xy + (size_t)(j - 1) * nx : sl.acc_xz + (size_t)(k - 1) * nx;
     const T *S = sl.buf[0] + bidx(d, 1, j, k);
-    for (int i = threadIdx.x; i < nx; i += blockDim.x) acc[i] = acc[i] + ((double)S[i] + sl.off) * d.avg_w;
+    // a variable step weighs its length / dt of the configured weight
+    const double w = d.vdt ? d.avg_w * (d.dt / d.dt0) : d.avg_w;
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) acc[i] = acc[i] + ((double)S[i] + sl.off) * w;
   }
 }
 

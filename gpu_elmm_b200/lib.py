@@ -82,6 +82,7 @@ def lib():
         L.elmm_batch_step.argtypes = [P, C.c_int32, C.POINTER(ElmmStats)]
         L.elmm_batch_cells.argtypes = [P]
         L.elmm_batch_cells.restype = C.c_int64
+        L.elmm_set_fault_injection.argtypes = [P, C.c_int32, C.c_int32]
         fp = C.POINTER(C.c_float)
         L.elmm_upload_state_float.argtypes = [P, fp, fp, fp, fp]
         L.elmm_download_state_float.argtypes = [P, fp, fp, fp, fp]
@@ -173,6 +174,10 @@ class Domain:
         check(lib().elmm_march_host(self.h, ptr(U), ptr(V), ptr(W), ptr(Pr), ptr(T), n, C.byref(st)),
               "elmm_march_host")
         return st
+
+    def set_fault_injection(self, wait_limit=1 << 20, skip_plane=-1):
+        """Fault injection for tests of the timeout path (elmm_set_fault_injection)."""
+        check(lib().elmm_set_fault_injection(self.h, wait_limit, skip_plane), "elmm_set_fault_injection")
 
     # single-precision host arrays (a host built with prec=sp): float32 arrays
     # in the same layouts

@@ -15,7 +15,7 @@ module elmm_gpu
   use iso_c_binding
   implicit none
 
-  integer(c_int32_t), parameter :: ELMM_ABI_VERSION = 4
+  integer(c_int32_t), parameter :: ELMM_ABI_VERSION = 5
 
   integer(c_int), parameter :: ELMM_OK = 0, ELMM_ERR_INVALID_CONFIG = 1, ELMM_ERR_OOM = 2, &
                                ELMM_ERR_NAN = 3, ELMM_ERR_CUDA = 4, ELMM_ERR_TIMEOUT = 5, &
@@ -105,6 +105,8 @@ module elmm_gpu
     type(elmm_point_source) :: point_sources(8)
     integer(c_int32_t) :: avg_slice_k, avg_slice_j   ! time-averaged slices of each scalar
     real(c_double)     :: avg_weight                 ! dt / (timeavg2 - timeavg1)
+    integer(c_int32_t) :: variable_time_steps, reserved1   ! TimeStepLength's variable branch
+    real(c_double)     :: CFL, dt_max, end_time
   end type
 
   type, bind(C) :: elmm_stats

@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define ELMM_ABI_VERSION 4
+#define ELMM_ABI_VERSION 5
 
 /* Status codes. */
 enum {
@@ -156,7 +156,22 @@ typedef struct elmm_config {
    * that spans the run.  In FP64 on both precision paths. */
   int32_t avg_slice_k;          /* horizontal plane k = 1..Prnz, 0: none */
   int32_t avg_slice_j;          /* vertical x-z plane j = 1..Prny, 0: none */
-  double avg_weight;
+  double avg_weight;            /* the weight of a step of length dt (variable steps: scaled by their length / dt) */
+  /* Variable time steps: the variable_time_steps branch of TimeStepLength
+   * (src/dynamics.f90:517-529, :547-548).  Each step takes, from the state
+   * at its start, dt = min(CFL / U_dx_max, dt_max) with U_dx_max the largest
+   * sum over the three directions of the larger face speed / spacing of a
+   * cell; dt_max when the flow is at rest; the smallest positive normal
+   * double when U_dx_max is NaN (the step then reports ELMM_ERR_NAN); and,
+   * with end_time > 0, the step that would pass end_time ends there.  A step
+   * that starts at end_time takes its CFL length and the call returns
+   * ELMM_ERR_INVALID_ARG (the run was over).  The length of the last step
+   * and the time come back in elmm_stats.  Off: the constant dt above. */
+  int32_t variable_time_steps;
+  int32_t reserved1;            /* 0 */
+  double CFL;                   /* target CFL number of the variable steps */
+  double dt_max;                /* the longest variable step */
+  double end_time;              /* > 0: no variable step passes this time */
 } elmm_config;
 
 /* Diagnostics of elmm_step / elmm_project. */
@@ -365,6 +380,18 @@ int elmm_march_host_float(elmm_handle *h, float *U, float *V, float *W, float *P
  *   stop = 3: the full stage (projection and swap)
  * stage is 1..3.  Fields are read back with elmm_download_field. */
 int elmm_run_stage(elmm_handle *h, int32_t stage, int32_t stop);
+
+/* Fault injection for tests of the failure path (no counterpart in the
+ * reference).  The momentum and SGS kernels wait for each plane's copies on
+ * an mbarrier with a bounded number of tries; after wait_limit tries
+ * (1048576 by default) a block gives up, waits (bounded) for its own copies
+ * still in flight, leaves the tile undone and makes elmm_step return
+ * ELMM_ERR_TIMEOUT; the handle stays usable.  skip_plane >= 0 makes the
+ * kernels issue no copy for that plane index (0..Prnz+1), so its wait runs
+ * out; -1 restores normal operation.  Set a small wait_limit with it (a few
+ * hundred tries) so that the test is quick; the state after such a step is
+ * incomplete and should be uploaded again. */
+int elmm_set_fault_injection(elmm_handle *h, int32_t wait_limit, int32_t skip_plane);
 
 /* Kernel timing of one stage (no counterpart in the reference; the
  * reference's per-part timers are src/tsteps.f90:113, :234-238): runs the

@@ -154,6 +154,9 @@ struct Domain {
   double dt, time;
   int enable_CFL_check;
   double CFL;
+  // variable time steps (t_s%variable_time_steps, CFL, dt_max, end_time)
+  int variable_time_steps;
+  double CFL_target, dt_max, end_time, dt0;
   A3 U, V, W, U2, V2, W2, Ustar, Vstar, Wstar, Pr, Viscosity, Phi, RHS;
   std::vector<WMPointUVW> wm[7][4];  // [direction][component]
   // Poisson
@@ -931,19 +934,22 @@ static void ScalarRK3(Domain &d, int stage, double dt) {
 // the two slice planes
 static void AccumulateScalarAverages(Domain &d) {
   const int nx = d.Prnx, ny = d.Prny, nz = d.Prnz;
+  // time_weight is proportional to the step's length: avg_weight belongs to a
+  // step of length dt, a variable step weighs its length / dt of it
+  const double avg_w = d.variable_time_steps ? d.avg_w * (d.dt / d.dt0) : d.avg_w;
   for (int sc = 0; sc < d.num_scalars; sc++) {
     const A3 &S = d.S[sc];
     if (d.avg_k > 0)
       for (int j = 1; j <= ny; j++)
         for (int i = 1; i <= nx; i++) {
           double &a = d.acc_xy[sc][(size_t)(j - 1) * nx + i - 1];
-          a = a + S(i, j, d.avg_k) * d.avg_w;
+          a = a + S(i, j, d.avg_k) * avg_w;
         }
     if (d.avg_j > 0)
       for (int k = 1; k <= nz; k++)
         for (int i = 1; i <= nx; i++) {
           double &a = d.acc_xz[sc][(size_t)(k - 1) * nx + i - 1];
-          a = a + S(i, d.avg_j, k) * d.avg_w;
+          a = a + S(i, d.avg_j, k) * avg_w;
         }
   }
 }
@@ -1667,8 +1673,9 @@ static void PressureCorrection(Domain &d, double coef, bool check_div, bool with
 
 // ---------------------------------------------- TimeStepLength, dynamics.f90:511-600
 static void TimeStepLength(Domain &d) {
-  if (!d.enable_CFL_check) { d.CFL = 0; return; }
+  if (!d.enable_CFL_check && !d.variable_time_steps) { d.CFL = 0; return; }
   double U_dx_max = 0;
+  bool nan = false;
   for (int k = 1; k <= d.Prnz; k++)
     for (int j = 1; j <= d.Prny; j++)
       for (int i = 1; i <= d.Prnx; i++) {
@@ -1679,7 +1686,18 @@ static void TimeStepLength(Domain &d) {
         p = p + std::max(std::fabs(d.V(i, j, k)), std::fabs(d.V(i, j - 1, k))) / dy;
         p = p + std::max(std::fabs(d.W(i, j, k)), std::fabs(d.W(i, j, k - 1))) / dz;
         U_dx_max = std::max(U_dx_max, p);
+        if (p != p) nan = true;
       }
+  if (d.variable_time_steps) {  // dynamics.f90:517-529
+    if (nan) d.dt = std::numeric_limits<double>::min();
+    else if (U_dx_max > 0) d.dt = std::min(d.CFL_target / U_dx_max, d.dt_max);
+    else d.dt = d.dt_max;
+    // the step that would pass end_time ends there (dynamics.f90:547-548)
+    if (d.end_time > 0 && d.end_time - d.time > 1e-12 * d.end_time && d.dt + d.time > d.end_time)
+      d.dt = d.end_time - d.time;
+    d.CFL = U_dx_max * d.dt;
+    return;
+  }
   d.CFL = U_dx_max * d.dt;
 }
 
@@ -1797,6 +1815,8 @@ void *orc_create(const elmm_config *c) {
   d->prgx = c->pr_gradient_x; d->prgy = c->pr_gradient_y;
   d->dt = c->dt; d->time = 0;
   d->enable_CFL_check = c->enable_CFL_check; d->CFL = 0; d->max_div = 0;
+  d->variable_time_steps = c->variable_time_steps;
+  d->CFL_target = c->CFL; d->dt_max = c->dt_max; d->end_time = c->end_time; d->dt0 = c->dt;
   init_grid(*d, *c);
   int nx = d->Prnx, ny = d->Prny, nz = d->Prnz;
   for (A3 *a : {&d->U, &d->U2, &d->Ustar}) a->init(-2, d->Unx + 3, -2, d->Uny + 3, -2, d->Unz + 3);
@@ -1981,6 +2001,14 @@ int orc_step(void *h, int nsteps, double *max_div, double *cfl) {
   for (int s = 0; s < nsteps; s++) TMarchRK3(*d);
   if (max_div) *max_div = d->max_div;
   if (cfl) *cfl = d->CFL;
+  return 0;
+}
+
+// the time and the length of the last step
+int orc_clock(void *h, double *out2) {
+  Domain *d = (Domain *)h;
+  out2[0] = d->time;
+  out2[1] = d->dt;
   return 0;
 }
 

@@ -51,6 +51,7 @@ def lib(native: bool = False):
         L.orc_project.argtypes = [P, C.c_double, dp]
         L.orc_step.argtypes = [P, C.c_int, dp, dp]
         L.orc_run_stage.argtypes = [P, C.c_int, C.c_int]
+        L.orc_clock.argtypes = [P, dp]
         L.orc_poisson.argtypes = [P, dp, dp]
         L.orc_bound_uvw.argtypes = [P]
         L.orc_num_threads.argtypes = [C.c_int]
@@ -133,6 +134,12 @@ class Oracle:
         cfl = C.c_double(0)
         self.L.orc_step(self.h, n, C.byref(md), C.byref(cfl))
         return md.value, cfl.value
+
+    def clock(self):
+        """(time, length of the last step)."""
+        out = (C.c_double * 2)()
+        self.L.orc_clock(self.h, out)
+        return out[0], out[1]
 
     def run_stage(self, stage, stop):
         r = self.L.orc_run_stage(self.h, stage, stop)
