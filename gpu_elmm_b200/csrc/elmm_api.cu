@@ -255,7 +255,11 @@ struct LaunchSet {
 };
 
 enum { LK_CELLS = 0, LK_BOX, LK_ROWS, LK_YCOLS, LK_TRI, LK_MOM, LK_SHELL, LK_XREG, LK_YREG, LK_TRIT, LK_TCOL, LK_DCOL,
-       LK_AVG, LK_COMMIT, LK_TPAIR, LK_PROJ, LK_PROJ2, LK_DCOL2, LK_N };
+       LK_AVG, LK_COMMIT, LK_TPAIR, LK_PROJ, LK_PROJ2, LK_DCOL2, LK_MOMT, LK_SGST, LK_N };
+
+// the z-chunk lengths (planes of a tile's column) the autotuner tries for
+// the momentum and SGS kernels
+constexpr int kChunks[3] = {8, 16, 32};
 
 // blocks of the host-layout pack / unpack kernels (8 per SM)
 constexpr int kPackBlocks = 148 * 8;
@@ -325,6 +329,8 @@ struct BatchT {
   // tile shapes chosen by the autotuner at the first step: rows of a tile of
   // the FP32 scalar stage, spectral columns of a tile of the z solve
   int tune_rows = 8, tune_cols = 16;
+  int tune_mom_kc = MKC, tune_sgs_kc = MKC;  // z chunks of k_momentum and k_sgs
+  int cap_mom[3] = {1, 1, 1}, cap_sgs[3] = {1, 1, 1};  // resident-block grids per chunk choice
   bool tuned = false;
   // parallel branches for the independent per-length launches of one
   // transform phase (a batch with several x or y lengths); joined back into
@@ -332,7 +338,7 @@ struct BatchT {
   static constexpr int kBranches = 4;
   cudaStream_t branch[kBranches] = {};
   cudaEvent_t ev_fork = nullptr, ev_join[kBranches] = {};
-  float tune_ms[4] = {0, 0, 0, 0};  // rows 8, rows 4, cols 16, cols 32
+  float tune_ms[10] = {};  // rows 8, rows 4, cols 16, cols 32, momentum chunks 8/16/32, SGS chunks 8/16/32
   // immersed solid bodies per domain (elmm_set_solids): the gathers of the
   // velocity IB points followed by the nullified points, the gathers of the
   // ScalFl viscosity, the solid-face wall-model points and their u* state
@@ -596,8 +602,12 @@ struct BatchT {
     CU(cudaFuncSetAttribute(k_fftx_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     CU(cudaFuncSetAttribute(k_ffty<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     CU(cudaFuncSetAttribute(k_tri<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-    CU(cudaFuncSetAttribute(k_momentum<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 1024));
-    CU(cudaFuncSetAttribute(k_sgs<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 1024));
+    CU(cudaFuncSetAttribute(k_momentum<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 1024));
+    CU(cudaFuncSetAttribute(k_momentum<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 1024));
+    CU(cudaFuncSetAttribute(k_momentum<T, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 1024));
+    CU(cudaFuncSetAttribute(k_sgs<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 1024));
+    CU(cudaFuncSetAttribute(k_sgs<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 1024));
+    CU(cudaFuncSetAttribute(k_sgs<T, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 1024));
     for (auto &h : hdom) {
       reg_x |= fft_reg_supported(h.nx);
       reg_y |= fft_reg_supported(h.ny);
@@ -624,6 +634,15 @@ struct BatchT {
     };
     grid_cap[0] = cap((const void *)k_sgs<T>, SgsShape<T>::threads, smem_sgs);
     grid_cap[1] = cap((const void *)k_momentum<T>, MomShape<T>::threads, smem_mom);
+    {
+      const void *fm[3] = {(const void *)k_momentum<T, 8>, (const void *)k_momentum<T, 16>,
+                           (const void *)k_momentum<T, 32>};
+      const void *fs[3] = {(const void *)k_sgs<T, 8>, (const void *)k_sgs<T, 16>, (const void *)k_sgs<T, 32>};
+      for (int q = 0; q < 3; q++) {
+        cap_mom[q] = cap(fm[q], MomShape<T>::threads, smem_mom);
+        cap_sgs[q] = cap(fs[q], SgsShape<T>::threads, smem_sgs);
+      }
+    }
     grid_cap[2] = cap((const void *)k_fftx_fwd<T>, kFFTThreads, smem_x);
     grid_cap[3] = cap((const void *)k_ffty<T>, kFFTThreads, smem_y);
     grid_cap[4] = cap((const void *)k_tri<T>, kTriThreads, smem_tri);
@@ -718,6 +737,8 @@ struct BatchT {
       case LK_ROWS: return fft_reg_supported(h.nx) ? 0 : (h.ny * h.nz + kRowsX - 1) / kRowsX;
       case LK_YCOLS: return fft_reg_supported(h.ny) ? 0 : ((h.nxh + TyOf<T>::v - 1) / TyOf<T>::v) * h.nz;
       case LK_MOM: return ((h.nx + MX - 1) / MX) * ((h.ny + MY - 1) / MY) * ((h.nz + MKC - 1) / MKC);
+      case LK_MOMT: return ((h.nx + MX - 1) / MX) * ((h.ny + MY - 1) / MY) * ((h.nz + tune_mom_kc - 1) / tune_mom_kc);
+      case LK_SGST: return ((h.nx + MX - 1) / MX) * ((h.ny + MY - 1) / MY) * ((h.nz + tune_sgs_kc - 1) / tune_sgs_kc);
       case LK_PROJ: return fp32_pairs(h) ? 0 : tiles(LK_MOM, h);
       case LK_PROJ2: return fp32_pairs(h) ? tiles(LK_MOM, h) : 0;
       case LK_SHELL: return (int)((shell_cells(h.nx, h.ny, h.nz) + kShellThreads - 1) / kShellThreads);
@@ -1015,9 +1036,23 @@ struct BatchT {
     k_ghosts<T><<<gsz(9, ls[LK_SHELL].total * nf), kShellThreads, 0, stream>>>(ddom, ls[LK_SHELL].l(), packed, nf,
                                                                                  gate, prref);
   }
+  static int chunk_index(int kc) { return kc == 8 ? 0 : kc == 16 ? 1 : 2; }
+  // k_sgs with the tuned z chunk; init: the initial viscosity and diffusivity
+  void sgs_kernel(int init) {
+    const int q = chunk_index(tune_sgs_kc), g = std::max(1, std::min(ls[LK_SGST].total, cap_sgs[q]));
+    if (tune_sgs_kc == 8) k_sgs<T, 8><<<g, SgsShape<T>::threads, smem_sgs, stream>>>(ddom, ls[LK_SGST].l(), init);
+    else if (tune_sgs_kc == 16) k_sgs<T, 16><<<g, SgsShape<T>::threads, smem_sgs, stream>>>(ddom, ls[LK_SGST].l(), init);
+    else k_sgs<T, 32><<<g, SgsShape<T>::threads, smem_sgs, stream>>>(ddom, ls[LK_SGST].l(), init);
+  }
+  void momentum_kernel(const StageCoef &sc) {
+    const int q = chunk_index(tune_mom_kc), g = std::max(1, std::min(ls[LK_MOMT].total, cap_mom[q]));
+    if (tune_mom_kc == 8) k_momentum<T, 8><<<g, MomShape<T>::threads, smem_mom, stream>>>(ddom, ls[LK_MOMT].l(), sc);
+    else if (tune_mom_kc == 16) k_momentum<T, 16><<<g, MomShape<T>::threads, smem_mom, stream>>>(ddom, ls[LK_MOMT].l(), sc);
+    else k_momentum<T, 32><<<g, MomShape<T>::threads, smem_mom, stream>>>(ddom, ls[LK_MOMT].l(), sc);
+  }
   int launch_sgs() {
     nlaunch++;
-    k_sgs<T><<<gsz(0, ls[LK_MOM].total), SgsShape<T>::threads, smem_sgs, stream>>>(ddom, ls[LK_MOM].l(), 0);
+    sgs_kernel(0);
     launch_ghosts({F_NU}, 0);
     return ELMM_OK;
   }
@@ -1026,7 +1061,7 @@ struct BatchT {
     nlaunch++;
     // no ghost pass for U2, V2, W2: their only reader, the divergence of the
     // forward x transform, folds its neighbours on the box faces itself
-    k_momentum<T><<<gsz(1, ls[LK_MOM].total), MomShape<T>::threads, smem_mom, stream>>>(ddom, ls[LK_MOM].l(), sc);
+    momentum_kernel(sc);
     return ELMM_OK;
   }
   void launch_project(double coef_alpha2, int use_dt, int in_place, int gate) {
@@ -1329,20 +1364,24 @@ struct BatchT {
   }
 
   // The autotuner: before the first step of a batch (or view), times each
-  // candidate tile shape of the z solve and of the FP32 scalar stage on the
-  // batch's own domains (three launches each, CUDA events) and keeps the
-  // fastest.  The launches it times only write scratch (the spectral buffer,
-  // the new scalar value and the tendency that a first stage overwrites), and
-  // no shape changes any result.
+  // candidate shape on the batch's own domains (a warm-up and ten launches
+  // each, CUDA events) and keeps the fastest: the spectral columns of a tile
+  // of the z solve (16, 32), the rows of a tile of the FP32 scalar stage (8,
+  // 4), and the z chunk of the momentum and SGS kernels (8, 16, 32 planes).
+  // The launches it times only write scratch or rewrite what the first step
+  // rewrites anyway (the spectral buffer, the new scalar value, the tendency
+  // and U2 of a first stage, the viscosity and the initial diffusivity of an
+  // unchanged state), and no shape changes any result: every cell's
+  // arithmetic is the same for every partition.
   int autotune() {
     tuned = true;
     cudaEvent_t a, b;
     CU(cudaEventCreate(&a));
     CU(cudaEventCreate(&b));
-    auto time3 = [&](auto launch) -> float {
+    auto time10 = [&](auto launch) -> float {
       launch();  // warm
       cudaEventRecord(a, stream);
-      for (int r = 0; r < 3; r++) launch();
+      for (int r = 0; r < 10; r++) launch();
       cudaEventRecord(b, stream);
       cudaEventSynchronize(b);
       float ms = 0;
@@ -1354,7 +1393,7 @@ struct BatchT {
       for (int v = 0; v < 2 && !r; v++) {
         tune_cols = v ? 32 : 16;
         if ((r = rebuild_ls(LK_TRIT))) break;
-        tune_ms[2 + v] = time3([&] { launch_tri(0); });
+        tune_ms[2 + v] = time10([&] { launch_tri(0); });
       }
       tune_cols = tune_ms[3] < tune_ms[2] ? 32 : 16;
       if (!r) r = rebuild_ls(LK_TRIT);
@@ -1363,15 +1402,64 @@ struct BatchT {
       for (int v = 0; v < 2 && !r; v++) {
         tune_rows = v ? 4 : 8;
         if ((r = rebuild_ls(LK_TPAIR))) break;
-        tune_ms[v] = time3([&] { launch_scalar_pair(1); });
+        tune_ms[v] = time10([&] { launch_scalar_pair(1); });
       }
       tune_rows = tune_ms[1] < tune_ms[0] ? 4 : 8;
       if (!r) r = rebuild_ls(LK_TPAIR);
     }
+    // the z chunks of the momentum kernel (a first stage: no old tendency
+    // read, U2 and the tendency rewritten by the first step) and of the SGS
+    // kernel (its initial mode, which leaves the wall model alone)
+    const StageCoef sc1{kRho[0], kBeta[0], 2 * kAlpha[0], 1};
+    int best_m = 1, best_s = 1;
+    for (int q = 0; q < 3 && !r; q++) {
+      tune_mom_kc = kChunks[q];
+      if ((r = rebuild_ls(LK_MOMT))) break;
+      tune_ms[4 + q] = time10([&] { momentum_kernel(sc1); });
+      if (tune_ms[4 + q] < tune_ms[4 + best_m]) best_m = q;
+    }
+    for (int q = 0; q < 3 && !r; q++) {
+      tune_sgs_kc = kChunks[q];
+      if ((r = rebuild_ls(LK_SGST))) break;
+      tune_ms[7 + q] = time10([&] { sgs_kernel(1); });
+      if (tune_ms[7 + q] < tune_ms[7 + best_s]) best_s = q;
+    }
+    tune_mom_kc = kChunks[best_m];
+    tune_sgs_kc = kChunks[best_s];
+    if (!r) r = rebuild_ls(LK_MOMT);
+    if (!r) r = rebuild_ls(LK_SGST);
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     if (r) return r;
     CU(cudaGetLastError());
+    return ELMM_OK;
+  }
+  // the shapes set by the caller instead of the autotuner (elmm_batch_set_tuning):
+  // out-of-set values are refused; nothing is timed
+  int set_tuning(const int32_t *v, int n) {
+    auto in = [](int x, std::initializer_list<int> set) {
+      for (int y : set) if (x == y) return true;
+      return false;
+    };
+    if (n > 0 && !in(v[0], {4, 8})) return fail(ELMM_ERR_INVALID_ARG, "scalar tile rows: 4 or 8");
+    if (n > 1 && !in(v[1], {16, 32})) return fail(ELMM_ERR_INVALID_ARG, "z-solve tile columns: 16 or 32");
+    if (n > 2 && !in(v[2], {8, 16, 32})) return fail(ELMM_ERR_INVALID_ARG, "momentum z chunk: 8, 16 or 32");
+    if (n > 3 && !in(v[3], {8, 16, 32})) return fail(ELMM_ERR_INVALID_ARG, "SGS z chunk: 8, 16 or 32");
+    CU(cudaSetDevice(device));
+    CU(cudaStreamSynchronize(stream));
+    if (n > 0) tune_rows = v[0];
+    if (n > 1) tune_cols = v[1];
+    if (n > 2) tune_mom_kc = v[2];
+    if (n > 3) tune_sgs_kc = v[3];
+    for (int kind : {LK_TPAIR, LK_TRIT, LK_MOMT, LK_SGST}) {
+      int r = rebuild_ls(kind);
+      if (r) return r;
+    }
+    if (step_exec) {  // the step graph holds the old launch shapes
+      cudaGraphExecDestroy(step_exec);
+      step_exec = nullptr;
+    }
+    tuned = true;
     return ELMM_OK;
   }
 
@@ -1760,7 +1848,7 @@ struct BatchT {
     launch_divmax();
     // the end of InitialConditions (src/initial.f90:4291-4313): eddy
     // viscosity of the projected field and, with scalars, their diffusivity
-    k_sgs<T><<<gsz(0, ls[LK_MOM].total), SgsShape<T>::threads, smem_sgs, stream>>>(ddom, ls[LK_MOM].l(), 1);
+    sgs_kernel(1);
     launch_ghosts({F_NU}, 0);
     CU(cudaEventRecord(t1, stream));
     CU(cudaStreamSynchronize(stream));
@@ -1788,10 +1876,10 @@ struct BatchT {
         cudaEventRecord(ev[2 * slot.size() + 1], stream);
         slot.push_back(k);
       };
-      timed(0, [&] { k_sgs<T><<<gsz(0, ls[LK_MOM].total), SgsShape<T>::threads, smem_sgs, stream>>>(ddom, ls[LK_MOM].l(), 0); });
+      timed(0, [&] { sgs_kernel(0); });
       timed(kGhost, [&] { launch_ghosts({F_NU}, 0); });
       timed(1, [&] {
-        k_momentum<T><<<gsz(1, ls[LK_MOM].total), MomShape<T>::threads, smem_mom, stream>>>(ddom, ls[LK_MOM].l(), sc);
+        momentum_kernel(sc);
       });
       timed(2, [&] { launch_fftx_fwd(a2, 1, 0, 0); });
       timed(3, [&] { launch_ffty(0, 0); });
@@ -2564,6 +2652,23 @@ int elmm_batch_tuning(const elmm_batch *b, int32_t out[2]) {
   out[0] = b->precision == ELMM_PREC_MIXED ? b->b32->tune_rows : b->b64->tune_rows;
   out[1] = b->precision == ELMM_PREC_MIXED ? b->b32->tune_cols : b->b64->tune_cols;
   return ELMM_OK;
+}
+
+int elmm_batch_get_tuning(const elmm_batch *b, int32_t *out, int32_t n) {
+  if (!b || !out || n < 0) return fail(ELMM_ERR_INVALID_ARG, "NULL argument");
+  int32_t v[ELMM_TUNE_KNOBS];
+  if (b->precision == ELMM_PREC_MIXED) {
+    v[0] = b->b32->tune_rows; v[1] = b->b32->tune_cols; v[2] = b->b32->tune_mom_kc; v[3] = b->b32->tune_sgs_kc;
+  } else {
+    v[0] = b->b64->tune_rows; v[1] = b->b64->tune_cols; v[2] = b->b64->tune_mom_kc; v[3] = b->b64->tune_sgs_kc;
+  }
+  for (int q = 0; q < n && q < ELMM_TUNE_KNOBS; q++) out[q] = v[q];
+  return ELMM_OK;
+}
+
+int elmm_batch_set_tuning(elmm_batch *b, const int32_t *vals, int32_t n) {
+  if (!b || !vals || n < 0 || n > ELMM_TUNE_KNOBS) return fail(ELMM_ERR_INVALID_ARG, "NULL argument or n out of range");
+  return DISPATCH(*b, set_tuning(vals, n));
 }
 
 static int batch_domain_ok(const elmm_batch *b, int32_t d) {

@@ -480,7 +480,9 @@ struct MomShape<float> {
   static constexpr int cpt = 2, slots = 4, threads = MX * MY / 2, min_blocks = 4, nnf = 4;
 };
 
-template <typename T>
+// KC: planes of a tile's column (a tuning choice: every cell's arithmetic is
+// the same for any KC)
+template <typename T, int KC = MKC>
 __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
     k_momentum(const Dom<T> *__restrict__ doms, Launch L, StageCoef sc) {
   constexpr int NNF = MomShape<T>::nnf;
@@ -490,8 +492,8 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
   T *ring = reinterpret_cast<T *>(dyn_smem);
   __shared__ __align__(8) uint64_t bars[NSL];
   __shared__ MomCtx<T> ctx;
-  // mixed path: offsets of U and V on planes k0-1 .. k0+MKC of the tile (see Dom::voff)
-  __shared__ float soff[2][MKC + 2];
+  // mixed path: offsets of U and V on planes k0-1 .. k0+KC of the tile (see Dom::voff)
+  __shared__ float soff[2][KC + 2];
   __shared__ int abort_flag;
   const int tx = threadIdx.x % TXN, ty = threadIdx.x / TXN;
   // tensor copies need 128-byte aligned destinations
@@ -514,8 +516,8 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
     const int bx = lt % ntx; lt /= ntx;
     const int by = lt % nty;
     const int bk = lt / nty;
-    const int i0 = bx * MX + 1, j0 = by * MY + 1, k0 = bk * MKC + 1;
-    const int k1 = min(k0 + MKC - 1, d.nz);
+    const int i0 = bx * MX + 1, j0 = by * MY + 1, k0 = bk * KC + 1;
+    const int k1 = min(k0 + KC - 1, d.nz);
     const int i = i0 + CPT * tx, j = j0 + ty;  // the thread's first cell
     const int nx = d.nx, ny = d.ny;
     const long long plane = d.plane;
@@ -528,8 +530,8 @@ __global__ void __launch_bounds__(MomShape<T>::threads, MomShape<T>::min_blocks)
     __syncthreads();  // every slot and the context of the previous tile are free
     if (threadIdx.x == 0) fill_ctx(ctx, d);
     if constexpr (sizeof(T) == 4) {
-      if (threadIdx.x < 2 * (MKC + 2)) {
-        const int c = threadIdx.x / (MKC + 2), kk = k0 - 1 + threadIdx.x % (MKC + 2);
+      if (threadIdx.x < 2 * (KC + 2)) {
+        const int c = threadIdx.x / (KC + 2), kk = k0 - 1 + threadIdx.x % (KC + 2);
         soff[c][kk - k0 + 1] = kk <= d.nz + 1 ? __ldg(d.voff + c * (d.nz + 2) + kk) : 0.f;
       }
     }
@@ -890,7 +892,7 @@ struct SgsShape<float> {
   static constexpr int cpt = 2, threads = MX * MY / 2, min_blocks = 6;
 };
 
-template <typename T>
+template <typename T, int KC = MKC>
 __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
     k_sgs(const Dom<T> *__restrict__ doms, Launch L, int init) {
   // planes of U, V, W (tile plus one-cell halo) arrive by tensor-map TMA in
@@ -902,7 +904,7 @@ __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
   __shared__ __align__(8) uint64_t bars[kRingSlots];
   __shared__ int abort_flag;
   // mixed path: the z-difference parts du, dv of the tile's planes (SgsK)
-  __shared__ float sdz[2][MKC];
+  __shared__ float sdz[2][KC];
   const int tx = threadIdx.x % TXN, ty = threadIdx.x / TXN;
   if (smem_addr(ring) & 127u) {  // tensor copies need 128-byte aligned destinations
     if (threadIdx.x == 0) doms[0].flags[1] = 1;
@@ -923,8 +925,8 @@ __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
     const int bx = lt % ntx; lt /= ntx;
     const int by = lt % nty;
     const int bk = lt / nty;
-    const int i0 = bx * MX + 1, j0 = by * MY + 1, k0 = bk * MKC + 1;
-    const int k1 = min(k0 + MKC - 1, d.nz);
+    const int i0 = bx * MX + 1, j0 = by * MY + 1, k0 = bk * KC + 1;
+    const int k1 = min(k0 + KC - 1, d.nz);
     const int i = i0 + CPT * tx, j = j0 + ty;  // the thread's first cell
     const int nx = d.nx, ny = d.ny, nz = d.nz;
     const int wide[3] = {F_U, F_V, F_W};
@@ -932,8 +934,8 @@ __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
     const CUtensorMap *maps = reinterpret_cast<const CUtensorMap *>(d.tmaps);
     __syncthreads();  // every slot and the z-difference parts of the previous tile are free
     if constexpr (sizeof(T) == 4) {
-      if (threadIdx.x < 2 * MKC) {
-        const int c = threadIdx.x / MKC, kk = k0 + threadIdx.x % MKC;
+      if (threadIdx.x < 2 * KC) {
+        const int c = threadIdx.x / KC, kk = k0 + threadIdx.x % KC;
         if (kk <= k1) {
           const float *o = d.voff + c * (d.nz + 2);
           sdz[c][kk - k0] = 2.f * (__ldg(o + kk + 1) - __ldg(o + kk - 1)) * (float)d.sgs_r2zz[kk];

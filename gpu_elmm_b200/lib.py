@@ -83,6 +83,8 @@ def lib():
         L.elmm_batch_cells.argtypes = [P]
         L.elmm_batch_cells.restype = C.c_int64
         L.elmm_set_fault_injection.argtypes = [P, C.c_int32, C.c_int32]
+        L.elmm_batch_get_tuning.argtypes = [P, C.POINTER(C.c_int32), C.c_int32]
+        L.elmm_batch_set_tuning.argtypes = [P, C.POINTER(C.c_int32), C.c_int32]
         fp = C.POINTER(C.c_float)
         L.elmm_upload_state_float.argtypes = [P, fp, fp, fp, fp]
         L.elmm_download_state_float.argtypes = [P, fp, fp, fp, fp]
@@ -336,11 +338,21 @@ class Batch:
               "elmm_batch_set_puffs")
         self.__dict__.setdefault("_puffs", {})[d] = (P, V)
 
+    TUNING_KEYS = ("scalar_tile_rows", "tri_tile_cols", "momentum_z_chunk", "sgs_z_chunk")
+
     def tuning(self):
-        """Tile shapes chosen by the autotuner at the first step."""
-        out = (C.c_int32 * 2)()
-        check(lib().elmm_batch_tuning(self.h, out), "elmm_batch_tuning")
-        return {"scalar_tile_rows": out[0], "tri_tile_cols": out[1]}
+        """Tile shapes chosen by the autotuner at the first step (or set)."""
+        out = (C.c_int32 * len(self.TUNING_KEYS))()
+        check(lib().elmm_batch_get_tuning(self.h, out, len(out)), "elmm_batch_get_tuning")
+        return dict(zip(self.TUNING_KEYS, list(out)))
+
+    def set_tuning(self, **shapes):
+        """Sets tile shapes instead of the autotuner (keys of TUNING_KEYS;
+        the ones not given keep their values)."""
+        cur = self.tuning()
+        cur.update(shapes)
+        vals = (C.c_int32 * len(self.TUNING_KEYS))(*[cur[k] for k in self.TUNING_KEYS])
+        check(lib().elmm_batch_set_tuning(self.h, vals, len(vals)), "elmm_batch_set_tuning")
 
     def profile_stage(self, stage=2, reps=5):
         """Mean device time (ms) of each kernel kind of one RK3 stage over the whole batch."""

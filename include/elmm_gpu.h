@@ -499,6 +499,17 @@ int elmm_batch_project(elmm_batch *b, double coef);
  * tile of the FP32 scalar stage, out[1]: spectral columns of a tile of the z
  * solve); the defaults before it. */
 int elmm_batch_tuning(const elmm_batch *b, int32_t out[2]);
+/* All the tile shapes (no counterpart in the reference, whose CPU loops take
+ * their L1-sized tiles from src/tiling.f90): out[0] rows of a scalar-stage
+ * tile (8, 4), out[1] spectral columns of a z-solve tile (16, 32), out[2]
+ * and out[3] the z chunk of the momentum and of the SGS kernel (8, 16, 32
+ * planes); the first n of ELMM_TUNE_KNOBS.  elmm_batch_set_tuning sets the
+ * first n shapes instead of the autotuner (the others keep their values;
+ * ELMM_ERR_INVALID_ARG for a value outside its set).  No shape changes a
+ * result. */
+#define ELMM_TUNE_KNOBS 4
+int elmm_batch_get_tuning(const elmm_batch *b, int32_t *out, int32_t n);
+int elmm_batch_set_tuning(elmm_batch *b, const int32_t *vals, int32_t n);
 
 /* elmm_set_solids and elmm_set_puffs for domain d of a batch: each domain
  * keeps its own bodies and puffs, and computes the same values as alone. */
