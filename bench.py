@@ -305,6 +305,7 @@ def run_ours(args, ws, rank, local):
 
     # roofline of the dominant kernel, timed live with CUDA events on the library's stream
     kt = dm.profile_stage(stage=2, reps=5)
+    tiles = dm.tuning()
     mom_ms = kt["momentum"]
     alg_bytes = MOMENTUM_WORDS * 4 * cells
     peak, peak_kind = peaks()
@@ -365,6 +366,7 @@ def run_ours(args, ws, rank, local):
                          "traffic": traffic, "traffic_source": traffic_source, "algorithmic_bytes": alg_bytes,
                          "ms": mom_ms},
             "kernel_ms_stage2": kt,
+            "autotuned_tiles": tiles,
             "e2e": {"value": e2e, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
             "gpu_launches": sm.kernels,
             "clocks": clk.summary(),

@@ -1365,23 +1365,28 @@ struct BatchT {
 
   // The autotuner: before the first step of a batch (or view), times each
   // candidate shape on the batch's own domains (a warm-up and ten launches
-  // each, CUDA events) and keeps the fastest: the spectral columns of a tile
-  // of the z solve (16, 32), the rows of a tile of the FP32 scalar stage (8,
-  // 4), and the z chunk of the momentum and SGS kernels (8, 16, 32 planes).
-  // The launches it times only write scratch or rewrite what the first step
-  // rewrites anyway (the spectral buffer, the new scalar value, the tendency
-  // and U2 of a first stage, the viscosity and the initial diffusivity of an
-  // unchanged state), and no shape changes any result: every cell's
-  // arithmetic is the same for every partition.
+  // each, three for the views of a serving loop, which are rebuilt often;
+  // CUDA events) and keeps the fastest: the spectral columns of a tile of
+  // the z solve (16, 32), the rows of a tile of the FP32 scalar stage (8, 4),
+  // and the z chunk of the momentum and SGS kernels (8, 16, 32 planes).  A
+  // view may be built between the steps of a running request, so the
+  // launches it times only write what the next step rewrites before reading
+  // it: the spectral buffer, the new value and tendency of a scalar stage,
+  // the momentum tendency (a function of the state alone) and U2, and the
+  // viscosity, wall-model fluxes and live diffusivity of the SGS kernel's
+  // stage mode (whose wall-model u* follows from the state alone).  No shape
+  // changes any result: every cell's arithmetic is the same for every
+  // partition.
   int autotune() {
     tuned = true;
     cudaEvent_t a, b;
     CU(cudaEventCreate(&a));
     CU(cudaEventCreate(&b));
+    const int reps = is_view ? 3 : 10;
     auto time10 = [&](auto launch) -> float {
       launch();  // warm
       cudaEventRecord(a, stream);
-      for (int r = 0; r < 10; r++) launch();
+      for (int r = 0; r < reps; r++) launch();
       cudaEventRecord(b, stream);
       cudaEventSynchronize(b);
       float ms = 0;
@@ -1407,10 +1412,9 @@ struct BatchT {
       tune_rows = tune_ms[1] < tune_ms[0] ? 4 : 8;
       if (!r) r = rebuild_ls(LK_TPAIR);
     }
-    // the z chunks of the momentum kernel (a first stage: no old tendency
-    // read, U2 and the tendency rewritten by the first step) and of the SGS
-    // kernel (its initial mode, which leaves the wall model alone)
-    const StageCoef sc1{kRho[0], kBeta[0], 2 * kAlpha[0], 1};
+    // the z chunks of the momentum kernel (timed as a second stage, which
+    // also reads the old tendency) and of the SGS kernel (its stage mode)
+    const StageCoef sc1{kRho[1], kBeta[1], 2 * kAlpha[1], 2};
     int best_m = 1, best_s = 1;
     for (int q = 0; q < 3 && !r; q++) {
       tune_mom_kc = kChunks[q];
@@ -1421,7 +1425,7 @@ struct BatchT {
     for (int q = 0; q < 3 && !r; q++) {
       tune_sgs_kc = kChunks[q];
       if ((r = rebuild_ls(LK_SGST))) break;
-      tune_ms[7 + q] = time10([&] { sgs_kernel(1); });
+      tune_ms[7 + q] = time10([&] { sgs_kernel(0); });
       if (tune_ms[7 + q] < tune_ms[7 + best_s]) best_s = q;
     }
     tune_mom_kc = kChunks[best_m];
@@ -2664,6 +2668,16 @@ int elmm_batch_get_tuning(const elmm_batch *b, int32_t *out, int32_t n) {
   }
   for (int q = 0; q < n && q < ELMM_TUNE_KNOBS; q++) out[q] = v[q];
   return ELMM_OK;
+}
+
+int elmm_get_tuning(const elmm_handle *h, int32_t *out, int32_t n) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  return elmm_batch_get_tuning(&h->b, out, n);
+}
+
+int elmm_set_tuning(elmm_handle *h, const int32_t *vals, int32_t n) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  return elmm_batch_set_tuning(&h->b, vals, n);
 }
 
 int elmm_batch_set_tuning(elmm_batch *b, const int32_t *vals, int32_t n) {

@@ -84,6 +84,8 @@ def lib():
         L.elmm_batch_cells.restype = C.c_int64
         L.elmm_set_fault_injection.argtypes = [P, C.c_int32, C.c_int32]
         L.elmm_batch_get_tuning.argtypes = [P, C.POINTER(C.c_int32), C.c_int32]
+        L.elmm_get_tuning.argtypes = [P, C.POINTER(C.c_int32), C.c_int32]
+        L.elmm_set_tuning.argtypes = [P, C.POINTER(C.c_int32), C.c_int32]
         L.elmm_batch_set_tuning.argtypes = [P, C.POINTER(C.c_int32), C.c_int32]
         fp = C.POINTER(C.c_float)
         L.elmm_upload_state_float.argtypes = [P, fp, fp, fp, fp]
@@ -176,6 +178,19 @@ class Domain:
         check(lib().elmm_march_host(self.h, ptr(U), ptr(V), ptr(W), ptr(Pr), ptr(T), n, C.byref(st)),
               "elmm_march_host")
         return st
+
+    def tuning(self):
+        """Tile shapes chosen by the autotuner at the first step (or set); the keys of Batch.TUNING_KEYS."""
+        out = (C.c_int32 * 4)()
+        check(lib().elmm_get_tuning(self.h, out, 4), "elmm_get_tuning")
+        return dict(zip(("scalar_tile_rows", "tri_tile_cols", "momentum_z_chunk", "sgs_z_chunk"), list(out)))
+
+    def set_tuning(self, **shapes):
+        cur = self.tuning()
+        cur.update(shapes)
+        keys = ("scalar_tile_rows", "tri_tile_cols", "momentum_z_chunk", "sgs_z_chunk")
+        vals = (C.c_int32 * 4)(*[cur[k] for k in keys])
+        check(lib().elmm_set_tuning(self.h, vals, 4), "elmm_set_tuning")
 
     def set_fault_injection(self, wait_limit=1 << 20, skip_plane=-1):
         """Fault injection for tests of the timeout path (elmm_set_fault_injection)."""

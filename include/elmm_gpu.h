@@ -510,6 +510,9 @@ int elmm_batch_tuning(const elmm_batch *b, int32_t out[2]);
 #define ELMM_TUNE_KNOBS 4
 int elmm_batch_get_tuning(const elmm_batch *b, int32_t *out, int32_t n);
 int elmm_batch_set_tuning(elmm_batch *b, const int32_t *vals, int32_t n);
+/* The same for a single-domain handle (tuned at its first step too). */
+int elmm_get_tuning(const elmm_handle *h, int32_t *out, int32_t n);
+int elmm_set_tuning(elmm_handle *h, const int32_t *vals, int32_t n);
 
 /* elmm_set_solids and elmm_set_puffs for domain d of a batch: each domain
  * keeps its own bodies and puffs, and computes the same values as alone. */
