@@ -2984,6 +2984,17 @@ static int noalloc_setup(int device, NoAllocDev *out) {
   return ELMM_OK;
 }
 
+// The caller's current device, made current again when the call returns.
+struct KeepDevice {
+  int dev = -1;
+  KeepDevice() {
+    if (cudaGetDevice(&dev) != cudaSuccess) dev = -1;
+  }
+  ~KeepDevice() {
+    if (dev >= 0) cudaSetDevice(dev);
+  }
+};
+
 extern "C" int elmm_poisson_solve_noalloc(const int32_t n[3], const double L[3], const int32_t bcs[6], int32_t device,
                                           double *Phi, const double *RHS, void *stream) {
   if (!n || !L || !bcs || !Phi || !RHS) return fail(ELMM_ERR_INVALID_ARG, "NULL argument");
@@ -3019,6 +3030,7 @@ extern "C" int elmm_poisson_solve_noalloc(const int32_t n[3], const double L[3],
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev || device >= 64)
     return fail(ELMM_ERR_INVALID_ARG, "no CUDA device " + std::to_string(device));
+  KeepDevice keep;
   CU(cudaSetDevice(device));
   NoAllocDev nd;
   if ((r = noalloc_setup(device, &nd))) return r;

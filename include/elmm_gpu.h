@@ -458,9 +458,9 @@ int elmm_poisson_solver_finalize_float(elmm_poisson *s);
  *   Phi  device pointer, Phi(-1:nx+2,-1:ny+2,-1:nz+2), interior written,
  *        ghosts untouched
  * n, L and bcs mean what they mean for elmm_poisson_solver_new.  The call
- * makes `device` current and enqueues its work on `stream` (a cudaStream_t;
- * NULL is the legacy default stream), then returns: Phi is ready once the
- * stream gets there.  Non-finite RHS values are not reported.
+ * enqueues its work on `stream` (a cudaStream_t of `device`; NULL is the
+ * legacy default stream) and returns with the caller's current device as it
+ * found it: Phi is ready once the stream gets there.  Non-finite RHS values are not reported.
  *
  * The first call on a device does a one-time set-up (it looks up the
  * array's device address and raises the kernels' shared-memory limit), so

@@ -1,5 +1,7 @@
 """The Python usage examples of the integration guide (section 4) run as
-written, on a B200."""
+written, on a B200.  The test reads the guide itself on purpose: the code
+blocks a user copies are the thing under test, so a copy kept elsewhere
+could drift from them unnoticed."""
 import re
 
 import numpy as np
