@@ -25,6 +25,7 @@
 #include "elmm_poisson_reg.cuh"
 #include "elmm_temperature.cuh"
 #include "elmm_solids.cuh"
+#include "elmm_slabs.cuh"
 #include "elmm_arena.h"
 
 using namespace elmm;
@@ -326,6 +327,12 @@ struct BatchT {
   size_t arena_bytes = 0;
   // a view steps domains whose fields other batches own, on a borrowed stream
   bool is_view = false;
+  // one z-slab of a split domain (SlabsT): its configuration carries
+  // BC_HALO on the shared faces (checked as the whole domain's beforehand),
+  // and its z grid is the whole domain's from level zk0 on
+  bool slab_mode = false;
+  const HostGrid *zparent = nullptr;
+  int zk0 = 0;
   // tile shapes chosen by the autotuner at the first step: rows of a tile of
   // the FP32 scalar stage, spectral columns of a tile of the z solve
   int tune_rows = 8, tune_cols = 16;
@@ -510,7 +517,7 @@ struct BatchT {
     nd = n;
     device = cfgs[0].device;
     for (int d = 0; d < n; d++) {
-      int r = check_config(cfgs[d]);
+      int r = slab_mode ? ELMM_OK : check_config(cfgs[d]);
       if (r) return r;
       if (cfgs[d].device != device) return fail(ELMM_ERR_INVALID_CONFIG, "all domains of a batch share one device");
       if (cfgs[d].precision != cfgs[0].precision) return fail(ELMM_ERR_INVALID_CONFIG, "all domains of a batch share one precision");
@@ -774,13 +781,24 @@ struct BatchT {
     const elmm_config &c = cfg[di];
     HostGrid &g = grid[di];
     make_grid(c, g);
+    if (zparent) {  // a slab: the levels of the whole domain from zk0 on, ghosts included
+      const HostGrid &G = *zparent;
+      for (int k = -2; k <= g.nz + 3; k++) {
+        g.zW[k + 2] = G.zW[zk0 + k + 2];
+        g.zPr[k + 2] = G.zPr[zk0 + k + 2];
+        g.dzPr[k + 2] = G.dzPr[zk0 + k + 2];
+      }
+      for (int k = -2; k <= g.nz + 2; k++) g.dzW[k + 2] = G.dzW[zk0 + k + 2];
+      for (int k = 1; k <= g.nz; k++) g.width[k] = G.width[zk0 + k];
+      g.dzmin = G.dzmin;
+    }
     Dom<T> h;
     memset(&h, 0, sizeof(h));
     h.nx = c.Prnx; h.ny = c.Prny; h.nz = c.Prnz;
     const int *b = c.Btype;
     int Unx = b[ELMM_EA] == ELMM_BC_PERIODIC ? h.nx : h.nx - 1;
     int Vny = b[ELMM_NO] == ELMM_BC_PERIODIC ? h.ny : h.ny - 1;
-    int Wnz = b[ELMM_TO] == ELMM_BC_PERIODIC ? h.nz : h.nz - 1;
+    int Wnz = b[ELMM_TO] == ELMM_BC_PERIODIC || b[ELMM_TO] == BC_HALO ? h.nz : h.nz - 1;
     int ext[3][3] = {{Unx, h.ny, h.nz}, {h.nx, Vny, h.nz}, {h.nx, h.ny, Wnz}};
     memcpy(h.ext, ext, sizeof(ext));
     h.aln = 128 / (int)sizeof(T);
@@ -871,7 +889,8 @@ struct BatchT {
       dzc[k] = zWf(k) - zWf(k - 1);
       dzf[k] = zP(k + 1) - zP(k);
     }
-    if (!h.zper) { Ab[1] = 0; At[h.nz] = 0; }
+    if (!h.zper && b[ELMM_BO] != BC_HALO) Ab[1] = 0;  // a slab face couples to the next slab
+    if (!h.zper && b[ELMM_TO] != BC_HALO) At[h.nz] = 0;
     if ((r = upload_table(&h.Ab, Ab))) return r;
     if ((r = upload_table(&h.At, At))) return r;
     if ((r = upload_table(&h.dzc, dzc))) return r;
@@ -2372,6 +2391,7 @@ static int with_float_host(elmm_batch &B, F f) {
 }
 
 #include "elmm_server.inl"
+#include "elmm_slabs.inl"
 
 extern "C" {
 

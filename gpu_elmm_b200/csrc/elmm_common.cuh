@@ -22,6 +22,10 @@
 namespace elmm {
 
 enum { BC_NOSLIP = 1, BC_FREESLIP = 2, BC_PERIODIC = 3, BC_NEUMANN = 5 };
+// The z face a slab of a split domain shares with the next slab (never a
+// user code): its ghost plane holds the neighbour's plane, copied in by the
+// slab exchange, and no kernel folds onto it.
+enum { BC_HALO = 9 };
 enum { SIDE_WE = 0, SIDE_EA = 1, SIDE_SO = 2, SIDE_NO = 3, SIDE_BO = 4, SIDE_TO = 5 };
 
 // box fields of a domain, the order of the tensor maps
@@ -208,6 +212,7 @@ ELMM_HD Fold fold_vel(int g, int n, int blo, int bhi, bool normal) {
         if (normal) { if (g == 0) { f.src = 1; f.zero = 1; } else { f.src = -g; f.sign = -1; } }
         else f.src = 1;
         break;
+      case BC_HALO: f.src = 0; break;  // the exchanged plane (deeper ghosts clamp onto it)
       default: f.src = 1; break;  // NEUMANN
     }
   } else {
@@ -221,10 +226,17 @@ ELMM_HD Fold fold_vel(int g, int n, int blo, int bhi, bool normal) {
         if (normal) { if (g == n + 1) { f.src = n; f.zero = 1; } else { f.src = 2 * n + 2 - g; f.sign = -1; } }
         else f.src = n;
         break;
+      case BC_HALO: f.src = n + 1; break;
       default: f.src = n; break;
     }
   }
   return f;
+}
+
+// whether z index k of a field with n interior levels lies in the ghost
+// plane of a slab face (filled by the exchange, skipped by the ghost passes)
+ELMM_HD bool halo_plane(int k, int n, const int *bt) {
+  return (k < 1 && bt[4] == BC_HALO) || (k > n && bt[5] == BC_HALO);
 }
 
 // Ghosts of Viscosity (BoundViscosity, src/scalarboundaries.f90:326-431) and

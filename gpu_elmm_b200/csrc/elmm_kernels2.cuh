@@ -102,7 +102,9 @@ __global__ void __launch_bounds__(MX *MY) k_project(const Dom<T> *__restrict__ d
     const bool px = d.bt[SIDE_WE] == BC_PERIODIC, py = d.bt[SIDE_SO] == BC_PERIODIC, pz = d.bt[SIDE_BO] == BC_PERIODIC;
     const long long oe = i < nx ? 1 : (px ? 1 - nx : 0);
     const long long on = j < ny ? pitch : (py ? pitch - (long long)ny * pitch : 0);
-    auto ot = [&](int kk) -> long long { return kk < nz ? plane : (pz ? plane - (long long)nz * plane : 0); };
+    // a slab's top neighbour plane is the exchanged ghost plane
+    const bool hz = d.bt[SIDE_TO] == BC_HALO;
+    auto ot = [&](int kk) -> long long { return kk < nz || hz ? plane : (pz ? plane - (long long)nz * plane : 0); };
     T phi = 0, pe = 0, pn = 0, pt = 0, u0 = 0, v0 = 0, w0 = 0, p0 = 0;
     if (inside) {
       phi = __ldg(Phi + c); pe = __ldg(Phi + c + oe); pn = __ldg(Phi + c + on); pt = __ldg(Phi + c + ot(k0));
@@ -208,7 +210,9 @@ __global__ void __launch_bounds__(MX *MY / 2) k_project_pair(const Dom<float> *_
     const bool last = i + 1 >= nx;
     const long long oe = !last ? 2 : (px ? 1 - i : 0);  // the neighbour pair; for a wall, the cell itself
     const long long on = j < ny ? pitch : (py ? pitch - (long long)ny * pitch : 0);
-    auto ot = [&](int kk) -> long long { return kk < nz ? plane : (pz ? plane - (long long)nz * plane : 0); };
+    // a slab's top neighbour plane is the exchanged ghost plane
+    const bool hz = d.bt[SIDE_TO] == BC_HALO;
+    auto ot = [&](int kk) -> long long { return kk < nz || hz ? plane : (pz ? plane - (long long)nz * plane : 0); };
     auto ld2 = [](const T *p, long long o) { return __ldg(reinterpret_cast<const float2 *>(p + o)); };
     float2 phi = {0, 0}, pe = {0, 0}, pn = {0, 0}, pt = {0, 0}, u0 = {0, 0}, v0 = {0, 0}, w0 = {0, 0}, p0 = {0, 0};
     auto east = [&](const float2 &own, long long cc) {
@@ -333,7 +337,7 @@ __global__ void k_prref(const Dom<T> *__restrict__ doms, int nd, int gate) {
 constexpr int kShellThreads = 256;
 
 template <typename T>
-__device__ __forceinline__ T *box_field(const Dom<T> &d, int f) {
+__host__ __device__ __forceinline__ T *box_field(const Dom<T> &d, int f) {
   switch (f) {
     case F_U: return d.U;
     case F_V: return d.V;
@@ -382,6 +386,7 @@ __global__ void __launch_bounds__(kShellThreads) k_ghosts(const Dom<T> *__restri
       w -= side * yf;
       k = w / rx; i = w - k * rx; k += 1; j = side ? ey + 1 : 0;
     }
+    if (halo_plane(k, ez, d.bt)) continue;  // the slab exchange fills it
     T *F = box_field(d, fid);
     const bool per[3] = {d.bt[SIDE_WE] == BC_PERIODIC, d.bt[SIDE_SO] == BC_PERIODIC, d.bt[SIDE_BO] == BC_PERIODIC};
     T v;
@@ -774,7 +779,7 @@ __global__ void k_halo_vel(const Dom<T> *__restrict__ dom, int comp) {
     int j = (int)(r % by), k = (int)(r / by);
     if (i > e[0] + 1 || j > e[1] + 1 || k > e[2] + 1) continue;
     bool gi = i < 1 || i > e[0], gj = j < 1 || j > e[1], gk = k < 1 || k > e[2];
-    if (!(gi || gj || gk)) continue;
+    if (!(gi || gj || gk) || halo_plane(k, e[2], d.bt)) continue;
     Fold fx = fold_vel(i, e[0], d.bt[0], d.bt[1], comp == 0);
     Fold fy = fold_vel(j, e[1], d.bt[2], d.bt[3], comp == 1);
     Fold fz = fold_vel(k, e[2], d.bt[4], d.bt[5], comp == 2);

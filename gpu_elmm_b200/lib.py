@@ -100,6 +100,13 @@ def lib():
                                                                  C.POINTER(C.c_int32), C.c_int32, C.c_int32]
         L.elmm_poisson_solver_execute_float.argtypes = [P, fp, fp]
         L.elmm_poisson_solver_finalize_float.argtypes = [P]
+        ip = C.POINTER(C.c_int32)
+        L.elmm_slabs_create.argtypes = [C.POINTER(ElmmConfig), C.c_int32, ip, ip, C.POINTER(P)]
+        L.elmm_slabs_destroy.argtypes = [P]
+        L.elmm_slabs_upload_state.argtypes = [P, _dp, _dp, _dp, _dp]
+        L.elmm_slabs_download_state.argtypes = [P, _dp, _dp, _dp, _dp]
+        L.elmm_slabs_project.argtypes = [P, C.c_double, C.POINTER(ElmmStats)]
+        L.elmm_slabs_step.argtypes = [P, C.c_int32, C.POINTER(ElmmStats)]
         _lib = L
     return _lib
 
@@ -374,6 +381,47 @@ class Batch:
         ms = (C.c_double * KERNEL_COUNT)()
         check(lib().elmm_batch_profile_stage(self.h, stage, reps, ms), "elmm_batch_profile_stage")
         return dict(zip(KERNEL_NAMES, list(ms)))
+
+
+class Slabs:
+    """One domain split into z-slabs (an elmm_slabs handle): slab s holds
+    levels k0+1..k0+nz[s] on GPU devices[s]; the host arrays are the whole
+    domain's, as for Domain."""
+
+    def __init__(self, cfg: ElmmConfig, nslabs: int, devices=None, nz=None):
+        self.cfg = cfg
+        self.grid: Grid = grid_of(cfg)
+        dv = (C.c_int32 * nslabs)(*devices) if devices is not None else None
+        nzs = (C.c_int32 * nslabs)(*nz) if nz is not None else None
+        h = C.c_void_p()
+        check(lib().elmm_slabs_create(C.byref(cfg), nslabs, dv, nzs, C.byref(h)), "elmm_slabs_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().elmm_slabs_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def upload(self, U, V, W, Pr=None):
+        check(lib().elmm_slabs_upload_state(self.h, ptr(U), ptr(V), ptr(W), ptr(Pr)), "elmm_slabs_upload_state")
+
+    def download(self):
+        g = self.grid
+        U, V, W, Pr = np.zeros(g.shape_u()), np.zeros(g.shape_v()), np.zeros(g.shape_w()), np.zeros(g.shape_p())
+        check(lib().elmm_slabs_download_state(self.h, ptr(U), ptr(V), ptr(W), ptr(Pr)), "elmm_slabs_download_state")
+        return U, V, W, Pr
+
+    def project(self, coef=1.0) -> ElmmStats:
+        st = ElmmStats()
+        check(lib().elmm_slabs_project(self.h, coef, C.byref(st)), "elmm_slabs_project")
+        return st
+
+    def step(self, n=1) -> ElmmStats:
+        st = ElmmStats()
+        check(lib().elmm_slabs_step(self.h, n, C.byref(st)), "elmm_slabs_step")
+        return st
 
 
 class PoissonSolver:

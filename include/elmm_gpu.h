@@ -599,6 +599,39 @@ int elmm_server_stats_get(elmm_server *s, elmm_server_stats *st);
 /* Seconds since the server was created, on the clock of elmm_request_info. */
 double elmm_server_now(const elmm_server *s);
 
+/* ------------------------------------------------------------------------
+ * One domain split into z-slabs over several GPUs (the reference's domain
+ * decomposition over MPI ranks, src/custom_mpi.f90:331-344, with its ghost
+ * exchanges, src/exchange_mpi.f90:84-503, and the PFFT solve,
+ * src/poisson.f90:107-114).  One process drives every slab: slab s holds
+ * levels k0+1 .. k0+nz_slab[s] on devices[s] (several slabs may share a
+ * device).  The slabs exchange one ghost plane per field with their
+ * neighbours (peer copies over NVLink between GPUs) and solve the z
+ * tridiagonal systems by exchanging three numbers per column and slab, so
+ * the spectral buffer never crosses between GPUs.  The result equals the
+ * single-domain handle's to rounding.
+ *
+ * Built for the flow: walls in z (no periodic z), constant dt, no
+ * temperature, scalars, solid bodies or defect-correction sweeps
+ * (ELMM_ERR_INVALID_CONFIG otherwise).  nz_slab may be NULL for an even
+ * split; every slab needs at least 4 levels, and the levels must add up to
+ * Prnz.  devices may be NULL for cfg->device.
+ *
+ * Host arrays are the whole domain's, in the layouts of elmm_upload_state;
+ * the download writes every element the single-domain download writes. */
+#define ELMM_MAX_SLABS 16
+typedef struct elmm_slabs elmm_slabs;
+int elmm_slabs_create(const elmm_config *cfg, int32_t nslabs, const int32_t *devices, const int32_t *nz_slab,
+                      elmm_slabs **out);
+int elmm_slabs_destroy(elmm_slabs *h);
+int elmm_slabs_upload_state(elmm_slabs *h, const double *U, const double *V, const double *W, const double *Pr);
+int elmm_slabs_download_state(elmm_slabs *h, double *U, double *V, double *W, double *Pr);
+/* PressureCorrection on the uploaded state, as elmm_project. */
+int elmm_slabs_project(elmm_slabs *h, double coef, elmm_stats *stats);
+/* nsteps RK3 steps, as elmm_step (launched eagerly; stats->elapsed_ms is
+ * the device time from the first slab's start to the last slab's end). */
+int elmm_slabs_step(elmm_slabs *h, int32_t nsteps, elmm_stats *stats);
+
 /* Last error message of this thread (static storage). */
 const char *elmm_last_error(void);
 
