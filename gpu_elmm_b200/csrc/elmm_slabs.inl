@@ -41,6 +41,11 @@ struct SlabsT {
     const double *dzc = nullptr, *dzf = nullptr;
   };
   std::vector<Tri> tri;
+  // slabs of at most kTriTileMaxNz levels take the tiled sweep kernels
+  static constexpr int kSlabCols = 16;
+  typedef SlabTile<T, kSlabCols> Tile;
+  bool tiled = false;
+  size_t smem_tile = 0;
   std::vector<cudaEvent_t> pre, post;
   cudaEvent_t t0 = nullptr, t1 = nullptr;
   double time = 0;
@@ -147,6 +152,19 @@ struct SlabsT {
             cudaGetLastError();
           }
         }
+    int maxnz = 0;
+    for (int s = 0; s < n; s++) maxnz = std::max(maxnz, nzl[s]);
+    tiled = maxnz <= kTriTileMaxNz;
+    smem_tile = Tile::smem(maxnz);
+    if (tiled)
+      for (int s = 0; s < n; s++) {
+        CU(cudaSetDevice(dev[s]));
+        int optin = 0;
+        CU(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev[s]));
+        CU(cudaFuncSetAttribute(k_slab_tri_fmap_tile<T, kSlabCols>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+        CU(cudaFuncSetAttribute(k_slab_tri_fwd_tile<T, kSlabCols>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+        CU(cudaFuncSetAttribute(k_slab_tri_bwd_tile<T, kSlabCols>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+      }
     pre.assign(n, nullptr);
     post.assign(n, nullptr);
     for (int s = 0; s < n; s++) {
@@ -246,9 +264,14 @@ struct SlabsT {
     std::vector<Copy> cps;
     each([&](int s, BatchT<T> &B) {
       const int ncol = B.hdom[0].ny * B.hdom[0].spitch;
-      k_slab_tri_fmap<T><<<(2 * ncol + 127) / 128, 128, 0, B.stream>>>(B.ddom, tri[s].iv,
-                                                                       tri[s].fmaps + 3LL * ncol * s, tri[s].zcol,
-                                                                       k0[s], nzg);
+      const int ntile = (ncol + kSlabCols - 1) / kSlabCols;
+      if (tiled)
+        k_slab_tri_fmap_tile<T, kSlabCols><<<ntile, Tile::THREADS, smem_tile, B.stream>>>(
+            B.ddom, tri[s].iv, tri[s].fmaps + 3LL * ncol * s, tri[s].zcol, k0[s], nzg);
+      else
+        k_slab_tri_fmap<T><<<(2 * ncol + 127) / 128, 128, 0, B.stream>>>(B.ddom, tri[s].iv, tri[s].fmaps + 3LL * ncol * s,
+                                                                         tri[s].zcol, k0[s], nzg);
+      B.nlaunch++;
       for (int t = 0; t < ns; t++) {
         if (t == s) continue;
         if (t > s) cps.push_back(Copy{s, t, tri[t].fmaps + 3LL * ncol * s, tri[s].fmaps + 3LL * ncol * s,
@@ -262,16 +285,29 @@ struct SlabsT {
     cps.clear();
     each([&](int s, BatchT<T> &B) {
       const int ncol = B.hdom[0].ny * B.hdom[0].spitch;
-      k_slab_tri_fwd<T><<<(2 * ncol + 127) / 128, 128, 0, B.stream>>>(B.ddom, tri[s].iv, tri[s].fmaps,
-                                                                      tri[s].bmaps + 3LL * ncol * s, tri[s].zcol,
-                                                                      tri[s].dzc, tri[s].dzf, k0[s], nzg, s);
+      const int ntile = (ncol + kSlabCols - 1) / kSlabCols;
+      if (tiled)
+        k_slab_tri_fwd_tile<T, kSlabCols><<<ntile, Tile::THREADS, smem_tile, B.stream>>>(
+            B.ddom, tri[s].iv, tri[s].fmaps, tri[s].bmaps + 3LL * ncol * s, tri[s].zcol, tri[s].dzc, tri[s].dzf, k0[s],
+            nzg, s);
+      else
+        k_slab_tri_fwd<T><<<(2 * ncol + 127) / 128, 128, 0, B.stream>>>(B.ddom, tri[s].iv, tri[s].fmaps,
+                                                                        tri[s].bmaps + 3LL * ncol * s, tri[s].zcol,
+                                                                        tri[s].dzc, tri[s].dzf, k0[s], nzg, s);
+      B.nlaunch++;
       for (int t = 0; t < s; t++)
         cps.push_back(Copy{s, t, tri[t].bmaps + 3LL * ncol * s, tri[s].bmaps + 3LL * ncol * s, sizeof(double) * 3 * ncol});
     });
     if ((r = exchange(cps))) return r;
     each([&](int s, BatchT<T> &B) {
       const int ncol = B.hdom[0].ny * B.hdom[0].spitch;
-      k_slab_tri_bwd<T><<<(2 * ncol + 127) / 128, 128, 0, B.stream>>>(B.ddom, tri[s].iv, tri[s].bmaps, s, ns);
+      const int ntile = (ncol + kSlabCols - 1) / kSlabCols;
+      if (tiled)
+        k_slab_tri_bwd_tile<T, kSlabCols><<<ntile, Tile::THREADS, smem_tile, B.stream>>>(B.ddom, tri[s].iv, tri[s].bmaps,
+                                                                                         s, ns);
+      else
+        k_slab_tri_bwd<T><<<(2 * ncol + 127) / 128, 128, 0, B.stream>>>(B.ddom, tri[s].iv, tri[s].bmaps, s, ns);
+      B.nlaunch++;
       B.launch_ffty(1, 0);
       B.launch_fftx_inv(0);
     });

@@ -11,6 +11,9 @@ times of one stage.
 --batched D runs the batched ensemble instead: D channel domains, each axis
 drawn from 32, 48, 64, 96, 128 (seed 0), one launch set for all of them.
 
+--slabs S splits the channel (without the temperature, which split domains
+do not carry) into S even z-slabs, all on GPU 0 (elmm_slabs_*).
+
 Under `ncu -k regex:<kernel> -s <skip> -c <count>` the launches of the
 profiled steps follow those of the projection and the warm-up steps; the
 NVTX range "timed_steps" brackets the profiled steps.
@@ -49,9 +52,12 @@ def main():
     ap.add_argument("--no-temperature", action="store_true", help="the channel without the temperature field")
     ap.add_argument("--batched", type=int, default=0, help="run the batched ensemble of this many domains")
     ap.add_argument("--cubes", action="store_true", help="run the array of cubes (384x384x96, stretched z)")
+    ap.add_argument("--slabs", type=int, default=0, help="split the channel into this many z-slabs on GPU 0")
     a = ap.parse_args()
     if a.batched:
         return batched(a)
+    if a.slabs:
+        return slabs(a)
     if a.cubes:
         return cubes(a)
     n = tuple(int(x) for x in a.n.split(","))
@@ -74,6 +80,23 @@ def main():
         out["stage2_kernel_ms"] = d.profile_stage(2, 5)
     print(json.dumps(out))
     d.close()
+
+
+def slabs(a):
+    n = tuple(int(x) for x in a.n.split(","))
+    cfg = make_config(*n, precision=1 if a.precision == "mixed" else 0)
+    b = L.Slabs(cfg, a.slabs, devices=[0] * a.slabs)
+    b.upload(*log_profile_state(grid_of(cfg), seed=0))
+    b.project(1.0)
+    if a.warmup:
+        b.step(a.warmup)
+    nvtx_push("timed_steps")
+    s = b.step(a.steps)
+    nvtx_pop()
+    print(json.dumps({"n": n, "slabs": a.slabs, "precision": a.precision, "steps": a.steps,
+                      "ms_per_step": s.elapsed_ms / max(1, a.steps), "max_div": s.max_div,
+                      "kernels_per_step": s.kernels / max(1, a.steps)}))
+    b.close()
 
 
 def cubes(a):

@@ -315,5 +315,40 @@ module elmm_gpu
       import
       type(c_ptr), value :: s
     end function
+    ! one domain split into z-slabs over several GPUs (the host arrays are
+    ! the whole domain's); devices and nz_slab may be c_null_ptr
+    integer(c_int) function elmm_slabs_create(cfg, nslabs, devices, nz_slab, h) bind(C)
+      import
+      type(elmm_config), intent(in) :: cfg
+      integer(c_int32_t), value :: nslabs
+      type(c_ptr), value :: devices, nz_slab
+      type(c_ptr) :: h
+    end function
+    integer(c_int) function elmm_slabs_destroy(h) bind(C)
+      import
+      type(c_ptr), value :: h
+    end function
+    integer(c_int) function elmm_slabs_upload_state(h, U, V, W, Pr) bind(C)
+      import
+      type(c_ptr), value :: h
+      real(c_double), intent(in) :: U(*), V(*), W(*), Pr(*)
+    end function
+    integer(c_int) function elmm_slabs_download_state(h, U, V, W, Pr) bind(C)
+      import
+      type(c_ptr), value :: h
+      real(c_double) :: U(*), V(*), W(*), Pr(*)
+    end function
+    integer(c_int) function elmm_slabs_project(h, coef, st) bind(C)
+      import
+      type(c_ptr), value :: h
+      real(c_double), value :: coef
+      type(elmm_stats) :: st
+    end function
+    integer(c_int) function elmm_slabs_step(h, nsteps, st) bind(C)
+      import
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: nsteps
+      type(elmm_stats) :: st
+    end function
   end interface
 end module elmm_gpu

@@ -11,7 +11,8 @@ oracle.
   value) of the single domain and of the oracle, max |div u| below 1e-10;
   the split changes only the order of the z solve's operations;
 * mixed: within 1e-5 of the single-domain mixed path;
-* even and uneven splits, 2 and 3 slabs, uniform and stretched z.
+* even and uneven splits, 2 and 3 slabs, uniform and stretched z, slabs
+  short enough for the tiled sweep kernels and taller ones.
 """
 import numpy as np
 import pytest
@@ -78,4 +79,24 @@ def test_fp64_slabs_follow_the_oracle_on_a_stretched_grid():
     e = _errs(interiors(g, *b.download()), interiors(g, *o.state()))
     print("stretched, 3 slabs, 4 steps vs oracle:", e, s.max_div)
     assert max(e[:3]) < 1e-12 and e[3] < 1e-11 and s.max_div < 1e-10, e
+    b.close()
+
+
+def test_tall_slabs_take_the_column_kernels():
+    """A slab taller than the tiled sweeps allow (300 levels) makes every
+    slab run the one-thread-per-column sweep kernels: FP64 against the
+    single domain."""
+    cfg = make_config(32, 32, 440, sgstype=0)
+    st = log_profile_state(grid_of(cfg), seed=2)
+    a, b = L.Domain(cfg), L.Slabs(cfg, 2, devices=[0, 0], nz=(300, 140))
+    a.upload(*st)
+    b.upload(*st)
+    a.project(1.0)
+    b.project(1.0)
+    a.step(2)
+    s = b.step(2)
+    e = _errs(b.download(), a.download())
+    print("300-level slabs vs single domain:", e, s.max_div)
+    assert max(e[:3]) < 1e-12 and e[3] < 1e-11 and s.max_div < 1e-10, e
+    a.close()
     b.close()
