@@ -309,6 +309,9 @@ struct BatchT {
   // the duration of such a call; fstage holds the floats on the device
   int hostf = 0;
   float *fstage = nullptr;
+  // the float side of the pipelined host transfers (upload_all /
+  // download_all with hostf): one buffer per double staging buffer
+  float *fpipe[2] = {nullptr, nullptr};
   cudaGraphExec_t step_exec = nullptr;
   bool step_has_cfl = false;
   double time = 0;
@@ -412,6 +415,45 @@ struct BatchT {
       n = std::max(n, pe);
     }
     return dalloc((void **)&fstage, n * sizeof(float));
+  }
+  int ensure_fpipe() {
+    for (auto &f : fpipe)
+      if (!f) {
+        int r = dalloc((void **)&f, stage_elems * sizeof(float));
+        if (r) return r;
+      }
+    return ELMM_OK;
+  }
+  // Pipelined host copy of n elements of a host array of the call's type
+  // into staging buffer b (on the side stream), then made double in dstage
+  // / dstage2 on the stream: returns the double buffer
+  int h2d_pipe(int b, const void *host, size_t n, double **out) {
+    double *stg = b ? dstage2 : dstage;
+    CU(cudaStreamWaitEvent(side, ev_stage[b][1], 0));
+    if (!hostf) {
+      CU(cudaMemcpyAsync(stg, host, n * sizeof(double), cudaMemcpyHostToDevice, side));
+      CU(cudaEventRecord(ev_stage[b][0], side));
+      CU(cudaStreamWaitEvent(stream, ev_stage[b][0], 0));
+    } else {
+      CU(cudaMemcpyAsync(fpipe[b], host, n * sizeof(float), cudaMemcpyHostToDevice, side));
+      CU(cudaEventRecord(ev_stage[b][0], side));
+      CU(cudaStreamWaitEvent(stream, ev_stage[b][0], 0));
+      k_widen<<<kPackBlocks, 256, 0, stream>>>(stg, fpipe[b], (long long)n);
+    }
+    *out = stg;
+    return ELMM_OK;
+  }
+  // the packed double buffer b to a host array of the call's type, the host
+  // copy on the side stream
+  int d2h_pipe(int b, void *host, size_t n) {
+    const double *stg = b ? dstage2 : dstage;
+    if (hostf) k_narrow<<<kPackBlocks, 256, 0, stream>>>(fpipe[b], stg, (long long)n);
+    CU(cudaEventRecord(ev_stage[b][0], stream));
+    CU(cudaStreamWaitEvent(side, ev_stage[b][0], 0));
+    if (hostf) CU(cudaMemcpyAsync(host, fpipe[b], n * sizeof(float), cudaMemcpyDeviceToHost, side));
+    else CU(cudaMemcpyAsync(host, stg, n * sizeof(double), cudaMemcpyDeviceToHost, side));
+    CU(cudaEventRecord(ev_stage[b][1], side));
+    return ELMM_OK;
   }
   // the offsets the pack of velocity component comp of domain d adds back, or null
   const float *pack_offsets(int d, int comp) const {
@@ -1940,8 +1982,9 @@ struct BatchT {
   // every host copy runs on the side stream into a staging buffer (Pr into
   // its own image) while the stream unpacks the field before it.  Needs the
   // two staging buffers; otherwise the field-by-field calls.
-  int upload_all(int d, const double *U, const double *V, const double *W, const double *Pr, const double *Th) {
-    if (!two_stages() || !ev_pr) {
+  // U..Th: host arrays of the call's type (double, or float with hostf)
+  int upload_all(int d, const void *U, const void *V, const void *W, const void *Pr, const void *Th) {
+    if (!two_stages() || !ev_pr || (hostf && ensure_fpipe())) {
       int r = upload(d, U, V, W, Pr);
       if (r || !Th) return r;
       return upload_temperature(d, Th);
@@ -1952,13 +1995,20 @@ struct BatchT {
     if (frame_pending) CU(cudaStreamWaitEvent(stream, ev_packed, 0));
     const Dom<T> &h = hdom[d];
     CU(cudaMemsetAsync(dbad, 0, sizeof(int), stream));
-    const double *src[4] = {U, V, W, Th};
+    const void *src[4] = {U, V, W, Th};
     int b = 0;
     for (int f = 0; f < 5; f++) {
-      if (f == 3) {  // Pr into its own image, no staging buffer
+      if (f == 3) {  // Pr into its own image, no staging buffer (a float Pr through a staging buffer)
         HostBox hp = hbox_p(d);
         size_t np = (size_t)hp.n0 * hp.n1 * hp.n2;
-        if (Pr) {
+        if (Pr && hostf) {
+          double *stg;
+          if (int r = h2d_pipe(b, Pr, np, &stg)) return r;
+          CU(cudaMemcpyAsync(pr_image[d], stg, np * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+          CU(cudaEventRecord(ev_stage[b][1], stream));
+          b ^= 1;
+          k_unpack<T><<<kPackBlocks, 256, 0, stream>>>(ddom + d, h.P, pr_image[d], hp, h.nx, h.ny, h.nz, dbad);
+        } else if (Pr) {
           CU(cudaMemcpyAsync(pr_image[d], Pr, np * sizeof(double), cudaMemcpyHostToDevice, side));
           CU(cudaEventRecord(ev_pr, side));
           CU(cudaStreamWaitEvent(stream, ev_pr, 0));
@@ -1973,11 +2023,8 @@ struct BatchT {
       if (c == 3 && !Th) continue;
       const size_t n = c < 3 ? (size_t)hbox_vel(d, c).n0 * hbox_vel(d, c).n1 * hbox_vel(d, c).n2
                              : (size_t)(h.nx + 6) * (h.ny + 6) * (h.nz + 6);
-      double *stg = b ? dstage2 : dstage;
-      CU(cudaStreamWaitEvent(side, ev_stage[b][1], 0));
-      CU(cudaMemcpyAsync(stg, src[c], n * sizeof(double), cudaMemcpyHostToDevice, side));
-      CU(cudaEventRecord(ev_stage[b][0], side));
-      CU(cudaStreamWaitEvent(stream, ev_stage[b][0], 0));
+      double *stg;
+      if (int r = h2d_pipe(b, src[c], n, &stg)) return r;
       if (c < 3) {
         HostBox hb = hbox_vel(d, c);
         const float *off = stage_offsets(d, c, stg, hb);
@@ -2002,15 +2049,15 @@ struct BatchT {
   }
   // the state and the temperature back to the host, the pack of one field
   // overlapping the host copy of the one before
-  int download_all(int d, double *U, double *V, double *W, double *Pr, double *Th) {
+  int download_all(int d, void *U, void *V, void *W, void *Pr, void *Th) {
     if (Th && !hdom[d].buoy) return fail(ELMM_ERR_INVALID_ARG, "no temperature field (enable_buoyancy is 0)");
-    if (!two_stages()) {
+    if (!two_stages() || (hostf && ensure_fpipe())) {
       int r = download(d, U, V, W, Pr);
       if (r || !Th) return r;
       return download_field(d, ELMM_FIELD_TEMPERATURE, Th);
     }
     CU(cudaSetDevice(device));
-    double *dst[5] = {U, V, W, Pr, Th};
+    void *dst[5] = {U, V, W, Pr, Th};
     const int fid[5] = {ELMM_FIELD_U, ELMM_FIELD_V, ELMM_FIELD_W, ELMM_FIELD_PR, ELMM_FIELD_TEMPERATURE};
     int b = 0;
     for (int f = 0; f < 5; f++) {
@@ -2018,10 +2065,7 @@ struct BatchT {
       double *stg = b ? dstage2 : dstage;
       CU(cudaStreamWaitEvent(stream, ev_stage[b][1], 0));
       size_t n = pack(d, fid[f], stg, stream);
-      CU(cudaEventRecord(ev_stage[b][0], stream));
-      CU(cudaStreamWaitEvent(side, ev_stage[b][0], 0));
-      CU(cudaMemcpyAsync(dst[f], stg, n * sizeof(double), cudaMemcpyDeviceToHost, side));
-      CU(cudaEventRecord(ev_stage[b][1], side));
+      if (int r = d2h_pipe(b, dst[f], n)) return r;
       b ^= 1;
     }
     CU(cudaStreamSynchronize(side));
@@ -2030,7 +2074,7 @@ struct BatchT {
     return ELMM_OK;
   }
   // TMarchRK3 on host arrays: upload, nsteps steps, download
-  int march_host(double *U, double *V, double *W, double *Pr, double *Th, int nsteps, elmm_stats *st) {
+  int march_host(void *U, void *V, void *W, void *Pr, void *Th, int nsteps, elmm_stats *st) {
     if (nd != 1) return fail(ELMM_ERR_INVALID_ARG, "host-array steps are per single-domain handle");
     int r = upload_all(0, U, V, W, Pr, Th);
     if (r) return r;
@@ -2539,14 +2583,7 @@ int elmm_march_host_float(elmm_handle *h, float *U, float *V, float *W, float *P
                           elmm_stats *stats) {
   if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
   if (nsteps < 0) return fail(ELMM_ERR_INVALID_ARG, "nsteps < 0");
-  return with_float_host(h->b, [&](auto &b) {
-    int r = b.upload(0, U, V, W, Pr);
-    if (!r && Temperature) r = b.upload_temperature(0, Temperature);
-    if (!r) r = b.step(nsteps, stats);
-    if (!r) r = b.download(0, U, V, W, Pr);
-    if (!r && Temperature) r = b.download_field(0, ELMM_FIELD_TEMPERATURE, Temperature);
-    return r;
-  });
+  return with_float_host(h->b, [&](auto &b) { return b.march_host(U, V, W, Pr, Temperature, nsteps, stats); });
 }
 
 int elmm_set_puffs(elmm_handle *h, const elmm_puff *puffs, int32_t npuffs, const elmm_puff_volume *volumes,
