@@ -788,8 +788,8 @@ struct BatchT {
       case LK_MOM: return ((h.nx + MX - 1) / MX) * ((h.ny + MY - 1) / MY) * ((h.nz + MKC - 1) / MKC);
       case LK_MOMT: return ((h.nx + MX - 1) / MX) * ((h.ny + MY - 1) / MY) * ((h.nz + tune_mom_kc - 1) / tune_mom_kc);
       case LK_SGST: return ((h.nx + MX - 1) / MX) * ((h.ny + MY - 1) / MY) * ((h.nz + tune_sgs_kc - 1) / tune_sgs_kc);
-      case LK_PROJ: return fp32_pairs(h) ? 0 : tiles(LK_MOM, h);
-      case LK_PROJ2: return fp32_pairs(h) ? tiles(LK_MOM, h) : 0;
+      case LK_PROJ: return fp32_pairs(h) && !slab_mode ? 0 : tiles(LK_MOM, h);
+      case LK_PROJ2: return fp32_pairs(h) && !slab_mode ? tiles(LK_MOM, h) : 0;
       case LK_SHELL: return (int)((shell_cells(h.nx, h.ny, h.nz) + kShellThreads - 1) / kShellThreads);
       case LK_XREG: {
         if (!fft_reg_supported(h.nx)) return 0;
@@ -1133,8 +1133,12 @@ struct BatchT {
   void k_project_any(double coef_alpha2, int use_dt, int in_place, int gate) {
     if (ls[LK_PROJ].total > 0) {
       nlaunch++;
-      k_project<T><<<gsz(6, ls[LK_PROJ].total), MX * MY, 0, stream>>>(ddom, ls[LK_PROJ].l(), coef_alpha2, use_dt,
-                                                                       in_place, gate);
+      if (slab_mode)
+        k_project<T, true><<<gsz(6, ls[LK_PROJ].total), MX * MY, 0, stream>>>(ddom, ls[LK_PROJ].l(), coef_alpha2,
+                                                                             use_dt, in_place, gate);
+      else
+        k_project<T><<<gsz(6, ls[LK_PROJ].total), MX * MY, 0, stream>>>(ddom, ls[LK_PROJ].l(), coef_alpha2, use_dt,
+                                                                         in_place, gate);
     }
     if constexpr (std::is_same<T, float>::value) {
       if (ls[LK_PROJ2].total > 0) {

@@ -65,7 +65,10 @@ __global__ void __launch_bounds__(kFFTThreads) k_fftx_inv(const Dom<T> *__restri
 // the partial sums of the top layer for FixPressureToReference.  A block
 // marches up an MX x MY column of MKC planes; the inputs of plane k+1 are in
 // flight while plane k is written, and Phi(k+1) of plane k is Phi of k+1.
-template <typename T>
+// HZ: the domains are slabs whose top face is shared (BC_HALO); a
+// compile-time choice, since a run-time test of the face here cost the
+// kernel a fifth of its speed.
+template <typename T, bool HZ = false>
 __global__ void __launch_bounds__(MX *MY) k_project(const Dom<T> *__restrict__ doms, Launch L, double coef_alpha2,
                                                     int use_dt, int in_place, int gate) {
   __shared__ double red[MX * MY / 32];
@@ -102,9 +105,11 @@ __global__ void __launch_bounds__(MX *MY) k_project(const Dom<T> *__restrict__ d
     const bool px = d.bt[SIDE_WE] == BC_PERIODIC, py = d.bt[SIDE_SO] == BC_PERIODIC, pz = d.bt[SIDE_BO] == BC_PERIODIC;
     const long long oe = i < nx ? 1 : (px ? 1 - nx : 0);
     const long long on = j < ny ? pitch : (py ? pitch - (long long)ny * pitch : 0);
-    // a slab's top neighbour plane is the exchanged ghost plane
-    const bool hz = d.bt[SIDE_TO] == BC_HALO;
-    auto ot = [&](int kk) -> long long { return kk < nz || hz ? plane : (pz ? plane - (long long)nz * plane : 0); };
+    // past the top: the periodic image, the cell itself, or (HZ: a slab's
+    // top face) the exchanged ghost plane
+    auto ot = [&](int kk) -> long long {
+      return kk < nz || HZ ? plane : (pz ? plane - (long long)nz * plane : 0);
+    };
     T phi = 0, pe = 0, pn = 0, pt = 0, u0 = 0, v0 = 0, w0 = 0, p0 = 0;
     if (inside) {
       phi = __ldg(Phi + c); pe = __ldg(Phi + c + oe); pn = __ldg(Phi + c + on); pt = __ldg(Phi + c + ot(k0));
@@ -174,7 +179,8 @@ __global__ void __launch_bounds__(MX *MY) k_project(const Dom<T> *__restrict__ d
 
 // k_project for FP32 domains with an even Prnx (x is periodic for every
 // domain): two x-adjacent cells per thread, float2 loads and stores, the
-// same tiles (MX x MY x MKC) and partial sums per tile column.
+// same tiles (MX x MY x MKC) and partial sums per tile column.  Slabs of a
+// split domain take k_project<float, true> instead.
 __global__ void __launch_bounds__(MX *MY / 2) k_project_pair(const Dom<float> *__restrict__ doms, Launch L,
                                                           double coef_alpha2, int use_dt, int in_place, int gate) {
   typedef float T;
@@ -210,9 +216,7 @@ __global__ void __launch_bounds__(MX *MY / 2) k_project_pair(const Dom<float> *_
     const bool last = i + 1 >= nx;
     const long long oe = !last ? 2 : (px ? 1 - i : 0);  // the neighbour pair; for a wall, the cell itself
     const long long on = j < ny ? pitch : (py ? pitch - (long long)ny * pitch : 0);
-    // a slab's top neighbour plane is the exchanged ghost plane
-    const bool hz = d.bt[SIDE_TO] == BC_HALO;
-    auto ot = [&](int kk) -> long long { return kk < nz || hz ? plane : (pz ? plane - (long long)nz * plane : 0); };
+    auto ot = [&](int kk) -> long long { return kk < nz ? plane : (pz ? plane - (long long)nz * plane : 0); };
     auto ld2 = [](const T *p, long long o) { return __ldg(reinterpret_cast<const float2 *>(p + o)); };
     float2 phi = {0, 0}, pe = {0, 0}, pn = {0, 0}, pt = {0, 0}, u0 = {0, 0}, v0 = {0, 0}, w0 = {0, 0}, p0 = {0, 0};
     auto east = [&](const float2 &own, long long cc) {

@@ -213,12 +213,18 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
 // the same order as k_scalar.  A block is 16 x 8 threads, a tile 32 x 8 cells.
 constexpr int SPX = 16;
 #ifndef ELMM_SCALAR_PAIR_MIN_BLOCKS
-#define ELMM_SCALAR_PAIR_MIN_BLOCKS 5
+#define ELMM_SCALAR_PAIR_MIN_BLOCKS 3
 #endif
 
 __device__ __forceinline__ float2 ld2(const float *p, long long o) {
   return __ldg(reinterpret_cast<const float2 *>(p + o));
 }
+
+// the in-plane inputs of a cell pair at one level (k_scalar_pair loads those
+// of level k + 1 while it computes level k)
+struct PairPlane {
+  float2 sm, sp, km, kp, um, u0, vs, vn, wt, sym2, sym1, syp1, syp2, kym, kyp, told;
+};
 
 // SPY: the rows of a tile, a tuning choice (8 or 4; the arithmetic of a
 // cell does not depend on it)
@@ -275,17 +281,33 @@ __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SP
     float2 wb = ld2(W, cc - plane);
     float2 fzb = make_float2(kappa_flux<T>(wb.x, sz[0].x, sz[1].x, sz[2].x, sz[3].x),
                              kappa_flux<T>(wb.y, sz[0].y, sz[1].y, sz[2].y, sz[3].y));
+    auto load_plane = [&](long long c) {
+      PairPlane p;
+      p.sm = ld2(S, c + oxm); p.sp = ld2(S, c + oxp);  // S(i-2, i-1), S(i+2, i+3)
+      p.km = ld2(K, c + oxm); p.kp = ld2(K, c + oxp);  // .y = K(i-1), .x = K(i+2)
+      p.um = ld2(U, c - 2); p.u0 = ld2(U, c);          // .y = U(i-1); U(i), U(i+1)
+      p.vs = ld2(V, c - pitch); p.vn = ld2(V, c);
+      p.wt = ld2(W, c);
+      p.sym2 = ld2(S, c + oy[0]); p.sym1 = ld2(S, c + oy[1]); p.syp1 = ld2(S, c + oy[3]); p.syp2 = ld2(S, c + oy[4]);
+      p.kym = ld2(K, c + oy[1]); p.kyp = ld2(K, c + oy[3]);
+      p.told = stage1 ? make_float2(0.f, 0.f) : ld2(Sadv, c);
+      return p;
+    };
+    PairPlane cur = load_plane(cc);
     for (int k = k0; k <= k1; k++) {
+      // the next level's inputs are requested before this level's arithmetic
+      PairPlane nxt = cur;
+      float2 sz_n = sz[4], kz_n = kz[2];
+      if (k < k1) {
+        nxt = load_plane(cc + plane);
+        sz_n = ld2(S, cc + 3 * plane + zoff(k + 3));
+        kz_n = ld2(K, cc + 2 * plane + zoff(k + 2));
+      }
       const float2 s0 = sz[2];
-      const float2 sm = ld2(S, cc + oxm), sp = ld2(S, cc + oxp);  // S(i-2, i-1), S(i+2, i+3)
-      const float2 km = ld2(K, cc + oxm), kp = ld2(K, cc + oxp);  // .y = K(i-1), .x = K(i+2)
-      const float2 um = ld2(U, cc - 2), u0 = ld2(U, cc);          // .y = U(i-1); U(i), U(i+1)
-      const float2 vs = ld2(V, cc - pitch), vn = ld2(V, cc);
-      const float2 wt = ld2(W, cc);
-      const float2 sym2 = ld2(S, cc + oy[0]), sym1 = ld2(S, cc + oy[1]), syp1 = ld2(S, cc + oy[3]),
-                   syp2 = ld2(S, cc + oy[4]);
-      const float2 kym = ld2(K, cc + oy[1]), kyp = ld2(K, cc + oy[3]);
-      const float2 told = stage1 ? make_float2(0.f, 0.f) : ld2(Sadv, cc);
+      const float2 sm = cur.sm, sp = cur.sp, km = cur.km, kp = cur.kp, um = cur.um, u0 = cur.u0;
+      const float2 vs = cur.vs, vn = cur.vn, wt = cur.wt;
+      const float2 sym2 = cur.sym2, sym1 = cur.sym1, syp1 = cur.syp1, syp2 = cur.syp2;
+      const float2 kym = cur.kym, kyp = cur.kyp, told = cur.told;
       // x faces: low face of cell i, the face between the pair, high face of
       // i+1, with the full face velocities (stored deviation + level offset)
       const T uo = vel_off(d, 0, k), vo = vel_off(d, 1, k);
@@ -352,16 +374,16 @@ __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SP
       *reinterpret_cast<float2 *>(Sadv + cc) = out_a;
       *reinterpret_cast<float2 *>(Snew + cc) = out_n;
       if (k < k1) {
-        const long long cn = cc + plane;
 #pragma unroll
         for (int q = 0; q < 4; q++) sz[q] = sz[q + 1];
-        sz[4] = ld2(S, cn + 2 * plane + zoff(k + 3));
+        sz[4] = sz_n;
         kz[0] = kz[1];
         kz[1] = kz[2];
-        kz[2] = ld2(K, cn + plane + zoff(k + 2));
+        kz[2] = kz_n;
         wb = wt;
         fzb = fzt;
-        cc = cn;
+        cc += plane;
+        cur = nxt;
       }
     }
   }
