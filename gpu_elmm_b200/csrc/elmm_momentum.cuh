@@ -889,7 +889,7 @@ struct SgsShape {
 };
 template <>
 struct SgsShape<float> {
-  static constexpr int cpt = 2, threads = MX * MY / 2, min_blocks = 6;
+  static constexpr int cpt = 2, threads = MX * MY / 2, min_blocks = 7;
 };
 
 template <typename T, int KC = MKC>
