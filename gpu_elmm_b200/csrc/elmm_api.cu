@@ -188,8 +188,8 @@ static int check_config(const elmm_config &c) {
   }
   if (c.wallmodeltype > 0)
     for (int s = 0; s < 6; s++)
-      if (c.Btype[s] == ELMM_BC_NOSLIP && !(c.z0[s] > 0))
-        return fail(ELMM_ERR_INVALID_CONFIG, "only the rough-wall (z0 > 0) wall model is implemented");
+      if (c.Btype[s] == ELMM_BC_NOSLIP && !(c.z0[s] >= 0))
+        return fail(ELMM_ERR_INVALID_CONFIG, "z0 must be zero (smooth wall) or positive (rough wall)");
   if (c.enable_buoyancy) {
     for (int s = 0; s < 6; s++) {
       const bool per = c.Btype[s] == ELMM_BC_PERIODIC;
@@ -1098,7 +1098,8 @@ struct BatchT {
                                                                                  gate, prref);
   }
   static int chunk_index(int kc) { return kc == 8 ? 0 : kc == 16 ? 1 : 2; }
-  // k_sgs with the tuned z chunk; init: the initial viscosity and diffusivity
+  // k_sgs with the tuned z chunk; init: 0 a stage, 1 the initial viscosity
+  // and diffusivity, 2 the autotuner's timing mode (k_sgs)
   void sgs_kernel(int init) {
     const int q = chunk_index(tune_sgs_kc), g = std::max(1, std::min(ls[LK_SGST].total, cap_sgs[q]));
     if (tune_sgs_kc == 8) k_sgs<T, 8><<<g, SgsShape<T>::threads, smem_sgs, stream>>>(ddom, ls[LK_SGST].l(), init);
@@ -1438,8 +1439,9 @@ struct BatchT {
   // launches it times only write what the next step rewrites before reading
   // it: the spectral buffer, the new value and tendency of a scalar stage,
   // the momentum tendency (a function of the state alone) and U2, and the
-  // viscosity, wall-model fluxes and live diffusivity of the SGS kernel's
-  // stage mode (whose wall-model u* follows from the state alone).  No shape
+  // viscosity and live diffusivity of the SGS kernel's timing mode (which
+  // leaves the wall-model points, and the u* a smooth wall carries from
+  // stage to stage, alone).  No shape
   // changes any result: every cell's arithmetic is the same for every
   // partition.
   int autotune() {
@@ -1490,7 +1492,7 @@ struct BatchT {
     for (int q = 0; q < 3 && !r; q++) {
       tune_sgs_kc = kChunks[q];
       if ((r = rebuild_ls(LK_SGST))) break;
-      tune_ms[7 + q] = time10([&] { sgs_kernel(0); });
+      tune_ms[7 + q] = time10([&] { sgs_kernel(2); });
       if (tune_ms[7 + q] < tune_ms[7 + best_s]) best_s = q;
     }
     tune_mom_kc = kChunks[best_m];
@@ -1721,9 +1723,10 @@ struct BatchT {
     for (int64_t q = 0; q < s->n_wm; q++) {
       const elmm_wm_point &p = s->wm[q];
       const int comp = p.component - 1;
-      if (comp < 0 || comp > 2 || p.direction < 1 || p.direction > 6 || !(p.z0 > 0) ||
+      if (comp < 0 || comp > 2 || p.direction < 1 || p.direction > 6 || !(p.z0 > 0 || (p.z0 == 0 && h.nu_mol > 0)) ||
           p.xi < 1 || p.xi > h.ext[comp][0] || p.yj < 1 || p.yj > h.ext[comp][1] || p.zk < 1 || p.zk > h.ext[comp][2])
-        return fail(ELMM_ERR_INVALID_ARG, "solid-face wall-model point out of range (rough walls only)");
+        return fail(ELMM_ERR_INVALID_ARG,
+                    "solid-face wall-model point out of range (or smooth, z0 = 0, without molecular viscosity)");
       WMSolid w{};
       w.c = bidx(h, p.xi, p.yj, p.zk);
       w.comp = comp;

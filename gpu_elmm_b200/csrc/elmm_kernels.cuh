@@ -79,6 +79,13 @@ __device__ inline double wm_rough_ustar(double ustar, double vel, double dist, d
   return vel * 0.41 / log(dist / z0);
 }
 
+// the u* of a wall point: WMRoughStress with a roughness length, else
+// WMFlatStress (src/wallmodels.f90:2262-2275, 1243-1265); ustar is the
+// point's value from the stage before (the start of the flat iteration)
+__device__ inline double wm_ustar(double ustar, double vel, double dist, double z0, double nu) {
+  return z0 > 0 ? wm_rough_ustar(ustar, vel, dist, z0, nu) : wm_flat_ustar(ustar, vel, dist, nu);
+}
+
 // ComputeUVWFluxesWM / fluxes for the point of component comp on side f at
 // cell (i,j,k) (src/wallmodels.f90:2159-2338); the wall-point distance is
 // the one of GetOutsideBoundariesWM_UVW (src/wallmodels.f90:690-909).
@@ -140,7 +147,7 @@ __device__ void wm_point(const Dom<T> &d, int comp, int f, int i, int j, int k, 
   double tv = norm2_3(t);
   const int face = comp * 6 + f;
   double ustar = d.wm_ustar[face][pidx];
-  if (tv != 0) ustar = wm_rough_ustar(ustar, tv, dd, d.z0[f], d.nu_mol);
+  if (tv != 0) ustar = wm_ustar(ustar, tv, dd, d.z0[f], d.nu_mol);
   if (ustar < 0) ustar = 0;
   d.wm_ustar[face][pidx] = ustar;
   double mag = norm2_3(t);

@@ -892,6 +892,10 @@ struct SgsShape<float> {
   static constexpr int cpt = 2, threads = MX * MY / 2, min_blocks = 7;
 };
 
+// init: 0 a stage (viscosity, diffusivity, wall-model points), 1 the initial
+// viscosity and diffusivity after the projection, 2 the autotuner's timing
+// launches (a stage's arithmetic without the wall-model points, whose u*
+// carries the start of the smooth-wall iteration from stage to stage)
 template <typename T, int KC = MKC>
 __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
     k_sgs(const Dom<T> *__restrict__ doms, Launch L, int init) {
@@ -962,7 +966,7 @@ __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
     // src/dynamics.f90:904), and once after the initial projection whenever
     // a scalar is transported (src/initial.f90:4296-4313, which uses the
     // first formula of ComputeTDiff for any molecular viscosity)
-    const bool buoy = d.tdiff_live != 0 || (init && d.nslot > 0);
+    const bool buoy = d.tdiff_live != 0 || (init == 1 && d.nslot > 0);
     const T kap = (T)d.kappa_mol;
     SgsK<T> q;
     q.rdx = (T)(1.0 / d.dx); q.rdy = (T)(1.0 / d.dy);
@@ -1005,7 +1009,7 @@ __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
           if (i == 1) nu[c + nx] = v.v.x;
           if (i + 1 == nx) nu[c + 1 - nx] = v.v.y;
           if (buoy) {
-            const float2 td = init ? make_float2((v.v.x - num) / 0.6f + kap, (v.v.y - num) / 0.6f + kap)
+            const float2 td = init == 1 ? make_float2((v.v.x - num) / 0.6f + kap, (v.v.y - num) / 0.6f + kap)
                                    : make_float2(tdiff_of(v.v.x, num, kap), tdiff_of(v.v.y, num, kap));
             *reinterpret_cast<float2 *>(d.TDiff + c) = td;
           }
@@ -1025,11 +1029,11 @@ __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
           nu[c + qc] = v;
           if (i + qc == 1) nu[c + qc + nx] = v;  // periodic x ghosts (the ghost pass covers y and z)
           if (i + qc == nx) nu[c + qc - nx] = v;
-          if (buoy) d.TDiff[c + qc] = init ? (v - num) / (T)0.6 + kap : tdiff_of(v, num, kap);
+          if (buoy) d.TDiff[c + qc] = init == 1 ? (v - num) / (T)0.6 + kap : tdiff_of(v, num, kap);
         }
       }
       const int wk = wtile | (wmask & ((k == 1 ? 16 : 0) | (k >= nz - 1 ? 32 : 0)));
-      if (ok && wk && !init) {  // the initial eddy viscosity leaves the wall model alone
+      if (ok && wk && init == 0) {  // the initial eddy viscosity and the timing mode leave the wall model alone
 #pragma unroll 1
         for (int qc = 0; qc < CPT; qc++) {
           const int iq = i + qc;

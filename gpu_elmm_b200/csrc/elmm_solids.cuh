@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(128) k_ib_wm(const Dom<T> *__restrict__ doms, 
     for (int m = 0; m < 3; m++) t[m] = t[m] - dot * dist[m] / (dd * dd);
     const double tv = norm2_3(t);
     double us = ustar_state[q];
-    if (tv != 0) us = wm_rough_ustar(us, tv, dd, p.z0, d.nu_mol);
+    if (tv != 0) us = wm_ustar(us, tv, dd, p.z0, d.nu_mol);
     if (us < 0) us = 0;
     ustar_state[q] = us;
     double fp = 0, fm = 0;

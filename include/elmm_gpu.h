@@ -120,7 +120,7 @@ typedef struct elmm_config {
   double filter_ratio;          /* filter_ratios(filtertype), 1.0 (src/filters.f90:14) */
   int32_t sgstype;              /* 0: molecular only, 1: Smagorinsky (src/subgrid.f90:15) */
   int32_t wallmodeltype;        /* 0: off, 1: log-law wall model at no-slip sides */
-  double z0[6];                 /* roughness per side z0W..z0T (src/parameters.f90:145) */
+  double z0[6];                 /* roughness per side z0W..z0T (src/parameters.f90:145); 0: smooth wall (WMFlatStress) */
   int32_t enable_pr_gradient_x_uniform, enable_pr_gradient_y_uniform;
   double pr_gradient_x, pr_gradient_y; /* mean pressure-gradient forcing (src/dynamics.f90:83-117) */
   int32_t precision;            /* ELMM_PREC_* */
@@ -289,7 +289,8 @@ typedef struct elmm_ib_point {
  * GetSolidBodiesWM_UVW, src/immersedboundary.f90:139-306): a free velocity
  * point of `component` (1 U, 2 V, 3 W) whose neighbour in `direction`
  * (1..6 = -x, +x, -y, +y, -z, +z) is solid; dist is the vector to the
- * nearest point of the body, z0 its roughness length (> 0). */
+ * nearest point of the body, z0 its roughness length (> 0; 0 for a smooth
+ * face, which needs a positive molecular viscosity). */
 typedef struct elmm_wm_point {
   int32_t component, direction;
   int32_t xi, yj, zk, reserved;

@@ -641,7 +641,12 @@ static void ComputeUVWFluxesWM(Domain &d) {
         double dot = t[0] * dist[0] + t[1] * dist[1] + t[2] * dist[2];
         for (int m = 0; m < 3; m++) t[m] = t[m] - dot * dist[m] / (dd * dd);
         double tv = norm2_3(t);
-        if (tv != 0) WMRoughUstar(d, p.ustar, tv, dd, p.z0);
+        // WMRoughStress with a roughness length, WMFlatStress for a smooth wall
+        // (wallmodels.f90:2262-2275; WMFlatStress, :1243-1265)
+        if (tv != 0) {
+          if (p.z0 > 0) WMRoughUstar(d, p.ustar, tv, dd, p.z0);
+          else WMFlatUstar(d, p.ustar, tv, dd);
+        }
         if (p.ustar < 0) p.ustar = 0;
         double mag = norm2_3(t);
         if (mag > eps) {

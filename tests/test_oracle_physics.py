@@ -263,3 +263,32 @@ def test_puff_windows_follow_prepare_puffs():
     # puff 0: release at t = 0.02 (negative fraction), full steps at 0.04, 0.06, then closed;
     # cleared at the next release (t = 0.12, the 7th step)
     assert s1 == [0.0, 0.0, 0.06, 0.12, 0.12, 0.12, 0.0, 0.06, 0.12]
+
+
+def test_smooth_wall_ustar_follows_the_log_law():
+    """A smooth bottom wall (z0 = 0, WMFlatStress): for a uniform flow U = 5
+    every diffusive and advective flux vanishes except the wall flux, so the
+    U tendency of the first level is -u*^2 / dz.  Its u* satisfies the law of
+    WMFlatUstar (src/wallmodels.f90:1190-1240) in the logarithmic layer,
+    u = u* (ln(z+)/0.4 + 5.5), to the iteration's tolerance (1e-4); a rough
+    wall gives u* = 0.41 u / ln(z/z0) instead (WMRoughUstar)."""
+    import math
+    nu, dz, vel = 1.0 / 70000, 0.5, 5.0
+    cfg = make_config(16, 12, 8, dz=dz, z0=0.0, nu=nu)
+    g = grid_of(cfg)
+    U, V, W, Pr = (np.zeros(s) for s in (g.shape_u(), g.shape_v(), g.shape_w(), g.shape_p()))
+    U[...] = vel
+    o = Oracle(cfg)
+    o.set_state(U, V, W, Pr)
+    o.run_stage(1, 2)                       # SGS with the wall fluxes, then the momentum tendency
+    tend = o.get_field(8)[2 + 1, 2 + 1:2 + 1 + g.Uny, 2 + 1:2 + 1 + g.Unx]   # Ustar(:, :, 1)
+    assert np.ptp(tend) == 0 and tend.max() < 0
+    us = math.sqrt(-tend.max() * dz)
+    zpl = (dz / 2) * us / nu
+    assert zpl > 30                         # the logarithmic branch
+    assert abs(vel / us - (math.log(zpl) / 0.4 + 5.5)) / (vel / us) < 1e-3
+    o2 = Oracle(make_config(16, 12, 8, dz=dz, z0=1e-4, nu=nu))
+    o2.set_state(U, V, W, Pr)
+    o2.run_stage(1, 2)
+    us2 = math.sqrt(-o2.get_field(8)[3, 3, 3] * dz)
+    assert abs(us2 - vel * 0.41 / math.log((dz / 2) / 1e-4)) < 1e-12

@@ -128,8 +128,8 @@ def test_mixed_cubes_follow_fp64():
 def test_set_solids_rejects_what_it_cannot_apply():
     """elmm_set_solids refuses (ELMM_ERR_INVALID_ARG = 6) lists it could not
     apply exactly: a forcing point next to a periodic boundary, an
-    interpolation point that is itself a forcing point, a smooth solid wall;
-    None removes the bodies again."""
+    interpolation point that is itself a forcing point, a negative
+    roughness length; None removes the bodies again."""
     from gpu_elmm_b200 import lib as L
     cfg = _cfg()
     s = build_solids(cfg, _boxes())
@@ -156,7 +156,7 @@ def test_set_solids_rejects_what_it_cannot_apply():
     assert code(bad) == 6
     bad = build_solids(cfg, _boxes())
     c, dr, i, j, k, dv, z0 = bad.wm[0]
-    bad.wm[0] = (c, dr, i, j, k, dv, 0.0)
+    bad.wm[0] = (c, dr, i, j, k, dv, -1.0)
     assert code(bad) == 6
     assert code(s) == 0 and code(None) == 0 and code(s) == 0
     d.step(1)
