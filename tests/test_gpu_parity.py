@@ -154,6 +154,38 @@ def test_pressure_conditioning_floor():
     assert gpu < 10 * max(floor, 1e-13)
 
 
+def test_fp64_pressure_gradient_and_rms_error():
+    """The FP64 pressure measured the other two ways: the error of its
+    gradient (the differences the momentum equation reads), relative to the
+    largest gradient, and the error of P relative to its RMS, after 10 steps
+    against the oracle.  Neither is below 1e-12 (measured: gradient ~4e-12,
+    RMS-relative ~3e-11): the error is not a shift of the pressure level
+    but the conditioning floor of the projection, so the bar is the
+    oracle's own spread, the oracle against itself with the initial state
+    perturbed by ~1 ulp, measured the same way; the GPU stays within 10 of it."""
+    cfg = make_config(64, 64, 32)
+    g, o, d, st = pair(cfg)
+    s0 = o.state()
+    rng = np.random.default_rng(4)
+    pert = [x * (1 + 1e-16 * rng.standard_normal(x.shape)) for x in s0[:3]] + [s0[3]]
+    o2 = Oracle(cfg)
+    o2.set_state(*pert)
+    o.step(10)
+    o2.step(10)
+    d.step(10)
+    Pg = interiors(g, *d.download())[3]
+    Po = interiors(g, *o.state())[3]
+    Pp = interiors(g, *o2.state())[3]
+
+    def measures(P):
+        grad = max(rel(np.diff(P, axis=a), np.diff(Po, axis=a)) for a in range(3))
+        return rel(P, Po), grad, float(np.abs(P - Po).max() / np.sqrt(np.mean(Po ** 2)))
+    gpu, floor = measures(Pg), measures(Pp)
+    print("FP64 pressure after 10 steps (max-relative, gradient, RMS-relative): gpu", gpu, "1-ulp floor", floor)
+    for a, b in zip(gpu, floor):
+        assert a < 10 * max(b, 1e-13), (gpu, floor)
+
+
 @pytest.mark.parametrize("case", ["noslip_top", "periodic_z", "stretched_z", "pr_gradient"])
 def test_boundary_and_grid_variants(case):
     kw = {}
