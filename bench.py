@@ -355,6 +355,7 @@ def run_ours(args, ws, rank, local):
     dm.close()
     long_run = long_run_leg(st, T0, local) if rank == 0 else None
     cubes = cubes_leg(local) if rank == 0 else None
+    slabs = slabs_leg(local) if rank == 0 else None
     batched = batched_leg(args, ws, rank, local)
     serving = serving_leg(args, ws, rank, local)
 
@@ -388,6 +389,7 @@ def run_ours(args, ws, rank, local):
             "wall_s_timed": wall,
             "long_run": long_run,
             "cubes": cubes,
+            "slabs": slabs,
             "batched": batched,
             "serving": serving,
         }
@@ -436,6 +438,37 @@ def long_run_leg(st, T0, local):
     return {"steps": LONG_STEPS, "rel_err_mixed_vs_fp64": errs,
             "profiles_rel_diff": compare(prof[1].result(), prof[0].result(), keys=("u", "tke", "theta")),
             "profiles_window": f"steps {LONG_STEPS // 2}..{LONG_STEPS}, every {LONG_STEPS // 20}"}
+
+
+def slabs_leg(local, steps=20):
+    """One domain split into z-slabs (elmm_slabs_*), every slab on this GPU:
+    the 256x256x128 channel without the temperature (split domains carry
+    none), mixed, its device time per step against the single-domain handle
+    on the same state, and whether the two states agree bit for bit after
+    the timed steps.  On one GPU this measures the cost of the split (the
+    exchanges, the split z solve, smaller launches), not a speed-up."""
+    from gpu_elmm_b200 import lib as L
+    cfg = make_config(*N, precision=1, cs=0.1)
+    st = log_profile_state(grid_of(cfg), seed=0)
+    out = {"workload": "256x256x128 channel without temperature, mixed, every slab on one GPU", "steps": steps}
+    a = L.Domain(make_config(*N, precision=1, cs=0.1, device=local))
+    a.upload(*st)
+    a.project(1.0)
+    a.step(3)
+    out["single_ms_per_step"] = a.step(steps).elapsed_ms / steps
+    ref = a.download()
+    a.close()
+    for ns in (2, 4):
+        b = L.Slabs(cfg, ns, devices=[local] * ns)
+        b.upload(*st)
+        b.project(1.0)
+        b.step(3)
+        s = b.step(steps)
+        out[f"slabs{ns}_ms_per_step"] = s.elapsed_ms / steps
+        out[f"slabs{ns}_kernels_per_step"] = s.kernels / steps
+        out[f"slabs{ns}_bit_equal_to_single"] = all(bool(np.array_equal(x, y)) for x, y in zip(b.download(), ref))
+        b.close()
+    return out
 
 
 def cubes_leg(local):

@@ -318,8 +318,8 @@ typedef struct elmm_solids {
  * arrays may be freed afterwards).  Requirements, checked here
  * (ELMM_ERR_INVALID_ARG otherwise): indices in range; no interpolation point
  * of a list is a forcing point of the same list; no forcing or nullified
- * point within one cell of a periodic boundary; a rough bottom wall with the
- * wall model; no temperature and no passive scalars.  The next elmm_step
+ * point within one cell of a periodic boundary; a no-slip bottom wall with
+ * the wall model; no temperature and no passive scalars.  The next elmm_step
  * applies IBMomentum once first, as the first call of TMarchRK3 does
  * (src/tsteps.f90:44-48).  Passing NULL removes the bodies. */
 int elmm_set_solids(elmm_handle *h, const elmm_solids *s);
