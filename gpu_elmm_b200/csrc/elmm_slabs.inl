@@ -47,11 +47,18 @@ struct SlabsT {
   bool tiled = false;
   size_t smem_tile = 0;
   std::vector<cudaEvent_t> pre, post;
-  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  cudaEvent_t t0 = nullptr, t1 = nullptr, ev_fork = nullptr;
   double time = 0;
   int kernels = 0;  // launches of the last call
+  // every slab on one device: one step captured once into a CUDA graph over
+  // the slabs' streams and replayed (slabs on several devices launch eagerly)
+  cudaGraphExec_t step_exec = nullptr;
+  bool step_has_cfl = false;
+  int step_kernels = 0;
 
   ~SlabsT() {
+    if (step_exec) cudaGraphExecDestroy(step_exec);
+    if (ev_fork) cudaEventDestroy(ev_fork);
     for (auto e : pre) if (e) cudaEventDestroy(e);
     for (auto e : post) if (e) cudaEventDestroy(e);
     if (t0) cudaEventDestroy(t0);
@@ -175,7 +182,13 @@ struct SlabsT {
     CU(cudaSetDevice(dev[0]));
     CU(cudaEventCreate(&t0));
     CU(cudaEventCreate(&t1));
+    CU(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
     return ELMM_OK;
+  }
+  bool one_device() const {
+    for (int s = 1; s < ns; s++)
+      if (dev[s] != dev[0]) return false;
+    return true;
   }
 
   // ------------------------------------------------------------ exchanges
@@ -323,9 +336,62 @@ struct SlabsT {
     if ((r = exchange_halos({F_W2}, true, false))) return r;
     return projection(2 * kAlpha[st - 1], 1);
   }
+  // one step of every slab for the captured graph: fork the slabs' streams
+  // from slab 0's, the step (the divergence check included, as in the
+  // single-domain graph), join them back
+  int enqueue_step(bool cfl) {
+    CU(cudaEventRecord(ev_fork, sl[0]->stream));
+    for (int s = 1; s < ns; s++) CU(cudaStreamWaitEvent(sl[s]->stream, ev_fork, 0));
+    if (cfl) each([&](int, BatchT<T> &B) { B.launch_cfl(); });
+    int r = ELMM_OK;
+    for (int st = 1; st <= 3 && !r; st++) r = stage(st);
+    if (r) return r;
+    each([&](int, BatchT<T> &B) { B.launch_divmax(); });
+    for (int s = 1; s < ns; s++) {
+      CU(cudaEventRecord(post[s], sl[s]->stream));
+      CU(cudaStreamWaitEvent(sl[0]->stream, post[s], 0));
+    }
+    return ELMM_OK;
+  }
+  int step_graph(int nsteps, bool cfl) {
+    CU(cudaSetDevice(dev[0]));
+    cudaStream_t s0 = sl[0]->stream;
+    if (!step_exec || step_has_cfl != cfl) {
+      if (step_exec) { cudaGraphExecDestroy(step_exec); step_exec = nullptr; }
+      for (int s = 0; s < ns; s++) sl[s]->nlaunch = 0;
+      CU(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
+      const int r = enqueue_step(cfl);
+      cudaGraph_t g = nullptr;
+      const cudaError_t e = cudaStreamEndCapture(s0, &g);  // ends the capture whatever happened
+      if (r) {
+        if (g) cudaGraphDestroy(g);
+        return r;
+      }
+      if (e != cudaSuccess) return fail(ELMM_ERR_CUDA, std::string("slab step capture: ") + cudaGetErrorString(e));
+      const cudaError_t ei = cudaGraphInstantiate(&step_exec, g, 0);
+      cudaGraphDestroy(g);
+      if (ei != cudaSuccess) return fail(ELMM_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ei));
+      step_has_cfl = cfl;
+      step_kernels = 0;
+      for (int s = 0; s < ns; s++) step_kernels += sl[s]->nlaunch;
+    }
+    CU(cudaEventRecord(t0, s0));
+    for (int n = 0; n < nsteps; n++) CU(cudaGraphLaunch(step_exec, s0));
+    CU(cudaEventRecord(t1, s0));
+    CU(cudaStreamSynchronize(s0));
+    CU(cudaGetLastError());
+    kernels = nsteps * step_kernels;
+    return ELMM_OK;
+  }
   int step(int nsteps, elmm_stats *stats) {
     if (nsteps < 0) return fail(ELMM_ERR_INVALID_ARG, "nsteps must be non-negative");
     const bool cfl = gcfg.enable_CFL_check != 0;
+    if (one_device() && nsteps > 0) {
+      int r = step_graph(nsteps, cfl);
+      if (r) return r;
+      time += nsteps * gcfg.dt;
+      return stats_of(stats, nsteps);
+    }
     int r = begin();
     if (r) return r;
     for (int n = 0; n < nsteps; n++) {

@@ -629,8 +629,10 @@ int elmm_slabs_upload_state(elmm_slabs *h, const double *U, const double *V, con
 int elmm_slabs_download_state(elmm_slabs *h, double *U, double *V, double *W, double *Pr);
 /* PressureCorrection on the uploaded state, as elmm_project. */
 int elmm_slabs_project(elmm_slabs *h, double coef, elmm_stats *stats);
-/* nsteps RK3 steps, as elmm_step (launched eagerly; stats->elapsed_ms is
- * the device time from the first slab's start to the last slab's end). */
+/* nsteps RK3 steps, as elmm_step: with every slab on one device each step
+ * is one CUDA graph over the slabs' streams (captured at the first call);
+ * slabs on several devices launch eagerly.  stats->elapsed_ms is the device
+ * time from the first slab's start to the last slab's end. */
 int elmm_slabs_step(elmm_slabs *h, int32_t nsteps, elmm_stats *stats);
 
 /* Last error message of this thread (static storage). */
