@@ -356,6 +356,7 @@ def run_ours(args, ws, rank, local):
     long_run = long_run_leg(st, T0, local) if rank == 0 else None
     cubes = cubes_leg(local) if rank == 0 else None
     slabs = slabs_leg(local) if rank == 0 else None
+    config0 = config0_leg(local) if rank == 0 and ws == 1 else None
     batched = batched_leg(args, ws, rank, local)
     serving = serving_leg(args, ws, rank, local)
 
@@ -390,6 +391,7 @@ def run_ours(args, ws, rank, local):
             "long_run": long_run,
             "cubes": cubes,
             "slabs": slabs,
+            "config0": config0,
             "batched": batched,
             "serving": serving,
         }
@@ -438,6 +440,47 @@ def long_run_leg(st, T0, local):
     return {"steps": LONG_STEPS, "rel_err_mixed_vs_fp64": errs,
             "profiles_rel_diff": compare(prof[1].result(), prof[0].result(), keys=("u", "tke", "theta")),
             "profiles_window": f"steps {LONG_STEPS // 2}..{LONG_STEPS}, every {LONG_STEPS // 20}"}
+
+
+def config0_leg(local, steps=100, cpu_steps=20):
+    """Config 0, the 64x64x32 channel for its 100 steps: mixed and FP64
+    device throughput from one projected state, the mixed error against FP64
+    after the 100 steps, and the FP64 oracle (native build, every host
+    thread) timed over cpu_steps steps from the same state, with the GPU's
+    FP64 state compared with the oracle's after those steps."""
+    from gpu_elmm_b200 import lib as L
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    orc.build(native=True)
+    threads = orc.set_threads(os.cpu_count() or 1, native=True)
+    n = (64, 64, 32)
+    g = grid_of(make_config(*n))
+    o = orc.Oracle(make_config(*n), native=True)
+    o.set_state(*log_profile_state(g, seed=0))
+    o.project(1.0)
+    st = o.state()
+    out = {"workload": "64x64x32 channel, config-0 physics (no temperature), 100 steps", "cells": g.cells()}
+    doms = {p: L.Domain(make_config(*n, precision=p, device=local)) for p in (0, 1)}
+    for p, d in doms.items():
+        d.upload(*st)
+    t0 = time.perf_counter()
+    o.step(cpu_steps)
+    cpu_s = time.perf_counter() - t0
+    doms[0].step(cpu_steps)
+    out["fp64_vs_oracle_after_%d" % cpu_steps] = [rel(a, b) for a, b in zip(interiors(g, *doms[0].download()),
+                                                                           interiors(g, *o.state()))]
+    doms[0].upload(*st)
+    for p, name in ((1, "mixed"), (0, "fp64")):
+        s_ = doms[p].step(steps)
+        out[name] = {"cell_steps_per_s": g.cells() * steps / (s_.elapsed_ms / 1e3), "ms_per_step": s_.elapsed_ms / steps}
+    out["mixed_over_fp64"] = out["mixed"]["cell_steps_per_s"] / out["fp64"]["cell_steps_per_s"]
+    out["rel_err_mixed_vs_fp64_after_%d" % steps] = [rel(a, b) for a, b in zip(interiors(g, *doms[1].download()),
+                                                                               interiors(g, *doms[0].download()))]
+    out["cpu_oracle"] = {"cell_steps_per_s": g.cells() * cpu_steps / cpu_s, "steps": cpu_steps, "threads": threads,
+                         "build": "oracle/elmm_oracle.cpp, -O3 -march=native -fopenmp (FMA contraction on)"}
+    for d in doms.values():
+        d.close()
+    return out
 
 
 def slabs_leg(local, steps=20):
