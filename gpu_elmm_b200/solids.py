@@ -1,10 +1,11 @@
 """Solid bodies on the staggered grid: the start-up geometry pass of the
-reference for bodies that are axis-aligned boxes, producing the point lists
-that `elmm_set_solids` (include/elmm_gpu.h) takes.
+reference for bodies that are axis-aligned boxes or spheres, producing the
+point lists that `elmm_set_solids` (include/elmm_gpu.h) takes.
 
 This is the host side of the immersed-boundary method, run once per domain;
-the library applies the lists every RK3 stage.  It restates, for convex
-polyhedra whose six planes are the faces of a box:
+the library applies the lists every RK3 stage.  It restates, for a body
+given by its inside test, closest point and closest point outwards
+(methods of Box and Sphere):
 
   * FindInsideCells (src/solidbodies.f90:75-206): Prtype/Utype/Vtype/Wtype
     = body number where the point lies inside the body grown by
@@ -20,6 +21,10 @@ polyhedra whose six planes are the faces of a box:
   * SetNullifiedPoints (src/initial.f90:4861-4962);
   * the bottom-wall points that GetOutsideBoundariesWM_UVW leaves out
     (src/wallmodels.f90:700-820: only Xtype(i,j,1) == 0 and Xtype(i,j,0) <= 0).
+
+Geometry of a sphere (GeometricShapes Sphere, src/geometricshapes.f90:1128-
+1149): inside within r + eps of the centre, Closest along the ray from the
+centre, ClosestOut = Closest (GeometricShape_ClosestOut, :343-349).
 
 Geometry of a box (GeometricShapes ConvexPolyhedron, src/geometricshapes.f90):
 its planes are, in this order, x >= x0, x <= x1, y >= y0, y <= y1, z >= z0,
@@ -63,6 +68,72 @@ class Box:
         # (axis, offset, gl): gl -> coordinate - offset >= -eps, else <= eps
         return ((0, self.x0, True), (0, self.x1, False), (1, self.y0, True), (1, self.y1, False),
                 (2, self.z0, True), (2, self.z1, False))
+
+    def inside(self, x, y, z, eps):
+        """ConvexPolyhedron_Inside: every plane (Plane_Inside, :632-642)."""
+        p = (x, y, z)
+        for axis, off, gl in self.planes():
+            v = p[axis] - off
+            if gl:
+                if not v >= -eps:
+                    return False
+            elif not v <= eps:
+                return False
+        return True
+
+    def mask(self, x, y, z, eps):
+        """inside() on the grid lines x, y, z (1-D arrays): a [k, j, i] mask."""
+        mx = (x - self.x0 >= -eps) & (x - self.x1 <= eps)
+        my = (y - self.y0 >= -eps) & (y - self.y1 <= eps)
+        mz = (z - self.z0 >= -eps) & (z - self.z1 <= eps)
+        return mz[:, None, None] & my[None, :, None] & mx[None, None, :]
+
+    def closest(self, x, y, z):
+        """The nearest point of the box (ConvexPolyhedron_Closest, :721-938)."""
+        return (min(max(x, self.x0), self.x1), min(max(y, self.y0), self.y1), min(max(z, self.z0), self.z1))
+
+    def closest_out(self, x, y, z):
+        """The projection onto the nearest face plane, the first on ties
+        (ConvexPolyhedron_ClosestOut, :940-966)."""
+        p = [x, y, z]
+        best, arg = math.inf, None
+        for axis, off, _ in self.planes():
+            d = abs(p[axis] - off)
+            if d >= 0 and d < best:
+                best, arg = d, (axis, off)
+        q = list(p)
+        q[arg[0]] = arg[1]
+        return tuple(q)
+
+
+@dataclass
+class Sphere:
+    """A solid sphere of radius r centred at (xc, yc, zc) with roughness z0r
+    (GeometricShapes Sphere, src/geometricshapes.f90:142-147)."""
+    xc: float
+    yc: float
+    zc: float
+    r: float
+    z0r: float = 0.1
+
+    def inside(self, x, y, z, eps):
+        """Sphere_Inside (:1128-1134)."""
+        return (self.xc - x) ** 2 + (self.yc - y) ** 2 + (self.zc - z) ** 2 <= (self.r + eps) ** 2
+
+    def mask(self, x, y, z, eps):
+        return ((self.xc - x[None, None, :]) ** 2 + (self.yc - y[None, :, None]) ** 2 +
+                (self.zc - z[:, None, None]) ** 2) <= (self.r + eps) ** 2
+
+    def closest(self, x, y, z):
+        """Sphere_Closest (:1136-1149): the point of the sphere on the ray
+        from the centre through (x, y, z)."""
+        a, b, c = x - self.xc, y - self.yc, z - self.zc
+        t = self.r / math.sqrt(a ** 2 + b ** 2 + c ** 2)
+        return (a * t + self.xc, b * t + self.yc, c * t + self.zc)
+
+    def closest_out(self, x, y, z):
+        """GeometricShape_ClosestOut (:343-349): Closest."""
+        return self.closest(x, y, z)
 
 
 def cube_array(n_per_side: int, edge: float, pitch: float, height: float, *, offset: float, depth: float,
@@ -154,35 +225,20 @@ class Geometry:
             y = y + c.ly
         return x, y, z
 
-    def inside(self, b: Box, x, y, z, eps):
+    def inside(self, b, x, y, z, eps):
+        """CInside: the body's inside test of the periodically wrapped point."""
         x, y, z = self._wrap(x, y, z)
-        p = (x, y, z)
-        for axis, off, gl in b.planes():
-            v = p[axis] - off
-            if gl:
-                if not v >= -eps:
-                    return False
-            elif not v <= eps:
-                return False
-        return True
+        return b.inside(x, y, z, eps)
 
     @staticmethod
-    def closest(b: Box, x, y, z):
-        return (min(max(x, b.x0), b.x1), min(max(y, b.y0), b.y1), min(max(z, b.z0), b.z1))
+    def closest(b, x, y, z):
+        return b.closest(x, y, z)
 
     @staticmethod
-    def closest_out(b: Box, x, y, z):
-        p = [x, y, z]
-        best, arg = math.inf, None
-        for axis, off, _ in b.planes():
-            d = abs(p[axis] - off)
-            if d >= 0 and d < best:
-                best, arg = d, (axis, off)
-        q = list(p)
-        q[arg[0]] = arg[1]
-        return tuple(q)
+    def closest_out(b, x, y, z):
+        return b.closest_out(x, y, z)
 
-    def closest_on_line_out(self, b: Box, x, y, z, x2, y2, z2):
+    def closest_on_line_out(self, b, x, y, z, x2, y2, z2):
         t1, t2 = 0.0, 1.0
         if self.inside(b, x2, y2, z2, 0.0):
             t1 = 1.0
@@ -213,11 +269,7 @@ class Geometry:
         e = self.delta
         xw, yw = np.array([self._wrap(x, 0, 0)[0] for x in xs]), np.array([self._wrap(0, y, 0)[1] for y in ys])
         for nb, b in enumerate(self.boxes, start=1):
-            mx = (xw - b.x0 >= -e) & (xw - b.x1 <= e)
-            my = (yw - b.y0 >= -e) & (yw - b.y1 <= e)
-            mz = (zs - b.z0 >= -e) & (zs - b.z1 <= e)
-            m = mz[:, None, None] & my[None, :, None] & mx[None, None, :]
-            t[m] = nb
+            t[b.mask(xw, yw, zs, e)] = nb
         return t
 
     def _aux_neighbours(self, q):
@@ -529,7 +581,8 @@ class Solids:
 
 
 def build_solids(cfg: ElmmConfig, boxes) -> Solids:
-    """GetSolidBodiesBC + SetNullifiedPoints for the given boxes."""
+    """GetSolidBodiesBC + SetNullifiedPoints for the given bodies (Box and
+    Sphere objects, numbered in list order)."""
     g = Geometry(cfg, boxes)
     s = Solids()
     for comp in (1, 2, 3):

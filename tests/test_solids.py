@@ -232,3 +232,82 @@ def test_batch_with_cubes_and_puffs_equals_the_runs_alone(precision):
     a.close()
     p.close()
     b.close()
+
+
+def _spheres():
+    # two spheres on the stretched grid: one sunk into the ground, one
+    # standing free, centres off the grid lines
+    from gpu_elmm_b200.solids import Sphere
+    return [Sphere(14.3, 13.7, 1.1, 6.2), Sphere(33.6, 31.2, 6.4, 3.7, z0r=0.05)]
+
+
+def test_sphere_geometry_lists():
+    """Spheres (Sphere_Inside / Sphere_Closest): forcing points solid and
+    interpolation points free, every interior solid point an IB point or
+    nullified, the solid volume close to the spheres' volume, the wall-model
+    points' distance vectors pointing from the free point towards the surface
+    (within the surface's curvature) with each sphere's roughness."""
+    cfg = _cfg()
+    bodies = _spheres()
+    s = build_solids(cfg, bodies)
+    g = s.geometry
+    c = s.counts()
+    assert min(c["ib"]) > 0 and min(c["null"]) > 0 and c["scalfl"] > 0 and c["wm"] > 0
+    for q in range(3):
+        t = g.types[q + 1]
+        for (i, j, k), pts, cf in s.ib[q]:
+            assert t[k + 2, j + 2, i + 2] > 0
+            for (a, b, cc) in pts:
+                assert t[cc + 2, b + 2, a + 2] <= 0
+        (nx, ny, nz) = g.grids[q + 1][0]
+        solid = int((t[3:nz + 3, 3:ny + 3, 3:nx + 3] > 0).sum())
+        assert solid == len(s.ib[q]) + len(s.null[q])
+    # Pr cells inside, against the volume above the ground (cell volumes of the stretched grid)
+    cz = g.c
+    t0 = g.types[0]
+    vol = 0.0
+    for k in range(1, NZ + 1):
+        dz = cz.x(cz.zW, k) - cz.x(cz.zW, k - 1)
+        vol += float((t0[k + 2, 3:48 + 3, 3:48 + 3] > 0).sum()) * dz
+    exact = 0.0
+    import math
+    for b in bodies:  # the part above z = 0 (a cap when the centre is near the ground)
+        h = min(2 * b.r, b.r + b.zc)
+        exact += math.pi * h * h * (3 * b.r - h) / 3
+    assert abs(vol - exact) / exact < 0.15, (vol, exact)
+    for comp, dr, i, j, k, dv, z0 in s.wm:
+        assert g.typ(comp, i, j, k) < 0 and z0 in (0.1, 0.05)
+        assert np.linalg.norm(dv) > 0
+
+
+@pytest.mark.gpu
+def test_fp64_spheres_match_the_oracle():
+    """The same device path as the cubes, given the point lists of the
+    spheres: FP64 against the oracle after 3 steps, and the mixed path
+    within 1e-5 of FP64."""
+    from gpu_elmm_b200 import lib as L
+    out = {}
+    for prec in (0, 1):
+        cfg = _cfg(prec)
+        s = build_solids(cfg, _spheres())
+        g, st = _state(cfg)
+        d = L.Domain(cfg)
+        d.upload(*st)
+        d.project(1.0)
+        d.set_solids(s)
+        sd = d.step(3)
+        out[prec] = (d.download(), sd.max_div)
+        d.close()
+    cfg = _cfg(0)
+    s = build_solids(cfg, _spheres())
+    g, st = _state(cfg)
+    o = Oracle(cfg)
+    o.set_state(*st)
+    o.project(1.0)
+    o.set_solids(s)
+    o.step(3)
+    e = [rel(a, b) for a, b in zip(interiors(g, *out[0][0]), interiors(g, *o.state()))]
+    em = [rel(a, b) for a, b in zip(interiors(g, *out[1][0])[:3], interiors(g, *out[0][0])[:3])]
+    print("spheres: FP64 vs oracle", e, "mixed vs FP64", em, "max div", out[0][1], out[1][1])
+    assert max(e[:3]) < 1e-11 and e[3] < 1e-10 and out[0][1] < 1e-10, e
+    assert max(em) < 1e-5 and out[1][1] < 1e-5, em
