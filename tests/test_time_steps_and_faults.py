@@ -152,3 +152,32 @@ def test_a_wait_that_runs_out_is_reported_and_the_handle_recovers(precision):
         assert np.array_equal(a, b)
     d.close()
     ref.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1])
+def test_variable_time_steps_in_a_batch_equal_the_runs_alone(precision):
+    """Each domain of a batch takes its own variable step (k_dt works per
+    domain): two domains of different sizes, targets and starting states,
+    stepped together, equal the same domains stepped alone, bit for bit."""
+    from gpu_elmm_b200 import lib as L
+    kws = [dict(variable_dt=True, cfl=0.35, dt_max=0.1), dict(variable_dt=True, cfl=0.2, dt_max=0.05)]
+    sizes = [(48, 32, 24), (32, 32, 16)]
+    cfgs = [make_config(*n, precision=precision, **kw) for n, kw in zip(sizes, kws)]
+    states = [log_profile_state(grid_of(c), seed=20 + q) for q, c in enumerate(cfgs)]
+    b = L.Batch(cfgs)
+    for q, st in enumerate(states):
+        b.upload(q, *st)
+    b.project(1.0)
+    b.step(4)
+    for q, (c, st) in enumerate(zip(cfgs, states)):
+        d = L.Domain(c)
+        d.upload(*st)
+        d.project(1.0)
+        d.set_tuning(**b.tuning())
+        s = d.step(4)
+        assert s.dt > 0
+        for x, y in zip(b.download(q), d.download()):
+            assert np.array_equal(x, y), q
+        d.close()
+    b.close()
