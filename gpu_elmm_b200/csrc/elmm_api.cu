@@ -330,6 +330,8 @@ struct BatchT {
   size_t arena_bytes = 0;
   // a view steps domains whose fields other batches own, on a borrowed stream
   bool is_view = false;
+  // shell cells per thread of the ghost passes: 4 for several domains, 1 for one
+  int shell_per = 1;
   // one z-slab of a split domain (SlabsT): its configuration carries
   // BC_HALO on the shared faces (checked as the whole domain's beforehand),
   // and its z grid is the whole domain's from level zk0 on
@@ -610,6 +612,7 @@ struct BatchT {
   // device tables of the domains, launch maps and kernel attributes
   int init_tables() {
     const int n = nd;
+    shell_per = n > 1 ? 4 : 1;
     CU(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
     for (int b = 1; b < kBranches; b++) {
       CU(cudaStreamCreateWithFlags(&branch[b], cudaStreamNonBlocking));
@@ -700,7 +703,8 @@ struct BatchT {
     grid_cap[10] = std::is_same<T, float>::value ? cap((const void *)k_project_pair, MX * MY / 2, 0) : 1;
     grid_cap[7] = cap((const void *)k_divres<T>, TX * TY, 0);
     grid_cap[8] = cap((const void *)k_cfl<T>, TX * TY, 0);
-    grid_cap[9] = cap((const void *)k_ghosts<T>, kShellThreads, 0);
+    grid_cap[9] = shell_per == 4 ? cap((const void *)k_ghosts<T, 4>, kShellThreads, 0)
+                                 : cap((const void *)k_ghosts<T>, kShellThreads, 0);
     grid_cap[13] = cap((const void *)k_tri_tile<T, 16>, tri_tile_threads<16>(), smem_trit);
     grid_cap[15] = cap((const void *)k_tri_tile<T, 32>, tri_tile_threads<32>(), smem_trit32);
     grid_cap[11] = cap((const void *)k_scalar<T>, TX * TY, 0);
@@ -790,7 +794,7 @@ struct BatchT {
       case LK_SGST: return ((h.nx + MX - 1) / MX) * ((h.ny + MY - 1) / MY) * ((h.nz + tune_sgs_kc - 1) / tune_sgs_kc);
       case LK_PROJ: return fp32_pairs(h) && !slab_mode ? 0 : tiles(LK_MOM, h);
       case LK_PROJ2: return fp32_pairs(h) && !slab_mode ? tiles(LK_MOM, h) : 0;
-      case LK_SHELL: return (int)((shell_cells(h.nx, h.ny, h.nz) + kShellThreads - 1) / kShellThreads);
+      case LK_SHELL: return (int)((shell_cells(h.nx, h.ny, h.nz) + kShellThreads * shell_per - 1) / (kShellThreads * shell_per));
       case LK_XREG: {
         if (!fft_reg_supported(h.nx)) return 0;
         const int rows = 2 * fft_reg_batch(h.nx);
@@ -1094,7 +1098,11 @@ struct BatchT {
     int nf = 0;
     for (int f : fields) packed |= (unsigned)f << (8 * nf++);
     nlaunch++;
-    k_ghosts<T><<<gsz(9, ls[LK_SHELL].total * nf), kShellThreads, 0, stream>>>(ddom, ls[LK_SHELL].l(), packed, nf,
+    if (shell_per == 4)
+      k_ghosts<T, 4><<<gsz(9, ls[LK_SHELL].total * nf), kShellThreads, 0, stream>>>(ddom, ls[LK_SHELL].l(), packed, nf,
+                                                                                    gate, prref);
+    else
+      k_ghosts<T><<<gsz(9, ls[LK_SHELL].total * nf), kShellThreads, 0, stream>>>(ddom, ls[LK_SHELL].l(), packed, nf,
                                                                                  gate, prref);
   }
   static int chunk_index(int kc) { return kc == 8 ? 0 : kc == 16 ? 1 : 2; }

@@ -337,7 +337,10 @@ __global__ void k_prref(const Dom<T> *__restrict__ doms, int nd, int gate) {
 // src/boundaries.f90:1817-1948), and the pressure only its periodic copies
 // (its other ghosts are never read before the next Bound_Pr).
 // fields: up to four field ids (F_*), one per byte; the grid covers
-// L.total shell tiles of kShellThreads cells per field.
+// L.total shell tiles of kShellThreads x PER cells per field; each thread
+// takes PER cells, all their sources read before any ghost is written (PER
+// 4 for batches, whose many small shells leave the launch latency-bound; 1
+// for a single domain).
 constexpr int kShellThreads = 256;
 
 template <typename T>
@@ -362,7 +365,7 @@ __host__ __device__ __forceinline__ long long shell_cells(int ex, int ey, int ez
   return 2LL * (ex + 2) * (ey + 2) + 2LL * (ex + 2) * ez;
 }
 
-template <typename T>
+template <typename T, int PER = 1>
 __global__ void __launch_bounds__(kShellThreads) k_ghosts(const Dom<T> *__restrict__ doms, Launch L, unsigned fields,
                                                           int nf, int gate, int prref = 0) {
   const int nblk = L.total * nf;  // shell tiles times fields (a few million at most)
@@ -375,43 +378,58 @@ __global__ void __launch_bounds__(kShellThreads) k_ghosts(const Dom<T> *__restri
     const bool vel = fid <= F_W2;
     const int comp = fid % 3;
     const int ex = vel ? d.ext[comp][0] : d.nx, ey = vel ? d.ext[comp][1] : d.ny, ez = vel ? d.ext[comp][2] : d.nz;
-    int w = (t - __ldg(L.starts + di)) * kShellThreads + threadIdx.x;
-    if (w >= (int)shell_cells(ex, ey, ez)) continue;
-    // z faces (full planes), then y faces (k in 1..ez)
-    int i, j, k;
-    const int rx = ex + 2, zf = rx * (ey + 2), yf = rx * ez;
-    if (w < 2 * zf) {
-      const int side = w >= zf;
-      w -= side * zf;
-      j = w / rx; i = w - j * rx; k = side ? ez + 1 : 0;
-    } else {
-      w -= 2 * zf;
-      const int side = w >= yf;
-      w -= side * yf;
-      k = w / rx; i = w - k * rx; k += 1; j = side ? ey + 1 : 0;
-    }
-    if (halo_plane(k, ez, d.bt)) continue;  // the slab exchange fills it
+    const int ncell = (int)shell_cells(ex, ey, ez);
+    const int base = (t - __ldg(L.starts + di)) * kShellThreads * PER + threadIdx.x;
     T *F = box_field(d, fid);
     const bool per[3] = {d.bt[SIDE_WE] == BC_PERIODIC, d.bt[SIDE_SO] == BC_PERIODIC, d.bt[SIDE_BO] == BC_PERIODIC};
-    T v;
-    if (vel) {
-      const Fold fx = fold_vel(i, ex, d.bt[0], d.bt[1], comp == 0);
-      const Fold fy = fold_vel(j, ey, d.bt[2], d.bt[3], comp == 1);
-      const Fold fz = fold_vel(k, ez, d.bt[4], d.bt[5], comp == 2);
-      if (fx.zero | fy.zero | fz.zero) {
-        v = (T)0;
+    const int rx = ex + 2, zf = rx * (ey + 2), yf = rx * ez;
+    // the thread's PER cells: every source read first, then the ghosts written
+    T val[PER];
+    long long dst[PER];
+    bool ok[PER];
+#pragma unroll
+    for (int r = 0; r < PER; r++) {
+      ok[r] = false;
+      int w = base + r * kShellThreads;
+      if (w >= ncell) continue;
+      // z faces (full planes), then y faces (k in 1..ez)
+      int i, j, k;
+      if (w < 2 * zf) {
+        const int side = w >= zf;
+        w -= side * zf;
+        j = w / rx; i = w - j * rx; k = side ? ez + 1 : 0;
       } else {
-        v = F[bidx(d, fx.src, fy.src, fz.src)];
-        if (fx.sign * fy.sign * fz.sign < 0) v = -v;
+        w -= 2 * zf;
+        const int side = w >= yf;
+        w -= side * yf;
+        k = w / rx; i = w - k * rx; k += 1; j = side ? ey + 1 : 0;
       }
-    } else if (fid == F_P) {
-      const bool gx = i < 1 || i > ex, gy = j < 1 || j > ey, gz = k < 1 || k > ez;
-      if ((gx && !per[0]) || (gy && !per[1]) || (gz && !per[2])) continue;
-      v = F[bidx(d, fold_rep(i, ex, true), fold_rep(j, ey, true), fold_rep(k, ez, true))];
-    } else {
-      v = F[bidx(d, fold_rep(i, ex, per[0]), fold_rep(j, ey, per[1]), fold_rep(k, ez, per[2]))];
+      if (halo_plane(k, ez, d.bt)) continue;  // the slab exchange fills it
+      T v;
+      if (vel) {
+        const Fold fx = fold_vel(i, ex, d.bt[0], d.bt[1], comp == 0);
+        const Fold fy = fold_vel(j, ey, d.bt[2], d.bt[3], comp == 1);
+        const Fold fz = fold_vel(k, ez, d.bt[4], d.bt[5], comp == 2);
+        if (fx.zero | fy.zero | fz.zero) {
+          v = (T)0;
+        } else {
+          v = F[bidx(d, fx.src, fy.src, fz.src)];
+          if (fx.sign * fy.sign * fz.sign < 0) v = -v;
+        }
+      } else if (fid == F_P) {
+        const bool gx = i < 1 || i > ex, gy = j < 1 || j > ey, gz = k < 1 || k > ez;
+        if ((gx && !per[0]) || (gy && !per[1]) || (gz && !per[2])) continue;
+        v = F[bidx(d, fold_rep(i, ex, true), fold_rep(j, ey, true), fold_rep(k, ez, true))];
+      } else {
+        v = F[bidx(d, fold_rep(i, ex, per[0]), fold_rep(j, ey, per[1]), fold_rep(k, ez, per[2]))];
+      }
+      val[r] = v;
+      dst[r] = bidx(d, i, j, k);
+      ok[r] = true;
     }
-    F[bidx(d, i, j, k)] = v;
+#pragma unroll
+    for (int r = 0; r < PER; r++)
+      if (ok[r]) F[dst[r]] = val[r];
   }
   // prref: the last blocks (one per domain, as many as there are) also reduce
   // the top-layer partial sums of the projection into the pressure reference
