@@ -7,7 +7,7 @@
 //
 // Alignment: the innermost box coordinate times the element size is a
 // multiple of 16 bytes and every shared-memory destination is 128-byte
-// aligned.  No multicast form is used.
+// aligned.  Every copy lands in the issuing block's own shared memory.
 #pragma once
 
 #include <cuda.h>
@@ -45,7 +45,7 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   return done != 0;
 }
 
-// One box of a 3-D tensor map (tile mode, no multicast) into shared memory;
+// One box of a 3-D tensor map (tile mode) into this block's shared memory;
 // x is the innermost element coordinate and must be a multiple of 16 bytes.
 // Boxes that reach past the tensor are zero-filled by the hardware.
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar) {
