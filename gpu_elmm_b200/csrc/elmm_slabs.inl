@@ -502,13 +502,18 @@ struct SlabsT {
   // the planes it owns: its interior, and the outer ghost planes for the
   // first and last slab.
   static size_t plane_elems(const HostBox &hb) { return (size_t)hb.n0 * hb.n1; }
-  int upload(const double *U, const double *V, const double *W, const double *Pr) {
+  // H: double, or float for the real32 arrays of a prec=sp host (widened
+  // and narrowed on the device, as the single-domain *_float calls)
+  template <typename H>
+  int upload(const H *U, const H *V, const H *W, const H *Pr) {
     if (!U || !V || !W) return fail(ELMM_ERR_INVALID_ARG, "NULL velocity array");
     for (int s = 0; s < ns; s++) {
       BatchT<T> &B = *sl[s];
       const size_t pv[3] = {plane_elems(B.hbox_vel(0, 0)), plane_elems(B.hbox_vel(0, 1)), plane_elems(B.hbox_vel(0, 2))};
       const size_t pp = plane_elems(B.hbox_p(0));
+      B.hostf = sizeof(H) == 4;
       int r = B.upload(0, U + pv[0] * k0[s], V + pv[1] * k0[s], W + pv[2] * k0[s], Pr ? Pr + pp * k0[s] : nullptr);
+      B.hostf = 0;
       if (r) return r;
     }
     int r = exchange_state();
@@ -519,25 +524,42 @@ struct SlabsT {
     }
     return ELMM_OK;
   }
-  int download(double *U, double *V, double *W, double *Pr) {
-    double *dst[4] = {U, V, W, Pr};
+  template <typename H>
+  int download(H *U, H *V, H *W, H *Pr) {
+    H *dst[4] = {U, V, W, Pr};
     for (int s = 0; s < ns; s++) {
       BatchT<T> &B = *sl[s];
       CU(cudaSetDevice(dev[s]));
+      if (sizeof(H) == 4) {
+        int r = B.ensure_fstage();
+        if (r) return r;
+      }
       for (int f = 0; f < 4; f++) {
         if (!dst[f]) continue;
         const HostBox hb = f < 3 ? B.hbox_vel(0, f) : B.hbox_p(0);
         const int top = f < 3 ? B.hdom[0].ext[f][2] : B.hdom[0].nz;
         const int kw0 = s == 0 ? hb.lo : 1, kw1 = s == ns - 1 ? hb.lo + hb.n2 - 1 : top;
-        const size_t pe = plane_elems(hb), skip = (size_t)(kw0 - hb.lo) * pe;
-        B.pack(0, f, B.dstage, B.stream);
-        CU(cudaMemcpyAsync(dst[f] + pe * k0[s] + skip, B.dstage + skip, sizeof(double) * pe * (kw1 - kw0 + 1),
-                           cudaMemcpyDeviceToHost, B.stream));
+        const size_t pe = plane_elems(hb), skip = (size_t)(kw0 - hb.lo) * pe, cnt = pe * (kw1 - kw0 + 1);
+        const size_t n = B.pack(0, f, B.dstage, B.stream);
+        const void *src = B.dstage + skip;
+        if (sizeof(H) == 4) {
+          k_narrow<<<kPackBlocks, 256, 0, B.stream>>>(B.fstage, B.dstage, (long long)n);
+          src = B.fstage + skip;
+        }
+        CU(cudaMemcpyAsync(dst[f] + pe * k0[s] + skip, src, sizeof(H) * cnt, cudaMemcpyDeviceToHost, B.stream));
         CU(cudaStreamSynchronize(B.stream));
       }
       CU(cudaGetLastError());
     }
     return ELMM_OK;
+  }
+  // TMarchRK3 on the whole domain's host arrays: upload, nsteps steps, download
+  template <typename H>
+  int march_host(H *U, H *V, H *W, H *Pr, int nsteps, elmm_stats *st) {
+    int r = upload<H>(U, V, W, Pr);
+    if (!r) r = step(nsteps, st);
+    if (!r) r = download<H>(U, V, W, Pr);
+    return r;
   }
 };
 
@@ -582,6 +604,31 @@ extern "C" int elmm_slabs_upload_state(elmm_slabs *h, const double *U, const dou
 extern "C" int elmm_slabs_download_state(elmm_slabs *h, double *U, double *V, double *W, double *Pr) {
   if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
   return SLAB_DISPATCH(h, download(U, V, W, Pr));
+}
+
+extern "C" int elmm_slabs_upload_state_float(elmm_slabs *h, const float *U, const float *V, const float *W,
+                                             const float *Pr) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  return SLAB_DISPATCH(h, upload(U, V, W, Pr));
+}
+
+extern "C" int elmm_slabs_download_state_float(elmm_slabs *h, float *U, float *V, float *W, float *Pr) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  return SLAB_DISPATCH(h, download(U, V, W, Pr));
+}
+
+extern "C" int elmm_slabs_march_host(elmm_slabs *h, double *U, double *V, double *W, double *Pr, int32_t nsteps,
+                                     elmm_stats *stats) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  if (nsteps < 0) return fail(ELMM_ERR_INVALID_ARG, "nsteps < 0");
+  return SLAB_DISPATCH(h, march_host(U, V, W, Pr, nsteps, stats));
+}
+
+extern "C" int elmm_slabs_march_host_float(elmm_slabs *h, float *U, float *V, float *W, float *Pr, int32_t nsteps,
+                                           elmm_stats *stats) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  if (nsteps < 0) return fail(ELMM_ERR_INVALID_ARG, "nsteps < 0");
+  return SLAB_DISPATCH(h, march_host(U, V, W, Pr, nsteps, stats));
 }
 
 extern "C" int elmm_slabs_project(elmm_slabs *h, double coef, elmm_stats *stats) {

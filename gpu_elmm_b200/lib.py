@@ -107,6 +107,10 @@ def lib():
         L.elmm_slabs_download_state.argtypes = [P, _dp, _dp, _dp, _dp]
         L.elmm_slabs_project.argtypes = [P, C.c_double, C.POINTER(ElmmStats)]
         L.elmm_slabs_step.argtypes = [P, C.c_int32, C.POINTER(ElmmStats)]
+        L.elmm_slabs_march_host.argtypes = [P, _dp, _dp, _dp, _dp, C.c_int32, C.POINTER(ElmmStats)]
+        L.elmm_slabs_upload_state_float.argtypes = [P, fp, fp, fp, fp]
+        L.elmm_slabs_download_state_float.argtypes = [P, fp, fp, fp, fp]
+        L.elmm_slabs_march_host_float.argtypes = [P, fp, fp, fp, fp, C.c_int32, C.POINTER(ElmmStats)]
         _lib = L
     return _lib
 
@@ -421,6 +425,30 @@ class Slabs:
     def step(self, n=1) -> ElmmStats:
         st = ElmmStats()
         check(lib().elmm_slabs_step(self.h, n, C.byref(st)), "elmm_slabs_step")
+        return st
+
+    def march_host(self, U, V, W, Pr, n=1) -> ElmmStats:
+        """elmm_slabs_march_host: the arrays are updated in place."""
+        st = ElmmStats()
+        check(lib().elmm_slabs_march_host(self.h, ptr(U), ptr(V), ptr(W), ptr(Pr), n, C.byref(st)),
+              "elmm_slabs_march_host")
+        return st
+
+    # real32 host arrays of a prec=sp host
+    def upload_f32(self, U, V, W, Pr=None):
+        check(lib().elmm_slabs_upload_state_float(self.h, fptr(U), fptr(V), fptr(W), fptr(Pr)),
+              "elmm_slabs_upload_state_float")
+
+    def download_f32(self):
+        g = self.grid
+        out = [np.zeros(s, dtype=np.float32) for s in (g.shape_u(), g.shape_v(), g.shape_w(), g.shape_p())]
+        check(lib().elmm_slabs_download_state_float(self.h, *[fptr(a) for a in out]), "elmm_slabs_download_state_float")
+        return tuple(out)
+
+    def march_host_f32(self, U, V, W, Pr, n=1) -> ElmmStats:
+        st = ElmmStats()
+        check(lib().elmm_slabs_march_host_float(self.h, fptr(U), fptr(V), fptr(W), fptr(Pr), n, C.byref(st)),
+              "elmm_slabs_march_host_float")
         return st
 
 

@@ -350,5 +350,29 @@ module elmm_gpu
       integer(c_int32_t), value :: nsteps
       type(elmm_stats) :: st
     end function
+    integer(c_int) function elmm_slabs_march_host(h, U, V, W, Pr, nsteps, st) bind(C)
+      import
+      type(c_ptr), value :: h
+      real(c_double) :: U(*), V(*), W(*), Pr(*)
+      integer(c_int32_t), value :: nsteps
+      type(elmm_stats) :: st
+    end function
+    integer(c_int) function elmm_slabs_upload_state_float(h, U, V, W, Pr) bind(C)
+      import
+      type(c_ptr), value :: h
+      real(c_float), intent(in) :: U(*), V(*), W(*), Pr(*)
+    end function
+    integer(c_int) function elmm_slabs_download_state_float(h, U, V, W, Pr) bind(C)
+      import
+      type(c_ptr), value :: h
+      real(c_float) :: U(*), V(*), W(*), Pr(*)
+    end function
+    integer(c_int) function elmm_slabs_march_host_float(h, U, V, W, Pr, nsteps, st) bind(C)
+      import
+      type(c_ptr), value :: h
+      real(c_float) :: U(*), V(*), W(*), Pr(*)
+      integer(c_int32_t), value :: nsteps
+      type(elmm_stats) :: st
+    end function
   end interface
 end module elmm_gpu

@@ -634,6 +634,16 @@ int elmm_slabs_project(elmm_slabs *h, double coef, elmm_stats *stats);
  * slabs on several devices launch eagerly.  stats->elapsed_ms is the device
  * time from the first slab's start to the last slab's end. */
 int elmm_slabs_step(elmm_slabs *h, int32_t nsteps, elmm_stats *stats);
+/* TMarchRK3 on the host arrays, as elmm_march_host: upload, nsteps steps,
+ * download into the same arrays. */
+int elmm_slabs_march_host(elmm_slabs *h, double *U, double *V, double *W, double *Pr, int32_t nsteps,
+                          elmm_stats *stats);
+/* The real32 host arrays of a prec=sp host (as elmm_upload_state_float):
+ * widened to double on the device after the copy, narrowed before it. */
+int elmm_slabs_upload_state_float(elmm_slabs *h, const float *U, const float *V, const float *W, const float *Pr);
+int elmm_slabs_download_state_float(elmm_slabs *h, float *U, float *V, float *W, float *Pr);
+int elmm_slabs_march_host_float(elmm_slabs *h, float *U, float *V, float *W, float *Pr, int32_t nsteps,
+                                elmm_stats *stats);
 
 /* Last error message of this thread (static storage). */
 const char *elmm_last_error(void);

@@ -11,6 +11,7 @@ oracle.
   value) of the single domain and of the oracle, max |div u| below 1e-10;
   the split changes only the order of the z solve's operations;
 * mixed: within 1e-5 of the single-domain mixed path;
+* march_host and the real32 host arrays against the double calls;
 * even and uneven splits, 2 and 3 slabs, uniform and stretched z, slabs
   short enough for the tiled sweep kernels and taller ones.
 """
@@ -98,5 +99,36 @@ def test_tall_slabs_take_the_column_kernels():
     e = _errs(b.download(), a.download())
     print("300-level slabs vs single domain:", e, s.max_div)
     assert max(e[:3]) < 1e-12 and e[3] < 1e-11 and s.max_div < 1e-10, e
+    a.close()
+    b.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_slab_host_arrays(precision):
+    """elmm_slabs_march_host equals upload, step, download on a second
+    handle, bit for bit; the real32 entry points equal the double ones on
+    the same values widened, their results rounded to float32."""
+    cfg = make_config(*N, precision=precision)
+    st = log_profile_state(grid_of(cfg), seed=5)
+    a, b = L.Slabs(cfg, 2, devices=[0, 0]), L.Slabs(cfg, 2, devices=[0, 0])
+    a.upload(*st)
+    a.step(2)
+    ref = a.download()
+    arrs = [x.copy() for x in st]
+    b.march_host(*arrs, n=2)
+    for x, y in zip(arrs, ref):
+        assert np.array_equal(x, y)
+    f32 = [x.astype(np.float32) for x in st]
+    wide = [x.astype(np.float64) for x in f32]
+    a.upload_f32(*f32)
+    b.upload(*wide)
+    for x, y in zip(a.download(), b.download()):
+        assert np.array_equal(x, y)
+    for x, y in zip(a.download_f32(), b.download()):
+        assert x.dtype == np.float32 and np.array_equal(x, y.astype(np.float32))
+    a.march_host_f32(*f32, n=2)
+    b.march_host(*wide, n=2)
+    for x, y in zip(f32, wide):
+        assert np.array_equal(x, y.astype(np.float32))
     a.close()
     b.close()
