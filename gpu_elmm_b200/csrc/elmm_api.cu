@@ -195,9 +195,12 @@ static int check_config(const elmm_config &c) {
       const bool per = c.Btype[s] == ELMM_BC_PERIODIC;
       if (per && c.TempBtype[s] != ELMM_BC_PERIODIC)
         return fail(ELMM_ERR_INVALID_CONFIG, "the temperature must be periodic where the flow is");
-      if (!per && !(c.TempBtype[s] == ELMM_BC_CONSTFLUX && c.sideTemp[s] == 0))
+      // a surface flux is carried by the wall-model points of a wall in z
+      const bool wm_wall = c.wallmodeltype > 0 && c.Btype[s] == ELMM_BC_NOSLIP && (s == ELMM_BO || s == ELMM_TO);
+      if (!per && !(c.TempBtype[s] == ELMM_BC_CONSTFLUX && (c.sideTemp[s] == 0 || (wm_wall && std::isfinite(c.sideTemp[s])))))
         return fail(ELMM_ERR_INVALID_CONFIG,
-                    "temperature walls must be adiabatic (ELMM_BC_CONSTFLUX with sideTemp = 0)");
+                    "temperature sides: ELMM_BC_CONSTFLUX, with a non-zero sideTemp (a surface heat flux) only at a "
+                    "wall-model wall at the bottom or top");
     }
     if (c.zW) return fail(ELMM_ERR_INVALID_CONFIG, "the temperature field needs a uniform z grid");
     if (c.Btype[ELMM_BO] == ELMM_BC_PERIODIC)
@@ -1025,6 +1028,16 @@ struct BatchT {
       }
       for (int s2 = 0; s2 < 6; s2++) sl.bt[s2] = c.TempBtype[s2];
       sl.off = h.toff;
+      // a surface heat flux at a wall-model wall: the temperature_flux of the
+      // side's wall-model points (src/wallmodels.f90:590-596, 650-656), and
+      // its term in the cells next to the wall with ComputeAreaFactor's
+      // boundary area over cell volume (src/wallmodels.f90:173-203)
+      const double dq = sqrt(h.dx * h.dy), area_factor = dq * (dq / 1.0) / (h.dx * h.dy * h.dz);
+      for (int side : {ELMM_BO, ELMM_TO})
+        if (h.wall[side] && c.TempBtype[side] == ELMM_BC_CONSTFLUX) {
+          h.tflux[side] = side == ELMM_BO ? c.sideTemp[side] : -c.sideTemp[side];
+          sl.wflux[side == ELMM_BO ? 0 : 1] = h.tflux[side] * area_factor;
+        }
       h.tdiff_live = 1;
     }
     h.kappa_mol = c.molecular_diffusivity;

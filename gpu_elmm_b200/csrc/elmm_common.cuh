@@ -56,6 +56,10 @@ struct ScalSlot {
   T *adv;                // the stage tendency
   int bt[6];             // BC per side (TempBtype / ScalBtype)
   double off;            // the box stores value - off
+  // surface flux term of the wall-model points at k = 1 and k = nz:
+  // temperature_flux * area_factor (src/scalars.f90:323-327); 0 for the
+  // passive scalars and adiabatic walls
+  double wflux[2];
   double *acc_xy, *acc_xz;  // time-averaged slices (FP64, [j][i] and [k][i]) or null
 };
 
@@ -156,6 +160,9 @@ struct Dom {
   int tbt[6];            // temperature BC per side
   T *Tm, *Tadv, *TDiff;
   double toff, tref, grav, kappa_mol;
+  // temperature_flux of the wall-model points per side: sideTemp at the
+  // bottom, -sideTemp at the top (src/wallmodels.f90:819-827, 870-878)
+  double tflux[6];
   // scalar slots of the ScalarRK3 kernel: slot 0 is the temperature when
   // buoy is set (Tm aliases its buf[0], Tadv its tendency), then the passive
   // scalars

@@ -86,6 +86,44 @@ __device__ inline double wm_ustar(double ustar, double vel, double dist, double 
   return z0 > 0 ? wm_rough_ustar(ustar, vel, dist, z0, nu) : wm_flat_ustar(ustar, vel, dist, nu);
 }
 
+// PsiM_MO, the Businger-Dyer stability function of momentum
+// (src/wallmodels.f90:1546-1556)
+__device__ inline double psim_mo(double zeta) {
+  if (zeta < 0) {
+    const double x = pow(1 - 15.0 * zeta, 0.25), h = (1 + x) / 2.0;
+    return log(((1 + x * x) / 2.0) * (h * h)) - 2.0 * atan(x) + 3.141592653589793 / 2;
+  }
+  return -4.8 * zeta;
+}
+
+// WM_MO_Flux_ustar (src/wallmodels.f90:1606-1660): u* of a rough wall under
+// a prescribed surface temperature flux, the log law corrected by PsiM_MO at
+// the Obukhov stability z/L, both relaxed by halves from the point's u* of
+// the stage before.  The tolerances 1e-3, 1e-4 and 1e-5 are default-real
+// literals in the reference (their float values widened).
+__device__ inline double wm_mo_flux_ustar(double ustar, double vel, double dist, double z0, double tflux,
+                                          double tref, double g, double nu) {
+  if (dist <= z0) {
+    if (nu <= 0) return 0;
+    if ((dist * ustar / nu) < 11.225) return sqrt(nu * vel / dist);
+    return vel / (log(fabs(ustar * dist / nu)) / 0.4 + 5.2);
+  }
+  double zL = 0, Psi = 0;
+  for (int i = 1;; i++) {  // at most 50 iterations
+    const double ustar2 = ustar;
+    ustar = ustar + (fmax(vel * 0.4 / log(fmax((dist / z0) - Psi, (double)1e-5f)), 0.0) - ustar) / 2;
+    if (ustar < (double)1e-4f) {
+      zL = -10000;
+    } else {  // Obukhov_zL (src/wallmodels.f90:1598-1602)
+      const double zL2 = dist * (0.4 * (g / tref) * tflux) / (-(ustar * ustar * ustar));
+      zL = zL + (zL2 - zL) / 2;
+    }
+    Psi = psim_mo(zL);
+    if (fabs(ustar - ustar2) / fmax(fabs(ustar), 1e-3) < (double)1e-3f) return ustar;
+    if (i >= 50) return 0;
+  }
+}
+
 // ComputeUVWFluxesWM / fluxes for the point of component comp on side f at
 // cell (i,j,k) (src/wallmodels.f90:2159-2338); the wall-point distance is
 // the one of GetOutsideBoundariesWM_UVW (src/wallmodels.f90:690-909).
@@ -147,7 +185,10 @@ __device__ void wm_point(const Dom<T> &d, int comp, int f, int i, int j, int k, 
   double tv = norm2_3(t);
   const int face = comp * 6 + f;
   double ustar = d.wm_ustar[face][pidx];
-  if (tv != 0) ustar = wm_ustar(ustar, tv, dd, d.z0[f], d.nu_mol);
+  if (d.z0[f] > 0 && d.tflux[f] > 0)  // WM_MO_FluxStress (src/wallmodels.f90:1836-1854, 2255-2259)
+    ustar = tv != 0 ? wm_mo_flux_ustar(ustar, tv, dd, d.z0[f], d.tflux[f], d.tref, d.grav, d.nu_mol) : 0.0;
+  else if (tv != 0)
+    ustar = wm_ustar(ustar, tv, dd, d.z0[f], d.nu_mol);
   if (ustar < 0) ustar = 0;
   d.wm_ustar[face][pidx] = ustar;
   double mag = norm2_3(t);

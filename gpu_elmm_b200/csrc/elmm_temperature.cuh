@@ -171,9 +171,10 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
         for (int q = 0; q < d.nsrc; q++)
           if (((srcm >> q) & 1u) && d.src_k[q] == k) a = a + (T)d.src_q[q];
       }
-      // wall-model point next to a wall-model side: + div * value (the
-      // surface flux is zero); div as DivergenceWM with dzPr(k)
+      // wall-model point next to a wall-model side: + the surface flux term,
+      // then + div * value; div as DivergenceWM with dzPr(k)
       if ((k == 1 && wm_lo) || (k == nz && wm_hi)) {
+        a = a + (T)sl.wflux[k == 1 ? 0 : 1];
         const T dzk = (T)d.dzPr[k + 2];
         T div = (T)0;
         div = div + ue / rdx;
@@ -355,6 +356,7 @@ __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SP
             if (((srcm >> q) & 1u) && d.src_i[q] == i + c && d.src_k[q] == k) a = a + (T)d.src_q[q];
         }
         if (wmk) {
+          a = a + (T)sl.wflux[k == 1 ? 0 : 1];
           const T dzk = (T)d.dzPr[k + 2];
           const T ue = c ? u0.y : u0.x, uw = c ? u0.x : um.y;
           const T wtc = c ? wt.y : wt.x, wbc = c ? wb.y : wb.x;

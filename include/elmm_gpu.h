@@ -131,7 +131,13 @@ typedef struct elmm_config {
   /* Potential temperature: transport by ScalarRK3 (src/scalars.f90:88-381) and
    * buoyancy in the W tendency (BuoyancyForce, src/dynamics.f90:608-690).
    * Supported: TempBtype periodic on the periodic x and y sides and
-   * ELMM_BC_CONSTFLUX with sideTemp = 0 (adiabatic) at the bottom and top. */
+   * ELMM_BC_CONSTFLUX at the bottom and top: sideTemp = 0 (adiabatic), or a
+   * surface heat flux (K m/s, positive upward: into the flow at the bottom,
+   * out of it at the top) at a wall-model wall.  The flux enters the cells next to the
+   * wall through the wall-model points (src/scalars.f90:323-327), and a
+   * flux into the flow (unstable stratification) over a rough wall makes
+   * the wall model's u* follow Monin-Obukhov similarity (WM_MO_FluxStress,
+   * src/wallmodels.f90:1836-1854, 2255-2259). */
   int32_t enable_buoyancy;      /* 0: no temperature field */
   int32_t TempBtype[6];         /* temperature BC per side (src/initial.f90:347-352) */
   double sideTemp[6];           /* BC values: the flux for ELMM_BC_CONSTFLUX */

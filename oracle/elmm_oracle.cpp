@@ -91,6 +91,7 @@ struct WMPointUVW {
   double z0 = 0;
   double ustar = 1;
   double wallu = 0, wallv = 0, wallw = 0;
+  double temperature_flux = 0;
 };
 
 // ------------------------------------------------------------------- FFT
@@ -170,6 +171,10 @@ struct Domain {
   int TempBtype[7];
   double sideTemp[7];
   double temperature_ref, grav_acc, molecular_diffusivity;
+  // temperature_flux of the wall-model points of the bottom and top walls and
+  // their ComputeAreaFactor (wallmodels.f90:173-203, 590-596, 650-656)
+  double wm_tflux[7] = {0, 0, 0, 0, 0, 0, 0};
+  double area_factor_z = 0;
   A3 T, Tadv, T2, TDiff;
   // passive scalars (ScalarRK3's loop over num_of_scalars, scalars.f90:217-223)
   int num_scalars;
@@ -291,6 +296,7 @@ static void add_wm_points(Domain &d) {
         for (int i = 1; i <= nx; i++) {
           p = WMPointUVW(); p.xi = i; p.yj = j; p.zk = 1;
           p.distz = d.zW(0) - z(1); p.z0 = d.z0s[Bo];
+          p.temperature_flux = d.wm_tflux[Bo];
           d.wm[MINUSZ][comp].push_back(p);
         }
     if (d.Btype[To] == BC_NOSLIP)
@@ -298,6 +304,7 @@ static void add_wm_points(Domain &d) {
         for (int i = 1; i <= nx; i++) {
           p = WMPointUVW(); p.xi = i; p.yj = j; p.zk = nz;
           p.distz = d.zW(d.Wnz + 1) - z(nz); p.z0 = d.z0s[To];
+          p.temperature_flux = d.wm_tflux[To];
           d.wm[PLUSZ][comp].push_back(p);
         }
   }
@@ -603,6 +610,48 @@ static void WMRoughUstar(const Domain &d, double &ustar, double vel, double dist
   }
 }
 
+// PsiM_MO, wallmodels.f90:1546-1556
+static double PsiM_MO(double zeta) {
+  if (zeta < 0) {
+    const double x = std::pow(1 - 15.0 * zeta, 1 / 4.0);
+    const double h = (1 + x) / 2.0;
+    return std::log(((1 + x * x) / 2.0) * (h * h)) - 2.0 * std::atan(x) + std::acos(-1.0) / 2;
+  }
+  return -4.8 * zeta;
+}
+
+// WM_MO_Flux_ustar, wallmodels.f90:1606-1660, with Obukhov_zL (:1598-1602);
+// eps = 1e-3, 1E-4 and 1E-5 are default-real literals there
+static void WM_MO_Flux_ustar(const Domain &d, double vel, double dist, double &ustar, double z0, double tflux) {
+  const double nu = d.molecular_viscosity;
+  const double eps = (double)1e-3f, yplcrit = 11.225;
+  if (dist <= z0) {
+    if (nu > 0) {
+      if ((dist * ustar / nu) < yplcrit) ustar = std::sqrt(nu * vel / dist);
+      else ustar = vel / (std::log(std::fabs(ustar * dist / nu)) / 0.4 + 5.2);
+    } else {
+      ustar = 0;
+    }
+    return;
+  }
+  int i = 0;
+  double zL = 0, Psi = 0;
+  for (;;) {
+    i = i + 1;
+    const double ustar2 = ustar;
+    ustar = ustar + (std::max(vel * 0.4 / (std::log(std::max((dist / z0) - Psi, (double)1e-5f))), 0.0) - ustar) / 2;
+    if (ustar < (double)1e-4f) {
+      zL = -10000;
+    } else {
+      const double zL2 = dist * (0.4 * (d.grav_acc / d.temperature_ref) * tflux) / (-(ustar * ustar * ustar));
+      zL = zL + (zL2 - zL) / 2;
+    }
+    Psi = PsiM_MO(zL);
+    if (std::fabs(ustar - ustar2) / std::max(std::fabs(ustar), 1.e-3) < eps) break;
+    if (i >= 50) { ustar = 0; break; }
+  }
+}
+
 // local_velocity, wallmodels.f90:2354-2396
 static void local_velocity(const Domain &d, int comp, int xi, int yj, int zk, double *vel) {
   const A3 &U = d.U, &V = d.V, &W = d.W;
@@ -621,7 +670,7 @@ static void local_velocity(const Domain &d, int comp, int xi, int yj, int zk, do
   }
 }
 
-// ComputeUVWFluxesWM / fluxes, wallmodels.f90:2159-2338 (rough wall, neutral)
+// ComputeUVWFluxesWM / fluxes, wallmodels.f90:2159-2338
 static void ComputeUVWFluxesWM(Domain &d) {
   const double eps = std::sqrt(2.220446049250313e-16);
   double drec[7] = {0, 1 / d.dxmin, 1 / d.dxmin, 1 / d.dymin, 1 / d.dymin, 1 / d.dzmin, 1 / d.dzmin};
@@ -641,9 +690,14 @@ static void ComputeUVWFluxesWM(Domain &d) {
         double dot = t[0] * dist[0] + t[1] * dist[1] + t[2] * dist[2];
         for (int m = 0; m < 3; m++) t[m] = t[m] - dot * dist[m] / (dd * dd);
         double tv = norm2_3(t);
-        // WMRoughStress with a roughness length, WMFlatStress for a smooth wall
-        // (wallmodels.f90:2262-2275; WMFlatStress, :1243-1265)
-        if (tv != 0) {
+        // WM_MO_FluxStress for a rough wall with a temperature flux into the
+        // flow, else WMRoughStress with a roughness length, WMFlatStress for a
+        // smooth wall (wallmodels.f90:2255-2275; WM_MO_FluxStress, :1836-1854;
+        // WMFlatStress, :1243-1265)
+        if (p.z0 > 0 && d.enable_buoyancy && p.temperature_flux > 0) {
+          if (tv != 0) WM_MO_Flux_ustar(d, tv, dd, p.ustar, p.z0, p.temperature_flux);
+          else p.ustar = 0;
+        } else if (tv != 0) {
           if (p.z0 > 0) WMRoughUstar(d, p.ustar, tv, dd, p.z0);
           else WMFlatUstar(d, p.ustar, tv, dd);
         }
@@ -758,6 +812,8 @@ static void CommonBase(Domain &d, A3 &a, const int *bt, const double *side) {
     for (int i = -1; i <= nx + 2; i++) {
       if (bt[Bo] == BC_PERIODIC) {
         for (int g = -2; g <= 0; g++) a(i, j, g) = a(i, j, nz + g);
+      } else if (bt[Bo] == 0) {  // mirror
+        for (int g = -2; g <= 0; g++) a(i, j, g) = a(i, j, 1 - g);
       } else {
         a(i, j, 0) = a(i, j, 1) + side[Bo] * d.dzW(0) / ((d.TDiff(i, j, 1) + d.TDiff(i, j, 0)) / 2.0);
         a(i, j, -1) = a(i, j, 0) - (a(i, j, 1) - a(i, j, 0));
@@ -765,6 +821,8 @@ static void CommonBase(Domain &d, A3 &a, const int *bt, const double *side) {
       }
       if (bt[To] == BC_PERIODIC) {
         for (int g = 1; g <= 3; g++) a(i, j, nz + g) = a(i, j, g);
+      } else if (bt[To] == 0) {  // mirror
+        for (int g = 1; g <= 3; g++) a(i, j, nz + g) = a(i, j, nz + 1 - g);
       } else {
         a(i, j, nz + 1) = a(i, j, nz) - side[To] * d.dzW(nz) / ((d.TDiff(i, j, nz) + d.TDiff(i, j, nz + 1)) / 2.0);
         a(i, j, nz + 2) = a(i, j, nz + 1) - (a(i, j, nz) - a(i, j, nz + 1));
@@ -853,10 +911,11 @@ static void ScalarDiffusion(Domain &d, A3 &S2, const A3 &S) {
 // stage() of ScalarRK3 (scalars.f90:233-299) for one field: the temperature
 // (sc = 0) or passive scalar sc.  The scalar wall-model points are the cells
 // next to a wall-model side (DivergenceWM, wallmodels.f90:1150-1166, with the
-// velocity at the start of the stage); TemperatureExtra adds a zero surface
-// flux and div * T there (scalars.f90:301-334), ScalarExtra first the volume
-// sources of the scalar (ScalarVolumeSources -> FluxKernel,
-// volumesources.f90:741-771) and then div * S (scalars.f90:364-379).
+// velocity at the start of the stage); TemperatureExtra adds the surface
+// flux (temperature_flux * area_factor) and div * T there
+// (scalars.f90:301-334), ScalarExtra first the volume sources of the scalar
+// (ScalarVolumeSources -> FluxKernel, volumesources.f90:741-771) and then
+// div * S (scalars.f90:364-379).
 static void ScalarStage(Domain &d, int stage, double dt, A3 &Arr, A3 &Arr2, A3 &Adv, int sc) {
   const int nx = d.Prnx, ny = d.Prny, nz = d.Prnz;
   auto bound = [&](A3 &a) { if (sc == 0) BoundTemperature(d, a); else BoundScalar(d, a); };
@@ -898,8 +957,14 @@ static void ScalarStage(Domain &d, int stage, double dt, A3 &Arr, A3 &Arr2, A3 &
             Adv(v.i, v.j, v.k) = Adv(v.i, v.j, v.k) + d.puffs[q].dt_fraction * v.flux;
   for (int j = 1; j <= ny; j++)
     for (int i = 1; i <= nx; i++) {
-      if (wb) Adv(i, j, 1) = Adv(i, j, 1) + divb[(size_t)(j - 1) * nx + i - 1] * Arr(i, j, 1);
-      if (wt) Adv(i, j, nz) = Adv(i, j, nz) + divt[(size_t)(j - 1) * nx + i - 1] * Arr(i, j, nz);
+      if (wb) {
+        if (sc == 0) Adv(i, j, 1) = Adv(i, j, 1) + d.wm_tflux[Bo] * d.area_factor_z;
+        Adv(i, j, 1) = Adv(i, j, 1) + divb[(size_t)(j - 1) * nx + i - 1] * Arr(i, j, 1);
+      }
+      if (wt) {
+        if (sc == 0) Adv(i, j, nz) = Adv(i, j, nz) + d.wm_tflux[To] * d.area_factor_z;
+        Adv(i, j, nz) = Adv(i, j, nz) + divt[(size_t)(j - 1) * nx + i - 1] * Arr(i, j, nz);
+      }
     }
   for (size_t q = 0; q < Arr2.v.size(); q++) Arr2.v[q] = Arr2.v[q] + Adv.v[q] * bdt;
   for (size_t q = 0; q < Arr.v.size(); q++) Arr.v[q] = Arr.v[q] + Arr2.v[q];
@@ -1866,7 +1931,21 @@ void *orc_create(const elmm_config *c) {
     d->acc_xy[sc].assign((size_t)nx * ny, 0.0);
     d->acc_xz[sc].assign((size_t)nx * nz, 0.0);
   }
-  if (d->wallmodeltype > 0) add_wm_points(*d);
+  if (d->wallmodeltype > 0) {
+    // GetOutsideBoundariesWM_UVW / _Pr (wallmodels.f90:570-627, 819-827):
+    // a constant temperature flux at a wall becomes the flux of its
+    // wall-model points, and the side's TempBtype becomes 0 (the mirror
+    // ghosts of CommonBase's last branch)
+    for (int side : {Bo, To})
+      if (d->Btype[side] == BC_NOSLIP && d->TempBtype[side] == ELMM_BC_CONSTFLUX) {
+        d->wm_tflux[side] = side == Bo ? d->sideTemp[side] : -d->sideTemp[side];
+        d->TempBtype[side] = 0;
+      }
+    // ComputeAreaFactor of a point below or above its cell: out_norm = e_z
+    const double dq = std::sqrt(d->dxmin * d->dymin), l = dq / 1.0;
+    d->area_factor_z = dq * l / (d->dxmin * d->dymin * d->dzmin);
+    add_wm_points(*d);
+  }
   if (!init_poisson(*d)) { delete d; return nullptr; }
   return d;
 }

@@ -88,10 +88,10 @@ def test_taylor_green_decay():
     assert rel(Vi, V0 * decay) < 1e-6
 
 
-def _buoyant_channel(seed=0, n=(16, 12, 10)):
+def _buoyant_channel(seed=0, n=(16, 12, 10), **kw):
     from gpu_elmm_b200.config import FIELD_TEMPERATURE, grid_of, make_config
     from gpu_elmm_b200.workloads import log_profile_state, temperature_state
-    cfg = make_config(*n, buoyancy=True)
+    cfg = make_config(*n, buoyancy=True, **kw)
     g = grid_of(cfg)
     o = Oracle(cfg)
     o.set_state(*log_profile_state(g, seed=seed))
@@ -292,3 +292,84 @@ def test_smooth_wall_ustar_follows_the_log_law():
     o2.run_stage(1, 2)
     us2 = math.sqrt(-o2.get_field(8)[3, 3, 3] * dz)
     assert abs(us2 - vel * 0.41 / math.log((dz / 2) / 1e-4)) < 1e-12
+
+
+@pytest.mark.parametrize("heat_flux", [(0.2, 0.0), (-0.1, 0.05)], ids=["heated", "cooled-with-top-flux"])
+def test_surface_heat_flux_enters_through_the_wall_points(heat_flux):
+    """A constant surface heat flux at a wall-model wall (TempBtype
+    CONSTFLUX, which becomes the flux of the side's wall-model points,
+    src/wallmodels.f90:590-627): the heat content grows by
+    (q_bottom - q_top) Lx Ly per unit time (RK3's weights add to one per
+    step), up to the wall-model divergence term.  The top here is a second
+    wall-model wall."""
+    from gpu_elmm_b200.config import FIELD_TEMPERATURE
+    from gpu_elmm_b200.workloads import interior
+    qb, qt = heat_flux
+    g, o = _buoyant_channel(btype=(BC_PERIODIC,) * 4 + (BC_NOSLIP, BC_NOSLIP), heat_flux=heat_flux)
+    n = (g.Prnx, g.Prny, g.Prnz)
+    h0 = interior(o.get_field(FIELD_TEMPERATURE), -2, n).sum()      # cells of 1 m^3
+    steps, dt = 4, 0.02
+    o.step(steps)
+    h1 = interior(o.get_field(FIELD_TEMPERATURE), -2, n).sum()
+    expect = (qb - qt) * g.Prnx * g.Prny * dt * steps
+    assert abs((h1 - h0) - expect) < 1e-9 * abs(expect) + 1e-12 * abs(h0)
+
+
+def test_unstable_surface_flux_follows_monin_obukhov():
+    """Uniform flow U over a rough bottom with a heat flux q > 0 into the
+    flow (WM_MO_FluxStress, src/wallmodels.f90:1606-1660, 1836-1854): the U
+    tendency of the first level is -u*^2 / dz.  u* is the reference's
+    iteration from the initial u* = 1 (u* and z/L relaxed by halves until u*
+    changes by less than 1e-3), restated here step by step; it stops within
+    2% of the fixed point U = u*/0.4 (ln(z/z0) - PsiM(z/L)) with the
+    Businger-Dyer PsiM and L = -u*^3 T_ref / (0.4 g q), found by bisection,
+    and gives more drag than the neutral law with the same von Karman
+    constant (0.4; the neutral WMRoughUstar uses 0.41).  A flux out of the
+    flow keeps WMRoughUstar."""
+    import math
+    from gpu_elmm_b200.config import FIELD_TEMPERATURE
+    from gpu_elmm_b200.workloads import temperature_state
+    dz, vel, z0, tref, grav = 1.0, 5.0, 0.01, 295.0, 9.81
+
+    def tendency_ustar(q):
+        cfg = make_config(16, 12, 8, dz=dz, z0=z0, buoyancy=True, heat_flux=(q, 0.0))
+        g = grid_of(cfg)
+        U, V, W, Pr = (np.zeros(s) for s in (g.shape_u(), g.shape_v(), g.shape_w(), g.shape_p()))
+        U[...] = vel
+        o = Oracle(cfg)
+        o.set_state(U, V, W, Pr)
+        o.set_field(FIELD_TEMPERATURE, temperature_state(g, gradient=0.0, amp=0.0, t0=tref))
+        o.run_stage(1, 2)
+        tend = o.get_field(8)[2 + 1, 2 + 1:2 + 1 + g.Uny, 2 + 1:2 + 1 + g.Unx]
+        assert np.ptp(tend) == 0 and tend.max() < 0
+        return math.sqrt(-tend.max() * dz)
+
+    def psim(zeta):
+        if zeta < 0:
+            x = (1 - 15 * zeta) ** 0.25
+            return math.log((1 + x * x) / 2 * ((1 + x) / 2) ** 2) - 2 * math.atan(x) + math.pi / 2
+        return -4.8 * zeta
+
+    z = dz / 2
+    neutral = vel * 0.41 / math.log(z / z0)
+    assert abs(tendency_ustar(-0.3) - neutral) < 1e-12
+    q = 0.3
+    us = tendency_ustar(q)
+    f32 = lambda v: float(np.float32(v))            # default-real literals of the reference
+    u, zl, psi = 1.0, 0.0, 0.0
+    for it in range(1, 51):
+        u2 = u
+        u = u + (max(vel * 0.4 / math.log(max(z / z0 - psi, f32(1e-5))), 0.0) - u) / 2
+        zl = -10000.0 if u < f32(1e-4) else zl + (z * (0.4 * (grav / tref) * q) / -(u * u * u) - zl) / 2
+        psi = psim(zl)
+        if abs(u - u2) / max(abs(u), 1e-3) < f32(1e-3):
+            break
+    assert it > 3 and abs(us - u) < 1e-13, (us, u)
+    # the fixed point of the similarity law, by bisection
+    fp = lambda v: v - 0.4 * vel / (math.log(z / z0) - psim(z * 0.4 * (grav / tref) * q / -v ** 3))
+    lo, hi = 0.05, 2.0
+    for _ in range(200):
+        mid = (lo + hi) / 2
+        lo, hi = (mid, hi) if fp(lo) * fp(mid) > 0 else (lo, mid)
+    assert abs(us - lo) / lo < 2e-2, (us, lo)
+    assert us > 0.4 * vel / math.log(z / z0)      # more drag than the neutral law with its 0.4
