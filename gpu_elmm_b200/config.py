@@ -239,7 +239,7 @@ def make_config(Prnx, Prny, Prnz, *, btype=(BC_PERIODIC, BC_PERIODIC, BC_PERIODI
                 refine_tol=1e-6, cfl_check=0, device=0, origin=(0.0, 0.0, 0.0), buoyancy=False,
                 temperature_ref=295.0, grav_acc=9.81, prandtl=0.7, num_scalars=0, point_sources=(),
                 avg_slice_k=0, avg_slice_j=0, avg_weight=0.0, variable_dt=False, cfl=0.5, dt_max=None,
-                end_time=0.0, heat_flux=(0.0, 0.0)):
+                end_time=0.0, heat_flux=(0.0, 0.0), temperature_bc=None, scalar_bc=None):
     """Builds an ElmmConfig.  The wall model defaults to on when an SGS model
     is on (src/initial.f90:2782-2787).  ``zW`` (Prnz+1 values) selects the
     stretched-z grid; the array is kept alive on the returned struct.
@@ -247,7 +247,10 @@ def make_config(Prnx, Prny, Prnz, *, btype=(BC_PERIODIC, BC_PERIODIC, BC_PERIODI
     (zero-flux) bottom and top and periodic x and y, or with the constant
     surface heat fluxes ``heat_flux`` = (sideTemp at the bottom, at the top),
     K m/s positive upward, at wall-model walls; ``num_scalars`` passive
-    scalars get zero-flux walls.  ``point_sources``: (scalar_number,
+    scalars get zero-flux walls.  ``temperature_bc`` / ``scalar_bc`` set the
+    bottom and top kinds of CommonBase instead: ((kind, value) at the
+    bottom, (kind, value) at the top), kind BC_CONSTFLUX, BC_DIRICHLET or
+    BC_NEUMANN.  ``point_sources``: (scalar_number,
     (x, y, z), flux) triples.  ``avg_slice_k`` / ``avg_slice_j`` select the
     time-averaged slices, ``avg_weight`` the weight of one step.
     ``variable_dt`` switches on the variable time steps of TimeStepLength
@@ -292,6 +295,8 @@ def make_config(Prnx, Prny, Prnz, *, btype=(BC_PERIODIC, BC_PERIODIC, BC_PERIODI
         c.TempBtype[s] = BC_PERIODIC if btype[s] == BC_PERIODIC else BC_CONSTFLUX
         c.sideTemp[s] = 0.0
     c.sideTemp[BO], c.sideTemp[TO] = heat_flux
+    if temperature_bc is not None:
+        (c.TempBtype[BO], c.sideTemp[BO]), (c.TempBtype[TO], c.sideTemp[TO]) = temperature_bc
     c.temperature_ref = temperature_ref
     c.grav_acc = grav_acc
     c.molecular_diffusivity = nu / prandtl
@@ -299,6 +304,8 @@ def make_config(Prnx, Prny, Prnz, *, btype=(BC_PERIODIC, BC_PERIODIC, BC_PERIODI
     for s in range(6):
         c.ScalBtype[s] = BC_PERIODIC if btype[s] == BC_PERIODIC else BC_CONSTFLUX
         c.sideScal[s] = 0.0
+    if scalar_bc is not None:
+        (c.ScalBtype[BO], c.sideScal[BO]), (c.ScalBtype[TO], c.sideScal[TO]) = scalar_bc
     assert len(point_sources) <= MAX_POINT_SOURCES
     c.num_point_sources = len(point_sources)
     for q, (sc, pos, flux) in enumerate(point_sources):

@@ -153,6 +153,26 @@ static void make_grid(const elmm_config &c, HostGrid &g) {
     g.width[k] = c.filter_ratio * std::pow(g.dxPr[1] * g.dyPr[1] * g.dzPr[k + 2], 1.0 / 3.0);
 }
 
+// the BC kinds of CommonBase a non-periodic scalar side takes
+// (src/scalarboundaries.f90:197-288)
+static bool scalar_bc_kind(int k) {
+  return k == ELMM_BC_CONSTFLUX || k == ELMM_BC_DIRICHLET || k == ELMM_BC_NEUMANN;
+}
+
+// the z sides of a scalar slot whose ghost plane k_scalar_zghost writes:
+// the rules of CommonBase a fold of the interior does not give (a zero
+// flux or gradient is the fold); a temperature flux at a wall with
+// wall-model points (wm_points[side]) enters through the points instead
+template <typename T>
+static void set_zghosts(ScalSlot<T> &sl, const int32_t *bt, const double *side, const int *wm_points) {
+  for (int h = 0; h < 2; h++) {
+    const int s = h ? ELMM_TO : ELMM_BO;
+    sl.zg[h] = bt[s] == ELMM_BC_DIRICHLET || (bt[s] == ELMM_BC_NEUMANN && side[s] != 0) ||
+               (bt[s] == ELMM_BC_CONSTFLUX && side[s] != 0 && !(wm_points && wm_points[s]));
+    sl.zside[h] = side[s];
+  }
+}
+
 static int check_config(const elmm_config &c) {
   if (c.abi_version != ELMM_ABI_VERSION) return fail(ELMM_ERR_INVALID_CONFIG, "abi_version mismatch");
   if (c.Prnx < 4 || c.Prny < 4 || c.Prnz < 4) return fail(ELMM_ERR_INVALID_CONFIG, "grid must be at least 4 cells per axis");
@@ -195,12 +215,16 @@ static int check_config(const elmm_config &c) {
       const bool per = c.Btype[s] == ELMM_BC_PERIODIC;
       if (per && c.TempBtype[s] != ELMM_BC_PERIODIC)
         return fail(ELMM_ERR_INVALID_CONFIG, "the temperature must be periodic where the flow is");
-      // a surface flux is carried by the wall-model points of a wall in z
+      // a surface flux at a wall in z is carried by its wall-model points,
+      // the other kinds and sides by the ghost rules of CommonBase
       const bool wm_wall = c.wallmodeltype > 0 && c.Btype[s] == ELMM_BC_NOSLIP && (s == ELMM_BO || s == ELMM_TO);
-      if (!per && !(c.TempBtype[s] == ELMM_BC_CONSTFLUX && (c.sideTemp[s] == 0 || (wm_wall && std::isfinite(c.sideTemp[s])))))
+      if (!per && (!scalar_bc_kind(c.TempBtype[s]) || !std::isfinite(c.sideTemp[s])))
         return fail(ELMM_ERR_INVALID_CONFIG,
-                    "temperature sides: ELMM_BC_CONSTFLUX, with a non-zero sideTemp (a surface heat flux) only at a "
-                    "wall-model wall at the bottom or top");
+                    "temperature sides: ELMM_BC_CONSTFLUX, ELMM_BC_DIRICHLET or ELMM_BC_NEUMANN with a finite sideTemp");
+      if (wm_wall && c.TempBtype[s] == ELMM_BC_DIRICHLET)
+        return fail(ELMM_ERR_INVALID_CONFIG,
+                    "a prescribed surface temperature at a wall-model wall (the Monin-Obukhov Dirichlet wall model) "
+                    "is not supported");
     }
     if (c.zW) return fail(ELMM_ERR_INVALID_CONFIG, "the temperature field needs a uniform z grid");
     if (c.Btype[ELMM_BO] == ELMM_BC_PERIODIC)
@@ -215,8 +239,9 @@ static int check_config(const elmm_config &c) {
       const bool per = c.Btype[s] == ELMM_BC_PERIODIC;
       if (per && c.ScalBtype[s] != ELMM_BC_PERIODIC)
         return fail(ELMM_ERR_INVALID_CONFIG, "the scalars must be periodic where the flow is");
-      if (!per && !(c.ScalBtype[s] == ELMM_BC_CONSTFLUX && c.sideScal[s] == 0))
-        return fail(ELMM_ERR_INVALID_CONFIG, "scalar walls must be zero-flux (ELMM_BC_CONSTFLUX with sideScal = 0)");
+      if (!per && (!scalar_bc_kind(c.ScalBtype[s]) || !std::isfinite(c.sideScal[s])))
+        return fail(ELMM_ERR_INVALID_CONFIG,
+                    "scalar sides: ELMM_BC_CONSTFLUX, ELMM_BC_DIRICHLET or ELMM_BC_NEUMANN with a finite sideScal");
     }
     if (c.zW) return fail(ELMM_ERR_INVALID_CONFIG, "the scalar fields need a uniform z grid");
     if (!(c.molecular_diffusivity >= 0)) return fail(ELMM_ERR_INVALID_CONFIG, "molecular_diffusivity must be non-negative");
@@ -1038,6 +1063,7 @@ struct BatchT {
           h.tflux[side] = side == ELMM_BO ? c.sideTemp[side] : -c.sideTemp[side];
           sl.wflux[side == ELMM_BO ? 0 : 1] = h.tflux[side] * area_factor;
         }
+      set_zghosts(sl, c.TempBtype, c.sideTemp, h.wall);
       h.tdiff_live = 1;
     }
     h.kappa_mol = c.molecular_diffusivity;
@@ -1047,6 +1073,7 @@ struct BatchT {
         if ((r = dalloc((void **)f, alloc_elems * sizeof(T)))) return r;
       for (int s2 = 0; s2 < 6; s2++) sl.bt[s2] = c.ScalBtype[s2];
       sl.off = 0;
+      set_zghosts(sl, c.ScalBtype, c.sideScal, nullptr);  // no wall-model points for a passive scalar
       if (c.avg_slice_k > 0 && (r = dalloc((void **)&sl.acc_xy, sizeof(double) * h.nx * h.ny))) return r;
       if (c.avg_slice_j > 0 && (r = dalloc((void **)&sl.acc_xz, sizeof(double) * h.nx * h.nz))) return r;
     }
@@ -1178,6 +1205,13 @@ struct BatchT {
   // copied to buf[0] where the host reads it
   void launch_scalars(int stage, int accumulate, bool standalone = false) {
     if (ls[LK_TCOL].total == 0 && ls[LK_TPAIR].total == 0) return;
+    bool zghost = false;
+    for (int d = 0; d < nd; d++)
+      for (int s = 0; s < hdom[d].nslot; s++) zghost |= hdom[d].slot[s].zg[0] || hdom[d].slot[s].zg[1];
+    if (zghost) {  // BoundTemperature / BoundScalar at the start of the stage, after the stage's TDiff
+      nlaunch++;
+      k_scalar_zghost<T><<<2 * 148, 256, 0, stream>>>(ddom, nd, stage);
+    }
     if (ls[LK_TCOL].total > 0) {
       nlaunch++;
       k_scalar<T><<<gsz(11, ls[LK_TCOL].total), TX * TY, 0, stream>>>(ddom, ls[LK_TCOL].l(), kRho[stage - 1],

@@ -21,7 +21,7 @@
 
 namespace elmm {
 
-enum { BC_NOSLIP = 1, BC_FREESLIP = 2, BC_PERIODIC = 3, BC_NEUMANN = 5 };
+enum { BC_NOSLIP = 1, BC_FREESLIP = 2, BC_PERIODIC = 3, BC_DIRICHLET = 4, BC_NEUMANN = 5, BC_CONSTFLUX = 6 };
 // The z face a slab of a split domain shares with the next slab (never a
 // user code): its ghost plane holds the neighbour's plane, copied in by the
 // slab exchange, and no kernel folds onto it.
@@ -61,6 +61,12 @@ struct ScalSlot {
   // passive scalars and adiabatic walls
   double wflux[2];
   double *acc_xy, *acc_xz;  // time-averaged slices (FP64, [j][i] and [k][i]) or null
+  // z sides whose ghost plane holds CommonBase's value (BC_DIRICHLET,
+  // BC_NEUMANN, or a non-zero BC_CONSTFLUX the rules of the ghost carry),
+  // written by k_scalar_zghost before each stage: [0] the plane below
+  // k = 1, [1] the plane above k = nz; zside: the BC value of the side
+  int zg[2];
+  double zside[2];
 };
 
 // Domain descriptor, copied to device memory once at creation.  Coefficients

@@ -61,6 +61,44 @@ __device__ __forceinline__ T kappa_flux(T vel, T a, T b, T c, T e) {
   return vel > 0 ? vel * (b + (b - a) * slope / (T)2) : vel * (c + (c - e) * slope / (T)2);
 }
 
+// BoundTemperature / BoundScalar on the z sides with a stored ghost plane
+// (CommonBase, src/scalarboundaries.f90:203-288), before the stage reads
+// them: the plane below k = 1 or above k = nz of the stage's input buffer
+// from the first interior level and, for a flux, the diffusivity, whose
+// ghost is its interior value (BoundViscosity, :403-425).  FP64 arithmetic
+// on the full values (the stored value plus the slot's offset).
+template <typename T>
+__global__ void k_scalar_zghost(const Dom<T> *__restrict__ doms, int nd, int stage) {
+  for (int di = 0; di < nd; di++) {
+    const Dom<T> &d = doms[di];
+    const int nx = d.nx, ny = d.ny, nz = d.nz;
+    for (int s = 0; s < d.nslot; s++) {
+      const ScalSlot<T> &sl = d.slot[s];
+#pragma unroll 1
+      for (int h = 0; h < 2; h++) {
+        if (!sl.zg[h]) continue;
+        T *S = sl.buf[(stage - 1) % 3];
+        const int kin = h ? nz : 1, kg = h ? nz + 1 : 0, kind = sl.bt[h ? SIDE_TO : SIDE_BO];
+        const double side = sl.zside[h], off = sl.off;
+        for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nx * ny; q += gridDim.x * blockDim.x) {
+          const int i = q % nx + 1, j = q / nx + 1;
+          const double t = (double)S[bidx(d, i, j, kin)] + off;
+          double g;
+          if (kind == BC_DIRICHLET) {
+            g = side - (t - side);
+          } else if (kind == BC_NEUMANN) {
+            g = h ? t + side * d.dzW[nz + 1 + 2] : t - side * d.dzW[0 + 2];
+          } else {  // BC_CONSTFLUX
+            const double kd = (double)d.TDiff[bidx(d, i, j, kin)];
+            g = h ? t - side * d.dzW[nz + 2] / ((kd + kd) / 2.0) : t + side * d.dzW[0 + 2] / ((kd + kd) / 2.0);
+          }
+          S[bidx(d, i, j, kg)] = (T)(g - off);
+        }
+      }
+    }
+  }
+}
+
 // A block owns a TX x TY column of cells of one scalar slot and marches up a
 // chunk of TMKC planes; the scalar (k-2..k+2), the diffusivity (k-1..k+1)
 // and W(k-1) ride along in registers, x and y neighbours come from offsets
@@ -101,6 +139,9 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
       oy[q] = (scal_fold(j - 2 + q, ny, py) - j) * (int)pitch;
     }
     auto zoff = [&](int kk) { return (long long)(scal_fold(kk, nz, pz) - kk) * plane; };  // fold of plane kk
+    // the scalar's planes: a stored ghost plane (k_scalar_zghost) is read as it is
+    const int zg0 = sl.zg[0], zg1 = sl.zg[1];
+    auto szoff = [&](int kk) { return (kk == 0 && zg0) || (kk == nz + 1 && zg1) ? 0LL : zoff(kk); };
     // volume sources of this slot in this column, in configuration order
     unsigned srcm = 0;
     for (int q = 0; q < d.nsrc; q++)
@@ -121,7 +162,7 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
     // column windows: the scalar at k-2..k+2, diffusivity at k-1..k+1, W at k-1
     T sz[5], kz[3];
 #pragma unroll
-    for (int q = 0; q < 5; q++) sz[q] = ld(S, cc + (long long)(q - 2) * plane + zoff(k0 - 2 + q));
+    for (int q = 0; q < 5; q++) sz[q] = ld(S, cc + (long long)(q - 2) * plane + szoff(k0 - 2 + q));
 #pragma unroll
     for (int q = 0; q < 3; q++) kz[q] = ld(K, cc + (long long)(q - 1) * plane + zoff(k0 - 1 + q));
     T wb = ld(W, cc - plane);
@@ -195,7 +236,7 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
         const long long cn = cc + plane;
 #pragma unroll
         for (int q = 0; q < 4; q++) sz[q] = sz[q + 1];
-        sz[4] = ld(S, cn + 2 * plane + zoff(k + 3));
+        sz[4] = ld(S, cn + 2 * plane + szoff(k + 3));
         kz[0] = kz[1];
         kz[1] = kz[2];
         kz[2] = ld(K, cn + plane + zoff(k + 2));
@@ -258,6 +299,8 @@ __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SP
 #pragma unroll
     for (int q = 0; q < 5; q++) oy[q] = (scal_fold(j - 2 + q, ny, py) - j) * (int)pitch;
     auto zoff = [&](int kk) { return (long long)(scal_fold(kk, nz, pz) - kk) * plane; };
+    const int zg0 = sl.zg[0], zg1 = sl.zg[1];
+    auto szoff = [&](int kk) { return (kk == 0 && zg0) || (kk == nz + 1 && zg1) ? 0LL : zoff(kk); };
     unsigned srcm = 0;  // volume sources of this slot in this pair's columns
     for (int q = 0; q < d.nsrc; q++)
       if (d.src_slot[q] == s && (d.src_i[q] == i || d.src_i[q] == i + 1) && d.src_j[q] == j) srcm |= 1u << q;
@@ -276,7 +319,7 @@ __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SP
     long long cc = bidx(d, i, j, k0);
     float2 sz[5], kz[3];
 #pragma unroll
-    for (int q = 0; q < 5; q++) sz[q] = ld2(S, cc + (long long)(q - 2) * plane + zoff(k0 - 2 + q));
+    for (int q = 0; q < 5; q++) sz[q] = ld2(S, cc + (long long)(q - 2) * plane + szoff(k0 - 2 + q));
 #pragma unroll
     for (int q = 0; q < 3; q++) kz[q] = ld2(K, cc + (long long)(q - 1) * plane + zoff(k0 - 1 + q));
     float2 wb = ld2(W, cc - plane);
@@ -301,7 +344,7 @@ __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SP
       float2 sz_n = sz[4], kz_n = kz[2];
       if (k < k1) {
         nxt = load_plane(cc + plane);
-        sz_n = ld2(S, cc + 3 * plane + zoff(k + 3));
+        sz_n = ld2(S, cc + 3 * plane + szoff(k + 3));
         kz_n = ld2(K, cc + 2 * plane + zoff(k + 2));
       }
       const float2 s0 = sz[2];

@@ -130,17 +130,20 @@ typedef struct elmm_config {
   int32_t device;               /* CUDA device ordinal */
   /* Potential temperature: transport by ScalarRK3 (src/scalars.f90:88-381) and
    * buoyancy in the W tendency (BuoyancyForce, src/dynamics.f90:608-690).
-   * Supported: TempBtype periodic on the periodic x and y sides and
-   * ELMM_BC_CONSTFLUX at the bottom and top: sideTemp = 0 (adiabatic), or a
-   * surface heat flux (K m/s, positive upward: into the flow at the bottom,
-   * out of it at the top) at a wall-model wall.  The flux enters the cells next to the
-   * wall through the wall-model points (src/scalars.f90:323-327), and a
-   * flux into the flow (unstable stratification) over a rough wall makes
-   * the wall model's u* follow Monin-Obukhov similarity (WM_MO_FluxStress,
-   * src/wallmodels.f90:1836-1854, 2255-2259). */
+   * Supported: TempBtype periodic on the periodic x and y sides, and at the
+   * bottom and top the kinds of CommonBase (src/scalarboundaries.f90:197-288):
+   * ELMM_BC_DIRICHLET (sideTemp the value at the face), ELMM_BC_NEUMANN
+   * (the gradient) or ELMM_BC_CONSTFLUX (the flux, K m/s positive upward;
+   * 0 is adiabatic).  At a wall-model wall a flux is a surface heat flux:
+   * it enters the cells next to the wall through the wall-model points
+   * (src/scalars.f90:323-327), and a flux into the flow over a rough wall
+   * makes the wall model's u* follow Monin-Obukhov similarity
+   * (WM_MO_FluxStress, src/wallmodels.f90:1836-1854, 2255-2259); a
+   * Dirichlet value there (the Monin-Obukhov Dirichlet wall model) is
+   * refused.  Elsewhere the ghost rules of CommonBase carry the kind. */
   int32_t enable_buoyancy;      /* 0: no temperature field */
   int32_t TempBtype[6];         /* temperature BC per side (src/initial.f90:347-352) */
-  double sideTemp[6];           /* BC values: the flux for ELMM_BC_CONSTFLUX */
+  double sideTemp[6];           /* BC values: value, gradient or flux of the kind */
   double temperature_ref;       /* src/parameters.f90:220 (295 K) */
   double grav_acc;              /* src/parameters.f90:146 (9.81) */
   double molecular_diffusivity; /* molecular_viscosity / Prandtl (src/initial.f90:791; Prandtl 0.7) */
@@ -149,10 +152,11 @@ typedef struct elmm_config {
    * term as the temperature, plus point sources.  Without buoyancy TDiff is
    * set once by the initial projection and then kept, as in the reference
    * (src/initial.f90:4296-4313; src/dynamics.f90:904 updates it only with
-   * buoyancy).  Supported ScalBtype: as TempBtype. */
+   * buoyancy).  Supported ScalBtype: as TempBtype, every kind by the ghost
+   * rules of CommonBase (the wall-model points carry no scalar flux). */
   int32_t num_scalars;          /* 0..ELMM_MAX_SCALARS */
   int32_t ScalBtype[6];         /* scalar BC per side (src/initial.f90:508-519) */
-  double sideScal[6];           /* BC values: the flux for ELMM_BC_CONSTFLUX */
+  double sideScal[6];           /* BC values: value, gradient or flux of the kind */
   int32_t num_point_sources;    /* 0..ELMM_MAX_POINT_SOURCES */
   int32_t reserved0;            /* 0 */
   elmm_point_source point_sources[ELMM_MAX_POINT_SOURCES];

@@ -769,9 +769,11 @@ static void BuoyancyForce(Domain &d, A3 &Wst) {
         Wst(i, j, k) = Wst(i, j, k) + A2 * (d.T(i, j, k + 1) + d.T(i, j, k)) - A * d.temperature_ref;
 }
 
-// BoundTemperature -> CommonBase, scalarboundaries.f90:12-300, for periodic
-// and constant-flux sides (the x, y loops run over the ranges of the
-// reference, corners included where it includes them)
+// BoundTemperature -> CommonBase, scalarboundaries.f90:12-300: periodic and
+// constant-flux x and y sides, and in z periodic, Dirichlet, Neumann,
+// constant-flux and (TempBtype 0 after GetOutsideBoundariesWM_Pr) mirror
+// sides (the x, y loops run over the ranges of the reference, corners
+// included where it includes them)
 static void CommonBase(Domain &d, A3 &a, const int *bt, const double *side) {
   const int nx = d.Prnx, ny = d.Prny, nz = d.Prnz;
   for (int k = 1; k <= nz; k++)
@@ -814,6 +816,12 @@ static void CommonBase(Domain &d, A3 &a, const int *bt, const double *side) {
         for (int g = -2; g <= 0; g++) a(i, j, g) = a(i, j, nz + g);
       } else if (bt[Bo] == 0) {  // mirror
         for (int g = -2; g <= 0; g++) a(i, j, g) = a(i, j, 1 - g);
+      } else if (bt[Bo] == ELMM_BC_DIRICHLET) {
+        for (int g = -2; g <= 0; g++) a(i, j, g) = side[Bo] - (a(i, j, 1 - g) - side[Bo]);
+      } else if (bt[Bo] == BC_NEUMANN) {
+        a(i, j, 0) = a(i, j, 1) - side[Bo] * d.dzW(0);
+        a(i, j, -1) = a(i, j, 1) - side[Bo] * (d.zPr(1) - d.zPr(-1));
+        a(i, j, -2) = a(i, j, 1) - side[Bo] * (d.zPr(1) - d.zPr(-2));
       } else {
         a(i, j, 0) = a(i, j, 1) + side[Bo] * d.dzW(0) / ((d.TDiff(i, j, 1) + d.TDiff(i, j, 0)) / 2.0);
         a(i, j, -1) = a(i, j, 0) - (a(i, j, 1) - a(i, j, 0));
@@ -823,6 +831,12 @@ static void CommonBase(Domain &d, A3 &a, const int *bt, const double *side) {
         for (int g = 1; g <= 3; g++) a(i, j, nz + g) = a(i, j, g);
       } else if (bt[To] == 0) {  // mirror
         for (int g = 1; g <= 3; g++) a(i, j, nz + g) = a(i, j, nz + 1 - g);
+      } else if (bt[To] == ELMM_BC_DIRICHLET) {
+        for (int g = 1; g <= 3; g++) a(i, j, nz + g) = side[To] - (a(i, j, nz + 1 - g) - side[To]);
+      } else if (bt[To] == BC_NEUMANN) {
+        a(i, j, nz + 1) = a(i, j, nz) + side[To] * d.dzW(nz + 1);
+        a(i, j, nz + 2) = a(i, j, nz) + side[To] * (d.zPr(nz + 2) - d.zPr(nz));
+        a(i, j, nz + 3) = a(i, j, nz) + side[To] * (d.zPr(nz + 3) - d.zPr(nz));
       } else {
         a(i, j, nz + 1) = a(i, j, nz) - side[To] * d.dzW(nz) / ((d.TDiff(i, j, nz) + d.TDiff(i, j, nz + 1)) / 2.0);
         a(i, j, nz + 2) = a(i, j, nz + 1) - (a(i, j, nz) - a(i, j, nz + 1));

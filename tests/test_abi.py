@@ -117,7 +117,7 @@ def test_config_defaults_and_errors_without_gpu():
     bad = cfgmod.make_config(64, 64, 32, num_scalars=1, avg_slice_k=33)
     assert lib.elmm_create(C.byref(bad), C.byref(h)) == 1
     bad = cfgmod.make_config(64, 64, 32, num_scalars=1)
-    bad.sideScal[4] = 1.0  # a non-zero wall flux is not supported
+    bad.ScalBtype[4] = 1  # no-slip is not a kind of scalar side
     assert lib.elmm_create(C.byref(bad), C.byref(h)) == 1
     assert lib.elmm_create(None, C.byref(h)) == 6
     assert lib.elmm_step(None, 1, None) == 6

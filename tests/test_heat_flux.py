@@ -14,8 +14,9 @@ src/wallmodels.f90:1606-1660, 1836-1854).
   velocity and theta - T_ref within 1e-5;
 * the heat content grows by (q_bottom - q_top) Lx Ly per unit time on both
   paths (advection and diffusion are in flux form);
-* a non-zero flux where no wall-model points carry it (a free-slip top) is
-  refused with ELMM_ERR_INVALID_CONFIG.
+* a non-finite flux is refused with ELMM_ERR_INVALID_CONFIG (a flux
+  through a free-slip top, which no wall-model points carry, takes
+  CommonBase's ghost rule: tests/test_scalar_bcs.py).
 """
 import numpy as np
 import pytest
@@ -107,12 +108,11 @@ def test_heat_content_follows_the_surface_fluxes(precision):
     d.close()
 
 
-def test_flux_without_wall_model_points_is_refused():
-    with pytest.raises(L.ElmmError) as e:
-        L.Domain(make_config(*N, buoyancy=True, heat_flux=(0.0, 0.1)))      # free-slip top
-    assert e.value.code == 1
+def test_non_finite_flux_is_refused():
     with pytest.raises(L.ElmmError) as e:
         L.Domain(make_config(*N, buoyancy=True, heat_flux=(float("nan"), 0.0)))
     assert e.value.code == 1
     L.Domain(make_config(*N, buoyancy=True, heat_flux=(0.1, 0.0))).close()
+    # a flux through the free-slip top has no wall-model points: the ghost rule carries it
     assert BC_FREESLIP == make_config(*N).Btype[5]
+    L.Domain(make_config(*N, buoyancy=True, heat_flux=(0.0, 0.1))).close()

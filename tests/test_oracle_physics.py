@@ -373,3 +373,60 @@ def test_unstable_surface_flux_follows_monin_obukhov():
         lo, hi = (mid, hi) if fp(lo) * fp(mid) > 0 else (lo, mid)
     assert abs(us - lo) / lo < 2e-2, (us, lo)
     assert us > 0.4 * vel / math.log(z / z0)      # more drag than the neutral law with its 0.4
+
+
+def test_linear_temperature_profile_is_steady():
+    """Fluid at rest with molecular diffusion only (no SGS model, so no
+    wall model), theta linear in z with the gradient of a Neumann bottom and
+    the value of a Dirichlet top at the top face (CommonBase BC_NEUMANN and
+    BC_DIRICHLET, src/scalarboundaries.f90:203-288): the ghost rules continue
+    the line, so the discrete Laplacian vanishes, and the buoyancy of a
+    z-only field is a gradient the projection removes; theta stays as it
+    is."""
+    from gpu_elmm_b200.config import BC_DIRICHLET, FIELD_TEMPERATURE
+    from gpu_elmm_b200.workloads import interior
+    n, gam, top = (16, 12, 10), 0.01, 300.0
+    cfg = make_config(*n, sgstype=0, buoyancy=True, temperature_bc=((BC_NEUMANN, gam), (BC_DIRICHLET, top)))
+    g = grid_of(cfg)
+    U, V, W, Pr = (np.zeros(s) for s in (g.shape_u(), g.shape_v(), g.shape_w(), g.shape_p()))
+    T = np.zeros(g.shape_t())
+    zpr = np.arange(1, n[2] + 1) - 0.5
+    interior(T, -2, n)[...] = (top + gam * (zpr - n[2]))[:, None, None]
+    o = Oracle(cfg)
+    o.set_state(U, V, W, Pr)
+    o.set_field(FIELD_TEMPERATURE, T)
+    o.project(1.0)
+    o.step(3)
+    T1 = interior(o.get_field(FIELD_TEMPERATURE), -2, n)
+    assert np.abs(T1 - interior(T, -2, n)).max() < 1e-11
+    assert np.abs(interiors(g, *o.state())[2]).max() < 1e-14
+
+
+@pytest.mark.parametrize("field", ["temperature", "scalar"])
+def test_ghost_rule_fluxes_change_the_content(field):
+    """CommonBase's BC_CONSTFLUX ghost rule, arr(nz+1) = arr(nz) -
+    q dzW(nz) / TDiff: a flux through the free-slip top of the temperature
+    (a flux at a free-slip side has no wall-model points), or through both z
+    sides of a passive scalar (the scalars keep the ghost rule at a
+    wall-model wall too), changes the content by (q_bottom - q_top) Lx Ly
+    per unit time."""
+    from gpu_elmm_b200.config import BC_CONSTFLUX, FIELD_SCALAR, FIELD_TEMPERATURE
+    from gpu_elmm_b200.workloads import interior, puff_state
+    n = (16, 12, 10)
+    if field == "temperature":
+        (qb, qt), fid = (0.15, 0.05), FIELD_TEMPERATURE
+        g, o = _buoyant_channel(n=n, temperature_bc=((BC_CONSTFLUX, qb), (BC_CONSTFLUX, qt)))
+    else:
+        (qb, qt), fid = (0.2, -0.1), FIELD_SCALAR
+        cfg = make_config(*n, num_scalars=1, scalar_bc=((BC_CONSTFLUX, qb), (BC_CONSTFLUX, qt)))
+        g = grid_of(cfg)
+        o = Oracle(cfg)
+        o.set_state(*log_profile_state(g, seed=2))
+        o.set_field(FIELD_SCALAR, puff_state(g, (8, 6, 4)))
+        o.project(1.0)
+    h0 = interior(o.get_field(fid), -2, n).sum()
+    steps, dt = 4, 0.02
+    o.step(steps)
+    h1 = interior(o.get_field(fid), -2, n).sum()
+    expect = (qb - qt) * n[0] * n[1] * dt * steps
+    assert abs((h1 - h0) - expect) < 1e-9 * abs(expect) + 1e-12 * abs(h0), (h1 - h0, expect)
