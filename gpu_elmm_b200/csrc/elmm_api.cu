@@ -161,14 +161,16 @@ static bool scalar_bc_kind(int k) {
 
 // the z sides of a scalar slot whose ghost plane k_scalar_zghost writes:
 // the rules of CommonBase a fold of the interior does not give (a zero
-// flux or gradient is the fold); a temperature flux at a wall with
-// wall-model points (wm_points[side]) enters through the points instead
+// flux or gradient is the fold); a temperature flux or surface temperature
+// at a wall with wall-model points (wm_points[side]) enters through the
+// points instead
 template <typename T>
 static void set_zghosts(ScalSlot<T> &sl, const int32_t *bt, const double *side, const int *wm_points) {
   for (int h = 0; h < 2; h++) {
     const int s = h ? ELMM_TO : ELMM_BO;
-    sl.zg[h] = bt[s] == ELMM_BC_DIRICHLET || (bt[s] == ELMM_BC_NEUMANN && side[s] != 0) ||
-               (bt[s] == ELMM_BC_CONSTFLUX && side[s] != 0 && !(wm_points && wm_points[s]));
+    const bool points = wm_points && wm_points[s];
+    sl.zg[h] = (bt[s] == ELMM_BC_DIRICHLET && !points) || (bt[s] == ELMM_BC_NEUMANN && side[s] != 0) ||
+               (bt[s] == ELMM_BC_CONSTFLUX && side[s] != 0 && !points);
     sl.zside[h] = side[s];
   }
 }
@@ -221,10 +223,10 @@ static int check_config(const elmm_config &c) {
       if (!per && (!scalar_bc_kind(c.TempBtype[s]) || !std::isfinite(c.sideTemp[s])))
         return fail(ELMM_ERR_INVALID_CONFIG,
                     "temperature sides: ELMM_BC_CONSTFLUX, ELMM_BC_DIRICHLET or ELMM_BC_NEUMANN with a finite sideTemp");
-      if (wm_wall && c.TempBtype[s] == ELMM_BC_DIRICHLET)
+      if (wm_wall && c.TempBtype[s] == ELMM_BC_DIRICHLET && !(c.z0[s] > 0))
         return fail(ELMM_ERR_INVALID_CONFIG,
-                    "a prescribed surface temperature at a wall-model wall (the Monin-Obukhov Dirichlet wall model) "
-                    "is not supported");
+                    "a prescribed surface temperature at a wall-model wall needs a rough wall (z0 > 0): the "
+                    "Monin-Obukhov Dirichlet wall model is the rough-wall branch");
     }
     if (c.zW) return fail(ELMM_ERR_INVALID_CONFIG, "the temperature field needs a uniform z grid");
     if (c.Btype[ELMM_BO] == ELMM_BC_PERIODIC)
@@ -1029,6 +1031,11 @@ struct BatchT {
         if ((r = dalloc((void **)&h.wm_ustar[f], np * sizeof(double)))) return r;
         std::vector<double> ones(np, 1.0);  // WMPointUVW%ustar = 1 initially (wallmodels.f90:80)
         CU(cudaMemcpy(h.wm_ustar[f], ones.data(), np * sizeof(double), cudaMemcpyHostToDevice));
+        if (c.enable_buoyancy && (s == ELMM_BO || s == ELMM_TO) && c.TempBtype[s] == ELMM_BC_DIRICHLET) {
+          // a prescribed surface temperature: the points' temperature_flux, 0 initially
+          if ((r = dalloc((void **)&h.wm_tfl[f], np * sizeof(double)))) return r;
+          CU(cudaMemset(h.wm_tfl[f], 0, np * sizeof(double)));
+        }
       }
     if (c.enable_buoyancy) {
       h.buoy = 1;
@@ -1062,7 +1069,21 @@ struct BatchT {
         if (h.wall[side] && c.TempBtype[side] == ELMM_BC_CONSTFLUX) {
           h.tflux[side] = side == ELMM_BO ? c.sideTemp[side] : -c.sideTemp[side];
           sl.wflux[side == ELMM_BO ? 0 : 1] = h.tflux[side] * area_factor;
+        } else if (h.wall[side] && c.TempBtype[side] == ELMM_BC_DIRICHLET) {
+          // a prescribed surface temperature (WM_MO_Dirichlet): the Pr points
+          // next to the wall with u* = 1 and no flux initially
+          // (src/wallmodels.f90:570-627)
+          const int hh = side == ELMM_BO ? 0 : 1;
+          const size_t np = (size_t)h.nx * h.ny;
+          h.tdir[side] = 1;
+          h.tsurf[side] = c.sideTemp[side];
+          if ((r = dalloc((void **)&h.wm_pr_us[hh], np * sizeof(double)))) return r;
+          if ((r = dalloc((void **)&h.wm_pr_tf[hh], np * sizeof(double)))) return r;
+          std::vector<double> ones(np, 1.0);
+          CU(cudaMemcpy(h.wm_pr_us[hh], ones.data(), np * sizeof(double), cudaMemcpyHostToDevice));
+          CU(cudaMemset(h.wm_pr_tf[hh], 0, np * sizeof(double)));
         }
+      h.wm_af = area_factor;
       set_zghosts(sl, c.TempBtype, c.sideTemp, h.wall);
       h.tdiff_live = 1;
     }
@@ -1147,12 +1168,17 @@ struct BatchT {
   }
   static int chunk_index(int kc) { return kc == 8 ? 0 : kc == 16 ? 1 : 2; }
   // k_sgs with the tuned z chunk; init: 0 a stage, 1 the initial viscosity
-  // and diffusivity, 2 the autotuner's timing mode (k_sgs)
-  void sgs_kernel(int init) {
+  // and diffusivity, 2 the autotuner's timing mode (k_sgs); stage: the RK3
+  // stage whose start temperature the wall model reads (1 outside a step)
+  void sgs_kernel(int init, int stage = 1) {
     const int q = chunk_index(tune_sgs_kc), g = std::max(1, std::min(ls[LK_SGST].total, cap_sgs[q]));
-    if (tune_sgs_kc == 8) k_sgs<T, 8><<<g, SgsShape<T>::threads, smem_sgs, stream>>>(ddom, ls[LK_SGST].l(), init);
-    else if (tune_sgs_kc == 16) k_sgs<T, 16><<<g, SgsShape<T>::threads, smem_sgs, stream>>>(ddom, ls[LK_SGST].l(), init);
-    else k_sgs<T, 32><<<g, SgsShape<T>::threads, smem_sgs, stream>>>(ddom, ls[LK_SGST].l(), init);
+    const int tb = (stage - 1) % 3;
+    if (tune_sgs_kc == 8)
+      k_sgs<T, 8><<<g, SgsShape<T>::threads, smem_sgs, stream>>>(ddom, ls[LK_SGST].l(), init, tb);
+    else if (tune_sgs_kc == 16)
+      k_sgs<T, 16><<<g, SgsShape<T>::threads, smem_sgs, stream>>>(ddom, ls[LK_SGST].l(), init, tb);
+    else
+      k_sgs<T, 32><<<g, SgsShape<T>::threads, smem_sgs, stream>>>(ddom, ls[LK_SGST].l(), init, tb);
   }
   void momentum_kernel(const StageCoef &sc) {
     const int q = chunk_index(tune_mom_kc), g = std::max(1, std::min(ls[LK_MOMT].total, cap_mom[q]));
@@ -1160,9 +1186,9 @@ struct BatchT {
     else if (tune_mom_kc == 16) k_momentum<T, 16><<<g, MomShape<T>::threads, smem_mom, stream>>>(ddom, ls[LK_MOMT].l(), sc);
     else k_momentum<T, 32><<<g, MomShape<T>::threads, smem_mom, stream>>>(ddom, ls[LK_MOMT].l(), sc);
   }
-  int launch_sgs() {
+  int launch_sgs(int stage) {
     nlaunch++;
-    sgs_kernel(0);
+    sgs_kernel(0, stage);
     launch_ghosts({F_NU}, 0);
     return ELMM_OK;
   }
@@ -1395,7 +1421,7 @@ struct BatchT {
         if (x.nwm > 0) {
           nlaunch++;
           k_ib_wm<T><<<std::min((x.nwm + 127) / 128, 148 * 8), 128, 0, stream>>>(ddom, d, x.wm, x.wm_ustar, x.nwm,
-                                                                               kBeta[stage - 1]);
+                                                                               kBeta[stage - 1], 0);
         }
         if (x.nib > 0) {
           nlaunch++;
@@ -1414,7 +1440,7 @@ struct BatchT {
   // IBMomentum replaces the IB points (the check of PostPoisson,
   // src/pressure.f90:884-989, is div U - Q on that field)
   int run_stage(int stage, int stop, int accumulate = 0, bool standalone = false, bool div = false) {
-    launch_sgs();
+    launch_sgs(stage);
     if (any_solids()) launch_ib(0, stage);  // after BoundViscosity (src/dynamics.f90:896-902)
     if (stop == 1) return ELMM_OK;
     launch_momentum(stage);
@@ -1973,9 +1999,15 @@ struct BatchT {
     launch_projection(coef, 0, 0);
     launch_refine(coef, 0);
     launch_divmax();
-    // the end of InitialConditions (src/initial.f90:4291-4313): eddy
-    // viscosity of the projected field and, with scalars, their diffusivity
+    // the end of InitialConditions (src/initial.f90:4291-4336): eddy
+    // viscosity of the projected field and, with scalars, their diffusivity,
+    // and the wall model once on the initial fields (the u* and fluxes its
+    // points carry into the first stage; the solid-face points' u* alone)
     sgs_kernel(1);
+    for (int d = 0; d < nd && d < (int)sol.size(); d++)
+      if (sol[d].on && sol[d].nwm > 0)
+        k_ib_wm<T><<<std::min((sol[d].nwm + 127) / 128, 148 * 8), 128, 0, stream>>>(ddom, d, sol[d].wm,
+                                                                                   sol[d].wm_ustar, sol[d].nwm, 0.0, 1);
     launch_ghosts({F_NU}, 0);
     CU(cudaEventRecord(t1, stream));
     CU(cudaStreamSynchronize(stream));
@@ -2003,7 +2035,7 @@ struct BatchT {
         cudaEventRecord(ev[2 * slot.size() + 1], stream);
         slot.push_back(k);
       };
-      timed(0, [&] { sgs_kernel(0); });
+      timed(0, [&] { sgs_kernel(0, stage); });
       timed(kGhost, [&] { launch_ghosts({F_NU}, 0); });
       timed(1, [&] {
         momentum_kernel(sc);

@@ -120,6 +120,15 @@ struct Dom {
   // wall model: per face plane fluxp/fluxm/ustar, plane dims from ext[]
   T *wm_fluxp[kFaces], *wm_fluxm[kFaces];
   double *wm_ustar[kFaces];
+  // a prescribed surface temperature at a wall-model wall (tdir[side], the
+  // value tsurf[side]): the temperature_flux state of the face's velocity
+  // points (as wm_ustar), the u* and flux of the Pr points next to the
+  // bottom [0] and top [1] per (i, j), and ComputeAreaFactor of the points
+  int tdir[6];
+  double tsurf[6];
+  double *wm_tfl[kFaces];
+  double *wm_pr_us[2], *wm_pr_tf[2];
+  double wm_af;
   // stretched z, packed FP32 momentum path: per-level factors kz2[q * (nz + 2) + k]
   // (q: kZ2 entries, see elmm_packed.cuh)
   const float *kz2;

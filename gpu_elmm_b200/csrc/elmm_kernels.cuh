@@ -124,11 +124,96 @@ __device__ inline double wm_mo_flux_ustar(double ustar, double vel, double dist,
   }
 }
 
+// PsiM_MO_mod / PsiH_MO_mod, the stability functions of Zilitinkevich and
+// Esau (2006) with L defined with the von Karman constant k_U
+// (src/wallmodels.f90:1572-1595)
+__device__ inline double psim_mo_mod(double zeta, double kU) {
+  if (zeta < 0) {
+    const double x = pow(1 - 6.0 * zeta * kU, 0.25), h = (1 + x) / 2.0;
+    return log(((1 + x * x) / 2.0) * (h * h)) - 2.0 * atan(x) + 3.141592653589793 / 2;
+  }
+  return -(3 * pow(zeta * kU, 5.0 / 6.0));
+}
+__device__ inline double psih_mo_mod(double zeta, double kU) {
+  if (zeta < 0) {
+    const double x = pow(1 - 6.0 * zeta * kU, 0.25);
+    return 2.0 * log((1 + x * x) / 2.0);
+  }
+  return -(2.5 * pow(zeta * kU, 4.0 / 5.0));
+}
+
+// WM_MO_Dirichlet_ustar_tfl (src/wallmodels.f90:1664-1716): u* and the
+// surface temperature flux of a rough wall with a prescribed surface
+// temperature, tempdif = theta(point) - theta(surface).  tflux comes in as
+// the point's flux of the stage before (the start of the stability
+// iteration, relaxed until z/L changes by less than 1e-3); its 1.1 is a
+// default-real literal in the reference.
+template <typename T>
+__device__ inline void wm_mo_dirichlet(const Dom<T> &d, double &ustar, double &tflux, double dist, double z0,
+                                       double vel, double tempdif) {
+  const double kU = 0.4, kT = 0.47, nu = d.nu_mol;
+  ustar = wm_rough_ustar(ustar, vel, dist, z0, nu);
+  double dist_plus = 1.7976931348623157e308;  // huge()
+  if (nu > 0) dist_plus = dist * sqrt(nu * vel / dist) / nu;
+  if (dist <= z0 || dist_plus < (double)1.1f * 11.225) {
+    tflux = -d.kappa_mol * tempdif / dist;
+    return;
+  }
+  double zL = 0, zL0 = -10000.0;
+  int i = 0;
+  for (;;) {
+    i++;
+    zL = -dist * d.grav * tflux / (kU * d.tref * (ustar * ustar * ustar));
+    const double pm = psim_mo_mod(zL, kU), ph = psih_mo_mod(zL, kU);
+    ustar = vel * kU / (log(dist / z0) - pm);
+    tflux = -tempdif * ustar * kT / (log(dist / z0) - ph);  // z0H = z0
+    if (i > 1 && fabs(zL - zL0) / fmax(fabs(zL), 1e-4) < 1e-3) break;
+    if (i >= 50 || zL > 10000) break;
+    zL0 = zL;
+  }
+  if (i >= 50 || zL > 10000) {
+    ustar = sqrt(nu * vel / dist);
+    tflux = -d.kappa_mol * tempdif / dist;
+  }
+}
+
+// ComputeViscsWM for the Pr point next to side f (bottom or top) at cell
+// (i, j, k) with a prescribed surface temperature (WM_MO_Dirichlet,
+// src/wallmodels.f90:1858-1884, 2080-2111): the point's u* and surface
+// temperature flux from the cell-centred velocity and theta at the start of
+// the stage (Tm); the viscosity it forms is overwritten by SubgridModel in
+// the reference and is not kept.
+template <typename T>
+__device__ void wm_pr_dirichlet(const Dom<T> &d, int f, int i, int j, int k, const T *Tm) {
+  const long long c = bidx(d, i, j, k);
+  double ou = 0, ov = 0;
+  if constexpr (sizeof(T) == 4) { ou = (double)vel_off(d, 0, k); ov = (double)vel_off(d, 1, k); }
+  const double uv[3] = {(((double)ld(d.U, c) + ou) + ((double)ld(d.U, c - 1) + ou)) / 2.0,
+                        (((double)ld(d.V, c) + ov) + ((double)ld(d.V, c - d.pitch) + ov)) / 2.0,
+                        ((double)ld(d.W, c) + (double)ld(d.W, c - d.plane)) / 2.0};
+  const double distz = f == SIDE_BO ? d.zW[0 + 2] - d.zPr[1 + 2] : d.zW[d.ext[2][2] + 1 + 2] - d.zPr[d.nz + 2];
+  const double dv[3] = {0.0, 0.0, distz};
+  const double dist = sqrt((dv[0] * dv[0] + dv[1] * dv[1]) + dv[2] * dv[2]);
+  const double dot = (uv[0] * dv[0] + uv[1] * dv[1]) + uv[2] * dv[2];
+  double vect[3];
+#pragma unroll
+  for (int m = 0; m < 3; m++) vect[m] = uv[m] - dot * dv[m] / (dist * dist);
+  const double vel = sqrt((vect[0] * vect[0] + vect[1] * vect[1]) + vect[2] * vect[2]);
+  const double tdif = ((double)ld(Tm, c) + d.toff) - d.tsurf[f];
+  const int h = f == SIDE_BO ? 0 : 1;
+  const long long q = (long long)(i - 1) + (long long)d.nx * (j - 1);
+  double ustar = d.wm_pr_us[h][q], tfl = d.wm_pr_tf[h][q];
+  wm_mo_dirichlet(d, ustar, tfl, dist, d.z0[f], vel, tdif);
+  if (ustar < 0) ustar = 0;
+  d.wm_pr_us[h][q] = ustar;
+  d.wm_pr_tf[h][q] = tfl;
+}
+
 // ComputeUVWFluxesWM / fluxes for the point of component comp on side f at
 // cell (i,j,k) (src/wallmodels.f90:2159-2338); the wall-point distance is
 // the one of GetOutsideBoundariesWM_UVW (src/wallmodels.f90:690-909).
 template <typename T>
-__device__ void wm_point(const Dom<T> &d, int comp, int f, int i, int j, int k, long long pidx) {
+__device__ void wm_point(const Dom<T> &d, int comp, int f, int i, int j, int k, long long pidx, const T *Tm) {
   const T *U = d.U, *V = d.V, *W = d.W;
   const long long c = bidx(d, i, j, k), sx = 1, sy = d.pitch, sz = d.plane;
   // full velocities: stored values plus the per-level offsets of U and V of
@@ -185,7 +270,16 @@ __device__ void wm_point(const Dom<T> &d, int comp, int f, int i, int j, int k, 
   double tv = norm2_3(t);
   const int face = comp * 6 + f;
   double ustar = d.wm_ustar[face][pidx];
-  if (d.z0[f] > 0 && d.tflux[f] > 0)  // WM_MO_FluxStress (src/wallmodels.f90:1836-1854, 2255-2259)
+  if (d.z0[f] > 0 && d.tdir[f]) {  // WM_MO_DirichletStress (src/wallmodels.f90:1922-1938, 2228-2253)
+    const double vel2 = sqrt((t[0] * t[0] + t[1] * t[1]) + t[2] * t[2]);  // sqrt(sum(tan_vect**2))
+    // local_value of theta at the point (src/wallmodels.f90:2340-2353), x and y periodic
+    const int i2 = comp == 0 ? (i + 1 > d.nx ? 1 : i + 1) : i, j2 = comp == 1 ? (j + 1 > d.ny ? 1 : j + 1) : j;
+    const double temp = (((double)ld(Tm, bidx(d, i2, j2, comp == 2 ? k + 1 : k)) + d.toff) +
+                         ((double)ld(Tm, bidx(d, i, j, k)) + d.toff)) / 2;
+    double tfl = d.wm_tfl[face][pidx];
+    wm_mo_dirichlet(d, ustar, tfl, dd, d.z0[f], vel2, temp - d.tsurf[f]);
+    d.wm_tfl[face][pidx] = tfl;
+  } else if (d.z0[f] > 0 && d.tflux[f] > 0)  // WM_MO_FluxStress (src/wallmodels.f90:1836-1854, 2255-2259)
     ustar = tv != 0 ? wm_mo_flux_ustar(ustar, tv, dd, d.z0[f], d.tflux[f], d.tref, d.grav, d.nu_mol) : 0.0;
   else if (tv != 0)
     ustar = wm_ustar(ustar, tv, dd, d.z0[f], d.nu_mol);

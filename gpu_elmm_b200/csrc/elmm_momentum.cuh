@@ -870,7 +870,9 @@ __device__ __forceinline__ F2 nusmag2(const SgsK<float> &q, const RT &R) {
 }
 
 template <typename T>
-__device__ void wm_point(const Dom<T> &d, int comp, int f, int i, int j, int k, long long pidx);
+__device__ void wm_point(const Dom<T> &d, int comp, int f, int i, int j, int k, long long pidx, const T *Tm);
+template <typename T>
+__device__ void wm_pr_dirichlet(const Dom<T> &d, int f, int i, int j, int k, const T *Tm);
 template <typename T>
 __device__ long long wm_plane_index(const Dom<T> &d, int comp, int f, int i, int j, int k);
 
@@ -893,12 +895,14 @@ struct SgsShape<float> {
 };
 
 // init: 0 a stage (viscosity, diffusivity, wall-model points), 1 the initial
-// viscosity and diffusivity after the projection, 2 the autotuner's timing
-// launches (a stage's arithmetic without the wall-model points, whose u*
-// carries the start of the smooth-wall iteration from stage to stage)
+// viscosity and diffusivity after the projection, with the wall model once
+// on the initial fields (src/initial.f90:4331-4336), 2 the autotuner's
+// timing launches (a stage's arithmetic without the wall-model points,
+// whose u* and fluxes carry the start of their iterations from stage to
+// stage).  tb: the temperature buffer of the stage (its start value).
 template <typename T, int KC = MKC>
 __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
-    k_sgs(const Dom<T> *__restrict__ doms, Launch L, int init) {
+    k_sgs(const Dom<T> *__restrict__ doms, Launch L, int init, int tb) {
   // planes of U, V, W (tile plus one-cell halo) arrive by tensor-map TMA in
   // a ring of kRingSlots slots, as in k_momentum
   typedef SlotLayout<T, 3, 0> Lay;
@@ -1033,7 +1037,8 @@ __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
         }
       }
       const int wk = wtile | (wmask & ((k == 1 ? 16 : 0) | (k >= nz - 1 ? 32 : 0)));
-      if (ok && wk && init == 0) {  // the initial eddy viscosity and the timing mode leave the wall model alone
+      if (ok && wk && init != 2) {  // the timing mode leaves the wall model alone
+        const T *Tm = d.buoy ? d.slot[0].buf[tb] : nullptr;
 #pragma unroll 1
         for (int qc = 0; qc < CPT; qc++) {
           const int iq = i + qc;
@@ -1044,8 +1049,9 @@ __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
 #pragma unroll 1
             for (int comp = 0; comp < 3; comp++) {
               long long p = wm_plane_index(d, comp, f, iq, j, k);
-              if (p >= 0) wm_point(d, comp, f, iq, j, k, p);
+              if (p >= 0) wm_point(d, comp, f, iq, j, k, p, Tm);
             }
+            if (d.tdir[f] && k == (f == SIDE_BO ? 1 : nz)) wm_pr_dirichlet(d, f, iq, j, k, Tm);
           }
         }
       }

@@ -330,7 +330,7 @@ struct SlabsT {
   }
   int stage(int st) {
     int r;
-    each([&](int, BatchT<T> &B) { B.launch_sgs(); });
+    each([&](int, BatchT<T> &B) { B.launch_sgs(st); });
     if ((r = exchange_halos({F_NU}, true, true))) return r;
     each([&](int, BatchT<T> &B) { B.launch_momentum(st); });
     if ((r = exchange_halos({F_W2}, true, false))) return r;

@@ -79,11 +79,12 @@ __global__ void __launch_bounds__(256) k_ib_gather(const Dom<T> *__restrict__ do
 // the face towards the solid, which the stencil added, is taken back and
 // the wall-model flux put in its place.  The tendency (Ustar) and U2
 // (+ beta dt of it, the RK combine of src/dynamics.f90:450-478) are updated
-// by atomics, as a free point can border two solid points.
+// by atomics, as a free point can border two solid points.  ustar_only:
+// the u* update alone (the wall model on the initial fields).
 template <typename T>
 __global__ void __launch_bounds__(128) k_ib_wm(const Dom<T> *__restrict__ doms, int di,
                                                const WMSolid *__restrict__ pts, double *__restrict__ ustar_state,
-                                               int n, double beta) {
+                                               int n, double beta, int ustar_only) {
   const Dom<T> &d = doms[di];
   const double beta_dt = beta * d.dt;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
@@ -116,6 +117,7 @@ __global__ void __launch_bounds__(128) k_ib_wm(const Dom<T> *__restrict__ doms, 
     if (tv != 0) us = wm_ustar(us, tv, dd, p.z0, d.nu_mol);
     if (us < 0) us = 0;
     ustar_state[q] = us;
+    if (ustar_only) continue;
     double fp = 0, fm = 0;
     if (tv > 1.4901161193847656e-08) {
       const double base = (t[comp] / tv) * (us * us);

@@ -216,6 +216,10 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
       // then + div * value; div as DivergenceWM with dzPr(k)
       if ((k == 1 && wm_lo) || (k == nz && wm_hi)) {
         a = a + (T)sl.wflux[k == 1 ? 0 : 1];
+        // a prescribed surface temperature: the flux of the point from the
+        // wall model of this stage (temperature slot only)
+        const double *tpr = s == 0 ? d.wm_pr_tf[k == 1 ? 0 : 1] : nullptr;
+        if (tpr) a = a + (T)(tpr[(i - 1) + (long long)nx * (j - 1)] * d.wm_af);
         const T dzk = (T)d.dzPr[k + 2];
         T div = (T)0;
         div = div + ue / rdx;
@@ -400,6 +404,8 @@ __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SP
         }
         if (wmk) {
           a = a + (T)sl.wflux[k == 1 ? 0 : 1];
+          const double *tpr = s == 0 ? d.wm_pr_tf[k == 1 ? 0 : 1] : nullptr;
+          if (tpr) a = a + (T)(tpr[(i + c - 1) + (long long)nx * (j - 1)] * d.wm_af);
           const T dzk = (T)d.dzPr[k + 2];
           const T ue = c ? u0.y : u0.x, uw = c ? u0.x : um.y;
           const T wtc = c ? wt.y : wt.x, wbc = c ? wb.y : wb.x;

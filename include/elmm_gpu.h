@@ -138,9 +138,12 @@ typedef struct elmm_config {
    * it enters the cells next to the wall through the wall-model points
    * (src/scalars.f90:323-327), and a flux into the flow over a rough wall
    * makes the wall model's u* follow Monin-Obukhov similarity
-   * (WM_MO_FluxStress, src/wallmodels.f90:1836-1854, 2255-2259); a
-   * Dirichlet value there (the Monin-Obukhov Dirichlet wall model) is
-   * refused.  Elsewhere the ghost rules of CommonBase carry the kind. */
+   * (WM_MO_FluxStress, src/wallmodels.f90:1836-1854, 2255-2259).  A
+   * Dirichlet value there is a surface temperature: the Monin-Obukhov wall
+   * model computes the points' u* and surface flux from the temperature
+   * difference each stage (WM_MO_Dirichlet / WM_MO_DirichletStress,
+   * src/wallmodels.f90:1664-1716, 1858-1938; rough walls, z0 > 0, only).
+   * Elsewhere the ghost rules of CommonBase carry the kind. */
   int32_t enable_buoyancy;      /* 0: no temperature field */
   int32_t TempBtype[6];         /* temperature BC per side (src/initial.f90:347-352) */
   double sideTemp[6];           /* BC values: value, gradient or flux of the kind */
@@ -349,7 +352,10 @@ int elmm_frame_wait(elmm_handle *h, double *U, double *V, double *W, double *Pr)
 
 /* PressureCorrection(U,V,W,Pr,Q,coef) on the resident state
  * (src/pressure.f90:169-266, Q = 0): the initial projection uses coef = 1
- * (src/initial.f90:4290). */
+ * (src/initial.f90:4290).  Then, as the end of InitialConditions
+ * (src/initial.f90:4291-4336): the initial eddy viscosity and scalar
+ * diffusivity, and the wall model once on the projected fields (the u* and
+ * surface fluxes its points carry into the first stage). */
 int elmm_project(elmm_handle *h, double coef, elmm_stats *stats);
 
 /* nsteps calls of TMarchRK3 (src/tsteps.f90:24-243) on the resident state. */

@@ -92,6 +92,17 @@ struct WMPointUVW {
   double ustar = 1;
   double wallu = 0, wallv = 0, wallw = 0;
   double temperature_flux = 0;
+  double temperature = 0;
+  bool prescribed_temperature = false;
+};
+
+// The WMPoint of a Pr cell next to a wall in z (src/wallmodels.f90:20-64,
+// 570-685), kept for the sides with a prescribed surface temperature: the
+// state of WM_MO_Dirichlet and the flux TemperatureExtra adds.
+struct WMPointPr {
+  int xi = 0, yj = 0, zk = 0;
+  double distz = 0, z0 = 0;
+  double ustar = 1, temperature_flux = 0, temperature = 0;
 };
 
 // ------------------------------------------------------------------- FFT
@@ -175,6 +186,9 @@ struct Domain {
   // their ComputeAreaFactor (wallmodels.f90:173-203, 590-596, 650-656)
   double wm_tflux[7] = {0, 0, 0, 0, 0, 0, 0};
   double area_factor_z = 0;
+  // Pr wall-model points of the bottom and top with a prescribed surface
+  // temperature (TempBtype BC_DIRICHLET at a wall-model wall)
+  std::vector<WMPointPr> wmpr[7];
   A3 T, Tadv, T2, TDiff;
   // passive scalars (ScalarRK3's loop over num_of_scalars, scalars.f90:217-223)
   int num_scalars;
@@ -297,6 +311,7 @@ static void add_wm_points(Domain &d) {
           p = WMPointUVW(); p.xi = i; p.yj = j; p.zk = 1;
           p.distz = d.zW(0) - z(1); p.z0 = d.z0s[Bo];
           p.temperature_flux = d.wm_tflux[Bo];
+          p.prescribed_temperature = !d.wmpr[Bo].empty(); p.temperature = d.sideTemp[Bo];
           d.wm[MINUSZ][comp].push_back(p);
         }
     if (d.Btype[To] == BC_NOSLIP)
@@ -305,6 +320,7 @@ static void add_wm_points(Domain &d) {
           p = WMPointUVW(); p.xi = i; p.yj = j; p.zk = nz;
           p.distz = d.zW(d.Wnz + 1) - z(nz); p.z0 = d.z0s[To];
           p.temperature_flux = d.wm_tflux[To];
+          p.prescribed_temperature = !d.wmpr[To].empty(); p.temperature = d.sideTemp[To];
           d.wm[PLUSZ][comp].push_back(p);
         }
   }
@@ -652,6 +668,92 @@ static void WM_MO_Flux_ustar(const Domain &d, double vel, double dist, double &u
   }
 }
 
+// PsiM_MO_mod / PsiH_MO_mod, wallmodels.f90:1572-1595
+static double PsiM_MO_mod(double zeta, double k_U) {
+  if (zeta < 0) {
+    const double x = std::pow(1 - 6.0 * zeta * k_U, 1 / 4.0);
+    const double h = (1 + x) / 2.0;
+    return std::log(((1 + x * x) / 2.0) * (h * h)) - 2.0 * std::atan(x) + std::acos(-1.0) / 2;
+  }
+  return -(3 * std::pow(zeta * k_U, 5.0 / 6.0));
+}
+
+static double PsiH_MO_mod(double zeta, double k_U) {
+  if (zeta < 0) {
+    const double x = std::pow(1 - 6.0 * zeta * k_U, 1 / 4.0);
+    return 2.0 * std::log((1 + x * x) / 2.0);
+  }
+  return -(2.5 * std::pow(zeta * k_U, 4.0 / 5.0));
+}
+
+// WM_MO_Dirichlet_ustar_tfl, wallmodels.f90:1664-1716 (its 1.1 is a
+// default-real literal); tempdif = theta(point) - theta(surface)
+static void WM_MO_Dirichlet_ustar_tfl(const Domain &d, double &ustar, double &tflux, double dist, double z0,
+                                      double z0H, double vel, double tempdif) {
+  const double eps = 1e-3, yplcrit = 11.225, k_U = 0.4, k_T = 0.47;
+  const double nu = d.molecular_viscosity;
+  WMRoughUstar(d, ustar, vel, dist, z0);
+  double dist_plus;
+  if (nu > 0) {
+    const double ustar_lam = std::sqrt(nu * vel / dist);
+    dist_plus = dist * ustar_lam / nu;
+  } else {
+    dist_plus = std::numeric_limits<double>::max();
+  }
+  if (dist <= z0 || dist_plus < (double)1.1f * yplcrit) {
+    tflux = -d.molecular_diffusivity * tempdif / dist;
+    return;
+  }
+  double zL = 0, zL0 = -10000.0;
+  int i = 0;
+  for (;;) {
+    i = i + 1;
+    zL = -dist * d.grav_acc * tflux / (k_U * d.temperature_ref * (ustar * ustar * ustar));
+    const double psi_m = PsiM_MO_mod(zL, k_U), psi_h = PsiH_MO_mod(zL, k_U);
+    ustar = vel * k_U / (std::log(dist / z0) - psi_m);
+    tflux = -tempdif * ustar * k_T / (std::log(dist / z0H) - psi_h);
+    if (i > 1 && std::fabs(zL - zL0) / std::max(std::fabs(zL), 1.e-4) < eps) break;
+    if (i >= 50 || zL > 10000) break;
+    zL0 = zL;
+  }
+  if (i >= 50 || zL > 10000) {
+    ustar = std::sqrt(nu * vel / dist);
+    tflux = -d.molecular_diffusivity * tempdif / dist;
+  }
+}
+
+// ComputeViscsWM, wallmodels.f90:2050-2152, for the Pr points with a
+// prescribed surface temperature (WM_MO_Dirichlet, :1858-1884): their u*
+// and surface temperature flux.  The viscosity it forms is overwritten by
+// SubgridModel in a stage (dynamics.f90:882-889) and is not kept.
+static void ComputeViscsWM(Domain &d) {
+  for (int side : {Bo, To})
+    for (WMPointPr &p : d.wmpr[side]) {
+      const int xi = p.xi, yj = p.yj, zk = p.zk;
+      const double dv[3] = {0, 0, p.distz};
+      const double uv[3] = {(d.U(xi, yj, zk) + d.U(xi - 1, yj, zk)) / 2.0,
+                            (d.V(xi, yj, zk) + d.V(xi, yj - 1, zk)) / 2.0,
+                            (d.W(xi, yj, zk) + d.W(xi, yj, zk - 1)) / 2.0};
+      const double tdif = d.T(xi, yj, zk) - p.temperature;
+      if (!(p.z0 > 0)) continue;
+      // WM_MO_Dirichlet: sqrt(sum(...**2)) and the tangential part
+      const double dist = std::sqrt((dv[0] * dv[0] + dv[1] * dv[1]) + dv[2] * dv[2]);
+      const double dot = (uv[0] * dv[0] + uv[1] * dv[1]) + uv[2] * dv[2];
+      double vect[3];
+      for (int m = 0; m < 3; m++) vect[m] = uv[m] - dot * dv[m] / (dist * dist);
+      const double vel = std::sqrt((vect[0] * vect[0] + vect[1] * vect[1]) + vect[2] * vect[2]);
+      WM_MO_Dirichlet_ustar_tfl(d, p.ustar, p.temperature_flux, dist, p.z0, p.z0, vel, tdif);
+      if (p.ustar < 0) p.ustar = 0;
+    }
+}
+
+// local_value, wallmodels.f90:2340-2353
+static double local_value(const A3 &C, int comp, int xi, int yj, int zk) {
+  if (comp == 1) return (C(xi + 1, yj, zk) + C(xi, yj, zk)) / 2;
+  if (comp == 2) return (C(xi, yj + 1, zk) + C(xi, yj, zk)) / 2;
+  return (C(xi, yj, zk + 1) + C(xi, yj, zk)) / 2;
+}
+
 // local_velocity, wallmodels.f90:2354-2396
 static void local_velocity(const Domain &d, int comp, int xi, int yj, int zk, double *vel) {
   const A3 &U = d.U, &V = d.V, &W = d.W;
@@ -694,7 +796,12 @@ static void ComputeUVWFluxesWM(Domain &d) {
         // flow, else WMRoughStress with a roughness length, WMFlatStress for a
         // smooth wall (wallmodels.f90:2255-2275; WM_MO_FluxStress, :1836-1854;
         // WMFlatStress, :1243-1265)
-        if (p.z0 > 0 && d.enable_buoyancy && p.temperature_flux > 0) {
+        if (p.z0 > 0 && d.enable_buoyancy && p.prescribed_temperature) {
+          // WM_MO_DirichletStress (:1922-1938): sqrt(sum(tan_vect**2))
+          const double vel2 = std::sqrt((t[0] * t[0] + t[1] * t[1]) + t[2] * t[2]);
+          const double temp = local_value(d.T, comp, p.xi, p.yj, p.zk);
+          WM_MO_Dirichlet_ustar_tfl(d, p.ustar, p.temperature_flux, dd, p.z0, p.z0, vel2, temp - p.temperature);
+        } else if (p.z0 > 0 && d.enable_buoyancy && p.temperature_flux > 0) {
           if (tv != 0) WM_MO_Flux_ustar(d, tv, dd, p.ustar, p.z0, p.temperature_flux);
           else p.ustar = 0;
         } else if (tv != 0) {
@@ -751,6 +858,7 @@ static double IBInterpolate(const elmm_ib_point &p, const A3 &F) {
 }
 
 static void SubgridStresses(Domain &d) {
+  if (d.wallmodeltype > 0) ComputeViscsWM(d);  // dynamics.f90:882-885
   SubgridModel(d);
   if (d.wallmodeltype > 0) ComputeUVWFluxesWM(d);
   BoundViscosity(d, d.Viscosity);
@@ -971,12 +1079,15 @@ static void ScalarStage(Domain &d, int stage, double dt, A3 &Arr, A3 &Arr2, A3 &
             Adv(v.i, v.j, v.k) = Adv(v.i, v.j, v.k) + d.puffs[q].dt_fraction * v.flux;
   for (int j = 1; j <= ny; j++)
     for (int i = 1; i <= nx; i++) {
+      const size_t q = (size_t)(j - 1) * nx + i - 1;
       if (wb) {
-        if (sc == 0) Adv(i, j, 1) = Adv(i, j, 1) + d.wm_tflux[Bo] * d.area_factor_z;
+        if (sc == 0 && !d.wmpr[Bo].empty()) Adv(i, j, 1) = Adv(i, j, 1) + d.wmpr[Bo][q].temperature_flux * d.area_factor_z;
+        else if (sc == 0) Adv(i, j, 1) = Adv(i, j, 1) + d.wm_tflux[Bo] * d.area_factor_z;
         Adv(i, j, 1) = Adv(i, j, 1) + divb[(size_t)(j - 1) * nx + i - 1] * Arr(i, j, 1);
       }
       if (wt) {
-        if (sc == 0) Adv(i, j, nz) = Adv(i, j, nz) + d.wm_tflux[To] * d.area_factor_z;
+        if (sc == 0 && !d.wmpr[To].empty()) Adv(i, j, nz) = Adv(i, j, nz) + d.wmpr[To][q].temperature_flux * d.area_factor_z;
+        else if (sc == 0) Adv(i, j, nz) = Adv(i, j, nz) + d.wm_tflux[To] * d.area_factor_z;
         Adv(i, j, nz) = Adv(i, j, nz) + divt[(size_t)(j - 1) * nx + i - 1] * Arr(i, j, nz);
       }
     }
@@ -1858,6 +1969,12 @@ static void InitialDiffusivity(Domain &d) {
     BoundViscosity(d, d.TDiff);
   }
   if (d.enable_buoyancy) BoundTemperature(d, d.T);
+  // the wall model once on the initial fields (initial.f90:4331-4336): the
+  // points' u* and surface fluxes, from which the first stage starts
+  if (d.wallmodeltype > 0) {
+    ComputeViscsWM(d);
+    ComputeUVWFluxesWM(d);
+  }
 }
 
 }  // namespace orc
@@ -1950,11 +2067,25 @@ void *orc_create(const elmm_config *c) {
     // a constant temperature flux at a wall becomes the flux of its
     // wall-model points, and the side's TempBtype becomes 0 (the mirror
     // ghosts of CommonBase's last branch)
-    for (int side : {Bo, To})
-      if (d->Btype[side] == BC_NOSLIP && d->TempBtype[side] == ELMM_BC_CONSTFLUX) {
+    for (int side : {Bo, To}) {
+      if (d->Btype[side] != BC_NOSLIP) continue;
+      if (d->TempBtype[side] == ELMM_BC_CONSTFLUX) {
         d->wm_tflux[side] = side == Bo ? d->sideTemp[side] : -d->sideTemp[side];
         d->TempBtype[side] = 0;
+      } else if (d->TempBtype[side] == ELMM_BC_DIRICHLET) {
+        const int k = side == Bo ? 1 : nz;
+        for (int j = 1; j <= ny; j++)
+          for (int i = 1; i <= nx; i++) {
+            WMPointPr p;
+            p.xi = i; p.yj = j; p.zk = k;
+            p.distz = side == Bo ? d->zW(0) - d->zPr(1) : d->zW(d->Wnz + 1) - d->zPr(nz);
+            p.z0 = d->z0s[side];
+            p.temperature = d->sideTemp[side];
+            d->wmpr[side].push_back(p);
+          }
+        d->TempBtype[side] = 0;
       }
+    }
     // ComputeAreaFactor of a point below or above its cell: out_norm = e_z
     const double dq = std::sqrt(d->dxmin * d->dymin), l = dq / 1.0;
     d->area_factor_z = dq * l / (d->dxmin * d->dymin * d->dzmin);

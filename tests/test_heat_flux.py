@@ -1,15 +1,21 @@
-"""A constant surface heat flux at a wall-model wall (TempBtype CONSTFLUX
-with a non-zero sideTemp at the bottom or top): the flux of the side's
-wall-model points enters the cells next to the wall
+"""Heat exchange at a wall-model wall.  A constant surface heat flux
+(TempBtype CONSTFLUX with a non-zero sideTemp at the bottom or top): the
+flux of the side's wall-model points enters the cells next to the wall
 (src/scalars.f90:323-327), and a flux into the flow over a rough wall makes
 the wall model's u* follow Monin-Obukhov similarity (WM_MO_FluxStress,
-src/wallmodels.f90:1606-1660, 1836-1854).
+src/wallmodels.f90:1606-1660, 1836-1854).  A prescribed surface
+temperature (TempBtype DIRICHLET): the wall model computes the points'
+u* and surface flux from the temperature difference each stage
+(WM_MO_Dirichlet / WM_MO_DirichletStress, src/wallmodels.f90:1664-1716,
+1858-1938), starting from the state the initial projection leaves (the
+wall model once on the initial fields, src/initial.f90:4331-4336).
 
 * FP64 GPU against the oracle after 1 and 5 steps: U, V, W within 1e-12,
   P within 1e-11, theta - T_ref within 1e-11 (relative to the largest
   value), for a heated rough bottom (the Monin-Obukhov u*), a cooled bottom
-  with a flux through a top wall (neutral u*, the flux terms alone) and a
-  heated smooth bottom (z0 = 0, WMFlatStress);
+  with a flux through a top wall (neutral u*, the flux terms alone), a
+  heated smooth bottom (z0 = 0, WMFlatStress), a surface warmer than the
+  air and, between two walls, a cool bottom and a warm top;
 * mixed against FP64 after one step from the same projected state:
   velocity and theta - T_ref within 1e-5;
 * the heat content grows by (q_bottom - q_top) Lx Ly per unit time on both
@@ -23,8 +29,8 @@ import pytest
 
 from conftest import rel
 from gpu_elmm_b200 import lib as L
-from gpu_elmm_b200.config import (BC_FREESLIP, BC_NOSLIP, BC_PERIODIC, FIELD_TEMPERATURE, grid_of,
-                                  make_config)
+from gpu_elmm_b200.config import (BC_CONSTFLUX, BC_DIRICHLET, BC_FREESLIP, BC_NOSLIP, BC_PERIODIC,
+                                  FIELD_TEMPERATURE, grid_of, make_config)
 from gpu_elmm_b200.workloads import interior, interiors, log_profile_state, temperature_state
 from oracle import Oracle
 
@@ -36,6 +42,8 @@ CASES = {
     "heated-rough": dict(heat_flux=(0.3, 0.0)),
     "cooled-top-flux": dict(heat_flux=(-0.1, 0.05), btype=TWO_WALLS),
     "heated-smooth": dict(heat_flux=(0.3, 0.0), z0=0.0),
+    "warm-surface": dict(temperature_bc=((BC_DIRICHLET, 296.0), (BC_CONSTFLUX, 0.0))),
+    "surfaces-two-walls": dict(temperature_bc=((BC_DIRICHLET, 294.0), (BC_DIRICHLET, 295.5)), btype=TWO_WALLS),
 }
 
 
@@ -111,6 +119,10 @@ def test_heat_content_follows_the_surface_fluxes(precision):
 def test_non_finite_flux_is_refused():
     with pytest.raises(L.ElmmError) as e:
         L.Domain(make_config(*N, buoyancy=True, heat_flux=(float("nan"), 0.0)))
+    assert e.value.code == 1
+    # the Dirichlet wall model is the rough-wall branch
+    with pytest.raises(L.ElmmError) as e:
+        L.Domain(make_config(*N, buoyancy=True, z0=0.0, temperature_bc=((BC_DIRICHLET, 296.0), (BC_CONSTFLUX, 0.0))))
     assert e.value.code == 1
     L.Domain(make_config(*N, buoyancy=True, heat_flux=(0.1, 0.0))).close()
     # a flux through the free-slip top has no wall-model points: the ghost rule carries it

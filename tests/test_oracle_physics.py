@@ -430,3 +430,50 @@ def test_ghost_rule_fluxes_change_the_content(field):
     h1 = interior(o.get_field(fid), -2, n).sum()
     expect = (qb - qt) * n[0] * n[1] * dt * steps
     assert abs((h1 - h0) - expect) < 1e-9 * abs(expect) + 1e-12 * abs(h0), (h1 - h0, expect)
+
+
+@pytest.mark.parametrize("dtheta", [2.0, -2.0], ids=["warm-surface", "cool-surface"])
+def test_surface_temperature_flux_follows_monin_obukhov(dtheta):
+    """A prescribed surface temperature at a rough wall-model bottom
+    (WM_MO_Dirichlet, src/wallmodels.f90:1664-1716, 1858-1884): for a
+    uniform flow U over air at a uniform theta every other temperature flux
+    vanishes, so the first level's temperature tendency is the wall-model
+    flux q over dz (TemperatureExtra's temperature_flux * area_factor).
+    q and u* solve the similarity laws of Zilitinkevich and Esau,
+    u* = 0.4 U / (ln(z/z0) - PsiM(z/L)), q = -(theta - theta_s) 0.47 u* /
+    (ln(z/z0) - PsiH(z/L)), z/L = -z g q / (0.4 T_ref u*^3), to the
+    iteration's tolerance on z/L (1e-3); a warm surface heats the air and a
+    cool one cools it."""
+    import math
+    from gpu_elmm_b200.config import BC_CONSTFLUX, BC_DIRICHLET, FIELD_TEMPERATURE, FIELD_TEMPERATURE_ADV
+    from gpu_elmm_b200.workloads import temperature_state
+    dz, vel, z0, tref, grav, ta = 1.0, 5.0, 0.01, 295.0, 9.81, 295.0
+    cfg = make_config(16, 12, 8, dz=dz, z0=z0, buoyancy=True,
+                      temperature_bc=((BC_DIRICHLET, ta + dtheta), (BC_CONSTFLUX, 0.0)))
+    g = grid_of(cfg)
+    U, V, W, Pr = (np.zeros(s) for s in (g.shape_u(), g.shape_v(), g.shape_w(), g.shape_p()))
+    U[...] = vel
+    o = Oracle(cfg)
+    o.set_state(U, V, W, Pr)
+    o.set_field(FIELD_TEMPERATURE, temperature_state(g, gradient=0.0, amp=0.0, t0=ta))
+    o.run_stage(1, 2)
+    tend = o.get_field(FIELD_TEMPERATURE_ADV)[2 + 1, 2 + 1:2 + 1 + g.Prny, 2 + 1:2 + 1 + g.Prnx]
+    assert np.ptp(tend) == 0
+    q = tend.max() * dz
+    assert (q > 0) == (dtheta > 0)
+
+    def psi(zeta):
+        if zeta < 0:
+            x = (1 - 6 * zeta * 0.4) ** 0.25
+            return (math.log((1 + x * x) / 2 * ((1 + x) / 2) ** 2) - 2 * math.atan(x) + math.pi / 2,
+                    2 * math.log((1 + x * x) / 2))
+        return -3 * (zeta * 0.4) ** (5 / 6), -2.5 * (zeta * 0.4) ** 0.8
+
+    z = dz / 2
+    qq, us = 0.0, 0.4 * vel / math.log(z / z0)
+    for _ in range(500):                      # the fixed point, by damped substitution
+        zl = -z * grav * qq / (0.4 * tref * us ** 3)
+        pm, ph = psi(zl)
+        us = 0.5 * us + 0.5 * 0.4 * vel / (math.log(z / z0) - pm)
+        qq = 0.5 * qq + 0.5 * (dtheta * us * 0.47 / (math.log(z / z0) - ph))
+    assert abs(q - qq) / abs(qq) < 1e-2, (q, qq)

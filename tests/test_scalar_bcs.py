@@ -14,8 +14,9 @@ before each stage.
   unit time, on both paths;
 * a batch of two domains with different scalar boundaries equals each
   domain run alone, bit for bit;
-* a Dirichlet temperature at a wall-model wall (the Monin-Obukhov Dirichlet
-  wall model), other kinds and non-finite values are refused.
+* a Dirichlet temperature at a smooth wall-model wall (the Monin-Obukhov
+  Dirichlet wall model is the rough-wall branch), other kinds and
+  non-finite values are refused.
 """
 import numpy as np
 import pytest
@@ -182,8 +183,8 @@ def test_batch_with_scalar_boundaries_equals_the_runs_alone(precision):
 
 def test_unsupported_scalar_boundaries_are_refused():
     walls = (3, 3, 3, 3, BC_NOSLIP, BC_NOSLIP)
-    bad = [dict(buoyancy=True, temperature_bc=((BC_DIRICHLET, 300.0), (BC_CONSTFLUX, 0.0))),   # wall-model wall
-           dict(buoyancy=True, btype=walls, temperature_bc=((BC_CONSTFLUX, 0.0), (BC_DIRICHLET, 300.0))),
+    bad = [dict(buoyancy=True, z0=0.0, temperature_bc=((BC_DIRICHLET, 300.0), (BC_CONSTFLUX, 0.0))),  # smooth wall
+           dict(buoyancy=True, btype=walls, z0=0.0, temperature_bc=((BC_CONSTFLUX, 0.0), (BC_DIRICHLET, 300.0))),
            dict(buoyancy=True, temperature_bc=((BC_NOSLIP, 0.0), (BC_CONSTFLUX, 0.0))),
            dict(num_scalars=1, scalar_bc=((BC_CONSTFLUX, float("inf")), (BC_CONSTFLUX, 0.0)))]
     for kw in bad:
