@@ -286,7 +286,7 @@ struct LaunchSet {
 };
 
 enum { LK_CELLS = 0, LK_BOX, LK_ROWS, LK_YCOLS, LK_TRI, LK_MOM, LK_SHELL, LK_XREG, LK_YREG, LK_TRIT, LK_TCOL, LK_DCOL,
-       LK_AVG, LK_COMMIT, LK_TPAIR, LK_PROJ, LK_PROJ2, LK_DCOL2, LK_MOMT, LK_SGST, LK_N };
+       LK_AVG, LK_COMMIT, LK_TPAIR, LK_PROJ, LK_PROJ2, LK_DCOL2, LK_MOMT, LK_SGST, LK_WM, LK_N };
 
 // the z-chunk lengths (planes of a tile's column) the autotuner tries for
 // the momentum and SGS kernels
@@ -822,6 +822,7 @@ struct BatchT {
       case LK_MOM: return ((h.nx + MX - 1) / MX) * ((h.ny + MY - 1) / MY) * ((h.nz + MKC - 1) / MKC);
       case LK_MOMT: return ((h.nx + MX - 1) / MX) * ((h.ny + MY - 1) / MY) * ((h.nz + tune_mom_kc - 1) / tune_mom_kc);
       case LK_SGST: return ((h.nx + MX - 1) / MX) * ((h.ny + MY - 1) / MY) * ((h.nz + tune_sgs_kc - 1) / tune_sgs_kc);
+      case LK_WM: return (int)((wm_points_of(h) + kWmThreads - 1) / kWmThreads);
       case LK_PROJ: return fp32_pairs(h) && !slab_mode ? 0 : tiles(LK_MOM, h);
       case LK_PROJ2: return fp32_pairs(h) && !slab_mode ? tiles(LK_MOM, h) : 0;
       case LK_SHELL: return (int)((shell_cells(h.nx, h.ny, h.nz) + kShellThreads * shell_per - 1) / (kShellThreads * shell_per));
@@ -1168,17 +1169,20 @@ struct BatchT {
   }
   static int chunk_index(int kc) { return kc == 8 ? 0 : kc == 16 ? 1 : 2; }
   // k_sgs with the tuned z chunk; init: 0 a stage, 1 the initial viscosity
-  // and diffusivity, 2 the autotuner's timing mode (k_sgs); stage: the RK3
-  // stage whose start temperature the wall model reads (1 outside a step)
-  void sgs_kernel(int init, int stage = 1) {
+  // and diffusivity, 2 the autotuner's timing mode (k_sgs)
+  void sgs_kernel(int init) {
     const int q = chunk_index(tune_sgs_kc), g = std::max(1, std::min(ls[LK_SGST].total, cap_sgs[q]));
-    const int tb = (stage - 1) % 3;
-    if (tune_sgs_kc == 8)
-      k_sgs<T, 8><<<g, SgsShape<T>::threads, smem_sgs, stream>>>(ddom, ls[LK_SGST].l(), init, tb);
-    else if (tune_sgs_kc == 16)
-      k_sgs<T, 16><<<g, SgsShape<T>::threads, smem_sgs, stream>>>(ddom, ls[LK_SGST].l(), init, tb);
-    else
-      k_sgs<T, 32><<<g, SgsShape<T>::threads, smem_sgs, stream>>>(ddom, ls[LK_SGST].l(), init, tb);
+    if (tune_sgs_kc == 8) k_sgs<T, 8><<<g, SgsShape<T>::threads, smem_sgs, stream>>>(ddom, ls[LK_SGST].l(), init);
+    else if (tune_sgs_kc == 16) k_sgs<T, 16><<<g, SgsShape<T>::threads, smem_sgs, stream>>>(ddom, ls[LK_SGST].l(), init);
+    else k_sgs<T, 32><<<g, SgsShape<T>::threads, smem_sgs, stream>>>(ddom, ls[LK_SGST].l(), init);
+  }
+  // the wall model of a stage (k_wm_points) from the state at its start, on
+  // stream s; stage 1 outside a step (the initial fields).  Returns 1 if it
+  // launched.
+  int wm_kernel(int stage, cudaStream_t s) {
+    if (ls[LK_WM].total == 0) return 0;
+    k_wm_points<T><<<std::min(ls[LK_WM].total, 148 * 16), kWmThreads, 0, s>>>(ddom, ls[LK_WM].l(), (stage - 1) % 3);
+    return 1;
   }
   void momentum_kernel(const StageCoef &sc) {
     const int q = chunk_index(tune_mom_kc), g = std::max(1, std::min(ls[LK_MOMT].total, cap_mom[q]));
@@ -1188,7 +1192,17 @@ struct BatchT {
   }
   int launch_sgs(int stage) {
     nlaunch++;
-    sgs_kernel(0, stage);
+    // the wall model on a branch beside k_sgs (a graph branch when
+    // captured): neither reads what the other writes
+    const bool wm = ls[LK_WM].total > 0 && branch[1];
+    if (wm) {
+      CU(cudaEventRecord(ev_fork, stream));
+      CU(cudaStreamWaitEvent(branch[1], ev_fork, 0));
+      nlaunch += wm_kernel(stage, branch[1]);
+      CU(cudaEventRecord(ev_join[1], branch[1]));
+    }
+    sgs_kernel(0);
+    if (wm) CU(cudaStreamWaitEvent(stream, ev_join[1], 0));
     launch_ghosts({F_NU}, 0);
     return ELMM_OK;
   }
@@ -1240,7 +1254,11 @@ struct BatchT {
     }
     if (ls[LK_TCOL].total > 0) {
       nlaunch++;
-      k_scalar<T><<<gsz(11, ls[LK_TCOL].total), TX * TY, 0, stream>>>(ddom, ls[LK_TCOL].l(), kRho[stage - 1],
+      if (scalar_bcs())
+        k_scalar<T, true><<<gsz(11, ls[LK_TCOL].total), TX * TY, 0, stream>>>(ddom, ls[LK_TCOL].l(), kRho[stage - 1],
+                                                                             kBeta[stage - 1], stage);
+      else
+        k_scalar<T><<<gsz(11, ls[LK_TCOL].total), TX * TY, 0, stream>>>(ddom, ls[LK_TCOL].l(), kRho[stage - 1],
                                                                        kBeta[stage - 1], stage);
     }
     if constexpr (std::is_same<T, float>::value) {
@@ -1317,14 +1335,29 @@ struct BatchT {
       }
     });
   }
+  // some slot of the batch has a stored z ghost plane, a surface flux or a
+  // surface temperature: the scalar kernels' instantiation with those terms
+  bool scalar_bcs() const {
+    for (int d = 0; d < nd; d++) {
+      const Dom<T> &h = hdom[d];
+      if (h.tdir[ELMM_BO] || h.tdir[ELMM_TO]) return true;
+      for (int s = 0; s < h.nslot; s++)
+        if (h.slot[s].zg[0] || h.slot[s].zg[1] || h.slot[s].wflux[0] != 0 || h.slot[s].wflux[1] != 0) return true;
+    }
+    return false;
+  }
   void launch_scalar_pair(int stage) {
     if constexpr (std::is_same<T, float>::value) {
-      if (tune_rows == 8)
-        k_scalar_pair<8><<<gsz(12, ls[LK_TPAIR].total), SPX * 8, 0, stream>>>(ddom, ls[LK_TPAIR].l(), kRho[stage - 1],
-                                                                             kBeta[stage - 1], stage);
-      else
-        k_scalar_pair<4><<<gsz(14, ls[LK_TPAIR].total), SPX * 4, 0, stream>>>(ddom, ls[LK_TPAIR].l(), kRho[stage - 1],
-                                                                             kBeta[stage - 1], stage);
+      const Launch l = ls[LK_TPAIR].l();
+      const double rho = kRho[stage - 1], beta = kBeta[stage - 1];
+      const bool bc = scalar_bcs();
+      if (tune_rows == 8) {
+        if (bc) k_scalar_pair<8, true><<<gsz(12, ls[LK_TPAIR].total), SPX * 8, 0, stream>>>(ddom, l, rho, beta, stage);
+        else k_scalar_pair<8><<<gsz(12, ls[LK_TPAIR].total), SPX * 8, 0, stream>>>(ddom, l, rho, beta, stage);
+      } else {
+        if (bc) k_scalar_pair<4, true><<<gsz(14, ls[LK_TPAIR].total), SPX * 4, 0, stream>>>(ddom, l, rho, beta, stage);
+        else k_scalar_pair<4><<<gsz(14, ls[LK_TPAIR].total), SPX * 4, 0, stream>>>(ddom, l, rho, beta, stage);
+      }
     }
   }
   void launch_tri(int gate) {
@@ -2004,6 +2037,7 @@ struct BatchT {
     // and the wall model once on the initial fields (the u* and fluxes its
     // points carry into the first stage; the solid-face points' u* alone)
     sgs_kernel(1);
+    wm_kernel(1, stream);
     for (int d = 0; d < nd && d < (int)sol.size(); d++)
       if (sol[d].on && sol[d].nwm > 0)
         k_ib_wm<T><<<std::min((sol[d].nwm + 127) / 128, 148 * 8), 128, 0, stream>>>(ddom, d, sol[d].wm,
@@ -2035,7 +2069,10 @@ struct BatchT {
         cudaEventRecord(ev[2 * slot.size() + 1], stream);
         slot.push_back(k);
       };
-      timed(0, [&] { sgs_kernel(0, stage); });
+      timed(0, [&] {
+        sgs_kernel(0);
+        wm_kernel(stage, stream);
+      });
       timed(kGhost, [&] { launch_ghosts({F_NU}, 0); });
       timed(1, [&] {
         momentum_kernel(sc);

@@ -309,18 +309,78 @@ __device__ void wm_point(const Dom<T> &d, int comp, int f, int i, int j, int k, 
   d.wm_fluxm[face][pidx] = (T)fm;
 }
 
-// index of cell (i,j,k) in the face plane of side f for component comp, or -1
+// SubgridStresses' wall model (src/dynamics.f90:879-888): ComputeViscsWM
+// for the Pr points with a prescribed surface temperature, and
+// ComputeUVWFluxesWM for every velocity point on a wall-model face, from the
+// state at the start of the stage (tb: its temperature buffer).  One thread
+// a point; a domain's points in the order: the Pr points of the bottom and
+// top (i + nx j), then per component and side its face plane in index
+// order (x sides: j + ny k, y sides: i + nx k, z sides: i + nx j).  The
+// parts touch disjoint state.  Launched after k_sgs (whose viscosity they do
+// not read) and, with the initial fields, at the end of the initial
+// projection.
+constexpr int kWmThreads = 128;
 template <typename T>
-__device__ long long wm_plane_index(const Dom<T> &d, int comp, int f, int i, int j, int k) {
+__host__ __device__ inline void wm_face_plane(const Dom<T> &d, int comp, int f, int &n0, int &n1) {
   const int *e = d.ext[comp];
-  if (i < 1 || i > e[0] || j < 1 || j > e[1] || k < 1 || k > e[2]) return -1;
-  switch (f) {
-    case SIDE_WE: return i == 1 ? (long long)(j - 1) + (long long)e[1] * (k - 1) : -1;
-    case SIDE_EA: return i == e[0] ? (long long)(j - 1) + (long long)e[1] * (k - 1) : -1;
-    case SIDE_SO: return j == 1 ? (long long)(i - 1) + (long long)e[0] * (k - 1) : -1;
-    case SIDE_NO: return j == e[1] ? (long long)(i - 1) + (long long)e[0] * (k - 1) : -1;
-    case SIDE_BO: return k == 1 ? (long long)(i - 1) + (long long)e[0] * (j - 1) : -1;
-    default: return k == e[2] ? (long long)(i - 1) + (long long)e[0] * (j - 1) : -1;
+  const int axis = f >> 1;
+  n0 = axis == 0 ? e[1] : e[0];
+  n1 = axis == 2 ? e[1] : e[2];
+}
+template <typename T>
+__host__ __device__ inline long long wm_points_of(const Dom<T> &d) {
+  long long n = 0;
+  for (int f = SIDE_BO; f <= SIDE_TO; f++)
+    if (d.tdir[f]) n += (long long)d.nx * d.ny;
+  for (int comp = 0; comp < 3; comp++)
+    for (int f = 0; f < 6; f++)
+      if (d.wall[f]) {
+        int n0, n1;
+        wm_face_plane(d, comp, f, n0, n1);
+        n += (long long)n0 * n1;
+      }
+  return n;
+}
+template <typename T>
+__global__ void __launch_bounds__(kWmThreads) k_wm_points(const Dom<T> *__restrict__ doms, Launch L, int tb) {
+  for (int t = blockIdx.x; t < L.total; t += gridDim.x) {
+    const int di = find_dom(L.starts, L.nd, t);
+    const Dom<T> &d = doms[di];
+    long long p = (long long)(t - __ldg(L.starts + di)) * kWmThreads + threadIdx.x;
+    const T *Tm = d.buoy ? d.slot[0].buf[tb] : nullptr;
+    bool done = false;
+#pragma unroll 1
+    for (int f = SIDE_BO; f <= SIDE_TO && !done; f++) {
+      if (!d.tdir[f]) continue;
+      const long long np = (long long)d.nx * d.ny;
+      if (p < np) {
+        wm_pr_dirichlet(d, f, (int)(p % d.nx) + 1, (int)(p / d.nx) + 1, f == SIDE_BO ? 1 : d.nz, Tm);
+        done = true;
+      } else {
+        p -= np;
+      }
+    }
+#pragma unroll 1
+    for (int comp = 0; comp < 3 && !done; comp++)
+#pragma unroll 1
+      for (int f = 0; f < 6 && !done; f++) {
+        if (!d.wall[f]) continue;
+        int n0, n1;
+        wm_face_plane(d, comp, f, n0, n1);
+        const long long np = (long long)n0 * n1;
+        if (p >= np) {
+          p -= np;
+          continue;
+        }
+        const int *e = d.ext[comp];
+        const int axis = f >> 1, hi = f & 1;
+        const int a = (int)(p % n0) + 1, b = (int)(p / n0) + 1;
+        const int i = axis == 0 ? (hi ? e[0] : 1) : a;
+        const int j = axis == 0 ? a : axis == 1 ? (hi ? e[1] : 1) : b;
+        const int k = axis == 2 ? (hi ? e[2] : 1) : b;
+        wm_point(d, comp, f, i, j, k, p, Tm);
+        done = true;
+      }
   }
 }
 

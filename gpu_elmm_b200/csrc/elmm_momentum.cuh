@@ -869,12 +869,6 @@ __device__ __forceinline__ F2 nusmag2(const SgsK<float> &q, const RT &R) {
   return Sbar * bc2(q.wc2);
 }
 
-template <typename T>
-__device__ void wm_point(const Dom<T> &d, int comp, int f, int i, int j, int k, long long pidx, const T *Tm);
-template <typename T>
-__device__ void wm_pr_dirichlet(const Dom<T> &d, int f, int i, int j, int k, const T *Tm);
-template <typename T>
-__device__ long long wm_plane_index(const Dom<T> &d, int comp, int f, int i, int j, int k);
 
 // ComputeTDiff (src/scalar_diffusion.f90:983-1009): the temperature
 // diffusivity from the viscosity, constant Pr_sgs = 0.6
@@ -894,15 +888,13 @@ struct SgsShape<float> {
   static constexpr int cpt = 2, threads = MX * MY / 2, min_blocks = 7;
 };
 
-// init: 0 a stage (viscosity, diffusivity, wall-model points), 1 the initial
-// viscosity and diffusivity after the projection, with the wall model once
-// on the initial fields (src/initial.f90:4331-4336), 2 the autotuner's
-// timing launches (a stage's arithmetic without the wall-model points,
-// whose u* and fluxes carry the start of their iterations from stage to
-// stage).  tb: the temperature buffer of the stage (its start value).
+// init: 0 a stage (viscosity and diffusivity), 1 the initial viscosity and
+// diffusivity after the projection, 2 the autotuner's timing launches (a
+// stage's arithmetic; its outputs the real stage overwrites).  The
+// wall-model points are k_wm_points'.
 template <typename T, int KC = MKC>
 __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
-    k_sgs(const Dom<T> *__restrict__ doms, Launch L, int init, int tb) {
+    k_sgs(const Dom<T> *__restrict__ doms, Launch L, int init) {
   // planes of U, V, W (tile plus one-cell halo) arrive by tensor-map TMA in
   // a ring of kRingSlots slots, as in k_momentum
   typedef SlotLayout<T, 3, 0> Lay;
@@ -958,12 +950,6 @@ __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
           issue_plane<T, 3, 0>(ring + (kk % kRingSlots) * Lay::SIZE, &bars[kk % kRingSlots], maps, wide, none, false,
                                d.aln, i0, j0, kk);
     }
-    // block-uniform: the wall sides whose wall-model points this tile can
-    // hold (a point sits next to its side: i in {1, nx-1, nx} and so on)
-    int wmask = 0;
-    for (int f = 0; f < 6; f++) wmask |= d.wall[f] ? (1 << f) : 0;
-    const int wtile = wmask & ((i0 == 1 ? 1 : 0) | (i0 + MX - 1 >= nx - 1 ? 2 : 0) | (j0 == 1 ? 4 : 0) |
-                               (j0 + MY - 1 >= ny - 1 ? 8 : 0));
     const T num = (T)d.nu_mol;
     const bool sgs = d.sgs != 0, addmol = d.nu_mol > 0;
     // the scalar diffusivity too: every stage with buoyancy (ComputeTDiff,
@@ -1034,25 +1020,6 @@ __global__ void __launch_bounds__(SgsShape<T>::threads, SgsShape<T>::min_blocks)
           if (i + qc == 1) nu[c + qc + nx] = v;  // periodic x ghosts (the ghost pass covers y and z)
           if (i + qc == nx) nu[c + qc - nx] = v;
           if (buoy) d.TDiff[c + qc] = init == 1 ? (v - num) / (T)0.6 + kap : tdiff_of(v, num, kap);
-        }
-      }
-      const int wk = wtile | (wmask & ((k == 1 ? 16 : 0) | (k >= nz - 1 ? 32 : 0)));
-      if (ok && wk && init != 2) {  // the timing mode leaves the wall model alone
-        const T *Tm = d.buoy ? d.slot[0].buf[tb] : nullptr;
-#pragma unroll 1
-        for (int qc = 0; qc < CPT; qc++) {
-          const int iq = i + qc;
-          if (!(iq <= nx && j <= ny)) continue;
-#pragma unroll 1
-          for (int f = 0; f < 6; f++) {
-            if (!((wk >> f) & 1)) continue;
-#pragma unroll 1
-            for (int comp = 0; comp < 3; comp++) {
-              long long p = wm_plane_index(d, comp, f, iq, j, k);
-              if (p >= 0) wm_point(d, comp, f, iq, j, k, p, Tm);
-            }
-            if (d.tdir[f] && k == (f == SIDE_BO ? 1 : nz)) wm_pr_dirichlet(d, f, iq, j, k, Tm);
-          }
         }
       }
       __syncthreads();  // plane k-1 is no longer read

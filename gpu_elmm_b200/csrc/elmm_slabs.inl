@@ -420,6 +420,7 @@ struct SlabsT {
     each([&](int, BatchT<T> &B) {
       B.launch_divmax();
       B.sgs_kernel(1);
+      B.wm_kernel(1, B.stream);
       B.launch_ghosts({F_NU}, 0);
     });
     if ((r = exchange_halos({F_NU}, true, true))) return r;

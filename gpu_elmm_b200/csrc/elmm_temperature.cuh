@@ -108,7 +108,9 @@ __global__ void k_scalar_zghost(const Dom<T> *__restrict__ doms, int nd, int sta
 #endif
 constexpr int TMKC = ELMM_SCALAR_CHUNK;
 
-template <typename T>
+// BC: some slot has a stored z ghost plane, a surface flux or a surface
+// temperature (the launch picks the plain instantiation otherwise)
+template <typename T, bool BC = false>
 __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
     k_scalar(const Dom<T> *__restrict__ doms, Launch L, double rho, double beta, int stage) {
   const int stage1 = stage == 1;
@@ -141,7 +143,7 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
     auto zoff = [&](int kk) { return (long long)(scal_fold(kk, nz, pz) - kk) * plane; };  // fold of plane kk
     // the scalar's planes: a stored ghost plane (k_scalar_zghost) is read as it is
     const int zg0 = sl.zg[0], zg1 = sl.zg[1];
-    auto szoff = [&](int kk) { return (kk == 0 && zg0) || (kk == nz + 1 && zg1) ? 0LL : zoff(kk); };
+    auto szoff = [&](int kk) { return BC && ((kk == 0 && zg0) || (kk == nz + 1 && zg1)) ? 0LL : zoff(kk); };
     // volume sources of this slot in this column, in configuration order
     unsigned srcm = 0;
     for (int q = 0; q < d.nsrc; q++)
@@ -215,11 +217,13 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
       // wall-model point next to a wall-model side: + the surface flux term,
       // then + div * value; div as DivergenceWM with dzPr(k)
       if ((k == 1 && wm_lo) || (k == nz && wm_hi)) {
-        a = a + (T)sl.wflux[k == 1 ? 0 : 1];
-        // a prescribed surface temperature: the flux of the point from the
-        // wall model of this stage (temperature slot only)
-        const double *tpr = s == 0 ? d.wm_pr_tf[k == 1 ? 0 : 1] : nullptr;
-        if (tpr) a = a + (T)(tpr[(i - 1) + (long long)nx * (j - 1)] * d.wm_af);
+        if constexpr (BC) {
+          a = a + (T)sl.wflux[k == 1 ? 0 : 1];
+          // a prescribed surface temperature: the flux of the point from the
+          // wall model of this stage (temperature slot only)
+          const double *tpr = s == 0 ? d.wm_pr_tf[k == 1 ? 0 : 1] : nullptr;
+          if (tpr) a = a + (T)(tpr[(i - 1) + (long long)nx * (j - 1)] * d.wm_af);
+        }
         const T dzk = (T)d.dzPr[k + 2];
         T div = (T)0;
         div = div + ue / rdx;
@@ -274,7 +278,7 @@ struct PairPlane {
 
 // SPY: the rows of a tile, a tuning choice (8 or 4; the arithmetic of a
 // cell does not depend on it)
-template <int SPY>
+template <int SPY, bool BC = false>
 __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SPY)
     k_scalar_pair(const Dom<float> *__restrict__ doms, Launch L, double rho, double beta, int stage) {
   typedef float T;
@@ -304,7 +308,7 @@ __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SP
     for (int q = 0; q < 5; q++) oy[q] = (scal_fold(j - 2 + q, ny, py) - j) * (int)pitch;
     auto zoff = [&](int kk) { return (long long)(scal_fold(kk, nz, pz) - kk) * plane; };
     const int zg0 = sl.zg[0], zg1 = sl.zg[1];
-    auto szoff = [&](int kk) { return (kk == 0 && zg0) || (kk == nz + 1 && zg1) ? 0LL : zoff(kk); };
+    auto szoff = [&](int kk) { return BC && ((kk == 0 && zg0) || (kk == nz + 1 && zg1)) ? 0LL : zoff(kk); };
     unsigned srcm = 0;  // volume sources of this slot in this pair's columns
     for (int q = 0; q < d.nsrc; q++)
       if (d.src_slot[q] == s && (d.src_i[q] == i || d.src_i[q] == i + 1) && d.src_j[q] == j) srcm |= 1u << q;
@@ -403,9 +407,11 @@ __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SP
             if (((srcm >> q) & 1u) && d.src_i[q] == i + c && d.src_k[q] == k) a = a + (T)d.src_q[q];
         }
         if (wmk) {
-          a = a + (T)sl.wflux[k == 1 ? 0 : 1];
-          const double *tpr = s == 0 ? d.wm_pr_tf[k == 1 ? 0 : 1] : nullptr;
-          if (tpr) a = a + (T)(tpr[(i + c - 1) + (long long)nx * (j - 1)] * d.wm_af);
+          if constexpr (BC) {
+            a = a + (T)sl.wflux[k == 1 ? 0 : 1];
+            const double *tpr = s == 0 ? d.wm_pr_tf[k == 1 ? 0 : 1] : nullptr;
+            if (tpr) a = a + (T)(tpr[(i + c - 1) + (long long)nx * (j - 1)] * d.wm_af);
+          }
           const T dzk = (T)d.dzPr[k + 2];
           const T ue = c ? u0.y : u0.x, uw = c ? u0.x : um.y;
           const T wtc = c ? wt.y : wt.x, wbc = c ? wb.y : wb.x;
