@@ -145,6 +145,8 @@ class ElmmSolids(C.Structure):
         ("n_scalfl", C.c_int64), ("scalfl", C.POINTER(ElmmIBPoint)),
         ("n_wm", C.c_int64), ("wm", C.POINTER(ElmmWMPoint)),
         ("n_bottom_skip", C.c_int64 * 3), ("bottom_skip_ij", C.POINTER(C.c_int32) * 3),
+        ("n_solid_pr", C.c_int64), ("solid_pr_ijk", C.POINTER(C.c_int32)),
+        ("n_wm_pr", C.c_int64), ("wm_pr_ijk", C.POINTER(C.c_int32)),
     ]
 
 

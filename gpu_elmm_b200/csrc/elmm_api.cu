@@ -393,6 +393,7 @@ struct BatchT {
     double *wm_ustar = nullptr;
     int nwm = 0;
     unsigned char *bskip[3] = {nullptr, nullptr, nullptr};
+    unsigned char *pmask = nullptr;  // the scalars' cell mask (Dom::pmask)
     bool on = false, primed = false;
   };
   std::vector<SolidSet> sol;
@@ -1340,7 +1341,7 @@ struct BatchT {
   bool scalar_bcs() const {
     for (int d = 0; d < nd; d++) {
       const Dom<T> &h = hdom[d];
-      if (h.tdir[ELMM_BO] || h.tdir[ELMM_TO]) return true;
+      if (h.tdir[ELMM_BO] || h.tdir[ELMM_TO] || h.pmask) return true;
       for (int s = 0; s < h.nslot; s++)
         if (h.slot[s].zg[0] || h.slot[s].zg[1] || h.slot[s].wflux[0] != 0 || h.slot[s].wflux[1] != 0) return true;
     }
@@ -1710,10 +1711,11 @@ struct BatchT {
     if (d >= (int)sol.size()) return;
     SolidSet &x = sol[d];
     for (void *p : {(void *)x.vel, (void *)x.visc, (void *)x.wm, (void *)x.wm_ustar, (void *)x.bskip[0],
-                    (void *)x.bskip[1], (void *)x.bskip[2], (void *)x.null})
+                    (void *)x.bskip[1], (void *)x.bskip[2], (void *)x.null, (void *)x.pmask})
       if (p) dfree(p);
     x = SolidSet();
     for (int c = 0; c < 3; c++) hdom[d].bskip[c] = nullptr;
+    hdom[d].pmask = nullptr;
   }
   // elmm_set_solids: checks the lists, turns (i, j, k) into box indices with
   // the ghost folds applied, uploads them and marks the step graph stale.
@@ -1745,8 +1747,10 @@ struct BatchT {
   int install_solids(int d, const elmm_solids *s) {
     Dom<T> &h = hdom[d];
     const elmm_config &c = cfg[d];
-    if (c.enable_buoyancy || c.num_scalars > 0)
-      return fail(ELMM_ERR_INVALID_ARG, "solid bodies with a temperature or passive scalars are not supported");
+    if (c.enable_buoyancy)
+      return fail(ELMM_ERR_INVALID_ARG,
+                  "solid bodies with a temperature are not supported (the fill of the solid cells after each "
+                  "temperature stage is not built)");
     if (!h.wall[SIDE_BO] || h.bt[SIDE_BO] != BC_NOSLIP)
       return fail(ELMM_ERR_INVALID_ARG, "solid bodies need the wall model on a no-slip bottom");
     const bool per[3] = {h.bt[SIDE_WE] == BC_PERIODIC, h.bt[SIDE_SO] == BC_PERIODIC, h.bt[SIDE_BO] == BC_PERIODIC};
@@ -1885,6 +1889,34 @@ struct BatchT {
         if ((r = up((void **)&x.bskip[comp], m.data(), m.size()))) return r;
         h.bskip[comp] = x.bskip[comp];
       }
+    }
+    if (c.num_scalars > 0) {
+      // the passive scalars' cell mask: bit 0 the solid Pr cells with their
+      // periodic x and y images in the ghost columns, bit 1 the Pr
+      // wall-model points of the scalar equations
+      if (s->n_solid_pr < 0 || (s->n_solid_pr > 0 && !s->solid_pr_ijk) || s->n_wm_pr < 0 ||
+          (s->n_wm_pr > 0 && !s->wm_pr_ijk))
+        return fail(ELMM_ERR_INVALID_ARG, "solid Pr cells or Pr wall-model points");
+      std::vector<unsigned char> m((size_t)h.plane * (h.nz + 2), 0);
+      auto in = [&](const int32_t *t) {
+        return t[0] >= 1 && t[0] <= h.nx && t[1] >= 1 && t[1] <= h.ny && t[2] >= 1 && t[2] <= h.nz;
+      };
+      for (int64_t q = 0; q < s->n_solid_pr; q++) {
+        const int32_t *t = s->solid_pr_ijk + 3 * q;
+        if (!in(t)) return fail(ELMM_ERR_INVALID_ARG, "solid Pr cell out of range");
+        for (int oi : {-h.nx, 0, h.nx})
+          for (int oj : {-h.ny, 0, h.ny}) {
+            const int i = t[0] + oi, j = t[1] + oj;
+            if (i >= 0 && i <= h.nx + 1 && j >= 0 && j <= h.ny + 1) m[bidx(h, i, j, t[2])] |= 1;
+          }
+      }
+      for (int64_t q = 0; q < s->n_wm_pr; q++) {
+        const int32_t *t = s->wm_pr_ijk + 3 * q;
+        if (!in(t)) return fail(ELMM_ERR_INVALID_ARG, "Pr wall-model point out of range");
+        m[bidx(h, t[0], t[1], t[2])] |= 2;
+      }
+      if ((r = up((void **)&x.pmask, m.data(), m.size()))) return r;
+      h.pmask = x.pmask;
     }
     x.on = true;
     x.primed = false;

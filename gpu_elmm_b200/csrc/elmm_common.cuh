@@ -135,6 +135,10 @@ struct Dom {
   // per component: 1 marks a bottom-plane point without a wall-model point
   // (next to or under a solid body), or null for none
   const unsigned char *bskip[3];
+  // solid bodies with passive scalars: per box cell, bit 0 a solid Pr cell
+  // (Prtype > 0; x and y ghost images too), bit 1 a Pr wall-model point of
+  // the scalar equations; null without bodies or scalars
+  const unsigned char *pmask;
   double z0[6];
   // pressure reference: stored P = true Pr + prm; top-layer partial sums
   double *prm;           // 1 value

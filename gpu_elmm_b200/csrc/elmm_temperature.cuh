@@ -202,6 +202,10 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
         a = a - Az * fzt;
         a = a + Az * fzb;
       }
+      // a solid cell keeps no advection tendency (src/scalars.f90:259-268)
+      if constexpr (BC) {
+        if (d.pmask && (d.pmask[cc] & 1)) a = (T)0;
+      }
       // diffusion, in the order of ScalarDiffusion_nobranch
       a = a + (kxp + k0v) * (sxp1 - s0) * Dx;
       a = a - (k0v + kxm) * (s0 - sxm1) * Dx;
@@ -214,9 +218,14 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
         for (int q = 0; q < d.nsrc; q++)
           if (((srcm >> q) & 1u) && d.src_k[q] == k) a = a + (T)d.src_q[q];
       }
-      // wall-model point next to a wall-model side: + the surface flux term,
-      // then + div * value; div as DivergenceWM with dzPr(k)
-      if ((k == 1 && wm_lo) || (k == nz && wm_hi)) {
+      // wall-model point next to a wall-model side (with solid bodies, a
+      // point of the mask): + the surface flux term, then + div * value; div
+      // as DivergenceWM with dzPr(k), without the faces towards solid cells
+      bool wmc = (k == 1 && wm_lo) || (k == nz && wm_hi);
+      if constexpr (BC) {
+        if (d.pmask) wmc = (d.pmask[cc] & 2) != 0;
+      }
+      if (wmc) {
         if constexpr (BC) {
           a = a + (T)sl.wflux[k == 1 ? 0 : 1];
           // a prescribed surface temperature: the flux of the point from the
@@ -226,12 +235,22 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
         }
         const T dzk = (T)d.dzPr[k + 2];
         T div = (T)0;
-        div = div + ue / rdx;
-        div = div - uw / rdx;
-        div = div + vn / rdy;
-        div = div - vs / rdy;
-        div = div + wt / dzk;
-        div = div - wb / dzk;
+        if (BC && d.pmask) {  // the offsets are zero with solid bodies: stored values are full ones
+          const unsigned char *pm = d.pmask;
+          if (!(pm[cc + 1] & 1)) div = div + ue / rdx;
+          if (!(pm[cc - 1] & 1)) div = div - uw / rdx;
+          if (!(pm[cc + pitch] & 1)) div = div + vn / rdy;
+          if (!(pm[cc - pitch] & 1)) div = div - vs / rdy;
+          if (!(pm[cc + plane] & 1)) div = div + wt / dzk;
+          if (!(pm[cc - plane] & 1)) div = div - wb / dzk;
+        } else {
+          div = div + ue / rdx;
+          div = div - uw / rdx;
+          div = div + vn / rdy;
+          div = div - vs / rdy;
+          div = div + wt / dzk;
+          div = div - wb / dzk;
+        }
         a = a + div * s0;
       }
       // RK combine of the stage: S2 = Sadv_old * (rho dt) + Sadv * (beta dt)
@@ -396,6 +415,9 @@ __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SP
         const T kym_c = c ? kym.y : kym.x, kyp_c = c ? kyp.y : kyp.x;
         const T zp = c ? sz[3].y : sz[3].x, zm = c ? sz[1].y : sz[1].x;
         const T kzp = c ? kz[2].y : kz[2].x, kzm = c ? kz[0].y : kz[0].x;
+        if constexpr (BC) {  // a solid cell keeps no advection tendency
+          if (d.pmask && (d.pmask[cc + c] & 1)) a = (T)0;
+        }
         a = a + (kxp + k0v) * (sxp1 - sc) * Dx;
         a = a - (k0v + kxm) * (sc - sxm1) * Dx;
         a = a + (kyp_c + k0v) * (b1 - sc) * Dy;
@@ -406,7 +428,11 @@ __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SP
           for (int q = 0; q < d.nsrc; q++)
             if (((srcm >> q) & 1u) && d.src_i[q] == i + c && d.src_k[q] == k) a = a + (T)d.src_q[q];
         }
-        if (wmk) {
+        bool wmc = wmk;
+        if constexpr (BC) {
+          if (d.pmask) wmc = (d.pmask[cc + c] & 2) != 0;
+        }
+        if (wmc) {
           if constexpr (BC) {
             a = a + (T)sl.wflux[k == 1 ? 0 : 1];
             const double *tpr = s == 0 ? d.wm_pr_tf[k == 1 ? 0 : 1] : nullptr;
@@ -416,12 +442,22 @@ __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SP
           const T ue = c ? u0.y : u0.x, uw = c ? u0.x : um.y;
           const T wtc = c ? wt.y : wt.x, wbc = c ? wb.y : wb.x;
           T div = (T)0;
-          div = div + ue / rdx;
-          div = div - uw / rdx;
-          div = div + (c ? vn.y : vn.x) / rdy;  // stored values: the level offset cancels
-          div = div - (c ? vs.y : vs.x) / rdy;
-          div = div + wtc / dzk;
-          div = div - wbc / dzk;
+          if (BC && d.pmask) {  // the offsets are zero with solid bodies
+            const unsigned char *pm = d.pmask + cc + c;
+            if (!(pm[1] & 1)) div = div + ue / rdx;
+            if (!(pm[-1] & 1)) div = div - uw / rdx;
+            if (!(pm[pitch] & 1)) div = div + (c ? vn.y : vn.x) / rdy;
+            if (!(pm[-pitch] & 1)) div = div - (c ? vs.y : vs.x) / rdy;
+            if (!(pm[plane] & 1)) div = div + wtc / dzk;
+            if (!(pm[-plane] & 1)) div = div - wbc / dzk;
+          } else {
+            div = div + ue / rdx;
+            div = div - uw / rdx;
+            div = div + (c ? vn.y : vn.x) / rdy;  // stored values: the level offset cancels
+            div = div - (c ? vs.y : vs.x) / rdy;
+            div = div + wtc / dzk;
+            div = div - wbc / dzk;
+          }
           a = a + div * sc;
         }
         T t2 = stage1 ? (T)0 : (c ? told.y : told.x) * rdt;

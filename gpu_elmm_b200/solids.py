@@ -44,7 +44,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .config import (BC_PERIODIC, IB_MAX_INTERP, ElmmConfig, ElmmIBPoint, ElmmSolids, ElmmWMPoint, grid_of)
+from .config import (BC_NOSLIP, BC_PERIODIC, IB_MAX_INTERP, ElmmConfig, ElmmIBPoint, ElmmSolids, ElmmWMPoint,
+                     grid_of)
 
 MINUSX, PLUSX, MINUSY, PLUSY, MINUSZ, PLUSZ = 1, 2, 3, 4, 5, 6
 _DIRS = {MINUSX: (-1, 0, 0), PLUSX: (1, 0, 0), MINUSY: (0, -1, 0), PLUSY: (0, 1, 0),
@@ -516,6 +517,33 @@ class Geometry:
                     out.append((comp, dr, i, j, k, tuple(dv), b.z0r if b.z0r > 0 else 0.0))
         return out
 
+    def solid_pr(self):
+        """Pr cells with Prtype > 0 inside the domain, (i, j, k) 1..n."""
+        g = self.g
+        t = self.types[0][3:g.Prnz + 3, 3:g.Prny + 3, 3:g.Prnx + 3]
+        k, j, i = np.nonzero(t > 0)
+        return np.stack([i + 1, j + 1, k + 1], axis=1).astype(np.int32) if len(i) else np.zeros((0, 3), np.int32)
+
+    def wm_pr(self):
+        """The Pr wall-model points of the scalar equations, each cell once:
+        GetSolidBodiesWM's free cells (Prtype <= 0) with a solid 6-neighbour
+        and GetOutsideBoundariesWM_Pr's cells of a no-slip z wall with
+        Prtype == 0 (the domain's x and y are periodic)."""
+        g, cfg = self.g, self.cfg
+        t = self.types[0]
+        nx, ny, nz = g.Prnx, g.Prny, g.Prnz
+        inner = t[3:nz + 3, 3:ny + 3, 3:nx + 3]
+        near = np.zeros(inner.shape, dtype=bool)
+        for dk, dj, di in ((0, 0, 1), (0, 0, -1), (0, 1, 0), (0, -1, 0), (1, 0, 0), (-1, 0, 0)):
+            near |= t[3 + dk:nz + 3 + dk, 3 + dj:ny + 3 + dj, 3 + di:nx + 3 + di] > 0
+        pts = (inner <= 0) & near
+        if cfg.Btype[4] == BC_NOSLIP:
+            pts[0] |= inner[0] == 0
+        if cfg.Btype[5] == BC_NOSLIP:
+            pts[nz - 1] |= inner[nz - 1] == 0
+        k, j, i = np.nonzero(pts)
+        return np.stack([i + 1, j + 1, k + 1], axis=1).astype(np.int32) if len(i) else np.zeros((0, 3), np.int32)
+
     def bottom_skip(self, q):
         (nx, ny, nz), _, _, _ = self.grids[q]
         t = self.types[q]
@@ -543,6 +571,8 @@ class Solids:
     scalfl: list = field(default_factory=list)
     wm: list = field(default_factory=list)
     bottom_skip: list = field(default_factory=lambda: [np.zeros((0, 2), np.int32)] * 3)
+    solid_pr: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.int32))
+    wm_pr: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.int32))
 
     def struct(self) -> ElmmSolids:
         """The elmm_solids view; the arrays stay referenced by this object."""
@@ -573,11 +603,17 @@ class Solids:
         self._keep.append(w)
         s.n_wm = len(self.wm)
         s.wm = C.cast(w, C.POINTER(ElmmWMPoint))
+        for name, arr in (("solid_pr", self.solid_pr), ("wm_pr", self.wm_pr)):
+            a = np.ascontiguousarray(arr, dtype=np.int32).reshape(-1)
+            self._keep.append(a)
+            setattr(s, "n_" + name, len(a) // 3)
+            setattr(s, name + "_ijk", a.ctypes.data_as(C.POINTER(C.c_int32)))
         return s
 
     def counts(self) -> dict:
         return {"ib": [len(x) for x in self.ib], "null": [len(x) for x in self.null],
-                "scalfl": len(self.scalfl), "wm": len(self.wm), "bottom_skip": [len(x) for x in self.bottom_skip]}
+                "scalfl": len(self.scalfl), "wm": len(self.wm), "bottom_skip": [len(x) for x in self.bottom_skip],
+                "solid_pr": len(self.solid_pr), "wm_pr": len(self.wm_pr)}
 
 
 def build_solids(cfg: ElmmConfig, boxes) -> Solids:
@@ -596,5 +632,7 @@ def build_solids(cfg: ElmmConfig, boxes) -> Solids:
     s.scalfl = [((i, j, k),) + g.scalfl_point(i, j, k) for (i, j, k) in g._boundary_points(0)]
     s.wm = g.wm_points()
     s.bottom_skip = [g.bottom_skip(q) for q in (1, 2, 3)]
+    s.solid_pr = g.solid_pr()
+    s.wm_pr = g.wm_pr()
     s.geometry = g
     return s

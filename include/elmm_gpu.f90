@@ -71,6 +71,10 @@ module elmm_gpu
     type(c_ptr)        :: wm                 ! solid-face WMPointUVW
     integer(c_int64_t) :: n_bottom_skip(3)
     type(c_ptr)        :: bottom_skip_ij(3)
+    integer(c_int64_t) :: n_solid_pr
+    type(c_ptr)        :: solid_pr_ijk       ! Prtype > 0 cells (passive scalars)
+    integer(c_int64_t) :: n_wm_pr
+    type(c_ptr)        :: wm_pr_ijk          ! Pr wall-model points of the scalars
   end type
 
   type, bind(C) :: elmm_config

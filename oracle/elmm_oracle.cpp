@@ -189,6 +189,11 @@ struct Domain {
   // Pr wall-model points of the bottom and top with a prescribed surface
   // temperature (TempBtype BC_DIRICHLET at a wall-model wall)
   std::vector<WMPointPr> wmpr[7];
+  // solid bodies with passive scalars: Prtype > 0 as 1 (periodic images in
+  // the x and y ghosts) and the Pr wall-model points of the scalars
+  bool scal_solids = false;
+  A3 Prsolid;
+  std::vector<std::array<int, 3>> wmprs;
   A3 T, Tadv, T2, TDiff;
   // passive scalars (ScalarRK3's loop over num_of_scalars, scalars.f90:217-223)
   int num_scalars;
@@ -1066,6 +1071,11 @@ static void ScalarStage(Domain &d, int stage, double dt, A3 &Arr, A3 &Arr2, A3 &
     Arr2.fill(0);
   }
   KappaScalar(d, Adv, Arr);
+  if (d.scal_solids)  // Array_adv = 0 at the solid cells (scalars.f90:259-268)
+    for (int k = 1; k <= nz; k++)
+      for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++)
+          if (d.Prsolid(i, j, k) != 0) Adv(i, j, k) = 0;
   ScalarDiffusion(d, Adv, Arr);
   if (sc > 0)
     for (const auto &v : d.flvolumes)
@@ -1077,7 +1087,21 @@ static void ScalarStage(Domain &d, int stage, double dt, A3 &Arr, A3 &Arr2, A3 &
         for (const auto &v : d.puffvols)
           if (v.puff == (int)q && v.sc == sc)
             Adv(v.i, v.j, v.k) = Adv(v.i, v.j, v.k) + d.puffs[q].dt_fraction * v.flux;
-  for (int j = 1; j <= ny; j++)
+  // with solid bodies: DivergenceWM over the points of the list, without the
+  // faces towards solid cells (wallmodels.f90:1150-1166)
+  if (d.scal_solids)
+    for (const auto &p : d.wmprs) {
+      const int i = p[0], j = p[1], k = p[2];
+      double div = 0;
+      if (d.Prsolid(i + 1, j, k) == 0) div = div + d.U(i, j, k) / d.dxmin;
+      if (d.Prsolid(i - 1, j, k) == 0) div = div - d.U(i - 1, j, k) / d.dxmin;
+      if (d.Prsolid(i, j + 1, k) == 0) div = div + d.V(i, j, k) / d.dymin;
+      if (d.Prsolid(i, j - 1, k) == 0) div = div - d.V(i, j - 1, k) / d.dymin;
+      if (d.Prsolid(i, j, k + 1) == 0) div = div + d.W(i, j, k) / d.dzPr(k);
+      if (d.Prsolid(i, j, k - 1) == 0) div = div - d.W(i, j, k - 1) / d.dzPr(k);
+      Adv(i, j, k) = Adv(i, j, k) + div * Arr(i, j, k);
+    }
+  for (int j = 1; j <= ny && !d.scal_solids; j++)
     for (int i = 1; i <= nx; i++) {
       const size_t q = (size_t)(j - 1) * nx + i - 1;
       if (wb) {
@@ -2124,7 +2148,26 @@ int orc_set_solids(void *h, const elmm_solids *s) {
   d.scalfl.clear();
   d.solids = false;
   d.called = 0;
+  d.scal_solids = false;
+  d.wmprs.clear();
   if (!s) return 0;
+  if (d.num_scalars > 0) {
+    const int nx = d.Prnx, ny = d.Prny, nz = d.Prnz;
+    d.Prsolid.init(-1, nx + 2, -1, ny + 2, -1, nz + 2);
+    for (int64_t q = 0; q < s->n_solid_pr; q++) {
+      const int32_t *t = s->solid_pr_ijk + 3 * q;
+      for (int oi : {-nx, 0, nx})
+        for (int oj : {-ny, 0, ny}) {
+          const int i = t[0] + oi, j = t[1] + oj;
+          if (i >= -1 && i <= nx + 2 && j >= -1 && j <= ny + 2) d.Prsolid(i, j, t[2]) = 1;
+        }
+    }
+    for (int64_t q = 0; q < s->n_wm_pr; q++) {
+      const int32_t *t = s->wm_pr_ijk + 3 * q;
+      d.wmprs.push_back({t[0], t[1], t[2]});
+    }
+    d.scal_solids = true;
+  }
   for (int c = 1; c <= 3; c++) {
     if (s->n_ib[c - 1] > 0) d.ibp[c].assign(s->ib[c - 1], s->ib[c - 1] + s->n_ib[c - 1]);
     for (int64_t q = 0; q < s->n_null[c - 1]; q++) {

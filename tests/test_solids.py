@@ -7,7 +7,9 @@ reference's construction gives them, and the oracle keeps the solid interior
 at rest.  GPU: the library, given the same lists, follows the oracle
 (IBMomentum, IBMassSources, NullInterior, the ScalFl viscosity and the
 wall-model fluxes at the solid faces) on the FP64 path to 1e-11, and the
-mixed path follows the FP64 one."""
+mixed path follows the FP64 one; so does a passive scalar among the bodies
+(no advection tendency in the solid cells, the wall-model div * S of the
+cells next to them)."""
 import numpy as np
 import pytest
 
@@ -311,3 +313,150 @@ def test_fp64_spheres_match_the_oracle():
     print("spheres: FP64 vs oracle", e, "mixed vs FP64", em, "max div", out[0][1], out[1][1])
     assert max(e[:3]) < 1e-11 and e[3] < 1e-10 and out[0][1] < 1e-10, e
     assert max(em) < 1e-5 and out[1][1] < 1e-5, em
+
+
+def _scalar_boxes_cfg(precision=0):
+    return make_config(40, 36, 20, pr_gradient_x=-2e-3, num_scalars=1, precision=precision,
+                       point_sources=[(1, (20.5, 16.5, 3.5), 2.0)])
+
+
+def _scalar_boxes():
+    from gpu_elmm_b200.solids import Box
+    return [Box(6.0, 14.0, 5.0, 13.0, -3.0, 6.0), Box(22.0, 30.0, 20.0, 30.0, -3.0, 9.0),
+            Box(31.0, 34.0, 6.0, 12.0, -3.0, 4.0)]
+
+
+def test_scalar_lists_of_the_bodies():
+    """The Pr lists for the passive scalars: the solid cells are the Prtype >
+    0 cells; the wall-model points are the free cells with a solid
+    6-neighbour (GetSolidBodiesWM) and the bottom cells with Prtype == 0
+    (GetOutsideBoundariesWM_Pr), each once, none of them solid."""
+    cfg = _scalar_boxes_cfg()
+    s = build_solids(cfg, _scalar_boxes())
+    g = s.geometry
+    nx, ny, nz = cfg.Prnx, cfg.Prny, cfg.Prnz
+    t = g.types[0]
+    T = lambda i, j, k: int(t[k + 2, j + 2, i + 2])
+    solid = {tuple(p) for p in s.solid_pr.tolist()}
+    assert len(solid) == len(s.solid_pr) == int((t[3:nz + 3, 3:ny + 3, 3:nx + 3] > 0).sum())
+    wm = [tuple(p) for p in s.wm_pr.tolist()]
+    assert len(wm) == len(set(wm)) and not (set(wm) & solid)
+    for (i, j, k) in wm:
+        near = any(T(i + a, j + b, k + c) > 0 for a, b, c in
+                   ((1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)))
+        assert T(i, j, k) <= 0 and (near or (k == 1 and T(i, j, k) == 0))
+    bottom = sum(1 for j in range(1, ny + 1) for i in range(1, nx + 1) if T(i, j, 1) == 0)
+    assert sum(1 for p in wm if p[2] == 1) >= bottom > 0
+
+
+def _scalar_pair(precision=0):
+    """The oracle and a library domain of the given precision, both from the
+    same seeded state and puff, projected, then given the bodies."""
+    from gpu_elmm_b200 import lib as L
+    from gpu_elmm_b200.config import FIELD_SCALAR
+    from gpu_elmm_b200.workloads import puff_state
+    cfg = _scalar_boxes_cfg(precision)
+    s = build_solids(cfg, _scalar_boxes())
+    g = grid_of(cfg)
+    st = log_profile_state(g, seed=9)
+    S0 = puff_state(g, (18, 17, 4), sigma=3.0)
+    o = Oracle(_scalar_boxes_cfg(0))
+    o.set_state(*st)
+    o.set_field(FIELD_SCALAR, S0)
+    o.project(1.0)
+    o.set_solids(s)
+    d = L.Domain(cfg)
+    d.upload(*st)
+    d.upload_scalar(1, S0)
+    d.project(1.0)  # the scalar diffusivity of the initial eddy viscosity, kept without buoyancy
+    d.set_solids(s)
+    return g, o, d
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nsteps", [1, 5])
+def test_fp64_passive_scalar_among_boxes(nsteps):
+    """A passive scalar (a puff and a continuous point source) among boxes on
+    a uniform grid: no advection tendency in the solid cells
+    (src/scalars.f90:259-268), and the wall-model points of the scalar, the
+    free cells next to a body and the bottom cells under none, add div * S
+    without the faces towards solid cells (DivergenceWM,
+    src/wallmodels.f90:1150-1166).  FP64 against the oracle: U, V, W within
+    1e-11, P within 1e-10, the scalar within 1e-11."""
+    from gpu_elmm_b200.config import FIELD_SCALAR
+    from gpu_elmm_b200.workloads import interior
+    g, o, d = _scalar_pair()
+    o.step(nsteps)
+    d.step(nsteps)
+    e = [rel(a, b) for a, b in zip(interiors(g, *d.download()), interiors(g, *o.state()))]
+    n = (g.Prnx, g.Prny, g.Prnz)
+    es = rel(interior(d.scalar(1), -2, n), interior(o.get_field(FIELD_SCALAR), -2, n))
+    print("passive scalar among boxes, FP64 vs oracle after", nsteps, "steps:", e, es)
+    assert max(e[:3]) < 1e-11 and e[3] < 1e-10 and es < 1e-11, (e, es)
+    d.close()
+
+
+@pytest.mark.gpu
+def test_mixed_passive_scalar_among_boxes():
+    from gpu_elmm_b200.workloads import interior
+    g, _, d64 = _scalar_pair(0)
+    _, _, dm = _scalar_pair(1)
+    d64.step(3)
+    dm.step(3)
+    n = (g.Prnx, g.Prny, g.Prnz)
+    e = [rel(a, b) for a, b in zip(interiors(g, *dm.download())[:3], interiors(g, *d64.download())[:3])]
+    es = rel(interior(dm.scalar(1), -2, n), interior(d64.scalar(1), -2, n))
+    print("passive scalar among boxes, mixed vs FP64 after 3 steps:", e, es)
+    assert max(e) < 1e-5 and es < 1e-5, (e, es)
+    d64.close()
+    dm.close()
+
+
+@pytest.mark.gpu
+def test_temperature_with_bodies_is_refused():
+    from gpu_elmm_b200 import lib as L
+    cfg = make_config(40, 36, 20, buoyancy=True)
+    d = L.Domain(cfg)
+    with pytest.raises(L.ElmmError) as e:
+        d.set_solids(build_solids(cfg, _scalar_boxes()))
+    assert e.value.code == 6
+    d.close()
+
+
+@pytest.mark.gpu
+def test_batch_with_a_scalar_among_boxes_equals_the_run_alone():
+    """The scalar's cell mask is per domain: a batch of the scalar-and-boxes
+    domain and a channel without bodies gives each its state alone, bit for
+    bit (mixed path)."""
+    from gpu_elmm_b200 import lib as L
+    from gpu_elmm_b200.workloads import puff_state
+    cfg_s = _scalar_boxes_cfg(1)
+    sol = build_solids(cfg_s, _scalar_boxes())
+    cfg_p = make_config(32, 24, 16, num_scalars=1, precision=1)
+    gs, gp = grid_of(cfg_s), grid_of(cfg_p)
+    st_s, st_p = log_profile_state(gs, seed=9), log_profile_state(gp, seed=6)
+    S_s, S_p = puff_state(gs, (18, 17, 4), sigma=3.0), puff_state(gp, (9, 7, 4))
+    b = L.Batch([cfg_s, cfg_p])
+    b.upload(0, *st_s)
+    b.upload(1, *st_p)
+    b.upload_scalar(0, 1, S_s)
+    b.upload_scalar(1, 1, S_p)
+    b.project(1.0)
+    b.set_solids(0, sol)
+    b.step(3)
+    _, _, a = _scalar_pair(1)
+    a.step(3)
+    p = L.Domain(cfg_p)
+    p.upload(*st_p)
+    p.upload_scalar(1, S_p)
+    p.project(1.0)
+    p.step(3)
+    for x, y in zip(a.download(), b.download(0)):
+        assert np.array_equal(x, y)
+    assert np.array_equal(a.scalar(1), b.scalar(0, 1))
+    for x, y in zip(p.download(), b.download(1)):
+        assert np.array_equal(x, y)
+    assert np.array_equal(p.scalar(1), b.scalar(1, 1))
+    a.close()
+    p.close()
+    b.close()
