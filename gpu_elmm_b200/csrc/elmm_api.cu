@@ -8,6 +8,8 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <array>
+#include <functional>
 #include <limits>
 #include <cmath>
 #include <cstdio>
@@ -394,6 +396,9 @@ struct BatchT {
     int nwm = 0;
     unsigned char *bskip[3] = {nullptr, nullptr, nullptr};
     unsigned char *pmask = nullptr;  // the scalars' cell mask (Dom::pmask)
+    // the temperature's fill of the solid cells (k_theta_fill)
+    FillCell *fill = nullptr;
+    int nfill = 0;
     bool on = false, primed = false;
   };
   std::vector<SolidSet> sol;
@@ -1268,6 +1273,13 @@ struct BatchT {
         launch_scalar_pair(stage);
       }
     }
+    // the temperature's fill of the solid cells (src/scalars.f90:129-198)
+    for (int d = 0; d < nd && d < (int)sol.size(); d++)
+      if (sol[d].on && sol[d].nfill > 0) {
+        nlaunch++;
+        k_theta_fill<T><<<std::min((sol[d].nfill + 255) / 256, 148 * 4), 256, 0, stream>>>(ddom, d, sol[d].fill,
+                                                                                          sol[d].nfill, stage % 3);
+      }
     bool puffs = false;
     for (int d = 0; d < nd; d++) puffs |= hdom[d].npv > 0;
     if (puffs) {
@@ -1711,7 +1723,7 @@ struct BatchT {
     if (d >= (int)sol.size()) return;
     SolidSet &x = sol[d];
     for (void *p : {(void *)x.vel, (void *)x.visc, (void *)x.wm, (void *)x.wm_ustar, (void *)x.bskip[0],
-                    (void *)x.bskip[1], (void *)x.bskip[2], (void *)x.null, (void *)x.pmask})
+                    (void *)x.bskip[1], (void *)x.bskip[2], (void *)x.null, (void *)x.pmask, (void *)x.fill})
       if (p) dfree(p);
     x = SolidSet();
     for (int c = 0; c < 3; c++) hdom[d].bskip[c] = nullptr;
@@ -1744,13 +1756,65 @@ struct BatchT {
     }
     return ELMM_OK;
   }
+  // The cells of the temperature's fill of the solid cells (k_theta_fill)
+  // from the solid Pr cells of s: the interior solid cells with a fluid
+  // 6-neighbour in range -1..n+2, each with its fluid neighbours' cells, a
+  // ghost cell through the rules of BoundTemperature for adiabatic sides
+  // (x, y periodic; z mirrored at a wall-model wall, the first level
+  // otherwise).
+  int build_fill(int d, const elmm_solids *s) {
+    Dom<T> &h = hdom[d];
+    SolidSet &x = sol[d];
+    const int nx = h.nx, ny = h.ny, nz = h.nz, ex = nx + 4, ey = ny + 4, ez = nz + 4;
+    auto at = [&](int i, int j, int k) { return (size_t)(i + 1) + (size_t)ex * ((size_t)(j + 1) + (size_t)ey * (k + 1)); };
+    std::vector<char> solid((size_t)ex * ey * ez, 0);
+    for (int64_t q = 0; q < s->n_solid_pr; q++) {
+      const int32_t *t = s->solid_pr_ijk + 3 * q;
+      for (int oi : {-nx, 0, nx})
+        for (int oj : {-ny, 0, ny}) {
+          const int i = t[0] + oi, j = t[1] + oj;
+          if (i >= -1 && i <= nx + 2 && j >= -1 && j <= ny + 2) solid[at(i, j, t[2])] = 1;
+        }
+    }
+    const bool mlo = h.wall[SIDE_BO] != 0, mhi = h.wall[SIDE_TO] != 0;
+    auto fold = [&](int i, int j, int k, int o[3]) {
+      o[0] = i < 1 ? i + nx : i > nx ? i - nx : i;
+      o[1] = j < 1 ? j + ny : j > ny ? j - ny : j;
+      o[2] = k < 1 ? (mlo ? 1 - k : 1) : k > nz ? (mhi ? 2 * nz + 1 - k : nz) : k;
+    };
+    static const int nb[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+    std::vector<FillCell> fc;
+    for (int k = 1; k <= nz; k++)
+      for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++) {
+          if (!solid[at(i, j, k)]) continue;
+          FillCell c{};
+          c.box = bidx(h, i, j, k);
+          for (auto &o : nb) {
+            const int a = i + o[0], b = j + o[1], e = k + o[2];
+            if (solid[at(a, b, e)]) continue;
+            int g[3];
+            fold(a, b, e, g);
+            if (solid[at(g[0], g[1], g[2])])
+              return fail(ELMM_ERR_INVALID_ARG, "a fluid ghost cell next to a body copies a solid cell");
+            c.ref[c.n++] = bidx(h, g[0], g[1], g[2]);
+          }
+          if (c.n > 0) fc.push_back(c);
+        }
+    if (fc.empty()) return ELMM_OK;
+    int rr = dalloc((void **)&x.fill, fc.size() * sizeof(FillCell));
+    if (rr) return rr;
+    CU(cudaMemcpy(x.fill, fc.data(), fc.size() * sizeof(FillCell), cudaMemcpyHostToDevice));
+    x.nfill = (int)fc.size();
+    return ELMM_OK;
+  }
   int install_solids(int d, const elmm_solids *s) {
     Dom<T> &h = hdom[d];
     const elmm_config &c = cfg[d];
     if (c.enable_buoyancy)
-      return fail(ELMM_ERR_INVALID_ARG,
-                  "solid bodies with a temperature are not supported (the fill of the solid cells after each "
-                  "temperature stage is not built)");
+      for (int side : {ELMM_BO, ELMM_TO})
+        if (c.TempBtype[side] != ELMM_BC_CONSTFLUX || c.sideTemp[side] != 0)
+          return fail(ELMM_ERR_INVALID_ARG, "solid bodies with a temperature need adiabatic bottom and top sides");
     if (!h.wall[SIDE_BO] || h.bt[SIDE_BO] != BC_NOSLIP)
       return fail(ELMM_ERR_INVALID_ARG, "solid bodies need the wall model on a no-slip bottom");
     const bool per[3] = {h.bt[SIDE_WE] == BC_PERIODIC, h.bt[SIDE_SO] == BC_PERIODIC, h.bt[SIDE_BO] == BC_PERIODIC};
@@ -1890,10 +1954,10 @@ struct BatchT {
         h.bskip[comp] = x.bskip[comp];
       }
     }
-    if (c.num_scalars > 0) {
-      // the passive scalars' cell mask: bit 0 the solid Pr cells with their
-      // periodic x and y images in the ghost columns, bit 1 the Pr
-      // wall-model points of the scalar equations
+    if (c.num_scalars > 0 || c.enable_buoyancy) {
+      // the scalars' cell mask: bit 0 the solid Pr cells with their periodic
+      // x and y images in the ghost columns (and the z ghost planes), bit 1
+      // the Pr wall-model points of the scalar equations
       if (s->n_solid_pr < 0 || (s->n_solid_pr > 0 && !s->solid_pr_ijk) || s->n_wm_pr < 0 ||
           (s->n_wm_pr > 0 && !s->wm_pr_ijk))
         return fail(ELMM_ERR_INVALID_ARG, "solid Pr cells or Pr wall-model points");
@@ -1903,7 +1967,9 @@ struct BatchT {
       };
       for (int64_t q = 0; q < s->n_solid_pr; q++) {
         const int32_t *t = s->solid_pr_ijk + 3 * q;
-        if (!in(t)) return fail(ELMM_ERR_INVALID_ARG, "solid Pr cell out of range");
+        if (t[0] < 1 || t[0] > h.nx || t[1] < 1 || t[1] > h.ny || t[2] < -1 || t[2] > h.nz + 2)
+          return fail(ELMM_ERR_INVALID_ARG, "solid Pr cell out of range");
+        if (t[2] < 0 || t[2] > h.nz + 1) continue;
         for (int oi : {-h.nx, 0, h.nx})
           for (int oj : {-h.ny, 0, h.ny}) {
             const int i = t[0] + oi, j = t[1] + oj;
@@ -1918,6 +1984,7 @@ struct BatchT {
       if ((r = up((void **)&x.pmask, m.data(), m.size()))) return r;
       h.pmask = x.pmask;
     }
+    if (c.enable_buoyancy && (r = build_fill(d, s))) return r;
     x.on = true;
     x.primed = false;
     return push_dom(d);

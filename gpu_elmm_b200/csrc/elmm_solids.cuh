@@ -70,6 +70,10 @@ __global__ void __launch_bounds__(256) k_ib_gather(const Dom<T> *__restrict__ do
     double v = 0;
     for (int m = 0; m < p.n; m++) v = v + p.coef[m] * (double)F[p.src[m]];
     F[p.tgt] = (T)v;
+    // with buoyancy the temperature diffusivity follows the viscosity the
+    // ScalFl point now has (ComputeTDiff after the interpolation,
+    // src/dynamics.f90:899-904)
+    if (p.comp == 3 && d.tdiff_live) d.TDiff[p.tgt] = tdiff_of((T)v, (T)d.nu_mol, (T)d.kappa_mol);
   }
 }
 
@@ -190,6 +194,35 @@ __global__ void __launch_bounds__(128) k_ib_wm(const Dom<T> *__restrict__ doms, 
     T *S2 = comp == 0 ? d.U2 : comp == 1 ? d.V2 : d.W2;
     atomicAdd(S + c, (T)delta);
     atomicAdd(S2 + c, (T)(beta_dt * delta));
+  }
+}
+
+// The temperature's fill of the solid cells after each stage
+// (src/scalars.f90:129-198): a solid Pr cell with fluid 6-neighbours (in
+// range -1..n+2) becomes the mean of those, in the order i-1, i+1, j-1,
+// j+1, k-1, k+1.  A cell deep inside a body keeps its value: the
+// reference's branch for it sums all neighbours but assigns nothing.  The
+// fill reads fluid cells only, which it never writes, so its order does not
+// matter; a cell of a z ghost layer is filled for nothing (the next
+// BoundTemperature replaces it before anything reads it) and is left out.
+struct FillCell {
+  long long box;     // the cell
+  long long ref[6];  // its fluid neighbours' cells (the ghost rule's source for a ghost cell)
+  int n;             // how many
+  int pad;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_theta_fill(const Dom<T> *__restrict__ doms, int di,
+                                                    const FillCell *__restrict__ cells, int n, int tb) {
+  const Dom<T> &d = doms[di];
+  T *S = d.slot[0].buf[tb];
+  const double off = d.slot[0].off;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    const FillCell &c = cells[q];
+    double t = 0;
+    for (int m = 0; m < c.n; m++) t = t + ((double)S[c.ref[m]] + off);
+    S[c.box] = (T)(t / c.n - off);
   }
 }
 

@@ -518,11 +518,13 @@ class Geometry:
         return out
 
     def solid_pr(self):
-        """Pr cells with Prtype > 0 inside the domain, (i, j, k) 1..n."""
+        """Pr cells with Prtype > 0: i, j in 1..n (the x and y ghosts are
+        periodic images) and k in -1..nz+2 (the z ghost layers the
+        temperature's fill of the solid cells reaches)."""
         g = self.g
-        t = self.types[0][3:g.Prnz + 3, 3:g.Prny + 3, 3:g.Prnx + 3]
+        t = self.types[0][1:g.Prnz + 5, 3:g.Prny + 3, 3:g.Prnx + 3]
         k, j, i = np.nonzero(t > 0)
-        return np.stack([i + 1, j + 1, k + 1], axis=1).astype(np.int32) if len(i) else np.zeros((0, 3), np.int32)
+        return np.stack([i + 1, j + 1, k - 1], axis=1).astype(np.int32) if len(i) else np.zeros((0, 3), np.int32)
 
     def wm_pr(self):
         """The Pr wall-model points of the scalar equations, each cell once:

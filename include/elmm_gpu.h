@@ -325,15 +325,17 @@ typedef struct elmm_solids {
    * where Xtype(i,j,1) == 0 and Xtype(i,j,0) <= 0 (src/wallmodels.f90:700-820) */
   int64_t n_bottom_skip[3];
   const int32_t *bottom_skip_ij[3];
-  /* With passive scalars (i, j, k) triples, 1..n: the solid Pr cells
-   * (Prtype > 0, FindInsideCells, src/solidbodies.f90:75-206), where the
-   * advection tendency of a scalar is zeroed (src/scalars.f90:259-268), and
+  /* With a temperature or passive scalars, (i, j, k) triples: the solid Pr
+   * cells (Prtype > 0, FindInsideCells, src/solidbodies.f90:75-206; i, j in
+   * 1..n, k in -1..nz+2, the z ghost layers included), where the advection
+   * tendency of a scalar is zeroed (src/scalars.f90:259-268), and
    * the Pr wall-model points of the scalar equations, whose div * S term
    * skips the faces towards solid cells (DivergenceWM,
    * src/wallmodels.f90:1117-1168): the fluid cells with a solid neighbour
    * (GetSolidBodiesWM, src/immersedboundary.f90:14-138) and the cells of a
    * wall-model wall with Prtype = 0 (src/wallmodels.f90:467-687), each
-   * once.  Without passive scalars both may be empty. */
+   * once (1..n).  Without a temperature or passive scalars both may be
+   * empty. */
   int64_t n_solid_pr;
   const int32_t *solid_pr_ijk;
   int64_t n_wm_pr;
@@ -345,9 +347,10 @@ typedef struct elmm_solids {
  * (ELMM_ERR_INVALID_ARG otherwise): indices in range; no interpolation point
  * of a list is a forcing point of the same list; no forcing or nullified
  * point within one cell of a periodic boundary; a no-slip bottom wall with
- * the wall model; no temperature (the reference's in-place fill of the
- * solid cells after each temperature stage, src/scalars.f90:129-198, is
- * not built); passive scalars with the Pr lists above.  The next elmm_step
+ * the wall model; with a temperature adiabatic bottom and top (the solid
+ * faces carry no heat flux) and the Pr lists above, as for passive
+ * scalars.  After each temperature stage the solid cells with fluid
+ * neighbours take the mean of those (src/scalars.f90:129-198).  The next elmm_step
  * applies IBMomentum once first, as the first call of TMarchRK3 does
  * (src/tsteps.f90:44-48).  Passing NULL removes the bodies. */
 int elmm_set_solids(elmm_handle *h, const elmm_solids *s);

@@ -1141,9 +1141,36 @@ static void PreparePuffs(Domain &d, int stage, double time, double dt) {
   }
 }
 
+// The fill of the solid cells after the temperature stage, scalars.f90:129-198,
+// in its loop order: a solid cell with fluid neighbours (range -1..n+2)
+// becomes their mean; for a cell without any the reference sums all six
+// neighbours and assigns nothing, so it keeps its value
+static void FillSolidTemperature(Domain &d) {
+  const int nx = d.Prnx, ny = d.Prny, nz = d.Prnz;
+  A3 &T = d.T;
+  const A3 &P = d.Prsolid;
+  for (int k = -1; k <= nz + 2; k++)
+    for (int j = -1; j <= ny + 2; j++)
+      for (int i = -1; i <= nx + 2; i++) {
+        if (P(i, j, k) == 0) continue;
+        double t = 0;
+        int n = 0;
+        if (i > -1 && P(i - 1, j, k) == 0) { t = t + T(i - 1, j, k); n = n + 1; }
+        if (i < nx + 2 && P(i + 1, j, k) == 0) { t = t + T(i + 1, j, k); n = n + 1; }
+        if (j > -1 && P(i, j - 1, k) == 0) { t = t + T(i, j - 1, k); n = n + 1; }
+        if (j < ny + 2 && P(i, j + 1, k) == 0) { t = t + T(i, j + 1, k); n = n + 1; }
+        if (k > -1 && P(i, j, k - 1) == 0) { t = t + T(i, j, k - 1); n = n + 1; }
+        if (k < nz + 2 && P(i, j, k + 1) == 0) { t = t + T(i, j, k + 1); n = n + 1; }
+        if (n > 0) T(i, j, k) = t / n;
+      }
+}
+
 // ScalarRK3 (scalars.f90:88-381): the temperature, then each passive scalar
 static void ScalarRK3(Domain &d, int stage, double dt) {
-  if (d.enable_buoyancy) ScalarStage(d, stage, dt, d.T, d.T2, d.Tadv, 0);
+  if (d.enable_buoyancy) {
+    ScalarStage(d, stage, dt, d.T, d.T2, d.Tadv, 0);
+    if (d.scal_solids) FillSolidTemperature(d);
+  }
   PreparePuffs(d, stage, d.time, dt);  // scalars.f90:217
   for (int sc = 1; sc <= d.num_scalars; sc++)
     ScalarStage(d, stage, dt, d.S[sc - 1], d.S2[sc - 1], d.Sadv[sc - 1], sc);
@@ -2151,7 +2178,7 @@ int orc_set_solids(void *h, const elmm_solids *s) {
   d.scal_solids = false;
   d.wmprs.clear();
   if (!s) return 0;
-  if (d.num_scalars > 0) {
+  if (d.num_scalars > 0 || d.enable_buoyancy) {
     const int nx = d.Prnx, ny = d.Prny, nz = d.Prnz;
     d.Prsolid.init(-1, nx + 2, -1, ny + 2, -1, nz + 2);
     for (int64_t q = 0; q < s->n_solid_pr; q++) {

@@ -327,8 +327,8 @@ def _scalar_boxes():
 
 
 def test_scalar_lists_of_the_bodies():
-    """The Pr lists for the passive scalars: the solid cells are the Prtype >
-    0 cells; the wall-model points are the free cells with a solid
+    """The Pr lists for the scalars: the solid cells are the Prtype > 0
+    cells, the z ghost layers included; the wall-model points are the free cells with a solid
     6-neighbour (GetSolidBodiesWM) and the bottom cells with Prtype == 0
     (GetOutsideBoundariesWM_Pr), each once, none of them solid."""
     cfg = _scalar_boxes_cfg()
@@ -338,7 +338,9 @@ def test_scalar_lists_of_the_bodies():
     t = g.types[0]
     T = lambda i, j, k: int(t[k + 2, j + 2, i + 2])
     solid = {tuple(p) for p in s.solid_pr.tolist()}
-    assert len(solid) == len(s.solid_pr) == int((t[3:nz + 3, 3:ny + 3, 3:nx + 3] > 0).sum())
+    assert len(solid) == len(s.solid_pr) == int((t[1:nz + 5, 3:ny + 3, 3:nx + 3] > 0).sum())
+    assert all(T(i, j, k) > 0 and -1 <= k <= nz + 2 for (i, j, k) in solid)
+    assert any(k < 1 for (_, _, k) in solid)    # the boxes reach below the ground
     wm = [tuple(p) for p in s.wm_pr.tolist()]
     assert len(wm) == len(set(wm)) and not (set(wm) & solid)
     for (i, j, k) in wm:
@@ -412,10 +414,75 @@ def test_mixed_passive_scalar_among_boxes():
     dm.close()
 
 
-@pytest.mark.gpu
-def test_temperature_with_bodies_is_refused():
+def _theta_pair(precision=0):
+    """The oracle and a library domain with the potential temperature among
+    the boxes (adiabatic walls), from the same state, projected, then given
+    the bodies."""
     from gpu_elmm_b200 import lib as L
-    cfg = make_config(40, 36, 20, buoyancy=True)
+    from gpu_elmm_b200.config import FIELD_TEMPERATURE
+    from gpu_elmm_b200.workloads import temperature_state
+    mk = lambda p: make_config(40, 36, 20, pr_gradient_x=-2e-3, buoyancy=True, precision=p)
+    cfg = mk(precision)
+    s = build_solids(cfg, _scalar_boxes())
+    g = grid_of(cfg)
+    st = log_profile_state(g, seed=4)
+    T0 = temperature_state(g, seed=4, gradient=0.02, amp=0.2)
+    o = Oracle(mk(0))
+    o.set_state(*st)
+    o.set_field(FIELD_TEMPERATURE, T0)
+    o.project(1.0)
+    o.set_solids(s)
+    d = L.Domain(cfg)
+    d.upload(*st)
+    d.upload_temperature(T0)
+    d.project(1.0)
+    d.set_solids(s)
+    return g, o, d
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nsteps", [1, 5])
+def test_fp64_temperature_among_boxes(nsteps):
+    """The potential temperature among boxes: no advection tendency in the
+    solid cells, the wall-model div * theta of the cells next to them, and
+    after each stage the fill of the solid cells with the mean of their
+    fluid neighbours (src/scalars.f90:129-198; cells deep inside a body
+    keep their value, as in the reference).  FP64 against the oracle: U, V,
+    W within 1e-11, P within 1e-10, theta - T_ref within 1e-11."""
+    from gpu_elmm_b200.config import FIELD_TEMPERATURE
+    from gpu_elmm_b200.workloads import interior
+    g, o, d = _theta_pair()
+    o.step(nsteps)
+    d.step(nsteps)
+    e = [rel(a, b) for a, b in zip(interiors(g, *d.download()), interiors(g, *o.state()))]
+    n = (g.Prnx, g.Prny, g.Prnz)
+    et = rel(interior(d.field(FIELD_TEMPERATURE), -2, n) - 295.0, interior(o.get_field(FIELD_TEMPERATURE), -2, n) - 295.0)
+    print("temperature among boxes, FP64 vs oracle after", nsteps, "steps:", e, et)
+    assert max(e[:3]) < 1e-11 and e[3] < 1e-10 and et < 1e-11, (e, et)
+    d.close()
+
+
+@pytest.mark.gpu
+def test_mixed_temperature_among_boxes():
+    from gpu_elmm_b200.config import FIELD_TEMPERATURE
+    from gpu_elmm_b200.workloads import interior
+    g, _, d64 = _theta_pair(0)
+    _, _, dm = _theta_pair(1)
+    d64.step(3)
+    dm.step(3)
+    n = (g.Prnx, g.Prny, g.Prnz)
+    e = [rel(a, b) for a, b in zip(interiors(g, *dm.download())[:3], interiors(g, *d64.download())[:3])]
+    et = rel(interior(dm.field(FIELD_TEMPERATURE), -2, n) - 295.0, interior(d64.field(FIELD_TEMPERATURE), -2, n) - 295.0)
+    print("temperature among boxes, mixed vs FP64 after 3 steps:", e, et)
+    assert max(e) < 1e-5 and et < 1e-5, (e, et)
+    d64.close()
+    dm.close()
+
+
+@pytest.mark.gpu
+def test_temperature_with_bodies_needs_adiabatic_walls():
+    from gpu_elmm_b200 import lib as L
+    cfg = make_config(40, 36, 20, buoyancy=True, heat_flux=(0.1, 0.0))
     d = L.Domain(cfg)
     with pytest.raises(L.ElmmError) as e:
         d.set_solids(build_solids(cfg, _scalar_boxes()))
