@@ -137,6 +137,121 @@ class Sphere:
         return self.closest(x, y, z)
 
 
+_EPS10 = 10 * 2.220446049250313e-16  # the default eps of GeometricShape_Inside, 10 * epsilon(1._knd)
+_TINY = 2.2250738585072014e-308      # tiny(1._knd)
+
+
+@dataclass
+class Cylinder:
+    """A solid cylinder between the centres p1 and p2 of its end caps, radius
+    r, roughness z0r (Cylinder, src/geometricshapes.f90:171-177, 1278-1440:
+    a CylJacket through p1 along p2 - p1 and, unless infinite, the cap planes
+    through p1 and p2 with the outward normals p1 - p2 and p2 - p1).  The
+    reference's Plane_Closest moves a point by the plane's signed distance
+    times the normal, which the cap planes leave unnormalised, so a cap's
+    closest point lies |p2 - p1| times the distance away; restated as
+    written, the wall-model distance vectors to a cap carry that factor (it
+    is 1 for a cylinder of unit length)."""
+    p1: tuple
+    p2: tuple
+    r: float
+    z0r: float = 0.1
+    infinite: bool = False
+
+    def __post_init__(self):
+        x1, y1, z1 = (float(v) for v in self.p1)
+        x2, y2, z2 = (float(v) for v in self.p2)
+        self.jac = (x1, y1, z1, x2 - x1, y2 - y1, z2 - z1)  # CylJacket_Init(point1, point2 - point1, radius)
+        # Plane_Init_3r(point, normal): d = -(a xc + b yc + c zc)
+        def plane(xc, yc, zc, a, b, c):
+            return (a, b, c, -(a * xc + b * yc + c * zc))
+        self.planes = () if self.infinite else (plane(x1, y1, z1, x1 - x2, y1 - y2, z1 - z2),
+                                                 plane(x2, y2, z2, x2 - x1, y2 - y1, z2 - z1))
+
+    # ------------------------------------------------------------ parts
+    def _jacket_inside(self, x, y, z, eps):
+        """CylJacket_Inside with LineDist (:380-391, :1300-1306)."""
+        xl, yl, zl, a, b, c = self.jac
+        t = (a * (x - xl) + b * (y - yl) + c * (z - zl)) / (a ** 2 + b ** 2 + c ** 2) \
+            if (a != 0 or b != 0 or c != 0) else 0 * x
+        return np.sqrt((xl + a * t - x) ** 2 + (yl + b * t - y) ** 2 + (zl + c * t - z) ** 2) <= self.r + eps
+
+    @staticmethod
+    def _plane_inside(pl, x, y, z, eps):
+        """Plane_Inside (:632-642) of a plane built with GL false."""
+        a, b, c, d = pl
+        return a * x + b * y + c * z + d <= eps * math.sqrt(a ** 2 + b ** 2 + c ** 2)
+
+    @staticmethod
+    def _plane_closest(pl, x, y, z):
+        """Plane_Closest (:644-660), the unnormalised step as written."""
+        a, b, c, d = pl
+        if abs(a) > _TINY or abs(b) > _TINY or abs(c) > _TINY:
+            t = -(a * x + b * y + c * z + d) / math.sqrt(a ** 2 + b ** 2 + c ** 2)
+        else:
+            t = 0.0
+        return (x + a * t, y + b * t, z + c * t)
+
+    def _jacket_closest(self, x, y, z):
+        """CylJacket_Closest (:1308-1325) through Line_Closest (:441-456)."""
+        xc, yc, zc, a, b, c = self.jac
+        t = (a * (x - xc) + b * (y - yc) + c * (z - zc)) / (a ** 2 + b ** 2 + c ** 2) \
+            if (a != 0 or b != 0 or c != 0) else 0.0
+        xl, yl, zl = xc + a * t, yc + b * t, zc + c * t
+        p, q, w = x - xl, y - yl, z - zl
+        with np.errstate(all="ignore"):  # a point on the axis: IEEE inf and nan, unused by the callers then
+            t = np.float64(self.r) / np.sqrt(np.float64(p ** 2 + q ** 2 + w ** 2))
+            return (float(p * t + xl), float(q * t + yl), float(w * t + zl))
+
+    @staticmethod
+    def _dist(x1, y1, z1, x2, y2, z2):
+        """PointDist (:374-378)."""
+        return math.sqrt((x1 - x2) ** 2 + (y1 - y2) ** 2 + (z1 - z2) ** 2)
+
+    # -------------------------------------------------------- interface
+    def inside(self, x, y, z, eps):
+        """Cylinder_Inside (:1330-1345)."""
+        if not self._jacket_inside(x, y, z, eps):
+            return False
+        return all(self._plane_inside(pl, x, y, z, eps) for pl in self.planes)
+
+    def mask(self, x, y, z, eps):
+        X, Y, Z = x[None, None, :], y[None, :, None], z[:, None, None]
+        m = self._jacket_inside(X, Y, Z, eps)
+        for pl in self.planes:
+            m = m & self._plane_inside(pl, X, Y, Z, eps)
+        return np.broadcast_to(m, (len(z), len(y), len(x)))
+
+    def closest(self, x, y, z):
+        """Cylinder_Closest (:1347-1400), for caps perpendicular to the axis."""
+        if not self.planes:
+            return self._jacket_closest(x, y, z)
+        pl1, pl2 = self.planes
+        j = self._jacket_closest(x, y, z)
+        p1 = self._plane_closest(pl1, x, y, z)
+        p2 = self._plane_closest(pl2, x, y, z)
+        if self._jacket_inside(x, y, z, _EPS10):
+            return p1 if self._dist(x, y, z, *p1) <= self._dist(x, y, z, *p2) else p2
+        if self._plane_inside(pl1, x, y, z, _EPS10) and self._plane_inside(pl2, x, y, z, _EPS10):
+            return j
+        if self._dist(x, y, z, *p1) <= self._dist(x, y, z, *p2):
+            return self._jacket_closest(*p1)
+        return self._jacket_closest(*p2)
+
+    def closest_out(self, x, y, z):
+        """Cylinder_ClosestOut (:1402-1440)."""
+        far = math.sqrt(1.7976931348623157e308) / 10
+        p1 = self._plane_closest(self.planes[0], x, y, z) if self.planes else (far, far, far)
+        p2 = self._plane_closest(self.planes[1], x, y, z) if self.planes else (far, far, far)
+        j = self._jacket_closest(x, y, z)
+        d1, d2, dj = self._dist(x, y, z, *p1), self._dist(x, y, z, *p2), self._dist(x, y, z, *j)
+        if d1 <= d2 and d1 <= dj:
+            return p1
+        if d2 <= d1 and d2 <= dj:
+            return p2
+        return j  # dj <= d1, d2; also when a NaN fails all three tests (a point on the axis)
+
+
 def cube_array(n_per_side: int, edge: float, pitch: float, height: float, *, offset: float, depth: float,
                z0r: float = 0.1):
     """n x n cubes of the given edge (x, y) and height at `pitch` spacing,

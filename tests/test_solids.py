@@ -283,15 +283,17 @@ def test_sphere_geometry_lists():
 
 
 @pytest.mark.gpu
-def test_fp64_spheres_match_the_oracle():
+@pytest.mark.parametrize("shape", ["spheres", "cylinders"])
+def test_fp64_spheres_match_the_oracle(shape):
     """The same device path as the cubes, given the point lists of the
-    spheres: FP64 against the oracle after 3 steps, and the mixed path
-    within 1e-5 of FP64."""
+    spheres or of the cylinders: FP64 against the oracle after 3 steps, and
+    the mixed path within 1e-5 of FP64."""
     from gpu_elmm_b200 import lib as L
+    bodies = _spheres if shape == "spheres" else _cylinders
     out = {}
     for prec in (0, 1):
         cfg = _cfg(prec)
-        s = build_solids(cfg, _spheres())
+        s = build_solids(cfg, bodies())
         g, st = _state(cfg)
         d = L.Domain(cfg)
         d.upload(*st)
@@ -301,7 +303,7 @@ def test_fp64_spheres_match_the_oracle():
         out[prec] = (d.download(), sd.max_div)
         d.close()
     cfg = _cfg(0)
-    s = build_solids(cfg, _spheres())
+    s = build_solids(cfg, bodies())
     g, st = _state(cfg)
     o = Oracle(cfg)
     o.set_state(*st)
@@ -310,7 +312,7 @@ def test_fp64_spheres_match_the_oracle():
     o.step(3)
     e = [rel(a, b) for a, b in zip(interiors(g, *out[0][0]), interiors(g, *o.state()))]
     em = [rel(a, b) for a, b in zip(interiors(g, *out[1][0])[:3], interiors(g, *out[0][0])[:3])]
-    print("spheres: FP64 vs oracle", e, "mixed vs FP64", em, "max div", out[0][1], out[1][1])
+    print(shape, ": FP64 vs oracle", e, "mixed vs FP64", em, "max div", out[0][1], out[1][1])
     assert max(e[:3]) < 1e-11 and e[3] < 1e-10 and out[0][1] < 1e-10, e
     assert max(em) < 1e-5 and out[1][1] < 1e-5, em
 
@@ -527,3 +529,60 @@ def test_batch_with_a_scalar_among_boxes_equals_the_run_alone():
     a.close()
     p.close()
     b.close()
+
+
+def _cylinders():
+    # a vertical cylinder sunk into the ground and a horizontal one lying
+    # free in y, axes off the grid lines; unit-length caps would make the
+    # cap distances exact, these are longer
+    from gpu_elmm_b200.solids import Cylinder
+    return [Cylinder((14.3, 13.7, -3.0), (14.3, 13.7, 6.0), 4.2),
+            Cylinder((33.6, 24.0, 7.3), (33.6, 38.0, 7.3), 3.1, z0r=0.05)]
+
+
+def test_cylinder_geometry_lists():
+    """Cylinders (Cylinder_Inside / _Closest / _ClosestOut): forcing points
+    solid and interpolation points free, every interior solid point an IB
+    point or nullified, the solid volume above the ground close to the
+    cylinders' volume, each cylinder's roughness on its wall-model points."""
+    import math
+    cfg = _cfg()
+    bodies = _cylinders()
+    s = build_solids(cfg, bodies)
+    g = s.geometry
+    c = s.counts()
+    assert min(c["ib"]) > 0 and min(c["null"]) > 0 and c["scalfl"] > 0 and c["wm"] > 0
+    for q in range(3):
+        t = g.types[q + 1]
+        for (i, j, k), pts, cf in s.ib[q]:
+            assert t[k + 2, j + 2, i + 2] > 0
+            for (a, b, cc) in pts:
+                assert t[cc + 2, b + 2, a + 2] <= 0
+        (nx, ny, nz) = g.grids[q + 1][0]
+        assert int((t[3:nz + 3, 3:ny + 3, 3:nx + 3] > 0).sum()) == len(s.ib[q]) + len(s.null[q])
+    cz = g.c
+    t0 = g.types[0]
+    vol = 0.0
+    for k in range(1, NZ + 1):
+        dz = cz.x(cz.zW, k) - cz.x(cz.zW, k - 1)
+        vol += float((t0[k + 2, 3:48 + 3, 3:48 + 3] > 0).sum()) * dz
+    exact = math.pi * 4.2 ** 2 * 6.0 + math.pi * 3.1 ** 2 * 14.0
+    assert abs(vol - exact) / exact < 0.15, (vol, exact)
+    for comp, dr, i, j, k, dv, z0 in s.wm:
+        assert g.typ(comp, i, j, k) < 0 and z0 in (0.1, 0.05) and np.linalg.norm(dv) > 0
+
+
+def test_cylinder_closest_points_as_written():
+    """The jacket's closest point is the radial projection; a cap's closest
+    point moves by the signed distance times the unnormalised cap normal
+    (Plane_Closest, src/geometricshapes.f90:644-660), exact for a cylinder
+    of unit length and |p2 - p1| times the distance otherwise."""
+    from gpu_elmm_b200.solids import Cylinder
+    c = Cylinder((10.0, 10.0, 0.0), (10.0, 10.0, 1.0), 3.0)
+    assert c.closest(15.0, 10.0, 0.5) == (13.0, 10.0, 0.5)
+    assert c.closest(10.2, 10.0, 5.0) == (10.2, 10.0, 1.0)
+    assert c.closest_out(10.2, 10.0, 0.9) == (10.2, 10.0, 1.0)
+    assert c.inside(12.9, 10.0, 0.5, 0.0) and not c.inside(10.0, 10.0, 1.2, 0.0)
+    long = Cylinder((10.0, 10.0, 0.0), (10.0, 10.0, 4.0), 3.0)
+    x, y, z = long.closest(10.2, 10.0, 5.0)
+    assert (x, y) == (10.2, 10.0) and abs(z - (5.0 - 4.0 * 1.0)) < 1e-12   # 4 x the distance 1 below
