@@ -1105,6 +1105,12 @@ struct BatchT {
       if (c.avg_slice_k > 0 && (r = dalloc((void **)&sl.acc_xy, sizeof(double) * h.nx * h.ny))) return r;
       if (c.avg_slice_j > 0 && (r = dalloc((void **)&sl.acc_xz, sizeof(double) * h.nx * h.nz))) return r;
     }
+    // a slab: the second halo planes of every scalar slot beyond its BC_HALO faces
+    for (int s = 0; s < h.nslot; s++)
+      for (int side = 0; side < 2; side++)
+        if (h.slot[s].bt[side ? SIDE_TO : SIDE_BO] == BC_HALO &&
+            (r = dalloc((void **)&h.slot[s].h2[side], (size_t)h.plane * sizeof(T))))
+          return r;
     h.avg_k = c.avg_slice_k;
     h.avg_j = c.avg_slice_j;
     h.avg_w = c.avg_weight;
@@ -1355,7 +1361,9 @@ struct BatchT {
       const Dom<T> &h = hdom[d];
       if (h.tdir[ELMM_BO] || h.tdir[ELMM_TO] || h.pmask) return true;
       for (int s = 0; s < h.nslot; s++)
-        if (h.slot[s].zg[0] || h.slot[s].zg[1] || h.slot[s].wflux[0] != 0 || h.slot[s].wflux[1] != 0) return true;
+        if (h.slot[s].zg[0] || h.slot[s].zg[1] || h.slot[s].wflux[0] != 0 || h.slot[s].wflux[1] != 0 ||
+            h.slot[s].bt[SIDE_BO] == BC_HALO || h.slot[s].bt[SIDE_TO] == BC_HALO)
+          return true;
     }
     return false;
   }

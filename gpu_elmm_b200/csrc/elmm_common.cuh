@@ -67,6 +67,11 @@ struct ScalSlot {
   // k = 1, [1] the plane above k = nz; zside: the BC value of the side
   int zg[2];
   double zside[2];
+  // a slab of a split domain: the second planes beyond its BC_HALO faces
+  // (level -1 below, nz + 2 above; the slab exchange fills them after each
+  // stage) for the two-deep z stencil of KappaScalar, one plane each in the
+  // in-plane layout of a box plane; null elsewhere
+  T *h2[2];
 };
 
 // Domain descriptor, copied to device memory once at creation.  Coefficients

@@ -70,8 +70,8 @@ struct SlabsT {
     if (r) return r;
     if (n < 1 || n > ELMM_MAX_SLABS) return fail(ELMM_ERR_INVALID_ARG, "nslabs in 1.." + std::to_string(ELMM_MAX_SLABS));
     if (c.Btype[ELMM_BO] == ELMM_BC_PERIODIC) return fail(ELMM_ERR_INVALID_CONFIG, "split domains need walls in z (periodic z is not built)");
-    if (c.enable_buoyancy || c.num_scalars > 0 || c.num_point_sources > 0)
-      return fail(ELMM_ERR_INVALID_CONFIG, "split domains carry no temperature or scalars");
+    if (c.avg_slice_k > 0 || c.avg_slice_j > 0)
+      return fail(ELMM_ERR_INVALID_CONFIG, "split domains keep no time-averaged slices");
     if (c.variable_time_steps) return fail(ELMM_ERR_INVALID_CONFIG, "split domains take constant time steps");
     if (c.max_refine_sweeps > 0) return fail(ELMM_ERR_INVALID_CONFIG, "split domains take no defect-correction sweeps");
     ns = n;
@@ -115,10 +115,17 @@ struct SlabsT {
       elmm_config cs = c;
       cs.Prnz = nzl[s];
       cs.device = dev[s];
-      if (s > 0) cs.Btype[ELMM_BO] = BC_HALO;
-      if (s < n - 1) cs.Btype[ELMM_TO] = BC_HALO;
+      if (s > 0) cs.Btype[ELMM_BO] = cs.TempBtype[ELMM_BO] = cs.ScalBtype[ELMM_BO] = BC_HALO;
+      if (s < n - 1) cs.Btype[ELMM_TO] = cs.TempBtype[ELMM_TO] = cs.ScalBtype[ELMM_TO] = BC_HALO;
       cs.zW = c.zW ? c.zW + k0[s] : nullptr;
       cs.zmin = c.zmin + k0[s] * c.dzmin;
+      // the point sources whose cell of the whole domain lies in this slab
+      cs.num_point_sources = 0;
+      for (int q = 0; q < c.num_point_sources; q++) {
+        int ip[3];
+        if (point_cell(c, c.point_sources[q].position, ip) && ip[2] > k0[s] && ip[2] <= k0[s] + nzl[s])
+          cs.point_sources[cs.num_point_sources++] = c.point_sources[q];
+      }
       sl[s].reset(new BatchT<T>());
       BatchT<T> &B = *sl[s];
       B.slab_mode = true;
@@ -249,6 +256,33 @@ struct SlabsT {
     halo_copies(cps, fs, up, down);
     return exchange(cps);
   }
+  // plane k of scalar slot q's buffer b of slab s, or of its diffusivity (q < 0)
+  T *splane(int s, int q, int b, int k) const {
+    const Dom<T> &h = sl[s]->hdom[0];
+    return (q < 0 ? h.TDiff : h.slot[q].buf[b]) + (size_t)k * h.plane;
+  }
+  int nslots() const { return sl[0]->hdom[0].nslot; }
+  // the halos of the scalar slots' buffer b: the top plane and the one below
+  // it up into the next slab's ghost plane and second halo plane, the first
+  // two planes down likewise (KappaScalar reads two levels either side)
+  void scalar_copies(std::vector<Copy> &cps, int b) const {
+    for (int q = 0; q < nslots(); q++)
+      for (int s = 0; s + 1 < ns; s++) {
+        const size_t pb = plane_bytes(s);
+        cps.push_back(Copy{s, s + 1, splane(s + 1, q, b, 0), splane(s, q, b, nzl[s]), pb});
+        cps.push_back(Copy{s, s + 1, sl[s + 1]->hdom[0].slot[q].h2[0], splane(s, q, b, nzl[s] - 1), pb});
+        cps.push_back(Copy{s + 1, s, splane(s, q, b, nzl[s] + 1), splane(s + 1, q, b, 1), pb});
+        cps.push_back(Copy{s + 1, s, sl[s]->hdom[0].slot[q].h2[1], splane(s + 1, q, b, 2), pb});
+      }
+  }
+  // the diffusivity's ghost planes at the shared faces, both ways
+  void tdiff_copies(std::vector<Copy> &cps) const {
+    if (!sl[0]->hdom[0].TDiff) return;
+    for (int s = 0; s + 1 < ns; s++) {
+      cps.push_back(Copy{s, s + 1, splane(s + 1, -1, 0, 0), splane(s, -1, 0, nzl[s]), plane_bytes(s)});
+      cps.push_back(Copy{s + 1, s, splane(s, -1, 0, nzl[s] + 1), splane(s + 1, -1, 0, 1), plane_bytes(s)});
+    }
+  }
   // after a projection: U V W P both ways, the top slab's pressure reference to all
   int exchange_state() {
     std::vector<Copy> cps;
@@ -330,10 +364,20 @@ struct SlabsT {
   }
   int stage(int st) {
     int r;
+    std::vector<Copy> cps;
     each([&](int, BatchT<T> &B) { B.launch_sgs(st); });
-    if ((r = exchange_halos({F_NU}, true, true))) return r;
-    each([&](int, BatchT<T> &B) { B.launch_momentum(st); });
-    if ((r = exchange_halos({F_W2}, true, false))) return r;
+    halo_copies(cps, {F_NU}, true, true);
+    tdiff_copies(cps);
+    if ((r = exchange(cps))) return r;
+    // ScalarRK3 between Convection and the projection (src/tsteps.f90:132-135)
+    each([&](int, BatchT<T> &B) {
+      B.launch_momentum(st);
+      B.launch_scalars(st, 0);
+    });
+    cps.clear();
+    halo_copies(cps, {F_W2}, true, false);
+    scalar_copies(cps, st % 3);
+    if ((r = exchange(cps))) return r;
     return projection(2 * kAlpha[st - 1], 1);
   }
   // one step of every slab for the captured graph: fork the slabs' streams
@@ -423,7 +467,12 @@ struct SlabsT {
       B.wm_kernel(1, B.stream);
       B.launch_ghosts({F_NU}, 0);
     });
-    if ((r = exchange_halos({F_NU}, true, true))) return r;
+    {
+      std::vector<Copy> cps;
+      halo_copies(cps, {F_NU}, true, true);
+      tdiff_copies(cps);
+      if ((r = exchange(cps))) return r;
+    }
     if ((r = finish())) return r;
     return stats_of(stats, 0);
   }
@@ -562,6 +611,53 @@ struct SlabsT {
     if (!r) r = download<H>(U, V, W, Pr);
     return r;
   }
+  // the temperature (sc = 0) or passive scalar sc from the whole domain's
+  // host array F(-2:nx+3, -2:ny+3, -2:nz+3): slab s takes the planes from its
+  // k0 on, then the slabs exchange their halos
+  int upload_scalar(int sc, const double *F) {
+    if (!F) return fail(ELMM_ERR_INVALID_ARG, "NULL array");
+    const Dom<T> &h0 = sl[0]->hdom[0];
+    if (sc == 0 ? !h0.buoy : (sc < 1 || sc > gcfg.num_scalars))
+      return fail(ELMM_ERR_INVALID_ARG, sc == 0 ? "no temperature field (enable_buoyancy is 0)"
+                                                : "scalar number outside 1..num_scalars");
+    const size_t ph = (size_t)(h0.nx + 6) * (h0.ny + 6);
+    for (int s = 0; s < ns; s++) {
+      BatchT<T> &B = *sl[s];
+      int r = sc == 0 ? B.upload_temperature(0, F + ph * k0[s]) : B.upload_scalar(0, sc, F + ph * k0[s]);
+      if (r) return r;
+    }
+    std::vector<Copy> cps;
+    scalar_copies(cps, 0);
+    int r = exchange(cps);
+    if (r) return r;
+    for (int s = 0; s < ns; s++) {
+      CU(cudaSetDevice(dev[s]));
+      CU(cudaStreamSynchronize(sl[s]->stream));
+    }
+    return ELMM_OK;
+  }
+  // ELMM_FIELD_TEMPERATURE or ELMM_FIELD_SCALAR + sc - 1 into the whole
+  // domain's host array, every element the single-domain download writes
+  int download_field(int field, double *host) {
+    if (!host) return fail(ELMM_ERR_INVALID_ARG, "NULL array");
+    const Dom<T> &h0 = sl[0]->hdom[0];
+    const bool ok = (field == ELMM_FIELD_TEMPERATURE && h0.buoy) ||
+                    (field >= ELMM_FIELD_SCALAR && field < ELMM_FIELD_SCALAR + gcfg.num_scalars);
+    if (!ok) return fail(ELMM_ERR_INVALID_ARG, "split domains download the temperature and the passive scalars");
+    const size_t ph = (size_t)(h0.nx + 6) * (h0.ny + 6);
+    for (int s = 0; s < ns; s++) {
+      BatchT<T> &B = *sl[s];
+      CU(cudaSetDevice(dev[s]));
+      const int kw0 = s == 0 ? -2 : 1, kw1 = s == ns - 1 ? nzl[s] + 3 : nzl[s];
+      const size_t skip = (size_t)(kw0 + 2) * ph;
+      B.pack(0, field, B.dstage, B.stream);
+      CU(cudaMemcpyAsync(host + ph * k0[s] + skip, B.dstage + skip, sizeof(double) * ph * (kw1 - kw0 + 1),
+                         cudaMemcpyDeviceToHost, B.stream));
+      CU(cudaStreamSynchronize(B.stream));
+      CU(cudaGetLastError());
+    }
+    return ELMM_OK;
+  }
 };
 
 struct elmm_slabs {
@@ -630,6 +726,22 @@ extern "C" int elmm_slabs_march_host_float(elmm_slabs *h, float *U, float *V, fl
   if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
   if (nsteps < 0) return fail(ELMM_ERR_INVALID_ARG, "nsteps < 0");
   return SLAB_DISPATCH(h, march_host(U, V, W, Pr, nsteps, stats));
+}
+
+extern "C" int elmm_slabs_upload_temperature(elmm_slabs *h, const double *T) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  return SLAB_DISPATCH(h, upload_scalar(0, T));
+}
+
+extern "C" int elmm_slabs_upload_scalar(elmm_slabs *h, int32_t sc, const double *S) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  if (sc < 1) return fail(ELMM_ERR_INVALID_ARG, "scalar number outside 1..num_scalars");
+  return SLAB_DISPATCH(h, upload_scalar(sc, S));
+}
+
+extern "C" int elmm_slabs_download_field(elmm_slabs *h, int32_t field, double *host) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  return SLAB_DISPATCH(h, download_field(field, host));
 }
 
 extern "C" int elmm_slabs_project(elmm_slabs *h, double coef, elmm_stats *stats) {

@@ -141,14 +141,25 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
       oy[q] = (scal_fold(j - 2 + q, ny, py) - j) * (int)pitch;
     }
     auto zoff = [&](int kk) { return (long long)(scal_fold(kk, nz, pz) - kk) * plane; };  // fold of plane kk
-    // the scalar's planes: a stored ghost plane (k_scalar_zghost) is read as it is
-    const int zg0 = sl.zg[0], zg1 = sl.zg[1];
-    auto szoff = [&](int kk) { return BC && ((kk == 0 && zg0) || (kk == nz + 1 && zg1)) ? 0LL : zoff(kk); };
+    const T *__restrict__ S = sl.buf[(stage - 1) % 3];
+    // the scalar's planes: a stored ghost plane (k_scalar_zghost, or a slab's
+    // halo) is read as it is; a slab's second halo planes live in h2
+    const bool hlo = BC && sl.bt[SIDE_BO] == BC_HALO, hhi = BC && sl.bt[SIDE_TO] == BC_HALO;
+    const int zs0 = sl.zg[0] || hlo, zs1 = sl.zg[1] || hhi;
+    auto szoff = [&](int kk) { return BC && ((kk == 0 && zs0) || (kk == nz + 1 && zs1)) ? 0LL : zoff(kk); };
+    auto kzoff = [&](int kk) { return (kk == 0 && hlo) || (kk == nz + 1 && hhi) ? 0LL : zoff(kk); };
+    // the scalar at level kk of this column, o its unfolded box index
+    auto lds = [&](int kk, long long o) -> T {
+      if constexpr (BC) {
+        if (kk == -1 && hlo) return ld(sl.h2[0], o + plane);
+        if (kk == nz + 2 && hhi) return ld(sl.h2[1], o - (long long)(nz + 2) * plane);
+      }
+      return ld(S, o + szoff(kk));
+    };
     // volume sources of this slot in this column, in configuration order
     unsigned srcm = 0;
     for (int q = 0; q < d.nsrc; q++)
       if (d.src_slot[q] == s && d.src_i[q] == i && d.src_j[q] == j) srcm |= 1u << q;
-    const T *__restrict__ S = sl.buf[(stage - 1) % 3];
     const T *__restrict__ K = d.TDiff;
     const T *__restrict__ U = d.U;
     const T *__restrict__ V = d.V;
@@ -164,9 +175,9 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
     // column windows: the scalar at k-2..k+2, diffusivity at k-1..k+1, W at k-1
     T sz[5], kz[3];
 #pragma unroll
-    for (int q = 0; q < 5; q++) sz[q] = ld(S, cc + (long long)(q - 2) * plane + szoff(k0 - 2 + q));
+    for (int q = 0; q < 5; q++) sz[q] = lds(k0 - 2 + q, cc + (long long)(q - 2) * plane);
 #pragma unroll
-    for (int q = 0; q < 3; q++) kz[q] = ld(K, cc + (long long)(q - 1) * plane + zoff(k0 - 1 + q));
+    for (int q = 0; q < 3; q++) kz[q] = ld(K, cc + (long long)(q - 1) * plane + kzoff(k0 - 1 + q));
     T wb = ld(W, cc - plane);
     // the bottom-face flux of plane k is the top-face flux of plane k-1
     T fzb = kappa_flux<T>(wb, sz[0], sz[1], sz[2], sz[3]);
@@ -263,10 +274,10 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
         const long long cn = cc + plane;
 #pragma unroll
         for (int q = 0; q < 4; q++) sz[q] = sz[q + 1];
-        sz[4] = ld(S, cn + 2 * plane + szoff(k + 3));
+        sz[4] = lds(k + 3, cn + 2 * plane);
         kz[0] = kz[1];
         kz[1] = kz[2];
-        kz[2] = ld(K, cn + plane + zoff(k + 2));
+        kz[2] = ld(K, cn + plane + kzoff(k + 2));
         wb = wt;
         fzb = fzt;
         cc = cn;
@@ -326,12 +337,21 @@ __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SP
 #pragma unroll
     for (int q = 0; q < 5; q++) oy[q] = (scal_fold(j - 2 + q, ny, py) - j) * (int)pitch;
     auto zoff = [&](int kk) { return (long long)(scal_fold(kk, nz, pz) - kk) * plane; };
-    const int zg0 = sl.zg[0], zg1 = sl.zg[1];
-    auto szoff = [&](int kk) { return BC && ((kk == 0 && zg0) || (kk == nz + 1 && zg1)) ? 0LL : zoff(kk); };
+    const T *__restrict__ S = sl.buf[(stage - 1) % 3];
+    const bool hlo = BC && sl.bt[SIDE_BO] == BC_HALO, hhi = BC && sl.bt[SIDE_TO] == BC_HALO;
+    const int zs0 = sl.zg[0] || hlo, zs1 = sl.zg[1] || hhi;
+    auto szoff = [&](int kk) { return BC && ((kk == 0 && zs0) || (kk == nz + 1 && zs1)) ? 0LL : zoff(kk); };
+    auto kzoff = [&](int kk) { return (kk == 0 && hlo) || (kk == nz + 1 && hhi) ? 0LL : zoff(kk); };
+    auto lds2 = [&](int kk, long long o) -> float2 {
+      if constexpr (BC) {
+        if (kk == -1 && hlo) return ld2(sl.h2[0], o + plane);
+        if (kk == nz + 2 && hhi) return ld2(sl.h2[1], o - (long long)(nz + 2) * plane);
+      }
+      return ld2(S, o + szoff(kk));
+    };
     unsigned srcm = 0;  // volume sources of this slot in this pair's columns
     for (int q = 0; q < d.nsrc; q++)
       if (d.src_slot[q] == s && (d.src_i[q] == i || d.src_i[q] == i + 1) && d.src_j[q] == j) srcm |= 1u << q;
-    const T *__restrict__ S = sl.buf[(stage - 1) % 3];
     const T *__restrict__ K = d.TDiff;
     const T *__restrict__ U = d.U;
     const T *__restrict__ V = d.V;
@@ -346,9 +366,9 @@ __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SP
     long long cc = bidx(d, i, j, k0);
     float2 sz[5], kz[3];
 #pragma unroll
-    for (int q = 0; q < 5; q++) sz[q] = ld2(S, cc + (long long)(q - 2) * plane + szoff(k0 - 2 + q));
+    for (int q = 0; q < 5; q++) sz[q] = lds2(k0 - 2 + q, cc + (long long)(q - 2) * plane);
 #pragma unroll
-    for (int q = 0; q < 3; q++) kz[q] = ld2(K, cc + (long long)(q - 1) * plane + zoff(k0 - 1 + q));
+    for (int q = 0; q < 3; q++) kz[q] = ld2(K, cc + (long long)(q - 1) * plane + kzoff(k0 - 1 + q));
     float2 wb = ld2(W, cc - plane);
     float2 fzb = make_float2(kappa_flux<T>(wb.x, sz[0].x, sz[1].x, sz[2].x, sz[3].x),
                              kappa_flux<T>(wb.y, sz[0].y, sz[1].y, sz[2].y, sz[3].y));
@@ -371,8 +391,8 @@ __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SP
       float2 sz_n = sz[4], kz_n = kz[2];
       if (k < k1) {
         nxt = load_plane(cc + plane);
-        sz_n = ld2(S, cc + 3 * plane + szoff(k + 3));
-        kz_n = ld2(K, cc + 2 * plane + zoff(k + 2));
+        sz_n = lds2(k + 3, cc + 3 * plane);
+        kz_n = ld2(K, cc + 2 * plane + kzoff(k + 2));
       }
       const float2 s0 = sz[2];
       const float2 sm = cur.sm, sp = cur.sp, km = cur.km, kp = cur.kp, um = cur.um, u0 = cur.u0;

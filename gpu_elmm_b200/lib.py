@@ -108,6 +108,9 @@ def lib():
         L.elmm_slabs_project.argtypes = [P, C.c_double, C.POINTER(ElmmStats)]
         L.elmm_slabs_step.argtypes = [P, C.c_int32, C.POINTER(ElmmStats)]
         L.elmm_slabs_march_host.argtypes = [P, _dp, _dp, _dp, _dp, C.c_int32, C.POINTER(ElmmStats)]
+        L.elmm_slabs_upload_temperature.argtypes = [P, _dp]
+        L.elmm_slabs_upload_scalar.argtypes = [P, C.c_int32, _dp]
+        L.elmm_slabs_download_field.argtypes = [P, C.c_int32, _dp]
         L.elmm_slabs_upload_state_float.argtypes = [P, fp, fp, fp, fp]
         L.elmm_slabs_download_state_float.argtypes = [P, fp, fp, fp, fp]
         L.elmm_slabs_march_host_float.argtypes = [P, fp, fp, fp, fp, C.c_int32, C.POINTER(ElmmStats)]
@@ -426,6 +429,21 @@ class Slabs:
         st = ElmmStats()
         check(lib().elmm_slabs_step(self.h, n, C.byref(st)), "elmm_slabs_step")
         return st
+
+    def upload_temperature(self, T):
+        check(lib().elmm_slabs_upload_temperature(self.h, ptr(T)), "elmm_slabs_upload_temperature")
+
+    def upload_scalar(self, sc, S):
+        check(lib().elmm_slabs_upload_scalar(self.h, sc, ptr(S)), "elmm_slabs_upload_scalar")
+
+    def field(self, fid):
+        """ELMM_FIELD_TEMPERATURE or ELMM_FIELD_SCALAR + sc - 1 of the whole domain."""
+        a = np.zeros(self.grid.shape_t())
+        check(lib().elmm_slabs_download_field(self.h, fid, ptr(a)), "elmm_slabs_download_field")
+        return a
+
+    def scalar(self, sc):
+        return self.field(FIELD_SCALAR + sc - 1)
 
     def march_host(self, U, V, W, Pr, n=1) -> ElmmStats:
         """elmm_slabs_march_host: the arrays are updated in place."""

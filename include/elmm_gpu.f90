@@ -342,6 +342,23 @@ module elmm_gpu
       type(c_ptr), value :: h
       real(c_double) :: U(*), V(*), W(*), Pr(*)
     end function
+    integer(c_int) function elmm_slabs_upload_temperature(h, T) bind(C)
+      import
+      type(c_ptr), value :: h
+      real(c_double), intent(in) :: T(*)
+    end function
+    integer(c_int) function elmm_slabs_upload_scalar(h, sc, S) bind(C)
+      import
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: sc
+      real(c_double), intent(in) :: S(*)
+    end function
+    integer(c_int) function elmm_slabs_download_field(h, field, host) bind(C)
+      import
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: field
+      real(c_double) :: host(*)
+    end function
     integer(c_int) function elmm_slabs_project(h, coef, st) bind(C)
       import
       type(c_ptr), value :: h

@@ -646,9 +646,12 @@ double elmm_server_now(const elmm_server *s);
  * the spectral buffer never crosses between GPUs.  The result equals the
  * single-domain handle's to rounding.
  *
- * Built for the flow: walls in z (no periodic z), constant dt, no
- * temperature, scalars, solid bodies or defect-correction sweeps
- * (ELMM_ERR_INVALID_CONFIG otherwise).  nz_slab may be NULL for an even
+ * Built for the flow, the temperature and passive scalars (with point
+ * sources): walls in z (no periodic z), constant dt, no solid bodies,
+ * puffs, time-averaged slices or defect-correction sweeps
+ * (ELMM_ERR_INVALID_CONFIG otherwise).  The slabs also exchange the
+ * scalars' two planes beyond each shared face (KappaScalar's stencil) and
+ * the diffusivity's ghost plane.  nz_slab may be NULL for an even
  * split; every slab needs at least 4 levels, and the levels must add up to
  * Prnz.  devices may be NULL for cfg->device.
  *
@@ -661,6 +664,13 @@ int elmm_slabs_create(const elmm_config *cfg, int32_t nslabs, const int32_t *dev
 int elmm_slabs_destroy(elmm_slabs *h);
 int elmm_slabs_upload_state(elmm_slabs *h, const double *U, const double *V, const double *W, const double *Pr);
 int elmm_slabs_download_state(elmm_slabs *h, double *U, double *V, double *W, double *Pr);
+/* The temperature and passive scalar sc (1..num_scalars) from the whole
+ * domain's arrays in the layout of elmm_upload_temperature, after the
+ * state and before elmm_slabs_project; elmm_slabs_download_field reads
+ * ELMM_FIELD_TEMPERATURE or ELMM_FIELD_SCALAR + sc - 1 back. */
+int elmm_slabs_upload_temperature(elmm_slabs *h, const double *T);
+int elmm_slabs_upload_scalar(elmm_slabs *h, int32_t sc, const double *S);
+int elmm_slabs_download_field(elmm_slabs *h, int32_t field, double *host);
 /* PressureCorrection on the uploaded state, as elmm_project. */
 int elmm_slabs_project(elmm_slabs *h, double coef, elmm_stats *stats);
 /* nsteps RK3 steps, as elmm_step: with every slab on one device each step

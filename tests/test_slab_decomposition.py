@@ -102,11 +102,13 @@ def test_slab_entry_points_check_their_arguments_first():
     assert lib.elmm_slabs_create(C.byref(cfg), 2, None, nz, C.byref(h)) == 6            # 14 != 16 levels
     nz = (C.c_int32 * 2)(13, 3)
     assert lib.elmm_slabs_create(C.byref(cfg), 2, None, nz, C.byref(h)) == 6            # a slab under 4 levels
-    warm = make_config(32, 32, 16, buoyancy=True)
-    assert lib.elmm_slabs_create(C.byref(warm), 2, None, None, C.byref(h)) == 1         # temperature: not built
+    sliced = make_config(32, 32, 16, num_scalars=1, avg_slice_k=3, avg_weight=0.1)
+    assert lib.elmm_slabs_create(C.byref(sliced), 2, None, None, C.byref(h)) == 1       # averaged slices: not built
     per = make_config(32, 32, 16, btype=(3, 3, 3, 3, 3, 3))
     assert lib.elmm_slabs_create(C.byref(per), 2, None, None, C.byref(h)) == 1          # periodic z: not built
     for f in (lib.elmm_slabs_destroy(None), lib.elmm_slabs_upload_state(None, None, None, None, None),
               lib.elmm_slabs_download_state(None, None, None, None, None),
-              lib.elmm_slabs_project(None, 1.0, None), lib.elmm_slabs_step(None, 1, None)):
+              lib.elmm_slabs_project(None, 1.0, None), lib.elmm_slabs_step(None, 1, None),
+              lib.elmm_slabs_upload_temperature(None, None), lib.elmm_slabs_upload_scalar(None, 1, None),
+              lib.elmm_slabs_download_field(None, 12, None)):
         assert f == 6

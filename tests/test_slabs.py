@@ -12,6 +12,8 @@ oracle.
   the split changes only the order of the z solve's operations;
 * mixed: within 1e-5 of the single-domain mixed path;
 * march_host and the real32 host arrays against the double calls;
+* the temperature and a passive scalar with point sources, the scalars'
+  two-deep halos exchanged, against the single domain;
 * even and uneven splits, 2 and 3 slabs, uniform and stretched z, slabs
   short enough for the tiled sweep kernels and taller ones.
 """
@@ -132,3 +134,54 @@ def test_slab_host_arrays(precision):
         assert np.array_equal(x, y.astype(np.float32))
     a.close()
     b.close()
+
+
+def _theta_scalar_cfg(precision, **kw):
+    return make_config(*N, precision=precision, buoyancy=True, num_scalars=1,
+                       point_sources=[(1, (20.5, 14.5, 12.2), 2.0), (1, (9.5, 20.5, 3.7), 1.0)], **kw)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("split", [(2, None), (3, (6, 10, 8))], ids=["even2", "uneven3"])
+def test_slabs_carry_temperature_and_scalars(precision, split):
+    """Config-1 physics with the potential temperature and a passive scalar
+    with two point sources (one in each half), split into slabs: the slabs
+    exchange the scalars' two planes beyond each shared face and the
+    diffusivity's ghost plane.  Against the single domain after the
+    projection and three steps: FP64 U, V, W within 1e-12, P within 1e-11,
+    theta - T_ref and the scalar within 1e-11; mixed within 1e-5."""
+    from gpu_elmm_b200.config import FIELD_TEMPERATURE
+    from gpu_elmm_b200.workloads import interior, puff_state, temperature_state
+    ns, nz = split
+    cfg = _theta_scalar_cfg(precision)
+    g = grid_of(cfg)
+    st = log_profile_state(g, seed=8)
+    T0 = temperature_state(g, seed=8, amp=0.2)
+    S0 = puff_state(g, (20, 14, 12), sigma=3.0)
+    a, b = L.Domain(cfg), L.Slabs(cfg, ns, devices=[0] * ns, nz=nz)
+    for h in (a, b):
+        h.upload(*st)
+        h.upload_temperature(T0)
+        h.upload_scalar(1, S0)
+    n = (g.Prnx, g.Prny, g.Prnz)
+    assert np.array_equal(b.field(FIELD_TEMPERATURE), a.field(FIELD_TEMPERATURE))
+    assert np.array_equal(b.scalar(1), a.scalar(1))
+    a.project(1.0)
+    b.project(1.0)
+    a.step(3)
+    sb = b.step(3)
+    tol = (1e-12, 1e-11, 1e-11) if precision == 0 else (1e-5, 1e-5, 1e-5)
+    e = _errs(b.download(), a.download())
+    et = rel(interior(b.field(FIELD_TEMPERATURE), -2, n) - 295.0, interior(a.field(FIELD_TEMPERATURE), -2, n) - 295.0)
+    es = rel(interior(b.scalar(1), -2, n), interior(a.scalar(1), -2, n))
+    print("temperature and scalar, slabs vs single domain:", precision, split, e, et, es)
+    assert max(e[:3]) < tol[0] and e[3] < tol[1] and et < tol[2] and es < tol[2], (e, et, es)
+    assert sb.max_div < (1e-10 if precision == 0 else 1e-6)
+    a.close()
+    b.close()
+
+
+def test_slabs_refuse_slices():
+    with pytest.raises(L.ElmmError) as e:
+        L.Slabs(make_config(*N, num_scalars=1, avg_slice_k=3, avg_weight=0.1), 2, devices=[0, 0])
+    assert e.value.code == 1
