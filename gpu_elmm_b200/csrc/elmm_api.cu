@@ -1512,6 +1512,22 @@ struct BatchT {
     }
     return ELMM_OK;
   }
+  // PreparePuffs before the first stage's scalars (src/scalars.f90:217),
+  // and the clearing of the scalars a restarting puff asks for
+  void launch_puff_prep() {
+    bool puffs = false, clear = false;
+    for (int d = 0; d < nd; d++) {
+      puffs |= hdom[d].npuff > 0;
+      clear |= hdom[d].puff_clear_any != 0;
+    }
+    if (!puffs) return;
+    nlaunch++;
+    k_puff_step<T><<<(nd + 127) / 128, 128, 0, stream>>>(ddom, nd);
+    if (clear) {
+      nlaunch++;
+      k_puff_clear<T><<<148 * 4, 256, 0, stream>>>(ddom, nd);
+    }
+  }
   int enqueue_step(bool cfl, bool div) {
     if (cfl) launch_cfl();
     bool vdt = false;
@@ -1520,19 +1536,7 @@ struct BatchT {
       nlaunch++;
       k_dt<T><<<(nd + 127) / 128, 128, 0, stream>>>(ddom, nd);
     }
-    bool puffs = false, clear = false;
-    for (int d = 0; d < nd; d++) {
-      puffs |= hdom[d].npuff > 0;
-      clear |= hdom[d].puff_clear_any != 0;
-    }
-    if (puffs) {  // PreparePuffs before the first stage's scalars (src/scalars.f90:217)
-      nlaunch++;
-      k_puff_step<T><<<(nd + 127) / 128, 128, 0, stream>>>(ddom, nd);
-      if (clear) {
-        nlaunch++;
-        k_puff_clear<T><<<148 * 4, 256, 0, stream>>>(ddom, nd);
-      }
-    }
+    launch_puff_prep();
     for (int s = 1; s <= 3; s++) run_stage(s, 3, s == 3, false, div && s == 3);
     if (div && !any_solids()) launch_divmax();
     return ELMM_OK;
@@ -1672,7 +1676,11 @@ struct BatchT {
   // ------------------------------------------------------------ puffs
   // elmm_set_puffs: windows and volumes into the descriptor, the state (last
   // release -huge, as PuffSource%last_start starts) and the clock on the device
-  int set_puffs(int d, const elmm_puff *pf, int np, const elmm_puff_volume *vol, int nv) {
+  // cvol, ncv: the volumes whose puffs' clear flags pick the scalars a
+  // restart clears (a slab of a split domain: the whole domain's volumes,
+  // its own ones elsewhere); the volumes' own list by default
+  int set_puffs(int d, const elmm_puff *pf, int np, const elmm_puff_volume *vol, int nv,
+                const elmm_puff_volume *cvol = nullptr, int ncv = 0) {
     CU(cudaSetDevice(device));
     CU(cudaStreamSynchronize(stream));
     Dom<T> &h = hdom[d];
@@ -1717,8 +1725,17 @@ struct BatchT {
       h.pv_j[q] = vol[q].yj;
       h.pv_k[q] = vol[q].zk;
       h.pv_q[q] = vol[q].flux;
-      if (pf[vol[q].puff].clear) {
-        h.puff_clear_slots[vol[q].puff] |= 1u << slot;
+    }
+    if (!cvol) {
+      cvol = vol;
+      ncv = nv;
+    }
+    for (int q = 0; q < ncv; q++) {
+      const elmm_puff_volume &v = cvol[q];
+      if (v.puff < 0 || v.puff >= np || v.scalar_number < 1 || v.scalar_number > c.num_scalars)
+        return fail(ELMM_ERR_INVALID_ARG, "puff volume: puff index or scalar out of range");
+      if (pf[v.puff].clear) {
+        h.puff_clear_slots[v.puff] |= 1u << ((h.buoy ? 1 : 0) + v.scalar_number - 1);
         h.puff_clear_any = 1;
       }
     }

@@ -70,8 +70,6 @@ struct SlabsT {
     if (r) return r;
     if (n < 1 || n > ELMM_MAX_SLABS) return fail(ELMM_ERR_INVALID_ARG, "nslabs in 1.." + std::to_string(ELMM_MAX_SLABS));
     if (c.Btype[ELMM_BO] == ELMM_BC_PERIODIC) return fail(ELMM_ERR_INVALID_CONFIG, "split domains need walls in z (periodic z is not built)");
-    if (c.avg_slice_k > 0 || c.avg_slice_j > 0)
-      return fail(ELMM_ERR_INVALID_CONFIG, "split domains keep no time-averaged slices");
     if (c.variable_time_steps) return fail(ELMM_ERR_INVALID_CONFIG, "split domains take constant time steps");
     if (c.max_refine_sweeps > 0) return fail(ELMM_ERR_INVALID_CONFIG, "split domains take no defect-correction sweeps");
     ns = n;
@@ -119,6 +117,8 @@ struct SlabsT {
       if (s < n - 1) cs.Btype[ELMM_TO] = cs.TempBtype[ELMM_TO] = cs.ScalBtype[ELMM_TO] = BC_HALO;
       cs.zW = c.zW ? c.zW + k0[s] : nullptr;
       cs.zmin = c.zmin + k0[s] * c.dzmin;
+      // the xy slice in the slab holding its level (the xz slice in every slab)
+      cs.avg_slice_k = c.avg_slice_k > k0[s] && c.avg_slice_k <= k0[s] + nzl[s] ? c.avg_slice_k - k0[s] : 0;
       // the point sources whose cell of the whole domain lies in this slab
       cs.num_point_sources = 0;
       for (int q = 0; q < c.num_point_sources; q++) {
@@ -372,7 +372,7 @@ struct SlabsT {
     // ScalarRK3 between Convection and the projection (src/tsteps.f90:132-135)
     each([&](int, BatchT<T> &B) {
       B.launch_momentum(st);
-      B.launch_scalars(st, 0);
+      B.launch_scalars(st, st == 3);
     });
     cps.clear();
     halo_copies(cps, {F_W2}, true, false);
@@ -387,6 +387,7 @@ struct SlabsT {
     CU(cudaEventRecord(ev_fork, sl[0]->stream));
     for (int s = 1; s < ns; s++) CU(cudaStreamWaitEvent(sl[s]->stream, ev_fork, 0));
     if (cfl) each([&](int, BatchT<T> &B) { B.launch_cfl(); });
+    each([&](int, BatchT<T> &B) { B.launch_puff_prep(); });
     int r = ELMM_OK;
     for (int st = 1; st <= 3 && !r; st++) r = stage(st);
     if (r) return r;
@@ -440,6 +441,7 @@ struct SlabsT {
     if (r) return r;
     for (int n = 0; n < nsteps; n++) {
       if (cfl) each([&](int, BatchT<T> &B) { B.launch_cfl(); });
+      each([&](int, BatchT<T> &B) { B.launch_puff_prep(); });
       for (int st = 1; st <= 3 && !r; st++) r = stage(st);
       if (r) return r;
       if (n == nsteps - 1) each([&](int, BatchT<T> &B) { B.launch_divmax(); });
@@ -636,6 +638,36 @@ struct SlabsT {
     }
     return ELMM_OK;
   }
+  // puff sources (elmm_set_puffs): every slab runs every puff's windows, and
+  // takes the volumes in its levels
+  int set_puffs(const elmm_puff *pf, int np, const elmm_puff_volume *vol, int nv) {
+    if (nv < 0 || nv > kMaxPuffVols || (nv > 0 && !vol)) return fail(ELMM_ERR_INVALID_ARG, "puff volumes");
+    if (step_exec) { cudaGraphExecDestroy(step_exec); step_exec = nullptr; }
+    for (int s = 0; s < ns; s++) {
+      std::vector<elmm_puff_volume> mine;
+      for (int q = 0; q < nv; q++)
+        if (vol[q].zk > k0[s] && vol[q].zk <= k0[s] + nzl[s]) {
+          elmm_puff_volume v = vol[q];
+          v.zk -= k0[s];
+          mine.push_back(v);
+        }
+      int r = sl[s]->set_puffs(0, pf, np, mine.data(), (int)mine.size(), vol, nv);  // a restart clears every slab
+      if (r) return r;
+    }
+    return ELMM_OK;
+  }
+  // the time-averaged slices of scalar sc: xy from the slab holding its
+  // level, xz(1:Prnx, 1:Prnz) row blocks from every slab
+  int download_scalar_slices(int sc, double *xy, double *xz) {
+    for (int s = 0; s < ns; s++) {
+      const bool has_xy = sl[s]->cfg[0].avg_slice_k > 0;
+      int r = sl[s]->download_scalar_slices(0, sc, has_xy ? xy : nullptr,
+                                           xz ? xz + (size_t)sl[s]->hdom[0].nx * k0[s] : nullptr);
+      if (r) return r;
+    }
+    if (xy && gcfg.avg_slice_k <= 0) return fail(ELMM_ERR_INVALID_ARG, "no such slice (avg_slice_k is 0)");
+    return ELMM_OK;
+  }
   // ELMM_FIELD_TEMPERATURE or ELMM_FIELD_SCALAR + sc - 1 into the whole
   // domain's host array, every element the single-domain download writes
   int download_field(int field, double *host) {
@@ -742,6 +774,17 @@ extern "C" int elmm_slabs_upload_scalar(elmm_slabs *h, int32_t sc, const double 
 extern "C" int elmm_slabs_download_field(elmm_slabs *h, int32_t field, double *host) {
   if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
   return SLAB_DISPATCH(h, download_field(field, host));
+}
+
+extern "C" int elmm_slabs_set_puffs(elmm_slabs *h, const elmm_puff *puffs, int32_t npuffs,
+                                    const elmm_puff_volume *volumes, int32_t nvolumes) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  return SLAB_DISPATCH(h, set_puffs(puffs, npuffs, volumes, nvolumes));
+}
+
+extern "C" int elmm_slabs_download_scalar_slices(elmm_slabs *h, int32_t sc, double *xy, double *xz) {
+  if (!h) return fail(ELMM_ERR_INVALID_ARG, "NULL handle");
+  return SLAB_DISPATCH(h, download_scalar_slices(sc, xy, xz));
 }
 
 extern "C" int elmm_slabs_project(elmm_slabs *h, double coef, elmm_stats *stats) {

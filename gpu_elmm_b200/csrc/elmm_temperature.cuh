@@ -573,6 +573,13 @@ __global__ void k_puff_clear(const Dom<T> *__restrict__ doms, int nd) {
       T *F = d.slot[s].buf[0];
       for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
         F[q] = (T)(0.0 - d.slot[s].off);
+      for (int side = 0; side < 2; side++) {  // a slab's second halo planes (every slab clears at once)
+        T *H = d.slot[s].h2[side];
+        if (!H) continue;
+        for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < d.plane;
+             q += (long long)gridDim.x * blockDim.x)
+          H[q] = (T)(0.0 - d.slot[s].off);
+      }
     }
   }
 }

@@ -111,6 +111,8 @@ def lib():
         L.elmm_slabs_upload_temperature.argtypes = [P, _dp]
         L.elmm_slabs_upload_scalar.argtypes = [P, C.c_int32, _dp]
         L.elmm_slabs_download_field.argtypes = [P, C.c_int32, _dp]
+        L.elmm_slabs_set_puffs.argtypes = [P, P, C.c_int32, P, C.c_int32]
+        L.elmm_slabs_download_scalar_slices.argtypes = [P, C.c_int32, _dp, _dp]
         L.elmm_slabs_upload_state_float.argtypes = [P, fp, fp, fp, fp]
         L.elmm_slabs_download_state_float.argtypes = [P, fp, fp, fp, fp]
         L.elmm_slabs_march_host_float.argtypes = [P, fp, fp, fp, fp, C.c_int32, C.POINTER(ElmmStats)]
@@ -444,6 +446,21 @@ class Slabs:
 
     def scalar(self, sc):
         return self.field(FIELD_SCALAR + sc - 1)
+
+    def set_puffs(self, puffs, volumes):
+        """Puff sources as Domain.set_puffs (cells of the whole domain)."""
+        from .config import make_puffs
+        P, n_p, V, n_v = make_puffs(puffs, volumes)
+        check(lib().elmm_slabs_set_puffs(self.h, C.cast(P, C.c_void_p), n_p, C.cast(V, C.c_void_p), n_v),
+              "elmm_slabs_set_puffs")
+        self._puffs = (P, V)
+
+    def scalar_slices(self, sc):
+        g = self.grid
+        xy = np.zeros((g.Prny, g.Prnx)) if self.cfg.avg_slice_k > 0 else None
+        xz = np.zeros((g.Prnz, g.Prnx)) if self.cfg.avg_slice_j > 0 else None
+        check(lib().elmm_slabs_download_scalar_slices(self.h, sc, ptr(xy), ptr(xz)), "elmm_slabs_download_scalar_slices")
+        return xy, xz
 
     def march_host(self, U, V, W, Pr, n=1) -> ElmmStats:
         """elmm_slabs_march_host: the arrays are updated in place."""

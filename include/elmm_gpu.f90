@@ -359,6 +359,17 @@ module elmm_gpu
       integer(c_int32_t), value :: field
       real(c_double) :: host(*)
     end function
+    integer(c_int) function elmm_slabs_set_puffs(h, puffs, npuffs, volumes, nvolumes) bind(C)
+      import
+      type(c_ptr), value :: h, puffs, volumes
+      integer(c_int32_t), value :: npuffs, nvolumes
+    end function
+    integer(c_int) function elmm_slabs_download_scalar_slices(h, sc, xy, xz) bind(C)
+      import
+      type(c_ptr), value :: h
+      integer(c_int32_t), value :: sc
+      type(c_ptr), value :: xy, xz
+    end function
     integer(c_int) function elmm_slabs_project(h, coef, st) bind(C)
       import
       type(c_ptr), value :: h

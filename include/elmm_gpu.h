@@ -646,10 +646,10 @@ double elmm_server_now(const elmm_server *s);
  * the spectral buffer never crosses between GPUs.  The result equals the
  * single-domain handle's to rounding.
  *
- * Built for the flow, the temperature and passive scalars (with point
- * sources): walls in z (no periodic z), constant dt, no solid bodies,
- * puffs, time-averaged slices or defect-correction sweeps
- * (ELMM_ERR_INVALID_CONFIG otherwise).  The slabs also exchange the
+ * Built for the flow, the temperature and passive scalars (point and puff
+ * sources, time-averaged slices): walls in z (no periodic z), constant dt,
+ * no solid bodies or defect-correction sweeps (ELMM_ERR_INVALID_CONFIG
+ * otherwise).  The slabs also exchange the
  * scalars' two planes beyond each shared face (KappaScalar's stencil) and
  * the diffusivity's ghost plane.  nz_slab may be NULL for an even
  * split; every slab needs at least 4 levels, and the levels must add up to
@@ -671,6 +671,12 @@ int elmm_slabs_download_state(elmm_slabs *h, double *U, double *V, double *W, do
 int elmm_slabs_upload_temperature(elmm_slabs *h, const double *T);
 int elmm_slabs_upload_scalar(elmm_slabs *h, int32_t sc, const double *S);
 int elmm_slabs_download_field(elmm_slabs *h, int32_t field, double *host);
+/* Puff sources (as elmm_set_puffs; the volumes' cells are the whole
+ * domain's) and the time-averaged slices of scalar sc (as
+ * elmm_download_scalar_slices: the xz slice assembled from every slab). */
+int elmm_slabs_set_puffs(elmm_slabs *h, const elmm_puff *puffs, int32_t npuffs, const elmm_puff_volume *volumes,
+                         int32_t nvolumes);
+int elmm_slabs_download_scalar_slices(elmm_slabs *h, int32_t sc, double *xy, double *xz);
 /* PressureCorrection on the uploaded state, as elmm_project. */
 int elmm_slabs_project(elmm_slabs *h, double coef, elmm_stats *stats);
 /* nsteps RK3 steps, as elmm_step: with every slab on one device each step

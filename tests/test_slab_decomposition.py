@@ -102,8 +102,8 @@ def test_slab_entry_points_check_their_arguments_first():
     assert lib.elmm_slabs_create(C.byref(cfg), 2, None, nz, C.byref(h)) == 6            # 14 != 16 levels
     nz = (C.c_int32 * 2)(13, 3)
     assert lib.elmm_slabs_create(C.byref(cfg), 2, None, nz, C.byref(h)) == 6            # a slab under 4 levels
-    sliced = make_config(32, 32, 16, num_scalars=1, avg_slice_k=3, avg_weight=0.1)
-    assert lib.elmm_slabs_create(C.byref(sliced), 2, None, None, C.byref(h)) == 1       # averaged slices: not built
+    refine = make_config(32, 32, 16, precision=1, max_refine_sweeps=2)
+    assert lib.elmm_slabs_create(C.byref(refine), 2, None, None, C.byref(h)) == 1       # defect correction: not built
     per = make_config(32, 32, 16, btype=(3, 3, 3, 3, 3, 3))
     assert lib.elmm_slabs_create(C.byref(per), 2, None, None, C.byref(h)) == 1          # periodic z: not built
     for f in (lib.elmm_slabs_destroy(None), lib.elmm_slabs_upload_state(None, None, None, None, None),
