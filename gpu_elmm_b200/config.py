@@ -134,7 +134,7 @@ class ElmmWMPoint(C.Structure):
     _fields_ = [
         ("component", C.c_int32), ("direction", C.c_int32),
         ("xi", C.c_int32), ("yj", C.c_int32), ("zk", C.c_int32), ("reserved", C.c_int32),
-        ("dist", C.c_double * 3), ("z0", C.c_double),
+        ("dist", C.c_double * 3), ("z0", C.c_double), ("temperature_flux", C.c_double),
     ]
 
 
@@ -147,6 +147,7 @@ class ElmmSolids(C.Structure):
         ("n_bottom_skip", C.c_int64 * 3), ("bottom_skip_ij", C.POINTER(C.c_int32) * 3),
         ("n_solid_pr", C.c_int64), ("solid_pr_ijk", C.POINTER(C.c_int32)),
         ("n_wm_pr", C.c_int64), ("wm_pr_ijk", C.POINTER(C.c_int32)),
+        ("n_heat_pr", C.c_int64), ("heat_pr_ijk", C.POINTER(C.c_int32)), ("heat_pr_q", C.POINTER(C.c_double)),
     ]
 
 

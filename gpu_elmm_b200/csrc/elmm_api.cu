@@ -399,6 +399,9 @@ struct BatchT {
     // the temperature's fill of the solid cells (k_theta_fill)
     FillCell *fill = nullptr;
     int nfill = 0;
+    // the heated Pr wall-model points at solid faces (k_heat_add)
+    HeatPoint *heat = nullptr;
+    int nheat = 0;
     bool on = false, primed = false;
   };
   std::vector<SolidSet> sol;
@@ -1279,7 +1282,15 @@ struct BatchT {
         launch_scalar_pair(stage);
       }
     }
-    // the temperature's fill of the solid cells (src/scalars.f90:129-198)
+    // the heat flux of the solid faces, then the fill of the solid cells
+    // (src/scalars.f90:129-198)
+    for (int d = 0; d < nd && d < (int)sol.size(); d++)
+      if (sol[d].on && sol[d].nheat > 0) {
+        nlaunch++;
+        k_heat_add<T><<<std::min((sol[d].nheat + 255) / 256, 148 * 4), 256, 0, stream>>>(ddom, d, sol[d].heat,
+                                                                                        sol[d].nheat, stage,
+                                                                                        kBeta[stage - 1]);
+      }
     for (int d = 0; d < nd && d < (int)sol.size(); d++)
       if (sol[d].on && sol[d].nfill > 0) {
         nlaunch++;
@@ -1748,7 +1759,7 @@ struct BatchT {
     if (d >= (int)sol.size()) return;
     SolidSet &x = sol[d];
     for (void *p : {(void *)x.vel, (void *)x.visc, (void *)x.wm, (void *)x.wm_ustar, (void *)x.bskip[0],
-                    (void *)x.bskip[1], (void *)x.bskip[2], (void *)x.null, (void *)x.pmask, (void *)x.fill})
+                    (void *)x.bskip[1], (void *)x.bskip[2], (void *)x.null, (void *)x.pmask, (void *)x.fill, (void *)x.heat})
       if (p) dfree(p);
     x = SolidSet();
     for (int c = 0; c < 3; c++) hdom[d].bskip[c] = nullptr;
@@ -1941,6 +1952,9 @@ struct BatchT {
       w.k = p.zk;
       for (int a = 0; a < 3; a++) w.dist[a] = p.dist[a];
       w.z0 = p.z0;
+      w.tflux = p.temperature_flux;
+      if (!std::isfinite(w.tflux) || (w.tflux != 0 && !c.enable_buoyancy))
+        return fail(ELMM_ERR_INVALID_ARG, "a solid face's heat flux needs the temperature field");
       if (!(norm_host(w.dist) > 0)) return fail(ELMM_ERR_INVALID_ARG, "wall-model point on the wall");
       wm.push_back(w);
     }
@@ -2010,6 +2024,21 @@ struct BatchT {
       h.pmask = x.pmask;
     }
     if (c.enable_buoyancy && (r = build_fill(d, s))) return r;
+    if (s->n_heat_pr < 0 || (s->n_heat_pr > 0 && (!s->heat_pr_ijk || !s->heat_pr_q)) ||
+        (s->n_heat_pr > 0 && !c.enable_buoyancy))
+      return fail(ELMM_ERR_INVALID_ARG, "heated Pr wall-model points (they need the temperature field)");
+    if (s->n_heat_pr > 0) {
+      std::vector<HeatPoint> hp;
+      for (int64_t q = 0; q < s->n_heat_pr; q++) {
+        const int32_t *t = s->heat_pr_ijk + 3 * q;
+        if (t[0] < 1 || t[0] > h.nx || t[1] < 1 || t[1] > h.ny || t[2] < 1 || t[2] > h.nz ||
+            !std::isfinite(s->heat_pr_q[q]))
+          return fail(ELMM_ERR_INVALID_ARG, "heated Pr wall-model point out of range");
+        hp.push_back(HeatPoint{bidx(h, t[0], t[1], t[2]), s->heat_pr_q[q]});
+      }
+      if ((r = up((void **)&x.heat, hp.data(), hp.size() * sizeof(HeatPoint)))) return r;
+      x.nheat = (int)hp.size();
+    }
     x.on = true;
     x.primed = false;
     return push_dom(d);

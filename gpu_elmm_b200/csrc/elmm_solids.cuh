@@ -31,6 +31,7 @@ struct WMSolid {
   int comp, dir, k, pad;
   double dist[3];
   double z0;
+  double tflux;  // the body's heat flux (with a temperature)
 };
 
 // mode 0: the gathers (after the projection, and the first IBMomentum of a
@@ -118,7 +119,10 @@ __global__ void __launch_bounds__(128) k_ib_wm(const Dom<T> *__restrict__ doms, 
     for (int m = 0; m < 3; m++) t[m] = t[m] - dot * dist[m] / (dd * dd);
     const double tv = norm2_3(t);
     double us = ustar_state[q];
-    if (tv != 0) us = wm_ustar(us, tv, dd, p.z0, d.nu_mol);
+    if (p.z0 > 0 && d.buoy && p.tflux > 0)  // WM_MO_FluxStress (src/wallmodels.f90:1836-1854, 2255-2259)
+      us = tv != 0 ? wm_mo_flux_ustar(us, tv, dd, p.z0, p.tflux, d.tref, d.grav, d.nu_mol) : 0.0;
+    else if (tv != 0)
+      us = wm_ustar(us, tv, dd, p.z0, d.nu_mol);
     if (us < 0) us = 0;
     ustar_state[q] = us;
     if (ustar_only) continue;
@@ -194,6 +198,27 @@ __global__ void __launch_bounds__(128) k_ib_wm(const Dom<T> *__restrict__ doms, 
     T *S2 = comp == 0 ? d.U2 : comp == 1 ? d.V2 : d.W2;
     atomicAdd(S + c, (T)delta);
     atomicAdd(S2 + c, (T)(beta_dt * delta));
+  }
+}
+
+// The heat flux of the Pr wall-model points at solid faces
+// (TemperatureExtra, src/scalars.f90:323-327) after a temperature stage: q
+// = temperature_flux x area_factor joins the stage tendency of its cell, and
+// beta dt of it the new value (the RK combine is linear in the tendency).
+struct HeatPoint {
+  long long c;
+  double q;
+};
+template <typename T>
+__global__ void k_heat_add(const Dom<T> *__restrict__ doms, int di, const HeatPoint *__restrict__ pts, int n,
+                           int stage, double beta) {
+  const Dom<T> &d = doms[di];
+  T *A = d.slot[0].adv, *S = d.slot[0].buf[stage % 3];
+  const double bdt = beta * d.dt;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    const HeatPoint p = pts[q];
+    A[p.c] = (T)((double)A[p.c] + p.q);
+    S[p.c] = (T)((double)S[p.c] + bdt * p.q);
   }
 }
 

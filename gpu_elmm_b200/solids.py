@@ -64,6 +64,7 @@ class Box:
     z0: float
     z1: float
     z0r: float = 0.1
+    heat_flux: float = 0.0
 
     def planes(self):
         # (axis, offset, gl): gl -> coordinate - offset >= -eps, else <= eps
@@ -116,6 +117,7 @@ class Sphere:
     zc: float
     r: float
     z0r: float = 0.1
+    heat_flux: float = 0.0
 
     def inside(self, x, y, z, eps):
         """Sphere_Inside (:1128-1134)."""
@@ -157,6 +159,7 @@ class Cylinder:
     r: float
     z0r: float = 0.1
     infinite: bool = False
+    heat_flux: float = 0.0
 
     def __post_init__(self):
         x1, y1, z1 = (float(v) for v in self.p1)
@@ -629,7 +632,9 @@ class Geometry:
                             dv = dv2
                     if math.sqrt(dv[0] ** 2 + dv[1] ** 2 + dv[2] ** 2) < mwd:
                         raise ValueError(f"wall-model point too close to the wall: {comp} {(i, j, k)}")
-                    out.append((comp, dr, i, j, k, tuple(dv), b.z0r if b.z0r > 0 else 0.0))
+                    rough = b.z0r > 0  # a rough body's points carry its z0 and heat flux
+                    out.append((comp, dr, i, j, k, tuple(dv), b.z0r if rough else 0.0,
+                                b.heat_flux if rough else 0.0))
         return out
 
     def solid_pr(self):
@@ -661,6 +666,57 @@ class Geometry:
         k, j, i = np.nonzero(pts)
         return np.stack([i + 1, j + 1, k + 1], axis=1).astype(np.int32) if len(i) else np.zeros((0, 3), np.int32)
 
+    def heat_pr(self):
+        """The Pr wall-model points at solid faces that carry a heat flux:
+        (i, j, k, temperature_flux x area_factor).  GetSolidBodiesWM
+        (src/immersedboundary.f90:14-138) gives a free cell with solid
+        6-neighbours the nearest of their bodies (Closest, in the order -x,
+        +x, -y, +y, -z, +z) and that body's flux if it is rough;
+        ComputeAreaFactor (src/wallmodels.f90:173-203) the boundary area over
+        the cell volume along the distance's dominant axis.  A cell that is
+        also a point of a no-slip bottom keeps one of the two
+        (RemoveDuplicateWMPoints, src/wallmodels.f90:373-410: the one closer
+        to its wall; on a tie the solid-face point, the first added, which
+        a stable sort keeps first)."""
+        g, cfg, c = self.g, self.cfg, self.c
+        nx, ny, nz = g.Prnx, g.Prny, g.Prnz
+        dzmin = c.dzmin
+        out = []
+        for k in range(1, nz + 1):
+            for j in range(1, ny + 1):
+                for i in range(1, nx + 1):
+                    if self.typ(0, i, j, k) > 0:
+                        continue
+                    nb, dist, dv = 0, math.inf, None
+                    x, y, z = c.x(c.xPr, i), c.x(c.yPr, j), c.x(c.zPr, k)
+                    for m, n, o in ((1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)):
+                        t = self.typ(0, i + m, j + n, k + o)
+                        if t > 0 and t != nb:
+                            near = self.closest(self.boxes[t - 1], x, y, z)
+                            dd = math.sqrt((near[0] - x) ** 2 + (near[1] - y) ** 2 + (near[2] - z) ** 2)
+                            if dd < dist:
+                                dist, nb, dv = dd, t, (near[0] - x, near[1] - y, near[2] - z)
+                    if nb == 0:
+                        continue
+                    b = self.boxes[nb - 1]
+                    flux = b.heat_flux if b.z0r > 0 else 0.0
+                    if k == 1 and cfg.Btype[4] == BC_NOSLIP and self.typ(0, i, j, k) == 0:
+                        dz = c.x(c.zW, 0) - z
+                        if dz * dz < dv[0] ** 2 + dv[1] ** 2 + dv[2] ** 2:
+                            continue  # the bottom point is closer: it is kept (no flux at an adiabatic wall)
+                    if flux == 0:
+                        continue
+                    on = [abs(-v) / dist for v in dv]
+                    if on[0] > on[1] and on[0] > on[2]:
+                        o, d = on[0], math.sqrt(cfg.dymin * dzmin)
+                    elif on[1] > on[0] and on[1] > on[2]:
+                        o, d = on[1], math.sqrt(cfg.dxmin * dzmin)
+                    else:
+                        o, d = on[2], math.sqrt(cfg.dxmin * cfg.dymin)
+                    af = d * (d / o) / (cfg.dxmin * cfg.dymin * dzmin)
+                    out.append((i, j, k, flux * af))
+        return out
+
     def bottom_skip(self, q):
         (nx, ny, nz), _, _, _ = self.grids[q]
         t = self.types[q]
@@ -690,6 +746,7 @@ class Solids:
     bottom_skip: list = field(default_factory=lambda: [np.zeros((0, 2), np.int32)] * 3)
     solid_pr: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.int32))
     wm_pr: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.int32))
+    heat_pr: list = field(default_factory=list)
 
     def struct(self) -> ElmmSolids:
         """The elmm_solids view; the arrays stay referenced by this object."""
@@ -713,10 +770,11 @@ class Solids:
         s.n_scalfl = len(self.scalfl)
         s.scalfl = C.cast(a, C.POINTER(ElmmIBPoint))
         w = (ElmmWMPoint * max(1, len(self.wm)))()
-        for n, (comp, dr, i, j, k, dv, z0) in enumerate(self.wm):
+        for n, (comp, dr, i, j, k, dv, z0, tf) in enumerate(self.wm):
             w[n].component, w[n].direction, w[n].xi, w[n].yj, w[n].zk = comp, dr, i, j, k
             w[n].dist[0], w[n].dist[1], w[n].dist[2] = dv
             w[n].z0 = z0
+            w[n].temperature_flux = tf
         self._keep.append(w)
         s.n_wm = len(self.wm)
         s.wm = C.cast(w, C.POINTER(ElmmWMPoint))
@@ -725,6 +783,12 @@ class Solids:
             self._keep.append(a)
             setattr(s, "n_" + name, len(a) // 3)
             setattr(s, name + "_ijk", a.ctypes.data_as(C.POINTER(C.c_int32)))
+        hi = np.ascontiguousarray([p[:3] for p in self.heat_pr], dtype=np.int32).reshape(-1)
+        hq = np.ascontiguousarray([p[3] for p in self.heat_pr], dtype=np.float64)
+        self._keep += [hi, hq]
+        s.n_heat_pr = len(self.heat_pr)
+        s.heat_pr_ijk = hi.ctypes.data_as(C.POINTER(C.c_int32))
+        s.heat_pr_q = hq.ctypes.data_as(C.POINTER(C.c_double))
         return s
 
     def counts(self) -> dict:
@@ -751,5 +815,6 @@ def build_solids(cfg: ElmmConfig, boxes) -> Solids:
     s.bottom_skip = [g.bottom_skip(q) for q in (1, 2, 3)]
     s.solid_pr = g.solid_pr()
     s.wm_pr = g.wm_pr()
+    s.heat_pr = g.heat_pr() if any(b.heat_flux != 0 for b in boxes) else []
     s.geometry = g
     return s

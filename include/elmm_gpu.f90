@@ -57,7 +57,7 @@ module elmm_gpu
 
   type, bind(C) :: elmm_wm_point            ! WMPointUVW at a solid face
     integer(c_int32_t) :: component, direction, xi, yj, zk, reserved
-    real(c_double)     :: dist(3), z0
+    real(c_double)     :: dist(3), z0, temperature_flux
   end type
 
   type, bind(C) :: elmm_solids
@@ -75,6 +75,9 @@ module elmm_gpu
     type(c_ptr)        :: solid_pr_ijk       ! Prtype > 0 cells (passive scalars)
     integer(c_int64_t) :: n_wm_pr
     type(c_ptr)        :: wm_pr_ijk          ! Pr wall-model points of the scalars
+    integer(c_int64_t) :: n_heat_pr
+    type(c_ptr)        :: heat_pr_ijk        ! heated Pr wall-model points at solid faces
+    type(c_ptr)        :: heat_pr_q          ! their temperature_flux x area_factor
   end type
 
   type, bind(C) :: elmm_config

@@ -303,12 +303,16 @@ typedef struct elmm_ib_point {
  * point of `component` (1 U, 2 V, 3 W) whose neighbour in `direction`
  * (1..6 = -x, +x, -y, +y, -z, +z) is solid; dist is the vector to the
  * nearest point of the body, z0 its roughness length (> 0; 0 for a smooth
- * face, which needs a positive molecular viscosity). */
+ * face, which needs a positive molecular viscosity), temperature_flux the
+ * body's heat flux (SolidBody%temperature_flux of a rough body; with a
+ * temperature, a flux into the flow makes the point's u* follow
+ * WM_MO_FluxStress). */
 typedef struct elmm_wm_point {
   int32_t component, direction;
   int32_t xi, yj, zk, reserved;
   double dist[3];
   double z0;
+  double temperature_flux;
 } elmm_wm_point;
 
 typedef struct elmm_solids {
@@ -340,6 +344,14 @@ typedef struct elmm_solids {
   const int32_t *solid_pr_ijk;
   int64_t n_wm_pr;
   const int32_t *wm_pr_ijk;
+  /* With a temperature: the Pr wall-model points at solid faces that carry
+   * a heat flux, (i, j, k) 1..n and temperature_flux x area_factor
+   * (K / s; ComputeAreaFactor, src/wallmodels.f90:173-203), which each
+   * temperature stage adds to the cell (TemperatureExtra,
+   * src/scalars.f90:323-327). */
+  int64_t n_heat_pr;
+  const int32_t *heat_pr_ijk;
+  const double *heat_pr_q;
 } elmm_solids;
 
 /* Installs the solid bodies of a single-domain handle (copied; the host

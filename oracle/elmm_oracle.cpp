@@ -193,6 +193,9 @@ struct Domain {
   // the x and y ghosts) and the Pr wall-model points of the scalars
   bool scal_solids = false;
   A3 Prsolid;
+  // temperature_flux x area_factor of the heated Pr wall-model points at
+  // solid faces (0 elsewhere)
+  A3 HeatQ;
   std::vector<std::array<int, 3>> wmprs;
   A3 T, Tadv, T2, TDiff;
   // passive scalars (ScalarRK3's loop over num_of_scalars, scalars.f90:217-223)
@@ -1099,6 +1102,7 @@ static void ScalarStage(Domain &d, int stage, double dt, A3 &Arr, A3 &Arr2, A3 &
       if (d.Prsolid(i, j - 1, k) == 0) div = div - d.V(i, j - 1, k) / d.dymin;
       if (d.Prsolid(i, j, k + 1) == 0) div = div + d.W(i, j, k) / d.dzPr(k);
       if (d.Prsolid(i, j, k - 1) == 0) div = div - d.W(i, j, k - 1) / d.dzPr(k);
+      if (sc == 0) Adv(i, j, k) = Adv(i, j, k) + d.HeatQ(i, j, k);  // temperature_flux * area_factor
       Adv(i, j, k) = Adv(i, j, k) + div * Arr(i, j, k);
     }
   for (int j = 1; j <= ny && !d.scal_solids; j++)
@@ -2193,6 +2197,11 @@ int orc_set_solids(void *h, const elmm_solids *s) {
       const int32_t *t = s->wm_pr_ijk + 3 * q;
       d.wmprs.push_back({t[0], t[1], t[2]});
     }
+    d.HeatQ.init(1, nx, 1, ny, 1, nz);
+    for (int64_t q = 0; q < s->n_heat_pr; q++) {
+      const int32_t *t = s->heat_pr_ijk + 3 * q;
+      d.HeatQ(t[0], t[1], t[2]) = s->heat_pr_q[q];
+    }
     d.scal_solids = true;
   }
   for (int c = 1; c <= 3; c++) {
@@ -2224,6 +2233,7 @@ int orc_set_solids(void *h, const elmm_solids *s) {
     p.xi = w.xi; p.yj = w.yj; p.zk = w.zk;
     p.distx = w.dist[0]; p.disty = w.dist[1]; p.distz = w.dist[2];
     p.z0 = w.z0;
+    p.temperature_flux = w.temperature_flux;
     d.wm[w.direction][w.component].push_back(p);
   }
   d.Q.init(0, d.Prnx + 1, 0, d.Prny + 1, 0, d.Prnz + 1);

@@ -61,7 +61,7 @@ def test_geometry_lists():
         (nx, ny, nz) = g.grids[q + 1][0]
         solid = int((g.types[q + 1][3:nz + 3, 3:ny + 3, 3:nx + 3] > 0).sum())
         assert solid == len(s.ib[q]) + len(s.null[q])
-    for comp, dr, i, j, k, dv, z0 in s.wm:
+    for comp, dr, i, j, k, dv, z0, _ in s.wm:
         assert g.typ(comp, i, j, k) < 0 and z0 == 0.1
         assert np.linalg.norm(dv) > 0
     # the ground next to and under the cubes has no wall-model point
@@ -157,8 +157,8 @@ def test_set_solids_rejects_what_it_cannot_apply():
     bad.ib[0][0] = (first[0], [other] + first[1][1:], first[2])
     assert code(bad) == 6
     bad = build_solids(cfg, _boxes())
-    c, dr, i, j, k, dv, z0 = bad.wm[0]
-    bad.wm[0] = (c, dr, i, j, k, dv, -1.0)
+    c, dr, i, j, k, dv, z0, tf = bad.wm[0]
+    bad.wm[0] = (c, dr, i, j, k, dv, -1.0, tf)
     assert code(bad) == 6
     assert code(s) == 0 and code(None) == 0 and code(s) == 0
     d.step(1)
@@ -277,7 +277,7 @@ def test_sphere_geometry_lists():
         h = min(2 * b.r, b.r + b.zc)
         exact += math.pi * h * h * (3 * b.r - h) / 3
     assert abs(vol - exact) / exact < 0.15, (vol, exact)
-    for comp, dr, i, j, k, dv, z0 in s.wm:
+    for comp, dr, i, j, k, dv, z0, _ in s.wm:
         assert g.typ(comp, i, j, k) < 0 and z0 in (0.1, 0.05)
         assert np.linalg.norm(dv) > 0
 
@@ -416,16 +416,22 @@ def test_mixed_passive_scalar_among_boxes():
     dm.close()
 
 
-def _theta_pair(precision=0):
+def _heated_boxes():
+    from gpu_elmm_b200.solids import Box
+    return [Box(6.0, 14.0, 5.0, 13.0, -3.0, 6.0, heat_flux=0.3), Box(22.0, 30.0, 20.0, 30.0, -3.0, 9.0),
+            Box(31.0, 34.0, 6.0, 12.0, -3.0, 4.0, heat_flux=0.15)]
+
+
+def _theta_pair(precision=0, heated=False):
     """The oracle and a library domain with the potential temperature among
-    the boxes (adiabatic walls), from the same state, projected, then given
-    the bodies."""
+    the boxes (adiabatic walls; with heated, two of them give off heat),
+    from the same state, projected, then given the bodies."""
     from gpu_elmm_b200 import lib as L
     from gpu_elmm_b200.config import FIELD_TEMPERATURE
     from gpu_elmm_b200.workloads import temperature_state
     mk = lambda p: make_config(40, 36, 20, pr_gradient_x=-2e-3, buoyancy=True, precision=p)
     cfg = mk(precision)
-    s = build_solids(cfg, _scalar_boxes())
+    s = build_solids(cfg, _heated_boxes() if heated else _scalar_boxes())
     g = grid_of(cfg)
     st = log_profile_state(g, seed=4)
     T0 = temperature_state(g, seed=4, gradient=0.02, amp=0.2)
@@ -479,6 +485,50 @@ def test_mixed_temperature_among_boxes():
     assert max(e) < 1e-5 and et < 1e-5, (e, et)
     d64.close()
     dm.close()
+
+
+def test_heated_face_points():
+    """The heated Pr wall-model points: free cells next to a heated rough
+    body, q = flux x area factor (1/dz for a face below or above the cell,
+    1/dx and 1/dy beside it on this grid), none next to the unheated body;
+    the velocity points of a heated body carry its flux."""
+    cfg = make_config(40, 36, 20, buoyancy=True)
+    s = build_solids(cfg, _heated_boxes())
+    g = s.geometry
+    assert len(s.heat_pr) > 0
+    for (i, j, k, q) in s.heat_pr:
+        assert g.typ(0, i, j, k) <= 0 and q in (0.3, 0.15), (i, j, k, q)   # unit cells: area factor 1
+    assert {tf for *_, tf in s.wm} == {0.0, 0.3, 0.15}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nsteps", [1, 5])
+def test_fp64_heated_boxes(nsteps):
+    """Heated bodies: the heat flux of the Pr wall-model points at their
+    faces enters the temperature, and the velocity points of their faces
+    take the Monin-Obukhov u* (WM_MO_FluxStress).  FP64 against the oracle:
+    U, V, W within 1e-11, P within 1e-10, theta - T_ref within 1e-11; the
+    mixed path within 1e-5 of FP64 after 3 steps."""
+    from gpu_elmm_b200.config import FIELD_TEMPERATURE
+    from gpu_elmm_b200.workloads import interior
+    g, o, d = _theta_pair(heated=True)
+    o.step(nsteps)
+    d.step(nsteps)
+    e = [rel(a, b) for a, b in zip(interiors(g, *d.download()), interiors(g, *o.state()))]
+    n = (g.Prnx, g.Prny, g.Prnz)
+    Td = interior(d.field(FIELD_TEMPERATURE), -2, n) - 295.0
+    et = rel(Td, interior(o.get_field(FIELD_TEMPERATURE), -2, n) - 295.0)
+    print("heated boxes, FP64 vs oracle after", nsteps, "steps:", e, et)
+    assert max(e[:3]) < 1e-11 and e[3] < 1e-10 and et < 1e-11, (e, et)
+    if nsteps == 5:
+        _, _, dm = _theta_pair(1, heated=True)
+        dm.step(5)
+        em = [rel(a, b) for a, b in zip(interiors(g, *dm.download())[:3], interiors(g, *d.download())[:3])]
+        etm = rel(interior(dm.field(FIELD_TEMPERATURE), -2, n) - 295.0, Td)
+        print("heated boxes, mixed vs FP64:", em, etm)
+        assert max(em) < 1e-5 and etm < 1e-5, (em, etm)
+        dm.close()
+    d.close()
 
 
 @pytest.mark.gpu
@@ -568,7 +618,7 @@ def test_cylinder_geometry_lists():
         vol += float((t0[k + 2, 3:48 + 3, 3:48 + 3] > 0).sum()) * dz
     exact = math.pi * 4.2 ** 2 * 6.0 + math.pi * 3.1 ** 2 * 14.0
     assert abs(vol - exact) / exact < 0.15, (vol, exact)
-    for comp, dr, i, j, k, dv, z0 in s.wm:
+    for comp, dr, i, j, k, dv, z0, _ in s.wm:
         assert g.typ(comp, i, j, k) < 0 and z0 in (0.1, 0.05) and np.linalg.norm(dv) > 0
 
 
