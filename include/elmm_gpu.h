@@ -359,10 +359,11 @@ typedef struct elmm_solids {
  * (ELMM_ERR_INVALID_ARG otherwise): indices in range; no interpolation point
  * of a list is a forcing point of the same list; no forcing or nullified
  * point within one cell of a periodic boundary; a no-slip bottom wall with
- * the wall model; with a temperature adiabatic bottom and top (the solid
- * faces carry no heat flux) and the Pr lists above, as for passive
- * scalars.  After each temperature stage the solid cells with fluid
- * neighbours take the mean of those (src/scalars.f90:129-198).  The next elmm_step
+ * the wall model; with a temperature adiabatic bottom and top, the Pr
+ * lists above as for passive scalars, and the heated faces' points (each
+ * body's heat flux, src/immersedboundary.f90:118, 267).  After each
+ * temperature stage the solid cells with fluid neighbours take the mean of
+ * those (src/scalars.f90:129-198).  The next elmm_step
  * applies IBMomentum once first, as the first call of TMarchRK3 does
  * (src/tsteps.f90:44-48).  Passing NULL removes the bodies. */
 int elmm_set_solids(elmm_handle *h, const elmm_solids *s);
