@@ -148,6 +148,7 @@ class ElmmSolids(C.Structure):
         ("n_solid_pr", C.c_int64), ("solid_pr_ijk", C.POINTER(C.c_int32)),
         ("n_wm_pr", C.c_int64), ("wm_pr_ijk", C.POINTER(C.c_int32)),
         ("n_heat_pr", C.c_int64), ("heat_pr_ijk", C.POINTER(C.c_int32)), ("heat_pr_q", C.POINTER(C.c_double)),
+        ("n_wall_pr", C.c_int64), ("wall_pr_ijk", C.POINTER(C.c_int32)),
     ]
 
 

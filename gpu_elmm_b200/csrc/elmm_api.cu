@@ -1847,10 +1847,11 @@ struct BatchT {
   int install_solids(int d, const elmm_solids *s) {
     Dom<T> &h = hdom[d];
     const elmm_config &c = cfg[d];
-    if (c.enable_buoyancy)
+    if (c.enable_buoyancy)  // the fill of the solid cells folds a side without wall-model points as adiabatic
       for (int side : {ELMM_BO, ELMM_TO})
-        if (c.TempBtype[side] != ELMM_BC_CONSTFLUX || c.sideTemp[side] != 0)
-          return fail(ELMM_ERR_INVALID_ARG, "solid bodies with a temperature need adiabatic bottom and top sides");
+        if (!h.wall[side] && (c.TempBtype[side] != ELMM_BC_CONSTFLUX || c.sideTemp[side] != 0))
+          return fail(ELMM_ERR_INVALID_ARG,
+                      "solid bodies with a temperature need an adiabatic side where there is no wall-model wall");
     if (!h.wall[SIDE_BO] || h.bt[SIDE_BO] != BC_NOSLIP)
       return fail(ELMM_ERR_INVALID_ARG, "solid bodies need the wall model on a no-slip bottom");
     const bool per[3] = {h.bt[SIDE_WE] == BC_PERIODIC, h.bt[SIDE_SO] == BC_PERIODIC, h.bt[SIDE_BO] == BC_PERIODIC};
@@ -2019,6 +2020,14 @@ struct BatchT {
         const int32_t *t = s->wm_pr_ijk + 3 * q;
         if (!in(t)) return fail(ELMM_ERR_INVALID_ARG, "Pr wall-model point out of range");
         m[bidx(h, t[0], t[1], t[2])] |= 2;
+      }
+      // bit 2: the wall points the deduplication keeps (they carry the wall's flux)
+      if (s->n_wall_pr < 0 || (s->n_wall_pr > 0 && !s->wall_pr_ijk))
+        return fail(ELMM_ERR_INVALID_ARG, "wall points");
+      for (int64_t q = 0; q < s->n_wall_pr; q++) {
+        const int32_t *t = s->wall_pr_ijk + 3 * q;
+        if (!in(t) || (t[2] != 1 && t[2] != h.nz)) return fail(ELMM_ERR_INVALID_ARG, "wall point out of range");
+        m[bidx(h, t[0], t[1], t[2])] |= 4;
       }
       if ((r = up((void **)&x.pmask, m.data(), m.size()))) return r;
       h.pmask = x.pmask;

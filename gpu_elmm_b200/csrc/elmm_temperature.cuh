@@ -238,11 +238,15 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 6 : 3)
       }
       if (wmc) {
         if constexpr (BC) {
-          a = a + (T)sl.wflux[k == 1 ? 0 : 1];
-          // a prescribed surface temperature: the flux of the point from the
-          // wall model of this stage (temperature slot only)
-          const double *tpr = s == 0 ? d.wm_pr_tf[k == 1 ? 0 : 1] : nullptr;
-          if (tpr) a = a + (T)(tpr[(i - 1) + (long long)nx * (j - 1)] * d.wm_af);
+          // the wall's surface flux at a wall point (with solid bodies, one
+          // the deduplication kept, bit 2 of the mask)
+          if (!d.pmask || (d.pmask[cc] & 4)) {
+            a = a + (T)sl.wflux[k == 1 ? 0 : 1];
+            // a prescribed surface temperature: the flux of the point from
+            // the wall model of this stage (temperature slot only)
+            const double *tpr = s == 0 ? d.wm_pr_tf[k == 1 ? 0 : 1] : nullptr;
+            if (tpr) a = a + (T)(tpr[(i - 1) + (long long)nx * (j - 1)] * d.wm_af);
+          }
         }
         const T dzk = (T)d.dzPr[k + 2];
         T div = (T)0;
@@ -454,9 +458,11 @@ __global__ void __launch_bounds__(SPX *SPY, ELMM_SCALAR_PAIR_MIN_BLOCKS * 8 / SP
         }
         if (wmc) {
           if constexpr (BC) {
-            a = a + (T)sl.wflux[k == 1 ? 0 : 1];
-            const double *tpr = s == 0 ? d.wm_pr_tf[k == 1 ? 0 : 1] : nullptr;
-            if (tpr) a = a + (T)(tpr[(i + c - 1) + (long long)nx * (j - 1)] * d.wm_af);
+            if (!d.pmask || (d.pmask[cc + c] & 4)) {
+              a = a + (T)sl.wflux[k == 1 ? 0 : 1];
+              const double *tpr = s == 0 ? d.wm_pr_tf[k == 1 ? 0 : 1] : nullptr;
+              if (tpr) a = a + (T)(tpr[(i + c - 1) + (long long)nx * (j - 1)] * d.wm_af);
+            }
           }
           const T dzk = (T)d.dzPr[k + 2];
           const T ue = c ? u0.y : u0.x, uw = c ? u0.x : um.y;

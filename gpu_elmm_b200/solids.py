@@ -666,12 +666,61 @@ class Geometry:
         k, j, i = np.nonzero(pts)
         return np.stack([i + 1, j + 1, k + 1], axis=1).astype(np.int32) if len(i) else np.zeros((0, 3), np.int32)
 
+    def _face_point(self, i, j, k):
+        """GetSolidBodiesWM's choice for a free cell: the nearest body among
+        its solid 6-neighbours' (Closest, in the order +x, -x, +y, -y, +z,
+        -z) and the distance vector, or (0, inf, None)."""
+        c = self.c
+        nb, dist, dv = 0, math.inf, None
+        x, y, z = c.x(c.xPr, i), c.x(c.yPr, j), c.x(c.zPr, k)
+        for m, n, o in ((1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)):
+            t = self.typ(0, i + m, j + n, k + o)
+            if t > 0 and t != nb:
+                near = self.closest(self.boxes[t - 1], x, y, z)
+                dd = math.sqrt((near[0] - x) ** 2 + (near[1] - y) ** 2 + (near[2] - z) ** 2)
+                if dd < dist:
+                    dist, nb, dv = dd, t, (near[0] - x, near[1] - y, near[2] - z)
+        return nb, dist, dv
+
+    def _wall_wins(self, i, j, k, dv):
+        """RemoveDuplicateWMPoints (src/wallmodels.f90:373-410) for a cell that
+        is a point of a no-slip z wall (Prtype == 0) and of a solid face: the
+        wall point is kept if it is strictly closer to its wall (on a tie the
+        solid-face point, the first added, which a stable sort keeps)."""
+        g, cfg, c = self.g, self.cfg, self.c
+        if self.typ(0, i, j, k) != 0:
+            return False
+        if k == 1 and cfg.Btype[4] == BC_NOSLIP:
+            dz = c.x(c.zW, 0) - c.x(c.zPr, 1)
+        elif k == g.Prnz and cfg.Btype[5] == BC_NOSLIP:
+            dz = c.x(c.zW, g.Prnz) - c.x(c.zPr, g.Prnz)
+        else:
+            return False
+        return dv is None or dz * dz < dv[0] ** 2 + dv[1] ** 2 + dv[2] ** 2
+
+    def wall_pr(self):
+        """The Pr wall-model points of the no-slip z walls that the
+        deduplication keeps (each carries its wall's temperature flux)."""
+        g, cfg = self.g, self.cfg
+        out = []
+        for k, side in ((1, 4), (g.Prnz, 5)):
+            if cfg.Btype[side] != BC_NOSLIP:
+                continue
+            for j in range(1, g.Prny + 1):
+                for i in range(1, g.Prnx + 1):
+                    if self.typ(0, i, j, k) != 0:
+                        continue
+                    nb, _, dv = self._face_point(i, j, k)
+                    if nb == 0 or self._wall_wins(i, j, k, dv):
+                        out.append((i, j, k))
+        return np.array(out, dtype=np.int32).reshape(-1, 3)
+
     def heat_pr(self):
         """The Pr wall-model points at solid faces that carry a heat flux:
         (i, j, k, temperature_flux x area_factor).  GetSolidBodiesWM
         (src/immersedboundary.f90:14-138) gives a free cell with solid
-        6-neighbours the nearest of their bodies (Closest, in the order -x,
-        +x, -y, +y, -z, +z) and that body's flux if it is rough;
+        6-neighbours the nearest of their bodies (_face_point) and that
+        body's flux if it is rough;
         ComputeAreaFactor (src/wallmodels.f90:173-203) the boundary area over
         the cell volume along the distance's dominant axis.  A cell that is
         also a point of a no-slip bottom keeps one of the two
@@ -687,23 +736,11 @@ class Geometry:
                 for i in range(1, nx + 1):
                     if self.typ(0, i, j, k) > 0:
                         continue
-                    nb, dist, dv = 0, math.inf, None
-                    x, y, z = c.x(c.xPr, i), c.x(c.yPr, j), c.x(c.zPr, k)
-                    for m, n, o in ((1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)):
-                        t = self.typ(0, i + m, j + n, k + o)
-                        if t > 0 and t != nb:
-                            near = self.closest(self.boxes[t - 1], x, y, z)
-                            dd = math.sqrt((near[0] - x) ** 2 + (near[1] - y) ** 2 + (near[2] - z) ** 2)
-                            if dd < dist:
-                                dist, nb, dv = dd, t, (near[0] - x, near[1] - y, near[2] - z)
-                    if nb == 0:
+                    nb, dist, dv = self._face_point(i, j, k)
+                    if nb == 0 or self._wall_wins(i, j, k, dv):
                         continue
                     b = self.boxes[nb - 1]
                     flux = b.heat_flux if b.z0r > 0 else 0.0
-                    if k == 1 and cfg.Btype[4] == BC_NOSLIP and self.typ(0, i, j, k) == 0:
-                        dz = c.x(c.zW, 0) - z
-                        if dz * dz < dv[0] ** 2 + dv[1] ** 2 + dv[2] ** 2:
-                            continue  # the bottom point is closer: it is kept (no flux at an adiabatic wall)
                     if flux == 0:
                         continue
                     on = [abs(-v) / dist for v in dv]
@@ -747,6 +784,7 @@ class Solids:
     solid_pr: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.int32))
     wm_pr: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.int32))
     heat_pr: list = field(default_factory=list)
+    wall_pr: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.int32))
 
     def struct(self) -> ElmmSolids:
         """The elmm_solids view; the arrays stay referenced by this object."""
@@ -778,7 +816,7 @@ class Solids:
         self._keep.append(w)
         s.n_wm = len(self.wm)
         s.wm = C.cast(w, C.POINTER(ElmmWMPoint))
-        for name, arr in (("solid_pr", self.solid_pr), ("wm_pr", self.wm_pr)):
+        for name, arr in (("solid_pr", self.solid_pr), ("wm_pr", self.wm_pr), ("wall_pr", self.wall_pr)):
             a = np.ascontiguousarray(arr, dtype=np.int32).reshape(-1)
             self._keep.append(a)
             setattr(s, "n_" + name, len(a) // 3)
@@ -816,5 +854,6 @@ def build_solids(cfg: ElmmConfig, boxes) -> Solids:
     s.solid_pr = g.solid_pr()
     s.wm_pr = g.wm_pr()
     s.heat_pr = g.heat_pr() if any(b.heat_flux != 0 for b in boxes) else []
+    s.wall_pr = g.wall_pr()
     s.geometry = g
     return s

@@ -78,6 +78,8 @@ module elmm_gpu
     integer(c_int64_t) :: n_heat_pr
     type(c_ptr)        :: heat_pr_ijk        ! heated Pr wall-model points at solid faces
     type(c_ptr)        :: heat_pr_q          ! their temperature_flux x area_factor
+    integer(c_int64_t) :: n_wall_pr
+    type(c_ptr)        :: wall_pr_ijk        ! wall points kept beside the bodies
   end type
 
   type, bind(C) :: elmm_config

@@ -352,6 +352,13 @@ typedef struct elmm_solids {
   int64_t n_heat_pr;
   const int32_t *heat_pr_ijk;
   const double *heat_pr_q;
+  /* With a temperature: the Pr wall-model points of the no-slip z walls
+   * that RemoveDuplicateWMPoints keeps (src/wallmodels.f90:373-410: the
+   * point closer to its wall, a cell next to a body keeping the solid-face
+   * point on a tie), (i, j, k) 1..n; they carry the wall's surface flux or
+   * surface temperature. */
+  int64_t n_wall_pr;
+  const int32_t *wall_pr_ijk;
 } elmm_solids;
 
 /* Installs the solid bodies of a single-domain handle (copied; the host
@@ -359,9 +366,10 @@ typedef struct elmm_solids {
  * (ELMM_ERR_INVALID_ARG otherwise): indices in range; no interpolation point
  * of a list is a forcing point of the same list; no forcing or nullified
  * point within one cell of a periodic boundary; a no-slip bottom wall with
- * the wall model; with a temperature adiabatic bottom and top, the Pr
- * lists above as for passive scalars, and the heated faces' points (each
- * body's heat flux, src/immersedboundary.f90:118, 267).  After each
+ * the wall model; with a temperature an adiabatic side where there is no
+ * wall-model wall, the Pr lists above as for passive scalars, the heated
+ * faces' points (each body's heat flux, src/immersedboundary.f90:118, 267)
+ * and the kept wall points.  After each
  * temperature stage the solid cells with fluid neighbours take the mean of
  * those (src/scalars.f90:129-198).  The next elmm_step
  * applies IBMomentum once first, as the first call of TMarchRK3 does

@@ -196,6 +196,8 @@ struct Domain {
   // temperature_flux x area_factor of the heated Pr wall-model points at
   // solid faces (0 elsewhere)
   A3 HeatQ;
+  // the wall points the deduplication keeps beside the bodies (1)
+  A3 WallPt;
   std::vector<std::array<int, 3>> wmprs;
   A3 T, Tadv, T2, TDiff;
   // passive scalars (ScalarRK3's loop over num_of_scalars, scalars.f90:217-223)
@@ -1102,7 +1104,15 @@ static void ScalarStage(Domain &d, int stage, double dt, A3 &Arr, A3 &Arr2, A3 &
       if (d.Prsolid(i, j - 1, k) == 0) div = div - d.V(i, j - 1, k) / d.dymin;
       if (d.Prsolid(i, j, k + 1) == 0) div = div + d.W(i, j, k) / d.dzPr(k);
       if (d.Prsolid(i, j, k - 1) == 0) div = div - d.W(i, j, k - 1) / d.dzPr(k);
-      if (sc == 0) Adv(i, j, k) = Adv(i, j, k) + d.HeatQ(i, j, k);  // temperature_flux * area_factor
+      if (sc == 0) {  // the kept point's temperature_flux * area_factor: the wall's, or the body's
+        double q = d.HeatQ(i, j, k);
+        if (d.WallPt(i, j, k) != 0) {
+          const int side = k == 1 ? Bo : To;
+          const size_t c = (size_t)(j - 1) * nx + i - 1;
+          q = (d.wmpr[side].empty() ? d.wm_tflux[side] : d.wmpr[side][c].temperature_flux) * d.area_factor_z;
+        }
+        Adv(i, j, k) = Adv(i, j, k) + q;
+      }
       Adv(i, j, k) = Adv(i, j, k) + div * Arr(i, j, k);
     }
   for (int j = 1; j <= ny && !d.scal_solids; j++)
@@ -2198,6 +2208,11 @@ int orc_set_solids(void *h, const elmm_solids *s) {
       d.wmprs.push_back({t[0], t[1], t[2]});
     }
     d.HeatQ.init(1, nx, 1, ny, 1, nz);
+    d.WallPt.init(1, nx, 1, ny, 1, nz);
+    for (int64_t q = 0; q < s->n_wall_pr; q++) {
+      const int32_t *t = s->wall_pr_ijk + 3 * q;
+      d.WallPt(t[0], t[1], t[2]) = 1;
+    }
     for (int64_t q = 0; q < s->n_heat_pr; q++) {
       const int32_t *t = s->heat_pr_ijk + 3 * q;
       d.HeatQ(t[0], t[1], t[2]) = s->heat_pr_q[q];

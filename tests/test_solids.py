@@ -422,14 +422,14 @@ def _heated_boxes():
             Box(31.0, 34.0, 6.0, 12.0, -3.0, 4.0, heat_flux=0.15)]
 
 
-def _theta_pair(precision=0, heated=False):
+def _theta_pair(precision=0, heated=False, **ground):
     """The oracle and a library domain with the potential temperature among
     the boxes (adiabatic walls; with heated, two of them give off heat),
     from the same state, projected, then given the bodies."""
     from gpu_elmm_b200 import lib as L
     from gpu_elmm_b200.config import FIELD_TEMPERATURE
     from gpu_elmm_b200.workloads import temperature_state
-    mk = lambda p: make_config(40, 36, 20, pr_gradient_x=-2e-3, buoyancy=True, precision=p)
+    mk = lambda p: make_config(40, 36, 20, pr_gradient_x=-2e-3, buoyancy=True, precision=p, **ground)
     cfg = mk(precision)
     s = build_solids(cfg, _heated_boxes() if heated else _scalar_boxes())
     g = grid_of(cfg)
@@ -502,6 +502,29 @@ def test_heated_face_points():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("ground", ["adiabatic", "heat-flux", "surface-temperature"])
+def test_heated_boxes_on_a_heated_ground(ground):
+    """Heated bodies on a ground with a surface heat flux or a surface
+    temperature: the bottom cells next to a body keep the wall point or the
+    solid-face point (the closer; the solid one on a tie), and the kept
+    point's flux enters.  FP64 against the oracle after 3 steps: U, V, W
+    within 1e-11, P within 1e-10, theta - T_ref within 1e-11."""
+    from gpu_elmm_b200.config import BC_CONSTFLUX, BC_DIRICHLET, FIELD_TEMPERATURE
+    from gpu_elmm_b200.workloads import interior
+    kw = {"adiabatic": {}, "heat-flux": {"heat_flux": (0.2, 0.0)},
+          "surface-temperature": {"temperature_bc": ((BC_DIRICHLET, 296.0), (BC_CONSTFLUX, 0.0))}}[ground]
+    g, o, d = _theta_pair(heated=True, **kw)
+    o.step(3)
+    d.step(3)
+    e = [rel(a, b) for a, b in zip(interiors(g, *d.download()), interiors(g, *o.state()))]
+    n = (g.Prnx, g.Prny, g.Prnz)
+    et = rel(interior(d.field(FIELD_TEMPERATURE), -2, n) - 295.0, interior(o.get_field(FIELD_TEMPERATURE), -2, n) - 295.0)
+    print("heated boxes on a", ground, "ground, FP64 vs oracle:", e, et)
+    assert max(e[:3]) < 1e-11 and e[3] < 1e-10 and et < 1e-11, (e, et)
+    d.close()
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("nsteps", [1, 5])
 def test_fp64_heated_boxes(nsteps):
     """Heated bodies: the heat flux of the Pr wall-model points at their
@@ -533,8 +556,10 @@ def test_fp64_heated_boxes(nsteps):
 
 @pytest.mark.gpu
 def test_temperature_with_bodies_needs_adiabatic_walls():
+    """A side without wall-model points (the free-slip top) must be adiabatic
+    with bodies: the fill of the solid cells folds it so."""
     from gpu_elmm_b200 import lib as L
-    cfg = make_config(40, 36, 20, buoyancy=True, heat_flux=(0.1, 0.0))
+    cfg = make_config(40, 36, 20, buoyancy=True, heat_flux=(0.0, 0.1))
     d = L.Domain(cfg)
     with pytest.raises(L.ElmmError) as e:
         d.set_solids(build_solids(cfg, _scalar_boxes()))
