@@ -221,14 +221,9 @@ static int check_config(const elmm_config &c) {
         return fail(ELMM_ERR_INVALID_CONFIG, "the temperature must be periodic where the flow is");
       // a surface flux at a wall in z is carried by its wall-model points,
       // the other kinds and sides by the ghost rules of CommonBase
-      const bool wm_wall = c.wallmodeltype > 0 && c.Btype[s] == ELMM_BC_NOSLIP && (s == ELMM_BO || s == ELMM_TO);
       if (!per && (!scalar_bc_kind(c.TempBtype[s]) || !std::isfinite(c.sideTemp[s])))
         return fail(ELMM_ERR_INVALID_CONFIG,
                     "temperature sides: ELMM_BC_CONSTFLUX, ELMM_BC_DIRICHLET or ELMM_BC_NEUMANN with a finite sideTemp");
-      if (wm_wall && c.TempBtype[s] == ELMM_BC_DIRICHLET && !(c.z0[s] > 0))
-        return fail(ELMM_ERR_INVALID_CONFIG,
-                    "a prescribed surface temperature at a wall-model wall needs a rough wall (z0 > 0): the "
-                    "Monin-Obukhov Dirichlet wall model is the rough-wall branch");
     }
     if (c.zW) return fail(ELMM_ERR_INVALID_CONFIG, "the temperature field needs a uniform z grid");
     if (c.Btype[ELMM_BO] == ELMM_BC_PERIODIC)

@@ -185,6 +185,7 @@ __device__ inline void wm_mo_dirichlet(const Dom<T> &d, double &ustar, double &t
 // the reference and is not kept.
 template <typename T>
 __device__ void wm_pr_dirichlet(const Dom<T> &d, int f, int i, int j, int k, const T *Tm) {
+  if (!(d.z0[f] > 0)) return;  // smooth wall: the flat branch leaves u* and the flux of a Pr point alone
   const long long c = bidx(d, i, j, k);
   double ou = 0, ov = 0;
   if constexpr (sizeof(T) == 4) { ou = (double)vel_off(d, 0, k); ov = (double)vel_off(d, 1, k); }

@@ -142,7 +142,10 @@ typedef struct elmm_config {
    * Dirichlet value there is a surface temperature: the Monin-Obukhov wall
    * model computes the points' u* and surface flux from the temperature
    * difference each stage (WM_MO_Dirichlet / WM_MO_DirichletStress,
-   * src/wallmodels.f90:1664-1716, 1858-1938; rough walls, z0 > 0, only).
+   * src/wallmodels.f90:1664-1716, 1858-1938) at a rough wall (z0 > 0);
+   * at a smooth wall (z0 = 0) the flat branch runs (WMFlat u*, and the
+   * points' flux keeps its initial zero, src/wallmodels.f90:2123-2146,
+   * 2265-2275).
    * Elsewhere the ghost rules of CommonBase carry the kind. */
   int32_t enable_buoyancy;      /* 0: no temperature field */
   int32_t TempBtype[6];         /* temperature BC per side (src/initial.f90:347-352) */

@@ -15,11 +15,16 @@ wall model once on the initial fields, src/initial.f90:4331-4336).
   value), for a heated rough bottom (the Monin-Obukhov u*), a cooled bottom
   with a flux through a top wall (neutral u*, the flux terms alone), a
   heated smooth bottom (z0 = 0, WMFlatStress), a surface warmer than the
-  air and, between two walls, a cool bottom and a warm top;
+  air, between two walls a cool bottom and a warm top, and a surface
+  temperature at a smooth bottom (the flat branch of ComputeViscsWM and
+  ComputeUVWFluxesWM, src/wallmodels.f90:2123-2146, 2265-2275: WMFlat u*,
+  and the points' temperature flux keeps its initial zero);
 * mixed against FP64 after one step from the same projected state:
   velocity and theta - T_ref within 1e-5;
 * the heat content grows by (q_bottom - q_top) Lx Ly per unit time on both
   paths (advection and diffusion are in flux form);
+* a smooth surface temperature exchanges no heat: the heat content stays
+  as it is on both paths;
 * a non-finite flux is refused with ELMM_ERR_INVALID_CONFIG (a flux
   through a free-slip top, which no wall-model points carry, takes
   CommonBase's ghost rule: tests/test_scalar_bcs.py).
@@ -44,6 +49,7 @@ CASES = {
     "heated-smooth": dict(heat_flux=(0.3, 0.0), z0=0.0),
     "warm-surface": dict(temperature_bc=((BC_DIRICHLET, 296.0), (BC_CONSTFLUX, 0.0))),
     "surfaces-two-walls": dict(temperature_bc=((BC_DIRICHLET, 294.0), (BC_DIRICHLET, 295.5)), btype=TWO_WALLS),
+    "warm-smooth-surface": dict(temperature_bc=((BC_DIRICHLET, 296.0), (BC_CONSTFLUX, 0.0)), z0=0.0),
 }
 
 
@@ -116,13 +122,24 @@ def test_heat_content_follows_the_surface_fluxes(precision):
     d.close()
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_smooth_surface_temperature_exchanges_no_heat(precision):
+    g, _, d = _pair("warm-smooth-surface", precision=precision)
+    d.project(1.0)
+    h0 = _theta(g, d.field(FIELD_TEMPERATURE)).sum()
+    d.step(5)
+    h1 = _theta(g, d.field(FIELD_TEMPERATURE)).sum()
+    scale = np.abs(_theta(g, d.field(FIELD_TEMPERATURE))).sum()
+    assert abs(h1 - h0) < (1e-12 if precision == 0 else 1e-5) * scale, (h1 - h0, scale)
+    d.close()
+
+
 def test_non_finite_flux_is_refused():
     with pytest.raises(L.ElmmError) as e:
         L.Domain(make_config(*N, buoyancy=True, heat_flux=(float("nan"), 0.0)))
     assert e.value.code == 1
-    # the Dirichlet wall model is the rough-wall branch
     with pytest.raises(L.ElmmError) as e:
-        L.Domain(make_config(*N, buoyancy=True, z0=0.0, temperature_bc=((BC_DIRICHLET, 296.0), (BC_CONSTFLUX, 0.0))))
+        L.Domain(make_config(*N, buoyancy=True, temperature_bc=((BC_DIRICHLET, float("inf")), (BC_CONSTFLUX, 0.0))))
     assert e.value.code == 1
     L.Domain(make_config(*N, buoyancy=True, heat_flux=(0.1, 0.0))).close()
     # a flux through the free-slip top has no wall-model points: the ghost rule carries it

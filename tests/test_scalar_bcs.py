@@ -14,9 +14,8 @@ before each stage.
   unit time, on both paths;
 * a batch of two domains with different scalar boundaries equals each
   domain run alone, bit for bit;
-* a Dirichlet temperature at a smooth wall-model wall (the Monin-Obukhov
-  Dirichlet wall model is the rough-wall branch), other kinds and
-  non-finite values are refused.
+* other kinds and non-finite values are refused; a Dirichlet temperature
+  at a smooth wall-model wall is accepted (tests/test_heat_flux.py).
 """
 import numpy as np
 import pytest
@@ -183,9 +182,7 @@ def test_batch_with_scalar_boundaries_equals_the_runs_alone(precision):
 
 def test_unsupported_scalar_boundaries_are_refused():
     walls = (3, 3, 3, 3, BC_NOSLIP, BC_NOSLIP)
-    bad = [dict(buoyancy=True, z0=0.0, temperature_bc=((BC_DIRICHLET, 300.0), (BC_CONSTFLUX, 0.0))),  # smooth wall
-           dict(buoyancy=True, btype=walls, z0=0.0, temperature_bc=((BC_CONSTFLUX, 0.0), (BC_DIRICHLET, 300.0))),
-           dict(buoyancy=True, temperature_bc=((BC_NOSLIP, 0.0), (BC_CONSTFLUX, 0.0))),
+    bad = [dict(buoyancy=True, temperature_bc=((BC_NOSLIP, 0.0), (BC_CONSTFLUX, 0.0))),
            dict(num_scalars=1, scalar_bc=((BC_CONSTFLUX, float("inf")), (BC_CONSTFLUX, 0.0)))]
     for kw in bad:
         with pytest.raises(L.ElmmError) as e:
@@ -194,3 +191,6 @@ def test_unsupported_scalar_boundaries_are_refused():
     # the same kinds where they are built
     L.Domain(make_config(*N, buoyancy=True, sgstype=0, temperature_bc=((BC_DIRICHLET, 300.0), (BC_CONSTFLUX, 0.0)))).close()
     L.Domain(make_config(*N, num_scalars=1, scalar_bc=((BC_DIRICHLET, 1.0), (BC_NEUMANN, 0.1)))).close()
+    L.Domain(make_config(*N, buoyancy=True, z0=0.0, temperature_bc=((BC_DIRICHLET, 300.0), (BC_CONSTFLUX, 0.0)))).close()
+    L.Domain(make_config(*N, buoyancy=True, btype=walls, z0=0.0,
+                         temperature_bc=((BC_CONSTFLUX, 0.0), (BC_DIRICHLET, 300.0)))).close()
