@@ -1792,9 +1792,11 @@ struct BatchT {
   // 6-neighbour in range -1..n+2, each with its fluid neighbours' cells, a
   // ghost cell through the rules of BoundTemperature for adiabatic sides
   // (x, y periodic; z mirrored at a wall-model wall, the first level
-  // otherwise).
+  // otherwise).  A body whose fill reads the ghost cell of a side with a
+  // heat flux or a prescribed value and no wall-model points is refused.
   int build_fill(int d, const elmm_solids *s) {
     Dom<T> &h = hdom[d];
+    const elmm_config &cf = cfg[d];
     SolidSet &x = sol[d];
     const int nx = h.nx, ny = h.ny, nz = h.nz, ex = nx + 4, ey = ny + 4, ez = nz + 4;
     auto at = [&](int i, int j, int k) { return (size_t)(i + 1) + (size_t)ex * ((size_t)(j + 1) + (size_t)ey * (k + 1)); };
@@ -1824,6 +1826,10 @@ struct BatchT {
           for (auto &o : nb) {
             const int a = i + o[0], b = j + o[1], e = k + o[2];
             if (solid[at(a, b, e)]) continue;
+            const int zs = e < 1 ? ELMM_BO : e > nz ? ELMM_TO : -1;
+            if (zs >= 0 && !h.wall[zs] && (cf.TempBtype[zs] != ELMM_BC_CONSTFLUX || cf.sideTemp[zs] != 0))
+              return fail(ELMM_ERR_INVALID_ARG,
+                          "a body next to a side with a heat flux or a prescribed temperature and no wall-model points");
             int g[3];
             fold(a, b, e, g);
             if (solid[at(g[0], g[1], g[2])])
@@ -1842,11 +1848,6 @@ struct BatchT {
   int install_solids(int d, const elmm_solids *s) {
     Dom<T> &h = hdom[d];
     const elmm_config &c = cfg[d];
-    if (c.enable_buoyancy)  // the fill of the solid cells folds a side without wall-model points as adiabatic
-      for (int side : {ELMM_BO, ELMM_TO})
-        if (!h.wall[side] && (c.TempBtype[side] != ELMM_BC_CONSTFLUX || c.sideTemp[side] != 0))
-          return fail(ELMM_ERR_INVALID_ARG,
-                      "solid bodies with a temperature need an adiabatic side where there is no wall-model wall");
     if (!h.wall[SIDE_BO] || h.bt[SIDE_BO] != BC_NOSLIP)
       return fail(ELMM_ERR_INVALID_ARG, "solid bodies need the wall model on a no-slip bottom");
     const bool per[3] = {h.bt[SIDE_WE] == BC_PERIODIC, h.bt[SIDE_SO] == BC_PERIODIC, h.bt[SIDE_BO] == BC_PERIODIC};

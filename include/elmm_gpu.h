@@ -369,8 +369,9 @@ typedef struct elmm_solids {
  * (ELMM_ERR_INVALID_ARG otherwise): indices in range; no interpolation point
  * of a list is a forcing point of the same list; no forcing or nullified
  * point within one cell of a periodic boundary; a no-slip bottom wall with
- * the wall model; with a temperature an adiabatic side where there is no
- * wall-model wall, the Pr lists above as for passive scalars, the heated
+ * the wall model; with a temperature no body whose solid cells border the
+ * ghost cells of a side that has a heat flux or a prescribed temperature
+ * and no wall-model points, the Pr lists above as for passive scalars, the heated
  * faces' points (each body's heat flux, src/immersedboundary.f90:118, 267)
  * and the kept wall points.  After each
  * temperature stage the solid cells with fluid neighbours take the mean of
