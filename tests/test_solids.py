@@ -560,7 +560,8 @@ def test_temperature_among_boxes_under_a_ghost_rule_top(top):
     """A free-slip top without wall-model points that carries a heat flux or
     a prescribed temperature by CommonBase's ghost rules, above boxes that
     stay clear of it: FP64 against the oracle after 3 steps (U, V, W within
-    1e-11, P within 1e-10, theta - T_ref within 1e-11).  A body up to the
+    1e-11, P within 1e-10, theta - T_ref within 1e-11), the mixed path
+    within 1e-5 of FP64.  A body up to the
     top face is refused with ELMM_ERR_INVALID_ARG (its velocity points
     above the body lie outside the domain; the library also refuses a fill
     that would read the ghost cell of such a side)."""
@@ -578,6 +579,13 @@ def test_temperature_among_boxes_under_a_ghost_rule_top(top):
     et = rel(interior(d.field(FIELD_TEMPERATURE), -2, n) - 295.0, interior(o.get_field(FIELD_TEMPERATURE), -2, n) - 295.0)
     print("boxes under a", top, "top, FP64 vs oracle:", e, et)
     assert max(e[:3]) < 1e-11 and e[3] < 1e-10 and et < 1e-11, (e, et)
+    _, _, dm = _theta_pair(1, **kw)
+    dm.step(3)
+    em = [rel(a, b) for a, b in zip(interiors(g, *dm.download())[:3], interiors(g, *d.download())[:3])]
+    etm = rel(interior(dm.field(FIELD_TEMPERATURE), -2, n) - 295.0, interior(d.field(FIELD_TEMPERATURE), -2, n) - 295.0)
+    print("boxes under a", top, "top, mixed vs FP64:", em, etm)
+    assert max(em) < 1e-5 and etm < 1e-5, (em, etm)
+    dm.close()
     d.close()
     cfg = make_config(40, 36, 20, buoyancy=True, **kw)
     d = L.Domain(cfg)
