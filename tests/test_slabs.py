@@ -182,6 +182,43 @@ def test_slabs_carry_temperature_and_scalars(precision, split):
 
 
 @pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("bc", ["warm-surface", "heated-smooth", "flux-dirichlet-top"])
+def test_slabs_carry_temperature_boundaries(precision, bc):
+    """The temperature's boundary kinds on split domains: a prescribed
+    surface temperature at the rough bottom (the Monin-Obukhov Dirichlet
+    wall model on the bottom slab), a heat flux at a smooth bottom, and a
+    heat flux at the bottom under a Dirichlet top by the ghost rule (the top
+    slab's ghost plane).  Two slabs against the single domain after the
+    projection and three steps: FP64 U, V, W within 1e-12, P within 1e-11,
+    theta - T_ref within 1e-11; mixed within 1e-5."""
+    from gpu_elmm_b200.config import BC_CONSTFLUX, BC_DIRICHLET, FIELD_TEMPERATURE
+    from gpu_elmm_b200.workloads import interior, temperature_state
+    kw = {"warm-surface": dict(temperature_bc=((BC_DIRICHLET, 296.0), (BC_CONSTFLUX, 0.0))),
+          "heated-smooth": dict(heat_flux=(0.3, 0.0), z0=0.0),
+          "flux-dirichlet-top": dict(temperature_bc=((BC_CONSTFLUX, 0.2), (BC_DIRICHLET, 295.5)))}[bc]
+    cfg = make_config(*N, precision=precision, buoyancy=True, **kw)
+    g = grid_of(cfg)
+    st = log_profile_state(g, seed=9)
+    T0 = temperature_state(g, seed=9, amp=0.2)
+    a, b = L.Domain(cfg), L.Slabs(cfg, 2, devices=[0, 0])
+    for h in (a, b):
+        h.upload(*st)
+        h.upload_temperature(T0)
+    n = (g.Prnx, g.Prny, g.Prnz)
+    a.project(1.0)
+    b.project(1.0)
+    a.step(3)
+    b.step(3)
+    tol = (1e-12, 1e-11, 1e-11) if precision == 0 else (1e-5, 1e-5, 1e-5)
+    e = _errs(b.download(), a.download())
+    et = rel(interior(b.field(FIELD_TEMPERATURE), -2, n) - 295.0, interior(a.field(FIELD_TEMPERATURE), -2, n) - 295.0)
+    print("temperature boundaries, slabs vs single domain:", bc, precision, e, et)
+    assert max(e[:3]) < tol[0] and e[3] < tol[1] and et < tol[2], (e, et)
+    a.close()
+    b.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
 def test_slabs_carry_puffs_and_slices(precision):
     """A passive scalar with a puff that restarts and clears the field, a
     second puff volume in the other slab, and both time-averaged slices (the
