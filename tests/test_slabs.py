@@ -188,14 +188,16 @@ def test_slabs_carry_temperature_boundaries(precision, bc):
     surface temperature at the rough bottom (the Monin-Obukhov Dirichlet
     wall model on the bottom slab), a heat flux at a smooth bottom, and a
     heat flux at the bottom under a Dirichlet top by the ghost rule (the top
-    slab's ghost plane).  Two slabs against the single domain after the
+    slab's ghost plane), there with a passive scalar between a Neumann
+    bottom and a Dirichlet top.  Two slabs against the single domain after the
     projection and three steps: FP64 U, V, W within 1e-12, P within 1e-11,
     theta - T_ref within 1e-11; mixed within 1e-5."""
-    from gpu_elmm_b200.config import BC_CONSTFLUX, BC_DIRICHLET, FIELD_TEMPERATURE
-    from gpu_elmm_b200.workloads import interior, temperature_state
+    from gpu_elmm_b200.config import BC_CONSTFLUX, BC_DIRICHLET, BC_NEUMANN, FIELD_TEMPERATURE
+    from gpu_elmm_b200.workloads import interior, puff_state, temperature_state
     kw = {"warm-surface": dict(temperature_bc=((BC_DIRICHLET, 296.0), (BC_CONSTFLUX, 0.0))),
           "heated-smooth": dict(heat_flux=(0.3, 0.0), z0=0.0),
-          "flux-dirichlet-top": dict(temperature_bc=((BC_CONSTFLUX, 0.2), (BC_DIRICHLET, 295.5)))}[bc]
+          "flux-dirichlet-top": dict(temperature_bc=((BC_CONSTFLUX, 0.2), (BC_DIRICHLET, 295.5)), num_scalars=1,
+                                     scalar_bc=((BC_NEUMANN, -0.01), (BC_DIRICHLET, 0.5)))}[bc]
     cfg = make_config(*N, precision=precision, buoyancy=True, **kw)
     g = grid_of(cfg)
     st = log_profile_state(g, seed=9)
@@ -204,6 +206,8 @@ def test_slabs_carry_temperature_boundaries(precision, bc):
     for h in (a, b):
         h.upload(*st)
         h.upload_temperature(T0)
+        if cfg.num_scalars:
+            h.upload_scalar(1, puff_state(g, (20, 14, 12), sigma=3.0))
     n = (g.Prnx, g.Prny, g.Prnz)
     a.project(1.0)
     b.project(1.0)
@@ -214,6 +218,10 @@ def test_slabs_carry_temperature_boundaries(precision, bc):
     et = rel(interior(b.field(FIELD_TEMPERATURE), -2, n) - 295.0, interior(a.field(FIELD_TEMPERATURE), -2, n) - 295.0)
     print("temperature boundaries, slabs vs single domain:", bc, precision, e, et)
     assert max(e[:3]) < tol[0] and e[3] < tol[1] and et < tol[2], (e, et)
+    if cfg.num_scalars:
+        es = rel(interior(b.scalar(1), -2, n), interior(a.scalar(1), -2, n))
+        print("  scalar with a Neumann bottom and a Dirichlet top:", es)
+        assert es < tol[2], es
     a.close()
     b.close()
 
